@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark: frames/s of the 4096x4096, 50,000-path mixed scene.
+
+One step renders one full frame through the whole path (scan count, pool
+prefix + backdrop cumsum, emit, tile binning, coarse count/prefix/emit, fine)
+with the scene resident in HBM (`value`), and end to end through the C ABI
+with the scene in pinned host memory, its host->device copy and the RGBA8
+image readback inside every step (`e2e`).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tileink|reference]
+
+Multi-GPU: one process per GPU (torchrun); every rank renders its own frame
+(replicas, weak scaling); the time is the max over ranks.
+`--impl reference` times the reference path's CPU restatement (the oracle
+port; the reference itself is Rust + HLSL and cannot run here) on the host
+cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "4K 50k-path frames/s"
+UNIT = "frames/s"
+WORKLOAD = "4096x4096 canvas, 50,000 paths (60% fills / 40% round-join strokes), cubic+quadratic, " \
+           "200 Gaussian clusters sigma 300 px, nonzero/even-odd, solid/linear/radial paint, " \
+           "10% in clip layers nested <=4"
+SEED = 2
+CPU_SAMPLE_DIV = 16
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="tileink", choices=["tileink", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=5)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--paths", type=int, default=0, help="override the path count (smaller trial runs)")
+    p.add_argument("--size", type=int, default=0, help="override the canvas side (smaller trial runs)")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=5)
+        return False
+
+    def summary(self, fallback_max=1965.0):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": fallback_max, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else fallback_max,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def scene(size=0, paths=0, device_plan=True, seed=SEED):
+    import tileink_b200 as tk
+    return tk.generate(2, seed, width=size, height=size, paths=paths, device_segment_plan=device_plan)
+
+
+def cpu_baseline(size, paths):
+    """The oracle (CPU restatement of the reference path) on all host cores,
+    on 1/16 of the workload's paths over the same canvas; the frame time is
+    scaled by 16 (scan, coarse and fine work grow linearly with paths)."""
+    import oracle
+    n = max(1, (paths or 50000) // CPU_SAMPLE_DIV)
+    c = scene(size, n, device_plan=False, seed=SEED + 1)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    run = oracle.OracleRun(c.scene_desc(), threads=threads)
+    dt = time.perf_counter() - t0
+    stages = run.stage_times()
+    del run
+    est = dt * CPU_SAMPLE_DIV
+    return {"value": 1.0 / est, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"same generator, {n} paths (1/{CPU_SAMPLE_DIV}) on the {size or 4096}^2 canvas; "
+                      f"one full oracle frame took {dt:.2f} s, scaled x{CPU_SAMPLE_DIV}",
+            "sample_seconds": dt, "stage_seconds": stages}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle  # noqa: F401
+    n = max(1, (args.paths or 50000) // CPU_SAMPLE_DIV)
+    c = scene(args.size, n, device_plan=False, seed=SEED + 1)
+    d = c.scene_desc()
+    threads = os.cpu_count() or 1
+    import oracle as O
+    for _ in range(args.warmup):
+        O.OracleRun(d, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.OracleRun(d, threads=threads)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 1.0 / (dt * CPU_SAMPLE_DIV)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * CPU_SAMPLE_DIV * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "width": args.size or 4096, "height": args.size or 4096,
+                       "paths": args.paths or 50000, "sample_paths": n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"oracle port of the reference path, {n} paths (1/{CPU_SAMPLE_DIV}) per step, "
+                                       f"scaled x{CPU_SAMPLE_DIV}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_scene(canvas):
+    """Copy the recorded scene into pinned host buffers (page-locked, like a
+    caller that keeps its records in pinned memory)."""
+    import torch
+    from tileink_b200 import _native as N
+    arrays = canvas.scene_arrays()
+    pinned = {}
+    keep = []
+    for k, v in arrays.items():
+        if isinstance(v, np.ndarray) and v.nbytes:
+            t = torch.empty(v.nbytes, dtype=torch.uint8, pin_memory=True)
+            view = t.numpy().view(v.dtype)
+            view[...] = v
+            keep.append(t)
+            pinned[k] = view
+        else:
+            pinned[k] = v
+    s = N.ArrayScene(pinned)
+    s._keep = keep
+    bytes_in = sum(v.nbytes for v in pinned.values() if isinstance(v, np.ndarray))
+    return s, bytes_in
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import tileink_b200 as tk
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    t_gen = time.perf_counter()
+    canvas = scene(args.size, args.paths)
+    gen_s = time.perf_counter() - t_gen
+    r = tk.NativeRenderer(local)
+    r.upload(canvas)
+    stream = torch.cuda.ExternalStream(r.stream)
+    for _ in range(max(args.warmup, 3)):
+        r.render()
+    r.synchronize()
+    stats = r.stats()
+    r.set_timing(True)
+    stage_sum = {k: 0.0 for k in r.STAGE_NAMES}
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            r.render()
+            for k, v in r.stage_times().items():
+                stage_sum[k] += v
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    r.set_timing(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * 1000.0 / ms
+
+    # end to end: pinned host scene -> H2D -> frame -> D2H image, every step
+    ps, bytes_in = pinned_scene(canvas)
+    out = torch.empty(r.width * r.height * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint32)
+    r.upload(ps)
+    r.render()
+    r.readback(out)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.e2e_steps):
+        r.upload(ps)
+        r.render()
+        r.readback(out)
+    s1.record(stream)
+    s1.synchronize()
+    e2e_ms = s0.elapsed_time(s1) / args.e2e_steps
+    wall_ms = (time.perf_counter() - t0) * 1000.0 / args.e2e_steps
+    e2e_ms = max(e2e_ms, wall_ms)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    bytes_out = out.nbytes
+
+    # roofline of the dominant kernel
+    stage_ms = {k: v / args.steps for k, v in stage_sum.items()}
+    peaks = measured_peaks()
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    fp32_peak = r.probe_fp32_tflops()
+    T = stats["tiles"]
+    L, B, S = stats["lines"], stats["backdrop_len"], stats["segments"]
+    K, refs = stats["ptcl_records"], stats["tile_draw_refs"]
+    fills, visits = stats["fill_particles"], stats["segment_visits"]
+    algo = {
+        # bytes per launch (SURVEY-defined algorithmic traffic)
+        "scan_count": ("hbm", 24 * L + 4 * S),
+        "pool_scan": ("hbm", (4 + 4 + 8 + 4 + 4) * B),
+        "scan_emit": ("hbm", 24 * L + 20 * S),
+        "bins": ("hbm", 4 * refs),
+        "coarse_count": ("hbm", 12 * refs + 24 * T),
+        "coarse_emit": ("hbm", 12 * refs + 24 * K),
+        "fine": ("fp32", 256 * (24 * visits + 10 * fills)),
+    }
+    rooflines = {}
+    for name, (bound, amount) in algo.items():
+        t = stage_ms.get(name, 0.0)
+        if t <= 0:
+            continue
+        if bound == "hbm":
+            ach = amount / (t * 1e-3) / 1e9
+            rooflines[name] = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                               "frac": ach / hbm_peak, "ms": t, "algorithmic_bytes": amount}
+        else:
+            ach = amount / (t * 1e-3) / 1e12
+            rooflines[name] = {"bound": "fp32", "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                               "frac": ach / fp32_peak, "ms": t, "algorithmic_flops": amount}
+    dominant = max(rooflines, key=lambda k: rooflines[k]["ms"])
+    roof = dict(rooflines[dominant])
+    roof["kernel"] = dominant
+    roof["peak_source"] = ("measured FMA probe (tk_probe_fp32_tflops)" if roof["bound"] == "fp32"
+                           else "measured (MEASURED_PEAKS.json hbm_gbs)")
+    traffic_file = ROOT / "profiles" / "ncu_traffic.json"
+    roof["traffic"] = None
+    if traffic_file.exists():
+        try:
+            tr = json.loads(traffic_file.read_text())
+            roof["traffic"] = tr.get(dominant)
+        except Exception:
+            pass
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.size, args.paths)
+
+    launches_per_frame = 5 + 5 * stats["passes"]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, seed 2)",
+            "config": {"workload": WORKLOAD, "width": args.size or 4096, "height": args.size or 4096,
+                       "paths": args.paths or 50000, "parallelism": f"replicas x{world}",
+                       "l2": "inputs > L2 (lines %.1f GB), no flush" % (L * 24 / 1e9),
+                       "segment_plan": "device"},
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
+                    "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms},
+            "gpu_launches": launches_per_frame * args.steps,
+            "roofline": roof,
+            "stage_ms": stage_ms,
+            "rooflines": rooflines,
+            "counts": {"lines": L, "backdrop_tiles": B, "segments": S, "ptcl_records": K, "tile_draw_refs": refs,
+                       "fill_particles": fills, "segment_visits": visits, "tiles": T, "passes": stats["passes"]},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "scene_generation_s": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

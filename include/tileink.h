@@ -1,0 +1,355 @@
+/*
+ * tileink_b200 — C ABI of the B200-native tile rasterization path.
+ *
+ * This header is the drop-in boundary. It replaces, for the vector
+ * rasterization path, the reference's internal compute boundary:
+ *   - `ComputeBatch` + `Adapter::submit_compute` + `Receipt::readback`
+ *     (src/native/runtime/compute.rs:68-120,195,307; adapter.rs:159;
+ *      submission.rs:120), and
+ *   - the public wrapper `NativeRenderer::render_to_image`
+ *     (src/native/renderer.rs:177-190).
+ * A thin Rust FFI crate binds these symbols with `#[repr(C)]` mirrors of the
+ * records below; the records are byte-identical to the reference's Pod types,
+ * so a `Canvas` can hand its vectors over unchanged.
+ *
+ * Conventions (all entry points):
+ *   - every call returns an int32 status: 0 = ok, negative = error
+ *     (TK_E_*); `tk_last_error(ctx)` returns the message of the last failure;
+ *   - no C++ exception crosses this ABI;
+ *   - a context is used by one host thread at a time (the reference's
+ *     `Rc<RefCell<..>>` runtime is `!Send` for the same reason);
+ *   - host pointers passed in are borrowed for the duration of the call only;
+ *     outputs go to caller-allocated buffers.
+ */
+#ifndef TILEINK_B200_H
+#define TILEINK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Algorithm constants (src/shaders/hlsl/constants.hlsli:7-19).              */
+/* ------------------------------------------------------------------------ */
+#define TK_TILE_SIZE 16u
+#define TK_TILE_PIXELS (TK_TILE_SIZE * TK_TILE_SIZE)
+#define TK_INVALID_INDEX 0xFFFFFFFFu
+#define TK_SHARED_BLUR_MAX_RADIUS 16u
+
+/* Draw tags (src/shared/draw_record.rs:7-17, shaders/hlsl/shared/draw_tags.hlsli) */
+#define TK_DRAW_BRUSH 0u
+#define TK_DRAW_CLIP 1u
+#define TK_DRAW_OPACITY 2u
+#define TK_DRAW_BLEND 3u
+#define TK_DRAW_ISOLATE 4u
+#define TK_DRAW_PATH_GLYPH 5u
+
+/* Layer stack tags (shaders/hlsl/shared/draw_tags.hlsli:7-9) */
+#define TK_LAYER_CLIP 0u
+#define TK_LAYER_OPACITY 1u
+#define TK_LAYER_BLEND 2u
+
+/* Fill rules (src/shared/fill.rs:1-6) */
+#define TK_FILL_NONZERO 0u
+#define TK_FILL_EVEN_ODD 1u
+
+/* PTCL tags (shaders/hlsl/shared/particle_tags.hlsli:3-16). */
+#define TK_PTCL_END 0u
+#define TK_PTCL_FILL 1u
+#define TK_PTCL_COLOR 2u
+#define TK_PTCL_BEGIN_CLIP 3u
+#define TK_PTCL_END_CLIP 4u
+#define TK_PTCL_BEGIN_OPACITY 5u
+#define TK_PTCL_END_OPACITY 6u
+#define TK_PTCL_BEGIN_BLEND 7u
+#define TK_PTCL_END_BLEND 8u
+#define TK_PTCL_SDF 9u
+#define TK_PTCL_GLYPH 10u
+#define TK_PTCL_PATH_GLYPH 11u
+#define TK_PTCL_BEGIN_SDF_CLIP 12u
+#define TK_PTCL_IMAGE 13u
+/* Merged-stream extension (no reference counterpart). All draw batches of a
+ * target pass share one PTCL stream per tile; each batch with particles in
+ * the tile opens its section with BATCH_BEGIN {segment_start = batch id,
+ * segment_end = record count of the section, color = tile kind | skip << 3
+ * of that batch}, followed by the reference's batch stream without its END;
+ * one END closes the tile. Fine stores the pixel to RGBA8 and reloads it at
+ * each BATCH_BEGIN (the reference's per-batch target store/load) and resets
+ * the clip/group state. */
+#define TK_PTCL_BATCH_BEGIN 14u
+
+/* Tile kinds (shaders/hlsl/shared/tile_kinds.hlsli:3-11) */
+#define TK_TILE_KIND_INTERPRETER 0u
+#define TK_TILE_KIND_EMPTY 1u
+#define TK_TILE_KIND_COLOR 2u
+#define TK_TILE_KIND_MASK 7u
+#define TK_TILE_PREFIX_SHIFT 3u
+
+/* Brush blob layout (shaders/hlsl/shared/brush/constants.hlsli:3-22,
+ * src/shared/brush.rs:249-340). A brush record is a 9-word header followed by
+ * 12 parameter words and an optional payload (gradient ramp). */
+#define TK_BRUSH_HEADER_WORDS 9u
+#define TK_BRUSH_PARAM_WORDS 12u
+#define TK_BRUSH_SOLID 1u
+#define TK_BRUSH_LINEAR 2u
+#define TK_BRUSH_RADIAL 3u
+#define TK_BRUSH_COLOR_WORD 4u
+#define TK_EXTEND_PAD 0u
+#define TK_EXTEND_REPEAT 1u
+#define TK_EXTEND_REFLECT 2u
+
+/* ------------------------------------------------------------------------ */
+/* Records. Layouts equal the reference's #[repr(C)] Pod types.              */
+/* ------------------------------------------------------------------------ */
+
+/* GpuAffine (src/shared/affine.rs:5-18): (x,y) -> (a x + c y + e, b x + d y + f) */
+typedef struct tk_affine {
+    float a, b, c, d, e, f;
+} tk_affine; /* 24 B */
+
+/* Line (src/shared/line.rs:1-9) */
+typedef struct tk_line {
+    uint32_t path_id;
+    float pad;
+    float p0[2];
+    float p1[2];
+} tk_line; /* 24 B */
+
+/* PathRecord (src/shared/path.rs:4-23; offsets scene_records.hlsli:5-19) */
+typedef struct tk_path_record {
+    uint32_t path_id;
+    uint32_t line_count;
+    uint32_t line_start;
+    uint32_t flags;
+    uint32_t data_offset;  /* first word of the path's backdrop slice */
+    uint32_t data_len;     /* bbox tile count */
+    uint32_t tile_x0, tile_y0, tile_x1, tile_y1;
+    uint32_t segment_start;
+    uint32_t segment_capacity;
+    uint32_t segment_count;
+    tk_affine transform;
+} tk_path_record; /* 76 B */
+
+/* PixelBounds (src/shared/bounds.rs:76-83) */
+typedef struct tk_pixel_bounds {
+    int32_t x0, y0, x1, y1;
+} tk_pixel_bounds;
+
+/* DrawRecord (src/shared/draw_record.rs:51-81; offsets draw_records.hlsli:5-17) */
+typedef struct tk_draw_record {
+    uint32_t path_id;
+    uint32_t glyph_run_id;
+    uint32_t sdf_offset;
+    uint32_t sdf_len;
+    uint32_t sdf_shadow_offset;
+    uint32_t sdf_shadow_len;
+    uint32_t brush_offset;
+    uint32_t brush_len;
+    uint32_t tag;
+    uint32_t fill_rule;
+    tk_pixel_bounds pixel_bounds;
+    tk_pixel_bounds local_pixel_bounds;
+    uint32_t solid_rect;
+    tk_affine transform;
+    tk_affine inverse_transform;
+} tk_draw_record; /* 124 B */
+
+/* LayerStackRecord (src/shared/gpu_coarse.rs:47-53) */
+typedef struct tk_layer_record {
+    uint32_t tag;
+    uint32_t draw;
+    uint32_t payload;
+} tk_layer_record; /* 12 B */
+
+/* PtclRecord (src/shared/gpu_coarse.rs:55-65) */
+typedef struct tk_ptcl_record {
+    uint32_t tag;
+    int32_t backdrop;
+    uint32_t fill_rule;
+    uint32_t segment_start;
+    uint32_t segment_end;
+    uint32_t color;
+} tk_ptcl_record; /* 24 B */
+
+/* LineSegment (src/shared/line_seg.rs:1-9): tile-local clipped segment */
+typedef struct tk_line_segment {
+    float p0x, p0y, p1x, p1y, y_edge;
+} tk_line_segment; /* 20 B */
+
+/* TileSegmentRange (src/shared/tile_seg_range.rs:1-6) */
+typedef struct tk_segment_range {
+    uint32_t start, end;
+} tk_segment_range; /* 8 B */
+
+/* TileCoarseRecord (src/shared/gpu_coarse.rs:1-10) */
+typedef struct tk_tile_record {
+    uint32_t ptcl_count, ptcl_start, ptcl_end;
+    uint32_t glyph_count, glyph_start, glyph_end;
+} tk_tile_record; /* 24 B */
+
+/* Linearised execution plan (the reference's ExecPlan ops,
+ * src/shared/execution.rs:98-124). DRAW_BATCH renders one batch into the
+ * current target; BLUR_BEGIN opens a transparent offscreen surface for the
+ * ops that follow (OffscreenLayer::Filter{Blur}); BLUR_END blurs it
+ * horizontally then vertically inside `bounds` and composites it src-over
+ * onto the enclosing target (render/filter_program/blur.rs:194-245,
+ * shared/composite_stack.hlsli:11-28). */
+#define TK_OP_DRAW_BATCH 0u
+#define TK_OP_BLUR_BEGIN 1u
+#define TK_OP_BLUR_END 2u
+typedef struct tk_op {
+    uint32_t kind;
+    uint32_t batch_id;     /* DRAW_BATCH: draw_batch_ids value of its draws */
+    uint32_t layer_start;  /* DRAW_BATCH: fused layer stack range */
+    uint32_t layer_end;
+    float sigma;           /* BLUR_BEGIN: physical standard deviation */
+    int32_t bounds[4];     /* BLUR_BEGIN: output bounds x0,y0,x1,y1 (children's
+                              paint bounds outset by ceil(3 sigma)) */
+} tk_op; /* 36 B */
+
+/* Scene flags */
+#define TK_SCENE_SEGMENTS_FROM_DEVICE 1u /* recompute segment_start on device */
+
+typedef struct tk_scene_desc {
+    uint32_t width, height;   /* physical canvas size in pixels */
+    uint32_t clear_color;     /* premultiplied RGBA8 (set_clear_color) */
+    uint32_t flags;
+    const tk_line* lines;
+    uint64_t line_count;
+    const tk_path_record* paths;
+    uint32_t path_count;
+    uint32_t draw_count;
+    const tk_draw_record* draws;
+    const uint32_t* brush_blob;
+    uint64_t brush_word_count;
+    const tk_layer_record* layers;
+    uint32_t layer_count;
+    uint32_t draw_order_count;
+    const uint32_t* draw_order;      /* painter order of drawn draws */
+    const uint32_t* draw_batch_ids;  /* per draw; TK_INVALID_INDEX = hidden */
+    const tk_op* ops;
+    uint32_t op_count;
+    uint32_t reserved;
+} tk_scene_desc;
+
+/* Per-scene counts measured by the device pipeline. */
+typedef struct tk_stats {
+    uint64_t lines;          /* L */
+    uint64_t backdrop_len;   /* B: sum of path bbox tiles */
+    uint64_t segments;       /* S: tile segments emitted */
+    uint64_t ptcl_records;   /* K: PTCL records over all target passes */
+    uint64_t tile_draw_refs; /* sum over draws of bbox tiles */
+    uint64_t fill_particles; /* fill-like PTCL records */
+    uint64_t segment_visits; /* sum over fill records of segment counts */
+    uint32_t passes;         /* coarse+fine passes (target segments) */
+    uint32_t tiles;          /* T */
+} tk_stats;
+
+/* Status codes */
+#define TK_OK 0
+#define TK_E_INVALID -1
+#define TK_E_CAPACITY -2
+#define TK_E_CUDA -3
+#define TK_E_TIMEOUT -4
+#define TK_E_STATE -5
+#define TK_E_ALLOC -6
+
+typedef struct tk_ctx tk_ctx;
+
+/* Library version string. */
+const char* tk_version(void);
+
+/* Context on CUDA device `device` with its own stream. */
+int32_t tk_ctx_create(int32_t device, tk_ctx** out);
+void tk_ctx_destroy(tk_ctx* ctx);
+const char* tk_last_error(const tk_ctx* ctx);
+/* The context's cudaStream_t (as void*), for callers that order their work. */
+void* tk_ctx_stream(tk_ctx* ctx);
+int32_t tk_synchronize(tk_ctx* ctx);
+
+/* Copy a recorded scene to the device and validate it (replaces the
+ * reference's per-frame record upload, native/runtime/renderer.rs:91-112).
+ * Host records are copied; the caller may free them after the call. */
+int32_t tk_scene_upload(tk_ctx* ctx, const tk_scene_desc* scene);
+
+/* Enqueue the whole frame on the context stream: scan (count, prefix,
+ * cumsum, emit), tile binning, and per target pass coarse + fine, with blur
+ * layers (replaces frame::record, native/runtime/renderer/frame.rs:6-80). */
+int32_t tk_render(tk_ctx* ctx);
+
+/* Wait for the frame and copy the premultiplied RGBA8 image
+ * (NativeImageSubmission::readback, src/native/submission.rs:120). */
+int32_t tk_readback(tk_ctx* ctx, uint32_t* rgba8, size_t pixel_count);
+
+/* upload + render + readback in one call
+ * (NativeRenderer::render_to_image, src/native/renderer.rs:177-190). */
+int32_t tk_render_to_image(tk_ctx* ctx, const tk_scene_desc* scene,
+                           uint32_t* rgba8, size_t pixel_count);
+
+int32_t tk_get_stats(tk_ctx* ctx, tk_stats* out);
+
+/* Debug readback of an intermediate buffer for parity tests. `index`
+ * selects the target pass for PTCL/TILES/KINDS. When `dst` is NULL only
+ * `*needed` (bytes) is written. */
+#define TK_STAGE_COUNTS 0u     /* u32[B] segment tile counts */
+#define TK_STAGE_BACKDROPS 1u  /* i32[B] after row cumsum */
+#define TK_STAGE_RANGES 2u     /* tk_segment_range[B] */
+#define TK_STAGE_SEGMENTS 3u   /* tk_line_segment[segment total] */
+#define TK_STAGE_PTCL 4u       /* tk_ptcl_record[] of pass `index` */
+#define TK_STAGE_TILES 5u      /* tk_tile_record[T] of pass `index` */
+#define TK_STAGE_KINDS 6u      /* u32[T] tile kind words of pass `index` */
+#define TK_STAGE_IMAGE 7u      /* u32[W*H] current target image */
+#define TK_STAGE_PATHS 8u      /* tk_path_record[P] (segment plan applied) */
+int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
+                          void* dst, size_t bytes, size_t* needed);
+
+/* Stage timing with CUDA events recorded on the context stream around each
+ * stage of tk_render (no reference counterpart; measurement support).
+ * Stages: 0 pool clear, 1 scan_count, 2 pool prefix + cumsum, 3 scan_emit,
+ * 4 tile binning, 5 coarse count + tile prefix, 6 coarse emit, 7 fine,
+ * 8 blur + composite. Times are summed over the passes of the last frame. */
+#define TK_TIMED_STAGES 9u
+int32_t tk_set_timing(tk_ctx* ctx, int32_t enabled);
+int32_t tk_get_stage_times(tk_ctx* ctx, float* ms, uint32_t count);
+
+/* FP32 FMA throughput of the device in TFLOP/s, measured by a short
+ * register-resident FMA loop (the fine stage's roofline denominator). */
+int32_t tk_probe_fp32_tflops(tk_ctx* ctx, double* tflops);
+
+/* ------------------------------------------------------------------------ */
+/* Stage harnesses on host buffers (the reference's per-kernel GPU test      */
+/* harnesses, src/native/runtime/tests/scan_cases.rs:8-213 and               */
+/* tests/shared_blur_gpu.rs:9-155).                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Per path p: ranges[t] over [data_offset, data_offset+data_len) is the
+ * exclusive/inclusive prefix of counts starting at segment_start (wrapping
+ * u32); cursors[t] = ranges[t].start; bumps[p] = path total. Elements outside
+ * every path slice are left as given. (scan/prefix_chunks.hlsl:16-38,
+ * scan/chunk_offsets.hlsl:14-26, scan/apply_chunk_offsets.hlsl:15-27) */
+int32_t tk_stage_scan_prefix(tk_ctx* ctx, const uint32_t* counts, uint64_t pool_len,
+                             const tk_path_record* paths, uint32_t path_count,
+                             tk_segment_range* ranges, uint32_t* cursors,
+                             uint32_t* bumps);
+
+/* scan_count on the given lines/paths (scan/count.hlsl:13-40). `backdrops`
+ * and `counts` are read, accumulated into and written back. */
+int32_t tk_stage_scan_count(tk_ctx* ctx, const tk_line* lines, uint64_t line_count,
+                            const tk_path_record* paths, uint32_t path_count,
+                            int32_t* backdrops, uint32_t* counts, uint64_t pool_len);
+
+/* One separable blur pass over an RGBA8 image (filter/blur_shared.hlsl:15-74,
+ * filter/blur.hlsl:10-17). Pixels outside `region` keep `dst`'s contents;
+ * samples outside `source` (x0,y0,x1,y1; empty = region) are transparent. */
+int32_t tk_stage_blur(tk_ctx* ctx, const uint32_t* src, uint32_t* dst,
+                      uint32_t width, uint32_t height, const uint32_t region[4],
+                      const uint32_t source[4], float sigma, uint32_t axis);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILEINK_B200_H */

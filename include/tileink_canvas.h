@@ -1,0 +1,111 @@
+/*
+ * tileink_b200 — host-side scene recording (the reference's `Canvas`).
+ *
+ * Mirrors the recording API of the reference's Canvas for the vector path:
+ *   push_path            src/canvas/primitives/paths.rs:50-60 -> canvas/paths.rs:42-156
+ *   push_stroke          src/canvas/primitives/paths.rs:24-48
+ *   push_clip_layer      src/canvas/layers.rs:7-28
+ *   push_blur_group      src/canvas/layers.rs:205-212
+ *   pop_layer            src/canvas/layers.rs
+ * and its compilation into draw batches (src/canvas/compile.rs:39-331,
+ * src/shared/execution/batches.rs). `tk_canvas_scene` exposes the recorded
+ * records as a tk_scene_desc for tk_scene_upload / tk_render_to_image.
+ *
+ * Flattening uses the project's own flattener (quadratic flattening by the
+ * parabola-integral method, cubics first approximated by quadratics); the
+ * reference delegates this to the kurbo crate (0.13.1).
+ */
+#ifndef TILEINK_B200_CANVAS_H
+#define TILEINK_B200_CANVAS_H
+
+#include "tileink.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tk_canvas tk_canvas;
+typedef struct tk_path tk_path;
+
+/* Path builder (kurbo::BezPath, f64 coordinates). */
+tk_path* tk_path_new(void);
+void tk_path_free(tk_path* p);
+void tk_path_move_to(tk_path* p, double x, double y);
+void tk_path_line_to(tk_path* p, double x, double y);
+void tk_path_quad_to(tk_path* p, double x1, double y1, double x2, double y2);
+void tk_path_cubic_to(tk_path* p, double x1, double y1, double x2, double y2, double x3, double y3);
+void tk_path_close(tk_path* p);
+
+/* Flatten a path into lines (PathFlatten::flatten, src/shared/path_flatten.rs:20-82).
+ * Returns the number of lines; writes at most `cap` into `out`. */
+uint64_t tk_path_flatten(const tk_path* p, float tolerance, uint32_t path_id, tk_line* out, uint64_t cap);
+
+/* Brushes. Colors are straight (unpremultiplied) sRGB RGBA in [0,1]. */
+#define TK_BRUSH_KIND_SOLID 0u
+#define TK_BRUSH_KIND_LINEAR 1u
+#define TK_BRUSH_KIND_RADIAL 2u
+typedef struct tk_gradient_stop {
+    float offset;
+    float rgba[4];
+} tk_gradient_stop;
+typedef struct tk_brush_desc {
+    uint32_t kind;
+    uint32_t extend;        /* TK_EXTEND_* */
+    float rgba[4];          /* SOLID */
+    float p0[2], p1[2];     /* LINEAR start/end; RADIAL start/end centers */
+    float r0, r1;           /* RADIAL radii */
+    uint32_t stop_count;
+    const tk_gradient_stop* stops;
+} tk_brush_desc;
+
+/* Canvas with logical size and scale factor (Canvas::new, canvas/surface.rs:16-21). */
+tk_canvas* tk_canvas_new(uint32_t logical_width, uint32_t logical_height, float scale);
+void tk_canvas_free(tk_canvas* c);
+/* When set (default), segment capacities are planned on the host with the
+ * scan-line planner at record time (canvas/storage.rs:131-142); otherwise the
+ * scene asks the device to plan them (TK_SCENE_SEGMENTS_FROM_DEVICE). */
+void tk_canvas_set_host_segment_plan(tk_canvas* c, int32_t enabled);
+void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul_rgba8);
+
+/* transform: 6 coefficients [a b c d e f] or NULL for identity. Returns the
+ * draw index, or -1 on error. */
+int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
+                            const double* transform, uint32_t fill_rule, double tolerance);
+int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
+                              double width, const double* transform, double tolerance);
+int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
+                                  uint32_t fill_rule, double tolerance);
+int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);
+int32_t tk_canvas_pop_layer(tk_canvas* c);
+
+/* Compile (if needed) and describe the recorded scene. Pointers stay valid
+ * until the canvas is modified or freed. */
+int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out);
+
+/* Seeded synthetic workloads. `config`: 1 = 640x360 240 cubic fills;
+ * 2 = 4096x4096 50k mixed fills/strokes/gradients/clips; 3 = 1920x1080 20k
+ * quadratic glyphs; 4 = one scene of the uneven batch (index = `variant`);
+ * 5 = 1024x1024 256 cubic paths inside a sigma-4 blur group. Zero fields in
+ * `overrides` keep the workload's defaults. */
+typedef struct tk_gen_params {
+    uint32_t width, height;   /* canvas size */
+    uint32_t paths;           /* path / glyph count */
+    uint32_t variant;         /* config 4: scene index */
+    float sigma;              /* config 5: blur sigma */
+    float jitter;             /* config 5: control point jitter (px) */
+    uint32_t flags;           /* 1: host segment planning off */
+    uint32_t reserved;
+} tk_gen_params;
+tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_params* overrides);
+
+/* Differentiable parameters of configs 1 and 5 (fills of cubic paths with
+ * solid colors): control points per path element and straight RGBA colors.
+ * Returns the number of floats of each array when the pointer is NULL. */
+uint64_t tk_canvas_param_points(const tk_canvas* c, double* out);  /* all path points, x,y */
+uint64_t tk_canvas_param_colors(const tk_canvas* c, float* out);   /* per draw straight RGBA */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILEINK_B200_CANVAS_H */

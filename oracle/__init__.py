@@ -1,0 +1,93 @@
+"""Oracle loader: CPU restatement of the reference's rasterization path.
+
+TEST INFRASTRUCTURE ONLY. Only tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg import this package, and only to check or time the CUDA
+path; the product (tileink_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+
+OR_COUNTS, OR_BACKDROPS, OR_RANGES, OR_SEGMENTS = 0, 1, 2, 3
+OR_BATCH_PTCL, OR_BATCH_TILES, OR_BATCH_KINDS, OR_IMAGE = 4, 5, 6, 7
+OR_PASS_PTCL, OR_PASS_TILES, OR_PASS_KINDS, OR_PATHS, OR_BUMPS = 8, 9, 10, 11, 12
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists() or LIB.stat().st_mtime < (HERE / "oracle.cpp").stat().st_mtime:
+            build()
+        l = C.CDLL(str(LIB))
+        P, U32, U64, I32, F32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
+        l.or_run.restype = I32
+        l.or_run.argtypes = [P, I32, U32, U32, C.POINTER(P)]
+        l.or_free.argtypes = [P]
+        l.or_error.restype = C.c_char_p
+        l.or_get.restype = C.c_size_t
+        l.or_get.argtypes = [P, U32, U32, P, C.c_size_t]
+        l.or_batch_count.restype = U32
+        l.or_batch_count.argtypes = [P]
+        l.or_pass_count.restype = U32
+        l.or_pass_count.argtypes = [P]
+        l.or_stage_times.argtypes = [P, P]
+        l.or_line_scanned_tile_count.restype = U32
+        l.or_line_scanned_tile_count.argtypes = [P, U32, U32, U32, U32]
+        l.or_scan_count.argtypes = [P, U64, P, U32, P, P]
+        l.or_scan_prefix.argtypes = [P, P, U32, P, P, P]
+        l.or_blur_pass.argtypes = [P, P, U32, U32, P, P, F32, U32]
+        l.or_fill_value.restype = F32
+        l.or_fill_value.argtypes = [P, U32, I32, U32, U32]
+        _lib = l
+    return _lib
+
+
+class OracleRun:
+    """Result of the reference frame restated on the CPU."""
+
+    def __init__(self, desc, threads: int = 1, tile_rows=(0, 0)):
+        self._l = lib()
+        h = C.c_void_p()
+        rc = self._l.or_run(C.byref(desc), int(threads), int(tile_rows[0]), int(tile_rows[1]), C.byref(h))
+        if rc != 0:
+            raise RuntimeError("oracle: " + self._l.or_error().decode())
+        self._h = h.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._l.or_free(self._h)
+            self._h = None
+
+    def get(self, what: int, dtype, index: int = 0) -> np.ndarray:
+        n = self._l.or_get(self._h, what, index, None, 0)
+        out = np.zeros(n // np.dtype(dtype).itemsize, dtype=dtype)
+        if n:
+            self._l.or_get(self._h, what, index, out.ctypes.data, n)
+        return out
+
+    @property
+    def batch_count(self) -> int:
+        return self._l.or_batch_count(self._h)
+
+    @property
+    def pass_count(self) -> int:
+        return self._l.or_pass_count(self._h)
+
+    def stage_times(self) -> list:
+        t = (C.c_double * 7)()
+        self._l.or_stage_times(self._h, t)
+        return list(t)

@@ -1,0 +1,1326 @@
+// Oracle: CPU restatement of the reference's tile rasterization path.
+// TEST INFRASTRUCTURE ONLY (see oracle.h). Built with -ffp-contract=off.
+#include "oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_error;
+
+// ---------------------------------------------------------------------------
+// f32 semantics of the reference shaders.
+// ---------------------------------------------------------------------------
+inline float fmin_(float a, float b) { return std::fmin(a, b); }
+inline float fmax_(float a, float b) { return std::fmax(a, b); }
+inline float clampf(float x, float lo, float hi) { return fmin_(fmax_(x, lo), hi); }
+inline float mad(float a, float b, float c) { return std::fma(a, b, c); }
+// HLSL round() is round-half-to-even (DXIL Round_ne).
+inline float round_ne(float x) { return std::nearbyint(x); }
+// float -> uint / int conversions saturate (NaN -> 0).
+inline uint32_t f2u(float x) {
+    if (!(x > 0.0f)) return 0u;
+    if (x >= 4294967296.0f) return 0xFFFFFFFFu;
+    return (uint32_t)x;
+}
+inline int32_t f2i(float x) {
+    if (x != x) return 0;
+    if (x >= 2147483648.0f) return 0x7FFFFFFF;
+    if (x <= -2147483648.0f) return (int32_t)0x80000000;
+    return (int32_t)x;
+}
+inline float bits_f(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline uint32_t f_bits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+
+const float SCAN_EPSILON = 1.0e-6f;
+const float TOP_TOUCH_EPSILON = 1.0e-12f;
+const float TILE_CLIP_NUDGE = 1.0e-3f;
+const float CHANNEL_SCALE = 1.0f / 255.0f;
+
+// --- shared/pixel.hlsli:7-66 -------------------------------------------------
+struct F4 { float r, g, b, a; };
+inline uint32_t coverage_to_u8(float c) { return f2u(clampf(c, 0.0f, 1.0f) * 255.0f + 0.5f); }
+inline uint32_t coverage_to_alpha(float v, uint32_t rule) {
+    float alpha = fmin_(std::fabs(v), 1.0f);
+    if (rule == 1u) alpha = std::fabs(v - 2.0f * round_ne(0.5f * v));
+    return coverage_to_u8(alpha);
+}
+inline float signum_f32(float v) { return v < 0.0f ? -1.0f : 1.0f; }
+inline uint32_t pack(uint32_t r, uint32_t g, uint32_t b, uint32_t a) { return r | (g << 8) | (b << 16) | (a << 24); }
+inline uint32_t unorm_to_rgba8(F4 p) {
+    return pack(f2u(clampf(p.r * 255.0f + 0.5f, 0.0f, 255.0f)), f2u(clampf(p.g * 255.0f + 0.5f, 0.0f, 255.0f)),
+                f2u(clampf(p.b * 255.0f + 0.5f, 0.0f, 255.0f)), f2u(clampf(p.a * 255.0f + 0.5f, 0.0f, 255.0f)));
+}
+inline F4 rgba8_to_unorm(uint32_t p) {
+    return {float(p & 255u) * CHANNEL_SCALE, float((p >> 8) & 255u) * CHANNEL_SCALE,
+            float((p >> 16) & 255u) * CHANNEL_SCALE, float(p >> 24) * CHANNEL_SCALE};
+}
+inline uint32_t mul_div255(uint32_t a, uint32_t b) { uint32_t p = a * b + 128u; return (p + (p >> 8)) >> 8; }
+inline uint32_t combine_alpha(uint32_t a, uint32_t b) { return mul_div255(a, b); }
+inline uint32_t scale_premul_u8(uint32_t s, uint32_t f) {
+    if (f == 0u) return 0u;
+    if (f == 255u) return s;
+    return pack(mul_div255(s & 255u, f), mul_div255((s >> 8) & 255u, f), mul_div255((s >> 16) & 255u, f),
+                mul_div255(s >> 24, f));
+}
+inline F4 scale_premul_u8_to_unorm(uint32_t s, uint32_t f) {
+    if (f == 0u || (s >> 24) == 0u) return {0, 0, 0, 0};
+    float scale = float(f) * (1.0f / 65025.0f);
+    return {float(s & 255u) * scale, float((s >> 8) & 255u) * scale, float((s >> 16) & 255u) * scale,
+            float(s >> 24) * scale};
+}
+inline uint32_t src_over_premul_u8(uint32_t d, uint32_t s) {
+    uint32_t a = s >> 24;
+    if (a == 0u) return d;
+    if (a == 255u) return s;
+    uint32_t inv = 255u - a;
+    return pack((s & 255u) + mul_div255(d & 255u, inv), ((s >> 8) & 255u) + mul_div255((d >> 8) & 255u, inv),
+                ((s >> 16) & 255u) + mul_div255((d >> 16) & 255u, inv), a + mul_div255(d >> 24, inv));
+}
+inline F4 src_over_premul_unorm(F4 d, F4 s) {
+    if (s.a <= 0.0f) return d;
+    if (s.a >= 1.0f) return s;
+    float k = 1.0f - s.a;
+    return {s.r + d.r * k, s.g + d.g * k, s.b + d.b * k, s.a + d.a * k};
+}
+inline uint32_t lerp_premul_u8(uint32_t a, uint32_t b, float t) {
+    uint32_t out = 0;
+    for (int c = 0; c < 4; ++c) {
+        float l = float((a >> (8 * c)) & 255u), r = float((b >> (8 * c)) & 255u);
+        out |= f2u(clampf(mad(r - l, t, l) + 0.5f, 0.0f, 255.0f)) << (8 * c);
+    }
+    return out;
+}
+inline float rem_euclid_f32(float v, float m) { return mad(-std::floor(v / m), m, v); }
+inline bool premul_u8_is_opaque(uint32_t p) { return (p >> 24) == 255u; }
+// RGBA8 UNORM render-target texel conversions.
+inline float unorm8_load(uint32_t k) { return float(k) / 255.0f; }
+inline F4 texel_load(uint32_t p) {
+    return {unorm8_load(p & 255u), unorm8_load((p >> 8) & 255u), unorm8_load((p >> 16) & 255u), unorm8_load(p >> 24)};
+}
+inline uint32_t unorm8_store(float x) { return (uint32_t)std::nearbyint(clampf(x, 0.0f, 1.0f) * 255.0f); }
+inline uint32_t texel_store(F4 p) { return pack(unorm8_store(p.r), unorm8_store(p.g), unorm8_store(p.b), unorm8_store(p.a)); }
+
+// ---------------------------------------------------------------------------
+// Scan traversal (scan/geometry.hlsli:12-114).
+// ---------------------------------------------------------------------------
+struct Scan {
+    uint32_t bx0, by0, bx1, by1;
+    uint32_t data_offset;
+    float qx0, qy0, qx1, qy1;  // sorted points (upper first)
+    bool down;
+    uint32_t count;
+    float a, b, sign, x0, y0;
+    uint32_t imin, imax;
+    int32_t ymin, ymax;
+};
+
+inline bool is_tile_boundary_y(float v) { return std::fabs(v - std::floor(v)) <= TOP_TOUCH_EPSILON; }
+inline int32_t ceil_tile_boundary_y(float v) {
+    if (is_tile_boundary_y(v)) return f2i(std::floor(v));
+    return f2i(std::ceil(v));
+}
+inline uint32_t span(float a, float b) {
+    float hi = std::ceil(a);
+    if (b > a) hi = std::ceil(b);
+    float lo = std::floor(a);
+    if (b < a) lo = std::floor(b);
+    float v = hi - lo;
+    if (v < 1.0f) v = 1.0f;
+    return f2u(v);
+}
+
+bool scan_geometry(const tk_line& line, const tk_path_record* paths, uint32_t path_count, Scan& s) {
+    s = Scan{};
+    uint32_t pid = line.path_id;
+    if (pid >= path_count) return false;
+    const tk_path_record& p = paths[pid];
+    s.bx0 = p.tile_x0; s.by0 = p.tile_y0; s.bx1 = p.tile_x1; s.by1 = p.tile_y1;
+    s.data_offset = p.data_offset;
+    if (s.bx1 - s.bx0 == 0u || s.by0 >= s.by1) return false;
+    const tk_affine& t = p.transform;
+    float p0x = t.a * line.p0[0] + t.c * line.p0[1] + t.e;
+    float p0y = t.b * line.p0[0] + t.d * line.p0[1] + t.f;
+    float p1x = t.a * line.p1[0] + t.c * line.p1[1] + t.e;
+    float p1y = t.b * line.p1[0] + t.d * line.p1[1] + t.f;
+    s.down = p1y >= p0y;
+    if (s.down) { s.qx0 = p0x; s.qy0 = p0y; s.qx1 = p1x; s.qy1 = p1y; }
+    else { s.qx0 = p1x; s.qy0 = p1y; s.qx1 = p0x; s.qy1 = p0y; }
+    const float ts = 1.0f / float(TK_TILE_SIZE);
+    float sx = s.qx0 * ts, sy = s.qy0 * ts, sz = s.qx1 * ts, sw = s.qy1 * ts;
+    uint32_t count_x = span(sx, sz) - 1u;
+    s.count = count_x + span(sy, sw);
+    float dx = std::fabs(sz - sx);
+    float dy = sw - sy;
+    if (dx + dy == 0.0f || (dy == 0.0f && std::floor(sy) == sy)) return false;
+    float rcp = 1.0f / (dx + dy);
+    s.a = dx * rcp;
+    bool positive = sz >= sx;
+    s.sign = positive ? 1.0f : -1.0f;
+    float xt0 = std::floor(sx * s.sign);
+    float c = sx * s.sign - xt0;
+    s.y0 = std::floor(sy);
+    float ytop = s.y0 + 1.0f;
+    if (sy == sw) ytop = std::ceil(sy);
+    s.b = fmin_((dy * c + dx * (ytop - sy)) * rcp, 0.99999994f);
+    float err = std::floor(s.a * (float(s.count) - 1.0f) + s.b) - float(count_x);
+    if (err != 0.0f) {
+        if (err > 0.0f) s.a -= 0.0000002f; else s.a += 0.0000002f;
+    }
+    s.x0 = positive ? xt0 * s.sign : xt0 * s.sign - 1.0f;
+    float xmin = fmin_(sx, sz);
+    if (sy >= float(s.by1) || sw <= float(s.by0) + TOP_TOUCH_EPSILON || xmin >= float(s.bx1)) return false;
+    s.imin = 0u;
+    if (sy < float(s.by0)) {
+        float first = round_ne((float(s.by0) - s.y0 + s.b - s.a) / (1.0f - s.a)) - 1.0f;
+        if (s.y0 + first - std::floor(s.a * first + s.b) < float(s.by0)) first += 1.0f;
+        s.imin = f2u(first);
+    }
+    s.imax = s.count;
+    if (sw > float(s.by1)) {
+        float last = round_ne((float(s.by1) - s.y0 + s.b - s.a) / (1.0f - s.a)) - 1.0f;
+        if (s.y0 + last - std::floor(s.a * last + s.b) < float(s.by1)) last += 1.0f;
+        s.imax = f2u(last);
+    }
+    s.ymin = 0; s.ymax = 0;
+    float xmax = fmax_(sx, sz);
+    if (xmax < float(s.bx0)) {
+        s.ymin = ceil_tile_boundary_y(sy);
+        s.ymax = ceil_tile_boundary_y(sw);
+        s.imax = s.imin;
+    } else {
+        float fudge = positive ? 0.0f : 1.0f;
+        if (xmin < float(s.bx0)) {
+            float cut = round_ne((s.sign * (float(s.bx0) - s.x0) - s.b + fudge) / s.a);
+            if ((s.x0 + s.sign * std::floor(s.a * cut + s.b) < float(s.bx0)) == positive) cut += 1.0f;
+            int32_t ynext = f2i(s.y0 + cut - std::floor(s.a * cut + s.b) + 1.0f);
+            if (positive) {
+                if (f2u(cut) > s.imin) {
+                    float ystart = s.y0 + 1.0f;
+                    if (is_tile_boundary_y(sy)) ystart = s.y0;
+                    s.ymin = f2i(ystart); s.ymax = ynext; s.imin = f2u(cut);
+                }
+            } else if (f2u(cut) < s.imax) {
+                s.ymin = ynext; s.ymax = ceil_tile_boundary_y(sw); s.imax = f2u(cut);
+            }
+        }
+        if (xmax > float(s.bx1)) {
+            float cut = round_ne((s.sign * (float(s.bx1) - s.x0) - s.b + fudge) / s.a);
+            if ((s.x0 + s.sign * std::floor(s.a * cut + s.b) < float(s.bx1)) == positive) cut += 1.0f;
+            if (positive) s.imax = std::min(s.imax, f2u(cut));
+            else s.imin = std::max(s.imin, f2u(cut));
+        }
+    }
+    s.imax = std::max(s.imin, s.imax);
+    s.ymin = std::max(s.ymin, (int32_t)s.by0);
+    s.ymax = std::min(s.ymax, (int32_t)s.by1);
+    return true;
+}
+inline void scan_tile(const Scan& s, uint32_t i, float z, int32_t& tx, int32_t& ty) {
+    tx = f2i(s.x0 + s.sign * z);
+    ty = f2i(s.y0 + float(i) - z);
+}
+inline bool scan_tile_inside(const Scan& s, int32_t tx, int32_t ty) {
+    return ty >= (int32_t)s.by0 && ty < (int32_t)s.by1 && tx >= (int32_t)s.bx0 && tx < (int32_t)s.bx1;
+}
+inline uint32_t scan_tile_offset(const Scan& s, int32_t tx, int32_t ty) {
+    return s.data_offset + (uint32_t(ty) - s.by0) * (s.bx1 - s.bx0) + uint32_t(tx) - s.bx0;
+}
+
+// scan/count.hlsl:13-40 for one line.
+void count_line(const tk_line& line, const tk_path_record* paths, uint32_t np, int32_t* backdrops,
+                uint32_t* counts) {
+    Scan s;
+    if (!scan_geometry(line, paths, np, s)) return;
+    int32_t delta = s.down ? -1 : 1;
+    int32_t stride = int32_t(s.bx1 - s.bx0);
+    for (int32_t y = s.ymin; y < s.ymax; ++y) {
+        uint32_t local = uint32_t((y - int32_t(s.by0)) * stride);
+        backdrops[s.data_offset + local] += delta;
+    }
+    float last_z = std::floor(s.a * (float(s.imin) - 1.0f) + s.b);
+    for (uint32_t i = s.imin; i < s.imax; ++i) {
+        float z = std::floor(s.a * float(i) + s.b);
+        int32_t tx, ty;
+        scan_tile(s, i, z, tx, ty);
+        if (scan_tile_inside(s, tx, ty)) {
+            bool top = last_z == z;
+            if (i == 0u) top = std::fabs(s.y0 - s.qy0 * (1.0f / float(TK_TILE_SIZE))) <= SCAN_EPSILON;
+            if (top && tx + 1 < int32_t(s.bx1)) {
+                int32_t x = std::max(tx + 1, int32_t(s.bx0));
+                uint32_t local = uint32_t((ty - int32_t(s.by0)) * stride + x - int32_t(s.bx0));
+                backdrops[s.data_offset + local] += delta;
+            }
+            counts[scan_tile_offset(s, tx, ty)] += 1u;
+        }
+        last_z = z;
+    }
+}
+
+// --- scan/clip.hlsli:10-75 -----------------------------------------------------
+inline float x_at_y(const Scan& s, float y) { return mad(s.qx1 - s.qx0, (y - s.qy0) / (s.qy1 - s.qy0), s.qx0); }
+inline float y_at_x(const Scan& s, float x) { return mad(s.qy1 - s.qy0, (x - s.qx0) / (s.qx1 - s.qx0), s.qy0); }
+inline float clip_y_at_x(const Scan& s, float x, float tmin_y, float tmax_y) {
+    float y = y_at_x(s, x);
+    if (y <= tmin_y + SCAN_EPSILON) {
+        float top_x = x_at_y(s, tmin_y);
+        if (std::fabs(top_x - x) > TILE_CLIP_NUDGE) return tmin_y;
+        return tmin_y + TILE_CLIP_NUDGE;
+    }
+    return clampf(y, tmin_y + TILE_CLIP_NUDGE, tmax_y);
+}
+tk_line_segment clipped_segment(const Scan& s, uint32_t sub, float z, int32_t tx, int32_t ty) {
+    const float ts = float(TK_TILE_SIZE);
+    float tminx = float(tx) * ts, tminy = float(ty) * ts;
+    float tmaxx = tminx + ts, tmaxy = tminy + ts;
+    float px = s.qx0, py = s.qy0, pz = s.qx1, pw = s.qy1;
+    if (sub > 0u) {
+        float prev = std::floor(s.a * (float(sub) - 1.0f) + s.b);
+        if (z == prev) {
+            float x = x_at_y(s, tminy);
+            x = clampf(x, tminx + TILE_CLIP_NUDGE, tmaxx);
+            px = x; py = tminy;
+        } else {
+            float xc = s.sign > 0.0f ? tminx : tmaxx;
+            px = xc; py = clip_y_at_x(s, xc, tminy, tmaxy);
+        }
+    }
+    if (sub < s.count - 1u) {
+        float next = std::floor(s.a * (float(sub) + 1.0f) + s.b);
+        if (z == next) {
+            float x = x_at_y(s, tmaxy);
+            x = clampf(x, tminx + TILE_CLIP_NUDGE, tmaxx);
+            pz = x; pw = tmaxy;
+        } else {
+            float xc = s.sign > 0.0f ? tmaxx : tminx;
+            pz = xc; pw = clip_y_at_x(s, xc, tminy, tmaxy);
+        }
+    }
+    float edge = 1000000000.0f;
+    float p0x = clampf(px - tminx, 0.0f, ts), p0y = clampf(py - tminy, 0.0f, ts);
+    float p1x = clampf(pz - tminx, 0.0f, ts), p1y = clampf(pw - tminy, 0.0f, ts);
+    if (p0x <= SCAN_EPSILON) p0x = 0.0f; else if (ts - p0x <= SCAN_EPSILON) p0x = ts;
+    if (p0y <= SCAN_EPSILON) p0y = 0.0f; else if (ts - p0y <= SCAN_EPSILON) p0y = ts;
+    if (p1x <= SCAN_EPSILON) p1x = 0.0f; else if (ts - p1x <= SCAN_EPSILON) p1x = ts;
+    if (p1y <= SCAN_EPSILON) p1y = 0.0f; else if (ts - p1y <= SCAN_EPSILON) p1y = ts;
+    if (p0x == 0.0f) {
+        if (p1x == 0.0f) {
+            p0x = SCAN_EPSILON;
+            if (p0y == 0.0f) { p1x = SCAN_EPSILON; p1y = ts; }
+            else { p1x = 2.0f * SCAN_EPSILON; p1y = p0y; }
+        } else if (p0y == 0.0f) p0x = SCAN_EPSILON;
+        else edge = p0y;
+    } else if (p1x == 0.0f) {
+        if (p1y == 0.0f) p1x = SCAN_EPSILON; else edge = p1y;
+    }
+    if (std::floor(p0x) == p0x && p0x != 0.0f) p0x -= SCAN_EPSILON;
+    if (std::floor(p1x) == p1x && p1x != 0.0f) p1x -= SCAN_EPSILON;
+    if (!s.down) { std::swap(p0x, p1x); std::swap(p0y, p1y); }
+    return {p0x, p0y, p1x, p1y, edge};
+}
+
+// Canonical emit order (or_emit_order): per path, lines in groups of 32
+// consecutive lines; within a group, DDA iteration r (i = imin + r) is the
+// outer loop and the line's lane (0..31) the inner loop. Each emitting step
+// takes the next cursor of its tile. This is one admissible interleaving of
+// the reference's atomic increments (each line's own steps stay in order).
+void emit_path(const tk_line* lines, const tk_path_record* paths, uint32_t np, uint32_t pid, uint32_t* cursors,
+               tk_line_segment* segments, uint64_t capacity) {
+    const tk_path_record& p = paths[pid];
+    for (uint32_t g = 0; g < p.line_count; g += 32u) {
+        uint32_t n = std::min(32u, p.line_count - g);
+        Scan sc[32];
+        bool ok[32];
+        uint32_t rounds = 0;
+        for (uint32_t l = 0; l < n; ++l) {
+            ok[l] = scan_geometry(lines[p.line_start + g + l], paths, np, sc[l]);
+            if (ok[l]) rounds = std::max(rounds, sc[l].imax - sc[l].imin);
+        }
+        for (uint32_t r = 0; r < rounds; ++r) {
+            for (uint32_t l = 0; l < n; ++l) {
+                if (!ok[l]) continue;
+                const Scan& s = sc[l];
+                if (r >= s.imax - s.imin) continue;
+                uint32_t i = s.imin + r;
+                float z = std::floor(s.a * float(i) + s.b);
+                int32_t tx, ty;
+                scan_tile(s, i, z, tx, ty);
+                if (!scan_tile_inside(s, tx, ty)) continue;
+                uint32_t dst = cursors[scan_tile_offset(s, tx, ty)]++;
+                if (dst < capacity) segments[dst] = clipped_segment(s, i, z, tx, ty);
+            }
+        }
+    }
+}
+
+// --- shared/coverage.hlsli:7-51 -------------------------------------------------
+struct Parts { float edge, dy, xmin, xmax; };
+inline Parts segment_row_parts(const tk_line_segment& g, uint32_t y) {
+    float delta_x = g.p1x - g.p0x, delta_y = g.p1y - g.p0y;
+    float row_y = float(y), local_y = g.p0y - row_y;
+    float y0 = clampf(local_y, 0.0f, 1.0f), y1 = clampf(g.p1y - row_y, 0.0f, 1.0f);
+    float dy = y0 - y1;
+    float row_edge = signum_f32(delta_x) * clampf(row_y - g.y_edge + 1.0f, 0.0f, 1.0f);
+    if (dy == 0.0f) return {row_edge, dy, 0.0f, 0.0f};
+    float slope = delta_x / delta_y;
+    bool nearer_p0 = std::fabs(local_y - 0.5f) <= std::fabs(g.p1y - row_y - 0.5f);
+    float anchor_x = nearer_p0 ? g.p0x : g.p1x;
+    float anchor_y = nearer_p0 ? local_y : g.p1y - row_y;
+    float sx0 = mad(y0 - anchor_y, slope, anchor_x);
+    float sx1 = mad(y1 - anchor_y, slope, anchor_x);
+    return {row_edge, dy, fmin_(sx0, sx1), fmax_(sx0, sx1)};
+}
+inline float segment_area_at(float xmin_abs, float xmax_abs, uint32_t x) {
+    float xmin = xmin_abs - float(x), xmax = xmax_abs - float(x);
+    float width = xmax - xmin;
+    if (width == 0.0f) return clampf(1.0f - xmin, 0.0f, 1.0f);
+    if (xmin >= 0.0f && xmax <= 1.0f) return mad(-0.5f, xmin + xmax, 1.0f);
+    float left = clampf(xmin, 0.0f, 1.0f), right = clampf(xmax, 0.0f, 1.0f);
+    float full = clampf(-xmin, 0.0f, width);
+    return mad(right - left, mad(-0.5f, left + right, 1.0f), full) / width;
+}
+inline float fill_value(const tk_line_segment* segs, uint32_t start, uint32_t end, int32_t backdrop, uint32_t x,
+                        uint32_t y) {
+    float base = float(backdrop), running = 0.0f, partial = 0.0f;
+    for (uint32_t i = start; i < end; ++i) {
+        Parts q = segment_row_parts(segs[i], y);
+        base += q.edge;
+        if (q.dy != 0.0f) {
+            int32_t full_start = std::min(std::max(f2i(std::ceil(q.xmax)), 0), int32_t(TK_TILE_SIZE));
+            if (full_start < int32_t(TK_TILE_SIZE) && int32_t(x) >= full_start) running += q.dy;
+            int32_t ps = std::min(std::max(f2i(std::floor(q.xmin)), 0), int32_t(TK_TILE_SIZE));
+            int32_t pe = std::min(std::max(f2i(std::ceil(q.xmax)), 0), int32_t(TK_TILE_SIZE));
+            if (int32_t(x) >= ps && int32_t(x) < pe) partial += segment_area_at(q.xmin, q.xmax, x) * q.dy;
+        }
+    }
+    return base + running + partial;
+}
+
+// ---------------------------------------------------------------------------
+// Brushes (shared/brush/*.hlsli, fine/draw.hlsli:16-21).
+// ---------------------------------------------------------------------------
+struct Paint {
+    const uint32_t* words;
+    uint64_t count;
+    uint32_t word(uint32_t base, uint32_t index) const {
+        if (base < count) {
+            if (index < count - base) return words[base + index];
+        }
+        return 0u;
+    }
+    float param(uint32_t base, uint32_t b, uint32_t i) const { return bits_f(word(base, b + i)); }
+};
+const float GRADIENT_FLOAT_EPSILON = 0.00000011920929f;
+const float RADIAL_QUADRATIC_EPSILON = 0.000001f;
+inline float apply_extend(float t, uint32_t extend) {
+    if (extend == TK_EXTEND_REPEAT) return rem_euclid_f32(t, 1.0f);
+    if (extend == TK_EXTEND_REFLECT) {
+        float v = rem_euclid_f32(t, 2.0f);
+        return v <= 1.0f ? v : 2.0f - v;
+    }
+    return clampf(t, 0.0f, 1.0f);
+}
+uint32_t sample_ramp(const Paint& P, uint32_t off, uint32_t len, float t, uint32_t extend) {
+    if (len == 0u) return 0u;
+    uint32_t last = len - 1u;
+    float ext = apply_extend(t, extend);
+    float pos = ext * float(last);
+    uint32_t li = f2u(std::floor(pos)), ri = std::min(li + 1u, last);
+    float frac = mad(ext, float(last), -float(li));
+    uint32_t l = P.word(0u, off + li), r = P.word(0u, off + ri);
+    if (frac <= GRADIENT_FLOAT_EPSILON || li == ri) return l;
+    return lerp_premul_u8(l, r, frac);
+}
+uint32_t sample_linear(const Paint& P, float x, float y, uint32_t base, uint32_t extend, uint32_t off, uint32_t len) {
+    float tx = mad(P.param(0, base, 4), x, mad(P.param(0, base, 6), y, P.param(0, base, 8)));
+    float ty = mad(P.param(0, base, 5), x, mad(P.param(0, base, 7), y, P.param(0, base, 9)));
+    float sx = P.param(0, base, 0), sy = P.param(0, base, 1), ex = P.param(0, base, 2), ey = P.param(0, base, 3);
+    float dx = ex - sx, dy = ey - sy;
+    float den = dx * dx + dy * dy, t = 0.0f;
+    if (den > GRADIENT_FLOAT_EPSILON) t = mad(tx - sx, dx, (ty - sy) * dy) / den;
+    return sample_ramp(P, off, len, t, extend);
+}
+uint32_t sample_radial(const Paint& P, float x, float y, uint32_t base, uint32_t extend, uint32_t off, uint32_t len) {
+    float tx = mad(P.param(0, base, 6), x, mad(P.param(0, base, 8), y, P.param(0, base, 10)));
+    float ty = mad(P.param(0, base, 7), x, mad(P.param(0, base, 9), y, P.param(0, base, 11)));
+    float sx = P.param(0, base, 0), sy = P.param(0, base, 1), ex = P.param(0, base, 2), ey = P.param(0, base, 3);
+    float sr = P.param(0, base, 4), er = P.param(0, base, 5);
+    float qx = tx - sx, qy = ty - sy, dcx = ex - sx, dcy = ey - sy, dr = er - sr;
+    float a = mad(dcx, dcx, mad(dcy, dcy, -dr * dr));
+    float b = -2.0f * mad(qx, dcx, mad(qy, dcy, sr * dr));
+    float c = mad(qx, qx, mad(qy, qy, -sr * sr));
+    bool has_t = false;
+    float t = 0.0f;
+    if (std::fabs(a) <= RADIAL_QUADRATIC_EPSILON) {
+        if (std::fabs(b) > RADIAL_QUADRATIC_EPSILON) {
+            float cand = -c / b;
+            if (mad(cand, dr, sr) >= 0.0f) { has_t = true; t = cand; }
+        }
+    } else {
+        float disc = mad(b, b, -4.0f * a * c);
+        if (disc >= 0.0f) {
+            float root = std::sqrt(disc);
+            float t0 = (-b - root) / (2.0f * a), t1 = (-b + root) / (2.0f * a);
+            bool v0 = mad(t0, dr, sr) >= 0.0f, v1 = mad(t1, dr, sr) >= 0.0f;
+            if (v0) { has_t = true; t = v1 ? fmax_(t0, t1) : t0; }
+            else if (v1) { has_t = true; t = t1; }
+        }
+    }
+    return has_t ? sample_ramp(P, off, len, t, extend) : 0u;
+}
+uint32_t sample_draw_brush(const Paint& P, const tk_draw_record& d, float x, float y) {
+    if (P.word(0u, d.brush_offset) == TK_BRUSH_SOLID) return P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD);
+    const tk_affine& m = d.inverse_transform;
+    float lx = mad(m.a, x, mad(m.c, y, m.e));
+    float ly = mad(m.b, x, mad(m.d, y, m.f));
+    uint32_t db = d.brush_offset;
+    uint32_t kind = P.word(0u, db), extend = P.word(0u, db + 1u);
+    uint32_t payload = db + P.word(0u, db + 2u), len = P.word(0u, db + 3u);
+    uint32_t base = db + TK_BRUSH_HEADER_WORDS;
+    uint32_t color = P.word(0u, db + TK_BRUSH_COLOR_WORD);
+    if (kind == TK_BRUSH_LINEAR) return sample_linear(P, lx, ly, base, extend, payload, len);
+    if (kind == TK_BRUSH_RADIAL) return sample_radial(P, lx, ly, base, extend, payload, len);
+    if (kind == 6u) return 0u;  // BRUSH_PATTERN
+    return color;               // other kinds are outside this path
+}
+
+// ---------------------------------------------------------------------------
+// Scene state.
+// ---------------------------------------------------------------------------
+struct BatchStream {
+    uint32_t batch;  // index into run's batch list
+    uint32_t kind;   // kind | skip << 3
+    std::vector<tk_ptcl_record> recs;  // reference stream including END
+};
+
+struct Batch {
+    uint32_t batch_id, layer_start, layer_end, pass;
+    uint64_t total;  // PTCL records of this batch
+};
+
+template <class F>
+void parallel_for(int threads, uint64_t n, F&& f) {
+    if (threads <= 1 || n < 2) {
+        for (uint64_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::atomic<uint64_t> next{0};
+    const uint64_t grain = std::max<uint64_t>(1, n / (uint64_t(threads) * 64));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) {
+        pool.emplace_back([&]() {
+            for (;;) {
+                uint64_t b = next.fetch_add(grain);
+                if (b >= n) return;
+                uint64_t e = std::min(n, b + grain);
+                for (uint64_t i = b; i < e; ++i) f(i);
+            }
+        });
+    }
+    for (auto& th : pool) th.join();
+}
+
+struct PixelBox { uint32_t x0, y0, x1, y1; };
+
+}  // namespace
+
+struct or_scene {
+    tk_scene_desc desc{};
+    std::vector<tk_path_record> paths;
+    std::vector<tk_draw_record> draws;
+    std::vector<tk_layer_record> layers;
+    std::vector<uint32_t> brush, batch_ids;
+    uint32_t tw = 0, th = 0, T = 0;
+    uint64_t B = 0, seg_capacity = 0;
+    std::vector<int32_t> backdrops;
+    std::vector<uint32_t> counts, cursors, bumps;
+    std::vector<tk_segment_range> ranges;
+    std::vector<tk_line_segment> segments;
+    std::vector<std::vector<uint32_t>> bins;  // per tile draw indices, painter order
+    std::vector<Batch> batches;
+    // per pass: per tile, streams of the pass's batches touching the tile
+    std::vector<std::vector<std::vector<BatchStream>>> pass_streams;
+    std::vector<uint32_t> image;
+    uint32_t ty0 = 0, ty1 = 0;
+    double times[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+inline double since(clk::time_point t) { return std::chrono::duration<double>(clk::now() - t).count(); }
+
+// --- shared/draw.hlsli:33-47 ------------------------------------------------------
+inline uint32_t tile_min_(int32_t px, uint32_t lim) { return px > 0 ? std::min(uint32_t(px) / TK_TILE_SIZE, lim) : 0u; }
+inline uint32_t tile_max_(int32_t px, uint32_t lim) {
+    return px > 0 ? std::min((uint32_t(px) + TK_TILE_SIZE - 1u) / TK_TILE_SIZE, lim) : 0u;
+}
+inline bool draw_hits_tile(const tk_draw_record& d, uint32_t tx, uint32_t ty, uint32_t tw, uint32_t th) {
+    uint32_t lx = tile_min_(d.pixel_bounds.x0, tw), ly = tile_min_(d.pixel_bounds.y0, th);
+    uint32_t ux = tile_max_(d.pixel_bounds.x1, tw), uy = tile_max_(d.pixel_bounds.y1, th);
+    return tx >= lx && ty >= ly && tx < ux && ty < uy;
+}
+inline uint32_t draw_backdrop(const or_scene& S, const tk_draw_record& d, uint32_t tx, uint32_t ty) {
+    if (d.path_id == TK_INVALID_INDEX || d.tag > TK_DRAW_PATH_GLYPH || d.path_id >= S.paths.size() ||
+        !draw_hits_tile(d, tx, ty, S.tw, S.th))
+        return TK_INVALID_INDEX;
+    const tk_path_record& p = S.paths[d.path_id];
+    if (p.tile_x1 <= p.tile_x0 || tx < p.tile_x0 || ty < p.tile_y0 || tx >= p.tile_x1 || ty >= p.tile_y1)
+        return TK_INVALID_INDEX;
+    return p.data_offset + (ty - p.tile_y0) * (p.tile_x1 - p.tile_x0) + tx - p.tile_x0;
+}
+
+// --- coarse/classify.hlsli:11-33 ------------------------------------------------
+uint32_t stack_wrapper_count(const or_scene& S, const Batch& b, uint32_t tx, uint32_t ty) {
+    uint32_t count = 0;
+    for (uint32_t i = b.layer_start; i < b.layer_end; ++i) {
+        const tk_layer_record& L = S.layers[i];
+        const tk_draw_record& d = S.draws[L.draw];
+        uint32_t bd = draw_backdrop(S, d, tx, ty);
+        if (bd == TK_INVALID_INDEX) return TK_INVALID_INDEX;
+        tk_segment_range r = S.ranges[bd];
+        int32_t w = S.backdrops[bd];
+        bool full = d.fill_rule == TK_FILL_EVEN_ODD ? (uint32_t(w) & 1u) != 0u : w != 0;
+        if (L.tag == TK_LAYER_CLIP && r.start == r.end && full) continue;
+        if (r.start == r.end && w == 0) return TK_INVALID_INDEX;
+        ++count;
+    }
+    return count;
+}
+// coarse/emit_stack.hlsli:9-17
+bool noop_stack_clip(const or_scene& S, const tk_layer_record& L, const tk_draw_record& d, uint32_t tx, uint32_t ty) {
+    if (L.tag != TK_LAYER_CLIP) return false;
+    uint32_t bd = draw_backdrop(S, d, tx, ty);
+    tk_segment_range r = S.ranges[bd];
+    uint32_t w = uint32_t(S.backdrops[bd]);
+    return r.start == r.end && (d.fill_rule == TK_FILL_EVEN_ODD ? (w & 1u) != 0u : w != 0u);
+}
+
+struct Particle {
+    bool valid = false;
+    uint32_t tag = TK_PTCL_FILL, winding = 0, fill_rule = 0, seg0 = 0, seg1 = 0, color = 0;
+};
+// coarse/emit_draw.hlsli:10-52 (path draws; coarse/paint.hlsli:14-21)
+Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t tx, uint32_t ty) {
+    Particle r;
+    if (di >= S.batch_ids.size() || S.batch_ids[di] != b.batch_id) return r;
+    const tk_draw_record& d = S.draws[di];
+    uint32_t bd = draw_backdrop(S, d, tx, ty);
+    if (bd == TK_INVALID_INDEX || (d.tag != TK_DRAW_BRUSH && d.tag != TK_DRAW_PATH_GLYPH && d.tag != TK_DRAW_CLIP))
+        return r;
+    tk_segment_range rg = S.ranges[bd];
+    uint32_t w = uint32_t(S.backdrops[bd]);
+    if (rg.start == rg.end && w == 0u) return r;
+    r.valid = true;
+    r.winding = w;
+    r.fill_rule = d.fill_rule;
+    r.seg0 = rg.start;
+    r.seg1 = rg.end;
+    Paint P{S.brush.data(), S.brush.size()};
+    bool nontransparent_solid = d.brush_offset != TK_INVALID_INDEX && P.word(0u, d.brush_offset) == TK_BRUSH_SOLID &&
+                                P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
+    if (d.tag == TK_DRAW_CLIP) r.tag = TK_PTCL_BEGIN_CLIP;
+    else if (d.tag == TK_DRAW_PATH_GLYPH) r.tag = TK_PTCL_PATH_GLYPH;
+    else if (d.solid_rect != 0u && d.transform.b == 0.0f && d.transform.c == 0.0f && nontransparent_solid &&
+             rg.start == rg.end)
+        r.tag = TK_PTCL_COLOR;
+    if (r.tag == TK_PTCL_COLOR) r.color = P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD);
+    else if (d.tag == TK_DRAW_BRUSH || d.tag == TK_DRAW_PATH_GLYPH) r.color = di;
+    return r;
+}
+
+const uint32_t CHUNK_CLASS_COLOR = 1u, CHUNK_CLASS_OTHER = 4u, CHUNK_CLASS_OCCLUDER = 8u;
+
+// coarse/occlusion.hlsli:12-34 on one tile stream (records [0, end)).
+uint32_t occluded_prefix(const std::vector<tk_ptcl_record>& recs, uint32_t end, uint32_t wrappers) {
+    uint32_t start = 0;
+    if (wrappers != 0u || end <= start || end - start <= 2u || end > recs.size()) return 0u;
+    if (recs[end - 1u].tag != TK_PTCL_END) return 0u;
+    uint32_t depth = 0;
+    for (uint32_t cur = end - 1u; cur > start;) {
+        const tk_ptcl_record& r = recs[--cur];
+        uint32_t tag = r.tag;
+        if (tag == TK_PTCL_END_CLIP || tag == TK_PTCL_END_OPACITY || tag == TK_PTCL_END_BLEND) ++depth;
+        else if (tag == TK_PTCL_BEGIN_CLIP || tag == TK_PTCL_BEGIN_SDF_CLIP || tag == TK_PTCL_BEGIN_OPACITY ||
+                 tag == TK_PTCL_BEGIN_BLEND) {
+            if (depth == 0u) return 0u;
+            --depth;
+        } else if (tag == TK_PTCL_COLOR && depth == 0u && (r.color >> 24) == 255u) {
+            return cur - start;
+        }
+    }
+    return 0u;
+}
+
+// coarse_count_bins (coarse/count.hlsl:48-73) + coarse_emit_bins
+// (coarse/emit.hlsl:82-142) for one (batch, tile); `first`/`last` bound the
+// tile's candidate run for this batch. Returns false when the tile has no
+// stream in this batch.
+bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, const uint32_t* cand, uint32_t n,
+                 BatchStream& out) {
+    uint32_t tx = tile % S.tw, ty = tile / S.tw;
+    uint32_t wrappers = stack_wrapper_count(S, b, tx, ty);
+    if (wrappers == TK_INVALID_INDEX) return false;
+    uint32_t count = 0;
+    for (uint32_t k = 0; k < n; ++k) count += draw_particle(S, b, cand[k], tx, ty).valid ? 1u : 0u;
+    if (count == 0u) return false;
+    count += wrappers * 2u + 1u;
+    out.batch = bi;
+    out.recs.assign(count, tk_ptcl_record{});
+    uint32_t p = 0;
+    uint32_t flags = wrappers != 0u ? CHUNK_CLASS_OTHER : 0u;
+    for (uint32_t i = b.layer_start; i < b.layer_end; ++i) {  // emit_stack_begins
+        const tk_layer_record& L = S.layers[i];
+        const tk_draw_record& d = S.draws[L.draw];
+        if (noop_stack_clip(S, L, d, tx, ty)) continue;
+        uint32_t bd = draw_backdrop(S, d, tx, ty);
+        uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_BEGIN_OPACITY
+                       : (L.tag == TK_LAYER_BLEND ? TK_PTCL_BEGIN_BLEND : TK_PTCL_BEGIN_CLIP);
+        out.recs[p++] = {tag, S.backdrops[bd], d.fill_rule, S.ranges[bd].start, S.ranges[bd].end, L.payload};
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        Particle q = draw_particle(S, b, cand[k], tx, ty);
+        if (!q.valid) continue;
+        flags |= q.tag == TK_PTCL_COLOR ? CHUNK_CLASS_COLOR : CHUNK_CLASS_OTHER;
+        if (wrappers == 0u && q.tag == TK_PTCL_COLOR && (q.color >> 24) == 255u && p > 0u) flags |= CHUNK_CLASS_OCCLUDER;
+        if (p < count) out.recs[p++] = {q.tag, int32_t(q.winding), q.fill_rule, q.seg0, q.seg1, q.color};
+    }
+    uint32_t q = p;
+    for (uint32_t i = b.layer_end; i > b.layer_start;) {  // emit_stack_ends
+        const tk_layer_record& L = S.layers[--i];
+        const tk_draw_record& d = S.draws[L.draw];
+        if (noop_stack_clip(S, L, d, tx, ty)) continue;
+        uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_END_OPACITY
+                       : (L.tag == TK_LAYER_BLEND ? TK_PTCL_END_BLEND : TK_PTCL_END_CLIP);
+        out.recs[q++] = {tag, 0, 0u, 0u, 0u, 0u};
+    }
+    out.recs[p + wrappers] = {TK_PTCL_END, 0, 0u, 0u, 0u, 0u};
+    uint32_t skip = (flags & CHUNK_CLASS_OCCLUDER) ? occluded_prefix(out.recs, p + wrappers + 1u, wrappers) : 0u;
+    uint32_t kind;  // coarse/tile_classification.hlsli:6-10
+    if (flags & CHUNK_CLASS_OTHER) kind = TK_TILE_KIND_INTERPRETER;
+    else kind = (flags & CHUNK_CLASS_COLOR) ? TK_TILE_KIND_COLOR : TK_TILE_KIND_EMPTY;
+    out.kind = kind | (skip << TK_TILE_PREFIX_SHIFT);
+    return true;
+}
+
+// --- fine/interpreter.hlsli:21-219 (clip stack and opacity groups) ------------
+struct Group { uint32_t kind; F4 parent; uint32_t parent_clip, layer_alpha, payload; };
+
+F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel,
+             uint32_t lx, uint32_t ly, uint32_t gx, uint32_t gy) {
+    Paint P{S.brush.data(), S.brush.size()};
+    uint32_t clip_mask = 255u;
+    std::vector<uint32_t> clip_stack;
+    std::vector<Group> groups;
+    for (uint32_t ix = begin; ix < end; ++ix) {
+        const tk_ptcl_record& r = recs[ix];
+        uint32_t tag = r.tag;
+        if (tag == TK_PTCL_END) break;
+        if (tag == TK_PTCL_COLOR) {
+            if (clip_mask != 0u) {
+                if (clip_mask == 255u && premul_u8_is_opaque(r.color)) pixel = rgba8_to_unorm(r.color);
+                else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(r.color, clip_mask));
+            }
+        } else if (tag == TK_PTCL_END_CLIP) {
+            if (!clip_stack.empty()) { clip_mask = clip_stack.back(); clip_stack.pop_back(); }
+            else clip_mask = 255u;
+        } else if (tag == TK_PTCL_END_OPACITY || tag == TK_PTCL_END_BLEND) {
+            if (!groups.empty()) {
+                Group v = groups.back();
+                groups.pop_back();
+                if (v.kind == TK_PTCL_BEGIN_OPACITY) {
+                    uint32_t alpha = combine_alpha(combine_alpha(v.layer_alpha, v.parent_clip), v.payload);
+                    pixel = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(pixel), alpha));
+                }
+                // blend groups are outside this path (rejected at load)
+            }
+        } else if (tag == TK_PTCL_FILL || tag == TK_PTCL_PATH_GLYPH || tag == TK_PTCL_BEGIN_CLIP ||
+                   tag == TK_PTCL_BEGIN_OPACITY || tag == TK_PTCL_BEGIN_BLEND) {
+            uint32_t alpha = coverage_to_alpha(
+                fill_value(S.segments.data(), r.segment_start, r.segment_end, r.backdrop, lx, ly), r.fill_rule);
+            if (tag == TK_PTCL_BEGIN_CLIP) {
+                clip_stack.push_back(clip_mask);
+                clip_mask = combine_alpha(clip_mask, alpha);
+            } else if (tag == TK_PTCL_BEGIN_OPACITY || tag == TK_PTCL_BEGIN_BLEND) {
+                // Parents beyond the two local slots are spilled as RGBA8
+                // (fine/group.hlsli:21-36).
+                F4 parent = groups.size() < 2 ? pixel : rgba8_to_unorm(unorm_to_rgba8(pixel));
+                groups.push_back({tag, parent, clip_mask, alpha, r.color});
+                pixel = {0, 0, 0, 0};
+            } else {
+                uint32_t masked = combine_alpha(alpha, clip_mask);
+                if (masked != 0u) {
+                    uint32_t color = sample_draw_brush(P, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f);
+                    if (masked == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+                    else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(color, masked));
+                }
+            }
+        }
+    }
+    return pixel;
+}
+// fine/specialized.hlsli:19-45
+F4 color_only(const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel) {
+    for (uint32_t ix = begin; ix < end; ++ix) {
+        const tk_ptcl_record& r = recs[ix];
+        if (r.tag == TK_PTCL_END) break;
+        if (premul_u8_is_opaque(r.color)) pixel = rgba8_to_unorm(r.color);
+        else pixel = src_over_premul_unorm(pixel, rgba8_to_unorm(r.color));
+    }
+    return pixel;
+}
+
+// --- filter/blur*.hlsl -----------------------------------------------------------
+inline void channels(uint32_t p, float c[4]) {
+    c[0] = float(p & 255u); c[1] = float((p >> 8) & 255u); c[2] = float((p >> 16) & 255u); c[3] = float(p >> 24);
+}
+inline uint32_t pack_average(const float acc[4], float sum) {
+    if (sum <= 0.0f) return 0u;
+    float inv = 1.0f / sum;
+    uint32_t o = 0;
+    for (int c = 0; c < 4; ++c) o |= f2u(clampf(acc[c] * inv + 0.5f, 0.0f, 255.0f)) << (8 * c);
+    return o;
+}
+inline int32_t blur_half_width(float sd) { return f2i(fmax_(std::ceil(sd * 3.0f), 1.0f)); }
+inline bool inside_b(int32_t x, int32_t y, const int32_t b[4]) { return x >= b[0] && y >= b[1] && x < b[2] && y < b[3]; }
+
+// filter/sample.hlsli:4-17 on an RGBA8 texture: texel loads are k/255.
+F4 sample_premul(const uint32_t* src, uint32_t w, uint32_t h, float px, float py) {
+    int32_t lastx = int32_t(w) - 1, lasty = int32_t(h) - 1;
+    px = clampf(px, 0.0f, float(lastx));
+    py = clampf(py, 0.0f, float(lasty));
+    int32_t fx = f2i(std::floor(px)), fy = f2i(std::floor(py));
+    int32_t nx = std::min(fx + 1, lastx), ny = std::min(fy + 1, lasty);
+    float phx = px - float(fx), phy = py - float(fy);
+    F4 a = texel_load(src[size_t(fy) * w + fx]), b = texel_load(src[size_t(fy) * w + nx]);
+    F4 c = texel_load(src[size_t(ny) * w + fx]), d = texel_load(src[size_t(ny) * w + nx]);
+    auto lerp = [](float u, float v, float t) { return mad(v - u, t, u); };
+    F4 top{lerp(a.r, b.r, phx), lerp(a.g, b.g, phx), lerp(a.b, b.b, phx), lerp(a.a, b.a, phx)};
+    F4 bot{lerp(c.r, d.r, phx), lerp(c.g, d.g, phx), lerp(c.b, d.b, phx), lerp(c.a, d.a, phx)};
+    return {lerp(top.r, bot.r, phy), lerp(top.g, bot.g, phy), lerp(top.b, bot.b, phy), lerp(top.a, bot.a, phy)};
+}
+
+// filter/blur.hlsli:40-94 (global route, used for radius > 16).
+uint32_t blur_pixel_global(const uint32_t* src, uint32_t w, uint32_t h, int32_t x, int32_t y, float sd,
+                           const int32_t bounds[4], uint32_t axis, float weight0, float decay) {
+    int32_t hw = blur_half_width(sd);
+    int32_t ax = axis == 0u ? 1 : 0, ay = axis == 0u ? 0 : 1;
+    bool interior = inside_b(x - ax * hw, y - ay * hw, bounds) && inside_b(x + ax * hw, y + ay * hw, bounds);
+    float sum = 1.0f;
+    uint32_t center = inside_b(x, y, bounds) ? src[size_t(y) * w + x] : 0u;
+    float acc[4];
+    channels(center, acc);
+    float weight = weight0;
+    float ratio = weight * decay;
+    auto tap = [&](int32_t px, int32_t py, float wgt) {
+        if (interior || inside_b(px, py, bounds)) {
+            float c[4];
+            channels(src[size_t(py) * w + px], c);
+            for (int k = 0; k < 4; ++k) acc[k] = mad(c[k], wgt, acc[k]);
+        }
+    };
+    auto pair_inside = [&](float off) {
+        float fx = float(x) + float(ax) * off, fy = float(y) + float(ay) * off;
+        float nx = fx + float(ax), ny = fy + float(ay);
+        return fx >= float(bounds[0]) && fy >= float(bounds[1]) && nx < float(bounds[2]) && ny < float(bounds[3]);
+    };
+    auto pair = [&](float off, float wgt) {
+        F4 s = sample_premul(src, w, h, float(x) + float(ax) * off, float(y) + float(ay) * off);
+        float c[4] = {s.r * 255.0f, s.g * 255.0f, s.b * 255.0f, s.a * 255.0f};
+        for (int k = 0; k < 4; ++k) acc[k] = mad(c[k], wgt, acc[k]);
+    };
+    for (int32_t d = 1; d <= hw; d += 2) {
+        int32_t nd = d + 1;
+        bool has_pair = nd <= hw;
+        float next_weight = weight * ratio;
+        float pw = weight + (has_pair ? next_weight : 0.0f);
+        sum += 2.0f * pw;
+        if (has_pair && (interior || pair_inside(float(d)))) {
+            pair(float(d) + next_weight / pw, pw);
+        } else {
+            tap(x + ax * d, y + ay * d, weight);
+            if (has_pair) tap(x + ax * nd, y + ay * nd, next_weight);
+        }
+        if (has_pair && (interior || pair_inside(-float(nd)))) {
+            pair(-(float(d) + next_weight / pw), pw);
+        } else {
+            tap(x - ax * d, y - ay * d, weight);
+            if (has_pair) tap(x - ax * nd, y - ay * nd, next_weight);
+        }
+        float next_ratio = ratio * decay;
+        weight = next_weight * next_ratio;
+        ratio = next_ratio * decay;
+    }
+    return pack_average(acc, sum);
+}
+
+void blur_pass(const uint32_t* src, uint32_t* dst, uint32_t w, uint32_t h, const uint32_t region[4],
+               const uint32_t source[4], float amount, uint32_t axis, int threads) {
+    float sd = fmax_(amount, 0.0f);
+    int32_t bounds[4];
+    bool sx = source[2] > source[0], sy = source[3] > source[1];
+    bounds[0] = int32_t(sx ? source[0] : region[0]);
+    bounds[1] = int32_t(sy ? source[1] : region[1]);
+    bounds[2] = int32_t(sx ? source[2] : region[0] + region[2]);
+    bounds[3] = int32_t(sy ? source[3] : region[1] + region[3]);
+    // region = x0, y0, width, height
+    uint32_t rx1 = std::min(region[0] + region[2], w), ry1 = std::min(region[1] + region[3], h);
+    float sigma = fmax_(sd, 0.0001f);
+    float two = 2.0f * sigma * sigma;
+    float weight0 = std::exp(-1.0f / two), decay = std::exp(-2.0f / two);
+    int32_t hw = blur_half_width(sd);
+    parallel_for(threads, ry1 > region[1] ? ry1 - region[1] : 0, [&](uint64_t row) {
+        int32_t y = int32_t(region[1] + row);
+        for (int32_t x = int32_t(region[0]); x < int32_t(rx1); ++x) {
+            uint32_t out;
+            if (sd <= 0.0f) {
+                out = src[size_t(y) * w + x];
+            } else if (hw > int32_t(TK_SHARED_BLUR_MAX_RADIUS)) {
+                out = blur_pixel_global(src, w, h, x, y, sd, bounds, axis, weight0, decay);
+            } else {  // filter/blur_shared.hlsl:39-73
+                auto at = [&](int32_t px, int32_t py) -> uint32_t {
+                    return inside_b(px, py, bounds) ? src[size_t(py) * w + px] : 0u;
+                };
+                int32_t ax = axis == 0u ? 1 : 0, ay = axis == 0u ? 0 : 1;
+                float acc[4];
+                channels(at(x, y), acc);
+                float sum = 1.0f, weight = weight0, ratio = weight0 * decay;
+                for (int32_t d = 1; d <= hw; ++d) {
+                    sum += 2.0f * weight;
+                    float c[4];
+                    channels(at(x + ax * d, y + ay * d), c);
+                    for (int k = 0; k < 4; ++k) acc[k] = mad(c[k], weight, acc[k]);
+                    channels(at(x - ax * d, y - ay * d), c);
+                    for (int k = 0; k < 4; ++k) acc[k] = mad(c[k], weight, acc[k]);
+                    weight = weight * ratio;
+                    ratio = ratio * decay;
+                }
+                out = pack_average(acc, sum);
+            }
+            dst[size_t(y) * w + x] = out;
+        }
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Frame driver.
+// ---------------------------------------------------------------------------
+void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int threads) {
+    auto& streams = S.pass_streams[pass];
+    parallel_for(threads, S.T, [&](uint64_t tile) {
+        uint32_t ty = uint32_t(tile) / S.tw, tx = uint32_t(tile) % S.tw;
+        if (ty < S.ty0 || ty >= S.ty1) return;
+        const auto& list = streams[tile];
+        if (list.empty()) return;  // EMPTY in every batch: target unchanged
+        for (uint32_t ly = 0; ly < TK_TILE_SIZE; ++ly) {
+            uint32_t gy = ty * TK_TILE_SIZE + ly;
+            if (gy >= S.desc.height) break;
+            for (uint32_t lx = 0; lx < TK_TILE_SIZE; ++lx) {
+                uint32_t gx = tx * TK_TILE_SIZE + lx;
+                if (gx >= S.desc.width) break;
+                uint32_t& texel = target[size_t(gy) * S.desc.width + gx];
+                for (const BatchStream& bs : list) {  // one reference fine dispatch per batch
+                    F4 pixel = texel_load(texel);     // fine_initial_pixel with load_target
+                    uint32_t kind = bs.kind & TK_TILE_KIND_MASK;
+                    uint32_t begin = bs.kind >> TK_TILE_PREFIX_SHIFT;
+                    uint32_t end = uint32_t(bs.recs.size());
+                    if (kind == TK_TILE_KIND_INTERPRETER) pixel = interpret(S, bs.recs, begin, end, pixel, lx, ly, gx, gy);
+                    else if (kind == TK_TILE_KIND_COLOR) pixel = color_only(bs.recs, begin, end, pixel);
+                    texel = texel_store(pixel);
+                }
+            }
+        }
+    });
+}
+
+void run_scene(or_scene& S, int threads) {
+    const tk_scene_desc& D = S.desc;
+    S.tw = (D.width + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+    S.th = (D.height + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+    S.T = S.tw * S.th;
+    if (S.ty1 == 0 || S.ty1 > S.th) S.ty1 = S.th;
+    uint32_t np = uint32_t(S.paths.size());
+    for (const auto& p : S.paths) {
+        S.B = std::max<uint64_t>(S.B, uint64_t(p.data_offset) + p.data_len);
+        S.seg_capacity = std::max<uint64_t>(S.seg_capacity, uint64_t(p.segment_start) + p.segment_capacity);
+    }
+    S.backdrops.assign(S.B, 0);
+    S.counts.assign(S.B, 0u);
+    S.ranges.assign(S.B, tk_segment_range{0, 0});
+    S.cursors.assign(S.B, 0u);
+    S.bumps.assign(np, 0u);
+
+    // scan_count: per path (disjoint slices), lines in order.
+    auto t0 = clk::now();
+    parallel_for(threads, np, [&](uint64_t pid) {
+        const tk_path_record& p = S.paths[pid];
+        for (uint32_t l = 0; l < p.line_count; ++l)
+            count_line(D.lines[p.line_start + l], S.paths.data(), np, S.backdrops.data(), S.counts.data());
+    });
+    S.times[0] = since(t0);
+
+    // prefix (scan_prefix_chunks + offsets) and row cumsum (cumsum.hlsl).
+    t0 = clk::now();
+    parallel_for(threads, np, [&](uint64_t pid) {
+        const tk_path_record& p = S.paths[pid];
+        uint32_t next = p.segment_start;
+        for (uint32_t k = 0; k < p.data_len; ++k) {
+            uint32_t t = p.data_offset + k;
+            uint32_t c = S.counts[t];
+            S.ranges[t] = {next, next + c};
+            S.cursors[t] = next;
+            next += c;
+        }
+        S.bumps[pid] = next - p.segment_start;
+        uint32_t stride = p.tile_x1 > p.tile_x0 ? p.tile_x1 - p.tile_x0 : 0u;
+        if (stride == 0u) return;
+        for (uint32_t row = 0; row * stride < p.data_len; ++row) {
+            int32_t acc = 0;
+            for (uint32_t k = 0; k < stride; ++k) {
+                int32_t& v = S.backdrops[p.data_offset + row * stride + k];
+                acc = int32_t(uint32_t(acc) + uint32_t(v));
+                v = acc;
+            }
+        }
+    });
+    S.times[1] = since(t0);
+
+    // scan_emit in canonical order.
+    t0 = clk::now();
+    S.segments.assign(S.seg_capacity, tk_line_segment{0, 0, 0, 0, 0});
+    parallel_for(threads, np, [&](uint64_t pid) {
+        emit_path(D.lines, S.paths.data(), np, uint32_t(pid), S.cursors.data(), S.segments.data(), S.seg_capacity);
+    });
+    S.times[2] = since(t0);
+
+    // Tile bins (tile_bins/build.rs:54-77).
+    t0 = clk::now();
+    S.bins.assign(S.T, {});
+    for (uint32_t k = 0; k < D.draw_order_count; ++k) {
+        uint32_t di = D.draw_order[k];
+        const tk_pixel_bounds& pb = S.draws[di].pixel_bounds;
+        uint32_t x0 = std::min(uint32_t(std::max(pb.x0, 0)) / TK_TILE_SIZE, S.tw);
+        uint32_t y0 = std::min(uint32_t(std::max(pb.y0, 0)) / TK_TILE_SIZE, S.th);
+        uint32_t x1 = std::min((uint32_t(std::max(pb.x1, 0)) + TK_TILE_SIZE - 1) / TK_TILE_SIZE, S.tw);
+        uint32_t y1 = std::min((uint32_t(std::max(pb.y1, 0)) + TK_TILE_SIZE - 1) / TK_TILE_SIZE, S.th);
+        for (uint32_t y = y0; y < y1; ++y)
+            for (uint32_t x = x0; x < x1; ++x) S.bins[size_t(y) * S.tw + x].push_back(di);
+    }
+    S.times[3] = since(t0);
+
+    // Walk ops: batches, passes, blur layers.
+    std::vector<uint32_t> main_target(size_t(D.width) * D.height, D.clear_color);
+    struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; };
+    std::vector<Surface> surfaces;
+    auto current = [&]() -> std::vector<uint32_t>& { return surfaces.empty() ? main_target : surfaces.back().img; };
+    bool pass_open = false;
+    std::vector<uint32_t> pass_batches;
+    auto flush_pass = [&]() {
+        if (!pass_open) return;
+        pass_open = false;
+        uint32_t pass = uint32_t(S.pass_streams.size());
+        S.pass_streams.emplace_back(S.T);
+        auto& streams = S.pass_streams.back();
+        auto tc = clk::now();
+        parallel_for(threads, S.T, [&](uint64_t tile) {
+            uint32_t ty = uint32_t(tile) / S.tw;
+            if (ty < S.ty0 || ty >= S.ty1) return;
+            const auto& cand = S.bins[tile];
+            for (uint32_t bi : pass_batches) {
+                const Batch& b = S.batches[bi];
+                // Candidates of one batch form a contiguous painter-order run.
+                uint32_t first = 0, n = 0;
+                for (uint32_t k = 0; k < cand.size(); ++k) {
+                    if (S.batch_ids[cand[k]] == b.batch_id) {
+                        if (n == 0) first = k;
+                        ++n;
+                    }
+                }
+                BatchStream bs;
+                if (b.layer_end > b.layer_start || n > 0) {
+                    // Non-contiguous runs cannot occur for compiled plans; fall back to the full list.
+                    bool contiguous = n == 0 || (first + n <= cand.size() && S.batch_ids[cand[first + n - 1]] == b.batch_id);
+                    bool ok = contiguous ? coarse_tile(S, b, bi, uint32_t(tile), cand.data() + first, n, bs)
+                                         : coarse_tile(S, b, bi, uint32_t(tile), cand.data(), uint32_t(cand.size()), bs);
+                    if (ok) streams[tile].push_back(std::move(bs));
+                }
+            }
+        });
+        for (uint32_t bi : pass_batches) {
+            uint64_t total = 0;
+            for (uint32_t t = 0; t < S.T; ++t)
+                for (const auto& bs : streams[t]) if (bs.batch == bi) total += bs.recs.size();
+            S.batches[bi].total = total;
+        }
+        S.times[4] += since(tc);
+        tc = clk::now();
+        fine_pass(S, pass, current(), threads);
+        S.times[5] += since(tc);
+        pass_batches.clear();
+    };
+    for (uint32_t oi = 0; oi < D.op_count; ++oi) {
+        const tk_op& op = D.ops[oi];
+        if (op.kind == TK_OP_DRAW_BATCH) {
+            if (!pass_open) pass_open = true;
+            uint32_t bi = uint32_t(S.batches.size());
+            S.batches.push_back({op.batch_id, op.layer_start, op.layer_end, uint32_t(S.pass_streams.size()), 0});
+            pass_batches.push_back(bi);
+        } else if (op.kind == TK_OP_BLUR_BEGIN) {
+            flush_pass();
+            Surface s;
+            s.img.assign(size_t(D.width) * D.height, 0u);
+            s.sigma = op.sigma;
+            std::memcpy(s.bounds, op.bounds, sizeof(s.bounds));
+            surfaces.push_back(std::move(s));
+        } else if (op.kind == TK_OP_BLUR_END) {
+            flush_pass();
+            if (surfaces.empty()) throw std::runtime_error("unbalanced BLUR_END");
+            Surface s = std::move(surfaces.back());
+            surfaces.pop_back();
+            auto tb = clk::now();
+            // Output bounds (op.bounds) and the surface they read from: the
+            // output outset by the blur radius, clipped to the canvas
+            // (shared/layer/filter.rs:510-531,599-601).
+            int32_t bx0 = std::max(s.bounds[0], 0), by0 = std::max(s.bounds[1], 0);
+            int32_t bx1 = std::min(s.bounds[2], int32_t(D.width)), by1 = std::min(s.bounds[3], int32_t(D.height));
+            int32_t rad = int32_t(std::ceil(fmax_(s.sigma, 0.0f) * 3.0f));
+            int32_t sx0 = std::max(s.bounds[0] - rad, 0), sy0 = std::max(s.bounds[1] - rad, 0);
+            int32_t sx1 = std::min(s.bounds[2] + rad, int32_t(D.width));
+            int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
+            if (bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
+                uint32_t region[4] = {uint32_t(sx0), uint32_t(sy0), uint32_t(sx1 - sx0), uint32_t(sy1 - sy0)};
+                uint32_t none[4] = {0, 0, 0, 0};
+                std::vector<uint32_t> temp(s.img.size(), 0u);
+                blur_pass(s.img.data(), temp.data(), D.width, D.height, region, none, s.sigma, 0, threads);
+                blur_pass(temp.data(), s.img.data(), D.width, D.height, region, none, s.sigma, 1, threads);
+            }
+            std::vector<uint32_t>& dst = current();
+            for (int32_t y = by0; y < by1; ++y)
+                for (int32_t x = bx0; x < bx1; ++x) {
+                    size_t i = size_t(y) * D.width + x;
+                    dst[i] = src_over_premul_u8(dst[i], scale_premul_u8(s.img[i], 255u));
+                }
+            S.times[6] += since(tb);
+        }
+    }
+    flush_pass();
+    if (!surfaces.empty()) throw std::runtime_error("unbalanced BLUR_BEGIN");
+    S.image = std::move(main_target);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* or_error(void) { return g_error.c_str(); }
+
+int32_t or_run(const tk_scene_desc* d, int32_t threads, uint32_t tile_y0, uint32_t tile_y1, or_scene** out) {
+    *out = nullptr;
+    try {
+        auto* S = new or_scene();
+        S->desc = *d;
+        S->paths.assign(d->paths, d->paths + d->path_count);
+        S->draws.assign(d->draws, d->draws + d->draw_count);
+        S->layers.assign(d->layers, d->layers + d->layer_count);
+        S->brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
+        S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        S->ty0 = tile_y0;
+        S->ty1 = tile_y1;
+        run_scene(*S, threads < 1 ? 1 : threads);
+        *out = S;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+void or_free(or_scene* s) { delete s; }
+uint32_t or_batch_count(const or_scene* s) { return uint32_t(s->batches.size()); }
+uint32_t or_pass_count(const or_scene* s) { return uint32_t(s->pass_streams.size()); }
+void or_stage_times(const or_scene* s, double out[7]) { std::memcpy(out, s->times, sizeof(s->times)); }
+
+static size_t copy_out(const void* src, size_t need, void* dst, size_t bytes) {
+    if (dst) std::memcpy(dst, src, std::min(need, bytes));
+    return need;
+}
+
+size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_t bytes) {
+    switch (what) {
+        case OR_COUNTS: return copy_out(s->counts.data(), s->counts.size() * 4, dst, bytes);
+        case OR_BACKDROPS: return copy_out(s->backdrops.data(), s->backdrops.size() * 4, dst, bytes);
+        case OR_RANGES: return copy_out(s->ranges.data(), s->ranges.size() * 8, dst, bytes);
+        case OR_SEGMENTS: return copy_out(s->segments.data(), s->segments.size() * sizeof(tk_line_segment), dst, bytes);
+        case OR_IMAGE: return copy_out(s->image.data(), s->image.size() * 4, dst, bytes);
+        case OR_PATHS: return copy_out(s->paths.data(), s->paths.size() * sizeof(tk_path_record), dst, bytes);
+        case OR_BUMPS: return copy_out(s->bumps.data(), s->bumps.size() * 4, dst, bytes);
+        case OR_BATCH_PTCL:
+        case OR_BATCH_TILES:
+        case OR_BATCH_KINDS: {
+            if (index >= s->batches.size()) return 0;
+            const Batch& b = s->batches[index];
+            const auto& streams = s->pass_streams[b.pass];
+            std::vector<tk_ptcl_record> ptcl;
+            std::vector<tk_tile_record> tiles(s->T, tk_tile_record{0, 0, 0, 0, 0, 0});
+            std::vector<uint32_t> kinds(s->T, TK_TILE_KIND_EMPTY);
+            uint32_t next = 0;
+            for (uint32_t t = 0; t < s->T; ++t) {
+                const BatchStream* found = nullptr;
+                for (const auto& bs : streams[t]) if (bs.batch == index) found = &bs;
+                uint32_t n = found ? uint32_t(found->recs.size()) : 0u;
+                tiles[t] = {n, next, next + n, 0, 0, 0};
+                if (found) {
+                    ptcl.insert(ptcl.end(), found->recs.begin(), found->recs.end());
+                    kinds[t] = found->kind;
+                }
+                next += n;
+            }
+            if (what == OR_BATCH_PTCL) return copy_out(ptcl.data(), ptcl.size() * sizeof(tk_ptcl_record), dst, bytes);
+            if (what == OR_BATCH_TILES) return copy_out(tiles.data(), tiles.size() * sizeof(tk_tile_record), dst, bytes);
+            return copy_out(kinds.data(), kinds.size() * 4, dst, bytes);
+        }
+        case OR_PASS_PTCL:
+        case OR_PASS_TILES:
+        case OR_PASS_KINDS: {
+            // Merged layout: per tile, for each batch with a stream:
+            // BATCH_BEGIN{segment_start=batch_id, segment_end=n-1, color=kind}
+            // followed by the batch's records without END; then one END.
+            if (index >= s->pass_streams.size()) return 0;
+            const auto& streams = s->pass_streams[index];
+            std::vector<tk_ptcl_record> ptcl;
+            std::vector<tk_tile_record> tiles(s->T, tk_tile_record{0, 0, 0, 0, 0, 0});
+            std::vector<uint32_t> kinds(s->T, TK_TILE_KIND_EMPTY);
+            uint32_t next = 0;
+            for (uint32_t t = 0; t < s->T; ++t) {
+                uint32_t n = 0;
+                for (const auto& bs : streams[t]) {
+                    uint32_t m = uint32_t(bs.recs.size());
+                    ptcl.push_back({TK_PTCL_BATCH_BEGIN, 0, 0u, s->batches[bs.batch].batch_id, m - 1u, bs.kind});
+                    ptcl.insert(ptcl.end(), bs.recs.begin(), bs.recs.end() - 1);
+                    n += m;
+                }
+                if (n) {
+                    ptcl.push_back({TK_PTCL_END, 0, 0u, 0u, 0u, 0u});
+                    n += 1;
+                    kinds[t] = TK_TILE_KIND_INTERPRETER;
+                }
+                tiles[t] = {n, next, next + n, 0, 0, 0};
+                next += n;
+            }
+            if (what == OR_PASS_PTCL) return copy_out(ptcl.data(), ptcl.size() * sizeof(tk_ptcl_record), dst, bytes);
+            if (what == OR_PASS_TILES) return copy_out(tiles.data(), tiles.size() * sizeof(tk_tile_record), dst, bytes);
+            return copy_out(kinds.data(), kinds.size() * 4, dst, bytes);
+        }
+        default: return 0;
+    }
+}
+
+uint32_t or_line_scanned_tile_count(const tk_line* line, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {
+    // src/shared/scan_line.rs:37-143 (Rust f32::round rounds half away from zero).
+    const float ts = 1.0f / float(TK_TILE_SIZE);
+    const float* p0 = line->p0;
+    const float* p1 = line->p1;
+    bool is_down = p1[1] >= p0[1];
+    const float* a0 = is_down ? p0 : p1;
+    const float* a1 = is_down ? p1 : p0;
+    float s0x = a0[0] * ts, s0y = a0[1] * ts, s1x = a1[0] * ts, s1y = a1[1] * ts;
+    auto span_r = [](float a, float b) {
+        float hi = std::ceil(fmax_(a, b)), lo = std::floor(fmin_(a, b));
+        return f2u(fmax_(hi - lo, 1.0f));
+    };
+    uint32_t count_x = span_r(s0x, s1x) - 1u;
+    uint32_t count = count_x + span_r(s0y, s1y);
+    float dx = std::fabs(s1x - s0x), dy = s1y - s0y;
+    if (dx + dy == 0.0f) return 0;
+    if (dy == 0.0f && std::floor(s0y) == s0y) return 0;
+    float idxdy = 1.0f / (dx + dy);
+    float a = dx * idxdy;
+    bool pos = s1x >= s0x;
+    float sign = pos ? 1.0f : -1.0f;
+    float xt0 = std::floor(s0x * sign);
+    float c = s0x * sign - xt0;
+    float y0f = std::floor(s0y);
+    float ytop = s0y == s1y ? std::ceil(s0y) : y0f + 1.0f;
+    float b = fmin_((dy * c + dx * (ytop - s0y)) * idxdy, 0.99999994f);
+    float err = std::floor(a * (float(count) - 1.0f) + b) - float(count_x);
+    if (err != 0.0f) a -= std::copysign(2e-7f, err);
+    float x0f = xt0 * sign + (pos ? 0.0f : -1.0f);
+    float xmin = fmin_(s0x, s1x);
+    if (s0y >= float(y1) || s1y <= float(y0) + TOP_TOUCH_EPSILON || xmin >= float(x1)) return 0;
+    uint32_t imin = 0, imax = count;
+    if (s0y < float(y0)) {
+        float f = std::round((float(y0) - y0f + b - a) / (1.0f - a)) - 1.0f;
+        if (y0f + f - std::floor(a * f + b) < float(y0)) f += 1.0f;
+        imin = f2u(f);
+    }
+    if (s1y > float(y1)) {
+        float f = std::round((float(y1) - y0f + b - a) / (1.0f - a)) - 1.0f;
+        if (y0f + f - std::floor(a * f + b) < float(y1)) f += 1.0f;
+        imax = f2u(f);
+    }
+    if (fmax_(s0x, s1x) < float(x0)) {
+        imax = imin;
+    } else {
+        float fudge = pos ? 0.0f : 1.0f;
+        if (xmin < float(x0)) {
+            float f = std::round((sign * (float(x0) - x0f) - b + fudge) / a);
+            if ((x0f + sign * std::floor(a * f + b) < float(x0)) == pos) f += 1.0f;
+            if (pos) { if (f2u(f) > imin) imin = f2u(f); }
+            else if (f2u(f) < imax) imax = f2u(f);
+        }
+        if (fmax_(s0x, s1x) > float(x1)) {
+            float f = std::round((sign * (float(x1) - x0f) - b + fudge) / a);
+            if ((x0f + sign * std::floor(a * f + b) < float(x1)) == pos) f += 1.0f;
+            if (pos) imax = std::min(imax, f2u(f)); else imin = std::max(imin, f2u(f));
+        }
+    }
+    imax = std::max(imin, imax);
+    uint32_t n = 0;
+    for (uint32_t i = imin; i < imax; ++i) {
+        float z = std::floor(a * float(i) + b);
+        int32_t y = f2i(y0f + float(i) - z);
+        int32_t x = f2i(x0f + sign * z);
+        n += (y >= int32_t(y0) && y < int32_t(y1) && x >= int32_t(x0) && x < int32_t(x1)) ? 1u : 0u;
+    }
+    return n;
+}
+
+void or_scan_count(const tk_line* lines, uint64_t line_count, const tk_path_record* paths, uint32_t path_count,
+                   int32_t* backdrops, uint32_t* counts) {
+    for (uint64_t l = 0; l < line_count; ++l) count_line(lines[l], paths, path_count, backdrops, counts);
+}
+
+void or_scan_prefix(const uint32_t* counts, const tk_path_record* paths, uint32_t path_count,
+                    tk_segment_range* ranges, uint32_t* cursors, uint32_t* bumps) {
+    for (uint32_t pid = 0; pid < path_count; ++pid) {
+        const tk_path_record& p = paths[pid];
+        uint32_t next = p.segment_start;
+        for (uint32_t k = 0; k < p.data_len; ++k) {
+            uint32_t t = p.data_offset + k;
+            ranges[t] = {next, next + counts[t]};
+            cursors[t] = next;
+            next += counts[t];
+        }
+        bumps[pid] = next - p.segment_start;
+    }
+}
+
+void or_blur_pass(const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t height, const uint32_t region[4],
+                  const uint32_t source[4], float sigma, uint32_t axis) {
+    blur_pass(src, dst, width, height, region, source, sigma, axis, 1);
+}
+
+float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t backdrop, uint32_t x, uint32_t y) {
+    return fill_value(segments, 0, count, backdrop, x, y);
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+/*
+ * Oracle: CPU restatement of the reference's tile rasterization path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is the checker for the CUDA path:
+ * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may
+ * load it. The product (tileink_b200) never links or calls it.
+ *
+ * It restates, sequentially (or on host threads where the reference runs
+ * independent GPU threads), the HLSL kernels and CPU planners of
+ * Jianqoq/tileink:
+ *   scan    src/shaders/hlsl/scan/{geometry.hlsli,count.hlsl,clip.hlsli,
+ *           emit.hlsl,prefix_chunks.hlsl,chunk_offsets.hlsl,
+ *           apply_chunk_offsets.hlsl}, cumsum.hlsl
+ *   planner src/shared/scan_line.rs, src/shared/gpu_plan/tile_bins/build.rs
+ *   coarse  src/shaders/hlsl/coarse/{count.hlsl,emit.hlsl,classify.hlsli,
+ *           emit_draw.hlsli,emit_stack.hlsli,occlusion.hlsli,prefix.hlsl,
+ *           tile_classification.hlsli}, shared/draw.hlsli
+ *   fine    src/shaders/hlsl/fine/{main.hlsl,interpreter.hlsli,
+ *           specialized.hlsli,clip.hlsli,group.hlsli}, shared/{coverage,
+ *           pixel,affine}.hlsli, shared/brush/{sample,linear,radial,ramp,
+ *           extend}.hlsli
+ *   blur    src/shaders/hlsl/filter/{blur.hlsli,blur_shared.hlsl,blur.hlsl,
+ *           sample.hlsli}, shared/composite_stack.hlsli
+ *
+ * Arithmetic contract: IEEE f32 with no contraction (built with
+ * -ffp-contract=off); HLSL `mad` is a fused multiply-add (std::fma); HLSL
+ * `round` rounds half to even; float->int conversions saturate; RGBA8 target
+ * loads are k/255 and stores round to nearest even. The only freedom the
+ * reference leaves open, the order of atomic increments, is fixed to the
+ * canonical order documented at or_emit_order.
+ */
+#ifndef TILEINK_ORACLE_H
+#define TILEINK_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../include/tileink.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_scene or_scene;
+
+/* Run the full reference frame (scan, cumsum, bins, per-batch coarse+fine,
+ * blur layers) on `threads` host threads. tile_y0/tile_y1 restrict coarse
+ * and fine to tile rows [tile_y0, tile_y1) (tile_y1 == 0: all rows); the
+ * scan always covers every line. */
+int32_t or_run(const tk_scene_desc* scene, int32_t threads, uint32_t tile_y0,
+               uint32_t tile_y1, or_scene** out);
+void or_free(or_scene* s);
+const char* or_error(void);
+
+/* Output access. Returns bytes needed; copies min(bytes, needed) into dst
+ * when dst != NULL. */
+#define OR_COUNTS 0u       /* u32[B] */
+#define OR_BACKDROPS 1u    /* i32[B] after cumsum */
+#define OR_RANGES 2u       /* tk_segment_range[B] */
+#define OR_SEGMENTS 3u     /* tk_line_segment[segment capacity], canonical order */
+#define OR_BATCH_PTCL 4u   /* reference layout PTCL of draw batch `index` */
+#define OR_BATCH_TILES 5u  /* tk_tile_record[T] of draw batch `index` */
+#define OR_BATCH_KINDS 6u  /* u32[T] of draw batch `index` */
+#define OR_IMAGE 7u        /* u32[W*H] final image */
+#define OR_PASS_PTCL 8u    /* merged PTCL of target pass `index` */
+#define OR_PASS_TILES 9u   /* tk_tile_record[T] of target pass `index` */
+#define OR_PASS_KINDS 10u  /* u32[T] of target pass `index` */
+#define OR_PATHS 11u       /* tk_path_record[P] as used */
+#define OR_BUMPS 12u       /* u32[P] per-path segment totals */
+size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_t bytes);
+/* Number of draw batches / target passes in the run. */
+uint32_t or_batch_count(const or_scene* s);
+uint32_t or_pass_count(const or_scene* s);
+/* Stage wall times in seconds: [scan_count, prefix+cumsum, emit, bins,
+ * coarse, fine, blur+composite]. */
+void or_stage_times(const or_scene* s, double out[7]);
+
+/* --- Kernel-level restatements used by the golden tests --------------- */
+
+/* CPU planner: tiles visited by one line inside a tile bbox
+ * (src/shared/scan_line.rs:17-31). */
+uint32_t or_line_scanned_tile_count(const tk_line* line, uint32_t x0, uint32_t y0,
+                                    uint32_t x1, uint32_t y1);
+
+/* scan_count for the given lines into backdrops/counts (accumulating). */
+void or_scan_count(const tk_line* lines, uint64_t line_count, const tk_path_record* paths,
+                   uint32_t path_count, int32_t* backdrops, uint32_t* counts);
+
+/* Per-path prefix (scan_prefix_chunks + chunk_offsets + apply). */
+void or_scan_prefix(const uint32_t* counts, const tk_path_record* paths, uint32_t path_count,
+                    tk_segment_range* ranges, uint32_t* cursors, uint32_t* bumps);
+
+/* One blur pass (filter_blur_shared_region with its global fallback). */
+void or_blur_pass(const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t height,
+                  const uint32_t region[4], const uint32_t source[4], float sigma,
+                  uint32_t axis);
+
+/* Analytic coverage of one pixel by a PTCL fill over the given tile-local
+ * segments, returned before u8 quantization (shared/coverage.hlsli:34-51). */
+float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t backdrop,
+                    uint32_t x, uint32_t y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TILEINK_ORACLE_H */

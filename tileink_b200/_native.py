@@ -1,0 +1,202 @@
+"""ctypes binding of libtileink_b200.so (include/tileink.h, include/tileink_canvas.h).
+
+The record types below are byte-identical to the reference's #[repr(C)] Pod
+records (src/shared/{line,path,draw_record,gpu_coarse,line_seg,tile_seg_range}.rs)
+and are exposed both as ctypes structures and as numpy structured dtypes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libtileink_b200.so"
+
+TILE_SIZE = 16
+INVALID = 0xFFFFFFFF
+
+# Status codes
+TK_OK, TK_E_INVALID, TK_E_CAPACITY, TK_E_CUDA, TK_E_TIMEOUT, TK_E_STATE, TK_E_ALLOC = 0, -1, -2, -3, -4, -5, -6
+
+# Debug stages
+STAGE_COUNTS, STAGE_BACKDROPS, STAGE_RANGES, STAGE_SEGMENTS = 0, 1, 2, 3
+STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS = 4, 5, 6, 7, 8
+
+# PTCL tags (shaders/hlsl/shared/particle_tags.hlsli) + merged-stream marker
+PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
+PTCL_BATCH_BEGIN = 14
+
+OP_DRAW_BATCH, OP_BLUR_BEGIN, OP_BLUR_END = 0, 1, 2
+SCENE_SEGMENTS_FROM_DEVICE = 1
+
+LINE_DTYPE = np.dtype([("path_id", "<u4"), ("pad", "<f4"), ("p0", "<f4", 2), ("p1", "<f4", 2)])
+AFFINE_DTYPE = np.dtype([(k, "<f4") for k in "abcdef"])
+PATH_DTYPE = np.dtype(
+    [(k, "<u4") for k in ("path_id", "line_count", "line_start", "flags", "data_offset", "data_len",
+                          "tile_x0", "tile_y0", "tile_x1", "tile_y1", "segment_start",
+                          "segment_capacity", "segment_count")]
+    + [("transform", AFFINE_DTYPE)]
+)
+BOUNDS_DTYPE = np.dtype([(k, "<i4") for k in ("x0", "y0", "x1", "y1")])
+DRAW_DTYPE = np.dtype(
+    [(k, "<u4") for k in ("path_id", "glyph_run_id", "sdf_offset", "sdf_len", "sdf_shadow_offset",
+                          "sdf_shadow_len", "brush_offset", "brush_len", "tag", "fill_rule")]
+    + [("pixel_bounds", BOUNDS_DTYPE), ("local_pixel_bounds", BOUNDS_DTYPE), ("solid_rect", "<u4"),
+       ("transform", AFFINE_DTYPE), ("inverse_transform", AFFINE_DTYPE)]
+)
+LAYER_DTYPE = np.dtype([("tag", "<u4"), ("draw", "<u4"), ("payload", "<u4")])
+PTCL_DTYPE = np.dtype([("tag", "<u4"), ("backdrop", "<i4"), ("fill_rule", "<u4"), ("segment_start", "<u4"),
+                       ("segment_end", "<u4"), ("color", "<u4")])
+SEGMENT_DTYPE = np.dtype([(k, "<f4") for k in ("p0x", "p0y", "p1x", "p1y", "y_edge")])
+RANGE_DTYPE = np.dtype([("start", "<u4"), ("end", "<u4")])
+TILE_DTYPE = np.dtype([(k, "<u4") for k in ("ptcl_count", "ptcl_start", "ptcl_end", "glyph_count",
+                                            "glyph_start", "glyph_end")])
+OP_DTYPE = np.dtype([("kind", "<u4"), ("batch_id", "<u4"), ("layer_start", "<u4"), ("layer_end", "<u4"),
+                     ("sigma", "<f4"), ("bounds", "<i4", 4)])
+assert LINE_DTYPE.itemsize == 24 and PATH_DTYPE.itemsize == 76 and DRAW_DTYPE.itemsize == 124
+assert LAYER_DTYPE.itemsize == 12 and PTCL_DTYPE.itemsize == 24 and SEGMENT_DTYPE.itemsize == 20
+assert TILE_DTYPE.itemsize == 24 and OP_DTYPE.itemsize == 36
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32), ("height", C.c_uint32), ("clear_color", C.c_uint32), ("flags", C.c_uint32),
+        ("lines", C.c_void_p), ("line_count", C.c_uint64),
+        ("paths", C.c_void_p), ("path_count", C.c_uint32),
+        ("draw_count", C.c_uint32), ("draws", C.c_void_p),
+        ("brush_blob", C.c_void_p), ("brush_word_count", C.c_uint64),
+        ("layers", C.c_void_p), ("layer_count", C.c_uint32),
+        ("draw_order_count", C.c_uint32), ("draw_order", C.c_void_p),
+        ("draw_batch_ids", C.c_void_p),
+        ("ops", C.c_void_p), ("op_count", C.c_uint32), ("reserved", C.c_uint32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [("lines", C.c_uint64), ("backdrop_len", C.c_uint64), ("segments", C.c_uint64),
+                ("ptcl_records", C.c_uint64), ("tile_draw_refs", C.c_uint64), ("fill_particles", C.c_uint64),
+                ("segment_visits", C.c_uint64), ("passes", C.c_uint32), ("tiles", C.c_uint32)]
+
+
+class GradientStop(C.Structure):
+    _fields_ = [("offset", C.c_float), ("rgba", C.c_float * 4)]
+
+
+class BrushDesc(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("extend", C.c_uint32), ("rgba", C.c_float * 4), ("p0", C.c_float * 2),
+                ("p1", C.c_float * 2), ("r0", C.c_float), ("r1", C.c_float), ("stop_count", C.c_uint32),
+                ("stops", C.POINTER(GradientStop))]
+
+
+class GenParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("paths", C.c_uint32), ("variant", C.c_uint32),
+                ("sigma", C.c_float), ("jitter", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+_LIB = None
+
+
+def library() -> C.CDLL:
+    """Load the in-tree native library; raise if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build it with `python -m tileink_b200.build` (nvcc, sm_100a)")
+    lib = C.CDLL(str(LIB_PATH))
+    P, U32, U64, I32, I64, F32, F64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_float, C.c_double
+    sig = {
+        "tk_version": (C.c_char_p, []),
+        "tk_ctx_create": (I32, [I32, C.POINTER(P)]),
+        "tk_ctx_destroy": (None, [P]),
+        "tk_last_error": (C.c_char_p, [P]),
+        "tk_ctx_stream": (P, [P]),
+        "tk_synchronize": (I32, [P]),
+        "tk_scene_upload": (I32, [P, C.POINTER(SceneDesc)]),
+        "tk_render": (I32, [P]),
+        "tk_readback": (I32, [P, P, C.c_size_t]),
+        "tk_render_to_image": (I32, [P, C.POINTER(SceneDesc), P, C.c_size_t]),
+        "tk_get_stats": (I32, [P, C.POINTER(Stats)]),
+        "tk_debug_readback": (I32, [P, U32, U32, P, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "tk_stage_scan_prefix": (I32, [P, P, U64, P, U32, P, P, P]),
+        "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
+        "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
+        "tk_set_timing": (I32, [P, I32]),
+        "tk_get_stage_times": (I32, [P, P, U32]),
+        "tk_probe_fp32_tflops": (I32, [P, C.POINTER(C.c_double)]),
+        "tk_path_new": (P, []),
+        "tk_path_free": (None, [P]),
+        "tk_path_move_to": (None, [P, F64, F64]),
+        "tk_path_line_to": (None, [P, F64, F64]),
+        "tk_path_quad_to": (None, [P, F64, F64, F64, F64]),
+        "tk_path_cubic_to": (None, [P, F64, F64, F64, F64, F64, F64]),
+        "tk_path_close": (None, [P]),
+        "tk_path_flatten": (U64, [P, F32, U32, P, U64]),
+        "tk_canvas_new": (P, [U32, U32, F32]),
+        "tk_canvas_free": (None, [P]),
+        "tk_canvas_set_host_segment_plan": (None, [P, I32]),
+        "tk_canvas_set_clear_color": (None, [P, U32]),
+        "tk_canvas_push_path": (I64, [P, P, C.POINTER(BrushDesc), P, U32, F64]),
+        "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
+        "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
+        "tk_canvas_push_blur_group": (I32, [P, F32]),
+        "tk_canvas_pop_layer": (I32, [P]),
+        "tk_canvas_scene": (I32, [P, C.POINTER(SceneDesc)]),
+        "tk_generate": (P, [U32, U64, C.POINTER(GenParams)]),
+        "tk_canvas_param_points": (U64, [P, P]),
+        "tk_canvas_param_colors": (U64, [P, P]),
+        "tk_plan_line_tile_count": (U32, [P, U32, U32, U32, U32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def ptr(a: np.ndarray | None) -> int | None:
+    return None if a is None or a.size == 0 else a.ctypes.data
+
+
+def desc_to_arrays(d: SceneDesc) -> dict:
+    """Copy a scene description into numpy arrays."""
+    def arr(p, n, dt):
+        if n == 0 or not p:
+            return np.zeros(0, dtype=dt)
+        buf = (C.c_uint8 * (n * np.dtype(dt).itemsize)).from_address(p)
+        return np.frombuffer(buf, dtype=dt).copy()
+    return {
+        "width": d.width, "height": d.height, "clear_color": d.clear_color, "flags": d.flags,
+        "lines": arr(d.lines, d.line_count, LINE_DTYPE),
+        "paths": arr(d.paths, d.path_count, PATH_DTYPE),
+        "draws": arr(d.draws, d.draw_count, DRAW_DTYPE),
+        "brush": arr(d.brush_blob, d.brush_word_count, np.uint32),
+        "layers": arr(d.layers, d.layer_count, LAYER_DTYPE),
+        "draw_order": arr(d.draw_order, d.draw_order_count, np.uint32),
+        "draw_batch_ids": arr(d.draw_batch_ids, d.draw_count, np.uint32),
+        "ops": arr(d.ops, d.op_count, OP_DTYPE),
+    }
+
+
+class ArrayScene:
+    """A scene held in numpy arrays with a SceneDesc pointing into them."""
+
+    def __init__(self, arrays: dict):
+        self.a = {k: (np.ascontiguousarray(v) if isinstance(v, np.ndarray) else v) for k, v in arrays.items()}
+        a = self.a
+        d = SceneDesc()
+        d.width, d.height, d.clear_color, d.flags = a["width"], a["height"], a["clear_color"], a.get("flags", 0)
+        d.lines, d.line_count = ptr(a["lines"]), len(a["lines"])
+        d.paths, d.path_count = ptr(a["paths"]), len(a["paths"])
+        d.draws, d.draw_count = ptr(a["draws"]), len(a["draws"])
+        d.brush_blob, d.brush_word_count = ptr(a["brush"]), len(a["brush"])
+        d.layers, d.layer_count = ptr(a["layers"]), len(a["layers"])
+        d.draw_order, d.draw_order_count = ptr(a["draw_order"]), len(a["draw_order"])
+        d.draw_batch_ids = ptr(a["draw_batch_ids"])
+        d.ops, d.op_count = ptr(a["ops"]), len(a["ops"])
+        self.desc = d

@@ -1,0 +1,202 @@
+"""Scene recording: the reference's `Canvas` recording API for the vector path.
+
+    Canvas.push_path        src/canvas/primitives/paths.rs:50-60
+    Canvas.push_stroke      src/canvas/primitives/paths.rs:24-48
+    Canvas.push_clip_layer  src/canvas/layers.rs:7-28
+    Canvas.push_blur_group  src/canvas/layers.rs:205-212
+    Canvas.pop_layer        src/canvas/layers.rs
+
+Recording, flattening, stroking, brush encoding and batch compilation run in
+the native library (tileink_b200/csrc/canvas.cpp).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+from . import _native as N
+
+FILL_NONZERO, FILL_EVEN_ODD = 0, 1
+EXTEND_PAD, EXTEND_REPEAT, EXTEND_REFLECT = 0, 1, 2
+
+
+class BezPath:
+    """Path builder (kurbo::BezPath): f64 move/line/quad/cubic/close."""
+
+    def __init__(self):
+        self._lib = N.library()
+        self._h = self._lib.tk_path_new()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.tk_path_free(h)
+            self._h = None
+
+    def move_to(self, x, y):
+        self._lib.tk_path_move_to(self._h, float(x), float(y))
+        return self
+
+    def line_to(self, x, y):
+        self._lib.tk_path_line_to(self._h, float(x), float(y))
+        return self
+
+    def quad_to(self, x1, y1, x2, y2):
+        self._lib.tk_path_quad_to(self._h, float(x1), float(y1), float(x2), float(y2))
+        return self
+
+    def cubic_to(self, x1, y1, x2, y2, x3, y3):
+        self._lib.tk_path_cubic_to(self._h, *(float(v) for v in (x1, y1, x2, y2, x3, y3)))
+        return self
+
+    def close(self):
+        self._lib.tk_path_close(self._h)
+        return self
+
+    def flatten(self, tolerance: float, path_id: int = 0) -> np.ndarray:
+        """PathFlatten::flatten (src/shared/path_flatten.rs:20-82) -> Line records."""
+        n = self._lib.tk_path_flatten(self._h, float(tolerance), int(path_id), None, 0)
+        out = np.zeros(n, dtype=N.LINE_DTYPE)
+        self._lib.tk_path_flatten(self._h, float(tolerance), int(path_id), N.ptr(out), n)
+        return out
+
+
+@dataclass
+class Brush:
+    """Solid color or linear/radial gradient with straight RGBA colors in [0, 1]."""
+    kind: int = 0
+    rgba: Sequence[float] = (0.0, 0.0, 0.0, 1.0)
+    p0: Sequence[float] = (0.0, 0.0)
+    p1: Sequence[float] = (0.0, 0.0)
+    r0: float = 0.0
+    r1: float = 0.0
+    stops: Sequence[tuple] = field(default_factory=list)  # (offset, (r, g, b, a))
+    extend: int = EXTEND_PAD
+
+    @staticmethod
+    def solid(r, g, b, a=1.0) -> "Brush":
+        return Brush(kind=0, rgba=(r, g, b, a))
+
+    @staticmethod
+    def linear(p0, p1, stops, extend=EXTEND_PAD) -> "Brush":
+        return Brush(kind=1, p0=p0, p1=p1, stops=list(stops), extend=extend)
+
+    @staticmethod
+    def radial(c0, r0, c1, r1, stops, extend=EXTEND_PAD) -> "Brush":
+        return Brush(kind=2, p0=c0, p1=c1, r0=r0, r1=r1, stops=list(stops), extend=extend)
+
+    def _desc(self):
+        d = N.BrushDesc()
+        d.kind, d.extend = self.kind, self.extend
+        d.rgba[:] = [float(v) for v in self.rgba]
+        d.p0[:] = [float(v) for v in self.p0]
+        d.p1[:] = [float(v) for v in self.p1]
+        d.r0, d.r1 = float(self.r0), float(self.r1)
+        stops = (N.GradientStop * max(1, len(self.stops)))()
+        for i, (off, rgba) in enumerate(self.stops):
+            stops[i].offset = float(off)
+            stops[i].rgba[:] = [float(v) for v in rgba]
+        d.stop_count = len(self.stops)
+        d.stops = C.cast(stops, C.POINTER(N.GradientStop))
+        return d, stops
+
+
+def _affine(transform):
+    if transform is None:
+        return None, None
+    arr = (C.c_double * 6)(*[float(v) for v in transform])
+    return C.cast(arr, C.c_void_p), arr
+
+
+class Canvas:
+    """Immediate-mode recording canvas (src/canvas.rs:86-126)."""
+
+    def __init__(self, width: int, height: int, scale: float = 1.0, *, _handle=None):
+        self._lib = N.library()
+        self._h = _handle if _handle is not None else self._lib.tk_canvas_new(int(width), int(height), float(scale))
+        if not self._h:
+            raise ValueError("invalid canvas surface")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.tk_canvas_free(h)
+            self._h = None
+
+    def set_clear_color(self, premul_rgba8: int):
+        self._lib.tk_canvas_set_clear_color(self._h, int(premul_rgba8) & 0xFFFFFFFF)
+
+    def set_host_segment_plan(self, enabled: bool):
+        self._lib.tk_canvas_set_host_segment_plan(self._h, 1 if enabled else 0)
+
+    def push_path(self, path: BezPath, brush: Brush, transform=None, fill_rule=FILL_NONZERO,
+                  tolerance: float = 0.1) -> int:
+        d, keep = brush._desc()
+        t, tk = _affine(transform)
+        r = self._lib.tk_canvas_push_path(self._h, path._h, C.byref(d), t, int(fill_rule), float(tolerance))
+        if r < 0:
+            raise ValueError("push_path rejected its arguments")
+        return r
+
+    def push_stroke(self, path: BezPath, brush: Brush, width: float, transform=None, tolerance: float = 0.1) -> int:
+        d, keep = brush._desc()
+        t, tk = _affine(transform)
+        r = self._lib.tk_canvas_push_stroke(self._h, path._h, C.byref(d), float(width), t, float(tolerance))
+        if r < 0:
+            raise ValueError("push_stroke rejected its arguments")
+        return r
+
+    def push_clip_layer(self, path: BezPath, transform=None, fill_rule=FILL_NONZERO, tolerance: float = 0.1):
+        t, tk = _affine(transform)
+        if self._lib.tk_canvas_push_clip_layer(self._h, path._h, t, int(fill_rule), float(tolerance)) != 0:
+            raise ValueError("push_clip_layer rejected its arguments")
+
+    def push_blur_group(self, sigma: float):
+        if self._lib.tk_canvas_push_blur_group(self._h, float(sigma)) != 0:
+            raise ValueError("blur sigma must be finite and nonnegative")
+
+    def pop_layer(self):
+        if self._lib.tk_canvas_pop_layer(self._h) != 0:
+            raise ValueError("no layer to pop")
+
+    def scene_desc(self) -> N.SceneDesc:
+        d = N.SceneDesc()
+        if self._lib.tk_canvas_scene(self._h, C.byref(d)) != 0:
+            raise RuntimeError("canvas compile failed")
+        return d
+
+    def scene_arrays(self) -> dict:
+        return N.desc_to_arrays(self.scene_desc())
+
+    def param_points(self) -> np.ndarray:
+        n = self._lib.tk_canvas_param_points(self._h, None)
+        out = np.zeros(n, dtype=np.float64)
+        self._lib.tk_canvas_param_points(self._h, N.ptr(out))
+        return out.reshape(-1, 2)
+
+    def param_colors(self) -> np.ndarray:
+        n = self._lib.tk_canvas_param_colors(self._h, None)
+        out = np.zeros(n, dtype=np.float32)
+        self._lib.tk_canvas_param_colors(self._h, N.ptr(out))
+        return out.reshape(-1, 4)
+
+
+def generate(config: int, seed: int, *, width=0, height=0, paths=0, variant=0, sigma=0.0, jitter=0.0,
+             device_segment_plan=False) -> Canvas:
+    """Seeded synthetic workload (1: 640x360 cubic fills, 2: 4096^2 50k mixed,
+    3: 1920x1080 glyphs, 4: one uneven batch scene, 5: 1024^2 blur group)."""
+    lib = N.library()
+    p = N.GenParams(width, height, paths, variant, sigma, jitter, 1 if device_segment_plan else 0, 0)
+    h = lib.tk_generate(int(config), int(seed), C.byref(p))
+    if not h:
+        raise ValueError(f"unknown workload {config}")
+    return Canvas(0, 0, _handle=h)
+
+
+def plan_line_tile_count(line: np.ndarray, bbox) -> int:
+    """Host scan-line planner (src/shared/scan_line.rs:17-31)."""
+    l = np.ascontiguousarray(np.asarray(line, dtype=N.LINE_DTYPE).reshape(1))
+    return N.library().tk_plan_line_tile_count(N.ptr(l), *[int(v) for v in bbox])

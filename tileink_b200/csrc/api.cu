@@ -1,0 +1,848 @@
+// C ABI of the B200 tile rasterization path: context, scene upload,
+// frame driver, readback, debug readback and stage harnesses.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tileink.h"
+#include "kernels.h"
+
+namespace {
+
+struct Fail {
+    int32_t code;
+    std::string msg;
+};
+
+#define TK_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) throw Fail{TK_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+// Device buffer that only grows.
+template <class T>
+struct DBuf {
+    T* ptr = nullptr;
+    size_t cap = 0;  // elements
+    void reserve(size_t n) {
+        if (n <= cap && ptr) return;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+        size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&ptr, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            ptr = nullptr;
+            throw Fail{TK_E_ALLOC, "device allocation of " + std::to_string(bytes) + " bytes failed"};
+        }
+        cap = std::max<size_t>(n, 1);
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+    }
+};
+
+struct Pass {
+    uint32_t order0 = 0, draw_n = 0, batch0 = 0, batch_n = 0;
+    std::vector<tk::PassBatch> batches;
+    DBuf<tk::PassBatch> d_batches;
+    DBuf<uint32_t> bin_lists, bin_counts;
+    DBuf<tk_tile_record> tiles;
+    DBuf<tk_ptcl_record> ptcl;
+    uint64_t ptcl_needed = 0;  // known after the first frame, 0 = unknown
+    uint64_t ptcl_used = 0;
+};
+
+enum StepKind { STEP_PASS, STEP_BLUR_BEGIN, STEP_BLUR_END };
+struct Step {
+    StepKind kind;
+    uint32_t pass;
+    float sigma;
+    int32_t bounds[4];
+};
+
+}  // namespace
+
+struct tk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    // scene
+    bool have_scene = false;
+    uint32_t width = 0, height = 0, tw = 0, th = 0, clear = 0, flags = 0;
+    uint64_t line_count = 0, brush_words = 0, pool_len = 0, host_segment_capacity = 0;
+    uint32_t path_count = 0, draw_count = 0, layer_count = 0, order_count = 0;
+    std::vector<tk_path_record> h_paths;
+    std::vector<tk::ScanItem> h_items;
+    std::vector<Pass> passes;
+    std::vector<Step> steps;
+    uint64_t tile_draw_refs = 0;
+    // device scene
+    DBuf<tk_line> lines;
+    DBuf<tk_path_record> paths;
+    DBuf<tk_draw_record> draws;
+    DBuf<uint32_t> brush, batch_ids, order;
+    DBuf<tk_layer_record> layers;
+    DBuf<tk::ScanItem> items;
+    DBuf<unsigned long long> item_desc, tile_desc, stats;
+    DBuf<int32_t> backdrops;
+    DBuf<uint32_t> counts, cursors, bumps, misc;  // misc: [0] error [1] ticket [2] seg total [3] ptcl total
+    DBuf<tk_segment_range> ranges;
+    DBuf<tk_line_segment> segments;
+    uint64_t segment_needed = 0;  // device plan: total from the last frame
+    DBuf<uint32_t> image, temp;
+    std::vector<DBuf<uint32_t>> surfaces;
+    bool rendered = false;
+    // stage timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+};
+
+namespace {
+
+int32_t fail(tk_ctx* c, const Fail& f) {
+    if (c) c->error = f.msg;
+    return f.code;
+}
+
+template <class F>
+int32_t guarded(tk_ctx* c, F&& f) {
+    if (!c) return TK_E_INVALID;
+    try {
+        TK_CUDA(cudaSetDevice(c->device));
+        f();
+        return TK_OK;
+    } catch (const Fail& e) {
+        return fail(c, e);
+    } catch (const std::exception& e) {
+        return fail(c, Fail{TK_E_INVALID, e.what()});
+    }
+}
+
+void invalid(const std::string& m) { throw Fail{TK_E_INVALID, m}; }
+
+template <class T>
+void upload(DBuf<T>& b, const T* src, size_t n, cudaStream_t st) {
+    b.reserve(n);
+    if (n) TK_CUDA(cudaMemcpyAsync(b.ptr, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+// Host validation of a scene against the contracts the kernels rely on.
+void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
+    if (d.width == 0 || d.height == 0) invalid("empty canvas");
+    uint32_t tw = (d.width + TK_TILE_SIZE - 1) / TK_TILE_SIZE, th = (d.height + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+    if (uint64_t(tw) * th > 0x7FFFFFFFull || tw > 65535u || th > 65535u) invalid("canvas too large");
+    if ((d.line_count && !d.lines) || (d.path_count && !d.paths) || (d.draw_count && !d.draws) ||
+        (d.brush_word_count && !d.brush_blob) || (d.layer_count && !d.layers) ||
+        (d.draw_order_count && !d.draw_order) || (d.draw_count && !d.draw_batch_ids) || (d.op_count && !d.ops))
+        invalid("null array with nonzero count");
+    bool device_plan = (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+    // Paths: line ranges partition the line array in path order; bbox inside
+    // the canvas; data_len matches the bbox.
+    uint64_t next_line = 0, pool = 0, seg_cap = 0;
+    uint32_t next_data = d.path_count ? d.paths[0].data_offset : 0u;
+    c->h_items.clear();
+    for (uint32_t p = 0; p < d.path_count; ++p) {
+        const tk_path_record& r = d.paths[p];
+        if (r.line_start != next_line) invalid("path " + std::to_string(p) + ": lines are not consecutive per path");
+        next_line += r.line_count;
+        if (r.tile_x1 > tw || r.tile_y1 > th) invalid("path " + std::to_string(p) + ": tile bbox outside the canvas");
+        uint32_t stride = r.tile_x1 > r.tile_x0 ? r.tile_x1 - r.tile_x0 : 0u;
+        uint32_t height = r.tile_y1 > r.tile_y0 ? r.tile_y1 - r.tile_y0 : 0u;
+        if (uint64_t(stride) * height != r.data_len) invalid("path " + std::to_string(p) + ": data_len != bbox tiles");
+        if (stride > tk::kScanItemElems) invalid("path bbox wider than 4096 tiles");
+        if (device_plan && r.data_offset != next_data)
+            invalid("device segment planning needs contiguous backdrop slices in path order");
+        next_data = r.data_offset + r.data_len;
+        pool = std::max<uint64_t>(pool, uint64_t(r.data_offset) + r.data_len);
+        if (pool > 0xFFFFFFFFull) invalid("backdrop pool exceeds u32 indexing");
+        seg_cap = std::max<uint64_t>(seg_cap, uint64_t(r.segment_start) + r.segment_capacity);
+        if (r.data_len) {
+            uint32_t rows_per = std::max<uint32_t>(1u, tk::kScanItemElems / stride);
+            for (uint32_t row = 0; row < height; row += rows_per)
+                c->h_items.push_back({p, row, std::min(rows_per, height - row), row == 0u ? 1u : 0u});
+        }
+    }
+    if (next_line != d.line_count) invalid("path line ranges do not cover the line array");
+    if (seg_cap > 0xFFFFFFFFull) invalid("segment capacity exceeds u32 indexing");
+    // Draws: only path fills/clips are on this path.
+    for (uint32_t i = 0; i < d.draw_count; ++i) {
+        const tk_draw_record& r = d.draws[i];
+        if (r.glyph_run_id != TK_INVALID_INDEX || r.sdf_offset != TK_INVALID_INDEX ||
+            r.sdf_shadow_offset != TK_INVALID_INDEX)
+            invalid("draw " + std::to_string(i) + ": text/SDF draws are outside this path");
+        if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
+            r.tag != TK_DRAW_ISOLATE)
+            invalid("draw " + std::to_string(i) + ": unsupported tag");
+        if (r.path_id != TK_INVALID_INDEX && r.path_id >= d.path_count) invalid("draw path out of range");
+        if (r.fill_rule > 1u) invalid("bad fill rule");
+    }
+    for (uint32_t i = 0; i < d.layer_count; ++i) {
+        if (d.layers[i].tag == TK_LAYER_BLEND) invalid("blend layers are outside this path");
+        if (d.layers[i].tag > TK_LAYER_BLEND) invalid("bad layer tag");
+        if (d.layers[i].draw >= d.draw_count) invalid("layer draw out of range");
+    }
+    // Painter order grouped by batch in op order.
+    std::vector<uint32_t> batch_draws;
+    for (uint32_t k = 0; k < d.draw_order_count; ++k) {
+        uint32_t di = d.draw_order[k];
+        if (di >= d.draw_count) invalid("draw order out of range");
+        uint32_t b = d.draw_batch_ids[di];
+        if (b == TK_INVALID_INDEX) invalid("ordered draw without a batch");
+        if (b + 1 > batch_draws.size()) batch_draws.resize(b + 1, 0u);
+        if (k && d.draw_batch_ids[d.draw_order[k - 1]] > b) invalid("draw order is not grouped by batch");
+        batch_draws[b]++;
+    }
+    // Ops -> passes and steps.
+    c->passes.clear();
+    c->steps.clear();
+    uint32_t order_pos = 0, depth = 0;
+    int64_t last_batch = -1;
+    bool open = false;
+    for (uint32_t i = 0; i < d.op_count; ++i) {
+        const tk_op& op = d.ops[i];
+        if (op.kind == TK_OP_DRAW_BATCH) {
+            if (int64_t(op.batch_id) != last_batch + 1) invalid("batch ids must be consecutive in op order");
+            last_batch = op.batch_id;
+            if (op.layer_start > op.layer_end || op.layer_end > d.layer_count) invalid("bad batch layer range");
+            if (!open) {
+                c->passes.emplace_back();
+                Pass& p = c->passes.back();
+                p.order0 = order_pos;
+                p.batch0 = op.batch_id;
+                c->steps.push_back({STEP_PASS, uint32_t(c->passes.size() - 1), 0.0f, {0, 0, 0, 0}});
+                open = true;
+            }
+            Pass& p = c->passes.back();
+            uint32_t n = op.batch_id < batch_draws.size() ? batch_draws[op.batch_id] : 0u;
+            p.batches.push_back({op.batch_id, op.layer_start, op.layer_end, 0u});
+            p.batch_n++;
+            p.draw_n += n;
+            order_pos += n;
+        } else if (op.kind == TK_OP_BLUR_BEGIN) {
+            open = false;
+            if (op.layer_end > op.layer_start) invalid("blur groups under clip layers are outside this path");
+            if (!(op.sigma >= 0.0f) || !std::isfinite(op.sigma)) invalid("bad blur sigma");
+            Step s{STEP_BLUR_BEGIN, 0u, op.sigma, {op.bounds[0], op.bounds[1], op.bounds[2], op.bounds[3]}};
+            c->steps.push_back(s);
+            ++depth;
+        } else if (op.kind == TK_OP_BLUR_END) {
+            open = false;
+            if (depth == 0) invalid("unbalanced BLUR_END");
+            --depth;
+            c->steps.push_back({STEP_BLUR_END, 0u, 0.0f, {0, 0, 0, 0}});
+        } else {
+            invalid("bad op kind");
+        }
+    }
+    if (depth) invalid("unbalanced BLUR_BEGIN");
+    if (order_pos != d.draw_order_count) invalid("draw order does not match the batches");
+    c->width = d.width;
+    c->height = d.height;
+    c->tw = tw;
+    c->th = th;
+    c->clear = d.clear_color;
+    c->flags = d.flags;
+    c->line_count = d.line_count;
+    c->path_count = d.path_count;
+    c->draw_count = d.draw_count;
+    c->layer_count = d.layer_count;
+    c->order_count = d.draw_order_count;
+    c->brush_words = d.brush_word_count;
+    c->pool_len = pool;
+    c->host_segment_capacity = seg_cap;
+    c->h_paths.assign(d.paths, d.paths + d.path_count);
+    // bbox tile references (binning work measure)
+    uint64_t refs = 0;
+    for (uint32_t k = 0; k < d.draw_order_count; ++k) {
+        const tk_pixel_bounds& pb = d.draws[d.draw_order[k]].pixel_bounds;
+        auto tmin = [](int32_t v, uint32_t lim) { return v > 0 ? std::min(uint32_t(v) / TK_TILE_SIZE, lim) : 0u; };
+        auto tmax = [](int32_t v, uint32_t lim) {
+            return v > 0 ? std::min((uint32_t(v) + TK_TILE_SIZE - 1) / TK_TILE_SIZE, lim) : 0u;
+        };
+        uint32_t x0 = tmin(pb.x0, tw), x1 = tmax(pb.x1, tw), y0 = tmin(pb.y0, th), y1 = tmax(pb.y1, th);
+        if (x1 > x0 && y1 > y0) refs += uint64_t(x1 - x0) * (y1 - y0);
+    }
+    c->tile_draw_refs = refs;
+}
+
+tk::SceneView view(tk_ctx* c) {
+    tk::SceneView s{};
+    s.lines = c->lines.ptr;
+    s.line_count = c->line_count;
+    s.paths = c->paths.ptr;
+    s.path_count = c->path_count;
+    s.draws = c->draws.ptr;
+    s.draw_count = c->draw_count;
+    s.brush = c->brush.ptr;
+    s.brush_words = c->brush_words;
+    s.layers = c->layers.ptr;
+    s.batch_ids = c->batch_ids.ptr;
+    s.order = c->order.ptr;
+    s.width = c->width;
+    s.height = c->height;
+    s.tw = c->tw;
+    s.th = c->th;
+    s.backdrops = c->backdrops.ptr;
+    s.counts = c->counts.ptr;
+    s.ranges = c->ranges.ptr;
+    s.cursors = c->cursors.ptr;
+    s.pool_len = c->pool_len;
+    s.segments = c->segments.ptr;
+    s.segment_capacity = c->segments.cap;
+    s.error = c->misc.ptr;
+    return s;
+}
+
+tk::PassView pass_view(tk_ctx* c, Pass& p) {
+    tk::PassView v{};
+    v.order0 = p.order0;
+    v.draw_n = p.draw_n;
+    v.batches = p.d_batches.ptr;
+    v.batch0 = p.batch0;
+    v.batch_n = p.batch_n;
+    v.nbx = (c->tw + 15) / 16;
+    v.nby = (c->th + 15) / 16;
+    v.bin_lists = p.bin_lists.ptr;
+    v.bin_counts = p.bin_counts.ptr;
+    v.tiles = p.tiles.ptr;
+    v.ptcl = p.ptcl.ptr;
+    v.ptcl_capacity = p.ptcl.ptr ? p.ptcl.cap : 0;
+    v.tile_desc = c->tile_desc.ptr;
+    v.ticket = c->misc.ptr + 1;
+    v.ptcl_total = c->misc.ptr + 3;
+    v.stats = c->stats.ptr;
+    return v;
+}
+
+uint32_t read_word(tk_ctx* c, const uint32_t* dptr) {
+    uint32_t v = 0;
+    TK_CUDA(cudaMemcpyAsync(&v, dptr, 4, cudaMemcpyDeviceToHost, c->stream));
+    TK_CUDA(cudaStreamSynchronize(c->stream));
+    return v;
+}
+
+void do_upload(tk_ctx* c, const tk_scene_desc& d) {
+    // A failed upload leaves no renderable scene behind.
+    c->have_scene = false;
+    c->rendered = false;
+    validate_and_plan(c, d);
+    cudaStream_t st = c->stream;
+    upload(c->lines, d.lines, d.line_count, st);
+    upload(c->paths, d.paths, d.path_count, st);
+    upload(c->draws, d.draws, d.draw_count, st);
+    upload(c->brush, d.brush_blob, d.brush_word_count, st);
+    upload(c->layers, d.layers, d.layer_count, st);
+    upload(c->batch_ids, d.draw_batch_ids, d.draw_count, st);
+    upload(c->order, d.draw_order, d.draw_order_count, st);
+    upload(c->items, c->h_items.data(), c->h_items.size(), st);
+    c->item_desc.reserve(c->h_items.size());
+    c->backdrops.reserve(c->pool_len);
+    c->counts.reserve(c->pool_len);
+    c->cursors.reserve(c->pool_len);
+    c->ranges.reserve(c->pool_len);
+    c->bumps.reserve(c->path_count);
+    c->misc.reserve(8);
+    c->stats.reserve(4);
+    uint32_t T = c->tw * c->th;
+    c->tile_desc.reserve((T + 4095) / 4096 + 1);
+    c->image.reserve(uint64_t(c->width) * c->height);
+    bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+    c->segment_needed = device_plan ? 0 : c->host_segment_capacity;
+    if (!device_plan) c->segments.reserve(c->host_segment_capacity + 1);
+    uint32_t nbins = ((c->tw + 15) / 16) * ((c->th + 15) / 16);
+    for (Pass& p : c->passes) {
+        upload(p.d_batches, p.batches.data(), p.batches.size(), st);
+        p.bin_lists.reserve(uint64_t(nbins) * std::max<uint32_t>(p.draw_n, 1));
+        p.bin_counts.reserve(nbins);
+        p.tiles.reserve(T);
+        p.ptcl_needed = 0;
+    }
+    size_t blur_depth = 0, cur = 0;
+    for (const Step& s : c->steps) {
+        if (s.kind == STEP_BLUR_BEGIN) blur_depth = std::max(blur_depth, ++cur);
+        if (s.kind == STEP_BLUR_END) --cur;
+    }
+    if (c->surfaces.size() < blur_depth) c->surfaces.resize(blur_depth);
+    for (size_t i = 0; i < blur_depth; ++i) c->surfaces[i].reserve(uint64_t(c->width) * c->height);
+    if (blur_depth) c->temp.reserve(uint64_t(c->width) * c->height);
+    TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
+    TK_CUDA(cudaGetLastError());
+    c->have_scene = true;
+    c->rendered = false;
+}
+
+void check_error_word(tk_ctx* c) {
+    uint32_t e = read_word(c, c->misc.ptr);
+    if (!e) return;
+    std::string m = "device error flags " + std::to_string(e) + ":";
+    if (e & tk::ERR_LOOKBACK_TIMEOUT) m += " look-back wait gave up;";
+    if (e & tk::ERR_LINE_PATH_MISMATCH) m += " a line's path_id does not match its path's line range;";
+    if (e & tk::ERR_SEGMENT_OVERFLOW) m += " segment capacity exceeded (segment_capacity below the scanned count);";
+    if (e & tk::ERR_PTCL_OVERFLOW) m += " PTCL capacity exceeded;";
+    if (e & tk::ERR_STACK_DEPTH) m += " clip/group stack deeper than supported;";
+    if (e & tk::ERR_UNSUPPORTED) m += " unsupported particle;";
+    TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 4, c->stream));
+    throw Fail{(e & (tk::ERR_SEGMENT_OVERFLOW | tk::ERR_PTCL_OVERFLOW)) ? TK_E_CAPACITY
+               : (e & tk::ERR_LOOKBACK_TIMEOUT)                         ? TK_E_TIMEOUT
+                                                                        : TK_E_INVALID,
+               m};
+}
+
+struct StageMark {
+    tk_ctx* c;
+    int stage;
+    cudaEvent_t a = nullptr;
+    StageMark(tk_ctx* ctx, int s) : c(ctx), stage(s) {
+        if (!c->timing) return;
+        a = next_event(c);
+        cudaEventRecord(a, c->stream);
+    }
+    ~StageMark() {
+        if (!a) return;
+        cudaEvent_t b = next_event(c);
+        cudaEventRecord(b, c->stream);
+        c->marks.push_back({stage, {a, b}});
+    }
+    static cudaEvent_t next_event(tk_ctx* c) {
+        if (c->ev_used == c->ev_pool.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+        return c->ev_pool[c->ev_used++];
+    }
+};
+
+void run_pass(tk_ctx* c, Pass& p, uint32_t* target) {
+    cudaStream_t st = c->stream;
+    tk::SceneView s = view(c);
+    tk::PassView v = pass_view(c, p);
+    {
+        StageMark m(c, 4);
+        tk::launch_bins(s, v, st);
+    }
+    {
+        StageMark m(c, 5);
+        tk::launch_coarse(s, v, false, st);
+        tk::launch_tile_prefix(s, v, st);
+    }
+    if (p.ptcl_needed == 0) {  // first frame of this scene: size the PTCL buffer
+        uint32_t total = read_word(c, c->misc.ptr + 3);
+        p.ptcl_needed = uint64_t(total) + 1;
+        p.ptcl.reserve(p.ptcl_needed);
+        v = pass_view(c, p);
+    }
+    p.ptcl_used = p.ptcl_needed - 1;
+    {
+        StageMark m(c, 6);
+        tk::launch_coarse(s, v, true, st);
+    }
+    {
+        StageMark m(c, 7);
+        tk::launch_fine(s, v, target, st);
+    }
+}
+
+void do_render(tk_ctx* c) {
+    if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
+    cudaStream_t st = c->stream;
+    bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+    tk::SceneView s = view(c);
+    c->ev_used = 0;
+    c->marks.clear();
+    {
+        StageMark m(c, 0);
+        if (c->pool_len) {
+            TK_CUDA(cudaMemsetAsync(c->backdrops.ptr, 0, c->pool_len * 4, st));
+            TK_CUDA(cudaMemsetAsync(c->counts.ptr, 0, c->pool_len * 4, st));
+        }
+        TK_CUDA(cudaMemsetAsync(c->stats.ptr, 0, 4 * sizeof(unsigned long long), st));
+    }
+    {
+        StageMark m(c, 1);
+        tk::launch_scan_count(s, st);
+    }
+    const uint32_t device_base = 0u;  // Canvas segment slices start at 0 (canvas/paths.rs:117)
+    {
+        StageMark m(c, 2);
+        tk::launch_pool_scan(s, c->items.ptr, uint32_t(c->h_items.size()), c->item_desc.ptr, c->misc.ptr + 1,
+                             device_plan, device_base, c->misc.ptr + 2, st);
+        tk::launch_path_totals(s, c->bumps.ptr, device_plan, c->misc.ptr + 2, st);
+    }
+    if (device_plan && c->segment_needed == 0) {
+        uint32_t total = read_word(c, c->misc.ptr + 2);
+        c->segment_needed = uint64_t(total) + 1;
+        c->segments.reserve(c->segment_needed);
+        s = view(c);
+    }
+    s.segment_capacity = device_plan ? c->segment_needed - 1 : c->host_segment_capacity;
+    {
+        StageMark m(c, 3);
+        tk::launch_scan_emit(s, st);
+    }
+    tk::launch_fill(c->image.ptr, uint64_t(c->width) * c->height, c->clear, st);
+    std::vector<uint32_t*> targets{c->image.ptr};
+    std::vector<const Step*> open;
+    for (const Step& step : c->steps) {
+        if (step.kind == STEP_PASS) {
+            run_pass(c, c->passes[step.pass], targets.back());
+        } else if (step.kind == STEP_BLUR_BEGIN) {
+            uint32_t* surf = c->surfaces[targets.size() - 1].ptr;
+            tk::launch_fill(surf, uint64_t(c->width) * c->height, 0u, st);
+            targets.push_back(surf);
+            open.push_back(&step);
+        } else {
+            const Step& b = *open.back();
+            open.pop_back();
+            uint32_t* surf = targets.back();
+            targets.pop_back();
+            // Output bounds and the surface region they read from
+            // (shared/layer/filter.rs:510-531,599-601).
+            int32_t W = int32_t(c->width), H = int32_t(c->height);
+            int32_t ob[4] = {std::max(b.bounds[0], 0), std::max(b.bounds[1], 0), std::min(b.bounds[2], W),
+                             std::min(b.bounds[3], H)};
+            int32_t rad = int32_t(std::ceil(std::fmax(b.sigma, 0.0f) * 3.0f));
+            int32_t sx0 = std::max(b.bounds[0] - rad, 0), sy0 = std::max(b.bounds[1] - rad, 0);
+            int32_t sx1 = std::min(b.bounds[2] + rad, W), sy1 = std::min(b.bounds[3] + rad, H);
+            StageMark m(c, 8);
+            if (ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
+                tk::BlurParams bp{};
+                bp.width = c->width;
+                bp.height = c->height;
+                bp.region[0] = uint32_t(sx0);
+                bp.region[1] = uint32_t(sy0);
+                bp.region[2] = uint32_t(sx1 - sx0);
+                bp.region[3] = uint32_t(sy1 - sy0);
+                bp.bounds[0] = sx0;
+                bp.bounds[1] = sy0;
+                bp.bounds[2] = sx1;
+                bp.bounds[3] = sy1;
+                bp.sigma = b.sigma;
+                bp.axis = 0;
+                tk::launch_blur(surf, c->temp.ptr, bp, st);
+                bp.axis = 1;
+                tk::launch_blur(c->temp.ptr, surf, bp, st);
+            }
+            if (ob[2] > ob[0] && ob[3] > ob[1]) tk::launch_composite(targets.back(), surf, c->width, ob, st);
+        }
+    }
+    TK_CUDA(cudaGetLastError());
+    c->rendered = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tk_version(void) { return "tileink_b200 0.1 (sm_100a)"; }
+
+int32_t tk_ctx_create(int32_t device, tk_ctx** out) {
+    if (!out) return TK_E_INVALID;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return TK_E_CUDA;
+    }
+    auto* c = new tk_ctx();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return TK_E_CUDA;
+    }
+    *out = c;
+    return TK_OK;
+}
+
+void tk_ctx_destroy(tk_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    c->lines.release(); c->paths.release(); c->draws.release(); c->brush.release();
+    c->batch_ids.release(); c->order.release(); c->layers.release(); c->items.release();
+    c->item_desc.release(); c->tile_desc.release(); c->stats.release(); c->backdrops.release();
+    c->counts.release(); c->cursors.release(); c->bumps.release(); c->misc.release();
+    c->ranges.release(); c->segments.release(); c->image.release(); c->temp.release();
+    for (auto& s : c->surfaces) s.release();
+    for (auto& p : c->passes) {
+        p.d_batches.release(); p.bin_lists.release(); p.bin_counts.release(); p.tiles.release(); p.ptcl.release();
+    }
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* tk_last_error(const tk_ctx* c) { return c ? c->error.c_str() : "null context"; }
+void* tk_ctx_stream(tk_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int32_t tk_synchronize(tk_ctx* c) {
+    return guarded(c, [&] { TK_CUDA(cudaStreamSynchronize(c->stream)); });
+}
+
+int32_t tk_scene_upload(tk_ctx* c, const tk_scene_desc* d) {
+    if (!d) return fail(c, Fail{TK_E_INVALID, "null scene"});
+    return guarded(c, [&] { do_upload(c, *d); });
+}
+
+int32_t tk_render(tk_ctx* c) {
+    return guarded(c, [&] { do_render(c); });
+}
+
+int32_t tk_readback(tk_ctx* c, uint32_t* rgba8, size_t pixel_count) {
+    return guarded(c, [&] {
+        if (!c->rendered) throw Fail{TK_E_STATE, "nothing rendered"};
+        size_t n = size_t(c->width) * c->height;
+        if (!rgba8 || pixel_count < n) throw Fail{TK_E_INVALID, "readback buffer too small"};
+        TK_CUDA(cudaMemcpyAsync(rgba8, c->image.ptr, n * 4, cudaMemcpyDeviceToHost, c->stream));
+        TK_CUDA(cudaStreamSynchronize(c->stream));
+        check_error_word(c);
+    });
+}
+
+int32_t tk_render_to_image(tk_ctx* c, const tk_scene_desc* d, uint32_t* rgba8, size_t pixel_count) {
+    int32_t rc = tk_scene_upload(c, d);
+    if (rc) return rc;
+    rc = tk_render(c);
+    if (rc) return rc;
+    return tk_readback(c, rgba8, pixel_count);
+}
+
+int32_t tk_get_stats(tk_ctx* c, tk_stats* out) {
+    return guarded(c, [&] {
+        if (!out) throw Fail{TK_E_INVALID, "null stats"};
+        std::memset(out, 0, sizeof(*out));
+        out->lines = c->line_count;
+        out->backdrop_len = c->pool_len;
+        out->tile_draw_refs = c->tile_draw_refs;
+        out->tiles = c->tw * c->th;
+        out->passes = uint32_t(c->passes.size());
+        bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+        if (c->rendered) {
+            TK_CUDA(cudaStreamSynchronize(c->stream));
+            if (device_plan) out->segments = c->segment_needed ? c->segment_needed - 1 : 0;
+            else out->segments = c->host_segment_capacity;
+            for (const Pass& p : c->passes) out->ptcl_records += p.ptcl_used;
+            unsigned long long st[2] = {0, 0};
+            TK_CUDA(cudaMemcpy(st, c->stats.ptr, sizeof(st), cudaMemcpyDeviceToHost));
+            out->fill_particles = st[0];
+            out->segment_visits = st[1];
+        }
+    });
+}
+
+int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, size_t bytes, size_t* needed) {
+    return guarded(c, [&] {
+        if (!c->rendered) throw Fail{TK_E_STATE, "nothing rendered"};
+        TK_CUDA(cudaStreamSynchronize(c->stream));
+        const void* src = nullptr;
+        size_t n = 0;
+        std::vector<uint32_t> kinds;
+        switch (stage) {
+            case TK_STAGE_COUNTS: src = c->counts.ptr; n = c->pool_len * 4; break;
+            case TK_STAGE_BACKDROPS: src = c->backdrops.ptr; n = c->pool_len * 4; break;
+            case TK_STAGE_RANGES: src = c->ranges.ptr; n = c->pool_len * 8; break;
+            case TK_STAGE_SEGMENTS: {
+                bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+                uint64_t cnt = device_plan ? (c->segment_needed ? c->segment_needed - 1 : 0) : c->host_segment_capacity;
+                src = c->segments.ptr;
+                n = cnt * sizeof(tk_line_segment);
+                break;
+            }
+            case TK_STAGE_IMAGE: src = c->image.ptr; n = size_t(c->width) * c->height * 4; break;
+            case TK_STAGE_PATHS: src = c->paths.ptr; n = size_t(c->path_count) * sizeof(tk_path_record); break;
+            case TK_STAGE_PTCL:
+            case TK_STAGE_TILES:
+            case TK_STAGE_KINDS: {
+                if (index >= c->passes.size()) throw Fail{TK_E_INVALID, "pass index out of range"};
+                Pass& p = c->passes[index];
+                uint32_t T = c->tw * c->th;
+                if (stage == TK_STAGE_PTCL) { src = p.ptcl.ptr; n = p.ptcl_used * sizeof(tk_ptcl_record); }
+                else if (stage == TK_STAGE_TILES) { src = p.tiles.ptr; n = size_t(T) * sizeof(tk_tile_record); }
+                else {
+                    std::vector<tk_tile_record> tiles(T);
+                    TK_CUDA(cudaMemcpy(tiles.data(), p.tiles.ptr, T * sizeof(tk_tile_record), cudaMemcpyDeviceToHost));
+                    kinds.resize(T);
+                    for (uint32_t t = 0; t < T; ++t)
+                        kinds[t] = tiles[t].ptcl_count ? TK_TILE_KIND_INTERPRETER : TK_TILE_KIND_EMPTY;
+                    n = size_t(T) * 4;
+                }
+                break;
+            }
+            default: throw Fail{TK_E_INVALID, "unknown stage"};
+        }
+        if (needed) *needed = n;
+        if (!dst) return;
+        size_t k = std::min(n, bytes);
+        if (!kinds.empty()) std::memcpy(dst, kinds.data(), k);
+        else if (k) TK_CUDA(cudaMemcpy(dst, src, k, cudaMemcpyDeviceToHost));
+    });
+}
+
+int32_t tk_set_timing(tk_ctx* c, int32_t enabled) {
+    return guarded(c, [&] { c->timing = enabled != 0; });
+}
+
+int32_t tk_get_stage_times(tk_ctx* c, float* ms, uint32_t count) {
+    return guarded(c, [&] {
+        if (!ms) invalid("null output");
+        for (uint32_t i = 0; i < count; ++i) ms[i] = 0.0f;
+        TK_CUDA(cudaStreamSynchronize(c->stream));
+        for (auto& mk : c->marks) {
+            float t = 0.0f;
+            TK_CUDA(cudaEventElapsedTime(&t, mk.second.first, mk.second.second));
+            if (uint32_t(mk.first) < count) ms[mk.first] += t;
+        }
+    });
+}
+
+int32_t tk_probe_fp32_tflops(tk_ctx* c, double* tflops) {
+    return guarded(c, [&] {
+        if (!tflops) invalid("null output");
+        *tflops = tk::probe_fp32_tflops(c->stream);
+    });
+}
+
+int32_t tk_stage_scan_prefix(tk_ctx* c, const uint32_t* counts, uint64_t pool_len, const tk_path_record* paths,
+                             uint32_t path_count, tk_segment_range* ranges, uint32_t* cursors, uint32_t* bumps) {
+    return guarded(c, [&] {
+        if ((pool_len && (!counts || !ranges || !cursors)) || (path_count && (!paths || !bumps)))
+            invalid("null buffer");
+        std::vector<tk::ScanItem> items;
+        for (uint32_t p = 0; p < path_count; ++p) {
+            const tk_path_record& r = paths[p];
+            uint32_t stride = r.tile_x1 > r.tile_x0 ? r.tile_x1 - r.tile_x0 : 0u;
+            uint32_t height = r.tile_y1 > r.tile_y0 ? r.tile_y1 - r.tile_y0 : 0u;
+            if (uint64_t(stride) * height != r.data_len) invalid("data_len != bbox tiles");
+            if (uint64_t(r.data_offset) + r.data_len > pool_len) invalid("path slice outside the pool");
+            if (stride > tk::kScanItemElems) invalid("bbox wider than 4096 tiles");
+            if (!r.data_len) continue;
+            uint32_t rows_per = std::max<uint32_t>(1u, tk::kScanItemElems / stride);
+            for (uint32_t row = 0; row < height; row += rows_per)
+                items.push_back({p, row, std::min(rows_per, height - row), row == 0u ? 1u : 0u});
+        }
+        cudaStream_t st = c->stream;
+        DBuf<uint32_t> d_counts, d_cursors, d_bumps, d_misc;
+        DBuf<int32_t> d_bd;
+        DBuf<tk_segment_range> d_ranges;
+        DBuf<tk_path_record> d_paths;
+        DBuf<tk::ScanItem> d_items;
+        DBuf<unsigned long long> d_desc;
+        upload(d_counts, counts, pool_len, st);
+        upload(d_cursors, cursors, pool_len, st);
+        upload(d_ranges, ranges, pool_len, st);
+        upload(d_paths, paths, path_count, st);
+        upload(d_items, items.data(), items.size(), st);
+        d_bd.reserve(pool_len);
+        TK_CUDA(cudaMemsetAsync(d_bd.ptr, 0, std::max<uint64_t>(pool_len, 1) * 4, st));
+        d_bumps.reserve(path_count);
+        d_misc.reserve(8);
+        TK_CUDA(cudaMemsetAsync(d_misc.ptr, 0, 32, st));
+        d_desc.reserve(items.size());
+        tk::SceneView s{};
+        s.paths = d_paths.ptr;
+        s.path_count = path_count;
+        s.counts = d_counts.ptr;
+        s.backdrops = d_bd.ptr;
+        s.ranges = d_ranges.ptr;
+        s.cursors = d_cursors.ptr;
+        s.pool_len = pool_len;
+        s.error = d_misc.ptr;
+        tk::launch_pool_scan(s, d_items.ptr, uint32_t(items.size()), d_desc.ptr, d_misc.ptr + 1, false, 0u,
+                             d_misc.ptr + 2, st);
+        tk::launch_path_totals(s, d_bumps.ptr, false, d_misc.ptr + 2, st);
+        TK_CUDA(cudaGetLastError());
+        if (pool_len) {
+            TK_CUDA(cudaMemcpyAsync(ranges, d_ranges.ptr, pool_len * 8, cudaMemcpyDeviceToHost, st));
+            TK_CUDA(cudaMemcpyAsync(cursors, d_cursors.ptr, pool_len * 4, cudaMemcpyDeviceToHost, st));
+        }
+        if (path_count) TK_CUDA(cudaMemcpyAsync(bumps, d_bumps.ptr, path_count * 4, cudaMemcpyDeviceToHost, st));
+        uint32_t err = 0;
+        TK_CUDA(cudaMemcpyAsync(&err, d_misc.ptr, 4, cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        d_counts.release(); d_cursors.release(); d_bumps.release(); d_misc.release(); d_bd.release();
+        d_ranges.release(); d_paths.release(); d_items.release(); d_desc.release();
+        if (err) throw Fail{TK_E_TIMEOUT, "prefix look-back gave up"};
+    });
+}
+
+int32_t tk_stage_scan_count(tk_ctx* c, const tk_line* lines, uint64_t line_count, const tk_path_record* paths,
+                            uint32_t path_count, int32_t* backdrops, uint32_t* counts, uint64_t pool_len) {
+    return guarded(c, [&] {
+        if ((line_count && !lines) || (path_count && !paths) || (pool_len && (!backdrops || !counts)))
+            invalid("null buffer");
+        for (uint32_t p = 0; p < path_count; ++p)
+            if (uint64_t(paths[p].data_offset) + paths[p].data_len > pool_len) invalid("path slice outside the pool");
+        cudaStream_t st = c->stream;
+        DBuf<tk_line> d_lines;
+        DBuf<tk_path_record> d_paths;
+        DBuf<int32_t> d_bd;
+        DBuf<uint32_t> d_counts;
+        upload(d_lines, lines, line_count, st);
+        upload(d_paths, paths, path_count, st);
+        upload(d_bd, backdrops, pool_len, st);
+        upload(d_counts, counts, pool_len, st);
+        tk::SceneView s{};
+        s.lines = d_lines.ptr;
+        s.line_count = line_count;
+        s.paths = d_paths.ptr;
+        s.path_count = path_count;
+        s.backdrops = d_bd.ptr;
+        s.counts = d_counts.ptr;
+        tk::launch_scan_count(s, st);
+        TK_CUDA(cudaGetLastError());
+        if (pool_len) {
+            TK_CUDA(cudaMemcpyAsync(backdrops, d_bd.ptr, pool_len * 4, cudaMemcpyDeviceToHost, st));
+            TK_CUDA(cudaMemcpyAsync(counts, d_counts.ptr, pool_len * 4, cudaMemcpyDeviceToHost, st));
+        }
+        TK_CUDA(cudaStreamSynchronize(st));
+        d_lines.release(); d_paths.release(); d_bd.release(); d_counts.release();
+    });
+}
+
+int32_t tk_stage_blur(tk_ctx* c, const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t height,
+                      const uint32_t region[4], const uint32_t source[4], float sigma, uint32_t axis) {
+    return guarded(c, [&] {
+        if (!src || !dst || !region || !source || width == 0 || height == 0) invalid("bad blur arguments");
+        if (uint64_t(region[0]) + region[2] > width || uint64_t(region[1]) + region[3] > height)
+            invalid("blur region outside the image");
+        if (axis > 1u) invalid("bad axis");
+        cudaStream_t st = c->stream;
+        size_t n = size_t(width) * height;
+        DBuf<uint32_t> d_src, d_dst;
+        upload(d_src, src, n, st);
+        upload(d_dst, dst, n, st);
+        tk::BlurParams b{};
+        b.width = width;
+        b.height = height;
+        std::memcpy(b.region, region, sizeof(b.region));
+        bool sx = source[2] > source[0], sy = source[3] > source[1];
+        b.bounds[0] = int32_t(sx ? source[0] : region[0]);
+        b.bounds[1] = int32_t(sy ? source[1] : region[1]);
+        b.bounds[2] = int32_t(sx ? source[2] : region[0] + region[2]);
+        b.bounds[3] = int32_t(sy ? source[3] : region[1] + region[3]);
+        b.sigma = sigma;
+        b.axis = axis;
+        tk::launch_blur(d_src.ptr, d_dst.ptr, b, st);
+        TK_CUDA(cudaGetLastError());
+        TK_CUDA(cudaMemcpyAsync(dst, d_dst.ptr, n * 4, cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        d_src.release();
+        d_dst.release();
+    });
+}
+
+}  // extern "C"

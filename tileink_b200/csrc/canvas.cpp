@@ -1,0 +1,1071 @@
+// Host-side scene recording: the reference's Canvas for the vector path.
+//
+// Record layouts and allocation rules follow src/canvas/paths.rs:65-156
+// (path records, backdrop pool, segment slices), src/shared/brush.rs:249-340
+// (brush blob), src/canvas/compile.rs:39-331 and
+// src/shared/execution/batches.rs (draw batches, painter order).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <vector>
+
+#include "../../include/tileink.h"
+#include "../../include/tileink_canvas.h"
+#include "planner.h"
+
+namespace {
+
+struct Pt {
+    double x, y;
+};
+inline Pt operator+(Pt a, Pt b) { return {a.x + b.x, a.y + b.y}; }
+inline Pt operator-(Pt a, Pt b) { return {a.x - b.x, a.y - b.y}; }
+inline Pt operator*(Pt a, double s) { return {a.x * s, a.y * s}; }
+
+enum Verb : uint8_t { MOVE, LINE, QUAD, CUBIC, CLOSE };
+struct El {
+    Verb verb;
+    Pt p[3];
+};
+
+}  // namespace
+
+struct tk_path {
+    std::vector<El> els;
+};
+
+namespace {
+
+// --------------------------------------------------------------------------
+// Flattening. Quadratics use the parabola-integral subdivision of R. Levien,
+// "Flattening quadratic Beziers" (2019): map the quadratic onto y = x^2, use
+// closed-form approximations of the arc-length-like integral and its inverse
+// to place n points with equal error. Cubics are first split into m
+// quadratics with the cubic-to-quadratic error bound
+// sqrt(3)/36 * |p3 - 3p2 + 3p1 - p0| / m^3.
+// --------------------------------------------------------------------------
+inline double approx_integral(double x) {
+    const double d = 0.67;
+    return x / (1.0 - d + std::sqrt(std::sqrt(d * d * d * d + 0.25 * x * x)));
+}
+inline double approx_inv_integral(double x) {
+    const double b = 0.39;
+    return x * (1.0 - b + std::sqrt(b * b + 0.25 * x * x));
+}
+inline Pt quad_eval(Pt p0, Pt p1, Pt p2, double t) {
+    double mt = 1.0 - t;
+    return p0 * (mt * mt) + p1 * (2.0 * mt * t) + p2 * (t * t);
+}
+template <class Emit>
+void flatten_quad(Pt p0, Pt p1, Pt p2, double tol, Emit&& emit) {
+    double ddx = 2.0 * p1.x - p0.x - p2.x, ddy = 2.0 * p1.y - p0.y - p2.y;
+    double u0 = (p1.x - p0.x) * ddx + (p1.y - p0.y) * ddy;
+    double u2 = (p2.x - p1.x) * ddx + (p2.y - p1.y) * ddy;
+    double cross = (p2.x - p0.x) * ddy - (p2.y - p0.y) * ddx;
+    double dd = std::hypot(ddx, ddy);
+    if (dd < 1e-12) {
+        emit(p2);
+        return;
+    }
+    double x0 = u0 / cross, x2 = u2 / cross;
+    double scale = std::fabs(cross) / (dd * std::fabs(x2 - x0));
+    if (!(std::isfinite(x0) && std::isfinite(x2) && std::isfinite(scale)) || std::fabs(cross) < 1e-12 * dd * dd) {
+        // Nearly collinear control points: uniform steps with the chord bound
+        // |B''| h^2 / 8 = |dd| h^2 / 4 <= tol.
+        int n = std::max(1, int(std::ceil(std::sqrt(dd / (4.0 * tol)))));
+        for (int i = 1; i < n; ++i) emit(quad_eval(p0, p1, p2, double(i) / n));
+        emit(p2);
+        return;
+    }
+    double a0 = approx_integral(x0), a2 = approx_integral(x2);
+    double count = 0.5 * std::fabs(a2 - a0) * std::sqrt(scale / tol);
+    int n = std::max(1, int(std::ceil(count)));
+    double v0 = approx_inv_integral(a0), v2 = approx_inv_integral(a2);
+    for (int i = 1; i < n; ++i) {
+        double v = approx_inv_integral(a0 + (a2 - a0) * double(i) / n);
+        double t = (v - v0) / (v2 - v0);
+        emit(quad_eval(p0, p1, p2, t));
+    }
+    emit(p2);
+}
+inline Pt cubic_eval(const Pt c[4], double t) {
+    double mt = 1.0 - t;
+    return c[0] * (mt * mt * mt) + c[1] * (3.0 * mt * mt * t) + c[2] * (3.0 * mt * t * t) + c[3] * (t * t * t);
+}
+inline Pt cubic_deriv(const Pt c[4], double t) {
+    double mt = 1.0 - t;
+    return (c[1] - c[0]) * (3.0 * mt * mt) + (c[2] - c[1]) * (6.0 * mt * t) + (c[3] - c[2]) * (3.0 * t * t);
+}
+template <class Emit>
+void flatten_cubic(const Pt c[4], double tol, Emit&& emit) {
+    const double quad_share = 0.1;
+    Pt third{c[3].x - 3.0 * c[2].x + 3.0 * c[1].x - c[0].x, c[3].y - 3.0 * c[2].y + 3.0 * c[1].y - c[0].y};
+    double err = std::sqrt(3.0) / 36.0 * std::hypot(third.x, third.y);
+    int m = std::max(1, int(std::ceil(std::cbrt(err / (quad_share * tol)))));
+    m = std::min(m, 1 << 16);
+    for (int j = 0; j < m; ++j) {
+        double t0 = double(j) / m, t1 = double(j + 1) / m, h = (t1 - t0) / 3.0;
+        Pt q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
+        Pt q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
+        Pt ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
+        if (j == m - 1) q3 = c[3];
+        flatten_quad(q0, ctrl, q3, (1.0 - quad_share) * tol, emit);
+    }
+}
+
+// PathFlatten::flatten (src/shared/path_flatten.rs:20-82): closes open
+// contours whose gap exceeds 1e-6 and drops edges with length^2 <= 1e-24.
+void flatten_path(const tk_path& path, double tol, uint32_t path_id, std::vector<tk_line>& out) {
+    bool has_start = false;
+    Pt start{0, 0}, last{0, 0};
+    auto push = [&](Pt a, Pt b) {
+        double dx = a.x - b.x, dy = a.y - b.y;
+        if (!(dx * dx + dy * dy > 1.0e-12 * 1.0e-12)) return;
+        out.push_back(tk_line{path_id, 0.0f, {float(a.x), float(a.y)}, {float(b.x), float(b.y)}});
+    };
+    auto open_close = [&]() {
+        if (!has_start) return;
+        double dx = start.x - last.x, dy = start.y - last.y;
+        if (dx * dx + dy * dy > 1.0e-6 * 1.0e-6) push(last, start);
+    };
+    auto emit = [&](Pt p) {
+        push(last, p);
+        last = p;
+    };
+    for (const El& e : path.els) {
+        switch (e.verb) {
+            case MOVE:
+                open_close();
+                start = last = e.p[0];
+                has_start = true;
+                break;
+            case LINE:
+                if (has_start) emit(e.p[0]);
+                else { start = last = e.p[0]; has_start = true; }
+                break;
+            case QUAD:
+                if (!has_start) { start = last = e.p[0]; has_start = true; }
+                flatten_quad(last, e.p[0], e.p[1], tol, emit);
+                break;
+            case CUBIC: {
+                if (!has_start) { start = last = e.p[0]; has_start = true; }
+                Pt c[4] = {last, e.p[0], e.p[1], e.p[2]};
+                flatten_cubic(c, tol, emit);
+                break;
+            }
+            case CLOSE:
+                if (has_start) {
+                    push(last, start);
+                    last = start;
+                }
+                break;
+        }
+    }
+    open_close();
+}
+
+// Tight bounding box of the curves (kurbo BezPath::bounding_box).
+struct Box {
+    double x0 = std::numeric_limits<double>::infinity(), y0 = x0, x1 = -x0, y1 = -x0;
+    void add(Pt p) {
+        x0 = std::min(x0, p.x); y0 = std::min(y0, p.y);
+        x1 = std::max(x1, p.x); y1 = std::max(y1, p.y);
+    }
+    bool empty() const { return !(x1 >= x0 && y1 >= y0); }
+};
+void quad_extrema(Pt p0, Pt p1, Pt p2, Box& b) {
+    for (int axis = 0; axis < 2; ++axis) {
+        double a = axis ? p0.y : p0.x, m = axis ? p1.y : p1.x, c = axis ? p2.y : p2.x;
+        double den = a - 2.0 * m + c;
+        if (den != 0.0) {
+            double t = (a - m) / den;
+            if (t > 0.0 && t < 1.0) b.add(quad_eval(p0, p1, p2, t));
+        }
+    }
+}
+void cubic_extrema(const Pt c[4], Box& b) {
+    for (int axis = 0; axis < 2; ++axis) {
+        double p0 = axis ? c[0].y : c[0].x, p1 = axis ? c[1].y : c[1].x;
+        double p2 = axis ? c[2].y : c[2].x, p3 = axis ? c[3].y : c[3].x;
+        double qa = -p0 + 3.0 * p1 - 3.0 * p2 + p3, qb = 2.0 * (p0 - 2.0 * p1 + p2), qc = p1 - p0;
+        double ts[2];
+        int nt = 0;
+        if (std::fabs(qa) < 1e-12) {
+            if (qb != 0.0) ts[nt++] = -qc / qb;
+        } else {
+            double disc = qb * qb - 4.0 * qa * qc;
+            if (disc >= 0.0) {
+                double r = std::sqrt(disc);
+                ts[nt++] = (-qb - r) / (2.0 * qa);
+                ts[nt++] = (-qb + r) / (2.0 * qa);
+            }
+        }
+        for (int k = 0; k < nt; ++k)
+            if (ts[k] > 0.0 && ts[k] < 1.0) b.add(cubic_eval(c, ts[k]));
+    }
+}
+Box path_bbox(const tk_path& path) {
+    Box b;
+    Pt last{0, 0};
+    for (const El& e : path.els) {
+        switch (e.verb) {
+            case MOVE: case LINE: b.add(e.p[0]); last = e.p[0]; break;
+            case QUAD: b.add(e.p[1]); quad_extrema(last, e.p[0], e.p[1], b); last = e.p[1]; break;
+            case CUBIC: {
+                Pt c[4] = {last, e.p[0], e.p[1], e.p[2]};
+                b.add(e.p[2]);
+                cubic_extrema(c, b);
+                last = e.p[2];
+                break;
+            }
+            case CLOSE: break;
+        }
+    }
+    return b;
+}
+
+tk_path transform_path(const tk_path& p, const double m[6]) {
+    tk_path out = p;
+    for (El& e : out.els)
+        for (Pt& q : e.p) q = {m[0] * q.x + m[2] * q.y + m[4], m[1] * q.x + m[3] * q.y + m[5]};
+    return out;
+}
+
+// --------------------------------------------------------------------------
+// Stroking with round joins and round caps: the centerline is flattened, each
+// segment is offset by +-w/2, outer joins get circular arcs, inner joins
+// pivot through the centerline vertex, and open ends get semicircular caps.
+// The outline is filled with the nonzero rule (kurbo::stroke's contract).
+// --------------------------------------------------------------------------
+struct Polyline {
+    std::vector<Pt> pts;
+    bool closed = false;
+};
+std::vector<Polyline> centerlines(const tk_path& path, double tol) {
+    std::vector<Polyline> out;
+    Pt last{0, 0};
+    auto cur = [&]() -> Polyline& { return out.back(); };
+    auto emit = [&](Pt p) {
+        if (out.empty()) out.push_back({{last}, false});
+        Pt q = cur().pts.back();
+        if (std::hypot(p.x - q.x, p.y - q.y) > 1e-9) cur().pts.push_back(p);
+        last = p;
+    };
+    for (const El& e : path.els) {
+        switch (e.verb) {
+            case MOVE: out.push_back({{e.p[0]}, false}); last = e.p[0]; break;
+            case LINE: emit(e.p[0]); break;
+            case QUAD: flatten_quad(last, e.p[0], e.p[1], tol, emit); break;
+            case CUBIC: {
+                Pt c[4] = {last, e.p[0], e.p[1], e.p[2]};
+                flatten_cubic(c, tol, emit);
+                break;
+            }
+            case CLOSE:
+                if (!out.empty()) {
+                    cur().closed = true;
+                    Pt s = cur().pts.front();
+                    if (cur().pts.size() > 1 && std::hypot(s.x - cur().pts.back().x, s.y - cur().pts.back().y) <= 1e-9)
+                        cur().pts.pop_back();
+                    last = s;
+                }
+                break;
+        }
+    }
+    return out;
+}
+void arc_points(Pt c, double r, double a0, double a1, double tol, std::vector<Pt>& out) {
+    // Sweep from angle a0 to a1 (signed) excluding a0, including a1.
+    double sweep = a1 - a0;
+    double step = r > tol ? 2.0 * std::acos(std::max(-1.0, 1.0 - tol / r)) : 3.2;
+    int n = std::max(1, int(std::ceil(std::fabs(sweep) / std::max(step, 1e-3))));
+    for (int i = 1; i <= n; ++i) {
+        double a = a0 + sweep * double(i) / n;
+        out.push_back({c.x + r * std::cos(a), c.y + r * std::sin(a)});
+    }
+}
+// One side of a polyline offset by h > 0 along the left normal (-dy, dx).
+// Outer joins (turning away from the normal) get a circular arc around the
+// vertex; inner joins pivot through the vertex.
+void offset_side(const std::vector<Pt>& v, bool closed, double h, double tol, std::vector<Pt>& out) {
+    size_t n = v.size();
+    size_t segs = closed ? n : n - 1;
+    auto dir = [&](size_t i) {
+        Pt a = v[i % n], b = v[(i + 1) % n];
+        double l = std::hypot(b.x - a.x, b.y - a.y);
+        return Pt{(b.x - a.x) / l, (b.y - a.y) / l};
+    };
+    auto nrm = [](Pt d) { return Pt{-d.y, d.x}; };
+    auto join = [&](Pt vertex, Pt din, Pt dout) {
+        Pt nin = nrm(din), nout = nrm(dout);
+        double cr = din.x * dout.y - din.y * dout.x;
+        if (cr < 0.0) {
+            double s0 = std::atan2(nin.y, nin.x), s1 = std::atan2(nout.y, nout.x);
+            double sw = s1 - s0;
+            while (sw > M_PI) sw -= 2 * M_PI;
+            while (sw < -M_PI) sw += 2 * M_PI;
+            arc_points(vertex, h, s0, s0 + sw, tol, out);
+        } else {
+            out.push_back(vertex);
+            out.push_back(vertex + nout * h);
+        }
+    };
+    if (closed) {
+        Pt dl = dir(segs - 1);
+        out.push_back(v[0] + nrm(dl) * h);
+        join(v[0], dl, dir(0));
+    } else {
+        out.push_back(v[0] + nrm(dir(0)) * h);
+    }
+    for (size_t i = 0; i < segs; ++i) {
+        Pt d = dir(i);
+        out.push_back(v[(i + 1) % n] + nrm(d) * h);
+        if (i + 1 < segs) join(v[(i + 1) % n], d, dir(i + 1));
+    }
+}
+tk_path stroke_path(const tk_path& path, double width, double tol) {
+    tk_path out;
+    double h = 0.5 * width;
+    auto add_loop = [&](const std::vector<Pt>& raw) {
+        std::vector<Pt> pts;
+        for (const Pt& p : raw)
+            if (pts.empty() || std::hypot(p.x - pts.back().x, p.y - pts.back().y) > 1e-9) pts.push_back(p);
+        while (pts.size() > 1 && std::hypot(pts[0].x - pts.back().x, pts[0].y - pts.back().y) <= 1e-9) pts.pop_back();
+        if (pts.size() < 3) return;
+        out.els.push_back({MOVE, {pts[0], {}, {}}});
+        for (size_t i = 1; i < pts.size(); ++i) out.els.push_back({LINE, {pts[i], {}, {}}});
+        out.els.push_back({CLOSE, {{}, {}, {}}});
+    };
+    for (const Polyline& pl : centerlines(path, tol)) {
+        const auto& v = pl.pts;
+        if (v.size() == 1) {  // dot: round caps make a disc
+            std::vector<Pt> disc{{v[0].x + h, v[0].y}};
+            arc_points(v[0], h, 0.0, 2 * M_PI, tol, disc);
+            disc.pop_back();
+            add_loop(disc);
+            continue;
+        }
+        if (pl.closed && v.size() >= 3) {
+            std::vector<Pt> left, right;
+            offset_side(v, true, h, tol, left);
+            std::vector<Pt> rv(v.rbegin(), v.rend());
+            offset_side(rv, true, h, tol, right);
+            add_loop(left);
+            add_loop(right);
+            continue;
+        }
+        std::vector<Pt> loop;
+        offset_side(v, false, h, tol, loop);
+        size_t n = v.size();
+        Pt de{v[n - 1].x - v[n - 2].x, v[n - 1].y - v[n - 2].y};
+        double ae = std::atan2(de.x, -de.y);  // angle of the left normal (-dy, dx)
+        arc_points(v[n - 1], h, ae, ae - M_PI, tol, loop);
+        std::vector<Pt> rv(v.rbegin(), v.rend());
+        offset_side(rv, false, h, tol, loop);
+        Pt ds{v[1].x - v[0].x, v[1].y - v[0].y};
+        double as = std::atan2(-ds.x, ds.y);  // angle of the right normal
+        arc_points(v[0], h, as, as - M_PI, tol, loop);
+        add_loop(loop);
+    }
+    return out;
+}
+
+// --------------------------------------------------------------------------
+// Brushes (src/shared/brush.rs:249-340, 638-767; src/shared/pixel.rs:14-21).
+// --------------------------------------------------------------------------
+inline uint32_t u8_sat(float v) {
+    if (!(v > 0.0f)) return 0u;
+    if (v >= 255.0f) return 255u;
+    return uint32_t(v);
+}
+inline uint32_t premul_f32_to_u32(const float c[4]) {
+    return u8_sat(c[0] * 255.0f + 0.5f) | (u8_sat(c[1] * 255.0f + 0.5f) << 8) | (u8_sat(c[2] * 255.0f + 0.5f) << 16) |
+           (u8_sat(c[3] * 255.0f + 0.5f) << 24);
+}
+inline uint32_t premul_color(const float rgba[4]) {
+    float p[4] = {rgba[0] * rgba[3], rgba[1] * rgba[3], rgba[2] * rgba[3], rgba[3]};
+    return premul_f32_to_u32(p);
+}
+size_t quantize_ramp_size(float span, size_t stops) {
+    size_t span_samples = size_t(std::ceil(std::max(span, 1.0f) * 2.0f));
+    size_t stop_samples = (std::max<size_t>(stops, 2) - 1) * 16;
+    size_t target = std::min<size_t>(std::max<size_t>(std::max(span_samples, stop_samples), 64), 4096);
+    size_t p = 1;
+    while (p < target) p <<= 1;
+    return std::min<size_t>(p, 4096);
+}
+// Ramp of premultiplied colors; stops interpolated in premultiplied sRGB.
+std::vector<uint32_t> build_ramp(const tk_gradient_stop* stops, uint32_t n, size_t size) {
+    size = std::max<size_t>(size, 2);
+    std::vector<uint32_t> ramp(size, 0u);
+    if (n == 0) return ramp;
+    std::vector<tk_gradient_stop> s(stops, stops + n);
+    std::stable_sort(s.begin(), s.end(), [](const tk_gradient_stop& a, const tk_gradient_stop& b) { return a.offset < b.offset; });
+    for (size_t ix = 0; ix < size; ++ix) {
+        float t = float(ix) / float(size - 1);
+        size_t upper = 0;
+        while (upper < s.size() && s[upper].offset < t) ++upper;
+        const tk_gradient_stop& l = upper == 0 ? s[0] : (upper >= s.size() ? s.back() : s[upper - 1]);
+        const tk_gradient_stop& r = upper == 0 ? s[0] : (upper >= s.size() ? s.back() : s[upper]);
+        float span = r.offset - l.offset;
+        float lt = std::fabs(span) <= 1.1920929e-7f ? 0.0f : std::min(std::max((t - l.offset) / span, 0.0f), 1.0f);
+        float lp[4] = {l.rgba[0] * l.rgba[3], l.rgba[1] * l.rgba[3], l.rgba[2] * l.rgba[3], l.rgba[3]};
+        float rp[4] = {r.rgba[0] * r.rgba[3], r.rgba[1] * r.rgba[3], r.rgba[2] * r.rgba[3], r.rgba[3]};
+        float c[4];
+        for (int k = 0; k < 4; ++k) c[k] = lp[k] + (rp[k] - lp[k]) * lt;
+        ramp[ix] = premul_f32_to_u32(c);
+    }
+    return ramp;
+}
+inline uint32_t fbits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+
+std::pair<uint32_t, uint32_t> push_brush(std::vector<uint32_t>& blob, const tk_brush_desc& b) {
+    uint32_t offset = uint32_t(blob.size());
+    uint32_t data[TK_BRUSH_HEADER_WORDS] = {TK_BRUSH_SOLID, TK_EXTEND_PAD, 0, 0, 0, 0, 0, 255, 0};
+    uint32_t params[TK_BRUSH_PARAM_WORDS] = {};
+    const float ident[6] = {1, 0, 0, 1, 0, 0};
+    std::vector<uint32_t> ramp;
+    if (b.kind == TK_BRUSH_KIND_SOLID) {
+        data[4] = premul_color(b.rgba);
+    } else if (b.kind == TK_BRUSH_KIND_LINEAR) {
+        data[0] = TK_BRUSH_LINEAR;
+        data[1] = b.extend;
+        params[0] = fbits(b.p0[0]); params[1] = fbits(b.p0[1]);
+        params[2] = fbits(b.p1[0]); params[3] = fbits(b.p1[1]);
+        for (int k = 0; k < 6; ++k) params[4 + k] = fbits(ident[k]);
+        float span = std::hypot(b.p1[0] - b.p0[0], b.p1[1] - b.p0[1]);
+        ramp = build_ramp(b.stops, b.stop_count, quantize_ramp_size(span, b.stop_count));
+    } else {
+        data[0] = TK_BRUSH_RADIAL;
+        data[1] = b.extend;
+        params[0] = fbits(b.p0[0]); params[1] = fbits(b.p0[1]);
+        params[2] = fbits(b.p1[0]); params[3] = fbits(b.p1[1]);
+        params[4] = fbits(b.r0); params[5] = fbits(b.r1);
+        for (int k = 0; k < 6; ++k) params[6 + k] = fbits(ident[k]);
+        float cs = std::hypot(b.p1[0] - b.p0[0], b.p1[1] - b.p0[1]);
+        float span = std::max(cs + std::fabs(b.r0) + std::fabs(b.r1), std::fabs(b.r1 - b.r0));
+        ramp = build_ramp(b.stops, b.stop_count, quantize_ramp_size(span, b.stop_count));
+    }
+    if (!ramp.empty()) {
+        data[2] = TK_BRUSH_HEADER_WORDS + TK_BRUSH_PARAM_WORDS;
+        data[3] = uint32_t(ramp.size());
+    }
+    blob.insert(blob.end(), data, data + TK_BRUSH_HEADER_WORDS);
+    blob.insert(blob.end(), params, params + TK_BRUSH_PARAM_WORDS);
+    blob.insert(blob.end(), ramp.begin(), ramp.end());
+    return {offset, uint32_t(blob.size()) - offset};
+}
+
+struct Cmd {
+    enum Kind { DRAW, CLIP, BLUR } kind;
+    uint32_t draw;
+    float sigma;
+    uint32_t children;
+};
+
+}  // namespace
+
+struct tk_canvas {
+    uint32_t W = 0, H = 0, tw = 0, th = 0;
+    float scale = 1.0f;
+    bool host_plan = true;
+    uint32_t clear = 0u;
+    std::vector<tk_line> lines;
+    std::vector<tk_path_record> paths;
+    std::vector<tk_draw_record> draws;
+    std::vector<uint32_t> brush;
+    uint32_t backdrop_pool = 0, tile_cnt = 0;
+    std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
+    std::vector<uint32_t> stack{0};
+    // compiled plan
+    bool dirty = true;
+    std::vector<tk_layer_record> layers;
+    std::vector<tk_op> ops;
+    std::vector<uint32_t> order, batch_ids;
+    // differentiable parameters (fills of recorded paths)
+    std::vector<double> points;
+    std::vector<float> colors;
+};
+
+namespace {
+
+int64_t push_path_with_tag(tk_canvas* c, const tk_path& src, const tk_brush_desc* brush, const double* transform,
+                           uint32_t rule, double tolerance, uint32_t tag, bool emit_command) {
+    uint32_t line_start = uint32_t(c->lines.size());
+    uint32_t path_id = uint32_t(c->paths.size());
+    double s = double(c->scale);
+    double m[6] = {1, 0, 0, 1, 0, 0};
+    if (transform) std::memcpy(m, transform, sizeof(m));
+    double dev[6] = {s * m[0], s * m[1], s * m[2], s * m[3], s * m[4], s * m[5]};
+    tk_path path = transform_path(src, dev);
+    flatten_path(path, tolerance * s, path_id, c->lines);
+    uint32_t line_count = uint32_t(c->lines.size()) - line_start;
+    Box bb = path_bbox(path);
+    tk_pixel_bounds pb{0, 0, 0, 0};
+    if (!bb.empty()) pb = {int32_t(std::floor(bb.x0)), int32_t(std::floor(bb.y0)), int32_t(std::ceil(bb.x1)), int32_t(std::ceil(bb.y1))};
+    // PixelBounds::tile_bbox (src/shared/bounds.rs:113-128)
+    uint32_t tx0 = std::min(uint32_t(std::max(pb.x0, 0)) / TK_TILE_SIZE, c->tw);
+    uint32_t ty0 = std::min(uint32_t(std::max(pb.y0, 0)) / TK_TILE_SIZE, c->th);
+    uint32_t tx1 = std::min((uint32_t(std::max(pb.x1, 0)) + TK_TILE_SIZE - 1) / TK_TILE_SIZE, c->tw);
+    uint32_t ty1 = std::min((uint32_t(std::max(pb.y1, 0)) + TK_TILE_SIZE - 1) / TK_TILE_SIZE, c->th);
+    uint32_t stride = tx1 > tx0 ? tx1 - tx0 : 0u, height = ty1 > ty0 ? ty1 - ty0 : 0u;
+    uint32_t capacity = 0;
+    if (c->host_plan) {
+        for (uint32_t l = 0; l < line_count; ++l)
+            capacity += tk_plan_line_tile_count(&c->lines[line_start + l], tx0, ty0, tx1, ty1);
+    }
+    tk_path_record rec{};
+    rec.path_id = path_id;
+    rec.line_count = line_count;
+    rec.line_start = line_start;
+    rec.data_offset = c->backdrop_pool;
+    rec.data_len = stride * height;
+    rec.tile_x0 = tx0; rec.tile_y0 = ty0; rec.tile_x1 = tx1; rec.tile_y1 = ty1;
+    rec.segment_start = c->tile_cnt;
+    rec.segment_capacity = capacity;
+    rec.transform = tk_affine{1, 0, 0, 1, 0, 0};
+    c->backdrop_pool += stride * height;
+    c->tile_cnt += capacity;
+    c->paths.push_back(rec);
+    tk_brush_desc transparent{};
+    transparent.kind = TK_BRUSH_KIND_SOLID;
+    auto br = push_brush(c->brush, brush ? *brush : transparent);
+    tk_draw_record d{};
+    d.path_id = path_id;
+    d.glyph_run_id = TK_INVALID_INDEX;
+    d.sdf_offset = TK_INVALID_INDEX;
+    d.sdf_shadow_offset = TK_INVALID_INDEX;
+    d.brush_offset = br.first;
+    d.brush_len = br.second;
+    d.tag = tag;
+    d.fill_rule = rule;
+    d.pixel_bounds = pb;
+    d.local_pixel_bounds = pb;
+    d.transform = tk_affine{1, 0, 0, 1, 0, 0};
+    d.inverse_transform = tk_affine{1, 0, 0, 1, 0, 0};
+    uint32_t draw_ix = uint32_t(c->draws.size());
+    c->draws.push_back(d);
+    if (emit_command) c->lists[c->stack.back()].push_back({Cmd::DRAW, draw_ix, 0.0f, 0u});
+    c->dirty = true;
+    return draw_ix;
+}
+
+void paint_bounds(const tk_canvas* c, uint32_t list, tk_pixel_bounds& b, bool& any) {
+    for (const Cmd& cmd : c->lists[list]) {
+        if (cmd.kind == Cmd::DRAW) {
+            const tk_pixel_bounds& p = c->draws[cmd.draw].pixel_bounds;
+            if (p.x0 >= p.x1 || p.y0 >= p.y1) continue;
+            if (!any) { b = p; any = true; }
+            else { b.x0 = std::min(b.x0, p.x0); b.y0 = std::min(b.y0, p.y0); b.x1 = std::max(b.x1, p.x1); b.y1 = std::max(b.y1, p.y1); }
+        } else {
+            paint_bounds(c, cmd.children, b, any);
+        }
+    }
+}
+
+struct Compiled {
+    struct Op {
+        tk_op op;
+        std::vector<uint32_t> draws;
+        std::vector<tk_layer_record> stack;
+    };
+    std::vector<Op> ops;
+};
+
+void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record>& stack, Compiled& out) {
+    std::vector<uint32_t> pending;
+    auto flush = [&]() {
+        if (pending.empty()) return;
+        Compiled::Op op{};
+        op.op.kind = TK_OP_DRAW_BATCH;
+        op.draws = std::move(pending);
+        op.stack = stack;
+        pending.clear();
+        out.ops.push_back(std::move(op));
+    };
+    for (const Cmd& cmd : c->lists[list]) {
+        if (cmd.kind == Cmd::DRAW) {
+            pending.push_back(cmd.draw);
+        } else if (cmd.kind == Cmd::CLIP) {
+            flush();
+            stack.push_back({TK_LAYER_CLIP, cmd.draw, 0u});
+            compile_into(c, cmd.children, stack, out);
+            stack.pop_back();
+        } else {
+            flush();
+            Compiled::Op begin{};
+            begin.op.kind = TK_OP_BLUR_BEGIN;
+            begin.op.sigma = cmd.sigma;
+            begin.stack = stack;  // outer clips
+            tk_pixel_bounds pb{0, 0, 0, 0};
+            bool any = false;
+            paint_bounds(c, cmd.children, pb, any);
+            int32_t out_r = int32_t(std::ceil(std::max(cmd.sigma, 0.0f) * 3.0f));
+            if (any) {
+                begin.op.bounds[0] = std::max(pb.x0 - out_r, 0);
+                begin.op.bounds[1] = std::max(pb.y0 - out_r, 0);
+                begin.op.bounds[2] = std::min(pb.x1 + out_r, int32_t(c->W));
+                begin.op.bounds[3] = std::min(pb.y1 + out_r, int32_t(c->H));
+            }
+            out.ops.push_back(std::move(begin));
+            std::vector<tk_layer_record> inner;
+            compile_into(c, cmd.children, inner, out);
+            Compiled::Op end{};
+            end.op.kind = TK_OP_BLUR_END;
+            out.ops.push_back(std::move(end));
+        }
+    }
+    flush();
+}
+
+void compile(tk_canvas* c) {
+    if (!c->dirty) return;
+    Compiled comp;
+    std::vector<tk_layer_record> stack;
+    compile_into(c, 0, stack, comp);
+    // coalesce adjacent batches with equal stacks (execution/batches.rs)
+    std::vector<Compiled::Op> merged;
+    for (auto& op : comp.ops) {
+        if (op.op.kind == TK_OP_DRAW_BATCH && !merged.empty() && merged.back().op.kind == TK_OP_DRAW_BATCH) {
+            const auto& a = merged.back().stack;
+            bool same = a.size() == op.stack.size();
+            for (size_t i = 0; same && i < a.size(); ++i)
+                same = a[i].tag == op.stack[i].tag && a[i].draw == op.stack[i].draw && a[i].payload == op.stack[i].payload;
+            if (same) {
+                merged.back().draws.insert(merged.back().draws.end(), op.draws.begin(), op.draws.end());
+                continue;
+            }
+        }
+        merged.push_back(std::move(op));
+    }
+    c->layers.clear();
+    c->ops.clear();
+    c->order.clear();
+    c->batch_ids.assign(c->draws.size(), TK_INVALID_INDEX);
+    uint32_t next_batch = 0;
+    for (auto& op : merged) {
+        tk_op o = op.op;
+        o.layer_start = uint32_t(c->layers.size());
+        c->layers.insert(c->layers.end(), op.stack.begin(), op.stack.end());
+        o.layer_end = uint32_t(c->layers.size());
+        if (o.kind == TK_OP_DRAW_BATCH) {
+            o.batch_id = next_batch++;
+            for (uint32_t d : op.draws) {
+                c->order.push_back(d);
+                c->batch_ids[d] = o.batch_id;
+            }
+        }
+        c->ops.push_back(o);
+    }
+    c->dirty = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+tk_path* tk_path_new(void) { return new tk_path(); }
+void tk_path_free(tk_path* p) { delete p; }
+void tk_path_move_to(tk_path* p, double x, double y) { p->els.push_back({MOVE, {{x, y}, {}, {}}}); }
+void tk_path_line_to(tk_path* p, double x, double y) { p->els.push_back({LINE, {{x, y}, {}, {}}}); }
+void tk_path_quad_to(tk_path* p, double x1, double y1, double x2, double y2) {
+    p->els.push_back({QUAD, {{x1, y1}, {x2, y2}, {}}});
+}
+void tk_path_cubic_to(tk_path* p, double x1, double y1, double x2, double y2, double x3, double y3) {
+    p->els.push_back({CUBIC, {{x1, y1}, {x2, y2}, {x3, y3}}});
+}
+void tk_path_close(tk_path* p) { p->els.push_back({CLOSE, {{}, {}, {}}}); }
+
+uint64_t tk_path_flatten(const tk_path* p, float tolerance, uint32_t path_id, tk_line* out, uint64_t cap) {
+    std::vector<tk_line> lines;
+    flatten_path(*p, double(tolerance), path_id, lines);
+    if (out) std::memcpy(out, lines.data(), std::min<uint64_t>(cap, lines.size()) * sizeof(tk_line));
+    return lines.size();
+}
+
+tk_canvas* tk_canvas_new(uint32_t lw, uint32_t lh, float scale) {
+    if (!(scale > 0.0f) || !std::isfinite(scale)) return nullptr;
+    auto* c = new tk_canvas();
+    c->scale = scale;
+    c->W = uint32_t(std::ceil(double(lw) * scale));
+    c->H = uint32_t(std::ceil(double(lh) * scale));
+    c->tw = (c->W + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+    c->th = (c->H + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+    return c;
+}
+void tk_canvas_free(tk_canvas* c) { delete c; }
+void tk_canvas_set_host_segment_plan(tk_canvas* c, int32_t enabled) { c->host_plan = enabled != 0; }
+void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul) { c->clear = premul; }
+
+int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, const double* transform,
+                            uint32_t fill_rule, double tolerance) {
+    if (!c || !path || fill_rule > 1u || !(tolerance > 0.0)) return -1;
+    return push_path_with_tag(c, *path, brush, transform, fill_rule, tolerance, TK_DRAW_BRUSH, true);
+}
+int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, double width,
+                              const double* transform, double tolerance) {
+    if (!c || !path || !(width > 0.0) || !(tolerance > 0.0)) return -1;
+    // Strokes are outlined in the path's local space (kurbo::stroke before
+    // the transform, src/canvas/primitives/paths.rs:24-48).
+    tk_path outline = stroke_path(*path, width, tolerance);
+    return push_path_with_tag(c, outline, brush, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_BRUSH, true);
+}
+int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform, uint32_t rule,
+                                  double tolerance) {
+    if (!c || !path || rule > 1u || !(tolerance > 0.0)) return -1;
+    int64_t draw = push_path_with_tag(c, *path, nullptr, transform, rule, tolerance, TK_DRAW_CLIP, false);
+    uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    c->lists[c->stack.back()].push_back({Cmd::CLIP, uint32_t(draw), 0.0f, child});
+    c->stack.push_back(child);
+    return 0;
+}
+int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) {
+    float physical = sigma * c->scale;
+    if (!(sigma >= 0.0f) || !std::isfinite(physical)) return -1;
+    uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    c->lists[c->stack.back()].push_back({Cmd::BLUR, 0u, physical, child});
+    c->stack.push_back(child);
+    c->dirty = true;
+    return 0;
+}
+int32_t tk_canvas_pop_layer(tk_canvas* c) {
+    if (c->stack.size() <= 1) return -1;
+    c->stack.pop_back();
+    c->dirty = true;
+    return 0;
+}
+
+int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
+    if (!c || !out) return -1;
+    compile(c);
+    std::memset(out, 0, sizeof(*out));
+    out->width = c->W;
+    out->height = c->H;
+    out->clear_color = c->clear;
+    out->flags = c->host_plan ? 0u : TK_SCENE_SEGMENTS_FROM_DEVICE;
+    out->lines = c->lines.data();
+    out->line_count = c->lines.size();
+    out->paths = c->paths.data();
+    out->path_count = uint32_t(c->paths.size());
+    out->draws = c->draws.data();
+    out->draw_count = uint32_t(c->draws.size());
+    out->brush_blob = c->brush.data();
+    out->brush_word_count = c->brush.size();
+    out->layers = c->layers.data();
+    out->layer_count = uint32_t(c->layers.size());
+    out->draw_order = c->order.data();
+    out->draw_order_count = uint32_t(c->order.size());
+    out->draw_batch_ids = c->batch_ids.data();
+    out->ops = c->ops.data();
+    out->op_count = uint32_t(c->ops.size());
+    return 0;
+}
+
+uint64_t tk_canvas_param_points(const tk_canvas* c, double* out) {
+    if (out) std::memcpy(out, c->points.data(), c->points.size() * sizeof(double));
+    return c->points.size();
+}
+uint64_t tk_canvas_param_colors(const tk_canvas* c, float* out) {
+    if (out) std::memcpy(out, c->colors.data(), c->colors.size() * sizeof(float));
+    return c->colors.size();
+}
+
+}  // extern "C"
+
+// Generators live in generate.cpp; they need push_path_with_tag's public
+// counterparts only.
+
+// ---------------------------------------------------------------------------
+// Seeded synthetic workloads (the five measured configurations).
+// ---------------------------------------------------------------------------
+#include <random>
+
+namespace {
+
+struct Rng {
+    std::mt19937_64 g;
+    explicit Rng(uint64_t seed) : g(seed) {}
+    double u01() { return double(g() >> 11) * (1.0 / 9007199254740992.0); }
+    double uniform(double a, double b) { return a + (b - a) * u01(); }
+    uint32_t range(uint32_t a, uint32_t b) { return a + uint32_t(g() % uint64_t(b - a + 1)); }
+    double normal() {
+        double u1 = std::max(u01(), 1e-300), u2 = u01();
+        return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * M_PI * u2);
+    }
+    float f32(double lo, double hi) { return float(uniform(lo, hi)); }
+};
+
+tk_brush_desc solid(float r, float g, float b, float a) {
+    tk_brush_desc d{};
+    d.kind = TK_BRUSH_KIND_SOLID;
+    d.rgba[0] = r; d.rgba[1] = g; d.rgba[2] = b; d.rgba[3] = a;
+    return d;
+}
+
+// Random closed path of `n` cubic segments with f32 control points drawn by `pt`.
+template <class P>
+void random_cubic_path(tk_path* p, uint32_t n, P&& pt, std::vector<double>* record) {
+    auto put = [&](double x, double y) { if (record) { record->push_back(x); record->push_back(y); } };
+    auto a = pt();
+    tk_path_move_to(p, a.first, a.second);
+    put(a.first, a.second);
+    for (uint32_t k = 0; k < n; ++k) {
+        auto c1 = pt(), c2 = pt(), c3 = pt();
+        tk_path_cubic_to(p, c1.first, c1.second, c2.first, c2.second, c3.first, c3.second);
+        put(c1.first, c1.second); put(c2.first, c2.second); put(c3.first, c3.second);
+    }
+    tk_path_close(p);
+}
+
+void gen_uniform_fills(tk_canvas* c, Rng& r, uint32_t w, uint32_t h, uint32_t paths, uint32_t seg_lo, uint32_t seg_hi,
+                       float alpha_lo, bool record) {
+    for (uint32_t i = 0; i < paths; ++i) {
+        tk_path* p = tk_path_new();
+        uint32_t n = r.range(seg_lo, seg_hi);
+        auto pt = [&]() { return std::make_pair(double(r.f32(0.0, w)), double(r.f32(0.0, h))); };
+        random_cubic_path(p, n, pt, record ? &c->points : nullptr);
+        float rgb[3] = {float(r.range(0, 255)) / 255.0f, float(r.range(0, 255)) / 255.0f, float(r.range(0, 255)) / 255.0f};
+        float a = r.f32(alpha_lo, 1.0);
+        tk_brush_desc b = solid(rgb[0], rgb[1], rgb[2], a);
+        if (record) { c->colors.insert(c->colors.end(), {rgb[0], rgb[1], rgb[2], a}); }
+        tk_canvas_push_path(c, p, &b, nullptr, TK_FILL_NONZERO, 0.1);
+        tk_path_free(p);
+    }
+}
+
+tk_brush_desc random_paint(Rng& r, double cx, double cy, std::vector<tk_gradient_stop>& stops) {
+    double kind = r.u01();
+    auto color = [&](float* out) {
+        out[0] = float(r.range(0, 255)) / 255.0f;
+        out[1] = float(r.range(0, 255)) / 255.0f;
+        out[2] = float(r.range(0, 255)) / 255.0f;
+        out[3] = r.f32(0.3, 1.0);
+    };
+    if (kind < 0.5) {
+        tk_brush_desc b{};
+        b.kind = TK_BRUSH_KIND_SOLID;
+        color(b.rgba);
+        return b;
+    }
+    uint32_t ns = r.range(2, 6);
+    stops.resize(ns);
+    for (uint32_t k = 0; k < ns; ++k) {
+        stops[k].offset = ns == 1 ? 0.0f : (k == 0 ? 0.0f : (k + 1 == ns ? 1.0f : r.f32(0.0, 1.0)));
+        color(stops[k].rgba);
+    }
+    tk_brush_desc b{};
+    b.stop_count = ns;
+    b.stops = stops.data();
+    b.extend = r.range(0, 2);
+    if (kind < 0.75) {
+        b.kind = TK_BRUSH_KIND_LINEAR;
+        b.p0[0] = float(cx + 300.0 * r.normal()); b.p0[1] = float(cy + 300.0 * r.normal());
+        b.p1[0] = float(cx + 300.0 * r.normal()); b.p1[1] = float(cy + 300.0 * r.normal());
+    } else {
+        b.kind = TK_BRUSH_KIND_RADIAL;
+        b.p0[0] = float(cx + 100.0 * r.normal()); b.p0[1] = float(cy + 100.0 * r.normal());
+        b.p1[0] = float(cx + 100.0 * r.normal()); b.p1[1] = float(cy + 100.0 * r.normal());
+        b.r0 = r.f32(0.0, 50.0);
+        b.r1 = r.f32(100.0, 600.0);
+    }
+    return b;
+}
+
+// Config 2: mixed fills/strokes clustered around Gaussian centers, half
+// nonzero / half even-odd, solid/linear/radial paint, 10% of paths in clip
+// layers nested 1-4 deep.
+void gen_mixed(tk_canvas* c, Rng& r, uint32_t w, uint32_t h, uint32_t paths) {
+    const uint32_t centers = 200;
+    const double sd = 300.0 * std::min(w, h) / 4096.0;
+    std::vector<std::pair<double, double>> ctr(centers);
+    for (auto& q : ctr) q = {r.uniform(0.0, w), r.uniform(0.0, h)};
+    std::vector<tk_gradient_stop> stops;
+    auto random_segments = [&](tk_path* p, uint32_t n, double cx, double cy, bool close) {
+        auto pt = [&]() { return std::make_pair(double(float(cx + sd * r.normal())), double(float(cy + sd * r.normal()))); };
+        auto a = pt();
+        tk_path_move_to(p, a.first, a.second);
+        for (uint32_t k = 0; k < n; ++k) {
+            if (r.u01() < 0.5) {
+                auto c1 = pt(), c2 = pt(), c3 = pt();
+                tk_path_cubic_to(p, c1.first, c1.second, c2.first, c2.second, c3.first, c3.second);
+            } else {
+                auto c1 = pt(), c2 = pt();
+                tk_path_quad_to(p, c1.first, c1.second, c2.first, c2.second);
+            }
+        }
+        if (close) tk_path_close(p);
+    };
+    uint32_t i = 0;
+    const double group_start = 0.0241;  // ~10% of paths end up clipped
+    while (i < paths) {
+        uint32_t depth = 0, group = 1;
+        if (r.u01() < group_start) {
+            depth = r.range(1, 4);
+            group = std::min(r.range(1, 8), paths - i);
+        }
+        auto k = ctr[r.range(0, centers - 1)];
+        for (uint32_t d = 0; d < depth; ++d) {
+            tk_path* cp = tk_path_new();
+            random_segments(cp, r.range(4, 16), k.first, k.second, true);
+            tk_canvas_push_clip_layer(c, cp, nullptr, TK_FILL_NONZERO, 0.1);
+            tk_path_free(cp);
+        }
+        for (uint32_t g = 0; g < group; ++g, ++i) {
+            auto q = g == 0 ? k : ctr[r.range(0, centers - 1)];
+            if (depth) q = k;
+            tk_path* p = tk_path_new();
+            bool fill = r.u01() < 0.6;
+            random_segments(p, r.range(4, 64), q.first, q.second, fill);
+            tk_brush_desc b = random_paint(r, q.first, q.second, stops);
+            if (fill) {
+                uint32_t rule = r.u01() < 0.5 ? TK_FILL_NONZERO : TK_FILL_EVEN_ODD;
+                tk_canvas_push_path(c, p, &b, nullptr, rule, 0.1);
+            } else {
+                tk_canvas_push_stroke(c, p, &b, r.uniform(0.5, 8.0), nullptr, 0.1);
+            }
+            tk_path_free(p);
+        }
+        for (uint32_t d = 0; d < depth; ++d) tk_canvas_pop_layer(c);
+    }
+}
+
+// Config 3: glyph-like paths (2-4 closed quadratic contours in a unit em box,
+// inner contours reversed so nonzero fill leaves holes) on baseline rows.
+void gen_glyphs(tk_canvas* c, Rng& r, uint32_t w, uint32_t h, uint32_t count) {
+    tk_brush_desc black = solid(0.0f, 0.0f, 0.0f, 1.0f);
+    double x = 2.0, baseline = 0.0, row_em = 0.0;
+    for (uint32_t i = 0; i < count; ++i) {
+        double em = r.uniform(8.0, 64.0);
+        if (x + 0.7 * em > w || baseline == 0.0) {
+            baseline += row_em > 0.0 ? 1.2 * row_em : 0.0;
+            if (baseline == 0.0 || baseline > h + 8.0) baseline = r.uniform(40.0, 70.0);
+            x = r.uniform(0.0, 8.0);
+            row_em = 0.0;
+        }
+        row_em = std::max(row_em, em);
+        double ox = x + r.uniform(0.0, 1.0), oy = baseline + r.uniform(0.0, 1.0);
+        tk_path* p = tk_path_new();
+        uint32_t contours = r.range(2, 4);
+        double cx = 0.5, cy = 0.45, rx = r.uniform(0.25, 0.4), ry = r.uniform(0.3, 0.42);
+        for (uint32_t k = 0; k < contours; ++k) {
+            double ccx = cx, ccy = cy, crx = rx, cry = ry;
+            bool inner = k > 0;
+            if (inner) {
+                crx = r.uniform(0.04, 0.12);
+                cry = r.uniform(0.04, 0.12);
+                ccx = cx + r.uniform(-0.5, 0.5) * (rx - crx);
+                ccy = cy + r.uniform(-0.5, 0.5) * (ry - cry);
+            }
+            uint32_t n = r.range(6, 24);
+            auto at = [&](double ang, double rad_scale) {
+                double sgn = inner ? -1.0 : 1.0;
+                double px = ccx + crx * rad_scale * std::cos(sgn * ang), py = ccy + cry * rad_scale * std::sin(sgn * ang);
+                return std::make_pair(ox + float(px * em), oy + float((py - 0.9) * em));
+            };
+            double jit = 0.08;
+            auto s = at(0.0, 1.0);
+            tk_path_move_to(p, s.first, s.second);
+            for (uint32_t q = 0; q < n; ++q) {
+                double a0 = 2.0 * M_PI * q / n, a1 = 2.0 * M_PI * (q + 1) / n;
+                auto cpt = at(0.5 * (a0 + a1), (1.0 / std::cos(M_PI / n)) * (1.0 + r.uniform(-jit, jit)));
+                auto end = q + 1 == n ? s : at(a1, 1.0 + r.uniform(-jit, jit));
+                tk_path_quad_to(p, cpt.first, cpt.second, end.first, end.second);
+            }
+            tk_path_close(p);
+        }
+        tk_canvas_push_path(c, p, &black, nullptr, TK_FILL_NONZERO, 0.1);
+        tk_path_free(p);
+        x += 0.62 * em;
+    }
+}
+
+}  // namespace
+
+extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_params* o) {
+    tk_gen_params z{};
+    if (!o) o = &z;
+    auto pick = [](uint32_t v, uint32_t d) { return v ? v : d; };
+    tk_canvas* c = nullptr;
+    switch (config) {
+        case 1: {
+            uint32_t w = pick(o->width, 640), h = pick(o->height, 360);
+            c = tk_canvas_new(w, h, 1.0f);
+            c->host_plan = !(o->flags & 1u);
+            c->clear = 0xFFFFFFFFu;
+            Rng r(seed);
+            gen_uniform_fills(c, r, w, h, pick(o->paths, 240), 8, 40, 0.3f, true);
+            break;
+        }
+        case 2: {
+            uint32_t w = pick(o->width, 4096), h = pick(o->height, 4096);
+            c = tk_canvas_new(w, h, 1.0f);
+            c->host_plan = !(o->flags & 1u);
+            c->clear = 0xFFFFFFFFu;
+            Rng r(seed);
+            gen_mixed(c, r, w, h, pick(o->paths, 50000));
+            break;
+        }
+        case 3: {
+            uint32_t w = pick(o->width, 1920), h = pick(o->height, 1080);
+            c = tk_canvas_new(w, h, 1.0f);
+            c->host_plan = !(o->flags & 1u);
+            c->clear = 0xFFFFFFFFu;
+            Rng r(seed);
+            gen_glyphs(c, r, w, h, pick(o->paths, 20000));
+            break;
+        }
+        case 4: {
+            Rng r(seed * 0x9E3779B97F4A7C15ull + o->variant + 1);
+            uint32_t w = o->width ? o->width : uint32_t(std::lround(std::exp(r.uniform(std::log(64.0), std::log(1024.0)))));
+            uint32_t h = o->height ? o->height : uint32_t(std::lround(std::exp(r.uniform(std::log(64.0), std::log(1024.0)))));
+            uint32_t n = o->paths ? o->paths : uint32_t(std::lround(std::exp(r.uniform(std::log(10.0), std::log(2000.0)))));
+            c = tk_canvas_new(w, h, 1.0f);
+            c->host_plan = !(o->flags & 1u);
+            c->clear = 0xFFFFFFFFu;
+            gen_uniform_fills(c, r, w, h, n, 8, 40, 0.3f, false);
+            break;
+        }
+        case 5: {
+            uint32_t w = pick(o->width, 1024), h = pick(o->height, 1024);
+            c = tk_canvas_new(w, h, 1.0f);
+            c->host_plan = !(o->flags & 1u);
+            c->clear = 0xFFFFFFFFu;
+            Rng r(seed);
+            Rng jr(seed ^ 0x6A09E667F3BCC909ull);  // jitter stream, independent of the scene stream
+            float sigma = o->sigma > 0.0f ? o->sigma : 4.0f;
+            tk_canvas_push_blur_group(c, sigma);
+            uint32_t paths = pick(o->paths, 256);
+            for (uint32_t i = 0; i < paths; ++i) {
+                tk_path* p = tk_path_new();
+                auto pt = [&]() { return std::make_pair(double(r.f32(0.0, w)), double(r.f32(0.0, h))); };
+                std::vector<double> pts;
+                random_cubic_path(p, 12, pt, &pts);
+                if (o->jitter > 0.0f) {
+                    tk_path_free(p);
+                    p = tk_path_new();
+                    for (double& v : pts) v = double(float(v + o->jitter * jr.normal()));
+                    tk_path_move_to(p, pts[0], pts[1]);
+                    for (size_t k = 2; k + 5 < pts.size(); k += 6)
+                        tk_path_cubic_to(p, pts[k], pts[k + 1], pts[k + 2], pts[k + 3], pts[k + 4], pts[k + 5]);
+                    tk_path_close(p);
+                }
+                c->points.insert(c->points.end(), pts.begin(), pts.end());
+                float rgba[4] = {r.f32(0.0, 1.0), r.f32(0.0, 1.0), r.f32(0.0, 1.0), r.f32(0.0, 1.0)};
+                c->colors.insert(c->colors.end(), rgba, rgba + 4);
+                tk_brush_desc b = solid(rgba[0], rgba[1], rgba[2], rgba[3]);
+                tk_canvas_push_path(c, p, &b, nullptr, TK_FILL_NONZERO, 0.1);
+                tk_path_free(p);
+            }
+            tk_canvas_pop_layer(c);
+            break;
+        }
+        default:
+            return nullptr;
+    }
+    return c;
+}

@@ -1,0 +1,438 @@
+// Coarse stage: tile binning, per-tile PTCL counting, tile prefix, emission.
+//
+// Binning replaces the reference's CPU TileDrawBins
+// (src/shared/gpu_plan/tile_bins/build.rs:4-83): one CTA per 16x16-tile bin
+// scans the pass's draws in painter order and compacts those whose tile bbox
+// meets the bin, preserving order.
+//
+// Counting and emission follow coarse_count_bins / coarse_emit_bins
+// (coarse/count.hlsl:48-73, coarse/emit.hlsl:82-142): one thread per tile
+// walks the bin's candidates in painter order. All draw batches of a target
+// pass are emitted into one merged stream per tile: each batch with particles
+// in the tile contributes TK_PTCL_BATCH_BEGIN{segment_start = batch id,
+// segment_end = record count, color = kind | skip << 3} followed by the
+// reference batch stream without its END; one END closes the tile.
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "kernels.h"
+
+namespace tk {
+namespace {
+
+using namespace tkd;
+
+constexpr int kBinSide = 16;
+constexpr int kCoarseThreads = kBinSide * kBinSide;
+constexpr uint32_t kChunkClassColor = 1u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
+
+__device__ __forceinline__ uint32_t tile_min_(int32_t px, uint32_t lim) {
+    return px > 0 ? min(uint32_t(px) / TK_TILE_SIZE, lim) : 0u;
+}
+__device__ __forceinline__ uint32_t tile_max_(int32_t px, uint32_t lim) {
+    return px > 0 ? min((uint32_t(px) + TK_TILE_SIZE - 1u) / TK_TILE_SIZE, lim) : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Binning.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    k_bins(const tk_draw_record* __restrict__ draws, const uint32_t* __restrict__ order, uint32_t order0,
+           uint32_t draw_n, uint32_t tw, uint32_t th, uint32_t nbx, uint32_t* bin_lists, uint32_t* bin_counts) {
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_base;
+    const uint32_t bin = blockIdx.x;
+    const uint32_t bx0 = (bin % nbx) * kBinSide, by0 = (bin / nbx) * kBinSide;
+    const uint32_t bx1 = min(bx0 + kBinSide, tw), by1 = min(by0 + kBinSide, th);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_base = 0u;
+    __syncthreads();
+    uint32_t* out = bin_lists + uint64_t(bin) * draw_n;
+    for (uint32_t c = 0; c < draw_n; c += 256u) {
+        uint32_t j = c + threadIdx.x;
+        bool hit = false;
+        uint32_t d = 0;
+        if (j < draw_n) {
+            d = __ldg(order + order0 + j);
+            const tk_pixel_bounds pb = draws[d].pixel_bounds;
+            uint32_t x0 = tile_min_(pb.x0, tw), y0 = tile_min_(pb.y0, th);
+            uint32_t x1 = tile_max_(pb.x1, tw), y1 = tile_max_(pb.y1, th);
+            hit = x0 < x1 && y0 < y1 && x0 < bx1 && x1 > bx0 && y0 < by1 && y1 > by0;
+        }
+        uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) s_warp[warp] = __popc(ballot);
+        __syncthreads();
+        uint32_t before = s_base;
+        for (int w = 0; w < warp; ++w) before += s_warp[w];
+        if (hit) out[before + __popc(ballot & ((1u << lane) - 1u))] = d;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (int w = 0; w < 8; ++w) t += s_warp[w];
+            s_base += t;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bin_counts[bin] = s_base;
+}
+
+// ---------------------------------------------------------------------------
+// Coarse count / emit.
+// ---------------------------------------------------------------------------
+struct DrawInfo {
+    uint32_t draw;
+    uint32_t tx, ty;         // draw tile bbox: x0 | x1 << 16, y0 | y1 << 16
+    uint32_t px, py;         // path tile bbox packed the same way
+    uint32_t data_offset;
+    uint32_t meta;           // tag | fill << 3 | valid_path << 4 | color_candidate << 5 | batch << 8
+    uint32_t color;
+};
+
+struct Ctx {
+    const tk_draw_record* draws;
+    const tk_path_record* paths;
+    uint32_t path_count;
+    const tk_layer_record* layers;
+    const uint32_t* brush;
+    uint64_t brush_words;
+    const int32_t* backdrops;
+    const tk_segment_range* ranges;
+    uint32_t tw, th;
+};
+
+__device__ __forceinline__ uint32_t brush_word(const Ctx& c, uint32_t i) {
+    return i < c.brush_words ? __ldg(c.brush + i) : 0u;
+}
+
+// draw_backdrop (shared/draw.hlsli:40-47) reading records from global memory.
+__device__ uint32_t draw_backdrop_g(const Ctx& c, uint32_t di, uint32_t tx, uint32_t ty) {
+    const tk_draw_record& d = c.draws[di];
+    if (d.path_id == TK_INVALID_INDEX || d.tag > TK_DRAW_PATH_GLYPH || d.path_id >= c.path_count) return TK_INVALID_INDEX;
+    uint32_t lx = tile_min_(d.pixel_bounds.x0, c.tw), ly = tile_min_(d.pixel_bounds.y0, c.th);
+    uint32_t ux = tile_max_(d.pixel_bounds.x1, c.tw), uy = tile_max_(d.pixel_bounds.y1, c.th);
+    if (!(tx >= lx && ty >= ly && tx < ux && ty < uy)) return TK_INVALID_INDEX;
+    const tk_path_record& p = c.paths[d.path_id];
+    if (p.tile_x1 <= p.tile_x0 || tx < p.tile_x0 || ty < p.tile_y0 || tx >= p.tile_x1 || ty >= p.tile_y1)
+        return TK_INVALID_INDEX;
+    return p.data_offset + (ty - p.tile_y0) * (p.tile_x1 - p.tile_x0) + tx - p.tile_x0;
+}
+
+// stack_wrapper_count (coarse/classify.hlsli:11-33).
+__device__ uint32_t stack_wrappers(const Ctx& c, const PassBatch& b, uint32_t tx, uint32_t ty) {
+    uint32_t count = 0;
+    for (uint32_t i = b.layer_start; i < b.layer_end; ++i) {
+        tk_layer_record L = c.layers[i];
+        uint32_t bd = draw_backdrop_g(c, L.draw, tx, ty);
+        if (bd == TK_INVALID_INDEX) return TK_INVALID_INDEX;
+        tk_segment_range r = c.ranges[bd];
+        int32_t w = c.backdrops[bd];
+        uint32_t rule = c.draws[L.draw].fill_rule;
+        bool full = rule == TK_FILL_EVEN_ODD ? (uint32_t(w) & 1u) != 0u : w != 0;
+        if (L.tag == TK_LAYER_CLIP && r.start == r.end && full) continue;
+        if (r.start == r.end && w == 0) return TK_INVALID_INDEX;
+        ++count;
+    }
+    return count;
+}
+
+__device__ __forceinline__ void store_ptcl(tk_ptcl_record* ptcl, uint64_t cap, uint64_t at, uint32_t tag,
+                                           uint32_t winding, uint32_t rule, uint32_t s0, uint32_t s1, uint32_t color,
+                                           uint32_t* error) {
+    if (at >= cap) {
+        atomicOr(error, ERR_PTCL_OVERFLOW);
+        return;
+    }
+    uint2* w = reinterpret_cast<uint2*>(ptcl + at);
+    w[0] = make_uint2(tag, winding);
+    w[1] = make_uint2(rule, s0);
+    w[2] = make_uint2(s1, color);
+}
+
+// emit_stack_begins / emit_stack_ends (coarse/emit_stack.hlsli:9-44).
+__device__ uint64_t emit_stack(const Ctx& c, const PassBatch& b, uint32_t tx, uint32_t ty, bool begin,
+                               tk_ptcl_record* ptcl, uint64_t cap, uint64_t at, uint32_t* error) {
+    uint32_t n = b.layer_end - b.layer_start;
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t i = begin ? b.layer_start + k : b.layer_end - 1u - k;
+        tk_layer_record L = c.layers[i];
+        uint32_t bd = draw_backdrop_g(c, L.draw, tx, ty);
+        tk_segment_range r = c.ranges[bd];
+        uint32_t w = uint32_t(c.backdrops[bd]);
+        uint32_t rule = c.draws[L.draw].fill_rule;
+        bool noop = L.tag == TK_LAYER_CLIP && r.start == r.end &&
+                    (rule == TK_FILL_EVEN_ODD ? (w & 1u) != 0u : w != 0u);
+        if (noop) continue;
+        if (begin) {
+            uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_BEGIN_OPACITY
+                           : (L.tag == TK_LAYER_BLEND ? TK_PTCL_BEGIN_BLEND : TK_PTCL_BEGIN_CLIP);
+            store_ptcl(ptcl, cap, at++, tag, w, rule, r.start, r.end, L.payload, error);
+        } else {
+            uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_END_OPACITY
+                           : (L.tag == TK_LAYER_BLEND ? TK_PTCL_END_BLEND : TK_PTCL_END_CLIP);
+            store_ptcl(ptcl, cap, at++, tag, 0u, 0u, 0u, 0u, 0u, error);
+        }
+    }
+    return at;
+}
+
+// occluded_particle_prefix (coarse/occlusion.hlsli:12-34) over records
+// [start, end) of one batch stream whose END is implied at `end`.
+__device__ uint32_t occluded_prefix_g(const tk_ptcl_record* ptcl, uint64_t start, uint64_t end) {
+    if (end - start + 1u <= 2u) return 0u;  // stream length incl. END
+    uint32_t depth = 0;
+    for (uint64_t cur = end; cur > start;) {
+        --cur;
+        uint32_t tag = ptcl[cur].tag;
+        if (tag == TK_PTCL_END_CLIP || tag == TK_PTCL_END_OPACITY || tag == TK_PTCL_END_BLEND) ++depth;
+        else if (tag == TK_PTCL_BEGIN_CLIP || tag == TK_PTCL_BEGIN_SDF_CLIP || tag == TK_PTCL_BEGIN_OPACITY ||
+                 tag == TK_PTCL_BEGIN_BLEND) {
+            if (depth == 0u) return 0u;
+            --depth;
+        } else if (tag == TK_PTCL_COLOR && depth == 0u && (ptcl[cur].color >> 24) == 255u) {
+            return uint32_t(cur - start);
+        }
+    }
+    return 0u;
+}
+
+template <bool EMIT>
+__global__ void __launch_bounds__(kCoarseThreads)
+    k_coarse(Ctx c, const uint32_t* __restrict__ bin_lists, const uint32_t* __restrict__ bin_counts, uint32_t draw_n,
+             uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
+             uint32_t batch0, tk_tile_record* tiles, tk_ptcl_record* ptcl, uint64_t cap,
+             unsigned long long* stats, uint32_t* error) {
+    __shared__ DrawInfo s_d[kCoarseThreads];
+    const uint32_t bin = blockIdx.x;
+    const uint32_t tx = (bin % nbx) * kBinSide + (threadIdx.x % kBinSide);
+    const uint32_t ty = (bin / nbx) * kBinSide + (threadIdx.x / kBinSide);
+    const bool live = tx < c.tw && ty < c.th;
+    const uint32_t tile = ty * c.tw + tx;
+    const uint32_t* list = bin_lists + uint64_t(bin) * draw_n;
+    const uint32_t n = bin_counts[bin];
+
+    uint64_t at = 0;
+    if (EMIT && live) at = tiles[tile].ptcl_start;
+    uint32_t total = 0;
+    uint32_t cur = 0xFFFFFFFFu, wrappers = 0, nb = 0, flags = 0;
+    bool rejected = false;
+    uint64_t section = 0;
+    unsigned long long fills = 0, visits = 0;
+
+    auto close = [&]() {
+        if (cur == 0xFFFFFFFFu || rejected || nb == 0u) return;
+        total += nb + 2u * wrappers + 1u;
+        if (EMIT) {
+            const PassBatch& b = batches[cur];
+            uint64_t end = emit_stack(c, b, tx, ty, false, ptcl, cap, at, error);
+            uint32_t skip = 0;
+            if (flags & kChunkClassOccluder) skip = wrappers ? 0u : occluded_prefix_g(ptcl, section + 1u, end);
+            uint32_t kind = (flags & kChunkClassOther) ? TK_TILE_KIND_INTERPRETER
+                            : ((flags & kChunkClassColor) ? TK_TILE_KIND_COLOR : TK_TILE_KIND_EMPTY);
+            store_ptcl(ptcl, cap, section, TK_PTCL_BATCH_BEGIN, 0u, 0u, b.batch_id, nb + 2u * wrappers,
+                       kind | (skip << TK_TILE_PREFIX_SHIFT), error);
+            at = end;
+        }
+    };
+
+    for (uint32_t c0 = 0; c0 < n; c0 += kCoarseThreads) {
+        __syncthreads();
+        uint32_t j = c0 + threadIdx.x;
+        if (j < n) {
+            uint32_t di = list[j];
+            const tk_draw_record& d = c.draws[di];
+            DrawInfo info;
+            info.draw = di;
+            info.tx = tile_min_(d.pixel_bounds.x0, c.tw) | (tile_max_(d.pixel_bounds.x1, c.tw) << 16);
+            info.ty = tile_min_(d.pixel_bounds.y0, c.th) | (tile_max_(d.pixel_bounds.y1, c.th) << 16);
+            bool valid_path = d.path_id != TK_INVALID_INDEX && d.tag <= TK_DRAW_PATH_GLYPH && d.path_id < c.path_count;
+            info.px = 0; info.py = 0; info.data_offset = 0;
+            if (valid_path) {
+                const tk_path_record& p = c.paths[d.path_id];
+                info.px = p.tile_x0 | (p.tile_x1 << 16);
+                info.py = p.tile_y0 | (p.tile_y1 << 16);
+                info.data_offset = p.data_offset;
+            }
+            bool color_candidate = false;
+            info.color = di;
+            if (d.tag == TK_DRAW_BRUSH && d.solid_rect != 0u && d.transform.b == 0.0f && d.transform.c == 0.0f &&
+                d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID) {
+                uint32_t col = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
+                if (col != 0u) { color_candidate = true; info.color = col; }
+            }
+            if (d.tag == TK_DRAW_CLIP) info.color = 0u;
+            uint32_t batch = batch_ids[di] - batch0;
+            info.meta = (d.tag & 7u) | ((d.fill_rule & 1u) << 3) | (uint32_t(valid_path) << 4) |
+                        (uint32_t(color_candidate) << 5) | (batch << 8);
+            s_d[threadIdx.x] = info;
+        }
+        __syncthreads();
+        if (!live) continue;
+        uint32_t m = min(uint32_t(kCoarseThreads), n - c0);
+        for (uint32_t k = 0; k < m; ++k) {
+            const DrawInfo& d = s_d[k];
+            if (!(tx >= (d.tx & 0xFFFFu) && tx < (d.tx >> 16) && ty >= (d.ty & 0xFFFFu) && ty < (d.ty >> 16))) continue;
+            uint32_t meta = d.meta;
+            if (!(meta & 16u)) continue;
+            uint32_t px0 = d.px & 0xFFFFu, px1 = d.px >> 16, py0 = d.py & 0xFFFFu, py1 = d.py >> 16;
+            if (px1 <= px0 || tx < px0 || ty < py0 || tx >= px1 || ty >= py1) continue;
+            uint32_t tag = meta & 7u;
+            if (tag != TK_DRAW_BRUSH && tag != TK_DRAW_PATH_GLYPH && tag != TK_DRAW_CLIP) continue;
+            uint32_t bd = d.data_offset + (ty - py0) * (px1 - px0) + tx - px0;
+            tk_segment_range r = c.ranges[bd];
+            uint32_t w = uint32_t(c.backdrops[bd]);
+            if (r.start == r.end && w == 0u) continue;
+            uint32_t batch = meta >> 8;
+            if (batch != cur) {
+                close();
+                cur = batch;
+                nb = 0;
+                wrappers = stack_wrappers(c, batches[batch], tx, ty);
+                rejected = wrappers == TK_INVALID_INDEX;
+                flags = (!rejected && wrappers) ? kChunkClassOther : 0u;
+                if (EMIT && !rejected) {
+                    section = at;
+                    at = emit_stack(c, batches[batch], tx, ty, true, ptcl, cap, at + 1u, error);
+                }
+            }
+            if (rejected) continue;
+            uint32_t ptag = TK_PTCL_FILL;
+            if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
+            else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
+            else if ((meta & 32u) && r.start == r.end) ptag = TK_PTCL_COLOR;
+            if (EMIT) {
+                flags |= ptag == TK_PTCL_COLOR ? kChunkClassColor : kChunkClassOther;
+                uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
+                if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
+                store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
+                if (ptag != TK_PTCL_COLOR) {
+                    fills += 1;
+                    visits += r.end - r.start;
+                }
+            }
+            ++nb;
+        }
+    }
+    if (!live) return;
+    close();
+    if (total) total += 1u;
+    if (EMIT) {
+        if (total) store_ptcl(ptcl, cap, at, TK_PTCL_END, 0u, 0u, 0u, 0u, 0u, error);
+        if (fills) {
+            atomicAdd(stats + 0, fills);
+            atomicAdd(stats + 1, visits);
+        }
+    } else {
+        tiles[tile].ptcl_count = total;
+    }
+}
+
+// Exclusive scan of tile counts into ptcl_start / ptcl_end (coarse/prefix.hlsl:11-63),
+// single pass with decoupled look-back over 4096-tile blocks.
+constexpr int kTileScanThreads = 256, kTilePer = 16, kTileBlock = kTileScanThreads * kTilePer;
+constexpr unsigned long long kAgg = 1ull << 62, kIncl = 2ull << 62;
+
+__global__ void __launch_bounds__(kTileScanThreads)
+    k_tile_prefix(tk_tile_record* tiles, uint32_t T, unsigned long long* desc, uint32_t* ticket, uint32_t* total,
+                  uint32_t* error) {
+    __shared__ uint32_t s_warp[8];
+    __shared__ uint32_t s_blk, s_prefix;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_blk = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t blk = s_blk;
+    const uint32_t base = blk * kTileBlock;
+    uint32_t v[kTilePer];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kTilePer; ++k) {
+        uint32_t t = base + tid * kTilePer + k;
+        v[k] = t < T ? tiles[t].ptcl_count : 0u;
+        sum += v[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t p = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += p;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0, agg = 0;
+    for (int w = 0; w < 8; ++w) {
+        if (w < warp) wpre += s_warp[w];
+        agg += s_warp[w];
+    }
+    if (tid == 0) {
+        uint32_t prefix = 0;
+        if (blk == 0) {
+            atomicExch(desc, kIncl | (unsigned long long)agg);
+        } else {
+            atomicExch(desc + blk, kAgg | (unsigned long long)agg);
+            uint32_t j = blk - 1, spins = 0;
+            for (;;) {
+                unsigned long long d = *((volatile unsigned long long*)(desc + j));
+                unsigned long long st = d & (3ull << 62);
+                if (st == 0ull) {
+                    if (++spins > (1u << 22)) { atomicOr(error, ERR_LOOKBACK_TIMEOUT); break; }
+                    __nanosleep(64);
+                    continue;
+                }
+                prefix += uint32_t(d);
+                if (st == kIncl) break;
+                --j;
+            }
+            __threadfence();
+            atomicExch(desc + blk, kIncl | (unsigned long long)(prefix + agg));
+        }
+        if ((blk + 1u) * kTileBlock >= T) *total = prefix + agg;
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + wpre + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kTilePer; ++k) {
+        uint32_t t = base + tid * kTilePer + k;
+        if (t < T) {
+            tiles[t].ptcl_start = run;
+            tiles[t].ptcl_end = run + v[k];
+            tiles[t].glyph_count = 0u;
+            tiles[t].glyph_start = 0u;
+            tiles[t].glyph_end = 0u;
+        }
+        run += v[k];
+    }
+}
+
+}  // namespace
+
+void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st) {
+    uint32_t nbins = p.nbx * p.nby;
+    if (p.draw_n == 0) {
+        cudaMemsetAsync(p.bin_counts, 0, sizeof(uint32_t) * nbins, st);
+        return;
+    }
+    k_bins<<<nbins, 256, 0, st>>>(s.draws, s.order, p.order0, p.draw_n, s.tw, s.th, p.nbx, p.bin_lists, p.bin_counts);
+}
+
+void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st) {
+    Ctx c{s.draws, s.paths, s.path_count, s.layers, s.brush, s.brush_words, s.backdrops, s.ranges, s.tw, s.th};
+    uint32_t nbins = p.nbx * p.nby;
+    if (emit)
+        k_coarse<true><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
+                                                         p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
+                                                         p.stats, s.error);
+    else
+        k_coarse<false><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
+                                                          p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
+                                                          p.stats, s.error);
+}
+
+void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {
+    uint32_t T = s.tw * s.th;
+    uint32_t blocks = (T + kTileBlock - 1) / kTileBlock;
+    cudaMemsetAsync(p.tile_desc, 0, sizeof(unsigned long long) * blocks, st);
+    cudaMemsetAsync(p.ticket, 0, sizeof(uint32_t), st);
+    k_tile_prefix<<<blocks, kTileScanThreads, 0, st>>>(p.tiles, T, p.tile_desc, p.ticket, p.ptcl_total, s.error);
+}
+
+}  // namespace tk

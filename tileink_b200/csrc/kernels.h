@@ -1,0 +1,101 @@
+// Host-side launchers of the device pipeline (implemented in *.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/tileink.h"
+
+namespace tk {
+
+// Error bits raised by kernels into a device word.
+constexpr uint32_t ERR_LOOKBACK_TIMEOUT = 1u << 0;
+constexpr uint32_t ERR_LINE_PATH_MISMATCH = 1u << 1;
+constexpr uint32_t ERR_SEGMENT_OVERFLOW = 1u << 2;
+constexpr uint32_t ERR_PTCL_OVERFLOW = 1u << 3;
+constexpr uint32_t ERR_STACK_DEPTH = 1u << 4;
+constexpr uint32_t ERR_UNSUPPORTED = 1u << 5;
+
+// One work item of the pool scan: whole rows [row0, row0 + rows) of `path`,
+// at most kScanItemElems elements.
+struct ScanItem {
+    uint32_t path, row0, rows, first;  // first: 1 when row0 == 0
+};
+constexpr uint32_t kScanItemElems = 4096;
+
+// Per draw-batch data of one target pass.
+struct PassBatch {
+    uint32_t batch_id, layer_start, layer_end, pad;
+};
+
+struct SceneView {
+    const tk_line* lines;
+    uint64_t line_count;
+    tk_path_record* paths;
+    uint32_t path_count;
+    const tk_draw_record* draws;
+    uint32_t draw_count;
+    const uint32_t* brush;
+    uint64_t brush_words;
+    const tk_layer_record* layers;
+    const uint32_t* batch_ids;
+    const uint32_t* order;
+    uint32_t width, height, tw, th;
+    // pool
+    int32_t* backdrops;
+    uint32_t* counts;
+    tk_segment_range* ranges;
+    uint32_t* cursors;
+    uint64_t pool_len;
+    tk_line_segment* segments;
+    uint64_t segment_capacity;
+    uint32_t* error;
+};
+
+void launch_scan_count(const SceneView& s, cudaStream_t st);
+// Row-blocked pool scan: segment ranges + cursors (per-path prefix from
+// segment_start, or one chain over all paths when device_plan), and the
+// row-wise backdrop cumsum. `total` receives the last inclusive value.
+void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* desc,
+                      uint32_t* ticket, bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st);
+void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, const uint32_t* total,
+                        cudaStream_t st);
+void launch_scan_emit(const SceneView& s, cudaStream_t st);
+
+// Target pass: binning, coarse count, tile prefix, coarse emit, fine.
+struct PassView {
+    uint32_t order0, draw_n;          // draw_order[order0 .. order0 + draw_n)
+    const PassBatch* batches;         // indexed by batch ordinal within the pass
+    uint32_t batch0;                  // first batch_id of the pass
+    uint32_t batch_n;
+    uint32_t nbx, nby;                // 16x16-tile bins
+    uint32_t* bin_lists;              // nbins * draw_n
+    uint32_t* bin_counts;             // nbins
+    tk_tile_record* tiles;            // T
+    tk_ptcl_record* ptcl;
+    uint64_t ptcl_capacity;
+    unsigned long long* tile_desc;    // lookback descriptors for the tile scan
+    uint32_t* ticket;
+    uint32_t* ptcl_total;
+    unsigned long long* stats;        // [0] fill records, [1] segment visits
+};
+void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
+void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
+void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st);
+void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st);
+
+// Images.
+void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);
+struct BlurParams {
+    uint32_t width, height;
+    uint32_t region[4];   // x0, y0, width, height
+    int32_t bounds[4];    // sample bounds x0, y0, x1, y1
+    float sigma;
+    uint32_t axis;
+};
+void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaStream_t st);
+void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st);
+
+// FP32 FMA peak probe (TFLOP/s).
+double probe_fp32_tflops(cudaStream_t st);
+
+}  // namespace tk

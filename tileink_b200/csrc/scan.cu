@@ -1,0 +1,350 @@
+// Scan stage: tile segment counts, pool prefix + backdrop cumsum, emit.
+//
+// scan_count  (scan/count.hlsl:13-40): one thread per line, atomics into the
+//             path's backdrop slice. Counts and backdrop deltas are sums, so
+//             their order does not matter.
+// pool scan   (scan/prefix_chunks.hlsl, chunk_offsets.hlsl,
+//             apply_chunk_offsets.hlsl, cumsum.hlsl): one CTA per work item of
+//             whole bbox rows; a decoupled look-back chains the items of a path
+//             (or of the whole pool when segment starts are planned on the
+//             device) in one pass, and the row-wise backdrop cumsum is a
+//             segmented scan inside the same CTA.
+// scan_emit   (scan/emit.hlsl:14-28, scan/clip.hlsli:10-75): one warp per
+//             path; lanes take 32 consecutive lines, DDA step r is the outer
+//             loop and lanes rank their slots with __match_any_sync, giving a
+//             fixed segment order inside every tile.
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "kernels.h"
+
+namespace tk {
+namespace {
+
+using namespace tkd;
+
+__device__ __forceinline__ tk_line load_line(const tk_line* lines, uint64_t i) {
+    const uint2* w = reinterpret_cast<const uint2*>(lines + i);
+    uint2 a = __ldg(w), b = __ldg(w + 1), c = __ldg(w + 2);
+    tk_line l;
+    l.path_id = a.x;
+    l.pad = __uint_as_float(a.y);
+    l.p0[0] = __uint_as_float(b.x);
+    l.p0[1] = __uint_as_float(b.y);
+    l.p1[0] = __uint_as_float(c.x);
+    l.p1[1] = __uint_as_float(c.y);
+    return l;
+}
+__device__ __forceinline__ tk_path_record load_path(const tk_path_record* paths, uint32_t i) {
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(paths + i);
+    tk_path_record p;
+    uint32_t* o = reinterpret_cast<uint32_t*>(&p);
+#pragma unroll
+    for (int k = 0; k < 19; ++k) o[k] = w[k];
+    return p;
+}
+
+__global__ void k_scan_count(const tk_line* __restrict__ lines, uint64_t line_count,
+                             const tk_path_record* __restrict__ paths, uint32_t path_count, int32_t* backdrops,
+                             uint32_t* counts) {
+    for (uint64_t li = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; li < line_count;
+         li += uint64_t(gridDim.x) * blockDim.x) {
+        tk_line line = load_line(lines, li);
+        if (line.path_id >= path_count) continue;
+        tk_path_record p = load_path(paths, line.path_id);
+        Scan s;
+        if (!scan_geometry(line, p, s)) continue;
+        int32_t delta = s.down ? -1 : 1;
+        int32_t stride = int32_t(s.bx1 - s.bx0);
+        for (int32_t y = s.ymin; y < s.ymax; ++y) {
+            uint32_t local = uint32_t((y - int32_t(s.by0)) * stride);
+            atomicAdd(backdrops + s.data_offset + local, delta);
+        }
+        float last_z = floorf(s.a * (float(s.imin) - 1.0f) + s.b);
+        for (uint32_t i = s.imin; i < s.imax; ++i) {
+            float z = floorf(s.a * float(i) + s.b);
+            int32_t tx, ty;
+            scan_tile(s, i, z, tx, ty);
+            if (scan_tile_inside(s, tx, ty)) {
+                bool top = last_z == z;
+                if (i == 0u) top = fabsf(s.y0 - s.qy0 * (1.0f / float(TK_TILE_SIZE))) <= SCAN_EPSILON;
+                if (top && tx + 1 < int32_t(s.bx1)) {
+                    int32_t x = max(tx + 1, int32_t(s.bx0));
+                    uint32_t local = uint32_t((ty - int32_t(s.by0)) * stride + x - int32_t(s.bx0));
+                    atomicAdd(backdrops + s.data_offset + local, delta);
+                }
+                atomicAdd(counts + scan_tile_offset(s, tx, ty), 1u);
+            }
+            last_z = z;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pool scan.
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanPerThread = kScanItemElems / kScanThreads;  // 16
+constexpr unsigned long long kStatusAgg = 1ull << 62;
+constexpr unsigned long long kStatusIncl = 2ull << 62;
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// Inclusive warp scan of (flag, value) pairs under the segmented operator
+// (f1, v1) + (f2, v2) = (f1 | f2, f2 ? v2 : v1 + v2).
+__device__ __forceinline__ void warp_seg_scan(uint32_t& f, uint32_t& v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t pf = __shfl_up_sync(0xffffffffu, f, o), pv = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) {
+            v = f ? v : pv + v;
+            f |= pf;
+        }
+    }
+}
+
+// Block-wide exclusive segmented scan of per-thread aggregates.
+__device__ __forceinline__ void block_seg_exclusive(uint32_t f, uint32_t v, uint32_t& ef, uint32_t& ev,
+                                                    uint32_t* sf, uint32_t* sv, uint32_t& tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl_f = f, incl_v = v;
+    warp_seg_scan(incl_f, incl_v);
+    if (lane == 31) { sf[warp] = incl_f; sv[warp] = incl_v; }
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t wf = lane < kScanThreads / 32 ? sf[lane] : 0u, wv = lane < kScanThreads / 32 ? sv[lane] : 0u;
+        warp_seg_scan(wf, wv);
+        if (lane < kScanThreads / 32) { sf[lane + 8] = wf; sv[lane + 8] = wv; }  // inclusive warp prefixes
+    }
+    __syncthreads();
+    // exclusive within warp
+    uint32_t xf = __shfl_up_sync(0xffffffffu, incl_f, 1), xv = __shfl_up_sync(0xffffffffu, incl_v, 1);
+    if (lane == 0) { xf = 0u; xv = 0u; }
+    // combine with the previous warps' inclusive prefix
+    uint32_t pf = warp ? sf[8 + warp - 1] : 0u, pv = warp ? sv[8 + warp - 1] : 0u;
+    ef = pf | xf;
+    ev = xf ? xv : pv + xv;
+    tot = sv[8 + kScanThreads / 32 - 1];
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+    k_pool_scan(const ScanItem* __restrict__ items, uint32_t n_items, tk_path_record* paths, uint32_t* counts,
+                int32_t* backdrops, tk_segment_range* ranges, uint32_t* cursors, unsigned long long* desc,
+                uint32_t* ticket, int device_plan, uint32_t device_base, uint32_t* total, uint32_t* error) {
+    __shared__ uint32_t s_cnt[kScanItemElems];
+    __shared__ int32_t s_bd[kScanItemElems];
+    __shared__ uint32_t s_f[24], s_v[24];
+    __shared__ uint32_t s_item, s_prefix;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_item = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t k = s_item;
+    if (k >= n_items) return;
+    const ScanItem it = items[k];
+    const tk_path_record& p = paths[it.path];
+    const uint32_t stride = p.tile_x1 - p.tile_x0;
+    const uint32_t n = it.rows * stride;
+    const uint64_t e0 = uint64_t(p.data_offset) + uint64_t(it.row0) * stride;
+    for (uint32_t i = tid; i < n; i += kScanThreads) {
+        s_cnt[i] = counts[e0 + i];
+        s_bd[i] = backdrops[e0 + i];
+    }
+    __syncthreads();
+    // thread-local sums over elements [tid*16, tid*16+16)
+    const uint32_t lo = tid * kScanPerThread;
+    uint32_t csum = 0u, bf = 0u, bsum = 0u;
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; ++j) {
+        uint32_t i = lo + j;
+        if (i < n) {
+            csum += s_cnt[i];
+            if (i % stride == 0u) { bf = 1u; bsum = 0u; }
+            bsum += uint32_t(s_bd[i]);
+        }
+    }
+    // counts: plain exclusive scan (flags 0)
+    uint32_t ef, ecount, agg;
+    block_seg_exclusive(0u, csum, ef, ecount, s_f, s_v, agg);
+    __syncthreads();
+    uint32_t bef, bexcl, btot;
+    block_seg_exclusive(bf, bsum, bef, bexcl, s_f, s_v, btot);
+    (void)btot;
+    (void)ef;
+    // look-back for the item prefix
+    if (tid == 0) {
+        bool chain_head = device_plan ? (k == 0u) : (it.first != 0u);
+        uint32_t prefix;
+        if (chain_head) {
+            prefix = device_plan ? device_base : p.segment_start;
+            atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
+        } else {
+            atomicExch(desc + k, kStatusAgg | (unsigned long long)agg);
+            prefix = 0u;
+            uint32_t j = k - 1u;
+            uint32_t spins = 0;
+            for (;;) {
+                unsigned long long d = *((volatile unsigned long long*)(desc + j));
+                unsigned long long st = d & (3ull << 62);
+                if (st == 0ull) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(error, ERR_LOOKBACK_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                prefix += uint32_t(d);
+                if (st == kStatusIncl) break;
+                --j;
+            }
+            __threadfence();
+            atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
+        }
+        if (k + 1u == n_items) *total = prefix + agg;
+        s_prefix = prefix;
+    }
+    __syncthreads();
+    const uint32_t prefix = s_prefix;
+    uint32_t run = prefix + ecount;
+    uint32_t brun = bexcl;
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; ++j) {
+        uint32_t i = lo + j;
+        if (i < n) {
+            uint32_t c = s_cnt[i];
+            s_cnt[i] = run;  // exclusive start
+            run += c;
+            if (i % stride == 0u) brun = 0u;
+            brun += uint32_t(s_bd[i]);
+            s_bd[i] = int32_t(brun);
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += kScanThreads) {
+        uint32_t start = s_cnt[i];
+        uint32_t end = (i + 1 < n) ? s_cnt[i + 1] : prefix + agg;
+        ranges[e0 + i] = tk_segment_range{start, end};
+        cursors[e0 + i] = start;
+        backdrops[e0 + i] = s_bd[i];
+    }
+}
+
+__global__ void k_path_totals(tk_path_record* paths, uint32_t path_count, const tk_segment_range* ranges,
+                              uint64_t pool_end, uint32_t* bumps, int device_plan, const uint32_t* total) {
+    uint32_t pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= path_count) return;
+    tk_path_record& p = paths[pid];
+    uint32_t start, count;
+    if (p.data_len > 0u) {
+        start = ranges[p.data_offset].start;
+        count = ranges[p.data_offset + p.data_len - 1u].end - start;
+    } else {
+        start = uint64_t(p.data_offset) < pool_end ? ranges[p.data_offset].start : *total;
+        count = 0u;
+    }
+    bumps[pid] = count;
+    if (device_plan) {
+        p.segment_start = start;
+        p.segment_capacity = count;
+    }
+}
+
+__global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
+                            uint32_t path_count, uint32_t* cursors, tk_line_segment* segments, uint64_t capacity,
+                            uint32_t* error) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t pid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pid < path_count; pid += warps) {
+        const tk_path_record p = load_path(paths, pid);
+        for (uint32_t g = 0; g < p.line_count; g += 32u) {
+            uint32_t l = g + lane;
+            Scan s;
+            bool ok = false;
+            if (l < p.line_count) {
+                tk_line line = load_line(lines, uint64_t(p.line_start) + l);
+                if (line.path_id != pid) atomicOr(error, ERR_LINE_PATH_MISMATCH);
+                else ok = scan_geometry(line, p, s);
+            }
+            uint32_t n = ok ? s.imax - s.imin : 0u;
+            uint32_t rounds = __reduce_max_sync(0xffffffffu, n);
+            for (uint32_t r = 0; r < rounds; ++r) {
+                bool emitting = false;
+                uint32_t off = 0xFFFFFFFFu, i = 0;
+                float z = 0.0f;
+                int32_t tx = 0, ty = 0;
+                if (r < n) {
+                    i = s.imin + r;
+                    z = floorf(s.a * float(i) + s.b);
+                    scan_tile(s, i, z, tx, ty);
+                    if (scan_tile_inside(s, tx, ty)) {
+                        emitting = true;
+                        off = scan_tile_offset(s, tx, ty);
+                    }
+                }
+                uint32_t group = __match_any_sync(0xffffffffu, off);
+                uint32_t base = 0;
+                if (emitting) base = *((volatile uint32_t*)(cursors + off));
+                __syncwarp();
+                if (emitting) {
+                    uint32_t leader = __ffs(group) - 1u;
+                    if (lane == leader) *((volatile uint32_t*)(cursors + off)) = base + __popc(group);
+                    uint32_t slot = base + __popc(group & lt_mask);
+                    if (slot < capacity) {
+                        tk_line_segment seg = clipped_segment(s, i, z, tx, ty);
+                        float* dst = reinterpret_cast<float*>(segments + slot);
+                        dst[0] = seg.p0x;
+                        dst[1] = seg.p0y;
+                        dst[2] = seg.p1x;
+                        dst[3] = seg.p1y;
+                        dst[4] = seg.y_edge;
+                    } else {
+                        atomicOr(error, ERR_SEGMENT_OVERFLOW);
+                    }
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+inline unsigned grid_for(uint64_t n, unsigned block, unsigned cap) {
+    uint64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return unsigned(g);
+}
+
+}  // namespace
+
+void launch_scan_count(const SceneView& s, cudaStream_t st) {
+    if (s.line_count == 0) return;
+    k_scan_count<<<grid_for(s.line_count, 256, 148 * 64), 256, 0, st>>>(s.lines, s.line_count, s.paths, s.path_count,
+                                                                       s.backdrops, s.counts);
+}
+
+void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* desc,
+                      uint32_t* ticket, bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st) {
+    cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
+    if (n_items == 0) return;
+    cudaMemsetAsync(desc, 0, sizeof(unsigned long long) * n_items, st);
+    cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
+    k_pool_scan<<<n_items, kScanThreads, 0, st>>>(items, n_items, s.paths, s.counts, s.backdrops, s.ranges, s.cursors,
+                                                  desc, ticket, device_plan ? 1 : 0, device_base, total, s.error);
+}
+
+void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, const uint32_t* total,
+                        cudaStream_t st) {
+    if (s.path_count == 0) return;
+    k_path_totals<<<(s.path_count + 255) / 256, 256, 0, st>>>(s.paths, s.path_count, s.ranges, s.pool_len, bumps,
+                                                             device_plan ? 1 : 0, total);
+}
+
+void launch_scan_emit(const SceneView& s, cudaStream_t st) {
+    if (s.path_count == 0) return;
+    uint64_t threads = uint64_t(s.path_count) * 32;
+    k_scan_emit<<<grid_for(threads, 256, 148 * 32), 256, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
+                                                                 s.segments, s.segment_capacity, s.error);
+}
+
+}  // namespace tk

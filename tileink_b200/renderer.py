@@ -1,0 +1,131 @@
+"""NativeRenderer: the reference's public render entry for the vector path
+(src/native/renderer.rs:51-260, render_to_image at 177-190), backed by the
+sm_100a C ABI (include/tileink.h).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class TileinkError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"tileink error {code}: {message}")
+        self.code = code
+
+
+class NativeRenderer:
+    """One CUDA context + stream on `device`; not thread-safe (like the reference's !Send runtime)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = N.library()
+        h = C.c_void_p()
+        rc = self._lib.tk_ctx_create(int(device), C.byref(h))
+        if rc != 0:
+            raise TileinkError(rc, f"cannot create a context on CUDA device {device}")
+        self._h = h.value
+        self.width = self.height = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.tk_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise TileinkError(rc, self._lib.tk_last_error(self._h).decode())
+
+    @property
+    def stream(self) -> int:
+        return self._lib.tk_ctx_stream(self._h)
+
+    def upload(self, scene) -> None:
+        d = scene.scene_desc() if hasattr(scene, "scene_desc") else scene.desc
+        self._check(self._lib.tk_scene_upload(self._h, C.byref(d)))
+        self.width, self.height = d.width, d.height
+
+    def render(self) -> None:
+        self._check(self._lib.tk_render(self._h))
+
+    def synchronize(self) -> None:
+        self._check(self._lib.tk_synchronize(self._h))
+
+    def readback(self, out: np.ndarray | None = None) -> np.ndarray:
+        n = self.width * self.height
+        if out is None:
+            out = np.empty(n, dtype=np.uint32)
+        self._check(self._lib.tk_readback(self._h, N.ptr(out), out.size))
+        return out
+
+    def render_to_image(self, scene) -> np.ndarray:
+        """Premultiplied RGBA8 image, shape (H, W, 4), uint8."""
+        self.upload(scene)
+        self.render()
+        return self.readback().view(np.uint8).reshape(self.height, self.width, 4)
+
+    STAGE_NAMES = ("pool_clear", "scan_count", "pool_scan", "scan_emit", "bins", "coarse_count", "coarse_emit",
+                   "fine", "blur")
+
+    def set_timing(self, enabled: bool) -> None:
+        self._check(self._lib.tk_set_timing(self._h, 1 if enabled else 0))
+
+    def stage_times(self) -> dict:
+        """Per-stage milliseconds of the last frame (CUDA events on the context stream)."""
+        out = (C.c_float * len(self.STAGE_NAMES))()
+        self._check(self._lib.tk_get_stage_times(self._h, out, len(self.STAGE_NAMES)))
+        return dict(zip(self.STAGE_NAMES, list(out)))
+
+    def probe_fp32_tflops(self) -> float:
+        v = C.c_double(0.0)
+        self._check(self._lib.tk_probe_fp32_tflops(self._h, C.byref(v)))
+        return v.value
+
+    def stats(self) -> dict:
+        s = N.Stats()
+        self._check(self._lib.tk_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in N.Stats._fields_}
+
+    def debug(self, stage: int, index: int = 0) -> np.ndarray:
+        need = C.c_size_t(0)
+        self._check(self._lib.tk_debug_readback(self._h, stage, index, None, 0, C.byref(need)))
+        dt = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
+              N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
+              N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE}[stage]
+        out = np.zeros(need.value // np.dtype(dt).itemsize, dtype=dt)
+        self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
+        return out
+
+    # --- stage harnesses -------------------------------------------------------
+    def stage_scan_prefix(self, counts, paths, ranges, cursors):
+        counts = np.ascontiguousarray(counts, dtype=np.uint32)
+        paths = np.ascontiguousarray(paths, dtype=N.PATH_DTYPE)
+        ranges = np.ascontiguousarray(ranges, dtype=N.RANGE_DTYPE).copy()
+        cursors = np.ascontiguousarray(cursors, dtype=np.uint32).copy()
+        bumps = np.zeros(len(paths), dtype=np.uint32)
+        self._check(self._lib.tk_stage_scan_prefix(self._h, N.ptr(counts), len(counts), N.ptr(paths), len(paths),
+                                                   N.ptr(ranges), N.ptr(cursors), N.ptr(bumps)))
+        return ranges, cursors, bumps
+
+    def stage_scan_count(self, lines, paths, backdrops, counts):
+        lines = np.ascontiguousarray(lines, dtype=N.LINE_DTYPE)
+        paths = np.ascontiguousarray(paths, dtype=N.PATH_DTYPE)
+        backdrops = np.ascontiguousarray(backdrops, dtype=np.int32).copy()
+        counts = np.ascontiguousarray(counts, dtype=np.uint32).copy()
+        self._check(self._lib.tk_stage_scan_count(self._h, N.ptr(lines), len(lines), N.ptr(paths), len(paths),
+                                                  N.ptr(backdrops), N.ptr(counts), len(counts)))
+        return backdrops, counts
+
+    def stage_blur(self, src, dst, width, height, region, source, sigma, axis):
+        src = np.ascontiguousarray(src, dtype=np.uint32)
+        dst = np.ascontiguousarray(dst, dtype=np.uint32).copy()
+        reg = np.asarray(region, dtype=np.uint32)
+        srcb = np.asarray(source, dtype=np.uint32)
+        self._check(self._lib.tk_stage_blur(self._h, N.ptr(src), N.ptr(dst), int(width), int(height), N.ptr(reg),
+                                            N.ptr(srcb), float(sigma), int(axis)))
+        return dst
