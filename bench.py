@@ -79,7 +79,12 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.rows.append([v.strip() for v in line.split(",")])
+            self.rows.append((time.perf_counter(), [v.strip() for v in line.split(",")]))
+
+    def window(self, t0, t1):
+        """Keep the samples taken inside [t0, t1] (all samples if none fell inside)."""
+        inside = [r for r in self.rows if t0 <= r[0] <= t1]
+        self.rows = inside or self.rows
 
     def __exit__(self, *exc):
         if self.proc:
@@ -88,18 +93,19 @@ class ClockSampler:
         return False
 
     def summary(self, fallback_max=1965.0):
-        if not self.rows:
+        rows = [r for _, r in self.rows]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": fallback_max, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for r in self.rows:
+        for r in rows:
             for k, name in enumerate(names):
                 if len(r) > 5 + k and r[5 + k].lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else fallback_max,
-                "reasons": sorted(reasons), "samples": len(self.rows)}
+                "reasons": sorted(reasons), "samples": len(rows)}
 
 
 def measured_peaks():
@@ -215,6 +221,7 @@ def main():
     r = tk.NativeRenderer(local)
     r.upload(canvas)
     stream = torch.cuda.ExternalStream(r.stream)
+    clocks = ClockSampler(local).__enter__()
     for _ in range(max(args.warmup, 3)):
         r.render()
     r.synchronize()
@@ -224,14 +231,18 @@ def main():
     barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        e0.record(stream)
-        for _ in range(args.steps):
-            r.render()
-            for k, v in r.stage_times().items():
-                stage_sum[k] += v
-        e1.record(stream)
-        e1.synchronize()
+    t_on = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        r.render()
+        for k, v in r.stage_times().items():
+            stage_sum[k] += v
+    e1.record(stream)
+    e1.synchronize()
+    t_off = time.perf_counter()
+    time.sleep(0.25)
+    clocks.__exit__(None, None, None)
+    clocks.window(t_on - 0.1, t_off + 0.1)
     torch.cuda.synchronize()
     barrier()
     ms = e0.elapsed_time(e1) / args.steps

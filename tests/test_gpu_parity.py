@@ -102,9 +102,10 @@ def test_gpu_blur_matches_oracle_and_f64_gaussian(renderer, size):
                 region, source = blur_config(width, height, inset)
                 out = renderer.stage_blur(src, untouched, width, height, region, source, sigma, axis)
                 exp = untouched.copy()
-                oracle.lib().or_blur_pass(N.ptr(src), N.ptr(exp), width, height,
-                                          N.ptr(np.array(region, dtype=np.uint32)),
-                                          N.ptr(np.array(source, dtype=np.uint32)), np.float32(sigma), axis)
+                reg = np.array(region, dtype=np.uint32)
+                srcb = np.array(source, dtype=np.uint32)
+                oracle.lib().or_blur_pass(N.ptr(src), N.ptr(exp), width, height, N.ptr(reg), N.ptr(srcb),
+                                          np.float32(sigma), axis)
                 assert np.array_equal(out, exp), (size, sigma, axis, inset)
                 o8 = out.view(np.uint8).reshape(-1, 4)
                 s32 = float(np.float32(sigma))
