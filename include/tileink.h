@@ -348,6 +348,47 @@ int32_t tk_stage_blur(tk_ctx* ctx, const uint32_t* src, uint32_t* dst,
                       uint32_t width, uint32_t height, const uint32_t region[4],
                       const uint32_t source[4], float sigma, uint32_t axis);
 
+/* ------------------------------------------------------------------------ */
+/* Allocation-free pool scan. No reference counterpart: the reference's      */
+/* scan runs on buffers its runtime allocated up front, and this entry point */
+/* gives C callers the same property.                                        */
+/* ------------------------------------------------------------------------ */
+
+#define TK_NOALLOC_MAX_PATHS 16384u
+#define TK_NOALLOC_MAX_SCAN_ITEMS 65536u   /* work items: whole bbox rows, <= 4096 tiles each */
+#define TK_NOALLOC_SCRATCH_BYTES 2818304u  /* per device, inside the library's module */
+
+/* The pool scan of tk_stage_scan_prefix (segment ranges, cursors, per-path
+ * totals) plus the row-wise backdrop cumsum, on DEVICE buffers the caller
+ * owns (`d_*`, pool_len elements each; d_bumps path_count elements) and
+ * `paths` on the host. It makes no device allocation and frees nothing: its
+ * look-back descriptors, work items, copy of `paths` and counter words live
+ * in one fixed array of TK_NOALLOC_SCRATCH_BYTES in device memory, one per
+ * device. For callers that cannot allocate: an application whose own
+ * allocator has reserved the device's memory, where cudaMalloc fails at an
+ * arbitrary point, or one that must not stall other streams, which
+ * cudaMalloc/cudaFree can do by synchronizing the whole device. The call
+ * orders its work on tk_ctx_stream(ctx) and waits for that stream only.
+ *
+ * Limits: path_count <= TK_NOALLOC_MAX_PATHS and at most
+ * TK_NOALLOC_MAX_SCAN_ITEMS work items; larger inputs return TK_E_CAPACITY
+ * with a message and launch nothing.
+ * Zero state: the descriptors, the ticket and the error word must be zero
+ * when the scan kernel starts; the call clears them on the stream before
+ * every launch. d_backdrops holds the per-tile backdrop deltas (0 where
+ * none) and is replaced by its row-wise inclusive cumsum; d_counts is read
+ * only; d_ranges, d_cursors, d_bumps are written (elements outside every
+ * path slice are left as they are).
+ * First call per device: it looks up the scratch address
+ * (cudaGetSymbolAddress with the context's device current), which may load
+ * the library's module; make that first call before any stream capture.
+ * Concurrency: the scratch is shared by every call on one device, so two
+ * calls in flight at the same time on one device race; serialize them. */
+int32_t tk_pool_scan_noalloc(tk_ctx* ctx, const tk_path_record* paths, uint32_t path_count,
+                             const uint32_t* d_counts, int32_t* d_backdrops,
+                             tk_segment_range* d_ranges, uint32_t* d_cursors,
+                             uint64_t pool_len, uint32_t* d_bumps);
+
 #ifdef __cplusplus
 }
 #endif

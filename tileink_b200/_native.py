@@ -125,6 +125,7 @@ def library() -> C.CDLL:
         "tk_stage_scan_prefix": (I32, [P, P, U64, P, U32, P, P, P]),
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
+        "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),
         "tk_set_timing": (I32, [P, I32]),
         "tk_get_stage_times": (I32, [P, P, U32]),
         "tk_probe_fp32_tflops": (I32, [P, C.POINTER(C.c_double)]),

@@ -845,4 +845,55 @@ int32_t tk_stage_blur(tk_ctx* c, const uint32_t* src, uint32_t* dst, uint32_t wi
     });
 }
 
+int32_t tk_pool_scan_noalloc(tk_ctx* c, const tk_path_record* paths, uint32_t path_count, const uint32_t* d_counts,
+                             int32_t* d_backdrops, tk_segment_range* d_ranges, uint32_t* d_cursors, uint64_t pool_len,
+                             uint32_t* d_bumps) {
+    return guarded(c, [&] {
+        if ((pool_len && (!d_counts || !d_backdrops || !d_ranges || !d_cursors)) || (path_count && (!paths || !d_bumps)))
+            invalid("null buffer");
+        if (path_count > TK_NOALLOC_MAX_PATHS)
+            throw Fail{TK_E_CAPACITY, std::to_string(path_count) + " paths exceed the allocation-free limit of " +
+                                          std::to_string(TK_NOALLOC_MAX_PATHS)};
+        uint64_t n_items = 0;
+        for (uint32_t p = 0; p < path_count; ++p) {
+            const tk_path_record& r = paths[p];
+            uint32_t stride = r.tile_x1 > r.tile_x0 ? r.tile_x1 - r.tile_x0 : 0u;
+            uint32_t height = r.tile_y1 > r.tile_y0 ? r.tile_y1 - r.tile_y0 : 0u;
+            if (uint64_t(stride) * height != r.data_len) invalid("data_len != bbox tiles");
+            if (uint64_t(r.data_offset) + r.data_len > pool_len) invalid("path slice outside the pool");
+            if (stride > tk::kScanItemElems) invalid("bbox wider than 4096 tiles");
+            if (!r.data_len) continue;
+            uint32_t rows_per = std::max<uint32_t>(1u, tk::kScanItemElems / stride);
+            n_items += (height + rows_per - 1u) / rows_per;
+        }
+        if (n_items > TK_NOALLOC_MAX_SCAN_ITEMS)
+            throw Fail{TK_E_CAPACITY, std::to_string(n_items) + " scan work items exceed the allocation-free limit of " +
+                                          std::to_string(TK_NOALLOC_MAX_SCAN_ITEMS)};
+        tk::NoAllocScratch sc{};
+        TK_CUDA(tk::noalloc_scratch(c->device, &sc));
+        cudaStream_t st = c->stream;
+        TK_CUDA(cudaMemsetAsync(sc.words, 0, 4 * sizeof(uint32_t), st));
+        if (path_count)
+            TK_CUDA(cudaMemcpyAsync(sc.paths, paths, size_t(path_count) * sizeof(tk_path_record),
+                                    cudaMemcpyHostToDevice, st));
+        tk::launch_build_scan_items(sc.paths, path_count, sc.items, st);
+        tk::SceneView s{};
+        s.paths = sc.paths;
+        s.path_count = path_count;
+        s.counts = const_cast<uint32_t*>(d_counts);
+        s.backdrops = d_backdrops;
+        s.ranges = d_ranges;
+        s.cursors = d_cursors;
+        s.pool_len = pool_len;
+        s.error = sc.words;
+        tk::launch_pool_scan(s, sc.items, uint32_t(n_items), sc.desc, sc.words + 1, false, 0u, sc.words + 2, st);
+        tk::launch_path_totals(s, d_bumps, false, sc.words + 2, st);
+        TK_CUDA(cudaGetLastError());
+        uint32_t err = 0;
+        TK_CUDA(cudaMemcpyAsync(&err, sc.words, 4, cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        if (err) throw Fail{TK_E_TIMEOUT, "prefix look-back gave up"};
+    });
+}
+
 }  // extern "C"

@@ -61,6 +61,18 @@ void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, c
                         cudaStream_t st);
 void launch_scan_emit(const SceneView& s, cudaStream_t st);
 
+// Fixed scratch of the allocation-free pool scan (one array per device).
+struct NoAllocScratch {
+    unsigned long long* desc;  // TK_NOALLOC_MAX_SCAN_ITEMS look-back descriptors
+    ScanItem* items;           // TK_NOALLOC_MAX_SCAN_ITEMS work items
+    tk_path_record* paths;     // TK_NOALLOC_MAX_PATHS path records
+    uint32_t* words;           // [0] error [1] ticket [2] total
+};
+// Resolves the scratch address of `device` (which must be current) once and
+// caches it.
+cudaError_t noalloc_scratch(int device, NoAllocScratch* out);
+void launch_build_scan_items(const tk_path_record* paths, uint32_t path_count, ScanItem* items, cudaStream_t st);
+
 // Target pass: binning, coarse count, tile prefix, coarse emit, fine.
 struct PassView {
     uint32_t order0, draw_n;          // draw_order[order0 .. order0 + draw_n)

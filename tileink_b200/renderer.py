@@ -112,6 +112,14 @@ class NativeRenderer:
                                                    N.ptr(ranges), N.ptr(cursors), N.ptr(bumps)))
         return ranges, cursors, bumps
 
+    def pool_scan_noalloc(self, paths, d_counts: int, d_backdrops: int, d_ranges: int, d_cursors: int,
+                          pool_len: int, d_bumps: int) -> None:
+        """Allocation-free pool scan on caller-owned device buffers (raw device
+        addresses); `paths` is a host array. Waits for the context's stream."""
+        paths = np.ascontiguousarray(paths, dtype=N.PATH_DTYPE)
+        self._check(self._lib.tk_pool_scan_noalloc(self._h, N.ptr(paths), len(paths), d_counts, d_backdrops,
+                                                   d_ranges, d_cursors, int(pool_len), d_bumps))
+
     def stage_scan_count(self, lines, paths, backdrops, counts):
         lines = np.ascontiguousarray(lines, dtype=N.LINE_DTYPE)
         paths = np.ascontiguousarray(paths, dtype=N.PATH_DTYPE)
