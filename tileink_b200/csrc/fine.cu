@@ -34,12 +34,16 @@ using namespace tkd;
 constexpr int kFineThreads = 256;
 constexpr uint32_t kRecChunk = 64;
 constexpr uint32_t kSegBudget = 128;
-constexpr uint32_t kProdCap = 4096;
-constexpr uint32_t kNoProd = 0xFFFFu;
+constexpr uint32_t kProdCap = 2560;
+static_assert(kRecChunk <= 64u && kSegBudget <= 256u, "offsets are scanned by one warp, two records a lane");
 constexpr uint32_t kClipSpill = 28;
 constexpr uint32_t kGroupDepth = 6;
 constexpr uint32_t kGroupLocal = 2;  // FINE_LOCAL_GROUP_DEPTH (fine/constants.hlsli:11)
 constexpr uint32_t kGradient = 0xFFFFFFFFu;
+constexpr uint32_t kGradParams = 24;
+constexpr uint32_t kGradConst = 0, kGradLinear = 1, kGradRadial = 2;  // decoded kinds
+constexpr uint32_t kGradDenOk = 1u << 16;    // linear: den > GRADIENT_FLOAT_EPSILON
+constexpr uint32_t kGradASmall = 1u << 16;   // radial: |a| <= RADIAL_QUADRATIC_EPSILON
 
 // Record classes driving the per-pixel dispatch.
 constexpr uint32_t kClsOther = 0, kClsFill = 1, kClsUniform = 2, kClsBatch = 3, kClsEnd = 4;
@@ -50,15 +54,18 @@ struct Group {
     uint32_t parent_clip, layer_alpha, payload;
 };
 
+// Crossing entry word: plo | phi << 5 | kEntSlow | (prod offset, or with
+// kEntSlow the staged segment index) << 16, where [plo, phi) is the partial
+// pixel range [clamp(floor(xmin)), clamp(ceil(xmax))) within [0, 16].
+constexpr uint32_t kEntSlow = 1u << 10;  // products did not fit: evaluate per pixel
+
 struct FineSmem {
-    // crossing (row, segment) entries: dy, xmin, xmax, and
-    // plo | phi << 8 | prod offset << 16 (plo/phi: the partial pixel range
-    // [clamp(floor(xmin)), clamp(ceil(xmax))) within [0, 16])
-    float4 ent[TK_TILE_SIZE][kSegBudget];
+    float2 ent[TK_TILE_SIZE][kSegBudget];        // crossing (row, segment) entries: dy, entry word
     uint16_t pos[TK_TILE_SIZE][kSegBudget + 1];  // crossing entries before staged segment j
     float prod[kProdCap];                        // segment_area_at(x) * dy per partial pixel
-    float seg[kSegBudget * 5];
-    float base[kRecChunk][TK_TILE_SIZE];
+    float4 sgp[kSegBudget];                      // staged segments: p0x, p0y, p1x, p1y
+    float2 sgx[kSegBudget];                      // y_edge, slope = (p1x - p0x) / (p1y - p0y)
+    float2 rb[kRecChunk][TK_TILE_SIZE];          // per (fill, row): base, k0 | k1 << 16
     float4 pfull[kRecChunk];                     // rgba8_to_unorm(paint) / uniform source
     float4 pcf[kRecChunk];                       // paint channels as floats
     uint4 rec_a[kRecChunk];                      // tag, backdrop, fill_rule, segment_start
@@ -67,8 +74,8 @@ struct FineSmem {
     uint32_t ualpha[kRecChunk];
     uint32_t umode[kRecChunk];                   // uniform fills: 1 replace, 2 src-over, 3 no-op
     uint32_t paint[kRecChunk];                   // solid premul color, or kGradient
-    uint32_t brush_off[kRecChunk];
-    float inv[kRecChunk][6];
+    float gp[kRecChunk][kGradParams];            // decoded gradient records (stage_gradient)
+    uint4 gk[kRecChunk];                         // kind | flags, ramp word (or color), ramp length, extend
     uint32_t nseg[kRecChunk];
     uint32_t off[kRecChunk + 1];
     float unorm[256];                            // k / 255 for RGBA8 texel reloads
@@ -84,6 +91,125 @@ __device__ __forceinline__ float4 texel_load_lut(const FineSmem& S, uint32_t p) 
     return make_float4(S.unorm[p & 255u], S.unorm[(p >> 8) & 255u], S.unorm[(p >> 16) & 255u], S.unorm[p >> 24]);
 }
 
+// Decodes the gradient brush at word `db` of a fill whose draw has the inverse
+// transform `m` into slot `i`: the transforms, and the terms of
+// sample_gradient (fine/paint.hlsli:40-96) that depend on the brush alone,
+// computed with the same f32 operations so that the per-pixel evaluation in
+// gradient_at gives the same bits.
+//   linear: gp[12..16] = sx, sy, dx = ex - sx, dy = ey - sy, den = dx*dx + dy*dy
+//   radial: gp[12..22] = sx, sy, dcx, dcy, sr*dr, -sr*sr, a, -4*a, 2*a, dr, sr
+//           with a = mad(dcx, dcx, mad(dcy, dcy, -dr*dr))
+__device__ void stage_gradient(FineSmem& S, uint32_t i, const Paint& P, uint32_t db, const float* __restrict__ m) {
+    float* g = S.gp[i];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g[k] = __ldg(m + k);
+    const uint32_t kind = P.word(db), extend = P.word(db + 1u);
+    const uint32_t payload = db + P.word(db + 2u), len = P.word(db + 3u);
+    const uint32_t base = db + TK_BRUSH_HEADER_WORDS;
+    uint32_t code = kGradConst, flags = 0u, word = 0u;
+    if (kind == TK_BRUSH_LINEAR) {
+        code = kGradLinear;
+        for (uint32_t k = 0; k < 6u; ++k) g[6 + k] = P.param(base, 4u + k);
+        const float sx = P.param(base, 0), sy = P.param(base, 1), ex = P.param(base, 2), ey = P.param(base, 3);
+        const float dx = ex - sx, dy = ey - sy;
+        const float den = dx * dx + dy * dy;
+        g[12] = sx;
+        g[13] = sy;
+        g[14] = dx;
+        g[15] = dy;
+        g[16] = den;
+        if (den > GRADIENT_FLOAT_EPSILON) flags = kGradDenOk;
+        word = payload;
+    } else if (kind == TK_BRUSH_RADIAL) {
+        code = kGradRadial;
+        for (uint32_t k = 0; k < 6u; ++k) g[6 + k] = P.param(base, 6u + k);
+        const float sx = P.param(base, 0), sy = P.param(base, 1), ex = P.param(base, 2), ey = P.param(base, 3);
+        const float sr = P.param(base, 4), er = P.param(base, 5);
+        const float dcx = ex - sx, dcy = ey - sy, dr = er - sr;
+        const float a = mad(dcx, dcx, mad(dcy, dcy, -dr * dr));
+        g[12] = sx;
+        g[13] = sy;
+        g[14] = dcx;
+        g[15] = dcy;
+        g[16] = sr * dr;
+        g[17] = -sr * sr;
+        g[18] = a;
+        g[19] = -4.0f * a;
+        g[20] = 2.0f * a;
+        g[21] = dr;
+        g[22] = sr;
+        if (fabsf(a) <= RADIAL_QUADRATIC_EPSILON) flags = kGradASmall;
+        word = payload;
+    } else {
+        word = kind == 6u ? 0u : P.word(db + TK_BRUSH_COLOR_WORD);  // BRUSH_PATTERN samples as 0
+    }
+    S.gk[i] = make_uint4(code | flags, word, len, extend);
+}
+
+// sample_gradient at pixel centre (px, py) for the gradient decoded in slot i.
+__device__ __forceinline__ uint32_t gradient_at(const FineSmem& S, const Paint& P, uint32_t i, float px, float py) {
+    const float* g = S.gp[i];
+    const uint4 k = S.gk[i];
+    const uint32_t code = k.x & 255u, extend = k.w;
+    if (code == kGradConst) return k.y;
+    const float x = mad(g[0], px, mad(g[2], py, g[4]));
+    const float y = mad(g[1], px, mad(g[3], py, g[5]));
+    const float tx = mad(g[6], x, mad(g[8], y, g[10]));
+    const float ty = mad(g[7], x, mad(g[9], y, g[11]));
+    float t = 0.0f;
+    if (code == kGradLinear) {
+        if (k.x & kGradDenOk) t = mad(tx - g[12], g[14], (ty - g[13]) * g[15]) / g[16];
+    } else {
+        const float qx = tx - g[12], qy = ty - g[13];
+        const float b = -2.0f * mad(qx, g[14], mad(qy, g[15], g[16]));
+        const float c = mad(qx, qx, mad(qy, qy, g[17]));
+        const float dr = g[21], sr = g[22];
+        bool has_t = false;
+        if (k.x & kGradASmall) {
+            if (fabsf(b) > RADIAL_QUADRATIC_EPSILON) {
+                const float cand = -c / b;
+                if (mad(cand, dr, sr) >= 0.0f) {
+                    has_t = true;
+                    t = cand;
+                }
+            }
+        } else {
+            const float disc = mad(b, b, g[19] * c);
+            if (disc >= 0.0f) {
+                const float root = sqrtf(disc);
+                const float t0 = (-b - root) / g[20], t1 = (-b + root) / g[20];
+                const bool v0 = mad(t0, dr, sr) >= 0.0f, v1 = mad(t1, dr, sr) >= 0.0f;
+                if (v0) {
+                    has_t = true;
+                    t = v1 ? fmaxf(t0, t1) : t0;
+                } else if (v1) {
+                    has_t = true;
+                    t = t1;
+                }
+            }
+        }
+        if (!has_t) return 0u;
+    }
+    return sample_ramp(P, k.y, k.z, t, extend);
+}
+
+// segment_row_parts (shared/coverage.hlsli:7-24) of staged segment j for
+// tile row `row`, with the slope division done once per segment at staging.
+__device__ __forceinline__ RowParts staged_row_parts(const FineSmem& S, uint32_t j, uint32_t row) {
+    const float4 g = S.sgp[j];
+    const float row_y = float(row), local_y = g.y - row_y, far_y = g.w - row_y;
+    const float y0 = clampf(local_y, 0.0f, 1.0f), y1 = clampf(far_y, 0.0f, 1.0f);
+    const float dy = y0 - y1;
+    if (dy == 0.0f) return {0.0f, dy, 0.0f, 0.0f};
+    const float slope = S.sgx[j].y;
+    const bool nearer_p0 = fabsf(local_y - 0.5f) <= fabsf(far_y - 0.5f);
+    const float anchor_x = nearer_p0 ? g.x : g.z;
+    const float anchor_y = nearer_p0 ? local_y : far_y;
+    const float sx0 = mad(y0 - anchor_y, slope, anchor_x);
+    const float sx1 = mad(y1 - anchor_y, slope, anchor_x);
+    return {0.0f, dy, fminf(sx0, sx1), fmaxf(sx0, sx1)};
+}
+
 // Crossing lists and partial products for staged segments [0, total): warp w
 // builds rows 2w and 2w + 1, lanes walk the segments in order.
 __device__ void stage_rows(FineSmem& S, uint32_t total) {
@@ -95,27 +221,38 @@ __device__ void stage_rows(FineSmem& S, uint32_t total) {
         for (uint32_t j0 = 0; j0 < total; j0 += 32u) {
             const uint32_t j = j0 + lane;
             RowParts rp{0.f, 0.f, 0.f, 0.f};
-            if (j < total) {
-                const float* g = S.seg + j * 5u;
-                rp = segment_row_parts(g[0], g[1], g[2], g[3], g[4], row);
-            }
+            if (j < total) rp = staged_row_parts(S, j, row);
             const bool crossing = j < total && rp.dy != 0.0f;
             const uint32_t ballot = __ballot_sync(0xffffffffu, crossing);
             const uint32_t k = count + __popc(ballot & lt);
             if (j < total) S.pos[row][j] = uint16_t(k);
+            uint32_t plo = 0u, phi = 0u, span = 0u;
             if (crossing) {
-                const int32_t plo = min(max(f2i(floorf(rp.xmin)), 0), int32_t(TK_TILE_SIZE));
-                const int32_t phi = min(max(f2i(ceilf(rp.xmax)), 0), int32_t(TK_TILE_SIZE));
-                const uint32_t span = phi > plo ? uint32_t(phi - plo) : 0u;
-                uint32_t o = atomicAdd(&S.nprod, span);
+                plo = uint32_t(min(max(f2i(floorf(rp.xmin)), 0), int32_t(TK_TILE_SIZE)));
+                phi = uint32_t(min(max(f2i(ceilf(rp.xmax)), 0), int32_t(TK_TILE_SIZE)));
+                span = phi > plo ? phi - plo : 0u;
+            }
+            // warp-aggregated allocation of the partial products
+            uint32_t incl = span;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= uint32_t(d)) incl += v;
+            }
+            uint32_t wbase = 0u;
+            if (lane == 31u && incl) wbase = atomicAdd(&S.nprod, incl);
+            wbase = __shfl_sync(0xffffffffu, wbase, 31);
+            if (crossing) {
+                const uint32_t o = wbase + incl - span;
+                uint32_t word = plo | (phi << 5);
                 if (o + span <= kProdCap) {
                     for (uint32_t x = 0; x < span; ++x)
-                        S.prod[o + x] = segment_area_at(rp.xmin, rp.xmax, uint32_t(plo) + x) * rp.dy;
+                        S.prod[o + x] = segment_area_at(rp.xmin, rp.xmax, plo + x) * rp.dy;
+                    word |= o << 16;
                 } else {
-                    o = kNoProd;
+                    word |= kEntSlow | (j << 16);
                 }
-                S.ent[row][k] = make_float4(rp.dy, rp.xmin, rp.xmax,
-                                            __uint_as_float(uint32_t(plo) | (uint32_t(phi) << 8) | (o << 16)));
+                S.ent[row][k] = make_float2(rp.dy, __uint_as_float(word));
             }
             count += __popc(ballot);
         }
@@ -123,7 +260,7 @@ __device__ void stage_rows(FineSmem& S, uint32_t total) {
     }
 }
 
-__global__ void __launch_bounds__(kFineThreads, 3)
+__global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const tk_line_segment* __restrict__ segments, const tk_draw_record* __restrict__ draws,
            const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
@@ -180,7 +317,6 @@ __global__ void __launch_bounds__(kFineThreads, 3)
             if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH) {
                 const tk_draw_record& d = draws[c.y];
                 const uint32_t bo = __ldg(&d.brush_offset);
-                S.brush_off[tid] = bo;
                 if (P.word(bo) == TK_BRUSH_SOLID) {
                     const uint32_t paint = P.word(bo + TK_BRUSH_COLOR_WORD);
                     S.paint[tid] = paint;
@@ -202,9 +338,7 @@ __global__ void __launch_bounds__(kFineThreads, 3)
                     }
                 } else {
                     S.paint[tid] = kGradient;
-                    const float* m = &d.inverse_transform.a;
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) S.inv[tid][k] = __ldg(m + k);
+                    stage_gradient(S, tid, P, bo, &d.inverse_transform.a);
                 }
             }
             S.cls[tid] = cls;
@@ -222,9 +356,9 @@ __global__ void __launch_bounds__(kFineThreads, 3)
                 if (tid >= uint32_t(o)) incl += q;
             }
             const uint32_t excl = incl - v;
-            S.off[tid * 2u] = excl;
-            S.off[tid * 2u + 1u] = excl + a0;
-            if (tid == 31) S.off[kRecChunk] = incl;
+            if (tid * 2u <= kRecChunk) S.off[tid * 2u] = excl;
+            if (tid * 2u + 1u <= kRecChunk) S.off[tid * 2u + 1u] = excl + a0;
+            if (tid == 31 && kRecChunk == 64u) S.off[kRecChunk] = incl;
             const bool fit0 = tid * 2u < avail && excl + a0 <= kSegBudget;
             const bool fit1 = tid * 2u + 1u < avail && excl + a0 + a1 <= kSegBudget;
             const uint32_t nfit = __popc(__ballot_sync(0xffffffffu, fit0)) + __popc(__ballot_sync(0xffffffffu, fit1));
@@ -235,29 +369,37 @@ __global__ void __launch_bounds__(kFineThreads, 3)
         const bool big = S.off[n] > kSegBudget;  // one record with more than kSegBudget segments
         if (!big) {
             const uint32_t total = S.off[n];
-            for (uint32_t j = tid; j < total * 5u; j += kFineThreads) {
-                const uint32_t sg = j / 5u, comp = j - sg * 5u;
+            for (uint32_t sg = tid; sg < total; sg += kFineThreads) {
                 uint32_t lo = 0, hi = n;  // record owning staged segment sg
                 while (hi - lo > 1u) {
                     const uint32_t mid = (lo + hi) >> 1;
                     if (S.off[mid] <= sg) lo = mid;
                     else hi = mid;
                 }
-                const uint32_t g = S.rec_a[lo].w + (sg - S.off[lo]);
-                S.seg[j] = __ldg(reinterpret_cast<const float*>(segments + g) + comp);
+                const float* g = reinterpret_cast<const float*>(segments + S.rec_a[lo].w + (sg - S.off[lo]));
+                const float p0x = __ldg(g), p0y = __ldg(g + 1), p1x = __ldg(g + 2), p1y = __ldg(g + 3);
+                const float ye = __ldg(g + 4);
+                const float delta_y = p1y - p0y;
+                S.sgp[sg] = make_float4(p0x, p0y, p1x, p1y);
+                S.sgx[sg] = make_float2(ye, delta_y != 0.0f ? (p1x - p0x) / delta_y : 0.0f);
             }
             __syncthreads();
             stage_rows(S, total);
+            __syncthreads();
             for (uint32_t k = tid; k < n * TK_TILE_SIZE; k += kFineThreads) {
                 const uint32_t ri = k >> 4, row = k & 15u;
-                if (S.nseg[ri] == 0u) continue;
+                const uint32_t j0 = S.off[ri], ns = S.nseg[ri];
+                if (ns == 0u) continue;
                 float bsum = float(int32_t(S.rec_a[ri].y));
-                for (uint32_t j = S.off[ri], e = S.off[ri] + S.nseg[ri]; j < e; ++j) {
-                    const float* g = S.seg + j * 5u;
-                    if (g[4] < 1000000000.0f)  // y_edge set: the segment touches the tile's left edge
-                        bsum += signum_f32(g[2] - g[0]) * clampf(float(row) - g[4] + 1.0f, 0.0f, 1.0f);
+                for (uint32_t j = j0; j < j0 + ns; ++j) {
+                    const float ye = S.sgx[j].x;
+                    if (ye < 1000000000.0f) {  // y_edge set: the segment touches the tile's left edge
+                        const float4 g = S.sgp[j];
+                        bsum += signum_f32(g.z - g.x) * clampf(float(row) - ye + 1.0f, 0.0f, 1.0f);
+                    }
                 }
-                S.base[ri][row] = bsum;
+                const uint32_t k0 = S.pos[row][j0], k1 = S.pos[row][j0 + ns];
+                S.rb[ri][row] = make_float2(bsum, __uint_as_float(k0 | (k1 << 16)));
             }
             __syncthreads();
         }
@@ -325,19 +467,24 @@ __global__ void __launch_bounds__(kFineThreads, 3)
                     alpha = S.ualpha[i];
                 } else if (!big) {
                     float running = 0.0f, partial = 0.0f;
-                    const float4* row = S.ent[ly];
-                    const uint32_t k0 = S.pos[ly][S.off[i]], k1 = S.pos[ly][S.off[i] + S.nseg[i]];
-                    for (uint32_t k = k0; k < k1; ++k) {
-                        const float4 e = row[k];
-                        const uint32_t pk = __float_as_uint(e.w);
-                        const uint32_t plo = pk & 0xFFu, phi = (pk >> 8) & 0xFFu;
+                    const float2* row = S.ent[ly];
+                    const float2 rb = S.rb[i][ly];
+                    const uint32_t kk = __float_as_uint(rb.y);
+                    for (uint32_t k = kk & 0xFFFFu, k1 = kk >> 16; k < k1; ++k) {
+                        const float2 e = row[k];
+                        const uint32_t pk = __float_as_uint(e.y);
+                        const uint32_t plo = pk & 31u, phi = (pk >> 5) & 31u;
                         if (lx >= phi) running += e.x;
                         if (lx >= plo && lx < phi) {
-                            const uint32_t o = pk >> 16;
-                            partial += o != kNoProd ? S.prod[o + lx - plo] : segment_area_at(e.y, e.z, lx) * e.x;
+                            if (!(pk & kEntSlow)) {
+                                partial += S.prod[(pk >> 16) + lx - plo];
+                            } else {
+                                const RowParts q = staged_row_parts(S, pk >> 16, ly);
+                                partial += segment_area_at(q.xmin, q.xmax, lx) * q.dy;
+                            }
                         }
                     }
-                    alpha = coverage_to_alpha(S.base[i][ly] + running + partial, qa.z);
+                    alpha = coverage_to_alpha(rb.x + running + partial, qa.z);
                 } else {
                     // more segments than one chunk holds: per-pixel evaluation
                     // of fill_alpha_at over 128-segment slices
@@ -345,12 +492,15 @@ __global__ void __launch_bounds__(kFineThreads, 3)
                     for (uint32_t c0 = qa.w; c0 < qb.x; c0 += kSegBudget) {
                         const uint32_t m = min(kSegBudget, qb.x - c0);
                         __syncthreads();
-                        for (uint32_t j = tid; j < m * 5u; j += kFineThreads)
-                            S.seg[j] = __ldg(reinterpret_cast<const float*>(segments + c0) + j);
+                        for (uint32_t j = tid; j < m; j += kFineThreads) {
+                            const float* g = reinterpret_cast<const float*>(segments + c0 + j);
+                            S.sgp[j] = make_float4(__ldg(g), __ldg(g + 1), __ldg(g + 2), __ldg(g + 3));
+                            S.sgx[j] = make_float2(__ldg(g + 4), 0.0f);
+                        }
                         __syncthreads();
                         for (uint32_t j = 0; j < m; ++j) {
-                            const float* g = S.seg + j * 5u;
-                            const RowParts q = segment_row_parts(g[0], g[1], g[2], g[3], g[4], ly);
+                            const float4 g = S.sgp[j];
+                            const RowParts q = segment_row_parts(g.x, g.y, g.z, g.w, S.sgx[j].x, ly);
                             base += q.edge;
                             if (q.dy != 0.0f) {
                                 const int32_t hi = min(max(f2i(ceilf(q.xmax)), 0), int32_t(TK_TILE_SIZE));
@@ -401,11 +551,7 @@ __global__ void __launch_bounds__(kFineThreads, 3)
                                     px = src_over_premul_unorm(px, make_float4(c.x * sc, c.y * sc, c.z * sc, c.w * sc));
                             }
                         } else {
-                            const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
-                            const float* m = S.inv[i];
-                            const float lxf = mad(m[0], sx, mad(m[2], sy, m[4]));
-                            const float lyf = mad(m[1], sx, mad(m[3], sy, m[5]));
-                            const uint32_t g = sample_gradient(P, S.brush_off[i], lxf, lyf);
+                            const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
                             if (masked == 255u && premul_u8_is_opaque(g)) px = rgba8_to_unorm(g);
                             else px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(g, masked));
                         }
