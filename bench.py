@@ -316,14 +316,16 @@ def main():
     roof["kernel"] = dominant
     roof["peak_source"] = ("measured FMA probe (tk_probe_fp32_tflops)" if roof["bound"] == "fp32"
                            else "measured (MEASURED_PEAKS.json hbm_gbs)")
-    traffic_file = ROOT / "profiles" / "ncu_traffic.json"
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
+    # the committed ncu launch list of the default 4096^2 / 50k workload; other
+    # sizes have no capture.
     roof["traffic"] = None
-    if traffic_file.exists():
-        try:
-            tr = json.loads(traffic_file.read_text())
-            roof["traffic"] = tr.get(dominant)
-        except Exception:
-            pass
+    traffic_file = ROOT / "profiles" / "dram_traffic_c2_4096x4096_50k.txt"
+    if traffic_file.exists() and (args.size or 4096) == 4096 and (args.paths or 50000) == 50000:
+        for line in traffic_file.read_text().splitlines():
+            parts = line.split()
+            if len(parts) == 2 and not line.startswith("#") and parts[0] == dominant:
+                roof["traffic"] = int(parts[1])
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
