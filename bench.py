@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--paths", type=int, default=0, help="override the path count (smaller trial runs)")
     p.add_argument("--size", type=int, default=0, help="override the canvas side (smaller trial runs)")
+    p.add_argument("--diff-steps", type=int, default=10, help="timed fwd+bwd steps of the blur-group workload (0: skip)")
     return p.parse_args()
 
 
@@ -118,6 +119,35 @@ def measured_peaks():
 def scene(size=0, paths=0, device_plan=True, seed=SEED):
     import tileink_b200 as tk
     return tk.generate(2, seed, width=size, height=size, paths=paths, device_segment_plan=device_plan)
+
+
+def diff_timing(renderer, steps, warmup):
+    """fwd+bwd latency of the differentiable blur-group workload (1024x1024,
+    256 closed paths x 12 cubics, sigma 4, MSE against the image of the
+    parameters jittered by N(0, 3^2) px) through the public API: host
+    parameters in, loss and host gradients out, flattening and scene build
+    included. The target is the GPU forward's own image of the jittered scene."""
+    from tileink_b200 import diff
+    sc = diff.blur_group_scene(5)
+    tg = diff.blur_group_scene(5, jitter=3.0)
+    _, target = renderer.diff_forward(tg, np.zeros((sc.height, sc.width, 4), np.float32), return_image=True)
+    for _ in range(max(warmup, 3)):
+        renderer.diff_forward(sc, target)
+        renderer.diff_backward()
+    fwd, bwd = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        loss = renderer.diff_forward(sc, target)
+        t1 = time.perf_counter()
+        dp, dc, ds = renderer.diff_backward()
+        t2 = time.perf_counter()
+        fwd.append((t1 - t0) * 1e3)
+        bwd.append((t2 - t1) * 1e3)
+    return {"workload": "1024x1024, 256 closed paths x 12 cubics, blur group sigma 4, MSE vs jittered target",
+            "fwd_bwd_ms": float(np.median(np.add(fwd, bwd))), "fwd_ms": float(np.median(fwd)),
+            "bwd_ms": float(np.median(bwd)), "steps": steps, "loss": loss,
+            "timing": "host wall clock per call (median), host buffers in and out",
+            "gradient_check": "tests/test_gpu_diff.py: FP64 central differences, relative error <= 1e-3"}
 
 
 def cpu_baseline(size, paths):
@@ -330,6 +360,7 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.size, args.paths)
+    diff_line = diff_timing(r, args.diff_steps, args.warmup) if (rank == 0 and args.diff_steps > 0) else None
 
     launches_per_frame = 5 + 5 * stats["passes"]
     if rank == 0:
@@ -351,6 +382,7 @@ def main():
                        "fill_particles": fills, "segment_visits": visits, "tiles": T, "passes": stats["passes"]},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "fwd_bwd": diff_line,
             "scene_generation_s": gen_s,
         }
         print(json.dumps(line), flush=True)

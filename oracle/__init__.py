@@ -30,7 +30,8 @@ def build() -> Path:
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
-        if not LIB.exists() or LIB.stat().st_mtime < (HERE / "oracle.cpp").stat().st_mtime:
+        sources = [HERE / "oracle.cpp", HERE / "diff_oracle.cpp", HERE / "oracle.h"]
+        if not LIB.exists() or any(LIB.stat().st_mtime < f.stat().st_mtime for f in sources):
             build()
         l = C.CDLL(str(LIB))
         P, U32, U64, I32, F32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
@@ -52,6 +53,8 @@ def lib() -> C.CDLL:
         l.or_blur_pass.argtypes = [P, P, U32, U32, P, P, F32, U32]
         l.or_fill_value.restype = F32
         l.or_fill_value.argtypes = [P, U32, I32, U32, U32]
+        l.or_diff_loss.restype = C.c_double
+        l.or_diff_loss.argtypes = [U32, U32, U32, U64, P, P, P, P, P, C.c_double, I32, P, P, P, I32]
         _lib = l
     return _lib
 
@@ -91,3 +94,27 @@ class OracleRun:
         t = (C.c_double * 7)()
         self._l.or_stage_times(self._h, t)
         return list(t)
+
+
+def diff_loss(scene, lines, endpoint_point, endpoint_weights, points, colors, sigma, target, radius=None,
+              return_image=False, threads=8):
+    """FP64 loss of the differentiable model for parameters (points, colors,
+    sigma) with the flattening (lines, endpoint weights) of a forward held
+    fixed; radius defaults to ceil(3 sigma) of the scene."""
+    import math
+    h, w = scene.height, scene.width
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1)
+    cols = np.ascontiguousarray(colors, dtype=np.float64).reshape(-1)
+    tgt = np.ascontiguousarray(target, dtype=np.float32)
+    bg = np.asarray(scene.background, dtype=np.float64)
+    r = int(math.ceil(3.0 * float(np.float32(scene.sigma)))) if radius is None else int(radius)
+    if scene.sigma <= 0:
+        r = 0
+    img = np.zeros((h, w, 4), dtype=np.float64) if return_image else None
+    lines = np.ascontiguousarray(lines)
+    ep = np.ascontiguousarray(endpoint_point, dtype=np.uint32)
+    ew = np.ascontiguousarray(endpoint_weights, dtype=np.float32)
+    loss = lib().or_diff_loss(w, h, scene.path_count, len(lines), lines.ctypes.data, ep.ctypes.data,
+                              ew.ctypes.data, pts.ctypes.data, cols.ctypes.data, float(sigma), r, bg.ctypes.data,
+                              tgt.ctypes.data, img.ctypes.data if img is not None else None, threads)
+    return (loss, img) if return_image else loss

@@ -100,6 +100,16 @@ void or_blur_pass(const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t h
 float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t backdrop,
                     uint32_t x, uint32_t y);
 
+/* FP64 loss of the differentiable model (include/tileink_diff.h) for the
+ * flattening `lines` / endpoint weights of a forward and the parameters
+ * `points` ([point][x, y]), `colors` ([path][rgba] straight), `sigma` with the
+ * blur radius held at `radius` (0: no blur). `target` is [H][W][4]; `image`
+ * (optional) receives the rendered image. diff_oracle.cpp. */
+double or_diff_loss(uint32_t width, uint32_t height, uint32_t path_count, uint64_t line_count,
+                    const tk_line* lines, const uint32_t* endpoint_point, const float* endpoint_weights,
+                    const double* points, const double* colors, double sigma, int32_t radius,
+                    const double* background, const float* target, double* image, int32_t threads);
+
 #ifdef __cplusplus
 }
 #endif

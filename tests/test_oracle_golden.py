@@ -321,3 +321,48 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_string():
     assert b"sm_100a" in N.library().tk_version()
+
+
+# --- differentiable path: flattening structure and the FP64 oracle -------------------
+def test_diff_flatten_matches_canvas_flattening_bitwise():
+    from tileink_b200 import diff
+    sc = diff.blur_group_scene(11, width=320, height=200, paths=12)
+    lines, ep, w = diff.flatten(sc)
+    canvas_lines = tk.generate(5, 11, width=320, height=200, paths=12).scene_arrays()["lines"]
+    assert len(lines) == len(canvas_lines)
+    assert lines.tobytes() == canvas_lines.tobytes()
+
+
+def test_diff_flatten_weights_reconstruct_line_endpoints():
+    from tileink_b200 import diff
+    sc = diff.blur_group_scene(12, width=256, height=256, paths=8)
+    lines, ep, w = diff.flatten(sc)
+    P = sc.points.reshape(-1, 2).astype(np.float64)
+    for e, key in ((0, "p0"), (1, "p1")):
+        pts = np.stack([P[ep[:, e] + i] for i in range(4)], axis=1)  # [L, 4, 2]
+        rec = np.einsum("li,lid->ld", w[:, e, :].astype(np.float64), pts)
+        assert np.abs(rec - lines[key]).max() < 1e-4
+    # weights of each endpoint sum to one (affine combinations of control points)
+    assert np.abs(w.sum(axis=2) - 1.0).max() < 1e-5
+    # consecutive lines share endpoints
+    assert np.array_equal(lines["p1"][:-1][lines["path_id"][:-1] == lines["path_id"][1:]],
+                          lines["p0"][1:][lines["path_id"][:-1] == lines["path_id"][1:]])
+
+
+def test_diff_oracle_exact_area_of_a_square():
+    # a 10x10 square with corners at half pixels, drawn as 4 straight cubics:
+    # interior pixels are fully covered, edge pixels half, corners a quarter
+    from tileink_b200 import diff
+    corners = [(3.5, 3.5), (13.5, 3.5), (13.5, 13.5), (3.5, 13.5)]
+    pts = [corners[0]]
+    for k in range(4):
+        a, b = np.array(corners[k]), np.array(corners[(k + 1) % 4])
+        pts += [tuple(a + (b - a) / 3), tuple(a + 2 * (b - a) / 3), tuple(b)]
+    sc = diff.DiffScene(20, 20, np.array([pts], np.float32), np.array([[1.0, 0.0, 0.0, 1.0]], np.float32),
+                        sigma=0.0, background=(0.0, 0.0, 0.0, 0.0))
+    lines, ep, w = diff.flatten(sc)
+    _, img = oracle.diff_loss(sc, lines, ep, w, sc.points, sc.colors, 0.0, np.zeros((20, 20, 4), np.float32),
+                              return_image=True)
+    a = img[..., 3]
+    assert abs(a[8, 8] - 1.0) < 1e-12 and abs(a[3, 8] - 0.5) < 1e-12 and abs(a[3, 3] - 0.25) < 1e-12
+    assert abs(a.sum() - 100.0) < 1e-9 and a[0, 0] == 0.0

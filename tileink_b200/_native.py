@@ -91,6 +91,13 @@ class BrushDesc(C.Structure):
                 ("stops", C.POINTER(GradientStop))]
 
 
+class DiffScene(C.Structure):
+    """tk_diff_scene (include/tileink_diff.h)."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("path_count", C.c_uint32),
+                ("cubics_per_path", C.c_uint32), ("points", C.c_void_p), ("colors", C.c_void_p),
+                ("sigma", C.c_float), ("tolerance", C.c_float), ("background", C.c_float * 4)]
+
+
 class GenParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("paths", C.c_uint32), ("variant", C.c_uint32),
                 ("sigma", C.c_float), ("jitter", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
@@ -126,6 +133,9 @@ def library() -> C.CDLL:
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
         "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),
+        "tk_diff_forward": (I32, [P, C.POINTER(DiffScene), P, C.POINTER(C.c_double), P]),
+        "tk_diff_backward": (I32, [P, P, P, P]),
+        "tk_diff_flatten": (U64, [C.POINTER(DiffScene), P, P, P, U64]),
         "tk_set_timing": (I32, [P, I32]),
         "tk_get_stage_times": (I32, [P, P, U32]),
         "tk_probe_fp32_tflops": (I32, [P, C.POINTER(C.c_double)]),

@@ -6,11 +6,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "../../include/tileink.h"
+#include "../../include/tileink_canvas.h"
+#include "../../include/tileink_diff.h"
 #include "kernels.h"
 
 namespace {
@@ -71,6 +74,22 @@ struct Step {
     int32_t bounds[4];
 };
 
+// State of the last differentiable forward, kept for its backward.
+struct DiffState {
+    bool ready = false;
+    uint32_t width = 0, height = 0, paths = 0, points = 0, pass = 0;
+    uint64_t lines = 0;
+    int32_t radius = 0;
+    float sigma = 0.0f;
+    float4 bg{};
+    std::vector<float> colors;  // straight RGBA per path
+    DBuf<float4> colp, target, layer, t1, blurred, gI, d0, d1;
+    DBuf<float2> scratch, line_acc;
+    DBuf<float> color_acc, dpoints, taps, dtaps, ep_w;
+    DBuf<uint32_t> ep_point;
+    DBuf<double> sums;  // [0] loss [1] dL/dsigma
+};
+
 }  // namespace
 
 struct tk_ctx {
@@ -103,6 +122,10 @@ struct tk_ctx {
     DBuf<uint32_t> image, temp;
     std::vector<DBuf<uint32_t>> surfaces;
     bool rendered = false;
+    // line index per emitted segment (differentiable mode only)
+    DBuf<uint32_t> seg_line;
+    bool want_seg_line = false;
+    DiffState diff;
     // stage timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -303,6 +326,7 @@ tk::SceneView view(tk_ctx* c) {
     s.segments = c->segments.ptr;
     s.segment_capacity = c->segments.cap;
     s.error = c->misc.ptr;
+    s.seg_line = c->want_seg_line ? c->seg_line.ptr : nullptr;
     return s;
 }
 
@@ -338,6 +362,8 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d) {
     // A failed upload leaves no renderable scene behind.
     c->have_scene = false;
     c->rendered = false;
+    c->diff.ready = false;
+    c->want_seg_line = false;
     validate_and_plan(c, d);
     cudaStream_t st = c->stream;
     upload(c->lines, d.lines, d.line_count, st);
@@ -426,7 +452,7 @@ struct StageMark {
     }
 };
 
-void run_pass(tk_ctx* c, Pass& p, uint32_t* target) {
+void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
     cudaStream_t st = c->stream;
     tk::SceneView s = view(c);
     tk::PassView v = pass_view(c, p);
@@ -450,13 +476,15 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target) {
         StageMark m(c, 6);
         tk::launch_coarse(s, v, true, st);
     }
+    if (!fine) return;
     {
         StageMark m(c, 7);
         tk::launch_fine(s, v, target, st);
     }
 }
 
-void do_render(tk_ctx* c) {
+// Pool clear, scan_count, pool scan, path totals and scan_emit.
+void scan_phase(tk_ctx* c) {
     if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
     cudaStream_t st = c->stream;
     bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
@@ -493,6 +521,11 @@ void do_render(tk_ctx* c) {
         StageMark m(c, 3);
         tk::launch_scan_emit(s, st);
     }
+}
+
+void do_render(tk_ctx* c) {
+    scan_phase(c);
+    cudaStream_t st = c->stream;
     tk::launch_fill(c->image.ptr, uint64_t(c->width) * c->height, c->clear, st);
     std::vector<uint32_t*> targets{c->image.ptr};
     std::vector<const Step*> open;
@@ -581,6 +614,12 @@ void tk_ctx_destroy(tk_ctx* c) {
     for (auto& p : c->passes) {
         p.d_batches.release(); p.bin_lists.release(); p.bin_counts.release(); p.tiles.release(); p.ptcl.release();
     }
+    c->seg_line.release();
+    DiffState& D = c->diff;
+    D.colp.release(); D.target.release(); D.layer.release(); D.t1.release(); D.blurred.release(); D.gI.release();
+    D.d0.release(); D.d1.release(); D.scratch.release(); D.line_acc.release(); D.color_acc.release();
+    D.dpoints.release(); D.taps.release(); D.dtaps.release(); D.ep_w.release(); D.ep_point.release();
+    D.sums.release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -893,6 +932,185 @@ int32_t tk_pool_scan_noalloc(tk_ctx* c, const tk_path_record* paths, uint32_t pa
         TK_CUDA(cudaMemcpyAsync(&err, sc.words, 4, cudaMemcpyDeviceToHost, st));
         TK_CUDA(cudaStreamSynchronize(st));
         if (err) throw Fail{TK_E_TIMEOUT, "prefix look-back gave up"};
+    });
+}
+
+int32_t tk_diff_forward(tk_ctx* c, const tk_diff_scene* sc, const float* target, double* loss, float* image) {
+    return guarded(c, [&] {
+        if (!sc || !sc->points || !sc->colors || !target || !loss) invalid("null argument");
+        if (sc->width == 0 || sc->height == 0 || sc->path_count == 0 || sc->cubics_per_path == 0)
+            invalid("empty differentiable scene");
+        if (!(sc->sigma >= 0.0f) || !std::isfinite(sc->sigma) || !(sc->tolerance > 0.0f))
+            invalid("sigma must be >= 0 and tolerance > 0");
+        DiffState& D = c->diff;
+        D.ready = false;
+        const uint32_t per = 1u + 3u * sc->cubics_per_path;
+        // flattening with endpoint weights
+        const uint64_t nl = tk_diff_flatten(sc, nullptr, nullptr, nullptr, 0);
+        std::vector<tk_line> lines(nl);
+        std::vector<uint32_t> ep_point(2 * nl);
+        std::vector<float> ep_w(8 * nl);
+        tk_diff_flatten(sc, lines.data(), ep_point.data(), ep_w.data(), nl);
+        // the same scene through the Canvas: blur group, one fill per path
+        std::unique_ptr<tk_canvas, void (*)(tk_canvas*)> cv(tk_canvas_new(sc->width, sc->height, 1.0f),
+                                                           tk_canvas_free);
+        if (sc->sigma > 0.0f) tk_canvas_push_blur_group(cv.get(), sc->sigma);
+        D.colors.assign(sc->colors, sc->colors + 4ull * sc->path_count);
+        std::vector<float4> colp(sc->path_count);
+        for (uint32_t p = 0; p < sc->path_count; ++p) {
+            const float* P = sc->points + size_t(2) * per * p;
+            tk_path* path = tk_path_new();
+            tk_path_move_to(path, P[0], P[1]);
+            for (uint32_t k = 0; k < sc->cubics_per_path; ++k) {
+                const float* q = P + 2 * (3 * k + 1);
+                tk_path_cubic_to(path, q[0], q[1], q[2], q[3], q[4], q[5]);
+            }
+            tk_path_close(path);
+            const float* col = sc->colors + 4 * p;
+            tk_brush_desc b{};
+            b.kind = TK_BRUSH_KIND_SOLID;
+            std::memcpy(b.rgba, col, sizeof(b.rgba));
+            tk_canvas_push_path(cv.get(), path, &b, nullptr, TK_FILL_NONZERO, double(sc->tolerance));
+            tk_path_free(path);
+            colp[p] = make_float4(col[0] * col[3], col[1] * col[3], col[2] * col[3], col[3]);
+        }
+        if (sc->sigma > 0.0f) tk_canvas_pop_layer(cv.get());
+        tk_scene_desc d{};
+        if (tk_canvas_scene(cv.get(), &d) != TK_OK) invalid("canvas compile failed");
+        if (d.line_count != nl || (nl && std::memcmp(d.lines, lines.data(), nl * sizeof(tk_line)) != 0))
+            throw Fail{TK_E_INVALID, "differentiable flattening differs from the canvas flattening"};
+        do_upload(c, d);
+        uint32_t pass = UINT32_MAX;
+        for (const Step& s : c->steps)
+            if (s.kind == STEP_PASS) {
+                if (pass != UINT32_MAX) invalid("differentiable scenes have one target pass");
+                pass = s.pass;
+            }
+        if (pass == UINT32_MAX) invalid("no draw pass");
+        cudaStream_t st = c->stream;
+        c->seg_line.reserve(std::max<uint64_t>(c->host_segment_capacity, 1));
+        c->want_seg_line = true;
+        scan_phase(c);
+        run_pass(c, c->passes[pass], nullptr, false);
+        check_error_word(c);
+        const uint64_t n = uint64_t(sc->width) * sc->height;
+        upload(D.colp, colp.data(), colp.size(), st);
+        upload(D.target, reinterpret_cast<const float4*>(target), n, st);
+        upload(D.ep_point, ep_point.data(), ep_point.size(), st);
+        upload(D.ep_w, ep_w.data(), ep_w.size(), st);
+        D.layer.reserve(n);
+        D.gI.reserve(n);
+        D.sums.reserve(2);
+        TK_CUDA(cudaMemsetAsync(D.sums.ptr, 0, 2 * sizeof(double), st));
+        tk::SceneView s = view(c);
+        tk::PassView v = pass_view(c, c->passes[pass]);
+        tk::launch_diff_fine_fwd(s, v, D.colp.ptr, D.layer.ptr, st);
+        const float4* B = D.layer.ptr;
+        D.radius = 0;
+        if (sc->sigma > 0.0f) {
+            // taps and their sigma derivatives, r = ceil(3 sigma)
+            const int32_t r = int32_t(std::ceil(3.0 * double(sc->sigma)));
+            const double sg = double(sc->sigma);
+            std::vector<double> e(2 * r + 1), de(2 * r + 1);
+            double S = 0.0, dS = 0.0;
+            for (int32_t k = -r; k <= r; ++k) {
+                e[k + r] = std::exp(-double(k) * k / (2.0 * sg * sg));
+                de[k + r] = e[k + r] * double(k) * k / (sg * sg * sg);
+                S += e[k + r];
+                dS += de[k + r];
+            }
+            std::vector<float> w(2 * r + 1), wd(2 * r + 1);
+            for (int32_t k = 0; k <= 2 * r; ++k) {
+                w[k] = float(e[k] / S);
+                wd[k] = float((de[k] * S - e[k] * dS) / (S * S));
+            }
+            upload(D.taps, w.data(), w.size(), st);
+            upload(D.dtaps, wd.data(), wd.size(), st);
+            D.t1.reserve(n);
+            D.blurred.reserve(n);
+            tk::launch_diff_blur(D.layer.ptr, D.t1.ptr, D.taps.ptr, r, sc->width, sc->height, 0, st);
+            tk::launch_diff_blur(D.t1.ptr, D.blurred.ptr, D.taps.ptr, r, sc->width, sc->height, 1, st);
+            B = D.blurred.ptr;
+            D.radius = r;
+        }
+        D.bg = make_float4(sc->background[0], sc->background[1], sc->background[2], sc->background[3]);
+        if (image) D.d0.reserve(n);
+        tk::launch_diff_composite(B, D.target.ptr, D.bg, n, image ? D.d0.ptr : nullptr, D.gI.ptr, D.sums.ptr, st);
+        TK_CUDA(cudaGetLastError());
+        check_error_word(c);
+        TK_CUDA(cudaMemcpyAsync(loss, D.sums.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (image) TK_CUDA(cudaMemcpyAsync(image, D.d0.ptr, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        D.width = sc->width;
+        D.height = sc->height;
+        D.paths = sc->path_count;
+        D.points = per * sc->path_count;
+        D.lines = nl;
+        D.sigma = sc->sigma;
+        D.pass = pass;
+        D.ready = true;
+    });
+}
+
+int32_t tk_diff_backward(tk_ctx* c, float* d_points, float* d_colors, float* d_sigma) {
+    return guarded(c, [&] {
+        DiffState& D = c->diff;
+        if (!D.ready || !c->have_scene) throw Fail{TK_E_STATE, "no differentiable forward to differentiate"};
+        cudaStream_t st = c->stream;
+        const uint64_t n = uint64_t(D.width) * D.height;
+        Pass& p = c->passes[D.pass];
+        D.d0.reserve(n);
+        D.d1.reserve(n);
+        D.line_acc.reserve(D.lines);
+        D.color_acc.reserve(5ull * c->draw_count);
+        D.dpoints.reserve(2ull * D.points);
+        D.scratch.reserve(std::max<uint64_t>(p.ptcl_used, 1) * 256);
+        TK_CUDA(cudaMemsetAsync(D.sums.ptr + 1, 0, sizeof(double), st));
+        TK_CUDA(cudaMemsetAsync(D.line_acc.ptr, 0, std::max<uint64_t>(D.lines, 1) * sizeof(float2), st));
+        TK_CUDA(cudaMemsetAsync(D.color_acc.ptr, 0, 5ull * std::max(c->draw_count, 1u) * sizeof(float), st));
+        TK_CUDA(cudaMemsetAsync(D.dpoints.ptr, 0, 2ull * D.points * sizeof(float), st));
+        const float4* dL = nullptr;
+        if (D.radius > 0) {
+            // B = Gy(Gx L): dT1 = Gy^T dB (+ <dB, Gy' T1>), dL = Gx^T dT1 (+ <dT1, Gx' L>)
+            tk::launch_diff_blur_bwd(D.gI.ptr, D.t1.ptr, D.d0.ptr, D.taps.ptr, D.dtaps.ptr, D.radius, D.width,
+                                     D.height, 1, true, D.bg, D.sums.ptr + 1, st);
+            tk::launch_diff_blur_bwd(D.d0.ptr, D.layer.ptr, D.d1.ptr, D.taps.ptr, D.dtaps.ptr, D.radius, D.width,
+                                     D.height, 0, false, D.bg, D.sums.ptr + 1, st);
+            dL = D.d1.ptr;
+        } else {
+            tk::launch_diff_composite_bwd(D.gI.ptr, D.bg, n, D.d0.ptr, st);
+            dL = D.d0.ptr;
+        }
+        tk::SceneView s = view(c);
+        tk::PassView v = pass_view(c, p);
+        tk::launch_diff_fine_bwd(s, v, c->seg_line.ptr, D.colp.ptr, dL, D.scratch.ptr, D.line_acc.ptr,
+                                 D.color_acc.ptr, st);
+        tk::launch_diff_lines_to_points(c->lines.ptr, D.line_acc.ptr, D.ep_point.ptr, D.ep_w.ptr, D.lines,
+                                        D.dpoints.ptr, st);
+        TK_CUDA(cudaGetLastError());
+        check_error_word(c);
+        std::vector<float> cacc(5ull * c->draw_count);
+        double dsig = 0.0;
+        if (d_points)
+            TK_CUDA(cudaMemcpyAsync(d_points, D.dpoints.ptr, 2ull * D.points * sizeof(float), cudaMemcpyDeviceToHost,
+                                    st));
+        if (!cacc.empty())
+            TK_CUDA(cudaMemcpyAsync(cacc.data(), D.color_acc.ptr, cacc.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                    st));
+        TK_CUDA(cudaMemcpyAsync(&dsig, D.sums.ptr + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        if (d_colors) {
+            // colp = (r a, g a, b a, a): chain to the straight colour
+            for (uint32_t i = 0; i < D.paths; ++i) {
+                const float* col = D.colors.data() + 4 * i;
+                const float* g = cacc.data() + 5 * i;
+                d_colors[4 * i + 0] = g[0] * col[3];
+                d_colors[4 * i + 1] = g[1] * col[3];
+                d_colors[4 * i + 2] = g[2] * col[3];
+                d_colors[4 * i + 3] = g[0] * col[0] + g[1] * col[1] + g[2] * col[2] + g[3] + g[4];
+            }
+        }
+        if (d_sigma) *d_sigma = float(dsig);
     });
 }
 

@@ -14,6 +14,7 @@
 
 #include "../../include/tileink.h"
 #include "../../include/tileink_canvas.h"
+#include "../../include/tileink_diff.h"
 #include "planner.h"
 
 namespace {
@@ -24,6 +25,23 @@ struct Pt {
 inline Pt operator+(Pt a, Pt b) { return {a.x + b.x, a.y + b.y}; }
 inline Pt operator-(Pt a, Pt b) { return {a.x - b.x, a.y - b.y}; }
 inline Pt operator*(Pt a, double s) { return {a.x * s, a.y * s}; }
+inline const Pt& val(const Pt& p) { return p; }
+
+// A flattened point together with its weights over the four control points of
+// the cubic being flattened: every point the flattener emits is a fixed linear
+// combination of them once the subdivision is fixed.
+struct WPt {
+    Pt v;
+    double w[4];
+};
+inline WPt operator+(const WPt& a, const WPt& b) {
+    return {a.v + b.v, {a.w[0] + b.w[0], a.w[1] + b.w[1], a.w[2] + b.w[2], a.w[3] + b.w[3]}};
+}
+inline WPt operator-(const WPt& a, const WPt& b) {
+    return {a.v - b.v, {a.w[0] - b.w[0], a.w[1] - b.w[1], a.w[2] - b.w[2], a.w[3] - b.w[3]}};
+}
+inline WPt operator*(const WPt& a, double s) { return {a.v * s, {a.w[0] * s, a.w[1] * s, a.w[2] * s, a.w[3] * s}}; }
+inline const Pt& val(const WPt& p) { return p.v; }
 
 enum Verb : uint8_t { MOVE, LINE, QUAD, CUBIC, CLOSE };
 struct El {
@@ -55,19 +73,21 @@ inline double approx_inv_integral(double x) {
     const double b = 0.39;
     return x * (1.0 - b + std::sqrt(b * b + 0.25 * x * x));
 }
-inline Pt quad_eval(Pt p0, Pt p1, Pt p2, double t) {
+template <class P>
+inline P quad_eval(P p0, P p1, P p2, double t) {
     double mt = 1.0 - t;
     return p0 * (mt * mt) + p1 * (2.0 * mt * t) + p2 * (t * t);
 }
-template <class Emit>
-void flatten_quad(Pt p0, Pt p1, Pt p2, double tol, Emit&& emit) {
+template <class P, class Emit>
+void flatten_quad(P q0, P q1, P q2, double tol, Emit&& emit) {
+    const Pt &p0 = val(q0), &p1 = val(q1), &p2 = val(q2);
     double ddx = 2.0 * p1.x - p0.x - p2.x, ddy = 2.0 * p1.y - p0.y - p2.y;
     double u0 = (p1.x - p0.x) * ddx + (p1.y - p0.y) * ddy;
     double u2 = (p2.x - p1.x) * ddx + (p2.y - p1.y) * ddy;
     double cross = (p2.x - p0.x) * ddy - (p2.y - p0.y) * ddx;
     double dd = std::hypot(ddx, ddy);
     if (dd < 1e-12) {
-        emit(p2);
+        emit(q2);
         return;
     }
     double x0 = u0 / cross, x2 = u2 / cross;
@@ -76,8 +96,8 @@ void flatten_quad(Pt p0, Pt p1, Pt p2, double tol, Emit&& emit) {
         // Nearly collinear control points: uniform steps with the chord bound
         // |B''| h^2 / 8 = |dd| h^2 / 4 <= tol.
         int n = std::max(1, int(std::ceil(std::sqrt(dd / (4.0 * tol)))));
-        for (int i = 1; i < n; ++i) emit(quad_eval(p0, p1, p2, double(i) / n));
-        emit(p2);
+        for (int i = 1; i < n; ++i) emit(quad_eval(q0, q1, q2, double(i) / n));
+        emit(q2);
         return;
     }
     double a0 = approx_integral(x0), a2 = approx_integral(x2);
@@ -87,30 +107,33 @@ void flatten_quad(Pt p0, Pt p1, Pt p2, double tol, Emit&& emit) {
     for (int i = 1; i < n; ++i) {
         double v = approx_inv_integral(a0 + (a2 - a0) * double(i) / n);
         double t = (v - v0) / (v2 - v0);
-        emit(quad_eval(p0, p1, p2, t));
+        emit(quad_eval(q0, q1, q2, t));
     }
-    emit(p2);
+    emit(q2);
 }
-inline Pt cubic_eval(const Pt c[4], double t) {
+template <class P>
+inline P cubic_eval(const P c[4], double t) {
     double mt = 1.0 - t;
     return c[0] * (mt * mt * mt) + c[1] * (3.0 * mt * mt * t) + c[2] * (3.0 * mt * t * t) + c[3] * (t * t * t);
 }
-inline Pt cubic_deriv(const Pt c[4], double t) {
+template <class P>
+inline P cubic_deriv(const P c[4], double t) {
     double mt = 1.0 - t;
     return (c[1] - c[0]) * (3.0 * mt * mt) + (c[2] - c[1]) * (6.0 * mt * t) + (c[3] - c[2]) * (3.0 * t * t);
 }
-template <class Emit>
-void flatten_cubic(const Pt c[4], double tol, Emit&& emit) {
+template <class P, class Emit>
+void flatten_cubic(const P c[4], double tol, Emit&& emit) {
     const double quad_share = 0.1;
-    Pt third{c[3].x - 3.0 * c[2].x + 3.0 * c[1].x - c[0].x, c[3].y - 3.0 * c[2].y + 3.0 * c[1].y - c[0].y};
+    const Pt &c0 = val(c[0]), &c1 = val(c[1]), &c2 = val(c[2]), &c3 = val(c[3]);
+    Pt third{c3.x - 3.0 * c2.x + 3.0 * c1.x - c0.x, c3.y - 3.0 * c2.y + 3.0 * c1.y - c0.y};
     double err = std::sqrt(3.0) / 36.0 * std::hypot(third.x, third.y);
     int m = std::max(1, int(std::ceil(std::cbrt(err / (quad_share * tol)))));
     m = std::min(m, 1 << 16);
     for (int j = 0; j < m; ++j) {
         double t0 = double(j) / m, t1 = double(j + 1) / m, h = (t1 - t0) / 3.0;
-        Pt q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
-        Pt q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
-        Pt ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
+        P q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
+        P q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
+        P ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
         if (j == m - 1) q3 = c[3];
         flatten_quad(q0, ctrl, q3, (1.0 - quad_share) * tol, emit);
     }
@@ -1068,4 +1091,57 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             return nullptr;
     }
     return c;
+}
+
+// The differentiable scene's flattening: flatten_path on move_to, cubic_to...,
+// close, with every point carrying its weights over the four control points of
+// its cubic (WPt), so that d(line endpoint)/d(control point) is known.
+uint64_t tk_diff_flatten(const tk_diff_scene* sc, tk_line* lines, uint32_t* endpoint_point, float* endpoint_weights,
+                         uint64_t capacity) {
+    if (!sc || !sc->points || sc->cubics_per_path == 0) return 0;
+    const uint32_t n = sc->cubics_per_path, per = 1u + 3u * n;
+    const double tol = double(sc->tolerance);
+    struct Node {
+        WPt p;
+        uint32_t base;  // global index of the first of the four control points the weights refer to
+    };
+    uint64_t count = 0;
+    for (uint32_t path = 0; path < sc->path_count; ++path) {
+        const float* P = sc->points + size_t(2) * per * path;
+        auto pt = [&](uint32_t j) { return Pt{double(P[2 * j]), double(P[2 * j + 1])}; };
+        const uint32_t first = path * per;
+        const Node start{{pt(0), {1.0, 0.0, 0.0, 0.0}}, first};
+        Node last = start;
+        auto push = [&](const Node& a, const Node& b) {
+            double dx = a.p.v.x - b.p.v.x, dy = a.p.v.y - b.p.v.y;
+            if (!(dx * dx + dy * dy > 1.0e-12 * 1.0e-12)) return;
+            if (count < capacity) {
+                if (lines)
+                    lines[count] = tk_line{path, 0.0f, {float(a.p.v.x), float(a.p.v.y)}, {float(b.p.v.x), float(b.p.v.y)}};
+                if (endpoint_point) {
+                    endpoint_point[2 * count] = a.base;
+                    endpoint_point[2 * count + 1] = b.base;
+                }
+                if (endpoint_weights)
+                    for (int i = 0; i < 4; ++i) {
+                        endpoint_weights[8 * count + i] = float(a.p.w[i]);
+                        endpoint_weights[8 * count + 4 + i] = float(b.p.w[i]);
+                    }
+            }
+            ++count;
+        };
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t base = first + 3u * k;
+            // c[0] is the previous cubic's exact end point, pt(3k)
+            const WPt c[4] = {{pt(3 * k), {1, 0, 0, 0}}, {pt(3 * k + 1), {0, 1, 0, 0}},
+                              {pt(3 * k + 2), {0, 0, 1, 0}}, {pt(3 * k + 3), {0, 0, 0, 1}}};
+            flatten_cubic(c, tol, [&](const WPt& q) {
+                const Node nd{q, base};
+                push(last, nd);
+                last = nd;
+            });
+        }
+        push(last, start);
+    }
+    return count;
 }

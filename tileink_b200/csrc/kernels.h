@@ -49,6 +49,7 @@ struct SceneView {
     tk_line_segment* segments;
     uint64_t segment_capacity;
     uint32_t* error;
+    uint32_t* seg_line;  // optional: line index of every emitted segment
 };
 
 void launch_scan_count(const SceneView& s, cudaStream_t st);
@@ -109,5 +110,20 @@ void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const 
 
 // FP32 FMA peak probe (TFLOP/s).
 double probe_fp32_tflops(cudaStream_t st);
+
+// Differentiable rendering (diff.cu): float forward and adjoint.
+void launch_diff_fine_fwd(const SceneView& s, const PassView& p, const float4* colp, float4* layer, cudaStream_t st);
+void launch_diff_blur(const float4* in, float4* out, const float* w, int32_t r, uint32_t width, uint32_t height,
+                      int32_t axis, cudaStream_t st);
+void launch_diff_composite(const float4* B, const float4* target, float4 bg, uint64_t n, float4* image, float4* gI,
+                           double* loss, cudaStream_t st);
+void launch_diff_blur_bwd(const float4* dout_src, const float4* fwd_in, float4* din, const float* w, const float* wd,
+                          int32_t r, uint32_t width, uint32_t height, int32_t axis, bool from_gI, float4 bg,
+                          double* sig, cudaStream_t st);
+void launch_diff_composite_bwd(const float4* gI, float4 bg, uint64_t n, float4* dL, cudaStream_t st);
+void launch_diff_fine_bwd(const SceneView& s, const PassView& p, const uint32_t* seg_line, const float4* colp,
+                          const float4* dlayer, float2* scratch, float2* line_acc, float* color_acc, cudaStream_t st);
+void launch_diff_lines_to_points(const tk_line* lines, const float2* line_acc, const uint32_t* ep_base,
+                                 const float* ep_w, uint64_t n, float* dpoints, cudaStream_t st);
 
 }  // namespace tk

@@ -251,7 +251,7 @@ __global__ void k_path_totals(tk_path_record* paths, uint32_t path_count, const 
 
 __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
                             uint32_t path_count, uint32_t* cursors, tk_line_segment* segments, uint64_t capacity,
-                            uint32_t* error) {
+                            uint32_t* error, uint32_t* seg_line) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -298,6 +298,7 @@ __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_rec
                         dst[2] = seg.p1x;
                         dst[3] = seg.p1y;
                         dst[4] = seg.y_edge;
+                        if (seg_line) seg_line[slot] = p.line_start + l;
                     } else {
                         atomicOr(error, ERR_SEGMENT_OVERFLOW);
                     }
@@ -344,7 +345,8 @@ void launch_scan_emit(const SceneView& s, cudaStream_t st) {
     if (s.path_count == 0) return;
     uint64_t threads = uint64_t(s.path_count) * 32;
     k_scan_emit<<<grid_for(threads, 256, 148 * 32), 256, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
-                                                                 s.segments, s.segment_capacity, s.error);
+                                                                 s.segments, s.segment_capacity, s.error,
+                                                                 s.seg_line);
 }
 
 }  // namespace tk

@@ -120,6 +120,30 @@ class NativeRenderer:
         self._check(self._lib.tk_pool_scan_noalloc(self._h, N.ptr(paths), len(paths), d_counts, d_backdrops,
                                                    d_ranges, d_cursors, int(pool_len), d_bumps))
 
+    # --- differentiable rendering ---------------------------------------------
+    def diff_forward(self, scene, target, return_image=False):
+        """Loss (and optionally the [H, W, 4] f32 image) of a DiffScene against
+        `target` ([H, W, 4] premultiplied f32)."""
+        d = scene.desc()
+        tgt = np.ascontiguousarray(target, dtype=np.float32)
+        if tgt.shape != (scene.height, scene.width, 4):
+            raise ValueError("target must be [height, width, 4]")
+        loss = C.c_double(0.0)
+        img = np.zeros_like(tgt) if return_image else None
+        self._check(self._lib.tk_diff_forward(self._h, C.byref(d), N.ptr(tgt), C.byref(loss),
+                                              N.ptr(img) if img is not None else None))
+        self._diff_shape = (scene.points.shape, scene.colors.shape)
+        return (loss.value, img) if return_image else loss.value
+
+    def diff_backward(self):
+        """(d_points, d_colors, d_sigma) of the last diff_forward."""
+        pshape, cshape = getattr(self, "_diff_shape", ((0, 0, 2), (0, 4)))
+        dp = np.zeros(pshape, dtype=np.float32)
+        dc = np.zeros(cshape, dtype=np.float32)
+        ds = C.c_float(0.0)
+        self._check(self._lib.tk_diff_backward(self._h, N.ptr(dp), N.ptr(dc), C.byref(ds)))
+        return dp, dc, ds.value
+
     def stage_scan_count(self, lines, paths, backdrops, counts):
         lines = np.ascontiguousarray(lines, dtype=N.LINE_DTYPE)
         paths = np.ascontiguousarray(paths, dtype=N.PATH_DTYPE)
