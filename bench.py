@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--paths", type=int, default=0, help="override the path count (smaller trial runs)")
     p.add_argument("--size", type=int, default=0, help="override the canvas side (smaller trial runs)")
     p.add_argument("--diff-steps", type=int, default=10, help="timed fwd+bwd steps of the blur-group workload (0: skip)")
+    p.add_argument("--batch-scenes", type=int, default=512, help="scenes of the batched-mode leg (0: skip)")
     return p.parse_args()
 
 
@@ -148,6 +149,50 @@ def diff_timing(renderer, steps, warmup):
             "bwd_ms": float(np.median(bwd)), "steps": steps, "loss": loss,
             "timing": "host wall clock per call (median), host buffers in and out",
             "gradient_check": "tests/test_gpu_diff.py: FP64 central differences, relative error <= 1e-3"}
+
+
+def batch_timing(n_scenes, steps):
+    """Batched vs serial scenes/s on the uneven-batch workload: n_scenes
+    independent scenes, width and height each log-uniform in [64, 1024],
+    log-uniform 10..2000 closed cubic paths with solid fills (seeds 1000..).
+    serial: upload + render + readback per scene through tk_render_to_image.
+    batched: the whole batch in one CUDA graph launch (tk_batch_render) after
+    the autotuner picked the pool-scan work item size; `value` with the
+    scenes resident on the device, `e2e` with upload and readback."""
+    import tileink_b200 as tk
+    scenes = [tk.generate(4, 1000 + i) for i in range(n_scenes)]
+    r = tk.NativeRenderer(0)
+    for c in scenes[:8]:
+        r.render_to_image(c)
+    t0 = time.perf_counter()
+    for c in scenes:
+        r.render_to_image(c)
+    serial_s = time.perf_counter() - t0
+    r.close()
+    b = tk.NativeRenderer(0)
+    t0 = time.perf_counter()
+    b.batch_upload(scenes)
+    b.batch_render()
+    imgs = b.batch_readback()
+    e2e_s = time.perf_counter() - t0
+    tune = b.autotune(3)
+    b.batch_render()
+    b.batch_readback()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b.batch_render()
+    b.batch_readback()
+    render_s = (time.perf_counter() - t0) / steps
+    del imgs
+    b.close()
+    return {"workload": f"{n_scenes} scenes, W and H log-uniform in [64, 1024], 10-2000 closed cubic paths, solid",
+            "serial_scenes_per_s": n_scenes / serial_s, "batched_scenes_per_s": n_scenes / render_s,
+            "batched_e2e_scenes_per_s": n_scenes / e2e_s, "speedup": serial_s / render_s,
+            "speedup_e2e": serial_s / e2e_s, "batched_ms": render_s * 1e3, "steps": steps,
+            "scan_item_elems": tune.scan_item_elems, "tile": f"{tune.tile_width}x{tune.tile_height}",
+            "tune_ms": {str(tune.candidate_elems[i]): tune.candidate_ms[i] for i in range(tune.candidates)},
+            "timing": "host wall clock; batched = graph replays + one readback, serial = per-scene upload, "
+                      "render and readback"}
 
 
 def cpu_baseline(size, paths):
@@ -361,6 +406,7 @@ def main():
     if rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.size, args.paths)
     diff_line = diff_timing(r, args.diff_steps, args.warmup) if (rank == 0 and args.diff_steps > 0) else None
+    batch_line = batch_timing(args.batch_scenes, 5) if (rank == 0 and args.batch_scenes > 0) else None
 
     launches_per_frame = 5 + 5 * stats["passes"]
     if rank == 0:
@@ -383,6 +429,7 @@ def main():
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "fwd_bwd": diff_line,
+            "batched": batch_line,
             "scene_generation_s": gen_s,
         }
         print(json.dumps(line), flush=True)

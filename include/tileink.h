@@ -349,6 +349,45 @@ int32_t tk_stage_blur(tk_ctx* ctx, const uint32_t* src, uint32_t* dst,
                       const uint32_t source[4], float sigma, uint32_t axis);
 
 /* ------------------------------------------------------------------------ */
+/* Batched mode: many independent scenes of uneven size rendered together.   */
+/* Every stage runs once for the whole batch (the scenes' paths, tiles, bins */
+/* and images are concatenated) and the stage sequence is one CUDA graph,    */
+/* instantiated on the first tk_batch_render and replayed after that.        */
+/* Each scene's PTCL equals its serial tk_render PTCL with the offsets of    */
+/* tk_batch_info added to segment, draw and batch indices.                   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct tk_batch_info {
+    uint32_t width, height;
+    uint32_t tile_base, tile_count;   /* the scene's tile records in the batch pass */
+    uint32_t path_base, draw_base, batch_base, line_base;
+    uint32_t layer_base, reserved;
+    uint64_t segment_base, pool_base; /* added to its segment / backdrop indices */
+    uint64_t image_offset;            /* its first pixel in the batch image */
+} tk_batch_info;
+
+/* Scenes with one target pass (draw batches and clip layers; no blur
+ * groups) and host segment planning. Replaces any uploaded scene. */
+int32_t tk_batch_upload(tk_ctx* ctx, const tk_scene_desc* scenes, uint32_t scene_count);
+/* Renders the whole batch on the context stream; asynchronous. */
+int32_t tk_batch_render(tk_ctx* ctx);
+int32_t tk_batch_info_get(tk_ctx* ctx, uint32_t scene, tk_batch_info* out);
+/* All images, scene after scene (tk_batch_info.image_offset). */
+int32_t tk_batch_readback(tk_ctx* ctx, uint32_t* rgba8, size_t pixel_count);
+
+/* Autotuner: renders the uploaded scene or batch with each pool-scan work
+ * item size (512, 1024, 2048, 4096 tiles; bbox rows are never split), keeps
+ * the fastest for later renders and reports the timings. Tiles are 16x16. */
+typedef struct tk_tune_result {
+    uint32_t scan_item_elems;     /* chosen */
+    uint32_t tile_width, tile_height;
+    uint32_t candidates;
+    uint32_t candidate_elems[8];
+    float candidate_ms[8];        /* median frame time of each candidate */
+} tk_tune_result;
+int32_t tk_autotune(tk_ctx* ctx, uint32_t iterations, tk_tune_result* out);
+
+/* ------------------------------------------------------------------------ */
 /* Allocation-free pool scan. No reference counterpart: the reference's      */
 /* scan runs on buffers its runtime allocated up front, and this entry point */
 /* gives C callers the same property.                                        */

@@ -98,6 +98,20 @@ class DiffScene(C.Structure):
                 ("sigma", C.c_float), ("tolerance", C.c_float), ("background", C.c_float * 4)]
 
 
+class BatchInfo(C.Structure):
+    """tk_batch_info (include/tileink.h)."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("tile_base", C.c_uint32), ("tile_count", C.c_uint32),
+                ("path_base", C.c_uint32), ("draw_base", C.c_uint32), ("batch_base", C.c_uint32),
+                ("line_base", C.c_uint32), ("layer_base", C.c_uint32), ("reserved", C.c_uint32),
+                ("segment_base", C.c_uint64), ("pool_base", C.c_uint64), ("image_offset", C.c_uint64)]
+
+
+class TuneResult(C.Structure):
+    """tk_tune_result (include/tileink.h)."""
+    _fields_ = [("scan_item_elems", C.c_uint32), ("tile_width", C.c_uint32), ("tile_height", C.c_uint32),
+                ("candidates", C.c_uint32), ("candidate_elems", C.c_uint32 * 8), ("candidate_ms", C.c_float * 8)]
+
+
 class GenParams(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("paths", C.c_uint32), ("variant", C.c_uint32),
                 ("sigma", C.c_float), ("jitter", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
@@ -133,6 +147,11 @@ def library() -> C.CDLL:
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
         "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),
+        "tk_batch_upload": (I32, [P, P, U32]),
+        "tk_batch_render": (I32, [P]),
+        "tk_batch_info_get": (I32, [P, U32, C.POINTER(BatchInfo)]),
+        "tk_batch_readback": (I32, [P, P, C.c_size_t]),
+        "tk_autotune": (I32, [P, U32, C.POINTER(TuneResult)]),
         "tk_diff_forward": (I32, [P, C.POINTER(DiffScene), P, C.POINTER(C.c_double), P]),
         "tk_diff_backward": (I32, [P, P, P, P]),
         "tk_diff_flatten": (U64, [C.POINTER(DiffScene), P, P, P, U64]),

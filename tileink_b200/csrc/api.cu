@@ -126,6 +126,17 @@ struct tk_ctx {
     DBuf<uint32_t> seg_line;
     bool want_seg_line = false;
     DiffState diff;
+    // pool-scan work item size in tiles (whole bbox rows up to this many)
+    uint32_t scan_item_elems = tk::kScanItemElems;
+    // batched mode: several canvases in one pass, rendered by one graph launch
+    bool batched = false;
+    std::vector<tk::BatchScene> h_scenes;
+    std::vector<tk_batch_info> h_batch_info;
+    DBuf<tk::BatchScene> d_scenes;
+    DBuf<uint32_t> bin_scene, tile_scene;
+    uint32_t total_bins = 0, total_tiles = 0;
+    uint64_t total_pixels = 0;
+    cudaGraphExec_t graph_exec = nullptr;
     // stage timing
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -193,7 +204,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         if (pool > 0xFFFFFFFFull) invalid("backdrop pool exceeds u32 indexing");
         seg_cap = std::max<uint64_t>(seg_cap, uint64_t(r.segment_start) + r.segment_capacity);
         if (r.data_len) {
-            uint32_t rows_per = std::max<uint32_t>(1u, tk::kScanItemElems / stride);
+            uint32_t rows_per = std::max<uint32_t>(1u, c->scan_item_elems / stride);
             for (uint32_t row = 0; row < height; row += rows_per)
                 c->h_items.push_back({p, row, std::min(rows_per, height - row), row == 0u ? 1u : 0u});
         }
@@ -348,6 +359,14 @@ tk::PassView pass_view(tk_ctx* c, Pass& p) {
     v.ticket = c->misc.ptr + 1;
     v.ptcl_total = c->misc.ptr + 3;
     v.stats = c->stats.ptr;
+    if (c->batched) {
+        v.scenes = c->d_scenes.ptr;
+        v.bin_scene = c->bin_scene.ptr;
+        v.tile_scene = c->tile_scene.ptr;
+        v.total_bins = c->total_bins;
+        v.total_tiles = c->total_tiles;
+        v.scene_count = uint32_t(c->h_scenes.size());
+    }
     return v;
 }
 
@@ -364,6 +383,9 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d) {
     c->rendered = false;
     c->diff.ready = false;
     c->want_seg_line = false;
+    c->batched = false;
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
     validate_and_plan(c, d);
     cudaStream_t st = c->stream;
     upload(c->lines, d.lines, d.line_count, st);
@@ -576,6 +598,252 @@ void do_render(tk_ctx* c) {
     c->rendered = true;
 }
 
+void drop_graph(tk_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+}
+
+// Pool-scan work items from the current paths and work item size.
+void rebuild_items(tk_ctx* c) {
+    c->h_items.clear();
+    for (uint32_t p = 0; p < uint32_t(c->h_paths.size()); ++p) {
+        const tk_path_record& r = c->h_paths[p];
+        const uint32_t stride = r.tile_x1 > r.tile_x0 ? r.tile_x1 - r.tile_x0 : 0u;
+        const uint32_t height = r.tile_y1 > r.tile_y0 ? r.tile_y1 - r.tile_y0 : 0u;
+        if (!r.data_len) continue;
+        const uint32_t rows_per = std::max<uint32_t>(1u, c->scan_item_elems / stride);
+        for (uint32_t row = 0; row < height; row += rows_per)
+            c->h_items.push_back({p, row, std::min(rows_per, height - row), row == 0u ? 1u : 0u});
+    }
+    upload(c->items, c->h_items.data(), c->h_items.size(), c->stream);
+    c->item_desc.reserve(c->h_items.size());
+}
+
+// Merges one-pass scenes into one batched pass: arrays concatenated with their
+// indices offset, one BatchScene per canvas.
+void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
+    c->have_scene = false;
+    c->rendered = false;
+    c->diff.ready = false;
+    c->want_seg_line = false;
+    c->batched = false;
+    drop_graph(c);
+    if (n == 0 || !scenes) invalid("empty batch");
+    // Lines, the bulk of a batch, go straight from each scene's array into the
+    // device buffer; their path ids are rebased on the device.
+    std::vector<uint64_t> line_base;
+    std::vector<uint32_t> line_path_base;
+    uint64_t total_lines = 0;
+    std::vector<tk_path_record> paths;
+    std::vector<tk_draw_record> draws;
+    std::vector<uint32_t> brush, order, batch_ids, bin_scene, tile_scene;
+    std::vector<tk_layer_record> layers;
+    std::vector<tk::PassBatch> batches;
+    std::vector<tk::BatchScene> table;
+    std::vector<tk_batch_info> info;
+    uint64_t pool = 0, segs = 0, list = 0, pixels = 0;
+    uint32_t tiles = 0, bins = 0, batch_base = 0;
+    for (uint32_t s = 0; s < n; ++s) {
+        const tk_scene_desc& d = scenes[s];
+        if (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) invalid("batched scenes use host segment planning");
+        validate_and_plan(c, d);
+        uint32_t npass = 0;
+        for (const Step& st : c->steps) {
+            if (st.kind != STEP_PASS) invalid("scene " + std::to_string(s) + ": blur groups are not batched");
+            ++npass;
+        }
+        if (npass > 1) invalid("scene " + std::to_string(s) + ": batched scenes have one target pass");
+        tk_batch_info bi{};
+        bi.width = d.width;
+        bi.height = d.height;
+        bi.tile_base = tiles;
+        bi.tile_count = c->tw * c->th;
+        bi.path_base = uint32_t(paths.size());
+        bi.draw_base = uint32_t(draws.size());
+        bi.batch_base = batch_base;
+        bi.line_base = uint32_t(total_lines);
+        bi.layer_base = uint32_t(layers.size());
+        bi.segment_base = segs;
+        bi.pool_base = pool;
+        bi.image_offset = pixels;
+        line_base.push_back(total_lines);
+        line_path_base.push_back(bi.path_base);
+        total_lines += d.line_count;
+        for (uint32_t i = 0; i < d.path_count; ++i) {
+            tk_path_record p = d.paths[i];
+            p.path_id += bi.path_base;
+            p.line_start += bi.line_base;
+            p.data_offset += uint32_t(bi.pool_base);
+            p.segment_start += uint32_t(bi.segment_base);
+            paths.push_back(p);
+        }
+        const uint32_t brush_base = uint32_t(brush.size());
+        for (uint32_t i = 0; i < d.draw_count; ++i) {
+            tk_draw_record r = d.draws[i];
+            if (r.path_id != TK_INVALID_INDEX) r.path_id += bi.path_base;
+            if (r.brush_offset != TK_INVALID_INDEX) r.brush_offset += brush_base;
+            draws.push_back(r);
+            batch_ids.push_back(d.draw_batch_ids[i] == TK_INVALID_INDEX ? TK_INVALID_INDEX
+                                                                        : d.draw_batch_ids[i] + batch_base);
+        }
+        brush.insert(brush.end(), d.brush_blob, d.brush_blob + d.brush_word_count);
+        for (uint32_t i = 0; i < d.layer_count; ++i) {
+            tk_layer_record L = d.layers[i];
+            L.draw += bi.draw_base;
+            layers.push_back(L);
+        }
+        const uint32_t order0 = uint32_t(order.size());
+        for (uint32_t i = 0; i < d.draw_order_count; ++i) order.push_back(d.draw_order[i] + bi.draw_base);
+        uint32_t nb = 0;
+        if (npass)
+            for (const tk::PassBatch& b : c->passes[0].batches) {
+                batches.push_back({b.batch_id + batch_base, b.layer_start + bi.layer_base, b.layer_end + bi.layer_base,
+                                   0u});
+                nb = std::max(nb, b.batch_id + 1u);
+            }
+        for (uint32_t i = 0; i < d.op_count; ++i)
+            if (d.ops[i].kind == TK_OP_DRAW_BATCH) nb = std::max(nb, d.ops[i].batch_id + 1u);
+        tk::BatchScene sc{};
+        sc.tile_base = tiles;
+        sc.bin_base = bins;
+        sc.list_base = list;
+        sc.tw = c->tw;
+        sc.th = c->th;
+        sc.nbx = (c->tw + 15) / 16;
+        sc.order0 = order0;
+        sc.draw_n = npass ? c->passes[0].draw_n : 0u;
+        sc.width = d.width;
+        sc.height = d.height;
+        sc.clear = d.clear_color;
+        sc.image_offset = pixels;
+        const uint32_t nbins = sc.nbx * ((c->th + 15) / 16);
+        for (uint32_t b = 0; b < nbins; ++b) bin_scene.push_back(s);
+        for (uint32_t t = 0; t < sc.tw * sc.th; ++t) tile_scene.push_back(s);
+        table.push_back(sc);
+        info.push_back(bi);
+        tiles += sc.tw * sc.th;
+        bins += nbins;
+        list += uint64_t(nbins) * sc.draw_n;
+        pixels += uint64_t(d.width) * d.height;
+        pool += c->pool_len;
+        segs += c->host_segment_capacity;
+        batch_base += nb;
+        if (pool > 0xFFFFFFFFull || segs > 0xFFFFFFFFull || total_lines > 0xFFFFFFFFull)
+            invalid("batch exceeds u32 indexing");
+    }
+    // merged scene state
+    cudaStream_t st = c->stream;
+    c->lines.reserve(total_lines);
+    for (uint32_t s = 0; s < n; ++s)
+        if (scenes[s].line_count)
+            TK_CUDA(cudaMemcpyAsync(c->lines.ptr + line_base[s], scenes[s].lines, scenes[s].line_count * sizeof(tk_line),
+                                    cudaMemcpyHostToDevice, st));
+    DBuf<uint64_t> d_line_base;
+    DBuf<uint32_t> d_path_base;
+    upload(d_line_base, line_base.data(), line_base.size(), st);
+    upload(d_path_base, line_path_base.data(), line_path_base.size(), st);
+    tk::launch_rebase_lines(c->lines.ptr, total_lines, d_line_base.ptr, d_path_base.ptr, n, st);
+    TK_CUDA(cudaStreamSynchronize(st));
+    d_line_base.release();
+    d_path_base.release();
+    c->flags = 0;
+    c->line_count = total_lines;
+    c->path_count = uint32_t(paths.size());
+    c->draw_count = uint32_t(draws.size());
+    c->layer_count = uint32_t(layers.size());
+    c->order_count = uint32_t(order.size());
+    c->brush_words = brush.size();
+    c->pool_len = pool;
+    c->host_segment_capacity = segs;
+    c->h_paths = paths;
+    c->width = c->height = 0;
+    c->tw = tiles;
+    c->th = 1;
+    c->steps.assign(1, Step{STEP_PASS, 0u, 0.0f, {0, 0, 0, 0}});
+    c->passes.clear();
+    c->passes.emplace_back();
+    Pass& p = c->passes.back();
+    p.order0 = 0;
+    p.draw_n = uint32_t(order.size());
+    p.batch0 = 0;
+    p.batch_n = uint32_t(batches.size());
+    p.batches = batches;
+    upload(c->paths, paths.data(), paths.size(), st);
+    upload(c->draws, draws.data(), draws.size(), st);
+    upload(c->brush, brush.data(), brush.size(), st);
+    upload(c->layers, layers.data(), layers.size(), st);
+    upload(c->batch_ids, batch_ids.data(), batch_ids.size(), st);
+    upload(c->order, order.data(), order.size(), st);
+    rebuild_items(c);
+    c->backdrops.reserve(pool);
+    c->counts.reserve(pool);
+    c->cursors.reserve(pool);
+    c->ranges.reserve(pool);
+    c->bumps.reserve(c->path_count);
+    c->misc.reserve(8);
+    c->stats.reserve(4);
+    c->tile_desc.reserve((tiles + 4095) / 4096 + 1);
+    c->image.reserve(pixels);
+    c->segment_needed = segs;
+    c->segments.reserve(segs + 1);
+    upload(p.d_batches, p.batches.data(), p.batches.size(), st);
+    p.bin_lists.reserve(std::max<uint64_t>(list, 1));
+    p.bin_counts.reserve(bins);
+    p.tiles.reserve(tiles);
+    p.ptcl_needed = 0;
+    upload(c->d_scenes, table.data(), table.size(), st);
+    upload(c->bin_scene, bin_scene.data(), bin_scene.size(), st);
+    upload(c->tile_scene, tile_scene.data(), tile_scene.size(), st);
+    c->h_scenes = table;
+    c->h_batch_info = info;
+    c->total_bins = bins;
+    c->total_tiles = tiles;
+    c->total_pixels = pixels;
+    TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
+    TK_CUDA(cudaGetLastError());
+    c->batched = true;
+    c->have_scene = true;
+}
+
+// The batched frame: scan, clear every canvas, bins, coarse, fine.
+void batch_frame(tk_ctx* c) {
+    scan_phase(c);
+    tk::launch_fill_scenes(c->image.ptr, c->d_scenes.ptr, uint32_t(c->h_scenes.size()), c->stream);
+    run_pass(c, c->passes[0], c->image.ptr);
+}
+
+void do_batch_render(tk_ctx* c) {
+    if (!c->have_scene || !c->batched) throw Fail{TK_E_STATE, "no batch uploaded"};
+    cudaStream_t st = c->stream;
+    if (!c->graph_exec) {
+        // First frame sizes the PTCL (a host read-back), then the same launch
+        // sequence is captured once and replayed from then on.
+        if (c->passes[0].ptcl_needed == 0) {
+            batch_frame(c);
+            check_error_word(c);
+        }
+        const bool timing = c->timing;
+        c->timing = false;
+        cudaGraph_t g = nullptr;
+        TK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        try {
+            batch_frame(c);
+        } catch (...) {
+            cudaStreamEndCapture(st, &g);
+            if (g) cudaGraphDestroy(g);
+            c->timing = timing;
+            throw;
+        }
+        c->timing = timing;
+        TK_CUDA(cudaStreamEndCapture(st, &g));
+        cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        TK_CUDA(e);
+    }
+    TK_CUDA(cudaGraphLaunch(c->graph_exec, st));
+    c->rendered = true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -615,6 +883,8 @@ void tk_ctx_destroy(tk_ctx* c) {
         p.d_batches.release(); p.bin_lists.release(); p.bin_counts.release(); p.tiles.release(); p.ptcl.release();
     }
     c->seg_line.release();
+    drop_graph(c);
+    c->d_scenes.release(); c->bin_scene.release(); c->tile_scene.release();
     DiffState& D = c->diff;
     D.colp.release(); D.target.release(); D.layer.release(); D.t1.release(); D.blurred.release(); D.gI.release();
     D.d0.release(); D.d1.release(); D.scratch.release(); D.line_acc.release(); D.color_acc.release();
@@ -638,7 +908,10 @@ int32_t tk_scene_upload(tk_ctx* c, const tk_scene_desc* d) {
 }
 
 int32_t tk_render(tk_ctx* c) {
-    return guarded(c, [&] { do_render(c); });
+    return guarded(c, [&] {
+        if (c->batched) do_batch_render(c);
+        else do_render(c);
+    });
 }
 
 int32_t tk_readback(tk_ctx* c, uint32_t* rgba8, size_t pixel_count) {
@@ -1111,6 +1384,96 @@ int32_t tk_diff_backward(tk_ctx* c, float* d_points, float* d_colors, float* d_s
             }
         }
         if (d_sigma) *d_sigma = float(dsig);
+    });
+}
+
+int32_t tk_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t scene_count) {
+    return guarded(c, [&] { do_batch_upload(c, scenes, scene_count); });
+}
+
+int32_t tk_batch_render(tk_ctx* c) {
+    return guarded(c, [&] { do_batch_render(c); });
+}
+
+int32_t tk_batch_info_get(tk_ctx* c, uint32_t scene, tk_batch_info* out) {
+    return guarded(c, [&] {
+        if (!c->batched) throw Fail{TK_E_STATE, "no batch uploaded"};
+        if (!out || scene >= c->h_batch_info.size()) invalid("bad scene index");
+        *out = c->h_batch_info[scene];
+    });
+}
+
+int32_t tk_batch_readback(tk_ctx* c, uint32_t* rgba8, size_t pixel_count) {
+    return guarded(c, [&] {
+        if (!c->batched || !c->rendered) throw Fail{TK_E_STATE, "no batch rendered"};
+        if (!rgba8 || pixel_count != c->total_pixels) invalid("pixel count does not match the batch");
+        check_error_word(c);
+        TK_CUDA(cudaMemcpyAsync(rgba8, c->image.ptr, pixel_count * 4, cudaMemcpyDeviceToHost, c->stream));
+        TK_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int32_t tk_autotune(tk_ctx* c, uint32_t iterations, tk_tune_result* out) {
+    return guarded(c, [&] {
+        if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
+        if (!out) invalid("null output");
+        *out = tk_tune_result{};
+        const uint32_t cand[4] = {512u, 1024u, 2048u, 4096u};
+        const uint32_t iters = std::max<uint32_t>(iterations, 1u);
+        cudaStream_t st = c->stream;
+        cudaEvent_t e0, e1;
+        TK_CUDA(cudaEventCreate(&e0));
+        TK_CUDA(cudaEventCreate(&e1));
+        const bool timing = c->timing;
+        c->timing = false;
+        auto frame = [&] {
+            if (c->batched) do_batch_render(c);
+            else do_render(c);
+        };
+        uint32_t best = c->scan_item_elems;
+        float best_ms = 0.0f;
+        try {
+            for (uint32_t k = 0; k < 4; ++k) {
+                c->scan_item_elems = cand[k];
+                rebuild_items(c);
+                drop_graph(c);
+                frame();  // warm-up (and graph capture in batched mode)
+                std::vector<float> ms;
+                for (uint32_t i = 0; i < iters; ++i) {
+                    TK_CUDA(cudaEventRecord(e0, st));
+                    frame();
+                    TK_CUDA(cudaEventRecord(e1, st));
+                    TK_CUDA(cudaEventSynchronize(e1));
+                    float t = 0.0f;
+                    TK_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                    ms.push_back(t);
+                }
+                check_error_word(c);
+                std::sort(ms.begin(), ms.end());
+                const float med = ms[ms.size() / 2];
+                out->candidate_elems[k] = cand[k];
+                out->candidate_ms[k] = med;
+                if (k == 0 || med < best_ms) {
+                    best_ms = med;
+                    best = cand[k];
+                }
+            }
+        } catch (...) {
+            c->timing = timing;
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        c->timing = timing;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c->scan_item_elems = best;
+        rebuild_items(c);
+        drop_graph(c);
+        out->scan_item_elems = best;
+        out->tile_width = TK_TILE_SIZE;
+        out->tile_height = TK_TILE_SIZE;
+        out->candidates = 4;
     });
 }
 

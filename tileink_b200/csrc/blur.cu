@@ -169,12 +169,47 @@ __global__ void k_composite(uint32_t* dst, const uint32_t* src, uint32_t width, 
     dst[o] = src_over_premul_u8(dst[o], scale_premul_u8(src[o], 255u));
 }
 
+// One block row per scene of a batched pass: its image region to its clear colour.
+__global__ void k_fill_scenes(uint32_t* image, const BatchScene* __restrict__ scenes) {
+    const BatchScene sc = scenes[blockIdx.y];
+    const uint64_t n = uint64_t(sc.width) * sc.height;
+    uint32_t* dst = image + sc.image_offset;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        dst[i] = sc.clear;
+}
+
+// Adds each batch scene's path base to the path ids of its lines; scene k owns
+// lines [line_base[k], line_base[k + 1]).
+__global__ void k_rebase_lines(tk_line* lines, uint64_t n, const uint64_t* __restrict__ line_base,
+                               const uint32_t* __restrict__ path_base, uint32_t scenes) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t lo = 0, hi = scenes;  // last scene with line_base <= i
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (line_base[mid] <= i) lo = mid;
+            else hi = mid;
+        }
+        lines[i].path_id += path_base[lo];
+    }
+}
+
 }  // namespace
+
+void launch_rebase_lines(tk_line* lines, uint64_t n, const uint64_t* line_base, const uint32_t* path_base,
+                         uint32_t scenes, cudaStream_t st) {
+    if (n == 0 || scenes == 0) return;
+    k_rebase_lines<<<148 * 8, 256, 0, st>>>(lines, n, line_base, path_base, scenes);
+}
 
 void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st) {
     if (n == 0) return;
     uint64_t g = (n + 255) / 256;
     k_fill<<<unsigned(g > 148 * 16 ? 148 * 16 : g), 256, 0, st>>>(image, n, value);
+}
+
+void launch_fill_scenes(uint32_t* image, const BatchScene* scenes, uint32_t scene_count, cudaStream_t st) {
+    if (scene_count == 0) return;
+    k_fill_scenes<<<dim3(8, scene_count), 256, 0, st>>>(image, scenes);
 }
 
 void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaStream_t st) {

@@ -38,16 +38,29 @@ __device__ __forceinline__ uint32_t tile_max_(int32_t px, uint32_t lim) {
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
     k_bins(const tk_draw_record* __restrict__ draws, const uint32_t* __restrict__ order, uint32_t order0,
-           uint32_t draw_n, uint32_t tw, uint32_t th, uint32_t nbx, uint32_t* bin_lists, uint32_t* bin_counts) {
+           uint32_t draw_n, uint32_t tw, uint32_t th, uint32_t nbx, uint32_t* bin_lists, uint32_t* bin_counts,
+           const BatchScene* __restrict__ scenes, const uint32_t* __restrict__ bin_scene) {
     __shared__ uint32_t s_warp[8];
     __shared__ uint32_t s_base;
     const uint32_t bin = blockIdx.x;
-    const uint32_t bx0 = (bin % nbx) * kBinSide, by0 = (bin / nbx) * kBinSide;
+    uint32_t lbin = bin;
+    uint64_t list = uint64_t(bin) * draw_n;
+    if (scenes) {  // batched pass: this bin's canvas
+        const BatchScene& sc = scenes[bin_scene[bin]];
+        lbin = bin - sc.bin_base;
+        tw = sc.tw;
+        th = sc.th;
+        nbx = sc.nbx;
+        order0 = sc.order0;
+        draw_n = sc.draw_n;
+        list = sc.list_base + uint64_t(lbin) * sc.draw_n;
+    }
+    const uint32_t bx0 = (lbin % nbx) * kBinSide, by0 = (lbin / nbx) * kBinSide;
     const uint32_t bx1 = min(bx0 + kBinSide, tw), by1 = min(by0 + kBinSide, th);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_base = 0u;
     __syncthreads();
-    uint32_t* out = bin_lists + uint64_t(bin) * draw_n;
+    uint32_t* out = bin_lists + list;
     for (uint32_t c = 0; c < draw_n; c += 256u) {
         uint32_t j = c + threadIdx.x;
         bool hit = false;
@@ -200,14 +213,27 @@ __global__ void __launch_bounds__(kCoarseThreads)
     k_coarse(Ctx c, const uint32_t* __restrict__ bin_lists, const uint32_t* __restrict__ bin_counts, uint32_t draw_n,
              uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
              uint32_t batch0, tk_tile_record* tiles, tk_ptcl_record* ptcl, uint64_t cap,
-             unsigned long long* stats, uint32_t* error) {
+             unsigned long long* stats, uint32_t* error, const BatchScene* __restrict__ scenes,
+             const uint32_t* __restrict__ bin_scene) {
     __shared__ DrawInfo s_d[kCoarseThreads];
     const uint32_t bin = blockIdx.x;
-    const uint32_t tx = (bin % nbx) * kBinSide + (threadIdx.x % kBinSide);
-    const uint32_t ty = (bin / nbx) * kBinSide + (threadIdx.x / kBinSide);
+    uint32_t lbin = bin, tile_base = 0u;
+    uint64_t list_at = uint64_t(bin) * draw_n;
+    if (scenes) {  // batched pass: this bin's canvas
+        const BatchScene& sc = scenes[bin_scene[bin]];
+        lbin = bin - sc.bin_base;
+        c.tw = sc.tw;
+        c.th = sc.th;
+        nbx = sc.nbx;
+        draw_n = sc.draw_n;
+        tile_base = sc.tile_base;
+        list_at = sc.list_base + uint64_t(lbin) * sc.draw_n;
+    }
+    const uint32_t tx = (lbin % nbx) * kBinSide + (threadIdx.x % kBinSide);
+    const uint32_t ty = (lbin / nbx) * kBinSide + (threadIdx.x / kBinSide);
     const bool live = tx < c.tw && ty < c.th;
-    const uint32_t tile = ty * c.tw + tx;
-    const uint32_t* list = bin_lists + uint64_t(bin) * draw_n;
+    const uint32_t tile = tile_base + ty * c.tw + tx;
+    const uint32_t* list = bin_lists + list_at;
     const uint32_t n = bin_counts[bin];
 
     uint64_t at = 0;
@@ -406,29 +432,32 @@ __global__ void __launch_bounds__(kTileScanThreads)
 }  // namespace
 
 void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st) {
-    uint32_t nbins = p.nbx * p.nby;
-    if (p.draw_n == 0) {
+    const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
+    if (nbins == 0) return;
+    if (!p.scenes && p.draw_n == 0) {
         cudaMemsetAsync(p.bin_counts, 0, sizeof(uint32_t) * nbins, st);
         return;
     }
-    k_bins<<<nbins, 256, 0, st>>>(s.draws, s.order, p.order0, p.draw_n, s.tw, s.th, p.nbx, p.bin_lists, p.bin_counts);
+    k_bins<<<nbins, 256, 0, st>>>(s.draws, s.order, p.order0, p.draw_n, s.tw, s.th, p.nbx, p.bin_lists, p.bin_counts,
+                                  p.scenes, p.bin_scene);
 }
 
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st) {
     Ctx c{s.draws, s.paths, s.path_count, s.layers, s.brush, s.brush_words, s.backdrops, s.ranges, s.tw, s.th};
-    uint32_t nbins = p.nbx * p.nby;
+    const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
+    if (nbins == 0) return;
     if (emit)
         k_coarse<true><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                          p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                         p.stats, s.error);
+                                                         p.stats, s.error, p.scenes, p.bin_scene);
     else
         k_coarse<false><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                           p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                          p.stats, s.error);
+                                                          p.stats, s.error, p.scenes, p.bin_scene);
 }
 
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {
-    uint32_t T = s.tw * s.th;
+    uint32_t T = p.scenes ? p.total_tiles : s.tw * s.th;
     uint32_t blocks = (T + kTileBlock - 1) / kTileBlock;
     cudaMemsetAsync(p.tile_desc, 0, sizeof(unsigned long long) * blocks, st);
     cudaMemsetAsync(p.ticket, 0, sizeof(uint32_t), st);

@@ -264,15 +264,25 @@ __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const tk_line_segment* __restrict__ segments, const tk_draw_record* __restrict__ draws,
            const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
-           uint32_t width, uint32_t height, uint32_t tw, uint32_t* error) {
+           uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
+           const uint32_t* __restrict__ tile_scene) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FineSmem& S = *reinterpret_cast<FineSmem*>(smem_raw);
     const uint32_t tile = blockIdx.x;
     const tk_tile_record rec = tiles[tile];
     if (rec.ptcl_start >= rec.ptcl_end) return;
+    uint32_t ltile = tile;
+    if (scenes) {  // batched pass: this tile's canvas and image
+        const BatchScene& sc = scenes[tile_scene[tile]];
+        ltile = tile - sc.tile_base;
+        tw = sc.tw;
+        width = sc.width;
+        height = sc.height;
+        target += sc.image_offset;
+    }
     const uint32_t tid = threadIdx.x;
     const uint32_t lx = tid & 15u, ly = tid >> 4;
-    const uint32_t gx = (tile % tw) * TK_TILE_SIZE + lx, gy = (tile / tw) * TK_TILE_SIZE + ly;
+    const uint32_t gx = (ltile % tw) * TK_TILE_SIZE + lx, gy = (ltile / tw) * TK_TILE_SIZE + ly;
     const bool inside = gx < width && gy < height;
     const uint64_t pix = uint64_t(gy) * width + gx;
     const Paint P{brush, brush_words};
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
 }  // namespace
 
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st) {
-    const uint32_t T = s.tw * s.th;
+    const uint32_t T = p.scenes ? p.total_tiles : s.tw * s.th;
     if (T == 0) return;
     static bool configured = false;
     if (!configured) {
@@ -576,7 +586,8 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
         configured = true;
     }
     k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.draws, s.brush, s.brush_words,
-                                                      s.segment_capacity, target, s.width, s.height, s.tw, s.error);
+                                                      s.segment_capacity, target, s.width, s.height, s.tw, s.error,
+                                                      p.scenes, p.tile_scene);
 }
 
 }  // namespace tk

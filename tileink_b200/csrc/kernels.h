@@ -74,6 +74,18 @@ struct NoAllocScratch {
 cudaError_t noalloc_scratch(int device, NoAllocScratch* out);
 void launch_build_scan_items(const tk_path_record* paths, uint32_t path_count, ScanItem* items, cudaStream_t st);
 
+// One canvas of a batched pass: several independent scenes go through each
+// stage in one launch; their tiles, bins and images are concatenated.
+struct BatchScene {
+    uint32_t tile_base, bin_base;  // first global tile / bin of the scene
+    uint64_t list_base;            // first word of the scene's bin lists
+    uint32_t tw, th, nbx;          // tile grid and bins per row
+    uint32_t order0, draw_n;       // draw_order[order0 .. order0 + draw_n)
+    uint32_t width, height;
+    uint32_t clear;                // premultiplied RGBA8 clear colour
+    uint64_t image_offset;         // first pixel of the scene's image
+};
+
 // Target pass: binning, coarse count, tile prefix, coarse emit, fine.
 struct PassView {
     uint32_t order0, draw_n;          // draw_order[order0 .. order0 + draw_n)
@@ -90,6 +102,12 @@ struct PassView {
     uint32_t* ticket;
     uint32_t* ptcl_total;
     unsigned long long* stats;        // [0] fill records, [1] segment visits
+    // batched pass (null for one canvas): per-scene geometry and the scene
+    // of every global bin and tile
+    const BatchScene* scenes;
+    const uint32_t* bin_scene;
+    const uint32_t* tile_scene;
+    uint32_t total_bins, total_tiles, scene_count;
 };
 void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
@@ -98,6 +116,12 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
 
 // Images.
 void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);
+// Batch upload: lines of scene k occupy [line_base[k], line_base[k + 1]) and
+// get path_base[k] added to their path ids.
+void launch_rebase_lines(tk_line* lines, uint64_t n, const uint64_t* line_base, const uint32_t* path_base,
+                         uint32_t scenes, cudaStream_t st);
+// Clears every scene's image region of a batched pass to its clear colour.
+void launch_fill_scenes(uint32_t* image, const BatchScene* scenes, uint32_t scene_count, cudaStream_t st);
 struct BlurParams {
     uint32_t width, height;
     uint32_t region[4];   // x0, y0, width, height

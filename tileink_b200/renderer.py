@@ -120,6 +120,37 @@ class NativeRenderer:
         self._check(self._lib.tk_pool_scan_noalloc(self._h, N.ptr(paths), len(paths), d_counts, d_backdrops,
                                                    d_ranges, d_cursors, int(pool_len), d_bumps))
 
+    # --- batched mode -----------------------------------------------------------
+    def batch_upload(self, canvases) -> None:
+        """Uploads independent one-pass scenes as one batch."""
+        descs = [c.scene_desc() if hasattr(c, "scene_desc") else c for c in canvases]
+        arr = (N.SceneDesc * len(descs))(*descs)
+        self._batch_keep = (canvases, descs, arr)
+        self._check(self._lib.tk_batch_upload(self._h, C.cast(arr, C.c_void_p), len(descs)))
+        self._batch_info = [self.batch_info(i) for i in range(len(descs))]
+
+    def batch_render(self) -> None:
+        self._check(self._lib.tk_batch_render(self._h))
+
+    def batch_info(self, scene: int) -> N.BatchInfo:
+        out = N.BatchInfo()
+        self._check(self._lib.tk_batch_info_get(self._h, int(scene), C.byref(out)))
+        return out
+
+    def batch_readback(self):
+        """Every scene's premultiplied RGBA8 image, (H, W, 4) uint8 each."""
+        infos = self._batch_info
+        total = sum(i.width * i.height for i in infos)
+        buf = np.zeros(total, dtype=np.uint32)
+        self._check(self._lib.tk_batch_readback(self._h, N.ptr(buf), total))
+        return [buf[i.image_offset:i.image_offset + i.width * i.height].view(np.uint8).reshape(i.height, i.width, 4)
+                for i in infos]
+
+    def autotune(self, iterations: int = 3) -> N.TuneResult:
+        out = N.TuneResult()
+        self._check(self._lib.tk_autotune(self._h, int(iterations), C.byref(out)))
+        return out
+
     # --- differentiable rendering ---------------------------------------------
     def diff_forward(self, scene, target, return_image=False):
         """Loss (and optionally the [H, W, 4] f32 image) of a DiffScene against
