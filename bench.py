@@ -110,6 +110,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest `value` over all ranks; every rank calls it at the same
+    point (NCCL on the GPUs, gloo in the CPU tests)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -322,10 +334,7 @@ def main():
     barrier()
     ms = e0.elapsed_time(e1) / args.steps
     r.set_timing(False)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, world)
     value = world * 1000.0 / ms
 
     # end to end: pinned host scene -> H2D -> frame -> D2H image, every step
@@ -347,11 +356,7 @@ def main():
     s1.synchronize()
     e2e_ms = s0.elapsed_time(s1) / args.e2e_steps
     wall_ms = (time.perf_counter() - t0) * 1000.0 / args.e2e_steps
-    e2e_ms = max(e2e_ms, wall_ms)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(max(e2e_ms, wall_ms), world)
     bytes_out = out.nbytes
 
     # roofline of the dominant kernel
