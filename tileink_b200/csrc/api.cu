@@ -122,6 +122,8 @@ struct tk_ctx {
     DBuf<uint32_t> image, temp;
     std::vector<DBuf<uint32_t>> surfaces;
     bool rendered = false;
+    // paths by decreasing line count: the order scan_emit's warps take them
+    DBuf<uint32_t> emit_order;
     // line index per emitted segment (differentiable mode only)
     DBuf<uint32_t> seg_line;
     bool want_seg_line = false;
@@ -338,6 +340,8 @@ tk::SceneView view(tk_ctx* c) {
     s.segment_capacity = c->segments.cap;
     s.error = c->misc.ptr;
     s.seg_line = c->want_seg_line ? c->seg_line.ptr : nullptr;
+    s.emit_order = c->emit_order.ptr;
+    s.emit_ticket = c->misc.ptr + 4;
     return s;
 }
 
@@ -377,6 +381,16 @@ uint32_t read_word(tk_ctx* c, const uint32_t* dptr) {
     return v;
 }
 
+// Paths by decreasing line count (stable), for scan_emit's path queue.
+void upload_emit_order(tk_ctx* c) {
+    std::vector<uint32_t> order(c->h_paths.size());
+    for (uint32_t i = 0; i < uint32_t(order.size()); ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        return c->h_paths[a].line_count > c->h_paths[b].line_count;
+    });
+    upload(c->emit_order, order.data(), order.size(), c->stream);
+}
+
 void do_upload(tk_ctx* c, const tk_scene_desc& d) {
     // A failed upload leaves no renderable scene behind.
     c->have_scene = false;
@@ -396,6 +410,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d) {
     upload(c->batch_ids, d.draw_batch_ids, d.draw_count, st);
     upload(c->order, d.draw_order, d.draw_order_count, st);
     upload(c->items, c->h_items.data(), c->h_items.size(), st);
+    upload_emit_order(c);
     c->item_desc.reserve(c->h_items.size());
     c->backdrops.reserve(c->pool_len);
     c->counts.reserve(c->pool_len);
@@ -775,6 +790,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     upload(c->batch_ids, batch_ids.data(), batch_ids.size(), st);
     upload(c->order, order.data(), order.size(), st);
     rebuild_items(c);
+    upload_emit_order(c);
     c->backdrops.reserve(pool);
     c->counts.reserve(pool);
     c->cursors.reserve(pool);
@@ -883,6 +899,7 @@ void tk_ctx_destroy(tk_ctx* c) {
         p.d_batches.release(); p.bin_lists.release(); p.bin_counts.release(); p.tiles.release(); p.ptcl.release();
     }
     c->seg_line.release();
+    c->emit_order.release();
     drop_graph(c);
     c->d_scenes.release(); c->bin_scene.release(); c->tile_scene.release();
     DiffState& D = c->diff;

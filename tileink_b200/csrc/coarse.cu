@@ -23,7 +23,12 @@ namespace {
 using namespace tkd;
 
 constexpr int kBinSide = 16;
-constexpr int kCoarseThreads = kBinSide * kBinSide;
+// Coarse runs one CTA per 8x8-tile quadrant of a bin (four per bin), so that a
+// 4096^2 canvas gives 1024 CTAs instead of 256; each quadrant walks its bin's
+// candidate list.
+constexpr int kQuadSide = 8;
+constexpr int kQuads = (kBinSide / kQuadSide) * (kBinSide / kQuadSide);
+constexpr int kCoarseThreads = kQuadSide * kQuadSide;
 constexpr uint32_t kChunkClassColor = 1u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
 
 __device__ __forceinline__ uint32_t tile_min_(int32_t px, uint32_t lim) {
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
              unsigned long long* stats, uint32_t* error, const BatchScene* __restrict__ scenes,
              const uint32_t* __restrict__ bin_scene) {
     __shared__ DrawInfo s_d[kCoarseThreads];
-    const uint32_t bin = blockIdx.x;
+    const uint32_t bin = blockIdx.x / kQuads, quad = blockIdx.x % kQuads;
     uint32_t lbin = bin, tile_base = 0u;
     uint64_t list_at = uint64_t(bin) * draw_n;
     if (scenes) {  // batched pass: this bin's canvas
@@ -229,8 +234,9 @@ __global__ void __launch_bounds__(kCoarseThreads)
         tile_base = sc.tile_base;
         list_at = sc.list_base + uint64_t(lbin) * sc.draw_n;
     }
-    const uint32_t tx = (lbin % nbx) * kBinSide + (threadIdx.x % kBinSide);
-    const uint32_t ty = (lbin / nbx) * kBinSide + (threadIdx.x / kBinSide);
+    const uint32_t qx = quad % (kBinSide / kQuadSide), qy = quad / (kBinSide / kQuadSide);
+    const uint32_t tx = (lbin % nbx) * kBinSide + qx * kQuadSide + (threadIdx.x % kQuadSide);
+    const uint32_t ty = (lbin / nbx) * kBinSide + qy * kQuadSide + (threadIdx.x / kQuadSide);
     const bool live = tx < c.tw && ty < c.th;
     const uint32_t tile = tile_base + ty * c.tw + tx;
     const uint32_t* list = bin_lists + list_at;
@@ -447,11 +453,11 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
     const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
     if (nbins == 0) return;
     if (emit)
-        k_coarse<true><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
+        k_coarse<true><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                          p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
                                                          p.stats, s.error, p.scenes, p.bin_scene);
     else
-        k_coarse<false><<<nbins, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
+        k_coarse<false><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                           p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
                                                           p.stats, s.error, p.scenes, p.bin_scene);
 }

@@ -50,6 +50,8 @@ struct SceneView {
     uint64_t segment_capacity;
     uint32_t* error;
     uint32_t* seg_line;  // optional: line index of every emitted segment
+    const uint32_t* emit_order;  // paths by decreasing line count (optional)
+    uint32_t* emit_ticket;       // path queue of scan_emit
 };
 
 void launch_scan_count(const SceneView& s, cudaStream_t st);

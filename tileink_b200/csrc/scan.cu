@@ -170,38 +170,48 @@ __global__ void __launch_bounds__(kScanThreads)
     block_seg_exclusive(bf, bsum, bef, bexcl, s_f, s_v, btot);
     (void)btot;
     (void)ef;
-    // look-back for the item prefix
-    if (tid == 0) {
-        bool chain_head = device_plan ? (k == 0u) : (it.first != 0u);
-        uint32_t prefix;
+    // look-back for the item prefix: warp 0 reads 32 predecessors per step and
+    // adds the aggregates down to the nearest inclusive prefix (wrapping u32)
+    if (tid < 32) {
+        const uint32_t lane = tid;
+        const bool chain_head = device_plan ? (k == 0u) : (it.first != 0u);
+        uint32_t prefix = 0u;
         if (chain_head) {
             prefix = device_plan ? device_base : p.segment_start;
-            atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
+            if (lane == 0) atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
         } else {
-            atomicExch(desc + k, kStatusAgg | (unsigned long long)agg);
-            prefix = 0u;
-            uint32_t j = k - 1u;
+            if (lane == 0) atomicExch(desc + k, kStatusAgg | (unsigned long long)agg);
+            int64_t j = int64_t(k) - 1;
             uint32_t spins = 0;
             for (;;) {
-                unsigned long long d = *((volatile unsigned long long*)(desc + j));
-                unsigned long long st = d & (3ull << 62);
-                if (st == 0ull) {
+                const int64_t idx = j - int64_t(lane);
+                unsigned long long d = kStatusIncl;  // before item 0: an empty inclusive prefix
+                if (idx >= 0) d = *((volatile unsigned long long*)(desc + idx));
+                const unsigned long long st = d & (3ull << 62);
+                const uint32_t incl = __ballot_sync(0xffffffffu, st == kStatusIncl);
+                const uint32_t zero = __ballot_sync(0xffffffffu, st == 0ull);
+                // lanes 0 .. nearest inclusive lane (all 32 without one)
+                const uint32_t first = incl ? uint32_t(__ffs(incl) - 1) : 31u;
+                const uint32_t need = first == 31u ? 0xffffffffu : ((2u << first) - 1u);
+                if (zero & need) {  // a predecessor has not published yet
                     if (++spins > kSpinLimit) {
-                        atomicOr(error, ERR_LOOKBACK_TIMEOUT);
+                        if (lane == 0) atomicOr(error, ERR_LOOKBACK_TIMEOUT);
                         break;
                     }
                     __nanosleep(64);
                     continue;
                 }
-                prefix += uint32_t(d);
-                if (st == kStatusIncl) break;
-                --j;
+                prefix += __reduce_add_sync(0xffffffffu, ((need >> lane) & 1u) ? uint32_t(d) : 0u);
+                if (incl) break;
+                j -= 32;
             }
             __threadfence();
-            atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
+            if (lane == 0) atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
         }
-        if (k + 1u == n_items) *total = prefix + agg;
-        s_prefix = prefix;
+        if (lane == 0) {
+            if (k + 1u == n_items) *total = prefix + agg;
+            s_prefix = prefix;
+        }
     }
     __syncthreads();
     const uint32_t prefix = s_prefix;
@@ -251,11 +261,18 @@ __global__ void k_path_totals(tk_path_record* paths, uint32_t path_count, const 
 
 __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
                             uint32_t path_count, uint32_t* cursors, tk_line_segment* segments, uint64_t capacity,
-                            uint32_t* error, uint32_t* seg_line) {
+                            uint32_t* error, uint32_t* seg_line, const uint32_t* __restrict__ order,
+                            uint32_t* ticket) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t pid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pid < path_count; pid += warps) {
+    // Warps take paths from a queue, longest first: the line counts are
+    // heavy-tailed and a path is one warp's sequential work.
+    for (;;) {
+        uint32_t k = 0;
+        if (lane == 0) k = atomicAdd(ticket, 1u);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= path_count) break;
+        const uint32_t pid = order ? __ldg(order + k) : k;
         const tk_path_record p = load_path(paths, pid);
         for (uint32_t g = 0; g < p.line_count; g += 32u) {
             uint32_t l = g + lane;
@@ -344,9 +361,10 @@ void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, c
 void launch_scan_emit(const SceneView& s, cudaStream_t st) {
     if (s.path_count == 0) return;
     uint64_t threads = uint64_t(s.path_count) * 32;
-    k_scan_emit<<<grid_for(threads, 256, 148 * 32), 256, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
-                                                                 s.segments, s.segment_capacity, s.error,
-                                                                 s.seg_line);
+    cudaMemsetAsync(s.emit_ticket, 0, sizeof(uint32_t), st);
+    k_scan_emit<<<grid_for(threads, 256, 148 * 8), 256, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
+                                                                s.segments, s.segment_capacity, s.error, s.seg_line,
+                                                                s.emit_order, s.emit_ticket);
 }
 
 }  // namespace tk
