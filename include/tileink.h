@@ -303,6 +303,7 @@ int32_t tk_get_stats(tk_ctx* ctx, tk_stats* out);
 #define TK_STAGE_KINDS 6u      /* u32[T] tile kind words of pass `index` */
 #define TK_STAGE_IMAGE 7u      /* u32[W*H] current target image */
 #define TK_STAGE_PATHS 8u      /* tk_path_record[P] (segment plan applied) */
+#define TK_STAGE_LINES 9u      /* tk_line[L] (device-flattened lines included) */
 int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
                           void* dst, size_t bytes, size_t* needed);
 
@@ -347,6 +348,39 @@ int32_t tk_stage_scan_count(tk_ctx* ctx, const tk_line* lines, uint64_t line_cou
 int32_t tk_stage_blur(tk_ctx* ctx, const uint32_t* src, uint32_t* dst,
                       uint32_t width, uint32_t height, const uint32_t region[4],
                       const uint32_t source[4], float sigma, uint32_t axis);
+
+/* ------------------------------------------------------------------------ */
+/* Device flattening: fill paths arrive as Bezier elements and are flattened */
+/* on the GPU at upload (the flattening step of Canvas::push_path,           */
+/* src/shared/path_flatten.rs:20-82). The lines are bit-identical to the     */
+/* host Canvas's: both run the same double-precision flattener.              */
+/* ------------------------------------------------------------------------ */
+
+#define TK_EL_LINE 1u
+#define TK_EL_QUAD 2u
+#define TK_EL_CUBIC 3u
+
+/* One element of a fill path with its start point: p[0] = start, then the
+ * end point (line), control + end point (quadratic) or two controls + end
+ * point (cubic). move_to / close are already resolved into line elements. */
+typedef struct tk_flatten_el {
+    uint32_t verb;
+    uint32_t path;        /* path index: the lines' path_id */
+    double tolerance;     /* flattening tolerance in device pixels */
+    double p[4][2];
+} tk_flatten_el; /* 80 B */
+
+typedef struct tk_flatten_desc {
+    const tk_flatten_el* elements;
+    uint64_t element_count;
+    const uint32_t* path_elements; /* [path_count][first, count]; count 0: the
+                                      path's lines are in tk_scene_desc.lines */
+} tk_flatten_desc;
+
+/* tk_scene_upload for a scene whose paths with elements are flattened on the
+ * device. tk_scene_desc.lines holds the other paths' lines; the device lines
+ * follow them. Requires TK_SCENE_SEGMENTS_FROM_DEVICE. */
+int32_t tk_scene_upload_flatten(tk_ctx* ctx, const tk_scene_desc* scene, const tk_flatten_desc* flatten);
 
 /* ------------------------------------------------------------------------ */
 /* Batched mode: many independent scenes of uneven size rendered together.   */

@@ -65,6 +65,13 @@ void tk_canvas_free(tk_canvas* c);
  * scan-line planner at record time (canvas/storage.rs:131-142); otherwise the
  * scene asks the device to plan them (TK_SCENE_SEGMENTS_FROM_DEVICE). */
 void tk_canvas_set_host_segment_plan(tk_canvas* c, int32_t enabled);
+/* Fill paths recorded after this keep their Bezier elements for
+ * tk_scene_upload_flatten instead of being flattened on the host; stroke
+ * outlines stay host lines. Turns host segment planning off. */
+void tk_canvas_set_device_flatten(tk_canvas* c, int32_t enabled);
+/* The recorded elements and per-path element ranges (valid until the canvas
+ * changes). */
+int32_t tk_canvas_flatten_desc(const tk_canvas* c, tk_flatten_desc* out);
 void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul_rgba8);
 
 /* transform: 6 coefficients [a b c d e f] or NULL for identity. Returns the
@@ -93,7 +100,7 @@ typedef struct tk_gen_params {
     uint32_t variant;         /* config 4: scene index */
     float sigma;              /* config 5: blur sigma */
     float jitter;             /* config 5: control point jitter (px) */
-    uint32_t flags;           /* 1: host segment planning off */
+    uint32_t flags;           /* 1: host segment planning off; 2: device flattening of fills */
     uint32_t reserved;
 } tk_gen_params;
 tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_params* overrides);

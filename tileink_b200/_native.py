@@ -23,7 +23,7 @@ TK_OK, TK_E_INVALID, TK_E_CAPACITY, TK_E_CUDA, TK_E_TIMEOUT, TK_E_STATE, TK_E_AL
 
 # Debug stages
 STAGE_COUNTS, STAGE_BACKDROPS, STAGE_RANGES, STAGE_SEGMENTS = 0, 1, 2, 3
-STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS = 4, 5, 6, 7, 8
+STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4, 5, 6, 7, 8, 9
 
 # PTCL tags (shaders/hlsl/shared/particle_tags.hlsli) + merged-stream marker
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
@@ -91,6 +91,11 @@ class BrushDesc(C.Structure):
                 ("stops", C.POINTER(GradientStop))]
 
 
+class FlattenDesc(C.Structure):
+    """tk_flatten_desc (include/tileink.h)."""
+    _fields_ = [("elements", C.c_void_p), ("element_count", C.c_uint64), ("path_elements", C.c_void_p)]
+
+
 class DiffScene(C.Structure):
     """tk_diff_scene (include/tileink_diff.h)."""
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("path_count", C.c_uint32),
@@ -138,6 +143,9 @@ def library() -> C.CDLL:
         "tk_ctx_stream": (P, [P]),
         "tk_synchronize": (I32, [P]),
         "tk_scene_upload": (I32, [P, C.POINTER(SceneDesc)]),
+        "tk_scene_upload_flatten": (I32, [P, C.POINTER(SceneDesc), C.POINTER(FlattenDesc)]),
+        "tk_canvas_set_device_flatten": (None, [P, I32]),
+        "tk_canvas_flatten_desc": (I32, [P, C.POINTER(FlattenDesc)]),
         "tk_render": (I32, [P]),
         "tk_readback": (I32, [P, P, C.c_size_t]),
         "tk_render_to_image": (I32, [P, C.POINTER(SceneDesc), P, C.c_size_t]),

@@ -132,6 +132,16 @@ class Canvas:
     def set_host_segment_plan(self, enabled: bool):
         self._lib.tk_canvas_set_host_segment_plan(self._h, 1 if enabled else 0)
 
+    def set_device_flatten(self, enabled: bool):
+        """Fills recorded from now on are flattened on the GPU at upload."""
+        self._lib.tk_canvas_set_device_flatten(self._h, 1 if enabled else 0)
+
+    def flatten_desc(self) -> N.FlattenDesc | None:
+        """The elements to flatten on the device, or None when there are none."""
+        f = N.FlattenDesc()
+        self._lib.tk_canvas_flatten_desc(self._h, C.byref(f))
+        return f if f.element_count else None
+
     def push_path(self, path: BezPath, brush: Brush, transform=None, fill_rule=FILL_NONZERO,
                   tolerance: float = 0.1) -> int:
         d, keep = brush._desc()
@@ -185,11 +195,14 @@ class Canvas:
 
 
 def generate(config: int, seed: int, *, width=0, height=0, paths=0, variant=0, sigma=0.0, jitter=0.0,
-             device_segment_plan=False) -> Canvas:
+             device_segment_plan=False, device_flatten=False) -> Canvas:
     """Seeded synthetic workload (1: 640x360 cubic fills, 2: 4096^2 50k mixed,
-    3: 1920x1080 glyphs, 4: one uneven batch scene, 5: 1024^2 blur group)."""
+    3: 1920x1080 glyphs, 4: one uneven batch scene, 5: 1024^2 blur group).
+    device_flatten keeps the fills as Bezier elements for GPU flattening
+    (and implies device segment planning)."""
     lib = N.library()
-    p = N.GenParams(width, height, paths, variant, sigma, jitter, 1 if device_segment_plan else 0, 0)
+    flags = (1 if device_segment_plan else 0) | (2 if device_flatten else 0)
+    p = N.GenParams(width, height, paths, variant, sigma, jitter, flags, 0)
     h = lib.tk_generate(int(config), int(seed), C.byref(p))
     if not h:
         raise ValueError(f"unknown workload {config}")

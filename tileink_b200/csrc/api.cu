@@ -391,7 +391,9 @@ void upload_emit_order(tk_ctx* c) {
     upload(c->emit_order, order.data(), order.size(), c->stream);
 }
 
-void do_upload(tk_ctx* c, const tk_scene_desc& d) {
+void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl);
+
+void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nullptr) {
     // A failed upload leaves no renderable scene behind.
     c->have_scene = false;
     c->rendered = false;
@@ -402,8 +404,9 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d) {
     c->graph_exec = nullptr;
     validate_and_plan(c, d);
     cudaStream_t st = c->stream;
-    upload(c->lines, d.lines, d.line_count, st);
     upload(c->paths, d.paths, d.path_count, st);
+    if (fl) flatten_on_device(c, d, *fl);  // the host lines, then the device lines
+    else upload(c->lines, d.lines, d.line_count, st);
     upload(c->draws, d.draws, d.draw_count, st);
     upload(c->brush, d.brush_blob, d.brush_word_count, st);
     upload(c->layers, d.layers, d.layer_count, st);
@@ -632,6 +635,65 @@ void rebuild_items(tk_ctx* c) {
     }
     upload(c->items, c->h_items.data(), c->h_items.size(), c->stream);
     c->item_desc.reserve(c->h_items.size());
+}
+
+// Lines of the element paths flattened on the device after the host lines;
+// their path records get their line ranges on the device.
+void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl) {
+    if (!(d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE)) invalid("device flattening needs device segment planning");
+    if ((fl.element_count && !fl.elements) || (d.path_count && !fl.path_elements)) invalid("null flatten arrays");
+    for (uint32_t p = 0; p < d.path_count; ++p) {
+        const uint64_t e0 = fl.path_elements[2 * p], ne = fl.path_elements[2 * p + 1];
+        if (!ne) continue;
+        if (e0 + ne > fl.element_count) invalid("path " + std::to_string(p) + ": elements out of range");
+        if (d.paths[p].line_count) invalid("path " + std::to_string(p) + ": both lines and elements");
+        for (uint64_t e = e0; e < e0 + ne; ++e) {
+            const tk_flatten_el& el = fl.elements[e];
+            if (el.path != p) invalid("element " + std::to_string(e) + ": path index mismatch");
+            if (el.verb < TK_EL_LINE || el.verb > TK_EL_CUBIC) invalid("element " + std::to_string(e) + ": bad verb");
+            // Bounded inputs bound one thread's subdivision work (about 1e6
+            // points for the worst element).
+            if (!(el.tolerance >= 1e-3) || !std::isfinite(el.tolerance))
+                invalid("flattening tolerance below 1e-3 px or not finite");
+            for (int k = 0; k <= int(el.verb); ++k)
+                for (int a = 0; a < 2; ++a)
+                    if (!(std::fabs(el.p[k][a]) <= 1e6))
+                        invalid("element " + std::to_string(e) + ": coordinates beyond 1e6 px or not finite");
+        }
+    }
+    cudaStream_t st = c->stream;
+    const uint64_t n = fl.element_count;
+    DBuf<tk_flatten_el> els;
+    DBuf<uint32_t> path_els, offsets, sums, words;
+    upload(els, fl.elements, n, st);
+    upload(path_els, fl.path_elements, 2ull * d.path_count, st);
+    offsets.reserve(n);
+    sums.reserve(tk::flatten_block_sums(n));
+    words.reserve(2);
+    TK_CUDA(cudaMemsetAsync(words.ptr, 0, 2 * sizeof(uint32_t), st));
+    tk::launch_flatten_count(els.ptr, n, offsets.ptr, sums.ptr, words.ptr, st);
+    uint32_t dev_lines = 0;
+    TK_CUDA(cudaMemcpyAsync(&dev_lines, words.ptr, 4, cudaMemcpyDeviceToHost, st));
+    TK_CUDA(cudaStreamSynchronize(st));
+    const uint64_t host_lines = d.line_count, total = host_lines + dev_lines;
+    if (total > 0xFFFFFFFFull) invalid("line count exceeds u32 indexing");
+    c->lines.reserve(total);
+    if (host_lines) TK_CUDA(cudaMemcpyAsync(c->lines.ptr, d.lines, host_lines * sizeof(tk_line), cudaMemcpyHostToDevice, st));
+    tk::launch_flatten_emit(els.ptr, n, offsets.ptr, words.ptr, c->paths.ptr, d.path_count, path_els.ptr, c->lines.ptr,
+                            host_lines, total, words.ptr + 1, st);
+    TK_CUDA(cudaGetLastError());
+    uint32_t err = 0;
+    TK_CUDA(cudaMemcpyAsync(&err, words.ptr + 1, 4, cudaMemcpyDeviceToHost, st));
+    TK_CUDA(cudaMemcpyAsync(c->h_paths.data(), c->paths.ptr, d.path_count * sizeof(tk_path_record),
+                            cudaMemcpyDeviceToHost, st));
+    TK_CUDA(cudaStreamSynchronize(st));
+    els.release();
+    path_els.release();
+    offsets.release();
+    sums.release();
+    words.release();
+    if (err) throw Fail{TK_E_INVALID, "device flattening wrote past its line count"};
+    c->line_count = total;
 }
 
 // Merges one-pass scenes into one batched pass: arrays concatenated with their
@@ -993,6 +1055,7 @@ int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, 
             }
             case TK_STAGE_IMAGE: src = c->image.ptr; n = size_t(c->width) * c->height * 4; break;
             case TK_STAGE_PATHS: src = c->paths.ptr; n = size_t(c->path_count) * sizeof(tk_path_record); break;
+            case TK_STAGE_LINES: src = c->lines.ptr; n = size_t(c->line_count) * sizeof(tk_line); break;
             case TK_STAGE_PTCL:
             case TK_STAGE_TILES:
             case TK_STAGE_KINDS: {
@@ -1401,6 +1464,13 @@ int32_t tk_diff_backward(tk_ctx* c, float* d_points, float* d_colors, float* d_s
             }
         }
         if (d_sigma) *d_sigma = float(dsig);
+    });
+}
+
+int32_t tk_scene_upload_flatten(tk_ctx* c, const tk_scene_desc* d, const tk_flatten_desc* fl) {
+    return guarded(c, [&] {
+        if (!d || !fl) invalid("null scene");
+        do_upload(c, *d, fl);
     });
 }
 

@@ -15,17 +15,12 @@
 #include "../../include/tileink.h"
 #include "../../include/tileink_canvas.h"
 #include "../../include/tileink_diff.h"
+#include "flatten_core.h"
 #include "planner.h"
 
 namespace {
 
-struct Pt {
-    double x, y;
-};
-inline Pt operator+(Pt a, Pt b) { return {a.x + b.x, a.y + b.y}; }
-inline Pt operator-(Pt a, Pt b) { return {a.x - b.x, a.y - b.y}; }
-inline Pt operator*(Pt a, double s) { return {a.x * s, a.y * s}; }
-inline const Pt& val(const Pt& p) { return p; }
+using tkf::Pt;
 
 // A flattened point together with its weights over the four control points of
 // the cubic being flattened: every point the flattener emits is a fixed linear
@@ -57,87 +52,9 @@ struct tk_path {
 
 namespace {
 
-// --------------------------------------------------------------------------
-// Flattening. Quadratics use the parabola-integral subdivision of R. Levien,
-// "Flattening quadratic Beziers" (2019): map the quadratic onto y = x^2, use
-// closed-form approximations of the arc-length-like integral and its inverse
-// to place n points with equal error. Cubics are first split into m
-// quadratics with the cubic-to-quadratic error bound
-// sqrt(3)/36 * |p3 - 3p2 + 3p1 - p0| / m^3.
-// --------------------------------------------------------------------------
-inline double approx_integral(double x) {
-    const double d = 0.67;
-    return x / (1.0 - d + std::sqrt(std::sqrt(d * d * d * d + 0.25 * x * x)));
-}
-inline double approx_inv_integral(double x) {
-    const double b = 0.39;
-    return x * (1.0 - b + std::sqrt(b * b + 0.25 * x * x));
-}
-template <class P>
-inline P quad_eval(P p0, P p1, P p2, double t) {
-    double mt = 1.0 - t;
-    return p0 * (mt * mt) + p1 * (2.0 * mt * t) + p2 * (t * t);
-}
-template <class P, class Emit>
-void flatten_quad(P q0, P q1, P q2, double tol, Emit&& emit) {
-    const Pt &p0 = val(q0), &p1 = val(q1), &p2 = val(q2);
-    double ddx = 2.0 * p1.x - p0.x - p2.x, ddy = 2.0 * p1.y - p0.y - p2.y;
-    double u0 = (p1.x - p0.x) * ddx + (p1.y - p0.y) * ddy;
-    double u2 = (p2.x - p1.x) * ddx + (p2.y - p1.y) * ddy;
-    double cross = (p2.x - p0.x) * ddy - (p2.y - p0.y) * ddx;
-    double dd = std::hypot(ddx, ddy);
-    if (dd < 1e-12) {
-        emit(q2);
-        return;
-    }
-    double x0 = u0 / cross, x2 = u2 / cross;
-    double scale = std::fabs(cross) / (dd * std::fabs(x2 - x0));
-    if (!(std::isfinite(x0) && std::isfinite(x2) && std::isfinite(scale)) || std::fabs(cross) < 1e-12 * dd * dd) {
-        // Nearly collinear control points: uniform steps with the chord bound
-        // |B''| h^2 / 8 = |dd| h^2 / 4 <= tol.
-        int n = std::max(1, int(std::ceil(std::sqrt(dd / (4.0 * tol)))));
-        for (int i = 1; i < n; ++i) emit(quad_eval(q0, q1, q2, double(i) / n));
-        emit(q2);
-        return;
-    }
-    double a0 = approx_integral(x0), a2 = approx_integral(x2);
-    double count = 0.5 * std::fabs(a2 - a0) * std::sqrt(scale / tol);
-    int n = std::max(1, int(std::ceil(count)));
-    double v0 = approx_inv_integral(a0), v2 = approx_inv_integral(a2);
-    for (int i = 1; i < n; ++i) {
-        double v = approx_inv_integral(a0 + (a2 - a0) * double(i) / n);
-        double t = (v - v0) / (v2 - v0);
-        emit(quad_eval(q0, q1, q2, t));
-    }
-    emit(q2);
-}
-template <class P>
-inline P cubic_eval(const P c[4], double t) {
-    double mt = 1.0 - t;
-    return c[0] * (mt * mt * mt) + c[1] * (3.0 * mt * mt * t) + c[2] * (3.0 * mt * t * t) + c[3] * (t * t * t);
-}
-template <class P>
-inline P cubic_deriv(const P c[4], double t) {
-    double mt = 1.0 - t;
-    return (c[1] - c[0]) * (3.0 * mt * mt) + (c[2] - c[1]) * (6.0 * mt * t) + (c[3] - c[2]) * (3.0 * t * t);
-}
-template <class P, class Emit>
-void flatten_cubic(const P c[4], double tol, Emit&& emit) {
-    const double quad_share = 0.1;
-    const Pt &c0 = val(c[0]), &c1 = val(c[1]), &c2 = val(c[2]), &c3 = val(c[3]);
-    Pt third{c3.x - 3.0 * c2.x + 3.0 * c1.x - c0.x, c3.y - 3.0 * c2.y + 3.0 * c1.y - c0.y};
-    double err = std::sqrt(3.0) / 36.0 * std::hypot(third.x, third.y);
-    int m = std::max(1, int(std::ceil(std::cbrt(err / (quad_share * tol)))));
-    m = std::min(m, 1 << 16);
-    for (int j = 0; j < m; ++j) {
-        double t0 = double(j) / m, t1 = double(j + 1) / m, h = (t1 - t0) / 3.0;
-        P q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
-        P q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
-        P ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
-        if (j == m - 1) q3 = c[3];
-        flatten_quad(q0, ctrl, q3, (1.0 - quad_share) * tol, emit);
-    }
-}
+// Flattening: the shared host/device flattener (flatten_core.h).
+using tkf::flatten_cubic;
+using tkf::flatten_quad;
 
 // PathFlatten::flatten (src/shared/path_flatten.rs:20-82): closes open
 // contours whose gap exceeds 1e-6 and drops edges with length^2 <= 1e-24.
@@ -511,12 +428,76 @@ struct tk_canvas {
     // differentiable parameters (fills of recorded paths)
     std::vector<double> points;
     std::vector<float> colors;
+    // device flattening: fills are kept as elements, flattened at upload
+    bool device_flatten = false;
+    std::vector<tk_flatten_el> els;
+    std::vector<uint32_t> path_els;  // per path: first element, element count
 };
 
 namespace {
 
+// flatten_path's walk with every flattening step recorded as an element
+// carrying its start point instead of being flattened here.
+void record_elements(const tk_path& path, double tol, uint32_t path_id, std::vector<tk_flatten_el>& out) {
+    bool has_start = false;
+    Pt start{0, 0}, last{0, 0};
+    auto element = [&](uint32_t verb, std::initializer_list<Pt> pts) {
+        tk_flatten_el e{};
+        e.verb = verb;
+        e.path = path_id;
+        e.tolerance = tol;
+        int k = 0;
+        for (const Pt& p : pts) {
+            e.p[k][0] = p.x;
+            e.p[k][1] = p.y;
+            ++k;
+        }
+        out.push_back(e);
+    };
+    auto open_close = [&]() {
+        if (!has_start) return;
+        double dx = start.x - last.x, dy = start.y - last.y;
+        if (dx * dx + dy * dy > 1.0e-6 * 1.0e-6) element(TK_EL_LINE, {last, start});
+    };
+    for (const El& e : path.els) {
+        switch (e.verb) {
+            case MOVE:
+                open_close();
+                start = last = e.p[0];
+                has_start = true;
+                break;
+            case LINE:
+                if (has_start) {
+                    element(TK_EL_LINE, {last, e.p[0]});
+                    last = e.p[0];
+                } else {
+                    start = last = e.p[0];
+                    has_start = true;
+                }
+                break;
+            case QUAD:
+                if (!has_start) { start = last = e.p[0]; has_start = true; }
+                element(TK_EL_QUAD, {last, e.p[0], e.p[1]});
+                last = e.p[1];
+                break;
+            case CUBIC:
+                if (!has_start) { start = last = e.p[0]; has_start = true; }
+                element(TK_EL_CUBIC, {last, e.p[0], e.p[1], e.p[2]});
+                last = e.p[2];
+                break;
+            case CLOSE:
+                if (has_start) {
+                    element(TK_EL_LINE, {last, start});
+                    last = start;
+                }
+                break;
+        }
+    }
+    open_close();
+}
+
 int64_t push_path_with_tag(tk_canvas* c, const tk_path& src, const tk_brush_desc* brush, const double* transform,
-                           uint32_t rule, double tolerance, uint32_t tag, bool emit_command) {
+                           uint32_t rule, double tolerance, uint32_t tag, bool emit_command, bool device_ok = true) {
     uint32_t line_start = uint32_t(c->lines.size());
     uint32_t path_id = uint32_t(c->paths.size());
     double s = double(c->scale);
@@ -524,7 +505,11 @@ int64_t push_path_with_tag(tk_canvas* c, const tk_path& src, const tk_brush_desc
     if (transform) std::memcpy(m, transform, sizeof(m));
     double dev[6] = {s * m[0], s * m[1], s * m[2], s * m[3], s * m[4], s * m[5]};
     tk_path path = transform_path(src, dev);
-    flatten_path(path, tolerance * s, path_id, c->lines);
+    const uint32_t el0 = uint32_t(c->els.size());
+    if (c->device_flatten && device_ok) record_elements(path, tolerance * s, path_id, c->els);
+    else flatten_path(path, tolerance * s, path_id, c->lines);
+    c->path_els.push_back(el0);
+    c->path_els.push_back(uint32_t(c->els.size()) - el0);
     uint32_t line_count = uint32_t(c->lines.size()) - line_start;
     Box bb = path_bbox(path);
     tk_pixel_bounds pb{0, 0, 0, 0};
@@ -721,6 +706,17 @@ tk_canvas* tk_canvas_new(uint32_t lw, uint32_t lh, float scale) {
 }
 void tk_canvas_free(tk_canvas* c) { delete c; }
 void tk_canvas_set_host_segment_plan(tk_canvas* c, int32_t enabled) { c->host_plan = enabled != 0; }
+void tk_canvas_set_device_flatten(tk_canvas* c, int32_t enabled) {
+    c->device_flatten = enabled != 0;
+    if (c->device_flatten) c->host_plan = false;  // segment capacities come from the device
+}
+int32_t tk_canvas_flatten_desc(const tk_canvas* c, tk_flatten_desc* out) {
+    if (!c || !out) return TK_E_INVALID;
+    out->elements = c->els.data();
+    out->element_count = c->els.size();
+    out->path_elements = c->path_els.data();
+    return TK_OK;
+}
 void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul) { c->clear = premul; }
 
 int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, const double* transform,
@@ -734,7 +730,8 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
     // Strokes are outlined in the path's local space (kurbo::stroke before
     // the transform, src/canvas/primitives/paths.rs:24-48).
     tk_path outline = stroke_path(*path, width, tolerance);
-    return push_path_with_tag(c, outline, brush, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_BRUSH, true);
+    // stroke outlines are polygons from the host stroker: they stay host lines
+    return push_path_with_tag(c, outline, brush, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_BRUSH, true, false);
 }
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform, uint32_t rule,
                                   double tolerance) {
@@ -1019,6 +1016,7 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             uint32_t w = pick(o->width, 640), h = pick(o->height, 360);
             c = tk_canvas_new(w, h, 1.0f);
             c->host_plan = !(o->flags & 1u);
+            if (o->flags & 2u) tk_canvas_set_device_flatten(c, 1);
             c->clear = 0xFFFFFFFFu;
             Rng r(seed);
             gen_uniform_fills(c, r, w, h, pick(o->paths, 240), 8, 40, 0.3f, true);
@@ -1028,6 +1026,7 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             uint32_t w = pick(o->width, 4096), h = pick(o->height, 4096);
             c = tk_canvas_new(w, h, 1.0f);
             c->host_plan = !(o->flags & 1u);
+            if (o->flags & 2u) tk_canvas_set_device_flatten(c, 1);
             c->clear = 0xFFFFFFFFu;
             Rng r(seed);
             gen_mixed(c, r, w, h, pick(o->paths, 50000));
@@ -1037,6 +1036,7 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             uint32_t w = pick(o->width, 1920), h = pick(o->height, 1080);
             c = tk_canvas_new(w, h, 1.0f);
             c->host_plan = !(o->flags & 1u);
+            if (o->flags & 2u) tk_canvas_set_device_flatten(c, 1);
             c->clear = 0xFFFFFFFFu;
             Rng r(seed);
             gen_glyphs(c, r, w, h, pick(o->paths, 20000));
@@ -1049,6 +1049,7 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             uint32_t n = o->paths ? o->paths : uint32_t(std::lround(std::exp(r.uniform(std::log(10.0), std::log(2000.0)))));
             c = tk_canvas_new(w, h, 1.0f);
             c->host_plan = !(o->flags & 1u);
+            if (o->flags & 2u) tk_canvas_set_device_flatten(c, 1);
             c->clear = 0xFFFFFFFFu;
             gen_uniform_fills(c, r, w, h, n, 8, 40, 0.3f, false);
             break;
@@ -1057,6 +1058,7 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
             uint32_t w = pick(o->width, 1024), h = pick(o->height, 1024);
             c = tk_canvas_new(w, h, 1.0f);
             c->host_plan = !(o->flags & 1u);
+            if (o->flags & 2u) tk_canvas_set_device_flatten(c, 1);
             c->clear = 0xFFFFFFFFu;
             Rng r(seed);
             Rng jr(seed ^ 0x6A09E667F3BCC909ull);  // jitter stream, independent of the scene stream

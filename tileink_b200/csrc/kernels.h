@@ -137,6 +137,15 @@ void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const 
 // FP32 FMA peak probe (TFLOP/s).
 double probe_fp32_tflops(cudaStream_t st);
 
+// Device flattening (flatten.cu): per-element line counts, exclusive offsets
+// in `counts` and the total; then path line ranges and the lines themselves.
+void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
+                          uint32_t* total, cudaStream_t st);
+void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* offsets, const uint32_t* total,
+                         tk_path_record* paths, uint32_t path_count, const uint32_t* path_els, tk_line* lines,
+                         uint64_t line_base, uint64_t line_end, uint32_t* error, cudaStream_t st);
+size_t flatten_block_sums(uint64_t n);
+
 // Differentiable rendering (diff.cu): float forward and adjoint.
 void launch_diff_fine_fwd(const SceneView& s, const PassView& p, const float4* colp, float4* layer, cudaStream_t st);
 void launch_diff_blur(const float4* in, float4* out, const float* w, int32_t r, uint32_t width, uint32_t height,

@@ -46,8 +46,14 @@ class NativeRenderer:
         return self._lib.tk_ctx_stream(self._h)
 
     def upload(self, scene) -> None:
+        """Uploads a Canvas (its fills flattened on the GPU when it recorded
+        them as elements) or a pre-flattened scene description."""
         d = scene.scene_desc() if hasattr(scene, "scene_desc") else scene.desc
-        self._check(self._lib.tk_scene_upload(self._h, C.byref(d)))
+        fl = scene.flatten_desc() if hasattr(scene, "flatten_desc") else getattr(scene, "flatten", None)
+        if fl is not None:
+            self._check(self._lib.tk_scene_upload_flatten(self._h, C.byref(d), C.byref(fl)))
+        else:
+            self._check(self._lib.tk_scene_upload(self._h, C.byref(d)))
         self.width, self.height = d.width, d.height
 
     def render(self) -> None:
@@ -96,7 +102,8 @@ class NativeRenderer:
         self._check(self._lib.tk_debug_readback(self._h, stage, index, None, 0, C.byref(need)))
         dt = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
               N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
-              N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE}[stage]
+              N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE,
+              N.STAGE_LINES: N.LINE_DTYPE}[stage]
         out = np.zeros(need.value // np.dtype(dt).itemsize, dtype=dt)
         self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
         return out
