@@ -263,6 +263,7 @@ def pinned_scene(canvas):
     import torch
     from tileink_b200 import _native as N
     arrays = canvas.scene_arrays()
+    arrays.update(canvas.flatten_arrays())
     pinned = {}
     keep = []
     for k, v in arrays.items():
@@ -338,25 +339,36 @@ def main():
     value = world * 1000.0 / ms
 
     # end to end: pinned host scene -> H2D -> frame -> D2H image, every step
-    ps, bytes_in = pinned_scene(canvas)
     out = torch.empty(r.width * r.height * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint32)
-    r.upload(ps)
-    r.render()
-    r.readback(out)
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s0.record(stream)
-    for _ in range(args.e2e_steps):
+
+    def e2e_ms_of(ps):
         r.upload(ps)
         r.render()
         r.readback(out)
-    s1.record(stream)
-    s1.synchronize()
-    e2e_ms = s0.elapsed_time(s1) / args.e2e_steps
-    wall_ms = (time.perf_counter() - t0) * 1000.0 / args.e2e_steps
-    e2e_ms = max_over_ranks(max(e2e_ms, wall_ms), world)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.e2e_steps):
+            r.upload(ps)
+            r.render()
+            r.readback(out)
+        s1.record(stream)
+        s1.synchronize()
+        dev_ms = s0.elapsed_time(s1) / args.e2e_steps
+        wall_ms = (time.perf_counter() - t0) * 1000.0 / args.e2e_steps
+        return max_over_ranks(max(dev_ms, wall_ms), world)
+
+    ps, bytes_in = pinned_scene(canvas)
+    e2e_ms = e2e_ms_of(ps)
+    del ps
+    # the same scene with its fills as Bezier elements, flattened on the GPU
+    # at upload (stroke outlines stay host lines)
+    flat_canvas = tk.generate(2, SEED, width=args.size, height=args.size, paths=args.paths, device_flatten=True)
+    ps_flat, bytes_in_flat = pinned_scene(flat_canvas)
+    e2e_flat_ms = e2e_ms_of(ps_flat)
+    del ps_flat, flat_canvas
     bytes_out = out.nbytes
 
     # roofline of the dominant kernel
@@ -424,7 +436,13 @@ def main():
                        "l2": "inputs > L2 (lines %.1f GB), no flush" % (L * 24 / 1e9),
                        "segment_plan": "device"},
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
-                    "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms,
+                    "input": "host-flattened lines (the reference's Line records)"},
+            "e2e_device_flatten": {"value": world * 1000.0 / e2e_flat_ms, "unit": UNIT,
+                                   "h2d_bytes_per_step": int(bytes_in_flat), "d2h_bytes_per_step": int(bytes_out),
+                                   "ms_per_step": e2e_flat_ms,
+                                   "input": "fills as Bezier elements flattened on the GPU at upload, "
+                                            "stroke outlines as lines"},
             "gpu_launches": launches_per_frame * args.steps,
             "roofline": roof,
             "stage_ms": stage_ms,

@@ -60,6 +60,16 @@ def test_gpu_device_flattening_rejects_inconsistent_elements(renderer):
     bad = N.FlattenDesc(f.elements, f.element_count, path_els.ctypes.data)
     with pytest.raises(tk.TileinkError):
         renderer._check(renderer._lib.tk_scene_upload_flatten(renderer._h, ctypes.byref(d), ctypes.byref(bad)))
+    # elements the device refuses to flatten (their work would be unbounded):
+    # reported, nothing flattened, the context stays usable
+    arrays = canvas.scene_arrays()
+    arrays.update(canvas.flatten_arrays())
+    arrays["elements"] = arrays["elements"].copy()
+    arrays["elements"]["tolerance"][0] = 1e-9
+    with pytest.raises(tk.TileinkError, match="tolerance"):
+        renderer.upload(N.ArrayScene(arrays))
+    img = renderer.render_to_image(canvas)
+    assert img.shape == (96, 128, 4)
     # a host-flattened scene without device planning cannot take elements either
     host = tk.generate(1, 3, width=128, height=96, paths=5)
     with pytest.raises(tk.TileinkError):

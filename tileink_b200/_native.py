@@ -56,6 +56,8 @@ TILE_DTYPE = np.dtype([(k, "<u4") for k in ("ptcl_count", "ptcl_start", "ptcl_en
                                             "glyph_start", "glyph_end")])
 OP_DTYPE = np.dtype([("kind", "<u4"), ("batch_id", "<u4"), ("layer_start", "<u4"), ("layer_end", "<u4"),
                      ("sigma", "<f4"), ("bounds", "<i4", 4)])
+FLATTEN_EL_DTYPE = np.dtype([("verb", "<u4"), ("path", "<u4"), ("tolerance", "<f8"), ("p", "<f8", (4, 2))])
+assert FLATTEN_EL_DTYPE.itemsize == 80
 assert LINE_DTYPE.itemsize == 24 and PATH_DTYPE.itemsize == 76 and DRAW_DTYPE.itemsize == 124
 assert LAYER_DTYPE.itemsize == 12 and PTCL_DTYPE.itemsize == 24 and SEGMENT_DTYPE.itemsize == 20
 assert TILE_DTYPE.itemsize == 24 and OP_DTYPE.itemsize == 36
@@ -238,3 +240,6 @@ class ArrayScene:
         d.draw_batch_ids = ptr(a["draw_batch_ids"])
         d.ops, d.op_count = ptr(a["ops"]), len(a["ops"])
         self.desc = d
+        self.flatten = None
+        if a.get("elements") is not None and len(a["elements"]):
+            self.flatten = FlattenDesc(ptr(a["elements"]), len(a["elements"]), ptr(a["path_elements"]))

@@ -142,6 +142,17 @@ class Canvas:
         self._lib.tk_canvas_flatten_desc(self._h, C.byref(f))
         return f if f.element_count else None
 
+    def flatten_arrays(self) -> dict:
+        """Copies of the device-flattening elements and per-path element ranges
+        (empty when the canvas flattens on the host)."""
+        f = self.flatten_desc()
+        n_paths = self.scene_desc().path_count
+        if f is None:
+            return {"elements": np.zeros(0, N.FLATTEN_EL_DTYPE), "path_elements": np.zeros(0, np.uint32)}
+        els = np.ctypeslib.as_array((C.c_uint8 * (f.element_count * 80)).from_address(f.elements))
+        pe = np.ctypeslib.as_array((C.c_uint32 * (2 * n_paths)).from_address(f.path_elements))
+        return {"elements": els.view(N.FLATTEN_EL_DTYPE).copy(), "path_elements": pe.copy()}
+
     def push_path(self, path: BezPath, brush: Brush, transform=None, fill_rule=FILL_NONZERO,
                   tolerance: float = 0.1) -> int:
         d, keep = brush._desc()

@@ -642,24 +642,14 @@ void rebuild_items(tk_ctx* c) {
 void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl) {
     if (!(d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE)) invalid("device flattening needs device segment planning");
     if ((fl.element_count && !fl.elements) || (d.path_count && !fl.path_elements)) invalid("null flatten arrays");
+    // Element ranges are checked here; the elements themselves (verb,
+    // tolerance >= 1e-3 px, coordinates within 1e6 px, owning path) on the
+    // device, which skips and reports any that fail.
     for (uint32_t p = 0; p < d.path_count; ++p) {
         const uint64_t e0 = fl.path_elements[2 * p], ne = fl.path_elements[2 * p + 1];
         if (!ne) continue;
         if (e0 + ne > fl.element_count) invalid("path " + std::to_string(p) + ": elements out of range");
         if (d.paths[p].line_count) invalid("path " + std::to_string(p) + ": both lines and elements");
-        for (uint64_t e = e0; e < e0 + ne; ++e) {
-            const tk_flatten_el& el = fl.elements[e];
-            if (el.path != p) invalid("element " + std::to_string(e) + ": path index mismatch");
-            if (el.verb < TK_EL_LINE || el.verb > TK_EL_CUBIC) invalid("element " + std::to_string(e) + ": bad verb");
-            // Bounded inputs bound one thread's subdivision work (about 1e6
-            // points for the worst element).
-            if (!(el.tolerance >= 1e-3) || !std::isfinite(el.tolerance))
-                invalid("flattening tolerance below 1e-3 px or not finite");
-            for (int k = 0; k <= int(el.verb); ++k)
-                for (int a = 0; a < 2; ++a)
-                    if (!(std::fabs(el.p[k][a]) <= 1e6))
-                        invalid("element " + std::to_string(e) + ": coordinates beyond 1e6 px or not finite");
-        }
     }
     cudaStream_t st = c->stream;
     const uint64_t n = fl.element_count;
@@ -671,7 +661,7 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     sums.reserve(tk::flatten_block_sums(n));
     words.reserve(2);
     TK_CUDA(cudaMemsetAsync(words.ptr, 0, 2 * sizeof(uint32_t), st));
-    tk::launch_flatten_count(els.ptr, n, offsets.ptr, sums.ptr, words.ptr, st);
+    tk::launch_flatten_count(els.ptr, n, offsets.ptr, sums.ptr, words.ptr, words.ptr + 1, st);
     uint32_t dev_lines = 0;
     TK_CUDA(cudaMemcpyAsync(&dev_lines, words.ptr, 4, cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaStreamSynchronize(st));
@@ -692,7 +682,13 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     offsets.release();
     sums.release();
     words.release();
-    if (err) throw Fail{TK_E_INVALID, "device flattening wrote past its line count"};
+    if (err) {
+        std::string m = "device flattening rejected the elements:";
+        if (err & tk::ERR_UNSUPPORTED) m += " bad verb, tolerance below 1e-3 px or coordinates beyond 1e6 px;";
+        if (err & tk::ERR_LINE_PATH_MISMATCH) m += " an element's path index differs from its path;";
+        if (err & tk::ERR_SEGMENT_OVERFLOW) m += " lines past the counted total;";
+        throw Fail{TK_E_INVALID, m};
+    }
     c->line_count = total;
 }
 

@@ -40,6 +40,18 @@ struct WriteEmit {
     }
 };
 
+// Elements the flattener accepts: a known verb, tolerance >= 1e-3 px and
+// finite coordinates within 1e6 px. These bounds bound one thread's work
+// (about 1e6 points for the worst element); anything else is flagged and
+// produces no lines.
+__device__ bool element_ok(const tk_flatten_el& e) {
+    if (e.verb < TK_EL_LINE || e.verb > TK_EL_CUBIC) return false;
+    if (!(e.tolerance >= 1e-3) || !isfinite(e.tolerance)) return false;
+    for (uint32_t k = 0; k <= e.verb; ++k)
+        if (!(fabs(e.p[k][0]) <= 1e6) || !(fabs(e.p[k][1]) <= 1e6)) return false;
+    return true;
+}
+
 template <class Emit>
 __device__ void flatten_element(const tk_flatten_el& e, Emit& emit) {
     const Pt from{e.p[0][0], e.p[0][1]};
@@ -53,11 +65,12 @@ __device__ void flatten_element(const tk_flatten_el& e, Emit& emit) {
     }
 }
 
-__global__ void k_flatten_count(const tk_flatten_el* __restrict__ els, uint64_t n, uint32_t* counts) {
+__global__ void k_flatten_count(const tk_flatten_el* __restrict__ els, uint64_t n, uint32_t* counts, uint32_t* error) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const tk_flatten_el e = els[i];
         CountEmit c{Pt{e.p[0][0], e.p[0][1]}, 0u};
-        flatten_element(e, c);
+        if (element_ok(e)) flatten_element(e, c);
+        else atomicOr(error, ERR_UNSUPPORTED);
         counts[i] = c.n;
     }
 }
@@ -139,11 +152,14 @@ __global__ void k_scan_add(uint32_t* v, uint64_t n, const uint32_t* sums) {
 // first element, + the elements' lines).
 __global__ void k_flatten_paths(tk_path_record* paths, uint32_t path_count, const uint32_t* __restrict__ path_els,
                                 const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ total,
-                                uint64_t n_els, uint32_t line_base) {
+                                uint64_t n_els, uint32_t line_base, const tk_flatten_el* __restrict__ els,
+                                uint32_t* error) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= path_count) return;
     const uint32_t e0 = path_els[2 * p], ne = path_els[2 * p + 1];
     if (ne == 0u) return;
+    for (uint32_t e = e0; e < e0 + ne; ++e)  // the path's elements carry its index
+        if (els[e].path != p) atomicOr(error, ERR_LINE_PATH_MISMATCH);
     const uint32_t a = offsets[e0];
     const uint32_t b = uint64_t(e0) + ne < n_els ? offsets[e0 + ne] : *total;
     paths[p].line_start = line_base + a;
@@ -155,19 +171,19 @@ __global__ void k_flatten_emit(const tk_flatten_el* __restrict__ els, uint64_t n
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const tk_flatten_el e = els[i];
         WriteEmit w{Pt{e.p[0][0], e.p[0][1]}, lines, line_base + offsets[i], line_end, e.path, error};
-        flatten_element(e, w);
+        if (element_ok(e)) flatten_element(e, w);
     }
 }
 
 }  // namespace
 
 void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
-                          uint32_t* total, cudaStream_t st) {
+                          uint32_t* total, uint32_t* error, cudaStream_t st) {
     if (n == 0) {
         cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
         return;
     }
-    k_flatten_count<<<148 * 16, 128, 0, st>>>(els, n, counts);
+    k_flatten_count<<<148 * 16, 128, 0, st>>>(els, n, counts, error);
     const uint32_t blocks = uint32_t((n + kScanBlock - 1) / kScanBlock);
     k_scan_local<<<blocks, kScanBlock, 0, st>>>(counts, n, block_sums);
     k_scan_sums<<<1, kScanBlock, 0, st>>>(block_sums, blocks, total);
@@ -178,7 +194,7 @@ void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* o
                          tk_path_record* paths, uint32_t path_count, const uint32_t* path_els, tk_line* lines,
                          uint64_t line_base, uint64_t line_end, uint32_t* error, cudaStream_t st) {
     if (path_count) k_flatten_paths<<<(path_count + 255) / 256, 256, 0, st>>>(paths, path_count, path_els, offsets,
-                                                                             total, n, uint32_t(line_base));
+                                                                             total, n, uint32_t(line_base), els, error);
     if (n) k_flatten_emit<<<148 * 16, 128, 0, st>>>(els, n, offsets, lines, line_base, line_end, error);
 }
 

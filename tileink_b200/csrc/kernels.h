@@ -140,7 +140,7 @@ double probe_fp32_tflops(cudaStream_t st);
 // Device flattening (flatten.cu): per-element line counts, exclusive offsets
 // in `counts` and the total; then path line ranges and the lines themselves.
 void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
-                          uint32_t* total, cudaStream_t st);
+                          uint32_t* total, uint32_t* error, cudaStream_t st);
 void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* offsets, const uint32_t* total,
                          tk_path_record* paths, uint32_t path_count, const uint32_t* path_els, tk_line* lines,
                          uint64_t line_base, uint64_t line_end, uint32_t* error, cudaStream_t st);
