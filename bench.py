@@ -363,8 +363,8 @@ def main():
     ps, bytes_in = pinned_scene(canvas)
     e2e_ms = e2e_ms_of(ps)
     del ps
-    # the same scene with its fills as Bezier elements, flattened on the GPU
-    # at upload (stroke outlines stay host lines)
+    # the same scene with its fills and stroke centerlines as Bezier
+    # elements, flattened and stroked on the GPU at upload
     flat_canvas = tk.generate(2, SEED, width=args.size, height=args.size, paths=args.paths, device_flatten=True)
     ps_flat, bytes_in_flat = pinned_scene(flat_canvas)
     e2e_flat_ms = e2e_ms_of(ps_flat)
@@ -441,8 +441,8 @@ def main():
             "e2e_device_flatten": {"value": world * 1000.0 / e2e_flat_ms, "unit": UNIT,
                                    "h2d_bytes_per_step": int(bytes_in_flat), "d2h_bytes_per_step": int(bytes_out),
                                    "ms_per_step": e2e_flat_ms,
-                                   "input": "fills as Bezier elements flattened on the GPU at upload, "
-                                            "stroke outlines as lines"},
+                                   "input": "fills and stroke centerlines as Bezier elements, flattened "
+                                            "and stroked on the GPU at upload"},
             "gpu_launches": launches_per_frame * args.steps,
             "roofline": roof,
             "stage_ms": stage_ms,

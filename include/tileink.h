@@ -370,16 +370,50 @@ typedef struct tk_flatten_el {
     double p[4][2];
 } tk_flatten_el; /* 80 B */
 
+/* Stroke centerlines (the stroking step of Canvas::push_stroke,
+ * src/canvas/primitives/paths.rs:24-48, kurbo::stroke with round joins and
+ * caps) are elements too, in the path's local units: each polyline is a
+ * TK_EL_MOVE element (p[0] = its start) followed by line / quadratic / cubic
+ * elements whose p[0] is the current point; `path` holds the polyline index and
+ * `tolerance` the stroking tolerance. The device flattens, offsets, joins, caps
+ * and transforms them into the stroke's outline lines. */
+#define TK_EL_MOVE 4u
+
+typedef struct tk_stroke_polyline {
+    uint32_t stroke;        /* index into tk_flatten_desc.strokes */
+    uint32_t element0;      /* its TK_EL_MOVE in stroke_elements */
+    uint32_t element_count; /* >= 1, the move included */
+    uint32_t closed;        /* 1 after a close */
+} tk_stroke_polyline; /* 16 B */
+
+typedef struct tk_stroke_desc {
+    uint32_t path;           /* the outline's path: its lines' path_id */
+    uint32_t polyline0;      /* first polyline */
+    uint32_t polyline_count;
+    uint32_t reserved;
+    double half_width;       /* width / 2 in local units, (0, 1e6] */
+    double tolerance;        /* arc tolerance in local units, >= 1e-3 */
+    double transform[6];     /* local -> device pixels: x' = t0 x + t2 y + t4, y' = t1 x + t3 y + t5 */
+} tk_stroke_desc; /* 80 B */
+
 typedef struct tk_flatten_desc {
     const tk_flatten_el* elements;
     uint64_t element_count;
     const uint32_t* path_elements; /* [path_count][first, count]; count 0: the
-                                      path's lines are in tk_scene_desc.lines */
+                                      path's lines are in tk_scene_desc.lines
+                                      or come from a stroke */
+    const tk_flatten_el* stroke_elements;
+    uint64_t stroke_element_count;
+    const tk_stroke_polyline* polylines;
+    uint32_t polyline_count;
+    uint32_t stroke_count;
+    const tk_stroke_desc* strokes;
 } tk_flatten_desc;
 
-/* tk_scene_upload for a scene whose paths with elements are flattened on the
- * device. tk_scene_desc.lines holds the other paths' lines; the device lines
- * follow them. Requires TK_SCENE_SEGMENTS_FROM_DEVICE. */
+/* tk_scene_upload for a scene whose paths with elements or strokes are
+ * flattened on the device. tk_scene_desc.lines holds the other paths' lines;
+ * the fills' device lines follow them, then the strokes' outline lines.
+ * Requires TK_SCENE_SEGMENTS_FROM_DEVICE. */
 int32_t tk_scene_upload_flatten(tk_ctx* ctx, const tk_scene_desc* scene, const tk_flatten_desc* flatten);
 
 /* ------------------------------------------------------------------------ */

@@ -75,3 +75,103 @@ def test_gpu_device_flattening_rejects_inconsistent_elements(renderer):
     with pytest.raises(tk.TileinkError):
         renderer._check(renderer._lib.tk_scene_upload_flatten(renderer._h, ctypes.byref(host.scene_desc()),
                                                               ctypes.byref(f)))
+
+
+def stroke_scene(device: bool):
+    """Every stroke shape of the CPU stroke tests, at several widths and
+    transforms (identity, rotation + scale, shear), plus seeded random curves:
+    open, closed, dots, multiple subpaths, a close followed by more drawing."""
+    from test_stroke import CASES
+    c = tk.Canvas(320, 240)
+    if device:
+        c.set_device_flatten(True)
+    else:
+        c.set_host_segment_plan(False)
+    transforms = [None, (0.9, 0.35, -0.35, 0.9, 40.0, -10.0), (1.0, 0.0, 0.4, 0.7, -20.0, 30.0)]
+    k = 0
+    for name in sorted(CASES):
+        build, _, width = CASES[name]
+        for t in transforms:
+            for w in (width, 0.75, 2.5):
+                p = tk.BezPath()
+                build(p)
+                c.push_stroke(p, tk.Brush.solid((k % 7) / 7, (k % 5) / 5, (k % 3) / 3, 0.6), w, transform=t,
+                              tolerance=0.05 + 0.05 * (k % 3))
+                k += 1
+    rng = np.random.default_rng(11)
+    for _ in range(60):
+        p = tk.BezPath()
+        p.move_to(*rng.uniform(0, 320, 2))
+        for _ in range(int(rng.integers(1, 9))):
+            if rng.random() < 0.5:
+                p.cubic_to(*rng.uniform(-20, 340, 6))
+            else:
+                p.quad_to(*rng.uniform(-20, 340, 4))
+        if rng.random() < 0.4:
+            p.close()
+        c.push_stroke(p, tk.Brush.solid(*rng.uniform(0, 1, 3), 0.8), float(rng.uniform(0.3, 12.0)),
+                      tolerance=float(rng.uniform(0.02, 0.3)))
+    return c
+
+
+def test_gpu_device_stroking_matches_host_stroking(renderer):
+    host = render_with(renderer, stroke_scene(False))
+    dev_canvas = stroke_scene(True)
+    f = dev_canvas.flatten_desc()
+    assert f is not None and f.stroke_count > 0 and dev_canvas.scene_desc().line_count == 0
+    dev = render_with(renderer, dev_canvas)
+    hp, dp = host["paths"], dev["paths"]
+    assert np.array_equal(hp["line_count"], dp["line_count"])
+    assert int(hp["line_count"].sum()) > 10000
+    for k in range(len(hp)):
+        a = host["lines"][hp["line_start"][k]:hp["line_start"][k] + hp["line_count"][k]]
+        b = dev["lines"][dp["line_start"][k]:dp["line_start"][k] + dp["line_count"][k]]
+        assert a.tobytes() == b.tobytes(), k
+    assert dev["segments"].tobytes() == host["segments"].tobytes()
+    for a, b in zip(host["ptcl"], dev["ptcl"]):
+        assert a.tobytes() == b.tobytes()
+    assert np.array_equal(dev["img"], host["img"])
+
+
+def test_gpu_device_stroking_rejects_inconsistent_strokes(renderer):
+    canvas = stroke_scene(True)
+    base = canvas.scene_arrays()
+    base.update(canvas.flatten_arrays())
+
+    def upload(mutate):
+        a = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in base.items()}
+        mutate(a)
+        renderer.upload(N.ArrayScene(a))
+
+    def set_(key, field, index, value):
+        def f(a):
+            a[key][field][index] = value
+        return f
+
+    bad = [
+        set_("strokes", "half_width", 0, 0.0),
+        set_("strokes", "half_width", 1, np.nan),
+        set_("strokes", "tolerance", 2, 1e-6),
+        set_("strokes", "transform", 3, np.inf),
+        set_("strokes", "path", 4, 10 ** 6),
+        set_("strokes", "path", 5, 4),                 # two strokes on one path
+        set_("strokes", "polyline_count", 6, 10 ** 6),
+        set_("polylines", "stroke", 0, 1),              # owned by another stroke
+        set_("polylines", "element_count", 1, 0),
+        set_("polylines", "element0", 2, 10 ** 9),
+    ]
+    for mutate in bad:
+        with pytest.raises(tk.TileinkError):
+            upload(mutate)
+    # element faults found on the device: reported, the context stays usable
+    device_bad = [
+        set_("stroke_elements", "verb", 0, N.EL_LINE),       # a polyline that does not start with a move
+        set_("stroke_elements", "path", 1, 7),               # an element of another polyline
+        set_("stroke_elements", "tolerance", 2, 1e-9),
+        set_("stroke_elements", "verb", 3, 9),
+    ]
+    for mutate in device_bad:
+        with pytest.raises(tk.TileinkError):
+            upload(mutate)
+    img = renderer.render_to_image(canvas)
+    assert img.shape == (240, 320, 4)

@@ -56,8 +56,12 @@ TILE_DTYPE = np.dtype([(k, "<u4") for k in ("ptcl_count", "ptcl_start", "ptcl_en
                                             "glyph_start", "glyph_end")])
 OP_DTYPE = np.dtype([("kind", "<u4"), ("batch_id", "<u4"), ("layer_start", "<u4"), ("layer_end", "<u4"),
                      ("sigma", "<f4"), ("bounds", "<i4", 4)])
+EL_LINE, EL_QUAD, EL_CUBIC, EL_MOVE = 1, 2, 3, 4
 FLATTEN_EL_DTYPE = np.dtype([("verb", "<u4"), ("path", "<u4"), ("tolerance", "<f8"), ("p", "<f8", (4, 2))])
-assert FLATTEN_EL_DTYPE.itemsize == 80
+POLYLINE_DTYPE = np.dtype([("stroke", "<u4"), ("element0", "<u4"), ("element_count", "<u4"), ("closed", "<u4")])
+STROKE_DTYPE = np.dtype([("path", "<u4"), ("polyline0", "<u4"), ("polyline_count", "<u4"), ("reserved", "<u4"),
+                         ("half_width", "<f8"), ("tolerance", "<f8"), ("transform", "<f8", (6,))])
+assert FLATTEN_EL_DTYPE.itemsize == 80 and POLYLINE_DTYPE.itemsize == 16 and STROKE_DTYPE.itemsize == 80
 assert LINE_DTYPE.itemsize == 24 and PATH_DTYPE.itemsize == 76 and DRAW_DTYPE.itemsize == 124
 assert LAYER_DTYPE.itemsize == 12 and PTCL_DTYPE.itemsize == 24 and SEGMENT_DTYPE.itemsize == 20
 assert TILE_DTYPE.itemsize == 24 and OP_DTYPE.itemsize == 36
@@ -95,7 +99,9 @@ class BrushDesc(C.Structure):
 
 class FlattenDesc(C.Structure):
     """tk_flatten_desc (include/tileink.h)."""
-    _fields_ = [("elements", C.c_void_p), ("element_count", C.c_uint64), ("path_elements", C.c_void_p)]
+    _fields_ = [("elements", C.c_void_p), ("element_count", C.c_uint64), ("path_elements", C.c_void_p),
+                ("stroke_elements", C.c_void_p), ("stroke_element_count", C.c_uint64), ("polylines", C.c_void_p),
+                ("polyline_count", C.c_uint32), ("stroke_count", C.c_uint32), ("strokes", C.c_void_p)]
 
 
 class DiffScene(C.Structure):
@@ -241,5 +247,12 @@ class ArrayScene:
         d.ops, d.op_count = ptr(a["ops"]), len(a["ops"])
         self.desc = d
         self.flatten = None
-        if a.get("elements") is not None and len(a["elements"]):
-            self.flatten = FlattenDesc(ptr(a["elements"]), len(a["elements"]), ptr(a["path_elements"]))
+        els, strokes = a.get("elements"), a.get("strokes")
+        if (els is not None and len(els)) or (strokes is not None and len(strokes)):
+            f = FlattenDesc()
+            f.elements, f.element_count, f.path_elements = ptr(els), len(els), ptr(a["path_elements"])
+            if strokes is not None and len(strokes):
+                f.stroke_elements, f.stroke_element_count = ptr(a["stroke_elements"]), len(a["stroke_elements"])
+                f.polylines, f.polyline_count = ptr(a["polylines"]), len(a["polylines"])
+                f.strokes, f.stroke_count = ptr(strokes), len(strokes)
+            self.flatten = f

@@ -133,25 +133,37 @@ class Canvas:
         self._lib.tk_canvas_set_host_segment_plan(self._h, 1 if enabled else 0)
 
     def set_device_flatten(self, enabled: bool):
-        """Fills recorded from now on are flattened on the GPU at upload."""
+        """Fills and strokes recorded from now on are flattened (and stroked)
+        on the GPU at upload."""
         self._lib.tk_canvas_set_device_flatten(self._h, 1 if enabled else 0)
 
     def flatten_desc(self) -> N.FlattenDesc | None:
-        """The elements to flatten on the device, or None when there are none."""
+        """The elements and strokes to flatten on the device, or None when
+        there are none."""
         f = N.FlattenDesc()
         self._lib.tk_canvas_flatten_desc(self._h, C.byref(f))
-        return f if f.element_count else None
+        return f if (f.element_count or f.stroke_count) else None
 
     def flatten_arrays(self) -> dict:
-        """Copies of the device-flattening elements and per-path element ranges
-        (empty when the canvas flattens on the host)."""
+        """Copies of the device-flattening elements, per-path element ranges
+        and strokes (empty when the canvas flattens on the host)."""
         f = self.flatten_desc()
         n_paths = self.scene_desc().path_count
+
+        def arr(addr, n, dtype):
+            if not n:
+                return np.zeros(0, dtype)
+            raw = np.ctypeslib.as_array((C.c_uint8 * (n * dtype.itemsize)).from_address(addr))
+            return raw.view(dtype).copy()
+
         if f is None:
-            return {"elements": np.zeros(0, N.FLATTEN_EL_DTYPE), "path_elements": np.zeros(0, np.uint32)}
-        els = np.ctypeslib.as_array((C.c_uint8 * (f.element_count * 80)).from_address(f.elements))
-        pe = np.ctypeslib.as_array((C.c_uint32 * (2 * n_paths)).from_address(f.path_elements))
-        return {"elements": els.view(N.FLATTEN_EL_DTYPE).copy(), "path_elements": pe.copy()}
+            f = N.FlattenDesc()
+            n_paths = 0
+        return {"elements": arr(f.elements, f.element_count, N.FLATTEN_EL_DTYPE),
+                "path_elements": arr(f.path_elements, 2 * n_paths, np.dtype(np.uint32)),
+                "stroke_elements": arr(f.stroke_elements, f.stroke_element_count, N.FLATTEN_EL_DTYPE),
+                "polylines": arr(f.polylines, f.polyline_count, N.POLYLINE_DTYPE),
+                "strokes": arr(f.strokes, f.stroke_count, N.STROKE_DTYPE)}
 
     def push_path(self, path: BezPath, brush: Brush, transform=None, fill_rule=FILL_NONZERO,
                   tolerance: float = 0.1) -> int:

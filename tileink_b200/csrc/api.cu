@@ -14,6 +14,7 @@
 #include "../../include/tileink.h"
 #include "../../include/tileink_canvas.h"
 #include "../../include/tileink_diff.h"
+#include "flatten_core.h"
 #include "kernels.h"
 
 namespace {
@@ -645,47 +646,109 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     // Element ranges are checked here; the elements themselves (verb,
     // tolerance >= 1e-3 px, coordinates within 1e6 px, owning path) on the
     // device, which skips and reports any that fail.
+    std::vector<uint8_t> taken(d.path_count, 0);  // paths whose lines come from the device
     for (uint32_t p = 0; p < d.path_count; ++p) {
         const uint64_t e0 = fl.path_elements[2 * p], ne = fl.path_elements[2 * p + 1];
         if (!ne) continue;
         if (e0 + ne > fl.element_count) invalid("path " + std::to_string(p) + ": elements out of range");
         if (d.paths[p].line_count) invalid("path " + std::to_string(p) + ": both lines and elements");
+        taken[p] = 1;
     }
+    // Strokes and their polylines are checked here (ranges, ownership, sizes);
+    // their elements on the device like the fills'.
+    const uint32_t ns = fl.stroke_count, npl = fl.polyline_count;
+    const uint64_t nse = fl.stroke_element_count;
+    if ((ns && !fl.strokes) || (npl && !fl.polylines) || (nse && !fl.stroke_elements)) invalid("null stroke arrays");
+    for (uint32_t s = 0; s < ns; ++s) {
+        const tk_stroke_desc& S = fl.strokes[s];
+        const std::string at = "stroke " + std::to_string(s) + ": ";
+        if (S.path >= d.path_count) invalid(at + "path out of range");
+        if (taken[S.path] || d.paths[S.path].line_count) invalid(at + "its path already has lines or elements");
+        taken[S.path] = 1;
+        if (!(S.half_width > 0.0 && S.half_width <= 1e6)) invalid(at + "half width outside (0, 1e6]");
+        if (!(S.tolerance >= 1e-3 && S.tolerance <= 1e6)) invalid(at + "tolerance outside [1e-3, 1e6]");
+        for (double t : S.transform)
+            if (!(std::fabs(t) <= 1e6)) invalid(at + "transform entries must be finite, within 1e6");
+        if (uint64_t(S.polyline0) + S.polyline_count > npl) invalid(at + "polylines out of range");
+        for (uint32_t k = S.polyline0; k < S.polyline0 + S.polyline_count; ++k)
+            if (fl.polylines[k].stroke != s) invalid(at + "polyline " + std::to_string(k) + " belongs elsewhere");
+    }
+    for (uint32_t k = 0; k < npl; ++k) {
+        const tk_stroke_polyline& P = fl.polylines[k];
+        if (P.stroke >= ns) invalid("polyline " + std::to_string(k) + ": stroke out of range");
+        if (!P.element_count || uint64_t(P.element0) + P.element_count > nse)
+            invalid("polyline " + std::to_string(k) + ": elements out of range");
+    }
+    if (nse > 0xFFFFFFFFull) invalid("stroke element count exceeds u32 indexing");
     cudaStream_t st = c->stream;
     const uint64_t n = fl.element_count;
-    DBuf<tk_flatten_el> els;
-    DBuf<uint32_t> path_els, offsets, sums, words;
+    DBuf<tk_flatten_el> els, sels;
+    DBuf<uint32_t> path_els, offsets, sums, words, soff, ssums, poly_n, line_off;
+    DBuf<tk_stroke_polyline> polys;
+    DBuf<tk_stroke_desc> strokes;
+    DBuf<unsigned long long> wide;
+    DBuf<tkf::Pt> pts;
     upload(els, fl.elements, n, st);
     upload(path_els, fl.path_elements, 2ull * d.path_count, st);
+    upload(sels, fl.stroke_elements, nse, st);
+    upload(polys, fl.polylines, npl, st);
+    upload(strokes, fl.strokes, ns, st);
     offsets.reserve(n);
     sums.reserve(tk::flatten_block_sums(n));
-    words.reserve(2);
-    TK_CUDA(cudaMemsetAsync(words.ptr, 0, 2 * sizeof(uint32_t), st));
+    soff.reserve(nse);
+    ssums.reserve(tk::flatten_block_sums(std::max<uint64_t>(nse, npl)));
+    poly_n.reserve(npl);
+    line_off.reserve(npl);
+    // words: [0] fill lines [1] error [2] stroke points [3] stroke lines
+    words.reserve(4);
+    wide.reserve(2);  // exact sums: [0] stroke points [1] stroke lines
+    TK_CUDA(cudaMemsetAsync(words.ptr, 0, 4 * sizeof(uint32_t), st));
+    TK_CUDA(cudaMemsetAsync(wide.ptr, 0, 2 * sizeof(unsigned long long), st));
     tk::launch_flatten_count(els.ptr, n, offsets.ptr, sums.ptr, words.ptr, words.ptr + 1, st);
-    uint32_t dev_lines = 0;
-    TK_CUDA(cudaMemcpyAsync(&dev_lines, words.ptr, 4, cudaMemcpyDeviceToHost, st));
+    tk::launch_stroke_count(sels.ptr, nse, soff.ptr, ssums.ptr, words.ptr + 2, wide.ptr, words.ptr + 1, st);
+    uint32_t w[4] = {0, 0, 0, 0};
+    unsigned long long wsum[2] = {0, 0};
+    TK_CUDA(cudaMemcpyAsync(w, words.ptr, sizeof(w), cudaMemcpyDeviceToHost, st));
+    TK_CUDA(cudaMemcpyAsync(wsum, wide.ptr, sizeof(wsum), cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaStreamSynchronize(st));
-    const uint64_t host_lines = d.line_count, total = host_lines + dev_lines;
+    if (wsum[0] > 0xFFFFFFFFull) invalid("stroke centerline points exceed u32 indexing");
+    tk::StrokeView sv{sels.ptr, nse,        soff.ptr, words.ptr + 2, nullptr,     0,
+                      polys.ptr, npl,       strokes.ptr, ns,         poly_n.ptr, line_off.ptr, words.ptr + 1};
+    if (npl) {
+        pts.reserve(std::max<uint64_t>(w[2], 1));
+        sv.pts = pts.ptr;
+        sv.pt_cap = w[2];
+        tk::launch_stroke_outline_count(sv, ssums.ptr, words.ptr + 3, wide.ptr + 1, st);
+        TK_CUDA(cudaMemcpyAsync(w, words.ptr, sizeof(w), cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaMemcpyAsync(wsum, wide.ptr, sizeof(wsum), cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+    }
+    const uint64_t host_lines = d.line_count, fill_lines = w[0], stroke_lines = wsum[1];
+    const uint64_t total = host_lines + fill_lines + stroke_lines;
     if (total > 0xFFFFFFFFull) invalid("line count exceeds u32 indexing");
     c->lines.reserve(total);
     if (host_lines) TK_CUDA(cudaMemcpyAsync(c->lines.ptr, d.lines, host_lines * sizeof(tk_line), cudaMemcpyHostToDevice, st));
     tk::launch_flatten_emit(els.ptr, n, offsets.ptr, words.ptr, c->paths.ptr, d.path_count, path_els.ptr, c->lines.ptr,
-                            host_lines, total, words.ptr + 1, st);
+                            host_lines, host_lines + fill_lines, words.ptr + 1, st);
+    tk::launch_stroke_emit(sv, words.ptr + 3, c->paths.ptr, c->lines.ptr, host_lines + fill_lines, total, st);
     TK_CUDA(cudaGetLastError());
     uint32_t err = 0;
     TK_CUDA(cudaMemcpyAsync(&err, words.ptr + 1, 4, cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaMemcpyAsync(c->h_paths.data(), c->paths.ptr, d.path_count * sizeof(tk_path_record),
                             cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaStreamSynchronize(st));
+    for (auto* b : {&path_els, &offsets, &sums, &words, &soff, &ssums, &poly_n, &line_off}) b->release();
     els.release();
-    path_els.release();
-    offsets.release();
-    sums.release();
-    words.release();
+    sels.release();
+    polys.release();
+    strokes.release();
+    wide.release();
+    pts.release();
     if (err) {
         std::string m = "device flattening rejected the elements:";
         if (err & tk::ERR_UNSUPPORTED) m += " bad verb, tolerance below 1e-3 px or coordinates beyond 1e6 px;";
-        if (err & tk::ERR_LINE_PATH_MISMATCH) m += " an element's path index differs from its path;";
+        if (err & tk::ERR_LINE_PATH_MISMATCH)
+            m += " an element's path or polyline index differs from its owner, or a polyline does not start with a move;";
         if (err & tk::ERR_SEGMENT_OVERFLOW) m += " lines past the counted total;";
         throw Fail{TK_E_INVALID, m};
     }

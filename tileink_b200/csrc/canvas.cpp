@@ -17,6 +17,7 @@
 #include "../../include/tileink_diff.h"
 #include "flatten_core.h"
 #include "planner.h"
+#include "stroke_core.h"
 
 namespace {
 
@@ -175,142 +176,83 @@ tk_path transform_path(const tk_path& p, const double m[6]) {
 }
 
 // --------------------------------------------------------------------------
-// Stroking with round joins and round caps: the centerline is flattened, each
-// segment is offset by +-w/2, outer joins get circular arcs, inner joins
-// pivot through the centerline vertex, and open ends get semicircular caps.
-// The outline is filled with the nonzero rule (kurbo::stroke's contract).
+// Stroking with round joins and round caps (stroke_core.h, shared with the
+// device stroker). The centerline is recorded as elements in local units:
+// a polyline starts at its first drawing element with a TK_EL_MOVE at the
+// current point (so a lone move_to strokes nothing), and a close marks it
+// closed and returns the current point to its start. Element `path` fields
+// hold the polyline index.
 // --------------------------------------------------------------------------
-struct Polyline {
-    std::vector<Pt> pts;
-    bool closed = false;
-};
-std::vector<Polyline> centerlines(const tk_path& path, double tol) {
-    std::vector<Polyline> out;
-    Pt last{0, 0};
-    auto cur = [&]() -> Polyline& { return out.back(); };
-    auto emit = [&](Pt p) {
-        if (out.empty()) out.push_back({{last}, false});
-        Pt q = cur().pts.back();
-        if (std::hypot(p.x - q.x, p.y - q.y) > 1e-9) cur().pts.push_back(p);
-        last = p;
+void record_centerlines(const tk_path& path, double tol, uint32_t stroke, std::vector<tk_flatten_el>& els,
+                        std::vector<tk_stroke_polyline>& polys) {
+    bool open = false;
+    Pt last{0, 0}, front{0, 0};
+    auto element = [&](uint32_t verb, std::initializer_list<Pt> pts) {
+        tk_flatten_el e{};
+        e.verb = verb;
+        e.path = uint32_t(polys.size() - 1);
+        e.tolerance = tol;
+        int k = 0;
+        for (const Pt& p : pts) {
+            e.p[k][0] = p.x;
+            e.p[k][1] = p.y;
+            ++k;
+        }
+        els.push_back(e);
+        ++polys.back().element_count;
+    };
+    auto begin = [&]() {
+        if (open) return;
+        polys.push_back({stroke, uint32_t(els.size()), 0u, 0u});
+        element(TK_EL_MOVE, {last});
+        front = last;
+        open = true;
     };
     for (const El& e : path.els) {
         switch (e.verb) {
-            case MOVE: out.push_back({{e.p[0]}, false}); last = e.p[0]; break;
-            case LINE: emit(e.p[0]); break;
-            case QUAD: flatten_quad(last, e.p[0], e.p[1], tol, emit); break;
-            case CUBIC: {
-                Pt c[4] = {last, e.p[0], e.p[1], e.p[2]};
-                flatten_cubic(c, tol, emit);
-                break;
-            }
+            case MOVE: open = false; last = e.p[0]; break;
+            case LINE: begin(); element(TK_EL_LINE, {last, e.p[0]}); last = e.p[0]; break;
+            case QUAD: begin(); element(TK_EL_QUAD, {last, e.p[0], e.p[1]}); last = e.p[1]; break;
+            case CUBIC: begin(); element(TK_EL_CUBIC, {last, e.p[0], e.p[1], e.p[2]}); last = e.p[2]; break;
             case CLOSE:
-                if (!out.empty()) {
-                    cur().closed = true;
-                    Pt s = cur().pts.front();
-                    if (cur().pts.size() > 1 && std::hypot(s.x - cur().pts.back().x, s.y - cur().pts.back().y) <= 1e-9)
-                        cur().pts.pop_back();
-                    last = s;
+                if (open) {
+                    polys.back().closed = 1u;
+                    last = front;
+                    open = false;
                 }
                 break;
         }
     }
-    return out;
 }
-void arc_points(Pt c, double r, double a0, double a1, double tol, std::vector<Pt>& out) {
-    // Sweep from angle a0 to a1 (signed) excluding a0, including a1.
-    double sweep = a1 - a0;
-    double step = r > tol ? 2.0 * std::acos(std::max(-1.0, 1.0 - tol / r)) : 3.2;
-    int n = std::max(1, int(std::ceil(std::fabs(sweep) / std::max(step, 1e-3))));
-    for (int i = 1; i <= n; ++i) {
-        double a = a0 + sweep * double(i) / n;
-        out.push_back({c.x + r * std::cos(a), c.y + r * std::sin(a)});
-    }
-}
-// One side of a polyline offset by h > 0 along the left normal (-dy, dx).
-// Outer joins (turning away from the normal) get a circular arc around the
-// vertex; inner joins pivot through the vertex.
-void offset_side(const std::vector<Pt>& v, bool closed, double h, double tol, std::vector<Pt>& out) {
-    size_t n = v.size();
-    size_t segs = closed ? n : n - 1;
-    auto dir = [&](size_t i) {
-        Pt a = v[i % n], b = v[(i + 1) % n];
-        double l = std::hypot(b.x - a.x, b.y - a.y);
-        return Pt{(b.x - a.x) / l, (b.y - a.y) / l};
-    };
-    auto nrm = [](Pt d) { return Pt{-d.y, d.x}; };
-    auto join = [&](Pt vertex, Pt din, Pt dout) {
-        Pt nin = nrm(din), nout = nrm(dout);
-        double cr = din.x * dout.y - din.y * dout.x;
-        if (cr < 0.0) {
-            double s0 = std::atan2(nin.y, nin.x), s1 = std::atan2(nout.y, nout.x);
-            double sw = s1 - s0;
-            while (sw > M_PI) sw -= 2 * M_PI;
-            while (sw < -M_PI) sw += 2 * M_PI;
-            arc_points(vertex, h, s0, s0 + sw, tol, out);
-        } else {
-            out.push_back(vertex);
-            out.push_back(vertex + nout * h);
+
+// The outline lines of a stroke's polylines, in the device stroker's order:
+// polyline by polyline, loop by loop, unit by unit.
+void outline_lines(const std::vector<tk_flatten_el>& els, const tk_stroke_polyline* polys, uint32_t npl,
+                   const tk_stroke_desc& S, std::vector<tk_line>& out) {
+    struct Push {
+        std::vector<tk_line>& out;
+        uint32_t path;
+        void operator()(Pt a, Pt b) {
+            out.push_back(tk_line{path, 0.0f, {float(a.x), float(a.y)}, {float(b.x), float(b.y)}});
         }
-    };
-    if (closed) {
-        Pt dl = dir(segs - 1);
-        out.push_back(v[0] + nrm(dl) * h);
-        join(v[0], dl, dir(0));
-    } else {
-        out.push_back(v[0] + nrm(dir(0)) * h);
+    } push{out, S.path};
+    tkf::Affine xf;
+    std::memcpy(xf.t, S.transform, sizeof(xf.t));
+    std::vector<Pt> v;
+    auto add = [&](Pt p) { v.push_back(p); };
+    for (uint32_t k = 0; k < npl; ++k) {
+        const tk_stroke_polyline& P = polys[k];
+        v.clear();
+        for (uint32_t e = P.element0; e < P.element0 + P.element_count; ++e) tkf::element_points(els[e], add);
+        const bool closed = P.closed != 0u;
+        const uint32_t n = tkf::dedupe_polyline(v, uint32_t(v.size()), closed);
+        const uint32_t loops = tkf::outline_loops(n, closed), units = tkf::outline_units(n, closed);
+        for (uint32_t loop = 0; loop < loops; ++loop)
+            for (uint32_t u = 0; u < units; ++u) {
+                tkf::EdgeChain<Push> chain{xf, push};
+                tkf::outline_unit(v, n, closed, loop, u, S.half_width, S.tolerance, chain);
+            }
     }
-    for (size_t i = 0; i < segs; ++i) {
-        Pt d = dir(i);
-        out.push_back(v[(i + 1) % n] + nrm(d) * h);
-        if (i + 1 < segs) join(v[(i + 1) % n], d, dir(i + 1));
-    }
-}
-tk_path stroke_path(const tk_path& path, double width, double tol) {
-    tk_path out;
-    double h = 0.5 * width;
-    auto add_loop = [&](const std::vector<Pt>& raw) {
-        std::vector<Pt> pts;
-        for (const Pt& p : raw)
-            if (pts.empty() || std::hypot(p.x - pts.back().x, p.y - pts.back().y) > 1e-9) pts.push_back(p);
-        while (pts.size() > 1 && std::hypot(pts[0].x - pts.back().x, pts[0].y - pts.back().y) <= 1e-9) pts.pop_back();
-        if (pts.size() < 3) return;
-        out.els.push_back({MOVE, {pts[0], {}, {}}});
-        for (size_t i = 1; i < pts.size(); ++i) out.els.push_back({LINE, {pts[i], {}, {}}});
-        out.els.push_back({CLOSE, {{}, {}, {}}});
-    };
-    for (const Polyline& pl : centerlines(path, tol)) {
-        const auto& v = pl.pts;
-        if (v.size() == 1) {  // dot: round caps make a disc
-            std::vector<Pt> disc{{v[0].x + h, v[0].y}};
-            arc_points(v[0], h, 0.0, 2 * M_PI, tol, disc);
-            disc.pop_back();
-            add_loop(disc);
-            continue;
-        }
-        if (pl.closed && v.size() >= 3) {
-            std::vector<Pt> left, right;
-            offset_side(v, true, h, tol, left);
-            std::vector<Pt> rv(v.rbegin(), v.rend());
-            offset_side(rv, true, h, tol, right);
-            add_loop(left);
-            add_loop(right);
-            continue;
-        }
-        std::vector<Pt> loop;
-        offset_side(v, false, h, tol, loop);
-        size_t n = v.size();
-        Pt de{v[n - 1].x - v[n - 2].x, v[n - 1].y - v[n - 2].y};
-        double ae = std::atan2(de.x, -de.y);  // angle of the left normal (-dy, dx)
-        arc_points(v[n - 1], h, ae, ae - M_PI, tol, loop);
-        std::vector<Pt> rv(v.rbegin(), v.rend());
-        offset_side(rv, false, h, tol, loop);
-        Pt ds{v[1].x - v[0].x, v[1].y - v[0].y};
-        double as = std::atan2(-ds.x, ds.y);  // angle of the right normal
-        arc_points(v[0], h, as, as - M_PI, tol, loop);
-        add_loop(loop);
-    }
-    return out;
 }
 
 // --------------------------------------------------------------------------
@@ -428,10 +370,14 @@ struct tk_canvas {
     // differentiable parameters (fills of recorded paths)
     std::vector<double> points;
     std::vector<float> colors;
-    // device flattening: fills are kept as elements, flattened at upload
+    // device flattening: fills are kept as elements and strokes as centerline
+    // elements, flattened (and stroked) at upload
     bool device_flatten = false;
     std::vector<tk_flatten_el> els;
     std::vector<uint32_t> path_els;  // per path: first element, element count
+    std::vector<tk_flatten_el> stroke_els;
+    std::vector<tk_stroke_polyline> polylines;
+    std::vector<tk_stroke_desc> strokes;
 };
 
 namespace {
@@ -496,22 +442,40 @@ void record_elements(const tk_path& path, double tol, uint32_t path_id, std::vec
     open_close();
 }
 
-int64_t push_path_with_tag(tk_canvas* c, const tk_path& src, const tk_brush_desc* brush, const double* transform,
-                           uint32_t rule, double tolerance, uint32_t tag, bool emit_command, bool device_ok = true) {
-    uint32_t line_start = uint32_t(c->lines.size());
-    uint32_t path_id = uint32_t(c->paths.size());
-    double s = double(c->scale);
+// The device transform: the canvas scale times the path's transform.
+void device_transform(const tk_canvas* c, const double* transform, double dev[6]) {
+    const double s = double(c->scale);
     double m[6] = {1, 0, 0, 1, 0, 0};
     if (transform) std::memcpy(m, transform, sizeof(m));
-    double dev[6] = {s * m[0], s * m[1], s * m[2], s * m[3], s * m[4], s * m[5]};
+    for (int k = 0; k < 6; ++k) dev[k] = s * m[k];
+}
+
+int64_t add_path(tk_canvas* c, const Box& bb, uint32_t line_start, uint32_t line_count, const tk_brush_desc* brush,
+                 uint32_t rule, uint32_t tag, bool emit_command);
+
+int64_t push_path_with_tag(tk_canvas* c, const tk_path& src, const tk_brush_desc* brush, const double* transform,
+                           uint32_t rule, double tolerance, uint32_t tag, bool emit_command) {
+    const uint32_t line_start = uint32_t(c->lines.size());
+    const uint32_t path_id = uint32_t(c->paths.size());
+    const double s = double(c->scale);
+    double dev[6];
+    device_transform(c, transform, dev);
     tk_path path = transform_path(src, dev);
     const uint32_t el0 = uint32_t(c->els.size());
-    if (c->device_flatten && device_ok) record_elements(path, tolerance * s, path_id, c->els);
+    if (c->device_flatten) record_elements(path, tolerance * s, path_id, c->els);
     else flatten_path(path, tolerance * s, path_id, c->lines);
     c->path_els.push_back(el0);
     c->path_els.push_back(uint32_t(c->els.size()) - el0);
-    uint32_t line_count = uint32_t(c->lines.size()) - line_start;
-    Box bb = path_bbox(path);
+    return add_path(c, path_bbox(path), line_start, uint32_t(c->lines.size()) - line_start, brush, rule, tag,
+                    emit_command);
+}
+
+// The path and draw records of a path whose lines are
+// lines[line_start, + line_count) (none yet when the device makes them),
+// with pixel bounds from `bb`.
+int64_t add_path(tk_canvas* c, const Box& bb, uint32_t line_start, uint32_t line_count, const tk_brush_desc* brush,
+                 uint32_t rule, uint32_t tag, bool emit_command) {
+    const uint32_t path_id = uint32_t(c->paths.size());
     tk_pixel_bounds pb{0, 0, 0, 0};
     if (!bb.empty()) pb = {int32_t(std::floor(bb.x0)), int32_t(std::floor(bb.y0)), int32_t(std::ceil(bb.x1)), int32_t(std::ceil(bb.y1))};
     // PixelBounds::tile_bbox (src/shared/bounds.rs:113-128)
@@ -715,6 +679,12 @@ int32_t tk_canvas_flatten_desc(const tk_canvas* c, tk_flatten_desc* out) {
     out->elements = c->els.data();
     out->element_count = c->els.size();
     out->path_elements = c->path_els.data();
+    out->stroke_elements = c->stroke_els.data();
+    out->stroke_element_count = c->stroke_els.size();
+    out->polylines = c->polylines.data();
+    out->polyline_count = uint32_t(c->polylines.size());
+    out->stroke_count = uint32_t(c->strokes.size());
+    out->strokes = c->strokes.data();
     return TK_OK;
 }
 void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul) { c->clear = premul; }
@@ -727,11 +697,40 @@ int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_de
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, double width,
                               const double* transform, double tolerance) {
     if (!c || !path || !(width > 0.0) || !(tolerance > 0.0)) return -1;
-    // Strokes are outlined in the path's local space (kurbo::stroke before
-    // the transform, src/canvas/primitives/paths.rs:24-48).
-    tk_path outline = stroke_path(*path, width, tolerance);
-    // stroke outlines are polygons from the host stroker: they stay host lines
-    return push_path_with_tag(c, outline, brush, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_BRUSH, true, false);
+    // Strokes are outlined in the path's local space, then transformed
+    // (kurbo::stroke before the transform, src/canvas/primitives/paths.rs:24-48).
+    tk_stroke_desc S{};
+    S.path = uint32_t(c->paths.size());
+    S.half_width = 0.5 * width;
+    S.tolerance = tolerance;
+    device_transform(c, transform, S.transform);
+    // Bounds: the transformed centerline's tight box grown by the half width
+    // and the flattening tolerance, stretched by the transform; it holds the
+    // outline, which lies within half_width of the flattened centerline.
+    Box bb = path_bbox(transform_path(*path, S.transform));
+    if (!bb.empty()) {
+        const double g = (S.half_width + tolerance) * tkf::max_stretch(S.transform) * (1.0 + 1e-12) + 1e-6;
+        bb.x0 -= g;
+        bb.y0 -= g;
+        bb.x1 += g;
+        bb.y1 += g;
+    }
+    const uint32_t line_start = uint32_t(c->lines.size());
+    if (c->device_flatten) {
+        S.polyline0 = uint32_t(c->polylines.size());
+        record_centerlines(*path, tolerance, uint32_t(c->strokes.size()), c->stroke_els, c->polylines);
+        S.polyline_count = uint32_t(c->polylines.size()) - S.polyline0;
+        c->strokes.push_back(S);
+    } else {
+        std::vector<tk_flatten_el> els;
+        std::vector<tk_stroke_polyline> polys;
+        record_centerlines(*path, tolerance, 0u, els, polys);
+        outline_lines(els, polys.data(), uint32_t(polys.size()), S, c->lines);
+    }
+    c->path_els.push_back(uint32_t(c->els.size()));  // no fill elements
+    c->path_els.push_back(0u);
+    return add_path(c, bb, line_start, uint32_t(c->lines.size()) - line_start, brush, TK_FILL_NONZERO, TK_DRAW_BRUSH,
+                    true);
 }
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform, uint32_t rule,
                                   double tolerance) {

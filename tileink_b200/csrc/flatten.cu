@@ -52,24 +52,11 @@ __device__ bool element_ok(const tk_flatten_el& e) {
     return true;
 }
 
-template <class Emit>
-__device__ void flatten_element(const tk_flatten_el& e, Emit& emit) {
-    const Pt from{e.p[0][0], e.p[0][1]};
-    if (e.verb == TK_EL_LINE) {
-        emit(Pt{e.p[1][0], e.p[1][1]});
-    } else if (e.verb == TK_EL_QUAD) {
-        tkf::flatten_quad(from, Pt{e.p[1][0], e.p[1][1]}, Pt{e.p[2][0], e.p[2][1]}, e.tolerance, emit);
-    } else if (e.verb == TK_EL_CUBIC) {
-        const Pt c[4] = {from, Pt{e.p[1][0], e.p[1][1]}, Pt{e.p[2][0], e.p[2][1]}, Pt{e.p[3][0], e.p[3][1]}};
-        tkf::flatten_cubic(c, e.tolerance, emit);
-    }
-}
-
 __global__ void k_flatten_count(const tk_flatten_el* __restrict__ els, uint64_t n, uint32_t* counts, uint32_t* error) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const tk_flatten_el e = els[i];
         CountEmit c{Pt{e.p[0][0], e.p[0][1]}, 0u};
-        if (element_ok(e)) flatten_element(e, c);
+        if (element_ok(e)) tkf::element_points(e, c);
         else atomicOr(error, ERR_UNSUPPORTED);
         counts[i] = c.n;
     }
@@ -171,23 +158,27 @@ __global__ void k_flatten_emit(const tk_flatten_el* __restrict__ els, uint64_t n
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const tk_flatten_el e = els[i];
         WriteEmit w{Pt{e.p[0][0], e.p[0][1]}, lines, line_base + offsets[i], line_end, e.path, error};
-        if (element_ok(e)) flatten_element(e, w);
+        if (element_ok(e)) tkf::element_points(e, w);
     }
 }
 
 }  // namespace
 
-void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
-                          uint32_t* total, uint32_t* error, cudaStream_t st) {
+void launch_exclusive_scan(uint32_t* v, uint64_t n, uint32_t* block_sums, uint32_t* total, cudaStream_t st) {
     if (n == 0) {
         cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
         return;
     }
-    k_flatten_count<<<148 * 16, 128, 0, st>>>(els, n, counts, error);
     const uint32_t blocks = uint32_t((n + kScanBlock - 1) / kScanBlock);
-    k_scan_local<<<blocks, kScanBlock, 0, st>>>(counts, n, block_sums);
+    k_scan_local<<<blocks, kScanBlock, 0, st>>>(v, n, block_sums);
     k_scan_sums<<<1, kScanBlock, 0, st>>>(block_sums, blocks, total);
-    k_scan_add<<<blocks, kScanBlock, 0, st>>>(counts, n, block_sums);
+    k_scan_add<<<blocks, kScanBlock, 0, st>>>(v, n, block_sums);
+}
+
+void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
+                          uint32_t* total, uint32_t* error, cudaStream_t st) {
+    if (n) k_flatten_count<<<148 * 16, 128, 0, st>>>(els, n, counts, error);
+    launch_exclusive_scan(counts, n, block_sums, total, st);
 }
 
 void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* offsets, const uint32_t* total,

@@ -12,6 +12,8 @@
 #pragma once
 #include <math.h>
 
+#include "../../include/tileink.h"
+
 #ifdef __CUDACC__
 #define TK_HD __host__ __device__
 #else
@@ -20,7 +22,7 @@
 
 namespace tkf {
 
-struct Pt {
+struct alignas(16) Pt {
     double x, y;
 };
 TK_HD inline Pt operator+(Pt a, Pt b) { return {a.x + b.x, a.y + b.y}; }
@@ -126,6 +128,23 @@ TK_HD void flatten_cubic(const P c[4], double tol, Emit&& emit) {
 TK_HD inline bool keep_edge(Pt a, Pt b) {
     double dx = a.x - b.x, dy = a.y - b.y;
     return dx * dx + dy * dy > 1.0e-12 * 1.0e-12;
+}
+
+// The points one element contributes to its contour, its start point
+// excluded: a move's point, a line's end, or the flattened curve.
+template <class Emit>
+TK_HD void element_points(const tk_flatten_el& e, Emit& emit) {
+    const Pt from{e.p[0][0], e.p[0][1]};
+    if (e.verb == TK_EL_MOVE) {
+        emit(from);
+    } else if (e.verb == TK_EL_LINE) {
+        emit(Pt{e.p[1][0], e.p[1][1]});
+    } else if (e.verb == TK_EL_QUAD) {
+        flatten_quad(from, Pt{e.p[1][0], e.p[1][1]}, Pt{e.p[2][0], e.p[2][1]}, e.tolerance, emit);
+    } else if (e.verb == TK_EL_CUBIC) {
+        const Pt c[4] = {from, Pt{e.p[1][0], e.p[1][1]}, Pt{e.p[2][0], e.p[2][1]}, Pt{e.p[3][0], e.p[3][1]}};
+        flatten_cubic(c, e.tolerance, emit);
+    }
 }
 
 }  // namespace tkf

@@ -5,6 +5,10 @@
 
 #include "../../include/tileink.h"
 
+namespace tkf {
+struct Pt;
+}
+
 namespace tk {
 
 // Error bits raised by kernels into a device word.
@@ -145,6 +149,37 @@ void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* o
                          tk_path_record* paths, uint32_t path_count, const uint32_t* path_els, tk_line* lines,
                          uint64_t line_base, uint64_t line_end, uint32_t* error, cudaStream_t st);
 size_t flatten_block_sums(uint64_t n);
+// Exclusive scan of n u32 values in place (1024 per block; block totals in
+// block_sums, flatten_block_sums(n) words); `total` receives the sum.
+void launch_exclusive_scan(uint32_t* v, uint64_t n, uint32_t* block_sums, uint32_t* total, cudaStream_t st);
+
+// Device stroking (stroke.cu). launch_stroke_count: raw centerline points per
+// stroke element, scanned into exclusive offsets (u32 total, plus the exact
+// u64 sum to catch wrap-around). launch_stroke_outline_count: writes the
+// points, cleans each polyline and counts its outline lines into line_off,
+// scanned into exclusive offsets. launch_stroke_emit: writes the lines and
+// the stroked paths' line ranges.
+struct StrokeView {
+    const tk_flatten_el* els;
+    uint64_t n_els;
+    const uint32_t* offsets;   // per element: first raw point
+    const uint32_t* pt_total;  // raw points
+    tkf::Pt* pts;
+    uint64_t pt_cap;
+    const tk_stroke_polyline* polys;
+    uint32_t npl;
+    const tk_stroke_desc* strokes;
+    uint32_t n_strokes;
+    uint32_t* poly_n;    // per polyline: points kept
+    uint32_t* line_off;  // per polyline: lines, then their exclusive offsets
+    uint32_t* error;
+};
+void launch_stroke_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
+                         uint32_t* total, unsigned long long* total64, uint32_t* error, cudaStream_t st);
+void launch_stroke_outline_count(const StrokeView& v, uint32_t* block_sums, uint32_t* line_total,
+                                 unsigned long long* line_total64, cudaStream_t st);
+void launch_stroke_emit(const StrokeView& v, const uint32_t* line_total, tk_path_record* paths, tk_line* lines,
+                        uint64_t line_base, uint64_t line_end, cudaStream_t st);
 
 // Differentiable rendering (diff.cu): float forward and adjoint.
 void launch_diff_fine_fwd(const SceneView& s, const PassView& p, const float4* colp, float4* layer, cudaStream_t st);
