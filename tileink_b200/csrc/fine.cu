@@ -260,6 +260,52 @@ __device__ void stage_rows(FineSmem& S, uint32_t total) {
     }
 }
 
+// fill_alpha_at's coverage sum (shared/coverage.hlsli:34-51) of staged fill
+// i at pixel (lx, ly): base + running + partial over the row's crossing
+// entries in segment order.
+__device__ __forceinline__ float staged_coverage(const FineSmem& S, uint32_t i, uint32_t lx, uint32_t ly) {
+    float running = 0.0f, partial = 0.0f;
+    const float2* row = S.ent[ly];
+    const float2 rb = S.rb[i][ly];
+    const uint32_t kk = __float_as_uint(rb.y);
+    for (uint32_t k = kk & 0xFFFFu, k1 = kk >> 16; k < k1; ++k) {
+        const float2 e = row[k];
+        const uint32_t pk = __float_as_uint(e.y);
+        const uint32_t plo = pk & 31u, phi = (pk >> 5) & 31u;
+        if (lx >= phi) running += e.x;
+        if (lx >= plo && lx < phi) {
+            if (!(pk & kEntSlow)) {
+                partial += S.prod[(pk >> 16) + lx - plo];
+            } else {
+                const RowParts q = staged_row_parts(S, pk >> 16, ly);
+                partial += segment_area_at(q.xmin, q.xmax, lx) * q.dy;
+            }
+        }
+    }
+    return rb.x + running + partial;
+}
+
+// Paints a fill's masked coverage over px (the brush branch of
+// fine/interpreter.hlsli's fill handling, fine/draw.hlsli:16-21).
+__device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, uint32_t i, uint32_t masked,
+                                           uint32_t gx, uint32_t gy, float4& px) {
+    const uint32_t paint = S.paint[i];
+    if (paint != kGradient) {
+        if (masked == 255u && premul_u8_is_opaque(paint)) {
+            px = S.pfull[i];
+        } else {
+            // scale_premul_u8_to_unorm with the channels staged as floats
+            const float sc = float(masked) * (1.0f / 65025.0f);
+            const float4 c = S.pcf[i];
+            if (c.w != 0.0f) px = src_over_premul_unorm(px, make_float4(c.x * sc, c.y * sc, c.z * sc, c.w * sc));
+        }
+    } else {
+        const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
+        if (masked == 255u && premul_u8_is_opaque(g)) px = rgba8_to_unorm(g);
+        else px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(g, masked));
+    }
+}
+
 __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const tk_line_segment* __restrict__ segments, const tk_draw_record* __restrict__ draws,
@@ -321,7 +367,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 }
                 n = s1 - s0;
                 if (n == 0u) S.ualpha[tid] = coverage_to_alpha(float(int32_t(a.y)), b.x);
-                if (a.x == TK_PTCL_FILL) cls = kClsFill;
+                if (a.x == TK_PTCL_FILL && n != 0u) cls = kClsFill;  // row sums staged below
             }
             S.nseg[tid] = n;
             if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH) {
@@ -421,6 +467,14 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 done = true;
                 break;
             }
+            if (cls == kClsFill && mode != TK_TILE_KIND_COLOR && !big) {
+                // the common record: a path fill with segments in the tile
+                const uint32_t alpha = coverage_to_alpha(staged_coverage(S, i, lx, ly), S.rec_a[i].z);
+                const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
+                if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
+                ++i;
+                continue;
+            }
             const uint2 qb = S.rec_b[i];
             if (cls == kClsBatch) {
                 // A new reference batch dispatch: store / reload the target
@@ -476,25 +530,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 if (S.nseg[i] == 0u) {
                     alpha = S.ualpha[i];
                 } else if (!big) {
-                    float running = 0.0f, partial = 0.0f;
-                    const float2* row = S.ent[ly];
-                    const float2 rb = S.rb[i][ly];
-                    const uint32_t kk = __float_as_uint(rb.y);
-                    for (uint32_t k = kk & 0xFFFFu, k1 = kk >> 16; k < k1; ++k) {
-                        const float2 e = row[k];
-                        const uint32_t pk = __float_as_uint(e.y);
-                        const uint32_t plo = pk & 31u, phi = (pk >> 5) & 31u;
-                        if (lx >= phi) running += e.x;
-                        if (lx >= plo && lx < phi) {
-                            if (!(pk & kEntSlow)) {
-                                partial += S.prod[(pk >> 16) + lx - plo];
-                            } else {
-                                const RowParts q = staged_row_parts(S, pk >> 16, ly);
-                                partial += segment_area_at(q.xmin, q.xmax, lx) * q.dy;
-                            }
-                        }
-                    }
-                    alpha = coverage_to_alpha(rb.x + running + partial, qa.z);
+                    alpha = coverage_to_alpha(staged_coverage(S, i, lx, ly), qa.z);
                 } else {
                     // more segments than one chunk holds: per-pixel evaluation
                     // of fill_alpha_at over 128-segment slices
@@ -549,22 +585,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                     const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
                     if (masked != 0u) {
                         if (tag == TK_PTCL_PATH_GLYPH) atomicOr(error, ERR_UNSUPPORTED);
-                        const uint32_t paint = S.paint[i];
-                        if (paint != kGradient) {
-                            if (masked == 255u && premul_u8_is_opaque(paint)) {
-                                px = S.pfull[i];
-                            } else {
-                                // scale_premul_u8_to_unorm with the channels staged as floats
-                                const float sc = float(masked) * (1.0f / 65025.0f);
-                                const float4 c = S.pcf[i];
-                                if (c.w != 0.0f)
-                                    px = src_over_premul_unorm(px, make_float4(c.x * sc, c.y * sc, c.z * sc, c.w * sc));
-                            }
-                        } else {
-                            const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
-                            if (masked == 255u && premul_u8_is_opaque(g)) px = rgba8_to_unorm(g);
-                            else px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(g, masked));
-                        }
+                        paint_fill(S, P, i, masked, gx, gy, px);
                     }
                 }
             }
