@@ -435,14 +435,16 @@ def main():
                        "paths": args.paths or 50000, "parallelism": f"replicas x{world}",
                        "l2": "inputs > L2 (lines %.1f GB), no flush" % (L * 24 / 1e9),
                        "segment_plan": "device"},
-            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
-                    "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms,
-                    "input": "host-flattened lines (the reference's Line records)"},
-            "e2e_device_flatten": {"value": world * 1000.0 / e2e_flat_ms, "unit": UNIT,
-                                   "h2d_bytes_per_step": int(bytes_in_flat), "d2h_bytes_per_step": int(bytes_out),
-                                   "ms_per_step": e2e_flat_ms,
-                                   "input": "fills and stroke centerlines as Bezier elements, flattened "
-                                            "and stroked on the GPU at upload"},
+            # the headline: the recorded Canvas (fills and stroke centerlines as
+            # Bezier elements) uploaded, flattened, stroked, rendered and read
+            # back every step
+            "e2e": {"value": world * 1000.0 / e2e_flat_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in_flat),
+                    "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_flat_ms,
+                    "input": "fills and stroke centerlines as Bezier elements, flattened and stroked on the GPU "
+                             "at upload"},
+            "e2e_host_lines": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
+                               "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms,
+                               "input": "host-flattened lines (the reference's Line records)"},
             "gpu_launches": launches_per_frame * args.steps,
             "roofline": roof,
             "stage_ms": stage_ms,

@@ -56,6 +56,26 @@ struct DBuf {
     }
 };
 
+// Scratch of device flattening and stroking, kept between uploads (grow-only)
+// so that a scene re-uploaded every frame does not allocate.
+struct FlattenScratch {
+    DBuf<tk_flatten_el> els, sels;
+    DBuf<uint32_t> path_els, offsets, sums, words, soff, ssums, poly_n, line_off;
+    DBuf<tk_stroke_polyline> polys;
+    DBuf<tk_stroke_desc> strokes;
+    DBuf<unsigned long long> wide;
+    DBuf<tkf::Pt> pts;
+    void release() {
+        for (auto* b : {&path_els, &offsets, &sums, &words, &soff, &ssums, &poly_n, &line_off}) b->release();
+        els.release();
+        sels.release();
+        polys.release();
+        strokes.release();
+        wide.release();
+        pts.release();
+    }
+};
+
 struct Pass {
     uint32_t order0 = 0, draw_n = 0, batch0 = 0, batch_n = 0;
     std::vector<tk::PassBatch> batches;
@@ -118,7 +138,7 @@ struct tk_ctx {
     DBuf<int32_t> backdrops;
     DBuf<uint32_t> counts, cursors, bumps, misc;  // misc: [0] error [1] ticket [2] seg total [3] ptcl total
     DBuf<tk_segment_range> ranges;
-    DBuf<tk_line_segment> segments;
+    DBuf<tk::SegmentRec> segments;
     uint64_t segment_needed = 0;  // device plan: total from the last frame
     DBuf<uint32_t> image, temp;
     std::vector<DBuf<uint32_t>> surfaces;
@@ -145,6 +165,7 @@ struct tk_ctx {
     std::vector<cudaEvent_t> ev_pool;
     size_t ev_used = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+    FlattenScratch flat;
 };
 
 namespace {
@@ -682,12 +703,14 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     if (nse > 0xFFFFFFFFull) invalid("stroke element count exceeds u32 indexing");
     cudaStream_t st = c->stream;
     const uint64_t n = fl.element_count;
-    DBuf<tk_flatten_el> els, sels;
-    DBuf<uint32_t> path_els, offsets, sums, words, soff, ssums, poly_n, line_off;
-    DBuf<tk_stroke_polyline> polys;
-    DBuf<tk_stroke_desc> strokes;
-    DBuf<unsigned long long> wide;
-    DBuf<tkf::Pt> pts;
+    FlattenScratch& F = c->flat;
+    auto &els = F.els, &sels = F.sels;
+    auto &path_els = F.path_els, &offsets = F.offsets, &sums = F.sums, &words = F.words, &soff = F.soff,
+         &ssums = F.ssums, &poly_n = F.poly_n, &line_off = F.line_off;
+    auto& polys = F.polys;
+    auto& strokes = F.strokes;
+    auto& wide = F.wide;
+    auto& pts = F.pts;
     upload(els, fl.elements, n, st);
     upload(path_els, fl.path_elements, 2ull * d.path_count, st);
     upload(sels, fl.stroke_elements, nse, st);
@@ -737,13 +760,6 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     TK_CUDA(cudaMemcpyAsync(c->h_paths.data(), c->paths.ptr, d.path_count * sizeof(tk_path_record),
                             cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaStreamSynchronize(st));
-    for (auto* b : {&path_els, &offsets, &sums, &words, &soff, &ssums, &poly_n, &line_off}) b->release();
-    els.release();
-    sels.release();
-    polys.release();
-    strokes.release();
-    wide.release();
-    pts.release();
     if (err) {
         std::string m = "device flattening rejected the elements:";
         if (err & tk::ERR_UNSUPPORTED) m += " bad verb, tolerance below 1e-3 px or coordinates beyond 1e6 px;";
@@ -1023,6 +1039,7 @@ void tk_ctx_destroy(tk_ctx* c) {
     c->emit_order.release();
     drop_graph(c);
     c->d_scenes.release(); c->bin_scene.release(); c->tile_scene.release();
+    c->flat.release();
     DiffState& D = c->diff;
     D.colp.release(); D.target.release(); D.layer.release(); D.t1.release(); D.blurred.release(); D.gI.release();
     D.d0.release(); D.d1.release(); D.scratch.release(); D.line_acc.release(); D.color_acc.release();
@@ -1101,6 +1118,7 @@ int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, 
         const void* src = nullptr;
         size_t n = 0;
         std::vector<uint32_t> kinds;
+        bool segment_records = false;  // 32-byte device records -> 20-byte LineSegments
         switch (stage) {
             case TK_STAGE_COUNTS: src = c->counts.ptr; n = c->pool_len * 4; break;
             case TK_STAGE_BACKDROPS: src = c->backdrops.ptr; n = c->pool_len * 4; break;
@@ -1110,6 +1128,7 @@ int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, 
                 uint64_t cnt = device_plan ? (c->segment_needed ? c->segment_needed - 1 : 0) : c->host_segment_capacity;
                 src = c->segments.ptr;
                 n = cnt * sizeof(tk_line_segment);
+                segment_records = true;
                 break;
             }
             case TK_STAGE_IMAGE: src = c->image.ptr; n = size_t(c->width) * c->height * 4; break;
@@ -1138,8 +1157,16 @@ int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, 
         if (needed) *needed = n;
         if (!dst) return;
         size_t k = std::min(n, bytes);
-        if (!kinds.empty()) std::memcpy(dst, kinds.data(), k);
-        else if (k) TK_CUDA(cudaMemcpy(dst, src, k, cudaMemcpyDeviceToHost));
+        if (!kinds.empty()) {
+            std::memcpy(dst, kinds.data(), k);
+        } else if (segment_records) {
+            const size_t rows = k / sizeof(tk_line_segment);  // whole records only
+            if (rows)
+                TK_CUDA(cudaMemcpy2D(dst, sizeof(tk_line_segment), src, sizeof(tk::SegmentRec), sizeof(tk_line_segment),
+                                     rows, cudaMemcpyDeviceToHost));
+        } else if (k) {
+            TK_CUDA(cudaMemcpy(dst, src, k, cudaMemcpyDeviceToHost));
+        }
     });
 }
 

@@ -43,16 +43,15 @@ struct DiffSmem {
 
 // Signed area A of one fill record at tile pixel (lx, ly): fill_alpha_at over
 // the record's segments, staged through shared memory in slices.
-__device__ float record_area(DiffSmem& S, const tk_line_segment* __restrict__ segments, uint32_t s0, uint32_t s1,
+__device__ float record_area(DiffSmem& S, const SegmentRec* __restrict__ segments, uint32_t s0, uint32_t s1,
                              int32_t backdrop, uint32_t lx, uint32_t ly) {
     float base = float(backdrop), running = 0.0f, partial = 0.0f;
     for (uint32_t c0 = s0; c0 < s1; c0 += kDiffSegStage) {
         const uint32_t m = min(kDiffSegStage, s1 - c0);
         __syncthreads();
         for (uint32_t j = threadIdx.x; j < m; j += kDiffThreads) {
-            const float* g = reinterpret_cast<const float*>(segments + c0 + j);
-            S.sgp[j] = make_float4(__ldg(g), __ldg(g + 1), __ldg(g + 2), __ldg(g + 3));
-            S.sgy[j] = __ldg(g + 4);
+            S.sgp[j] = __ldg(reinterpret_cast<const float4*>(segments + c0 + j));
+            S.sgy[j] = __ldg(&segments[c0 + j].y_edge);
         }
         __syncthreads();
         for (uint32_t j = 0; j < m; ++j) {
@@ -75,7 +74,7 @@ __device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a
 // Forward: the float layer image of one target pass.
 __global__ void __launch_bounds__(kDiffThreads)
     k_diff_fine_fwd(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
-                    const tk_line_segment* __restrict__ segments, const float4* __restrict__ colp, float4* layer,
+                    const SegmentRec* __restrict__ segments, const float4* __restrict__ colp, float4* layer,
                     uint32_t width, uint32_t height, uint32_t tw, uint32_t* error) {
     __shared__ DiffSmem S;
     const uint32_t tile = blockIdx.x;
@@ -235,7 +234,7 @@ __device__ float2 segment_boundary_sums(const float* __restrict__ gA, float4 q, 
 // `scratch`), then the records in reverse.
 __global__ void __launch_bounds__(kDiffThreads)
     k_diff_fine_bwd(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
-                    const tk_line_segment* __restrict__ segments, const uint32_t* __restrict__ seg_line,
+                    const SegmentRec* __restrict__ segments, const uint32_t* __restrict__ seg_line,
                     const tk_line* __restrict__ lines, const float4* __restrict__ colp,
                     const float4* __restrict__ dlayer, float2* scratch, float2* line_acc, float* color_acc,
                     uint32_t width, uint32_t height, uint32_t tw, uint32_t* error) {
@@ -295,8 +294,7 @@ __global__ void __launch_bounds__(kDiffThreads)
             if (s != 0.0f) atomicAdd(color_acc + uint64_t(q.color) * 5u + tid, s);
         }
         for (uint32_t j = q.segment_start + tid; j < q.segment_end; j += kDiffThreads) {
-            const float* sg = reinterpret_cast<const float*>(segments + j);
-            const float4 seg = make_float4(__ldg(sg), __ldg(sg + 1), __ldg(sg + 2), __ldg(sg + 3));
+            const float4 seg = __ldg(reinterpret_cast<const float4*>(segments + j));
             const uint32_t li = seg_line[j];
             const tk_line ln = lines[li];
             const float2 P0 = make_float2(ln.p0[0] - float(ox), ln.p0[1] - float(oy));

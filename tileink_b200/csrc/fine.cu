@@ -308,7 +308,7 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
 
 __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
-           const tk_line_segment* __restrict__ segments, const tk_draw_record* __restrict__ draws,
+           const SegmentRec* __restrict__ segments, const tk_draw_record* __restrict__ draws,
            const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
            const uint32_t* __restrict__ tile_scene) {
@@ -432,12 +432,10 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                     if (S.off[mid] <= sg) lo = mid;
                     else hi = mid;
                 }
-                const float* g = reinterpret_cast<const float*>(segments + S.rec_a[lo].w + (sg - S.off[lo]));
-                const float p0x = __ldg(g), p0y = __ldg(g + 1), p1x = __ldg(g + 2), p1y = __ldg(g + 3);
-                const float ye = __ldg(g + 4);
-                const float delta_y = p1y - p0y;
-                S.sgp[sg] = make_float4(p0x, p0y, p1x, p1y);
-                S.sgx[sg] = make_float2(ye, delta_y != 0.0f ? (p1x - p0x) / delta_y : 0.0f);
+                const float4* g = reinterpret_cast<const float4*>(segments + S.rec_a[lo].w + (sg - S.off[lo]));
+                S.sgp[sg] = __ldg(g);
+                const float4 e = __ldg(g + 1);  // y_edge, slope
+                S.sgx[sg] = make_float2(e.x, e.y);
             }
             __syncthreads();
             stage_rows(S, total);
@@ -539,9 +537,8 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                         const uint32_t m = min(kSegBudget, qb.x - c0);
                         __syncthreads();
                         for (uint32_t j = tid; j < m; j += kFineThreads) {
-                            const float* g = reinterpret_cast<const float*>(segments + c0 + j);
-                            S.sgp[j] = make_float4(__ldg(g), __ldg(g + 1), __ldg(g + 2), __ldg(g + 3));
-                            S.sgx[j] = make_float2(__ldg(g + 4), 0.0f);
+                            S.sgp[j] = __ldg(reinterpret_cast<const float4*>(segments + c0 + j));
+                            S.sgx[j] = make_float2(__ldg(&segments[c0 + j].y_edge), 0.0f);
                         }
                         __syncthreads();
                         for (uint32_t j = 0; j < m; ++j) {

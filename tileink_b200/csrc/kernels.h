@@ -31,6 +31,18 @@ struct PassBatch {
     uint32_t batch_id, layer_start, layer_end, pad;
 };
 
+// A tile segment as the device stores it: the LineSegment fields
+// (src/shared/line_seg.rs:1-9) padded to one 32-byte sector, so that every
+// segment write covers whole sectors (20-byte records left partly written
+// sectors at the edges of short tile ranges, which HBM had to read back), plus
+// the slope (p1x - p0x) / (p1y - p0y) (0 when p1y == p0y) that fine raster
+// needs per segment. Debug readback strips it to the 20-byte record.
+struct alignas(32) SegmentRec {
+    float p0x, p0y, p1x, p1y, y_edge, slope;
+    uint32_t pad[2];
+};
+static_assert(sizeof(SegmentRec) == 32, "one sector per segment");
+
 struct SceneView {
     const tk_line* lines;
     uint64_t line_count;
@@ -50,7 +62,7 @@ struct SceneView {
     tk_segment_range* ranges;
     uint32_t* cursors;
     uint64_t pool_len;
-    tk_line_segment* segments;
+    SegmentRec* segments;
     uint64_t segment_capacity;
     uint32_t* error;
     uint32_t* seg_line;  // optional: line index of every emitted segment

@@ -145,20 +145,44 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t stride = p.tile_x1 - p.tile_x0;
     const uint32_t n = it.rows * stride;
     const uint64_t e0 = uint64_t(p.data_offset) + uint64_t(it.row0) * stride;
-    for (uint32_t i = tid; i < n; i += kScanThreads) {
-        s_cnt[i] = counts[e0 + i];
-        s_bd[i] = backdrops[e0 + i];
+    // coalesced loads, eight of a thread's in flight before the first is used
+#pragma unroll
+    for (int j0 = 0; j0 < kScanPerThread; j0 += 8) {
+        uint32_t vc[8];
+        int32_t vb[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t i = tid + uint32_t(j0 + j) * kScanThreads;
+            vc[j] = i < n ? counts[e0 + i] : 0u;
+            vb[j] = i < n ? backdrops[e0 + i] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t i = tid + uint32_t(j0 + j) * kScanThreads;
+            if (i < n) {
+                s_cnt[i] = vc[j];
+                s_bd[i] = vb[j];
+            }
+        }
     }
     __syncthreads();
-    // thread-local sums over elements [tid*16, tid*16+16)
+    // thread-local sums over elements [tid*16, tid*16+16); rows start at
+    // multiples of stride, the first at or after lo found with one division
+    // (n == 0 when stride == 0, and then no element is visited)
     const uint32_t lo = tid * kScanPerThread;
+    const uint32_t row_start0 = stride ? (lo + stride - 1u) / stride * stride : 0u;
     uint32_t csum = 0u, bf = 0u, bsum = 0u;
+    uint32_t row_start = row_start0;
 #pragma unroll
     for (int j = 0; j < kScanPerThread; ++j) {
         uint32_t i = lo + j;
         if (i < n) {
             csum += s_cnt[i];
-            if (i % stride == 0u) { bf = 1u; bsum = 0u; }
+            if (i == row_start) {
+                bf = 1u;
+                bsum = 0u;
+                row_start += stride;
+            }
             bsum += uint32_t(s_bd[i]);
         }
     }
@@ -217,6 +241,7 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t prefix = s_prefix;
     uint32_t run = prefix + ecount;
     uint32_t brun = bexcl;
+    row_start = row_start0;
 #pragma unroll
     for (int j = 0; j < kScanPerThread; ++j) {
         uint32_t i = lo + j;
@@ -224,7 +249,10 @@ __global__ void __launch_bounds__(kScanThreads)
             uint32_t c = s_cnt[i];
             s_cnt[i] = run;  // exclusive start
             run += c;
-            if (i % stride == 0u) brun = 0u;
+            if (i == row_start) {
+                brun = 0u;
+                row_start += stride;
+            }
             brun += uint32_t(s_bd[i]);
             s_bd[i] = int32_t(brun);
         }
@@ -260,7 +288,7 @@ __global__ void k_path_totals(tk_path_record* paths, uint32_t path_count, const 
 }
 
 __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
-                            uint32_t path_count, uint32_t* cursors, tk_line_segment* segments, uint64_t capacity,
+                            uint32_t path_count, uint32_t* cursors, SegmentRec* segments, uint64_t capacity,
                             uint32_t* error, uint32_t* seg_line, const uint32_t* __restrict__ order,
                             uint32_t* ticket) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -299,22 +327,29 @@ __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_rec
                         off = scan_tile_offset(s, tx, ty);
                     }
                 }
+                // A path's cursors are read and written by its warp alone;
+                // __syncwarp orders the lanes' accesses, so they can be plain
+                // (L1-cached) loads and stores. The cursor load is issued
+                // first and the clipped segment computed while it is in flight.
                 uint32_t group = __match_any_sync(0xffffffffu, off);
                 uint32_t base = 0;
-                if (emitting) base = *((volatile uint32_t*)(cursors + off));
+                if (emitting) base = cursors[off];
+                tk_line_segment seg{};
+                float slope = 0.0f;
+                if (emitting) {
+                    seg = clipped_segment(s, i, z, tx, ty);
+                    const float delta_y = seg.p1y - seg.p0y;
+                    slope = delta_y != 0.0f ? (seg.p1x - seg.p0x) / delta_y : 0.0f;
+                }
                 __syncwarp();
                 if (emitting) {
                     uint32_t leader = __ffs(group) - 1u;
-                    if (lane == leader) *((volatile uint32_t*)(cursors + off)) = base + __popc(group);
+                    if (lane == leader) cursors[off] = base + __popc(group);
                     uint32_t slot = base + __popc(group & lt_mask);
                     if (slot < capacity) {
-                        tk_line_segment seg = clipped_segment(s, i, z, tx, ty);
-                        float* dst = reinterpret_cast<float*>(segments + slot);
-                        dst[0] = seg.p0x;
-                        dst[1] = seg.p0y;
-                        dst[2] = seg.p1x;
-                        dst[3] = seg.p1y;
-                        dst[4] = seg.y_edge;
+                        float4* dst = reinterpret_cast<float4*>(segments + slot);
+                        dst[0] = make_float4(seg.p0x, seg.p0y, seg.p1x, seg.p1y);
+                        dst[1] = make_float4(seg.y_edge, slope, 0.0f, 0.0f);
                         if (seg_line) seg_line[slot] = p.line_start + l;
                     } else {
                         atomicOr(error, ERR_SEGMENT_OVERFLOW);
