@@ -469,7 +469,7 @@ int32_t tk_autotune(tk_ctx* ctx, uint32_t iterations, tk_tune_result* out);
  * totals) plus the row-wise backdrop cumsum, on DEVICE buffers the caller
  * owns (`d_*`, pool_len elements each; d_bumps path_count elements) and
  * `paths` on the host. It makes no device allocation and frees nothing: its
- * look-back descriptors, work items, copy of `paths` and counter words live
+ * per-item sums and prefixes, work items, copy of `paths` and counter words live
  * in one fixed array of TK_NOALLOC_SCRATCH_BYTES in device memory, one per
  * device. For callers that cannot allocate: an application whose own
  * allocator has reserved the device's memory, where cudaMalloc fails at an

@@ -568,8 +568,8 @@ void scan_phase(tk_ctx* c) {
     const uint32_t device_base = 0u;  // Canvas segment slices start at 0 (canvas/paths.rs:117)
     {
         StageMark m(c, 2);
-        tk::launch_pool_scan(s, c->items.ptr, uint32_t(c->h_items.size()), c->item_desc.ptr, c->misc.ptr + 1,
-                             device_plan, device_base, c->misc.ptr + 2, st);
+        tk::launch_pool_scan(s, c->items.ptr, uint32_t(c->h_items.size()), c->item_desc.ptr, device_plan, device_base,
+                             c->misc.ptr + 2, st);
         tk::launch_path_totals(s, c->bumps.ptr, device_plan, c->misc.ptr + 2, st);
     }
     if (device_plan && c->segment_needed == 0) {
@@ -1239,8 +1239,7 @@ int32_t tk_stage_scan_prefix(tk_ctx* c, const uint32_t* counts, uint64_t pool_le
         s.cursors = d_cursors.ptr;
         s.pool_len = pool_len;
         s.error = d_misc.ptr;
-        tk::launch_pool_scan(s, d_items.ptr, uint32_t(items.size()), d_desc.ptr, d_misc.ptr + 1, false, 0u,
-                             d_misc.ptr + 2, st);
+        tk::launch_pool_scan(s, d_items.ptr, uint32_t(items.size()), d_desc.ptr, false, 0u, d_misc.ptr + 2, st);
         tk::launch_path_totals(s, d_bumps.ptr, false, d_misc.ptr + 2, st);
         TK_CUDA(cudaGetLastError());
         if (pool_len) {
@@ -1248,12 +1247,9 @@ int32_t tk_stage_scan_prefix(tk_ctx* c, const uint32_t* counts, uint64_t pool_le
             TK_CUDA(cudaMemcpyAsync(cursors, d_cursors.ptr, pool_len * 4, cudaMemcpyDeviceToHost, st));
         }
         if (path_count) TK_CUDA(cudaMemcpyAsync(bumps, d_bumps.ptr, path_count * 4, cudaMemcpyDeviceToHost, st));
-        uint32_t err = 0;
-        TK_CUDA(cudaMemcpyAsync(&err, d_misc.ptr, 4, cudaMemcpyDeviceToHost, st));
         TK_CUDA(cudaStreamSynchronize(st));
         d_counts.release(); d_cursors.release(); d_bumps.release(); d_misc.release(); d_bd.release();
         d_ranges.release(); d_paths.release(); d_items.release(); d_desc.release();
-        if (err) throw Fail{TK_E_TIMEOUT, "prefix look-back gave up"};
     });
 }
 
@@ -1364,13 +1360,10 @@ int32_t tk_pool_scan_noalloc(tk_ctx* c, const tk_path_record* paths, uint32_t pa
         s.cursors = d_cursors;
         s.pool_len = pool_len;
         s.error = sc.words;
-        tk::launch_pool_scan(s, sc.items, uint32_t(n_items), sc.desc, sc.words + 1, false, 0u, sc.words + 2, st);
+        tk::launch_pool_scan(s, sc.items, uint32_t(n_items), sc.desc, false, 0u, sc.words + 2, st);
         tk::launch_path_totals(s, d_bumps, false, sc.words + 2, st);
         TK_CUDA(cudaGetLastError());
-        uint32_t err = 0;
-        TK_CUDA(cudaMemcpyAsync(&err, sc.words, 4, cudaMemcpyDeviceToHost, st));
         TK_CUDA(cudaStreamSynchronize(st));
-        if (err) throw Fail{TK_E_TIMEOUT, "prefix look-back gave up"};
     });
 }
 

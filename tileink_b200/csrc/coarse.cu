@@ -30,6 +30,9 @@ constexpr int kQuadSide = 8;
 constexpr int kQuads = (kBinSide / kQuadSide) * (kBinSide / kQuadSide);
 constexpr int kCoarseThreads = kQuadSide * kQuadSide;
 constexpr uint32_t kChunkClassColor = 1u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
+// Candidates whose tile loads are in flight together, per pass (emission
+// keeps more state live and holds fewer).
+constexpr uint32_t kPrefetchCount = 8, kPrefetchEmit = 4;
 
 __device__ __forceinline__ uint32_t tile_min_(int32_t px, uint32_t lim) {
     return px > 0 ? min(uint32_t(px) / TK_TILE_SIZE, lim) : 0u;
@@ -300,48 +303,71 @@ __global__ void __launch_bounds__(kCoarseThreads)
         __syncthreads();
         if (!live) continue;
         uint32_t m = min(uint32_t(kCoarseThreads), n - c0);
-        for (uint32_t k = 0; k < m; ++k) {
-            const DrawInfo& d = s_d[k];
-            if (!(tx >= (d.tx & 0xFFFFu) && tx < (d.tx >> 16) && ty >= (d.ty & 0xFFFFu) && ty < (d.ty >> 16))) continue;
-            uint32_t meta = d.meta;
-            if (!(meta & 16u)) continue;
-            uint32_t px0 = d.px & 0xFFFFu, px1 = d.px >> 16, py0 = d.py & 0xFFFFu, py1 = d.py >> 16;
-            if (px1 <= px0 || tx < px0 || ty < py0 || tx >= px1 || ty >= py1) continue;
-            uint32_t tag = meta & 7u;
-            if (tag != TK_DRAW_BRUSH && tag != TK_DRAW_PATH_GLYPH && tag != TK_DRAW_CLIP) continue;
-            uint32_t bd = d.data_offset + (ty - py0) * (px1 - px0) + tx - px0;
-            tk_segment_range r = c.ranges[bd];
-            uint32_t w = uint32_t(c.backdrops[bd]);
-            if (r.start == r.end && w == 0u) continue;
-            uint32_t batch = meta >> 8;
-            if (batch != cur) {
-                close();
-                cur = batch;
-                nb = 0;
-                wrappers = stack_wrappers(c, batches[batch], tx, ty);
-                rejected = wrappers == TK_INVALID_INDEX;
-                flags = (!rejected && wrappers) ? kChunkClassOther : 0u;
-                if (EMIT && !rejected) {
-                    section = at;
-                    at = emit_stack(c, batches[batch], tx, ty, true, ptcl, cap, at + 1u, error);
-                }
+        // Candidates in groups of kPrefetch: the tile tests and the range /
+        // backdrop loads of a whole group are issued first, so that their
+        // latencies overlap; the group is then walked in painter order.
+        constexpr uint32_t kPrefetch = EMIT ? kPrefetchEmit : kPrefetchCount;
+        for (uint32_t k0 = 0; k0 < m; k0 += kPrefetch) {
+            tk_segment_range rr[kPrefetch];
+            uint32_t ww[kPrefetch];
+            uint32_t hit = 0u;
+#pragma unroll
+            for (uint32_t q = 0; q < kPrefetch; ++q) {
+                rr[q] = tk_segment_range{0u, 0u};
+                ww[q] = 0u;
+                const uint32_t k = k0 + q;
+                if (k >= m) continue;
+                const DrawInfo& d = s_d[k];
+                if (!(tx >= (d.tx & 0xFFFFu) && tx < (d.tx >> 16) && ty >= (d.ty & 0xFFFFu) && ty < (d.ty >> 16))) continue;
+                const uint32_t meta = d.meta;
+                if (!(meta & 16u)) continue;
+                const uint32_t px0 = d.px & 0xFFFFu, px1 = d.px >> 16, py0 = d.py & 0xFFFFu, py1 = d.py >> 16;
+                if (px1 <= px0 || tx < px0 || ty < py0 || tx >= px1 || ty >= py1) continue;
+                const uint32_t tag = meta & 7u;
+                if (tag != TK_DRAW_BRUSH && tag != TK_DRAW_PATH_GLYPH && tag != TK_DRAW_CLIP) continue;
+                const uint32_t bd = d.data_offset + (ty - py0) * (px1 - px0) + tx - px0;
+                rr[q] = c.ranges[bd];
+                ww[q] = uint32_t(c.backdrops[bd]);
+                hit |= 1u << q;
             }
-            if (rejected) continue;
-            uint32_t ptag = TK_PTCL_FILL;
-            if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
-            else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
-            else if ((meta & 32u) && r.start == r.end) ptag = TK_PTCL_COLOR;
-            if (EMIT) {
-                flags |= ptag == TK_PTCL_COLOR ? kChunkClassColor : kChunkClassOther;
-                uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
-                if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
-                store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
-                if (ptag != TK_PTCL_COLOR) {
-                    fills += 1;
-                    visits += r.end - r.start;
+#pragma unroll
+            for (uint32_t q = 0; q < kPrefetch; ++q) {
+                if (!(hit & (1u << q))) continue;
+                const DrawInfo& d = s_d[k0 + q];
+                const uint32_t meta = d.meta, tag = meta & 7u;
+                const tk_segment_range r = rr[q];
+                const uint32_t w = ww[q];
+                if (r.start == r.end && w == 0u) continue;
+                uint32_t batch = meta >> 8;
+                if (batch != cur) {
+                    close();
+                    cur = batch;
+                    nb = 0;
+                    wrappers = stack_wrappers(c, batches[batch], tx, ty);
+                    rejected = wrappers == TK_INVALID_INDEX;
+                    flags = (!rejected && wrappers) ? kChunkClassOther : 0u;
+                    if (EMIT && !rejected) {
+                        section = at;
+                        at = emit_stack(c, batches[batch], tx, ty, true, ptcl, cap, at + 1u, error);
+                    }
                 }
+                if (rejected) continue;
+                uint32_t ptag = TK_PTCL_FILL;
+                if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
+                else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
+                else if ((meta & 32u) && r.start == r.end) ptag = TK_PTCL_COLOR;
+                if (EMIT) {
+                    flags |= ptag == TK_PTCL_COLOR ? kChunkClassColor : kChunkClassOther;
+                    uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
+                    if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
+                    store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
+                    if (ptag != TK_PTCL_COLOR) {
+                        fills += 1;
+                        visits += r.end - r.start;
+                    }
+                }
+                ++nb;
             }
-            ++nb;
         }
     }
     if (!live) return;

@@ -73,16 +73,18 @@ struct SceneView {
 void launch_scan_count(const SceneView& s, cudaStream_t st);
 // Row-blocked pool scan: segment ranges + cursors (per-path prefix from
 // segment_start, or one chain over all paths when device_plan), and the
-// row-wise backdrop cumsum. `total` receives the last inclusive value.
-void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* desc,
-                      uint32_t* ticket, bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st);
+// row-wise backdrop cumsum, in three passes (item sums, item prefixes, apply).
+// item_scratch holds 8 bytes per item; `total` receives the last inclusive
+// value.
+void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* item_scratch,
+                      bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st);
 void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, const uint32_t* total,
                         cudaStream_t st);
 void launch_scan_emit(const SceneView& s, cudaStream_t st);
 
 // Fixed scratch of the allocation-free pool scan (one array per device).
 struct NoAllocScratch {
-    unsigned long long* desc;  // TK_NOALLOC_MAX_SCAN_ITEMS look-back descriptors
+    unsigned long long* desc;  // TK_NOALLOC_MAX_SCAN_ITEMS item sum / prefix pairs
     ScanItem* items;           // TK_NOALLOC_MAX_SCAN_ITEMS work items
     tk_path_record* paths;     // TK_NOALLOC_MAX_PATHS path records
     uint32_t* words;           // [0] error [1] ticket [2] total

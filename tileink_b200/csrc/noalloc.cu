@@ -1,5 +1,5 @@
 // Scratch for the allocation-free pool scan: one file-scope device array per
-// device holding the look-back descriptors, the work items, a copy of the path
+// device holding the per-item sums and prefixes, the work items, a copy of the path
 // records and the counter words, plus the kernel that builds the work items
 // from the path records on the device.
 #include <cuda_runtime.h>

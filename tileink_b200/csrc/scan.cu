@@ -4,11 +4,13 @@
 //             path's backdrop slice. Counts and backdrop deltas are sums, so
 //             their order does not matter.
 // pool scan   (scan/prefix_chunks.hlsl, chunk_offsets.hlsl,
-//             apply_chunk_offsets.hlsl, cumsum.hlsl): one CTA per work item of
-//             whole bbox rows; a decoupled look-back chains the items of a path
-//             (or of the whole pool when segment starts are planned on the
-//             device) in one pass, and the row-wise backdrop cumsum is a
-//             segmented scan inside the same CTA.
+//             apply_chunk_offsets.hlsl, cumsum.hlsl): work items of whole bbox
+//             rows. Pass 1 sums each item's counts (one CTA per item), pass 2
+//             scans the item sums in one CTA (chained per path, or over the
+//             whole pool when segment starts are planned on the device), pass 3
+//             writes each item's ranges and cursors from its prefix and does
+//             the row-wise backdrop cumsum as a segmented scan in the same
+//             CTA. No CTA waits on another.
 // scan_emit   (scan/emit.hlsl:14-28, scan/clip.hlsli:10-75): one warp per
 //             path; lanes take 32 consecutive lines, DDA step r is the outer
 //             loop and lanes rank their slots with __match_any_sync, giving a
@@ -85,9 +87,6 @@ __global__ void k_scan_count(const tk_line* __restrict__ lines, uint64_t line_co
 // ---------------------------------------------------------------------------
 constexpr int kScanThreads = 256;
 constexpr int kScanPerThread = kScanItemElems / kScanThreads;  // 16
-constexpr unsigned long long kStatusAgg = 1ull << 62;
-constexpr unsigned long long kStatusIncl = 2ull << 62;
-constexpr uint32_t kSpinLimit = 1u << 22;
 
 // Inclusive warp scan of (flag, value) pairs under the segmented operator
 // (f1, v1) + (f2, v2) = (f1 | f2, f2 ? v2 : v1 + v2).
@@ -127,19 +126,109 @@ __device__ __forceinline__ void block_seg_exclusive(uint32_t f, uint32_t v, uint
     tot = sv[8 + kScanThreads / 32 - 1];
 }
 
+// Element range of work item k: [e0, e0 + n) of the pool, rows of `stride`.
+struct ItemSpan {
+    uint64_t e0;
+    uint32_t n, stride;
+};
+__device__ __forceinline__ ItemSpan item_span(const ScanItem& it, const tk_path_record* paths) {
+    const tk_path_record& p = paths[it.path];
+    const uint32_t stride = p.tile_x1 - p.tile_x0;
+    return {uint64_t(p.data_offset) + uint64_t(it.row0) * stride, it.rows * stride, stride};
+}
+
+// Pass 1: the segment count of every work item (its sum of tile counts).
 __global__ void __launch_bounds__(kScanThreads)
-    k_pool_scan(const ScanItem* __restrict__ items, uint32_t n_items, tk_path_record* paths, uint32_t* counts,
-                int32_t* backdrops, tk_segment_range* ranges, uint32_t* cursors, unsigned long long* desc,
-                uint32_t* ticket, int device_plan, uint32_t device_base, uint32_t* total, uint32_t* error) {
-    __shared__ uint32_t s_cnt[kScanItemElems];
-    __shared__ int32_t s_bd[kScanItemElems];
-    __shared__ uint32_t s_f[24], s_v[24];
-    __shared__ uint32_t s_item, s_prefix;
-    const int tid = threadIdx.x;
-    if (tid == 0) s_item = atomicAdd(ticket, 1u);
+    k_item_sums(const ScanItem* __restrict__ items, const tk_path_record* __restrict__ paths,
+                const uint32_t* __restrict__ counts, uint32_t* item_words) {
+    __shared__ uint32_t s_w[kScanThreads / 32];
+    const uint32_t k = blockIdx.x, tid = threadIdx.x;
+    const ItemSpan sp = item_span(items[k], paths);
+    uint32_t v[kScanPerThread];
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; ++j) {
+        const uint32_t i = tid + uint32_t(j) * kScanThreads;
+        v[j] = i < sp.n ? counts[sp.e0 + i] : 0u;
+    }
+    uint32_t sum = 0u;
+#pragma unroll
+    for (int j = 0; j < kScanPerThread; ++j) sum += v[j];
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    if ((tid & 31u) == 0u) s_w[tid >> 5] = sum;
     __syncthreads();
-    const uint32_t k = s_item;
-    if (k >= n_items) return;
+    if (tid == 0) {
+        uint32_t t = 0u;
+        for (int w = 0; w < kScanThreads / 32; ++w) t += s_w[w];
+        item_words[2u * k] = t;
+    }
+}
+
+// Pass 2 (one CTA): item prefixes, a segmented exclusive scan of the item
+// sums in item order (u32, wrapping). A chain starts at item 0 with
+// device_base when the segment slices are planned on the device, else at
+// every path's first item with the path's segment_start. `total` receives the
+// last item's prefix + sum.
+constexpr uint32_t kPrefixThreads = 1024;
+__global__ void __launch_bounds__(kPrefixThreads)
+    k_item_prefix(const ScanItem* __restrict__ items, uint32_t n_items, const tk_path_record* __restrict__ paths,
+                  uint32_t* item_words, int device_plan, uint32_t device_base, uint32_t* total) {
+    __shared__ uint32_t s_f[kPrefixThreads / 32], s_v[kPrefixThreads / 32];
+    __shared__ uint32_t s_carry;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    if (tid == 0) s_carry = 0u;
+    __syncthreads();
+    for (uint32_t k0 = 0; k0 < n_items; k0 += kPrefixThreads) {
+        const uint32_t k = k0 + tid;
+        uint32_t f = 0u, v = 0u, agg = 0u;
+        if (k < n_items) {
+            const ScanItem it = items[k];
+            agg = item_words[2u * k];
+            const bool head = device_plan ? k == 0u : it.first != 0u;
+            f = head ? 1u : 0u;
+            v = head ? (device_plan ? device_base : paths[it.path].segment_start) + agg : agg;
+        }
+        // inclusive segmented scan: warps, then the warp totals
+        warp_seg_scan(f, v);
+        if (lane == 31u) {
+            s_f[warp] = f;
+            s_v[warp] = v;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t wf = s_f[lane], wv = s_v[lane];
+            warp_seg_scan(wf, wv);
+            s_f[lane] = wf;
+            s_v[lane] = wv;
+        }
+        __syncthreads();
+        if (warp > 0 && !f) v += s_v[warp - 1];
+        const uint32_t fw = f | (warp > 0 ? s_f[warp - 1] : 0u);
+        if (!fw) v += s_carry;  // no chain head at or before k within this block
+        if (k < n_items) {
+            item_words[2u * k + 1u] = v - agg;  // exclusive prefix
+            if (k + 1u == n_items) *total = v;
+        }
+        __syncthreads();
+        if (tid == kPrefixThreads - 1u) s_carry = v;
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ uint32_t pad16(uint32_t i) { return i + (i >> 4); }
+
+// Pass 3: per work item the exclusive prefix of the tile counts (segment
+// ranges and cursors, starting at the item's prefix) and the row-wise backdrop
+// cumsum.
+__global__ void __launch_bounds__(kScanThreads)
+    k_pool_scan(const ScanItem* __restrict__ items, tk_path_record* paths, uint32_t* counts, int32_t* backdrops,
+                tk_segment_range* ranges, uint32_t* cursors, const uint32_t* __restrict__ item_words) {
+    // element i lives at pad(i) = i + i / 16, so that thread t's run of 16
+    // elements starts at 17 t and a warp's sequential walk meets 32 banks
+    __shared__ uint32_t s_cnt[kScanItemElems + kScanItemElems / 16];
+    __shared__ int32_t s_bd[kScanItemElems + kScanItemElems / 16];
+    __shared__ uint32_t s_f[24], s_v[24];
+    const int tid = threadIdx.x;
+    const uint32_t k = blockIdx.x;
     const ScanItem it = items[k];
     const tk_path_record& p = paths[it.path];
     const uint32_t stride = p.tile_x1 - p.tile_x0;
@@ -160,8 +249,8 @@ __global__ void __launch_bounds__(kScanThreads)
         for (int j = 0; j < 8; ++j) {
             const uint32_t i = tid + uint32_t(j0 + j) * kScanThreads;
             if (i < n) {
-                s_cnt[i] = vc[j];
-                s_bd[i] = vb[j];
+                s_cnt[pad16(i)] = vc[j];
+                s_bd[pad16(i)] = vb[j];
             }
         }
     }
@@ -177,13 +266,13 @@ __global__ void __launch_bounds__(kScanThreads)
     for (int j = 0; j < kScanPerThread; ++j) {
         uint32_t i = lo + j;
         if (i < n) {
-            csum += s_cnt[i];
+            csum += s_cnt[pad16(i)];
             if (i == row_start) {
                 bf = 1u;
                 bsum = 0u;
                 row_start += stride;
             }
-            bsum += uint32_t(s_bd[i]);
+            bsum += uint32_t(s_bd[pad16(i)]);
         }
     }
     // counts: plain exclusive scan (flags 0)
@@ -194,51 +283,7 @@ __global__ void __launch_bounds__(kScanThreads)
     block_seg_exclusive(bf, bsum, bef, bexcl, s_f, s_v, btot);
     (void)btot;
     (void)ef;
-    // look-back for the item prefix: warp 0 reads 32 predecessors per step and
-    // adds the aggregates down to the nearest inclusive prefix (wrapping u32)
-    if (tid < 32) {
-        const uint32_t lane = tid;
-        const bool chain_head = device_plan ? (k == 0u) : (it.first != 0u);
-        uint32_t prefix = 0u;
-        if (chain_head) {
-            prefix = device_plan ? device_base : p.segment_start;
-            if (lane == 0) atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
-        } else {
-            if (lane == 0) atomicExch(desc + k, kStatusAgg | (unsigned long long)agg);
-            int64_t j = int64_t(k) - 1;
-            uint32_t spins = 0;
-            for (;;) {
-                const int64_t idx = j - int64_t(lane);
-                unsigned long long d = kStatusIncl;  // before item 0: an empty inclusive prefix
-                if (idx >= 0) d = *((volatile unsigned long long*)(desc + idx));
-                const unsigned long long st = d & (3ull << 62);
-                const uint32_t incl = __ballot_sync(0xffffffffu, st == kStatusIncl);
-                const uint32_t zero = __ballot_sync(0xffffffffu, st == 0ull);
-                // lanes 0 .. nearest inclusive lane (all 32 without one)
-                const uint32_t first = incl ? uint32_t(__ffs(incl) - 1) : 31u;
-                const uint32_t need = first == 31u ? 0xffffffffu : ((2u << first) - 1u);
-                if (zero & need) {  // a predecessor has not published yet
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0) atomicOr(error, ERR_LOOKBACK_TIMEOUT);
-                        break;
-                    }
-                    __nanosleep(64);
-                    continue;
-                }
-                prefix += __reduce_add_sync(0xffffffffu, ((need >> lane) & 1u) ? uint32_t(d) : 0u);
-                if (incl) break;
-                j -= 32;
-            }
-            __threadfence();
-            if (lane == 0) atomicExch(desc + k, kStatusIncl | (unsigned long long)(prefix + agg));
-        }
-        if (lane == 0) {
-            if (k + 1u == n_items) *total = prefix + agg;
-            s_prefix = prefix;
-        }
-    }
-    __syncthreads();
-    const uint32_t prefix = s_prefix;
+    const uint32_t prefix = item_words[2u * k + 1u];
     uint32_t run = prefix + ecount;
     uint32_t brun = bexcl;
     row_start = row_start0;
@@ -246,24 +291,24 @@ __global__ void __launch_bounds__(kScanThreads)
     for (int j = 0; j < kScanPerThread; ++j) {
         uint32_t i = lo + j;
         if (i < n) {
-            uint32_t c = s_cnt[i];
-            s_cnt[i] = run;  // exclusive start
+            uint32_t c = s_cnt[pad16(i)];
+            s_cnt[pad16(i)] = run;  // exclusive start
             run += c;
             if (i == row_start) {
                 brun = 0u;
                 row_start += stride;
             }
-            brun += uint32_t(s_bd[i]);
-            s_bd[i] = int32_t(brun);
+            brun += uint32_t(s_bd[pad16(i)]);
+            s_bd[pad16(i)] = int32_t(brun);
         }
     }
     __syncthreads();
     for (uint32_t i = tid; i < n; i += kScanThreads) {
-        uint32_t start = s_cnt[i];
-        uint32_t end = (i + 1 < n) ? s_cnt[i + 1] : prefix + agg;
+        uint32_t start = s_cnt[pad16(i)];
+        uint32_t end = (i + 1 < n) ? s_cnt[pad16(i + 1)] : prefix + agg;
         ranges[e0 + i] = tk_segment_range{start, end};
         cursors[e0 + i] = start;
-        backdrops[e0 + i] = s_bd[i];
+        backdrops[e0 + i] = s_bd[pad16(i)];
     }
 }
 
@@ -376,14 +421,14 @@ void launch_scan_count(const SceneView& s, cudaStream_t st) {
                                                                        s.backdrops, s.counts);
 }
 
-void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* desc,
-                      uint32_t* ticket, bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st) {
+void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_items, unsigned long long* item_scratch,
+                      bool device_plan, uint32_t device_base, uint32_t* total, cudaStream_t st) {
     cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
     if (n_items == 0) return;
-    cudaMemsetAsync(desc, 0, sizeof(unsigned long long) * n_items, st);
-    cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
-    k_pool_scan<<<n_items, kScanThreads, 0, st>>>(items, n_items, s.paths, s.counts, s.backdrops, s.ranges, s.cursors,
-                                                  desc, ticket, device_plan ? 1 : 0, device_base, total, s.error);
+    uint32_t* words = reinterpret_cast<uint32_t*>(item_scratch);  // per item: sum, prefix
+    k_item_sums<<<n_items, kScanThreads, 0, st>>>(items, s.paths, s.counts, words);
+    k_item_prefix<<<1, kPrefixThreads, 0, st>>>(items, n_items, s.paths, words, device_plan ? 1 : 0, device_base, total);
+    k_pool_scan<<<n_items, kScanThreads, 0, st>>>(items, s.paths, s.counts, s.backdrops, s.ranges, s.cursors, words);
 }
 
 void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, const uint32_t* total,
