@@ -417,6 +417,44 @@ typedef struct tk_flatten_desc {
 int32_t tk_scene_upload_flatten(tk_ctx* ctx, const tk_scene_desc* scene, const tk_flatten_desc* flatten);
 
 /* ------------------------------------------------------------------------ */
+/* Incremental rendering: the damage-driven redraw of the retained path      */
+/* (NativeRenderer::render_retained, src/native/renderer/retained.rs:17-218; */
+/* damage planning, src/render/incremental.rs:1-297). The uploaded scene is  */
+/* scanned in full, then coarse and fine run only on the tiles under the     */
+/* damage; every other pixel keeps the context's previous frame. The result  */
+/* equals a full tk_render of the scene whenever the damage covers every     */
+/* pixel whose value changed since that frame (tk_retained_materialize       */
+/* reports such damage).                                                     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct tk_damage {
+    uint32_t full;          /* 1: redraw everything */
+    uint32_t rect_count;
+    const int32_t* rects;   /* rect_count x {x0, y0, x1, y1}, physical pixels, half-open */
+} tk_damage;
+
+/* Why a frame was drawn in full (FullRedrawReason,
+ * src/render/incremental/config.rs:52-63). */
+#define TK_FULL_NONE 0u         /* incremental */
+#define TK_FULL_REQUESTED 1u    /* damage.full (ExplicitInvalidation) */
+#define TK_FULL_NO_HISTORY 2u   /* no previous frame of this size and clear colour in the context (FirstFrame) */
+#define TK_FULL_THRESHOLD 3u    /* dirty tiles >= full_redraw_ratio of all (DirtyTileThreshold) */
+#define TK_FULL_FILTERS 4u      /* the scene has blur layers, whose reach crosses tiles */
+
+typedef struct tk_incremental_stats {
+    uint32_t total_tiles;
+    uint32_t dirty_tiles;   /* tiles redrawn */
+    uint32_t full_redraw;   /* 1 when every tile was redrawn */
+    uint32_t reason;        /* TK_FULL_* */
+} tk_incremental_stats;
+
+/* Renders the uploaded scene, redrawing only the tiles that meet `damage`
+ * unless a full redraw is needed (see TK_FULL_*; full_redraw_ratio in (0, 1],
+ * the reference's default is 0.7). `stats` may be null. */
+int32_t tk_render_incremental(tk_ctx* ctx, const tk_damage* damage, float full_redraw_ratio,
+                              tk_incremental_stats* stats);
+
+/* ------------------------------------------------------------------------ */
 /* Batched mode: many independent scenes of uneven size rendered together.   */
 /* Every stage runs once for the whole batch (the scenes' paths, tiles, bins */
 /* and images are concatenated) and the stage sequence is one CUDA graph,    */

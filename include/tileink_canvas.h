@@ -65,9 +65,10 @@ void tk_canvas_free(tk_canvas* c);
  * scan-line planner at record time (canvas/storage.rs:131-142); otherwise the
  * scene asks the device to plan them (TK_SCENE_SEGMENTS_FROM_DEVICE). */
 void tk_canvas_set_host_segment_plan(tk_canvas* c, int32_t enabled);
-/* Fill paths recorded after this keep their Bezier elements for
- * tk_scene_upload_flatten instead of being flattened on the host; stroke
- * outlines stay host lines. Turns host segment planning off. */
+/* Fill paths and stroke centerlines recorded after this keep their Bezier
+ * elements for tk_scene_upload_flatten, which flattens and strokes them on the
+ * device, instead of being flattened on the host. Turns host segment planning
+ * off. */
 void tk_canvas_set_device_flatten(tk_canvas* c, int32_t enabled);
 /* The recorded elements and per-path element ranges (valid until the canvas
  * changes). */
@@ -88,6 +89,52 @@ int32_t tk_canvas_pop_layer(tk_canvas* c);
 /* Compile (if needed) and describe the recorded scene. Pointers stay valid
  * until the canvas is modified or freed. */
 int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out);
+
+/* Command log: when set, the canvas also keeps every later push / pop call
+ * with its original geometry, brush and transform, so that it can be replayed
+ * into another canvas (and become a retained scene node). */
+void tk_canvas_set_keep_commands(tk_canvas* c, int32_t enabled);
+/* Replays `src`'s logged calls into `dst`, each call's transform preceded by
+ * `transform` (NULL: as recorded). `src` must keep commands and have every
+ * layer it opened closed. */
+int32_t tk_canvas_replay(tk_canvas* dst, const tk_canvas* src, const double* transform);
+
+/* ------------------------------------------------------------------------ */
+/* Retained scene (RetainedScene, src/retained_scene/scene.rs:14-140 and     */
+/* transaction.rs:74-255): nodes in painter order, each a copy of a          */
+/* command-keeping canvas's calls under a node transform. Every mutation     */
+/* bumps the version. tk_retained_materialize records the nodes into one     */
+/* canvas and reports the damage since the previous materialization: the     */
+/* pixel bounds, before and after, of every node inserted, replaced,         */
+/* transformed, moved or removed, plus invalidated rectangles; everything    */
+/* on the first call, after invalidate_all or a clear colour change, and     */
+/* when a changed node has clip or blur layers (which can regroup the draw   */
+/* batches of other nodes). That damage drives tk_render_incremental.        */
+/* ------------------------------------------------------------------------ */
+typedef struct tk_retained tk_retained;
+tk_retained* tk_retained_new(uint32_t logical_width, uint32_t logical_height, float scale);
+void tk_retained_free(tk_retained* rs);
+void tk_retained_set_clear_color(tk_retained* rs, uint32_t premul_rgba8);
+/* Materialized canvases record fills and stroke centerlines as elements for
+ * device flattening (the lines are the same either way). */
+void tk_retained_set_device_flatten(tk_retained* rs, int32_t enabled);
+uint64_t tk_retained_version(const tk_retained* rs);
+/* id != 0 and unused; before = 0 appends, else the node goes in front of
+ * node `before`. transform NULL = identity. Returns 0, or -1 on error. */
+int32_t tk_retained_insert(tk_retained* rs, uint64_t id, const tk_canvas* content, const double* transform,
+                           uint64_t before);
+int32_t tk_retained_replace(tk_retained* rs, uint64_t id, const tk_canvas* content);
+int32_t tk_retained_set_transform(tk_retained* rs, uint64_t id, const double* transform);
+/* sibling = 0 moves the node to the end (painted last). */
+int32_t tk_retained_move_before(tk_retained* rs, uint64_t id, uint64_t sibling);
+int32_t tk_retained_remove(tk_retained* rs, uint64_t id);
+/* rect: {x0, y0, x1, y1} in physical pixels, half-open. */
+int32_t tk_retained_invalidate_rect(tk_retained* rs, const int32_t rect[4]);
+int32_t tk_retained_invalidate_all(tk_retained* rs);
+/* The scene as one canvas (owned by `rs`, valid until the next call or
+ * tk_retained_free) and, in `damage` (may be NULL), what changed since the
+ * previous call; damage->rects points into `rs` with the same lifetime. */
+tk_canvas* tk_retained_materialize(tk_retained* rs, tk_damage* damage);
 
 /* Seeded synthetic workloads. `config`: 1 = 640x360 240 cubic fills;
  * 2 = 4096x4096 50k mixed fills/strokes/gradients/clips; 3 = 1920x1080 20k

@@ -1,0 +1,124 @@
+"""Incremental rendering of retained scenes: after any sequence of mutations,
+redrawing only the damaged tiles over the previous frame gives exactly the
+image a full render of the same scene gives, and frames fall back to full
+redraws where they must (FullRedrawReason, src/render/incremental/config.rs:52-63)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import tileink_b200 as tk
+from tileink_b200 import _native as N
+
+from test_retained import calls, node_canvas
+
+pytestmark = pytest.mark.gpu
+
+W, H = 512, 384
+
+
+@pytest.fixture(scope="module")
+def reference_renderer():
+    r = tk.NativeRenderer(0)
+    yield r
+    r.close()
+
+
+def full_image(r, canvas):
+    return r.render_to_image(canvas)
+
+
+def incremental_image(renderer, scene, ratio=0.7):
+    stats = renderer.render_retained(scene, ratio)
+    img = renderer.readback().view(np.uint8).reshape(H, W, 4)
+    return img, stats
+
+
+def big_node(seed, n):
+    """n seeded fills and strokes spread over the canvas."""
+    c = tk.Canvas(W, H)
+    c.keep_commands()
+    rng = np.random.default_rng(seed)
+    for k in range(n):
+        cx, cy = rng.uniform(20, W - 20), rng.uniform(20, H - 20)
+        p = tk.BezPath()
+        p.move_to(cx, cy)
+        for _ in range(3):
+            p.cubic_to(*(rng.uniform(-40, 40, 6) + np.tile([cx, cy], 3)))
+        p.close()
+        b = tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.4, 1.0)))
+        if k % 3 == 2:
+            c.push_stroke(p, b, float(rng.uniform(0.5, 5.0)))
+        else:
+            c.push_path(p, b, fill_rule=k % 2)
+    return c
+
+
+@pytest.mark.parametrize("device_flatten", [False, True])
+def test_gpu_incremental_frames_equal_full_frames(renderer, reference_renderer, device_flatten):
+    rs = tk.RetainedScene(W, H, device_flatten=device_flatten)
+    rs.set_clear_color(0xFFFFFFFF)
+    for k in range(12):
+        rs.insert(k + 1, big_node(100 + k, 8), None if k % 2 else (1, 0, 0, 1, 2.0 * k, 0.0))
+    img, st = incremental_image(renderer, rs)
+    assert st["full_redraw"] == 1 and st["reason"] == N.FULL_REQUESTED  # the first materialization
+    canvas = rs.materialize()[0]  # no change: the same canvas again
+    assert np.array_equal(img, full_image(reference_renderer, canvas))
+
+    small = [
+        lambda: rs.set_transform(3, (1, 0, 0, 1, 6.5, -4.25)),
+        lambda: rs.set_transform(3, (0.9, 0.2, -0.2, 0.9, 30.0, 10.0)),
+        lambda: rs.remove(7),
+        lambda: rs.replace(5, node_canvas(calls(77, n=3))),
+        lambda: rs.move_before(12, 1),
+        lambda: rs.insert(40, node_canvas(calls(41, n=2)), (1, 0, 0, 1, 100.0, 60.0), before=4),
+        lambda: rs.invalidate_rect(0, 0, 40, 40),
+        lambda: None,  # nothing changed
+    ]
+    for step, mutate in enumerate(small):
+        mutate()
+        img, st = incremental_image(renderer, rs)
+        canvas = rs.materialize()[0]
+        want = full_image(reference_renderer, canvas)
+        assert np.array_equal(img, want), step
+        assert st["full_redraw"] == 0, (step, st)
+        assert st["dirty_tiles"] < st["total_tiles"], (step, st)
+
+    # a node with clip layers: every tile
+    rs.insert(50, node_canvas(calls(8, n=3, layered=True)))
+    img, st = incremental_image(renderer, rs)
+    assert st["full_redraw"] == 1 and st["reason"] == N.FULL_REQUESTED
+    assert np.array_equal(img, full_image(reference_renderer, rs.materialize()[0]))
+    # damage over the threshold: every tile
+    rs.set_transform(1, (1, 0, 0, 1, 1.0, 1.0))
+    rs.invalidate_rect(0, 0, W, H // 2 + 64)
+    img, st = incremental_image(renderer, rs, ratio=0.5)
+    assert st["full_redraw"] == 1 and st["reason"] == N.FULL_THRESHOLD
+    assert np.array_equal(img, full_image(reference_renderer, rs.materialize()[0]))
+
+
+def test_gpu_incremental_fallbacks(renderer):
+    # blur layers reach across tiles: full redraws
+    blur = tk.generate(5, 1, width=256, height=256, paths=12)
+    renderer.upload(blur)
+    st = renderer.render_incremental({"full": False, "rects": [[0, 0, 16, 16]]})
+    assert st["full_redraw"] == 1
+    st = renderer.render_incremental({"full": False, "rects": [[0, 0, 16, 16]]})
+    assert st["full_redraw"] == 1 and st["reason"] == N.FULL_FILTERS
+    # a new size has no history
+    c = tk.generate(1, 2, width=200, height=120, paths=20, device_segment_plan=True)
+    renderer.upload(c)
+    st = renderer.render_incremental({"full": False, "rects": [[0, 0, 16, 16]]})
+    assert st["reason"] == N.FULL_NO_HISTORY
+    first = renderer.readback().copy()
+    # the same scene again with empty damage: nothing is redrawn, the frame stands
+    renderer.upload(c)
+    st = renderer.render_incremental({"full": False, "rects": np.zeros((0, 4), np.int32)})
+    assert st["full_redraw"] == 0 and st["dirty_tiles"] == 0
+    assert np.array_equal(renderer.readback(), first)
+    # and with damage somewhere: those tiles are redrawn to the same pixels
+    st = renderer.render_incremental({"full": False, "rects": [[10, 10, 90, 50]]})
+    assert st["full_redraw"] == 0 and 0 < st["dirty_tiles"] < st["total_tiles"]
+    assert np.array_equal(renderer.readback(), first)
+    with pytest.raises(tk.TileinkError):
+        renderer.render_incremental({"full": False, "rects": [[0, 0, 1, 1]]}, full_redraw_ratio=0.0)

@@ -5,9 +5,9 @@ rendering goes through the C ABI in include/tileink.h (tileink_b200.renderer).
 The CUDA library must be built in-tree first (python -m tileink_b200.build);
 there is no CPU fallback.
 """
-from .canvas import BezPath, Brush, Canvas, generate, plan_line_tile_count, FILL_NONZERO, FILL_EVEN_ODD
+from .canvas import BezPath, Brush, Canvas, RetainedScene, generate, plan_line_tile_count, FILL_NONZERO, FILL_EVEN_ODD
 from .renderer import NativeRenderer, TileinkError
 from . import _native as native
 
-__all__ = ["BezPath", "Brush", "Canvas", "generate", "plan_line_tile_count", "NativeRenderer", "TileinkError",
+__all__ = ["BezPath", "Brush", "Canvas", "RetainedScene", "generate", "plan_line_tile_count", "NativeRenderer", "TileinkError",
            "native", "FILL_NONZERO", "FILL_EVEN_ODD"]

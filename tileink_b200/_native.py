@@ -130,6 +130,19 @@ class GenParams(C.Structure):
                 ("sigma", C.c_float), ("jitter", C.c_float), ("flags", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class Damage(C.Structure):
+    """tk_damage (include/tileink.h)."""
+    _fields_ = [("full", C.c_uint32), ("rect_count", C.c_uint32), ("rects", C.c_void_p)]
+
+
+class IncrementalStats(C.Structure):
+    """tk_incremental_stats (include/tileink.h)."""
+    _fields_ = [("total_tiles", C.c_uint32), ("dirty_tiles", C.c_uint32), ("full_redraw", C.c_uint32),
+                ("reason", C.c_uint32)]
+
+
+FULL_NONE, FULL_REQUESTED, FULL_NO_HISTORY, FULL_THRESHOLD, FULL_FILTERS = 0, 1, 2, 3, 4
+
 _LIB = None
 
 
@@ -155,6 +168,7 @@ def library() -> C.CDLL:
         "tk_canvas_set_device_flatten": (None, [P, I32]),
         "tk_canvas_flatten_desc": (I32, [P, C.POINTER(FlattenDesc)]),
         "tk_render": (I32, [P]),
+        "tk_render_incremental": (I32, [P, C.POINTER(Damage), F32, C.POINTER(IncrementalStats)]),
         "tk_readback": (I32, [P, P, C.c_size_t]),
         "tk_render_to_image": (I32, [P, C.POINTER(SceneDesc), P, C.c_size_t]),
         "tk_get_stats": (I32, [P, C.POINTER(Stats)]),
@@ -192,6 +206,21 @@ def library() -> C.CDLL:
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),
         "tk_canvas_scene": (I32, [P, C.POINTER(SceneDesc)]),
+        "tk_canvas_set_keep_commands": (None, [P, I32]),
+        "tk_canvas_replay": (I32, [P, P, P]),
+        "tk_retained_new": (P, [U32, U32, F32]),
+        "tk_retained_free": (None, [P]),
+        "tk_retained_set_clear_color": (None, [P, U32]),
+        "tk_retained_set_device_flatten": (None, [P, I32]),
+        "tk_retained_version": (U64, [P]),
+        "tk_retained_insert": (I32, [P, U64, P, P, U64]),
+        "tk_retained_replace": (I32, [P, U64, P]),
+        "tk_retained_set_transform": (I32, [P, U64, P]),
+        "tk_retained_move_before": (I32, [P, U64, U64]),
+        "tk_retained_remove": (I32, [P, U64]),
+        "tk_retained_invalidate_rect": (I32, [P, P]),
+        "tk_retained_invalidate_all": (I32, [P]),
+        "tk_retained_materialize": (P, [P, C.POINTER(Damage)]),
         "tk_generate": (P, [U32, U64, C.POINTER(GenParams)]),
         "tk_canvas_param_points": (U64, [P, P]),
         "tk_canvas_param_colors": (U64, [P, P]),

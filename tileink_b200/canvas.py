@@ -114,17 +114,29 @@ def _affine(transform):
 class Canvas:
     """Immediate-mode recording canvas (src/canvas.rs:86-126)."""
 
-    def __init__(self, width: int, height: int, scale: float = 1.0, *, _handle=None):
+    def __init__(self, width: int, height: int, scale: float = 1.0, *, _handle=None, _owner=None):
         self._lib = N.library()
         self._h = _handle if _handle is not None else self._lib.tk_canvas_new(int(width), int(height), float(scale))
+        self._owner = _owner  # a canvas owned by another object (a retained scene's materialization)
         if not self._h:
             raise ValueError("invalid canvas surface")
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and getattr(self, "_owner", None) is None:
             self._lib.tk_canvas_free(h)
-            self._h = None
+        self._h = None
+
+    def keep_commands(self, enabled: bool = True):
+        """Keep every later push / pop call with its original geometry, so
+        the canvas can be replayed or become a RetainedScene node."""
+        self._lib.tk_canvas_set_keep_commands(self._h, 1 if enabled else 0)
+
+    def replay(self, src: "Canvas", transform=None):
+        """Replays `src`'s kept calls into this canvas under `transform`."""
+        t, keep = _affine(transform)
+        if self._lib.tk_canvas_replay(self._h, src._h, t) != 0:
+            raise ValueError("replay needs a command-keeping source with its layers closed")
 
     def set_clear_color(self, premul_rgba8: int):
         self._lib.tk_canvas_set_clear_color(self._h, int(premul_rgba8) & 0xFFFFFFFF)
@@ -236,3 +248,76 @@ def plan_line_tile_count(line: np.ndarray, bbox) -> int:
     """Host scan-line planner (src/shared/scan_line.rs:17-31)."""
     l = np.ascontiguousarray(np.asarray(line, dtype=N.LINE_DTYPE).reshape(1))
     return N.library().tk_plan_line_tile_count(N.ptr(l), *[int(v) for v in bbox])
+
+
+class RetainedScene:
+    """Retained scene (RetainedScene, src/retained_scene/scene.rs:14-140;
+    transaction.rs:74-255): nodes in painter order, each a command-keeping
+    Canvas under a node transform. `materialize()` gives the scene as one
+    Canvas and the damage since the previous call, which
+    NativeRenderer.render_incremental turns into a redraw of those tiles."""
+
+    def __init__(self, width: int, height: int, scale: float = 1.0, device_flatten: bool = False):
+        self._lib = N.library()
+        self._h = self._lib.tk_retained_new(int(width), int(height), float(scale))
+        if not self._h:
+            raise ValueError("invalid retained scene surface")
+        self._lib.tk_retained_set_device_flatten(self._h, 1 if device_flatten else 0)
+        self._canvas = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._canvas = None
+            self._lib.tk_retained_free(h)
+            self._h = None
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            raise ValueError(f"retained scene: {what} rejected its arguments")
+
+    @property
+    def version(self) -> int:
+        return int(self._lib.tk_retained_version(self._h))
+
+    def set_clear_color(self, premul_rgba8: int):
+        self._lib.tk_retained_set_clear_color(self._h, int(premul_rgba8) & 0xFFFFFFFF)
+
+    def insert(self, node_id: int, content: Canvas, transform=None, before: int = 0):
+        t, keep = _affine(transform)
+        self._check(self._lib.tk_retained_insert(self._h, int(node_id), content._h, t, int(before)), "insert")
+
+    def replace(self, node_id: int, content: Canvas):
+        self._check(self._lib.tk_retained_replace(self._h, int(node_id), content._h), "replace")
+
+    def set_transform(self, node_id: int, transform=None):
+        t, keep = _affine(transform)
+        self._check(self._lib.tk_retained_set_transform(self._h, int(node_id), t), "set_transform")
+
+    def move_before(self, node_id: int, sibling: int = 0):
+        self._check(self._lib.tk_retained_move_before(self._h, int(node_id), int(sibling)), "move_before")
+
+    def remove(self, node_id: int):
+        self._check(self._lib.tk_retained_remove(self._h, int(node_id)), "remove")
+
+    def invalidate_rect(self, x0: int, y0: int, x1: int, y1: int):
+        r = (C.c_int32 * 4)(int(x0), int(y0), int(x1), int(y1))
+        self._check(self._lib.tk_retained_invalidate_rect(self._h, r), "invalidate_rect")
+
+    def invalidate_all(self):
+        self._check(self._lib.tk_retained_invalidate_all(self._h), "invalidate_all")
+
+    def materialize(self):
+        """(Canvas, damage): the scene recorded as one canvas (valid until the
+        next materialize) and a dict {full, rects (n x 4 int32 array)}."""
+        d = N.Damage()
+        h = self._lib.tk_retained_materialize(self._h, C.byref(d))
+        if not h:
+            raise ValueError("retained scene: materialization failed")
+        if self._canvas is not None:
+            self._canvas._h = None  # its native canvas was just replaced
+        self._canvas = Canvas(0, 0, _handle=h, _owner=self)
+        rects = np.zeros((0, 4), np.int32)
+        if d.rect_count:
+            rects = np.ctypeslib.as_array((C.c_int32 * (4 * d.rect_count)).from_address(d.rects)).reshape(-1, 4).copy()
+        return self._canvas, {"full": bool(d.full), "rects": rects}

@@ -166,6 +166,18 @@ struct tk_ctx {
     size_t ev_used = 0;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
     FlattenScratch flat;
+    // incremental rendering: whether `image` holds the last single-scene
+    // frame (and its size and clear colour), and the redrawn tiles of the
+    // frame in progress (null outside tk_render_incremental)
+    bool history = false;
+    uint32_t history_w = 0, history_h = 0, history_clear = 0;
+    std::vector<uint8_t> h_active;
+    std::vector<uint32_t> h_active_list;
+    DBuf<uint8_t> tile_active;
+    DBuf<uint32_t> tile_list;
+    const uint8_t* active_mask = nullptr;
+    const uint32_t* active_list = nullptr;
+    uint32_t active_n = 0;
 };
 
 namespace {
@@ -393,6 +405,9 @@ tk::PassView pass_view(tk_ctx* c, Pass& p) {
         v.total_tiles = c->total_tiles;
         v.scene_count = uint32_t(c->h_scenes.size());
     }
+    v.tile_active = c->active_mask;
+    v.tile_list = c->active_list;
+    v.tile_list_n = c->active_n;
     return v;
 }
 
@@ -446,6 +461,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nu
     c->stats.reserve(4);
     uint32_t T = c->tw * c->th;
     c->tile_desc.reserve((T + 4095) / 4096 + 1);
+    if (uint64_t(c->width) * c->height > c->image.cap) c->history = false;  // reallocated below
     c->image.reserve(uint64_t(c->width) * c->height);
     bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
     c->segment_needed = device_plan ? 0 : c->host_segment_capacity;
@@ -527,13 +543,20 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
         tk::launch_coarse(s, v, false, st);
         tk::launch_tile_prefix(s, v, st);
     }
-    if (p.ptcl_needed == 0) {  // first frame of this scene: size the PTCL buffer
+    if (c->active_mask) {  // incremental frame: size for its tiles, keep the full-frame size unknown
         uint32_t total = read_word(c, c->misc.ptr + 3);
-        p.ptcl_needed = uint64_t(total) + 1;
-        p.ptcl.reserve(p.ptcl_needed);
+        p.ptcl.reserve(uint64_t(total) + 1);
+        p.ptcl_used = total;
         v = pass_view(c, p);
+    } else {
+        if (p.ptcl_needed == 0) {  // first frame of this scene: size the PTCL buffer
+            uint32_t total = read_word(c, c->misc.ptr + 3);
+            p.ptcl_needed = uint64_t(total) + 1;
+            p.ptcl.reserve(p.ptcl_needed);
+            v = pass_view(c, p);
+        }
+        p.ptcl_used = p.ptcl_needed - 1;
     }
-    p.ptcl_used = p.ptcl_needed - 1;
     {
         StageMark m(c, 6);
         tk::launch_coarse(s, v, true, st);
@@ -586,6 +609,7 @@ void scan_phase(tk_ctx* c) {
 }
 
 void do_render(tk_ctx* c) {
+    c->history = false;
     scan_phase(c);
     cudaStream_t st = c->stream;
     tk::launch_fill(c->image.ptr, uint64_t(c->width) * c->height, c->clear, st);
@@ -636,6 +660,42 @@ void do_render(tk_ctx* c) {
     }
     TK_CUDA(cudaGetLastError());
     c->rendered = true;
+    c->history = true;
+    c->history_w = c->width;
+    c->history_h = c->height;
+    c->history_clear = c->clear;
+}
+
+// The incremental frame: a full scan, then coarse and fine of the active
+// tiles only, over the previous frame (scenes without blur layers: one pass
+// per batch group straight into the image).
+void do_render_tiles(tk_ctx* c) {
+    c->history = false;
+    scan_phase(c);
+    cudaStream_t st = c->stream;
+    const uint32_t T = c->tw * c->th;
+    upload(c->tile_active, c->h_active.data(), T, st);
+    upload(c->tile_list, c->h_active_list.data(), c->h_active_list.size(), st);
+    tk::launch_fill_tiles(c->image.ptr, c->width, c->height, c->tw, c->tile_list.ptr,
+                          uint32_t(c->h_active_list.size()), c->clear, st);
+    c->active_mask = c->tile_active.ptr;
+    c->active_list = c->tile_list.ptr;
+    c->active_n = uint32_t(c->h_active_list.size());
+    struct Reset {
+        tk_ctx* c;
+        ~Reset() {
+            c->active_mask = nullptr;
+            c->active_list = nullptr;
+            c->active_n = 0;
+        }
+    } reset{c};
+    for (const Step& step : c->steps) run_pass(c, c->passes[step.pass], c->image.ptr);
+    TK_CUDA(cudaGetLastError());
+    c->rendered = true;
+    c->history = true;
+    c->history_w = c->width;
+    c->history_h = c->height;
+    c->history_clear = c->clear;
 }
 
 void drop_graph(tk_ctx* c) {
@@ -774,6 +834,7 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
 // Merges one-pass scenes into one batched pass: arrays concatenated with their
 // indices offset, one BatchScene per canvas.
 void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
+    c->history = false;  // the image becomes the batch's canvases
     c->have_scene = false;
     c->rendered = false;
     c->diff.ready = false;
@@ -1040,6 +1101,8 @@ void tk_ctx_destroy(tk_ctx* c) {
     drop_graph(c);
     c->d_scenes.release(); c->bin_scene.release(); c->tile_scene.release();
     c->flat.release();
+    c->tile_active.release();
+    c->tile_list.release();
     DiffState& D = c->diff;
     D.colp.release(); D.target.release(); D.layer.release(); D.t1.release(); D.blurred.release(); D.gI.release();
     D.d0.release(); D.d1.release(); D.scratch.release(); D.line_acc.release(); D.color_acc.release();
@@ -1066,6 +1129,55 @@ int32_t tk_render(tk_ctx* c) {
     return guarded(c, [&] {
         if (c->batched) do_batch_render(c);
         else do_render(c);
+    });
+}
+
+int32_t tk_render_incremental(tk_ctx* c, const tk_damage* damage, float full_redraw_ratio,
+                              tk_incremental_stats* stats) {
+    return guarded(c, [&] {
+        if (!damage) invalid("null damage");
+        if (damage->rect_count && !damage->rects) invalid("null damage rects");
+        if (!(full_redraw_ratio > 0.0f && full_redraw_ratio <= 1.0f)) invalid("full_redraw_ratio outside (0, 1]");
+        if (c->batched) invalid("incremental rendering takes one uploaded scene, not a batch");
+        if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
+        const uint32_t T = c->tw * c->th;
+        tk_incremental_stats out{};
+        out.total_tiles = T;
+        uint32_t reason = TK_FULL_NONE;
+        if (damage->full) reason = TK_FULL_REQUESTED;
+        else if (!c->history || c->history_w != c->width || c->history_h != c->height || c->history_clear != c->clear)
+            reason = TK_FULL_NO_HISTORY;
+        else if (c->steps.size() != c->passes.size()) reason = TK_FULL_FILTERS;  // blur begin/end steps
+        if (reason == TK_FULL_NONE) {
+            // DamageTiles: every tile that meets a damage rectangle
+            c->h_active.assign(T, 0u);
+            for (uint32_t k = 0; k < damage->rect_count; ++k) {
+                const int32_t* r = damage->rects + 4 * size_t(k);
+                const int32_t x0 = std::max(r[0], 0), y0 = std::max(r[1], 0);
+                const int32_t x1 = std::min(r[2], int32_t(c->width)), y1 = std::min(r[3], int32_t(c->height));
+                if (x1 <= x0 || y1 <= y0) continue;
+                const uint32_t tx0 = uint32_t(x0) / TK_TILE_SIZE, ty0 = uint32_t(y0) / TK_TILE_SIZE;
+                const uint32_t tx1 = (uint32_t(x1) + TK_TILE_SIZE - 1u) / TK_TILE_SIZE;
+                const uint32_t ty1 = (uint32_t(y1) + TK_TILE_SIZE - 1u) / TK_TILE_SIZE;
+                for (uint32_t ty = ty0; ty < ty1; ++ty)
+                    std::memset(c->h_active.data() + size_t(ty) * c->tw + tx0, 1, tx1 - tx0);
+            }
+            c->h_active_list.clear();
+            for (uint32_t t = 0; t < T; ++t)
+                if (c->h_active[t]) c->h_active_list.push_back(t);
+            if (double(c->h_active_list.size()) >= double(full_redraw_ratio) * double(T)) reason = TK_FULL_THRESHOLD;
+        }
+        if (reason != TK_FULL_NONE) {
+            do_render(c);
+            out.dirty_tiles = T;
+            out.full_redraw = 1u;
+        } else {
+            out.dirty_tiles = uint32_t(c->h_active_list.size());
+            if (out.dirty_tiles) do_render_tiles(c);
+            else c->rendered = true;  // nothing changed: the image is the frame
+        }
+        out.reason = reason;
+        if (stats) *stats = out;
     });
 }
 

@@ -170,6 +170,14 @@ __global__ void k_composite(uint32_t* dst, const uint32_t* src, uint32_t width, 
 }
 
 // One block row per scene of a batched pass: its image region to its clear colour.
+// One CTA per listed tile, one thread per pixel.
+__global__ void k_fill_tiles(uint32_t* image, uint32_t width, uint32_t height, uint32_t tw,
+                             const uint32_t* __restrict__ tiles, uint32_t value) {
+    const uint32_t t = tiles[blockIdx.x];
+    const uint32_t x = (t % tw) * TK_TILE_SIZE + (threadIdx.x & 15u), y = (t / tw) * TK_TILE_SIZE + (threadIdx.x >> 4);
+    if (x < width && y < height) image[uint64_t(y) * width + x] = value;
+}
+
 __global__ void k_fill_scenes(uint32_t* image, const BatchScene* __restrict__ scenes) {
     const BatchScene sc = scenes[blockIdx.y];
     const uint64_t n = uint64_t(sc.width) * sc.height;
@@ -205,6 +213,11 @@ void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st) {
     if (n == 0) return;
     uint64_t g = (n + 255) / 256;
     k_fill<<<unsigned(g > 148 * 16 ? 148 * 16 : g), 256, 0, st>>>(image, n, value);
+}
+
+void launch_fill_tiles(uint32_t* image, uint32_t width, uint32_t height, uint32_t tw, const uint32_t* tiles,
+                       uint32_t n, uint32_t value, cudaStream_t st) {
+    if (n) k_fill_tiles<<<n, TK_TILE_PIXELS, 0, st>>>(image, width, height, tw, tiles, value);
 }
 
 void launch_fill_scenes(uint32_t* image, const BatchScene* scenes, uint32_t scene_count, cudaStream_t st) {

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/tileink.h"
@@ -348,6 +349,38 @@ struct Cmd {
     uint32_t children;
 };
 
+// One recorded Canvas call with its original geometry, for replay into
+// another canvas under an extra transform (a retained scene node's content).
+struct RecCmd {
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP } kind = FILL;
+    tk_path path;
+    bool has_brush = false;
+    tk_brush_desc brush{};
+    std::vector<tk_gradient_stop> stops;
+    bool has_transform = false;
+    double t[6] = {1, 0, 0, 1, 0, 0};
+    uint32_t rule = 0;
+    double tolerance = 0.1, width = 0.0;
+    float sigma = 0.0f;
+};
+
+RecCmd rec_cmd(RecCmd::Kind kind, const tk_path* path, const tk_brush_desc* brush, const double* transform) {
+    RecCmd r;
+    r.kind = kind;
+    if (path) r.path = *path;
+    if (brush) {
+        r.has_brush = true;
+        r.brush = *brush;
+        if (brush->stop_count && brush->stops) r.stops.assign(brush->stops, brush->stops + brush->stop_count);
+        r.brush.stops = nullptr;
+    }
+    if (transform) {
+        r.has_transform = true;
+        std::memcpy(r.t, transform, sizeof(r.t));
+    }
+    return r;
+}
+
 }  // namespace
 
 struct tk_canvas {
@@ -378,6 +411,9 @@ struct tk_canvas {
     std::vector<tk_flatten_el> stroke_els;
     std::vector<tk_stroke_polyline> polylines;
     std::vector<tk_stroke_desc> strokes;
+    // command log for replay (tk_canvas_set_keep_commands)
+    bool keep = false;
+    std::vector<RecCmd> log;
 };
 
 namespace {
@@ -692,7 +728,14 @@ void tk_canvas_set_clear_color(tk_canvas* c, uint32_t premul) { c->clear = premu
 int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, const double* transform,
                             uint32_t fill_rule, double tolerance) {
     if (!c || !path || fill_rule > 1u || !(tolerance > 0.0)) return -1;
-    return push_path_with_tag(c, *path, brush, transform, fill_rule, tolerance, TK_DRAW_BRUSH, true);
+    const int64_t draw = push_path_with_tag(c, *path, brush, transform, fill_rule, tolerance, TK_DRAW_BRUSH, true);
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::FILL, path, brush, transform);
+        r.rule = fill_rule;
+        r.tolerance = tolerance;
+        c->log.push_back(std::move(r));
+    }
+    return draw;
 }
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, double width,
                               const double* transform, double tolerance) {
@@ -729,6 +772,12 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
     }
     c->path_els.push_back(uint32_t(c->els.size()));  // no fill elements
     c->path_els.push_back(0u);
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::STROKE, path, brush, transform);
+        r.width = width;
+        r.tolerance = tolerance;
+        c->log.push_back(std::move(r));
+    }
     return add_path(c, bb, line_start, uint32_t(c->lines.size()) - line_start, brush, TK_FILL_NONZERO, TK_DRAW_BRUSH,
                     true);
 }
@@ -740,6 +789,12 @@ int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const doubl
     c->lists.emplace_back();
     c->lists[c->stack.back()].push_back({Cmd::CLIP, uint32_t(draw), 0.0f, child});
     c->stack.push_back(child);
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::CLIP, path, nullptr, transform);
+        r.rule = rule;
+        r.tolerance = tolerance;
+        c->log.push_back(std::move(r));
+    }
     return 0;
 }
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) {
@@ -750,13 +805,23 @@ int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) {
     c->lists[c->stack.back()].push_back({Cmd::BLUR, 0u, physical, child});
     c->stack.push_back(child);
     c->dirty = true;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::BLUR, nullptr, nullptr, nullptr);
+        r.sigma = sigma;
+        c->log.push_back(std::move(r));
+    }
     return 0;
 }
 int32_t tk_canvas_pop_layer(tk_canvas* c) {
     if (c->stack.size() <= 1) return -1;
     c->stack.pop_back();
     c->dirty = true;
+    if (c->keep) c->log.push_back(rec_cmd(RecCmd::POP, nullptr, nullptr, nullptr));
     return 0;
+}
+
+void tk_canvas_set_keep_commands(tk_canvas* c, int32_t enabled) {
+    if (c) c->keep = enabled != 0;
 }
 
 int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
@@ -1146,3 +1211,284 @@ uint64_t tk_diff_flatten(const tk_diff_scene* sc, tk_line* lines, uint32_t* endp
     }
     return count;
 }
+
+// ---------------------------------------------------------------------------
+// Replay and retained scenes (RetainedScene, src/retained_scene/scene.rs and
+// transaction.rs; the materializer's damage, src/render/incremental.rs).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+// The affine map `outer` applied after `inner` (x' = a x + c y + e,
+// y' = b x + d y + f).
+void affine_after(const double o[6], const double i[6], double out[6]) {
+    out[0] = o[0] * i[0] + o[2] * i[1];
+    out[1] = o[1] * i[0] + o[3] * i[1];
+    out[2] = o[0] * i[2] + o[2] * i[3];
+    out[3] = o[1] * i[2] + o[3] * i[3];
+    out[4] = o[0] * i[4] + o[2] * i[5] + o[4];
+    out[5] = o[1] * i[4] + o[3] * i[5] + o[5];
+}
+
+int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
+    double m[6];
+    const double* t = nullptr;
+    if (node_t && r.has_transform) {
+        affine_after(node_t, r.t, m);
+        t = m;
+    } else if (node_t) {
+        t = node_t;
+    } else if (r.has_transform) {
+        t = r.t;
+    }
+    tk_brush_desc b = r.brush;
+    b.stops = r.stops.empty() ? nullptr : r.stops.data();
+    const tk_brush_desc* bp = r.has_brush ? &b : nullptr;
+    switch (r.kind) {
+        case RecCmd::FILL: return tk_canvas_push_path(dst, &r.path, bp, t, r.rule, r.tolerance) < 0 ? -1 : 0;
+        case RecCmd::STROKE: return tk_canvas_push_stroke(dst, &r.path, bp, r.width, t, r.tolerance) < 0 ? -1 : 0;
+        case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
+        case RecCmd::BLUR: return tk_canvas_push_blur_group(dst, r.sigma);
+        case RecCmd::POP: return tk_canvas_pop_layer(dst);
+    }
+    return -1;
+}
+
+bool has_layers(const std::vector<RecCmd>& log) {
+    for (const RecCmd& r : log)
+        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR) return true;
+    return false;
+}
+
+using Content = std::shared_ptr<const std::vector<RecCmd>>;
+
+struct RNode {
+    uint64_t id;
+    Content content;
+    bool layered;
+    bool has_t;
+    double t[6];
+    uint64_t rev;
+};
+
+struct Drawn {
+    uint64_t rev;
+    bool layered;
+    std::vector<tk_pixel_bounds> rects;
+};
+
+}  // namespace
+
+struct tk_retained {
+    uint32_t lw = 0, lh = 0;
+    float scale = 1.0f;
+    uint32_t clear = 0;
+    bool device_flatten = false;
+    std::vector<RNode> nodes;  // painter order
+    uint64_t version = 0, next_rev = 1;
+    bool materialized = false, pending_all = true;
+    std::vector<int32_t> pending_rects;
+    std::unordered_map<uint64_t, Drawn> drawn;  // per node at the last materialization
+    tk_canvas* canvas = nullptr;
+    std::vector<int32_t> damage;
+};
+
+namespace {
+
+int64_t find_node(const tk_retained* rs, uint64_t id) {
+    for (size_t k = 0; k < rs->nodes.size(); ++k)
+        if (rs->nodes[k].id == id) return int64_t(k);
+    return -1;
+}
+
+// A node's content: the canvas's command log, which must be kept and close
+// every layer it opens.
+bool content_of(const tk_canvas* c, Content& out, bool& layered) {
+    if (!c || !c->keep || c->stack.size() != 1) return false;
+    out = std::make_shared<const std::vector<RecCmd>>(c->log);
+    layered = has_layers(c->log);
+    return true;
+}
+
+void set_node_transform(RNode& n, const double* t) {
+    n.has_t = t != nullptr;
+    if (t) std::memcpy(n.t, t, sizeof(n.t));
+}
+
+void touched(tk_retained* rs, RNode& n) {
+    n.rev = rs->next_rev++;
+    ++rs->version;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t tk_canvas_replay(tk_canvas* dst, const tk_canvas* src, const double* transform) {
+    if (!dst || !src || !src->keep || src->stack.size() != 1) return -1;
+    for (const RecCmd& r : src->log)
+        if (replay_one(dst, r, transform) != 0) return -1;
+    return 0;
+}
+
+tk_retained* tk_retained_new(uint32_t logical_width, uint32_t logical_height, float scale) {
+    if (!(scale > 0.0f) || !std::isfinite(scale) || !logical_width || !logical_height) return nullptr;
+    auto* rs = new tk_retained();
+    rs->lw = logical_width;
+    rs->lh = logical_height;
+    rs->scale = scale;
+    return rs;
+}
+void tk_retained_free(tk_retained* rs) {
+    if (!rs) return;
+    tk_canvas_free(rs->canvas);
+    delete rs;
+}
+void tk_retained_set_clear_color(tk_retained* rs, uint32_t premul) {
+    if (!rs || rs->clear == premul) return;
+    rs->clear = premul;
+    rs->pending_all = true;
+    ++rs->version;
+}
+void tk_retained_set_device_flatten(tk_retained* rs, int32_t enabled) {
+    if (rs) rs->device_flatten = enabled != 0;  // the same lines either way: no damage
+}
+uint64_t tk_retained_version(const tk_retained* rs) { return rs ? rs->version : 0; }
+
+int32_t tk_retained_insert(tk_retained* rs, uint64_t id, const tk_canvas* content, const double* transform,
+                           uint64_t before) {
+    if (!rs || id == 0 || find_node(rs, id) >= 0) return -1;
+    RNode n{};
+    n.id = id;
+    if (!content_of(content, n.content, n.layered)) return -1;
+    set_node_transform(n, transform);
+    size_t at = rs->nodes.size();
+    if (before) {
+        const int64_t k = find_node(rs, before);
+        if (k < 0) return -1;
+        at = size_t(k);
+    }
+    touched(rs, n);
+    rs->nodes.insert(rs->nodes.begin() + int64_t(at), std::move(n));
+    return 0;
+}
+int32_t tk_retained_replace(tk_retained* rs, uint64_t id, const tk_canvas* content) {
+    const int64_t k = rs ? find_node(rs, id) : -1;
+    if (k < 0) return -1;
+    RNode& n = rs->nodes[size_t(k)];
+    Content c;
+    bool layered = false;
+    if (!content_of(content, c, layered)) return -1;
+    n.content = std::move(c);
+    n.layered = layered;
+    touched(rs, n);
+    return 0;
+}
+int32_t tk_retained_set_transform(tk_retained* rs, uint64_t id, const double* transform) {
+    const int64_t k = rs ? find_node(rs, id) : -1;
+    if (k < 0) return -1;
+    RNode& n = rs->nodes[size_t(k)];
+    set_node_transform(n, transform);
+    touched(rs, n);
+    return 0;
+}
+int32_t tk_retained_move_before(tk_retained* rs, uint64_t id, uint64_t sibling) {
+    const int64_t k = rs ? find_node(rs, id) : -1;
+    if (k < 0 || sibling == id) return -1;
+    if (sibling && find_node(rs, sibling) < 0) return -1;
+    RNode n = std::move(rs->nodes[size_t(k)]);
+    rs->nodes.erase(rs->nodes.begin() + k);
+    size_t at = rs->nodes.size();
+    if (sibling) at = size_t(find_node(rs, sibling));
+    touched(rs, n);
+    rs->nodes.insert(rs->nodes.begin() + int64_t(at), std::move(n));
+    return 0;
+}
+int32_t tk_retained_remove(tk_retained* rs, uint64_t id) {
+    const int64_t k = rs ? find_node(rs, id) : -1;
+    if (k < 0) return -1;
+    rs->nodes.erase(rs->nodes.begin() + k);
+    ++rs->version;
+    return 0;
+}
+int32_t tk_retained_invalidate_rect(tk_retained* rs, const int32_t rect[4]) {
+    if (!rs || !rect) return -1;
+    rs->pending_rects.insert(rs->pending_rects.end(), rect, rect + 4);
+    ++rs->version;
+    return 0;
+}
+int32_t tk_retained_invalidate_all(tk_retained* rs) {
+    if (!rs) return -1;
+    rs->pending_all = true;
+    ++rs->version;
+    return 0;
+}
+
+tk_canvas* tk_retained_materialize(tk_retained* rs, tk_damage* damage) {
+    if (!rs) return nullptr;
+    tk_canvas* c = tk_canvas_new(rs->lw, rs->lh, rs->scale);
+    if (!c) return nullptr;
+    c->host_plan = false;
+    if (rs->device_flatten) tk_canvas_set_device_flatten(c, 1);
+    c->clear = rs->clear;
+    std::unordered_map<uint64_t, Drawn> now;
+    for (const RNode& n : rs->nodes) {
+        const size_t d0 = c->draws.size();
+        for (const RecCmd& r : *n.content) {
+            if (replay_one(c, r, n.has_t ? n.t : nullptr) != 0) {
+                tk_canvas_free(c);
+                return nullptr;
+            }
+        }
+        Drawn d{n.rev, n.layered, {}};
+        for (size_t k = d0; k < c->draws.size(); ++k) {
+            const tk_pixel_bounds& b = c->draws[k].pixel_bounds;
+            if (b.x1 > b.x0 && b.y1 > b.y0) d.rects.push_back(b);
+        }
+        now.emplace(n.id, std::move(d));
+    }
+    // Damage: the draw rectangles, before and after, of every node inserted,
+    // changed, moved or removed since the last materialization. A change to a
+    // node with clip or blur layers can merge or split the draw batches of
+    // other nodes (and so where pixels are stored as RGBA8 between them),
+    // which a rectangle does not bound: such changes damage everything.
+    bool full = !rs->materialized || rs->pending_all;
+    rs->damage.clear();
+    auto add = [&](const std::vector<tk_pixel_bounds>& rects) {
+        for (const tk_pixel_bounds& b : rects) rs->damage.insert(rs->damage.end(), {b.x0, b.y0, b.x1, b.y1});
+    };
+    if (!full) {
+        for (const auto& kv : now) {
+            auto it = rs->drawn.find(kv.first);
+            if (it == rs->drawn.end()) {
+                full = full || kv.second.layered;
+                add(kv.second.rects);
+            } else if (it->second.rev != kv.second.rev) {
+                full = full || kv.second.layered || it->second.layered;
+                add(it->second.rects);
+                add(kv.second.rects);
+            }
+        }
+        for (const auto& kv : rs->drawn) {
+            if (now.count(kv.first)) continue;
+            full = full || kv.second.layered;
+            add(kv.second.rects);
+        }
+        rs->damage.insert(rs->damage.end(), rs->pending_rects.begin(), rs->pending_rects.end());
+    }
+    if (full) rs->damage.clear();
+    rs->drawn = std::move(now);
+    rs->pending_rects.clear();
+    rs->pending_all = false;
+    rs->materialized = true;
+    tk_canvas_free(rs->canvas);
+    rs->canvas = c;
+    if (damage) {
+        damage->full = full ? 1u : 0u;
+        damage->rect_count = uint32_t(rs->damage.size() / 4);
+        damage->rects = rs->damage.empty() ? nullptr : rs->damage.data();
+    }
+    return c;
+}
+
+}  // extern "C"

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
              uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
              uint32_t batch0, tk_tile_record* tiles, tk_ptcl_record* ptcl, uint64_t cap,
              unsigned long long* stats, uint32_t* error, const BatchScene* __restrict__ scenes,
-             const uint32_t* __restrict__ bin_scene) {
+             const uint32_t* __restrict__ bin_scene, const uint8_t* __restrict__ tile_active) {
     __shared__ DrawInfo s_d[kCoarseThreads];
     const uint32_t bin = blockIdx.x / kQuads, quad = blockIdx.x % kQuads;
     uint32_t lbin = bin, tile_base = 0u;
@@ -240,8 +240,14 @@ __global__ void __launch_bounds__(kCoarseThreads)
     const uint32_t qx = quad % (kBinSide / kQuadSide), qy = quad / (kBinSide / kQuadSide);
     const uint32_t tx = (lbin % nbx) * kBinSide + qx * kQuadSide + (threadIdx.x % kQuadSide);
     const uint32_t ty = (lbin / nbx) * kBinSide + qy * kQuadSide + (threadIdx.x / kQuadSide);
-    const bool live = tx < c.tw && ty < c.th;
+    const bool in_canvas = tx < c.tw && ty < c.th;
     const uint32_t tile = tile_base + ty * c.tw + tx;
+    // incremental render: tiles that are not redrawn get no particles
+    const bool live = in_canvas && (!tile_active || tile_active[tile]);
+    if (!__syncthreads_or(live)) {
+        if (!EMIT && in_canvas) tiles[tile].ptcl_count = 0u;
+        return;
+    }
     const uint32_t* list = bin_lists + list_at;
     const uint32_t n = bin_counts[bin];
 
@@ -370,7 +376,10 @@ __global__ void __launch_bounds__(kCoarseThreads)
             }
         }
     }
-    if (!live) return;
+    if (!live) {
+        if (!EMIT && in_canvas) tiles[tile].ptcl_count = 0u;
+        return;
+    }
     close();
     if (total) total += 1u;
     if (EMIT) {
@@ -481,11 +490,11 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
     if (emit)
         k_coarse<true><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                          p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                         p.stats, s.error, p.scenes, p.bin_scene);
+                                                         p.stats, s.error, p.scenes, p.bin_scene, p.tile_active);
     else
         k_coarse<false><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                           p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                          p.stats, s.error, p.scenes, p.bin_scene);
+                                                          p.stats, s.error, p.scenes, p.bin_scene, p.tile_active);
 }
 
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {

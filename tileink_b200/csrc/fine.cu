@@ -311,10 +311,10 @@ __global__ void __launch_bounds__(kFineThreads, 4)
            const SegmentRec* __restrict__ segments, const tk_draw_record* __restrict__ draws,
            const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
-           const uint32_t* __restrict__ tile_scene) {
+           const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FineSmem& S = *reinterpret_cast<FineSmem*>(smem_raw);
-    const uint32_t tile = blockIdx.x;
+    const uint32_t tile = tile_list ? tile_list[blockIdx.x] : blockIdx.x;
     const tk_tile_record rec = tiles[tile];
     if (rec.ptcl_start >= rec.ptcl_end) return;
     uint32_t ltile = tile;
@@ -596,7 +596,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
 }  // namespace
 
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st) {
-    const uint32_t T = p.scenes ? p.total_tiles : s.tw * s.th;
+    const uint32_t T = p.tile_list ? p.tile_list_n : (p.scenes ? p.total_tiles : s.tw * s.th);
     if (T == 0) return;
     static bool configured = false;
     if (!configured) {
@@ -605,7 +605,7 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     }
     k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.draws, s.brush, s.brush_words,
                                                       s.segment_capacity, target, s.width, s.height, s.tw, s.error,
-                                                      p.scenes, p.tile_scene);
+                                                      p.scenes, p.tile_scene, p.tile_list);
 }
 
 }  // namespace tk

@@ -128,6 +128,11 @@ struct PassView {
     const uint32_t* bin_scene;
     const uint32_t* tile_scene;
     uint32_t total_bins, total_tiles, scene_count;
+    // incremental render (null: every tile): per tile 1 when it is redrawn,
+    // and the list of those tiles
+    const uint8_t* tile_active;
+    const uint32_t* tile_list;
+    uint32_t tile_list_n;
 };
 void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
@@ -140,6 +145,9 @@ void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);
 // get path_base[k] added to their path ids.
 void launch_rebase_lines(tk_line* lines, uint64_t n, const uint64_t* line_base, const uint32_t* path_base,
                          uint32_t scenes, cudaStream_t st);
+// Sets the pixels of the listed 16x16 tiles of a width x height image to value.
+void launch_fill_tiles(uint32_t* image, uint32_t width, uint32_t height, uint32_t tw, const uint32_t* tiles,
+                       uint32_t n, uint32_t value, cudaStream_t st);
 // Clears every scene's image region of a batched pass to its clear colour.
 void launch_fill_scenes(uint32_t* image, const BatchScene* scenes, uint32_t scene_count, cudaStream_t st);
 struct BlurParams {

@@ -59,6 +59,30 @@ class NativeRenderer:
     def render(self) -> None:
         self._check(self._lib.tk_render(self._h))
 
+    def render_incremental(self, damage=None, full_redraw_ratio: float = 0.7) -> dict:
+        """Renders the uploaded scene, redrawing only the tiles under `damage`
+        ({"full": bool, "rects": n x 4 int32 [x0, y0, x1, y1] pixels}; None =
+        everything) over the previous frame, or everything when it must
+        (tk_render_incremental). Returns the frame's statistics."""
+        d = N.Damage()
+        rects = None
+        if damage is None or damage.get("full"):
+            d.full = 1
+        else:
+            rects = np.ascontiguousarray(np.asarray(damage["rects"], dtype=np.int32).reshape(-1, 4))
+            d.rect_count = len(rects)
+            d.rects = rects.ctypes.data if len(rects) else None
+        st = N.IncrementalStats()
+        self._check(self._lib.tk_render_incremental(self._h, C.byref(d), float(full_redraw_ratio), C.byref(st)))
+        return {k: int(getattr(st, k)) for k, _ in N.IncrementalStats._fields_}
+
+    def render_retained(self, scene, full_redraw_ratio: float = 0.7) -> dict:
+        """NativeRenderer::render_retained (src/native/renderer/retained.rs:17-23):
+        materializes the retained scene, uploads it and redraws its damage."""
+        canvas, damage = scene.materialize()
+        self.upload(canvas)
+        return self.render_incremental(damage, full_redraw_ratio)
+
     def synchronize(self) -> None:
         self._check(self._lib.tk_synchronize(self._h))
 
