@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--size", type=int, default=0, help="override the canvas side (smaller trial runs)")
     p.add_argument("--diff-steps", type=int, default=10, help="timed fwd+bwd steps of the blur-group workload (0: skip)")
     p.add_argument("--batch-scenes", type=int, default=512, help="scenes of the batched-mode leg (0: skip)")
+    p.add_argument("--incremental-steps", type=int, default=10, help="frames of the incremental leg (0: skip)")
     return p.parse_args()
 
 
@@ -205,6 +206,34 @@ def batch_timing(n_scenes, steps):
             "tune_ms": {str(tune.candidate_elems[i]): tune.candidate_ms[i] for i in range(tune.candidates)},
             "timing": "host wall clock; batched = graph replays + one readback, serial = per-scene upload, "
                       "render and readback"}
+
+
+def incremental_timing(r, size, steps):
+    """Incremental frames of the resident scene (tk_render_incremental, the
+    retained path's damage-driven redraw): each frame a 256x256-pixel damage
+    rectangle at a new place, the scene scanned in full and coarse + fine run
+    on the damaged tiles only over the previous frame; against full frames of
+    the same scene. Host wall clock per frame, synchronized."""
+    side = 256
+    W = size or 4096
+    r.render_incremental(None)  # the history frame
+    r.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(2):
+        r.render_incremental(None)
+    r.synchronize()
+    full_ms = (time.perf_counter() - t0) * 1e3 / 2
+    st = None
+    t0 = time.perf_counter()
+    for k in range(steps):
+        x, y = (k * 331) % (W - side), (k * 197) % (W - side)
+        st = r.render_incremental({"full": False, "rects": [[x, y, x + side, y + side]]})
+    r.synchronize()
+    inc_ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"workload": f"the frame's scene, a {side}x{side}-pixel damage rectangle moved every frame",
+            "incremental_ms": inc_ms, "full_ms": full_ms, "speedup": full_ms / inc_ms,
+            "dirty_tiles": st["dirty_tiles"], "total_tiles": st["total_tiles"], "steps": steps,
+            "timing": "host wall clock per frame, synchronized"}
 
 
 def cpu_baseline(size, paths):
@@ -368,6 +397,9 @@ def main():
     flat_canvas = tk.generate(2, SEED, width=args.size, height=args.size, paths=args.paths, device_flatten=True)
     ps_flat, bytes_in_flat = pinned_scene(flat_canvas)
     e2e_flat_ms = e2e_ms_of(ps_flat)
+    inc_line = None
+    if rank == 0 and args.incremental_steps > 0:
+        inc_line = incremental_timing(r, args.size, args.incremental_steps)
     del ps_flat, flat_canvas
     bytes_out = out.nbytes
 
@@ -455,6 +487,7 @@ def main():
             "cpu_baseline": cpu,
             "fwd_bwd": diff_line,
             "batched": batch_line,
+            "incremental": inc_line,
             "scene_generation_s": gen_s,
         }
         print(json.dumps(line), flush=True)
