@@ -139,6 +139,7 @@ struct tk_ctx {
     DBuf<uint32_t> counts, cursors, bumps, misc;  // misc: [0] error [1] ticket [2] seg total [3] ptcl total
     DBuf<tk_segment_range> ranges;
     DBuf<tk::SegmentRec> segments;
+    DBuf<tk::PaintInfo> paints;  // per draw, built at upload
     uint64_t segment_needed = 0;  // device plan: total from the last frame
     DBuf<uint32_t> image, temp;
     std::vector<DBuf<uint32_t>> surfaces;
@@ -374,6 +375,7 @@ tk::SceneView view(tk_ctx* c) {
     s.segment_capacity = c->segments.cap;
     s.error = c->misc.ptr;
     s.seg_line = c->want_seg_line ? c->seg_line.ptr : nullptr;
+    s.paints = c->paints.ptr;
     s.emit_order = c->emit_order.ptr;
     s.emit_ticket = c->misc.ptr + 4;
     return s;
@@ -446,6 +448,8 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nu
     else upload(c->lines, d.lines, d.line_count, st);
     upload(c->draws, d.draws, d.draw_count, st);
     upload(c->brush, d.brush_blob, d.brush_word_count, st);
+    c->paints.reserve(d.draw_count);
+    tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count, c->paints.ptr, st);
     upload(c->layers, d.layers, d.layer_count, st);
     upload(c->batch_ids, d.draw_batch_ids, d.draw_count, st);
     upload(c->order, d.draw_order, d.draw_order_count, st);
@@ -984,6 +988,8 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     upload(c->paths, paths.data(), paths.size(), st);
     upload(c->draws, draws.data(), draws.size(), st);
     upload(c->brush, brush.data(), brush.size(), st);
+    c->paints.reserve(draws.size());
+    tk::launch_paint_table(c->draws.ptr, uint32_t(draws.size()), c->brush.ptr, brush.size(), c->paints.ptr, st);
     upload(c->layers, layers.data(), layers.size(), st);
     upload(c->batch_ids, batch_ids.data(), batch_ids.size(), st);
     upload(c->order, order.data(), order.size(), st);
@@ -1101,6 +1107,7 @@ void tk_ctx_destroy(tk_ctx* c) {
     drop_graph(c);
     c->d_scenes.release(); c->bin_scene.release(); c->tile_scene.release();
     c->flat.release();
+    c->paints.release();
     c->tile_active.release();
     c->tile_list.release();
     DiffState& D = c->diff;

@@ -6,8 +6,8 @@
 // whose fills together reference at most 128 tile segments. Per chunk the CTA
 // stages into shared memory, with coalesced loads and no dependent global
 // round trips per record:
-//   - the records and each fill's paint, resolved from draw -> brush once per
-//     record;
+//   - the records and each fill's paint, one load of the draw's PaintInfo
+//     (decoded once per upload by k_paint_table);
 //   - the chunk's segments and, per tile row, the compacted list of segments
 //     that cross the row (dy != 0) with their terms of segment_row_parts
 //     (shared/coverage.hlsli:7-24). A segment crosses 4-5 of the 16 rows on
@@ -74,7 +74,7 @@ struct FineSmem {
     uint32_t ualpha[kRecChunk];
     uint32_t umode[kRecChunk];                   // uniform fills: 1 replace, 2 src-over, 3 no-op
     uint32_t paint[kRecChunk];                   // solid premul color, or kGradient
-    float gp[kRecChunk][kGradParams];            // decoded gradient records (stage_gradient)
+    alignas(16) float gp[kRecChunk][kGradParams];  // gradient terms of the chunk's fills (PaintInfo::g)
     uint4 gk[kRecChunk];                         // kind | flags, ramp word (or color), ramp length, extend
     uint32_t nseg[kRecChunk];
     uint32_t off[kRecChunk + 1];
@@ -92,15 +92,14 @@ __device__ __forceinline__ float4 texel_load_lut(const FineSmem& S, uint32_t p) 
 }
 
 // Decodes the gradient brush at word `db` of a fill whose draw has the inverse
-// transform `m` into slot `i`: the transforms, and the terms of
+// transform `m` into g[0..23] and gk: the transforms, and the terms of
 // sample_gradient (fine/paint.hlsli:40-96) that depend on the brush alone,
 // computed with the same f32 operations so that the per-pixel evaluation in
 // gradient_at gives the same bits.
 //   linear: gp[12..16] = sx, sy, dx = ex - sx, dy = ey - sy, den = dx*dx + dy*dy
 //   radial: gp[12..22] = sx, sy, dcx, dcy, sr*dr, -sr*sr, a, -4*a, 2*a, dr, sr
 //           with a = mad(dcx, dcx, mad(dcy, dcy, -dr*dr))
-__device__ void stage_gradient(FineSmem& S, uint32_t i, const Paint& P, uint32_t db, const float* __restrict__ m) {
-    float* g = S.gp[i];
+__device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db, const float* __restrict__ m) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) g[k] = __ldg(m + k);
     const uint32_t kind = P.word(db), extend = P.word(db + 1u);
@@ -143,7 +142,25 @@ __device__ void stage_gradient(FineSmem& S, uint32_t i, const Paint& P, uint32_t
     } else {
         word = kind == 6u ? 0u : P.word(db + TK_BRUSH_COLOR_WORD);  // BRUSH_PATTERN samples as 0
     }
-    S.gk[i] = make_uint4(code | flags, word, len, extend);
+    gk = make_uint4(code | flags, word, len, extend);
+}
+
+// One thread per draw: the draw's PaintInfo (solid colour, or the decoded
+// gradient of its brush under its inverse transform).
+__global__ void k_paint_table(const tk_draw_record* __restrict__ draws, uint32_t n, const uint32_t* __restrict__ brush,
+                              uint64_t brush_words, PaintInfo* out) {
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= n) return;
+    const Paint P{brush, brush_words};
+    const uint32_t bo = draws[d].brush_offset;
+    PaintInfo info{};
+    if (P.word(bo) == TK_BRUSH_SOLID) {
+        info.paint = P.word(bo + TK_BRUSH_COLOR_WORD);
+    } else {
+        info.paint = kGradient;
+        decode_gradient(info.g, info.gk, P, bo, &draws[d].inverse_transform.a);
+    }
+    out[d] = info;
 }
 
 // sample_gradient at pixel centre (px, py) for the gradient decoded in slot i.
@@ -308,7 +325,7 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
 
 __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
-           const SegmentRec* __restrict__ segments, const tk_draw_record* __restrict__ draws,
+           const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
            const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
            const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list) {
@@ -371,10 +388,9 @@ __global__ void __launch_bounds__(kFineThreads, 4)
             }
             S.nseg[tid] = n;
             if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH) {
-                const tk_draw_record& d = draws[c.y];
-                const uint32_t bo = __ldg(&d.brush_offset);
-                if (P.word(bo) == TK_BRUSH_SOLID) {
-                    const uint32_t paint = P.word(bo + TK_BRUSH_COLOR_WORD);
+                const PaintInfo* pi = paints + c.y;
+                const uint32_t paint = __ldg(&pi->paint);
+                if (paint != kGradient) {
                     S.paint[tid] = paint;
                     S.pcf[tid] = make_float4(float(paint & 255u), float((paint >> 8) & 255u),
                                              float((paint >> 16) & 255u), float(paint >> 24));
@@ -394,7 +410,11 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                     }
                 } else {
                     S.paint[tid] = kGradient;
-                    stage_gradient(S, tid, P, bo, &d.inverse_transform.a);
+                    S.gk[tid] = __ldg(&pi->gk);
+                    const float4* g = reinterpret_cast<const float4*>(pi->g);
+                    float4* dst = reinterpret_cast<float4*>(S.gp[tid]);
+#pragma unroll
+                    for (int k = 0; k < kGradParams / 4; ++k) dst[k] = __ldg(g + k);
                 }
             }
             S.cls[tid] = cls;
@@ -595,6 +615,11 @@ __global__ void __launch_bounds__(kFineThreads, 4)
 
 }  // namespace
 
+void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
+                        uint64_t brush_words, PaintInfo* out, cudaStream_t st) {
+    if (draw_count) k_paint_table<<<(draw_count + 255) / 256, 256, 0, st>>>(draws, draw_count, brush, brush_words, out);
+}
+
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st) {
     const uint32_t T = p.tile_list ? p.tile_list_n : (p.scenes ? p.total_tiles : s.tw * s.th);
     if (T == 0) return;
@@ -603,7 +628,7 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
         cudaFuncSetAttribute(k_fine, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
         configured = true;
     }
-    k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.draws, s.brush, s.brush_words,
+    k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
                                                       s.segment_capacity, target, s.width, s.height, s.tw, s.error,
                                                       p.scenes, p.tile_scene, p.tile_list);
 }

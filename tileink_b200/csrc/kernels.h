@@ -43,6 +43,17 @@ struct alignas(32) SegmentRec {
 };
 static_assert(sizeof(SegmentRec) == 32, "one sector per segment");
 
+// A draw's paint as fine raster needs it, decoded once per upload from the
+// draw record and its brush (fine.cu): the solid premultiplied colour, or
+// kGradient with the gradient's brush-only terms.
+struct alignas(16) PaintInfo {
+    uint32_t paint;      // premultiplied RGBA8, or 0xFFFFFFFF for a gradient
+    uint32_t pad[3];
+    uint4 gk;            // kind | flags, ramp word (or colour), ramp length, extend
+    float g[24];         // transforms and brush terms (fine.cu stage_gradient)
+};
+static_assert(sizeof(PaintInfo) == 128, "two 64-byte halves");
+
 struct SceneView {
     const tk_line* lines;
     uint64_t line_count;
@@ -66,6 +77,7 @@ struct SceneView {
     uint64_t segment_capacity;
     uint32_t* error;
     uint32_t* seg_line;  // optional: line index of every emitted segment
+    const PaintInfo* paints;     // per draw (launch_paint_table)
     const uint32_t* emit_order;  // paths by decreasing line count (optional)
     uint32_t* emit_ticket;       // path queue of scan_emit
 };
@@ -138,6 +150,9 @@ void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st);
+// The per-draw PaintInfo table of the uploaded draws and brush blob.
+void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
+                        uint64_t brush_words, PaintInfo* out, cudaStream_t st);
 
 // Images.
 void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);
