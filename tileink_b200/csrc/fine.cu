@@ -65,6 +65,8 @@ struct FineSmem {
     float prod[kProdCap];                        // segment_area_at(x) * dy per partial pixel
     float4 sgp[kSegBudget];                      // staged segments: p0x, p0y, p1x, p1y
     float2 sgx[kSegBudget];                      // y_edge, slope = (p1x - p0x) / (p1y - p0y)
+    uint16_t rmask[kSegBudget];                  // rows the staged segment crosses (dy != 0)
+    uint16_t rpre[kSegBudget + 1];               // crossings of staged segments before j
     float2 rb[kRecChunk][TK_TILE_SIZE];          // per (fill, row): base, k0 | k1 << 16
     float4 pfull[kRecChunk];                     // rgba8_to_unorm(paint) / uniform source
     float4 pcf[kRecChunk];                       // paint channels as floats
@@ -227,8 +229,24 @@ __device__ __forceinline__ RowParts staged_row_parts(const FineSmem& S, uint32_t
     return {0.0f, dy, fminf(sx0, sx1), fmaxf(sx0, sx1)};
 }
 
-// Crossing lists and partial products for staged segments [0, total): warp w
-// builds rows 2w and 2w + 1, lanes walk the segments in order.
+// The rows a segment crosses, i.e. where segment_row_parts gives dy != 0:
+// with lo < hi the segment's y extent, clamp(y - row, 0, 1) differs between
+// its ends exactly for rows floor(lo) .. ceil(hi) - 1 (y - row is exact for y
+// in [row, row + 1], and rounds to the same side of that interval otherwise).
+__device__ __forceinline__ uint32_t crossed_rows(float p0y, float p1y) {
+    const float lo = fminf(p0y, p1y), hi = fmaxf(p0y, p1y);
+    if (!(lo < hi)) return 0u;
+    const int32_t r0 = max(f2i(floorf(lo)), 0), r1 = min(f2i(ceilf(hi)) - 1, int32_t(TK_TILE_SIZE) - 1);
+    if (r1 < r0) return 0u;
+    return ((2u << r1) - 1u) & ~((1u << r0) - 1u);
+}
+
+// Crossing lists and partial products for staged segments [0, total).
+// Positions: warp w ranks rows 2w and 2w + 1, lanes walk the segments in
+// order and rank the crossing ones by ballot (warp 0 also prefixes the
+// segments' crossing counts). Entries: the (segment, row) crossings are spread
+// evenly over the CTA, and only they evaluate segment_row_parts and their
+// partial-area products.
 __device__ void stage_rows(FineSmem& S, uint32_t total) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
@@ -237,43 +255,55 @@ __device__ void stage_rows(FineSmem& S, uint32_t total) {
         uint32_t count = 0;
         for (uint32_t j0 = 0; j0 < total; j0 += 32u) {
             const uint32_t j = j0 + lane;
-            RowParts rp{0.f, 0.f, 0.f, 0.f};
-            if (j < total) rp = staged_row_parts(S, j, row);
-            const bool crossing = j < total && rp.dy != 0.0f;
+            const bool crossing = j < total && ((S.rmask[j] >> row) & 1u);
             const uint32_t ballot = __ballot_sync(0xffffffffu, crossing);
-            const uint32_t k = count + __popc(ballot & lt);
-            if (j < total) S.pos[row][j] = uint16_t(k);
-            uint32_t plo = 0u, phi = 0u, span = 0u;
-            if (crossing) {
-                plo = uint32_t(min(max(f2i(floorf(rp.xmin)), 0), int32_t(TK_TILE_SIZE)));
-                phi = uint32_t(min(max(f2i(ceilf(rp.xmax)), 0), int32_t(TK_TILE_SIZE)));
-                span = phi > plo ? phi - plo : 0u;
-            }
-            // warp-aggregated allocation of the partial products
-            uint32_t incl = span;
+            if (j < total) S.pos[row][j] = uint16_t(count + __popc(ballot & lt));
+            count += __popc(ballot);
+        }
+        if (lane == 0) S.pos[row][total] = uint16_t(count);
+    }
+    if (warp == 0) {
+        uint32_t run = 0;
+        for (uint32_t j0 = 0; j0 < total; j0 += 32u) {
+            const uint32_t j = j0 + lane;
+            const uint32_t c = j < total ? __popc(S.rmask[j]) : 0u;
+            uint32_t incl = c;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
                 if (lane >= uint32_t(d)) incl += v;
             }
-            uint32_t wbase = 0u;
-            if (lane == 31u && incl) wbase = atomicAdd(&S.nprod, incl);
-            wbase = __shfl_sync(0xffffffffu, wbase, 31);
-            if (crossing) {
-                const uint32_t o = wbase + incl - span;
-                uint32_t word = plo | (phi << 5);
-                if (o + span <= kProdCap) {
-                    for (uint32_t x = 0; x < span; ++x)
-                        S.prod[o + x] = segment_area_at(rp.xmin, rp.xmax, plo + x) * rp.dy;
-                    word |= o << 16;
-                } else {
-                    word |= kEntSlow | (j << 16);
-                }
-                S.ent[row][k] = make_float2(rp.dy, __uint_as_float(word));
-            }
-            count += __popc(ballot);
+            if (j < total) S.rpre[j] = uint16_t(run + incl - c);
+            run += __shfl_sync(0xffffffffu, incl, 31);
         }
-        if (lane == 0) S.pos[row][total] = uint16_t(count);
+        if (lane == 0) S.rpre[total] = uint16_t(run);
+    }
+    __syncthreads();
+    const uint32_t items = S.rpre[total];
+    for (uint32_t it = threadIdx.x; it < items; it += kFineThreads) {
+        uint32_t lo = 0, hi = total;  // staged segment j with rpre[j] <= it < rpre[j + 1]
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (S.rpre[mid] <= it) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t j = lo;
+        uint32_t m = S.rmask[j];  // the row of this crossing: its (it - rpre[j])-th set bit
+        for (uint32_t k = it - S.rpre[j]; k; --k) m &= m - 1u;
+        const uint32_t row = uint32_t(__ffs(m) - 1);
+        const RowParts rp = staged_row_parts(S, j, row);
+        const uint32_t plo = uint32_t(min(max(f2i(floorf(rp.xmin)), 0), int32_t(TK_TILE_SIZE)));
+        const uint32_t phi = uint32_t(min(max(f2i(ceilf(rp.xmax)), 0), int32_t(TK_TILE_SIZE)));
+        const uint32_t span = phi > plo ? phi - plo : 0u;
+        uint32_t word = plo | (phi << 5);
+        const uint32_t o = span ? atomicAdd(&S.nprod, span) : 0u;
+        if (o + span <= kProdCap) {
+            for (uint32_t x = 0; x < span; ++x) S.prod[o + x] = segment_area_at(rp.xmin, rp.xmax, plo + x) * rp.dy;
+            word |= o << 16;
+        } else {
+            word |= kEntSlow | (j << 16);
+        }
+        S.ent[row][S.pos[row][j]] = make_float2(rp.dy, __uint_as_float(word));
     }
 }
 
@@ -453,9 +483,11 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                     else hi = mid;
                 }
                 const float4* g = reinterpret_cast<const float4*>(segments + S.rec_a[lo].w + (sg - S.off[lo]));
-                S.sgp[sg] = __ldg(g);
+                const float4 q = __ldg(g);
                 const float4 e = __ldg(g + 1);  // y_edge, slope
+                S.sgp[sg] = q;
                 S.sgx[sg] = make_float2(e.x, e.y);
+                S.rmask[sg] = uint16_t(crossed_rows(q.y, q.w));
             }
             __syncthreads();
             stage_rows(S, total);
