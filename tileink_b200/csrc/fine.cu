@@ -241,13 +241,14 @@ __device__ __forceinline__ uint32_t crossed_rows(float p0y, float p1y) {
     return ((2u << r1) - 1u) & ~((1u << r0) - 1u);
 }
 
-// Crossing lists and partial products for staged segments [0, total).
+// Crossing lists and partial products for staged segments [0, total) of the
+// chunk's first n records, and the per (fill, row) base sums.
 // Positions: warp w ranks rows 2w and 2w + 1, lanes walk the segments in
 // order and rank the crossing ones by ballot (warp 0 also prefixes the
 // segments' crossing counts). Entries: the (segment, row) crossings are spread
 // evenly over the CTA, and only they evaluate segment_row_parts and their
 // partial-area products.
-__device__ void stage_rows(FineSmem& S, uint32_t total) {
+__device__ void stage_rows(FineSmem& S, uint32_t total, uint32_t n) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     for (uint32_t rr = 0; rr < 2u; ++rr) {
@@ -279,6 +280,23 @@ __device__ void stage_rows(FineSmem& S, uint32_t total) {
         if (lane == 0) S.rpre[total] = uint16_t(run);
     }
     __syncthreads();
+    // per (fill, row): the base sum and the row's entry range (needs the
+    // positions only, so it shares this phase with the entries below)
+    for (uint32_t k = threadIdx.x; k < n * TK_TILE_SIZE; k += kFineThreads) {
+        const uint32_t ri = k >> 4, row = k & 15u;
+        const uint32_t j0 = S.off[ri], ns = S.nseg[ri];
+        if (ns == 0u) continue;
+        float bsum = float(int32_t(S.rec_a[ri].y));
+        for (uint32_t j = j0; j < j0 + ns; ++j) {
+            const float ye = S.sgx[j].x;
+            if (ye < 1000000000.0f) {  // y_edge set: the segment touches the tile's left edge
+                const float4 g = S.sgp[j];
+                bsum += signum_f32(g.z - g.x) * clampf(float(row) - ye + 1.0f, 0.0f, 1.0f);
+            }
+        }
+        const uint32_t k0 = S.pos[row][j0], k1 = S.pos[row][j0 + ns];
+        S.rb[ri][row] = make_float2(bsum, __uint_as_float(k0 | (k1 << 16)));
+    }
     const uint32_t items = S.rpre[total];
     for (uint32_t it = threadIdx.x; it < items; it += kFineThreads) {
         uint32_t lo = 0, hi = total;  // staged segment j with rpre[j] <= it < rpre[j + 1]
@@ -490,23 +508,7 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 S.rmask[sg] = uint16_t(crossed_rows(q.y, q.w));
             }
             __syncthreads();
-            stage_rows(S, total);
-            __syncthreads();
-            for (uint32_t k = tid; k < n * TK_TILE_SIZE; k += kFineThreads) {
-                const uint32_t ri = k >> 4, row = k & 15u;
-                const uint32_t j0 = S.off[ri], ns = S.nseg[ri];
-                if (ns == 0u) continue;
-                float bsum = float(int32_t(S.rec_a[ri].y));
-                for (uint32_t j = j0; j < j0 + ns; ++j) {
-                    const float ye = S.sgx[j].x;
-                    if (ye < 1000000000.0f) {  // y_edge set: the segment touches the tile's left edge
-                        const float4 g = S.sgp[j];
-                        bsum += signum_f32(g.z - g.x) * clampf(float(row) - ye + 1.0f, 0.0f, 1.0f);
-                    }
-                }
-                const uint32_t k0 = S.pos[row][j0], k1 = S.pos[row][j0 + ns];
-                S.rb[ri][row] = make_float2(bsum, __uint_as_float(k0 | (k1 << 16)));
-            }
+            stage_rows(S, total, n);
             __syncthreads();
         }
         // ---- interpret the chunk -------------------------------------------------
