@@ -85,8 +85,29 @@ extern "C" {
 #define TK_TILE_KIND_INTERPRETER 0u
 #define TK_TILE_KIND_EMPTY 1u
 #define TK_TILE_KIND_COLOR 2u
+#define TK_TILE_KIND_SDF 3u
+#define TK_TILE_KIND_MIXED 4u
 #define TK_TILE_KIND_MASK 7u
 #define TK_TILE_PREFIX_SHIFT 3u
+
+/* SDF records (src/shared/gpu_sdf.rs:27-46, shaders/hlsl/shared/sdf/
+ * constants.hlsli:3-21): TK_SDF_RECORD_WORDS words per shape, word 0 the kind,
+ * then four coordinate, four radius, four stroke and four shadow words as
+ * floats (coverage.hlsli:13-30). A draw's sdf_offset indexes the scene's
+ * sdf_blob, its sdf_shadow_offset the sdf_shadow_blob. The kinds below are
+ * the ones this library renders; other kinds are rejected at upload. */
+#define TK_SDF_RECORD_WORDS 17u
+#define TK_SDF_RECT 1u
+#define TK_SDF_CIRCLE 2u
+#define TK_SDF_RECT_STROKE 3u
+#define TK_SDF_CIRCLE_STROKE 4u
+#define TK_SDF_LINE 6u
+#define TK_SDF_RECT_SHADOW 7u
+#define TK_SDF_CIRCLE_SHADOW 10u
+#define TK_SDF_LINE_SHADOW 11u
+#define TK_SDF_CAP_BUTT 0u
+#define TK_SDF_CAP_SQUARE 1u
+#define TK_SDF_CAP_ROUND 2u
 
 /* Brush blob layout (shaders/hlsl/shared/brush/constants.hlsli:3-22,
  * src/shared/brush.rs:249-340). A brush record is a 9-word header followed by
@@ -233,6 +254,11 @@ typedef struct tk_scene_desc {
     const tk_op* ops;
     uint32_t op_count;
     uint32_t reserved;
+    /* Canvas::sdf_blob / sdf_shadow_blob (src/canvas.rs:92-93) */
+    const uint32_t* sdf_blob;
+    uint64_t sdf_word_count;
+    const uint32_t* sdf_shadow_blob;
+    uint64_t sdf_shadow_word_count;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

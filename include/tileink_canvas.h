@@ -4,6 +4,8 @@
  * Mirrors the recording API of the reference's Canvas for the vector path:
  *   push_path            src/canvas/primitives/paths.rs:50-60 -> canvas/paths.rs:42-156
  *   push_stroke          src/canvas/primitives/paths.rs:24-48
+ *   push_rect / push_circle / push_line and their strokes and shadows
+ *                        src/canvas/primitives/{rectangles,shapes,shadows}.rs
  *   push_clip_layer      src/canvas/layers.rs:7-28
  *   push_blur_group      src/canvas/layers.rs:205-212
  *   pop_layer            src/canvas/layers.rs
@@ -81,6 +83,32 @@ int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_de
                             const double* transform, uint32_t fill_rule, double tolerance);
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
                               double width, const double* transform, double tolerance);
+/* Analytic SDF shapes (Canvas::push_rect, push_rect_stroke(_widths),
+ * push_circle, push_circle_stroke, push_line and push_{rect,circle,line}_shadow,
+ * src/canvas/primitives/{rectangles,shapes,shadows}.rs:5-110), in logical
+ * coordinates. kind selects the fields used:
+ *   TK_SDF_RECT           p0, p1 corners; radii
+ *   TK_SDF_RECT_STROKE    p0, p1; radii; widths (full side widths)
+ *   TK_SDF_CIRCLE         p0 centre; radius
+ *   TK_SDF_CIRCLE_STROKE  p0; radius; width (full stroke width)
+ *   TK_SDF_LINE           p0, p1 ends; width; cap
+ *   TK_SDF_*_SHADOW       the shape's fields plus shadow
+ * The draw is recorded as one SDF record (identity draw transform) whose
+ * pixel bounds follow the reference's Sdf::bounds / SdfShadow::bounds. */
+typedef struct tk_sdf_shape {
+    uint32_t kind;       /* TK_SDF_* */
+    uint32_t cap;        /* lines: TK_SDF_CAP_* */
+    double p0[2], p1[2];
+    double radius;       /* circles */
+    double width;        /* circle strokes and lines */
+    float radii[4];      /* corner radii: top-left, top-right, bottom-left, bottom-right */
+    float widths[4];     /* rect stroke side widths: top, right, bottom, left */
+    float shadow[4];     /* offset x, offset y, expand (falloff length), intensity */
+} tk_sdf_shape;
+/* Returns the draw index, -2 when the shape draws nothing (a non-positive
+ * stroke width, an empty line, a shadow of zero intensity: the reference's
+ * None), or -1 on error. */
+int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush);
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
                                   uint32_t fill_rule, double tolerance);
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);

@@ -53,6 +53,10 @@ def lib() -> C.CDLL:
         l.or_blur_pass.argtypes = [P, P, U32, U32, P, P, F32, U32]
         l.or_fill_value.restype = F32
         l.or_fill_value.argtypes = [P, U32, I32, U32, U32]
+        l.or_sdf_coverage.restype = F32
+        l.or_sdf_coverage.argtypes = [P, F32, F32, P]
+        l.or_exp_nonpos.restype = F32
+        l.or_exp_nonpos.argtypes = [F32]
         l.or_diff_loss.restype = C.c_double
         l.or_diff_loss.argtypes = [U32, U32, U32, U64, P, P, P, P, P, C.c_double, I32, P, P, P, I32]
         _lib = l

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <functional>
+#include <limits>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -493,6 +494,174 @@ uint32_t sample_draw_brush(const Paint& P, const tk_draw_record& d, float x, flo
     return color;               // other kinds are outside this path
 }
 
+
+// ---------------------------------------------------------------------------
+// SDF shapes (shared/sdf/{base,basic,line,coverage}.hlsli). `length` is
+// sqrt(x*x + y*y) unfused; `mad` sites are fused as everywhere in this file.
+// ---------------------------------------------------------------------------
+struct SdfS { float dist, nx, ny; };
+
+// shared/sdf/base.hlsli:7-12
+float sdf_len(float x, float y) {
+    float m = std::sqrt(x * x + y * y);
+    if (m > 0.0f && std::isfinite(m)) return m;
+    float axis = fmax_(std::fabs(x), std::fabs(y));
+    if (axis == 0.0f) return 0.0f;
+    float sx = x / axis, sy = y / axis;
+    return axis * std::sqrt(sx * sx + sy * sy);
+}
+// shared/sdf/base.hlsli:14-23
+void sdf_unit_or(float x, float y, float fx, float fy, float& ox, float& oy) {
+    float m = std::sqrt(x * x + y * y);
+    if (m > 0.0f && std::isfinite(m)) { ox = x / m; oy = y / m; return; }
+    float axis = fmax_(std::fabs(x), std::fabs(y));
+    if (axis == 0.0f) { ox = fx; oy = fy; return; }
+    float sx = x / axis, sy = y / axis, l = std::sqrt(sx * sx + sy * sy);
+    ox = sx / l;
+    oy = sy / l;
+}
+// shared/sdf/basic.hlsli:6-19
+SdfS sdf_rounded_box(float px, float py, float hx, float hy, float radius) {
+    float qx = std::fabs(px) - hx + radius, qy = std::fabs(py) - hy + radius;
+    float ox = fmax_(qx, 0.0f), oy = fmax_(qy, 0.0f);
+    float ol = sdf_len(ox, oy);
+    float dist = fmin_(fmax_(qx, qy), 0.0f) + ol - radius;
+    float sgx = px >= 0.0f ? 1.0f : -1.0f, sgy = py >= 0.0f ? 1.0f : -1.0f;
+    if (ol > 0.0f) return {dist, ox / ol * sgx, oy / ol * sgy};
+    if (qx > qy) return {dist, sgx, 0.0f};
+    return {dist, 0.0f, sgy};
+}
+// shared/sdf/basic.hlsli:21-25
+SdfS sdf_line_rect(float axis, float normal, float x0, float x1, float hh) {
+    float center = (x0 + x1) * 0.5f, hw = (x1 - x0) * 0.5f;
+    return sdf_rounded_box(axis - center, normal, hw, hh, 0.0f);
+}
+// shared/sdf/basic.hlsli:27-32
+SdfS sdf_circle(float x, float y, float cx, float cy, float radius) {
+    float dx = x - cx, dy = y - cy;
+    SdfS r;
+    r.dist = sdf_len(dx, dy) - radius;
+    sdf_unit_or(dx, dy, 1.0f, 0.0f, r.nx, r.ny);
+    return r;
+}
+// shared/sdf/basic.hlsli:34-57
+SdfS sdf_rect(float x, float y, float x0r, float y0r, float x1r, float y1r, float tl, float tr, float bl, float br) {
+    float x0 = fmin_(x0r, x1r), y0 = fmin_(y0r, y1r), x1 = fmax_(x0r, x1r), y1 = fmax_(y0r, y1r);
+    float cx = (x0 + x1) * 0.5f, cy = (y0 + y1) * 0.5f, hx = (x1 - x0) * 0.5f, hy = (y1 - y0) * 0.5f;
+    float px = x - cx, py = y - cy;
+    float radius = tl;
+    if (px >= 0.0f) {
+        radius = py <= 0.0f ? tr : br;
+    } else if (py > 0.0f) {
+        radius = bl;
+    }
+    return sdf_rounded_box(px, py, hx, hy, fmax_(fmin_(fmin_(radius, hx), hy), 0.0f));
+}
+// shared/sdf/line.hlsli:8-14, 41-76
+SdfS sdf_line(float x, float y, float sx, float sy, float ex, float ey, float width, float cap) {
+    float he = fmax_(width, 0.0f) * 0.5f;
+    float dx = ex - sx, dy = ey - sy;
+    float len = sdf_len(dx, dy);
+    SdfS r{std::numeric_limits<float>::infinity(), 1.0f, 0.0f};
+    if (len == 0.0f) {
+        if (cap >= 0.5f) {
+            if (cap > 1.5f) {
+                float ax = x - sx, ay = y - sy;
+                r.dist = sdf_len(ax, ay) - he;
+                sdf_unit_or(ax, ay, 1.0f, 0.0f, r.nx, r.ny);
+            } else {
+                r = sdf_line_rect(x - sx, y - sy, -he, he, he);
+            }
+        }
+        return r;
+    }
+    float ux = dx / len, uy = dy / len;
+    float px = x - sx, py = y - sy;
+    float axis = px * ux + py * uy;
+    float normal = -px * uy + py * ux;
+    if (cap < 0.5f) {
+        r = sdf_line_rect(axis, normal, 0.0f, len, he);
+    } else if (cap < 1.5f) {
+        r = sdf_line_rect(axis, normal, -he, len + he, he);
+    } else {
+        float nearest = clampf(axis, 0.0f, len);
+        float ax = axis - nearest;
+        r.dist = sdf_len(ax, normal) - he;
+        sdf_unit_or(ax, normal, 0.0f, 1.0f, r.nx, r.ny);
+    }
+    return {r.dist, r.nx * ux - r.ny * uy, r.nx * uy + r.ny * ux};
+}
+// shared/sdf/base.hlsli:39-52
+float sdf_cov(const SdfS& s, const tk_affine& inv) {
+    float gx = mad(inv.a, s.nx, inv.b * s.ny);
+    float gy = mad(inv.c, s.nx, inv.d * s.ny);
+    float fp = sdf_len(gx, gy);
+    if (fp == 0.0f) return s.dist < 0.0f ? 1.0f : (s.dist > 0.0f ? 0.0f : 0.5f);
+    return clampf(0.5f - s.dist / fp, 0.0f, 1.0f);
+}
+// The library evaluates the shadow falloff exp(x), x <= 0, in double as
+// 2^k * e^r (k nearest to x / ln 2, e^r by its degree-13 Taylor series) with
+// only exactly rounded operations; restated so that the two agree bit for
+// bit. Its distance to exp is checked in the tests.
+float exp_nonpos(float x) {
+    if (!(x <= 0.0f)) return x != x ? x : 1.0f;
+    if (x < -104.0f) return 0.0f;
+    const double ln2 = 0.69314718055994530942;
+    double xd = double(x);
+    double k = std::floor(xd / ln2 + 0.5);
+    double r = xd - k * ln2;
+    double p = 1.0;
+    for (int n = 13; n >= 1; --n) p = 1.0 + r * p / double(n);
+    int64_t bits = int64_t(1023 + int64_t(k)) << 52;
+    double scale;
+    std::memcpy(&scale, &bits, sizeof(scale));
+    return float(p * scale);
+}
+// shared/sdf/base.hlsli:54-62
+float sdf_shadow_cov(const SdfS& s, const tk_affine& inv, float expand, float intensity) {
+    float ci = clampf(intensity, 0.0f, 1.0f);
+    if (expand > 0.0f) return clampf(exp_nonpos(-fmax_(s.dist, 0.0f) / expand) * ci, 0.0f, 1.0f);
+    return sdf_cov(s, inv) * ci;
+}
+// sdf_coverage_from_blob (shared/sdf/coverage.hlsli:13-236) for the kinds the
+// library accepts; others have no coverage.
+float sdf_blob_coverage(const uint32_t* w, float x, float y, const tk_affine& inv) {
+    auto f = [&](int i) { return bits_f(w[i]); };
+    uint32_t kind = w[0];
+    float x0 = f(1), y0 = f(2), x1 = f(3), y1 = f(4), r0 = f(5), r1 = f(6), r2 = f(7), r3 = f(8);
+    float st = f(9), sr = f(10), sb = f(11), sl = f(12), ox = f(13), oy = f(14), ex = f(15), in = f(16);
+    if (kind == TK_SDF_RECT) return sdf_cov(sdf_rect(x, y, x0, y0, x1, y1, r0, r1, r2, r3), inv);
+    if (kind == TK_SDF_RECT_STROKE) {
+        float ht = fmax_(st, 0.0f), hr = fmax_(sr, 0.0f), hb = fmax_(sb, 0.0f), hl = fmax_(sl, 0.0f);
+        float rx0 = fmin_(x0, x1), ry0 = fmin_(y0, y1), rx1 = fmax_(x0, x1), ry1 = fmax_(y0, y1);
+        float outer = sdf_cov(sdf_rect(x, y, rx0 - hl, ry0 - ht, rx1 + hr, ry1 + hb, r0 + fmax_(ht, hl),
+                                       r1 + fmax_(ht, hr), r2 + fmax_(hb, hl), r3 + fmax_(hb, hr)),
+                              inv);
+        float ix0 = rx0 + hl, iy0 = ry0 + ht, ix1 = rx1 - hr, iy1 = ry1 - hb;
+        float inner = 0.0f;
+        if (ix0 < ix1 && iy0 < iy1)
+            inner = sdf_cov(sdf_rect(x, y, ix0, iy0, ix1, iy1, fmax_(r0 - fmax_(ht, hl), 0.0f),
+                                     fmax_(r1 - fmax_(ht, hr), 0.0f), fmax_(r2 - fmax_(hb, hl), 0.0f),
+                                     fmax_(r3 - fmax_(hb, hr), 0.0f)),
+                            inv);
+        return clampf(outer - inner, 0.0f, 1.0f);
+    }
+    if (kind == TK_SDF_RECT_SHADOW)
+        return sdf_shadow_cov(sdf_rect(x - ox, y - oy, x0, y0, x1, y1, r0, r1, r2, r3), inv, ex, in);
+    if (kind == TK_SDF_CIRCLE) return sdf_cov(sdf_circle(x, y, x0, y0, x1), inv);
+    if (kind == TK_SDF_CIRCLE_STROKE) {
+        float he = fmax_(st, 0.0f), radius = fmax_(x1, 0.0f);
+        float outer = sdf_cov(sdf_circle(x, y, x0, y0, radius + he), inv);
+        float inner = radius > he ? sdf_cov(sdf_circle(x, y, x0, y0, radius - he), inv) : 0.0f;
+        return clampf(outer - inner, 0.0f, 1.0f);
+    }
+    if (kind == TK_SDF_CIRCLE_SHADOW) return sdf_shadow_cov(sdf_circle(x - ox, y - oy, x0, y0, x1), inv, ex, in);
+    if (kind == TK_SDF_LINE) return sdf_cov(sdf_line(x, y, x0, y0, x1, y1, r0, r1), inv);
+    if (kind == TK_SDF_LINE_SHADOW)
+        return sdf_shadow_cov(sdf_line(x - ox, y - oy, x0, y0, x1, y1, r0, r1), inv, ex, in);
+    return 0.0f;
+}
+
 // ---------------------------------------------------------------------------
 // Scene state.
 // ---------------------------------------------------------------------------
@@ -539,6 +708,7 @@ struct or_scene {
     std::vector<tk_draw_record> draws;
     std::vector<tk_layer_record> layers;
     std::vector<uint32_t> brush, batch_ids;
+    std::vector<uint32_t> sdf, shadow;  // Canvas::sdf_blob, sdf_shadow_blob
     uint32_t tw = 0, th = 0, T = 0;
     uint64_t B = 0, seg_capacity = 0;
     std::vector<int32_t> backdrops;
@@ -605,6 +775,99 @@ bool noop_stack_clip(const or_scene& S, const tk_layer_record& L, const tk_draw_
     return r.start == r.end && (d.fill_rule == TK_FILL_EVEN_ODD ? (w & 1u) != 0u : w != 0u);
 }
 
+
+// --- coarse/sdf_clip.hlsli:8-56 and coarse/paint.hlsli:13-40 -------------------
+bool rounded_corner_covers(float px, float py, float cx, float cy, float ccx, float ccy, float radius, float inset) {
+    bool in_square = radius > 0.0f && std::fabs(px - cx) < radius && std::fabs(py - cy) < radius;
+    float inner = radius - inset;
+    float dx = px - ccx, dy = py - ccy;
+    return !in_square || (inner > 0.0f && dx * dx + dy * dy <= inner * inner);
+}
+bool rect_covers_tile(const float rect[4], const float radii_in[4], const tk_draw_record& d, uint32_t tx, uint32_t ty,
+                      float inset) {
+    float lx = fmin_(rect[0], rect[2]), ly = fmin_(rect[1], rect[3]);
+    float ux = fmax_(rect[0], rect[2]), uy = fmax_(rect[1], rect[3]);
+    float tlx = float(tx * TK_TILE_SIZE) + 0.5f - d.transform.e, tly = float(ty * TK_TILE_SIZE) + 0.5f - d.transform.f;
+    float tux = tlx + float(TK_TILE_SIZE - 1u), tuy = tly + float(TK_TILE_SIZE - 1u);
+    float sx = ux - lx, sy = uy - ly;
+    float need = float(TK_TILE_SIZE - 1u) + 2.0f * inset;
+    if (sx < need || sy < need || tlx < lx + inset || tly < ly + inset || tux > ux - inset || tuy > uy - inset)
+        return false;
+    float limit = fmin_(sx, sy) * 0.5f;
+    for (int k = 0; k < 4; ++k)
+        if (!(std::fabs(rect[k]) <= 65536.0f) || !(std::fabs(radii_in[k]) <= 65536.0f)) return false;
+    if (!(std::fabs(d.transform.e) <= 65536.0f) || !(std::fabs(d.transform.f) <= 65536.0f)) return false;
+    float q[4];
+    for (int k = 0; k < 4; ++k) q[k] = fmin_(fmax_(radii_in[k], 0.0f), limit);
+    return rounded_corner_covers(tlx, tly, lx, ly, lx + q[0], ly + q[0], q[0], inset) &&
+           rounded_corner_covers(tux, tly, ux, ly, ux - q[1], ly + q[1], q[1], inset) &&
+           rounded_corner_covers(tlx, tuy, lx, uy, lx + q[2], uy - q[2], q[2], inset) &&
+           rounded_corner_covers(tux, tuy, ux, uy, ux - q[3], uy - q[3], q[3], inset);
+}
+inline bool identity_linear(const tk_draw_record& d) {
+    return d.transform.a == 1.0f && d.transform.b == 0.0f && d.transform.c == 0.0f && d.transform.d == 1.0f;
+}
+inline bool has_sdf(const tk_draw_record& d) {
+    return d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX;
+}
+bool sdf_clip_covers(const or_scene& S, const tk_draw_record& d, uint32_t tx, uint32_t ty) {
+    if (d.sdf_offset == TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX || d.sdf_len < 9u) return false;
+    const uint32_t* w = S.sdf.data() + d.sdf_offset;
+    if (w[0] != TK_SDF_RECT || !identity_linear(d)) return false;
+    float rect[4], radii[4];
+    for (int k = 0; k < 4; ++k) { rect[k] = bits_f(w[1 + k]); radii[k] = bits_f(w[5 + k]); }
+    return rect_covers_tile(rect, radii, d, tx, ty, 0.5f);
+}
+bool sdf_stroke_empty(const or_scene& S, const tk_draw_record& d, uint32_t tx, uint32_t ty) {
+    if (d.sdf_offset == TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX || d.sdf_len < 13u ||
+        !identity_linear(d))
+        return false;
+    const uint32_t* w = S.sdf.data() + d.sdf_offset;
+    if (w[0] != TK_SDF_RECT_STROKE) return false;
+    float rect[4], radii[4], stroke[4];
+    for (int k = 0; k < 4; ++k) {
+        rect[k] = bits_f(w[1 + k]);
+        radii[k] = bits_f(w[5 + k]);
+        stroke[k] = bits_f(w[9 + k]);
+    }
+    for (int k = 0; k < 4; ++k)
+        if (!(std::fabs(rect[k]) <= 65536.0f) || !(std::fabs(radii[k]) <= 65536.0f) ||
+            !(std::fabs(stroke[k]) <= 65536.0f))
+            return false;
+    float hw[4];
+    for (int k = 0; k < 4; ++k) hw[k] = fmax_(stroke[k], 0.0f);  // top, right, bottom, left
+    float lx = fmin_(rect[0], rect[2]), ly = fmin_(rect[1], rect[3]);
+    float ux = fmax_(rect[0], rect[2]), uy = fmax_(rect[1], rect[3]);
+    float inner[4] = {lx + hw[3], ly + hw[0], ux - hw[1], uy - hw[2]};
+    if (inner[0] >= inner[2] || inner[1] >= inner[3]) return false;
+    float corner[4] = {fmax_(hw[0], hw[3]), fmax_(hw[0], hw[1]), fmax_(hw[2], hw[3]), fmax_(hw[2], hw[1])};
+    float r[4];
+    for (int k = 0; k < 4; ++k) r[k] = fmax_(radii[k] - corner[k], 0.0f);
+    return rect_covers_tile(inner, r, d, tx, ty, 1.0f);
+}
+bool nontransparent_solid(const or_scene& S, const tk_draw_record& d) {
+    Paint P{S.brush.data(), S.brush.size()};
+    return d.brush_offset != TK_INVALID_INDEX && P.word(0u, d.brush_offset) == TK_BRUSH_SOLID &&
+           P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
+}
+bool solid_supported_sdf(const or_scene& S, const tk_draw_record& d) {
+    if (!nontransparent_solid(S, d) || d.sdf_offset == TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX ||
+        d.sdf_len == 0u)
+        return false;
+    uint32_t kind = S.sdf[d.sdf_offset];
+    return kind == TK_SDF_RECT || kind == 5u /* candlestick */ || kind == 14u /* checkerboard */;
+}
+// sdf_coverage_from_draw (fine/draw.hlsli:21-26)
+float sdf_coverage_from_draw(const or_scene& S, const tk_draw_record& d, float x, float y) {
+    const tk_affine& m = d.inverse_transform;
+    float lx = mad(m.a, x, mad(m.c, y, m.e));
+    float ly = mad(m.b, x, mad(m.d, y, m.f));
+    if (d.sdf_offset != TK_INVALID_INDEX) return sdf_blob_coverage(S.sdf.data() + d.sdf_offset, lx, ly, m);
+    if (d.sdf_shadow_offset != TK_INVALID_INDEX)
+        return sdf_blob_coverage(S.shadow.data() + d.sdf_shadow_offset, lx, ly, m);
+    return 0.0f;
+}
+
 struct Particle {
     bool valid = false;
     uint32_t tag = TK_PTCL_FILL, winding = 0, fill_rule = 0, seg0 = 0, seg1 = 0, color = 0;
@@ -614,6 +877,24 @@ Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t 
     Particle r;
     if (di >= S.batch_ids.size() || S.batch_ids[di] != b.batch_id) return r;
     const tk_draw_record& d = S.draws[di];
+    if (has_sdf(d)) {  // coarse/emit_draw.hlsli:22-30
+        if (d.tag == TK_DRAW_BRUSH && !sdf_stroke_empty(S, d, tx, ty)) {
+            r.valid = true;
+            Paint P{S.brush.data(), S.brush.size()};
+            uint32_t color = nontransparent_solid(S, d) && sdf_clip_covers(S, d, tx, ty)
+                                 ? P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD)
+                                 : 0u;
+            if (color != 0u) {
+                r.tag = TK_PTCL_COLOR;
+                r.color = color;
+            } else {
+                r.tag = TK_PTCL_SDF;
+                r.seg0 = di;
+                r.color = di;
+            }
+        }
+        return r;
+    }
     uint32_t bd = draw_backdrop(S, d, tx, ty);
     if (bd == TK_INVALID_INDEX || (d.tag != TK_DRAW_BRUSH && d.tag != TK_DRAW_PATH_GLYPH && d.tag != TK_DRAW_CLIP))
         return r;
@@ -638,7 +919,7 @@ Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t 
     return r;
 }
 
-const uint32_t CHUNK_CLASS_COLOR = 1u, CHUNK_CLASS_OTHER = 4u, CHUNK_CLASS_OCCLUDER = 8u;
+const uint32_t CHUNK_CLASS_COLOR = 1u, CHUNK_CLASS_SDF = 2u, CHUNK_CLASS_OTHER = 4u, CHUNK_CLASS_OCCLUDER = 8u;
 
 // coarse/occlusion.hlsli:12-34 on one tile stream (records [0, end)).
 uint32_t occluded_prefix(const std::vector<tk_ptcl_record>& recs, uint32_t end, uint32_t wrappers) {
@@ -690,7 +971,10 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
     for (uint32_t k = 0; k < n; ++k) {
         Particle q = draw_particle(S, b, cand[k], tx, ty);
         if (!q.valid) continue;
-        flags |= q.tag == TK_PTCL_COLOR ? CHUNK_CLASS_COLOR : CHUNK_CLASS_OTHER;
+        // particle_class_flags (coarse/paint.hlsli:35-40)
+        if (q.tag == TK_PTCL_COLOR) flags |= CHUNK_CLASS_COLOR;
+        else if (q.tag == TK_PTCL_SDF && solid_supported_sdf(S, S.draws[cand[k]])) flags |= CHUNK_CLASS_SDF;
+        else flags |= CHUNK_CLASS_OTHER;
         if (wrappers == 0u && q.tag == TK_PTCL_COLOR && (q.color >> 24) == 255u && p > 0u) flags |= CHUNK_CLASS_OCCLUDER;
         if (p < count) out.recs[p++] = {q.tag, int32_t(q.winding), q.fill_rule, q.seg0, q.seg1, q.color};
     }
@@ -707,6 +991,7 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
     uint32_t skip = (flags & CHUNK_CLASS_OCCLUDER) ? occluded_prefix(out.recs, p + wrappers + 1u, wrappers) : 0u;
     uint32_t kind;  // coarse/tile_classification.hlsli:6-10
     if (flags & CHUNK_CLASS_OTHER) kind = TK_TILE_KIND_INTERPRETER;
+    else if (flags & CHUNK_CLASS_SDF) kind = (flags & CHUNK_CLASS_COLOR) ? TK_TILE_KIND_MIXED : TK_TILE_KIND_SDF;
     else kind = (flags & CHUNK_CLASS_COLOR) ? TK_TILE_KIND_COLOR : TK_TILE_KIND_EMPTY;
     out.kind = kind | (skip << TK_TILE_PREFIX_SHIFT);
     return true;
@@ -743,6 +1028,17 @@ F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_
                 }
                 // blend groups are outside this path (rejected at load)
             }
+        } else if (tag == TK_PTCL_SDF) {  // fine/interpreter.hlsli:70-84
+            if (clip_mask != 0u) {
+                const tk_draw_record& d = S.draws[r.color];
+                float x = float(gx) + 0.5f, y = float(gy) + 0.5f;
+                uint32_t alpha = combine_alpha(coverage_to_u8(sdf_coverage_from_draw(S, d, x, y)), clip_mask);
+                if (alpha != 0u) {
+                    uint32_t color = sample_draw_brush(P, d, x, y);
+                    if (alpha == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+                    else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(color, alpha));
+                }
+            }
         } else if (tag == TK_PTCL_FILL || tag == TK_PTCL_PATH_GLYPH || tag == TK_PTCL_BEGIN_CLIP ||
                    tag == TK_PTCL_BEGIN_OPACITY || tag == TK_PTCL_BEGIN_BLEND) {
             uint32_t alpha = coverage_to_alpha(
@@ -775,6 +1071,33 @@ F4 color_only(const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t 
         if (r.tag == TK_PTCL_END) break;
         if (premul_u8_is_opaque(r.color)) pixel = rgba8_to_unorm(r.color);
         else pixel = src_over_premul_unorm(pixel, rgba8_to_unorm(r.color));
+    }
+    return pixel;
+}
+
+// fine/specialized.hlsli:47-108 (SDF and MIXED tiles: colours and solid SDFs,
+// no stacks; full-tile images are not produced on this path)
+F4 analytic_solid(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel,
+                  uint32_t gx, uint32_t gy) {
+    Paint P{S.brush.data(), S.brush.size()};
+    float x = float(gx) + 0.5f, y = float(gy) + 0.5f;
+    for (uint32_t ix = begin; ix < end; ++ix) {
+        const tk_ptcl_record& r = recs[ix];
+        if (r.tag == TK_PTCL_END) break;
+        if (r.tag == TK_PTCL_COLOR) {
+            if (premul_u8_is_opaque(r.color)) pixel = rgba8_to_unorm(r.color);
+            else pixel = src_over_premul_unorm(pixel, rgba8_to_unorm(r.color));
+        } else {
+            const tk_draw_record& d = S.draws[r.color];
+            bool inside = int32_t(gx) >= d.pixel_bounds.x0 && int32_t(gy) >= d.pixel_bounds.y0 &&
+                          int32_t(gx) < d.pixel_bounds.x1 && int32_t(gy) < d.pixel_bounds.y1;
+            uint32_t alpha = coverage_to_u8(inside ? sdf_coverage_from_draw(S, d, x, y) : 0.0f);
+            if (alpha != 0u) {
+                uint32_t color = P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD);
+                if (alpha == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+                else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(color, alpha));
+            }
+        }
     }
     return pixel;
 }
@@ -935,6 +1258,8 @@ void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int th
                     uint32_t end = uint32_t(bs.recs.size());
                     if (kind == TK_TILE_KIND_INTERPRETER) pixel = interpret(S, bs.recs, begin, end, pixel, lx, ly, gx, gy);
                     else if (kind == TK_TILE_KIND_COLOR) pixel = color_only(bs.recs, begin, end, pixel);
+                    else if (kind == TK_TILE_KIND_SDF || kind == TK_TILE_KIND_MIXED)
+                        pixel = analytic_solid(S, bs.recs, begin, end, pixel, gx, gy);
                     texel = texel_store(pixel);
                 }
             }
@@ -1132,6 +1457,8 @@ int32_t or_run(const tk_scene_desc* d, int32_t threads, uint32_t tile_y0, uint32
         S->draws.assign(d->draws, d->draws + d->draw_count);
         S->layers.assign(d->layers, d->layers + d->layer_count);
         S->brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
+        S->sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
+        S->shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
         S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
         S->ty0 = tile_y0;
         S->ty1 = tile_y1;
@@ -1322,5 +1649,10 @@ void or_blur_pass(const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t h
 float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t backdrop, uint32_t x, uint32_t y) {
     return fill_value(segments, 0, count, backdrop, x, y);
 }
+
+float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine* inv) {
+    return sdf_blob_coverage(record, x, y, *inv);
+}
+float or_exp_nonpos(float x) { return exp_nonpos(x); }
 
 }  // extern "C"

@@ -100,6 +100,13 @@ void or_blur_pass(const uint32_t* src, uint32_t* dst, uint32_t width, uint32_t h
 float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t backdrop,
                     uint32_t x, uint32_t y);
 
+/* Coverage of one SDF record (TK_SDF_RECORD_WORDS words) at local point
+ * (x, y) under the draw inverse transform `inv` (sdf_coverage_from_blob,
+ * shared/sdf/coverage.hlsli:13-236), and the library's exp(x) for x <= 0
+ * used by shadow falloffs. */
+float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine* inv);
+float or_exp_nonpos(float x);
+
 /* FP64 loss of the differentiable model (include/tileink_diff.h) for the
  * flattening `lines` / endpoint weights of a forward and the parameters
  * `points` ([point][x, y]), `colors` ([path][rgba] straight), `sigma` with the

@@ -36,6 +36,9 @@ def unoffset(records, info):
     r["segment_end"][fill_like] -= np.uint32(info.segment_base)
     fill = r["tag"] == N.PTCL_FILL
     r["color"][fill] -= np.uint32(info.draw_base)
+    sdf = r["tag"] == N.PTCL_SDF  # SDF records name their draw in segment_start and color
+    r["segment_start"][sdf] -= np.uint32(info.draw_base)
+    r["color"][sdf] -= np.uint32(info.draw_base)
     bb = r["tag"] == N.PTCL_BATCH_BEGIN
     r["segment_start"][bb] -= np.uint32(info.batch_base)
     return r

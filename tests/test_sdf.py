@@ -1,0 +1,226 @@
+"""Analytic SDF shapes on the host: their physical records and pixel bounds
+(Sdf::bounds / SdfShadow::bounds, src/shared/sdf/{rect,circle,line,shadow}.rs;
+encode_sdf, src/shared/gpu_sdf.rs:48-260), the oracle's coverage
+(shared/sdf/coverage.hlsli) against closed-form distances, and the coarse
+particles SDF draws give (coarse/emit_draw.hlsli:22-30,
+coarse/sdf_clip.hlsli:8-56, coarse/tile_classification.hlsli). The device
+path is compared with the oracle in test_gpu_sdf.py."""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import tileink_b200 as tk
+from tileink_b200 import _native as N
+
+SOLID = tk.Brush.solid(0.2, 0.5, 0.9, 1.0)
+
+
+def record(canvas, draw):
+    a = canvas.scene_arrays()
+    d = a["draws"][draw]
+    if d["sdf_offset"] != 0xFFFFFFFF:
+        w = a["sdf"][d["sdf_offset"]:d["sdf_offset"] + d["sdf_len"]]
+    else:
+        w = a["sdf_shadow"][d["sdf_shadow_offset"]:d["sdf_shadow_offset"] + d["sdf_shadow_len"]]
+    return int(w[0]), w[1:].view(np.float32), tuple(int(v) for v in d["pixel_bounds"])
+
+
+def test_sdf_records_and_bounds():
+    c = tk.Canvas(320, 240)
+    # src/shared/sdf.rs:126-142: Rect (12, 24)-(28, 40), radius 3 -> bounds (12, 24, 28, 40)
+    kind, f, pb = record(c, c.push_rect(12, 24, 28, 40, SOLID, radius=3))
+    assert kind == N.SDF_RECT and pb == (12, 24, 28, 40)
+    assert list(f[:8]) == [12, 24, 28, 40, 3, 3, 3, 3] and not f[8:].any()
+    # corners are stored sorted; radii in top-left, top-right, bottom-left, bottom-right order
+    kind, f, pb = record(c, c.push_rect(28.5, 40.25, 12.75, 24, SOLID, radius=(1, 2, 3, 4)))
+    assert list(f[:8]) == [12.75, 24, 28.5, 40.25, 1, 2, 3, 4] and pb == (12, 24, 29, 41)
+    # src/shared/gpu_sdf/tests.rs:86-101: side widths top 2, right 4, bottom 6, left 8 are
+    # stored as half widths; the bounds are the outer rectangle
+    kind, f, pb = record(c, c.push_rect_stroke(4, 5, 40, 41, (2, 4, 6, 8), SOLID, radius=(1, 2, 4, 3)))
+    assert kind == N.SDF_RECT_STROKE
+    assert list(f[:12]) == [4, 5, 40, 41, 1, 2, 4, 3, 1, 2, 3, 4]
+    assert pb == (4 - 4, 5 - 1, 40 + 2, 41 + 3)
+    # circles: bounds in f32 (src/shared/sdf/circle.rs:13-20)
+    kind, f, pb = record(c, c.push_circle(100.5, 120.25, 30, SOLID))
+    assert kind == N.SDF_CIRCLE and list(f[:4]) == [100.5, 120.25, 30, 0] and pb == (70, 90, 131, 151)
+    kind, f, pb = record(c, c.push_circle_stroke(100, 100, 20, 5, SOLID))
+    assert kind == N.SDF_CIRCLE_STROKE and list(f[8:12]) == [2.5] * 4 and pb == (77, 77, 123, 123)
+    # lines: width and cap in the radius words; square caps extend the bounds along the axis
+    kind, f, pb = record(c, c.push_line(10, 150, 300, 150, 3, SOLID, cap=N.CAP_SQUARE))
+    assert kind == N.SDF_LINE and list(f[:6]) == [10, 150, 300, 150, 3, N.CAP_SQUARE]
+    assert pb == (7, 148, 303, 152)
+    kind, f, pb = record(c, c.push_line(10, 150, 300, 180, 3, SOLID, cap=N.CAP_ROUND))
+    assert pb == (8, 148, 302, 182)
+    # shadows: the shape's bounds outset by 4 expand + 1 and moved by the offset (shadow.rs:35-43)
+    kind, f, pb = record(c, c.push_rect_shadow(50, 50, 150, 120, SOLID, offset=(3, 4), expand=6, intensity=0.7,
+                                                 radius=10))
+    assert kind == N.SDF_RECT_SHADOW and list(f[12:16]) == [3, 4, 6, np.float32(0.7)]
+    assert pb == (50 + 3 - 25, 50 + 4 - 25, 150 + 3 + 25, 120 + 4 + 25)
+    kind, f, pb = record(c, c.push_circle_shadow(60, 60, 10, SOLID, expand=-2, intensity=3))
+    assert kind == N.SDF_CIRCLE_SHADOW and list(f[12:16]) == [0, 0, 0, 1]  # normalized options
+    assert pb == (49, 49, 71, 71)
+    # shapes that draw nothing: the reference's None
+    assert c.push_rect_stroke(0, 0, 10, 10, 0, SOLID) is None
+    assert c.push_circle_stroke(0, 0, 10, -1, SOLID) is None
+    assert c.push_line(5, 5, 5, 5, 2, SOLID) is None  # butt-capped point
+    assert c.push_line(5, 5, 9, 5, 0, SOLID) is None
+    assert c.push_rect_shadow(0, 0, 10, 10, SOLID, intensity=0) is None
+    assert c.push_line(5, 5, 5, 5, 2, SOLID, cap=N.CAP_ROUND) is not None  # a round dot
+    with pytest.raises(ValueError):
+        c.push_rect(0, 0, 1, 1, SOLID, radius=(1, 2))
+
+
+def test_sdf_physical_scale():
+    c = tk.Canvas(100, 80, scale=2.0)
+    kind, f, pb = record(c, c.push_rect_stroke(10, 10, 30, 20, 3, SOLID, radius=2))
+    assert list(f[:12]) == [20, 20, 60, 40, 4, 4, 4, 4, 3, 3, 3, 3] and pb == (17, 17, 63, 43)
+    kind, f, pb = record(c, c.push_circle_shadow(20, 20, 5, SOLID, offset=(1, -1), expand=2, intensity=0.5))
+    assert list(f[:3]) == [40, 40, 10] and list(f[12:16]) == [2, -2, 4, 0.5]
+    kind, f, pb = record(c, c.push_line(0, 0, 10, 0, 1.5, SOLID))
+    assert list(f[:5]) == [0, 0, 20, 0, 3]
+
+
+def test_oracle_exp_is_correctly_rounded():
+    lib = oracle.lib()
+    xs = np.concatenate([-np.logspace(-8, 2, 4001), [0.0, -1e-30, -87.0, -103.0]]).astype(np.float32)
+    got = np.array([lib.or_exp_nonpos(float(x)) for x in xs], np.float64)
+    ref = np.exp(xs.astype(np.float64))
+    ulp = np.spacing(ref.astype(np.float32)).astype(np.float64)
+    normal = ref > np.finfo(np.float32).tiny
+    assert (np.abs(got - ref)[normal] <= 0.5 * ulp[normal] * (1 + 1e-6)).all()
+    assert lib.or_exp_nonpos(-200.0) == 0.0 and lib.or_exp_nonpos(0.0) == 1.0
+
+
+def sdf_words(kind, coords=(0, 0, 0, 0), radii=(0, 0, 0, 0), stroke=(0, 0, 0, 0), shadow=(0, 0, 0, 0)):
+    w = np.zeros(N.SDF_RECORD_WORDS, np.uint32)
+    w[0] = kind
+    pad = lambda v: list(v) + [0] * (4 - len(v))
+    w[1:].view(np.float32)[:] = np.float32(pad(coords) + pad(radii) + pad(stroke) + pad(shadow))
+    return w
+
+
+def coverage(words, x, y, inv=(1, 0, 0, 1, 0, 0)):
+    m = (C.c_float * 6)(*inv)
+    return oracle.lib().or_sdf_coverage(words.ctypes.data, float(x), float(y), C.cast(m, C.c_void_p))
+
+
+# The oracle evaluates in f32: a few ulps of coordinates near 50-100.
+TOL = 2e-5
+
+
+def test_oracle_sdf_coverage_against_closed_forms():
+    rect = sdf_words(N.SDF_RECT, (10, 10, 20, 30))
+    for x, y, d in [(15, 20, -5), (10, 20, 0), (9.75, 20, 0.25), (10.25, 20, -0.25), (21, 20, 1), (15, 30.4, 0.4)]:
+        assert coverage(rect, x, y) == pytest.approx(min(max(0.5 - d, 0), 1), abs=TOL)
+    # rounded corner: distance to the corner circle
+    rr = sdf_words(N.SDF_RECT, (0, 0, 40, 40), (8, 8, 8, 8))
+    d = math.hypot(2 - 8, 2 - 8) - 8
+    assert coverage(rr, 2, 2) == pytest.approx(min(max(0.5 - d, 0), 1), abs=TOL)
+    circle = sdf_words(N.SDF_CIRCLE, (50, 60, 10))
+    for x, y in [(50, 60), (60.2, 60), (57, 67.3), (49.5, 49.8)]:
+        d = math.hypot(x - 50, y - 60) - 10
+        assert coverage(circle, x, y) == pytest.approx(min(max(0.5 - d, 0), 1), abs=TOL)
+    # a circle stroke covers the ring: outer minus inner coverage
+    ring = sdf_words(N.SDF_CIRCLE_STROKE, (0, 0, 20), stroke=(3, 3, 3, 3))
+    assert coverage(ring, 20, 0) == 1.0 and coverage(ring, 0, 0) == 0.0
+    assert coverage(ring, 23.2, 0) == pytest.approx(0.3, abs=TOL)
+    # a rect stroke's hole is empty, its band full
+    band = sdf_words(N.SDF_RECT_STROKE, (0, 0, 100, 60), stroke=(2, 2, 2, 2))
+    assert coverage(band, 50, 30) == 0.0 and coverage(band, 50, 0) == 1.0
+    # lines: butt ends stop at the end points, square ends reach half the width further
+    for cap, reach in [(N.CAP_BUTT, 0.0), (N.CAP_SQUARE, 2.0)]:
+        line = sdf_words(N.SDF_LINE, (10, 10, 50, 10), (4, cap))
+        assert coverage(line, 30, 10) == 1.0 and coverage(line, 30, 12.25) == pytest.approx(0.25, abs=TOL)
+        assert coverage(line, 50 + reach + 0.3, 10) == pytest.approx(0.2, abs=TOL)
+    line = sdf_words(N.SDF_LINE, (10, 10, 50, 10), (4, N.CAP_ROUND))
+    d = math.hypot(1.5, 1.5) - 2  # past the end: distance to the end point
+    assert coverage(line, 51.5, 11.5) == pytest.approx(min(max(0.5 - d, 0), 1), abs=TOL)
+    # shadows: exp(-max(d, 0) / expand) * intensity outside, intensity inside
+    sh = sdf_words(N.SDF_RECT_SHADOW, (0, 0, 20, 20), shadow=(2, 3, 4, 0.5))
+    assert coverage(sh, 12, 13) == pytest.approx(0.5)
+    assert coverage(sh, 22 + 6, 13) == pytest.approx(0.5 * math.exp(-6 / 4), rel=1e-6)
+    # an anisotropic inverse transform scales the distance by the normal's footprint
+    inv = (0.5, 0, 0, 2, 0, 0)
+    assert coverage(rect, 20.25, 20, inv) == pytest.approx(0.5 - 0.25 / 0.5, abs=TOL)
+
+
+def ptcl_of(canvas):
+    run = oracle.OracleRun(canvas.scene_desc(), threads=4)
+    return (run.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0), run.get(oracle.OR_PASS_TILES, N.TILE_DTYPE, 0),
+            run.get(oracle.OR_PASS_KINDS, np.uint32, 0))
+
+
+def tile_stream(ptcl, tiles, t):
+    r = tiles[t]
+    return ptcl[r["ptcl_start"]:r["ptcl_end"]]
+
+
+def test_oracle_sdf_particles_and_tile_kinds():
+    W, H = 384, 128
+    tw = W // 16
+    c = tk.Canvas(W, H)
+    c.push_rect(20, 20, 200, 108, tk.Brush.solid(0.9, 0.1, 0.1, 1.0))            # draw 0: solid rect
+    c.push_rect_stroke(208, 8, 376, 120, 4, tk.Brush.solid(0.1, 0.8, 0.1, 1.0))  # draw 1: hollow stroke
+    c.push_circle(64, 64, 20, tk.Brush.solid(0.1, 0.1, 0.9, 0.5))               # draw 2: circle
+    ptcl, tiles, kinds = ptcl_of(c)
+
+    def draws_in(tx, ty):
+        s = tile_stream(ptcl, tiles, ty * tw + tx)
+        return [(int(p["tag"]), int(p["color"])) for p in s if p["tag"] not in (N.PTCL_BATCH_BEGIN, N.PTCL_END)]
+
+    def kind_of(tx, ty):
+        return int(tile_stream(ptcl, tiles, ty * tw + tx)[0]["color"]) & 7
+
+    a = c.scene_arrays()
+    color = int(a["brush"][a["draws"][0]["brush_offset"] + 4])
+    # every pixel centre of the tile at least half a pixel inside the solid rect:
+    # one colour particle (full_tile_solid), a COLOR tile
+    assert draws_in(8, 3) == [(N.PTCL_COLOR, color)] and kind_of(8, 3) == N.TILE_KIND_COLOR
+    # on the rect's edge it is an SDF particle of draw 0; solid rects are
+    # solid-supported SDFs, so the tile is an SDF tile
+    assert draws_in(1, 1) == [(N.PTCL_SDF, 0)] and kind_of(1, 1) == N.TILE_KIND_SDF
+    assert draws_in(8, 6) == [(N.PTCL_SDF, 0)]
+    # the circle's tiles: the rect as a colour, the circle (not solid-supported) interpreted
+    assert draws_in(3, 3) == [(N.PTCL_COLOR, color), (N.PTCL_SDF, 2)]
+    assert kind_of(3, 3) == N.TILE_KIND_INTERPRETER
+    # tiles at least a pixel inside the stroke's hole have no particle (sdf_stroke_empty)
+    for tx in range(14, 23):
+        for ty in range(1, 7):
+            assert draws_in(tx, ty) == [], (tx, ty)
+    assert draws_in(13, 3) == [(N.PTCL_SDF, 1)] and draws_in(23, 3) == [(N.PTCL_SDF, 1)]
+    # MIXED: a colour particle and a solid-supported SDF particle in one tile
+    m = tk.Canvas(64, 64)
+    m.push_rect(0, 0, 64, 64, tk.Brush.solid(1, 1, 1, 1))
+    m.push_rect(5.5, 5.5, 40, 40, tk.Brush.solid(0, 0, 0, 1))
+    p2, t2, k2 = ptcl_of(m)
+    assert int(tile_stream(p2, t2, 0)[0]["color"]) & 7 == N.TILE_KIND_MIXED
+
+
+def test_sdf_nodes_replay_under_translations_only():
+    node = tk.Canvas(200, 100)
+    node.keep_commands()
+    node.push_rect(10, 10, 50, 40, SOLID, radius=4)
+    node.push_line(0, 0, 30, 20, 2, SOLID, cap=N.CAP_ROUND)
+    moved = tk.Canvas(200, 100)
+    moved.replay(node, (1, 0, 0, 1, 7.5, -3))
+    direct = tk.Canvas(200, 100)
+    direct.push_rect(17.5, 7, 57.5, 37, SOLID, radius=4)
+    direct.push_line(7.5, -3, 37.5, 17, 2, SOLID, cap=N.CAP_ROUND)
+    a, b = moved.scene_arrays(), direct.scene_arrays()
+    for k in ("draws", "sdf", "brush", "draw_order"):
+        assert a[k].tobytes() == b[k].tobytes(), k
+    with pytest.raises(ValueError):
+        tk.Canvas(200, 100).replay(node, (0.9, 0.1, -0.1, 0.9, 0, 0))
+    # a retained scene reports the shapes' pixel bounds as damage when a node moves
+    rs = tk.RetainedScene(200, 100)
+    rs.insert(1, node)
+    rs.materialize()
+    rs.set_transform(1, (1, 0, 0, 1, 20, 0))
+    canvas, damage = rs.materialize()
+    rects = {tuple(r) for r in damage["rects"].tolist()}
+    assert (10, 10, 50, 40) in rects and (30, 10, 70, 40) in rects

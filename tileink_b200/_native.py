@@ -28,6 +28,13 @@ STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4,
 # PTCL tags (shaders/hlsl/shared/particle_tags.hlsli) + merged-stream marker
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
 PTCL_BATCH_BEGIN = 14
+PTCL_SDF = 9
+TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIND_MIXED = 0, 1, 2, 3, 4
+# SDF kinds (src/shared/gpu_types.rs) and line caps
+SDF_RECT, SDF_CIRCLE, SDF_RECT_STROKE, SDF_CIRCLE_STROKE, SDF_LINE = 1, 2, 3, 4, 6
+SDF_RECT_SHADOW, SDF_CIRCLE_SHADOW, SDF_LINE_SHADOW = 7, 10, 11
+SDF_RECORD_WORDS = 17
+CAP_BUTT, CAP_SQUARE, CAP_ROUND = 0, 1, 2
 
 OP_DRAW_BATCH, OP_BLUR_BEGIN, OP_BLUR_END = 0, 1, 2
 SCENE_SEGMENTS_FROM_DEVICE = 1
@@ -78,6 +85,8 @@ class SceneDesc(C.Structure):
         ("draw_order_count", C.c_uint32), ("draw_order", C.c_void_p),
         ("draw_batch_ids", C.c_void_p),
         ("ops", C.c_void_p), ("op_count", C.c_uint32), ("reserved", C.c_uint32),
+        ("sdf_blob", C.c_void_p), ("sdf_word_count", C.c_uint64),
+        ("sdf_shadow_blob", C.c_void_p), ("sdf_shadow_word_count", C.c_uint64),
     ]
 
 
@@ -95,6 +104,12 @@ class BrushDesc(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("extend", C.c_uint32), ("rgba", C.c_float * 4), ("p0", C.c_float * 2),
                 ("p1", C.c_float * 2), ("r0", C.c_float), ("r1", C.c_float), ("stop_count", C.c_uint32),
                 ("stops", C.POINTER(GradientStop))]
+
+
+class SdfShape(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("cap", C.c_uint32), ("p0", C.c_double * 2), ("p1", C.c_double * 2),
+                ("radius", C.c_double), ("width", C.c_double), ("radii", C.c_float * 4), ("widths", C.c_float * 4),
+                ("shadow", C.c_float * 4)]
 
 
 class FlattenDesc(C.Structure):
@@ -202,6 +217,7 @@ def library() -> C.CDLL:
         "tk_canvas_set_clear_color": (None, [P, U32]),
         "tk_canvas_push_path": (I64, [P, P, C.POINTER(BrushDesc), P, U32, F64]),
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
+        "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),
@@ -255,6 +271,8 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "draw_order": arr(d.draw_order, d.draw_order_count, np.uint32),
         "draw_batch_ids": arr(d.draw_batch_ids, d.draw_count, np.uint32),
         "ops": arr(d.ops, d.op_count, OP_DTYPE),
+        "sdf": arr(d.sdf_blob, d.sdf_word_count, np.uint32),
+        "sdf_shadow": arr(d.sdf_shadow_blob, d.sdf_shadow_word_count, np.uint32),
     }
 
 
@@ -274,6 +292,11 @@ class ArrayScene:
         d.draw_order, d.draw_order_count = ptr(a["draw_order"]), len(a["draw_order"])
         d.draw_batch_ids = ptr(a["draw_batch_ids"])
         d.ops, d.op_count = ptr(a["ops"]), len(a["ops"])
+        sdf, shadow = a.get("sdf"), a.get("sdf_shadow")
+        if sdf is not None and len(sdf):
+            d.sdf_blob, d.sdf_word_count = ptr(sdf), len(sdf)
+        if shadow is not None and len(shadow):
+            d.sdf_shadow_blob, d.sdf_shadow_word_count = ptr(shadow), len(shadow)
         self.desc = d
         self.flatten = None
         els, strokes = a.get("elements"), a.get("strokes")

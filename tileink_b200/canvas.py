@@ -2,6 +2,9 @@
 
     Canvas.push_path        src/canvas/primitives/paths.rs:50-60
     Canvas.push_stroke      src/canvas/primitives/paths.rs:24-48
+    Canvas.push_rect / push_rect_stroke / push_circle / push_circle_stroke /
+    push_line and push_{rect,circle,line}_shadow
+                            src/canvas/primitives/{rectangles,shapes,shadows}.rs
     Canvas.push_clip_layer  src/canvas/layers.rs:7-28
     Canvas.push_blur_group  src/canvas/layers.rs:205-212
     Canvas.pop_layer        src/canvas/layers.rs
@@ -104,6 +107,16 @@ class Brush:
         return d, stops
 
 
+def _four(v):
+    """One value for all four corners / sides, or four values."""
+    if np.ndim(v) == 0:
+        return [float(v)] * 4
+    v = [float(x) for x in v]
+    if len(v) != 4:
+        raise ValueError("expected one value or four")
+    return v
+
+
 def _affine(transform):
     if transform is None:
         return None, None
@@ -193,6 +206,64 @@ class Canvas:
         if r < 0:
             raise ValueError("push_stroke rejected its arguments")
         return r
+
+    # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
+    def _push_sdf(self, brush: Brush, kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0,
+                  widths=0.0, shadow=None, cap=N.CAP_BUTT):
+        s = N.SdfShape()
+        s.kind, s.cap = kind, int(cap)
+        s.p0[:] = [float(v) for v in p0]
+        s.p1[:] = [float(v) for v in p1]
+        s.radius, s.width = float(radius), float(width)
+        s.radii[:] = _four(radii)
+        s.widths[:] = _four(widths)
+        if shadow is not None:
+            s.shadow[:] = [float(v) for v in shadow]
+        d, keep = brush._desc()
+        r = self._lib.tk_canvas_push_sdf(self._h, C.byref(s), C.byref(d))
+        if r == -2:
+            return None  # the shape draws nothing
+        if r < 0:
+            raise ValueError("SDF shape rejected its arguments")
+        return r
+
+    def push_rect(self, x0, y0, x1, y1, brush: Brush, radius=0.0):
+        """Canvas::push_rect: a filled rectangle, corner radii one value or
+        (top-left, top-right, bottom-left, bottom-right)."""
+        return self._push_sdf(brush, N.SDF_RECT, (x0, y0), (x1, y1), radii=radius)
+
+    def push_rect_stroke(self, x0, y0, x1, y1, widths, brush: Brush, radius=0.0):
+        """Canvas::push_rect_stroke(_widths): a centred stroke, full widths one
+        value or (top, right, bottom, left). None when every width is <= 0."""
+        return self._push_sdf(brush, N.SDF_RECT_STROKE, (x0, y0), (x1, y1), radii=radius, widths=widths)
+
+    def push_circle(self, cx, cy, r, brush: Brush):
+        return self._push_sdf(brush, N.SDF_CIRCLE, (cx, cy), radius=r)
+
+    def push_circle_stroke(self, cx, cy, r, width, brush: Brush):
+        """None when width <= 0."""
+        return self._push_sdf(brush, N.SDF_CIRCLE_STROKE, (cx, cy), radius=r, width=width)
+
+    def push_line(self, x0, y0, x1, y1, width, brush: Brush, cap=N.CAP_BUTT):
+        """Canvas::push_line (SdfLine): None for an empty line (width <= 0, or a
+        butt-capped point)."""
+        return self._push_sdf(brush, N.SDF_LINE, (x0, y0), (x1, y1), width=width, cap=cap)
+
+    def push_rect_shadow(self, x0, y0, x1, y1, brush: Brush, offset=(0.0, 0.0), expand=0.0, intensity=1.0,
+                         radius=0.0):
+        """Canvas::push_rect_shadow: exponential falloff over `expand` pixels
+        (a plain antialiased edge when 0). None when intensity <= 0."""
+        return self._push_sdf(brush, N.SDF_RECT_SHADOW, (x0, y0), (x1, y1), radii=radius,
+                              shadow=(offset[0], offset[1], expand, intensity))
+
+    def push_circle_shadow(self, cx, cy, r, brush: Brush, offset=(0.0, 0.0), expand=0.0, intensity=1.0):
+        return self._push_sdf(brush, N.SDF_CIRCLE_SHADOW, (cx, cy), radius=r,
+                              shadow=(offset[0], offset[1], expand, intensity))
+
+    def push_line_shadow(self, x0, y0, x1, y1, width, brush: Brush, offset=(0.0, 0.0), expand=0.0,
+                         intensity=1.0, cap=N.CAP_BUTT):
+        return self._push_sdf(brush, N.SDF_LINE_SHADOW, (x0, y0), (x1, y1), width=width, cap=cap,
+                              shadow=(offset[0], offset[1], expand, intensity))
 
     def push_clip_layer(self, path: BezPath, transform=None, fill_rule=FILL_NONZERO, tolerance: float = 0.1):
         t, tk = _affine(transform)

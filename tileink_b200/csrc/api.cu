@@ -121,6 +121,7 @@ struct tk_ctx {
     bool have_scene = false;
     uint32_t width = 0, height = 0, tw = 0, th = 0, clear = 0, flags = 0;
     uint64_t line_count = 0, brush_words = 0, pool_len = 0, host_segment_capacity = 0;
+    uint64_t sdf_words = 0, sdf_shadow_base = 0;  // SDF buffer: sdf_blob, then sdf_shadow_blob
     uint32_t path_count = 0, draw_count = 0, layer_count = 0, order_count = 0;
     std::vector<tk_path_record> h_paths;
     std::vector<tk::ScanItem> h_items;
@@ -131,7 +132,7 @@ struct tk_ctx {
     DBuf<tk_line> lines;
     DBuf<tk_path_record> paths;
     DBuf<tk_draw_record> draws;
-    DBuf<uint32_t> brush, batch_ids, order;
+    DBuf<uint32_t> brush, sdf, batch_ids, order;
     DBuf<tk_layer_record> layers;
     DBuf<tk::ScanItem> items;
     DBuf<unsigned long long> item_desc, tile_desc, stats;
@@ -217,6 +218,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     if (uint64_t(tw) * th > 0x7FFFFFFFull || tw > 65535u || th > 65535u) invalid("canvas too large");
     if ((d.line_count && !d.lines) || (d.path_count && !d.paths) || (d.draw_count && !d.draws) ||
         (d.brush_word_count && !d.brush_blob) || (d.layer_count && !d.layers) ||
+        (d.sdf_word_count && !d.sdf_blob) || (d.sdf_shadow_word_count && !d.sdf_shadow_blob) ||
         (d.draw_order_count && !d.draw_order) || (d.draw_count && !d.draw_batch_ids) || (d.op_count && !d.ops))
         invalid("null array with nonzero count");
     bool device_plan = (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
@@ -248,12 +250,29 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     }
     if (next_line != d.line_count) invalid("path line ranges do not cover the line array");
     if (seg_cap > 0xFFFFFFFFull) invalid("segment capacity exceeds u32 indexing");
-    // Draws: only path fills/clips are on this path.
+    if (d.sdf_word_count + d.sdf_shadow_word_count > 0xFFFFFFFFull) invalid("SDF blobs exceed u32 indexing");
+    // Draws: path fills/clips, and brush draws of the SDF kinds this library
+    // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
     for (uint32_t i = 0; i < d.draw_count; ++i) {
         const tk_draw_record& r = d.draws[i];
-        if (r.glyph_run_id != TK_INVALID_INDEX || r.sdf_offset != TK_INVALID_INDEX ||
-            r.sdf_shadow_offset != TK_INVALID_INDEX)
-            invalid("draw " + std::to_string(i) + ": text/SDF draws are outside this path");
+        const std::string at = "draw " + std::to_string(i);
+        if (r.glyph_run_id != TK_INVALID_INDEX) invalid(at + ": text draws are outside this path");
+        const bool plain = r.sdf_offset != TK_INVALID_INDEX, shadow = r.sdf_shadow_offset != TK_INVALID_INDEX;
+        if (plain || shadow) {
+            if (plain && shadow) invalid(at + ": both an SDF and a shadow record");
+            if (r.tag != TK_DRAW_BRUSH) invalid(at + ": SDF clips and groups are outside this path");
+            if (r.path_id != TK_INVALID_INDEX) invalid(at + ": an SDF draw with a path");
+            const uint64_t off = plain ? r.sdf_offset : r.sdf_shadow_offset;
+            const uint64_t len = plain ? r.sdf_len : r.sdf_shadow_len;
+            const uint64_t words = plain ? d.sdf_word_count : d.sdf_shadow_word_count;
+            if (len != TK_SDF_RECORD_WORDS || off + len > words) invalid(at + ": SDF record outside its blob");
+            const uint32_t kind = (plain ? d.sdf_blob : d.sdf_shadow_blob)[off];
+            const bool ok = plain ? (kind == TK_SDF_RECT || kind == TK_SDF_CIRCLE || kind == TK_SDF_RECT_STROKE ||
+                                     kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_LINE)
+                                  : (kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW ||
+                                     kind == TK_SDF_LINE_SHADOW);
+            if (!ok) invalid(at + ": SDF kind " + std::to_string(kind) + " is not supported");
+        }
         if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
             r.tag != TK_DRAW_ISOLATE)
             invalid("draw " + std::to_string(i) + ": unsupported tag");
@@ -264,6 +283,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         if (d.layers[i].tag == TK_LAYER_BLEND) invalid("blend layers are outside this path");
         if (d.layers[i].tag > TK_LAYER_BLEND) invalid("bad layer tag");
         if (d.layers[i].draw >= d.draw_count) invalid("layer draw out of range");
+        if (d.draws[d.layers[i].draw].path_id == TK_INVALID_INDEX) invalid("layer draws must be path draws");
     }
     // Painter order grouped by batch in op order.
     std::vector<uint32_t> batch_draws;
@@ -332,6 +352,8 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     c->layer_count = d.layer_count;
     c->order_count = d.draw_order_count;
     c->brush_words = d.brush_word_count;
+    c->sdf_words = d.sdf_word_count + d.sdf_shadow_word_count;
+    c->sdf_shadow_base = d.sdf_word_count;
     c->pool_len = pool;
     c->host_segment_capacity = seg_cap;
     c->h_paths.assign(d.paths, d.paths + d.path_count);
@@ -359,6 +381,9 @@ tk::SceneView view(tk_ctx* c) {
     s.draw_count = c->draw_count;
     s.brush = c->brush.ptr;
     s.brush_words = c->brush_words;
+    s.sdf = c->sdf.ptr;
+    s.sdf_words = c->sdf_words;
+    s.sdf_shadow_base = c->sdf_shadow_base;
     s.layers = c->layers.ptr;
     s.batch_ids = c->batch_ids.ptr;
     s.order = c->order.ptr;
@@ -448,8 +473,15 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nu
     else upload(c->lines, d.lines, d.line_count, st);
     upload(c->draws, d.draws, d.draw_count, st);
     upload(c->brush, d.brush_blob, d.brush_word_count, st);
+    c->sdf.reserve(c->sdf_words);
+    if (d.sdf_word_count)
+        TK_CUDA(cudaMemcpyAsync(c->sdf.ptr, d.sdf_blob, d.sdf_word_count * 4, cudaMemcpyHostToDevice, st));
+    if (d.sdf_shadow_word_count)
+        TK_CUDA(cudaMemcpyAsync(c->sdf.ptr + d.sdf_word_count, d.sdf_shadow_blob, d.sdf_shadow_word_count * 4,
+                                cudaMemcpyHostToDevice, st));
     c->paints.reserve(d.draw_count);
-    tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count, c->paints.ptr, st);
+    tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count,
+                           uint32_t(c->sdf_shadow_base), c->paints.ptr, st);
     upload(c->layers, d.layers, d.layer_count, st);
     upload(c->batch_ids, d.draw_batch_ids, d.draw_count, st);
     upload(c->order, d.draw_order, d.draw_order_count, st);
@@ -853,7 +885,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     uint64_t total_lines = 0;
     std::vector<tk_path_record> paths;
     std::vector<tk_draw_record> draws;
-    std::vector<uint32_t> brush, order, batch_ids, bin_scene, tile_scene;
+    std::vector<uint32_t> brush, sdf, shadow, order, batch_ids, bin_scene, tile_scene;
     std::vector<tk_layer_record> layers;
     std::vector<tk::PassBatch> batches;
     std::vector<tk::BatchScene> table;
@@ -895,15 +927,21 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
             paths.push_back(p);
         }
         const uint32_t brush_base = uint32_t(brush.size());
+        const uint32_t sdf_base = uint32_t(sdf.size()), shadow_base = uint32_t(shadow.size());
         for (uint32_t i = 0; i < d.draw_count; ++i) {
             tk_draw_record r = d.draws[i];
             if (r.path_id != TK_INVALID_INDEX) r.path_id += bi.path_base;
             if (r.brush_offset != TK_INVALID_INDEX) r.brush_offset += brush_base;
+            if (r.sdf_offset != TK_INVALID_INDEX) r.sdf_offset += sdf_base;
+            if (r.sdf_shadow_offset != TK_INVALID_INDEX) r.sdf_shadow_offset += shadow_base;
             draws.push_back(r);
             batch_ids.push_back(d.draw_batch_ids[i] == TK_INVALID_INDEX ? TK_INVALID_INDEX
                                                                         : d.draw_batch_ids[i] + batch_base);
         }
         brush.insert(brush.end(), d.brush_blob, d.brush_blob + d.brush_word_count);
+        sdf.insert(sdf.end(), d.sdf_blob, d.sdf_blob + d.sdf_word_count);
+        shadow.insert(shadow.end(), d.sdf_shadow_blob, d.sdf_shadow_blob + d.sdf_shadow_word_count);
+        if (sdf.size() + shadow.size() > 0xFFFFFFFFull) invalid("batch SDF blobs exceed u32 indexing");
         for (uint32_t i = 0; i < d.layer_count; ++i) {
             tk_layer_record L = d.layers[i];
             L.draw += bi.draw_base;
@@ -970,6 +1008,9 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     c->layer_count = uint32_t(layers.size());
     c->order_count = uint32_t(order.size());
     c->brush_words = brush.size();
+    c->sdf_shadow_base = sdf.size();
+    sdf.insert(sdf.end(), shadow.begin(), shadow.end());
+    c->sdf_words = sdf.size();
     c->pool_len = pool;
     c->host_segment_capacity = segs;
     c->h_paths = paths;
@@ -988,8 +1029,10 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     upload(c->paths, paths.data(), paths.size(), st);
     upload(c->draws, draws.data(), draws.size(), st);
     upload(c->brush, brush.data(), brush.size(), st);
+    upload(c->sdf, sdf.data(), sdf.size(), st);
     c->paints.reserve(draws.size());
-    tk::launch_paint_table(c->draws.ptr, uint32_t(draws.size()), c->brush.ptr, brush.size(), c->paints.ptr, st);
+    tk::launch_paint_table(c->draws.ptr, uint32_t(draws.size()), c->brush.ptr, brush.size(),
+                           uint32_t(c->sdf_shadow_base), c->paints.ptr, st);
     upload(c->layers, layers.data(), layers.size(), st);
     upload(c->batch_ids, batch_ids.data(), batch_ids.size(), st);
     upload(c->order, order.data(), order.size(), st);
@@ -1093,7 +1136,7 @@ void tk_ctx_destroy(tk_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
-    c->lines.release(); c->paths.release(); c->draws.release(); c->brush.release();
+    c->lines.release(); c->paths.release(); c->draws.release(); c->brush.release(); c->sdf.release();
     c->batch_ids.release(); c->order.release(); c->layers.release(); c->items.release();
     c->item_desc.release(); c->tile_desc.release(); c->stats.release(); c->backdrops.release();
     c->counts.release(); c->cursors.release(); c->bumps.release(); c->misc.release();

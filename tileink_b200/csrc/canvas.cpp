@@ -352,8 +352,9 @@ struct Cmd {
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF } kind = FILL;
     tk_path path;
+    tk_sdf_shape shape{};
     bool has_brush = false;
     tk_brush_desc brush{};
     std::vector<tk_gradient_stop> stops;
@@ -392,6 +393,7 @@ struct tk_canvas {
     std::vector<tk_path_record> paths;
     std::vector<tk_draw_record> draws;
     std::vector<uint32_t> brush;
+    std::vector<uint32_t> sdf, shadow;  // SDF and SDF shadow records (Canvas::sdf_blob, sdf_shadow_blob)
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -671,6 +673,138 @@ void compile(tk_canvas* c) {
     c->dirty = false;
 }
 
+
+// ---------------------------------------------------------------------------
+// SDF shapes: physical geometry (canvas/surface.rs:193-245, 435-555), pixel
+// bounds (src/shared/sdf/{rect,circle,line,shadow}.rs) and the 17-word
+// records (src/shared/gpu_sdf.rs:48-260).
+// ---------------------------------------------------------------------------
+// Rust's float-to-int `as` cast: saturating, NaN to 0.
+int32_t sat_i32(double v) {
+    if (v != v) return 0;
+    if (v <= -2147483648.0) return INT32_MIN;
+    if (v >= 2147483647.0) return INT32_MAX;
+    return int32_t(v);
+}
+tk_pixel_bounds box_bounds(double x0, double y0, double x1, double y1) {
+    return {sat_i32(std::floor(x0)), sat_i32(std::floor(y0)), sat_i32(std::ceil(x1)), sat_i32(std::ceil(y1))};
+}
+// shadow_bounds (src/shared/sdf/shadow.rs:35-43), in f32
+tk_pixel_bounds shadow_bounds(const tk_pixel_bounds& b, const float opt[4]) {
+    const float outset = opt[2] * 4.0f + 1.0f;
+    return {sat_i32(std::floor(float(b.x0) + opt[0] - outset)), sat_i32(std::floor(float(b.y0) + opt[1] - outset)),
+            sat_i32(std::ceil(float(b.x1) + opt[0] + outset)), sat_i32(std::ceil(float(b.y1) + opt[1] + outset))};
+}
+// Circle::bounds (src/shared/sdf/circle.rs:13-20), in f32
+tk_pixel_bounds circle_bounds(double cx, double cy, float r) {
+    return {sat_i32(std::floor(float(cx) - r)), sat_i32(std::floor(float(cy) - r)), sat_i32(std::ceil(float(cx) + r)),
+            sat_i32(std::ceil(float(cy) + r))};
+}
+// Line::bounds (src/shared/sdf/line.rs:51-83)
+tk_pixel_bounds line_bounds(double sx, double sy, double ex, double ey, float width, uint32_t cap) {
+    const double half = double(width) * 0.5;
+    const double dx = ex - sx, dy = ey - sy, len = std::hypot(dx, dy);
+    if (len == 0.0) return box_bounds(sx - half, sy - half, sx + half, sy + half);
+    const double ux = dx / len, uy = dy / len;
+    double x0 = sx, y0 = sy, x1 = ex, y1 = ey;
+    if (cap == TK_SDF_CAP_SQUARE) {
+        x0 -= ux * half;
+        y0 -= uy * half;
+        x1 += ux * half;
+        y1 += uy * half;
+    }
+    return box_bounds(std::min(x0, x1) - half, std::min(y0, y1) - half, std::max(x0, x1) + half,
+                      std::max(y0, y1) + half);
+}
+
+// The physical record and bounds of `s` (logical); false when the shape draws
+// nothing (the reference's None).
+bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_RECORD_WORDS], tk_pixel_bounds& pb) {
+    const float sc = c->scale;
+    const double sd = double(sc);
+    std::memset(rec, 0, TK_SDF_RECORD_WORDS * 4);
+    rec[0] = s.kind;
+    auto put = [&](int i, float v) { rec[i] = fbits(v); };
+    const bool shadow = s.kind == TK_SDF_RECT_SHADOW || s.kind == TK_SDF_CIRCLE_SHADOW || s.kind == TK_SDF_LINE_SHADOW;
+    float opt[4] = {0, 0, 0, 0};
+    if (shadow) {  // ShadowOptions::normalized, then physical_shadow_options
+        const float intensity = std::min(std::max(s.shadow[3], 0.0f), 1.0f);
+        if (!(intensity > 0.0f)) return false;
+        opt[0] = s.shadow[0] * sc;
+        opt[1] = s.shadow[1] * sc;
+        opt[2] = std::max(s.shadow[2], 0.0f) * sc;
+        opt[3] = intensity;
+        for (int k = 0; k < 4; ++k) put(13 + k, opt[k]);
+    }
+    const double x0 = s.p0[0] * sd, y0 = s.p0[1] * sd, x1 = s.p1[0] * sd, y1 = s.p1[1] * sd;
+    switch (s.kind) {
+        case TK_SDF_RECT:
+        case TK_SDF_RECT_STROKE:
+        case TK_SDF_RECT_SHADOW: {
+            const double ax0 = std::min(x0, x1), ay0 = std::min(y0, y1), ax1 = std::max(x0, x1), ay1 = std::max(y0, y1);
+            put(1, float(ax0));
+            put(2, float(ay0));
+            put(3, float(ax1));
+            put(4, float(ay1));
+            for (int k = 0; k < 4; ++k) put(5 + k, s.radii[k] * sc);
+            pb = box_bounds(ax0, ay0, ax1, ay1);
+            if (s.kind == TK_SDF_RECT_STROKE) {
+                float half[4];  // StrokeWidths::half of the physical clamped widths
+                bool any = false;
+                for (int k = 0; k < 4; ++k) {
+                    const float w = std::max(s.widths[k], 0.0f);
+                    any = any || w != 0.0f;
+                    half[k] = std::max(w * sc, 0.0f) * 0.5f;
+                }
+                if (!any) return false;
+                for (int k = 0; k < 4; ++k) put(9 + k, half[k]);
+                // RectStroke::bounds: the outer rectangle (top, right, bottom, left)
+                pb = box_bounds(ax0 - double(half[3]), ay0 - double(half[0]), ax1 + double(half[1]),
+                                ay1 + double(half[2]));
+            }
+            if (shadow) pb = shadow_bounds(pb, opt);
+            return true;
+        }
+        case TK_SDF_CIRCLE:
+        case TK_SDF_CIRCLE_STROKE:
+        case TK_SDF_CIRCLE_SHADOW: {
+            const float r = float(s.radius) * sc;
+            put(1, float(x0));
+            put(2, float(y0));
+            put(3, r);
+            pb = circle_bounds(x0, y0, r);
+            if (s.kind == TK_SDF_CIRCLE_STROKE) {
+                if (!(s.width > 0.0)) return false;
+                const float hw = float(s.width * 0.5) * sc;
+                for (int k = 0; k < 4; ++k) put(9 + k, hw);
+                pb = circle_bounds(x0, y0, r + std::max(hw, 0.0f));
+            }
+            if (shadow) pb = shadow_bounds(pb, opt);
+            return true;
+        }
+        case TK_SDF_LINE:
+        case TK_SDF_LINE_SHADOW: {
+            // Line::is_empty (src/shared/sdf/line.rs:45-49)
+            const float w = float(s.width);
+            if (s.cap > TK_SDF_CAP_ROUND) return false;
+            if (w <= 0.0f || !(w == w) || (s.cap == TK_SDF_CAP_BUTT && s.p0[0] == s.p1[0] && s.p0[1] == s.p1[1]))
+                return false;
+            const float pw = w * sc;
+            put(1, float(x0));
+            put(2, float(y0));
+            put(3, float(x1));
+            put(4, float(y1));
+            put(5, pw);
+            put(6, float(s.cap));
+            pb = line_bounds(x0, y0, x1, y1, pw, s.cap);
+            if (shadow) pb = shadow_bounds(pb, opt);
+            return true;
+        }
+        default:
+            return false;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -781,6 +915,49 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
     return add_path(c, bb, line_start, uint32_t(c->lines.size()) - line_start, brush, TK_FILL_NONZERO, TK_DRAW_BRUSH,
                     true);
 }
+int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush) {
+    if (!c || !shape) return -1;
+    const uint32_t k = shape->kind;
+    if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
+        k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW)
+        return -1;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::SDF, nullptr, brush, nullptr);
+        r.shape = *shape;
+        c->log.push_back(std::move(r));
+    }
+    uint32_t rec[TK_SDF_RECORD_WORDS];
+    tk_pixel_bounds pb{0, 0, 0, 0};
+    if (!encode_sdf(c, *shape, rec, pb)) return -2;
+    const bool shadow = k == TK_SDF_RECT_SHADOW || k == TK_SDF_CIRCLE_SHADOW || k == TK_SDF_LINE_SHADOW;
+    std::vector<uint32_t>& blob = shadow ? c->shadow : c->sdf;
+    const uint32_t off = uint32_t(blob.size());
+    blob.insert(blob.end(), rec, rec + TK_SDF_RECORD_WORDS);
+    tk_brush_desc transparent{};
+    transparent.kind = TK_BRUSH_KIND_SOLID;
+    auto br = push_brush(c->brush, brush ? *brush : transparent);
+    // push_physical_sdf_record / push_physical_sdf_shadow_record (canvas/paths.rs:207-300)
+    tk_draw_record d{};
+    d.path_id = TK_INVALID_INDEX;
+    d.glyph_run_id = TK_INVALID_INDEX;
+    d.sdf_offset = shadow ? TK_INVALID_INDEX : off;
+    d.sdf_len = shadow ? 0u : TK_SDF_RECORD_WORDS;
+    d.sdf_shadow_offset = shadow ? off : TK_INVALID_INDEX;
+    d.sdf_shadow_len = shadow ? TK_SDF_RECORD_WORDS : 0u;
+    d.brush_offset = br.first;
+    d.brush_len = br.second;
+    d.tag = TK_DRAW_BRUSH;
+    d.fill_rule = TK_FILL_NONZERO;
+    d.pixel_bounds = pb;
+    d.local_pixel_bounds = pb;
+    d.transform = tk_affine{1, 0, 0, 1, 0, 0};
+    d.inverse_transform = tk_affine{1, 0, 0, 1, 0, 0};
+    const uint32_t draw_ix = uint32_t(c->draws.size());
+    c->draws.push_back(d);
+    c->lists[c->stack.back()].push_back({Cmd::DRAW, draw_ix, 0.0f, 0u});
+    c->dirty = true;
+    return draw_ix;
+}
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform, uint32_t rule,
                                   double tolerance) {
     if (!c || !path || rule > 1u || !(tolerance > 0.0)) return -1;
@@ -840,6 +1017,10 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->draw_count = uint32_t(c->draws.size());
     out->brush_blob = c->brush.data();
     out->brush_word_count = c->brush.size();
+    out->sdf_blob = c->sdf.data();
+    out->sdf_word_count = c->sdf.size();
+    out->sdf_shadow_blob = c->shadow.data();
+    out->sdf_shadow_word_count = c->shadow.size();
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -1250,6 +1431,18 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::BLUR: return tk_canvas_push_blur_group(dst, r.sigma);
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
+        case RecCmd::SDF: {
+            // SDF records carry no draw transform: they replay under translations
+            tk_sdf_shape sh = r.shape;
+            if (t) {
+                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+                sh.p0[0] += t[4];
+                sh.p0[1] += t[5];
+                sh.p1[0] += t[4];
+                sh.p1[1] += t[5];
+            }
+            return tk_canvas_push_sdf(dst, &sh, bp) == -1 ? -1 : 0;
+        }
     }
     return -1;
 }

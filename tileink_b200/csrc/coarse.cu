@@ -16,6 +16,7 @@
 
 #include "device.cuh"
 #include "kernels.h"
+#include "sdf.cuh"
 
 namespace tk {
 namespace {
@@ -29,7 +30,11 @@ constexpr int kBinSide = 16;
 constexpr int kQuadSide = 8;
 constexpr int kQuads = (kBinSide / kQuadSide) * (kBinSide / kQuadSide);
 constexpr int kCoarseThreads = kQuadSide * kQuadSide;
-constexpr uint32_t kChunkClassColor = 1u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
+constexpr uint32_t kChunkClassColor = 1u, kChunkClassSdf = 2u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
+// DrawInfo::meta bits
+constexpr uint32_t kMetaPath = 16u, kMetaSolid = 32u, kMetaSdf = 64u, kMetaSdfSolidClass = 128u;
+// DrawInfo::py bits of an SDF draw (px holds its first SDF word)
+constexpr uint32_t kSdfPlain = 256u, kSdfIdentity = 512u;
 // Candidates whose tile loads are in flight together, per pass (emission
 // keeps more state live and holds fewer).
 constexpr uint32_t kPrefetchCount = 8, kPrefetchEmit = 4;
@@ -103,9 +108,9 @@ __global__ void __launch_bounds__(256)
 struct DrawInfo {
     uint32_t draw;
     uint32_t tx, ty;         // draw tile bbox: x0 | x1 << 16, y0 | y1 << 16
-    uint32_t px, py;         // path tile bbox packed the same way
+    uint32_t px, py;         // path tile bbox packed the same way; SDF draws: first SDF word, kind | flags
     uint32_t data_offset;
-    uint32_t meta;           // tag | fill << 3 | valid_path << 4 | color_candidate << 5 | batch << 8
+    uint32_t meta;           // tag | fill << 3 | kMeta* bits | batch << 8
     uint32_t color;
 };
 
@@ -116,6 +121,8 @@ struct Ctx {
     const tk_layer_record* layers;
     const uint32_t* brush;
     uint64_t brush_words;
+    const uint32_t* sdf;
+    uint64_t sdf_shadow_base;
     const int32_t* backdrops;
     const tk_segment_range* ranges;
     uint32_t tw, th;
@@ -267,8 +274,11 @@ __global__ void __launch_bounds__(kCoarseThreads)
             uint64_t end = emit_stack(c, b, tx, ty, false, ptcl, cap, at, error);
             uint32_t skip = 0;
             if (flags & kChunkClassOccluder) skip = wrappers ? 0u : occluded_prefix_g(ptcl, section + 1u, end);
-            uint32_t kind = (flags & kChunkClassOther) ? TK_TILE_KIND_INTERPRETER
-                            : ((flags & kChunkClassColor) ? TK_TILE_KIND_COLOR : TK_TILE_KIND_EMPTY);
+            // classify_tile_flags (coarse/tile_classification.hlsli:6-10)
+            uint32_t kind = TK_TILE_KIND_EMPTY;
+            if (flags & kChunkClassOther) kind = TK_TILE_KIND_INTERPRETER;
+            else if (flags & kChunkClassSdf) kind = (flags & kChunkClassColor) ? TK_TILE_KIND_MIXED : TK_TILE_KIND_SDF;
+            else if (flags & kChunkClassColor) kind = TK_TILE_KIND_COLOR;
             store_ptcl(ptcl, cap, section, TK_PTCL_BATCH_BEGIN, 0u, 0u, b.batch_id, nb + 2u * wrappers,
                        kind | (skip << TK_TILE_PREFIX_SHIFT), error);
             at = end;
@@ -295,15 +305,36 @@ __global__ void __launch_bounds__(kCoarseThreads)
             }
             bool color_candidate = false;
             info.color = di;
-            if (d.tag == TK_DRAW_BRUSH && d.solid_rect != 0u && d.transform.b == 0.0f && d.transform.c == 0.0f &&
-                d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID) {
-                uint32_t col = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
-                if (col != 0u) { color_candidate = true; info.color = col; }
+            // nontransparent_solid (coarse/paint.hlsli:13-17)
+            const bool solid = d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID &&
+                               brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
+            const bool has_sdf = d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX;
+            uint32_t sdf_bits = 0u;
+            if (has_sdf) {
+                // draw_has_sdf (shared/draw.hlsli:31): only brush draws give a particle
+                valid_path = false;
+                const bool plain = d.sdf_offset != TK_INVALID_INDEX;
+                info.px = plain ? d.sdf_offset : uint32_t(c.sdf_shadow_base) + d.sdf_shadow_offset;
+                const uint32_t kind = __ldg(c.sdf + info.px);
+                const bool ident = d.transform.a == 1.0f && d.transform.b == 0.0f && d.transform.c == 0.0f &&
+                                   d.transform.d == 1.0f;
+                info.py = (kind & 255u) | (plain ? kSdfPlain : 0u) | (ident ? kSdfIdentity : 0u);
+                if (d.tag == TK_DRAW_BRUSH) sdf_bits |= kMetaSdf;
+                if (solid) {
+                    color_candidate = true;
+                    info.color = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
+                }
+                // solid_supported_sdf (coarse/paint.hlsli:21-25)
+                if (solid && plain && kind == TK_SDF_RECT) sdf_bits |= kMetaSdfSolidClass;
+            } else if (d.tag == TK_DRAW_BRUSH && d.solid_rect != 0u && d.transform.b == 0.0f &&
+                       d.transform.c == 0.0f && solid) {
+                color_candidate = true;
+                info.color = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
             }
             if (d.tag == TK_DRAW_CLIP) info.color = 0u;
             uint32_t batch = batch_ids[di] - batch0;
-            info.meta = (d.tag & 7u) | ((d.fill_rule & 1u) << 3) | (uint32_t(valid_path) << 4) |
-                        (uint32_t(color_candidate) << 5) | (batch << 8);
+            info.meta = (d.tag & 7u) | ((d.fill_rule & 1u) << 3) | (valid_path ? kMetaPath : 0u) |
+                        (color_candidate ? kMetaSolid : 0u) | sdf_bits | (batch << 8);
             s_d[threadIdx.x] = info;
         }
         __syncthreads();
@@ -316,7 +347,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
         for (uint32_t k0 = 0; k0 < m; k0 += kPrefetch) {
             tk_segment_range rr[kPrefetch];
             uint32_t ww[kPrefetch];
-            uint32_t hit = 0u;
+            uint32_t hit = 0u, sdf_hit = 0u;
 #pragma unroll
             for (uint32_t q = 0; q < kPrefetch; ++q) {
                 rr[q] = tk_segment_range{0u, 0u};
@@ -326,7 +357,11 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 const DrawInfo& d = s_d[k];
                 if (!(tx >= (d.tx & 0xFFFFu) && tx < (d.tx >> 16) && ty >= (d.ty & 0xFFFFu) && ty < (d.ty >> 16))) continue;
                 const uint32_t meta = d.meta;
-                if (!(meta & 16u)) continue;
+                if (meta & kMetaSdf) {
+                    sdf_hit |= 1u << q;
+                    continue;
+                }
+                if (!(meta & kMetaPath)) continue;
                 const uint32_t px0 = d.px & 0xFFFFu, px1 = d.px >> 16, py0 = d.py & 0xFFFFu, py1 = d.py >> 16;
                 if (px1 <= px0 || tx < px0 || ty < py0 || tx >= px1 || ty >= py1) continue;
                 const uint32_t tag = meta & 7u;
@@ -338,12 +373,32 @@ __global__ void __launch_bounds__(kCoarseThreads)
             }
 #pragma unroll
             for (uint32_t q = 0; q < kPrefetch; ++q) {
-                if (!(hit & (1u << q))) continue;
+                if (!((hit | sdf_hit) & (1u << q))) continue;
                 const DrawInfo& d = s_d[k0 + q];
                 const uint32_t meta = d.meta, tag = meta & 7u;
                 const tk_segment_range r = rr[q];
                 const uint32_t w = ww[q];
-                if (r.start == r.end && w == 0u) continue;
+                uint32_t sdf_tag = 0u;  // the SDF draw's particle: TK_PTCL_SDF or TK_PTCL_COLOR
+                if (sdf_hit & (1u << q)) {
+                    // draw_particle for SDF draws (coarse/emit_draw.hlsli:22-30): no
+                    // particle inside a rect stroke's hole (sdf_stroke_empty); a solid
+                    // rect covering the tile becomes a colour (full_tile_solid)
+                    const uint32_t kind = d.py & 255u;
+                    const bool proof = (d.py & kSdfPlain) && (d.py & kSdfIdentity) &&
+                                       (kind == TK_SDF_RECT_STROKE || (kind == TK_SDF_RECT && (meta & kMetaSolid)));
+                    sdf_tag = TK_PTCL_SDF;
+                    if (proof) {
+                        const tk_draw_record& dr = c.draws[d.draw];
+                        const float ex = dr.transform.e, ey = dr.transform.f;
+                        if (kind == TK_SDF_RECT_STROKE) {
+                            if (sdf_stroke_empty(c.sdf + d.px, ex, ey, tx, ty)) continue;
+                        } else if (sdf_rect_covers(c.sdf + d.px, ex, ey, tx, ty)) {
+                            sdf_tag = TK_PTCL_COLOR;
+                        }
+                    }
+                } else if (r.start == r.end && w == 0u) {
+                    continue;
+                }
                 uint32_t batch = meta >> 8;
                 if (batch != cur) {
                     close();
@@ -358,10 +413,22 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     }
                 }
                 if (rejected) continue;
+                if (sdf_tag) {
+                    if (EMIT) {
+                        // particle_class_flags (coarse/paint.hlsli:35-40)
+                        const bool color = sdf_tag == TK_PTCL_COLOR;
+                        flags |= color ? kChunkClassColor : ((meta & kMetaSdfSolidClass) ? kChunkClassSdf : kChunkClassOther);
+                        if (wrappers == 0u && color && (d.color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
+                        if (color) store_ptcl(ptcl, cap, at++, TK_PTCL_COLOR, 0u, 0u, 0u, 0u, d.color, error);
+                        else store_ptcl(ptcl, cap, at++, TK_PTCL_SDF, 0u, 0u, d.draw, 0u, d.draw, error);
+                    }
+                    ++nb;
+                    continue;
+                }
                 uint32_t ptag = TK_PTCL_FILL;
                 if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
                 else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
-                else if ((meta & 32u) && r.start == r.end) ptag = TK_PTCL_COLOR;
+                else if ((meta & kMetaSolid) && r.start == r.end) ptag = TK_PTCL_COLOR;
                 if (EMIT) {
                     flags |= ptag == TK_PTCL_COLOR ? kChunkClassColor : kChunkClassOther;
                     uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
@@ -484,7 +551,8 @@ void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st) {
 }
 
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st) {
-    Ctx c{s.draws, s.paths, s.path_count, s.layers, s.brush, s.brush_words, s.backdrops, s.ranges, s.tw, s.th};
+    Ctx c{s.draws, s.paths, s.path_count, s.layers, s.brush, s.brush_words, s.sdf, s.sdf_shadow_base, s.backdrops,
+          s.ranges, s.tw, s.th};
     const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
     if (nbins == 0) return;
     if (emit)

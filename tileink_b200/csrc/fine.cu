@@ -25,6 +25,7 @@
 
 #include "device.cuh"
 #include "kernels.h"
+#include "sdf.cuh"
 
 namespace tk {
 namespace {
@@ -74,7 +75,8 @@ struct FineSmem {
     uint2 rec_b[kRecChunk];                      // segment_end, color
     uint32_t cls[kRecChunk];
     uint32_t ualpha[kRecChunk];
-    uint32_t umode[kRecChunk];                   // uniform fills: 1 replace, 2 src-over, 3 no-op
+    uint32_t umode[kRecChunk];                   // uniform fills: 1 replace, 2 src-over, 3 no-op;
+                                                 // SDF records: first word of the shape
     uint32_t paint[kRecChunk];                   // solid premul color, or kGradient
     alignas(16) float gp[kRecChunk][kGradParams];  // gradient terms of the chunk's fills (PaintInfo::g)
     uint4 gk[kRecChunk];                         // kind | flags, ramp word (or color), ramp length, extend
@@ -150,12 +152,15 @@ __device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db
 // One thread per draw: the draw's PaintInfo (solid colour, or the decoded
 // gradient of its brush under its inverse transform).
 __global__ void k_paint_table(const tk_draw_record* __restrict__ draws, uint32_t n, const uint32_t* __restrict__ brush,
-                              uint64_t brush_words, PaintInfo* out) {
+                              uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out) {
     const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
     const Paint P{brush, brush_words};
     const uint32_t bo = draws[d].brush_offset;
     PaintInfo info{};
+    // sdf_coverage_from_draw (fine/draw.hlsli:21-26): the SDF record, else the shadow record
+    const uint32_t so = draws[d].sdf_offset, ho = draws[d].sdf_shadow_offset;
+    info.sdf = so != TK_INVALID_INDEX ? so : (ho != TK_INVALID_INDEX ? sdf_shadow_base + ho : TK_INVALID_INDEX);
     if (P.word(bo) == TK_BRUSH_SOLID) {
         info.paint = P.word(bo + TK_BRUSH_COLOR_WORD);
     } else {
@@ -374,7 +379,8 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
 __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
-           const uint32_t* __restrict__ brush, uint64_t brush_words, uint64_t seg_capacity, uint32_t* target,
+           const uint32_t* __restrict__ brush, uint64_t brush_words, const tk_draw_record* __restrict__ draws,
+           const uint32_t* __restrict__ sdf, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
            const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -435,8 +441,9 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 if (a.x == TK_PTCL_FILL && n != 0u) cls = kClsFill;  // row sums staged below
             }
             S.nseg[tid] = n;
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH) {
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || a.x == TK_PTCL_SDF) {
                 const PaintInfo* pi = paints + c.y;
+                if (a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
                 const uint32_t paint = __ldg(&pi->paint);
                 if (paint != kGradient) {
                     S.paint[tid] = paint;
@@ -577,6 +584,21 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                         px = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(px), a));
                     }
                 }
+            } else if (tag == TK_PTCL_SDF) {
+                // PTCL_SDF (fine/interpreter.hlsli:70-84): analytic coverage of the
+                // draw's SDF record at the pixel centre mapped to draw space
+                // (affine_record_point, shared/affine.hlsli:14-18)
+                if (clip != 0u) {
+                    const tk_affine* t = &draws[qb.y].inverse_transform;
+                    const tk_affine inv{__ldg(&t->a), __ldg(&t->b), __ldg(&t->c),
+                                        __ldg(&t->d), __ldg(&t->e), __ldg(&t->f)};
+                    const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
+                    const float ux = __fmaf_rn(inv.a, sx, __fmaf_rn(inv.c, sy, inv.e));
+                    const float uy = __fmaf_rn(inv.b, sx, __fmaf_rn(inv.d, sy, inv.f));
+                    const float cov = sdf_coverage(sdf + S.umode[i], ux, uy, inv);
+                    const uint32_t masked = combine_alpha(coverage_to_u8(cov), clip);
+                    if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
+                }
             } else if (is_fill_like(tag)) {
                 uint32_t alpha;
                 if (S.nseg[i] == 0u) {
@@ -650,8 +672,10 @@ __global__ void __launch_bounds__(kFineThreads, 4)
 }  // namespace
 
 void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
-                        uint64_t brush_words, PaintInfo* out, cudaStream_t st) {
-    if (draw_count) k_paint_table<<<(draw_count + 255) / 256, 256, 0, st>>>(draws, draw_count, brush, brush_words, out);
+                        uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out, cudaStream_t st) {
+    if (draw_count)
+        k_paint_table<<<(draw_count + 255) / 256, 256, 0, st>>>(draws, draw_count, brush, brush_words,
+                                                                sdf_shadow_base, out);
 }
 
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st) {
@@ -663,7 +687,7 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
         configured = true;
     }
     k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
-                                                      s.segment_capacity, target, s.width, s.height, s.tw, s.error,
+                                                      s.draws, s.sdf, s.segment_capacity, target, s.width, s.height, s.tw, s.error,
                                                       p.scenes, p.tile_scene, p.tile_list);
 }
 

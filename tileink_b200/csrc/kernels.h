@@ -45,10 +45,12 @@ static_assert(sizeof(SegmentRec) == 32, "one sector per segment");
 
 // A draw's paint as fine raster needs it, decoded once per upload from the
 // draw record and its brush (fine.cu): the solid premultiplied colour, or
-// kGradient with the gradient's brush-only terms.
+// kGradient with the gradient's brush-only terms, and the first word of the
+// draw's SDF record in the device SDF buffer (TK_INVALID_INDEX for none).
 struct alignas(16) PaintInfo {
     uint32_t paint;      // premultiplied RGBA8, or 0xFFFFFFFF for a gradient
-    uint32_t pad[3];
+    uint32_t sdf;
+    uint32_t pad[2];
     uint4 gk;            // kind | flags, ramp word (or colour), ramp length, extend
     float g[24];         // transforms and brush terms (fine.cu stage_gradient)
 };
@@ -63,6 +65,10 @@ struct SceneView {
     uint32_t draw_count;
     const uint32_t* brush;
     uint64_t brush_words;
+    // SDF records: the scene's sdf_blob followed by its sdf_shadow_blob
+    const uint32_t* sdf;
+    uint64_t sdf_words;
+    uint64_t sdf_shadow_base;
     const tk_layer_record* layers;
     const uint32_t* batch_ids;
     const uint32_t* order;
@@ -150,9 +156,10 @@ void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st);
-// The per-draw PaintInfo table of the uploaded draws and brush blob.
+// The per-draw PaintInfo table of the uploaded draws and brush blob; shadow
+// records start at word sdf_shadow_base of the device SDF buffer.
 void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
-                        uint64_t brush_words, PaintInfo* out, cudaStream_t st);
+                        uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out, cudaStream_t st);
 
 // Images.
 void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);

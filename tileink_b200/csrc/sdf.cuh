@@ -1,0 +1,294 @@
+// Analytic SDF shapes: the distance samples, their pixel coverage, and the
+// coarse-stage tile proofs (full-tile colour, hollow stroke interiors).
+//
+// Follows shared/sdf/{base,basic,line,coverage}.hlsli and
+// coarse/sdf_clip.hlsli of the reference. Every operation is an IEEE
+// single-precision add, multiply, divide or square root (no contraction: the
+// library is built with -fmad=false) or an explicit fused multiply-add where
+// the reference writes `mad`, so a host restatement with the same operation
+// order gives identical bits. Shadow falloff uses sdf_exp_nonpos below
+// instead of the device exp for the same reason.
+#pragma once
+#include <math.h>
+#include <stdint.h>
+
+#include "../../include/tileink.h"
+
+namespace tkd {
+
+struct SdfSample {
+    float d, nx, ny;
+};
+
+// sdf_length (shared/sdf/base.hlsli:7-12): the plain length, rescaled by the
+// larger axis only when the squared length leaves the float range.
+__device__ __forceinline__ float sdf_length(float x, float y) {
+    const float m = sqrtf(x * x + y * y);
+    if (m > 0.0f && isfinite(m)) return m;
+    const float axis = fmaxf(fabsf(x), fabsf(y));
+    if (axis == 0.0f) return 0.0f;
+    const float sx = x / axis, sy = y / axis;
+    return axis * sqrtf(sx * sx + sy * sy);
+}
+
+// normalized_or (shared/sdf/base.hlsli:14-23).
+__device__ __forceinline__ void normalized_or(float x, float y, float fx, float fy, float& ox, float& oy) {
+    const float m = sqrtf(x * x + y * y);
+    if (m > 0.0f && isfinite(m)) {
+        ox = x / m;
+        oy = y / m;
+        return;
+    }
+    const float axis = fmaxf(fabsf(x), fabsf(y));
+    if (axis == 0.0f) {
+        ox = fx;
+        oy = fy;
+        return;
+    }
+    const float sx = x / axis, sy = y / axis;
+    const float l = sqrtf(sx * sx + sy * sy);
+    ox = sx / l;
+    oy = sy / l;
+}
+
+// rounded_box_sdf_sample (shared/sdf/basic.hlsli:6-19).
+__device__ __forceinline__ SdfSample rounded_box(float px, float py, float hx, float hy, float radius) {
+    const float qx = fabsf(px) - hx + radius, qy = fabsf(py) - hy + radius;
+    const float ox = fmaxf(qx, 0.0f), oy = fmaxf(qy, 0.0f);
+    const float ol = sdf_length(ox, oy);
+    const float d = fminf(fmaxf(qx, qy), 0.0f) + ol - radius;
+    const float sx = px >= 0.0f ? 1.0f : -1.0f, sy = py >= 0.0f ? 1.0f : -1.0f;
+    if (ol > 0.0f) return SdfSample{d, ox / ol * sx, oy / ol * sy};
+    if (qx > qy) return SdfSample{d, sx, 0.0f};
+    return SdfSample{d, 0.0f, sy};
+}
+
+// local_line_rect_sample (shared/sdf/basic.hlsli:21-25).
+__device__ __forceinline__ SdfSample line_rect(float axis, float normal, float x0, float x1, float half_height) {
+    const float center = (x0 + x1) * 0.5f, half_width = (x1 - x0) * 0.5f;
+    return rounded_box(axis - center, normal, half_width, half_height, 0.0f);
+}
+
+// circle_sdf_sample (shared/sdf/basic.hlsli:27-32).
+__device__ __forceinline__ SdfSample circle_sample(float x, float y, float cx, float cy, float radius) {
+    const float dx = x - cx, dy = y - cy;
+    SdfSample s;
+    s.d = sdf_length(dx, dy) - radius;
+    normalized_or(dx, dy, 1.0f, 0.0f, s.nx, s.ny);
+    return s;
+}
+
+// rect_sdf_sample (shared/sdf/basic.hlsli:34-57): the corner radius of the
+// quadrant the point is in, clamped to the half extents.
+__device__ __forceinline__ SdfSample rect_sample(float x, float y, float x0r, float y0r, float x1r, float y1r, float tl,
+                                                 float tr, float bl, float br) {
+    const float x0 = fminf(x0r, x1r), y0 = fminf(y0r, y1r), x1 = fmaxf(x0r, x1r), y1 = fmaxf(y0r, y1r);
+    const float cx = (x0 + x1) * 0.5f, cy = (y0 + y1) * 0.5f;
+    const float hx = (x1 - x0) * 0.5f, hy = (y1 - y0) * 0.5f;
+    const float px = x - cx, py = y - cy;
+    float radius = tl;
+    if (px >= 0.0f) radius = py <= 0.0f ? tr : br;
+    else if (py > 0.0f) radius = bl;
+    const float r = fmaxf(fminf(fminf(radius, hx), hy), 0.0f);
+    return rounded_box(px, py, hx, hy, r);
+}
+
+// line_sdf_sample (shared/sdf/line.hlsli:8-76): butt (cap 0), square (1) or
+// round (2) ends; the normal is rotated back from the line frame.
+__device__ __forceinline__ SdfSample line_sample(float x, float y, float sx, float sy, float ex, float ey, float width,
+                                                 float cap) {
+    const float he = fmaxf(width, 0.0f) * 0.5f;
+    const float dx = ex - sx, dy = ey - sy;
+    const float len = sdf_length(dx, dy);
+    SdfSample s{__int_as_float(0x7f800000), 1.0f, 0.0f};
+    if (len == 0.0f) {
+        if (cap >= 0.5f) {
+            if (cap > 1.5f) {
+                const float px = x - sx, py = y - sy;
+                s.d = sdf_length(px, py) - he;
+                normalized_or(px, py, 1.0f, 0.0f, s.nx, s.ny);
+            } else {
+                s = line_rect(x - sx, y - sy, -he, he, he);
+            }
+        }
+        return s;
+    }
+    const float ux = dx / len, uy = dy / len;
+    const float px = x - sx, py = y - sy;
+    const float axis = px * ux + py * uy;
+    const float normal = -px * uy + py * ux;
+    if (cap < 0.5f) {
+        s = line_rect(axis, normal, 0.0f, len, he);
+    } else if (cap < 1.5f) {
+        s = line_rect(axis, normal, -he, len + he, he);
+    } else {
+        const float nearest = fminf(fmaxf(axis, 0.0f), len);
+        const float ax = axis - nearest;
+        s.d = sdf_length(ax, normal) - he;
+        normalized_or(ax, normal, 0.0f, 1.0f, s.nx, s.ny);
+    }
+    return SdfSample{s.d, s.nx * ux - s.ny * uy, s.nx * uy + s.ny * ux};
+}
+
+// sdf_coverage_from_dist / sdf_coverage_from_sample
+// (shared/sdf/base.hlsli:39-52): the distance in device pixels is the local
+// distance over the length of the inverse transform applied to the normal.
+__device__ __forceinline__ float coverage_from_sample(const SdfSample& s, const tk_affine& inv) {
+    const float gx = __fmaf_rn(inv.a, s.nx, inv.b * s.ny);
+    const float gy = __fmaf_rn(inv.c, s.nx, inv.d * s.ny);
+    const float footprint = sdf_length(gx, gy);
+    if (footprint == 0.0f) return s.d < 0.0f ? 1.0f : (s.d > 0.0f ? 0.0f : 0.5f);
+    return fminf(fmaxf(0.5f - s.d / footprint, 0.0f), 1.0f);
+}
+
+// exp(x) for x <= 0 (positive x is not used and gives 1): evaluated in double
+// as 2^k * e^r with k the nearest integer to x / ln 2 and |r| <= ln 2 / 2,
+// e^r by its Taylor series to degree 13 (truncation below 2^-57), 2^k
+// assembled from its exponent bits. Only exactly rounded double operations are
+// used, so host and device agree bit for bit; the float result is within half
+// an ulp of exp(x) over the tested range.
+__device__ __forceinline__ float sdf_exp_nonpos(float x) {
+    if (!(x <= 0.0f)) return x != x ? x : 1.0f;
+    if (x < -104.0f) return 0.0f;
+    const double ln2 = 0.69314718055994530942;
+    const double xd = double(x);
+    const double k = floor(xd / ln2 + 0.5);
+    const double r = xd - k * ln2;
+    double p = 1.0;
+    for (int n = 13; n >= 1; --n) p = 1.0 + r * p / double(n);
+    const double scale = __longlong_as_double((long long)(1023 + (long long)k) << 52);
+    return float(p * scale);
+}
+
+// sdf_shadow_coverage_from_sample (shared/sdf/base.hlsli:54-62).
+__device__ __forceinline__ float shadow_coverage(const SdfSample& s, const tk_affine& inv, float expand,
+                                                 float intensity) {
+    const float ci = fminf(fmaxf(intensity, 0.0f), 1.0f);
+    if (expand > 0.0f) return fminf(fmaxf(sdf_exp_nonpos(-fmaxf(s.d, 0.0f) / expand) * ci, 0.0f), 1.0f);
+    return coverage_from_sample(s, inv) * ci;
+}
+
+__device__ __forceinline__ float sdf_word_f(const uint32_t* w, uint32_t i) { return __uint_as_float(__ldg(w + i)); }
+
+// sdf_coverage_from_blob (shared/sdf/coverage.hlsli:13-236) for the record at
+// `w` (TK_SDF_RECORD_WORDS words), sampled at local point (x, y).
+__device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float y, const tk_affine& inv) {
+    const uint32_t kind = __ldg(w);
+    const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
+    const float r0 = sdf_word_f(w, 5), r1 = sdf_word_f(w, 6), r2 = sdf_word_f(w, 7), r3 = sdf_word_f(w, 8);
+    switch (kind) {
+        case TK_SDF_RECT:
+            return coverage_from_sample(rect_sample(x, y, x0, y0, x1, y1, r0, r1, r2, r3), inv);
+        case TK_SDF_RECT_STROKE: {
+            const float ht = fmaxf(sdf_word_f(w, 9), 0.0f), hr = fmaxf(sdf_word_f(w, 10), 0.0f);
+            const float hb = fmaxf(sdf_word_f(w, 11), 0.0f), hl = fmaxf(sdf_word_f(w, 12), 0.0f);
+            const float rx0 = fminf(x0, x1), ry0 = fminf(y0, y1), rx1 = fmaxf(x0, x1), ry1 = fmaxf(y0, y1);
+            const float outer = coverage_from_sample(
+                rect_sample(x, y, rx0 - hl, ry0 - ht, rx1 + hr, ry1 + hb, r0 + fmaxf(ht, hl), r1 + fmaxf(ht, hr),
+                            r2 + fmaxf(hb, hl), r3 + fmaxf(hb, hr)),
+                inv);
+            const float ix0 = rx0 + hl, iy0 = ry0 + ht, ix1 = rx1 - hr, iy1 = ry1 - hb;
+            float inner = 0.0f;
+            if (ix0 < ix1 && iy0 < iy1)
+                inner = coverage_from_sample(
+                    rect_sample(x, y, ix0, iy0, ix1, iy1, fmaxf(r0 - fmaxf(ht, hl), 0.0f),
+                                fmaxf(r1 - fmaxf(ht, hr), 0.0f), fmaxf(r2 - fmaxf(hb, hl), 0.0f),
+                                fmaxf(r3 - fmaxf(hb, hr), 0.0f)),
+                    inv);
+            return fminf(fmaxf(outer - inner, 0.0f), 1.0f);
+        }
+        case TK_SDF_RECT_SHADOW:
+            return shadow_coverage(rect_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1, y1, r0, r1,
+                                               r2, r3),
+                                   inv, sdf_word_f(w, 15), sdf_word_f(w, 16));
+        case TK_SDF_CIRCLE:
+            return coverage_from_sample(circle_sample(x, y, x0, y0, x1), inv);
+        case TK_SDF_CIRCLE_STROKE: {
+            const float he = fmaxf(sdf_word_f(w, 9), 0.0f), radius = fmaxf(x1, 0.0f);
+            const float outer = coverage_from_sample(circle_sample(x, y, x0, y0, radius + he), inv);
+            float inner = 0.0f;
+            if (radius > he) inner = coverage_from_sample(circle_sample(x, y, x0, y0, radius - he), inv);
+            return fminf(fmaxf(outer - inner, 0.0f), 1.0f);
+        }
+        case TK_SDF_CIRCLE_SHADOW:
+            return shadow_coverage(circle_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1), inv,
+                                   sdf_word_f(w, 15), sdf_word_f(w, 16));
+        case TK_SDF_LINE:
+            return coverage_from_sample(line_sample(x, y, x0, y0, x1, y1, r0, r1), inv);
+        case TK_SDF_LINE_SHADOW:
+            return shadow_coverage(line_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1, y1, r0, r1),
+                                   inv, sdf_word_f(w, 15), sdf_word_f(w, 16));
+        default:
+            return 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Coarse tile proofs (coarse/sdf_clip.hlsli:8-56). `tx, ty` is the tile and
+// (ex, ey) the draw's translation.
+// ---------------------------------------------------------------------------
+constexpr float kFullTileSdfInset = 0.5f;
+
+__device__ __forceinline__ bool rounded_corner_covers(float px, float py, float cx, float cy, float ccx, float ccy,
+                                                      float radius, float inset) {
+    const bool in_square = radius > 0.0f && fabsf(px - cx) < radius && fabsf(py - cy) < radius;
+    const float inner = radius - inset;
+    const float dx = px - ccx, dy = py - ccy;
+    return !in_square || (inner > 0.0f && dx * dx + dy * dy <= inner * inner);
+}
+
+// rect_covers_tile: every pixel centre of the tile lies at least `inset`
+// inside the (rounded) rectangle.
+__device__ __forceinline__ bool rect_covers_tile(float rx0, float ry0, float rx1, float ry1, float q0, float q1,
+                                                 float q2, float q3, float ex, float ey, uint32_t tx, uint32_t ty,
+                                                 float inset) {
+    const float lx = fminf(rx0, rx1), ly = fminf(ry0, ry1), ux = fmaxf(rx0, rx1), uy = fmaxf(ry0, ry1);
+    const float tlx = float(tx * TK_TILE_SIZE) + 0.5f - ex, tly = float(ty * TK_TILE_SIZE) + 0.5f - ey;
+    const float tux = tlx + float(TK_TILE_SIZE - 1u), tuy = tly + float(TK_TILE_SIZE - 1u);
+    const float sx = ux - lx, sy = uy - ly;
+    const float need = float(TK_TILE_SIZE - 1u) + 2.0f * inset;
+    if (sx < need || sy < need || tlx < lx + inset || tly < ly + inset || tux > ux - inset || tuy > uy - inset)
+        return false;
+    const float limit = fminf(sx, sy) * 0.5f;
+    const float big = 65536.0f;
+    if (!(fabsf(rx0) <= big && fabsf(ry0) <= big && fabsf(rx1) <= big && fabsf(ry1) <= big)) return false;
+    if (!(fabsf(q0) <= big && fabsf(q1) <= big && fabsf(q2) <= big && fabsf(q3) <= big)) return false;
+    if (!(fabsf(ex) <= big && fabsf(ey) <= big)) return false;
+    q0 = fminf(fmaxf(q0, 0.0f), limit);
+    q1 = fminf(fmaxf(q1, 0.0f), limit);
+    q2 = fminf(fmaxf(q2, 0.0f), limit);
+    q3 = fminf(fmaxf(q3, 0.0f), limit);
+    return rounded_corner_covers(tlx, tly, lx, ly, lx + q0, ly + q0, q0, inset) &&
+           rounded_corner_covers(tux, tly, ux, ly, ux - q1, ly + q1, q1, inset) &&
+           rounded_corner_covers(tlx, tuy, lx, uy, lx + q2, uy - q2, q2, inset) &&
+           rounded_corner_covers(tux, tuy, ux, uy, ux - q3, uy - q3, q3, inset);
+}
+
+// sdf_clip_covers for a RECT record `w` (identity linear part checked by the
+// caller): the rectangle covers the whole tile.
+__device__ __forceinline__ bool sdf_rect_covers(const uint32_t* w, float ex, float ey, uint32_t tx, uint32_t ty) {
+    return rect_covers_tile(sdf_word_f(w, 1), sdf_word_f(w, 2), sdf_word_f(w, 3), sdf_word_f(w, 4), sdf_word_f(w, 5),
+                            sdf_word_f(w, 6), sdf_word_f(w, 7), sdf_word_f(w, 8), ex, ey, tx, ty,
+                            kFullTileSdfInset);
+}
+
+// sdf_stroke_empty for a RECT_STROKE record: the tile lies inside the
+// stroke's hole, at least one pixel from its inner edge.
+__device__ __forceinline__ bool sdf_stroke_empty(const uint32_t* w, float ex, float ey, uint32_t tx, uint32_t ty) {
+    const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
+    const float r0 = sdf_word_f(w, 5), r1 = sdf_word_f(w, 6), r2 = sdf_word_f(w, 7), r3 = sdf_word_f(w, 8);
+    const float s0 = sdf_word_f(w, 9), s1 = sdf_word_f(w, 10), s2 = sdf_word_f(w, 11), s3 = sdf_word_f(w, 12);
+    const float big = 65536.0f;
+    if (!(fabsf(x0) <= big && fabsf(y0) <= big && fabsf(x1) <= big && fabsf(y1) <= big)) return false;
+    if (!(fabsf(r0) <= big && fabsf(r1) <= big && fabsf(r2) <= big && fabsf(r3) <= big)) return false;
+    if (!(fabsf(s0) <= big && fabsf(s1) <= big && fabsf(s2) <= big && fabsf(s3) <= big)) return false;
+    const float ht = fmaxf(s0, 0.0f), hr = fmaxf(s1, 0.0f), hb = fmaxf(s2, 0.0f), hl = fmaxf(s3, 0.0f);
+    const float lx = fminf(x0, x1), ly = fminf(y0, y1), ux = fmaxf(x0, x1), uy = fmaxf(y0, y1);
+    const float ix0 = lx + hl, iy0 = ly + ht, ix1 = ux - hr, iy1 = uy - hb;
+    if (ix0 >= ix1 || iy0 >= iy1) return false;
+    const float c0 = fmaxf(ht, hl), c1 = fmaxf(ht, hr), c2 = fmaxf(hb, hl), c3 = fmaxf(hb, hr);
+    return rect_covers_tile(ix0, iy0, ix1, iy1, fmaxf(r0 - c0, 0.0f), fmaxf(r1 - c1, 0.0f), fmaxf(r2 - c2, 0.0f),
+                            fmaxf(r3 - c3, 0.0f), ex, ey, tx, ty, 1.0f);
+}
+
+}  // namespace tkd
