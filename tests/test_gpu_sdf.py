@@ -148,6 +148,20 @@ def test_gpu_sdf_batch_matches_serial(renderer):
         r.close()
 
 
+def small_shapes(c, rng, ox, oy):
+    """One of each SDF kind, within about 40 pixels of (ox, oy)."""
+    b = lambda: tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.4, 1)))
+    r = lambda lo, hi: float(rng.uniform(lo, hi))
+    c.push_rect(ox, oy, ox + r(5, 30), oy + r(5, 30), b(), radius=r(0, 6))
+    c.push_rect_stroke(ox + 3, oy + 3, ox + r(10, 35), oy + r(10, 35), r(0.5, 4), b(), radius=(1, 2, 3, 4))
+    c.push_circle(ox + r(5, 30), oy + r(5, 30), r(2, 10), b())
+    c.push_circle_stroke(ox + 20, oy + 20, r(5, 15), r(0.5, 3), b())
+    c.push_line(ox, oy + r(0, 30), ox + r(5, 35), oy + r(0, 30), r(0.5, 4), b(), cap=int(rng.integers(0, 3)))
+    c.push_rect_shadow(ox + 5, oy + 5, ox + 25, oy + 20, b(), offset=(2, 3), expand=r(0, 3), intensity=0.6)
+    c.push_circle_shadow(ox + 15, oy + 15, r(3, 8), b(), expand=r(0, 2), intensity=0.8)
+    c.push_line_shadow(ox, oy, ox + 30, oy + 25, r(1, 3), b(), offset=(1, 1), expand=1.5, cap=N.CAP_ROUND)
+
+
 def test_gpu_sdf_incremental_frames_equal_full_frames(renderer):
     W, H = 384, 256
     full = tk.NativeRenderer(0)
@@ -155,20 +169,21 @@ def test_gpu_sdf_incremental_frames_equal_full_frames(renderer):
         rs = tk.RetainedScene(W, H)
         rs.set_clear_color(0xFFFFFFFF)
         nodes = []
-        for k in range(6):
+        for k in range(8):
             node = tk.Canvas(W, H)
             node.keep_commands()
-            random_shapes(node, np.random.default_rng(200 + k), 12, W // 2, H // 2)
+            small_shapes(node, np.random.default_rng(200 + k), 0.0, 0.0)
             nodes.append(node)
-            rs.insert(k + 1, node, (1, 0, 0, 1, 30.0 * k, 10.0 * k))
+            rs.insert(k + 1, node, (1, 0, 0, 1, 40.0 * k + 10.5, 25.0 * (k % 4) + 8.25))
         renderer.render_retained(rs)
-        for step, mutate in enumerate([lambda: rs.set_transform(2, (1, 0, 0, 1, 77.5, 31.25)),
+        for step, mutate in enumerate([lambda: rs.set_transform(2, (1, 0, 0, 1, 177.5, 131.25)),
                                        lambda: rs.remove(4),
                                        lambda: rs.move_before(6, 1),
-                                       lambda: rs.replace(3, nodes[0])]):
+                                       lambda: rs.replace(3, nodes[0]),
+                                       lambda: None]):
             mutate()
             st = renderer.render_retained(rs)
-            assert st["full_redraw"] == 0, (step, st)
+            assert st["full_redraw"] == 0 and st["dirty_tiles"] < st["total_tiles"], (step, st)
             img = renderer.readback().view(np.uint8).reshape(H, W, 4)
             want = full.render_to_image(rs.materialize()[0])
             assert np.array_equal(img, want), step
