@@ -223,7 +223,25 @@ __device__ uint32_t occluded_prefix_g(const tk_ptcl_record* ptcl, uint64_t start
     return 0u;
 }
 
-template <bool EMIT>
+// draw_particle for an SDF draw in tile (tx, ty) (coarse/emit_draw.hlsli:22-30):
+// 0 inside a rect stroke's hole (sdf_stroke_empty), TK_PTCL_COLOR for a solid
+// rect that covers the tile (full_tile_solid), else TK_PTCL_SDF. Out of line
+// so that the walk over path candidates keeps its registers.
+static __device__ __noinline__ uint32_t sdf_particle(const tk_draw_record* draws, const uint32_t* sdf, uint32_t draw,
+                                                     uint32_t word, uint32_t bits, uint32_t meta, uint32_t tx,
+                                                     uint32_t ty) {
+    const uint32_t kind = bits & 255u;
+    const bool proof = (bits & kSdfPlain) && (bits & kSdfIdentity) &&
+                       (kind == TK_SDF_RECT_STROKE || (kind == TK_SDF_RECT && (meta & kMetaSolid)));
+    if (!proof) return TK_PTCL_SDF;
+    const float ex = draws[draw].transform.e, ey = draws[draw].transform.f;
+    if (kind == TK_SDF_RECT_STROKE) return sdf_stroke_empty(sdf + word, ex, ey, tx, ty) ? 0u : TK_PTCL_SDF;
+    return sdf_rect_covers(sdf + word, ex, ey, tx, ty) ? TK_PTCL_COLOR : TK_PTCL_SDF;
+}
+
+// SDF: whether the scene has SDF records; path-only scenes run the instance
+// without the SDF candidate handling.
+template <bool EMIT, bool SDF>
 __global__ void __launch_bounds__(kCoarseThreads)
     k_coarse(Ctx c, const uint32_t* __restrict__ bin_lists, const uint32_t* __restrict__ bin_counts, uint32_t draw_n,
              uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
@@ -305,10 +323,13 @@ __global__ void __launch_bounds__(kCoarseThreads)
             }
             bool color_candidate = false;
             info.color = di;
-            // nontransparent_solid (coarse/paint.hlsli:13-17)
-            const bool solid = d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID &&
-                               brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
-            const bool has_sdf = d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX;
+            // nontransparent_solid (coarse/paint.hlsli:13-17), read only for the
+            // draws that can use it
+            auto solid_paint = [&]() {
+                return d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID &&
+                       brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
+            };
+            const bool has_sdf = SDF && (d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX);
             uint32_t sdf_bits = 0u;
             if (has_sdf) {
                 // draw_has_sdf (shared/draw.hlsli:31): only brush draws give a particle
@@ -320,6 +341,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                                    d.transform.d == 1.0f;
                 info.py = (kind & 255u) | (plain ? kSdfPlain : 0u) | (ident ? kSdfIdentity : 0u);
                 if (d.tag == TK_DRAW_BRUSH) sdf_bits |= kMetaSdf;
+                const bool solid = solid_paint();
                 if (solid) {
                     color_candidate = true;
                     info.color = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
@@ -327,13 +349,14 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 // solid_supported_sdf (coarse/paint.hlsli:21-25)
                 if (solid && plain && kind == TK_SDF_RECT) sdf_bits |= kMetaSdfSolidClass;
             } else if (d.tag == TK_DRAW_BRUSH && d.solid_rect != 0u && d.transform.b == 0.0f &&
-                       d.transform.c == 0.0f && solid) {
+                       d.transform.c == 0.0f && solid_paint()) {
                 color_candidate = true;
                 info.color = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
             }
             if (d.tag == TK_DRAW_CLIP) info.color = 0u;
             uint32_t batch = batch_ids[di] - batch0;
-            info.meta = (d.tag & 7u) | ((d.fill_rule & 1u) << 3) | (valid_path ? kMetaPath : 0u) |
+            const uint32_t rule = has_sdf ? 0u : (d.fill_rule & 1u);  // SDF particles carry rule 0
+            info.meta = (d.tag & 7u) | (rule << 3) | (valid_path ? kMetaPath : 0u) |
                         (color_candidate ? kMetaSolid : 0u) | sdf_bits | (batch << 8);
             s_d[threadIdx.x] = info;
         }
@@ -357,7 +380,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 const DrawInfo& d = s_d[k];
                 if (!(tx >= (d.tx & 0xFFFFu) && tx < (d.tx >> 16) && ty >= (d.ty & 0xFFFFu) && ty < (d.ty >> 16))) continue;
                 const uint32_t meta = d.meta;
-                if (meta & kMetaSdf) {
+                if (SDF && (meta & kMetaSdf)) {
                     sdf_hit |= 1u << q;
                     continue;
                 }
@@ -376,28 +399,19 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 if (!((hit | sdf_hit) & (1u << q))) continue;
                 const DrawInfo& d = s_d[k0 + q];
                 const uint32_t meta = d.meta, tag = meta & 7u;
-                const tk_segment_range r = rr[q];
-                const uint32_t w = ww[q];
-                uint32_t sdf_tag = 0u;  // the SDF draw's particle: TK_PTCL_SDF or TK_PTCL_COLOR
-                if (sdf_hit & (1u << q)) {
-                    // draw_particle for SDF draws (coarse/emit_draw.hlsli:22-30): no
-                    // particle inside a rect stroke's hole (sdf_stroke_empty); a solid
-                    // rect covering the tile becomes a colour (full_tile_solid)
-                    const uint32_t kind = d.py & 255u;
-                    const bool proof = (d.py & kSdfPlain) && (d.py & kSdfIdentity) &&
-                                       (kind == TK_SDF_RECT_STROKE || (kind == TK_SDF_RECT && (meta & kMetaSolid)));
-                    sdf_tag = TK_PTCL_SDF;
-                    if (proof) {
-                        const tk_draw_record& dr = c.draws[d.draw];
-                        const float ex = dr.transform.e, ey = dr.transform.f;
-                        if (kind == TK_SDF_RECT_STROKE) {
-                            if (sdf_stroke_empty(c.sdf + d.px, ex, ey, tx, ty)) continue;
-                        } else if (sdf_rect_covers(c.sdf + d.px, ex, ey, tx, ty)) {
-                            sdf_tag = TK_PTCL_COLOR;
-                        }
-                    }
-                } else if (r.start == r.end && w == 0u) {
-                    continue;
+                tk_segment_range r = rr[q];
+                const uint32_t w = ww[q];  // 0 for SDF draws
+                uint32_t ptag = TK_PTCL_FILL;
+                if (SDF && (sdf_hit & (1u << q))) {
+                    ptag = sdf_particle(c.draws, c.sdf, d.draw, d.px, d.py, meta, tx, ty);
+                    if (ptag == 0u) continue;
+                    // an SDF particle names its draw in segment_start (coarse/emit_draw.hlsli:28)
+                    r = ptag == TK_PTCL_SDF ? tk_segment_range{d.draw, 0u} : tk_segment_range{0u, 0u};
+                } else {
+                    if (r.start == r.end && w == 0u) continue;
+                    if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
+                    else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
+                    else if ((meta & kMetaSolid) && r.start == r.end) ptag = TK_PTCL_COLOR;
                 }
                 uint32_t batch = meta >> 8;
                 if (batch != cur) {
@@ -413,28 +427,16 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     }
                 }
                 if (rejected) continue;
-                if (sdf_tag) {
-                    if (EMIT) {
-                        // particle_class_flags (coarse/paint.hlsli:35-40)
-                        const bool color = sdf_tag == TK_PTCL_COLOR;
-                        flags |= color ? kChunkClassColor : ((meta & kMetaSdfSolidClass) ? kChunkClassSdf : kChunkClassOther);
-                        if (wrappers == 0u && color && (d.color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
-                        if (color) store_ptcl(ptcl, cap, at++, TK_PTCL_COLOR, 0u, 0u, 0u, 0u, d.color, error);
-                        else store_ptcl(ptcl, cap, at++, TK_PTCL_SDF, 0u, 0u, d.draw, 0u, d.draw, error);
-                    }
-                    ++nb;
-                    continue;
-                }
-                uint32_t ptag = TK_PTCL_FILL;
-                if (tag == TK_DRAW_CLIP) ptag = TK_PTCL_BEGIN_CLIP;
-                else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
-                else if ((meta & kMetaSolid) && r.start == r.end) ptag = TK_PTCL_COLOR;
                 if (EMIT) {
-                    flags |= ptag == TK_PTCL_COLOR ? kChunkClassColor : kChunkClassOther;
+                    // particle_class_flags (coarse/paint.hlsli:35-40)
+                    uint32_t cls = kChunkClassOther;
+                    if (ptag == TK_PTCL_COLOR) cls = kChunkClassColor;
+                    else if (ptag == TK_PTCL_SDF && (meta & kMetaSdfSolidClass)) cls = kChunkClassSdf;
+                    flags |= cls;
                     uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
                     if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
                     store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
-                    if (ptag != TK_PTCL_COLOR) {
+                    if (ptag != TK_PTCL_COLOR && ptag != TK_PTCL_SDF) {
                         fills += 1;
                         visits += r.end - r.start;
                     }
@@ -555,14 +557,12 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
           s.ranges, s.tw, s.th};
     const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
     if (nbins == 0) return;
-    if (emit)
-        k_coarse<true><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
-                                                         p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                         p.stats, s.error, p.scenes, p.bin_scene, p.tile_active);
-    else
-        k_coarse<false><<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
-                                                          p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity,
-                                                          p.stats, s.error, p.scenes, p.bin_scene, p.tile_active);
+    const bool sdf = s.sdf_words != 0;
+    auto kernel = emit ? (sdf ? k_coarse<true, true> : k_coarse<true, false>)
+                       : (sdf ? k_coarse<false, true> : k_coarse<false, false>);
+    kernel<<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
+                                                      p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity, p.stats,
+                                                      s.error, p.scenes, p.bin_scene, p.tile_active);
 }
 
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {

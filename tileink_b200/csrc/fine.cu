@@ -355,6 +355,18 @@ __device__ __forceinline__ float staged_coverage(const FineSmem& S, uint32_t i, 
     return rb.x + running + partial;
 }
 
+// Analytic coverage of the SDF record `w` at the centre of pixel (gx, gy)
+// mapped to draw space by the draw's inverse transform (affine_record_point,
+// shared/affine.hlsli:14-18). Inlined: an out-of-line call costs the record
+// loop more (register saves around the call) than the shape switch does.
+static __device__ __forceinline__ float sdf_coverage_at(const uint32_t* w, const tk_affine* t, uint32_t gx, uint32_t gy) {
+    const tk_affine inv{__ldg(&t->a), __ldg(&t->b), __ldg(&t->c), __ldg(&t->d), __ldg(&t->e), __ldg(&t->f)};
+    const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
+    const float ux = __fmaf_rn(inv.a, sx, __fmaf_rn(inv.c, sy, inv.e));
+    const float uy = __fmaf_rn(inv.b, sx, __fmaf_rn(inv.d, sy, inv.f));
+    return sdf_coverage(w, ux, uy, inv);
+}
+
 // Paints a fill's masked coverage over px (the brush branch of
 // fine/interpreter.hlsli's fill handling, fine/draw.hlsli:16-21).
 __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, uint32_t i, uint32_t masked,
@@ -376,6 +388,10 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
     }
 }
 
+// SDF: whether the scene has SDF records. Path-only scenes run the instance
+// without the PTCL_SDF branch, which costs the record loop about 3% even when
+// it is never taken.
+template <bool SDF>
 __global__ void __launch_bounds__(kFineThreads, 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
@@ -441,9 +457,9 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 if (a.x == TK_PTCL_FILL && n != 0u) cls = kClsFill;  // row sums staged below
             }
             S.nseg[tid] = n;
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || a.x == TK_PTCL_SDF) {
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (SDF && a.x == TK_PTCL_SDF)) {
                 const PaintInfo* pi = paints + c.y;
-                if (a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
+                if (SDF && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
                 const uint32_t paint = __ldg(&pi->paint);
                 if (paint != kGradient) {
                     S.paint[tid] = paint;
@@ -584,18 +600,10 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                         px = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(px), a));
                     }
                 }
-            } else if (tag == TK_PTCL_SDF) {
-                // PTCL_SDF (fine/interpreter.hlsli:70-84): analytic coverage of the
-                // draw's SDF record at the pixel centre mapped to draw space
-                // (affine_record_point, shared/affine.hlsli:14-18)
+            } else if (SDF && tag == TK_PTCL_SDF) {
+                // PTCL_SDF (fine/interpreter.hlsli:70-84)
                 if (clip != 0u) {
-                    const tk_affine* t = &draws[qb.y].inverse_transform;
-                    const tk_affine inv{__ldg(&t->a), __ldg(&t->b), __ldg(&t->c),
-                                        __ldg(&t->d), __ldg(&t->e), __ldg(&t->f)};
-                    const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
-                    const float ux = __fmaf_rn(inv.a, sx, __fmaf_rn(inv.c, sy, inv.e));
-                    const float uy = __fmaf_rn(inv.b, sx, __fmaf_rn(inv.d, sy, inv.f));
-                    const float cov = sdf_coverage(sdf + S.umode[i], ux, uy, inv);
+                    const float cov = sdf_coverage_at(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy);
                     const uint32_t masked = combine_alpha(coverage_to_u8(cov), clip);
                     if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
                 }
@@ -683,12 +691,14 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     if (T == 0) return;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_fine, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        cudaFuncSetAttribute(k_fine<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        cudaFuncSetAttribute(k_fine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
         configured = true;
     }
-    k_fine<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
-                                                      s.draws, s.sdf, s.segment_capacity, target, s.width, s.height, s.tw, s.error,
-                                                      p.scenes, p.tile_scene, p.tile_list);
+    auto kernel = s.sdf_words ? k_fine<true> : k_fine<false>;
+    kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
+                                                      s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,
+                                                      s.tw, s.error, p.scenes, p.tile_scene, p.tile_list);
 }
 
 }  // namespace tk
