@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--diff-steps", type=int, default=10, help="timed fwd+bwd steps of the blur-group workload (0: skip)")
     p.add_argument("--batch-scenes", type=int, default=512, help="scenes of the batched-mode leg (0: skip)")
     p.add_argument("--incremental-steps", type=int, default=10, help="frames of the incremental leg (0: skip)")
+    p.add_argument("--sdf-steps", type=int, default=10, help="frames of the SDF-shape leg (0: skip)")
     return p.parse_args()
 
 
@@ -236,6 +237,98 @@ def incremental_timing(r, size, steps):
             "timing": "host wall clock per frame, synchronized"}
 
 
+def sdf_scene(size, n, seed):
+    """n SDF shapes on a size^2 canvas, clustered like the path workload (200
+    Gaussian centres, sigma 300 px): rects (half rounded), rect strokes,
+    circles, circle strokes, lines with butt/square/round caps and rect,
+    circle and line shadows, 4-160 px; paint 50% opaque solid, 25%
+    translucent solid, 25% linear/radial gradients."""
+    import tileink_b200 as tk
+    from tileink_b200 import _native as N
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(size, size)
+    c.set_clear_color(0xFFFFFFFF)
+    centres = rng.uniform(0, size, (200, 2))
+    for k in range(n):
+        x, y = centres[rng.integers(200)] + rng.normal(0, 300, 2)
+        w, h = rng.uniform(4, 160, 2)
+        u = rng.uniform()
+        if u < 0.5:
+            b = tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0)
+        elif u < 0.75:
+            b = tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.2, 0.9)))
+        else:
+            stops = [(0.0, (*rng.uniform(0, 1, 3), 1.0)), (1.0, (*rng.uniform(0, 1, 3), float(rng.uniform(0.3, 1))))]
+            b = (tk.Brush.linear((x, y), (x + w, y + h), stops) if rng.uniform() < 0.5
+                 else tk.Brush.radial((x, y), 0.0, (x, y), float(max(w, h)), stops))
+        kind = k % 9
+        if kind in (0, 1):
+            c.push_rect(x, y, x + w, y + h, b, radius=float(rng.uniform(0, 20)) if kind else 0.0)
+        elif kind == 2:
+            c.push_rect_stroke(x, y, x + w, y + h, float(rng.uniform(1, 8)), b, radius=float(rng.uniform(0, 12)))
+        elif kind == 3:
+            c.push_circle(x, y, w / 2, b)
+        elif kind == 4:
+            c.push_circle_stroke(x, y, w / 2, float(rng.uniform(1, 6)), b)
+        elif kind == 5:
+            c.push_line(x, y, x + rng.uniform(-w, w), y + rng.uniform(-h, h), float(rng.uniform(1, 8)), b,
+                        cap=int(rng.integers(0, 3)))
+        elif kind == 6:
+            c.push_rect_shadow(x, y, x + w, y + h, b, offset=(4, 4), expand=float(rng.uniform(0, 8)),
+                               intensity=0.5, radius=8.0)
+        elif kind == 7:
+            c.push_circle_shadow(x, y, w / 2, b, offset=(3, 3), expand=float(rng.uniform(0, 6)), intensity=0.6)
+        else:
+            c.push_line_shadow(x, y, x + w, y + h, float(rng.uniform(1, 6)), b, offset=(2, 2), expand=3.0,
+                               intensity=0.5, cap=N.CAP_ROUND)
+    return c
+
+
+def sdf_timing(r, size, steps, cpu):
+    """Frames of an SDF-shape scene (PTCL_SDF coverage in fine, full-tile
+    colour and hollow-stroke proofs in coarse), device stage times by CUDA
+    events; and the oracle on 1/4 of the shapes, scaled, as its CPU
+    baseline."""
+    from tileink_b200 import _native as N
+    n = 50000
+    size = size or 4096
+    c = sdf_scene(size, n, SEED + 7)
+    r.upload(c)
+    r.set_timing(True)
+    for _ in range(3):
+        r.render()
+    r.synchronize()
+    acc = {}
+    for _ in range(steps):
+        r.render()
+        r.synchronize()
+        for k, v in r.stage_times().items():
+            acc[k] = acc.get(k, 0.0) + v / steps
+    frame_ms = sum(acc.values())
+    ptcl = r.debug(N.STAGE_PTCL, 0)
+    tags = ptcl["tag"]
+    kinds = ptcl["color"][tags == N.PTCL_BATCH_BEGIN] & 7
+    line = {"workload": f"{size}x{size} canvas, {n} SDF shapes of every kind (rects, rounded rects, rect strokes, "
+                        "circles, circle strokes, lines, rect/circle/line shadows), 200 Gaussian clusters "
+                        "sigma 300 px, 50% opaque / 25% translucent solid / 25% gradient paint",
+            "frames_per_s": 1e3 / frame_ms, "ms_per_frame": frame_ms, "stage_ms": acc, "steps": steps,
+            "sdf_records": int((tags == N.PTCL_SDF).sum()), "color_records": int((tags == N.PTCL_COLOR).sum()),
+            "tile_kinds": {name: int((kinds == k).sum()) for k, name in
+                           ((0, "interpreter"), (1, "empty"), (2, "color"), (3, "sdf"), (4, "mixed"))},
+            "timing": "device, CUDA events per stage, summed"}
+    if cpu:
+        import oracle
+        div = 4  # the oracle renders SDF shapes faster than paths: a larger sample
+        small = sdf_scene(size, n // div, SEED + 7)
+        t0 = time.perf_counter()
+        run = oracle.OracleRun(small.scene_desc(), threads=os.cpu_count() or 1)
+        dt = time.perf_counter() - t0
+        del run
+        line["cpu_baseline"] = {"frames_per_s": 1.0 / (dt * div), "cores": os.cpu_count() or 1,
+                                "kind": "port", "sample": f"{n // div} shapes (1/{div}), {dt:.2f} s, scaled x{div}"}
+    return line
+
+
 def cpu_baseline(size, paths):
     """The oracle (CPU restatement of the reference path) on all host cores,
     on 1/16 of the workload's paths over the same canvas; the frame time is
@@ -400,6 +493,9 @@ def main():
     inc_line = None
     if rank == 0 and args.incremental_steps > 0:
         inc_line = incremental_timing(r, args.size, args.incremental_steps)
+    sdf_line = None
+    if rank == 0 and args.sdf_steps > 0:
+        sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline)
     del ps_flat, flat_canvas
     bytes_out = out.nbytes
 
@@ -488,6 +584,7 @@ def main():
             "fwd_bwd": diff_line,
             "batched": batch_line,
             "incremental": inc_line,
+            "sdf": sdf_line,
             "scene_generation_s": gen_s,
         }
         print(json.dumps(line), flush=True)

@@ -600,18 +600,23 @@ float sdf_cov(const SdfS& s, const tk_affine& inv) {
     return clampf(0.5f - s.dist / fp, 0.0f, 1.0f);
 }
 // The library evaluates the shadow falloff exp(x), x <= 0, in double as
-// 2^k * e^r (k nearest to x / ln 2, e^r by its degree-13 Taylor series) with
-// only exactly rounded operations; restated so that the two agree bit for
-// bit. Its distance to exp is checked in the tests.
+// 2^k * e^r (k nearest to x / ln 2, e^r by its degree-12 Taylor polynomial in
+// Horner form) with only exactly rounded multiplies and adds; restated so
+// that the two agree bit for bit. Its distance to exp is checked in the tests.
 float exp_nonpos(float x) {
     if (!(x <= 0.0f)) return x != x ? x : 1.0f;
     if (x < -104.0f) return 0.0f;
-    const double ln2 = 0.69314718055994530942;
+    const double ln2 = 0.69314718055994530942, inv_ln2 = 1.4426950408889634074;
     double xd = double(x);
-    double k = std::floor(xd / ln2 + 0.5);
+    double k = std::floor(xd * inv_ln2 + 0.5);
     double r = xd - k * ln2;
-    double p = 1.0;
-    for (int n = 13; n >= 1; --n) p = 1.0 + r * p / double(n);
+    const double c[11] = {1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0, 1.0 / 362880.0, 1.0 / 40320.0,
+                          1.0 / 5040.0,      1.0 / 720.0,       1.0 / 120.0,     1.0 / 24.0,     1.0 / 6.0,
+                          0.5};
+    double p = c[0];
+    for (int n = 1; n < 11; ++n) p = p * r + c[n];
+    p = p * r + 1.0;
+    p = p * r + 1.0;
     int64_t bits = int64_t(1023 + int64_t(k)) << 52;
     double scale;
     std::memcpy(&scale, &bits, sizeof(scale));

@@ -142,20 +142,28 @@ __device__ __forceinline__ float coverage_from_sample(const SdfSample& s, const 
 }
 
 // exp(x) for x <= 0 (positive x is not used and gives 1): evaluated in double
-// as 2^k * e^r with k the nearest integer to x / ln 2 and |r| <= ln 2 / 2,
-// e^r by its Taylor series to degree 13 (truncation below 2^-57), 2^k
-// assembled from its exponent bits. Only exactly rounded double operations are
-// used, so host and device agree bit for bit; the float result is within half
-// an ulp of exp(x) over the tested range.
+// as 2^k * e^r with k the nearest integer to x / ln 2 (|r| <= ln 2 / 2 plus
+// rounding), e^r by its Taylor polynomial of degree 12 in Horner form
+// (truncation below 2e-16), 2^k assembled from its exponent bits. Only
+// exactly rounded double multiplies and adds are used, so host and device
+// agree bit for bit; the float result is within half an ulp of exp(x) over the
+// tested range.
 __device__ __forceinline__ float sdf_exp_nonpos(float x) {
     if (!(x <= 0.0f)) return x != x ? x : 1.0f;
     if (x < -104.0f) return 0.0f;
-    const double ln2 = 0.69314718055994530942;
+    const double ln2 = 0.69314718055994530942, inv_ln2 = 1.4426950408889634074;
     const double xd = double(x);
-    const double k = floor(xd / ln2 + 0.5);
+    const double k = floor(xd * inv_ln2 + 0.5);
     const double r = xd - k * ln2;
-    double p = 1.0;
-    for (int n = 13; n >= 1; --n) p = 1.0 + r * p / double(n);
+    // 1/n! for n = 12 .. 2
+    const double c[11] = {1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0, 1.0 / 362880.0, 1.0 / 40320.0,
+                          1.0 / 5040.0,      1.0 / 720.0,       1.0 / 120.0,     1.0 / 24.0,     1.0 / 6.0,
+                          0.5};
+    double p = c[0];
+#pragma unroll
+    for (int n = 1; n < 11; ++n) p = p * r + c[n];
+    p = p * r + 1.0;
+    p = p * r + 1.0;
     const double scale = __longlong_as_double((long long)(1023 + (long long)k) << 52);
     return float(p * scale);
 }
@@ -171,56 +179,61 @@ __device__ __forceinline__ float shadow_coverage(const SdfSample& s, const tk_af
 __device__ __forceinline__ float sdf_word_f(const uint32_t* w, uint32_t i) { return __uint_as_float(__ldg(w + i)); }
 
 // sdf_coverage_from_blob (shared/sdf/coverage.hlsli:13-236) for the record at
-// `w` (TK_SDF_RECORD_WORDS words), sampled at local point (x, y).
+// `w` (TK_SDF_RECORD_WORDS words), sampled at local point (x, y). The kinds
+// share one copy of each sampler: a shape (rect, circle or line) sampled in
+// one pass, or two for strokes (outer minus inner coverage), with shadows
+// shifted by their offset and weighted by their falloff. The operations and
+// their order per kind are those of the reference's per-kind branches; the
+// sharing only keeps the code small enough for the instruction cache.
 __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float y, const tk_affine& inv) {
     const uint32_t kind = __ldg(w);
+    const bool rect = kind == TK_SDF_RECT || kind == TK_SDF_RECT_STROKE || kind == TK_SDF_RECT_SHADOW;
+    const bool circle = kind == TK_SDF_CIRCLE || kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_CIRCLE_SHADOW;
+    const bool line = kind == TK_SDF_LINE || kind == TK_SDF_LINE_SHADOW;
+    if (!(rect || circle || line)) return 0.0f;
+    const bool shadow = kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW || kind == TK_SDF_LINE_SHADOW;
+    const bool stroke = kind == TK_SDF_RECT_STROKE || kind == TK_SDF_CIRCLE_STROKE;
     const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
     const float r0 = sdf_word_f(w, 5), r1 = sdf_word_f(w, 6), r2 = sdf_word_f(w, 7), r3 = sdf_word_f(w, 8);
-    switch (kind) {
-        case TK_SDF_RECT:
-            return coverage_from_sample(rect_sample(x, y, x0, y0, x1, y1, r0, r1, r2, r3), inv);
-        case TK_SDF_RECT_STROKE: {
-            const float ht = fmaxf(sdf_word_f(w, 9), 0.0f), hr = fmaxf(sdf_word_f(w, 10), 0.0f);
-            const float hb = fmaxf(sdf_word_f(w, 11), 0.0f), hl = fmaxf(sdf_word_f(w, 12), 0.0f);
-            const float rx0 = fminf(x0, x1), ry0 = fminf(y0, y1), rx1 = fmaxf(x0, x1), ry1 = fmaxf(y0, y1);
-            const float outer = coverage_from_sample(
-                rect_sample(x, y, rx0 - hl, ry0 - ht, rx1 + hr, ry1 + hb, r0 + fmaxf(ht, hl), r1 + fmaxf(ht, hr),
-                            r2 + fmaxf(hb, hl), r3 + fmaxf(hb, hr)),
-                inv);
-            const float ix0 = rx0 + hl, iy0 = ry0 + ht, ix1 = rx1 - hr, iy1 = ry1 - hb;
-            float inner = 0.0f;
-            if (ix0 < ix1 && iy0 < iy1)
-                inner = coverage_from_sample(
-                    rect_sample(x, y, ix0, iy0, ix1, iy1, fmaxf(r0 - fmaxf(ht, hl), 0.0f),
-                                fmaxf(r1 - fmaxf(ht, hr), 0.0f), fmaxf(r2 - fmaxf(hb, hl), 0.0f),
-                                fmaxf(r3 - fmaxf(hb, hr), 0.0f)),
-                    inv);
-            return fminf(fmaxf(outer - inner, 0.0f), 1.0f);
-        }
-        case TK_SDF_RECT_SHADOW:
-            return shadow_coverage(rect_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1, y1, r0, r1,
-                                               r2, r3),
-                                   inv, sdf_word_f(w, 15), sdf_word_f(w, 16));
-        case TK_SDF_CIRCLE:
-            return coverage_from_sample(circle_sample(x, y, x0, y0, x1), inv);
-        case TK_SDF_CIRCLE_STROKE: {
-            const float he = fmaxf(sdf_word_f(w, 9), 0.0f), radius = fmaxf(x1, 0.0f);
-            const float outer = coverage_from_sample(circle_sample(x, y, x0, y0, radius + he), inv);
-            float inner = 0.0f;
-            if (radius > he) inner = coverage_from_sample(circle_sample(x, y, x0, y0, radius - he), inv);
-            return fminf(fmaxf(outer - inner, 0.0f), 1.0f);
-        }
-        case TK_SDF_CIRCLE_SHADOW:
-            return shadow_coverage(circle_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1), inv,
-                                   sdf_word_f(w, 15), sdf_word_f(w, 16));
-        case TK_SDF_LINE:
-            return coverage_from_sample(line_sample(x, y, x0, y0, x1, y1, r0, r1), inv);
-        case TK_SDF_LINE_SHADOW:
-            return shadow_coverage(line_sample(x - sdf_word_f(w, 13), y - sdf_word_f(w, 14), x0, y0, x1, y1, r0, r1),
-                                   inv, sdf_word_f(w, 15), sdf_word_f(w, 16));
-        default:
-            return 0.0f;
+    float px = x, py = y, expand = 0.0f, intensity = 0.0f;
+    if (shadow) {
+        px = x - sdf_word_f(w, 13);
+        py = y - sdf_word_f(w, 14);
+        expand = sdf_word_f(w, 15);
+        intensity = sdf_word_f(w, 16);
     }
+    // pass 0: the shape (a stroke's outer edge); pass 1: a stroke's inner edge
+    float o[8] = {x0, y0, x1, y1, r0, r1, r2, r3}, in[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool inner = false;
+    if (kind == TK_SDF_RECT_STROKE) {
+        const float ht = fmaxf(sdf_word_f(w, 9), 0.0f), hr = fmaxf(sdf_word_f(w, 10), 0.0f);
+        const float hb = fmaxf(sdf_word_f(w, 11), 0.0f), hl = fmaxf(sdf_word_f(w, 12), 0.0f);
+        const float rx0 = fminf(x0, x1), ry0 = fminf(y0, y1), rx1 = fmaxf(x0, x1), ry1 = fmaxf(y0, y1);
+        const float c0 = fmaxf(ht, hl), c1 = fmaxf(ht, hr), c2 = fmaxf(hb, hl), c3 = fmaxf(hb, hr);
+        o[0] = rx0 - hl; o[1] = ry0 - ht; o[2] = rx1 + hr; o[3] = ry1 + hb;
+        o[4] = r0 + c0; o[5] = r1 + c1; o[6] = r2 + c2; o[7] = r3 + c3;
+        in[0] = rx0 + hl; in[1] = ry0 + ht; in[2] = rx1 - hr; in[3] = ry1 - hb;
+        in[4] = fmaxf(r0 - c0, 0.0f); in[5] = fmaxf(r1 - c1, 0.0f);
+        in[6] = fmaxf(r2 - c2, 0.0f); in[7] = fmaxf(r3 - c3, 0.0f);
+        inner = in[0] < in[2] && in[1] < in[3];
+    } else if (kind == TK_SDF_CIRCLE_STROKE) {
+        const float he = fmaxf(sdf_word_f(w, 9), 0.0f), radius = fmaxf(x1, 0.0f);
+        o[2] = radius + he;
+        in[0] = x0; in[1] = y0; in[2] = radius - he;
+        inner = radius > he;
+    }
+    float cov[2] = {0.0f, 0.0f};
+    for (int pass = 0; pass < (inner ? 2 : 1); ++pass) {
+        float q[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) q[k] = pass ? in[k] : o[k];
+        SdfSample s;
+        if (rect) s = rect_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+        else if (circle) s = circle_sample(px, py, q[0], q[1], q[2]);
+        else s = line_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5]);
+        cov[pass] = shadow ? shadow_coverage(s, inv, expand, intensity) : coverage_from_sample(s, inv);
+    }
+    return stroke ? fminf(fmaxf(cov[0] - cov[1], 0.0f), 1.0f) : cov[0];
 }
 
 // ---------------------------------------------------------------------------
