@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--batch-scenes", type=int, default=512, help="scenes of the batched-mode leg (0: skip)")
     p.add_argument("--incremental-steps", type=int, default=10, help="frames of the incremental leg (0: skip)")
     p.add_argument("--sdf-steps", type=int, default=10, help="frames of the SDF-shape leg (0: skip)")
+    p.add_argument("--sdf-shapes", type=int, default=50000, help="shapes of the SDF-shape leg")
+    p.add_argument("--sdf-only", action="store_true",
+                   help="run only the SDF-shape leg (rank 0, one GPU) and print its line (profiling runs)")
     return p.parse_args()
 
 
@@ -284,13 +287,12 @@ def sdf_scene(size, n, seed):
     return c
 
 
-def sdf_timing(r, size, steps, cpu):
+def sdf_timing(r, size, steps, cpu, n=50000):
     """Frames of an SDF-shape scene (PTCL_SDF coverage in fine, full-tile
     colour and hollow-stroke proofs in coarse), device stage times by CUDA
     events; and the oracle on 1/4 of the shapes, scaled, as its CPU
     baseline."""
     from tileink_b200 import _native as N
-    n = 50000
     size = size or 4096
     c = sdf_scene(size, n, SEED + 7)
     r.upload(c)
@@ -413,6 +415,12 @@ def main():
 
     import tileink_b200 as tk
 
+    if args.sdf_only:
+        r = tk.NativeRenderer(0)
+        print(json.dumps({"sdf": sdf_timing(r, args.size, max(args.sdf_steps, 1), False, args.sdf_shapes)}),
+              flush=True)
+        r.close()
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -495,7 +503,7 @@ def main():
         inc_line = incremental_timing(r, args.size, args.incremental_steps)
     sdf_line = None
     if rank == 0 and args.sdf_steps > 0:
-        sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline)
+        sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline, args.sdf_shapes)
     del ps_flat, flat_canvas
     bytes_out = out.nbytes
 

@@ -57,6 +57,8 @@ def lib() -> C.CDLL:
         l.or_sdf_coverage.argtypes = [P, F32, F32, P]
         l.or_exp_nonpos.restype = F32
         l.or_exp_nonpos.argtypes = [F32]
+        l.or_interpret_sdf_draws.restype = I32
+        l.or_interpret_sdf_draws.argtypes = [P, P]
         l.or_diff_loss.restype = C.c_double
         l.or_diff_loss.argtypes = [U32, U32, U32, U64, P, P, P, P, P, C.c_double, I32, P, P, P, I32]
         _lib = l
@@ -122,3 +124,12 @@ def diff_loss(scene, lines, endpoint_point, endpoint_weights, points, colors, si
                               ew.ctypes.data, pts.ctypes.data, cols.ctypes.data, float(sigma), r, bg.ctypes.data,
                               tgt.ctypes.data, img.ctypes.data if img is not None else None, threads)
     return (loss, img) if return_image else loss
+
+
+def interpret_sdf_draws(desc) -> np.ndarray:
+    """Fine-only image (H, W, 4 RGBA8) of a scene of SDF draws: every draw
+    interpreted as a PTCL_SDF particle in every tile, no coarse stage."""
+    img = np.zeros((desc.height, desc.width, 4), np.uint8)
+    if lib().or_interpret_sdf_draws(C.byref(desc), img.ctypes.data) != 0:
+        raise RuntimeError("oracle: " + lib().or_error().decode())
+    return img

@@ -1660,4 +1660,35 @@ float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine*
 }
 float or_exp_nonpos(float x) { return exp_nonpos(x); }
 
+// Fine-only oracle (src/native/runtime/tests/coarse_count/rect_pixels.rs:3-13):
+// every draw interpreted as a PTCL_SDF particle in every tile, in draw-record
+// order, from the clear colour, with no coarse stage, so an incorrect
+// full-tile proof, hollow-stroke proof or occlusion skip changes pixels.
+int32_t or_interpret_sdf_draws(const tk_scene_desc* d, uint32_t* image) {
+    try {
+        or_scene S;
+        S.desc = *d;
+        S.draws.assign(d->draws, d->draws + d->draw_count);
+        S.brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
+        S.sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
+        S.shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
+        std::vector<tk_ptcl_record> recs;
+        for (uint32_t k = 0; k < d->draw_count; ++k) recs.push_back({TK_PTCL_SDF, 0, 0u, 0u, 0u, k});
+        recs.push_back({TK_PTCL_END, 0, 0u, 0u, 0u, 0u});
+        const uint32_t n = uint32_t(recs.size());
+        parallel_for(8, d->height, [&](uint64_t y) {
+            for (uint32_t x = 0; x < d->width; ++x) {
+                F4 pixel = rgba8_to_unorm(d->clear_color);  // fine_initial_pixel without load_target
+                pixel = interpret(S, recs, 0u, n, pixel, x % TK_TILE_SIZE, uint32_t(y) % TK_TILE_SIZE, x,
+                                  uint32_t(y));
+                image[y * d->width + x] = texel_store(pixel);
+            }
+        });
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 }  // extern "C"

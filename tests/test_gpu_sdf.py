@@ -208,3 +208,21 @@ def test_gpu_rejects_unsupported_sdf_records(renderer):
             renderer.upload(N.ArrayScene(arrays))
         assert e.value.code == N.TK_E_INVALID
     renderer.render_to_image(c)
+
+
+def test_gpu_rect_known_answers_match_fine_only_oracle(renderer):
+    """The reference's coarse known-answer pixel tests for SDF rects
+    (coarse_count/rect_pixels.rs:110-283, occlusion_pixels.rs:85-116): the
+    sm_100a pipeline, with coarse's full-tile colour, hollow-stroke and
+    occlusion proofs, gives exactly the pixels of fine interpreting every draw
+    in every tile. Edge, huge (1e7, 1.7e38) and far-translated geometry, draw
+    transforms, 0-257 stacked rects of alpha 0/127/255."""
+    import oracle
+    from sdf_cases import all_cases, desc_of
+    for name, scene in all_cases():
+        keep, d = desc_of(scene)
+        want = oracle.interpret_sdf_draws(d)
+        renderer.upload(keep)
+        renderer.render()
+        got = renderer.readback().view(np.uint8).reshape(want.shape)
+        assert np.array_equal(got, want), (name, int((got != want).any(axis=2).sum()))

@@ -224,3 +224,16 @@ def test_sdf_nodes_replay_under_translations_only():
     canvas, damage = rs.materialize()
     rects = {tuple(r) for r in damage["rects"].tolist()}
     assert (10, 10, 50, 40) in rects and (30, 10, 70, 40) in rects
+
+
+def test_oracle_coarse_proofs_match_fine_only_oracle():
+    """The oracle's full pipeline (coarse with its full-tile colour,
+    hollow-stroke and occlusion proofs, then fine) gives the fine-only
+    oracle's pixels on the reference's rect known-answer scenes."""
+    from sdf_cases import all_cases, desc_of
+    for name, scene in all_cases():
+        keep, d = desc_of(scene)
+        want = oracle.interpret_sdf_draws(d)
+        run = oracle.OracleRun(d, threads=4)
+        got = run.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(want.shape)
+        assert np.array_equal(got, want), (name, int((got != want).any(axis=2).sum()))
