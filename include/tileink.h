@@ -101,10 +101,14 @@ extern "C" {
 #define TK_SDF_CIRCLE 2u
 #define TK_SDF_RECT_STROKE 3u
 #define TK_SDF_CIRCLE_STROKE 4u
+#define TK_SDF_CANDLESTICK 5u
 #define TK_SDF_LINE 6u
 #define TK_SDF_RECT_SHADOW 7u
 #define TK_SDF_CIRCLE_SHADOW 10u
 #define TK_SDF_LINE_SHADOW 11u
+#define TK_SDF_DASH_LINE 12u
+#define TK_SDF_TRIANGLE 13u
+#define TK_SDF_CHECKERBOARD 14u
 #define TK_SDF_CAP_BUTT 0u
 #define TK_SDF_CAP_SQUARE 1u
 #define TK_SDF_CAP_ROUND 2u

@@ -92,18 +92,27 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
  *   TK_SDF_CIRCLE         p0 centre; radius
  *   TK_SDF_CIRCLE_STROKE  p0; radius; width (full stroke width)
  *   TK_SDF_LINE           p0, p1 ends; width; cap
+ *   TK_SDF_DASH_LINE      p0, p1; width; cap; dash (dash and gap lengths, offset)
+ *   TK_SDF_TRIANGLE       p0, p1, p2 vertices; radius (corner radius)
+ *   TK_SDF_CHECKERBOARD   p0, p1 corners; radius (cell size): the even cells
+ *                         only (Canvas::push_checkerboard adds the base rect)
+ *   TK_SDF_CANDLESTICK    p0 = (centre x, high y), p1 = (body top y, body
+ *                         bottom y), p2 = (low y, unused), widths[0] body and
+ *                         widths[1] wick width (whole pixels, > 0)
  *   TK_SDF_*_SHADOW       the shape's fields plus shadow
  * The draw is recorded as one SDF record (identity draw transform) whose
  * pixel bounds follow the reference's Sdf::bounds / SdfShadow::bounds. */
 typedef struct tk_sdf_shape {
     uint32_t kind;       /* TK_SDF_* */
     uint32_t cap;        /* lines: TK_SDF_CAP_* */
-    double p0[2], p1[2];
-    double radius;       /* circles */
+    double p0[2], p1[2], p2[2];
+    double radius;       /* circles; triangle corner radius; checkerboard cell size */
     double width;        /* circle strokes and lines */
     float radii[4];      /* corner radii: top-left, top-right, bottom-left, bottom-right */
     float widths[4];     /* rect stroke side widths: top, right, bottom, left */
     float shadow[4];     /* offset x, offset y, expand (falloff length), intensity */
+    float dash[3];       /* dash lines: dash length, gap length, dash offset */
+    uint32_t reserved;
 } tk_sdf_shape;
 /* Returns the draw index, -2 when the shape draws nothing (a non-positive
  * stroke width, an empty line, a shadow of zero intensity: the reference's

@@ -628,6 +628,121 @@ float sdf_shadow_cov(const SdfS& s, const tk_affine& inv, float expand, float in
     if (expand > 0.0f) return clampf(exp_nonpos(-fmax_(s.dist, 0.0f) / expand) * ci, 0.0f, 1.0f);
     return sdf_cov(s, inv) * ci;
 }
+// nearer_sdf_sample / farther_sdf_sample (shared/sdf/base.hlsli:25-37)
+SdfS sdf_nearer(const SdfS& a, const SdfS& b) { return a.dist <= b.dist ? a : b; }
+SdfS sdf_farther(const SdfS& a, const SdfS& b) { return a.dist >= b.dist ? a : b; }
+// distance_to_segment_sdf_sample (shared/sdf/polygon.hlsli:7-26)
+SdfS sdf_segment(float px, float py, float ax, float ay, float bx, float by, float fx, float fy) {
+    float dx = bx - ax, dy = by - ay;
+    float len2 = dx * dx + dy * dy;
+    float nx = ax, ny = ay;
+    if (len2 >= 1.175494351e-38f && std::isfinite(len2)) {
+        float t = clampf(((px - ax) * dx + (py - ay) * dy) / len2, 0.0f, 1.0f);
+        nx = ax + dx * t;
+        ny = ay + dy * t;
+    } else {
+        float axis = fmax_(std::fabs(dx), std::fabs(dy));
+        if (axis > 0.0f) {
+            float sx = dx / axis, sy = dy / axis;
+            float dot = sx * sx + sy * sy;
+            float qx = sx / dot, qy = sy / dot;
+            float t = clampf(((px - ax) * qx + (py - ay) * qy) / axis, 0.0f, 1.0f);
+            nx = ax + dx * t;
+            ny = ay + dy * t;
+        }
+    }
+    SdfS r;
+    r.dist = sdf_len(px - nx, py - ny);
+    sdf_unit_or(px - nx, py - ny, fx, fy, r.nx, r.ny);
+    return r;
+}
+// triangle_sdf_sample (shared/sdf/polygon.hlsli:32-85)
+SdfS sdf_triangle(float x, float y, float ax, float ay, float bx, float by, float cx, float cy, float corner) {
+    float abx = bx - ax, aby = by - ay, bcx = cx - bx, bcy = cy - by, cax = ax - cx, cay = ay - cy;
+    float tb[2] = {bx - ax, by - ay}, tc[2] = {cx - ax, cy - ay}, tp[2] = {x - ax, y - ay};
+    auto cross = [](float a0, float a1, float b0, float b1) { return a0 * b1 - a1 * b0; };
+    float area = cross(tb[0], tb[1], tc[0], tc[1]);
+    float lo[2] = {fmin_(fmin_(ax, bx), cx), fmin_(fmin_(ay, by), cy)};
+    float hi[2] = {fmax_(fmax_(ax, bx), cx), fmax_(fmax_(ay, by), cy)};
+    if (area == 0.0f || !std::isfinite(area)) {
+        float span[2] = {hi[0] - lo[0], hi[1] - lo[1]};
+        if (span[0] > 0.0f && span[1] > 0.0f) {
+            for (int k = 0; k < 2; ++k) { tb[k] /= span[k]; tc[k] /= span[k]; tp[k] /= span[k]; }
+            area = cross(tb[0], tb[1], tc[0], tc[1]);
+        }
+    }
+    float o = area >= 0.0f ? 1.0f : -1.0f;
+    float n[3][2];
+    sdf_unit_or(aby * o, -abx * o, 1.0f, 0.0f, n[0][0], n[0][1]);
+    sdf_unit_or(bcy * o, -bcx * o, 1.0f, 0.0f, n[1][0], n[1][1]);
+    sdf_unit_or(cay * o, -cax * o, 1.0f, 0.0f, n[2][0], n[2][1]);
+    SdfS r = sdf_nearer(sdf_segment(x, y, ax, ay, bx, by, n[0][0], n[0][1]),
+                        sdf_segment(x, y, bx, by, cx, cy, n[1][0], n[1][1]));
+    r = sdf_nearer(r, sdf_segment(x, y, cx, cy, ax, ay, n[2][0], n[2][1]));
+    float side_ab = cross(tb[0], tb[1], tp[0], tp[1]) * o;
+    float side_bc = cross(tc[0] - tb[0], tc[1] - tb[1], tp[0] - tb[0], tp[1] - tb[1]) * o;
+    float side_ca = cross(-tc[0], -tc[1], tp[0] - tc[0], tp[1] - tc[1]) * o;
+    if (area != 0.0f && x >= lo[0] && y >= lo[1] && x <= hi[0] && y <= hi[1] && side_ab >= 0.0f && side_bc >= 0.0f &&
+        side_ca >= 0.0f)
+        r = {-r.dist, -r.nx, -r.ny};
+    return {r.dist - fmax_(corner, 0.0f), r.nx, r.ny};
+}
+// checkerboard_sdf_sample (shared/sdf/effects.hlsli:8-36)
+SdfS sdf_checkerboard(float x, float y, float x0, float y0, float x1, float y1, float cell_raw) {
+    float left = fmin_(x0, x1), top = fmin_(y0, y1), right = fmax_(x0, x1), bottom = fmax_(y0, y1);
+    SdfS outer = sdf_rect(x, y, left, top, right, bottom, 0.0f, 0.0f, 0.0f, 0.0f);
+    float cell = fmax_(cell_raw, 0.000001f);
+    float cell_x = std::floor((x - left) / cell), cell_y = std::floor((y - top) / cell);
+    float lx = rem_euclid_f32(x - left, cell), ly = rem_euclid_f32(y - top, cell);
+    float e = lx, nx = 1.0f, ny = 0.0f;
+    if (cell - lx < e) { e = cell - lx; nx = -1.0f; ny = 0.0f; }
+    if (ly < e) { e = ly; nx = 0.0f; ny = 1.0f; }
+    if (cell - ly < e) { e = cell - ly; nx = 0.0f; ny = -1.0f; }
+    // (int(cell_x) + int(cell_y)) % 2 == 0, as two's complement parity
+    bool filled = ((uint32_t(f2i(cell_x)) + uint32_t(f2i(cell_y))) & 1u) == 0u;
+    return sdf_farther(outer, {filled ? -e : e, nx, ny});
+}
+// line_segment_sdf_sample (shared/sdf/line.hlsli:16-26)
+SdfS sdf_line_segment(float axis, float normal, float start, float end, float he, float cap) {
+    float nearest = clampf(axis, start, end);
+    SdfS r;
+    r.dist = sdf_len(axis - nearest, normal) - he;
+    sdf_unit_or(axis - nearest, normal, 0.0f, 1.0f, r.nx, r.ny);
+    if (cap < 0.5f) r = sdf_line_rect(axis, normal, start, end, he);
+    else if (cap < 1.5f) r = sdf_line_rect(axis, normal, start - he, end + he, he);
+    return r;
+}
+// dash_line_sdf_sample (shared/sdf/line.hlsli:28-39, 78-105)
+SdfS sdf_dash_line(float x, float y, float sx, float sy, float ex, float ey, float width, float cap, float dash_raw,
+                   float gap_raw, float offset_raw) {
+    float dash = fmax_(dash_raw, 0.0f), gap = fmax_(gap_raw, 0.0f);
+    SdfS r = sdf_line(x, y, sx, sy, ex, ey, width, cap);
+    if (dash > 0.0f && gap > 0.0f) {
+        float he = fmax_(width, 0.0f) * 0.5f;
+        float dx = ex - sx, dy = ey - sy;
+        float len = sdf_len(dx, dy);
+        if (len > 0.0f) {
+            float ux = dx / len, uy = dy / len, px = x - sx, py = y - sy;
+            float axis = px * ux + py * uy;
+            float normal = -px * uy + py * ux;
+            float cycle = dash + gap;
+            float offset = rem_euclid_f32(offset_raw, cycle);
+            float base = std::floor((axis + offset) / cycle);
+            auto seg = [&](float ix) {
+                float s0 = ix * cycle - offset, s1 = s0 + dash;
+                SdfS q{std::numeric_limits<float>::infinity(), 1.0f, 0.0f};
+                if (s1 > 0.0f && s0 < len) {
+                    float start = fmax_(s0, 0.0f), end = fmin_(s1, len);
+                    if (end > start) q = sdf_line_segment(axis, normal, start, end, he, cap);
+                }
+                return q;
+            };
+            SdfS l = sdf_nearer(sdf_nearer(seg(base - 1.0f), seg(base)), seg(base + 1.0f));
+            r = {l.dist, l.nx * ux - l.ny * uy, l.nx * uy + l.ny * ux};
+        }
+    }
+    return r;
+}
 // sdf_coverage_from_blob (shared/sdf/coverage.hlsli:13-236) for the kinds the
 // library accepts; others have no coverage.
 float sdf_blob_coverage(const uint32_t* w, float x, float y, const tk_affine& inv) {
@@ -664,6 +779,22 @@ float sdf_blob_coverage(const uint32_t* w, float x, float y, const tk_affine& in
     if (kind == TK_SDF_LINE) return sdf_cov(sdf_line(x, y, x0, y0, x1, y1, r0, r1), inv);
     if (kind == TK_SDF_LINE_SHADOW)
         return sdf_shadow_cov(sdf_line(x - ox, y - oy, x0, y0, x1, y1, r0, r1), inv, ex, in);
+    if (kind == TK_SDF_CANDLESTICK) {  // candlestick_sdf_coverage (shared/sdf/effects.hlsli:38-70)
+        float cx = x0, high = y0, low = x1, top = y1, bottom = r0, body_w = r1, wick_w = r2;
+        float wh = fmax_(wick_w, 1.0f) * 0.5f;
+        float wick = sdf_cov(sdf_rect(x, y, cx - wh, fmin_(high, low), cx + wh, fmax_(high, low), 0, 0, 0, 0), inv);
+        float bh = fmax_(body_w, 1.0f) * 0.5f;
+        float by0 = fmin_(top, bottom), by1 = fmax_(top, bottom);
+        if (by0 == by1) {
+            by0 = by0 - 0.5f;
+            by1 = by1 + 0.5f;
+        }
+        float body = sdf_cov(sdf_rect(x, y, cx - bh, by0, cx + bh, by1, 0, 0, 0, 0), inv);
+        return fmax_(wick, body);
+    }
+    if (kind == TK_SDF_DASH_LINE) return sdf_cov(sdf_dash_line(x, y, x0, y0, x1, y1, r0, r1, r2, r3, st), inv);
+    if (kind == TK_SDF_TRIANGLE) return sdf_cov(sdf_triangle(x, y, x0, y0, x1, y1, r0, r1, r2), inv);
+    if (kind == TK_SDF_CHECKERBOARD) return sdf_cov(sdf_checkerboard(x, y, x0, y0, x1, y1, r0), inv);
     return 0.0f;
 }
 

@@ -62,6 +62,34 @@ def random_shapes(c, rng, n, w, h):
                                cap=int(rng.integers(0, 3)))
 
 
+def extended_shapes(c, rng, n, w, h):
+    """n seeded shapes of the extended kinds (triangles, dash lines,
+    checkerboards, candlesticks), degenerate ones included."""
+    for k in range(n):
+        b = gradient(rng, w, h) if rng.uniform() < 0.25 else tk.Brush.solid(*rng.uniform(0, 1, 3),
+                                                                          float(rng.choice([1.0, rng.uniform(0.2, 1)])))
+        x0, y0 = rng.uniform(-20, w), rng.uniform(-20, h)
+        kind = k % 4
+        if kind == 0:
+            pts = [(x0, y0)] + [(x0 + rng.uniform(-90, 90), y0 + rng.uniform(-90, 90)) for _ in range(2)]
+            if rng.uniform() < 0.1:
+                pts[2] = (pts[0][0] + 1e-3, pts[0][1] + 2e-3)  # a sliver
+            c.push_triangle(*pts, b, corner_radius=float(rng.choice([0.0, rng.uniform(0, 6)])))
+        elif kind == 1:
+            c.push_dash_line(x0, y0, x0 + rng.uniform(-250, 250), y0 + rng.uniform(-250, 250),
+                             float(rng.uniform(0.5, 6)), float(rng.uniform(0.5, 20)),
+                             float(rng.choice([0.0, rng.uniform(0.5, 15)])), b, cap=int(rng.integers(0, 3)),
+                             dash_offset=float(rng.uniform(-30, 30)))
+        elif kind == 2:
+            c.push_checkerboard(x0, y0, x0 + rng.uniform(1, 200), y0 + rng.uniform(1, 200),
+                                float(rng.choice([rng.uniform(0.3, 2), rng.uniform(2, 40)])), b,
+                                tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0))
+        else:
+            top, bottom = rng.uniform(y0, y0 + 120, 2)
+            c.push_candlestick(x0, y0, y0 + rng.uniform(0, 160), top, float(rng.choice([bottom, top])),
+                               int(rng.integers(1, 15)), int(rng.integers(1, 4)), b)
+
+
 def cubic_path(rng, w, h, n=6):
     p = tk.BezPath()
     cx, cy = rng.uniform(0, w), rng.uniform(0, h)
@@ -128,6 +156,20 @@ def test_gpu_random_sdf_scenes(renderer, seed, scale):
     compare_frame(renderer, c)
 
 
+@pytest.mark.parametrize("seed,scale", [(11, 1.0), (12, 1.25)])
+def test_gpu_extended_sdf_kinds(renderer, seed, scale):
+    W, H = 480, 360
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(W, H, scale=scale)
+    c.set_clear_color(0xFF303030)
+    extended_shapes(c, rng, 160, W, H)
+    random_shapes(c, rng, 40, W, H)
+    c.push_clip_layer(cubic_path(rng, W, H, 8))
+    extended_shapes(c, rng, 40, W, H)
+    c.pop_layer()
+    compare_frame(renderer, c)
+
+
 def sdf_scene(seed, w, h, n):
     rng = np.random.default_rng(seed)
     c = tk.Canvas(w, h)
@@ -137,6 +179,9 @@ def sdf_scene(seed, w, h, n):
 
 def test_gpu_sdf_batch_matches_serial(renderer):
     scenes = [sdf_scene(50 + i, 96 + 64 * i, 80 + 48 * i, 30 + 20 * i) for i in range(6)]
+    ext = tk.Canvas(200, 150)
+    extended_shapes(ext, np.random.default_rng(60), 40, 200, 150)
+    scenes.append(ext)
     scenes += [tk.generate(4, 9)]
     serial = [serial_outputs(renderer, c) for c in scenes]
     r = tk.NativeRenderer(0)

@@ -237,3 +237,44 @@ def test_oracle_coarse_proofs_match_fine_only_oracle():
         run = oracle.OracleRun(d, threads=4)
         got = run.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(want.shape)
         assert np.array_equal(got, want), (name, int((got != want).any(axis=2).sum()))
+
+
+def test_extended_sdf_kinds_records_and_bounds():
+    c = tk.Canvas(200, 120)
+    # src/shared/sdf/triangle.rs:95-105 and candlestick.rs:97-102
+    kind, f, pb = record(c, c.push_triangle((8, 4), (20, 16), (8, 28), SOLID, corner_radius=2.0))
+    assert kind == N.SDF_TRIANGLE and list(f[:7]) == [8, 4, 20, 16, 8, 28, 2] and pb == (6, 2, 22, 30)
+    kind, f, pb = record(c, c.push_candlestick(16.5, 4.0, 28.0, 10.0, 22.0, 7, 1, SOLID))
+    assert kind == N.SDF_CANDLESTICK and list(f[:7]) == [16.5, 4, 28, 10, 22, 7, 1] and pb == (13, 4, 20, 28)
+    kind, f, pb = record(c, c.push_dash_line(10, 100, 190, 100, 3, 6, 4, SOLID, cap=N.CAP_ROUND, dash_offset=2))
+    assert kind == N.SDF_DASH_LINE and list(f[:9]) == [10, 100, 190, 100, 3, N.CAP_ROUND, 6, 4, 2]
+    base, cells = c.push_checkerboard(100, 10, 180, 70, 8, SOLID, tk.Brush.solid(1, 1, 1, 1))
+    kind, f, pb = record(c, cells)
+    assert kind == N.SDF_CHECKERBOARD and list(f[:5]) == [100, 10, 180, 70, 8] and record(c, base)[0] == N.SDF_RECT
+    # the reference's None: collinear triangle, no visible dash, empty checkerboard
+    assert c.push_triangle((0, 0), (1, 1), (2, 2), SOLID) is None
+    assert c.push_dash_line(0, 0, 1, 0, 1, 1, 10, SOLID, dash_offset=2) is None
+    assert c.push_checkerboard(0, 0, 0, 10, 2, SOLID, SOLID) is None
+    with pytest.raises(ValueError):
+        c.push_candlestick(1, 2, 3, 4, 5, 0, 1, SOLID)  # CandleStick::new rejects a zero width
+
+
+def test_oracle_extended_kinds_against_closed_forms():
+    # triangle: inside, the distance to the nearest edge, negated
+    tri = sdf_words(N.SDF_TRIANGLE, (0, 0, 40, 0), (0, 40, 0))
+    assert coverage(tri, 10, 10) == 1.0 and coverage(tri, 30, 30) == 0.0
+    d = (25.0 + 25.0 - 40.0) / math.sqrt(2.0)  # (25, 25) lies outside the hypotenuse x + y = 40
+    assert coverage(tri, 25, 25) == pytest.approx(min(max(0.5 - d, 0), 1), abs=TOL)
+    assert coverage(tri, 0.25, 20) == pytest.approx(0.75, abs=TOL)
+    # checkerboard: even cells (cell x + cell y even) covered, odd ones not
+    cb = sdf_words(N.SDF_CHECKERBOARD, (0, 0, 64, 64), (8,))
+    assert coverage(cb, 4, 4) == 1.0 and coverage(cb, 12, 4) == 0.0 and coverage(cb, 12, 12) == 1.0
+    assert coverage(cb, 8.25, 4) == pytest.approx(0.25, abs=TOL)  # a quarter pixel into the odd cell
+    # dash line: dashes of 6 with gaps of 4 from x = 0; a gap's middle is empty
+    dash = sdf_words(N.SDF_DASH_LINE, (0, 10, 100, 10), (2, N.CAP_BUTT, 6, 4))
+    assert coverage(dash, 3, 10) == 1.0 and coverage(dash, 8, 10) == 0.0 and coverage(dash, 13, 10) == 1.0
+    assert coverage(dash, 6.25, 10) == pytest.approx(0.25, abs=TOL)
+    # candlestick: wick or body, whichever covers more
+    candle = sdf_words(N.SDF_CANDLESTICK, (20, 0, 60, 20), (40, 9, 1))
+    assert coverage(candle, 20, 5) == pytest.approx(1.0) and coverage(candle, 24, 30) == pytest.approx(1.0)
+    assert coverage(candle, 24.75, 30) == pytest.approx(0.25, abs=TOL) and coverage(candle, 24, 5) == 0.0

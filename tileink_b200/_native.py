@@ -33,6 +33,7 @@ TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIN
 # SDF kinds (src/shared/gpu_types.rs) and line caps
 SDF_RECT, SDF_CIRCLE, SDF_RECT_STROKE, SDF_CIRCLE_STROKE, SDF_LINE = 1, 2, 3, 4, 6
 SDF_RECT_SHADOW, SDF_CIRCLE_SHADOW, SDF_LINE_SHADOW = 7, 10, 11
+SDF_CANDLESTICK, SDF_DASH_LINE, SDF_TRIANGLE, SDF_CHECKERBOARD = 5, 12, 13, 14
 SDF_RECORD_WORDS = 17
 CAP_BUTT, CAP_SQUARE, CAP_ROUND = 0, 1, 2
 
@@ -108,8 +109,9 @@ class BrushDesc(C.Structure):
 
 class SdfShape(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("cap", C.c_uint32), ("p0", C.c_double * 2), ("p1", C.c_double * 2),
-                ("radius", C.c_double), ("width", C.c_double), ("radii", C.c_float * 4), ("widths", C.c_float * 4),
-                ("shadow", C.c_float * 4)]
+                ("p2", C.c_double * 2), ("radius", C.c_double), ("width", C.c_double), ("radii", C.c_float * 4),
+                ("widths", C.c_float * 4), ("shadow", C.c_float * 4), ("dash", C.c_float * 3),
+                ("reserved", C.c_uint32)]
 
 
 class FlattenDesc(C.Structure):

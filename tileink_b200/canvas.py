@@ -3,7 +3,8 @@
     Canvas.push_path        src/canvas/primitives/paths.rs:50-60
     Canvas.push_stroke      src/canvas/primitives/paths.rs:24-48
     Canvas.push_rect / push_rect_stroke / push_circle / push_circle_stroke /
-    push_line and push_{rect,circle,line}_shadow
+    push_line / push_dash_line / push_triangle / push_checkerboard /
+    push_candlestick and push_{rect,circle,line}_shadow
                             src/canvas/primitives/{rectangles,shapes,shadows}.rs
     Canvas.push_clip_layer  src/canvas/layers.rs:7-28
     Canvas.push_blur_group  src/canvas/layers.rs:205-212
@@ -209,11 +210,13 @@ class Canvas:
 
     # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
     def _push_sdf(self, brush: Brush, kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0,
-                  widths=0.0, shadow=None, cap=N.CAP_BUTT):
+                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0)):
         s = N.SdfShape()
         s.kind, s.cap = kind, int(cap)
         s.p0[:] = [float(v) for v in p0]
         s.p1[:] = [float(v) for v in p1]
+        s.p2[:] = [float(v) for v in p2]
+        s.dash[:] = [float(v) for v in dash]
         s.radius, s.width = float(radius), float(width)
         s.radii[:] = _four(radii)
         s.widths[:] = _four(widths)
@@ -248,6 +251,35 @@ class Canvas:
         """Canvas::push_line (SdfLine): None for an empty line (width <= 0, or a
         butt-capped point)."""
         return self._push_sdf(brush, N.SDF_LINE, (x0, y0), (x1, y1), width=width, cap=cap)
+
+    def push_dash_line(self, x0, y0, x1, y1, width, dash_length, gap_length, brush: Brush, cap=N.CAP_BUTT,
+                       dash_offset=0.0):
+        """Canvas::push_dash_line (SdfDashLine::with_offset): None when no dash
+        is visible."""
+        return self._push_sdf(brush, N.SDF_DASH_LINE, (x0, y0), (x1, y1), width=width, cap=cap,
+                              dash=(dash_length, gap_length, dash_offset))
+
+    def push_triangle(self, a, b, c, brush: Brush, corner_radius=0.0):
+        """Canvas::push_triangle: None for collinear or non-finite vertices."""
+        return self._push_sdf(brush, N.SDF_TRIANGLE, a, b, p2=c, radius=corner_radius)
+
+    def push_checkerboard(self, x0, y0, x1, y1, cell_size, first: Brush, second: Brush):
+        """Canvas::push_checkerboard (src/canvas/primitives/rectangles.rs:9-26):
+        the rectangle in `second`, then the even cells in `first`; returns the
+        two draw ids, or None (and no draw) for an invalid rectangle or cell."""
+        import math
+        ok = all(math.isfinite(v) for v in (x0, y0, x1, y1)) and x1 - x0 > 0 and y1 - y0 > 0
+        if not ok or not (math.isfinite(cell_size) and cell_size > 0):
+            return None
+        base = self.push_rect(x0, y0, x1, y1, second)
+        return base, self._push_sdf(first, N.SDF_CHECKERBOARD, (x0, y0), (x1, y1), radius=cell_size)
+
+    def push_candlestick(self, center_x, high_y, low_y, body_top_y, body_bottom_y, body_width: int,
+                         wick_width: int, brush: Brush):
+        """Canvas::push_candlestick (SdfCandleStick): a wick from high to low and
+        a body between its top and bottom; widths whole pixels > 0."""
+        return self._push_sdf(brush, N.SDF_CANDLESTICK, (center_x, high_y), (body_top_y, body_bottom_y),
+                              p2=(low_y, 0.0), widths=(float(body_width), float(wick_width), 0.0, 0.0))
 
     def push_rect_shadow(self, x0, y0, x1, y1, brush: Brush, offset=(0.0, 0.0), expand=0.0, intensity=1.0,
                          radius=0.0):

@@ -122,6 +122,7 @@ struct tk_ctx {
     uint32_t width = 0, height = 0, tw = 0, th = 0, clear = 0, flags = 0;
     uint64_t line_count = 0, brush_words = 0, pool_len = 0, host_segment_capacity = 0;
     uint64_t sdf_words = 0, sdf_shadow_base = 0;  // SDF buffer: sdf_blob, then sdf_shadow_blob
+    bool sdf_ext = false;                          // a candlestick, dash line, triangle or checkerboard
     uint32_t path_count = 0, draw_count = 0, layer_count = 0, order_count = 0;
     std::vector<tk_path_record> h_paths;
     std::vector<tk::ScanItem> h_items;
@@ -251,6 +252,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     if (next_line != d.line_count) invalid("path line ranges do not cover the line array");
     if (seg_cap > 0xFFFFFFFFull) invalid("segment capacity exceeds u32 indexing");
     if (d.sdf_word_count + d.sdf_shadow_word_count > 0xFFFFFFFFull) invalid("SDF blobs exceed u32 indexing");
+    bool sdf_ext = false;
     // Draws: path fills/clips, and brush draws of the SDF kinds this library
     // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
     for (uint32_t i = 0; i < d.draw_count; ++i) {
@@ -267,11 +269,14 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             const uint64_t words = plain ? d.sdf_word_count : d.sdf_shadow_word_count;
             if (len != TK_SDF_RECORD_WORDS || off + len > words) invalid(at + ": SDF record outside its blob");
             const uint32_t kind = (plain ? d.sdf_blob : d.sdf_shadow_blob)[off];
-            const bool ok = plain ? (kind == TK_SDF_RECT || kind == TK_SDF_CIRCLE || kind == TK_SDF_RECT_STROKE ||
-                                     kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_LINE)
-                                  : (kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW ||
-                                     kind == TK_SDF_LINE_SHADOW);
+            const bool ext = plain && (kind == TK_SDF_CANDLESTICK || kind == TK_SDF_DASH_LINE ||
+                                       kind == TK_SDF_TRIANGLE || kind == TK_SDF_CHECKERBOARD);
+            const bool ok = ext || (plain ? (kind == TK_SDF_RECT || kind == TK_SDF_CIRCLE || kind == TK_SDF_RECT_STROKE ||
+                                             kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_LINE)
+                                          : (kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW ||
+                                             kind == TK_SDF_LINE_SHADOW));
             if (!ok) invalid(at + ": SDF kind " + std::to_string(kind) + " is not supported");
+            sdf_ext = sdf_ext || ext;
         }
         if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
             r.tag != TK_DRAW_ISOLATE)
@@ -354,6 +359,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     c->brush_words = d.brush_word_count;
     c->sdf_words = d.sdf_word_count + d.sdf_shadow_word_count;
     c->sdf_shadow_base = d.sdf_word_count;
+    c->sdf_ext = sdf_ext;
     c->pool_len = pool;
     c->host_segment_capacity = seg_cap;
     c->h_paths.assign(d.paths, d.paths + d.path_count);
@@ -384,6 +390,7 @@ tk::SceneView view(tk_ctx* c) {
     s.sdf = c->sdf.ptr;
     s.sdf_words = c->sdf_words;
     s.sdf_shadow_base = c->sdf_shadow_base;
+    s.sdf_ext = c->sdf_ext;
     s.layers = c->layers.ptr;
     s.batch_ids = c->batch_ids.ptr;
     s.order = c->order.ptr;
@@ -892,10 +899,12 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     std::vector<tk_batch_info> info;
     uint64_t pool = 0, segs = 0, list = 0, pixels = 0;
     uint32_t tiles = 0, bins = 0, batch_base = 0;
+    bool ext = false;  // some scene has SDF records of an extended kind
     for (uint32_t s = 0; s < n; ++s) {
         const tk_scene_desc& d = scenes[s];
         if (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) invalid("batched scenes use host segment planning");
         validate_and_plan(c, d);
+        ext = ext || c->sdf_ext;
         uint32_t npass = 0;
         for (const Step& st : c->steps) {
             if (st.kind != STEP_PASS) invalid("scene " + std::to_string(s) + ": blur groups are not batched");
@@ -1009,6 +1018,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     c->order_count = uint32_t(order.size());
     c->brush_words = brush.size();
     c->sdf_shadow_base = sdf.size();
+    c->sdf_ext = ext;
     sdf.insert(sdf.end(), shadow.begin(), shadow.end());
     c->sdf_words = sdf.size();
     c->pool_len = pool;

@@ -800,6 +800,99 @@ bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_R
             if (shadow) pb = shadow_bounds(pb, opt);
             return true;
         }
+        case TK_SDF_DASH_LINE: {
+            // DashLine::is_empty (src/shared/sdf/line.rs:140-148) on the logical line
+            const float w = float(s.width), dash = s.dash[0], gap = s.dash[1], off = s.dash[2];
+            if (s.cap > TK_SDF_CAP_ROUND || !(gap >= 0.0f) || !(dash == dash) || !(off == off)) return false;
+            if (w <= 0.0f || !(w == w) || (s.cap == TK_SDF_CAP_BUTT && s.p0[0] == s.p1[0] && s.p0[1] == s.p1[1]))
+                return false;
+            if (dash <= 0.0f) return false;
+            const double len = std::hypot(s.p1[0] - s.p0[0], s.p1[1] - s.p0[1]);
+            if (len > 0.0 && gap > 0.0f) {  // has_visible_dash
+                const double cycle = double(dash) + double(gap);
+                double o = std::fmod(double(off), cycle);
+                if (o < 0.0) o += cycle;  // f64::rem_euclid
+                if (!(o < double(dash) || cycle - o < len)) return false;
+            }
+            const float pw = w * sc;
+            put(1, float(x0));
+            put(2, float(y0));
+            put(3, float(x1));
+            put(4, float(y1));
+            put(5, pw);
+            put(6, float(s.cap));
+            put(7, dash * sc);
+            put(8, gap * sc);
+            put(9, off * sc);
+            pb = line_bounds(x0, y0, x1, y1, pw, s.cap);
+            return true;
+        }
+        case TK_SDF_TRIANGLE: {
+            // Triangle::is_empty / bounds (src/shared/sdf/triangle.rs:37-66)
+            const float corner = float(s.radius);
+            const double v[6] = {s.p0[0], s.p0[1], s.p1[0], s.p1[1], s.p2[0], s.p2[1]};
+            for (double q : v)
+                if (!std::isfinite(q)) return false;
+            const double area = (v[2] - v[0]) * (v[5] - v[1]) - (v[3] - v[1]) * (v[4] - v[0]);
+            if (!std::isfinite(corner) || corner < 0.0f || !std::isfinite(area) || area == 0.0) return false;
+            double p[6];
+            for (int k = 0; k < 6; ++k) p[k] = v[k] * sd;
+            const float pc = corner * sc;
+            put(1, float(p[0]));
+            put(2, float(p[1]));
+            put(3, float(p[2]));
+            put(4, float(p[3]));
+            put(5, float(p[4]));
+            put(6, float(p[5]));
+            put(7, pc);
+            const double r = double(pc);
+            pb = box_bounds(std::min(std::min(p[0], p[2]), p[4]) - r, std::min(std::min(p[1], p[3]), p[5]) - r,
+                            std::max(std::max(p[0], p[2]), p[4]) + r, std::max(std::max(p[1], p[3]), p[5]) + r);
+            return true;
+        }
+        case TK_SDF_CHECKERBOARD: {
+            // Checkerboard::is_empty / bounds (src/shared/sdf/checkerboard.rs:32-58)
+            const float cell = float(s.radius);
+            if (!std::isfinite(s.p0[0]) || !std::isfinite(s.p0[1]) || !std::isfinite(s.p1[0]) ||
+                !std::isfinite(s.p1[1]) || !std::isfinite(cell) || cell <= 0.0f || s.p0[0] == s.p1[0] ||
+                s.p0[1] == s.p1[1])
+                return false;
+            const double ax0 = std::min(x0, x1), ay0 = std::min(y0, y1), ax1 = std::max(x0, x1), ay1 = std::max(y0, y1);
+            put(1, float(ax0));
+            put(2, float(ay0));
+            put(3, float(ax1));
+            put(4, float(ay1));
+            put(5, cell * sc);
+            pb = box_bounds(ax0, ay0, ax1, ay1);
+            return true;
+        }
+        case TK_SDF_CANDLESTICK: {
+            // physical_sdf (canvas/surface.rs:459-469, scaled_positive_u32 canvas.rs:214-219)
+            // and CandleStick::bounds (src/shared/sdf/candlestick.rs:58-70)
+            auto scaled_u32 = [&](float w) {
+                const float v = std::min(std::max(std::round(w * sc), 1.0f), 4294967295.0f);
+                return float(uint32_t(v));
+            };
+            const float cx = float(s.p0[0]) * sc, high = float(s.p0[1]) * sc, low = float(s.p2[0]) * sc;
+            const float top = float(s.p1[0]) * sc, bottom = float(s.p1[1]) * sc;
+            const float bw = scaled_u32(s.widths[0]), ww = scaled_u32(s.widths[1]);
+            put(1, cx);
+            put(2, high);
+            put(3, low);
+            put(4, top);
+            put(5, bottom);
+            put(6, bw);
+            put(7, ww);
+            const float bh = bw * 0.5f, wh = ww * 0.5f;
+            float by0 = std::min(top, bottom), by1 = std::max(top, bottom);
+            if (by0 == by1) {
+                by0 -= 0.5f;
+                by1 += 0.5f;
+            }
+            pb = {sat_i32(std::floor(std::min(cx - bh, cx - wh))), sat_i32(std::floor(std::min(by0, std::min(high, low)))),
+                  sat_i32(std::ceil(std::max(cx + bh, cx + wh))), sat_i32(std::ceil(std::max(by1, std::max(high, low))))};
+            return true;
+        }
         default:
             return false;
     }
@@ -919,8 +1012,12 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     if (!c || !shape) return -1;
     const uint32_t k = shape->kind;
     if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
-        k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW)
+        k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW &&
+        k != TK_SDF_DASH_LINE && k != TK_SDF_TRIANGLE && k != TK_SDF_CHECKERBOARD && k != TK_SDF_CANDLESTICK)
         return -1;
+    // CandleStick::new and DashLine::new reject these (the reference panics)
+    if (k == TK_SDF_CANDLESTICK && !(shape->widths[0] > 0.0f && shape->widths[1] > 0.0f)) return -1;
+    if (k == TK_SDF_DASH_LINE && !(shape->dash[1] >= 0.0f)) return -1;
     if (c->keep) {
         RecCmd r = rec_cmd(RecCmd::SDF, nullptr, brush, nullptr);
         r.shape = *shape;
@@ -1440,6 +1537,13 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
                 sh.p0[1] += t[5];
                 sh.p1[0] += t[4];
                 sh.p1[1] += t[5];
+                if (sh.kind == TK_SDF_CANDLESTICK) {  // y values in p1, p2[0]
+                    sh.p1[0] += t[5] - t[4];
+                    sh.p2[0] += t[5];
+                } else {
+                    sh.p2[0] += t[4];
+                    sh.p2[1] += t[5];
+                }
             }
             return tk_canvas_push_sdf(dst, &sh, bp) == -1 ? -1 : 0;
         }

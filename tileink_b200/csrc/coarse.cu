@@ -347,7 +347,8 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     info.color = brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD);
                 }
                 // solid_supported_sdf (coarse/paint.hlsli:21-25)
-                if (solid && plain && kind == TK_SDF_RECT) sdf_bits |= kMetaSdfSolidClass;
+                if (solid && plain && (kind == TK_SDF_RECT || kind == TK_SDF_CANDLESTICK || kind == TK_SDF_CHECKERBOARD))
+                    sdf_bits |= kMetaSdfSolidClass;
             } else if (d.tag == TK_DRAW_BRUSH && d.solid_rect != 0u && d.transform.b == 0.0f &&
                        d.transform.c == 0.0f && solid_paint()) {
                 color_candidate = true;

@@ -359,12 +359,13 @@ __device__ __forceinline__ float staged_coverage(const FineSmem& S, uint32_t i, 
 // mapped to draw space by the draw's inverse transform (affine_record_point,
 // shared/affine.hlsli:14-18). Inlined: an out-of-line call costs the record
 // loop more (register saves around the call) than the shape switch does.
+template <bool EXT>
 static __device__ __forceinline__ float sdf_coverage_at(const uint32_t* w, const tk_affine* t, uint32_t gx, uint32_t gy) {
     const tk_affine inv{__ldg(&t->a), __ldg(&t->b), __ldg(&t->c), __ldg(&t->d), __ldg(&t->e), __ldg(&t->f)};
     const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
     const float ux = __fmaf_rn(inv.a, sx, __fmaf_rn(inv.c, sy, inv.e));
     const float uy = __fmaf_rn(inv.b, sx, __fmaf_rn(inv.d, sy, inv.f));
-    return sdf_coverage(w, ux, uy, inv);
+    return sdf_coverage<EXT>(w, ux, uy, inv);
 }
 
 // Paints a fill's masked coverage over px (the brush branch of
@@ -388,11 +389,14 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
     }
 }
 
-// SDF: whether the scene has SDF records. Path-only scenes run the instance
-// without the PTCL_SDF branch, which costs the record loop about 3% even when
-// it is never taken.
-template <bool SDF>
-__global__ void __launch_bounds__(kFineThreads, 4)
+// SDF: 0 for scenes without SDF records, 1 with SDF records of the base
+// kinds, 2 with the extended kinds (candlestick, dash line, triangle,
+// checkerboard). Path-only scenes run the instance without the PTCL_SDF
+// branch, which costs the record loop about 3% even when never taken; the
+// extended kinds' code costs the base kinds more, so it has its own instance,
+// with the registers of 3 CTAs per SM.
+template <uint32_t SDF>
+__global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
            const uint32_t* __restrict__ brush, uint64_t brush_words, const tk_draw_record* __restrict__ draws,
@@ -457,9 +461,9 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                 if (a.x == TK_PTCL_FILL && n != 0u) cls = kClsFill;  // row sums staged below
             }
             S.nseg[tid] = n;
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (SDF && a.x == TK_PTCL_SDF)) {
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (SDF != 0u && a.x == TK_PTCL_SDF)) {
                 const PaintInfo* pi = paints + c.y;
-                if (SDF && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
+                if (SDF != 0u && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
                 const uint32_t paint = __ldg(&pi->paint);
                 if (paint != kGradient) {
                     S.paint[tid] = paint;
@@ -600,10 +604,10 @@ __global__ void __launch_bounds__(kFineThreads, 4)
                         px = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(px), a));
                     }
                 }
-            } else if (SDF && tag == TK_PTCL_SDF) {
+            } else if (SDF != 0u && tag == TK_PTCL_SDF) {
                 // PTCL_SDF (fine/interpreter.hlsli:70-84)
                 if (clip != 0u) {
-                    const float cov = sdf_coverage_at(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy);
+                    const float cov = sdf_coverage_at<SDF == 2u>(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy);
                     const uint32_t masked = combine_alpha(coverage_to_u8(cov), clip);
                     if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
                 }
@@ -691,11 +695,12 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     if (T == 0) return;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_fine<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
-        cudaFuncSetAttribute(k_fine<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        cudaFuncSetAttribute(k_fine<0u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        cudaFuncSetAttribute(k_fine<1u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        cudaFuncSetAttribute(k_fine<2u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
         configured = true;
     }
-    auto kernel = s.sdf_words ? k_fine<true> : k_fine<false>;
+    auto kernel = !s.sdf_words ? k_fine<0u> : (s.sdf_ext ? k_fine<2u> : k_fine<1u>);
     kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
                                                       s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,
                                                       s.tw, s.error, p.scenes, p.tile_scene, p.tile_list);

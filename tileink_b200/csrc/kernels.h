@@ -69,6 +69,7 @@ struct SceneView {
     const uint32_t* sdf;
     uint64_t sdf_words;
     uint64_t sdf_shadow_base;
+    bool sdf_ext;  // some record is of an extended kind (fine's k_fine<2>)
     const tk_layer_record* layers;
     const uint32_t* batch_ids;
     const uint32_t* order;

@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include "../../include/tileink.h"
+#include "device.cuh"
 
 namespace tkd {
 
@@ -178,6 +179,131 @@ __device__ __forceinline__ float shadow_coverage(const SdfSample& s, const tk_af
 
 __device__ __forceinline__ float sdf_word_f(const uint32_t* w, uint32_t i) { return __uint_as_float(__ldg(w + i)); }
 
+__device__ __forceinline__ SdfSample nearer(const SdfSample& a, const SdfSample& b) { return a.d <= b.d ? a : b; }
+__device__ __forceinline__ SdfSample farther(const SdfSample& a, const SdfSample& b) { return a.d >= b.d ? a : b; }
+
+// distance_to_segment_sdf_sample (shared/sdf/polygon.hlsli:7-26): unsigned
+// distance to segment a-b, `f` the normal where the point is on it.
+__device__ __forceinline__ SdfSample segment_sample(float px, float py, float ax, float ay, float bx, float by, float fx,
+                                                    float fy) {
+    const float dx = bx - ax, dy = by - ay;
+    const float len2 = dx * dx + dy * dy;
+    float nx = ax, ny = ay;
+    if (len2 >= 1.175494351e-38f && isfinite(len2)) {
+        const float t = fminf(fmaxf(((px - ax) * dx + (py - ay) * dy) / len2, 0.0f), 1.0f);
+        nx = ax + dx * t;
+        ny = ay + dy * t;
+    } else {
+        const float axis = fmaxf(fabsf(dx), fabsf(dy));
+        if (axis > 0.0f) {
+            const float sx = dx / axis, sy = dy / axis;
+            const float dd = sx * sx + sy * sy;
+            const float qx = sx / dd, qy = sy / dd;
+            const float t = fminf(fmaxf(((px - ax) * qx + (py - ay) * qy) / axis, 0.0f), 1.0f);
+            nx = ax + dx * t;
+            ny = ay + dy * t;
+        }
+    }
+    const float ex = px - nx, ey = py - ny;
+    SdfSample s;
+    s.d = sdf_length(ex, ey);
+    normalized_or(ex, ey, fx, fy, s.nx, s.ny);
+    return s;
+}
+
+// triangle_sdf_sample (shared/sdf/polygon.hlsli:32-85): the nearest edge,
+// negated inside, less the corner radius. 
+__device__ __forceinline__ SdfSample triangle_sample(float x, float y, float ax, float ay, float bx, float by,
+                                                         float cx, float cy, float corner) {
+    float tbx = bx - ax, tby = by - ay, tcx = cx - ax, tcy = cy - ay, tpx = x - ax, tpy = y - ay;
+    float area = tbx * tcy - tby * tcx;
+    const float lox = fminf(fminf(ax, bx), cx), loy = fminf(fminf(ay, by), cy);
+    const float hix = fmaxf(fmaxf(ax, bx), cx), hiy = fmaxf(fmaxf(ay, by), cy);
+    if (area == 0.0f || !isfinite(area)) {
+        const float spx = hix - lox, spy = hiy - loy;
+        if (spx > 0.0f && spy > 0.0f) {
+            tbx /= spx; tby /= spy; tcx /= spx; tcy /= spy; tpx /= spx; tpy /= spy;
+            area = tbx * tcy - tby * tcx;
+        }
+    }
+    const float o = area >= 0.0f ? 1.0f : -1.0f;
+    float n0x, n0y, n1x, n1y, n2x, n2y;
+    normalized_or((by - ay) * o, -(bx - ax) * o, 1.0f, 0.0f, n0x, n0y);
+    normalized_or((cy - by) * o, -(cx - bx) * o, 1.0f, 0.0f, n1x, n1y);
+    normalized_or((ay - cy) * o, -(ax - cx) * o, 1.0f, 0.0f, n2x, n2y);
+    SdfSample s = nearer(segment_sample(x, y, ax, ay, bx, by, n0x, n0y), segment_sample(x, y, bx, by, cx, cy, n1x, n1y));
+    s = nearer(s, segment_sample(x, y, cx, cy, ax, ay, n2x, n2y));
+    const float side_ab = (tbx * tpy - tby * tpx) * o;
+    const float side_bc = ((tcx - tbx) * (tpy - tby) - (tcy - tby) * (tpx - tbx)) * o;
+    const float side_ca = ((-tcx) * (tpy - tcy) - (-tcy) * (tpx - tcx)) * o;
+    if (area != 0.0f && x >= lox && y >= loy && x <= hix && y <= hiy && side_ab >= 0.0f && side_bc >= 0.0f &&
+        side_ca >= 0.0f)
+        s = SdfSample{-s.d, -s.nx, -s.ny};
+    return SdfSample{s.d - fmaxf(corner, 0.0f), s.nx, s.ny};
+}
+
+// checkerboard_sdf_sample (shared/sdf/effects.hlsli:8-36): the cells of even
+// parity, inside the rectangle. 
+__device__ __forceinline__ SdfSample checkerboard_sample(float x, float y, float x0, float y0, float x1, float y1,
+                                                             float cell_raw) {
+    const float left = fminf(x0, x1), top = fminf(y0, y1), right = fmaxf(x0, x1), bottom = fmaxf(y0, y1);
+    const SdfSample outer = rect_sample(x, y, left, top, right, bottom, 0.0f, 0.0f, 0.0f, 0.0f);
+    const float cell = fmaxf(cell_raw, 0.000001f);
+    const float cell_x = floorf((x - left) / cell), cell_y = floorf((y - top) / cell);
+    const float lx = rem_euclid_f32(x - left, cell), ly = rem_euclid_f32(y - top, cell);
+    float e = lx, nx = 1.0f, ny = 0.0f;
+    if (cell - lx < e) { e = cell - lx; nx = -1.0f; ny = 0.0f; }
+    if (ly < e) { e = ly; nx = 0.0f; ny = 1.0f; }
+    if (cell - ly < e) { e = cell - ly; nx = 0.0f; ny = -1.0f; }
+    const bool filled = ((uint32_t(f2i(cell_x)) + uint32_t(f2i(cell_y))) & 1u) == 0u;
+    return farther(outer, SdfSample{filled ? -e : e, nx, ny});
+}
+
+// line_segment_sdf_sample (shared/sdf/line.hlsli:16-26) in the line's frame.
+__device__ __forceinline__ SdfSample dash_segment(float axis, float normal, float start, float end, float he, float cap) {
+    if (cap < 0.5f) return line_rect(axis, normal, start, end, he);
+    if (cap < 1.5f) return line_rect(axis, normal, start - he, end + he, he);
+    const float nearest = fminf(fmaxf(axis, start), end);
+    const float dx = axis - nearest;
+    SdfSample s;
+    s.d = sdf_length(dx, normal) - he;
+    normalized_or(dx, normal, 0.0f, 1.0f, s.nx, s.ny);
+    return s;
+}
+
+// The dashes of dash_line_sdf_sample (shared/sdf/line.hlsli:28-39, 78-105):
+// the nearest of the dashes before, under and after the point along the
+// line; `s` (the plain line's sample) when there are no gaps.
+__device__ __forceinline__ SdfSample dash_sample(SdfSample s, float x, float y, float sx, float sy, float ex,
+                                                     float ey, float width, float cap, float dash_raw, float gap_raw,
+                                                     float offset_raw) {
+    const float dash = fmaxf(dash_raw, 0.0f), gap = fmaxf(gap_raw, 0.0f);
+    if (!(dash > 0.0f && gap > 0.0f)) return s;
+    const float he = fmaxf(width, 0.0f) * 0.5f;
+    const float dx = ex - sx, dy = ey - sy;
+    const float len = sdf_length(dx, dy);
+    if (!(len > 0.0f)) return s;
+    const float ux = dx / len, uy = dy / len;
+    const float px = x - sx, py = y - sy;
+    const float axis = px * ux + py * uy;
+    const float normal = -px * uy + py * ux;
+    const float cycle = dash + gap;
+    const float offset = rem_euclid_f32(offset_raw, cycle);
+    const float base = floorf((axis + offset) / cycle);
+    // dash_line_segment_sample for dash index ix
+    auto dash_at = [&](float ix) {
+        const float dash_start = ix * cycle - offset, dash_end = dash_start + dash;
+        SdfSample d{__int_as_float(0x7f800000), 1.0f, 0.0f};
+        if (dash_end > 0.0f && dash_start < len) {
+            const float start = fmaxf(dash_start, 0.0f), end = fminf(dash_end, len);
+            if (end > start) d = dash_segment(axis, normal, start, end, he, cap);
+        }
+        return d;
+    };
+    const SdfSample l = nearer(nearer(dash_at(base - 1.0f), dash_at(base)), dash_at(base + 1.0f));
+    return SdfSample{l.d, l.nx * ux - l.ny * uy, l.nx * uy + l.ny * ux};
+}
+
 // sdf_coverage_from_blob (shared/sdf/coverage.hlsli:13-236) for the record at
 // `w` (TK_SDF_RECORD_WORDS words), sampled at local point (x, y). The kinds
 // share one copy of each sampler: a shape (rect, circle or line) sampled in
@@ -185,12 +311,20 @@ __device__ __forceinline__ float sdf_word_f(const uint32_t* w, uint32_t i) { ret
 // shifted by their offset and weighted by their falloff. The operations and
 // their order per kind are those of the reference's per-kind branches; the
 // sharing only keeps the code small enough for the instruction cache.
+//
+// EXT adds the candlestick, dash line, triangle and checkerboard kinds; their
+// code costs the other kinds 18% and more of fine time (registers and
+// instruction cache), so scenes without them use the instance without.
+template <bool EXT>
 __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float y, const tk_affine& inv) {
     const uint32_t kind = __ldg(w);
-    const bool rect = kind == TK_SDF_RECT || kind == TK_SDF_RECT_STROKE || kind == TK_SDF_RECT_SHADOW;
+    const bool candle = EXT && kind == TK_SDF_CANDLESTICK;
+    const bool rect = kind == TK_SDF_RECT || kind == TK_SDF_RECT_STROKE || kind == TK_SDF_RECT_SHADOW || candle;
     const bool circle = kind == TK_SDF_CIRCLE || kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_CIRCLE_SHADOW;
-    const bool line = kind == TK_SDF_LINE || kind == TK_SDF_LINE_SHADOW;
-    if (!(rect || circle || line)) return 0.0f;
+    const bool dashed = EXT && kind == TK_SDF_DASH_LINE;
+    const bool line = kind == TK_SDF_LINE || kind == TK_SDF_LINE_SHADOW || dashed;
+    const bool triangle = EXT && kind == TK_SDF_TRIANGLE, checker = EXT && kind == TK_SDF_CHECKERBOARD;
+    if (!(rect || circle || line || triangle || checker)) return 0.0f;
     const bool shadow = kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW || kind == TK_SDF_LINE_SHADOW;
     const bool stroke = kind == TK_SDF_RECT_STROKE || kind == TK_SDF_CIRCLE_STROKE;
     const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
@@ -221,18 +355,43 @@ __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float 
         o[2] = radius + he;
         in[0] = x0; in[1] = y0; in[2] = radius - he;
         inner = radius > he;
+    } else if (candle) {
+        // candlestick_sdf_coverage (shared/sdf/effects.hlsli:38-70): the wick and
+        // the body, max of their coverages; words: centre x, high y, low y,
+        // body top y, body bottom y, body width, wick width
+        const float cx = x0, wh = fmaxf(r2, 1.0f) * 0.5f, bh = fmaxf(r1, 1.0f) * 0.5f;
+        o[0] = cx - wh; o[1] = fminf(y0, x1); o[2] = cx + wh; o[3] = fmaxf(y0, x1);
+        float by0 = fminf(y1, r0), by1 = fmaxf(y1, r0);
+        if (by0 == by1) {
+            by0 = by0 - 0.5f;
+            by1 = by1 + 0.5f;
+        }
+        in[0] = cx - bh; in[1] = by0; in[2] = cx + bh; in[3] = by1;
+        o[4] = o[5] = o[6] = o[7] = 0.0f;
+        inner = true;
     }
     float cov[2] = {0.0f, 0.0f};
     for (int pass = 0; pass < (inner ? 2 : 1); ++pass) {
         float q[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) q[k] = pass ? in[k] : o[k];
-        SdfSample s;
-        if (rect) s = rect_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
-        else if (circle) s = circle_sample(px, py, q[0], q[1], q[2]);
-        else s = line_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5]);
+        SdfSample s{0.0f, 1.0f, 0.0f};
+        if (rect) {
+            s = rect_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7]);
+        } else if (circle) {
+            s = circle_sample(px, py, q[0], q[1], q[2]);
+        } else if (line) {
+            s = line_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5]);
+            if (dashed)
+                s = dash_sample(s, px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], sdf_word_f(w, 9));
+        } else if (triangle) {
+            s = triangle_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6]);
+        } else if (checker) {
+            s = checkerboard_sample(px, py, q[0], q[1], q[2], q[3], q[4]);
+        }
         cov[pass] = shadow ? shadow_coverage(s, inv, expand, intensity) : coverage_from_sample(s, inv);
     }
+    if (candle) return fmaxf(cov[0], cov[1]);
     return stroke ? fminf(fmaxf(cov[0] - cov[1], 0.0f), 1.0f) : cov[0];
 }
 
