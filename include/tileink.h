@@ -109,6 +109,9 @@ extern "C" {
 #define TK_SDF_DASH_LINE 12u
 #define TK_SDF_TRIANGLE 13u
 #define TK_SDF_CHECKERBOARD 14u
+#define TK_SDF_CALLOUT 17u
+#define TK_SDF_CALLOUT_STROKE 18u
+#define TK_SDF_CALLOUT_SHADOW 19u
 #define TK_SDF_CAP_BUTT 0u
 #define TK_SDF_CAP_SQUARE 1u
 #define TK_SDF_CAP_ROUND 2u

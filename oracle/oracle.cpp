@@ -687,6 +687,29 @@ SdfS sdf_triangle(float x, float y, float ax, float ay, float bx, float by, floa
         r = {-r.dist, -r.nx, -r.ny};
     return {r.dist - fmax_(corner, 0.0f), r.nx, r.ny};
 }
+// callout_sdf_sample (shared/sdf/polygon.hlsli:87-136)
+SdfS sdf_callout(float x, float y, float x0r, float y0r, float x1r, float y1r, float body_radius, float tail_offset,
+                 float tail_width, float tail_length, float tail_radius, float side, float visible) {
+    float x0 = fmin_(x0r, x1r), y0 = fmin_(y0r, y1r), x1 = fmax_(x0r, x1r), y1 = fmax_(y0r, y1r);
+    SdfS body = sdf_rect(x, y, x0, y0, x1, y1, body_radius, body_radius, body_radius, body_radius);
+    if (visible < 0.5f) return body;
+    bool vertical = side < 0.5f || (side >= 1.5f && side < 2.5f);
+    float span = vertical ? x1 - x0 : y1 - y0;
+    float width = fmin_(fmax_(tail_width, 0.0f), span);
+    float half = width * 0.5f;
+    float center = clampf(tail_offset, half, fmax_(span - half, half));
+    float radius = clampf(tail_radius, 0.0f, fmin_(fmax_(half * 0.499f, 0.0f), fmax_(tail_length * 0.499f, 0.0f)));
+    float sh = half - radius, sl = tail_length - radius;
+    float a[2] = {x0 + center - sh, y0}, b[2] = {x0 + center + sh, y0}, c[2] = {x0 + center, y0 - sl};
+    if (side >= 0.5f && side < 1.5f) {
+        a[0] = x1; a[1] = y0 + center - sh; b[0] = x1; b[1] = y0 + center + sh; c[0] = x1 + sl; c[1] = y0 + center;
+    } else if (side >= 1.5f && side < 2.5f) {
+        a[0] = x0 + center - sh; a[1] = y1; b[0] = x0 + center + sh; b[1] = y1; c[0] = x0 + center; c[1] = y1 + sl;
+    } else if (side >= 2.5f) {
+        a[0] = x0; a[1] = y0 + center - sh; b[0] = x0; b[1] = y0 + center + sh; c[0] = x0 - sl; c[1] = y0 + center;
+    }
+    return sdf_nearer(body, sdf_triangle(x, y, a[0], a[1], b[0], b[1], c[0], c[1], radius));
+}
 // checkerboard_sdf_sample (shared/sdf/effects.hlsli:8-36)
 SdfS sdf_checkerboard(float x, float y, float x0, float y0, float x1, float y1, float cell_raw) {
     float left = fmin_(x0, x1), top = fmin_(y0, y1), right = fmax_(x0, x1), bottom = fmax_(y0, y1);
@@ -795,6 +818,15 @@ float sdf_blob_coverage(const uint32_t* w, float x, float y, const tk_affine& in
     if (kind == TK_SDF_DASH_LINE) return sdf_cov(sdf_dash_line(x, y, x0, y0, x1, y1, r0, r1, r2, r3, st), inv);
     if (kind == TK_SDF_TRIANGLE) return sdf_cov(sdf_triangle(x, y, x0, y0, x1, y1, r0, r1, r2), inv);
     if (kind == TK_SDF_CHECKERBOARD) return sdf_cov(sdf_checkerboard(x, y, x0, y0, x1, y1, r0), inv);
+    // callouts: words 9-12 tail radius, side, stroke half width, tail visible
+    if (kind == TK_SDF_CALLOUT) return sdf_cov(sdf_callout(x, y, x0, y0, x1, y1, r0, r1, r2, r3, st, sr, sl), inv);
+    if (kind == TK_SDF_CALLOUT_STROKE) {  // callout_stroke_sdf_sample (polygon.hlsli:138-156)
+        SdfS c = sdf_callout(x, y, x0, y0, x1, y1, r0, r1, r2, r3, st, sr, sl);
+        SdfS s{std::fabs(c.dist) - fmax_(sb, 0.0f), c.dist >= 0.0f ? c.nx : -c.nx, c.dist >= 0.0f ? c.ny : -c.ny};
+        return sdf_cov(s, inv);
+    }
+    if (kind == TK_SDF_CALLOUT_SHADOW)
+        return sdf_shadow_cov(sdf_callout(x - ox, y - oy, x0, y0, x1, y1, r0, r1, r2, r3, st, sr, sl), inv, ex, in);
     return 0.0f;
 }
 

@@ -64,13 +64,27 @@ def random_shapes(c, rng, n, w, h):
 
 def extended_shapes(c, rng, n, w, h):
     """n seeded shapes of the extended kinds (triangles, dash lines,
-    checkerboards, candlesticks), degenerate ones included."""
+    checkerboards, candlesticks, callouts and their strokes and shadows),
+    degenerate ones included."""
     for k in range(n):
         b = gradient(rng, w, h) if rng.uniform() < 0.25 else tk.Brush.solid(*rng.uniform(0, 1, 3),
                                                                           float(rng.choice([1.0, rng.uniform(0.2, 1)])))
         x0, y0 = rng.uniform(-20, w), rng.uniform(-20, h)
-        kind = k % 4
-        if kind == 0:
+        kind = k % 7
+        if kind >= 4:  # callouts: fill, stroke, shadow
+            rect = (x0, y0, x0 + rng.uniform(1, 160), y0 + rng.uniform(1, 120))
+            tail = None if rng.uniform() < 0.2 else (int(rng.integers(0, 4)), float(rng.uniform(-20, 180)),
+                                                     float(rng.uniform(0.5, 60)), float(rng.uniform(0.5, 40)),
+                                                     float(rng.uniform(0, 10)))
+            body_radius = float(rng.choice([0.0, rng.uniform(0, 30)]))
+            if kind == 4:
+                c.push_callout(rect, body_radius, tail, b)
+            elif kind == 5:
+                c.push_callout_stroke(rect, body_radius, tail, float(rng.uniform(0.5, 8)), b)
+            else:
+                c.push_callout_shadow(rect, body_radius, tail, b, offset=tuple(rng.uniform(-6, 6, 2)),
+                                      expand=float(rng.uniform(0, 8)), intensity=float(rng.uniform(0.2, 1)))
+        elif kind == 0:
             pts = [(x0, y0)] + [(x0 + rng.uniform(-90, 90), y0 + rng.uniform(-90, 90)) for _ in range(2)]
             if rng.uniform() < 0.1:
                 pts[2] = (pts[0][0] + 1e-3, pts[0][1] + 2e-3)  # a sliver

@@ -278,3 +278,37 @@ def test_oracle_extended_kinds_against_closed_forms():
     candle = sdf_words(N.SDF_CANDLESTICK, (20, 0, 60, 20), (40, 9, 1))
     assert coverage(candle, 20, 5) == pytest.approx(1.0) and coverage(candle, 24, 30) == pytest.approx(1.0)
     assert coverage(candle, 24.75, 30) == pytest.approx(0.25, abs=TOL) and coverage(candle, 24, 5) == 0.0
+
+
+def test_callout_bounds_match_the_reference():
+    """src/shared/sdf/callout.rs:279-340: a 100 x 40 body with radius 8 and a
+    tail (offset 50, width 10, length 6, radius 1.5) on each side, its stroke
+    and shadow, and the hidden tail."""
+    c = tk.Canvas(200, 120)
+    body, tail = (10, 20, 110, 60), (50.0, 10.0, 6.0, 1.5)
+    want = [(10, 14, 110, 60), (10, 20, 116, 60), (10, 20, 110, 66), (4, 20, 110, 60)]
+    for side in range(4):
+        assert record(c, c.push_callout(body, 8.0, (side,) + tail, SOLID))[2] == want[side]
+    assert record(c, c.push_callout_stroke(body, 8.0, (N.SIDE_BOTTOM,) + tail, 2.0, SOLID))[2] == (9, 19, 111, 67)
+    kind, f, pb = record(c, c.push_callout_shadow(body, 8.0, (N.SIDE_BOTTOM,) + tail, SOLID, offset=(0, 2), expand=4,
+                                                  intensity=0.5))
+    assert kind == N.SDF_CALLOUT_SHADOW and pb == (-7, 5, 127, 85)
+    assert list(f[:12]) == [10, 20, 110, 60, 8, 50, 10, 6, 1.5, 2, 0, 1]
+    assert record(c, c.push_callout(body, 8.0, None, SOLID))[2] == (10, 20, 110, 60)
+    assert record(c, c.push_callout_stroke(body, 8.0, None, 2.0, SOLID))[2] == (9, 19, 111, 61)
+    # empty: a flat body, a zero tail width, a zero stroke
+    assert c.push_callout((0, 0, 10, 0), 1.0, None, SOLID) is None
+    assert c.push_callout(body, 8.0, (0, 50.0, 0.0, 6.0, 1.5), SOLID) is None
+    assert c.push_callout_stroke(body, 8.0, None, 0.0, SOLID) is None
+
+
+def test_oracle_callout_coverage():
+    # body (0, 0)-(100, 40) radius 0, tail on the bottom: offset 50, width 20, length 10
+    w = sdf_words(N.SDF_CALLOUT, (0, 0, 100, 40), (0, 50, 20, 10), (0, N.SIDE_BOTTOM, 0, 1))
+    assert coverage(w, 20, 20) == 1.0 and coverage(w, 20, 45) == 0.0
+    assert coverage(w, 50, 44) == 1.0  # inside the tail
+    assert coverage(w, 50, 50.25) == pytest.approx(0.25, abs=TOL)  # just past the tail's tip
+    hidden = sdf_words(N.SDF_CALLOUT, (0, 0, 100, 40), (0, 50, 20, 10), (0, N.SIDE_BOTTOM, 0, 0))
+    assert coverage(hidden, 50, 44) == 0.0
+    stroke = sdf_words(N.SDF_CALLOUT_STROKE, (0, 0, 100, 40), (0, 50, 20, 10), (0, N.SIDE_BOTTOM, 1.5, 1))
+    assert coverage(stroke, 20, 20) == 0.0 and coverage(stroke, 0, 20) == 1.0

@@ -210,13 +210,14 @@ class Canvas:
 
     # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
     def _push_sdf(self, brush: Brush, kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0,
-                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0)):
+                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0), flags=0):
         s = N.SdfShape()
         s.kind, s.cap = kind, int(cap)
         s.p0[:] = [float(v) for v in p0]
         s.p1[:] = [float(v) for v in p1]
         s.p2[:] = [float(v) for v in p2]
         s.dash[:] = [float(v) for v in dash]
+        s.flags = int(flags)
         s.radius, s.width = float(radius), float(width)
         s.radii[:] = _four(radii)
         s.widths[:] = _four(widths)
@@ -280,6 +281,27 @@ class Canvas:
         a body between its top and bottom; widths whole pixels > 0."""
         return self._push_sdf(brush, N.SDF_CANDLESTICK, (center_x, high_y), (body_top_y, body_bottom_y),
                               p2=(low_y, 0.0), widths=(float(body_width), float(wick_width), 0.0, 0.0))
+
+    def _callout(self, brush, kind, rect, body_radius, tail, width=0.0, shadow=None):
+        if tail is None:  # CalloutTail::hidden()
+            return self._push_sdf(brush, kind, rect[:2], rect[2:], radius=body_radius, width=width, shadow=shadow,
+                                  cap=N.SIDE_BOTTOM, flags=1)
+        side, offset, tail_width, length, radius = tail
+        return self._push_sdf(brush, kind, rect[:2], rect[2:], radius=body_radius, width=width, shadow=shadow,
+                              cap=side, widths=(offset, tail_width, length, radius))
+
+    def push_callout(self, rect, body_radius, tail, brush: Brush):
+        """Canvas::push_callout: a rounded body (x0, y0, x1, y1) and a tail
+        (side, offset, width, length, corner radius), or tail None for none."""
+        return self._callout(brush, N.SDF_CALLOUT, rect, body_radius, tail)
+
+    def push_callout_stroke(self, rect, body_radius, tail, width, brush: Brush):
+        return self._callout(brush, N.SDF_CALLOUT_STROKE, rect, body_radius, tail, width=width)
+
+    def push_callout_shadow(self, rect, body_radius, tail, brush: Brush, offset=(0.0, 0.0), expand=0.0,
+                            intensity=1.0):
+        return self._callout(brush, N.SDF_CALLOUT_SHADOW, rect, body_radius, tail,
+                             shadow=(offset[0], offset[1], expand, intensity))
 
     def push_rect_shadow(self, x0, y0, x1, y1, brush: Brush, offset=(0.0, 0.0), expand=0.0, intensity=1.0,
                          radius=0.0):

@@ -725,7 +725,8 @@ bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_R
     std::memset(rec, 0, TK_SDF_RECORD_WORDS * 4);
     rec[0] = s.kind;
     auto put = [&](int i, float v) { rec[i] = fbits(v); };
-    const bool shadow = s.kind == TK_SDF_RECT_SHADOW || s.kind == TK_SDF_CIRCLE_SHADOW || s.kind == TK_SDF_LINE_SHADOW;
+    const bool shadow = s.kind == TK_SDF_RECT_SHADOW || s.kind == TK_SDF_CIRCLE_SHADOW ||
+                        s.kind == TK_SDF_LINE_SHADOW || s.kind == TK_SDF_CALLOUT_SHADOW;
     float opt[4] = {0, 0, 0, 0};
     if (shadow) {  // ShadowOptions::normalized, then physical_shadow_options
         const float intensity = std::min(std::max(s.shadow[3], 0.0f), 1.0f);
@@ -864,6 +865,54 @@ bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_R
             put(4, float(ay1));
             put(5, cell * sc);
             pb = box_bounds(ax0, ay0, ax1, ay1);
+            return true;
+        }
+        case TK_SDF_CALLOUT:
+        case TK_SDF_CALLOUT_STROKE:
+        case TK_SDF_CALLOUT_SHADOW: {
+            // Callout::is_empty / physical / expanded_bounds (src/shared/sdf/callout.rs:83-195)
+            const bool visible = !(s.flags & TK_SDF_CALLOUT_TAIL_HIDDEN);
+            const float br = float(s.radius);
+            const float off = s.widths[0], tw = s.widths[1], tl = s.widths[2], tr = s.widths[3];
+            const double lx0 = std::min(s.p0[0], s.p1[0]), ly0 = std::min(s.p0[1], s.p1[1]);
+            const double lx1 = std::max(s.p0[0], s.p1[0]), ly1 = std::max(s.p0[1], s.p1[1]);
+            if (!std::isfinite(lx0) || !std::isfinite(ly0) || !std::isfinite(lx1) || !std::isfinite(ly1) ||
+                lx0 >= lx1 || ly0 >= ly1 || !std::isfinite(br) || br < 0.0f || s.cap > 3u)
+                return false;
+            if (visible && (!std::isfinite(off) || !std::isfinite(tw) || tw <= 0.0f || !std::isfinite(tl) ||
+                            tl <= 0.0f || !std::isfinite(tr) || tr < 0.0f))
+                return false;
+            float half = 0.0f;
+            if (s.kind == TK_SDF_CALLOUT_STROKE) {  // CalloutStroke::is_empty
+                const float hl = float(s.width) * 0.5f;
+                if (!std::isfinite(hl) || hl <= 0.0f) return false;
+                half = hl * sc;
+            }
+            const double ax0 = std::min(x0, x1), ay0 = std::min(y0, y1), ax1 = std::max(x0, x1), ay1 = std::max(y0, y1);
+            const float ptl = visible ? tl * sc : 0.0f;
+            put(1, float(ax0));
+            put(2, float(ay0));
+            put(3, float(ax1));
+            put(4, float(ay1));
+            put(5, br * sc);
+            put(6, visible ? off * sc : 0.0f);
+            put(7, visible ? tw * sc : 0.0f);
+            put(8, ptl);
+            put(9, visible ? tr * sc : 0.0f);
+            put(10, visible ? float(s.cap) : 2.0f);  // a hidden tail is CalloutTail::hidden(): bottom, zeros
+            put(11, half);
+            put(12, visible ? 1.0f : 0.0f);
+            double bx0 = ax0, by0 = ay0, bx1 = ax1, by1 = ay1;
+            if (visible) {
+                const double t = double(ptl);
+                if (s.cap == 0u) by0 -= t;
+                else if (s.cap == 1u) bx1 += t;
+                else if (s.cap == 2u) by1 += t;
+                else bx0 -= t;
+            }
+            const double extra = double(std::max(half, 0.0f));
+            pb = box_bounds(bx0 - extra, by0 - extra, bx1 + extra, by1 + extra);
+            if (shadow) pb = shadow_bounds(pb, opt);
             return true;
         }
         case TK_SDF_CANDLESTICK: {
@@ -1013,7 +1062,8 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     const uint32_t k = shape->kind;
     if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
         k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW &&
-        k != TK_SDF_DASH_LINE && k != TK_SDF_TRIANGLE && k != TK_SDF_CHECKERBOARD && k != TK_SDF_CANDLESTICK)
+        k != TK_SDF_DASH_LINE && k != TK_SDF_TRIANGLE && k != TK_SDF_CHECKERBOARD && k != TK_SDF_CANDLESTICK &&
+        k != TK_SDF_CALLOUT && k != TK_SDF_CALLOUT_STROKE && k != TK_SDF_CALLOUT_SHADOW)
         return -1;
     // CandleStick::new and DashLine::new reject these (the reference panics)
     if (k == TK_SDF_CANDLESTICK && !(shape->widths[0] > 0.0f && shape->widths[1] > 0.0f)) return -1;
@@ -1026,7 +1076,8 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     uint32_t rec[TK_SDF_RECORD_WORDS];
     tk_pixel_bounds pb{0, 0, 0, 0};
     if (!encode_sdf(c, *shape, rec, pb)) return -2;
-    const bool shadow = k == TK_SDF_RECT_SHADOW || k == TK_SDF_CIRCLE_SHADOW || k == TK_SDF_LINE_SHADOW;
+    const bool shadow = k == TK_SDF_RECT_SHADOW || k == TK_SDF_CIRCLE_SHADOW || k == TK_SDF_LINE_SHADOW ||
+                        k == TK_SDF_CALLOUT_SHADOW;
     std::vector<uint32_t>& blob = shadow ? c->shadow : c->sdf;
     const uint32_t off = uint32_t(blob.size());
     blob.insert(blob.end(), rec, rec + TK_SDF_RECORD_WORDS);

@@ -242,6 +242,34 @@ __device__ __forceinline__ SdfSample triangle_sample(float x, float y, float ax,
     return SdfSample{s.d - fmaxf(corner, 0.0f), s.nx, s.ny};
 }
 
+// callout_sdf_sample (shared/sdf/polygon.hlsli:87-136): a rounded body and,
+// unless hidden, a rounded triangular tail on side 0 top, 1 right, 2 bottom
+// or 3 left, nearest of the two.
+__device__ __forceinline__ SdfSample callout_sample(float x, float y, float x0r, float y0r, float x1r, float y1r,
+                                                    float body_radius, float tail_offset, float tail_width,
+                                                    float tail_length, float tail_radius, float side, float visible) {
+    const float x0 = fminf(x0r, x1r), y0 = fminf(y0r, y1r), x1 = fmaxf(x0r, x1r), y1 = fmaxf(y0r, y1r);
+    const SdfSample body = rect_sample(x, y, x0, y0, x1, y1, body_radius, body_radius, body_radius, body_radius);
+    if (visible < 0.5f) return body;
+    const bool vertical = side < 0.5f || (side >= 1.5f && side < 2.5f);
+    const float span = vertical ? x1 - x0 : y1 - y0;
+    const float width = fminf(fmaxf(tail_width, 0.0f), span);
+    const float hw = width * 0.5f;
+    const float center = fminf(fmaxf(tail_offset, hw), fmaxf(span - hw, hw));
+    const float radius =
+        fminf(fmaxf(tail_radius, 0.0f), fminf(fmaxf(hw * 0.499f, 0.0f), fmaxf(tail_length * 0.499f, 0.0f)));
+    const float shw = hw - radius, sl = tail_length - radius;
+    float ax = x0 + center - shw, ay = y0, bx = x0 + center + shw, by = y0, cx = x0 + center, cy = y0 - sl;
+    if (side >= 0.5f && side < 1.5f) {
+        ax = x1; ay = y0 + center - shw; bx = x1; by = y0 + center + shw; cx = x1 + sl; cy = y0 + center;
+    } else if (side >= 1.5f && side < 2.5f) {
+        ax = x0 + center - shw; ay = y1; bx = x0 + center + shw; by = y1; cx = x0 + center; cy = y1 + sl;
+    } else if (side >= 2.5f) {
+        ax = x0; ay = y0 + center - shw; bx = x0; by = y0 + center + shw; cx = x0 - sl; cy = y0 + center;
+    }
+    return nearer(body, triangle_sample(x, y, ax, ay, bx, by, cx, cy, radius));
+}
+
 // checkerboard_sdf_sample (shared/sdf/effects.hlsli:8-36): the cells of even
 // parity, inside the rectangle. 
 __device__ __forceinline__ SdfSample checkerboard_sample(float x, float y, float x0, float y0, float x1, float y1,
@@ -312,7 +340,8 @@ __device__ __forceinline__ SdfSample dash_sample(SdfSample s, float x, float y, 
 // their order per kind are those of the reference's per-kind branches; the
 // sharing only keeps the code small enough for the instruction cache.
 //
-// EXT adds the candlestick, dash line, triangle and checkerboard kinds; their
+// EXT adds the candlestick, dash line, triangle, checkerboard and callout
+// kinds; their
 // code costs the other kinds 18% and more of fine time (registers and
 // instruction cache), so scenes without them use the instance without.
 template <bool EXT>
@@ -324,8 +353,10 @@ __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float 
     const bool dashed = EXT && kind == TK_SDF_DASH_LINE;
     const bool line = kind == TK_SDF_LINE || kind == TK_SDF_LINE_SHADOW || dashed;
     const bool triangle = EXT && kind == TK_SDF_TRIANGLE, checker = EXT && kind == TK_SDF_CHECKERBOARD;
-    if (!(rect || circle || line || triangle || checker)) return 0.0f;
-    const bool shadow = kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW || kind == TK_SDF_LINE_SHADOW;
+    const bool callout = EXT && (kind == TK_SDF_CALLOUT || kind == TK_SDF_CALLOUT_STROKE || kind == TK_SDF_CALLOUT_SHADOW);
+    if (!(rect || circle || line || triangle || checker || callout)) return 0.0f;
+    const bool shadow = kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW || kind == TK_SDF_LINE_SHADOW ||
+                        (EXT && kind == TK_SDF_CALLOUT_SHADOW);
     const bool stroke = kind == TK_SDF_RECT_STROKE || kind == TK_SDF_CIRCLE_STROKE;
     const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
     const float r0 = sdf_word_f(w, 5), r1 = sdf_word_f(w, 6), r2 = sdf_word_f(w, 7), r3 = sdf_word_f(w, 8);
@@ -388,6 +419,13 @@ __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float 
             s = triangle_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6]);
         } else if (checker) {
             s = checkerboard_sample(px, py, q[0], q[1], q[2], q[3], q[4]);
+        } else if (callout) {
+            // words 9-12: tail radius, side, stroke half width, tail visible
+            s = callout_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], sdf_word_f(w, 9),
+                               sdf_word_f(w, 10), sdf_word_f(w, 12));
+            if (kind == TK_SDF_CALLOUT_STROKE)  // callout_stroke_sdf_sample (polygon.hlsli:138-156)
+                s = s.d >= 0.0f ? SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 11), 0.0f), s.nx, s.ny}
+                                : SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 11), 0.0f), -s.nx, -s.ny};
         }
         cov[pass] = shadow ? shadow_coverage(s, inv, expand, intensity) : coverage_from_sample(s, inv);
     }
