@@ -104,11 +104,15 @@ extern "C" {
 #define TK_SDF_CANDLESTICK 5u
 #define TK_SDF_LINE 6u
 #define TK_SDF_RECT_SHADOW 7u
+#define TK_SDF_ARC 8u
+#define TK_SDF_ARC_SHADOW 9u
 #define TK_SDF_CIRCLE_SHADOW 10u
 #define TK_SDF_LINE_SHADOW 11u
 #define TK_SDF_DASH_LINE 12u
 #define TK_SDF_TRIANGLE 13u
 #define TK_SDF_CHECKERBOARD 14u
+#define TK_SDF_STAR 15u
+#define TK_SDF_STAR_STROKE 16u
 #define TK_SDF_CALLOUT 17u
 #define TK_SDF_CALLOUT_STROKE 18u
 #define TK_SDF_CALLOUT_SHADOW 19u

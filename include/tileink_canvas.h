@@ -99,6 +99,11 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
  *   TK_SDF_CANDLESTICK    p0 = (centre x, high y), p1 = (body top y, body
  *                         bottom y), p2 = (low y, unused), widths[0] body and
  *                         widths[1] wick width (whole pixels, > 0)
+ *   TK_SDF_ARC            p0 centre; radius; width; cap; angle = start,
+ *                         sweep (radians)
+ *   TK_SDF_STAR(_STROKE)  p0 centre; radius (outer radius); widths[0] inner
+ *                         and widths[1] corner radius; angle[0] rotation;
+ *                         strokes: width (full stroke width)
  *   TK_SDF_CALLOUT(_STROKE)  p0, p1 body corners; radius (body corner
  *                         radius); cap = tail side (0 top, 1 right, 2 bottom,
  *                         3 left); widths = tail offset, width, length and
@@ -118,6 +123,7 @@ typedef struct tk_sdf_shape {
     float shadow[4];     /* offset x, offset y, expand (falloff length), intensity */
     float dash[3];       /* dash lines: dash length, gap length, dash offset */
     uint32_t flags;      /* callouts: TK_SDF_CALLOUT_TAIL_HIDDEN */
+    float angle[2];      /* arcs: start and sweep; stars: rotation */
 } tk_sdf_shape;
 #define TK_SDF_CALLOUT_TAIL_HIDDEN 1u
 /* Returns the draw index, -2 when the shape draws nothing (a non-positive

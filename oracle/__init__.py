@@ -57,6 +57,9 @@ def lib() -> C.CDLL:
         l.or_sdf_coverage.argtypes = [P, F32, F32, P]
         l.or_exp_nonpos.restype = F32
         l.or_exp_nonpos.argtypes = [F32]
+        l.or_sincos.argtypes = [F32, P, P]
+        l.or_atan2.restype = F32
+        l.or_atan2.argtypes = [F32, F32]
         l.or_interpret_sdf_draws.restype = I32
         l.or_interpret_sdf_draws.argtypes = [P, P]
         l.or_diff_loss.restype = C.c_double

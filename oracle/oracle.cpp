@@ -710,6 +710,157 @@ SdfS sdf_callout(float x, float y, float x0r, float y0r, float x1r, float y1r, f
     }
     return sdf_nearer(body, sdf_triangle(x, y, a[0], a[1], b[0], b[1], c[0], c[1], radius));
 }
+// The library's sin, cos and atan2 for the arc and star kinds, in double with
+// exactly rounded operations (Cody-Waite reduction by pi/2 with fdlibm's
+// two-part constant and Taylor polynomials of degree 19 / 18; atan by
+// reduction to |t| <= tan(pi/12) and its odd series to degree 27); restated so
+// that the two agree bit for bit. Their distance to the C library is checked
+// in the tests.
+void lib_sincos(float a, float& s, float& c) {
+    double x = double(a);
+    if (!(std::fabs(x) < 1.0e9)) {
+        s = c = std::numeric_limits<float>::quiet_NaN();
+        return;
+    }
+    const double pio2_hi = 1.57079632673412561417e+00, pio2_lo = 6.07710050650619224932e-11;
+    double k = std::floor(x * 0.63661977236758134308 + 0.5);
+    double r = (x - k * pio2_hi) - k * pio2_lo, r2 = r * r;
+    static const double sin_c[10] = {-1.0 / 121645100408832000.0, 1.0 / 355687428096000.0, -1.0 / 1307674368000.0,
+                                     1.0 / 6227020800.0, -1.0 / 39916800.0, 1.0 / 362880.0, -1.0 / 5040.0,
+                                     1.0 / 120.0, -1.0 / 6.0, 1.0};
+    static const double cos_c[9] = {1.0 / 6402373705728000.0, -1.0 / 20922789888000.0, 1.0 / 87178291200.0,
+                                    -1.0 / 479001600.0, 1.0 / 3628800.0, -1.0 / 40320.0, 1.0 / 720.0, -1.0 / 24.0,
+                                    0.5};
+    double ps = sin_c[0];
+    for (int i = 1; i < 10; ++i) ps = ps * r2 + sin_c[i];
+    double pc = cos_c[0];
+    for (int i = 1; i < 9; ++i) pc = pc * r2 + cos_c[i];
+    double sr = ps * r, cr = 1.0 - pc * r2;
+    int q = int(std::fmod(k, 4.0) + 4.0) & 3;
+    double vs[4] = {sr, cr, -sr, -cr}, vc[4] = {cr, -sr, -cr, sr};
+    s = float(vs[q]);
+    c = float(vc[q]);
+}
+float lib_atan2(float yf, float xf) {
+    double y = double(yf), x = double(xf), ax = std::fabs(x), ay = std::fabs(y);
+    bool swap = ay > ax;
+    double z = swap ? ax / ay : ay / ax;
+    const double sqrt3 = 1.73205080756887729353, pi6 = 0.52359877559829887308;
+    const double pi2 = 1.57079632679489661923, pi = 3.14159265358979323846;
+    bool reduce = z > 0.26794919243112270647;
+    double t = reduce ? (z * sqrt3 - 1.0) / (z + sqrt3) : z, t2 = t * t;
+    double p = 1.0 / 27.0;
+    for (int n = 25; n >= 1; n -= 2) p = p * t2 * -1.0 + 1.0 / double(n);
+    double a = p * t;
+    if (reduce) a = pi6 + a;
+    if (swap) a = pi2 - a;
+    if (x < 0.0) a = pi - a;
+    if (y < 0.0) a = -a;
+    return float(a);
+}
+// arc.hlsli:10-16
+bool arc_in_sweep(float angle, float start, float sweep) {
+    const float tau = 6.2831855f;
+    if (sweep >= 0.0f) return rem_euclid_f32(angle - start, tau) <= sweep;
+    return rem_euclid_f32(start - angle, tau) <= -sweep;
+}
+// arc.hlsli:18-34
+SdfS arc_cap_segment(float vx, float vy, float radius, float angle, float he, float sweep, bool end_cap) {
+    float inner = fmax_(radius - he, 0.0f), outer = radius + he, si, co;
+    lib_sincos(angle, si, co);
+    float dir = sweep >= 0.0f ? 1.0f : -1.0f;
+    float tx = -si * dir, ty = co * dir;
+    return sdf_segment(vx, vy, inner * co, inner * si, outer * co, outer * si, end_cap ? tx : -tx, end_cap ? ty : -ty);
+}
+// arc.hlsli:36-41
+SdfS arc_endpoint(float vx, float vy, float radius, float angle, float he) {
+    float si, co;
+    lib_sincos(angle, si, co);
+    float dx = vx - radius * co, dy = vy - radius * si;
+    SdfS r;
+    r.dist = sdf_len(dx, dy) - he;
+    sdf_unit_or(dx, dy, co, si, r.nx, r.ny);
+    return r;
+}
+// arc.hlsli:66-85
+SdfS arc_square_cap(float vx, float vy, float radius, float angle, float sweep, float x0, float x1, float he) {
+    float dir = sweep < 0.0f ? -1.0f : 1.0f, si, co;
+    lib_sincos(angle, si, co);
+    float tx = -si * dir, ty = co * dir;
+    float px = vx - radius * co, py = vy - radius * si;
+    SdfS l = sdf_line_rect(px * tx + py * ty, -px * ty + py * tx, x0, x1, he);
+    return {l.dist, l.nx * tx - l.ny * ty, l.nx * ty + l.ny * tx};
+}
+// arc_sdf_sample with arc_butt_sdf_sample (arc.hlsli:43-64, 87-123)
+SdfS sdf_arc(float x, float y, float cx, float cy, float radius_raw, float width_raw, float start, float sweep,
+             float cap) {
+    float radius = fmax_(radius_raw, 0.0f), width = fmax_(width_raw, 0.0f);
+    SdfS s{std::numeric_limits<float>::infinity(), 1.0f, 0.0f};
+    if (!(radius > 0.0f && width > 0.0f && sweep != 0.0f)) return s;
+    float vx = x - cx, vy = y - cy, len = sdf_len(vx, vy), he = width * 0.5f;
+    if (std::fabs(sweep) >= 6.2831855f) {
+        float nx, ny;
+        sdf_unit_or(vx, vy, 1.0f, 0.0f, nx, ny);
+        float sg = len >= radius ? 1.0f : -1.0f;
+        return {std::fabs(len - radius) - he, nx * sg, ny * sg};
+    }
+    auto caps = [&]() {
+        return sdf_nearer(arc_cap_segment(vx, vy, radius, start, he, sweep, false),
+                          arc_cap_segment(vx, vy, radius, start + sweep, he, sweep, true));
+    };
+    if (len == 0.0f) {
+        s = caps();
+    } else {
+        float angle = lib_atan2(vy, vx);
+        if (arc_in_sweep(angle, start, sweep)) {
+            float sg = len >= radius ? 1.0f : -1.0f;
+            s = {std::fabs(len - radius) - he, vx / len * sg, vy / len * sg};
+        } else {
+            s = caps();
+        }
+    }
+    if (cap > 1.5f) {
+        s = sdf_nearer(sdf_nearer(s, arc_endpoint(vx, vy, radius, start, he)),
+                       arc_endpoint(vx, vy, radius, start + sweep, he));
+    } else if (cap >= 0.5f) {
+        s = sdf_nearer(sdf_nearer(s, arc_square_cap(vx, vy, radius, start, sweep, -he, 0.0f, he)),
+                       arc_square_cap(vx, vy, radius, start + sweep, sweep, 0.0f, he, he));
+    }
+    return s;
+}
+// star_vertex / star_sdf_sample (polygon.hlsli:158-206)
+SdfS sdf_star(float x, float y, float cx, float cy, float outer, float inner, float corner, float rotation) {
+    float sn, cs;
+    lib_sincos(rotation, sn, cs);
+    float rx = x - cx, ry = y - cy;
+    float px = cs * rx + sn * ry, py = -sn * rx + cs * ry;
+    auto vertex = [&](uint32_t i, float& vx, float& vy) {
+        float r = (i & 1u) == 0u ? outer : inner, vs, vc;
+        lib_sincos(float(i) * 0.62831855f, vs, vc);
+        vx = vc * r;
+        vy = vs * r;
+    };
+    SdfS nearest{std::numeric_limits<float>::infinity(), 1.0f, 0.0f};
+    bool inside = false;
+    float qx, qy;
+    vertex(9u, qx, qy);
+    for (uint32_t i = 0; i < 10u; ++i) {
+        float ux, uy;
+        vertex(i, ux, uy);
+        float ex = ux - qx, ey = uy - qy, fx, fy;
+        sdf_unit_or(ey, -ex, 1.0f, 0.0f, fx, fy);
+        nearest = sdf_nearer(nearest, sdf_segment(px, py, qx, qy, ux, uy, fx, fy));
+        if ((qy > py) != (uy > py)) {
+            float fraction = (py - qy) / (uy - qy);
+            float crossing = qx + fraction * (ux - qx);
+            if (px < crossing) inside = !inside;
+        }
+        qx = ux;
+        qy = uy;
+    }
+    if (inside) nearest = {-nearest.dist, -nearest.nx, -nearest.ny};
+    return {nearest.dist - fmax_(corner, 0.0f), cs * nearest.nx - sn * nearest.ny, sn * nearest.nx + cs * nearest.ny};
+}
 // checkerboard_sdf_sample (shared/sdf/effects.hlsli:8-36)
 SdfS sdf_checkerboard(float x, float y, float x0, float y0, float x1, float y1, float cell_raw) {
     float left = fmin_(x0, x1), top = fmin_(y0, y1), right = fmax_(x0, x1), bottom = fmax_(y0, y1);
@@ -827,6 +978,17 @@ float sdf_blob_coverage(const uint32_t* w, float x, float y, const tk_affine& in
     }
     if (kind == TK_SDF_CALLOUT_SHADOW)
         return sdf_shadow_cov(sdf_callout(x - ox, y - oy, x0, y0, x1, y1, r0, r1, r2, r3, st, sr, sl), inv, ex, in);
+    // arcs: centre, radius, width; start angle, sweep, cap
+    if (kind == TK_SDF_ARC) return sdf_cov(sdf_arc(x, y, x0, y0, x1, y1, r0, r1, r2), inv);
+    if (kind == TK_SDF_ARC_SHADOW) return sdf_shadow_cov(sdf_arc(x - ox, y - oy, x0, y0, x1, y1, r0, r1, r2), inv, ex, in);
+    // stars: centre, outer and inner radius; corner radius, rotation; stroke half width
+    if (kind == TK_SDF_STAR) return sdf_cov(sdf_star(x, y, x0, y0, x1, y1, r0, r1), inv);
+    if (kind == TK_SDF_STAR_STROKE) {  // star_stroke_sdf_sample (polygon.hlsli:208-221)
+        SdfS c = sdf_star(x, y, x0, y0, x1, y1, r0, r1);
+        return sdf_cov({std::fabs(c.dist) - fmax_(st, 0.0f), c.dist >= 0.0f ? c.nx : -c.nx,
+                        c.dist >= 0.0f ? c.ny : -c.ny},
+                       inv);
+    }
     return 0.0f;
 }
 
@@ -1822,6 +1984,8 @@ float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine*
     return sdf_blob_coverage(record, x, y, *inv);
 }
 float or_exp_nonpos(float x) { return exp_nonpos(x); }
+void or_sincos(float x, float* s, float* c) { lib_sincos(x, *s, *c); }
+float or_atan2(float y, float x) { return lib_atan2(y, x); }
 
 // Fine-only oracle (src/native/runtime/tests/coarse_count/rect_pixels.rs:3-13):
 // every draw interpreted as a PTCL_SDF particle in every tile, in draw-record

@@ -106,6 +106,9 @@ float or_fill_value(const tk_line_segment* segments, uint32_t count, int32_t bac
  * used by shadow falloffs. */
 float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine* inv);
 float or_exp_nonpos(float x);
+/* The library's sin / cos and atan2 for the arc and star kinds. */
+void or_sincos(float x, float* s, float* c);
+float or_atan2(float y, float x);
 /* Fine-only image of a scene of SDF draws: every draw interpreted in every
  * tile as a PTCL_SDF particle, from the clear colour (no coarse stage). */
 int32_t or_interpret_sdf_draws(const tk_scene_desc* scene, uint32_t* image);

@@ -64,14 +64,30 @@ def random_shapes(c, rng, n, w, h):
 
 def extended_shapes(c, rng, n, w, h):
     """n seeded shapes of the extended kinds (triangles, dash lines,
-    checkerboards, candlesticks, callouts and their strokes and shadows),
-    degenerate ones included."""
+    checkerboards, candlesticks, callouts, arcs and stars, with their
+    strokes and shadows), degenerate ones included."""
     for k in range(n):
         b = gradient(rng, w, h) if rng.uniform() < 0.25 else tk.Brush.solid(*rng.uniform(0, 1, 3),
                                                                           float(rng.choice([1.0, rng.uniform(0.2, 1)])))
         x0, y0 = rng.uniform(-20, w), rng.uniform(-20, h)
-        kind = k % 7
-        if kind >= 4:  # callouts: fill, stroke, shadow
+        kind = k % 11
+        if kind >= 7:  # arcs and stars, fill, stroke and shadow
+            r = float(rng.uniform(2, 80))
+            if kind == 7:
+                c.push_sdf_arc(x0, y0, r, float(rng.uniform(-7, 7)), float(rng.choice([rng.uniform(-7, 7), 6.3, -0.01])),
+                               float(rng.uniform(0.5, 12)), b, cap=int(rng.integers(0, 3)))
+            elif kind == 8:
+                c.push_arc_shadow(x0, y0, r, float(rng.uniform(-7, 7)), float(rng.uniform(-7, 7)),
+                                  float(rng.uniform(0.5, 12)), b, offset=tuple(rng.uniform(-5, 5, 2)),
+                                  expand=float(rng.uniform(0, 6)), intensity=float(rng.uniform(0.2, 1)),
+                                  cap=int(rng.integers(0, 3)))
+            elif kind == 9:
+                c.push_star(x0, y0, r, r * float(rng.uniform(0.2, 0.95)), b, corner_radius=float(rng.uniform(0, 4)),
+                            rotation=float(rng.uniform(-4, 4)))
+            else:
+                c.push_star_stroke(x0, y0, r, r * float(rng.uniform(0.2, 0.95)), float(rng.uniform(0.5, 6)), b,
+                                   corner_radius=float(rng.uniform(0, 4)), rotation=float(rng.uniform(-4, 4)))
+        elif kind >= 4:  # callouts: fill, stroke, shadow
             rect = (x0, y0, x0 + rng.uniform(1, 160), y0 + rng.uniform(1, 120))
             tail = None if rng.uniform() < 0.2 else (int(rng.integers(0, 4)), float(rng.uniform(-20, 180)),
                                                      float(rng.uniform(0.5, 60)), float(rng.uniform(0.5, 40)),

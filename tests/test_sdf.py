@@ -312,3 +312,54 @@ def test_oracle_callout_coverage():
     assert coverage(hidden, 50, 44) == 0.0
     stroke = sdf_words(N.SDF_CALLOUT_STROKE, (0, 0, 100, 40), (0, 50, 20, 10), (0, N.SIDE_BOTTOM, 1.5, 1))
     assert coverage(stroke, 20, 20) == 0.0 and coverage(stroke, 0, 20) == 1.0
+
+
+def test_arc_and_star_bounds_match_the_reference():
+    c = tk.Canvas(100, 100)
+    # src/shared/sdf/arc.rs (tests): radius 10 at (20, 20), sweep pi, width 4 -> (7, 17, 33, 33)
+    kind, f, pb = record(c, c.push_sdf_arc(20, 20, 10, 0.0, math.pi, 4, SOLID))
+    assert kind == N.SDF_ARC and pb == (7, 17, 33, 33)
+    assert list(f[:7]) == [20, 20, 10, 4, 0, np.float32(math.pi), N.CAP_BUTT]
+    # src/shared/sdf/star.rs (tests): star at (16, 20), radii 8 / 3.5, corner 1.25, rotation -pi/2
+    kind, f, pb = record(c, c.push_star(16, 20, 8, 3.5, SOLID, corner_radius=1.25, rotation=-math.pi / 2))
+    assert kind == N.SDF_STAR and pb == (7, 10, 25, 28)
+    assert record(c, c.push_star_stroke(16, 20, 8, 3.5, 2.5, SOLID, corner_radius=1.25,
+                                        rotation=-math.pi / 2))[2] == (5, 9, 27, 29)
+    kind, f, pb = record(c, c.push_arc_shadow(50, 50, 20, 1.0, -2.0, 3, SOLID, offset=(1, 2), expand=2,
+                                              intensity=0.5, cap=N.CAP_ROUND))
+    assert kind == N.SDF_ARC_SHADOW and list(f[12:16]) == [1, 2, 2, 0.5]
+    # the reference's None: zero sweep, inner radius not below outer
+    assert c.push_sdf_arc(20, 20, 10, 0.0, 0.0, 4, SOLID) is None
+    assert c.push_star(16, 20, 3, 3, SOLID) is None
+
+
+def test_oracle_trig_is_correctly_rounded():
+    lib = oracle.lib()
+    rng = np.random.default_rng(3)
+    xs = np.concatenate([rng.uniform(-30, 30, 3000), [0.0, math.pi, -math.pi / 2, 1e-7, 700.25]]).astype(np.float32)
+    s, c = C.c_float(), C.c_float()
+    for x in xs:
+        lib.or_sincos(float(x), C.byref(s), C.byref(c))
+        for got, ref in ((s.value, math.sin(float(x))), (c.value, math.cos(float(x)))):
+            assert abs(got - ref) <= 0.5 * abs(float(np.spacing(np.float32(ref)))) * (1 + 1e-6), (x, got, ref)
+    for y, x in rng.uniform(-50, 50, (3000, 2)).astype(np.float32):
+        ref = math.atan2(float(y), float(x))
+        assert abs(lib.or_atan2(float(y), float(x)) - ref) <= 0.5 * abs(float(np.spacing(np.float32(ref)))) * (1 + 1e-6)
+
+
+def test_oracle_arc_and_star_coverage():
+    # a half ring of radius 20, width 4, from angle 0 over pi (y grows downwards: the lower half)
+    arc = sdf_words(N.SDF_ARC, (0, 0, 20, 4), (0, math.pi, N.CAP_BUTT))
+    assert coverage(arc, 0, 20) == 1.0 and coverage(arc, 0, -20) == 0.0 and coverage(arc, 0, 0) == 0.0
+    assert coverage(arc, 0, 22.25) == pytest.approx(0.25, abs=TOL)
+    # a round cap reaches half the width past the end at (20, 0)
+    round_arc = sdf_words(N.SDF_ARC, (0, 0, 20, 4), (0, math.pi, N.CAP_ROUND))
+    assert coverage(round_arc, 20, -1.75) == pytest.approx(0.75, abs=1e-4) and coverage(arc, 20, -1.75) == 0.0
+    # a star of outer radius 30, inner 12: its centre inside, far points outside
+    star = sdf_words(N.SDF_STAR, (50, 50, 30, 12), (0, 0))
+    assert coverage(star, 50, 50) == 1.0 and coverage(star, 50, 10) == 0.0
+    # a quarter pixel inside the tip at angle 0: the edges meet there at +-h from the axis, so
+    # the nearest edge is 0.25 sin(h) away
+    ix, iy = 12 * math.cos(math.pi / 5), 12 * math.sin(math.pi / 5)
+    h = math.atan2(iy, 30 - ix)
+    assert coverage(star, 79.75, 50) == pytest.approx(0.5 + 0.25 * math.sin(h), abs=1e-4)

@@ -35,6 +35,7 @@ SDF_RECT, SDF_CIRCLE, SDF_RECT_STROKE, SDF_CIRCLE_STROKE, SDF_LINE = 1, 2, 3, 4,
 SDF_RECT_SHADOW, SDF_CIRCLE_SHADOW, SDF_LINE_SHADOW = 7, 10, 11
 SDF_CANDLESTICK, SDF_DASH_LINE, SDF_TRIANGLE, SDF_CHECKERBOARD = 5, 12, 13, 14
 SDF_CALLOUT, SDF_CALLOUT_STROKE, SDF_CALLOUT_SHADOW = 17, 18, 19
+SDF_ARC, SDF_ARC_SHADOW, SDF_STAR, SDF_STAR_STROKE = 8, 9, 15, 16
 SIDE_TOP, SIDE_RIGHT, SIDE_BOTTOM, SIDE_LEFT = 0, 1, 2, 3
 SDF_RECORD_WORDS = 17
 CAP_BUTT, CAP_SQUARE, CAP_ROUND = 0, 1, 2
@@ -113,7 +114,7 @@ class SdfShape(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("cap", C.c_uint32), ("p0", C.c_double * 2), ("p1", C.c_double * 2),
                 ("p2", C.c_double * 2), ("radius", C.c_double), ("width", C.c_double), ("radii", C.c_float * 4),
                 ("widths", C.c_float * 4), ("shadow", C.c_float * 4), ("dash", C.c_float * 3),
-                ("flags", C.c_uint32)]
+                ("flags", C.c_uint32), ("angle", C.c_float * 2)]
 
 
 class FlattenDesc(C.Structure):

@@ -210,7 +210,8 @@ class Canvas:
 
     # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
     def _push_sdf(self, brush: Brush, kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0,
-                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0), flags=0):
+                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0), flags=0,
+                  angle=(0.0, 0.0)):
         s = N.SdfShape()
         s.kind, s.cap = kind, int(cap)
         s.p0[:] = [float(v) for v in p0]
@@ -218,6 +219,7 @@ class Canvas:
         s.p2[:] = [float(v) for v in p2]
         s.dash[:] = [float(v) for v in dash]
         s.flags = int(flags)
+        s.angle[:] = [float(v) for v in angle]
         s.radius, s.width = float(radius), float(width)
         s.radii[:] = _four(radii)
         s.widths[:] = _four(widths)
@@ -281,6 +283,27 @@ class Canvas:
         a body between its top and bottom; widths whole pixels > 0."""
         return self._push_sdf(brush, N.SDF_CANDLESTICK, (center_x, high_y), (body_top_y, body_bottom_y),
                               p2=(low_y, 0.0), widths=(float(body_width), float(wick_width), 0.0, 0.0))
+
+    def push_sdf_arc(self, cx, cy, radius, start_angle, sweep_angle, width, brush: Brush, cap=N.CAP_BUTT):
+        """Canvas::push_sdf_arc (SdfArc): a circular stroke from start_angle
+        over sweep_angle (radians); None when radius, width or sweep is 0."""
+        return self._push_sdf(brush, N.SDF_ARC, (cx, cy), radius=radius, width=width, cap=cap,
+                              angle=(start_angle, sweep_angle))
+
+    def push_arc_shadow(self, cx, cy, radius, start_angle, sweep_angle, width, brush: Brush, offset=(0.0, 0.0),
+                        expand=0.0, intensity=1.0, cap=N.CAP_BUTT):
+        return self._push_sdf(brush, N.SDF_ARC_SHADOW, (cx, cy), radius=radius, width=width, cap=cap,
+                              angle=(start_angle, sweep_angle), shadow=(offset[0], offset[1], expand, intensity))
+
+    def push_star(self, cx, cy, outer_radius, inner_radius, brush: Brush, corner_radius=0.0, rotation=0.0):
+        """Canvas::push_star (SdfStar): a five-point star; None for invalid radii."""
+        return self._push_sdf(brush, N.SDF_STAR, (cx, cy), radius=outer_radius,
+                              widths=(inner_radius, corner_radius, 0.0, 0.0), angle=(rotation, 0.0))
+
+    def push_star_stroke(self, cx, cy, outer_radius, inner_radius, width, brush: Brush, corner_radius=0.0,
+                         rotation=0.0):
+        return self._push_sdf(brush, N.SDF_STAR_STROKE, (cx, cy), radius=outer_radius, width=width,
+                              widths=(inner_radius, corner_radius, 0.0, 0.0), angle=(rotation, 0.0))
 
     def _callout(self, brush, kind, rect, body_radius, tail, width=0.0, shadow=None):
         if tail is None:  # CalloutTail::hidden()

@@ -271,8 +271,9 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             const uint32_t kind = (plain ? d.sdf_blob : d.sdf_shadow_blob)[off];
             const bool ext = plain ? (kind == TK_SDF_CANDLESTICK || kind == TK_SDF_DASH_LINE || kind == TK_SDF_TRIANGLE ||
                                       kind == TK_SDF_CHECKERBOARD || kind == TK_SDF_CALLOUT ||
-                                      kind == TK_SDF_CALLOUT_STROKE)
-                                   : kind == TK_SDF_CALLOUT_SHADOW;
+                                      kind == TK_SDF_CALLOUT_STROKE || kind == TK_SDF_ARC ||
+                                      kind == TK_SDF_STAR || kind == TK_SDF_STAR_STROKE)
+                                   : (kind == TK_SDF_CALLOUT_SHADOW || kind == TK_SDF_ARC_SHADOW);
             const bool ok = ext || (plain ? (kind == TK_SDF_RECT || kind == TK_SDF_CIRCLE || kind == TK_SDF_RECT_STROKE ||
                                              kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_LINE)
                                           : (kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW ||

@@ -726,7 +726,7 @@ bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_R
     rec[0] = s.kind;
     auto put = [&](int i, float v) { rec[i] = fbits(v); };
     const bool shadow = s.kind == TK_SDF_RECT_SHADOW || s.kind == TK_SDF_CIRCLE_SHADOW ||
-                        s.kind == TK_SDF_LINE_SHADOW || s.kind == TK_SDF_CALLOUT_SHADOW;
+                        s.kind == TK_SDF_LINE_SHADOW || s.kind == TK_SDF_CALLOUT_SHADOW || s.kind == TK_SDF_ARC_SHADOW;
     float opt[4] = {0, 0, 0, 0};
     if (shadow) {  // ShadowOptions::normalized, then physical_shadow_options
         const float intensity = std::min(std::max(s.shadow[3], 0.0f), 1.0f);
@@ -865,6 +865,82 @@ bool encode_sdf(const tk_canvas* c, const tk_sdf_shape& s, uint32_t rec[TK_SDF_R
             put(4, float(ay1));
             put(5, cell * sc);
             pb = box_bounds(ax0, ay0, ax1, ay1);
+            return true;
+        }
+        case TK_SDF_ARC:
+        case TK_SDF_ARC_SHADOW: {
+            // Rc::is_empty / bounds (src/shared/sdf/arc.rs:43-98) of the physical arc
+            const float r = float(s.radius), wd = float(s.width), start = s.angle[0], sweep = s.angle[1];
+            if (s.cap > TK_SDF_CAP_ROUND || r <= 0.0f || wd <= 0.0f || sweep == 0.0f) return false;
+            const float pr = r * sc, pw = wd * sc, cx = float(x0), cy = float(y0), half = pw * 0.5f;
+            put(1, cx);
+            put(2, cy);
+            put(3, pr);
+            put(4, pw);
+            put(5, start);
+            put(6, sweep);
+            put(7, float(s.cap));
+            const float tau = 6.2831855f;
+            if (std::fabs(sweep) >= tau) {
+                const float rr = pr + half;
+                pb = {sat_i32(std::floor(cx - rr)), sat_i32(std::floor(cy - rr)), sat_i32(std::ceil(cx + rr)),
+                      sat_i32(std::ceil(cy + rr))};
+            } else {
+                float bx0 = INFINITY, by0 = INFINITY, bx1 = -INFINITY, by1 = -INFINITY;
+                auto include = [&](float a) {
+                    const float px = cx + pr * std::cos(a), py = cy + pr * std::sin(a);
+                    bx0 = std::min(bx0, px);
+                    by0 = std::min(by0, py);
+                    bx1 = std::max(bx1, px);
+                    by1 = std::max(by1, py);
+                };
+                auto norm = [&](float a) { return a - std::floor(a / tau) * tau; };  // normalize_angle
+                include(start);
+                include(start + sweep);
+                const float axes[4] = {0.0f, 1.5707964f, 3.1415927f, 3.1415927f + 1.5707964f};
+                for (float a : axes)
+                    if (sweep >= 0.0f ? norm(a - start) <= sweep : norm(start - a) <= -sweep) include(a);
+                const float outset = half + 1.0f;
+                pb = {sat_i32(std::floor(bx0 - outset)), sat_i32(std::floor(by0 - outset)),
+                      sat_i32(std::ceil(bx1 + outset)), sat_i32(std::ceil(by1 + outset))};
+            }
+            if (shadow) pb = shadow_bounds(pb, opt);
+            return true;
+        }
+        case TK_SDF_STAR:
+        case TK_SDF_STAR_STROKE: {
+            // Star::is_empty / expanded_bounds (src/shared/sdf/star.rs:37-90) of the physical star
+            const float outer = float(s.radius), inner = s.widths[0], corner = s.widths[1], rot = s.angle[0];
+            if (!std::isfinite(s.p0[0]) || !std::isfinite(s.p0[1]) || !std::isfinite(outer) || outer <= 0.0f ||
+                !std::isfinite(inner) || inner <= 0.0f || inner >= outer || !std::isfinite(corner) || corner < 0.0f ||
+                !std::isfinite(rot))
+                return false;
+            float half = 0.0f;
+            if (s.kind == TK_SDF_STAR_STROKE) {
+                const float hl = float(s.width) * 0.5f;
+                if (!std::isfinite(hl) || hl <= 0.0f) return false;
+                half = hl * sc;
+            }
+            const float po = outer * sc, pi_ = inner * sc, pc = corner * sc;
+            put(1, float(x0));
+            put(2, float(y0));
+            put(3, po);
+            put(4, pi_);
+            put(5, pc);
+            put(6, rot);
+            put(9, half);
+            double bx0 = INFINITY, by0 = INFINITY, bx1 = -INFINITY, by1 = -INFINITY;
+            for (int i = 0; i < 10; ++i) {
+                const double rr = double(i % 2 == 0 ? po : pi_);
+                const double a = double(rot) + double(i) * 3.14159265358979323846 / 5.0;
+                const double px = x0 + rr * std::cos(a), py = y0 + rr * std::sin(a);
+                bx0 = std::min(bx0, px);
+                by0 = std::min(by0, py);
+                bx1 = std::max(bx1, px);
+                by1 = std::max(by1, py);
+            }
+            const double e = double(pc) + double(half);
+            pb = box_bounds(bx0 - e, by0 - e, bx1 + e, by1 + e);
             return true;
         }
         case TK_SDF_CALLOUT:
@@ -1063,7 +1139,8 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
         k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW &&
         k != TK_SDF_DASH_LINE && k != TK_SDF_TRIANGLE && k != TK_SDF_CHECKERBOARD && k != TK_SDF_CANDLESTICK &&
-        k != TK_SDF_CALLOUT && k != TK_SDF_CALLOUT_STROKE && k != TK_SDF_CALLOUT_SHADOW)
+        k != TK_SDF_CALLOUT && k != TK_SDF_CALLOUT_STROKE && k != TK_SDF_CALLOUT_SHADOW && k != TK_SDF_ARC &&
+        k != TK_SDF_ARC_SHADOW && k != TK_SDF_STAR && k != TK_SDF_STAR_STROKE)
         return -1;
     // CandleStick::new and DashLine::new reject these (the reference panics)
     if (k == TK_SDF_CANDLESTICK && !(shape->widths[0] > 0.0f && shape->widths[1] > 0.0f)) return -1;
@@ -1077,7 +1154,7 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     tk_pixel_bounds pb{0, 0, 0, 0};
     if (!encode_sdf(c, *shape, rec, pb)) return -2;
     const bool shadow = k == TK_SDF_RECT_SHADOW || k == TK_SDF_CIRCLE_SHADOW || k == TK_SDF_LINE_SHADOW ||
-                        k == TK_SDF_CALLOUT_SHADOW;
+                        k == TK_SDF_CALLOUT_SHADOW || k == TK_SDF_ARC_SHADOW;
     std::vector<uint32_t>& blob = shadow ? c->shadow : c->sdf;
     const uint32_t off = uint32_t(blob.size());
     blob.insert(blob.end(), rec, rec + TK_SDF_RECORD_WORDS);

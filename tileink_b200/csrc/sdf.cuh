@@ -242,6 +242,209 @@ __device__ __forceinline__ SdfSample triangle_sample(float x, float y, float ax,
     return SdfSample{s.d - fmaxf(corner, 0.0f), s.nx, s.ny};
 }
 
+// ---------------------------------------------------------------------------
+// Trigonometry for the arc and star kinds, evaluated in double with exactly
+// rounded operations only, so host and device agree bit for bit (the float
+// results are within half an ulp of sin, cos and atan2 over the tested
+// ranges).
+//   sin, cos: x = k pi/2 + r (Cody-Waite reduction with fdlibm's two-part
+//   pi/2, exact products for |k| < 2^20), sin r and cos r by their Taylor
+//   polynomials of degree 19 and 18 (|r| <= pi/4), the quadrant from k mod 4.
+//   atan2: the angle of the smaller over the larger coordinate in [0, 1],
+//   reduced by atan z = pi/6 + atan((z sqrt3 - 1)/(z + sqrt3)) above
+//   tan(pi/12), the odd series to degree 27, then placed in its quadrant.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sdf_sincos(float a, float& s, float& c) {
+    const double x = double(a);
+    if (!(fabs(x) < 1.0e9)) {
+        s = c = __int_as_float(0x7fc00000);
+        return;
+    }
+    const double pio2_hi = 1.57079632673412561417e+00, pio2_lo = 6.07710050650619224932e-11;
+    const double k = floor(x * 0.63661977236758134308 + 0.5);
+    const double r = (x - k * pio2_hi) - k * pio2_lo;
+    const double r2 = r * r;
+    // sin r = r (1 - r^2/3! + ... - r^18/19!), cos r = 1 - r^2/2! + ... + r^18/18!
+    double ps = -1.0 / 121645100408832000.0;
+    ps = ps * r2 + 1.0 / 355687428096000.0;
+    ps = ps * r2 - 1.0 / 1307674368000.0;
+    ps = ps * r2 + 1.0 / 6227020800.0;
+    ps = ps * r2 - 1.0 / 39916800.0;
+    ps = ps * r2 + 1.0 / 362880.0;
+    ps = ps * r2 - 1.0 / 5040.0;
+    ps = ps * r2 + 1.0 / 120.0;
+    ps = ps * r2 - 1.0 / 6.0;
+    ps = ps * r2 + 1.0;
+    const double sr = ps * r;
+    double pc = 1.0 / 6402373705728000.0;
+    pc = pc * r2 - 1.0 / 20922789888000.0;
+    pc = pc * r2 + 1.0 / 87178291200.0;
+    pc = pc * r2 - 1.0 / 479001600.0;
+    pc = pc * r2 + 1.0 / 3628800.0;
+    pc = pc * r2 - 1.0 / 40320.0;
+    pc = pc * r2 + 1.0 / 720.0;
+    pc = pc * r2 - 1.0 / 24.0;
+    pc = pc * r2 + 0.5;
+    const double cr = 1.0 - pc * r2;
+    const int q = int(fmod(k, 4.0) + 4.0) & 3;
+    const double ss = q == 0 ? sr : (q == 1 ? cr : (q == 2 ? -sr : -cr));
+    const double cc = q == 0 ? cr : (q == 1 ? -sr : (q == 2 ? -cr : sr));
+    s = float(ss);
+    c = float(cc);
+}
+
+__device__ __forceinline__ float sdf_atan2(float yf, float xf) {
+    const double y = double(yf), x = double(xf);
+    const double ax = fabs(x), ay = fabs(y);
+    const bool swap = ay > ax;
+    const double z = swap ? ax / ay : ay / ax;  // in [0, 1]; NaN for 0/0 and inf/inf
+    const double sqrt3 = 1.73205080756887729353, pi6 = 0.52359877559829887308;
+    const double pi2 = 1.57079632679489661923, pi = 3.14159265358979323846;
+    const bool reduce = z > 0.26794919243112270647;
+    const double t = reduce ? (z * sqrt3 - 1.0) / (z + sqrt3) : z;
+    const double t2 = t * t;
+    double p = 1.0 / 27.0;
+    p = p * t2 * -1.0 + 1.0 / 25.0;
+    p = p * t2 * -1.0 + 1.0 / 23.0;
+    p = p * t2 * -1.0 + 1.0 / 21.0;
+    p = p * t2 * -1.0 + 1.0 / 19.0;
+    p = p * t2 * -1.0 + 1.0 / 17.0;
+    p = p * t2 * -1.0 + 1.0 / 15.0;
+    p = p * t2 * -1.0 + 1.0 / 13.0;
+    p = p * t2 * -1.0 + 1.0 / 11.0;
+    p = p * t2 * -1.0 + 1.0 / 9.0;
+    p = p * t2 * -1.0 + 1.0 / 7.0;
+    p = p * t2 * -1.0 + 1.0 / 5.0;
+    p = p * t2 * -1.0 + 1.0 / 3.0;
+    p = p * t2 * -1.0 + 1.0;
+    double a = p * t;
+    if (reduce) a = pi6 + a;
+    if (swap) a = pi2 - a;
+    if (x < 0.0) a = pi - a;
+    if (y < 0.0) a = -a;
+    return float(a);
+}
+
+// arc_angle_in_sweep (shared/sdf/arc.hlsli:10-16)
+__device__ __forceinline__ bool arc_in_sweep(float angle, float start, float sweep) {
+    const float tau = 6.2831855f;
+    if (sweep >= 0.0f) return rem_euclid_f32(angle - start, tau) <= sweep;
+    return rem_euclid_f32(start - angle, tau) <= -sweep;
+}
+
+// arc_cap_segment_sdf_sample (arc.hlsli:18-34)
+__device__ __forceinline__ SdfSample arc_cap_segment(float vx, float vy, float radius, float angle, float he,
+                                                     float sweep, bool end_cap) {
+    const float inner = fmaxf(radius - he, 0.0f), outer = radius + he;
+    float si, co;
+    sdf_sincos(angle, si, co);
+    const float dir = sweep >= 0.0f ? 1.0f : -1.0f;
+    const float tx = -si * dir, ty = co * dir;
+    return segment_sample(vx, vy, inner * co, inner * si, outer * co, outer * si, end_cap ? tx : -tx,
+                          end_cap ? ty : -ty);
+}
+
+// arc_endpoint_sdf_sample (arc.hlsli:36-41)
+__device__ __forceinline__ SdfSample arc_endpoint(float vx, float vy, float radius, float angle, float he) {
+    float si, co;
+    sdf_sincos(angle, si, co);
+    const float dx = vx - radius * co, dy = vy - radius * si;
+    SdfSample s;
+    s.d = sdf_length(dx, dy) - he;
+    normalized_or(dx, dy, co, si, s.nx, s.ny);
+    return s;
+}
+
+// arc_square_cap_sdf_sample (arc.hlsli:66-85)
+__device__ __forceinline__ SdfSample arc_square_cap(float vx, float vy, float radius, float angle, float sweep,
+                                                    float x0, float x1, float he) {
+    const float dir = sweep < 0.0f ? -1.0f : 1.0f;
+    float si, co;
+    sdf_sincos(angle, si, co);
+    const float tx = -si * dir, ty = co * dir;
+    const float px = vx - radius * co, py = vy - radius * si;
+    const float lx = px * tx + py * ty, ly = -px * ty + py * tx;
+    const SdfSample l = line_rect(lx, ly, x0, x1, he);
+    return SdfSample{l.d, l.nx * tx - l.ny * ty, l.nx * ty + l.ny * tx};
+}
+
+// arc_sdf_sample (arc.hlsli:43-64, 87-123): a ring sector with butt, square or
+// round ends.
+__device__ __forceinline__ SdfSample arc_sample(float x, float y, float cx, float cy, float radius_raw,
+                                                float width_raw, float start, float sweep, float cap) {
+    const float radius = fmaxf(radius_raw, 0.0f), width = fmaxf(width_raw, 0.0f);
+    SdfSample s{__int_as_float(0x7f800000), 1.0f, 0.0f};
+    if (!(radius > 0.0f && width > 0.0f && sweep != 0.0f)) return s;
+    const float vx = x - cx, vy = y - cy;
+    const float len = sdf_length(vx, vy);
+    const float he = width * 0.5f;
+    if (fabsf(sweep) >= 6.2831855f) {
+        float nx, ny;
+        normalized_or(vx, vy, 1.0f, 0.0f, nx, ny);
+        const float sg = len >= radius ? 1.0f : -1.0f;
+        return SdfSample{fabsf(len - radius) - he, nx * sg, ny * sg};
+    }
+    // arc_butt_sdf_sample (arc.hlsli:43-64)
+    bool on_ring = false;
+    if (len != 0.0f) {
+        const float angle = sdf_atan2(vy, vx);
+        if (arc_in_sweep(angle, start, sweep)) {
+            const float sg = len >= radius ? 1.0f : -1.0f;
+            s = SdfSample{fabsf(len - radius) - he, vx / len * sg, vy / len * sg};
+            on_ring = true;
+        }
+    }
+    if (!on_ring)
+        s = nearer(arc_cap_segment(vx, vy, radius, start, he, sweep, false),
+                   arc_cap_segment(vx, vy, radius, start + sweep, he, sweep, true));
+    if (cap > 1.5f) {
+        s = nearer(nearer(s, arc_endpoint(vx, vy, radius, start, he)), arc_endpoint(vx, vy, radius, start + sweep, he));
+    } else if (cap >= 0.5f) {
+        s = nearer(nearer(s, arc_square_cap(vx, vy, radius, start, sweep, -he, 0.0f, he)),
+                   arc_square_cap(vx, vy, radius, start + sweep, sweep, 0.0f, he, he));
+    }
+    return s;
+}
+
+// star_sdf_sample (shared/sdf/polygon.hlsli:158-206): a five-point star, its
+// ten vertices alternating outer and inner radius every pi/5, rotated.
+__device__ __forceinline__ SdfSample star_sample(float x, float y, float cx, float cy, float outer, float inner,
+                                                 float corner, float rotation) {
+    float sn, cs;
+    sdf_sincos(rotation, sn, cs);
+    const float rx = x - cx, ry = y - cy;
+    const float px = cs * rx + sn * ry, py = -sn * rx + cs * ry;
+    SdfSample nearest{__int_as_float(0x7f800000), 1.0f, 0.0f};
+    bool inside = false;
+    auto vertex = [&](uint32_t i, float& vx, float& vy) {  // star_vertex
+        const float r = (i & 1u) == 0u ? outer : inner;
+        float vs, vc;
+        sdf_sincos(float(i) * 0.62831855f, vs, vc);
+        vx = vc * r;
+        vy = vs * r;
+    };
+    float qx, qy;
+    vertex(9u, qx, qy);
+    for (uint32_t i = 0; i < 10u; ++i) {
+        float ux, uy;
+        vertex(i, ux, uy);
+        const float ex = ux - qx, ey = uy - qy;
+        float fx, fy;
+        normalized_or(ey, -ex, 1.0f, 0.0f, fx, fy);
+        nearest = nearer(nearest, segment_sample(px, py, qx, qy, ux, uy, fx, fy));
+        if ((qy > py) != (uy > py)) {
+            const float fraction = (py - qy) / (uy - qy);
+            const float crossing = qx + fraction * (ux - qx);
+            if (px < crossing) inside = !inside;
+        }
+        qx = ux;
+        qy = uy;
+    }
+    if (inside) nearest = SdfSample{-nearest.d, -nearest.nx, -nearest.ny};
+    const float d = nearest.d - fmaxf(corner, 0.0f);
+    return SdfSample{d, cs * nearest.nx - sn * nearest.ny, sn * nearest.nx + cs * nearest.ny};
+}
+
 // callout_sdf_sample (shared/sdf/polygon.hlsli:87-136): a rounded body and,
 // unless hidden, a rounded triangular tail on side 0 top, 1 right, 2 bottom
 // or 3 left, nearest of the two.
@@ -354,9 +557,11 @@ __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float 
     const bool line = kind == TK_SDF_LINE || kind == TK_SDF_LINE_SHADOW || dashed;
     const bool triangle = EXT && kind == TK_SDF_TRIANGLE, checker = EXT && kind == TK_SDF_CHECKERBOARD;
     const bool callout = EXT && (kind == TK_SDF_CALLOUT || kind == TK_SDF_CALLOUT_STROKE || kind == TK_SDF_CALLOUT_SHADOW);
-    if (!(rect || circle || line || triangle || checker || callout)) return 0.0f;
+    const bool arc = EXT && (kind == TK_SDF_ARC || kind == TK_SDF_ARC_SHADOW);
+    const bool star = EXT && (kind == TK_SDF_STAR || kind == TK_SDF_STAR_STROKE);
+    if (!(rect || circle || line || triangle || checker || callout || arc || star)) return 0.0f;
     const bool shadow = kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW || kind == TK_SDF_LINE_SHADOW ||
-                        (EXT && kind == TK_SDF_CALLOUT_SHADOW);
+                        (EXT && (kind == TK_SDF_CALLOUT_SHADOW || kind == TK_SDF_ARC_SHADOW));
     const bool stroke = kind == TK_SDF_RECT_STROKE || kind == TK_SDF_CIRCLE_STROKE;
     const float x0 = sdf_word_f(w, 1), y0 = sdf_word_f(w, 2), x1 = sdf_word_f(w, 3), y1 = sdf_word_f(w, 4);
     const float r0 = sdf_word_f(w, 5), r1 = sdf_word_f(w, 6), r2 = sdf_word_f(w, 7), r3 = sdf_word_f(w, 8);
@@ -426,6 +631,15 @@ __device__ __forceinline__ float sdf_coverage(const uint32_t* w, float x, float 
             if (kind == TK_SDF_CALLOUT_STROKE)  // callout_stroke_sdf_sample (polygon.hlsli:138-156)
                 s = s.d >= 0.0f ? SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 11), 0.0f), s.nx, s.ny}
                                 : SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 11), 0.0f), -s.nx, -s.ny};
+        } else if (arc) {
+            // words: centre, radius, width; start angle, sweep, cap
+            s = arc_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5], q[6]);
+        } else if (star) {
+            // words: centre, outer and inner radius; corner radius, rotation; stroke half width
+            s = star_sample(px, py, q[0], q[1], q[2], q[3], q[4], q[5]);
+            if (kind == TK_SDF_STAR_STROKE)  // star_stroke_sdf_sample (polygon.hlsli:208-221)
+                s = s.d >= 0.0f ? SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 9), 0.0f), s.nx, s.ny}
+                                : SdfSample{fabsf(s.d) - fmaxf(sdf_word_f(w, 9), 0.0f), -s.nx, -s.ny};
         }
         cov[pass] = shadow ? shadow_coverage(s, inv, expand, intensity) : coverage_from_sample(s, inv);
     }
