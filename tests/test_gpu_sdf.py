@@ -272,7 +272,7 @@ def test_gpu_rejects_unsupported_sdf_records(renderer):
     a = c.scene_arrays()
     bad_kind = dict(a)
     bad_kind["sdf"] = a["sdf"].copy()
-    bad_kind["sdf"][0] = 8  # arc: not rendered by this library
+    bad_kind["sdf"][0] = 20  # no such kind
     short = dict(a)
     short["sdf"] = a["sdf"][:10].copy()  # the record runs past the blob
     clip = dict(a)
