@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--incremental-steps", type=int, default=10, help="frames of the incremental leg (0: skip)")
     p.add_argument("--sdf-steps", type=int, default=10, help="frames of the SDF-shape leg (0: skip)")
     p.add_argument("--sdf-shapes", type=int, default=50000, help="shapes of the SDF-shape leg")
+    p.add_argument("--sdf-kinds", default="base", choices=["base", "all"],
+                   help="SDF-only runs: the base kinds, or all nineteen (the extended-kind kernel instance)")
     p.add_argument("--sdf-only", action="store_true",
                    help="run only the SDF-shape leg (rank 0, one GPU) and print its line (profiling runs)")
     return p.parse_args()
@@ -240,7 +242,7 @@ def incremental_timing(r, size, steps):
             "timing": "host wall clock per frame, synchronized"}
 
 
-def sdf_scene(size, n, seed):
+def sdf_scene(size, n, seed, kinds="base"):
     """n SDF shapes on a size^2 canvas, clustered like the path workload (200
     Gaussian centres, sigma 300 px): rects (half rounded), rect strokes,
     circles, circle strokes, lines with butt/square/round caps and rect,
@@ -264,8 +266,34 @@ def sdf_scene(size, n, seed):
             stops = [(0.0, (*rng.uniform(0, 1, 3), 1.0)), (1.0, (*rng.uniform(0, 1, 3), float(rng.uniform(0.3, 1))))]
             b = (tk.Brush.linear((x, y), (x + w, y + h), stops) if rng.uniform() < 0.5
                  else tk.Brush.radial((x, y), 0.0, (x, y), float(max(w, h)), stops))
-        kind = k % 9
-        if kind in (0, 1):
+        kind = k % 9 if kinds == "base" else k % 19
+        if kind >= 9:  # the extended kinds
+            r = float(max(w, h) / 2)
+            if kind == 9:
+                c.push_dash_line(x, y, x + w, y + h, float(rng.uniform(1, 6)), 8.0, 4.0, b, cap=int(rng.integers(0, 3)))
+            elif kind == 10:
+                c.push_triangle((x, y), (x + w, y + rng.uniform(0, h)), (x + rng.uniform(0, w), y + h), b,
+                                corner_radius=float(rng.uniform(0, 4)))
+            elif kind == 11:
+                c.push_checkerboard(x, y, x + w, y + h, float(rng.uniform(4, 16)), b, tk.Brush.solid(1, 1, 1, 1))
+            elif kind == 12:
+                c.push_candlestick(x, y, y + h, y + h / 4, y + 3 * h / 4, int(rng.integers(3, 20)), 1, b)
+            elif kind in (13, 14):
+                c.push_sdf_arc(x, y, r, float(rng.uniform(0, 6.28)), float(rng.uniform(-6, 6)), float(rng.uniform(1, 8)),
+                               b, cap=int(rng.integers(0, 3))) if kind == 13 else \
+                    c.push_arc_shadow(x, y, r, 0.5, 4.0, 4.0, b, offset=(3, 3), expand=4.0, intensity=0.5)
+            elif kind in (15, 16):
+                if kind == 15:
+                    c.push_star(x, y, r, r * 0.45, b, corner_radius=1.0, rotation=float(rng.uniform(-3, 3)))
+                else:
+                    c.push_star_stroke(x, y, r, r * 0.45, 2.0, b, rotation=float(rng.uniform(-3, 3)))
+            else:
+                tail = (int(rng.integers(0, 4)), w / 2, float(min(w, h) / 3), 12.0, 2.0)
+                if kind == 17:
+                    c.push_callout((x, y, x + w, y + h), 8.0, tail, b)
+                else:
+                    c.push_callout_stroke((x, y, x + w, y + h), 8.0, tail, 2.0, b)
+        elif kind in (0, 1):
             c.push_rect(x, y, x + w, y + h, b, radius=float(rng.uniform(0, 20)) if kind else 0.0)
         elif kind == 2:
             c.push_rect_stroke(x, y, x + w, y + h, float(rng.uniform(1, 8)), b, radius=float(rng.uniform(0, 12)))
@@ -287,14 +315,14 @@ def sdf_scene(size, n, seed):
     return c
 
 
-def sdf_timing(r, size, steps, cpu, n=50000):
+def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
     """Frames of an SDF-shape scene (PTCL_SDF coverage in fine, full-tile
     colour and hollow-stroke proofs in coarse), device stage times by CUDA
     events; and the oracle on 1/4 of the shapes, scaled, as its CPU
     baseline."""
     from tileink_b200 import _native as N
     size = size or 4096
-    c = sdf_scene(size, n, SEED + 7)
+    c = sdf_scene(size, n, SEED + 7, kinds)
     r.upload(c)
     r.set_timing(True)
     for _ in range(3):
@@ -310,8 +338,10 @@ def sdf_timing(r, size, steps, cpu, n=50000):
     ptcl = r.debug(N.STAGE_PTCL, 0)
     tags = ptcl["tag"]
     kinds = ptcl["color"][tags == N.PTCL_BATCH_BEGIN] & 7
-    line = {"workload": f"{size}x{size} canvas, {n} SDF shapes of every kind (rects, rounded rects, rect strokes, "
-                        "circles, circle strokes, lines, rect/circle/line shadows), 200 Gaussian clusters "
+    what = ("rects, rounded rects, rect strokes, circles, circle strokes, lines, rect/circle/line shadows"
+            if kinds == "base" else "all nineteen kinds: the base kinds plus dash lines, triangles, checkerboards, "
+            "candlesticks, arcs, arc shadows, stars, star strokes, callouts and callout strokes")
+    line = {"workload": f"{size}x{size} canvas, {n} SDF shapes ({what}), 200 Gaussian clusters "
                         "sigma 300 px, 50% opaque / 25% translucent solid / 25% gradient paint",
             "frames_per_s": 1e3 / frame_ms, "ms_per_frame": frame_ms, "stage_ms": acc, "steps": steps,
             "sdf_records": int((tags == N.PTCL_SDF).sum()), "color_records": int((tags == N.PTCL_COLOR).sum()),
@@ -417,8 +447,8 @@ def main():
 
     if args.sdf_only:
         r = tk.NativeRenderer(0)
-        print(json.dumps({"sdf": sdf_timing(r, args.size, max(args.sdf_steps, 1), False, args.sdf_shapes)}),
-              flush=True)
+        print(json.dumps({"sdf": sdf_timing(r, args.size, max(args.sdf_steps, 1), False, args.sdf_shapes,
+                                            args.sdf_kinds)}), flush=True)
         r.close()
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))

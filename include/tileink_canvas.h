@@ -130,6 +130,11 @@ typedef struct tk_sdf_shape {
  * stroke width, an empty line, a shadow of zero intensity: the reference's
  * None), or -1 on error. */
 int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush);
+/* Clip layer of an SDF shape (Canvas::push_clip_sdf_layer and its rect,
+ * circle, arc and line forms, canvas/layers.rs:34-78): later draws until the
+ * matching pop are masked by the shape's coverage. Shadows are not clips;
+ * a shape that draws nothing is rejected (-1). */
+int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape);
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
                                   uint32_t fill_rule, double tolerance);
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);

@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
         l.or_sincos.argtypes = [F32, P, P]
         l.or_atan2.restype = F32
         l.or_atan2.argtypes = [F32, F32]
+        l.or_interpret_particles.restype = I32
+        l.or_interpret_particles.argtypes = [P, P, U32, P]
         l.or_interpret_sdf_draws.restype = I32
         l.or_interpret_sdf_draws.argtypes = [P, P]
         l.or_diff_loss.restype = C.c_double
@@ -127,6 +129,15 @@ def diff_loss(scene, lines, endpoint_point, endpoint_weights, points, colors, si
                               ew.ctypes.data, pts.ctypes.data, cols.ctypes.data, float(sigma), r, bg.ctypes.data,
                               tgt.ctypes.data, img.ctypes.data if img is not None else None, threads)
     return (loss, img) if return_image else loss
+
+
+def interpret_particles(desc, particles: np.ndarray) -> np.ndarray:
+    """Fine-only image with `particles` (PTCL records) as every tile's stream."""
+    img = np.zeros((desc.height, desc.width, 4), np.uint8)
+    p = np.ascontiguousarray(particles)
+    if lib().or_interpret_particles(C.byref(desc), p.ctypes.data, len(p), img.ctypes.data) != 0:
+        raise RuntimeError("oracle: " + lib().or_error().decode())
+    return img
 
 
 def interpret_sdf_draws(desc) -> np.ndarray:

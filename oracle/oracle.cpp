@@ -1080,11 +1080,19 @@ inline uint32_t draw_backdrop(const or_scene& S, const tk_draw_record& d, uint32
 }
 
 // --- coarse/classify.hlsli:11-33 ------------------------------------------------
+inline bool has_sdf(const tk_draw_record& d);
+bool sdf_clip_covers(const or_scene& S, const tk_draw_record& d, uint32_t tx, uint32_t ty);
 uint32_t stack_wrapper_count(const or_scene& S, const Batch& b, uint32_t tx, uint32_t ty) {
     uint32_t count = 0;
     for (uint32_t i = b.layer_start; i < b.layer_end; ++i) {
         const tk_layer_record& L = S.layers[i];
         const tk_draw_record& d = S.draws[L.draw];
+        if (has_sdf(d)) {  // SDF draws of layers are clips
+            if (sdf_clip_covers(S, d, tx, ty)) continue;
+            if (!draw_hits_tile(d, tx, ty, S.tw, S.th)) return TK_INVALID_INDEX;
+            ++count;
+            continue;
+        }
         uint32_t bd = draw_backdrop(S, d, tx, ty);
         if (bd == TK_INVALID_INDEX) return TK_INVALID_INDEX;
         tk_segment_range r = S.ranges[bd];
@@ -1099,6 +1107,7 @@ uint32_t stack_wrapper_count(const or_scene& S, const Batch& b, uint32_t tx, uin
 // coarse/emit_stack.hlsli:9-17
 bool noop_stack_clip(const or_scene& S, const tk_layer_record& L, const tk_draw_record& d, uint32_t tx, uint32_t ty) {
     if (L.tag != TK_LAYER_CLIP) return false;
+    if (has_sdf(d)) return sdf_clip_covers(S, d, tx, ty);
     uint32_t bd = draw_backdrop(S, d, tx, ty);
     tk_segment_range r = S.ranges[bd];
     uint32_t w = uint32_t(S.backdrops[bd]);
@@ -1293,6 +1302,10 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
         const tk_layer_record& L = S.layers[i];
         const tk_draw_record& d = S.draws[L.draw];
         if (noop_stack_clip(S, L, d, tx, ty)) continue;
+        if (has_sdf(d)) {
+            out.recs[p++] = {TK_PTCL_BEGIN_SDF_CLIP, 0, 0u, 0u, 0u, L.draw};
+            continue;
+        }
         uint32_t bd = draw_backdrop(S, d, tx, ty);
         uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_BEGIN_OPACITY
                        : (L.tag == TK_LAYER_BLEND ? TK_PTCL_BEGIN_BLEND : TK_PTCL_BEGIN_CLIP);
@@ -1358,6 +1371,12 @@ F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_
                 }
                 // blend groups are outside this path (rejected at load)
             }
+        } else if (tag == TK_PTCL_BEGIN_SDF_CLIP) {  // fine/interpreter.hlsli:131-150
+            uint32_t parent = clip_mask, alpha = 0u;
+            if (parent != 0u)
+                alpha = coverage_to_u8(sdf_coverage_from_draw(S, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f));
+            clip_stack.push_back(parent);
+            clip_mask = combine_alpha(parent, alpha);
         } else if (tag == TK_PTCL_SDF) {  // fine/interpreter.hlsli:70-84
             if (clip_mask != 0u) {
                 const tk_draw_record& d = S.draws[r.color];
@@ -1991,7 +2010,17 @@ float or_atan2(float y, float x) { return lib_atan2(y, x); }
 // every draw interpreted as a PTCL_SDF particle in every tile, in draw-record
 // order, from the clear colour, with no coarse stage, so an incorrect
 // full-tile proof, hollow-stroke proof or occlusion skip changes pixels.
+int32_t or_interpret_particles(const tk_scene_desc* d, const tk_ptcl_record* particles, uint32_t count,
+                               uint32_t* image);
 int32_t or_interpret_sdf_draws(const tk_scene_desc* d, uint32_t* image) {
+    std::vector<tk_ptcl_record> recs;
+    for (uint32_t k = 0; k < d->draw_count; ++k) recs.push_back({TK_PTCL_SDF, 0, 0u, 0u, 0u, k});
+    return or_interpret_particles(d, recs.data(), uint32_t(recs.size()), image);
+}
+// The fine-only oracle with a given particle stream for every tile
+// (interpret_particles, src/native/runtime/tests/coarse_count/rect_pixels.rs:15-110).
+int32_t or_interpret_particles(const tk_scene_desc* d, const tk_ptcl_record* particles, uint32_t count,
+                               uint32_t* image) {
     try {
         or_scene S;
         S.desc = *d;
@@ -1999,8 +2028,7 @@ int32_t or_interpret_sdf_draws(const tk_scene_desc* d, uint32_t* image) {
         S.brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
         S.sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
         S.shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
-        std::vector<tk_ptcl_record> recs;
-        for (uint32_t k = 0; k < d->draw_count; ++k) recs.push_back({TK_PTCL_SDF, 0, 0u, 0u, 0u, k});
+        std::vector<tk_ptcl_record> recs(particles, particles + count);
         recs.push_back({TK_PTCL_END, 0, 0u, 0u, 0u, 0u});
         const uint32_t n = uint32_t(recs.size());
         parallel_for(8, d->height, [&](uint64_t y) {

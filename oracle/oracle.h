@@ -112,6 +112,9 @@ float or_atan2(float y, float x);
 /* Fine-only image of a scene of SDF draws: every draw interpreted in every
  * tile as a PTCL_SDF particle, from the clear colour (no coarse stage). */
 int32_t or_interpret_sdf_draws(const tk_scene_desc* scene, uint32_t* image);
+/* The same with the given particle stream in every tile. */
+int32_t or_interpret_particles(const tk_scene_desc* scene, const tk_ptcl_record* particles, uint32_t count,
+                               uint32_t* image);
 
 /* FP64 loss of the differentiable model (include/tileink_diff.h) for the
  * flattening `lines` / endpoint weights of a forward and the parameters

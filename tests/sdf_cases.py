@@ -117,3 +117,34 @@ def desc_of(scene):
         s = N.ArrayScene(scene)
         return s, s.desc
     return scene, scene.scene_desc()
+
+
+def particles(records):
+    """PTCL records (tag, color) for the fine-only oracle's tile stream."""
+    out = np.zeros(len(records), N.PTCL_DTYPE)
+    for k, (tag, color) in enumerate(records):
+        out[k]["tag"], out[k]["color"] = tag, color
+    return out
+
+
+def partial_clip_cases():
+    """occlusion_pixels.rs:48-83: an opaque background, then, inside a
+    (rounded, grown) SDF rect clip, 128 translucent full-canvas rects and an
+    opaque cover; the expected stream interprets every draw in every tile
+    inside the clip. (name, canvas, particle stream) triples."""
+    out = []
+    for radius in (0.0, 41.0):
+        for grow in (0.0, 4.375):
+            c = tk.Canvas(W, H)
+            c.set_clear_color(BLACK)
+            c.push_rect(0, 0, 129, 113, rgba8(0, 0, 0, 255))
+            c.push_clip_sdf_rect_layer(*inset((0.0, 0.0, 129.0, 113.0), grow), radius=radius)
+            for i in range(128):
+                c.push_rect(0, 0, 129, 113, rgba8((i * 17) % 256, (i * 29) % 256, (i * 3) % 256, 120))
+            c.push_rect(0, 0, 129, 113, rgba8(23, 47, 93, 255))
+            c.pop_layer()
+            n = len(c.scene_arrays()["draws"])
+            stream = [(N.PTCL_SDF, 0), (N.PTCL_BEGIN_SDF_CLIP, 1)] + [(N.PTCL_SDF, d) for d in range(2, n)] + \
+                     [(N.PTCL_END_CLIP, 0)]
+            out.append((f"partial_clip_{radius}_{grow}", c, particles(stream)))
+    return out

@@ -301,3 +301,50 @@ def test_gpu_rect_known_answers_match_fine_only_oracle(renderer):
         renderer.render()
         got = renderer.readback().view(np.uint8).reshape(want.shape)
         assert np.array_equal(got, want), (name, int((got != want).any(axis=2).sum()))
+
+
+def test_gpu_partial_sdf_clip_matches_fine_only_oracle(renderer):
+    """occlusion_pixels.rs:48-83 on the GPU: the pipeline with SDF clip
+    wrappers gives exactly the fine-only oracle's pixels."""
+    import oracle
+    from sdf_cases import partial_clip_cases
+    for name, canvas, stream in partial_clip_cases():
+        want = oracle.interpret_particles(canvas.scene_desc(), stream)
+        got = renderer.render_to_image(canvas)
+        assert np.array_equal(got, want), name
+
+
+@pytest.mark.parametrize("seed", [21, 22])
+def test_gpu_sdf_clip_layers(renderer, seed):
+    """Nested SDF clip layers (rect, circle, line, arc) around paths and
+    shapes, next to path clips, against the oracle bit for bit."""
+    W, H = 400, 300
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(W, H)
+    c.set_clear_color(0xFFFFFFFF)
+    random_shapes(c, rng, 30, W, H)
+    for depth in range(3):
+        k = int(rng.integers(0, 4))
+        x0, y0 = rng.uniform(-20, W / 2), rng.uniform(-20, H / 2)
+        if k == 0:
+            c.push_clip_sdf_rect_layer(x0, y0, x0 + rng.uniform(40, 300), y0 + rng.uniform(40, 250),
+                                       radius=float(rng.uniform(0, 40)))
+        elif k == 1:
+            c.push_clip_sdf_circle_layer(x0 + 60, y0 + 60, float(rng.uniform(20, 150)))
+        elif k == 2:
+            c.push_clip_sdf_line_layer(x0, y0, x0 + rng.uniform(50, 300), y0 + rng.uniform(50, 200),
+                                       float(rng.uniform(4, 60)), cap=int(rng.integers(0, 3)))
+        else:
+            c.push_clip_sdf_arc_layer(x0 + 80, y0 + 80, float(rng.uniform(30, 120)), float(rng.uniform(-3, 3)),
+                                      float(rng.uniform(-5, 5)), float(rng.uniform(6, 40)))
+        random_shapes(c, rng, 20, W, H)
+        c.push_path(cubic_path(rng, W, H), tk.Brush.solid(*rng.uniform(0, 1, 3), 0.7))
+        if depth == 1:
+            c.push_clip_layer(cubic_path(rng, W, H, 8))
+            extended_shapes(c, rng, 12, W, H)
+            c.pop_layer()
+    for _ in range(3):
+        c.pop_layer()
+    img, ref = compare_frame(renderer, c)
+    ptcl = renderer.debug(N.STAGE_PTCL, 0)
+    assert (ptcl["tag"] == N.PTCL_BEGIN_SDF_CLIP).any()

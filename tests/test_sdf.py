@@ -363,3 +363,15 @@ def test_oracle_arc_and_star_coverage():
     ix, iy = 12 * math.cos(math.pi / 5), 12 * math.sin(math.pi / 5)
     h = math.atan2(iy, 30 - ix)
     assert coverage(star, 79.75, 50) == pytest.approx(0.5 + 0.25 * math.sin(h), abs=1e-4)
+
+
+def test_oracle_partial_sdf_clip_matches_fine_only_oracle():
+    """occlusion_pixels.rs:48-83 on the oracle: coarse's SDF clip wrappers
+    (dropped where the clip rect covers the tile) and the occlusion skip give
+    the pixels of the explicit clip stream interpreted in every tile."""
+    from sdf_cases import partial_clip_cases
+    for name, canvas, stream in partial_clip_cases():
+        d = canvas.scene_desc()
+        want = oracle.interpret_particles(d, stream)
+        got = oracle.OracleRun(d, threads=4).get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(want.shape)
+        assert np.array_equal(got, want), name

@@ -29,6 +29,7 @@ STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4,
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
 PTCL_BATCH_BEGIN = 14
 PTCL_SDF = 9
+PTCL_BEGIN_SDF_CLIP = 12
 TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIND_MIXED = 0, 1, 2, 3, 4
 # SDF kinds (src/shared/gpu_types.rs) and line caps
 SDF_RECT, SDF_CIRCLE, SDF_RECT_STROKE, SDF_CIRCLE_STROKE, SDF_LINE = 1, 2, 3, 4, 6
@@ -223,6 +224,7 @@ def library() -> C.CDLL:
         "tk_canvas_push_path": (I64, [P, P, C.POINTER(BrushDesc), P, U32, F64]),
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
+        "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),

@@ -209,9 +209,9 @@ class Canvas:
         return r
 
     # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
-    def _push_sdf(self, brush: Brush, kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0,
-                  widths=0.0, shadow=None, cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0), flags=0,
-                  angle=(0.0, 0.0)):
+    @staticmethod
+    def _shape(kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0, widths=0.0, shadow=None,
+               cap=N.CAP_BUTT, p2=(0.0, 0.0), dash=(0.0, 0.0, 0.0), flags=0, angle=(0.0, 0.0)) -> N.SdfShape:
         s = N.SdfShape()
         s.kind, s.cap = kind, int(cap)
         s.p0[:] = [float(v) for v in p0]
@@ -225,6 +225,10 @@ class Canvas:
         s.widths[:] = _four(widths)
         if shadow is not None:
             s.shadow[:] = [float(v) for v in shadow]
+        return s
+
+    def _push_sdf(self, brush: Brush, kind: int, *args, **fields):
+        s = self._shape(kind, *args, **fields)
         d, keep = brush._desc()
         r = self._lib.tk_canvas_push_sdf(self._h, C.byref(s), C.byref(d))
         if r == -2:
@@ -232,6 +236,25 @@ class Canvas:
         if r < 0:
             raise ValueError("SDF shape rejected its arguments")
         return r
+
+    def _push_clip_sdf(self, kind: int, **fields):
+        if self._lib.tk_canvas_push_clip_sdf_layer(self._h, C.byref(self._shape(kind, **fields))) != 0:
+            raise ValueError("SDF clip layer rejected its arguments")
+
+    def push_clip_sdf_rect_layer(self, x0, y0, x1, y1, radius=0.0):
+        """Canvas::push_clip_sdf_rect_layer: later draws until pop_layer are
+        masked by the (rounded) rectangle's analytic coverage."""
+        self._push_clip_sdf(N.SDF_RECT, p0=(x0, y0), p1=(x1, y1), radii=radius)
+
+    def push_clip_sdf_circle_layer(self, cx, cy, r):
+        self._push_clip_sdf(N.SDF_CIRCLE, p0=(cx, cy), radius=r)
+
+    def push_clip_sdf_line_layer(self, x0, y0, x1, y1, width, cap=N.CAP_BUTT):
+        self._push_clip_sdf(N.SDF_LINE, p0=(x0, y0), p1=(x1, y1), width=width, cap=cap)
+
+    def push_clip_sdf_arc_layer(self, cx, cy, radius, start_angle, sweep_angle, width, cap=N.CAP_BUTT):
+        self._push_clip_sdf(N.SDF_ARC, p0=(cx, cy), radius=radius, width=width, cap=cap,
+                            angle=(start_angle, sweep_angle))
 
     def push_rect(self, x0, y0, x1, y1, brush: Brush, radius=0.0):
         """Canvas::push_rect: a filled rectangle, corner radii one value or

@@ -262,7 +262,8 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         const bool plain = r.sdf_offset != TK_INVALID_INDEX, shadow = r.sdf_shadow_offset != TK_INVALID_INDEX;
         if (plain || shadow) {
             if (plain && shadow) invalid(at + ": both an SDF and a shadow record");
-            if (r.tag != TK_DRAW_BRUSH) invalid(at + ": SDF clips and groups are outside this path");
+            if (r.tag != TK_DRAW_BRUSH && !(r.tag == TK_DRAW_CLIP && plain))
+                invalid(at + ": SDF groups and shadow clips are outside this path");
             if (r.path_id != TK_INVALID_INDEX) invalid(at + ": an SDF draw with a path");
             const uint64_t off = plain ? r.sdf_offset : r.sdf_shadow_offset;
             const uint64_t len = plain ? r.sdf_len : r.sdf_shadow_len;
@@ -291,7 +292,10 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         if (d.layers[i].tag == TK_LAYER_BLEND) invalid("blend layers are outside this path");
         if (d.layers[i].tag > TK_LAYER_BLEND) invalid("bad layer tag");
         if (d.layers[i].draw >= d.draw_count) invalid("layer draw out of range");
-        if (d.draws[d.layers[i].draw].path_id == TK_INVALID_INDEX) invalid("layer draws must be path draws");
+        const tk_draw_record& ld = d.draws[d.layers[i].draw];
+        const bool sdf_clip = ld.sdf_offset != TK_INVALID_INDEX && ld.tag == TK_DRAW_CLIP;
+        if (sdf_clip ? d.layers[i].tag != TK_LAYER_CLIP : ld.path_id == TK_INVALID_INDEX)
+            invalid("layer draws must be path draws, or SDF draws of clip layers");
     }
     // Painter order grouped by batch in op order.
     std::vector<uint32_t> batch_draws;

@@ -352,7 +352,7 @@ struct Cmd {
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP } kind = FILL;
     tk_path path;
     tk_sdf_shape shape{};
     bool has_brush = false;
@@ -1133,8 +1133,52 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
     return add_path(c, bb, line_start, uint32_t(c->lines.size()) - line_start, brush, TK_FILL_NONZERO, TK_DRAW_BRUSH,
                     true);
 }
+}  // extern "C"
+
+namespace {
+// The SDF draw of `shape` with `tag`; -2 when it draws nothing, -1 on error.
+int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush, uint32_t tag,
+                     bool emit_command);
+}  // namespace
+
+extern "C" {
+
 int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush) {
     if (!c || !shape) return -1;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::SDF, nullptr, brush, nullptr);
+        r.shape = *shape;
+        c->log.push_back(std::move(r));
+    }
+    return add_sdf_draw(c, shape, brush, TK_DRAW_BRUSH, true);
+}
+
+int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape) {
+    if (!c || !shape) return -1;
+    const uint32_t k = shape->kind;
+    if (k == TK_SDF_RECT_SHADOW || k == TK_SDF_CIRCLE_SHADOW || k == TK_SDF_LINE_SHADOW || k == TK_SDF_ARC_SHADOW ||
+        k == TK_SDF_CALLOUT_SHADOW)
+        return -1;  // shadows are not clips
+    // push_clip_sdf_layer (canvas/layers.rs:64-78): a transparent clip draw outside the draw order
+    const int64_t draw = add_sdf_draw(c, shape, nullptr, TK_DRAW_CLIP, false);
+    if (draw < 0) return -1;  // a shape that draws nothing is no clip
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::SDF_CLIP, nullptr, nullptr, nullptr);
+        r.shape = *shape;
+        c->log.push_back(std::move(r));
+    }
+    const uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    c->lists[c->stack.back()].push_back({Cmd::CLIP, uint32_t(draw), 0.0f, child});
+    c->stack.push_back(child);
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush, uint32_t tag,
+                     bool emit_command) {
     const uint32_t k = shape->kind;
     if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
         k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW &&
@@ -1145,11 +1189,6 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     // CandleStick::new and DashLine::new reject these (the reference panics)
     if (k == TK_SDF_CANDLESTICK && !(shape->widths[0] > 0.0f && shape->widths[1] > 0.0f)) return -1;
     if (k == TK_SDF_DASH_LINE && !(shape->dash[1] >= 0.0f)) return -1;
-    if (c->keep) {
-        RecCmd r = rec_cmd(RecCmd::SDF, nullptr, brush, nullptr);
-        r.shape = *shape;
-        c->log.push_back(std::move(r));
-    }
     uint32_t rec[TK_SDF_RECORD_WORDS];
     tk_pixel_bounds pb{0, 0, 0, 0};
     if (!encode_sdf(c, *shape, rec, pb)) return -2;
@@ -1171,7 +1210,7 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     d.sdf_shadow_len = shadow ? TK_SDF_RECORD_WORDS : 0u;
     d.brush_offset = br.first;
     d.brush_len = br.second;
-    d.tag = TK_DRAW_BRUSH;
+    d.tag = tag;
     d.fill_rule = TK_FILL_NONZERO;
     d.pixel_bounds = pb;
     d.local_pixel_bounds = pb;
@@ -1179,10 +1218,13 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
     d.inverse_transform = tk_affine{1, 0, 0, 1, 0, 0};
     const uint32_t draw_ix = uint32_t(c->draws.size());
     c->draws.push_back(d);
-    c->lists[c->stack.back()].push_back({Cmd::DRAW, draw_ix, 0.0f, 0u});
+    if (emit_command) c->lists[c->stack.back()].push_back({Cmd::DRAW, draw_ix, 0.0f, 0u});
     c->dirty = true;
     return draw_ix;
 }
+}  // namespace
+
+extern "C" {
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform, uint32_t rule,
                                   double tolerance) {
     if (!c || !path || rule > 1u || !(tolerance > 0.0)) return -1;
@@ -1656,7 +1698,8 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::BLUR: return tk_canvas_push_blur_group(dst, r.sigma);
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
-        case RecCmd::SDF: {
+        case RecCmd::SDF:
+        case RecCmd::SDF_CLIP: {
             // SDF records carry no draw transform: they replay under translations
             tk_sdf_shape sh = r.shape;
             if (t) {
@@ -1673,7 +1716,8 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
                     sh.p2[1] += t[5];
                 }
             }
-            return tk_canvas_push_sdf(dst, &sh, bp) == -1 ? -1 : 0;
+            return r.kind == RecCmd::SDF_CLIP ? tk_canvas_push_clip_sdf_layer(dst, &sh)
+                                              : (tk_canvas_push_sdf(dst, &sh, bp) == -1 ? -1 : 0);
         }
     }
     return -1;
@@ -1681,7 +1725,7 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
 
 bool has_layers(const std::vector<RecCmd>& log) {
     for (const RecCmd& r : log)
-        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR) return true;
+        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::SDF_CLIP) return true;
     return false;
 }
 

@@ -145,11 +145,36 @@ __device__ uint32_t draw_backdrop_g(const Ctx& c, uint32_t di, uint32_t tx, uint
     return p.data_offset + (ty - p.tile_y0) * (p.tile_x1 - p.tile_x0) + tx - p.tile_x0;
 }
 
+// An SDF clip layer's draw (coarse/sdf_clip.hlsli:35-40): a rect with an
+// identity linear part that covers the whole tile clips nothing there.
+__device__ __forceinline__ bool sdf_clip_draw(const Ctx& c, uint32_t di, uint32_t tx, uint32_t ty, bool& covers,
+                                              bool& hits) {
+    const tk_draw_record& d = c.draws[di];
+    if (d.sdf_offset == TK_INVALID_INDEX && d.sdf_shadow_offset == TK_INVALID_INDEX) return false;
+    covers = false;
+    if (d.sdf_offset != TK_INVALID_INDEX && d.sdf_shadow_offset == TK_INVALID_INDEX && d.sdf_len >= 9u &&
+        __ldg(c.sdf + d.sdf_offset) == TK_SDF_RECT && d.transform.a == 1.0f && d.transform.b == 0.0f &&
+        d.transform.c == 0.0f && d.transform.d == 1.0f)
+        covers = sdf_rect_covers(c.sdf + d.sdf_offset, d.transform.e, d.transform.f, tx, ty);
+    // draw_hits_tile (shared/draw.hlsli:36-40)
+    hits = tx >= tile_min_(d.pixel_bounds.x0, c.tw) && ty >= tile_min_(d.pixel_bounds.y0, c.th) &&
+           tx < tile_max_(d.pixel_bounds.x1, c.tw) && ty < tile_max_(d.pixel_bounds.y1, c.th);
+    return true;
+}
+
 // stack_wrapper_count (coarse/classify.hlsli:11-33).
+template <bool SDF>
 __device__ uint32_t stack_wrappers(const Ctx& c, const PassBatch& b, uint32_t tx, uint32_t ty) {
     uint32_t count = 0;
     for (uint32_t i = b.layer_start; i < b.layer_end; ++i) {
         tk_layer_record L = c.layers[i];
+        bool covers, hits;
+        if (SDF && sdf_clip_draw(c, L.draw, tx, ty, covers, hits)) {
+            if (covers) continue;
+            if (!hits) return TK_INVALID_INDEX;
+            ++count;
+            continue;
+        }
         uint32_t bd = draw_backdrop_g(c, L.draw, tx, ty);
         if (bd == TK_INVALID_INDEX) return TK_INVALID_INDEX;
         tk_segment_range r = c.ranges[bd];
@@ -176,13 +201,22 @@ __device__ __forceinline__ void store_ptcl(tk_ptcl_record* ptcl, uint64_t cap, u
     w[2] = make_uint2(s1, color);
 }
 
-// emit_stack_begins / emit_stack_ends (coarse/emit_stack.hlsli:9-44).
+// emit_stack_begins / emit_stack_ends (coarse/emit_stack.hlsli:9-44); SDF
+// clips open with BEGIN_SDF_CLIP naming their draw.
+template <bool SDF>
 __device__ uint64_t emit_stack(const Ctx& c, const PassBatch& b, uint32_t tx, uint32_t ty, bool begin,
                                tk_ptcl_record* ptcl, uint64_t cap, uint64_t at, uint32_t* error) {
     uint32_t n = b.layer_end - b.layer_start;
     for (uint32_t k = 0; k < n; ++k) {
         uint32_t i = begin ? b.layer_start + k : b.layer_end - 1u - k;
         tk_layer_record L = c.layers[i];
+        bool covers, hits;
+        if (SDF && sdf_clip_draw(c, L.draw, tx, ty, covers, hits)) {
+            if (covers) continue;  // noop_stack_clip
+            if (begin) store_ptcl(ptcl, cap, at++, TK_PTCL_BEGIN_SDF_CLIP, 0u, 0u, 0u, 0u, L.draw, error);
+            else store_ptcl(ptcl, cap, at++, TK_PTCL_END_CLIP, 0u, 0u, 0u, 0u, 0u, error);
+            continue;
+        }
         uint32_t bd = draw_backdrop_g(c, L.draw, tx, ty);
         tk_segment_range r = c.ranges[bd];
         uint32_t w = uint32_t(c.backdrops[bd]);
@@ -289,7 +323,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
         total += nb + 2u * wrappers + 1u;
         if (EMIT) {
             const PassBatch& b = batches[cur];
-            uint64_t end = emit_stack(c, b, tx, ty, false, ptcl, cap, at, error);
+            uint64_t end = emit_stack<SDF>(c, b, tx, ty, false, ptcl, cap, at, error);
             uint32_t skip = 0;
             if (flags & kChunkClassOccluder) skip = wrappers ? 0u : occluded_prefix_g(ptcl, section + 1u, end);
             // classify_tile_flags (coarse/tile_classification.hlsli:6-10)
@@ -419,12 +453,12 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     close();
                     cur = batch;
                     nb = 0;
-                    wrappers = stack_wrappers(c, batches[batch], tx, ty);
+                    wrappers = stack_wrappers<SDF>(c, batches[batch], tx, ty);
                     rejected = wrappers == TK_INVALID_INDEX;
                     flags = (!rejected && wrappers) ? kChunkClassOther : 0u;
                     if (EMIT && !rejected) {
                         section = at;
-                        at = emit_stack(c, batches[batch], tx, ty, true, ptcl, cap, at + 1u, error);
+                        at = emit_stack<SDF>(c, batches[batch], tx, ty, true, ptcl, cap, at + 1u, error);
                     }
                 }
                 if (rejected) continue;

@@ -461,6 +461,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                 if (a.x == TK_PTCL_FILL && n != 0u) cls = kClsFill;  // row sums staged below
             }
             S.nseg[tid] = n;
+            if (SDF != 0u && a.x == TK_PTCL_BEGIN_SDF_CLIP) S.umode[tid] = __ldg(&paints[c.y].sdf);
             if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (SDF != 0u && a.x == TK_PTCL_SDF)) {
                 const PaintInfo* pi = paints + c.y;
                 if (SDF != 0u && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
@@ -604,11 +605,26 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                         px = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(px), a));
                     }
                 }
-            } else if (SDF != 0u && tag == TK_PTCL_SDF) {
-                // PTCL_SDF (fine/interpreter.hlsli:70-84)
-                if (clip != 0u) {
-                    const float cov = sdf_coverage_at<SDF == 2u>(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy);
-                    const uint32_t masked = combine_alpha(coverage_to_u8(cov), clip);
+            } else if (SDF != 0u && (tag == TK_PTCL_SDF || tag == TK_PTCL_BEGIN_SDF_CLIP)) {
+                // PTCL_SDF (fine/interpreter.hlsli:70-84) and BEGIN_SDF_CLIP (131-150):
+                // the shape's quantized coverage, one evaluation for both
+                uint32_t alpha = 0u;
+                if (clip != 0u)
+                    alpha = coverage_to_u8(
+                        sdf_coverage_at<SDF == 2u>(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy));
+                if (tag == TK_PTCL_BEGIN_SDF_CLIP) {  // push the mask, then narrow it
+                    if (cdepth < 4u) {
+                        cregs = (cregs & ~(255u << (8u * cdepth))) | (clip << (8u * cdepth));
+                        ++cdepth;
+                    } else if (cdepth - 4u < kClipSpill) {
+                        cspill[cdepth - 4u] = clip;
+                        ++cdepth;
+                    } else {
+                        atomicOr(error, ERR_STACK_DEPTH);
+                    }
+                    clip = combine_alpha(clip, alpha);
+                } else {
+                    const uint32_t masked = combine_alpha(alpha, clip);
                     if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
                 }
             } else if (is_fill_like(tag)) {
