@@ -277,7 +277,7 @@ def test_gpu_rejects_unsupported_sdf_records(renderer):
     short["sdf"] = a["sdf"][:10].copy()  # the record runs past the blob
     clip = dict(a)
     clip["draws"] = a["draws"].copy()
-    clip["draws"]["tag"][0] = 1  # an SDF clip: outside this path
+    clip["draws"]["tag"][0] = 2  # an SDF opacity group: outside this path
     for arrays in (bad_kind, short, clip):
         with pytest.raises(tk.TileinkError) as e:
             renderer.upload(N.ArrayScene(arrays))
