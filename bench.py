@@ -337,7 +337,7 @@ def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
     frame_ms = sum(acc.values())
     ptcl = r.debug(N.STAGE_PTCL, 0)
     tags = ptcl["tag"]
-    kinds = ptcl["color"][tags == N.PTCL_BATCH_BEGIN] & 7
+    tile_kind = ptcl["color"][tags == N.PTCL_BATCH_BEGIN] & 7
     what = ("rects, rounded rects, rect strokes, circles, circle strokes, lines, rect/circle/line shadows"
             if kinds == "base" else "all nineteen kinds: the base kinds plus dash lines, triangles, checkerboards, "
             "candlesticks, arcs, arc shadows, stars, star strokes, callouts and callout strokes")
@@ -345,7 +345,7 @@ def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
                         "sigma 300 px, 50% opaque / 25% translucent solid / 25% gradient paint",
             "frames_per_s": 1e3 / frame_ms, "ms_per_frame": frame_ms, "stage_ms": acc, "steps": steps,
             "sdf_records": int((tags == N.PTCL_SDF).sum()), "color_records": int((tags == N.PTCL_COLOR).sum()),
-            "tile_kinds": {name: int((kinds == k).sum()) for k, name in
+            "tile_kinds": {name: int((tile_kind == k).sum()) for k, name in
                            ((0, "interpreter"), (1, "empty"), (2, "color"), (3, "sdf"), (4, "mixed"))},
             "timing": "device, CUDA events per stage, summed"}
     if cpu:
