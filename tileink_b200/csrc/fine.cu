@@ -697,6 +697,16 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
     if (inside) target[pix] = texel_store(px);
 }
 
+// g_star_dir: the star vertex directions, by the same sdf_sincos the pixels
+// would call.
+__global__ void k_star_table() {
+    if (threadIdx.x < 10u) {
+        float s, c;
+        sdf_sincos(float(threadIdx.x) * 0.62831855f, s, c);
+        g_star_dir[threadIdx.x] = make_float2(c, s);
+    }
+}
+
 }  // namespace
 
 void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
@@ -716,6 +726,7 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
         cudaFuncSetAttribute(k_fine<2u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
         configured = true;
     }
+    if (s.sdf_ext) k_star_table<<<1, 32, 0, st>>>();
     auto kernel = !s.sdf_words ? k_fine<0u> : (s.sdf_ext ? k_fine<2u> : k_fine<1u>);
     kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
                                                       s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,

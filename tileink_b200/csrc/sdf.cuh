@@ -406,6 +406,12 @@ __device__ __forceinline__ SdfSample arc_sample(float x, float y, float cx, floa
     return s;
 }
 
+// cos and sin of the star vertex angles i pi/5 (star_vertex's float(i) *
+// 0.6283185307179586), i = 0..9, by sdf_sincos: written by fine's
+// k_star_table before the kernels that read them, so that star pixels need
+// one sincos (the rotation) instead of eleven.
+static __device__ float2 g_star_dir[10];
+
 // star_sdf_sample (shared/sdf/polygon.hlsli:158-206): a five-point star, its
 // ten vertices alternating outer and inner radius every pi/5, rotated.
 __device__ __forceinline__ SdfSample star_sample(float x, float y, float cx, float cy, float outer, float inner,
@@ -418,10 +424,9 @@ __device__ __forceinline__ SdfSample star_sample(float x, float y, float cx, flo
     bool inside = false;
     auto vertex = [&](uint32_t i, float& vx, float& vy) {  // star_vertex
         const float r = (i & 1u) == 0u ? outer : inner;
-        float vs, vc;
-        sdf_sincos(float(i) * 0.62831855f, vs, vc);
-        vx = vc * r;
-        vy = vs * r;
+        const float2 dir = g_star_dir[i];  // (cos, sin) of float(i) * 0.62831855f
+        vx = dir.x * r;
+        vy = dir.y * r;
     };
     float qx, qy;
     vertex(9u, qx, qy);
