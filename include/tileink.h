@@ -129,9 +129,28 @@ extern "C" {
 #define TK_BRUSH_LINEAR 2u
 #define TK_BRUSH_RADIAL 3u
 #define TK_BRUSH_COLOR_WORD 4u
+/* Image pattern brush (BRUSH_PATTERN_RESOURCE, shared/brush/constants.hlsli:9-21,
+ * src/shared/brush.rs:325-339): header word 1 extend, 4 placement
+ * (TK_BRUSH_TEXTURE_PLACEMENT_BIT | index into tk_scene_desc.images), 5 and 6
+ * the image's width and height, 7 opacity (0..255), 8 sampling; parameter
+ * words 0..5 the f32 transform [a b c d e f] from pixel space to the unit
+ * square of the image. */
+#define TK_BRUSH_PATTERN_RESOURCE 7u
+#define TK_BRUSH_IMAGE_ALPHA_WORD 7u
+#define TK_BRUSH_TEXTURE_PLACEMENT_BIT 0x80000000u
+#define TK_PATTERN_NEAREST 0u
+#define TK_PATTERN_BILINEAR 1u
 #define TK_EXTEND_PAD 0u
 #define TK_EXTEND_REPEAT 1u
 #define TK_EXTEND_REFLECT 2u
+
+/* One image of a scene's texture table: premultiplied RGBA8 texels (red in
+ * the low byte), row-major and tightly packed, width * height words. */
+typedef struct tk_image_desc {
+    const uint32_t* premul_rgba8;
+    uint32_t width;
+    uint32_t height;
+} tk_image_desc;
 
 /* ------------------------------------------------------------------------ */
 /* Records. Layouts equal the reference's #[repr(C)] Pod types.              */
@@ -270,6 +289,11 @@ typedef struct tk_scene_desc {
     uint64_t sdf_word_count;
     const uint32_t* sdf_shadow_blob;
     uint64_t sdf_shadow_word_count;
+    /* The texture table that image pattern brushes index (the scene's
+     * registered images, canvas/primitives/images.rs:42-52). */
+    const tk_image_desc* images;
+    uint32_t image_count;
+    uint32_t image_reserved;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

@@ -135,6 +135,19 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
  * matching pop are masked by the shape's coverage. Shadows are not clips;
  * a shape that draws nothing is rejected (-1). */
 int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape);
+/* Registers an image with the canvas (Canvas::register_scene_image,
+ * canvas/primitives/images.rs:42-52): the texels (premultiplied RGBA8, red in
+ * the low byte, width * height words, row-major) are copied. Returns the
+ * image's index, or -1 for an empty image. */
+int32_t tk_canvas_add_image(tk_canvas* c, const uint32_t* premul_rgba8, uint32_t width, uint32_t height);
+/* Canvas::push_image (canvas/primitives/images.rs:9-26): a rect from
+ * (x0, y0) to (x1, y1), in logical coordinates, filled with registered image
+ * `image` scaled into it (Brush::for_rect_resource, shared/brush.rs:557-580),
+ * with extend TK_EXTEND_*, sampling TK_PATTERN_* and opacity 0..255 (the
+ * reference's push_image uses 255). Returns the draw index, or -1 for an
+ * empty or non-finite rect or an unknown image. */
+int64_t tk_canvas_push_image(tk_canvas* c, const double rect[4], uint32_t image, uint32_t extend,
+                             uint32_t sampling, uint32_t opacity);
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
                                   uint32_t fill_rule, double tolerance);
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);

@@ -412,6 +412,8 @@ inline float fill_value(const tk_line_segment* segs, uint32_t start, uint32_t en
 struct Paint {
     const uint32_t* words;
     uint64_t count;
+    const tk_image_desc* images = nullptr;  // the scene's texture table
+    uint32_t image_count = 0;
     uint32_t word(uint32_t base, uint32_t index) const {
         if (base < count) {
             if (index < count - base) return words[base + index];
@@ -478,6 +480,64 @@ uint32_t sample_radial(const Paint& P, float x, float y, uint32_t base, uint32_t
     }
     return has_t ? sample_ramp(P, off, len, t, extend) : 0u;
 }
+// --- shared/brush/pattern.hlsli:9-17, texture.hlsli:7-31, pattern_transform.hlsli:7-11 ---
+uint32_t extend_coord_i32(int32_t value, uint32_t size, uint32_t extend) {
+    if (size <= 1u) return 0u;
+    if (extend == TK_EXTEND_REPEAT || extend == TK_EXTEND_REFLECT) {
+        uint32_t period = size * (extend == TK_EXTEND_REFLECT ? 2u : 1u);
+        // euclidean_remainder_i32 (shared/integer.hlsli:5-9)
+        uint32_t magnitude = value < 0 ? 0u - uint32_t(value) : uint32_t(value);
+        uint32_t remainder = magnitude % period;
+        uint32_t coord = value < 0 && remainder != 0u ? period - remainder : remainder;
+        return coord < size ? coord : period - coord - 1u;
+    }
+    return uint32_t(std::min(std::max(value, 0), int32_t(size) - 1));
+}
+float pattern_transform_component(float a, float b, float offset, float x, float y) {
+    float by = b * y;
+    float dot_product = mad(a, x, by) + mad(b, y, -by);
+    return dot_product + offset;
+}
+uint32_t texel(const tk_image_desc& im, uint32_t col, uint32_t row) {
+    return im.premul_rgba8[uint64_t(row) * im.width + col];
+}
+F4 lerp_unorm(F4 a, F4 b, float t) {
+    return {mad(b.r - a.r, t, a.r), mad(b.g - a.g, t, a.g), mad(b.b - a.b, t, a.b), mad(b.a - a.a, t, a.a)};
+}
+// sample_resource_pattern_texture. The bilinear pad-extended form is the
+// texture unit's filter there (SampleLevel, clamp-to-edge addressing), restated
+// as the exact filter: texel centres at half-integers, f32 weights, one
+// rounding to 8 bits.
+uint32_t sample_pattern_texture(const tk_image_desc& im, float px, float py, uint32_t opacity, uint32_t extend,
+                                uint32_t sampling) {
+    const uint32_t w = im.width, h = im.height;
+    uint32_t color;
+    if (sampling == TK_PATTERN_BILINEAR && extend == TK_EXTEND_PAD) {
+        float sx = clampf(px, 0.0f, float(w)) - 0.5f, sy = clampf(py, 0.0f, float(h)) - 0.5f;
+        float bx = std::floor(sx), by = std::floor(sy), fx = sx - bx, fy = sy - by;
+        int32_t ix = f2i(bx), iy = f2i(by);
+        auto cl = [](int32_t v, uint32_t n) { return uint32_t(std::min(std::max(v, 0), int32_t(n) - 1)); };
+        uint32_t x0 = cl(ix, w), x1 = cl(ix + 1, w), y0 = cl(iy, h), y1 = cl(iy + 1, h);
+        F4 top = lerp_unorm(rgba8_to_unorm(texel(im, x0, y0)), rgba8_to_unorm(texel(im, x1, y0)), fx);
+        F4 bot = lerp_unorm(rgba8_to_unorm(texel(im, x0, y1)), rgba8_to_unorm(texel(im, x1, y1)), fx);
+        color = unorm_to_rgba8(lerp_unorm(top, bot, fy));
+    } else if (sampling == TK_PATTERN_BILINEAR) {
+        float sx = px - 0.5f, sy = py - 0.5f;
+        float bx = std::floor(sx), by = std::floor(sy), fx = sx - bx, fy = sy - by;
+        int32_t ix = f2i(bx), iy = f2i(by);
+        int32_t jx = int32_t(uint32_t(ix) + 1u), jy = int32_t(uint32_t(iy) + 1u);
+        uint32_t tl = texel(im, extend_coord_i32(ix, w, extend), extend_coord_i32(iy, h, extend));
+        uint32_t tr = texel(im, extend_coord_i32(jx, w, extend), extend_coord_i32(iy, h, extend));
+        uint32_t bl = texel(im, extend_coord_i32(ix, w, extend), extend_coord_i32(jy, h, extend));
+        uint32_t br = texel(im, extend_coord_i32(jx, w, extend), extend_coord_i32(jy, h, extend));
+        color = lerp_premul_u8(lerp_premul_u8(tl, tr, fx), lerp_premul_u8(bl, br, fx), fy);
+    } else {
+        color = texel(im, extend_coord_i32(f2i(std::floor(px)), w, extend),
+                      extend_coord_i32(f2i(std::floor(py)), h, extend));
+    }
+    return scale_premul_u8(color, opacity);
+}
+
 uint32_t sample_draw_brush(const Paint& P, const tk_draw_record& d, float x, float y) {
     if (P.word(0u, d.brush_offset) == TK_BRUSH_SOLID) return P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD);
     const tk_affine& m = d.inverse_transform;
@@ -491,7 +551,16 @@ uint32_t sample_draw_brush(const Paint& P, const tk_draw_record& d, float x, flo
     if (kind == TK_BRUSH_LINEAR) return sample_linear(P, lx, ly, base, extend, payload, len);
     if (kind == TK_BRUSH_RADIAL) return sample_radial(P, lx, ly, base, extend, payload, len);
     if (kind == 6u) return 0u;  // BRUSH_PATTERN
-    return color;               // other kinds are outside this path
+    if (kind != TK_BRUSH_PATTERN_RESOURCE) return color;  // other kinds are outside this path
+    // sample_brush's texture-table branch (shared/brush/sample.hlsli:32-41)
+    uint32_t placement = P.word(0u, db + 4u), w = P.word(0u, db + 5u), h = P.word(0u, db + 6u);
+    if (w == 0u || h == 0u) return 0u;
+    uint32_t index = placement & ~TK_BRUSH_TEXTURE_PLACEMENT_BIT;
+    if (!(placement & TK_BRUSH_TEXTURE_PLACEMENT_BIT) || index >= P.image_count) return 0u;
+    float tx = pattern_transform_component(P.param(0u, base, 0u), P.param(0u, base, 2u), P.param(0u, base, 4u), lx, ly) * float(w);
+    float ty = pattern_transform_component(P.param(0u, base, 1u), P.param(0u, base, 3u), P.param(0u, base, 5u), lx, ly) * float(h);
+    return sample_pattern_texture(P.images[index], tx, ty, P.word(0u, db + TK_BRUSH_IMAGE_ALPHA_WORD), extend,
+                                  P.word(0u, db + 8u));
 }
 
 
@@ -1185,7 +1254,7 @@ bool sdf_stroke_empty(const or_scene& S, const tk_draw_record& d, uint32_t tx, u
     return rect_covers_tile(inner, r, d, tx, ty, 1.0f);
 }
 bool nontransparent_solid(const or_scene& S, const tk_draw_record& d) {
-    Paint P{S.brush.data(), S.brush.size()};
+    Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
     return d.brush_offset != TK_INVALID_INDEX && P.word(0u, d.brush_offset) == TK_BRUSH_SOLID &&
            P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
 }
@@ -1219,13 +1288,20 @@ Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t 
     if (has_sdf(d)) {  // coarse/emit_draw.hlsli:22-30
         if (d.tag == TK_DRAW_BRUSH && !sdf_stroke_empty(S, d, tx, ty)) {
             r.valid = true;
-            Paint P{S.brush.data(), S.brush.size()};
+            Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
             uint32_t color = nontransparent_solid(S, d) && sdf_clip_covers(S, d, tx, ty)
                                  ? P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD)
                                  : 0u;
+            // full_tile_image (coarse/paint.hlsli:30-34)
+            const bool image = d.brush_offset != TK_INVALID_INDEX &&
+                               P.word(0u, d.brush_offset) == TK_BRUSH_PATTERN_RESOURCE &&
+                               P.word(0u, d.brush_offset + TK_BRUSH_IMAGE_ALPHA_WORD) == 255u;
             if (color != 0u) {
                 r.tag = TK_PTCL_COLOR;
                 r.color = color;
+            } else if (image && sdf_clip_covers(S, d, tx, ty)) {
+                r.tag = TK_PTCL_IMAGE;
+                r.color = di;
             } else {
                 r.tag = TK_PTCL_SDF;
                 r.seg0 = di;
@@ -1245,7 +1321,7 @@ Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t 
     r.fill_rule = d.fill_rule;
     r.seg0 = rg.start;
     r.seg1 = rg.end;
-    Paint P{S.brush.data(), S.brush.size()};
+    Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
     bool nontransparent_solid = d.brush_offset != TK_INVALID_INDEX && P.word(0u, d.brush_offset) == TK_BRUSH_SOLID &&
                                 P.word(0u, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
     if (d.tag == TK_DRAW_CLIP) r.tag = TK_PTCL_BEGIN_CLIP;
@@ -1316,7 +1392,8 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
         if (!q.valid) continue;
         // particle_class_flags (coarse/paint.hlsli:35-40)
         if (q.tag == TK_PTCL_COLOR) flags |= CHUNK_CLASS_COLOR;
-        else if (q.tag == TK_PTCL_SDF && solid_supported_sdf(S, S.draws[cand[k]])) flags |= CHUNK_CLASS_SDF;
+        else if (q.tag == TK_PTCL_IMAGE || (q.tag == TK_PTCL_SDF && solid_supported_sdf(S, S.draws[cand[k]])))
+            flags |= CHUNK_CLASS_SDF;
         else flags |= CHUNK_CLASS_OTHER;
         if (wrappers == 0u && q.tag == TK_PTCL_COLOR && (q.color >> 24) == 255u && p > 0u) flags |= CHUNK_CLASS_OCCLUDER;
         if (p < count) out.recs[p++] = {q.tag, int32_t(q.winding), q.fill_rule, q.seg0, q.seg1, q.color};
@@ -1345,7 +1422,7 @@ struct Group { uint32_t kind; F4 parent; uint32_t parent_clip, layer_alpha, payl
 
 F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel,
              uint32_t lx, uint32_t ly, uint32_t gx, uint32_t gy) {
-    Paint P{S.brush.data(), S.brush.size()};
+    Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
     uint32_t clip_mask = 255u;
     std::vector<uint32_t> clip_stack;
     std::vector<Group> groups;
@@ -1377,6 +1454,12 @@ F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_
                 alpha = coverage_to_u8(sdf_coverage_from_draw(S, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f));
             clip_stack.push_back(parent);
             clip_mask = combine_alpha(parent, alpha);
+        } else if (tag == TK_PTCL_IMAGE) {  // fine/interpreter.hlsli:65-69
+            if (clip_mask != 0u) {
+                uint32_t color = sample_draw_brush(P, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f);
+                if (clip_mask == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+                else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(color, clip_mask));
+            }
         } else if (tag == TK_PTCL_SDF) {  // fine/interpreter.hlsli:70-84
             if (clip_mask != 0u) {
                 const tk_draw_record& d = S.draws[r.color];
@@ -1428,7 +1511,7 @@ F4 color_only(const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t 
 // no stacks; full-tile images are not produced on this path)
 F4 analytic_solid(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel,
                   uint32_t gx, uint32_t gy) {
-    Paint P{S.brush.data(), S.brush.size()};
+    Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
     float x = float(gx) + 0.5f, y = float(gy) + 0.5f;
     for (uint32_t ix = begin; ix < end; ++ix) {
         const tk_ptcl_record& r = recs[ix];
@@ -1436,6 +1519,10 @@ F4 analytic_solid(const or_scene& S, const std::vector<tk_ptcl_record>& recs, ui
         if (r.tag == TK_PTCL_COLOR) {
             if (premul_u8_is_opaque(r.color)) pixel = rgba8_to_unorm(r.color);
             else pixel = src_over_premul_unorm(pixel, rgba8_to_unorm(r.color));
+        } else if (r.tag == TK_PTCL_IMAGE) {  // fine/specialized.hlsli:84-90
+            uint32_t color = sample_draw_brush(P, S.draws[r.color], x, y);
+            if (premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+            else pixel = src_over_premul_unorm(pixel, rgba8_to_unorm(color));
         } else {
             const tk_draw_record& d = S.draws[r.color];
             bool inside = int32_t(gx) >= d.pixel_bounds.x0 && int32_t(gy) >= d.pixel_bounds.y0 &&

@@ -29,6 +29,8 @@ STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4,
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
 PTCL_BATCH_BEGIN = 14
 PTCL_SDF = 9
+PTCL_IMAGE = 13
+PATTERN_NEAREST, PATTERN_BILINEAR = 0, 1
 PTCL_BEGIN_SDF_CLIP = 12
 TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIND_MIXED = 0, 1, 2, 3, 4
 # SDF kinds (src/shared/gpu_types.rs) and line caps
@@ -92,7 +94,13 @@ class SceneDesc(C.Structure):
         ("ops", C.c_void_p), ("op_count", C.c_uint32), ("reserved", C.c_uint32),
         ("sdf_blob", C.c_void_p), ("sdf_word_count", C.c_uint64),
         ("sdf_shadow_blob", C.c_void_p), ("sdf_shadow_word_count", C.c_uint64),
+        ("images", C.c_void_p), ("image_count", C.c_uint32), ("image_reserved", C.c_uint32),
     ]
+
+
+class ImageDesc(C.Structure):
+    """tk_image_desc: premultiplied RGBA8 texels (red in the low byte), row-major."""
+    _fields_ = [("premul_rgba8", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 
 class Stats(C.Structure):
@@ -225,6 +233,8 @@ def library() -> C.CDLL:
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
+        "tk_canvas_add_image": (I32, [P, P, U32, U32]),
+        "tk_canvas_push_image": (C.c_int64, [P, C.POINTER(C.c_double), U32, U32, U32, U32]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),
@@ -280,6 +290,8 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "ops": arr(d.ops, d.op_count, OP_DTYPE),
         "sdf": arr(d.sdf_blob, d.sdf_word_count, np.uint32),
         "sdf_shadow": arr(d.sdf_shadow_blob, d.sdf_shadow_word_count, np.uint32),
+        "images": [arr(im.premul_rgba8, im.width * im.height, np.uint32).reshape(im.height, im.width)
+                   for im in (C.cast(d.images, C.POINTER(ImageDesc))[k] for k in range(d.image_count))],
     }
 
 
@@ -304,6 +316,12 @@ class ArrayScene:
             d.sdf_blob, d.sdf_word_count = ptr(sdf), len(sdf)
         if shadow is not None and len(shadow):
             d.sdf_shadow_blob, d.sdf_shadow_word_count = ptr(shadow), len(shadow)
+        images = [np.ascontiguousarray(im, dtype=np.uint32) for im in a.get("images", [])]
+        if images:
+            self._images = images
+            self._image_table = (ImageDesc * len(images))(*[ImageDesc(ptr(im), im.shape[1], im.shape[0])
+                                                            for im in images])
+            d.images, d.image_count = C.addressof(self._image_table), len(images)
         self.desc = d
         self.flatten = None
         els, strokes = a.get("elements"), a.get("strokes")

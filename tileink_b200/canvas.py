@@ -237,6 +237,29 @@ class Canvas:
             raise ValueError("SDF shape rejected its arguments")
         return r
 
+    def add_image(self, premul_rgba8) -> int:
+        """Registers an image (H, W) uint32 array of premultiplied RGBA8
+        texels, red in the low byte (Canvas::register_scene_image); returns
+        its index for push_image."""
+        im = np.ascontiguousarray(premul_rgba8, dtype=np.uint32)
+        if im.ndim != 2:
+            raise ValueError("image must be a (height, width) uint32 array")
+        r = self._lib.tk_canvas_add_image(self._h, im.ctypes.data, im.shape[1], im.shape[0])
+        if r < 0:
+            raise ValueError("empty image")
+        return r
+
+    def push_image(self, x0, y0, x1, y1, image: int, extend=EXTEND_PAD, sampling=N.PATTERN_NEAREST, opacity=255):
+        """Canvas::push_image: registered image `image` scaled into the rect
+        (x0, y0)-(x1, y1) with extend EXTEND_* and sampling PATTERN_*."""
+        rect = (C.c_double * 4)(x0, y0, x1, y1)
+        r = self._lib.tk_canvas_push_image(self._h, rect, int(image), int(extend), int(sampling), int(opacity))
+        if r == -2:
+            return None  # the rect draws nothing
+        if r < 0:
+            raise ValueError("image rect or options rejected")
+        return r
+
     def _push_clip_sdf(self, kind: int, **fields):
         if self._lib.tk_canvas_push_clip_sdf_layer(self._h, C.byref(self._shape(kind, **fields))) != 0:
             raise ValueError("SDF clip layer rejected its arguments")

@@ -134,6 +134,8 @@ struct tk_ctx {
     DBuf<tk_path_record> paths;
     DBuf<tk_draw_record> draws;
     DBuf<uint32_t> brush, sdf, batch_ids, order;
+    DBuf<uint32_t> texels;  // the scene's images, concatenated
+    DBuf<uint4> image_tab;  // per image: first texel, width, height
     DBuf<tk_layer_record> layers;
     DBuf<tk::ScanItem> items;
     DBuf<unsigned long long> item_desc, tile_desc, stats;
@@ -220,6 +222,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     if ((d.line_count && !d.lines) || (d.path_count && !d.paths) || (d.draw_count && !d.draws) ||
         (d.brush_word_count && !d.brush_blob) || (d.layer_count && !d.layers) ||
         (d.sdf_word_count && !d.sdf_blob) || (d.sdf_shadow_word_count && !d.sdf_shadow_blob) ||
+        (d.image_count && !d.images) ||
         (d.draw_order_count && !d.draw_order) || (d.draw_count && !d.draw_batch_ids) || (d.op_count && !d.ops))
         invalid("null array with nonzero count");
     bool device_plan = (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
@@ -252,6 +255,13 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     if (next_line != d.line_count) invalid("path line ranges do not cover the line array");
     if (seg_cap > 0xFFFFFFFFull) invalid("segment capacity exceeds u32 indexing");
     if (d.sdf_word_count + d.sdf_shadow_word_count > 0xFFFFFFFFull) invalid("SDF blobs exceed u32 indexing");
+    uint64_t texel_words = 0;
+    for (uint32_t k = 0; k < d.image_count; ++k) {
+        const tk_image_desc& im = d.images[k];
+        if (!im.premul_rgba8 || im.width == 0u || im.height == 0u) invalid("image " + std::to_string(k) + " is empty");
+        texel_words += uint64_t(im.width) * im.height;
+    }
+    if (texel_words > 0xFFFFFFFFull) invalid("images exceed u32 indexing");
     bool sdf_ext = false;
     // Draws: path fills/clips, and brush draws of the SDF kinds this library
     // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
@@ -281,6 +291,21 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                                              kind == TK_SDF_LINE_SHADOW));
             if (!ok) invalid(at + ": SDF kind " + std::to_string(kind) + " is not supported");
             sdf_ext = sdf_ext || ext;
+        }
+        // image pattern brushes (shared/brush/sample.hlsli:32-41): texture-table
+        // placement of a registered image, sized as that image
+        const uint64_t bo = r.brush_offset;
+        if (bo != TK_INVALID_INDEX && bo < d.brush_word_count && d.brush_blob[bo] == TK_BRUSH_PATTERN_RESOURCE) {
+            if (bo + TK_BRUSH_HEADER_WORDS + TK_BRUSH_PARAM_WORDS > d.brush_word_count)
+                invalid(at + ": image brush outside the brush blob");
+            const uint32_t* w = d.brush_blob + bo;
+            const uint32_t ix = w[4] & ~TK_BRUSH_TEXTURE_PLACEMENT_BIT;
+            if (!(w[4] & TK_BRUSH_TEXTURE_PLACEMENT_BIT)) invalid(at + ": atlas image placement is outside this path");
+            if (ix >= d.image_count) invalid(at + ": image index out of range");
+            if (w[5] != d.images[ix].width || w[6] != d.images[ix].height)
+                invalid(at + ": image brush size differs from its image");
+            if (w[1] > TK_EXTEND_REFLECT || w[7] > 255u || w[8] > TK_PATTERN_BILINEAR)
+                invalid(at + ": bad image brush extend, opacity or sampling");
         }
         if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
             r.tag != TK_DRAW_ISOLATE)
@@ -398,6 +423,7 @@ tk::SceneView view(tk_ctx* c) {
     s.sdf_words = c->sdf_words;
     s.sdf_shadow_base = c->sdf_shadow_base;
     s.sdf_ext = c->sdf_ext;
+    s.texels = c->texels.ptr;
     s.layers = c->layers.ptr;
     s.batch_ids = c->batch_ids.ptr;
     s.order = c->order.ptr;
@@ -493,9 +519,21 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nu
     if (d.sdf_shadow_word_count)
         TK_CUDA(cudaMemcpyAsync(c->sdf.ptr + d.sdf_word_count, d.sdf_shadow_blob, d.sdf_shadow_word_count * 4,
                                 cudaMemcpyHostToDevice, st));
+    // the texture table: texels concatenated, per image its first texel and size
+    std::vector<uint4> tab(d.image_count);
+    uint64_t texel_words = 0;
+    for (uint32_t k = 0; k < d.image_count; ++k) {
+        tab[k] = make_uint4(uint32_t(texel_words), d.images[k].width, d.images[k].height, 0u);
+        texel_words += uint64_t(d.images[k].width) * d.images[k].height;
+    }
+    c->texels.reserve(texel_words);
+    for (uint32_t k = 0; k < d.image_count; ++k)
+        TK_CUDA(cudaMemcpyAsync(c->texels.ptr + tab[k].x, d.images[k].premul_rgba8,
+                                uint64_t(tab[k].y) * tab[k].z * 4, cudaMemcpyHostToDevice, st));
+    upload(c->image_tab, tab.data(), tab.size(), st);
     c->paints.reserve(d.draw_count);
     tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count,
-                           uint32_t(c->sdf_shadow_base), c->paints.ptr, st);
+                           uint32_t(c->sdf_shadow_base), c->image_tab.ptr, d.image_count, c->paints.ptr, st);
     upload(c->layers, d.layers, d.layer_count, st);
     upload(c->batch_ids, d.draw_batch_ids, d.draw_count, st);
     upload(c->order, d.draw_order, d.draw_order_count, st);
@@ -910,6 +948,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     for (uint32_t s = 0; s < n; ++s) {
         const tk_scene_desc& d = scenes[s];
         if (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) invalid("batched scenes use host segment planning");
+        if (d.image_count) invalid("scene " + std::to_string(s) + ": image patterns are not batched");
         validate_and_plan(c, d);
         ext = ext || c->sdf_ext;
         uint32_t npass = 0;
@@ -1049,7 +1088,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     upload(c->sdf, sdf.data(), sdf.size(), st);
     c->paints.reserve(draws.size());
     tk::launch_paint_table(c->draws.ptr, uint32_t(draws.size()), c->brush.ptr, brush.size(),
-                           uint32_t(c->sdf_shadow_base), c->paints.ptr, st);
+                           uint32_t(c->sdf_shadow_base), nullptr, 0u, c->paints.ptr, st);
     upload(c->layers, layers.data(), layers.size(), st);
     upload(c->batch_ids, batch_ids.data(), batch_ids.size(), st);
     upload(c->order, order.data(), order.size(), st);

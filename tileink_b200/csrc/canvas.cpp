@@ -352,9 +352,12 @@ struct Cmd {
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE } kind = FILL;
     tk_path path;
     tk_sdf_shape shape{};
+    // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options
+    std::shared_ptr<const std::vector<uint32_t>> texels;
+    uint32_t iw = 0, ih = 0, extend = 0, sampling = 0, opacity = 255;
     bool has_brush = false;
     tk_brush_desc brush{};
     std::vector<tk_gradient_stop> stops;
@@ -394,6 +397,9 @@ struct tk_canvas {
     std::vector<tk_draw_record> draws;
     std::vector<uint32_t> brush;
     std::vector<uint32_t> sdf, shadow;  // SDF and SDF shadow records (Canvas::sdf_blob, sdf_shadow_blob)
+    // registered images (Canvas::scene_images) and their texture table
+    std::vector<std::shared_ptr<const std::vector<uint32_t>>> images;
+    std::vector<tk_image_desc> image_table;
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -1138,7 +1144,14 @@ int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_
 namespace {
 // The SDF draw of `shape` with `tag`; -2 when it draws nothing, -1 on error.
 int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush, uint32_t tag,
-                     bool emit_command);
+                     bool emit_command, const uint32_t* brush_words = nullptr);
+int32_t add_image(tk_canvas* c, std::shared_ptr<const std::vector<uint32_t>> texels, uint32_t w, uint32_t h) {
+    for (size_t k = 0; k < c->images.size(); ++k)  // register_scene_image: one entry per image
+        if (c->images[k] == texels) return int32_t(k);
+    c->images.push_back(texels);
+    c->image_table.push_back(tk_image_desc{texels->data(), w, h});
+    return int32_t(c->images.size() - 1);
+}
 }  // namespace
 
 extern "C" {
@@ -1151,6 +1164,62 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
         c->log.push_back(std::move(r));
     }
     return add_sdf_draw(c, shape, brush, TK_DRAW_BRUSH, true);
+}
+
+int32_t tk_canvas_add_image(tk_canvas* c, const uint32_t* premul_rgba8, uint32_t width, uint32_t height) {
+    if (!c || !premul_rgba8 || width == 0u || height == 0u) return -1;
+    const size_t n = size_t(width) * height;
+    return add_image(c, std::make_shared<const std::vector<uint32_t>>(premul_rgba8, premul_rgba8 + n), width, height);
+}
+
+int64_t tk_canvas_push_image(tk_canvas* c, const double rect[4], uint32_t image, uint32_t extend,
+                             uint32_t sampling, uint32_t opacity) {
+    if (!c || !rect || image >= c->images.size() || extend > TK_EXTEND_REFLECT || sampling > TK_PATTERN_BILINEAR ||
+        opacity > 255u)
+        return -1;
+    // image_rect_is_valid / rect_is_valid_image_target (shared/brush.rs:627-634)
+    const double x0 = rect[0], y0 = rect[1], x1 = rect[2], y1 = rect[3];
+    if (!std::isfinite(x0) || !std::isfinite(y0) || !std::isfinite(x1) || !std::isfinite(y1) || !(x1 - x0 > 0.0) ||
+        !(y1 - y0 > 0.0))
+        return -1;
+    const tk_image_desc& im = c->image_table[image];
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::IMAGE, nullptr, nullptr, nullptr);
+        r.shape.p0[0] = x0;
+        r.shape.p0[1] = y0;
+        r.shape.p1[0] = x1;
+        r.shape.p1[1] = y1;
+        r.texels = c->images[image];
+        r.iw = im.width;
+        r.ih = im.height;
+        r.extend = extend;
+        r.sampling = sampling;
+        r.opacity = opacity;
+        c->log.push_back(std::move(r));
+    }
+    // Brush::for_rect_resource (shared/brush.rs:557-580), then physical_brush's
+    // scale_brush_transform(transform, 1 / scale) (canvas/surface.rs:395-400, canvas.rs:203-212)
+    const float sx = 1.0f / float(x1 - x0), sy = 1.0f / float(y1 - y0);
+    const float inv_scale = 1.0f / c->scale;
+    const float t[6] = {sx * inv_scale, 0.0f * inv_scale, 0.0f * inv_scale, sy * inv_scale, -float(x0) * sx,
+                        -float(y0) * sy};
+    uint32_t words[TK_BRUSH_HEADER_WORDS + TK_BRUSH_PARAM_WORDS] = {};
+    words[0] = TK_BRUSH_PATTERN_RESOURCE;
+    words[1] = extend;
+    words[4] = TK_BRUSH_TEXTURE_PLACEMENT_BIT | image;
+    words[5] = im.width;
+    words[6] = im.height;
+    words[7] = opacity;
+    words[8] = sampling;
+    for (int k = 0; k < 6; ++k) words[TK_BRUSH_HEADER_WORDS + k] = fbits(t[k]);
+    // Canvas::push_rect(rect, Radius::ZERO, brush)
+    tk_sdf_shape shape{};
+    shape.kind = TK_SDF_RECT;
+    shape.p0[0] = x0;
+    shape.p0[1] = y0;
+    shape.p1[0] = x1;
+    shape.p1[1] = y1;
+    return add_sdf_draw(c, &shape, nullptr, TK_DRAW_BRUSH, true, words);
 }
 
 int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape) {
@@ -1178,7 +1247,7 @@ int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape) {
 
 namespace {
 int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush, uint32_t tag,
-                     bool emit_command) {
+                     bool emit_command, const uint32_t* brush_words) {
     const uint32_t k = shape->kind;
     if (k != TK_SDF_RECT && k != TK_SDF_RECT_STROKE && k != TK_SDF_RECT_SHADOW && k != TK_SDF_CIRCLE &&
         k != TK_SDF_CIRCLE_STROKE && k != TK_SDF_CIRCLE_SHADOW && k != TK_SDF_LINE && k != TK_SDF_LINE_SHADOW &&
@@ -1199,7 +1268,13 @@ int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_des
     blob.insert(blob.end(), rec, rec + TK_SDF_RECORD_WORDS);
     tk_brush_desc transparent{};
     transparent.kind = TK_BRUSH_KIND_SOLID;
-    auto br = push_brush(c->brush, brush ? *brush : transparent);
+    std::pair<uint32_t, uint32_t> br;
+    if (brush_words) {  // a prebuilt image pattern brush
+        br = {uint32_t(c->brush.size()), TK_BRUSH_HEADER_WORDS + TK_BRUSH_PARAM_WORDS};
+        c->brush.insert(c->brush.end(), brush_words, brush_words + br.second);
+    } else {
+        br = push_brush(c->brush, brush ? *brush : transparent);
+    }
     // push_physical_sdf_record / push_physical_sdf_shadow_record (canvas/paths.rs:207-300)
     tk_draw_record d{};
     d.path_id = TK_INVALID_INDEX;
@@ -1288,6 +1363,8 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->sdf_word_count = c->sdf.size();
     out->sdf_shadow_blob = c->shadow.data();
     out->sdf_shadow_word_count = c->shadow.size();
+    out->images = c->image_table.data();
+    out->image_count = uint32_t(c->image_table.size());
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -1718,6 +1795,19 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
             }
             return r.kind == RecCmd::SDF_CLIP ? tk_canvas_push_clip_sdf_layer(dst, &sh)
                                               : (tk_canvas_push_sdf(dst, &sh, bp) == -1 ? -1 : 0);
+        }
+        case RecCmd::IMAGE: {
+            // the brush maps the image into the rect: a translated rect carries it along
+            double rect[4] = {r.shape.p0[0], r.shape.p0[1], r.shape.p1[0], r.shape.p1[1]};
+            if (t) {
+                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+                rect[0] += t[4];
+                rect[1] += t[5];
+                rect[2] += t[4];
+                rect[3] += t[5];
+            }
+            const int32_t ix = add_image(dst, r.texels, r.iw, r.ih);
+            return tk_canvas_push_image(dst, rect, uint32_t(ix), r.extend, r.sampling, r.opacity) == -1 ? -1 : 0;
         }
     }
     return -1;

@@ -34,7 +34,7 @@ constexpr uint32_t kChunkClassColor = 1u, kChunkClassSdf = 2u, kChunkClassOther 
 // DrawInfo::meta bits
 constexpr uint32_t kMetaPath = 16u, kMetaSolid = 32u, kMetaSdf = 64u, kMetaSdfSolidClass = 128u;
 // DrawInfo::py bits of an SDF draw (px holds its first SDF word)
-constexpr uint32_t kSdfPlain = 256u, kSdfIdentity = 512u;
+constexpr uint32_t kSdfPlain = 256u, kSdfIdentity = 512u, kSdfImage = 1024u;
 // Candidates whose tile loads are in flight together, per pass (emission
 // keeps more state live and holds fewer).
 constexpr uint32_t kPrefetchCount = 8, kPrefetchEmit = 4;
@@ -266,11 +266,14 @@ static __device__ __noinline__ uint32_t sdf_particle(const tk_draw_record* draws
                                                      uint32_t ty) {
     const uint32_t kind = bits & 255u;
     const bool proof = (bits & kSdfPlain) && (bits & kSdfIdentity) &&
-                       (kind == TK_SDF_RECT_STROKE || (kind == TK_SDF_RECT && (meta & kMetaSolid)));
+                       (kind == TK_SDF_RECT_STROKE ||
+                        (kind == TK_SDF_RECT && ((meta & kMetaSolid) || (bits & kSdfImage))));
     if (!proof) return TK_PTCL_SDF;
     const float ex = draws[draw].transform.e, ey = draws[draw].transform.f;
     if (kind == TK_SDF_RECT_STROKE) return sdf_stroke_empty(sdf + word, ex, ey, tx, ty) ? 0u : TK_PTCL_SDF;
-    return sdf_rect_covers(sdf + word, ex, ey, tx, ty) ? TK_PTCL_COLOR : TK_PTCL_SDF;
+    // full_tile_solid, then full_tile_image (coarse/paint.hlsli:27-34)
+    if (!sdf_rect_covers(sdf + word, ex, ey, tx, ty)) return TK_PTCL_SDF;
+    return (meta & kMetaSolid) ? TK_PTCL_COLOR : TK_PTCL_IMAGE;
 }
 
 // SDF: whether the scene has SDF records; path-only scenes run the instance
@@ -373,7 +376,12 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 const uint32_t kind = __ldg(c.sdf + info.px);
                 const bool ident = d.transform.a == 1.0f && d.transform.b == 0.0f && d.transform.c == 0.0f &&
                                    d.transform.d == 1.0f;
-                info.py = (kind & 255u) | (plain ? kSdfPlain : 0u) | (ident ? kSdfIdentity : 0u);
+                // full_tile_image's brush test: an image pattern at full opacity
+                const bool image = d.brush_offset != TK_INVALID_INDEX &&
+                                   brush_word(c, d.brush_offset) == TK_BRUSH_PATTERN_RESOURCE &&
+                                   brush_word(c, d.brush_offset + TK_BRUSH_IMAGE_ALPHA_WORD) == 255u;
+                info.py = (kind & 255u) | (plain ? kSdfPlain : 0u) | (ident ? kSdfIdentity : 0u) |
+                          (image ? kSdfImage : 0u);
                 if (d.tag == TK_DRAW_BRUSH) sdf_bits |= kMetaSdf;
                 const bool solid = solid_paint();
                 if (solid) {
@@ -466,7 +474,8 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     // particle_class_flags (coarse/paint.hlsli:35-40)
                     uint32_t cls = kChunkClassOther;
                     if (ptag == TK_PTCL_COLOR) cls = kChunkClassColor;
-                    else if (ptag == TK_PTCL_SDF && (meta & kMetaSdfSolidClass)) cls = kChunkClassSdf;
+                    else if (ptag == TK_PTCL_IMAGE || (ptag == TK_PTCL_SDF && (meta & kMetaSdfSolidClass)))
+                        cls = kChunkClassSdf;
                     flags |= cls;
                     uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
                     if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;

@@ -326,6 +326,7 @@ __device__ __forceinline__ float segment_area_at(float xmin_abs, float xmax_abs,
 struct Paint {
     const uint32_t* __restrict__ words;
     uint64_t count;
+    const uint32_t* __restrict__ texels = nullptr;  // the scene's images (PaintInfo gives each one's first texel)
     __device__ __forceinline__ uint32_t word(uint32_t index) const { return index < count ? __ldg(words + index) : 0u; }
     __device__ __forceinline__ float param(uint32_t base, uint32_t i) const { return __uint_as_float(word(base + i)); }
 };

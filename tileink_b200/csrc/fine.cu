@@ -42,7 +42,8 @@ constexpr uint32_t kGroupDepth = 6;
 constexpr uint32_t kGroupLocal = 2;  // FINE_LOCAL_GROUP_DEPTH (fine/constants.hlsli:11)
 constexpr uint32_t kGradient = 0xFFFFFFFFu;
 constexpr uint32_t kGradParams = 24;
-constexpr uint32_t kGradConst = 0, kGradLinear = 1, kGradRadial = 2;  // decoded kinds
+constexpr uint32_t kGradConst = 0, kGradLinear = 1, kGradRadial = 2, kGradPattern = 3;  // decoded kinds
+constexpr uint32_t kGradBilinear = 1u << 16;  // pattern: bilinear sampling
 constexpr uint32_t kGradDenOk = 1u << 16;    // linear: den > GRADIENT_FLOAT_EPSILON
 constexpr uint32_t kGradASmall = 1u << 16;   // radial: |a| <= RADIAL_QUADRATIC_EPSILON
 
@@ -103,11 +104,13 @@ __device__ __forceinline__ float4 texel_load_lut(const FineSmem& S, uint32_t p) 
 //   linear: gp[12..16] = sx, sy, dx = ex - sx, dy = ey - sy, den = dx*dx + dy*dy
 //   radial: gp[12..22] = sx, sy, dcx, dcy, sr*dr, -sr*sr, a, -4*a, 2*a, dr, sr
 //           with a = mad(dcx, dcx, mad(dcy, dcy, -dr*dr))
-__device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db, const float* __restrict__ m) {
+__device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db, const float* __restrict__ m,
+                                const uint4* __restrict__ images, uint32_t image_count) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) g[k] = __ldg(m + k);
     const uint32_t kind = P.word(db), extend = P.word(db + 1u);
-    const uint32_t payload = db + P.word(db + 2u), len = P.word(db + 3u);
+    const uint32_t payload = db + P.word(db + 2u);
+    uint32_t len = P.word(db + 3u);
     const uint32_t base = db + TK_BRUSH_HEADER_WORDS;
     uint32_t code = kGradConst, flags = 0u, word = 0u;
     if (kind == TK_BRUSH_LINEAR) {
@@ -143,6 +146,23 @@ __device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db
         g[22] = sr;
         if (fabsf(a) <= RADIAL_QUADRATIC_EPSILON) flags = kGradASmall;
         word = payload;
+    } else if (kind == TK_BRUSH_PATTERN_RESOURCE) {
+        // sample_brush's texture-table branch (shared/brush/sample.hlsli:32-41):
+        //   gp[6..11] the pattern transform, gp[12..13] the size as floats,
+        //   gp[14..15] the size as integers; gk = kind, first texel, opacity, extend
+        const uint32_t placement = P.word(db + 4u), w = P.word(db + 5u), h = P.word(db + 6u);
+        const uint32_t ix = placement & ~TK_BRUSH_TEXTURE_PLACEMENT_BIT;
+        if (w != 0u && h != 0u && (placement & TK_BRUSH_TEXTURE_PLACEMENT_BIT) && ix < image_count) {
+            code = kGradPattern;
+            for (uint32_t k = 0; k < 6u; ++k) g[6 + k] = P.param(base, k);
+            g[12] = float(w);
+            g[13] = float(h);
+            g[14] = __uint_as_float(w);
+            g[15] = __uint_as_float(h);
+            if (P.word(db + 8u) == TK_PATTERN_BILINEAR) flags = kGradBilinear;
+            word = images[ix].x;
+            len = P.word(db + TK_BRUSH_IMAGE_ALPHA_WORD);
+        }
     } else {
         word = kind == 6u ? 0u : P.word(db + TK_BRUSH_COLOR_WORD);  // BRUSH_PATTERN samples as 0
     }
@@ -152,7 +172,8 @@ __device__ void decode_gradient(float* g, uint4& gk, const Paint& P, uint32_t db
 // One thread per draw: the draw's PaintInfo (solid colour, or the decoded
 // gradient of its brush under its inverse transform).
 __global__ void k_paint_table(const tk_draw_record* __restrict__ draws, uint32_t n, const uint32_t* __restrict__ brush,
-                              uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out) {
+                              uint64_t brush_words, uint32_t sdf_shadow_base, const uint4* __restrict__ images,
+                              uint32_t image_count, PaintInfo* out) {
     const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d >= n) return;
     const Paint P{brush, brush_words};
@@ -165,9 +186,79 @@ __global__ void k_paint_table(const tk_draw_record* __restrict__ draws, uint32_t
         info.paint = P.word(bo + TK_BRUSH_COLOR_WORD);
     } else {
         info.paint = kGradient;
-        decode_gradient(info.g, info.gk, P, bo, &draws[d].inverse_transform.a);
+        decode_gradient(info.g, info.gk, P, bo, &draws[d].inverse_transform.a, images, image_count);
     }
     out[d] = info;
+}
+
+// extend_coord_i32 (shared/brush/pattern.hlsli:9-17) with
+// euclidean_remainder_i32 (shared/integer.hlsli:5-9).
+__device__ __forceinline__ uint32_t extend_coord(int32_t v, uint32_t size, uint32_t extend) {
+    if (size <= 1u) return 0u;
+    if (extend == TK_EXTEND_REPEAT || extend == TK_EXTEND_REFLECT) {
+        const uint32_t period = size * (extend == TK_EXTEND_REFLECT ? 2u : 1u);
+        const uint32_t mag = v < 0 ? 0u - uint32_t(v) : uint32_t(v), rem = mag % period;
+        const uint32_t coord = v < 0 && rem != 0u ? period - rem : rem;
+        return coord < size ? coord : period - coord - 1u;
+    }
+    return uint32_t(min(max(v, 0), int32_t(size) - 1));
+}
+
+// lerp_premul_u8 (shared/pixel.hlsli:55-62): one fused interpolation per channel.
+__device__ __forceinline__ uint32_t lerp_premul_u8(uint32_t a, uint32_t b, float t) {
+    uint32_t out = 0u;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float l = float((a >> (8 * c)) & 255u), r = float((b >> (8 * c)) & 255u);
+        out |= f2u(clampf(mad(r - l, t, l) + 0.5f, 0.0f, 255.0f)) << (8 * c);
+    }
+    return out;
+}
+
+// The image pattern decoded in g / k at brush-space point (x, y):
+// pattern_transform_component (shared/pattern_transform.hlsli:7-11) and
+// sample_resource_pattern_texture (shared/brush/texture.hlsli:11-31). Float to
+// integer conversions saturate and take NaN to 0. The bilinear, pad-extended
+// form is the texture unit's filter in the reference (SampleLevel with
+// clamp-to-edge addressing); here it is that filter computed exactly: texel
+// centres at half-integers, f32 weights, one rounding to 8 bits.
+__device__ __noinline__ uint32_t pattern_at(const Paint& P, const float* g, uint4 k, float x, float y) {
+    const float bx = g[8] * y, by = g[9] * y;
+    const float tx = ((mad(g[6], x, bx) + mad(g[8], y, -bx)) + g[10]) * g[12];
+    const float ty = ((mad(g[7], x, by) + mad(g[9], y, -by)) + g[11]) * g[13];
+    const uint32_t w = __float_as_uint(g[14]), h = __float_as_uint(g[15]), extend = k.w;
+    const uint32_t* __restrict__ tex = P.texels + k.y;
+    uint32_t color;
+    if ((k.x & kGradBilinear) && extend == TK_EXTEND_PAD) {
+        const float sx = clampf(tx, 0.0f, g[12]) - 0.5f, sy = clampf(ty, 0.0f, g[13]) - 0.5f;
+        const float fx0 = floorf(sx), fy0 = floorf(sy), fx = sx - fx0, fy = sy - fy0;
+        const int32_t ix = __float2int_rz(fx0), iy = __float2int_rz(fy0);
+        const uint32_t x0 = uint32_t(min(max(ix, 0), int32_t(w) - 1)), x1 = uint32_t(min(max(ix + 1, 0), int32_t(w) - 1));
+        const uint32_t y0 = uint32_t(min(max(iy, 0), int32_t(h) - 1)), y1 = uint32_t(min(max(iy + 1, 0), int32_t(h) - 1));
+        const float4 tl = rgba8_to_unorm(__ldg(tex + uint64_t(y0) * w + x0)), tr = rgba8_to_unorm(__ldg(tex + uint64_t(y0) * w + x1));
+        const float4 bl = rgba8_to_unorm(__ldg(tex + uint64_t(y1) * w + x0)), br = rgba8_to_unorm(__ldg(tex + uint64_t(y1) * w + x1));
+        const float4 top = make_float4(mad(tr.x - tl.x, fx, tl.x), mad(tr.y - tl.y, fx, tl.y), mad(tr.z - tl.z, fx, tl.z),
+                                       mad(tr.w - tl.w, fx, tl.w));
+        const float4 bot = make_float4(mad(br.x - bl.x, fx, bl.x), mad(br.y - bl.y, fx, bl.y), mad(br.z - bl.z, fx, bl.z),
+                                       mad(br.w - bl.w, fx, bl.w));
+        color = unorm_to_rgba8(make_float4(mad(bot.x - top.x, fy, top.x), mad(bot.y - top.y, fy, top.y),
+                                           mad(bot.z - top.z, fy, top.z), mad(bot.w - top.w, fy, top.w)));
+    } else if (k.x & kGradBilinear) {
+        const float sx = tx - 0.5f, sy = ty - 0.5f;
+        const float fx0 = floorf(sx), fy0 = floorf(sy), fx = sx - fx0, fy = sy - fy0;
+        const int32_t ix = __float2int_rz(fx0), iy = __float2int_rz(fy0);
+        const int32_t jx = int32_t(uint32_t(ix) + 1u), jy = int32_t(uint32_t(iy) + 1u);
+        const uint64_t r0 = uint64_t(extend_coord(iy, h, extend)) * w, r1 = uint64_t(extend_coord(jy, h, extend)) * w;
+        const uint32_t c0 = extend_coord(ix, w, extend), c1 = extend_coord(jx, w, extend);
+        const uint32_t top = lerp_premul_u8(__ldg(tex + r0 + c0), __ldg(tex + r0 + c1), fx);
+        const uint32_t bot = lerp_premul_u8(__ldg(tex + r1 + c0), __ldg(tex + r1 + c1), fx);
+        color = lerp_premul_u8(top, bot, fy);
+    } else {
+        const uint32_t c = extend_coord(__float2int_rz(floorf(tx)), w, extend);
+        const uint32_t r = extend_coord(__float2int_rz(floorf(ty)), h, extend);
+        color = __ldg(tex + uint64_t(r) * w + c);
+    }
+    return scale_premul_u8(color, k.z);
 }
 
 // sample_gradient at pixel centre (px, py) for the gradient decoded in slot i.
@@ -178,6 +269,7 @@ __device__ __forceinline__ uint32_t gradient_at(const FineSmem& S, const Paint& 
     if (code == kGradConst) return k.y;
     const float x = mad(g[0], px, mad(g[2], py, g[4]));
     const float y = mad(g[1], px, mad(g[3], py, g[5]));
+    if (code == kGradPattern) return pattern_at(P, g, k, x, y);
     const float tx = mad(g[6], x, mad(g[8], y, g[10]));
     const float ty = mad(g[7], x, mad(g[9], y, g[11]));
     float t = 0.0f;
@@ -399,8 +491,8 @@ template <uint32_t SDF>
 __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
-           const uint32_t* __restrict__ brush, uint64_t brush_words, const tk_draw_record* __restrict__ draws,
-           const uint32_t* __restrict__ sdf, uint64_t seg_capacity, uint32_t* target,
+           const uint32_t* __restrict__ brush, uint64_t brush_words, const uint32_t* __restrict__ texels,
+           const tk_draw_record* __restrict__ draws, const uint32_t* __restrict__ sdf, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
            const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -422,7 +514,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
     const uint32_t gx = (ltile % tw) * TK_TILE_SIZE + lx, gy = (ltile / tw) * TK_TILE_SIZE + ly;
     const bool inside = gx < width && gy < height;
     const uint64_t pix = uint64_t(gy) * width + gx;
-    const Paint P{brush, brush_words};
+    const Paint P{brush, brush_words, texels};
     S.unorm[tid] = float(tid) / 255.0f;
     __syncthreads();
     float4 px = inside ? texel_load_lut(S, target[pix]) : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -462,7 +554,8 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
             }
             S.nseg[tid] = n;
             if (SDF != 0u && a.x == TK_PTCL_BEGIN_SDF_CLIP) S.umode[tid] = __ldg(&paints[c.y].sdf);
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (SDF != 0u && a.x == TK_PTCL_SDF)) {
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH ||
+                (SDF != 0u && (a.x == TK_PTCL_SDF || a.x == TK_PTCL_IMAGE))) {
                 const PaintInfo* pi = paints + c.y;
                 if (SDF != 0u && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
                 const uint32_t paint = __ldg(&pi->paint);
@@ -605,13 +698,15 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                         px = src_over_premul_unorm(v.parent, scale_premul_u8_to_unorm(unorm_to_rgba8(px), a));
                     }
                 }
-            } else if (SDF != 0u && (tag == TK_PTCL_SDF || tag == TK_PTCL_BEGIN_SDF_CLIP)) {
+            } else if (SDF != 0u && (tag == TK_PTCL_SDF || tag == TK_PTCL_BEGIN_SDF_CLIP || tag == TK_PTCL_IMAGE)) {
                 // PTCL_SDF (fine/interpreter.hlsli:70-84) and BEGIN_SDF_CLIP (131-150):
-                // the shape's quantized coverage, one evaluation for both
+                // the shape's quantized coverage, one evaluation for both;
+                // PTCL_IMAGE (65-69): the brush over the whole tile
                 uint32_t alpha = 0u;
                 if (clip != 0u)
-                    alpha = coverage_to_u8(
-                        sdf_coverage_at<SDF == 2u>(sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy));
+                    alpha = tag == TK_PTCL_IMAGE ? 255u
+                                                 : coverage_to_u8(sdf_coverage_at<SDF == 2u>(
+                                                       sdf + S.umode[i], &draws[qb.y].inverse_transform, gx, gy));
                 if (tag == TK_PTCL_BEGIN_SDF_CLIP) {  // push the mask, then narrow it
                     if (cdepth < 4u) {
                         cregs = (cregs & ~(255u << (8u * cdepth))) | (clip << (8u * cdepth));
@@ -623,6 +718,10 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                         atomicOr(error, ERR_STACK_DEPTH);
                     }
                     clip = combine_alpha(clip, alpha);
+                } else if (tag == TK_PTCL_IMAGE && (mode == TK_TILE_KIND_SDF || mode == TK_TILE_KIND_MIXED)) {
+                    // analytic tiles (fine/specialized.hlsli:84-90): the sample over the pixel, unscaled
+                    const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
+                    px = premul_u8_is_opaque(g) ? rgba8_to_unorm(g) : src_over_premul_unorm(px, rgba8_to_unorm(g));
                 } else {
                     const uint32_t masked = combine_alpha(alpha, clip);
                     if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
@@ -710,10 +809,11 @@ __global__ void k_star_table() {
 }  // namespace
 
 void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
-                        uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out, cudaStream_t st) {
+                        uint64_t brush_words, uint32_t sdf_shadow_base, const uint4* images, uint32_t image_count,
+                        PaintInfo* out, cudaStream_t st) {
     if (draw_count)
         k_paint_table<<<(draw_count + 255) / 256, 256, 0, st>>>(draws, draw_count, brush, brush_words,
-                                                                sdf_shadow_base, out);
+                                                                sdf_shadow_base, images, image_count, out);
 }
 
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st) {
@@ -729,7 +829,7 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     if (s.sdf_ext) k_star_table<<<1, 32, 0, st>>>();
     auto kernel = !s.sdf_words ? k_fine<0u> : (s.sdf_ext ? k_fine<2u> : k_fine<1u>);
     kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
-                                                      s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,
+                                                      s.texels, s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,
                                                       s.tw, s.error, p.scenes, p.tile_scene, p.tile_list);
 }
 

@@ -70,6 +70,7 @@ struct SceneView {
     uint64_t sdf_words;
     uint64_t sdf_shadow_base;
     bool sdf_ext;  // some record is of an extended kind (fine's k_fine<2>)
+    const uint32_t* texels;  // the scene's images, concatenated (premultiplied RGBA8)
     const tk_layer_record* layers;
     const uint32_t* batch_ids;
     const uint32_t* order;
@@ -159,8 +160,10 @@ void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st);
 // The per-draw PaintInfo table of the uploaded draws and brush blob; shadow
 // records start at word sdf_shadow_base of the device SDF buffer.
+// images: per image of the texture table its first texel, width and height.
 void launch_paint_table(const tk_draw_record* draws, uint32_t draw_count, const uint32_t* brush,
-                        uint64_t brush_words, uint32_t sdf_shadow_base, PaintInfo* out, cudaStream_t st);
+                        uint64_t brush_words, uint32_t sdf_shadow_base, const uint4* images, uint32_t image_count,
+                        PaintInfo* out, cudaStream_t st);
 
 // Images.
 void launch_fill(uint32_t* image, uint64_t n, uint32_t value, cudaStream_t st);
