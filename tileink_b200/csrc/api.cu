@@ -304,6 +304,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             if (ix >= d.image_count) invalid(at + ": image index out of range");
             if (w[5] != d.images[ix].width || w[6] != d.images[ix].height)
                 invalid(at + ": image brush size differs from its image");
+            if (!plain) invalid(at + ": image patterns fill SDF rects only");
             if (w[1] > TK_EXTEND_REFLECT || w[7] > 255u || w[8] > TK_PATTERN_BILINEAR)
                 invalid(at + ": bad image brush extend, opacity or sampling");
         }

@@ -262,6 +262,8 @@ __device__ __noinline__ uint32_t pattern_at(const Paint& P, const float* g, uint
 }
 
 // sample_gradient at pixel centre (px, py) for the gradient decoded in slot i.
+// IMG: whether image patterns can occur (only SDF draws carry them).
+template <bool IMG>
 __device__ __forceinline__ uint32_t gradient_at(const FineSmem& S, const Paint& P, uint32_t i, float px, float py) {
     const float* g = S.gp[i];
     const uint4 k = S.gk[i];
@@ -269,7 +271,7 @@ __device__ __forceinline__ uint32_t gradient_at(const FineSmem& S, const Paint& 
     if (code == kGradConst) return k.y;
     const float x = mad(g[0], px, mad(g[2], py, g[4]));
     const float y = mad(g[1], px, mad(g[3], py, g[5]));
-    if (code == kGradPattern) return pattern_at(P, g, k, x, y);
+    if (IMG && code == kGradPattern) return pattern_at(P, g, k, x, y);
     const float tx = mad(g[6], x, mad(g[8], y, g[10]));
     const float ty = mad(g[7], x, mad(g[9], y, g[11]));
     float t = 0.0f;
@@ -462,6 +464,7 @@ static __device__ __forceinline__ float sdf_coverage_at(const uint32_t* w, const
 
 // Paints a fill's masked coverage over px (the brush branch of
 // fine/interpreter.hlsli's fill handling, fine/draw.hlsli:16-21).
+template <bool IMG>
 __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, uint32_t i, uint32_t masked,
                                            uint32_t gx, uint32_t gy, float4& px) {
     const uint32_t paint = S.paint[i];
@@ -475,7 +478,7 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
             if (c.w != 0.0f) px = src_over_premul_unorm(px, make_float4(c.x * sc, c.y * sc, c.z * sc, c.w * sc));
         }
     } else {
-        const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
+        const uint32_t g = gradient_at<IMG>(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
         if (masked == 255u && premul_u8_is_opaque(g)) px = rgba8_to_unorm(g);
         else px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(g, masked));
     }
@@ -644,7 +647,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                 // the common record: a path fill with segments in the tile
                 const uint32_t alpha = coverage_to_alpha(staged_coverage(S, i, lx, ly), S.rec_a[i].z);
                 const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
-                if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
+                if (masked != 0u) paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                 ++i;
                 continue;
             }
@@ -720,11 +723,11 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                     clip = combine_alpha(clip, alpha);
                 } else if (tag == TK_PTCL_IMAGE && (mode == TK_TILE_KIND_SDF || mode == TK_TILE_KIND_MIXED)) {
                     // analytic tiles (fine/specialized.hlsli:84-90): the sample over the pixel, unscaled
-                    const uint32_t g = gradient_at(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
+                    const uint32_t g = gradient_at<true>(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
                     px = premul_u8_is_opaque(g) ? rgba8_to_unorm(g) : src_over_premul_unorm(px, rgba8_to_unorm(g));
                 } else {
                     const uint32_t masked = combine_alpha(alpha, clip);
-                    if (masked != 0u) paint_fill(S, P, i, masked, gx, gy, px);
+                    if (masked != 0u) paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                 }
             } else if (is_fill_like(tag)) {
                 uint32_t alpha;
@@ -785,7 +788,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                     const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
                     if (masked != 0u) {
                         if (tag == TK_PTCL_PATH_GLYPH) atomicOr(error, ERR_UNSUPPORTED);
-                        paint_fill(S, P, i, masked, gx, gy, px);
+                        paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                     }
                 }
             }
