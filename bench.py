@@ -129,6 +129,15 @@ def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def fp32_peak_tflops() -> float:
+    """The FP32 FMA peak measured on a B200 by fp32_probe.cu, committed in
+    profiles/fp32_peak_fma.txt."""
+    for line in (ROOT / "profiles" / "fp32_peak_fma.txt").read_text().splitlines():
+        if line.startswith("fp32_tflops "):
+            return float(line.split()[1])
+    raise RuntimeError("profiles/fp32_peak_fma.txt has no fp32_tflops line")
+
+
 def measured_peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -541,13 +550,13 @@ def main():
     stage_ms = {k: v / args.steps for k, v in stage_sum.items()}
     peaks = measured_peaks()
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    fp32_peak = r.probe_fp32_tflops()
+    fp32_peak = fp32_peak_tflops()
     T = stats["tiles"]
     L, B, S = stats["lines"], stats["backdrop_len"], stats["segments"]
     K, refs = stats["ptcl_records"], stats["tile_draw_refs"]
     fills, visits = stats["fill_particles"], stats["segment_visits"]
     algo = {
-        # bytes per launch (SURVEY-defined algorithmic traffic)
+        # algorithmic bytes per launch (the bytes each stage must move)
         "scan_count": ("hbm", 24 * L + 4 * S),
         "pool_scan": ("hbm", (4 + 4 + 8 + 4 + 4) * B),
         "scan_emit": ("hbm", 24 * L + 20 * S),
@@ -572,7 +581,7 @@ def main():
     dominant = max(rooflines, key=lambda k: rooflines[k]["ms"])
     roof = dict(rooflines[dominant])
     roof["kernel"] = dominant
-    roof["peak_source"] = ("measured FMA probe (tk_probe_fp32_tflops)" if roof["bound"] == "fp32"
+    roof["peak_source"] = ("measured FMA probe (fp32_probe.cu, profiles/fp32_peak_fma.txt)" if roof["bound"] == "fp32"
                            else "measured (MEASURED_PEAKS.json hbm_gbs)")
     # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from
     # the committed ncu launch list of the default 4096^2 / 50k workload; other

@@ -145,7 +145,13 @@ extern "C" {
 #define TK_EXTEND_REFLECT 2u
 
 /* One image of a scene's texture table: premultiplied RGBA8 texels (red in
- * the low byte), row-major and tightly packed, width * height words. */
+ * the low byte), row-major and tightly packed, width * height words. Width
+ * and height are at most TK_MAX_IMAGE_DIMENSION: the reference rejects a
+ * texture larger than the device's 2D image limit
+ * (src/native/runtime/vulkan/limits.rs:111-121), 16384 on its DX12 and
+ * Vulkan targets, and the pattern sampler's reflect period (twice the size)
+ * must stay inside 32-bit arithmetic. */
+#define TK_MAX_IMAGE_DIMENSION 16384u
 typedef struct tk_image_desc {
     const uint32_t* premul_rgba8;
     uint32_t width;
@@ -323,6 +329,21 @@ typedef struct tk_ctx tk_ctx;
 /* Library version string. */
 const char* tk_version(void);
 
+/* Layout of every struct in tileink.h, tileink_canvas.h and tileink_diff.h as
+ * the library was compiled: one entry per struct (field "" with its size)
+ * followed by one per field (byte offset and size). A binding (the Rust
+ * #[repr(C)] mirrors, ctypes) checks its own declarations against it, as the
+ * reference checks its record layouts (src/shared/gpu_coarse.rs:210-286,
+ * src/shared/draw_record.rs:165-175). Returns the entry count; the table is
+ * static. Needs no device. */
+typedef struct tk_abi_field {
+    const char* type;
+    const char* field;
+    uint32_t offset;
+    uint32_t size;
+} tk_abi_field;
+uint32_t tk_abi_layout(const tk_abi_field** table);
+
 /* Context on CUDA device `device` with its own stream. */
 int32_t tk_ctx_create(int32_t device, tk_ctx** out);
 void tk_ctx_destroy(tk_ctx* ctx);
@@ -377,10 +398,6 @@ int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
 int32_t tk_set_timing(tk_ctx* ctx, int32_t enabled);
 int32_t tk_get_stage_times(tk_ctx* ctx, float* ms, uint32_t count);
 
-/* FP32 FMA throughput of the device in TFLOP/s, measured by a short
- * register-resident FMA loop (the fine stage's roofline denominator). */
-int32_t tk_probe_fp32_tflops(tk_ctx* ctx, double* tflops);
-
 /* ------------------------------------------------------------------------ */
 /* Stage harnesses on host buffers (the reference's per-kernel GPU test      */
 /* harnesses, src/native/runtime/tests/scan_cases.rs:8-213 and               */
@@ -396,6 +413,19 @@ int32_t tk_stage_scan_prefix(tk_ctx* ctx, const uint32_t* counts, uint64_t pool_
                              const tk_path_record* paths, uint32_t path_count,
                              tk_segment_range* ranges, uint32_t* cursors,
                              uint32_t* bumps);
+
+/* Tile prefix (coarse/prefix.hlsl:11-63) on host tile records: the exclusive
+ * scan of tiles[i].ptcl_count into ptcl_start / ptcl_end (glyph words
+ * cleared) and the total record count. The scan's look-back wait gives up
+ * after `poll_limit` polls (0: the renderer's limit, 2^22), and the call then
+ * returns TK_E_TIMEOUT with the context still usable; this is the library's
+ * bounded-wait failure path (the reference latches a failed submission on
+ * its context instead, src/native/runtime/adapter.rs:8-15). withhold_first = 1
+ * is the test of that path: the block tickets start at 1, so block 0's
+ * descriptor is never published and every look-back reaches a predecessor
+ * that never publishes. */
+int32_t tk_stage_tile_prefix(tk_ctx* ctx, tk_tile_record* tiles, uint32_t tile_count,
+                             uint32_t poll_limit, uint32_t withhold_first, uint32_t* total);
 
 /* scan_count on the given lines/paths (scan/count.hlsl:13-40). `backdrops`
  * and `counts` are read, accumulated into and written back. */
@@ -579,12 +609,13 @@ int32_t tk_autotune(tk_ctx* ctx, uint32_t iterations, tk_tune_result* out);
  * Limits: path_count <= TK_NOALLOC_MAX_PATHS and at most
  * TK_NOALLOC_MAX_SCAN_ITEMS work items; larger inputs return TK_E_CAPACITY
  * with a message and launch nothing.
- * Zero state: the descriptors, the ticket and the error word must be zero
- * when the scan kernel starts; the call clears them on the stream before
- * every launch. d_backdrops holds the per-tile backdrop deltas (0 where
- * none) and is replaced by its row-wise inclusive cumsum; d_counts is read
- * only; d_ranges, d_cursors, d_bumps are written (elements outside every
- * path slice are left as they are).
+ * State between calls: the per-item sums and prefixes, the work items and
+ * the copy of `paths` are rewritten by every call before it reads them, so
+ * nothing a previous call left there is used; the call clears its counter
+ * words on the stream before it launches. d_backdrops holds the per-tile
+ * backdrop deltas (0 where none) and is replaced by its row-wise inclusive
+ * cumsum; d_counts is read only; d_ranges, d_cursors, d_bumps are written
+ * (elements outside every path slice are left as they are).
  * First call per device: it looks up the scratch address
  * (cudaGetSymbolAddress with the context's device current), which may load
  * the library's module; make that first call before any stream capture.

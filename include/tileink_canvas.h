@@ -138,7 +138,8 @@ int32_t tk_canvas_push_clip_sdf_layer(tk_canvas* c, const tk_sdf_shape* shape);
 /* Registers an image with the canvas (Canvas::register_scene_image,
  * canvas/primitives/images.rs:42-52): the texels (premultiplied RGBA8, red in
  * the low byte, width * height words, row-major) are copied. Returns the
- * image's index, or -1 for an empty image. */
+ * image's index, or -1 for an empty image or one wider or taller than
+ * TK_MAX_IMAGE_DIMENSION. */
 int32_t tk_canvas_add_image(tk_canvas* c, const uint32_t* premul_rgba8, uint32_t width, uint32_t height);
 /* Canvas::push_image (canvas/primitives/images.rs:9-26): a rect from
  * (x0, y0) to (x1, y1), in logical coordinates, filled with registered image

@@ -63,3 +63,9 @@ def test_gpu_rejects_bad_image_brushes(renderer):
     b["images"] = []
     with pytest.raises(Exception):
         renderer.upload(N.ArrayScene(b))
+    # one side above the 2D texture limit (a reflect period of 2^32 would
+    # wrap the sampler's index arithmetic)
+    wide = c.scene_arrays()
+    wide["images"] = [np.zeros((1, N.MAX_IMAGE_DIMENSION + 1), np.uint32)]
+    with pytest.raises(Exception, match="texture limit"):
+        renderer.upload(N.ArrayScene(wide))

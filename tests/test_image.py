@@ -48,6 +48,11 @@ def test_push_image_rejects_bad_rects_and_images():
         c.push_image(0, 0, 4, 4, ix + 1)
     with pytest.raises(ValueError):
         c.add_image(np.zeros((0, 3), np.uint32))
+    # sides above the 2D texture limit
+    for shape in [(1, N.MAX_IMAGE_DIMENSION + 1), (N.MAX_IMAGE_DIMENSION + 1, 1)]:
+        with pytest.raises(ValueError):
+            c.add_image(np.zeros(shape, np.uint32))
+    assert c.add_image(np.zeros((1, N.MAX_IMAGE_DIMENSION), np.uint32)) >= 0
 
 
 def test_oracle_exact_placement_reproduces_texels():

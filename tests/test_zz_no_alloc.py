@@ -91,8 +91,8 @@ def check_against_stage_harness(renderer, counts, paths, backdrops):
 def test_noalloc_pool_scan_matches_stage_harness_on_consecutive_calls(renderer):
     big = long_paths_case(5)
     small = guard_case()
-    # large, then smaller (stale descriptors beyond the second call's items),
-    # then the large case again
+    # large, then smaller (the first call's per-item sums and prefixes stay
+    # beyond the second call's items), then the large case again
     for counts, paths, backdrops in (big, small, big, long_paths_case(6)):
         check_against_stage_harness(renderer, counts, paths, backdrops)
 

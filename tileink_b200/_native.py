@@ -31,6 +31,7 @@ PTCL_BATCH_BEGIN = 14
 PTCL_SDF = 9
 PTCL_IMAGE = 13
 PATTERN_NEAREST, PATTERN_BILINEAR = 0, 1
+MAX_IMAGE_DIMENSION = 16384  # TK_MAX_IMAGE_DIMENSION
 PTCL_BEGIN_SDF_CLIP = 12
 TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIND_MIXED = 0, 1, 2, 3, 4
 # SDF kinds (src/shared/gpu_types.rs) and line caps
@@ -170,6 +171,27 @@ class IncrementalStats(C.Structure):
                 ("reason", C.c_uint32)]
 
 
+class AbiField(C.Structure):
+    """tk_abi_field (include/tileink.h)."""
+    _fields_ = [("type", C.c_char_p), ("field", C.c_char_p), ("offset", C.c_uint32), ("size", C.c_uint32)]
+
+
+def abi_layout() -> dict:
+    """{struct: {"": size, field: (offset, size), ...}} as the library was
+    compiled (tk_abi_layout)."""
+    t = C.POINTER(AbiField)()
+    n = library().tk_abi_layout(C.byref(t))
+    out: dict = {}
+    for k in range(n):
+        e = t[k]
+        d = out.setdefault(e.type.decode(), {})
+        if e.field:
+            d[e.field.decode()] = (e.offset, e.size)
+        else:
+            d[""] = e.size
+    return out
+
+
 FULL_NONE, FULL_REQUESTED, FULL_NO_HISTORY, FULL_THRESHOLD, FULL_FILTERS = 0, 1, 2, 3, 4
 
 _LIB = None
@@ -187,6 +209,7 @@ def library() -> C.CDLL:
     P, U32, U64, I32, I64, F32, F64 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64, C.c_float, C.c_double
     sig = {
         "tk_version": (C.c_char_p, []),
+        "tk_abi_layout": (U32, [C.POINTER(C.POINTER(AbiField))]),
         "tk_ctx_create": (I32, [I32, C.POINTER(P)]),
         "tk_ctx_destroy": (None, [P]),
         "tk_last_error": (C.c_char_p, [P]),
@@ -203,6 +226,7 @@ def library() -> C.CDLL:
         "tk_get_stats": (I32, [P, C.POINTER(Stats)]),
         "tk_debug_readback": (I32, [P, U32, U32, P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "tk_stage_scan_prefix": (I32, [P, P, U64, P, U32, P, P, P]),
+        "tk_stage_tile_prefix": (I32, [P, P, U32, U32, U32, C.POINTER(U32)]),
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
         "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),
@@ -216,7 +240,6 @@ def library() -> C.CDLL:
         "tk_diff_flatten": (U64, [C.POINTER(DiffScene), P, P, P, U64]),
         "tk_set_timing": (I32, [P, I32]),
         "tk_get_stage_times": (I32, [P, P, U32]),
-        "tk_probe_fp32_tflops": (I32, [P, C.POINTER(C.c_double)]),
         "tk_path_new": (P, []),
         "tk_path_free": (None, [P]),
         "tk_path_move_to": (None, [P, F64, F64]),

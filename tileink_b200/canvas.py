@@ -246,7 +246,7 @@ class Canvas:
             raise ValueError("image must be a (height, width) uint32 array")
         r = self._lib.tk_canvas_add_image(self._h, im.ctypes.data, im.shape[1], im.shape[0])
         if r < 0:
-            raise ValueError("empty image")
+            raise ValueError(f"empty image, or a side above {N.MAX_IMAGE_DIMENSION} texels")
         return r
 
     def push_image(self, x0, y0, x1, y1, image: int, extend=EXTEND_PAD, sampling=N.PATTERN_NEAREST, opacity=255):

@@ -259,6 +259,9 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     for (uint32_t k = 0; k < d.image_count; ++k) {
         const tk_image_desc& im = d.images[k];
         if (!im.premul_rgba8 || im.width == 0u || im.height == 0u) invalid("image " + std::to_string(k) + " is empty");
+        if (im.width > TK_MAX_IMAGE_DIMENSION || im.height > TK_MAX_IMAGE_DIMENSION)
+            invalid("image " + std::to_string(k) + " exceeds the 2D texture limit of " +
+                    std::to_string(TK_MAX_IMAGE_DIMENSION));
         texel_words += uint64_t(im.width) * im.height;
     }
     if (texel_words > 0xFFFFFFFFull) invalid("images exceed u32 indexing");
@@ -1406,13 +1409,6 @@ int32_t tk_get_stage_times(tk_ctx* c, float* ms, uint32_t count) {
     });
 }
 
-int32_t tk_probe_fp32_tflops(tk_ctx* c, double* tflops) {
-    return guarded(c, [&] {
-        if (!tflops) invalid("null output");
-        *tflops = tk::probe_fp32_tflops(c->stream);
-    });
-}
-
 int32_t tk_stage_scan_prefix(tk_ctx* c, const uint32_t* counts, uint64_t pool_len, const tk_path_record* paths,
                              uint32_t path_count, tk_segment_range* ranges, uint32_t* cursors, uint32_t* bumps) {
     return guarded(c, [&] {
@@ -1469,6 +1465,38 @@ int32_t tk_stage_scan_prefix(tk_ctx* c, const uint32_t* counts, uint64_t pool_le
         TK_CUDA(cudaStreamSynchronize(st));
         d_counts.release(); d_cursors.release(); d_bumps.release(); d_misc.release(); d_bd.release();
         d_ranges.release(); d_paths.release(); d_items.release(); d_desc.release();
+    });
+}
+
+int32_t tk_stage_tile_prefix(tk_ctx* c, tk_tile_record* tiles, uint32_t tile_count, uint32_t poll_limit,
+                             uint32_t withhold_first, uint32_t* total) {
+    return guarded(c, [&] {
+        if ((tile_count && !tiles) || !total) invalid("null buffer");
+        if (withhold_first > 1u) invalid("withhold_first must be 0 or 1");
+        cudaStream_t st = c->stream;
+        DBuf<tk_tile_record> d_tiles;
+        DBuf<uint32_t> d_misc;
+        DBuf<unsigned long long> d_desc;
+        upload(d_tiles, tiles, tile_count, st);
+        d_misc.reserve(4);
+        TK_CUDA(cudaMemsetAsync(d_misc.ptr, 0, 16, st));
+        d_desc.reserve(tk::tile_prefix_blocks(tile_count) + 1u);
+        tk::launch_tile_prefix_on(d_tiles.ptr, tile_count, d_desc.ptr, d_misc.ptr + 1, d_misc.ptr + 2, d_misc.ptr,
+                                  poll_limit ? poll_limit : tk::kTilePrefixPollLimit, withhold_first, st);
+        TK_CUDA(cudaGetLastError());
+        uint32_t words[4] = {0, 0, 0, 0};
+        TK_CUDA(cudaMemcpyAsync(words, d_misc.ptr, sizeof(words), cudaMemcpyDeviceToHost, st));
+        if (tile_count)
+            TK_CUDA(cudaMemcpyAsync(tiles, d_tiles.ptr, size_t(tile_count) * sizeof(tk_tile_record),
+                                    cudaMemcpyDeviceToHost, st));
+        TK_CUDA(cudaStreamSynchronize(st));
+        d_tiles.release(); d_misc.release(); d_desc.release();
+        *total = words[2];
+        if (words[0] & tk::ERR_LOOKBACK_TIMEOUT)
+            throw Fail{TK_E_TIMEOUT, "device error flags " + std::to_string(words[0]) +
+                                         ": look-back wait gave up after " +
+                                         std::to_string(poll_limit ? poll_limit : tk::kTilePrefixPollLimit) +
+                                         " polls"};
     });
 }
 

@@ -1167,7 +1167,9 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
 }
 
 int32_t tk_canvas_add_image(tk_canvas* c, const uint32_t* premul_rgba8, uint32_t width, uint32_t height) {
-    if (!c || !premul_rgba8 || width == 0u || height == 0u) return -1;
+    if (!c || !premul_rgba8 || width == 0u || height == 0u || width > TK_MAX_IMAGE_DIMENSION ||
+        height > TK_MAX_IMAGE_DIMENSION)
+        return -1;
     const size_t n = size_t(width) * height;
     return add_image(c, std::make_shared<const std::vector<uint32_t>>(premul_rgba8, premul_rgba8 + n), width, height);
 }
@@ -1385,9 +1387,6 @@ uint64_t tk_canvas_param_colors(const tk_canvas* c, float* out) {
 }
 
 }  // extern "C"
-
-// Generators live in generate.cpp; they need push_path_with_tag's public
-// counterparts only.
 
 // ---------------------------------------------------------------------------
 // Seeded synthetic workloads (the five measured configurations).

@@ -507,13 +507,16 @@ __global__ void __launch_bounds__(kCoarseThreads)
 }
 
 // Exclusive scan of tile counts into ptcl_start / ptcl_end (coarse/prefix.hlsl:11-63),
-// single pass with decoupled look-back over 4096-tile blocks.
+// single pass with decoupled look-back over 4096-tile blocks. Blocks take
+// their position from a ticket, so every predecessor a block waits for is
+// already running; each wait still gives up after `poll_limit` polls, sets
+// ERR_LOOKBACK_TIMEOUT and carries on, so the kernel always ends.
 constexpr int kTileScanThreads = 256, kTilePer = 16, kTileBlock = kTileScanThreads * kTilePer;
 constexpr unsigned long long kAgg = 1ull << 62, kIncl = 2ull << 62;
 
 __global__ void __launch_bounds__(kTileScanThreads)
     k_tile_prefix(tk_tile_record* tiles, uint32_t T, unsigned long long* desc, uint32_t* ticket, uint32_t* total,
-                  uint32_t* error) {
+                  uint32_t* error, uint32_t poll_limit) {
     __shared__ uint32_t s_warp[8];
     __shared__ uint32_t s_blk, s_prefix;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -553,7 +556,7 @@ __global__ void __launch_bounds__(kTileScanThreads)
                 unsigned long long d = *((volatile unsigned long long*)(desc + j));
                 unsigned long long st = d & (3ull << 62);
                 if (st == 0ull) {
-                    if (++spins > (1u << 22)) { atomicOr(error, ERR_LOOKBACK_TIMEOUT); break; }
+                    if (++spins > poll_limit) { atomicOr(error, ERR_LOOKBACK_TIMEOUT); break; }
                     __nanosleep(64);
                     continue;
                 }
@@ -611,10 +614,20 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
 
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {
     uint32_t T = p.scenes ? p.total_tiles : s.tw * s.th;
-    uint32_t blocks = (T + kTileBlock - 1) / kTileBlock;
-    cudaMemsetAsync(p.tile_desc, 0, sizeof(unsigned long long) * blocks, st);
-    cudaMemsetAsync(p.ticket, 0, sizeof(uint32_t), st);
-    k_tile_prefix<<<blocks, kTileScanThreads, 0, st>>>(p.tiles, T, p.tile_desc, p.ticket, p.ptcl_total, s.error);
+    launch_tile_prefix_on(p.tiles, T, p.tile_desc, p.ticket, p.ptcl_total, s.error, kTilePrefixPollLimit, 0u, st);
+}
+
+uint32_t tile_prefix_blocks(uint32_t T) { return (T + kTileBlock - 1) / kTileBlock; }
+
+void launch_tile_prefix_on(tk_tile_record* tiles, uint32_t T, unsigned long long* desc, uint32_t* ticket,
+                           uint32_t* total, uint32_t* error, uint32_t poll_limit, uint32_t first_ticket,
+                           cudaStream_t st) {
+    const uint32_t blocks = tile_prefix_blocks(T);
+    cudaMemsetAsync(desc, 0, sizeof(unsigned long long) * (blocks + first_ticket), st);
+    cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
+    if (first_ticket) cudaMemcpyAsync(ticket, &first_ticket, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    if (blocks)
+        k_tile_prefix<<<blocks, kTileScanThreads, 0, st>>>(tiles, T, desc, ticket, total, error, poll_limit);
 }
 
 }  // namespace tk

@@ -107,7 +107,7 @@ struct NoAllocScratch {
     unsigned long long* desc;  // TK_NOALLOC_MAX_SCAN_ITEMS item sum / prefix pairs
     ScanItem* items;           // TK_NOALLOC_MAX_SCAN_ITEMS work items
     tk_path_record* paths;     // TK_NOALLOC_MAX_PATHS path records
-    uint32_t* words;           // [0] error [1] ticket [2] total
+    uint32_t* words;           // [0] error [1] unused [2] total
 };
 // Resolves the scratch address of `device` (which must be current) once and
 // caches it.
@@ -157,6 +157,15 @@ struct PassView {
 void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st);
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st);
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st);
+// The tile prefix on explicit buffers: `desc` holds tile_prefix_blocks(T) +
+// first_ticket words. The block ticket starts at `first_ticket` (1 leaves
+// block 0's descriptor unpublished: the bounded-wait test); each look-back
+// wait gives up after `poll_limit` polls.
+constexpr uint32_t kTilePrefixPollLimit = 1u << 22;
+uint32_t tile_prefix_blocks(uint32_t T);
+void launch_tile_prefix_on(tk_tile_record* tiles, uint32_t T, unsigned long long* desc, uint32_t* ticket,
+                           uint32_t* total, uint32_t* error, uint32_t poll_limit, uint32_t first_ticket,
+                           cudaStream_t st);
 void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaStream_t st);
 // The per-draw PaintInfo table of the uploaded draws and brush blob; shadow
 // records start at word sdf_shadow_base of the device SDF buffer.
@@ -186,8 +195,6 @@ struct BlurParams {
 void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaStream_t st);
 void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st);
 
-// FP32 FMA peak probe (TFLOP/s).
-double probe_fp32_tflops(cudaStream_t st);
 
 // Device flattening (flatten.cu): per-element line counts, exclusive offsets
 // in `counts` and the total; then path line ranges and the lines themselves.

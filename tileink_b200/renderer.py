@@ -111,11 +111,6 @@ class NativeRenderer:
         self._check(self._lib.tk_get_stage_times(self._h, out, len(self.STAGE_NAMES)))
         return dict(zip(self.STAGE_NAMES, list(out)))
 
-    def probe_fp32_tflops(self) -> float:
-        v = C.c_double(0.0)
-        self._check(self._lib.tk_probe_fp32_tflops(self._h, C.byref(v)))
-        return v.value
-
     def stats(self) -> dict:
         s = N.Stats()
         self._check(self._lib.tk_get_stats(self._h, C.byref(s)))
@@ -142,6 +137,16 @@ class NativeRenderer:
         self._check(self._lib.tk_stage_scan_prefix(self._h, N.ptr(counts), len(counts), N.ptr(paths), len(paths),
                                                    N.ptr(ranges), N.ptr(cursors), N.ptr(bumps)))
         return ranges, cursors, bumps
+
+    def stage_tile_prefix(self, tiles, poll_limit: int = 0, withhold_first: bool = False):
+        """Tile prefix (tk_stage_tile_prefix) on TILE_DTYPE records whose
+        ptcl_count is set; returns (tiles, total). Raises TileinkError with
+        code TK_E_TIMEOUT when the look-back wait gives up."""
+        tiles = np.ascontiguousarray(tiles, dtype=N.TILE_DTYPE).copy()
+        total = C.c_uint32(0)
+        self._check(self._lib.tk_stage_tile_prefix(self._h, N.ptr(tiles), len(tiles), int(poll_limit),
+                                                   1 if withhold_first else 0, C.byref(total)))
+        return tiles, total.value
 
     def pool_scan_noalloc(self, paths, d_counts: int, d_backdrops: int, d_ranges: int, d_cursors: int,
                           pool_len: int, d_bumps: int) -> None:
