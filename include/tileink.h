@@ -388,6 +388,12 @@ int32_t tk_get_stats(tk_ctx* ctx, tk_stats* out);
 #define TK_STAGE_LINES 9u      /* tk_line[L] (device-flattened lines included) */
 int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
                           void* dst, size_t bytes, size_t* needed);
+/* Elements [first, first + count) of the same buffers (count clipped to the
+ * buffer), for buffers larger than a host copy should hold at once (the
+ * 4096^2 / 50,000-path frame has 335 M segments); *total receives the
+ * buffer's element count. */
+int32_t tk_debug_readback_range(tk_ctx* ctx, uint32_t stage, uint32_t index, uint64_t first,
+                                uint64_t count, void* dst, uint64_t* total);
 
 /* Stage timing with CUDA events recorded on the context stream around each
  * stage of tk_render (no reference counterpart; measurement support).

@@ -37,6 +37,12 @@ def lib() -> C.CDLL:
         P, U32, U64, I32, F32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int32, C.c_float
         l.or_run.restype = I32
         l.or_run.argtypes = [P, I32, U32, U32, C.POINTER(P)]
+        l.or_prepare.restype = I32
+        l.or_prepare.argtypes = [P, I32, C.POINTER(P)]
+        l.or_raster.restype = I32
+        l.or_raster.argtypes = [P, I32, U32, U32, U32]
+        l.or_get_range.restype = U64
+        l.or_get_range.argtypes = [P, U32, U64, U64, P]
         l.or_free.argtypes = [P]
         l.or_error.restype = C.c_char_p
         l.or_get.restype = C.c_size_t
@@ -71,15 +77,46 @@ def lib() -> C.CDLL:
 
 
 class OracleRun:
-    """Result of the reference frame restated on the CPU."""
+    """Result of the reference frame restated on the CPU.
 
-    def __init__(self, desc, threads: int = 1, tile_rows=(0, 0)):
+    OracleRun(desc, threads, tile_rows=(y0, y1)) runs the whole frame, with
+    coarse and fine restricted to tile rows [y0, y1) (y1 == 0: all rows).
+    OracleRun.prepare(desc, threads) runs only the scan and the tile bins;
+    raster(y0, y1, row_step) then draws tile rows y0, y0 + row_step, ... < y1
+    and may be called again for other rows of the same frame."""
+
+    def __init__(self, desc, threads: int = 1, tile_rows=(0, 0), _prepare_only=False):
         self._l = lib()
+        self._desc = desc
         h = C.c_void_p()
-        rc = self._l.or_run(C.byref(desc), int(threads), int(tile_rows[0]), int(tile_rows[1]), C.byref(h))
+        if _prepare_only:
+            rc = self._l.or_prepare(C.byref(desc), int(threads), C.byref(h))
+        else:
+            rc = self._l.or_run(C.byref(desc), int(threads), int(tile_rows[0]), int(tile_rows[1]), C.byref(h))
         if rc != 0:
             raise RuntimeError("oracle: " + self._l.or_error().decode())
         self._h = h.value
+
+    @classmethod
+    def prepare(cls, desc, threads: int = 1) -> "OracleRun":
+        return cls(desc, threads, _prepare_only=True)
+
+    def raster(self, tile_y0: int = 0, tile_y1: int = 0, row_step: int = 1, threads: int = 1) -> None:
+        if self._l.or_raster(self._h, int(threads), int(tile_y0), int(tile_y1), int(row_step)) != 0:
+            raise RuntimeError("oracle: " + self._l.or_error().decode())
+
+    def get_range(self, what: int, dtype, first: int, count: int) -> np.ndarray:
+        """Elements [first, first + count) of a flat output (counts,
+        backdrops, ranges, segments, image, bumps)."""
+        n = self._l.or_get_range(self._h, what, 0, 0, None)
+        k = max(0, min(count, n - first))
+        out = np.zeros(k, dtype=dtype)
+        if k:
+            self._l.or_get_range(self._h, what, first, k, out.ctypes.data)
+        return out
+
+    def size(self, what: int) -> int:
+        return self._l.or_get_range(self._h, what, 0, 0, None)
 
     def __del__(self):
         if getattr(self, "_h", None):

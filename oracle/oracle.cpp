@@ -1119,7 +1119,10 @@ struct or_scene {
     // per pass: per tile, streams of the pass's batches touching the tile
     std::vector<std::vector<std::vector<BatchStream>>> pass_streams;
     std::vector<uint32_t> image;
-    uint32_t ty0 = 0, ty1 = 0;
+    // coarse and fine cover the tile rows ty0 <= ty < ty1 with
+    // (ty - ty0) % row_step == 0 (a band, or every row_step-th row)
+    uint32_t ty0 = 0, ty1 = 0, row_step = 1;
+    bool in_band(uint32_t ty) const { return ty >= ty0 && ty < ty1 && (ty - ty0) % row_step == 0u; }
     double times[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
@@ -1677,7 +1680,7 @@ void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int th
     auto& streams = S.pass_streams[pass];
     parallel_for(threads, S.T, [&](uint64_t tile) {
         uint32_t ty = uint32_t(tile) / S.tw, tx = uint32_t(tile) % S.tw;
-        if (ty < S.ty0 || ty >= S.ty1) return;
+        if (!S.in_band(ty)) return;
         const auto& list = streams[tile];
         if (list.empty()) return;  // EMPTY in every batch: target unchanged
         for (uint32_t ly = 0; ly < TK_TILE_SIZE; ++ly) {
@@ -1703,12 +1706,13 @@ void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int th
     });
 }
 
-void run_scene(or_scene& S, int threads) {
+// Scan (count, prefix + cumsum, emit) over every line and the tile bins of
+// every draw: the frame's work that does not depend on the tile rows drawn.
+void scan_scene(or_scene& S, int threads) {
     const tk_scene_desc& D = S.desc;
     S.tw = (D.width + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
     S.th = (D.height + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
     S.T = S.tw * S.th;
-    if (S.ty1 == 0 || S.ty1 > S.th) S.ty1 = S.th;
     uint32_t np = uint32_t(S.paths.size());
     for (const auto& p : S.paths) {
         S.B = std::max<uint64_t>(S.B, uint64_t(p.data_offset) + p.data_len);
@@ -1777,7 +1781,17 @@ void run_scene(or_scene& S, int threads) {
             for (uint32_t x = x0; x < x1; ++x) S.bins[size_t(y) * S.tw + x].push_back(di);
     }
     S.times[3] = since(t0);
+}
 
+// Coarse and fine of every target pass, and the blur layers, over the tile
+// rows of S.in_band (the rows outside keep the clear colour).
+void raster_scene(or_scene& S, int threads) {
+    const tk_scene_desc& D = S.desc;
+    if (S.ty1 == 0 || S.ty1 > S.th) S.ty1 = S.th;
+    if (S.row_step == 0u) S.row_step = 1u;
+    S.batches.clear();
+    S.pass_streams.clear();
+    S.times[4] = S.times[5] = S.times[6] = 0.0;
     // Walk ops: batches, passes, blur layers.
     std::vector<uint32_t> main_target(size_t(D.width) * D.height, D.clear_color);
     struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; };
@@ -1794,7 +1808,7 @@ void run_scene(or_scene& S, int threads) {
         auto tc = clk::now();
         parallel_for(threads, S.T, [&](uint64_t tile) {
             uint32_t ty = uint32_t(tile) / S.tw;
-            if (ty < S.ty0 || ty >= S.ty1) return;
+            if (!S.in_band(ty)) return;
             const auto& cand = S.bins[tile];
             for (uint32_t bi : pass_batches) {
                 const Batch& b = S.batches[bi];
@@ -1898,8 +1912,43 @@ int32_t or_run(const tk_scene_desc* d, int32_t threads, uint32_t tile_y0, uint32
         S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
         S->ty0 = tile_y0;
         S->ty1 = tile_y1;
-        run_scene(*S, threads < 1 ? 1 : threads);
+        scan_scene(*S, threads < 1 ? 1 : threads);
+        raster_scene(*S, threads < 1 ? 1 : threads);
         *out = S;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int32_t or_prepare(const tk_scene_desc* d, int32_t threads, or_scene** out) {
+    *out = nullptr;
+    try {
+        auto* S = new or_scene();
+        S->desc = *d;
+        S->paths.assign(d->paths, d->paths + d->path_count);
+        S->draws.assign(d->draws, d->draws + d->draw_count);
+        S->layers.assign(d->layers, d->layers + d->layer_count);
+        S->brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
+        S->sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
+        S->shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
+        S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        scan_scene(*S, threads < 1 ? 1 : threads);
+        *out = S;
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
+int32_t or_raster(or_scene* S, int32_t threads, uint32_t tile_y0, uint32_t tile_y1, uint32_t row_step) {
+    try {
+        S->ty0 = tile_y0;
+        S->ty1 = tile_y1;
+        S->row_step = row_step ? row_step : 1u;
+        raster_scene(*S, threads < 1 ? 1 : threads);
         return 0;
     } catch (const std::exception& e) {
         g_error = e.what();
@@ -1985,6 +2034,30 @@ size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_
         }
         default: return 0;
     }
+}
+
+uint64_t or_get_range(const or_scene* s, uint32_t what, uint64_t first, uint64_t count, void* dst) {
+    const unsigned char* src = nullptr;
+    uint64_t n = 0;
+    size_t es = 4;
+    switch (what) {
+        case OR_COUNTS: src = reinterpret_cast<const unsigned char*>(s->counts.data()); n = s->counts.size(); break;
+        case OR_BACKDROPS:
+            src = reinterpret_cast<const unsigned char*>(s->backdrops.data());
+            n = s->backdrops.size();
+            break;
+        case OR_RANGES: src = reinterpret_cast<const unsigned char*>(s->ranges.data()); n = s->ranges.size(); es = 8; break;
+        case OR_SEGMENTS:
+            src = reinterpret_cast<const unsigned char*>(s->segments.data());
+            n = s->segments.size();
+            es = sizeof(tk_line_segment);
+            break;
+        case OR_IMAGE: src = reinterpret_cast<const unsigned char*>(s->image.data()); n = s->image.size(); break;
+        case OR_BUMPS: src = reinterpret_cast<const unsigned char*>(s->bumps.data()); n = s->bumps.size(); break;
+        default: return 0;
+    }
+    if (dst && first < n) std::memcpy(dst, src + first * es, std::min(count, n - first) * es);
+    return n;
 }
 
 uint32_t or_line_scanned_tile_count(const tk_line* line, uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1) {

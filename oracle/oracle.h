@@ -51,6 +51,14 @@ int32_t or_run(const tk_scene_desc* scene, int32_t threads, uint32_t tile_y0,
                uint32_t tile_y1, or_scene** out);
 void or_free(or_scene* s);
 const char* or_error(void);
+/* The same frame in two steps: or_prepare runs the scan (count, prefix +
+ * cumsum, emit) over every line and bins every draw; or_raster then runs
+ * coarse and fine of every pass, and the blur layers, over the tile rows
+ * ty (tile_y0 <= ty < tile_y1, tile_y1 == 0: to the last row) with
+ * (ty - tile_y0) % row_step == 0, replacing the previous raster's passes and
+ * image. A scan serves any number of rasters (row bands of one frame). */
+int32_t or_prepare(const tk_scene_desc* scene, int32_t threads, or_scene** out);
+int32_t or_raster(or_scene* s, int32_t threads, uint32_t tile_y0, uint32_t tile_y1, uint32_t row_step);
 
 /* Output access. Returns bytes needed; copies min(bytes, needed) into dst
  * when dst != NULL. */
@@ -68,6 +76,10 @@ const char* or_error(void);
 #define OR_PATHS 11u       /* tk_path_record[P] as used */
 #define OR_BUMPS 12u       /* u32[P] per-path segment totals */
 size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_t bytes);
+/* Elements [first, first + count) of OR_COUNTS, OR_BACKDROPS, OR_RANGES,
+ * OR_SEGMENTS, OR_IMAGE or OR_BUMPS (count clipped); returns the array's
+ * element count. */
+uint64_t or_get_range(const or_scene* s, uint32_t what, uint64_t first, uint64_t count, void* dst);
 /* Number of draw batches / target passes in the run. */
 uint32_t or_batch_count(const or_scene* s);
 uint32_t or_pass_count(const or_scene* s);

@@ -366,3 +366,40 @@ def test_diff_oracle_exact_area_of_a_square():
     a = img[..., 3]
     assert abs(a[8, 8] - 1.0) < 1e-12 and abs(a[3, 8] - 0.5) < 1e-12 and abs(a[3, 3] - 0.25) < 1e-12
     assert abs(a.sum() - 100.0) < 1e-9 and a[0, 0] == 0.0
+
+
+def test_oracle_band_rasters_compose_the_full_frame():
+    """One scan, then interleaved tile-row sets rastered one after another:
+    each set's rows, tile records and PTCL equal the full frame's."""
+    c = tk.generate(2, 7, width=320, height=272, paths=120)
+    d = c.scene_desc()
+    from oracle import OracleRun, OR_IMAGE, OR_PASS_TILES, OR_PASS_PTCL, OR_SEGMENTS
+    full = OracleRun(d, threads=4)
+    img = full.get(OR_IMAGE, np.uint32).reshape(272, 320)
+    tiles = full.get(OR_PASS_TILES, N.TILE_DTYPE, 0)
+    ptcl = full.get(OR_PASS_PTCL, N.PTCL_DTYPE, 0)
+    tw, th = 20, 17
+    part = OracleRun.prepare(d, threads=4)
+    assert np.array_equal(part.get(OR_SEGMENTS, N.SEGMENT_DTYPE), full.get(OR_SEGMENTS, N.SEGMENT_DTYPE))
+    seen = np.zeros(th, bool)
+    for k in range(3):
+        part.raster(k, 0, 3, threads=4)
+        rows = np.arange(k, th, 3)
+        seen[rows] = True
+        pimg = part.get(OR_IMAGE, np.uint32).reshape(272, 320)
+        ptiles = part.get(OR_PASS_TILES, N.TILE_DTYPE, 0)
+        pptcl = part.get(OR_PASS_PTCL, N.PTCL_DTYPE, 0)
+        for ty in range(th):
+            px = slice(ty * 16, ty * 16 + 16)
+            t = slice(ty * tw, ty * tw + tw)
+            if ty in rows:
+                assert np.array_equal(pimg[px], img[px])
+                assert np.array_equal(ptiles["ptcl_count"][t], tiles["ptcl_count"][t])
+                for i in range(ty * tw, ty * tw + tw):
+                    a, b = int(ptiles["ptcl_start"][i]), int(ptiles["ptcl_end"][i])
+                    e, f = int(tiles["ptcl_start"][i]), int(tiles["ptcl_end"][i])
+                    assert pptcl[a:b].tobytes() == ptcl[e:f].tobytes()
+            else:
+                assert not ptiles["ptcl_count"][t].any()
+                assert np.all(pimg[px] == c.scene_desc().clear_color)
+    assert seen.all()

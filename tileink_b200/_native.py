@@ -227,6 +227,7 @@ def library() -> C.CDLL:
         "tk_debug_readback": (I32, [P, U32, U32, P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "tk_stage_scan_prefix": (I32, [P, P, U64, P, U32, P, P, P]),
         "tk_stage_tile_prefix": (I32, [P, P, U32, U32, U32, C.POINTER(U32)]),
+        "tk_debug_readback_range": (I32, [P, U32, U32, U64, U64, P, C.POINTER(U64)]),
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
         "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),

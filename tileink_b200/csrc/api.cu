@@ -1333,62 +1333,111 @@ int32_t tk_get_stats(tk_ctx* c, tk_stats* out) {
     });
 }
 
+namespace {
+
+// Copies elements [first, first + count) of a debug stage buffer (count
+// clipped to the buffer) and returns the buffer's element count.
+uint64_t debug_read(tk_ctx* c, uint32_t stage, uint32_t index, uint64_t first, uint64_t count, void* dst) {
+    if (!c->rendered) throw Fail{TK_E_STATE, "nothing rendered"};
+    TK_CUDA(cudaStreamSynchronize(c->stream));
+    const unsigned char* src = nullptr;
+    uint64_t n = 0;     // elements
+    size_t es = 4;      // bytes per element on the host side
+    size_t dev_es = 0;  // bytes per element on the device when it differs
+    std::vector<uint32_t> kinds;
+    switch (stage) {
+        case TK_STAGE_COUNTS: src = reinterpret_cast<const unsigned char*>(c->counts.ptr); n = c->pool_len; break;
+        case TK_STAGE_BACKDROPS:
+            src = reinterpret_cast<const unsigned char*>(c->backdrops.ptr);
+            n = c->pool_len;
+            break;
+        case TK_STAGE_RANGES: src = reinterpret_cast<const unsigned char*>(c->ranges.ptr); n = c->pool_len; es = 8; break;
+        case TK_STAGE_SEGMENTS: {
+            // 32-byte device records -> 20-byte LineSegments
+            bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+            n = device_plan ? (c->segment_needed ? c->segment_needed - 1 : 0) : c->host_segment_capacity;
+            src = reinterpret_cast<const unsigned char*>(c->segments.ptr);
+            es = sizeof(tk_line_segment);
+            dev_es = sizeof(tk::SegmentRec);
+            break;
+        }
+        case TK_STAGE_IMAGE: src = reinterpret_cast<const unsigned char*>(c->image.ptr); n = uint64_t(c->width) * c->height; break;
+        case TK_STAGE_PATHS:
+            src = reinterpret_cast<const unsigned char*>(c->paths.ptr);
+            n = c->path_count;
+            es = sizeof(tk_path_record);
+            break;
+        case TK_STAGE_LINES:
+            src = reinterpret_cast<const unsigned char*>(c->lines.ptr);
+            n = c->line_count;
+            es = sizeof(tk_line);
+            break;
+        case TK_STAGE_PTCL:
+        case TK_STAGE_TILES:
+        case TK_STAGE_KINDS: {
+            if (index >= c->passes.size()) throw Fail{TK_E_INVALID, "pass index out of range"};
+            Pass& p = c->passes[index];
+            uint32_t T = c->tw * c->th;
+            if (stage == TK_STAGE_PTCL) {
+                src = reinterpret_cast<const unsigned char*>(p.ptcl.ptr);
+                n = p.ptcl_used;
+                es = sizeof(tk_ptcl_record);
+            } else if (stage == TK_STAGE_TILES) {
+                src = reinterpret_cast<const unsigned char*>(p.tiles.ptr);
+                n = T;
+                es = sizeof(tk_tile_record);
+            } else {
+                std::vector<tk_tile_record> tiles(T);
+                TK_CUDA(cudaMemcpy(tiles.data(), p.tiles.ptr, T * sizeof(tk_tile_record), cudaMemcpyDeviceToHost));
+                kinds.resize(T);
+                for (uint32_t t = 0; t < T; ++t)
+                    kinds[t] = tiles[t].ptcl_count ? TK_TILE_KIND_INTERPRETER : TK_TILE_KIND_EMPTY;
+                n = T;
+            }
+            break;
+        }
+        default: throw Fail{TK_E_INVALID, "unknown stage"};
+    }
+    if (!dst || first >= n) return n;
+    const uint64_t k = std::min(count, n - first);
+    if (!k) return n;
+    if (!kinds.empty()) {
+        std::memcpy(dst, kinds.data() + first, k * 4);
+    } else if (dev_es) {
+        TK_CUDA(cudaMemcpy2D(dst, es, src + first * dev_es, dev_es, es, k, cudaMemcpyDeviceToHost));
+    } else {
+        TK_CUDA(cudaMemcpy(dst, src + first * es, k * es, cudaMemcpyDeviceToHost));
+    }
+    return n;
+}
+
+size_t debug_elem_bytes(uint32_t stage) {
+    switch (stage) {
+        case TK_STAGE_RANGES: return 8;
+        case TK_STAGE_SEGMENTS: return sizeof(tk_line_segment);
+        case TK_STAGE_PATHS: return sizeof(tk_path_record);
+        case TK_STAGE_LINES: return sizeof(tk_line);
+        case TK_STAGE_PTCL: return sizeof(tk_ptcl_record);
+        case TK_STAGE_TILES: return sizeof(tk_tile_record);
+        default: return 4;
+    }
+}
+
+}  // namespace
+
 int32_t tk_debug_readback(tk_ctx* c, uint32_t stage, uint32_t index, void* dst, size_t bytes, size_t* needed) {
     return guarded(c, [&] {
-        if (!c->rendered) throw Fail{TK_E_STATE, "nothing rendered"};
-        TK_CUDA(cudaStreamSynchronize(c->stream));
-        const void* src = nullptr;
-        size_t n = 0;
-        std::vector<uint32_t> kinds;
-        bool segment_records = false;  // 32-byte device records -> 20-byte LineSegments
-        switch (stage) {
-            case TK_STAGE_COUNTS: src = c->counts.ptr; n = c->pool_len * 4; break;
-            case TK_STAGE_BACKDROPS: src = c->backdrops.ptr; n = c->pool_len * 4; break;
-            case TK_STAGE_RANGES: src = c->ranges.ptr; n = c->pool_len * 8; break;
-            case TK_STAGE_SEGMENTS: {
-                bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
-                uint64_t cnt = device_plan ? (c->segment_needed ? c->segment_needed - 1 : 0) : c->host_segment_capacity;
-                src = c->segments.ptr;
-                n = cnt * sizeof(tk_line_segment);
-                segment_records = true;
-                break;
-            }
-            case TK_STAGE_IMAGE: src = c->image.ptr; n = size_t(c->width) * c->height * 4; break;
-            case TK_STAGE_PATHS: src = c->paths.ptr; n = size_t(c->path_count) * sizeof(tk_path_record); break;
-            case TK_STAGE_LINES: src = c->lines.ptr; n = size_t(c->line_count) * sizeof(tk_line); break;
-            case TK_STAGE_PTCL:
-            case TK_STAGE_TILES:
-            case TK_STAGE_KINDS: {
-                if (index >= c->passes.size()) throw Fail{TK_E_INVALID, "pass index out of range"};
-                Pass& p = c->passes[index];
-                uint32_t T = c->tw * c->th;
-                if (stage == TK_STAGE_PTCL) { src = p.ptcl.ptr; n = p.ptcl_used * sizeof(tk_ptcl_record); }
-                else if (stage == TK_STAGE_TILES) { src = p.tiles.ptr; n = size_t(T) * sizeof(tk_tile_record); }
-                else {
-                    std::vector<tk_tile_record> tiles(T);
-                    TK_CUDA(cudaMemcpy(tiles.data(), p.tiles.ptr, T * sizeof(tk_tile_record), cudaMemcpyDeviceToHost));
-                    kinds.resize(T);
-                    for (uint32_t t = 0; t < T; ++t)
-                        kinds[t] = tiles[t].ptcl_count ? TK_TILE_KIND_INTERPRETER : TK_TILE_KIND_EMPTY;
-                    n = size_t(T) * 4;
-                }
-                break;
-            }
-            default: throw Fail{TK_E_INVALID, "unknown stage"};
-        }
-        if (needed) *needed = n;
-        if (!dst) return;
-        size_t k = std::min(n, bytes);
-        if (!kinds.empty()) {
-            std::memcpy(dst, kinds.data(), k);
-        } else if (segment_records) {
-            const size_t rows = k / sizeof(tk_line_segment);  // whole records only
-            if (rows)
-                TK_CUDA(cudaMemcpy2D(dst, sizeof(tk_line_segment), src, sizeof(tk::SegmentRec), sizeof(tk_line_segment),
-                                     rows, cudaMemcpyDeviceToHost));
-        } else if (k) {
-            TK_CUDA(cudaMemcpy(dst, src, k, cudaMemcpyDeviceToHost));
-        }
+        const size_t es = debug_elem_bytes(stage);
+        const uint64_t n = debug_read(c, stage, index, 0, bytes / es, dst);  // whole elements only
+        if (needed) *needed = size_t(n * es);
+    });
+}
+
+int32_t tk_debug_readback_range(tk_ctx* c, uint32_t stage, uint32_t index, uint64_t first, uint64_t count,
+                                void* dst, uint64_t* total) {
+    return guarded(c, [&] {
+        const uint64_t n = debug_read(c, stage, index, first, count, dst);
+        if (total) *total = n;
     });
 }
 

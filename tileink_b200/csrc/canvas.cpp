@@ -280,7 +280,11 @@ size_t quantize_ramp_size(float span, size_t stops) {
     while (p < target) p <<= 1;
     return std::min<size_t>(p, 4096);
 }
-// Ramp of premultiplied colors; stops interpolated in premultiplied sRGB.
+// Ramp of premultiplied colors (build_ramp, src/shared/brush.rs:638-689):
+// each entry is peniko's premultiplied sRGB interpolation between its two
+// stops, as the `color` crate evaluates it: premul = p1 + (p2 - p1) * t and
+// alpha = a1 + t * (a2 - a1), un-premultiplied (scale by 1 / alpha, by 1 at
+// alpha 0) and premultiplied again before the RGBA8 store.
 std::vector<uint32_t> build_ramp(const tk_gradient_stop* stops, uint32_t n, size_t size) {
     size = std::max<size_t>(size, 2);
     std::vector<uint32_t> ramp(size, 0u);
@@ -297,8 +301,14 @@ std::vector<uint32_t> build_ramp(const tk_gradient_stop* stops, uint32_t n, size
         float lt = std::fabs(span) <= 1.1920929e-7f ? 0.0f : std::min(std::max((t - l.offset) / span, 0.0f), 1.0f);
         float lp[4] = {l.rgba[0] * l.rgba[3], l.rgba[1] * l.rgba[3], l.rgba[2] * l.rgba[3], l.rgba[3]};
         float rp[4] = {r.rgba[0] * r.rgba[3], r.rgba[1] * r.rgba[3], r.rgba[2] * r.rgba[3], r.rgba[3]};
+        const float alpha = lp[3] + lt * (rp[3] - lp[3]);
+        const float inv = alpha == 0.0f ? 1.0f : 1.0f / alpha;
         float c[4];
-        for (int k = 0; k < 4; ++k) c[k] = lp[k] + (rp[k] - lp[k]) * lt;
+        for (int k = 0; k < 3; ++k) {
+            const float premul = lp[k] + (rp[k] - lp[k]) * lt;
+            c[k] = (premul * inv) * alpha;
+        }
+        c[3] = alpha;
         ramp[ix] = premul_f32_to_u32(c);
     }
     return ramp;

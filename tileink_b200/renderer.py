@@ -127,6 +127,26 @@ class NativeRenderer:
         self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
         return out
 
+    DEBUG_DTYPES = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
+                    N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
+                    N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE,
+                    N.STAGE_LINES: N.LINE_DTYPE}
+
+    def debug_size(self, stage: int, index: int = 0) -> int:
+        """Element count of a debug stage buffer."""
+        total = C.c_uint64(0)
+        self._check(self._lib.tk_debug_readback_range(self._h, stage, index, 0, 0, None, C.byref(total)))
+        return total.value
+
+    def debug_range(self, stage: int, first: int, count: int, index: int = 0) -> np.ndarray:
+        """Elements [first, first + count) of a debug stage buffer (clipped)."""
+        total = self.debug_size(stage, index)
+        k = max(0, min(count, total - first))
+        out = np.zeros(k, dtype=self.DEBUG_DTYPES[stage])
+        if k:
+            self._check(self._lib.tk_debug_readback_range(self._h, stage, index, first, k, N.ptr(out), None))
+        return out
+
     # --- stage harnesses -------------------------------------------------------
     def stage_scan_prefix(self, counts, paths, ranges, cursors):
         counts = np.ascontiguousarray(counts, dtype=np.uint32)
