@@ -152,7 +152,21 @@ int64_t tk_canvas_push_image(tk_canvas* c, const double rect[4], uint32_t image,
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
                                   uint32_t fill_rule, double tolerance);
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);
+/* Canvas::push_opacity_layer (src/canvas/layers.rs:122-140): the children
+ * until the matching pop are composited at `opacity` (clamped to [0, 1],
+ * stored as opacity_f32_to_u8) through the nonzero coverage of `path`. The
+ * layer is fused into each batch's layer stack (a BEGIN_OPACITY / END_OPACITY
+ * pair per tile), which is how the reference compiles it when the subtree
+ * draws in one stack (src/canvas/compile.rs:342-353). A subtree that does not
+ * (a blur group below it, or draws both beside and inside a nested layer)
+ * needs the reference's offscreen group: tk_canvas_scene then fails and
+ * tk_canvas_last_error says why. Returns -1 for a null path, a tolerance
+ * <= 0 or a non-finite opacity. */
+int32_t tk_canvas_push_opacity_layer(tk_canvas* c, const tk_path* path, const double* transform,
+                                     double tolerance, float opacity);
 int32_t tk_canvas_pop_layer(tk_canvas* c);
+/* Why the last tk_canvas_scene failed ("" when it did not). */
+const char* tk_canvas_last_error(const tk_canvas* c);
 
 /* Compile (if needed) and describe the recorded scene. Pointers stay valid
  * until the canvas is modified or freed. */

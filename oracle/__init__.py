@@ -68,6 +68,8 @@ def lib() -> C.CDLL:
         l.or_atan2.argtypes = [F32, F32]
         l.or_interpret_particles.restype = I32
         l.or_interpret_particles.argtypes = [P, P, U32, P]
+        l.or_interpret_path_draws.restype = I32
+        l.or_interpret_path_draws.argtypes = [P, I32, P]
         l.or_interpret_sdf_draws.restype = I32
         l.or_interpret_sdf_draws.argtypes = [P, P]
         l.or_diff_loss.restype = C.c_double
@@ -173,6 +175,16 @@ def interpret_particles(desc, particles: np.ndarray) -> np.ndarray:
     img = np.zeros((desc.height, desc.width, 4), np.uint8)
     p = np.ascontiguousarray(particles)
     if lib().or_interpret_particles(C.byref(desc), p.ctypes.data, len(p), img.ctypes.data) != 0:
+        raise RuntimeError("oracle: " + lib().or_error().decode())
+    return img
+
+
+def interpret_path_draws(desc, threads: int = 8) -> np.ndarray:
+    """Fine-only image (H, W, 4 RGBA8) of a scene of path and SDF draws in
+    clip / opacity layers: every batch's stack and draws interpreted in every
+    tile after the scan, with no coarse stage."""
+    img = np.zeros((desc.height, desc.width, 4), np.uint8)
+    if lib().or_interpret_path_draws(C.byref(desc), int(threads), img.ctypes.data) != 0:
         raise RuntimeError("oracle: " + lib().or_error().decode())
     return img
 

@@ -2172,6 +2172,97 @@ float or_atan2(float y, float x) { return lib_atan2(y, x); }
 // full-tile proof, hollow-stroke proof or occlusion skip changes pixels.
 int32_t or_interpret_particles(const tk_scene_desc* d, const tk_ptcl_record* particles, uint32_t count,
                                uint32_t* image);
+// Fine-only oracle for path draws, the method of rect_pixels.rs:3-13 applied
+// to fills: after the scan (count, prefix + cumsum, emit), every batch's
+// stream in every tile is its whole layer stack (BEGIN_CLIP / BEGIN_OPACITY
+// with the layer path's segment range and cumsum backdrop in the tile, or
+// BEGIN_SDF_CLIP), then every draw of the batch in painter order (FILL with
+// the tile's segment range and backdrop, or SDF), then the reversed ends.
+// Outside a path's bbox the range is empty and the backdrop 0. No tile bins,
+// no particle elision, no stack-wrapper elision, no colour promotion and no
+// occlusion skip: an error in any coarse decision changes pixels. Each batch
+// loads and stores the RGBA8 target, as the reference's per-batch fine
+// dispatch does. Scenes with blur layers are rejected.
+int32_t or_interpret_path_draws(const tk_scene_desc* d, int32_t threads, uint32_t* image) {
+    try {
+        or_scene S;
+        S.desc = *d;
+        S.paths.assign(d->paths, d->paths + d->path_count);
+        S.draws.assign(d->draws, d->draws + d->draw_count);
+        S.layers.assign(d->layers, d->layers + d->layer_count);
+        S.brush.assign(d->brush_blob, d->brush_blob + d->brush_word_count);
+        S.sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
+        S.shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
+        S.batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        threads = threads < 1 ? 1 : threads;
+        scan_scene(S, threads);
+        const uint32_t W = d->width, H = d->height;
+        for (size_t i = 0; i < size_t(W) * H; ++i) image[i] = d->clear_color;
+        auto range_in_tile = [&](const tk_draw_record& dr, uint32_t tx, uint32_t ty, int32_t& w, uint32_t& s0,
+                                 uint32_t& s1) {
+            const uint32_t bd = draw_backdrop(S, dr, tx, ty);
+            if (bd == TK_INVALID_INDEX) { w = 0; s0 = s1 = 0u; return; }
+            w = S.backdrops[bd];
+            s0 = S.ranges[bd].start;
+            s1 = S.ranges[bd].end;
+        };
+        for (uint32_t oi = 0; oi < d->op_count; ++oi) {
+            const tk_op& op = d->ops[oi];
+            if (op.kind != TK_OP_DRAW_BATCH) throw std::runtime_error("fine-only path oracle: blur layers unsupported");
+            std::vector<uint32_t> draws;
+            for (uint32_t k = 0; k < d->draw_order_count; ++k)
+                if (S.batch_ids[d->draw_order[k]] == op.batch_id) draws.push_back(d->draw_order[k]);
+            parallel_for(threads, S.T, [&](uint64_t tile) {
+                const uint32_t tx = uint32_t(tile) % S.tw, ty = uint32_t(tile) / S.tw;
+                std::vector<tk_ptcl_record> recs;
+                int32_t w;
+                uint32_t s0, s1;
+                for (uint32_t i = op.layer_start; i < op.layer_end; ++i) {
+                    const tk_layer_record& L = S.layers[i];
+                    const tk_draw_record& dr = S.draws[L.draw];
+                    if (has_sdf(dr)) {
+                        recs.push_back({TK_PTCL_BEGIN_SDF_CLIP, 0, 0u, 0u, 0u, L.draw});
+                        continue;
+                    }
+                    range_in_tile(dr, tx, ty, w, s0, s1);
+                    const uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_BEGIN_OPACITY : TK_PTCL_BEGIN_CLIP;
+                    recs.push_back({tag, w, dr.fill_rule, s0, s1, L.payload});
+                }
+                for (uint32_t di : draws) {
+                    const tk_draw_record& dr = S.draws[di];
+                    if (has_sdf(dr)) {
+                        recs.push_back({TK_PTCL_SDF, 0, 0u, di, 0u, di});
+                        continue;
+                    }
+                    range_in_tile(dr, tx, ty, w, s0, s1);
+                    recs.push_back({TK_PTCL_FILL, w, dr.fill_rule, s0, s1, di});
+                }
+                for (uint32_t i = op.layer_end; i > op.layer_start;) {
+                    const tk_layer_record& L = S.layers[--i];
+                    recs.push_back({L.tag == TK_LAYER_OPACITY ? TK_PTCL_END_OPACITY : TK_PTCL_END_CLIP, 0, 0u, 0u, 0u,
+                                    0u});
+                }
+                recs.push_back({TK_PTCL_END, 0, 0u, 0u, 0u, 0u});
+                const uint32_t n = uint32_t(recs.size());
+                for (uint32_t ly = 0; ly < TK_TILE_SIZE; ++ly) {
+                    const uint32_t gy = ty * TK_TILE_SIZE + ly;
+                    if (gy >= H) break;
+                    for (uint32_t lx = 0; lx < TK_TILE_SIZE; ++lx) {
+                        const uint32_t gx = tx * TK_TILE_SIZE + lx;
+                        if (gx >= W) break;
+                        uint32_t& texel = image[size_t(gy) * W + gx];
+                        texel = texel_store(interpret(S, recs, 0u, n, texel_load(texel), lx, ly, gx, gy));
+                    }
+                }
+            });
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+
 int32_t or_interpret_sdf_draws(const tk_scene_desc* d, uint32_t* image) {
     std::vector<tk_ptcl_record> recs;
     for (uint32_t k = 0; k < d->draw_count; ++k) recs.push_back({TK_PTCL_SDF, 0, 0u, 0u, 0u, k});

@@ -124,6 +124,12 @@ float or_atan2(float y, float x);
 /* Fine-only image of a scene of SDF draws: every draw interpreted in every
  * tile as a PTCL_SDF particle, from the clear colour (no coarse stage). */
 int32_t or_interpret_sdf_draws(const tk_scene_desc* scene, uint32_t* image);
+/* Fine-only image of a scene of path (and SDF) draws in clip and opacity
+ * layers: after the scan, every batch's whole layer stack and every draw of
+ * the batch are interpreted in every tile with the tile's segment range and
+ * backdrop (empty outside a path's bbox), batch after batch, with no tile
+ * bins, coarse elision, colour promotion or occlusion skip. No blur layers. */
+int32_t or_interpret_path_draws(const tk_scene_desc* scene, int32_t threads, uint32_t* image);
 /* The same with the given particle stream in every tile. */
 int32_t or_interpret_particles(const tk_scene_desc* scene, const tk_ptcl_record* particles, uint32_t count,
                                uint32_t* image);

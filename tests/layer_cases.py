@@ -1,0 +1,76 @@
+"""Scenes with clip, SDF-clip and opacity layers (the reference's fused
+layer stacks, src/canvas/compile.rs:342-353 and src/shared/gpu_coarse.rs:
+314-332), shared by the oracle and GPU tests."""
+from __future__ import annotations
+
+import numpy as np
+
+import tileink_b200 as tk
+
+
+def blob(rng, cx, cy, r, n=7):
+    """A closed cubic blob around (cx, cy)."""
+    a = np.sort(rng.uniform(0, 2 * np.pi, n))
+    pts = [(cx + r * rng.uniform(0.5, 1.2) * np.cos(t), cy + r * rng.uniform(0.5, 1.2) * np.sin(t)) for t in a]
+    p = tk.BezPath().move_to(*pts[0])
+    for k in range(1, n + 1):
+        q0, q1 = pts[(k - 1) % n], pts[k % n]
+        p.cubic_to(q0[0] + (q1[0] - q0[0]) / 3 + rng.normal(0, r / 6), q0[1] + (q1[1] - q0[1]) / 3,
+                   q0[0] + 2 * (q1[0] - q0[0]) / 3, q0[1] + 2 * (q1[1] - q0[1]) / 3 + rng.normal(0, r / 6),
+                   q1[0], q1[1])
+    return p.close()
+
+
+def opacity_scene(seed, w=256, h=192):
+    """Opacity layers (path-masked, opacities 0..1) nested with path clips and
+    SDF clips, over fills with solid and gradient paint; layers open and close
+    between draws so batches split and merge."""
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(w, h)
+    c.set_clear_color(0xFFFFFFFF)
+
+    def fill(k):
+        x, y = rng.uniform(0, w), rng.uniform(0, h)
+        r = float(rng.uniform(10, 60))
+        if k % 3 == 2:
+            b = tk.Brush.linear((x - r, y), (x + r, y + r), [(0.0, (*rng.uniform(0, 1, 3), 1.0)),
+                                                            (1.0, (*rng.uniform(0, 1, 3), 0.6))])
+        else:
+            b = tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.choice([1.0, rng.uniform(0.3, 1)])))
+        c.push_path(blob(rng, x, y, r), b, fill_rule=int(k % 2))
+
+    for k in range(4):
+        fill(k)
+    # an opacity layer over one stack of draws
+    c.push_opacity_layer(blob(rng, w * 0.5, h * 0.5, min(w, h) * 0.45), 0.6)
+    for k in range(6):
+        fill(k)
+    c.pop_layer()
+    # clip > opacity (covers every tile: no segments) > SDF clip > draws
+    c.push_clip_layer(blob(rng, w * 0.4, h * 0.45, min(w, h) * 0.35))
+    c.push_opacity_layer(tk.BezPath().move_to(-5, -5).line_to(w + 5, -5).line_to(w + 5, h + 5)
+                         .line_to(-5, h + 5).close(), 0.35)
+    c.push_clip_sdf_circle_layer(w * 0.55, h * 0.5, min(w, h) * 0.3)
+    for k in range(5):
+        fill(k)
+    c.pop_layer()
+    c.pop_layer()
+    c.pop_layer()
+    # a clip with draws beside an opacity layer (the clip fuses, the batches split)
+    c.push_clip_layer(blob(rng, w * 0.6, h * 0.6, min(w, h) * 0.4))
+    fill(0)
+    c.push_opacity_layer(blob(rng, w * 0.65, h * 0.55, min(w, h) * 0.3), 0.5)
+    for k in range(3):
+        fill(k)
+    c.pop_layer()
+    fill(2)
+    c.pop_layer()
+    # nested opacity layers, the inner one fully transparent
+    c.push_opacity_layer(blob(rng, w * 0.7, h * 0.3, 40), 1.0)
+    c.push_opacity_layer(blob(rng, w * 0.72, h * 0.32, 45), 0.0)
+    fill(1)
+    c.pop_layer()
+    c.pop_layer()
+    for k in range(4):
+        fill(k)
+    return c

@@ -1,0 +1,97 @@
+"""Clip, SDF-clip and opacity layers on the GPU: fused opacity layers against
+the oracle (every stage) and the fine-only oracle, the reference's
+nested-stack END order (src/native/runtime/tests/coarse_count/emit.rs:58-84)
+and its draw-count cases across 256-draw pages (emit.rs:5-34)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import tileink_b200 as tk
+from tileink_b200 import _native as N
+
+from layer_cases import opacity_scene
+from test_gpu_parity import compare_frame
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_gpu_opacity_layers_match_oracle_and_fine_only(renderer, seed):
+    c = opacity_scene(seed)
+    img, ref = compare_frame(renderer, c)
+    tags = renderer.debug(N.STAGE_PTCL, 0)["tag"]
+    assert (tags == N.PTCL_BEGIN_OPACITY).sum() > 10
+    want = oracle.interpret_path_draws(c.scene_desc(), threads=8)
+    assert np.array_equal(img, want), int((img != want).any(axis=2).sum())
+
+
+def tile_stream(ptcl, tiles, t):
+    return ptcl[int(tiles["ptcl_start"][t]):int(tiles["ptcl_end"][t])]
+
+
+def test_gpu_nested_stack_end_order(renderer):
+    """emit.rs:58-84 restated without the blend wrapper (blend layers are
+    outside this path): an opacity layer, a clip that covers the tile (a
+    no-op wrapper, dropped at both ends) and an SDF clip around a draw give
+    BEGIN_OPACITY (payload in `color`), BEGIN_SDF_CLIP, the draw, then the
+    ends in reverse: END_CLIP, END_OPACITY, END."""
+    c = tk.Canvas(32, 32)
+    c.set_clear_color(0xFFFFFFFF)
+    c.push_opacity_layer(tk.BezPath().move_to(2, 3).line_to(14, 1).line_to(12, 15).line_to(1, 12).close(), 0.3)
+    c.push_clip_layer(tk.BezPath().move_to(-40, -30).line_to(70, -35).line_to(75, 70).line_to(-35, 72).close())
+    c.push_clip_sdf_circle_layer(8.0, 8.0, 6.5)
+    c.push_path(tk.BezPath().move_to(3, 3).line_to(13, 4).line_to(9, 13).close(), tk.Brush.solid(0.2, 0.4, 0.8, 1))
+    c.pop_layer()
+    c.pop_layer()
+    c.pop_layer()
+    layers = c.scene_arrays()["layers"]
+    assert list(layers["tag"]) == [N.LAYER_OPACITY, N.LAYER_CLIP, N.LAYER_CLIP]
+    img = renderer.render_to_image(c)
+    ptcl, tiles = renderer.debug(N.STAGE_PTCL, 0), renderer.debug(N.STAGE_TILES, 0)
+    s = tile_stream(ptcl, tiles, 0)
+    assert list(s["tag"]) == [N.PTCL_BATCH_BEGIN, N.PTCL_BEGIN_OPACITY, N.PTCL_BEGIN_SDF_CLIP, N.PTCL_FILL,
+                              N.PTCL_END_CLIP, N.PTCL_END_OPACITY, N.PTCL_END]
+    assert s[1]["color"] == 77  # opacity_f32_to_u8(0.3)
+    assert s[2]["color"] == layers[2]["draw"]
+    assert s[1]["segment_end"] > s[1]["segment_start"]
+    ref = oracle.OracleRun(c.scene_desc(), threads=2)
+    assert np.array_equal(ptcl, ref.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0))
+    assert np.array_equal(img, ref.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(img.shape))
+    assert np.array_equal(img, oracle.interpret_path_draws(c.scene_desc(), threads=2))
+
+
+@pytest.mark.parametrize("draws", [0, 1, 255, 256, 257, 513])
+@pytest.mark.parametrize("stack", [0, 1, 2, 3])
+def test_gpu_draw_counts_across_pages(renderer, draws, stack):
+    """emit.rs:5-34's draw counts around 256-draw pages under 0-3 clip
+    wrappers: tile 0 of a 48x16 canvas holds every draw, in painter order,
+    between its wrappers; the other tiles hold none."""
+    rng = np.random.default_rng(draws * 7 + stack)
+    c = tk.Canvas(48, 16)
+    c.set_clear_color(0xFFFFFFFF)
+    for k in range(stack):
+        r = 7.5 - k
+        c.push_clip_layer(tk.BezPath().move_to(8 - r, 8).line_to(8, 8 - r).line_to(8 + r, 8).line_to(8, 8 + r)
+                          .close())
+    for k in range(draws):
+        x, y = rng.uniform(1, 12, 2)
+        c.push_path(tk.BezPath().move_to(x, y).line_to(x + 3, y + 0.5).line_to(x + 1, y + 2.5).close(),
+                    tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.2, 1))))
+    for k in range(stack):
+        c.pop_layer()
+    c.push_path(tk.BezPath().move_to(20, 2).line_to(30, 3).line_to(25, 12).close(), tk.Brush.solid(0, 0, 0, 1))
+    img = renderer.render_to_image(c)
+    ptcl, tiles = renderer.debug(N.STAGE_PTCL, 0), renderer.debug(N.STAGE_TILES, 0)
+    s = tile_stream(ptcl, tiles, 0)
+    if draws:
+        fills = s[s["tag"] == N.PTCL_FILL]
+        assert len(fills) == draws
+        assert list(fills["color"]) == list(range(stack, stack + draws))  # painter order: draw indices
+        assert (s["tag"] == N.PTCL_BEGIN_CLIP).sum() == stack and (s["tag"] == N.PTCL_END_CLIP).sum() == stack
+    ref = oracle.OracleRun(c.scene_desc(), threads=4)
+    assert np.array_equal(tiles, ref.get(oracle.OR_PASS_TILES, N.TILE_DTYPE, 0))
+    assert np.array_equal(ptcl, ref.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0))
+    assert np.array_equal(img, ref.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(img.shape))
+    assert np.array_equal(img, oracle.interpret_path_draws(c.scene_desc(), threads=4))

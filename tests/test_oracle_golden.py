@@ -403,3 +403,71 @@ def test_oracle_band_rasters_compose_the_full_frame():
                 assert not ptiles["ptcl_count"][t].any()
                 assert np.all(pimg[px] == c.scene_desc().clear_color)
     assert seen.all()
+
+
+@pytest.mark.parametrize("config, kw", [
+    (1, dict(width=640, height=360)),
+    (2, dict(width=768, height=512, paths=600)),
+    (2, dict(width=333, height=210, paths=150, variant=0)),
+    (3, dict(width=480, height=270, paths=600)),
+])
+def test_oracle_pipeline_equals_fine_only_path_oracle(config, kw):
+    """coarse_count/rect_pixels.rs:3-13's method for path fills: the oracle's
+    full pipeline (bins, coarse elision, colour promotion, occlusion skip)
+    gives the pixels of interpreting every draw in every tile."""
+    from oracle import OracleRun, OR_IMAGE, interpret_path_draws
+    c = tk.generate(config, 7, **kw)
+    d = c.scene_desc()
+    full = OracleRun(d, threads=8).get(OR_IMAGE, np.uint32).view(np.uint8).reshape(d.height, d.width, 4)
+    only = interpret_path_draws(d, threads=8)
+    assert np.array_equal(full, only), int((full != only).any(axis=2).sum())
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_oracle_opacity_layers_equal_fine_only_oracle(seed):
+    """Fused opacity layers (BEGIN_OPACITY / END_OPACITY) nested with path
+    and SDF clips: the full pipeline equals interpreting every layer and draw
+    in every tile."""
+    from oracle import OracleRun, OR_IMAGE, OR_PASS_PTCL, interpret_path_draws
+    from layer_cases import opacity_scene
+    c = opacity_scene(seed)
+    d = c.scene_desc()
+    assert (c.scene_arrays()["layers"]["tag"] == N.LAYER_OPACITY).sum() >= 4
+    run = OracleRun(d, threads=8)
+    tags = run.get(OR_PASS_PTCL, N.PTCL_DTYPE, 0)["tag"]
+    assert (tags == N.PTCL_BEGIN_OPACITY).any() and (tags == N.PTCL_END_OPACITY).any()
+    full = run.get(OR_IMAGE, np.uint32).view(np.uint8).reshape(d.height, d.width, 4)
+    only = interpret_path_draws(d, threads=8)
+    assert np.array_equal(full, only), int((full != only).any(axis=2).sum())
+
+
+def test_opacity_layer_payload_and_fusion_rules():
+    c = tk.Canvas(64, 64)
+    sq = tk.BezPath().move_to(0, 0).line_to(64, 0).line_to(64, 64).line_to(0, 64).close()
+    for op, want in [(0.6, 153), (1.0, 255), (0.0, 0), (-2.0, 0), (7.0, 255), (0.5, 128)]:
+        c.push_opacity_layer(sq, op)
+        c.push_path(sq, tk.Brush.solid(1, 0, 0, 1))
+        c.pop_layer()
+        layers = c.scene_arrays()["layers"]
+        assert layers[-1]["tag"] == N.LAYER_OPACITY and layers[-1]["payload"] == want
+    with pytest.raises(ValueError):
+        c.push_opacity_layer(sq, float("nan"))
+    # draws beside and inside a nested layer: the reference needs an
+    # offscreen group there (Canvas::can_fuse is false)
+    bad = tk.Canvas(64, 64)
+    bad.push_opacity_layer(sq, 0.5)
+    bad.push_path(sq, tk.Brush.solid(1, 0, 0, 1))
+    bad.push_clip_layer(sq)
+    bad.push_path(sq, tk.Brush.solid(0, 1, 0, 1))
+    bad.pop_layer()
+    bad.pop_layer()
+    with pytest.raises(RuntimeError, match="offscreen group"):
+        bad.scene_desc()
+    # a nested layer alone under the opacity layer is one stack: fused
+    ok = tk.Canvas(64, 64)
+    ok.push_opacity_layer(sq, 0.5)
+    ok.push_clip_layer(sq)
+    ok.push_path(sq, tk.Brush.solid(0, 1, 0, 1))
+    ok.pop_layer()
+    ok.pop_layer()
+    assert list(ok.scene_arrays()["layers"]["tag"]) == [N.LAYER_OPACITY, N.LAYER_CLIP]

@@ -27,6 +27,9 @@ STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4,
 
 # PTCL tags (shaders/hlsl/shared/particle_tags.hlsli) + merged-stream marker
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
+PTCL_BEGIN_OPACITY, PTCL_END_OPACITY = 5, 6
+# Layer stack tags (shaders/hlsl/shared/draw_tags.hlsli:7-9)
+LAYER_CLIP, LAYER_OPACITY, LAYER_BLEND = 0, 1, 2
 PTCL_BATCH_BEGIN = 14
 PTCL_SDF = 9
 PTCL_IMAGE = 13
@@ -260,6 +263,8 @@ def library() -> C.CDLL:
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),
         "tk_canvas_push_image": (C.c_int64, [P, C.POINTER(C.c_double), U32, U32, U32, U32]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
+        "tk_canvas_push_opacity_layer": (I32, [P, P, P, F64, F32]),
+        "tk_canvas_last_error": (C.c_char_p, [P]),
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),
         "tk_canvas_scene": (I32, [P, C.POINTER(SceneDesc)]),

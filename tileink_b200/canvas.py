@@ -393,6 +393,13 @@ class Canvas:
         if self._lib.tk_canvas_push_clip_layer(self._h, path._h, t, int(fill_rule), float(tolerance)) != 0:
             raise ValueError("push_clip_layer rejected its arguments")
 
+    def push_opacity_layer(self, path: BezPath, opacity: float, transform=None, tolerance: float = 0.1):
+        """Canvas::push_opacity_layer: the children until pop_layer are
+        composited at `opacity` through the nonzero coverage of `path`."""
+        t, tk = _affine(transform)
+        if self._lib.tk_canvas_push_opacity_layer(self._h, path._h, t, float(tolerance), float(opacity)) != 0:
+            raise ValueError("push_opacity_layer rejected its arguments")
+
     def push_blur_group(self, sigma: float):
         if self._lib.tk_canvas_push_blur_group(self._h, float(sigma)) != 0:
             raise ValueError("blur sigma must be finite and nonnegative")
@@ -404,7 +411,7 @@ class Canvas:
     def scene_desc(self) -> N.SceneDesc:
         d = N.SceneDesc()
         if self._lib.tk_canvas_scene(self._h, C.byref(d)) != 0:
-            raise RuntimeError("canvas compile failed")
+            raise RuntimeError("canvas compile failed: " + (self._lib.tk_canvas_last_error(self._h) or b"").decode())
         return d
 
     def scene_arrays(self) -> dict:

@@ -10,6 +10,8 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <stdexcept>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -353,16 +355,17 @@ std::pair<uint32_t, uint32_t> push_brush(std::vector<uint32_t>& blob, const tk_b
 }
 
 struct Cmd {
-    enum Kind { DRAW, CLIP, BLUR } kind;
+    enum Kind { DRAW, CLIP, BLUR, OPACITY } kind;
     uint32_t draw;
     float sigma;
     uint32_t children;
+    uint32_t payload = 0u;  // OPACITY: opacity_f32_to_u8 of the layer's opacity
 };
 
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY } kind = FILL;
     tk_path path;
     tk_sdf_shape shape{};
     // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options
@@ -375,7 +378,7 @@ struct RecCmd {
     double t[6] = {1, 0, 0, 1, 0, 0};
     uint32_t rule = 0;
     double tolerance = 0.1, width = 0.0;
-    float sigma = 0.0f;
+    float sigma = 0.0f;  // BLUR: sigma; OPACITY: opacity
 };
 
 RecCmd rec_cmd(RecCmd::Kind kind, const tk_path* path, const tk_brush_desc* brush, const double* transform) {
@@ -432,6 +435,8 @@ struct tk_canvas {
     // command log for replay (tk_canvas_set_keep_commands)
     bool keep = false;
     std::vector<RecCmd> log;
+    // why the last compile failed (empty: it did not)
+    std::string compile_error;
 };
 
 namespace {
@@ -601,6 +606,23 @@ struct Compiled {
     std::vector<Op> ops;
 };
 
+// command_list_has_single_stack (src/canvas/compile.rs:355-378): every draw
+// under `list` sits in one command list once clip and opacity layers are
+// entered; a blur group below splits the draws into separate surfaces.
+bool single_stack(const tk_canvas* c, uint32_t list, uint32_t stack, int64_t& first) {
+    for (const Cmd& cmd : c->lists[list]) {
+        if (cmd.kind == Cmd::DRAW) {
+            if (first < 0) first = stack;
+            else if (first != int64_t(stack)) return false;
+        } else if (cmd.kind == Cmd::CLIP || cmd.kind == Cmd::OPACITY) {
+            if (!single_stack(c, cmd.children, cmd.children, first)) return false;
+        } else {
+            return false;
+        }
+    }
+    return true;
+}
+
 void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record>& stack, Compiled& out) {
     std::vector<uint32_t> pending;
     auto flush = [&]() {
@@ -618,6 +640,20 @@ void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record
         } else if (cmd.kind == Cmd::CLIP) {
             flush();
             stack.push_back({TK_LAYER_CLIP, cmd.draw, 0u});
+            compile_into(c, cmd.children, stack, out);
+            stack.pop_back();
+        } else if (cmd.kind == Cmd::OPACITY) {
+            // A path-masked opacity layer fuses into the batch's layer stack
+            // when its subtree draws in one stack (Canvas::can_fuse,
+            // src/canvas/compile.rs:342-353); fine opens and closes the group
+            // per batch (BEGIN_OPACITY / END_OPACITY).
+            int64_t first = -1;
+            if (!single_stack(c, cmd.children, cmd.children, first))
+                throw std::runtime_error(
+                    "an opacity layer over draws in several layer stacks needs an offscreen group, which this "
+                    "path does not build");
+            flush();
+            stack.push_back({TK_LAYER_OPACITY, cmd.draw, cmd.payload});
             compile_into(c, cmd.children, stack, out);
             stack.pop_back();
         } else {
@@ -651,7 +687,13 @@ void compile(tk_canvas* c) {
     if (!c->dirty) return;
     Compiled comp;
     std::vector<tk_layer_record> stack;
-    compile_into(c, 0, stack, comp);
+    c->compile_error.clear();
+    try {
+        compile_into(c, 0, stack, comp);
+    } catch (const std::exception& e) {
+        c->compile_error = e.what();
+        return;
+    }
     // coalesce adjacent batches with equal stacks (execution/batches.rs)
     std::vector<Compiled::Op> merged;
     for (auto& op : comp.ops) {
@@ -1343,6 +1385,28 @@ int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) {
     }
     return 0;
 }
+int32_t tk_canvas_push_opacity_layer(tk_canvas* c, const tk_path* path, const double* transform, double tolerance,
+                                     float opacity) {
+    if (!c || !path || !(tolerance > 0.0) || !std::isfinite(opacity)) return -1;
+    // push_layer_path(DrawTag::Opacity, .., FillRule::NonZero, ..) (canvas/layers.rs:122-140)
+    int64_t draw = push_path_with_tag(c, *path, nullptr, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_OPACITY, false);
+    if (draw < 0) return -1;
+    // opacity_f32_to_u8 (src/shared/pixel.rs:3-6): the stack record's payload
+    const uint32_t alpha = uint32_t(std::min(std::max(opacity, 0.0f), 1.0f) * 255.0f + 0.5f);
+    uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    c->lists[c->stack.back()].push_back({Cmd::OPACITY, uint32_t(draw), 0.0f, child, alpha});
+    c->stack.push_back(child);
+    c->dirty = true;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::OPACITY, path, nullptr, transform);
+        r.tolerance = tolerance;
+        r.sigma = opacity;
+        c->log.push_back(std::move(r));
+    }
+    return 0;
+}
+const char* tk_canvas_last_error(const tk_canvas* c) { return c ? c->compile_error.c_str() : ""; }
 int32_t tk_canvas_pop_layer(tk_canvas* c) {
     if (c->stack.size() <= 1) return -1;
     c->stack.pop_back();
@@ -1358,6 +1422,7 @@ void tk_canvas_set_keep_commands(tk_canvas* c, int32_t enabled) {
 int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     if (!c || !out) return -1;
     compile(c);
+    if (!c->compile_error.empty()) return -1;
     std::memset(out, 0, sizeof(*out));
     out->width = c->W;
     out->height = c->H;
@@ -1782,6 +1847,7 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
         case RecCmd::FILL: return tk_canvas_push_path(dst, &r.path, bp, t, r.rule, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::STROKE: return tk_canvas_push_stroke(dst, &r.path, bp, r.width, t, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
+        case RecCmd::OPACITY: return tk_canvas_push_opacity_layer(dst, &r.path, t, r.tolerance, r.sigma);
         case RecCmd::BLUR: return tk_canvas_push_blur_group(dst, r.sigma);
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
         case RecCmd::SDF:
@@ -1824,7 +1890,9 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
 
 bool has_layers(const std::vector<RecCmd>& log) {
     for (const RecCmd& r : log)
-        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::SDF_CLIP) return true;
+        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::SDF_CLIP ||
+            r.kind == RecCmd::OPACITY)
+            return true;
     return false;
 }
 
