@@ -9,11 +9,16 @@ image readback inside every step (`e2e`).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tileink|reference]
 
-Multi-GPU: one process per GPU (torchrun); every rank renders its own frame
-(replicas, weak scaling); the time is the max over ranks.
+Multi-GPU: one process per GPU (torchrun). The frame is split into tile-row
+bands, one per rank (tk_set_band: each rank scans only the lines that reach
+its band and draws only its rows), and every step ends with an NCCL
+all-gather of the bands, so `value` is whole frames/s (strong scaling); the
+time is the max over ranks. The batched leg splits the scenes over ranks and
+the differentiable leg splits the loss rows and all-reduces the gradients.
 `--impl reference` times the reference path's CPU restatement (the oracle
 port; the reference itself is Rust + HLSL and cannot run here) on the host
-cores, on a bounded sample of the same workload.
+cores: each step draws every 16th tile row of the same frame, with the
+whole-scene scan once per 16 steps.
 """
 from __future__ import annotations
 
@@ -38,7 +43,6 @@ WORKLOAD = "4096x4096 canvas, 50,000 paths (60% fills / 40% round-join strokes),
            "200 Gaussian clusters sigma 300 px, nonzero/even-odd, solid/linear/radial paint, " \
            "10% in clip layers nested <=4"
 SEED = 2
-CPU_SAMPLE_DIV = 16
 
 
 def parse():
@@ -58,6 +62,10 @@ def parse():
     p.add_argument("--sdf-shapes", type=int, default=50000, help="shapes of the SDF-shape leg")
     p.add_argument("--sdf-kinds", default="base", choices=["base", "all"],
                    help="SDF-only runs: the base kinds, or all nineteen (the extended-kind kernel instance)")
+    p.add_argument("--config-steps", type=int, default=10,
+                   help="frames of the 640x360 and 1920x1080 glyph legs (0: skip)")
+    p.add_argument("--cpu-profile", action="store_true",
+                   help="time only the oracle on the benchmarked frame (full, 16 bands, one thread) and print it")
     p.add_argument("--sdf-only", action="store_true",
                    help="run only the SDF-shape leg (rank 0, one GPU) and print its line (profiling runs)")
     return p.parse_args()
@@ -177,6 +185,80 @@ def diff_timing(renderer, steps, warmup):
             "bwd_ms": float(np.median(bwd)), "steps": steps, "loss": loss,
             "timing": "host wall clock per call (median), host buffers in and out",
             "gradient_check": "tests/test_gpu_diff.py: FP64 central differences, relative error <= 1e-3"}
+
+
+def diff_split_timing(device, steps, warmup, world, rank):
+    """fwd+bwd of the blur-group workload over N GPUs: every rank renders the
+    frame and takes the loss and the adjoint of its own pixel rows
+    (tk_diff_scene.loss_row0/1); the partial gradients are all-reduced
+    (NCCL sum). The time of a step is the max over ranks."""
+    import torch
+    import torch.distributed as dist
+    import tileink_b200 as tk
+    from tileink_b200 import diff
+    r = tk.NativeRenderer(device)
+    sc = diff.blur_group_scene(5)
+    tg = diff.blur_group_scene(5, jitter=3.0)
+    _, target = r.diff_forward(tg, np.zeros((sc.height, sc.width, 4), np.float32), return_image=True)
+    h = sc.height
+    sc.loss_rows = (h * rank // world, h * (rank + 1) // world)
+    grads = torch.zeros(sc.points.size + sc.colors.size + 1, dtype=torch.float32, device="cuda")
+
+    def step():
+        loss = r.diff_forward(sc, target)
+        dp, dc, ds = r.diff_backward()
+        grads.copy_(torch.from_numpy(np.concatenate([dp.reshape(-1), dc.reshape(-1), [np.float32(ds)]])))
+        dist.all_reduce(grads)
+        lt = torch.tensor([loss], dtype=torch.float64, device="cuda")
+        dist.all_reduce(lt)
+        return float(lt.item())
+
+    for _ in range(max(warmup, 3)):
+        step()
+    dist.barrier()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        loss = step()
+        torch.cuda.synchronize()
+        times.append(max_over_ranks((time.perf_counter() - t0) * 1e3, world))
+    r.close()
+    return {"workload": "1024x1024, 256 closed paths x 12 cubics, blur group sigma 4, MSE vs jittered target; "
+                        f"loss rows split over {world} ranks, gradients all-reduced",
+            "fwd_bwd_ms": float(np.median(times)), "steps": steps, "loss": loss,
+            "timing": "host wall clock per step (forward, backward, NCCL all-reduce), max over ranks, median"}
+
+
+def batch_parallel_timing(device, n_scenes, steps, world, rank):
+    """The uneven-batch workload over N GPUs: scenes partitioned by line
+    count (shard.scene_partition), each rank batch-renders its own (one CUDA
+    graph launch); scenes/s of the whole batch from the max over ranks."""
+    import torch
+    import tileink_b200 as tk
+    from tileink_b200 import shard
+    scenes = [tk.generate(4, 1000 + i) for i in range(n_scenes)]
+    parts = shard.scene_partition([int(s.scene_desc().line_count) for s in scenes], world)
+    mine = [scenes[i] for i in parts[rank]]
+    b = tk.NativeRenderer(device)
+    t0 = time.perf_counter()
+    b.batch_upload(mine)
+    b.batch_render()
+    b.batch_readback()
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    b.batch_render()
+    b.batch_readback()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b.batch_render()
+    b.batch_readback()
+    render_s = max_over_ranks((time.perf_counter() - t0) / steps, world)
+    b.close()
+    return {"workload": f"{n_scenes} scenes, W and H log-uniform in [64, 1024], 10-2000 closed cubic paths, solid; "
+                        f"scenes split over {world} ranks by line count",
+            "batched_scenes_per_s": n_scenes / render_s, "batched_e2e_scenes_per_s": n_scenes / e2e_s,
+            "batched_ms": render_s * 1e3, "steps": steps, "scenes_per_rank": [len(p) for p in parts],
+            "timing": "host wall clock, max over ranks; batched = graph replays + one readback"}
 
 
 def batch_timing(n_scenes, steps):
@@ -370,54 +452,193 @@ def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
     return line
 
 
-def cpu_baseline(size, paths):
-    """The oracle (CPU restatement of the reference path) on all host cores,
-    on 1/16 of the workload's paths over the same canvas; the frame time is
-    scaled by 16 (scan, coarse and fine work grow linearly with paths)."""
+BANDS = 16  # the CPU arms' step: every BANDS-th tile row of the frame
+
+
+def oracle_band_step(run, desc, k, threads):
+    """Step k of the CPU rotation over the frame: at the start of every
+    rotation the whole-scene scan (count, prefix + cumsum, emit) and the tile
+    bins (OracleRun.prepare), then coarse and fine of the tile rows
+    ty = k mod BANDS, k mod BANDS + BANDS, ... Returns (run, scan seconds or
+    None, raster seconds)."""
     import oracle
-    n = max(1, (paths or 50000) // CPU_SAMPLE_DIV)
-    c = scene(size, n, device_plan=False, seed=SEED + 1)
-    threads = os.cpu_count() or 1
+    t_scan = None
+    if k % BANDS == 0 or run is None:
+        t0 = time.perf_counter()
+        run = oracle.OracleRun.prepare(desc, threads=threads)
+        t_scan = time.perf_counter() - t0
     t0 = time.perf_counter()
-    run = oracle.OracleRun(c.scene_desc(), threads=threads)
-    dt = time.perf_counter() - t0
+    run.raster(k % BANDS, 0, BANDS, threads=threads)
+    return run, t_scan, time.perf_counter() - t0
+
+
+def cpu_baseline(desc, threads=None):
+    """The oracle (the CPU restatement of the reference path) on the host
+    cores, on a bounded sample of the benchmarked frame itself: the
+    whole-scene scan plus one interleaved band (every 16th tile row); the
+    frame time is the scan plus 16 times the band."""
+    threads = threads or os.cpu_count() or 1
+    run, t_scan, t_band = oracle_band_step(None, desc, 0, threads)
     stages = run.stage_times()
     del run
-    est = dt * CPU_SAMPLE_DIV
-    return {"value": 1.0 / est, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"same generator, {n} paths (1/{CPU_SAMPLE_DIV}) on the {size or 4096}^2 canvas; "
-                      f"one full oracle frame took {dt:.2f} s, scaled x{CPU_SAMPLE_DIV}",
-            "sample_seconds": dt, "stage_seconds": stages}
+    frame_s = t_scan + BANDS * t_band
+    return {"value": 1.0 / frame_s, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the benchmarked scene: the whole-scene scan ({t_scan:.2f} s) and tile rows 0, 16, 32, ... "
+                      f"({t_band:.2f} s, 1/{BANDS} of the rows); frame = scan + {BANDS} x band",
+            "scan_seconds": t_scan, "band_seconds": t_band, "stage_seconds": stages}
 
 
 def run_reference(args):
+    """The reference arm: the oracle port of the reference path on all host
+    cores, on the same 4096^2, 50,000-path scene (seed 2) as the GPU arm.
+    Step k draws tile rows k mod 16, k mod 16 + 16, ... of the frame (coarse
+    and fine); the whole-scene scan and tile bins run once per 16-step
+    rotation, inside the step that starts it. frames/s = 1 / (scan + the 16
+    band times), each measured in this run."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import oracle  # noqa: F401
-    n = max(1, (args.paths or 50000) // CPU_SAMPLE_DIV)
-    c = scene(args.size, n, device_plan=False, seed=SEED + 1)
+    c = scene(args.size, args.paths, device_plan=False)
     d = c.scene_desc()
     threads = os.cpu_count() or 1
-    import oracle as O
-    for _ in range(args.warmup):
-        O.OracleRun(d, threads=threads)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        O.OracleRun(d, threads=threads)
-    dt = (time.perf_counter() - t0) / args.steps
-    value = 1.0 / (dt * CPU_SAMPLE_DIV)
+    warmup = max(args.warmup, 3)
+    run = None
+    for k in range(warmup):
+        run, _, _ = oracle_band_step(run, d, k, threads)
+    step_s, band_s, scan_s = [], {}, []
+    for k in range(warmup, warmup + args.steps):
+        run, t_scan, t_band = oracle_band_step(run, d, k, threads)
+        step_s.append(t_band + (t_scan or 0.0))
+        band_s.setdefault(k % BANDS, []).append(t_band)
+        if t_scan is not None:
+            scan_s.append(t_scan)
+    if not scan_s:  # no rotation started inside the timed steps: time the scan once more
+        run, t_scan, _ = oracle_band_step(None, d, 0, threads)
+        scan_s.append(t_scan)
+    del run
+    measured = sorted(band_s)
+    band_mean = {b: statistics.mean(v) for b, v in band_s.items()}
+    if len(measured) == BANDS:
+        frame_s = statistics.mean(scan_s) + sum(band_mean.values())
+        how = f"scan + all {BANDS} bands, each measured in this run"
+    else:
+        frame_s = statistics.mean(scan_s) + BANDS * statistics.mean(band_mean.values())
+        how = f"scan + {BANDS} x the mean of the {len(measured)} bands measured (fewer steps than bands)"
+    value = 1.0 / frame_s
+    sample = (f"oracle port of the reference path on the benchmarked scene; each step draws every {BANDS}th tile "
+              f"row (1/{BANDS} of the frame), the whole-scene scan once per {BANDS}-step rotation; frame = {how}")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * CPU_SAMPLE_DIV * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded generator)",
+            "steps": args.steps, "warmup": warmup, "ms_per_step": statistics.mean(step_s) * 1e3,
+            "frame_ms": frame_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded generator, seed 2)",
             "config": {"workload": WORKLOAD, "width": args.size or 4096, "height": args.size or 4096,
-                       "paths": args.paths or 50000, "sample_paths": n},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"oracle port of the reference path, {n} paths (1/{CPU_SAMPLE_DIV}) per step, "
-                                       f"scaled x{CPU_SAMPLE_DIV}"},
+                       "paths": args.paths or 50000, "step": f"tile rows k mod {BANDS} (+ the scan at k mod "
+                                                          f"{BANDS} == 0)", "segment_plan": "host"},
+            "scan_ms": statistics.mean(scan_s) * 1e3,
+            "band_ms": {str(b): band_mean[b] * 1e3 for b in measured},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def config_leg(r, config, seed, steps, cpu, name, what):
+    """One of the other measured configurations at full size: device-resident
+    frames (CUDA events on the context stream), the same frame end to end
+    through tk_render_to_image (host records in, RGBA8 image out), and the
+    oracle's full frame on all host threads and on one thread."""
+    import torch
+    import tileink_b200 as tk
+    c = tk.generate(config, seed)
+    d = c.scene_desc()
+    img = r.render_to_image(c)  # uploads, warms up
+    for _ in range(3):
+        r.render()
+    r.synchronize()
+    stream = torch.cuda.ExternalStream(r.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        r.render()
+    e1.record(stream)
+    e1.synchronize()
+    gpu_ms = e0.elapsed_time(e1) / steps
+    r.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        img = r.render_to_image(c)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
+    line = {"workload": what, "gpu_frame_ms": gpu_ms, "frames_per_s": 1e3 / gpu_ms,
+            "gpix_per_s": d.width * d.height / (gpu_ms * 1e-3) / 1e9, "e2e_ms": e2e_ms,
+            "e2e_timing": "host wall clock per tk_render_to_image call (host records in, image out)",
+            "steps": steps, "data": f"synthetic (seeded generator, seed {seed})"}
+    if cpu:
+        import oracle
+        for threads in (os.cpu_count() or 1, 1):
+            t0 = time.perf_counter()
+            run = oracle.OracleRun(d, threads=threads)
+            dt = time.perf_counter() - t0
+            if threads > 1:
+                ok = np.array_equal(img.reshape(-1).view(np.uint32), run.get(oracle.OR_IMAGE, np.uint32))
+                line["cpu_matches_gpu"] = bool(ok)
+            del run
+            line[f"cpu_frame_ms_{threads}t" if threads == 1 else "cpu_frame_ms"] = dt * 1e3
+        line["cpu_threads"] = os.cpu_count() or 1
+        line["cpu_kind"] = "port"
+    return line
+
+
+def cpu_profile(args):
+    """The oracle on the benchmarked frame, for profiles/: the unbanded frame
+    on all threads, the 16-band rotation on all threads (scan once plus every
+    band), and one thread on the scan and on 1/256 of the tile rows."""
+    import oracle
+    c = scene(args.size, args.paths, device_plan=False)
+    d = c.scene_desc()
+    threads = os.cpu_count() or 1
+    out = {"workload": WORKLOAD, "threads": threads}
+    t0 = time.perf_counter()
+    run = oracle.OracleRun(d, threads=threads)
+    out["full_frame_s"] = time.perf_counter() - t0
+    out["full_frame_stage_s"] = run.stage_times()
+    del run
+    run, bands = None, []
+    scan = None
+    for k in range(BANDS):
+        run, t_scan, t_band = oracle_band_step(run, d, k, threads)
+        scan = t_scan if t_scan is not None else scan
+        bands.append(t_band)
+    del run
+    out["rotation_scan_s"] = scan
+    out["rotation_band_s"] = bands
+    out["rotation_frame_s"] = scan + sum(bands)
+    out["rotation_over_full"] = out["rotation_frame_s"] / out["full_frame_s"]
+    t0 = time.perf_counter()
+    run = oracle.OracleRun.prepare(d, threads=1)
+    out["one_thread_scan_s"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    run.raster(0, 0, 256, threads=1)
+    out["one_thread_rows_1_in_256_s"] = time.perf_counter() - t0
+    del run
+    out["one_thread_frame_s"] = out["one_thread_scan_s"] + 256 * out["one_thread_rows_1_in_256_s"]
+    print(json.dumps(out), flush=True)
+
+
+def bin_ref_count(canvas):
+    """(bin-list entries, bins, drawn draws) of the binning stage: every drawn
+    draw lands in each 16x16-tile bin its tile box meets."""
+    a = canvas.scene_arrays()
+    d = canvas.scene_desc()
+    tw, th = (d.width + 15) // 16, (d.height + 15) // 16
+    nbx, nby = (tw + 15) // 16, (th + 15) // 16
+    pb = a["draws"]["pixel_bounds"][a["draw_order"]]
+    x0 = np.minimum(np.maximum(pb["x0"], 0) // 16, tw)
+    y0 = np.minimum(np.maximum(pb["y0"], 0) // 16, th)
+    x1 = np.minimum((np.maximum(pb["x1"], 0) + 15) // 16, tw)
+    y1 = np.minimum((np.maximum(pb["y1"], 0) + 15) // 16, th)
+    ok = (x0 < x1) & (y0 < y1)
+    bx = (x1 - 1) // 16 - x0 // 16 + 1
+    by = (y1 - 1) // 16 - y0 // 16 + 1
+    return int((bx * by)[ok].sum()), nbx * nby, len(pb)
 
 
 def pinned_scene(canvas):
@@ -449,6 +670,9 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.cpu_profile:
+        cpu_profile(args)
+        return
     import torch
     import torch.distributed as dist
 
@@ -476,12 +700,34 @@ def main():
     canvas = scene(args.size, args.paths)
     gen_s = time.perf_counter() - t_gen
     r = tk.NativeRenderer(local)
+    # N GPUs: one frame split into tile-row bands (tk_set_band), balanced by
+    # backdrop tiles per row; each step renders every band and all-gathers
+    # the bands' pixels into the whole frame on every rank (NCCL)
+    from tileink_b200 import shard
+    d0 = canvas.scene_desc()
+    H, W = d0.height, d0.width
+    bands = shard.band_partition(shard.row_weights(canvas.scene_arrays()["paths"], (H + 15) // 16), world)
+    band = bands[rank]
+    rows = shard.pixel_rows(band, H)
+    if world > 1:
+        r.set_band(*band)
+        tallest = max(b - a for a, b in (shard.pixel_rows(x, H) for x in bands))
+        band_buf = torch.zeros((tallest, W), dtype=torch.int32, device="cuda")
+        frame_buf = torch.empty((world * tallest, W), dtype=torch.int32, device="cuda")
     r.upload(canvas)
     stream = torch.cuda.ExternalStream(r.stream)
+
+    def frame():
+        r.render()
+        if world > 1:  # this band's rows into the gather buffer, then the all-gather
+            r.readback_rows(rows[0], rows[1], out=band_buf.data_ptr())
+            dist.all_gather_into_tensor(frame_buf, band_buf)
+
     clocks = ClockSampler(local).__enter__()
     for _ in range(max(args.warmup, 3)):
-        r.render()
+        frame()
     r.synchronize()
+    torch.cuda.synchronize()
     stats = r.stats()
     r.set_timing(True)
     stage_sum = {k: 0.0 for k in r.STAGE_NAMES}
@@ -491,10 +737,13 @@ def main():
     t_on = time.perf_counter()
     e0.record(stream)
     for _ in range(args.steps):
-        r.render()
+        frame()
         for k, v in r.stage_times().items():
             stage_sum[k] += v
-    e1.record(stream)
+    if world > 1:
+        e1.record(torch.cuda.current_stream())  # after the last all-gather
+    else:
+        e1.record(stream)
     e1.synchronize()
     t_off = time.perf_counter()
     time.sleep(0.25)
@@ -505,15 +754,37 @@ def main():
     ms = e0.elapsed_time(e1) / args.steps
     r.set_timing(False)
     ms = max_over_ranks(ms, world)
-    value = world * 1000.0 / ms
+    value = 1000.0 / ms  # whole frames: all ranks' bands make one frame
+
+    # the oracle on a bounded sample of this frame (the scan and 1/16 of the
+    # tile rows), with the device's segment plan (equal to the host
+    # planner's: tests/test_gpu_fullsize.py)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from tileink_b200 import _native as N
+        arrays = canvas.scene_arrays()
+        arrays["paths"] = r.debug(N.STAGE_PATHS).copy()
+        cpu_scene = N.ArrayScene(arrays)
+        cpu = cpu_baseline(cpu_scene.desc)
+        del cpu_scene, arrays
+    # tile-draw refs per 16x16-tile bin, for the binning stage's bytes
+    bin_refs, nbins, draw_n = bin_ref_count(canvas)
 
     # end to end: pinned host scene -> H2D -> frame -> D2H image, every step
     out = torch.empty(r.width * r.height * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint32)
 
+    out_rows = out.reshape(r.height, r.width)[rows[0]:rows[1]]
+
+    def read_frame():
+        if world > 1:  # this rank's band rows (each rank reads its own)
+            r.readback_rows(rows[0], rows[1], out=out_rows)
+        else:
+            r.readback(out)
+
     def e2e_ms_of(ps):
         r.upload(ps)
         r.render()
-        r.readback(out)
+        read_frame()
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -522,7 +793,7 @@ def main():
         for _ in range(args.e2e_steps):
             r.upload(ps)
             r.render()
-            r.readback(out)
+            read_frame()
         s1.record(stream)
         s1.synchronize()
         dev_ms = s0.elapsed_time(s1) / args.e2e_steps
@@ -538,13 +809,15 @@ def main():
     ps_flat, bytes_in_flat = pinned_scene(flat_canvas)
     e2e_flat_ms = e2e_ms_of(ps_flat)
     inc_line = None
-    if rank == 0 and args.incremental_steps > 0:
+    if rank == 0 and world == 1 and args.incremental_steps > 0:
         inc_line = incremental_timing(r, args.size, args.incremental_steps)
     sdf_line = None
-    if rank == 0 and args.sdf_steps > 0:
+    if rank == 0 and world == 1 and args.sdf_steps > 0:
         sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline, args.sdf_shapes)
     del ps_flat, flat_canvas
-    bytes_out = out.nbytes
+    bytes_out = out.nbytes  # the whole frame per step (with N GPUs: every rank's band together)
+    if world > 1:
+        bytes_in, bytes_in_flat = world * bytes_in, world * bytes_in_flat  # every rank uploads the scene
 
     # roofline of the dominant kernel
     stage_ms = {k: v / args.steps for k, v in stage_sum.items()}
@@ -560,7 +833,8 @@ def main():
         "scan_count": ("hbm", 24 * L + 4 * S),
         "pool_scan": ("hbm", (4 + 4 + 8 + 4 + 4) * B),
         "scan_emit": ("hbm", 24 * L + 20 * S),
-        "bins": ("hbm", 4 * refs),
+        # each draw's order word and bounds read once, one word per (bin, draw) hit written
+        "bins": ("hbm", 20 * draw_n + 4 * bin_refs + 4 * nbins),
         "coarse_count": ("hbm", 12 * refs + 24 * T),
         "coarse_emit": ("hbm", 12 * refs + 24 * K),
         "fine": ("fp32", 256 * (24 * visits + 10 * fills)),
@@ -594,30 +868,50 @@ def main():
             if len(parts) == 2 and not line.startswith("#") and parts[0] == dominant:
                 roof["traffic"] = int(parts[1])
 
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.size, args.paths)
-    diff_line = diff_timing(r, args.diff_steps, args.warmup) if (rank == 0 and args.diff_steps > 0) else None
-    batch_line = batch_timing(args.batch_scenes, 5) if (rank == 0 and args.batch_scenes > 0) else None
+    configs = None
+    if rank == 0 and world == 1 and args.config_steps > 0:
+        configs = {
+            "c1_640x360_240_paths": config_leg(
+                r, 1, 1, args.config_steps, not args.no_cpu_baseline, "c1",
+                "640x360, 240 closed paths of 8-40 cubics, nonzero, alpha 0.3-1 over white"),
+            "c3_1920x1080_20k_glyphs": config_leg(
+                r, 3, 3, args.config_steps, not args.no_cpu_baseline, "c3",
+                "1920x1080, 20,000 glyphs of 2-4 quadratic contours (6-24 segments), 8-64 px em, black on white"),
+        }
+    if world == 1:
+        diff_line = diff_timing(r, args.diff_steps, args.warmup) if args.diff_steps > 0 else None
+        batch_line = batch_timing(args.batch_scenes, 5) if args.batch_scenes > 0 else None
+    else:  # every rank takes part: split objective and scene-parallel batches
+        diff_line = diff_split_timing(local, args.diff_steps, args.warmup, world, rank) if args.diff_steps > 0 else None
+        batch_line = (batch_parallel_timing(local, args.batch_scenes, 5, world, rank)
+                      if args.batch_scenes > 0 else None)
 
-    launches_per_frame = 5 + 5 * stats["passes"]
+    # per frame: pool clear (k_fill), scan count, item sums, item prefix,
+    # pool scan, path totals, scan emit; per target pass: bins, coarse count,
+    # tile prefix, coarse emit, fine
+    launches_per_frame = 7 + 5 * stats["passes"]
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong" if world > 1 else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, seed 2)",
             "config": {"workload": WORKLOAD, "width": args.size or 4096, "height": args.size or 4096,
-                       "paths": args.paths or 50000, "parallelism": f"replicas x{world}",
+                       "paths": args.paths or 50000,
+                       "parallelism": (f"band split x{world}: tile rows {bands} (one band per rank, paths clamped "
+                                       "to the band at upload), NCCL all-gather of the bands every frame"
+                                       if world > 1 else "one GPU"),
                        "l2": "inputs > L2 (lines %.1f GB), no flush" % (L * 24 / 1e9),
-                       "segment_plan": "device"},
+                       "segment_plan": "device",
+                       "stage_times": "rank 0's band" if world > 1 else "the frame"},
             # the headline: the recorded Canvas (fills and stroke centerlines as
             # Bezier elements) uploaded, flattened, stroked, rendered and read
             # back every step
-            "e2e": {"value": world * 1000.0 / e2e_flat_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in_flat),
+            "e2e": {"value": 1000.0 / e2e_flat_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in_flat),
                     "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_flat_ms,
                     "input": "fills and stroke centerlines as Bezier elements, flattened and stroked on the GPU "
                              "at upload"},
-            "e2e_host_lines": {"value": world * 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
+            "e2e_host_lines": {"value": 1000.0 / e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(bytes_in),
                                "d2h_bytes_per_step": int(bytes_out), "ms_per_step": e2e_ms,
                                "input": "host-flattened lines (the reference's Line records)"},
             "gpu_launches": launches_per_frame * args.steps,
@@ -632,6 +926,7 @@ def main():
             "batched": batch_line,
             "incremental": inc_line,
             "sdf": sdf_line,
+            "configs": configs,
             "scene_generation_s": gen_s,
         }
         print(json.dumps(line), flush=True)

@@ -395,6 +395,28 @@ int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
 int32_t tk_debug_readback_range(tk_ctx* ctx, uint32_t stage, uint32_t index, uint64_t first,
                                 uint64_t count, void* dst, uint64_t* total);
 
+/* Band split (multi-GPU): one rank per GPU renders tile rows
+ * [tile_y0, tile_y1) of the frame. The next tk_scene_upload (or
+ * tk_scene_upload_flatten) clamps every path's tile bbox to those rows, so
+ * the rank scans only the lines that reach its band (tile rows are
+ * independent after the scan: a backdrop is the row-wise cumsum of its own
+ * row's deltas), repacks the backdrop slices and plans segments on the
+ * device; tk_render then runs coarse and fine on the band's tiles only.
+ * Rows outside the band are left unwritten. tile_y0 == tile_y1 returns to
+ * whole frames. Scenes with blur layers are rejected in band mode (a blur
+ * reaches across bands). Band pixels equal the whole frame's. */
+int32_t tk_set_band(tk_ctx* ctx, uint32_t tile_y0, uint32_t tile_y1);
+/* The path records tk_set_band uploads for a band (host only, no device):
+ * each tile bbox clamped to rows [tile_y0, tile_y1) (a path that misses the
+ * band gets rows [tile_y0, tile_y0) and data_len 0), backdrop slices repacked
+ * contiguously in path order, segment_start and segment_capacity 0 for the
+ * device's segment plan (TK_SCENE_SEGMENTS_FROM_DEVICE). */
+void tk_band_paths(const tk_path_record* paths, uint32_t path_count, uint32_t tile_y0, uint32_t tile_y1,
+                   tk_path_record* out);
+/* Pixel rows [row0, row1) of the current image into `rgba8` (host or device
+ * memory: cudaMemcpyDefault), width * (row1 - row0) words. */
+int32_t tk_readback_rows(tk_ctx* ctx, uint32_t row0, uint32_t row1, uint32_t* rgba8, size_t pixel_count);
+
 /* Stage timing with CUDA events recorded on the context stream around each
  * stage of tk_render (no reference counterpart; measurement support).
  * Stages: 0 pool clear, 1 scan_count, 2 pool prefix + cumsum, 3 scan_emit,

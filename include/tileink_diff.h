@@ -43,6 +43,11 @@ typedef struct tk_diff_scene {
     float sigma;               /* blur group sigma (> 0), or 0 for no blur group */
     float tolerance;           /* flattening tolerance, pixels */
     float background[4];       /* premultiplied RGBA under the group */
+    /* Pixel rows [loss_row0, loss_row1) of the loss (loss_row1 == 0: every
+     * row). The mean still divides by all W * H * 4 values, so losses and
+     * gradients of row ranges that partition the image sum to the whole
+     * image's: ranks of a row-split objective all-reduce (sum) them. */
+    uint32_t loss_row0, loss_row1;
 } tk_diff_scene;
 
 /* Renders `scene`, returns the loss against `target` ([height][width][4]

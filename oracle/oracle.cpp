@@ -1733,6 +1733,21 @@ void scan_scene(or_scene& S, int threads) {
     });
     S.times[0] = since(t0);
 
+    // Device segment plan (TK_SCENE_SEGMENTS_FROM_DEVICE, the library's
+    // chained pool scan): capacities are the scanned totals and segment
+    // slices follow each other from 0 in path order.
+    if (D.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) {
+        uint64_t next = 0;
+        for (tk_path_record& p : S.paths) {
+            uint32_t total = 0;
+            for (uint32_t k = 0; k < p.data_len; ++k) total += S.counts[p.data_offset + k];
+            p.segment_start = uint32_t(next);
+            p.segment_capacity = total;
+            next += total;
+        }
+        S.seg_capacity = next;
+    }
+
     // prefix (scan_prefix_chunks + offsets) and row cumsum (cumsum.hlsl).
     t0 = clk::now();
     parallel_for(threads, np, [&](uint64_t pid) {

@@ -45,6 +45,28 @@ def test_every_header_struct_is_in_the_table(layout):
     assert names == set(layout), names ^ set(layout)
 
 
+def header_fields() -> dict:
+    """{struct: [field, ...]} parsed from the three public headers."""
+    out = {}
+    for h in ("tileink.h", "tileink_canvas.h", "tileink_diff.h"):
+        text = re.sub(r"/\*.*?\*/", "", (ROOT / "include" / h).read_text(), flags=re.S)
+        for m in re.finditer(r"typedef struct (\w+) \{(.*?)\} (\w+);", text, flags=re.S):
+            fields = []
+            for decl in m.group(2).split(";"):
+                decl = decl.strip()
+                if not decl:
+                    continue
+                names = decl.split(None, 2 if decl.startswith("const") else 1)[-1].replace("*", "")
+                fields += [re.sub(r"\[.*", "", n).strip() for n in names.split(",")]
+            out[m.group(3)] = fields
+    return out
+
+
+def test_table_lists_every_header_field_in_order(layout):
+    for name, fields in header_fields().items():
+        assert [k for k in layout[name] if k] == fields, name
+
+
 def test_record_sizes_equal_the_reference_pod_types(layout):
     # src/shared/{line,path,draw_record,line_seg,gpu_coarse}.rs
     want = {"tk_line": 24, "tk_path_record": 76, "tk_draw_record": 124, "tk_layer_record": 12,

@@ -141,7 +141,8 @@ class DiffScene(C.Structure):
     """tk_diff_scene (include/tileink_diff.h)."""
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("path_count", C.c_uint32),
                 ("cubics_per_path", C.c_uint32), ("points", C.c_void_p), ("colors", C.c_void_p),
-                ("sigma", C.c_float), ("tolerance", C.c_float), ("background", C.c_float * 4)]
+                ("sigma", C.c_float), ("tolerance", C.c_float), ("background", C.c_float * 4),
+                ("loss_row0", C.c_uint32), ("loss_row1", C.c_uint32)]
 
 
 class BatchInfo(C.Structure):
@@ -231,6 +232,9 @@ def library() -> C.CDLL:
         "tk_stage_scan_prefix": (I32, [P, P, U64, P, U32, P, P, P]),
         "tk_stage_tile_prefix": (I32, [P, P, U32, U32, U32, C.POINTER(U32)]),
         "tk_debug_readback_range": (I32, [P, U32, U32, U64, U64, P, C.POINTER(U64)]),
+        "tk_set_band": (I32, [P, U32, U32]),
+        "tk_band_paths": (None, [P, U32, U32, U32, P]),
+        "tk_readback_rows": (I32, [P, U32, U32, P, C.c_size_t]),
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),
         "tk_stage_blur": (I32, [P, P, P, U32, U32, P, P, F32, U32]),
         "tk_pool_scan_noalloc": (I32, [P, P, U32, P, P, P, P, U64, P]),

@@ -107,6 +107,7 @@ const tk_abi_field kLayout[] = {
     F(tk_diff_scene, width), F(tk_diff_scene, height), F(tk_diff_scene, path_count),
     F(tk_diff_scene, cubics_per_path), F(tk_diff_scene, points), F(tk_diff_scene, colors), F(tk_diff_scene, sigma),
     F(tk_diff_scene, tolerance), F(tk_diff_scene, background),
+    F(tk_diff_scene, loss_row0), F(tk_diff_scene, loss_row1),
 };
 
 #undef S

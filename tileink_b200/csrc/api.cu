@@ -183,6 +183,11 @@ struct tk_ctx {
     const uint8_t* active_mask = nullptr;
     const uint32_t* active_list = nullptr;
     uint32_t active_n = 0;
+    // band split (tk_set_band): tile rows [band_y0, band_y1) of the frame;
+    // paths are clamped to them at upload
+    bool band = false;
+    uint32_t band_y0 = 0, band_y1 = 0;
+    std::vector<tk_path_record> band_paths;
 };
 
 namespace {
@@ -501,7 +506,27 @@ void upload_emit_order(tk_ctx* c) {
 
 void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl);
 
-void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nullptr) {
+// The scene of one band of tile rows: every path's tile bbox clamped to the
+// band's rows (tile rows are independent after the scan: a backdrop is the
+// row-wise cumsum of its own row's deltas, and the scan's tile walk and
+// clipped segments depend on the line and the tile only), backdrop slices
+// repacked in path order and segments planned on the device. Paths that miss
+// the band keep their lines but get an empty bbox, so the scan skips them.
+tk_scene_desc band_scene(tk_ctx* c, const tk_scene_desc& d) {
+    tk_scene_desc b = d;
+    c->band_paths.resize(d.path_count);
+    tk_band_paths(d.paths, d.path_count, c->band_y0, c->band_y1, c->band_paths.data());
+    b.paths = c->band_paths.data();
+    b.flags |= TK_SCENE_SEGMENTS_FROM_DEVICE;
+    return b;
+}
+
+void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl = nullptr) {
+    if (c->band) {
+        const uint32_t th = (scene.height + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
+        if (c->band_y1 > th) invalid("band rows beyond the canvas");
+    }
+    const tk_scene_desc d = c->band ? band_scene(c, scene) : scene;
     // A failed upload leaves no renderable scene behind.
     c->have_scene = false;
     c->rendered = false;
@@ -574,6 +599,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc* fl = nu
     if (c->surfaces.size() < blur_depth) c->surfaces.resize(blur_depth);
     for (size_t i = 0; i < blur_depth; ++i) c->surfaces[i].reserve(uint64_t(c->width) * c->height);
     if (blur_depth) c->temp.reserve(uint64_t(c->width) * c->height);
+    if (c->band && blur_depth) invalid("band rendering takes scenes without blur layers (their reach crosses bands)");
     TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
     TK_CUDA(cudaGetLastError());
     c->have_scene = true;
@@ -788,6 +814,20 @@ void do_render_tiles(tk_ctx* c) {
     c->history_w = c->width;
     c->history_h = c->height;
     c->history_clear = c->clear;
+}
+
+// The band's frame: the scan of the band scene, then coarse and fine of the
+// band's tiles only (the other rows of the image are left as they are).
+void do_render_band(tk_ctx* c) {
+    const uint32_t T = c->tw * c->th;
+    c->h_active.assign(T, 0u);
+    c->h_active_list.clear();
+    for (uint32_t ty = c->band_y0; ty < c->band_y1; ++ty) {
+        std::memset(c->h_active.data() + size_t(ty) * c->tw, 1, c->tw);
+        for (uint32_t tx = 0; tx < c->tw; ++tx) c->h_active_list.push_back(ty * c->tw + tx);
+    }
+    do_render_tiles(c);
+    c->history = false;
 }
 
 void drop_graph(tk_ctx* c) {
@@ -1238,7 +1278,57 @@ int32_t tk_scene_upload(tk_ctx* c, const tk_scene_desc* d) {
 int32_t tk_render(tk_ctx* c) {
     return guarded(c, [&] {
         if (c->batched) do_batch_render(c);
+        else if (c->band) do_render_band(c);
         else do_render(c);
+    });
+}
+
+void tk_band_paths(const tk_path_record* in, uint32_t path_count, uint32_t tile_y0, uint32_t tile_y1,
+                   tk_path_record* out) {
+    uint32_t next = 0;
+    for (uint32_t p = 0; p < path_count; ++p) {
+        tk_path_record r = in[p];
+        const uint32_t stride = r.tile_x1 > r.tile_x0 ? r.tile_x1 - r.tile_x0 : 0u;
+        const uint32_t y0 = std::max(r.tile_y0, tile_y0), y1 = std::min(r.tile_y1, tile_y1);
+        if (y0 >= y1 || stride == 0u) {
+            r.tile_y0 = r.tile_y1 = tile_y0;
+            r.data_len = 0u;
+        } else {
+            r.tile_y0 = y0;
+            r.tile_y1 = y1;
+            r.data_len = stride * (y1 - y0);
+        }
+        r.data_offset = next;
+        next += r.data_len;
+        r.segment_start = 0u;
+        r.segment_capacity = 0u;
+        out[p] = r;
+    }
+}
+
+int32_t tk_set_band(tk_ctx* c, uint32_t tile_y0, uint32_t tile_y1) {
+    return guarded(c, [&] {
+        if (tile_y0 > tile_y1) invalid("band rows reversed");
+        c->band = tile_y1 > tile_y0;
+        c->band_y0 = c->band ? tile_y0 : 0u;
+        c->band_y1 = c->band ? tile_y1 : 0u;
+        c->have_scene = false;  // the next upload applies it
+        c->rendered = false;
+        c->history = false;
+    });
+}
+
+int32_t tk_readback_rows(tk_ctx* c, uint32_t row0, uint32_t row1, uint32_t* rgba8, size_t pixel_count) {
+    return guarded(c, [&] {
+        if (!c->rendered) throw Fail{TK_E_STATE, "nothing rendered"};
+        if (row0 > row1 || row1 > c->height) invalid("rows outside the image");
+        const size_t n = size_t(c->width) * (row1 - row0);
+        if (n && (!rgba8 || pixel_count < n)) invalid("readback buffer too small");
+        if (n)
+            TK_CUDA(cudaMemcpyAsync(rgba8, c->image.ptr + size_t(row0) * c->width, n * 4, cudaMemcpyDefault,
+                                    c->stream));
+        TK_CUDA(cudaStreamSynchronize(c->stream));
+        check_error_word(c);
     });
 }
 
@@ -1763,7 +1853,11 @@ int32_t tk_diff_forward(tk_ctx* c, const tk_diff_scene* sc, const float* target,
         }
         D.bg = make_float4(sc->background[0], sc->background[1], sc->background[2], sc->background[3]);
         if (image) D.d0.reserve(n);
-        tk::launch_diff_composite(B, D.target.ptr, D.bg, n, image ? D.d0.ptr : nullptr, D.gI.ptr, D.sums.ptr, st);
+        // the loss's pixel rows (all of them unless the objective is split by rows)
+        const uint32_t r0 = sc->loss_row1 ? std::min(sc->loss_row0, sc->height) : 0u;
+        const uint32_t r1 = sc->loss_row1 ? std::min(sc->loss_row1, sc->height) : sc->height;
+        tk::launch_diff_composite(B, D.target.ptr, D.bg, n, uint64_t(r0) * sc->width, uint64_t(std::max(r0, r1)) * sc->width,
+                                  image ? D.d0.ptr : nullptr, D.gI.ptr, D.sums.ptr, st);
         TK_CUDA(cudaGetLastError());
         check_error_word(c);
         TK_CUDA(cudaMemcpyAsync(loss, D.sums.ptr, sizeof(double), cudaMemcpyDeviceToHost, st));

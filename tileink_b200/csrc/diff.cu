@@ -127,8 +127,11 @@ __global__ void k_diff_blur(const float4* __restrict__ in, float4* out, const fl
 }
 
 // I = B + bg (1 - B.a); gI = 2 (I - target) / (4 W H); loss partial sums.
+// Only pixels [lo, hi) enter the loss (a row range of a split objective);
+// the mean still divides by every pixel, so the row ranges' losses and
+// gradients sum to the whole frame's.
 __global__ void k_diff_composite(const float4* __restrict__ B, const float4* __restrict__ target, float4 bg,
-                                 uint64_t n, float4* image, float4* gI, double* loss) {
+                                 uint64_t n, uint64_t lo, uint64_t hi, float4* image, float4* gI, double* loss) {
     double acc = 0.0;
     const double inv = 1.0 / (4.0 * double(n));
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
@@ -138,6 +141,10 @@ __global__ void k_diff_composite(const float4* __restrict__ B, const float4* __r
         const float4 t = target[i];
         const float4 d = make_float4(I.x - t.x, I.y - t.y, I.z - t.z, I.w - t.w);
         if (image) image[i] = I;
+        if (i < lo || i >= hi) {
+            gI[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
         const float s = float(2.0 * inv);
         gI[i] = make_float4(s * d.x, s * d.y, s * d.z, s * d.w);
         acc += double(d.x) * d.x + double(d.y) * d.y + double(d.z) * d.z + double(d.w) * d.w;
@@ -345,9 +352,9 @@ void launch_diff_blur(const float4* in, float4* out, const float* w, int32_t r, 
     k_diff_blur<<<grid, 256, 0, st>>>(in, out, w, r, width, height, axis);
 }
 
-void launch_diff_composite(const float4* B, const float4* target, float4 bg, uint64_t n, float4* image, float4* gI,
-                           double* loss, cudaStream_t st) {
-    k_diff_composite<<<148 * 8, 256, 0, st>>>(B, target, bg, n, image, gI, loss);
+void launch_diff_composite(const float4* B, const float4* target, float4 bg, uint64_t n, uint64_t lo, uint64_t hi,
+                           float4* image, float4* gI, double* loss, cudaStream_t st) {
+    k_diff_composite<<<148 * 8, 256, 0, st>>>(B, target, bg, n, lo, hi, image, gI, loss);
 }
 
 void launch_diff_blur_bwd(const float4* dout_src, const float4* fwd_in, float4* din, const float* w, const float* wd,

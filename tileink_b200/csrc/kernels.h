@@ -240,8 +240,8 @@ void launch_stroke_emit(const StrokeView& v, const uint32_t* line_total, tk_path
 void launch_diff_fine_fwd(const SceneView& s, const PassView& p, const float4* colp, float4* layer, cudaStream_t st);
 void launch_diff_blur(const float4* in, float4* out, const float* w, int32_t r, uint32_t width, uint32_t height,
                       int32_t axis, cudaStream_t st);
-void launch_diff_composite(const float4* B, const float4* target, float4 bg, uint64_t n, float4* image, float4* gI,
-                           double* loss, cudaStream_t st);
+void launch_diff_composite(const float4* B, const float4* target, float4 bg, uint64_t n, uint64_t lo, uint64_t hi,
+                           float4* image, float4* gI, double* loss, cudaStream_t st);
 void launch_diff_blur_bwd(const float4* dout_src, const float4* fwd_in, float4* din, const float* w, const float* wd,
                           int32_t r, uint32_t width, uint32_t height, int32_t axis, bool from_gI, float4 bg,
                           double* sig, cudaStream_t st);

@@ -26,6 +26,9 @@ class DiffScene:
     sigma: float = 4.0
     tolerance: float = 0.1
     background: tuple = (1.0, 1.0, 1.0, 1.0)
+    # pixel rows [r0, r1) of the loss; None: every row (the rows of a
+    # row-split objective, whose ranks sum their gradients)
+    loss_rows: tuple | None = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -49,13 +52,16 @@ class DiffScene:
         d.sigma, d.tolerance = float(self.sigma), float(self.tolerance)
         for i in range(4):
             d.background[i] = float(self.background[i])
+        if self.loss_rows is not None:
+            d.loss_row0, d.loss_row1 = int(self.loss_rows[0]), int(self.loss_rows[1])
         return d
 
     def with_params(self, points=None, colors=None, sigma=None) -> "DiffScene":
         return DiffScene(self.width, self.height,
                          self.points if points is None else np.asarray(points, dtype=np.float32),
                          self.colors if colors is None else np.asarray(colors, dtype=np.float32),
-                         self.sigma if sigma is None else float(sigma), self.tolerance, self.background)
+                         self.sigma if sigma is None else float(sigma), self.tolerance, self.background,
+                         self.loss_rows)
 
 
 def blur_group_scene(seed: int, *, width=1024, height=1024, paths=256, sigma=4.0, jitter=0.0) -> DiffScene:

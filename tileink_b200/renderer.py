@@ -127,6 +127,23 @@ class NativeRenderer:
         self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
         return out
 
+    def set_band(self, tile_y0: int, tile_y1: int) -> None:
+        """Render tile rows [tile_y0, tile_y1) from the next upload on
+        (tk_set_band); (0, 0) returns to whole frames."""
+        self._check(self._lib.tk_set_band(self._h, int(tile_y0), int(tile_y1)))
+
+    def readback_rows(self, row0: int, row1: int, out=None) -> np.ndarray:
+        """Pixel rows [row0, row1) as a (rows, width) uint32 array; `out` may
+        be a host array or (int) a device address of that many words."""
+        n = self.width * (row1 - row0)
+        if isinstance(out, int):
+            self._check(self._lib.tk_readback_rows(self._h, int(row0), int(row1), out, n))
+            return None
+        if out is None:
+            out = np.zeros((row1 - row0, self.width), np.uint32)
+        self._check(self._lib.tk_readback_rows(self._h, int(row0), int(row1), N.ptr(out), n))
+        return out
+
     DEBUG_DTYPES = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
                     N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
                     N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE,
