@@ -17,8 +17,8 @@ time is the max over ranks. The batched leg splits the scenes over ranks and
 the differentiable leg splits the loss rows and all-reduces the gradients.
 `--impl reference` times the reference path's CPU restatement (the oracle
 port; the reference itself is Rust + HLSL and cannot run here) on the host
-cores: each step draws every 16th tile row of the same frame, with the
-whole-scene scan once per 16 steps.
+cores: each step draws every 32nd tile row of the same frame, with the
+whole-scene scan once per 32 steps.
 """
 from __future__ import annotations
 
@@ -65,7 +65,7 @@ def parse():
     p.add_argument("--config-steps", type=int, default=10,
                    help="frames of the 640x360 and 1920x1080 glyph legs (0: skip)")
     p.add_argument("--cpu-profile", action="store_true",
-                   help="time only the oracle on the benchmarked frame (full, 16 bands, one thread) and print it")
+                   help="time only the oracle on the benchmarked frame (full, every band, one thread) and print it")
     p.add_argument("--sdf-only", action="store_true",
                    help="run only the SDF-shape leg (rank 0, one GPU) and print its line (profiling runs)")
     return p.parse_args()
@@ -452,7 +452,7 @@ def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
     return line
 
 
-BANDS = 16  # the CPU arms' step: every BANDS-th tile row of the frame
+BANDS = 32  # the CPU arms' step: every BANDS-th tile row of the frame
 
 
 def oracle_band_step(run, desc, k, threads):
@@ -475,8 +475,8 @@ def oracle_band_step(run, desc, k, threads):
 def cpu_baseline(desc, threads=None):
     """The oracle (the CPU restatement of the reference path) on the host
     cores, on a bounded sample of the benchmarked frame itself: the
-    whole-scene scan plus one interleaved band (every 16th tile row); the
-    frame time is the scan plus 16 times the band."""
+    whole-scene scan plus one interleaved band (every BANDS-th tile row);
+    the frame time is the scan plus BANDS times the band."""
     threads = threads or os.cpu_count() or 1
     run, t_scan, t_band = oracle_band_step(None, desc, 0, threads)
     stages = run.stage_times()
@@ -491,10 +491,12 @@ def cpu_baseline(desc, threads=None):
 def run_reference(args):
     """The reference arm: the oracle port of the reference path on all host
     cores, on the same 4096^2, 50,000-path scene (seed 2) as the GPU arm.
-    Step k draws tile rows k mod 16, k mod 16 + 16, ... of the frame (coarse
-    and fine); the whole-scene scan and tile bins run once per 16-step
-    rotation, inside the step that starts it. frames/s = 1 / (scan + the 16
-    band times), each measured in this run."""
+    Step k draws tile rows k mod BANDS, k mod BANDS + BANDS, ... of the frame
+    (coarse and fine); the whole-scene scan and tile bins run once per
+    BANDS-step rotation, inside the step that starts it. frames/s =
+    1 / (scan + the BANDS band times) when every band was timed, else
+    1 / (scan + BANDS x the mean timed band): the bands interleave rows over
+    the whole frame, so each is an even sample of it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -589,7 +591,7 @@ def config_leg(r, config, seed, steps, cpu, name, what):
 
 def cpu_profile(args):
     """The oracle on the benchmarked frame, for profiles/: the unbanded frame
-    on all threads, the 16-band rotation on all threads (scan once plus every
+    on all threads, the band rotation on all threads (scan once plus every
     band), and one thread on the scan and on 1/256 of the tile rows."""
     import oracle
     c = scene(args.size, args.paths, device_plan=False)
@@ -756,8 +758,8 @@ def main():
     ms = max_over_ranks(ms, world)
     value = 1000.0 / ms  # whole frames: all ranks' bands make one frame
 
-    # the oracle on a bounded sample of this frame (the scan and 1/16 of the
-    # tile rows), with the device's segment plan (equal to the host
+    # the oracle on a bounded sample of this frame (the scan and 1/BANDS of
+    # the tile rows), with the device's segment plan (equal to the host
     # planner's: tests/test_gpu_fullsize.py)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -565,11 +565,15 @@ typedef struct tk_incremental_stats {
     uint32_t dirty_tiles;   /* tiles redrawn */
     uint32_t full_redraw;   /* 1 when every tile was redrawn */
     uint32_t reason;        /* TK_FULL_* */
+    uint32_t scan_reused;   /* 1 when the uploaded scene's last scan served the frame */
 } tk_incremental_stats;
 
 /* Renders the uploaded scene, redrawing only the tiles that meet `damage`
  * unless a full redraw is needed (see TK_FULL_*; full_redraw_ratio in (0, 1],
- * the reference's default is 0.7). `stats` may be null. */
+ * the reference's default is 0.7). A partial redraw of a scene that has not
+ * been re-uploaded since its last scan reuses that scan (counts, backdrops,
+ * ranges, segments) and runs only coarse and fine of the damaged tiles.
+ * `stats` may be null. */
 int32_t tk_render_incremental(tk_ctx* ctx, const tk_damage* damage, float full_redraw_ratio,
                               tk_incremental_stats* stats);
 

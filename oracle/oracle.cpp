@@ -1123,6 +1123,7 @@ struct or_scene {
     // (ty - ty0) % row_step == 0 (a band, or every row_step-th row)
     uint32_t ty0 = 0, ty1 = 0, row_step = 1;
     bool in_band(uint32_t ty) const { return ty >= ty0 && ty < ty1 && (ty - ty0) % row_step == 0u; }
+    std::vector<uint32_t> band_tiles;  // the tiles of the rows in_band, row-major
     double times[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
@@ -1678,9 +1679,9 @@ void blur_pass(const uint32_t* src, uint32_t* dst, uint32_t w, uint32_t h, const
 // ---------------------------------------------------------------------------
 void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int threads) {
     auto& streams = S.pass_streams[pass];
-    parallel_for(threads, S.T, [&](uint64_t tile) {
-        uint32_t ty = uint32_t(tile) / S.tw, tx = uint32_t(tile) % S.tw;
-        if (!S.in_band(ty)) return;
+    parallel_for(threads, S.band_tiles.size(), [&](uint64_t bt) {
+        const uint32_t tile = S.band_tiles[bt];
+        uint32_t ty = tile / S.tw, tx = tile % S.tw;
         const auto& list = streams[tile];
         if (list.empty()) return;  // EMPTY in every batch: target unchanged
         for (uint32_t ly = 0; ly < TK_TILE_SIZE; ++ly) {
@@ -1807,6 +1808,10 @@ void raster_scene(or_scene& S, int threads) {
     S.batches.clear();
     S.pass_streams.clear();
     S.times[4] = S.times[5] = S.times[6] = 0.0;
+    S.band_tiles.clear();
+    for (uint32_t ty = 0; ty < S.th; ++ty)
+        if (S.in_band(ty))
+            for (uint32_t tx = 0; tx < S.tw; ++tx) S.band_tiles.push_back(ty * S.tw + tx);
     // Walk ops: batches, passes, blur layers.
     std::vector<uint32_t> main_target(size_t(D.width) * D.height, D.clear_color);
     struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; };
@@ -1821,18 +1826,34 @@ void raster_scene(or_scene& S, int threads) {
         S.pass_streams.emplace_back(S.T);
         auto& streams = S.pass_streams.back();
         auto tc = clk::now();
-        parallel_for(threads, S.T, [&](uint64_t tile) {
-            uint32_t ty = uint32_t(tile) / S.tw;
-            if (!S.in_band(ty)) return;
+        // Batch ids grow along the draw order and along the pass's batches in
+        // compiled plans, so each tile's candidates of one batch are one
+        // painter-order run that a single walk finds (the reference's
+        // per-batch bins); other plans search the whole candidate list.
+        bool sorted = true;
+        for (size_t k = 1; k < pass_batches.size(); ++k)
+            sorted = sorted && S.batches[pass_batches[k - 1]].batch_id < S.batches[pass_batches[k]].batch_id;
+        for (uint32_t k = 1; k < D.draw_order_count && sorted; ++k)
+            sorted = S.batch_ids[D.draw_order[k - 1]] <= S.batch_ids[D.draw_order[k]];
+        parallel_for(threads, S.band_tiles.size(), [&](uint64_t bt) {
+            const uint32_t tile = S.band_tiles[bt];
             const auto& cand = S.bins[tile];
+            uint32_t walk = 0;
             for (uint32_t bi : pass_batches) {
                 const Batch& b = S.batches[bi];
                 // Candidates of one batch form a contiguous painter-order run.
                 uint32_t first = 0, n = 0;
-                for (uint32_t k = 0; k < cand.size(); ++k) {
-                    if (S.batch_ids[cand[k]] == b.batch_id) {
-                        if (n == 0) first = k;
-                        ++n;
+                if (sorted) {
+                    while (walk < cand.size() && S.batch_ids[cand[walk]] < b.batch_id) ++walk;
+                    first = walk;
+                    while (walk < cand.size() && S.batch_ids[cand[walk]] == b.batch_id) ++walk;
+                    n = walk - first;
+                } else {
+                    for (uint32_t k = 0; k < cand.size(); ++k) {
+                        if (S.batch_ids[cand[k]] == b.batch_id) {
+                            if (n == 0) first = k;
+                            ++n;
+                        }
                     }
                 }
                 BatchStream bs;

@@ -122,3 +122,27 @@ def test_gpu_incremental_fallbacks(renderer):
     assert np.array_equal(renderer.readback(), first)
     with pytest.raises(tk.TileinkError):
         renderer.render_incremental({"full": False, "rects": [[0, 0, 1, 1]]}, full_redraw_ratio=0.0)
+
+
+def test_gpu_incremental_frames_reuse_the_unchanged_scan(renderer, reference_renderer):
+    """Partial redraws of a scene that was not uploaded again reuse its scan
+    (scene_scan.rs:116-125's unchanged-history reuse) and still equal full
+    renders; an upload ends the reuse."""
+    c = tk.generate(2, 11, width=W, height=H, paths=300)
+    want = full_image(reference_renderer, c).copy()
+    renderer.upload(c)
+    st = renderer.render_incremental(None)
+    assert st["full_redraw"] == 1 and st["scan_reused"] == 0
+    for k, rect in enumerate([[0, 0, 100, 80], [200, 150, 330, 300], [400, 0, 512, 384]]):
+        st = renderer.render_incremental({"full": False, "rects": [rect]})
+        assert st["full_redraw"] == 0 and st["scan_reused"] == 1, st
+        img = renderer.readback().view(np.uint8).reshape(H, W, 4)
+        assert np.array_equal(img, want), k
+    renderer.upload(c)
+    renderer.render_incremental(None)
+    st = renderer.render_incremental({"full": False, "rects": [[10, 10, 50, 50]]})
+    assert st["scan_reused"] == 1
+    renderer.upload(c)
+    st = renderer.render_incremental({"full": False, "rects": [[10, 10, 50, 50]]})
+    assert st["full_redraw"] == 0 and st["scan_reused"] == 0
+    assert np.array_equal(renderer.readback().view(np.uint8).reshape(H, W, 4), want)

@@ -172,7 +172,7 @@ class Damage(C.Structure):
 class IncrementalStats(C.Structure):
     """tk_incremental_stats (include/tileink.h)."""
     _fields_ = [("total_tiles", C.c_uint32), ("dirty_tiles", C.c_uint32), ("full_redraw", C.c_uint32),
-                ("reason", C.c_uint32)]
+                ("reason", C.c_uint32), ("scan_reused", C.c_uint32)]
 
 
 class AbiField(C.Structure):

@@ -188,6 +188,9 @@ struct tk_ctx {
     bool band = false;
     uint32_t band_y0 = 0, band_y1 = 0;
     std::vector<tk_path_record> band_paths;
+    // the scan buffers hold the scan of the uploaded scene (nothing has
+    // been uploaded or scanned into them since)
+    bool scan_valid = false;
 };
 
 namespace {
@@ -529,6 +532,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     const tk_scene_desc d = c->band ? band_scene(c, scene) : scene;
     // A failed upload leaves no renderable scene behind.
     c->have_scene = false;
+    c->scan_valid = false;
     c->rendered = false;
     c->diff.ready = false;
     c->want_seg_line = false;
@@ -689,6 +693,7 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
 // Pool clear, scan_count, pool scan, path totals and scan_emit.
 void scan_phase(tk_ctx* c) {
     if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
+    c->scan_valid = false;
     cudaStream_t st = c->stream;
     bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
     tk::SceneView s = view(c);
@@ -724,6 +729,7 @@ void scan_phase(tk_ctx* c) {
         StageMark m(c, 3);
         tk::launch_scan_emit(s, st);
     }
+    c->scan_valid = true;
 }
 
 void do_render(tk_ctx* c) {
@@ -787,9 +793,14 @@ void do_render(tk_ctx* c) {
 // The incremental frame: a full scan, then coarse and fine of the active
 // tiles only, over the previous frame (scenes without blur layers: one pass
 // per batch group straight into the image).
-void do_render_tiles(tk_ctx* c) {
+void do_render_tiles(tk_ctx* c, bool reuse_scan = false) {
     c->history = false;
-    scan_phase(c);
+    if (reuse_scan && c->scan_valid) {  // the uploaded scene's scan is still in place
+        c->ev_used = 0;
+        c->marks.clear();
+    } else {
+        scan_phase(c);
+    }
     cudaStream_t st = c->stream;
     const uint32_t T = c->tw * c->th;
     upload(c->tile_active, c->h_active.data(), T, st);
@@ -967,6 +978,7 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
 // indices offset, one BatchScene per canvas.
 void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     c->history = false;  // the image becomes the batch's canvases
+    c->scan_valid = false;
     c->have_scene = false;
     c->rendered = false;
     c->diff.ready = false;
@@ -1315,6 +1327,7 @@ int32_t tk_set_band(tk_ctx* c, uint32_t tile_y0, uint32_t tile_y1) {
         c->have_scene = false;  // the next upload applies it
         c->rendered = false;
         c->history = false;
+        c->scan_valid = false;
     });
 }
 
@@ -1373,7 +1386,11 @@ int32_t tk_render_incremental(tk_ctx* c, const tk_damage* damage, float full_red
             out.full_redraw = 1u;
         } else {
             out.dirty_tiles = uint32_t(c->h_active_list.size());
-            if (out.dirty_tiles) do_render_tiles(c);
+            // The uploaded scene's scan is reused when nothing was uploaded or
+            // scanned since it (the reference reuses an unchanged scene's scan
+            // history, src/native/runtime/program/scene_scan.rs:116-125).
+            out.scan_reused = c->scan_valid ? 1u : 0u;
+            if (out.dirty_tiles) do_render_tiles(c, true);
             else c->rendered = true;  // nothing changed: the image is the frame
         }
         out.reason = reason;
