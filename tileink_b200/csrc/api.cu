@@ -15,6 +15,7 @@
 #include "../../include/tileink_canvas.h"
 #include "../../include/tileink_diff.h"
 #include "flatten_core.h"
+#include "host.h"
 #include "kernels.h"
 
 namespace {
@@ -109,6 +110,10 @@ struct DiffState {
     DBuf<float> color_acc, dpoints, taps, dtaps, ep_w;
     DBuf<uint32_t> ep_point;
     DBuf<double> sums;  // [0] loss [1] dL/dsigma
+    // the forward's host flattening and its device check, kept between calls
+    std::vector<tk_line> h_lines, h_dev_lines;
+    std::vector<uint32_t> h_ep_point;
+    std::vector<float> h_ep_w;
 };
 
 }  // namespace
@@ -722,6 +727,10 @@ void scan_phase(tk_ctx* c) {
         uint32_t total = read_word(c, c->misc.ptr + 2);
         c->segment_needed = uint64_t(total) + 1;
         c->segments.reserve(c->segment_needed);
+        s = view(c);
+    }
+    if (c->want_seg_line) {  // the line of every segment (differentiable mode)
+        c->seg_line.reserve(device_plan ? c->segment_needed : std::max<uint64_t>(c->host_segment_capacity, 1));
         s = view(c);
     }
     s.segment_capacity = device_plan ? c->segment_needed - 1 : c->host_segment_capacity;
@@ -1780,15 +1789,17 @@ int32_t tk_diff_forward(tk_ctx* c, const tk_diff_scene* sc, const float* target,
         DiffState& D = c->diff;
         D.ready = false;
         const uint32_t per = 1u + 3u * sc->cubics_per_path;
-        // flattening with endpoint weights
-        const uint64_t nl = tk_diff_flatten(sc, nullptr, nullptr, nullptr, 0);
-        std::vector<tk_line> lines(nl);
-        std::vector<uint32_t> ep_point(2 * nl);
-        std::vector<float> ep_w(8 * nl);
-        tk_diff_flatten(sc, lines.data(), ep_point.data(), ep_w.data(), nl);
-        // the same scene through the Canvas: blur group, one fill per path
+        // flattening with endpoint weights (paths on host threads)
+        std::vector<tk_line>& lines = D.h_lines;
+        std::vector<uint32_t>& ep_point = D.h_ep_point;
+        std::vector<float>& ep_w = D.h_ep_w;
+        tk_diff_flatten_all(sc, lines, ep_point, ep_w);
+        const uint64_t nl = lines.size();
+        // the same scene through the Canvas: blur group, one fill per path,
+        // kept as Bezier elements and flattened on the device at upload
         std::unique_ptr<tk_canvas, void (*)(tk_canvas*)> cv(tk_canvas_new(sc->width, sc->height, 1.0f),
                                                            tk_canvas_free);
+        tk_canvas_set_device_flatten(cv.get(), 1);
         if (sc->sigma > 0.0f) tk_canvas_push_blur_group(cv.get(), sc->sigma);
         D.colors.assign(sc->colors, sc->colors + 4ull * sc->path_count);
         std::vector<float4> colp(sc->path_count);
@@ -1811,10 +1822,21 @@ int32_t tk_diff_forward(tk_ctx* c, const tk_diff_scene* sc, const float* target,
         }
         if (sc->sigma > 0.0f) tk_canvas_pop_layer(cv.get());
         tk_scene_desc d{};
-        if (tk_canvas_scene(cv.get(), &d) != TK_OK) invalid("canvas compile failed");
-        if (d.line_count != nl || (nl && std::memcmp(d.lines, lines.data(), nl * sizeof(tk_line)) != 0))
-            throw Fail{TK_E_INVALID, "differentiable flattening differs from the canvas flattening"};
-        do_upload(c, d);
+        tk_flatten_desc fl{};
+        if (tk_canvas_scene(cv.get(), &d) != TK_OK || tk_canvas_flatten_desc(cv.get(), &fl) != TK_OK)
+            invalid("canvas compile failed");
+        do_upload(c, d, &fl);
+        // the device's lines must be the weighted flattening's, line for line
+        {
+            std::vector<tk_line>& dev = D.h_dev_lines;
+            dev.resize(c->line_count);
+            if (c->line_count)
+                TK_CUDA(cudaMemcpyAsync(dev.data(), c->lines.ptr, c->line_count * sizeof(tk_line),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            TK_CUDA(cudaStreamSynchronize(c->stream));
+            if (c->line_count != nl || (nl && std::memcmp(dev.data(), lines.data(), nl * sizeof(tk_line)) != 0))
+                throw Fail{TK_E_INVALID, "differentiable flattening differs from the canvas flattening"};
+        }
         uint32_t pass = UINT32_MAX;
         for (const Step& s : c->steps)
             if (s.kind == STEP_PASS) {
@@ -1823,8 +1845,7 @@ int32_t tk_diff_forward(tk_ctx* c, const tk_diff_scene* sc, const float* target,
             }
         if (pass == UINT32_MAX) invalid("no draw pass");
         cudaStream_t st = c->stream;
-        c->seg_line.reserve(std::max<uint64_t>(c->host_segment_capacity, 1));
-        c->want_seg_line = true;
+        c->want_seg_line = true;  // sized by the scan (device segment plan)
         scan_phase(c);
         run_pass(c, c->passes[pass], nullptr, false);
         check_error_word(c);

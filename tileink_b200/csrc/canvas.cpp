@@ -10,8 +10,10 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <atomic>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -19,6 +21,7 @@
 #include "../../include/tileink_canvas.h"
 #include "../../include/tileink_diff.h"
 #include "flatten_core.h"
+#include "host.h"
 #include "planner.h"
 #include "stroke_core.h"
 
@@ -1761,54 +1764,104 @@ extern "C" tk_canvas* tk_generate(uint32_t config, uint64_t seed, const tk_gen_p
 // The differentiable scene's flattening: flatten_path on move_to, cubic_to...,
 // close, with every point carrying its weights over the four control points of
 // its cubic (WPt), so that d(line endpoint)/d(control point) is known.
-uint64_t tk_diff_flatten(const tk_diff_scene* sc, tk_line* lines, uint32_t* endpoint_point, float* endpoint_weights,
-                         uint64_t capacity) {
-    if (!sc || !sc->points || sc->cubics_per_path == 0) return 0;
+namespace {
+// One path of the differentiable flattening: its lines in order, each handed
+// to emit(line, base0, w0[4], base1, w1[4]) with its endpoints' control-point
+// base indices and weights.
+template <class Emit>
+void diff_flatten_path(const tk_diff_scene* sc, uint32_t path, Emit&& emit) {
     const uint32_t n = sc->cubics_per_path, per = 1u + 3u * n;
     const double tol = double(sc->tolerance);
     struct Node {
         WPt p;
         uint32_t base;  // global index of the first of the four control points the weights refer to
     };
-    uint64_t count = 0;
-    for (uint32_t path = 0; path < sc->path_count; ++path) {
-        const float* P = sc->points + size_t(2) * per * path;
-        auto pt = [&](uint32_t j) { return Pt{double(P[2 * j]), double(P[2 * j + 1])}; };
-        const uint32_t first = path * per;
-        const Node start{{pt(0), {1.0, 0.0, 0.0, 0.0}}, first};
-        Node last = start;
-        auto push = [&](const Node& a, const Node& b) {
-            double dx = a.p.v.x - b.p.v.x, dy = a.p.v.y - b.p.v.y;
-            if (!(dx * dx + dy * dy > 1.0e-12 * 1.0e-12)) return;
-            if (count < capacity) {
-                if (lines)
-                    lines[count] = tk_line{path, 0.0f, {float(a.p.v.x), float(a.p.v.y)}, {float(b.p.v.x), float(b.p.v.y)}};
-                if (endpoint_point) {
-                    endpoint_point[2 * count] = a.base;
-                    endpoint_point[2 * count + 1] = b.base;
-                }
-                if (endpoint_weights)
-                    for (int i = 0; i < 4; ++i) {
-                        endpoint_weights[8 * count + i] = float(a.p.w[i]);
-                        endpoint_weights[8 * count + 4 + i] = float(b.p.w[i]);
-                    }
-            }
-            ++count;
-        };
-        for (uint32_t k = 0; k < n; ++k) {
-            const uint32_t base = first + 3u * k;
-            // c[0] is the previous cubic's exact end point, pt(3k)
-            const WPt c[4] = {{pt(3 * k), {1, 0, 0, 0}}, {pt(3 * k + 1), {0, 1, 0, 0}},
-                              {pt(3 * k + 2), {0, 0, 1, 0}}, {pt(3 * k + 3), {0, 0, 0, 1}}};
-            flatten_cubic(c, tol, [&](const WPt& q) {
-                const Node nd{q, base};
-                push(last, nd);
-                last = nd;
-            });
-        }
-        push(last, start);
+    const float* P = sc->points + size_t(2) * per * path;
+    auto pt = [&](uint32_t j) { return Pt{double(P[2 * j]), double(P[2 * j + 1])}; };
+    const uint32_t first = path * per;
+    const Node start{{pt(0), {1.0, 0.0, 0.0, 0.0}}, first};
+    Node last = start;
+    auto push = [&](const Node& a, const Node& b) {
+        double dx = a.p.v.x - b.p.v.x, dy = a.p.v.y - b.p.v.y;
+        if (!(dx * dx + dy * dy > 1.0e-12 * 1.0e-12)) return;
+        emit(tk_line{path, 0.0f, {float(a.p.v.x), float(a.p.v.y)}, {float(b.p.v.x), float(b.p.v.y)}}, a.base,
+             a.p.w, b.base, b.p.w);
+    };
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t base = first + 3u * k;
+        // c[0] is the previous cubic's exact end point, pt(3k)
+        const WPt c[4] = {{pt(3 * k), {1, 0, 0, 0}}, {pt(3 * k + 1), {0, 1, 0, 0}},
+                          {pt(3 * k + 2), {0, 0, 1, 0}}, {pt(3 * k + 3), {0, 0, 0, 1}}};
+        flatten_cubic(c, tol, [&](const WPt& q) {
+            const Node nd{q, base};
+            push(last, nd);
+            last = nd;
+        });
     }
-    return count;
+    push(last, start);
+}
+
+// f(p) for every path p on host threads.
+template <class F>
+void for_each_path(uint32_t np, F&& f) {
+    const uint32_t nt = std::max<uint32_t>(1u, std::min<uint32_t>(np, std::thread::hardware_concurrency()));
+    std::atomic<uint32_t> next{0};
+    auto work = [&]() {
+        for (uint32_t p; (p = next.fetch_add(1)) < np;) f(p);
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+}
+}  // namespace
+
+void tk_diff_flatten_all(const tk_diff_scene* sc, std::vector<tk_line>& lines, std::vector<uint32_t>& ep_point,
+                         std::vector<float>& ep_w) {
+    lines.clear();
+    ep_point.clear();
+    ep_w.clear();
+    if (!sc || !sc->points || sc->cubics_per_path == 0 || sc->path_count == 0) return;
+    // paths are independent: count every path's lines on host threads, then
+    // each thread writes its paths at their offsets (the vectors keep their
+    // capacity between calls, so a steady caller touches no fresh pages)
+    const uint32_t np = sc->path_count;
+    std::vector<uint64_t> off(np + 1, 0);
+    for_each_path(np, [&](uint32_t p) {
+        uint64_t n = 0;
+        diff_flatten_path(sc, p, [&](const tk_line&, uint32_t, const double*, uint32_t, const double*) { ++n; });
+        off[p + 1] = n;
+    });
+    for (uint32_t p = 0; p < np; ++p) off[p + 1] += off[p];
+    lines.resize(off[np]);
+    ep_point.resize(2 * off[np]);
+    ep_w.resize(8 * off[np]);
+    for_each_path(np, [&](uint32_t p) {
+        uint64_t at = off[p];
+        diff_flatten_path(sc, p, [&](const tk_line& l, uint32_t b0, const double* w0, uint32_t b1, const double* w1) {
+            lines[at] = l;
+            ep_point[2 * at] = b0;
+            ep_point[2 * at + 1] = b1;
+            for (int i = 0; i < 4; ++i) {
+                ep_w[8 * at + i] = float(w0[i]);
+                ep_w[8 * at + 4 + i] = float(w1[i]);
+            }
+            ++at;
+        });
+    });
+}
+
+uint64_t tk_diff_flatten(const tk_diff_scene* sc, tk_line* lines, uint32_t* endpoint_point, float* endpoint_weights,
+                         uint64_t capacity) {
+    std::vector<tk_line> L;
+    std::vector<uint32_t> E;
+    std::vector<float> Wt;
+    tk_diff_flatten_all(sc, L, E, Wt);
+    const uint64_t k = std::min<uint64_t>(capacity, L.size());
+    if (lines) std::copy(L.begin(), L.begin() + k, lines);
+    if (endpoint_point) std::copy(E.begin(), E.begin() + 2 * k, endpoint_point);
+    if (endpoint_weights) std::copy(Wt.begin(), Wt.begin() + 8 * k, endpoint_weights);
+    return L.size();
 }
 
 // ---------------------------------------------------------------------------
