@@ -257,9 +257,22 @@ typedef struct tk_tile_record {
 #define TK_OP_DRAW_BATCH 0u
 #define TK_OP_BLUR_BEGIN 1u
 #define TK_OP_BLUR_END 2u
+/* BLUR_BEGIN's batch_id word is the blur's sampling (Filter::Blur's
+ * BlurSampling, src/shared/layer/filter.rs:183-227): factor | downsample
+ * filter << 8 | upsample filter << 16. Factor 0 or 1 blurs at full
+ * resolution; a factor f > 1 reduces the output bounds by f (nearest or box
+ * filter), blurs there at sigma / f and restores them (nearest or bilinear),
+ * render/filter_program/blur.rs:24-73, filter/resample.hlsli. */
+#define TK_BLUR_SAMPLING(factor, down, up) ((uint32_t)(factor) | ((uint32_t)(down) << 8) | ((uint32_t)(up) << 16))
+#define TK_BLUR_DOWNSAMPLE_NEAREST 0u
+#define TK_BLUR_DOWNSAMPLE_BOX 1u
+#define TK_BLUR_UPSAMPLE_NEAREST 0u
+#define TK_BLUR_UPSAMPLE_BILINEAR 1u
+#define TK_BLUR_MAX_FACTOR 64u
 typedef struct tk_op {
     uint32_t kind;
-    uint32_t batch_id;     /* DRAW_BATCH: draw_batch_ids value of its draws */
+    uint32_t batch_id;     /* DRAW_BATCH: draw_batch_ids value of its draws;
+                              BLUR_BEGIN: TK_BLUR_SAMPLING word (0: full resolution) */
     uint32_t layer_start;  /* DRAW_BATCH: fused layer stack range */
     uint32_t layer_end;
     float sigma;           /* BLUR_BEGIN: physical standard deviation */

@@ -152,6 +152,12 @@ int64_t tk_canvas_push_image(tk_canvas* c, const double rect[4], uint32_t image,
 int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const double* transform,
                                   uint32_t fill_rule, double tolerance);
 int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);
+/* The same group blurred with a BlurSampling (TK_BLUR_SAMPLING(factor,
+ * downsample filter, upsample filter); factor <= TK_BLUR_MAX_FACTOR): the
+ * reference's Filter::Blur { std_dev, std_dev, sampling }
+ * (src/shared/layer/filter.rs:53-60) over the group's output bounds.
+ * Returns -1 for a bad sigma or sampling word. */
+int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sampling);
 /* Canvas::push_opacity_layer (src/canvas/layers.rs:122-140): the children
  * until the matching pop are composited at `opacity` (clamped to [0, 1],
  * stored as opacity_f32_to_u8) through the nonzero coverage of `path`. The

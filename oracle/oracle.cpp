@@ -1674,6 +1674,59 @@ void blur_pass(const uint32_t* src, uint32_t* dst, uint32_t w, uint32_t h, const
     });
 }
 
+// --- filter/resample.hlsli: reduced-resolution blur (BlurSampling factor > 1) ---
+// filter_downsample_pixel for every low texel of `low_rect`: the cell's centre
+// texel (filter 0) or its byte average rounded half up (filter 1).
+void downsample_region(const uint32_t* src, uint32_t* low, uint32_t width, const int32_t rect[4],
+                       const int32_t low_rect[4], uint32_t factor, uint32_t filter) {
+    const uint32_t x0 = uint32_t(rect[0]), y0 = uint32_t(rect[1]), x1 = uint32_t(rect[2]), y1 = uint32_t(rect[3]);
+    for (uint32_t ly = uint32_t(low_rect[1]); ly < uint32_t(low_rect[3]); ++ly)
+        for (uint32_t lx = uint32_t(low_rect[0]); lx < uint32_t(low_rect[2]); ++lx) {
+            const uint32_t bx = std::max(lx * factor, x0), by = std::max(ly * factor, y0);
+            const uint32_t ex = std::min((lx + 1u) * factor, x1), ey = std::min((ly + 1u) * factor, y1);
+            uint32_t out = 0u;
+            if (bx < ex && by < ey) {
+                if (filter == 0u) {
+                    const uint32_t px = std::min(std::max((bx + ex - 1u) / 2u, x0), x1 - 1u);
+                    const uint32_t py = std::min(std::max((by + ey - 1u) / 2u, y0), y1 - 1u);
+                    out = src[size_t(py) * width + px];
+                } else {
+                    float sum[4] = {0, 0, 0, 0};
+                    for (uint32_t sy = by; sy < ey; ++sy)
+                        for (uint32_t sx = bx; sx < ex; ++sx) {
+                            const uint32_t p = src[size_t(sy) * width + sx];
+                            for (int c = 0; c < 4; ++c) sum[c] += float((p >> (8 * c)) & 255u);
+                        }
+                    const float inv = 1.0f / float((ex - bx) * (ey - by));
+                    uint32_t b[4];
+                    for (int c = 0; c < 4; ++c) b[c] = f2u(clampf(mad(sum[c], inv, 0.5f), 0.0f, 255.0f));
+                    out = pack(b[0], b[1], b[2], b[3]);
+                }
+            }
+            low[size_t(ly) * width + lx] = out;
+        }
+}
+// filter_upsample_pixel for every texel of `rect`: the nearest low texel
+// (filter 0) or the bilinear sample stored by pack_premul_rgba8 (filter 1).
+void upsample_region(const uint32_t* low, uint32_t* dst, uint32_t width, uint32_t height, const int32_t rect[4],
+                     const int32_t low_rect[4], uint32_t factor, uint32_t filter) {
+    const float f = float(std::max(factor, 1u));
+    for (uint32_t y = uint32_t(rect[1]); y < uint32_t(rect[3]); ++y)
+        for (uint32_t x = uint32_t(rect[0]); x < uint32_t(rect[2]); ++x) {
+            const float px = clampf((float(x) + 0.5f) / f - 0.5f, float(low_rect[0]), float(uint32_t(low_rect[2]) - 1u));
+            const float py = clampf((float(y) + 0.5f) / f - 0.5f, float(low_rect[1]), float(uint32_t(low_rect[3]) - 1u));
+            uint32_t out;
+            if (filter == 0u) {
+                out = low[size_t(f2i(round_ne(py))) * width + uint32_t(f2i(round_ne(px)))];
+            } else {
+                const F4 p = sample_premul(low, width, height, px, py);
+                out = pack(f2u(clampf(p.r, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(p.g, 0.0f, 1.0f) * 255.0f + 0.5f),
+                           f2u(clampf(p.b, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(p.a, 0.0f, 1.0f) * 255.0f + 0.5f));
+            }
+            dst[size_t(y) * width + x] = out;
+        }
+}
+
 // ---------------------------------------------------------------------------
 // Frame driver.
 // ---------------------------------------------------------------------------
@@ -1814,7 +1867,7 @@ void raster_scene(or_scene& S, int threads) {
             for (uint32_t tx = 0; tx < S.tw; ++tx) S.band_tiles.push_back(ty * S.tw + tx);
     // Walk ops: batches, passes, blur layers.
     std::vector<uint32_t> main_target(size_t(D.width) * D.height, D.clear_color);
-    struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; };
+    struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; uint32_t sampling; };
     std::vector<Surface> surfaces;
     auto current = [&]() -> std::vector<uint32_t>& { return surfaces.empty() ? main_target : surfaces.back().img; };
     bool pass_open = false;
@@ -1891,6 +1944,7 @@ void raster_scene(or_scene& S, int threads) {
             s.img.assign(size_t(D.width) * D.height, 0u);
             s.sigma = op.sigma;
             std::memcpy(s.bounds, op.bounds, sizeof(s.bounds));
+            s.sampling = (op.batch_id & 255u) > 1u ? op.batch_id : 0u;  // BlurSampling word
             surfaces.push_back(std::move(s));
         } else if (op.kind == TK_OP_BLUR_END) {
             flush_pass();
@@ -1907,7 +1961,23 @@ void raster_scene(or_scene& S, int threads) {
             int32_t sx0 = std::max(s.bounds[0] - rad, 0), sy0 = std::max(s.bounds[1] - rad, 0);
             int32_t sx1 = std::min(s.bounds[2] + rad, int32_t(D.width));
             int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
-            if (bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
+            if (s.sampling != 0u && bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
+                // BlurSampling factor > 1 (render/filter_program/blur.rs:24-73): reduce
+                // the output bounds, blur at sigma / factor, restore
+                const uint32_t factor = s.sampling & 255u;
+                const int32_t f = int32_t(factor);
+                auto fdiv = [](int32_t v, int32_t d) { return v >= 0 ? v / d : -((-v + d - 1) / d); };
+                const int32_t rect[4] = {bx0, by0, bx1, by1};
+                const int32_t lr[4] = {fdiv(bx0, f), fdiv(by0, f), -fdiv(-bx1, f), -fdiv(-by1, f)};
+                std::vector<uint32_t> low(s.img.size(), 0u), temp(s.img.size(), 0u);
+                downsample_region(s.img.data(), low.data(), D.width, rect, lr, factor, (s.sampling >> 8) & 255u);
+                uint32_t region[4] = {uint32_t(lr[0]), uint32_t(lr[1]), uint32_t(lr[2] - lr[0]), uint32_t(lr[3] - lr[1])};
+                uint32_t none[4] = {0, 0, 0, 0};
+                const float low_sigma = s.sigma / float(factor);
+                blur_pass(low.data(), temp.data(), D.width, D.height, region, none, low_sigma, 0, threads);
+                blur_pass(temp.data(), low.data(), D.width, D.height, region, none, low_sigma, 1, threads);
+                upsample_region(low.data(), s.img.data(), D.width, D.height, rect, lr, factor, (s.sampling >> 16) & 255u);
+            } else if (bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
                 uint32_t region[4] = {uint32_t(sx0), uint32_t(sy0), uint32_t(sx1 - sx0), uint32_t(sy1 - sy0)};
                 uint32_t none[4] = {0, 0, 0, 0};
                 std::vector<uint32_t> temp(s.img.size(), 0u);

@@ -74,3 +74,21 @@ def opacity_scene(seed, w=256, h=192):
     for k in range(4):
         fill(k)
     return c
+
+
+def sampled_blur_scene(seed, factor, down, up, w=200, h=150, sigma=5.0):
+    """Fills inside a blur group blurred through a copy reduced by `factor`
+    (BlurSampling), over fills outside it."""
+    from tileink_b200 import _native as N
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(w, h)
+    c.set_clear_color(0xFFFFFFFF)
+    for _ in range(4):
+        c.push_path(blob(rng, rng.uniform(0, w), rng.uniform(0, h), 30), tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0))
+    c.push_blur_group(sigma, factor=factor, downsample=down, upsample=up)
+    for k in range(8):
+        c.push_path(blob(rng, rng.uniform(10, w - 10), rng.uniform(10, h - 10), rng.uniform(8, 40)),
+                    tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.4, 1))), fill_rule=k % 2)
+    c.pop_layer()
+    c.push_path(blob(rng, w * 0.5, h * 0.5, 20), tk.Brush.solid(0.1, 0.2, 0.3, 0.5))
+    return c

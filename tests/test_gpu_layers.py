@@ -95,3 +95,12 @@ def test_gpu_draw_counts_across_pages(renderer, draws, stack):
     assert np.array_equal(ptcl, ref.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0))
     assert np.array_equal(img, ref.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(img.shape))
     assert np.array_equal(img, oracle.interpret_path_draws(c.scene_desc(), threads=4))
+
+
+@pytest.mark.parametrize("factor, down, up", [(2, 1, 1), (3, 1, 1), (4, 0, 0), (4, 1, 0), (8, 0, 1), (5, 1, 1)])
+def test_gpu_sampled_blur_matches_oracle(renderer, factor, down, up):
+    """Blur groups through a copy reduced by `factor` (BlurSampling;
+    filter/resample.hlsli): downsample, Gaussian at sigma / factor,
+    upsample, composite — bit-exact against the oracle."""
+    from layer_cases import sampled_blur_scene
+    compare_frame(renderer, sampled_blur_scene(factor * 7 + down, factor, down, up, sigma=6.5))

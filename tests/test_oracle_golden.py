@@ -471,3 +471,35 @@ def test_opacity_layer_payload_and_fusion_rules():
     ok.pop_layer()
     ok.pop_layer()
     assert list(ok.scene_arrays()["layers"]["tag"]) == [N.LAYER_OPACITY, N.LAYER_CLIP]
+
+
+def test_sampled_blur_factor_one_records_a_full_resolution_blur():
+    from layer_cases import sampled_blur_scene
+    a = sampled_blur_scene(3, 1, N.BLUR_DOWNSAMPLE_BOX, N.BLUR_UPSAMPLE_BILINEAR)
+    ops = a.scene_arrays()["ops"]
+    assert ops[ops["kind"] == N.OP_BLUR_BEGIN]["batch_id"].tolist() == [0]
+
+
+@pytest.mark.parametrize("factor, down, up", [(2, 1, 1), (4, 1, 1), (3, 0, 0), (4, 1, 0), (8, 0, 1)])
+def test_oracle_sampled_blur_stays_near_the_full_resolution_blur(factor, down, up):
+    """A reduced-resolution blur (BlurSampling, filter/resample.hlsli)
+    approximates the full-resolution Gaussian of the same group: uniform
+    regions stay uniform and the images differ by a few levels at most."""
+    from oracle import OracleRun, OR_IMAGE
+    from layer_cases import sampled_blur_scene
+    full = sampled_blur_scene(5, 1, 1, 1, sigma=8.0)
+    red = sampled_blur_scene(5, factor, down, up, sigma=8.0)
+    ops = red.scene_arrays()["ops"]
+    assert ops[ops["kind"] == N.OP_BLUR_BEGIN]["batch_id"].tolist() == [N.blur_sampling(factor, down, up)]
+    a = OracleRun(full.scene_desc(), threads=4).get(OR_IMAGE, np.uint32).view(np.uint8).reshape(150, 200, 4)
+    b = OracleRun(red.scene_desc(), threads=4).get(OR_IMAGE, np.uint32).view(np.uint8).reshape(150, 200, 4)
+    diff = np.abs(a.astype(int) - b.astype(int))
+    assert np.median(diff) <= 1
+    assert diff.max() <= (40 if up == 0 else 24)
+
+
+def test_sampled_blur_rejects_bad_sampling():
+    c = tk.Canvas(64, 64)
+    for f, d, u in [(65, 1, 1), (2, 2, 1), (2, 1, 2)]:
+        with pytest.raises(ValueError):
+            c.push_blur_group(4.0, factor=f, downsample=d, upsample=u)

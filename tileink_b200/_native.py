@@ -35,6 +35,13 @@ PTCL_SDF = 9
 PTCL_IMAGE = 13
 PATTERN_NEAREST, PATTERN_BILINEAR = 0, 1
 MAX_IMAGE_DIMENSION = 16384  # TK_MAX_IMAGE_DIMENSION
+BLUR_DOWNSAMPLE_NEAREST, BLUR_DOWNSAMPLE_BOX = 0, 1
+BLUR_UPSAMPLE_NEAREST, BLUR_UPSAMPLE_BILINEAR = 0, 1
+
+
+def blur_sampling(factor: int, down: int = BLUR_DOWNSAMPLE_BOX, up: int = BLUR_UPSAMPLE_BILINEAR) -> int:
+    """TK_BLUR_SAMPLING(factor, downsample filter, upsample filter)."""
+    return int(factor) | (int(down) << 8) | (int(up) << 16)
 PTCL_BEGIN_SDF_CLIP = 12
 TILE_KIND_INTERPRETER, TILE_KIND_EMPTY, TILE_KIND_COLOR, TILE_KIND_SDF, TILE_KIND_MIXED = 0, 1, 2, 3, 4
 # SDF kinds (src/shared/gpu_types.rs) and line caps
@@ -268,6 +275,7 @@ def library() -> C.CDLL:
         "tk_canvas_push_image": (C.c_int64, [P, C.POINTER(C.c_double), U32, U32, U32, U32]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
         "tk_canvas_push_opacity_layer": (I32, [P, P, P, F64, F32]),
+        "tk_canvas_push_blur_group_sampled": (I32, [P, F32, U32]),
         "tk_canvas_last_error": (C.c_char_p, [P]),
         "tk_canvas_push_blur_group": (I32, [P, F32]),
         "tk_canvas_pop_layer": (I32, [P]),

@@ -400,9 +400,13 @@ class Canvas:
         if self._lib.tk_canvas_push_opacity_layer(self._h, path._h, t, float(tolerance), float(opacity)) != 0:
             raise ValueError("push_opacity_layer rejected its arguments")
 
-    def push_blur_group(self, sigma: float):
-        if self._lib.tk_canvas_push_blur_group(self._h, float(sigma)) != 0:
-            raise ValueError("blur sigma must be finite and nonnegative")
+    def push_blur_group(self, sigma: float, factor: int = 1, downsample: int = N.BLUR_DOWNSAMPLE_BOX,
+                        upsample: int = N.BLUR_UPSAMPLE_BILINEAR):
+        """Canvas::push_blur_group; factor > 1 blurs through a copy reduced
+        by `factor` (the BlurSampling of Filter::Blur)."""
+        word = N.blur_sampling(factor, downsample, upsample) if factor > 1 else 0
+        if self._lib.tk_canvas_push_blur_group_sampled(self._h, float(sigma), word) != 0:
+            raise ValueError("blur sigma must be finite and nonnegative, and the sampling valid")
 
     def pop_layer(self):
         if self._lib.tk_canvas_pop_layer(self._h) != 0:

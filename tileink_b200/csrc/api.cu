@@ -94,6 +94,7 @@ struct Step {
     uint32_t pass;
     float sigma;
     int32_t bounds[4];
+    uint32_t sampling = 0u;  // BLUR_BEGIN: TK_BLUR_SAMPLING_* word (0: full resolution)
 };
 
 // State of the last differentiable forward, kept for its backward.
@@ -150,7 +151,7 @@ struct tk_ctx {
     DBuf<tk::SegmentRec> segments;
     DBuf<tk::PaintInfo> paints;  // per draw, built at upload
     uint64_t segment_needed = 0;  // device plan: total from the last frame
-    DBuf<uint32_t> image, temp;
+    DBuf<uint32_t> image, temp, low;  // target, blur temporary, reduced-resolution blur surface
     std::vector<DBuf<uint32_t>> surfaces;
     bool rendered = false;
     // paths by decreasing line count: the order scan_emit's warps take them
@@ -380,7 +381,12 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             open = false;
             if (op.layer_end > op.layer_start) invalid("blur groups under clip layers are outside this path");
             if (!(op.sigma >= 0.0f) || !std::isfinite(op.sigma)) invalid("bad blur sigma");
-            Step s{STEP_BLUR_BEGIN, 0u, op.sigma, {op.bounds[0], op.bounds[1], op.bounds[2], op.bounds[3]}};
+            // BLUR_BEGIN's batch_id word carries the blur's sampling
+            const uint32_t factor = op.batch_id & 255u, down = (op.batch_id >> 8) & 255u, up = (op.batch_id >> 16) & 255u;
+            if ((op.batch_id >> 24) != 0u || down > 1u || up > 1u || factor > TK_BLUR_MAX_FACTOR)
+                invalid("bad blur sampling");
+            Step s{STEP_BLUR_BEGIN, 0u, op.sigma, {op.bounds[0], op.bounds[1], op.bounds[2], op.bounds[3]},
+                   factor > 1u ? op.batch_id : 0u};
             c->steps.push_back(s);
             ++depth;
         } else if (op.kind == TK_OP_BLUR_END) {
@@ -608,6 +614,9 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     if (c->surfaces.size() < blur_depth) c->surfaces.resize(blur_depth);
     for (size_t i = 0; i < blur_depth; ++i) c->surfaces[i].reserve(uint64_t(c->width) * c->height);
     if (blur_depth) c->temp.reserve(uint64_t(c->width) * c->height);
+    bool reduced = false;
+    for (const Step& s : c->steps) reduced = reduced || s.sampling != 0u;
+    if (reduced) c->low.reserve(uint64_t(c->width) * c->height);
     if (c->band && blur_depth) invalid("band rendering takes scenes without blur layers (their reach crosses bands)");
     TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
     TK_CUDA(cudaGetLastError());
@@ -770,7 +779,12 @@ void do_render(tk_ctx* c) {
             int32_t sx0 = std::max(b.bounds[0] - rad, 0), sy0 = std::max(b.bounds[1] - rad, 0);
             int32_t sx1 = std::min(b.bounds[2] + rad, W), sy1 = std::min(b.bounds[3] + rad, H);
             StageMark m(c, 8);
-            if (ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
+            if (b.sampling != 0u && ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
+                // BlurSampling with factor > 1 (render/filter_program/blur.rs:194-212):
+                // reduce, blur at sigma / factor, restore, over the output bounds
+                tk::launch_blur_downsampled(surf, c->low.ptr, c->temp.ptr, c->width, c->height, ob, b.sigma,
+                                            b.sampling, st);
+            } else if (ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
                 tk::BlurParams bp{};
                 bp.width = c->width;
                 bp.height = c->height;

@@ -263,6 +263,105 @@ void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaSt
         k_blur_shared<1><<<grid, kBX * kBY, 0, st>>>(src, dst, b.width, b.height, region, bounds, wt);
 }
 
+namespace {
+
+using namespace tkd;
+
+// filter_downsample_pixel (filter/resample.hlsli): low-resolution texel (lx, ly)
+// of the rect `rect` (x0, y0, x1, y1) reduced by `factor`: the centre source
+// texel of its cell (filter 0, nearest) or the cell's byte average rounded
+// half up (filter 1, box), transparent for a cell outside the rect.
+__global__ void k_blur_downsample(const uint32_t* __restrict__ src, uint32_t* __restrict__ low, uint32_t width,
+                                  int4 rect, int4 low_rect, uint32_t factor, uint32_t filter) {
+    const uint32_t lx = uint32_t(low_rect.x) + blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ly = uint32_t(low_rect.y) + blockIdx.y;
+    if (lx >= uint32_t(low_rect.z) || ly >= uint32_t(low_rect.w)) return;
+    const uint32_t x0 = uint32_t(rect.x), y0 = uint32_t(rect.y), x1 = uint32_t(rect.z), y1 = uint32_t(rect.w);
+    const uint32_t bx = max(lx * factor, x0), by = max(ly * factor, y0);
+    const uint32_t ex = min((lx + 1u) * factor, x1), ey = min((ly + 1u) * factor, y1);
+    uint32_t out = 0u;
+    if (bx < ex && by < ey) {
+        if (filter == 0u) {
+            const uint32_t px = min(max((bx + ex - 1u) / 2u, x0), x1 - 1u);
+            const uint32_t py = min(max((by + ey - 1u) / 2u, y0), y1 - 1u);
+            out = src[uint64_t(py) * width + px];
+        } else {
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (uint32_t sy = by; sy < ey; ++sy)
+                for (uint32_t sx = bx; sx < ex; ++sx) {
+                    const uint32_t p = src[uint64_t(sy) * width + sx];
+                    sum.x += float(p & 255u);
+                    sum.y += float((p >> 8) & 255u);
+                    sum.z += float((p >> 16) & 255u);
+                    sum.w += float(p >> 24);
+                }
+            const float inv = 1.0f / float((ex - bx) * (ey - by));
+            out = pack4(f2u(clampf(mad(sum.x, inv, 0.5f), 0.0f, 255.0f)), f2u(clampf(mad(sum.y, inv, 0.5f), 0.0f, 255.0f)),
+                        f2u(clampf(mad(sum.z, inv, 0.5f), 0.0f, 255.0f)), f2u(clampf(mad(sum.w, inv, 0.5f), 0.0f, 255.0f)));
+        }
+    }
+    low[uint64_t(ly) * width + lx] = out;
+}
+
+// filter_upsample_pixel (filter/resample.hlsli): texel (x, y) of `rect` from the
+// low-resolution rect: the nearest low texel (filter 0) or the bilinear sample
+// of filter/sample.hlsli (filter 1) stored by pack_premul_rgba8.
+__global__ void k_blur_upsample(const uint32_t* __restrict__ low, uint32_t* __restrict__ dst, uint32_t width,
+                                uint32_t height, int4 rect, int4 low_rect, uint32_t factor, uint32_t filter) {
+    const uint32_t x = uint32_t(rect.x) + blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = uint32_t(rect.y) + blockIdx.y;
+    if (x >= uint32_t(rect.z) || y >= uint32_t(rect.w)) return;
+    const float f = float(max(factor, 1u));
+    const float px = clampf((float(x) + 0.5f) / f - 0.5f, float(low_rect.x), float(uint32_t(low_rect.z) - 1u));
+    const float py = clampf((float(y) + 0.5f) / f - 0.5f, float(low_rect.y), float(uint32_t(low_rect.w) - 1u));
+    uint32_t out;
+    if (filter == 0u) {
+        out = low[uint64_t(f2i(rintf(py))) * width + uint32_t(f2i(rintf(px)))];
+    } else {
+        const float4 p = sample_premul(low, width, height, px, py);
+        out = pack4(f2u(clampf(p.x, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(p.y, 0.0f, 1.0f) * 255.0f + 0.5f),
+                    f2u(clampf(p.z, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(p.w, 0.0f, 1.0f) * 255.0f + 0.5f));
+    }
+    dst[uint64_t(y) * width + x] = out;
+}
+
+}  // namespace
+
+int32_t launch_blur_downsampled(uint32_t* surface, uint32_t* low, uint32_t* temp, uint32_t width, uint32_t height,
+                                const int32_t rect[4], float sigma, uint32_t sampling, cudaStream_t st) {
+    const uint32_t factor = sampling & 255u, down = (sampling >> 8) & 255u, up = (sampling >> 16) & 255u;
+    // downsampled_bounds (render/filter_program/mod.rs:93-102): floor and ceil division
+    auto fdiv = [](int32_t v, int32_t d) { return v >= 0 ? v / d : -((-v + d - 1) / d); };
+    auto cdiv = [&](int32_t v, int32_t d) { return -fdiv(-v, d); };
+    const int32_t f = int32_t(factor);
+    const int4 r = make_int4(rect[0], rect[1], rect[2], rect[3]);
+    const int4 lr = make_int4(fdiv(r.x, f), fdiv(r.y, f), cdiv(r.z, f), cdiv(r.w, f));
+    if (r.z <= r.x || r.w <= r.y || lr.z <= lr.x || lr.w <= lr.y) return 0;
+    const uint32_t lw = uint32_t(lr.z - lr.x), lh = uint32_t(lr.w - lr.y);
+    k_blur_downsample<<<dim3((lw + 127) / 128, lh), 128, 0, st>>>(surface, low, width, r, lr, factor, down);
+    // the Gaussian at low resolution: sigma / factor, horizontal then vertical
+    // over the low rect (render/filter_program/blur.rs:31-62)
+    BlurParams b{};
+    b.width = width;
+    b.height = height;
+    b.region[0] = uint32_t(lr.x);
+    b.region[1] = uint32_t(lr.y);
+    b.region[2] = lw;
+    b.region[3] = lh;
+    b.bounds[0] = lr.x;
+    b.bounds[1] = lr.y;
+    b.bounds[2] = lr.z;
+    b.bounds[3] = lr.w;
+    b.sigma = sigma / float(factor);
+    b.axis = 0;
+    launch_blur(low, temp, b, st);
+    b.axis = 1;
+    launch_blur(temp, low, b, st);
+    const uint32_t w = uint32_t(r.z - r.x), h = uint32_t(r.w - r.y);
+    k_blur_upsample<<<dim3((w + 127) / 128, h), 128, 0, st>>>(low, surface, width, height, r, lr, factor, up);
+    return 1;
+}
+
 void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st) {
     int w = bounds[2] - bounds[0], h = bounds[3] - bounds[1];
     if (w <= 0 || h <= 0) return;

@@ -371,7 +371,8 @@ struct RecCmd {
     enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY } kind = FILL;
     tk_path path;
     tk_sdf_shape shape{};
-    // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options
+    // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options;
+    // BLUR: `sampling` is the TK_BLUR_SAMPLING word
     std::shared_ptr<const std::vector<uint32_t>> texels;
     uint32_t iw = 0, ih = 0, extend = 0, sampling = 0, opacity = 255;
     bool has_brush = false;
@@ -664,6 +665,7 @@ void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record
             Compiled::Op begin{};
             begin.op.kind = TK_OP_BLUR_BEGIN;
             begin.op.sigma = cmd.sigma;
+            begin.op.batch_id = cmd.payload;  // the blur's sampling
             begin.stack = stack;  // outer clips
             tk_pixel_bounds pb{0, 0, 0, 0};
             bool any = false;
@@ -1373,21 +1375,27 @@ int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const doubl
     }
     return 0;
 }
-int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) {
+int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sampling) {
     float physical = sigma * c->scale;
     if (!(sigma >= 0.0f) || !std::isfinite(physical)) return -1;
+    const uint32_t factor = sampling & 255u, down = (sampling >> 8) & 255u, up = (sampling >> 16) & 255u;
+    if ((sampling >> 24) != 0u || factor > TK_BLUR_MAX_FACTOR || down > TK_BLUR_DOWNSAMPLE_BOX ||
+        up > TK_BLUR_UPSAMPLE_BILINEAR)
+        return -1;
     uint32_t child = uint32_t(c->lists.size());
     c->lists.emplace_back();
-    c->lists[c->stack.back()].push_back({Cmd::BLUR, 0u, physical, child});
+    c->lists[c->stack.back()].push_back({Cmd::BLUR, 0u, physical, child, factor > 1u ? sampling : 0u});
     c->stack.push_back(child);
     c->dirty = true;
     if (c->keep) {
         RecCmd r = rec_cmd(RecCmd::BLUR, nullptr, nullptr, nullptr);
         r.sigma = sigma;
+        r.sampling = factor > 1u ? sampling : 0u;
         c->log.push_back(std::move(r));
     }
     return 0;
 }
+int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma) { return tk_canvas_push_blur_group_sampled(c, sigma, 0u); }
 int32_t tk_canvas_push_opacity_layer(tk_canvas* c, const tk_path* path, const double* transform, double tolerance,
                                      float opacity) {
     if (!c || !path || !(tolerance > 0.0) || !std::isfinite(opacity)) return -1;
@@ -1901,7 +1909,7 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
         case RecCmd::STROKE: return tk_canvas_push_stroke(dst, &r.path, bp, r.width, t, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::OPACITY: return tk_canvas_push_opacity_layer(dst, &r.path, t, r.tolerance, r.sigma);
-        case RecCmd::BLUR: return tk_canvas_push_blur_group(dst, r.sigma);
+        case RecCmd::BLUR: return tk_canvas_push_blur_group_sampled(dst, r.sigma, r.sampling);
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
         case RecCmd::SDF:
         case RecCmd::SDF_CLIP: {

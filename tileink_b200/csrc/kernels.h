@@ -194,6 +194,14 @@ struct BlurParams {
 };
 void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaStream_t st);
 void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st);
+// The blur of `surface` inside `rect` (x0, y0, x1, y1) through a reduced copy
+// (BlurSampling with factor > 1, filter/resample.hlsli): downsample into
+// `low`, blur there at sigma / factor (`temp` holds the horizontal pass),
+// upsample back into `surface` over `rect`. `sampling` = factor | downsample
+// filter << 8 | upsample filter << 16 (TK_BLUR_SAMPLING_*). All three buffers
+// are width x height. Returns 0 when the rect is empty.
+int32_t launch_blur_downsampled(uint32_t* surface, uint32_t* low, uint32_t* temp, uint32_t width, uint32_t height,
+                                const int32_t rect[4], float sigma, uint32_t sampling, cudaStream_t st);
 
 
 // Device flattening (flatten.cu): per-element line counts, exclusive offsets
