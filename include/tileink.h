@@ -370,6 +370,22 @@ int32_t tk_synchronize(tk_ctx* ctx);
  * Host records are copied; the caller may free them after the call. */
 int32_t tk_scene_upload(tk_ctx* ctx, const tk_scene_desc* scene);
 
+/* Upload a scene that replaces the context's current one path for path,
+ * keeping the current scan for every path that did not change (the
+ * reference's selective rescan of its scan history,
+ * src/native/runtime/program/scene_scan.rs:116-192). `changed` lists the
+ * paths whose lines differ from the last upload (the caller's journal; their
+ * lines are uploaded, the others' stay on the device); the library adds
+ * every path whose record changed. The next render rescans only those paths
+ * (their slices cleared, counted, prefixed and emitted), which gives the
+ * scan of the whole new scene. It applies when the current scene was
+ * scanned, uses host segment plans, and the new one has the same path and
+ * line counts and keeps the backdrop pool and segment layout; otherwise the
+ * scene is uploaded whole and scanned in full. `*rescan_paths` (may be null)
+ * receives the number of paths the next render scans. */
+int32_t tk_scene_upload_delta(tk_ctx* ctx, const tk_scene_desc* scene, const uint32_t* changed,
+                              uint32_t changed_count, uint32_t* rescan_paths);
+
 /* Enqueue the whole frame on the context stream: scan (count, prefix,
  * cumsum, emit), tile binning, and per target pass coarse + fine, with blur
  * layers (replaces frame::record, native/runtime/renderer/frame.rs:6-80). */
@@ -579,6 +595,7 @@ typedef struct tk_incremental_stats {
     uint32_t full_redraw;   /* 1 when every tile was redrawn */
     uint32_t reason;        /* TK_FULL_* */
     uint32_t scan_reused;   /* 1 when the uploaded scene's last scan served the frame */
+    uint32_t scanned_paths; /* paths scanned for the frame (all, those a delta upload replaced, or 0) */
 } tk_incremental_stats;
 
 /* Renders the uploaded scene, redrawing only the tiles that meet `damage`

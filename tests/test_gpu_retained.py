@@ -146,3 +146,97 @@ def test_gpu_incremental_frames_reuse_the_unchanged_scan(renderer, reference_ren
     st = renderer.render_incremental({"full": False, "rects": [[10, 10, 50, 50]]})
     assert st["full_redraw"] == 0 and st["scan_reused"] == 0
     assert np.array_equal(renderer.readback().view(np.uint8).reshape(H, W, 4), want)
+
+
+def jittered_paths(arrays, candidates, dx):
+    """A copy of the scene arrays with the lines of some candidate paths moved
+    by dx, keeping their records: only paths whose every line keeps its
+    planned tile count (and so its segment slice) are moved."""
+    b = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in arrays.items()}
+    moved = []
+    for p in candidates:
+        rec = b["paths"][p]
+        s, n = int(rec["line_start"]), int(rec["line_count"])
+        bbox = (int(rec["tile_x0"]), int(rec["tile_y0"]), int(rec["tile_x1"]), int(rec["tile_y1"]))
+        new = b["lines"][s:s + n].copy()
+        new["p0"][:, 0] += dx
+        new["p1"][:, 0] += dx
+        if all(tk.plan_line_tile_count(new[i], bbox) == tk.plan_line_tile_count(b["lines"][s + i], bbox)
+               for i in range(n)):
+            b["lines"][s:s + n] = new
+            moved.append(p)
+    return b, moved
+
+
+def test_gpu_delta_upload_rescans_only_changed_paths(renderer, reference_renderer):
+    """tk_scene_upload_delta: the paths whose lines changed are scanned again
+    and the others keep their scan; the frame equals a full upload and
+    render of the new scene, stage by stage."""
+    c = tk.generate(2, 13, width=W, height=H, paths=200)
+    a = c.scene_arrays()
+    renderer.upload(c)
+    renderer.render()
+    b, moved = jittered_paths(a, range(0, 200, 17), 0.03125)
+    assert len(moved) >= 3
+    scene = N.ArrayScene(b)
+    assert renderer.upload_delta(scene, moved) == len(moved)
+    renderer.render()
+    img = renderer.readback().copy()
+    segs = renderer.debug(N.STAGE_SEGMENTS).copy()
+    ptcl = renderer.debug(N.STAGE_PTCL).copy()
+    want = reference_renderer.render_to_image(N.ArrayScene(b))
+    assert np.array_equal(img.view(np.uint8).reshape(want.shape), want)
+    assert segs.tobytes() == reference_renderer.debug(N.STAGE_SEGMENTS).tobytes()
+    assert np.array_equal(ptcl, reference_renderer.debug(N.STAGE_PTCL))
+    # an incremental frame after a delta scans just the replaced paths
+    b2, moved2 = jittered_paths(b, moved[:2], -0.0625)
+    assert renderer.upload_delta(N.ArrayScene(b2), moved2) == len(moved2)
+    st = renderer.render_incremental({"full": False, "rects": [[0, 0, W, 64]]})
+    assert st["full_redraw"] == 0 and st["scanned_paths"] == len(moved2) and st["scan_reused"] == 0
+    st = renderer.render_incremental({"full": True})
+    want2 = reference_renderer.render_to_image(N.ArrayScene(b2))
+    assert np.array_equal(renderer.readback().view(np.uint8).reshape(want2.shape), want2)
+
+
+def test_gpu_delta_upload_falls_back_when_the_layout_changes(renderer, reference_renderer):
+    c = tk.generate(2, 14, width=W, height=H, paths=120)
+    renderer.upload(c)
+    renderer.render()
+    other = tk.generate(2, 15, width=W, height=H, paths=121)  # other counts: a whole upload
+    assert renderer.upload_delta(other, []) == other.scene_arrays()["paths"].shape[0]
+    renderer.render()
+    want = reference_renderer.render_to_image(other)
+    assert np.array_equal(renderer.readback().view(np.uint8).reshape(want.shape), want)
+
+
+def test_gpu_retained_recolor_keeps_the_whole_scan(renderer, reference_renderer):
+    """A node replaced by the same geometry in another colour changes no
+    line and no path record: the frame reuses the whole scan."""
+    rs = tk.RetainedScene(W, H)
+    rs.set_clear_color(0xFFFFFFFF)
+    for k in range(6):
+        rs.insert(k + 1, big_node(300 + k, 6))
+    incremental_image(renderer, rs)
+    recolored = tk.Canvas(W, H)
+    recolored.keep_commands()
+    src = big_node(302, 6)
+    rng = np.random.default_rng(302)
+    for k in range(6):
+        cx, cy = rng.uniform(20, W - 20), rng.uniform(20, H - 20)
+        p = tk.BezPath()
+        p.move_to(cx, cy)
+        for _ in range(3):
+            p.cubic_to(*(rng.uniform(-40, 40, 6) + np.tile([cx, cy], 3)))
+        p.close()
+        rng.uniform(0, 1, 3), rng.uniform(0.4, 1.0)  # the original colour draws
+        b = tk.Brush.solid(0.1 * k, 0.5, 0.9, 0.7)
+        if k % 3 == 2:
+            recolored.push_stroke(p, b, float(rng.uniform(0.5, 5.0)))
+        else:
+            recolored.push_path(p, b, fill_rule=k % 2)
+    del src
+    rs.replace(3, recolored)
+    img, st = incremental_image(renderer, rs)
+    assert st["full_redraw"] == 0
+    assert st.get("rescan_paths") == 0 and st["scan_reused"] == 1 and st["scanned_paths"] == 0, st
+    assert np.array_equal(img, full_image(reference_renderer, rs.materialize()[0]))

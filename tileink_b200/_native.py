@@ -179,7 +179,7 @@ class Damage(C.Structure):
 class IncrementalStats(C.Structure):
     """tk_incremental_stats (include/tileink.h)."""
     _fields_ = [("total_tiles", C.c_uint32), ("dirty_tiles", C.c_uint32), ("full_redraw", C.c_uint32),
-                ("reason", C.c_uint32), ("scan_reused", C.c_uint32)]
+                ("reason", C.c_uint32), ("scan_reused", C.c_uint32), ("scanned_paths", C.c_uint32)]
 
 
 class AbiField(C.Structure):
@@ -240,6 +240,7 @@ def library() -> C.CDLL:
         "tk_stage_tile_prefix": (I32, [P, P, U32, U32, U32, C.POINTER(U32)]),
         "tk_debug_readback_range": (I32, [P, U32, U32, U64, U64, P, C.POINTER(U64)]),
         "tk_set_band": (I32, [P, U32, U32]),
+        "tk_scene_upload_delta": (I32, [P, C.POINTER(SceneDesc), P, U32, C.POINTER(U32)]),
         "tk_band_paths": (None, [P, U32, U32, U32, P]),
         "tk_readback_rows": (I32, [P, U32, U32, P, C.c_size_t]),
         "tk_stage_scan_count": (I32, [P, P, U64, P, U32, P, P, U64]),

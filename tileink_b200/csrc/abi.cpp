@@ -82,7 +82,7 @@ const tk_abi_field kLayout[] = {
     S(tk_incremental_stats),
     F(tk_incremental_stats, total_tiles), F(tk_incremental_stats, dirty_tiles),
     F(tk_incremental_stats, full_redraw), F(tk_incremental_stats, reason),
-    F(tk_incremental_stats, scan_reused),
+    F(tk_incremental_stats, scan_reused), F(tk_incremental_stats, scanned_paths),
     S(tk_batch_info),
     F(tk_batch_info, width), F(tk_batch_info, height), F(tk_batch_info, tile_base), F(tk_batch_info, tile_count),
     F(tk_batch_info, path_base), F(tk_batch_info, draw_base), F(tk_batch_info, batch_base),

@@ -195,8 +195,14 @@ struct tk_ctx {
     uint32_t band_y0 = 0, band_y1 = 0;
     std::vector<tk_path_record> band_paths;
     // the scan buffers hold the scan of the uploaded scene (nothing has
-    // been uploaded or scanned into them since)
+    // been uploaded or scanned into them since), except for the paths in
+    // `rescan`, whose records or lines a delta upload replaced
     bool scan_valid = false;
+    std::vector<uint32_t> rescan;
+    DBuf<uint32_t> rescan_list;
+    DBuf<tk::ScanItem> rescan_items;
+    DBuf<unsigned long long> rescan_desc;
+    uint32_t last_scan_paths = 0;  // paths the last scan covered
 };
 
 namespace {
@@ -535,7 +541,10 @@ tk_scene_desc band_scene(tk_ctx* c, const tk_scene_desc& d) {
     return b;
 }
 
-void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl = nullptr) {
+// line_dirty (a delta upload): per path, whether its lines are uploaded; the
+// other paths' lines are already on the device at the same positions.
+void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl = nullptr,
+               const std::vector<uint8_t>* line_dirty = nullptr) {
     if (c->band) {
         const uint32_t th = (scene.height + TK_TILE_SIZE - 1) / TK_TILE_SIZE;
         if (c->band_y1 > th) invalid("band rows beyond the canvas");
@@ -553,8 +562,23 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     validate_and_plan(c, d);
     cudaStream_t st = c->stream;
     upload(c->paths, d.paths, d.path_count, st);
-    if (fl) flatten_on_device(c, d, *fl);  // the host lines, then the device lines
-    else upload(c->lines, d.lines, d.line_count, st);
+    if (fl) {
+        flatten_on_device(c, d, *fl);  // the host lines, then the device lines
+    } else if (line_dirty) {  // the changed paths' line ranges, runs coalesced
+        c->lines.reserve(d.line_count);
+        for (uint32_t p = 0; p < d.path_count;) {
+            if (!(*line_dirty)[p]) { ++p; continue; }
+            uint32_t q = p;
+            while (q < d.path_count && (*line_dirty)[q]) ++q;
+            const uint64_t a = d.paths[p].line_start, b = uint64_t(d.paths[q - 1].line_start) + d.paths[q - 1].line_count;
+            if (b > a)
+                TK_CUDA(cudaMemcpyAsync(c->lines.ptr + a, d.lines + a, (b - a) * sizeof(tk_line),
+                                        cudaMemcpyHostToDevice, st));
+            p = q;
+        }
+    } else {
+        upload(c->lines, d.lines, d.line_count, st);
+    }
     upload(c->draws, d.draws, d.draw_count, st);
     upload(c->brush, d.brush_blob, d.brush_word_count, st);
     c->sdf.reserve(c->sdf_words);
@@ -704,9 +728,58 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
     }
 }
 
-// Pool clear, scan_count, pool scan, path totals and scan_emit.
+// The scan of the paths a delta upload replaced (scene_scan.rs:116-192's
+// selected paths): their slices cleared and counted, their pool scan items,
+// their segments emitted; every other path's scan output stays as it is.
+void scan_phase_partial(tk_ctx* c) {
+    cudaStream_t st = c->stream;
+    tk::SceneView s = view(c);
+    c->ev_used = 0;
+    c->marks.clear();
+    c->scan_valid = false;
+    const uint32_t n = uint32_t(c->rescan.size());
+    upload(c->rescan_list, c->rescan.data(), n, st);
+    std::vector<uint8_t> sel(c->path_count, 0u);
+    for (uint32_t p : c->rescan) sel[p] = 1u;
+    std::vector<tk::ScanItem> items;
+    for (const tk::ScanItem& it : c->h_items)
+        if (sel[it.path]) items.push_back(it);
+    upload(c->rescan_items, items.data(), items.size(), st);
+    c->rescan_desc.reserve(std::max<size_t>(items.size(), 1));
+    {
+        StageMark m(c, 0);
+        TK_CUDA(cudaMemsetAsync(c->stats.ptr, 0, 4 * sizeof(unsigned long long), st));
+    }
+    {
+        StageMark m(c, 1);
+        tk::launch_scan_count_paths(s, c->rescan_list.ptr, n, st);
+    }
+    {
+        StageMark m(c, 2);
+        tk::launch_pool_scan(s, c->rescan_items.ptr, uint32_t(items.size()), c->rescan_desc.ptr, false, 0u,
+                             c->misc.ptr + 2, st);
+        tk::launch_path_totals(s, c->bumps.ptr, false, c->misc.ptr + 2, st);
+    }
+    s.segment_capacity = c->host_segment_capacity;
+    {
+        StageMark m(c, 3);
+        tk::launch_scan_emit_paths(s, c->rescan_list.ptr, n, st);
+    }
+    c->last_scan_paths = n;
+    c->rescan.clear();
+    c->scan_valid = true;
+}
+
+// Pool clear, scan_count, pool scan, path totals and scan_emit; only the
+// paths a delta upload replaced when the rest of the scan is in place.
 void scan_phase(tk_ctx* c) {
     if (!c->have_scene) throw Fail{TK_E_STATE, "no scene uploaded"};
+    if (c->scan_valid && !c->rescan.empty()) {
+        scan_phase_partial(c);
+        return;
+    }
+    c->rescan.clear();
+    c->last_scan_paths = c->path_count;
     c->scan_valid = false;
     cudaStream_t st = c->stream;
     bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
@@ -818,7 +891,7 @@ void do_render(tk_ctx* c) {
 // per batch group straight into the image).
 void do_render_tiles(tk_ctx* c, bool reuse_scan = false) {
     c->history = false;
-    if (reuse_scan && c->scan_valid) {  // the uploaded scene's scan is still in place
+    if (reuse_scan && c->scan_valid && c->rescan.empty()) {  // the uploaded scene's scan is still in place
         c->ev_used = 0;
         c->marks.clear();
     } else {
@@ -1310,6 +1383,47 @@ int32_t tk_scene_upload(tk_ctx* c, const tk_scene_desc* d) {
     return guarded(c, [&] { do_upload(c, *d); });
 }
 
+int32_t tk_scene_upload_delta(tk_ctx* c, const tk_scene_desc* d, const uint32_t* changed, uint32_t changed_count,
+                              uint32_t* rescan_paths) {
+    if (!d) return fail(c, Fail{TK_E_INVALID, "null scene"});
+    return guarded(c, [&] {
+        if (changed_count && !changed) invalid("null changed-path list");
+        const bool device_plan = (c->flags | d->flags) & TK_SCENE_SEGMENTS_FROM_DEVICE;
+        const bool can = c->have_scene && !c->batched && !c->band && c->scan_valid && !c->want_seg_line &&
+                         !device_plan && d->path_count == c->path_count && d->line_count == c->line_count &&
+                         d->path_count && d->paths;
+        if (!can) {  // no scan to keep: a whole upload
+            do_upload(c, *d);
+            if (rescan_paths) *rescan_paths = d->path_count;
+            return;
+        }
+        // The paths to rescan: the caller's (lines changed), the ones whose
+        // records changed, and any still pending from an earlier delta.
+        const std::vector<tk_path_record> old = c->h_paths;
+        const uint64_t old_pool = c->pool_len, old_cap = c->host_segment_capacity;
+        std::vector<uint8_t> dirty(d->path_count, 0u);
+        for (uint32_t k = 0; k < changed_count; ++k) {
+            if (changed[k] >= d->path_count) invalid("changed path index out of range");
+            dirty[changed[k]] = 1u;
+        }
+        for (uint32_t p : c->rescan) dirty[p] = 1u;
+        for (uint32_t p = 0; p < d->path_count; ++p)
+            if (std::memcmp(&old[p], &d->paths[p], sizeof(tk_path_record)) != 0) dirty[p] = 1u;
+        do_upload(c, *d, nullptr, &dirty);
+        // the kept scan is valid only over the same pool and segment layout;
+        // otherwise the next render scans everything
+        c->rescan.clear();
+        if (c->pool_len != old_pool || c->host_segment_capacity != old_cap) {
+            if (rescan_paths) *rescan_paths = d->path_count;
+            return;
+        }
+        for (uint32_t p = 0; p < d->path_count; ++p)
+            if (dirty[p]) c->rescan.push_back(p);
+        c->scan_valid = true;
+        if (rescan_paths) *rescan_paths = uint32_t(c->rescan.size());
+    });
+}
+
 int32_t tk_render(tk_ctx* c) {
     return guarded(c, [&] {
         if (c->batched) do_batch_render(c);
@@ -1404,6 +1518,7 @@ int32_t tk_render_incremental(tk_ctx* c, const tk_damage* damage, float full_red
             if (double(c->h_active_list.size()) >= double(full_redraw_ratio) * double(T)) reason = TK_FULL_THRESHOLD;
         }
         if (reason != TK_FULL_NONE) {
+            c->last_scan_paths = 0;
             do_render(c);
             out.dirty_tiles = T;
             out.full_redraw = 1u;
@@ -1412,10 +1527,12 @@ int32_t tk_render_incremental(tk_ctx* c, const tk_damage* damage, float full_red
             // The uploaded scene's scan is reused when nothing was uploaded or
             // scanned since it (the reference reuses an unchanged scene's scan
             // history, src/native/runtime/program/scene_scan.rs:116-125).
-            out.scan_reused = c->scan_valid ? 1u : 0u;
+            out.scan_reused = c->scan_valid && c->rescan.empty() ? 1u : 0u;
+            c->last_scan_paths = 0;
             if (out.dirty_tiles) do_render_tiles(c, true);
             else c->rendered = true;  // nothing changed: the image is the frame
         }
+        out.scanned_paths = c->last_scan_paths;
         out.reason = reason;
         if (stats) *stats = out;
     });

@@ -101,6 +101,11 @@ void launch_pool_scan(const SceneView& s, const ScanItem* items, uint32_t n_item
 void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, const uint32_t* total,
                         cudaStream_t st);
 void launch_scan_emit(const SceneView& s, cudaStream_t st);
+// The scan of the listed paths only (n entries of `list`, device memory):
+// clear their backdrop and count slices and count their lines; emit their
+// segments. Their pool scan runs through launch_pool_scan with their items.
+void launch_scan_count_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st);
+void launch_scan_emit_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st);
 
 // Fixed scratch of the allocation-free pool scan (one array per device).
 struct NoAllocScratch {

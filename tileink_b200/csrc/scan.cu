@@ -46,6 +46,37 @@ __device__ __forceinline__ tk_path_record load_path(const tk_path_record* paths,
     return p;
 }
 
+// scan/count.hlsl:13-40 for one line: backdrop deltas and tile counts.
+__device__ __forceinline__ void count_line(const tk_line& line, const tk_path_record* __restrict__ paths,
+                                           int32_t* backdrops, uint32_t* counts) {
+    tk_path_record p = load_path(paths, line.path_id);
+    Scan s;
+    if (!scan_geometry(line, p, s)) return;
+    int32_t delta = s.down ? -1 : 1;
+    int32_t stride = int32_t(s.bx1 - s.bx0);
+    for (int32_t y = s.ymin; y < s.ymax; ++y) {
+        uint32_t local = uint32_t((y - int32_t(s.by0)) * stride);
+        atomicAdd(backdrops + s.data_offset + local, delta);
+    }
+    float last_z = floorf(s.a * (float(s.imin) - 1.0f) + s.b);
+    for (uint32_t i = s.imin; i < s.imax; ++i) {
+        float z = floorf(s.a * float(i) + s.b);
+        int32_t tx, ty;
+        scan_tile(s, i, z, tx, ty);
+        if (scan_tile_inside(s, tx, ty)) {
+            bool top = last_z == z;
+            if (i == 0u) top = fabsf(s.y0 - s.qy0 * (1.0f / float(TK_TILE_SIZE))) <= SCAN_EPSILON;
+            if (top && tx + 1 < int32_t(s.bx1)) {
+                int32_t x = max(tx + 1, int32_t(s.bx0));
+                uint32_t local = uint32_t((ty - int32_t(s.by0)) * stride + x - int32_t(s.bx0));
+                atomicAdd(backdrops + s.data_offset + local, delta);
+            }
+            atomicAdd(counts + scan_tile_offset(s, tx, ty), 1u);
+        }
+        last_z = z;
+    }
+}
+
 __global__ void k_scan_count(const tk_line* __restrict__ lines, uint64_t line_count,
                              const tk_path_record* __restrict__ paths, uint32_t path_count, int32_t* backdrops,
                              uint32_t* counts) {
@@ -53,32 +84,26 @@ __global__ void k_scan_count(const tk_line* __restrict__ lines, uint64_t line_co
          li += uint64_t(gridDim.x) * blockDim.x) {
         tk_line line = load_line(lines, li);
         if (line.path_id >= path_count) continue;
-        tk_path_record p = load_path(paths, line.path_id);
-        Scan s;
-        if (!scan_geometry(line, p, s)) continue;
-        int32_t delta = s.down ? -1 : 1;
-        int32_t stride = int32_t(s.bx1 - s.bx0);
-        for (int32_t y = s.ymin; y < s.ymax; ++y) {
-            uint32_t local = uint32_t((y - int32_t(s.by0)) * stride);
-            atomicAdd(backdrops + s.data_offset + local, delta);
-        }
-        float last_z = floorf(s.a * (float(s.imin) - 1.0f) + s.b);
-        for (uint32_t i = s.imin; i < s.imax; ++i) {
-            float z = floorf(s.a * float(i) + s.b);
-            int32_t tx, ty;
-            scan_tile(s, i, z, tx, ty);
-            if (scan_tile_inside(s, tx, ty)) {
-                bool top = last_z == z;
-                if (i == 0u) top = fabsf(s.y0 - s.qy0 * (1.0f / float(TK_TILE_SIZE))) <= SCAN_EPSILON;
-                if (top && tx + 1 < int32_t(s.bx1)) {
-                    int32_t x = max(tx + 1, int32_t(s.bx0));
-                    uint32_t local = uint32_t((ty - int32_t(s.by0)) * stride + x - int32_t(s.bx0));
-                    atomicAdd(backdrops + s.data_offset + local, delta);
-                }
-                atomicAdd(counts + scan_tile_offset(s, tx, ty), 1u);
-            }
-            last_z = z;
-        }
+        count_line(line, paths, backdrops, counts);
+    }
+}
+
+// The selected paths only (a partial rescan): one CTA per listed path clears
+// its backdrop and count slices, then counts its lines.
+__global__ void k_scan_count_paths(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
+                                   uint32_t path_count, const uint32_t* __restrict__ list, int32_t* backdrops,
+                                   uint32_t* counts) {
+    const uint32_t pid = list[blockIdx.x];
+    const tk_path_record p = load_path(paths, pid);
+    for (uint32_t k = threadIdx.x; k < p.data_len; k += blockDim.x) {
+        backdrops[p.data_offset + k] = 0;
+        counts[p.data_offset + k] = 0u;
+    }
+    __syncthreads();
+    for (uint32_t l = threadIdx.x; l < p.line_count; l += blockDim.x) {
+        tk_line line = load_line(lines, uint64_t(p.line_start) + l);
+        if (line.path_id != pid || pid >= path_count) continue;  // the emit pass reports mismatches
+        count_line(line, paths, backdrops, counts);
     }
 }
 
@@ -436,6 +461,19 @@ void launch_path_totals(const SceneView& s, uint32_t* bumps, bool device_plan, c
     if (s.path_count == 0) return;
     k_path_totals<<<(s.path_count + 255) / 256, 256, 0, st>>>(s.paths, s.path_count, s.ranges, s.pool_len, bumps,
                                                              device_plan ? 1 : 0, total);
+}
+
+void launch_scan_count_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st) {
+    if (n == 0) return;
+    k_scan_count_paths<<<n, 256, 0, st>>>(s.lines, s.paths, s.path_count, list, s.backdrops, s.counts);
+}
+
+void launch_scan_emit_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st) {
+    if (n == 0) return;
+    cudaMemsetAsync(s.emit_ticket, 0, sizeof(uint32_t), st);
+    k_scan_emit<<<grid_for(uint64_t(n) * 32, 256, 148 * 8), 256, 0, st>>>(s.lines, s.paths, n, s.cursors, s.segments,
+                                                                        s.segment_capacity, s.error, s.seg_line, list,
+                                                                        s.emit_ticket);
 }
 
 void launch_scan_emit(const SceneView& s, cudaStream_t st) {

@@ -78,10 +78,30 @@ class NativeRenderer:
 
     def render_retained(self, scene, full_redraw_ratio: float = 0.7) -> dict:
         """NativeRenderer::render_retained (src/native/renderer/retained.rs:17-23):
-        materializes the retained scene, uploads it and redraws its damage."""
+        materializes the retained scene, uploads it and redraws its damage.
+        A materialization with the same path and line counts as the last one
+        goes through tk_scene_upload_delta with the paths whose lines changed,
+        so only they (and paths whose records changed) are scanned again."""
         canvas, damage = scene.materialize()
-        self.upload(canvas)
-        return self.render_incremental(damage, full_redraw_ratio)
+        prev = getattr(self, "_retained_lines", None)
+        stats_extra = {}
+        if canvas.flatten_desc() is None:
+            a = canvas.scene_arrays()
+            lines = a["lines"]
+            if prev is not None and len(prev) == len(lines) and len(prev):
+                differs = (prev.view(np.uint8).reshape(-1, N.LINE_DTYPE.itemsize) !=
+                           lines.view(np.uint8).reshape(-1, N.LINE_DTYPE.itemsize)).any(axis=1)
+                changed = np.unique(lines["path_id"][differs])
+                stats_extra["rescan_paths"] = self.upload_delta(canvas, changed)
+            else:
+                self.upload(canvas)
+            self._retained_lines = lines.copy()
+        else:
+            self._retained_lines = None
+            self.upload(canvas)
+        st = self.render_incremental(damage, full_redraw_ratio)
+        st.update(stats_extra)
+        return st
 
     def synchronize(self) -> None:
         self._check(self._lib.tk_synchronize(self._h))
@@ -126,6 +146,19 @@ class NativeRenderer:
         out = np.zeros(need.value // np.dtype(dt).itemsize, dtype=dt)
         self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
         return out
+
+    def upload_delta(self, scene, changed_paths=()) -> int:
+        """tk_scene_upload_delta: replace the uploaded scene, keeping the scan
+        of every path whose record and lines (`changed_paths` lists the
+        paths whose lines changed) are unchanged. Returns how many paths the
+        next render scans."""
+        d = scene.scene_desc() if hasattr(scene, "scene_desc") else scene.desc
+        ch = np.ascontiguousarray(np.asarray(list(changed_paths), dtype=np.uint32))
+        n = C.c_uint32(0)
+        self._check(self._lib.tk_scene_upload_delta(self._h, C.byref(d), N.ptr(ch) if len(ch) else None, len(ch),
+                                                    C.byref(n)))
+        self.width, self.height = d.width, d.height
+        return n.value
 
     def set_band(self, tile_y0: int, tile_y1: int) -> None:
         """Render tile rows [tile_y0, tile_y1) from the next upload on
