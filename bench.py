@@ -308,9 +308,10 @@ def batch_timing(n_scenes, steps):
 def incremental_timing(r, size, steps):
     """Incremental frames of the resident scene (tk_render_incremental, the
     retained path's damage-driven redraw): each frame a 256x256-pixel damage
-    rectangle at a new place, the scene scanned in full and coarse + fine run
-    on the damaged tiles only over the previous frame; against full frames of
-    the same scene. Host wall clock per frame, synchronized."""
+    rectangle at a new place, the scene's scan reused (nothing was uploaded
+    since) and coarse + fine run on the damaged tiles only over the previous
+    frame; against full frames of the same scene (scan included). Host wall
+    clock per frame, synchronized."""
     side = 256
     W = size or 4096
     r.render_incremental(None)  # the history frame
@@ -331,6 +332,39 @@ def incremental_timing(r, size, steps):
             "incremental_ms": inc_ms, "full_ms": full_ms, "speedup": full_ms / inc_ms,
             "dirty_tiles": st["dirty_tiles"], "total_tiles": st["total_tiles"], "steps": steps,
             "timing": "host wall clock per frame, synchronized"}
+
+
+def delta_timing(r, canvas, steps, k=8):
+    """Delta frames (tk_scene_upload_delta + tk_render_incremental, the
+    retained path after an edit): each frame the scene is uploaded again
+    with k paths listed as changed (their lines re-uploaded), only
+    those paths are scanned again (counted, prefixed, emitted into the slices
+    the device plan gave them) and their tiles redrawn. Host wall clock per
+    frame from the upload call to the synchronized render."""
+    a = canvas.scene_arrays()
+    paths = a["paths"]
+    cut = np.percentile(paths["data_len"], 2)  # the smallest 2% of the paths' bboxes
+    small = np.nonzero((paths["data_len"] > 0) & (paths["data_len"] <= cut))[0]
+    k = min(k, len(small))
+    rng = np.random.default_rng(5)
+    r.upload(canvas)
+    r.render_incremental(None)
+    r.synchronize()
+    times, st, n = [], None, 0
+    for _ in range(steps):
+        pick = np.sort(rng.choice(small, k, replace=False)).astype(np.uint32)
+        rects = [[int(paths["tile_x0"][p]) * 16, int(paths["tile_y0"][p]) * 16, int(paths["tile_x1"][p]) * 16,
+                  int(paths["tile_y1"][p]) * 16] for p in pick]
+        t0 = time.perf_counter()
+        n = r.upload_delta(canvas, pick)
+        st = r.render_incremental({"full": False, "rects": rects})
+        r.synchronize()
+        times.append((time.perf_counter() - t0) * 1e3)
+    return {"workload": f"the frame's scene uploaded again with {k} paths (among the 2% with the smallest bboxes, "
+                        f"<= {int(cut)} tiles) listed as changed each frame; their bbox tiles redrawn",
+            "delta_ms": float(np.median(times)), "rescan_paths": int(n), "scanned_paths": int(st["scanned_paths"]),
+            "dirty_tiles": int(st["dirty_tiles"]), "scan_reused": int(st["scan_reused"]), "steps": steps,
+            "timing": "host wall clock per frame (upload call to synchronized render), median"}
 
 
 def sdf_scene(size, n, seed, kinds="base"):
@@ -813,6 +847,7 @@ def main():
     inc_line = None
     if rank == 0 and world == 1 and args.incremental_steps > 0:
         inc_line = incremental_timing(r, args.size, args.incremental_steps)
+        inc_line["delta"] = delta_timing(r, canvas, args.incremental_steps)
     sdf_line = None
     if rank == 0 and world == 1 and args.sdf_steps > 0:
         sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline, args.sdf_shapes)

@@ -379,10 +379,15 @@ int32_t tk_scene_upload(tk_ctx* ctx, const tk_scene_desc* scene);
  * every path whose record changed. The next render rescans only those paths
  * (their slices cleared, counted, prefixed and emitted), which gives the
  * scan of the whole new scene. It applies when the current scene was
- * scanned, uses host segment plans, and the new one has the same path and
- * line counts and keeps the backdrop pool and segment layout; otherwise the
- * scene is uploaded whole and scanned in full. `*rescan_paths` (may be null)
- * receives the number of paths the next render scans. */
+ * scanned, the new one has the same path and line counts, the same kind of
+ * segment plan, and keeps the backdrop pool (and, with host plans, the
+ * segment layout); otherwise the scene is uploaded whole and scanned in
+ * full. With device segment plans (TK_SCENE_SEGMENTS_FROM_DEVICE) every path
+ * keeps the segment slice the last scan planned; the next render counts the
+ * replaced paths and, if any of their segment totals changed (which moves
+ * every later slice), scans the whole scene instead. `*rescan_paths` (may be
+ * null) receives the number of paths the next render scans (with device
+ * plans: unless that check finds a changed total). */
 int32_t tk_scene_upload_delta(tk_ctx* ctx, const tk_scene_desc* scene, const uint32_t* changed,
                               uint32_t changed_count, uint32_t* rescan_paths);
 

@@ -168,34 +168,73 @@ def jittered_paths(arrays, candidates, dx):
     return b, moved
 
 
-def test_gpu_delta_upload_rescans_only_changed_paths(renderer, reference_renderer):
+def array_scene(arrays, device_plan):
+    scene = N.ArrayScene(arrays)
+    if device_plan:
+        scene.desc.flags |= N.SCENE_SEGMENTS_FROM_DEVICE
+    return scene
+
+
+def same_scan_and_frame(renderer, reference_renderer, scene):
+    """The renderer's last frame equals a full upload and render of `scene`
+    in another context: image, segments, PTCL and path records."""
+    img = renderer.readback().copy()
+    segs = renderer.debug(N.STAGE_SEGMENTS).copy()
+    ptcl = renderer.debug(N.STAGE_PTCL).copy()
+    paths = renderer.debug(N.STAGE_PATHS).copy()
+    want = reference_renderer.render_to_image(scene)
+    assert np.array_equal(img.view(np.uint8).reshape(want.shape), want)
+    assert segs.tobytes() == reference_renderer.debug(N.STAGE_SEGMENTS).tobytes()
+    assert np.array_equal(ptcl, reference_renderer.debug(N.STAGE_PTCL))
+    assert paths.tobytes() == reference_renderer.debug(N.STAGE_PATHS).tobytes()
+
+
+@pytest.mark.parametrize("device_plan", [False, True])
+def test_gpu_delta_upload_rescans_only_changed_paths(renderer, reference_renderer, device_plan):
     """tk_scene_upload_delta: the paths whose lines changed are scanned again
     and the others keep their scan; the frame equals a full upload and
-    render of the new scene, stage by stage."""
-    c = tk.generate(2, 13, width=W, height=H, paths=200)
+    render of the new scene, stage by stage, with host segment plans and with
+    device plans (each path keeps the slice the last scan planned)."""
+    c = tk.generate(2, 13, width=W, height=H, paths=200, device_segment_plan=device_plan)
     a = c.scene_arrays()
     renderer.upload(c)
     renderer.render()
     b, moved = jittered_paths(a, range(0, 200, 17), 0.03125)
     assert len(moved) >= 3
-    scene = N.ArrayScene(b)
-    assert renderer.upload_delta(scene, moved) == len(moved)
+    assert renderer.upload_delta(array_scene(b, device_plan), moved) == len(moved)
     renderer.render()
-    img = renderer.readback().copy()
-    segs = renderer.debug(N.STAGE_SEGMENTS).copy()
-    ptcl = renderer.debug(N.STAGE_PTCL).copy()
-    want = reference_renderer.render_to_image(N.ArrayScene(b))
-    assert np.array_equal(img.view(np.uint8).reshape(want.shape), want)
-    assert segs.tobytes() == reference_renderer.debug(N.STAGE_SEGMENTS).tobytes()
-    assert np.array_equal(ptcl, reference_renderer.debug(N.STAGE_PTCL))
+    same_scan_and_frame(renderer, reference_renderer, array_scene(b, device_plan))
     # an incremental frame after a delta scans just the replaced paths
     b2, moved2 = jittered_paths(b, moved[:2], -0.0625)
-    assert renderer.upload_delta(N.ArrayScene(b2), moved2) == len(moved2)
+    assert renderer.upload_delta(array_scene(b2, device_plan), moved2) == len(moved2)
     st = renderer.render_incremental({"full": False, "rects": [[0, 0, W, 64]]})
     assert st["full_redraw"] == 0 and st["scanned_paths"] == len(moved2) and st["scan_reused"] == 0
     st = renderer.render_incremental({"full": True})
-    want2 = reference_renderer.render_to_image(N.ArrayScene(b2))
+    want2 = reference_renderer.render_to_image(array_scene(b2, device_plan))
     assert np.array_equal(renderer.readback().view(np.uint8).reshape(want2.shape), want2)
+
+
+def test_gpu_device_plan_delta_with_a_changed_total_scans_everything(renderer, reference_renderer):
+    """Device plans: a replaced path whose segment total changes would move
+    every later slice, so the render finds that after counting it and scans
+    the whole scene; the frame still equals a full upload and render."""
+    c = tk.generate(2, 16, width=W, height=H, paths=150, device_segment_plan=True)
+    a = c.scene_arrays()
+    renderer.upload(c)
+    renderer.render()
+    b = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in a.items()}
+    rec = b["paths"][40]
+    s, n = int(rec["line_start"]), int(rec["line_count"])
+    seg = b["lines"][s:s + n]
+    cx, cy = float(seg["p0"][:, 0].mean()), float(seg["p0"][:, 1].mean())
+    for end in ("p0", "p1"):  # shrunk about its centre: inside its bbox, fewer tile crossings
+        seg[end][:, 0] = cx + 0.25 * (seg[end][:, 0] - cx)
+        seg[end][:, 1] = cy + 0.25 * (seg[end][:, 1] - cy)
+    b["lines"][s:s + n] = seg
+    assert renderer.upload_delta(array_scene(b, True), [40]) == 1
+    st = renderer.render_incremental({"full": True})
+    assert st["scanned_paths"] == len(a["paths"])
+    same_scan_and_frame(renderer, reference_renderer, array_scene(b, True))
 
 
 def test_gpu_delta_upload_falls_back_when_the_layout_changes(renderer, reference_renderer):

@@ -202,6 +202,10 @@ struct tk_ctx {
     DBuf<uint32_t> rescan_list;
     DBuf<tk::ScanItem> rescan_items;
     DBuf<unsigned long long> rescan_desc;
+    // device segment plans: the rescanned paths keep their planned slices
+    // only if their counted totals still fill them exactly (checked after
+    // counting; otherwise the whole scene is scanned)
+    bool rescan_check = false;
     uint32_t last_scan_paths = 0;  // paths the last scan covered
 };
 
@@ -728,6 +732,8 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
     }
 }
 
+void scan_phase(tk_ctx* c);
+
 // The scan of the paths a delta upload replaced (scene_scan.rs:116-192's
 // selected paths): their slices cleared and counted, their pool scan items,
 // their segments emitted; every other path's scan output stays as it is.
@@ -760,7 +766,20 @@ void scan_phase_partial(tk_ctx* c) {
                              c->misc.ptr + 2, st);
         tk::launch_path_totals(s, c->bumps.ptr, false, c->misc.ptr + 2, st);
     }
-    s.segment_capacity = c->host_segment_capacity;
+    if (c->rescan_check) {
+        // device plans: a replaced path whose segment total changed moves
+        // every later path's slice, so the scene is scanned whole
+        tk::launch_check_path_totals(s, c->bumps.ptr, c->rescan_list.ptr, n, c->misc.ptr + 5, st);
+        c->rescan_check = false;
+        if (read_word(c, c->misc.ptr + 5)) {
+            c->rescan.clear();
+            c->segment_needed = 0;
+            scan_phase(c);
+            return;
+        }
+    }
+    const bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
+    s.segment_capacity = device_plan ? c->segment_needed - 1 : c->host_segment_capacity;
     {
         StageMark m(c, 3);
         tk::launch_scan_emit_paths(s, c->rescan_list.ptr, n, st);
@@ -779,6 +798,7 @@ void scan_phase(tk_ctx* c) {
         return;
     }
     c->rescan.clear();
+    c->rescan_check = false;
     c->last_scan_paths = c->path_count;
     c->scan_valid = false;
     cudaStream_t st = c->stream;
@@ -1388,10 +1408,11 @@ int32_t tk_scene_upload_delta(tk_ctx* c, const tk_scene_desc* d, const uint32_t*
     if (!d) return fail(c, Fail{TK_E_INVALID, "null scene"});
     return guarded(c, [&] {
         if (changed_count && !changed) invalid("null changed-path list");
-        const bool device_plan = (c->flags | d->flags) & TK_SCENE_SEGMENTS_FROM_DEVICE;
+        const bool device_plan = (c->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u;
         const bool can = c->have_scene && !c->batched && !c->band && c->scan_valid && !c->want_seg_line &&
-                         !device_plan && d->path_count == c->path_count && d->line_count == c->line_count &&
-                         d->path_count && d->paths;
+                         device_plan == ((d->flags & TK_SCENE_SEGMENTS_FROM_DEVICE) != 0u) &&
+                         (!device_plan || c->segment_needed) && d->path_count == c->path_count &&
+                         d->line_count == c->line_count && d->path_count && d->paths;
         if (!can) {  // no scan to keep: a whole upload
             do_upload(c, *d);
             if (rescan_paths) *rescan_paths = d->path_count;
@@ -1400,7 +1421,7 @@ int32_t tk_scene_upload_delta(tk_ctx* c, const tk_scene_desc* d, const uint32_t*
         // The paths to rescan: the caller's (lines changed), the ones whose
         // records changed, and any still pending from an earlier delta.
         const std::vector<tk_path_record> old = c->h_paths;
-        const uint64_t old_pool = c->pool_len, old_cap = c->host_segment_capacity;
+        const uint64_t old_pool = c->pool_len, old_cap = c->host_segment_capacity, old_needed = c->segment_needed;
         std::vector<uint8_t> dirty(d->path_count, 0u);
         for (uint32_t k = 0; k < changed_count; ++k) {
             if (changed[k] >= d->path_count) invalid("changed path index out of range");
@@ -1409,16 +1430,37 @@ int32_t tk_scene_upload_delta(tk_ctx* c, const tk_scene_desc* d, const uint32_t*
         for (uint32_t p : c->rescan) dirty[p] = 1u;
         for (uint32_t p = 0; p < d->path_count; ++p)
             if (std::memcmp(&old[p], &d->paths[p], sizeof(tk_path_record)) != 0) dirty[p] = 1u;
-        do_upload(c, *d, nullptr, &dirty);
+        // Device plans: every path keeps the segment slice the last scan
+        // planned for it (the device records hold it), so the records go up
+        // with those slices and only the replaced paths are counted again.
+        tk_scene_desc dd = *d;
+        std::vector<tk_path_record> planned;
+        if (device_plan) {
+            planned.resize(d->path_count);
+            TK_CUDA(cudaMemcpyAsync(planned.data(), c->paths.ptr, d->path_count * sizeof(tk_path_record),
+                                    cudaMemcpyDeviceToHost, c->stream));
+            TK_CUDA(cudaStreamSynchronize(c->stream));
+            for (uint32_t p = 0; p < d->path_count; ++p) {
+                const uint32_t start = planned[p].segment_start, cap = planned[p].segment_capacity;
+                planned[p] = d->paths[p];
+                planned[p].segment_start = start;
+                planned[p].segment_capacity = cap;
+            }
+            dd.paths = planned.data();
+        }
+        do_upload(c, dd, nullptr, &dirty);
+        c->h_paths.assign(d->paths, d->paths + d->path_count);  // the caller's records, compared next time
         // the kept scan is valid only over the same pool and segment layout;
         // otherwise the next render scans everything
         c->rescan.clear();
-        if (c->pool_len != old_pool || c->host_segment_capacity != old_cap) {
+        if (c->pool_len != old_pool || (!device_plan && c->host_segment_capacity != old_cap)) {
             if (rescan_paths) *rescan_paths = d->path_count;
             return;
         }
+        if (device_plan) c->segment_needed = old_needed;  // the segment buffer as the last scan sized it
         for (uint32_t p = 0; p < d->path_count; ++p)
             if (dirty[p]) c->rescan.push_back(p);
+        c->rescan_check = device_plan && !c->rescan.empty();
         c->scan_valid = true;
         if (rescan_paths) *rescan_paths = uint32_t(c->rescan.size());
     });

@@ -106,6 +106,10 @@ void launch_scan_emit(const SceneView& s, cudaStream_t st);
 // segments. Their pool scan runs through launch_pool_scan with their items.
 void launch_scan_count_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st);
 void launch_scan_emit_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st);
+// *changed = 1 when a listed path's segment total (bumps, from
+// launch_path_totals) differs from its planned segment_capacity.
+void launch_check_path_totals(const SceneView& s, const uint32_t* bumps, const uint32_t* list, uint32_t n,
+                              uint32_t* changed, cudaStream_t st);
 
 // Fixed scratch of the allocation-free pool scan (one array per device).
 struct NoAllocScratch {

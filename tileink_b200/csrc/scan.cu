@@ -431,6 +431,16 @@ __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_rec
     }
 }
 
+// The listed paths' counted segment totals (bumps) against the segment
+// slices they were planned (segment_capacity): any difference sets *changed.
+__global__ void k_check_path_totals(const tk_path_record* __restrict__ paths, const uint32_t* __restrict__ bumps,
+                                    const uint32_t* __restrict__ list, uint32_t n, uint32_t* changed) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t p = __ldg(list + k);
+    if (__ldg(bumps + p) != paths[p].segment_capacity) atomicOr(changed, 1u);
+}
+
 inline unsigned grid_for(uint64_t n, unsigned block, unsigned cap) {
     uint64_t g = (n + block - 1) / block;
     if (g < 1) g = 1;
@@ -474,6 +484,12 @@ void launch_scan_emit_paths(const SceneView& s, const uint32_t* list, uint32_t n
     k_scan_emit<<<grid_for(uint64_t(n) * 32, 256, 148 * 8), 256, 0, st>>>(s.lines, s.paths, n, s.cursors, s.segments,
                                                                         s.segment_capacity, s.error, s.seg_line, list,
                                                                         s.emit_ticket);
+}
+
+void launch_check_path_totals(const SceneView& s, const uint32_t* bumps, const uint32_t* list, uint32_t n,
+                              uint32_t* changed, cudaStream_t st) {
+    cudaMemsetAsync(changed, 0, sizeof(uint32_t), st);
+    if (n) k_check_path_totals<<<(n + 255) / 256, 256, 0, st>>>(s.paths, bumps, list, n, changed);
 }
 
 void launch_scan_emit(const SceneView& s, cudaStream_t st) {
