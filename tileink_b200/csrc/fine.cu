@@ -74,7 +74,7 @@ struct FineSmem {
     float4 pcf[kRecChunk];                       // paint channels as floats
     uint4 rec_a[kRecChunk];                      // tag, backdrop, fill_rule, segment_start
     uint2 rec_b[kRecChunk];                      // segment_end, color
-    uint32_t cls[kRecChunk];                     // class | fill rule << 4 | covered rows << 16 (fills)
+    uint32_t cls[kRecChunk];
     uint32_t ualpha[kRecChunk];
     uint32_t umode[kRecChunk];                   // uniform fills: 1 replace, 2 src-over, 3 no-op;
                                                  // SDF records: first word of the shape
@@ -380,32 +380,21 @@ __device__ void stage_rows(FineSmem& S, uint32_t total, uint32_t n) {
     }
     __syncthreads();
     // per (fill, row): the base sum and the row's entry range (needs the
-    // positions only, so it shares this phase with the entries below), and
-    // per fill the rows where it can cover anything: a row whose base sum is
-    // zero and that no segment of the fill crosses has coverage 0 at every
-    // pixel (fill_alpha_at sums base + 0 + 0), so its warp skips the fill.
-    for (uint32_t k0i = 0; k0i < n * TK_TILE_SIZE; k0i += kFineThreads) {
-        const uint32_t k = k0i + threadIdx.x;
-        const bool valid = k < n * TK_TILE_SIZE;  // whole 16-lane halves of a warp
+    // positions only, so it shares this phase with the entries below)
+    for (uint32_t k = threadIdx.x; k < n * TK_TILE_SIZE; k += kFineThreads) {
         const uint32_t ri = k >> 4, row = k & 15u;
-        const uint32_t ns = valid ? S.nseg[ri] : 0u;
-        bool covers = false;
-        if (ns != 0u) {
-            const uint32_t j0 = S.off[ri];
-            float bsum = float(int32_t(S.rec_a[ri].y));
-            for (uint32_t j = j0; j < j0 + ns; ++j) {
-                const float ye = S.sgx[j].x;
-                if (ye < 1000000000.0f) {  // y_edge set: the segment touches the tile's left edge
-                    const float4 g = S.sgp[j];
-                    bsum += signum_f32(g.z - g.x) * clampf(float(row) - ye + 1.0f, 0.0f, 1.0f);
-                }
+        const uint32_t j0 = S.off[ri], ns = S.nseg[ri];
+        if (ns == 0u) continue;
+        float bsum = float(int32_t(S.rec_a[ri].y));
+        for (uint32_t j = j0; j < j0 + ns; ++j) {
+            const float ye = S.sgx[j].x;
+            if (ye < 1000000000.0f) {  // y_edge set: the segment touches the tile's left edge
+                const float4 g = S.sgp[j];
+                bsum += signum_f32(g.z - g.x) * clampf(float(row) - ye + 1.0f, 0.0f, 1.0f);
             }
-            const uint32_t k0 = S.pos[row][j0], k1 = S.pos[row][j0 + ns];
-            S.rb[ri][row] = make_float2(bsum, __uint_as_float(k0 | (k1 << 16)));
-            covers = bsum != 0.0f || k1 > k0;
         }
-        const uint32_t rows = __ballot_sync(0xffffffffu, covers);
-        if (valid && ns != 0u && row == 0u) S.cls[ri] |= ((rows >> (threadIdx.x & 16u)) & 0xFFFFu) << 16;
+        const uint32_t k0 = S.pos[row][j0], k1 = S.pos[row][j0 + ns];
+        S.rb[ri][row] = make_float2(bsum, __uint_as_float(k0 | (k1 << 16)));
     }
     const uint32_t items = S.rpre[total];
     for (uint32_t it = threadIdx.x; it < items; it += kFineThreads) {
@@ -473,24 +462,6 @@ static __device__ __forceinline__ float sdf_coverage_at(const uint32_t* w, const
     return sdf_coverage<EXT>(w, ux, uy, inv);
 }
 
-// src_over_premul_unorm(d, s * sc) (shared/pixel.hlsli) with the four
-// channels in two packed f32x2 multiplies and adds. Each lane of a packed op
-// is one IEEE operation rounded to nearest, exactly the scalar multiply and
-// add (nothing is fused), so the result has the scalar sequence's bits.
-__device__ __forceinline__ void src_over_scaled(float4& d, float4 c, float sc) {
-    const float2 s01 = __fmul2_rn(make_float2(c.x, c.y), make_float2(sc, sc));
-    const float2 s23 = __fmul2_rn(make_float2(c.z, c.w), make_float2(sc, sc));
-    if (s23.y <= 0.0f) return;
-    if (s23.y >= 1.0f) {
-        d = make_float4(s01.x, s01.y, s23.x, s23.y);
-        return;
-    }
-    const float k = 1.0f - s23.y;
-    const float2 d01 = __fadd2_rn(s01, __fmul2_rn(make_float2(d.x, d.y), make_float2(k, k)));
-    const float2 d23 = __fadd2_rn(s23, __fmul2_rn(make_float2(d.z, d.w), make_float2(k, k)));
-    d = make_float4(d01.x, d01.y, d23.x, d23.y);
-}
-
 // Paints a fill's masked coverage over px (the brush branch of
 // fine/interpreter.hlsli's fill handling, fine/draw.hlsli:16-21).
 template <bool IMG>
@@ -504,15 +475,12 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
             // scale_premul_u8_to_unorm with the channels staged as floats
             const float sc = float(masked) * (1.0f / 65025.0f);
             const float4 c = S.pcf[i];
-            if (c.w != 0.0f) src_over_scaled(px, c, sc);
+            if (c.w != 0.0f) px = src_over_premul_unorm(px, make_float4(c.x * sc, c.y * sc, c.z * sc, c.w * sc));
         }
     } else {
         const uint32_t g = gradient_at<IMG>(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
         if (masked == 255u && premul_u8_is_opaque(g)) px = rgba8_to_unorm(g);
-        else if (masked != 0u && (g >> 24) != 0u)  // scale_premul_u8_to_unorm: 0 otherwise
-            src_over_scaled(px, make_float4(float(g & 255u), float((g >> 8) & 255u), float((g >> 16) & 255u),
-                                            float(g >> 24)),
-                            float(masked) * (1.0f / 65025.0f));
+        else px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(g, masked));
     }
 }
 
@@ -621,7 +589,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                     for (int k = 0; k < kGradParams / 4; ++k) dst[k] = __ldg(g + k);
                 }
             }
-            S.cls[tid] = cls | ((b.x & 1u) << 4);
+            S.cls[tid] = cls;
         }
         if (tid == 0) S.nprod = 0u;
         __syncthreads();
@@ -670,24 +638,18 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
         // ---- interpret the chunk -------------------------------------------------
         uint32_t i = 0;
         while (i < n) {
-            const uint32_t meta = S.cls[i];
-            const uint32_t cls = meta & 15u;
+            const uint32_t cls = S.cls[i];
+            if (cls == kClsEnd) {
+                done = true;
+                break;
+            }
             if (cls == kClsFill && mode != TK_TILE_KIND_COLOR && !big) {
-                // the common record: a path fill with segments in the tile;
-                // warps whose rows it cannot cover skip it (warp-uniform)
-                if (!((meta >> (16u + (ly & 14u))) & 3u)) {  // this warp's rows 2w, 2w + 1
-                    ++i;
-                    continue;
-                }
-                const uint32_t alpha = coverage_to_alpha(staged_coverage(S, i, lx, ly), (meta >> 4) & 1u);
+                // the common record: a path fill with segments in the tile
+                const uint32_t alpha = coverage_to_alpha(staged_coverage(S, i, lx, ly), S.rec_a[i].z);
                 const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
                 if (masked != 0u) paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                 ++i;
                 continue;
-            }
-            if (cls == kClsEnd) {
-                done = true;
-                break;
             }
             const uint2 qb = S.rec_b[i];
             if (cls == kClsBatch) {
