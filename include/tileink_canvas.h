@@ -83,6 +83,15 @@ int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_de
                             const double* transform, uint32_t fill_rule, double tolerance);
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
                               double width, const double* transform, double tolerance);
+/* Canvas::push_text_layout_as_path (src/canvas/primitives/text.rs:107-147)
+ * after shaping: `path` holds the glyph outlines of a laid-out text run (the
+ * caller's shaping and outline extraction), filled nonzero with `brush` as a
+ * DrawTag::PathGlyph draw, which fine raster composites with the text
+ * coverage correction (src_over_mask_linear_auto_u8,
+ * fine/text/auto.hlsli:28-33) instead of plain source-over. Returns the draw
+ * index, or -1 on error. */
+int64_t tk_canvas_push_glyph_outlines(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
+                                      const double* transform, double tolerance);
 /* Analytic SDF shapes (Canvas::push_rect, push_rect_stroke(_widths),
  * push_circle, push_circle_stroke, push_line and push_{rect,circle,line}_shadow,
  * src/canvas/primitives/{rectangles,shapes,shadows}.rs:5-110), in logical

@@ -66,6 +66,10 @@ def lib() -> C.CDLL:
         l.or_sincos.argtypes = [F32, P, P]
         l.or_atan2.restype = F32
         l.or_atan2.argtypes = [F32, F32]
+        l.or_text_pow.restype = F32
+        l.or_text_pow.argtypes = [F32, F32]
+        l.or_glyph_over.restype = U32
+        l.or_glyph_over.argtypes = [U32, U32, U32]
         l.or_interpret_particles.restype = I32
         l.or_interpret_particles.argtypes = [P, P, U32, P]
         l.or_interpret_path_draws.restype = I32

@@ -1421,6 +1421,98 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
     return true;
 }
 
+// --- fine/text/{gamma,auto,basic}.hlsli: glyph outline compositing -----------
+// The shaders' pow as exp(y ln x) in double with exactly rounded operations
+// (ln m = 2 atanh((m - 1)/(m + 1)) by its odd series to s^21 after
+// m = x / 2^e in [sqrt(1/2), sqrt(2)); exp by Cody-Waite reduction with
+// fdlibm's two-part ln 2 and its Taylor polynomial to degree 16), the same
+// steps as the library's, so that the two agree bit for bit; its distance to
+// the C library's pow is checked in the tests. `lerp(a, b, t)` is
+// a + t (b - a) and `dot` is (x x' + y y') + z z', each operation rounded.
+float text_pow(float x, float y) {
+    int e = 0;
+    double m = std::frexp(double(x), &e);
+    if (m < 0.70710678118654752440) {
+        m *= 2.0;
+        --e;
+    }
+    const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+    static const double odd[11] = {1.0 / 21.0, 1.0 / 19.0, 1.0 / 17.0, 1.0 / 15.0, 1.0 / 13.0, 1.0 / 11.0,
+                                   1.0 / 9.0,  1.0 / 7.0,  1.0 / 5.0,  1.0 / 3.0,  1.0};
+    double p = odd[0];
+    for (int k = 1; k < 11; ++k) p = p * s2 + odd[k];
+    const double ln2_hi = 6.93147180369123816490e-01, ln2_lo = 1.90821492927058770002e-10;
+    const double lnx = (double(e) * ln2_hi + 2.0 * s * p) + double(e) * ln2_lo;
+    const double t = double(y) * lnx;
+    const double k = std::nearbyint(t * 1.44269504088896338700);
+    const double r = (t - k * ln2_hi) - k * ln2_lo;
+    // 1/16!, 1/15!, ..., 1/2!, 1, 1
+    static const double inv_fact[17] = {1.0 / 20922789888000.0, 1.0 / 1307674368000.0, 1.0 / 87178291200.0,
+                                        1.0 / 6227020800.0, 1.0 / 479001600.0, 1.0 / 39916800.0, 1.0 / 3628800.0,
+                                        1.0 / 362880.0, 1.0 / 40320.0, 1.0 / 5040.0, 1.0 / 720.0, 1.0 / 120.0,
+                                        1.0 / 24.0, 1.0 / 6.0, 0.5, 1.0, 1.0};
+    double q = inv_fact[0];
+    for (int i = 1; i < 17; ++i) q = q * r + inv_fact[i];
+    return float(std::ldexp(q, int(k)));
+}
+// gamma.hlsli:5-23
+float srgb_to_linear(float value) {
+    float v = clampf(value, 0.0f, 1.0f);
+    float result = v / 12.92f;
+    if (v > 0.04045f) result = text_pow((v + 0.055f) / 1.055f, 2.4f);
+    return result;
+}
+float linear_to_srgb(float value) {
+    float v = clampf(value, 0.0f, 1.0f);
+    float result = v * 12.92f;
+    if (v > 0.0031308f) result = 1.055f * text_pow(v, 1.0f / 2.4f) - 0.055f;
+    return result;
+}
+// auto.hlsli:6-9, dotted with the luminance weights
+float text_foreground_luma(uint32_t source) {
+    float alpha = float(source >> 24);
+    if (!(alpha > 0.0f)) return 0.0f;
+    float r = clampf(float(source & 255u) / alpha, 0.0f, 1.0f);
+    float g = clampf(float((source >> 8) & 255u) / alpha, 0.0f, 1.0f);
+    float b = clampf(float((source >> 16) & 255u) / alpha, 0.0f, 1.0f);
+    return (r * 0.2126f + g * 0.7152f) + b * 0.0722f;
+}
+// auto.hlsli:15-26
+float text_correcting_coverage(uint32_t coverage, float foreground) {
+    if (coverage == 0u || coverage == 255u) return float(coverage) * (1.0f / 255.0f);
+    float raw = float(coverage) * (1.0f / 255.0f);
+    float background = 1.0f - foreground;
+    float bg_linear = srgb_to_linear(background);
+    float enhanced = raw + raw * (1.0f - raw) * bg_linear;
+    float difference = foreground - background;
+    if (std::fabs(difference) < (1.0f / 256.0f)) return enhanced;
+    float fg_linear = srgb_to_linear(foreground);
+    float output = linear_to_srgb(bg_linear + enhanced * (fg_linear - bg_linear));
+    return clampf((output - background) / difference, 0.0f, 1.0f);
+}
+// basic.hlsli:95-109 with the same coverage in the three channels
+uint32_t src_over_subpixel_mask_f32(uint32_t destination, uint32_t source, float cr, float cg, float cb) {
+    if ((source >> 24) == 0u || (cr == 0.0f && cg == 0.0f && cb == 0.0f)) return destination;
+    if ((destination >> 24) != 255u) {
+        float gray = (cr + cg + cb) / 3.0f;
+        cr = cg = cb = gray;
+    }
+    float alpha = float(source >> 24) * (1.0f / 255.0f);
+    float ar = alpha * cr, ag = alpha * cg, ab = alpha * cb;
+    float r = float(source & 255u) * cr + float(destination & 255u) * (1.0f - ar);
+    float g = float((source >> 8) & 255u) * cg + float((destination >> 8) & 255u) * (1.0f - ag);
+    float b = float((source >> 16) & 255u) * cb + float((destination >> 16) & 255u) * (1.0f - ab);
+    float maximum = fmax_(fmax_(ar, ag), ab);
+    float a = maximum * 255.0f + float(destination >> 24) * (1.0f - maximum);
+    return pack(f2u(r + 0.5f), f2u(g + 0.5f), f2u(b + 0.5f), f2u(a + 0.5f));
+}
+// auto.hlsli:28-33
+uint32_t src_over_mask_linear_auto_u8(uint32_t destination, uint32_t source, uint32_t coverage) {
+    if ((source >> 24) == 0u || coverage == 0u) return destination;
+    float corrected = text_correcting_coverage(coverage, text_foreground_luma(source));
+    return src_over_subpixel_mask_f32(destination, source, corrected, corrected, corrected);
+}
+
 // --- fine/interpreter.hlsli:21-219 (clip stack and opacity groups) ------------
 struct Group { uint32_t kind; F4 parent; uint32_t parent_clip, layer_alpha, payload; };
 
@@ -1492,7 +1584,9 @@ F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_
                 uint32_t masked = combine_alpha(alpha, clip_mask);
                 if (masked != 0u) {
                     uint32_t color = sample_draw_brush(P, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f);
-                    if (masked == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
+                    if (tag == TK_PTCL_PATH_GLYPH)  // interpreter.hlsli:205-206
+                        pixel = rgba8_to_unorm(src_over_mask_linear_auto_u8(unorm_to_rgba8(pixel), color, masked));
+                    else if (masked == 255u && premul_u8_is_opaque(color)) pixel = rgba8_to_unorm(color);
                     else pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(color, masked));
                 }
             }
@@ -2271,6 +2365,10 @@ float or_sdf_coverage(const uint32_t* record, float x, float y, const tk_affine*
 float or_exp_nonpos(float x) { return exp_nonpos(x); }
 void or_sincos(float x, float* s, float* c) { lib_sincos(x, *s, *c); }
 float or_atan2(float y, float x) { return lib_atan2(y, x); }
+float or_text_pow(float x, float y) { return text_pow(x, y); }
+uint32_t or_glyph_over(uint32_t destination, uint32_t source, uint32_t coverage) {
+    return src_over_mask_linear_auto_u8(destination, source, coverage);
+}
 
 // Fine-only oracle (src/native/runtime/tests/coarse_count/rect_pixels.rs:3-13):
 // every draw interpreted as a PTCL_SDF particle in every tile, in draw-record
@@ -2341,7 +2439,8 @@ int32_t or_interpret_path_draws(const tk_scene_desc* d, int32_t threads, uint32_
                         continue;
                     }
                     range_in_tile(dr, tx, ty, w, s0, s1);
-                    recs.push_back({TK_PTCL_FILL, w, dr.fill_rule, s0, s1, di});
+                    recs.push_back({dr.tag == TK_DRAW_PATH_GLYPH ? TK_PTCL_PATH_GLYPH : TK_PTCL_FILL, w, dr.fill_rule,
+                                    s0, s1, di});
                 }
                 for (uint32_t i = op.layer_end; i > op.layer_start;) {
                     const tk_layer_record& L = S.layers[--i];

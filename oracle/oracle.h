@@ -121,6 +121,10 @@ float or_exp_nonpos(float x);
 /* The library's sin / cos and atan2 for the arc and star kinds. */
 void or_sincos(float x, float* s, float* c);
 float or_atan2(float y, float x);
+/* The library's pow for the text gamma (x > 0), and the glyph outline
+ * composite src_over_mask_linear_auto_u8 (fine/text/auto.hlsli:28-33). */
+float or_text_pow(float x, float y);
+uint32_t or_glyph_over(uint32_t destination, uint32_t source, uint32_t coverage);
 /* Fine-only image of a scene of SDF draws: every draw interpreted in every
  * tile as a PTCL_SDF particle, from the clear colour (no coarse stage). */
 int32_t or_interpret_sdf_draws(const tk_scene_desc* scene, uint32_t* image);

@@ -28,6 +28,10 @@ STAGE_PTCL, STAGE_TILES, STAGE_KINDS, STAGE_IMAGE, STAGE_PATHS, STAGE_LINES = 4,
 # PTCL tags (shaders/hlsl/shared/particle_tags.hlsli) + merged-stream marker
 PTCL_END, PTCL_FILL, PTCL_COLOR, PTCL_BEGIN_CLIP, PTCL_END_CLIP = 0, 1, 2, 3, 4
 PTCL_BEGIN_OPACITY, PTCL_END_OPACITY = 5, 6
+PTCL_PATH_GLYPH = 11
+# Draw tags (src/shared/draw_record.rs:7-13)
+DRAW_BRUSH, DRAW_CLIP, DRAW_OPACITY, DRAW_PATH_GLYPH = 0, 1, 2, 5
+FILL_NONZERO, FILL_EVEN_ODD = 0, 1
 # Layer stack tags (shaders/hlsl/shared/draw_tags.hlsli:7-9)
 LAYER_CLIP, LAYER_OPACITY, LAYER_BLEND = 0, 1, 2
 PTCL_BATCH_BEGIN = 14
@@ -270,6 +274,7 @@ def library() -> C.CDLL:
         "tk_canvas_set_clear_color": (None, [P, U32]),
         "tk_canvas_push_path": (I64, [P, P, C.POINTER(BrushDesc), P, U32, F64]),
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
+        "tk_canvas_push_glyph_outlines": (I64, [P, P, C.POINTER(BrushDesc), P, F64]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),

@@ -208,6 +208,18 @@ class Canvas:
             raise ValueError("push_stroke rejected its arguments")
         return r
 
+    def push_glyph_outlines(self, path: BezPath, brush: Brush, transform=None, tolerance: float = 0.1) -> int:
+        """Canvas::push_text_layout_as_path (src/canvas/primitives/text.rs:107-147)
+        after shaping: the glyph outlines of a laid-out run as one nonzero
+        DrawTag::PathGlyph fill, composited with the text coverage
+        correction (fine/text/auto.hlsli)."""
+        d, keep = brush._desc()
+        t, tk = _affine(transform)
+        r = self._lib.tk_canvas_push_glyph_outlines(self._h, path._h, C.byref(d), t, float(tolerance))
+        if r < 0:
+            raise ValueError("push_glyph_outlines rejected its arguments")
+        return r
+
     # -- analytic SDF shapes (src/canvas/primitives/{rectangles,shapes,shadows}.rs) --
     @staticmethod
     def _shape(kind: int, p0=(0.0, 0.0), p1=(0.0, 0.0), radius=0.0, width=0.0, radii=0.0, widths=0.0, shadow=None,

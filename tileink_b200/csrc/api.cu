@@ -336,8 +336,10 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                 invalid(at + ": bad image brush extend, opacity or sampling");
         }
         if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
-            r.tag != TK_DRAW_ISOLATE)
+            r.tag != TK_DRAW_ISOLATE && r.tag != TK_DRAW_PATH_GLYPH)
             invalid("draw " + std::to_string(i) + ": unsupported tag");
+        if (r.tag == TK_DRAW_PATH_GLYPH && r.path_id == TK_INVALID_INDEX)
+            invalid("draw " + std::to_string(i) + ": a glyph outline draw without a path");
         if (r.path_id != TK_INVALID_INDEX && r.path_id >= d.path_count) invalid("draw path out of range");
         if (r.fill_rule > 1u) invalid("bad fill rule");
     }

@@ -368,7 +368,7 @@ struct Cmd {
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS } kind = FILL;
     tk_path path;
     tk_sdf_shape shape{};
     // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options;
@@ -1152,6 +1152,18 @@ int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_de
     }
     return draw;
 }
+int64_t tk_canvas_push_glyph_outlines(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
+                                      const double* transform, double tolerance) {
+    if (!c || !path || !(tolerance > 0.0)) return -1;
+    const int64_t draw =
+        push_path_with_tag(c, *path, brush, transform, TK_FILL_NONZERO, tolerance, TK_DRAW_PATH_GLYPH, true);
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::GLYPHS, path, brush, transform);
+        r.tolerance = tolerance;
+        c->log.push_back(std::move(r));
+    }
+    return draw;
+}
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush, double width,
                               const double* transform, double tolerance) {
     if (!c || !path || !(width > 0.0) || !(tolerance > 0.0)) return -1;
@@ -1672,7 +1684,7 @@ void gen_glyphs(tk_canvas* c, Rng& r, uint32_t w, uint32_t h, uint32_t count) {
             }
             tk_path_close(p);
         }
-        tk_canvas_push_path(c, p, &black, nullptr, TK_FILL_NONZERO, 0.1);
+        tk_canvas_push_glyph_outlines(c, p, &black, nullptr, 0.1);  // text as outlines: PathGlyph draws
         tk_path_free(p);
         x += 0.62 * em;
     }
@@ -1906,6 +1918,7 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
     const tk_brush_desc* bp = r.has_brush ? &b : nullptr;
     switch (r.kind) {
         case RecCmd::FILL: return tk_canvas_push_path(dst, &r.path, bp, t, r.rule, r.tolerance) < 0 ? -1 : 0;
+        case RecCmd::GLYPHS: return tk_canvas_push_glyph_outlines(dst, &r.path, bp, t, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::STROKE: return tk_canvas_push_stroke(dst, &r.path, bp, r.width, t, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::OPACITY: return tk_canvas_push_opacity_layer(dst, &r.path, t, r.tolerance, r.sigma);

@@ -26,6 +26,7 @@
 #include "device.cuh"
 #include "kernels.h"
 #include "sdf.cuh"
+#include "text.cuh"
 
 namespace tk {
 namespace {
@@ -484,6 +485,20 @@ __device__ __forceinline__ void paint_fill(const FineSmem& S, const Paint& P, ui
     }
 }
 
+// Paints a glyph outline fill's masked coverage over px: the brush colour
+// composited by src_over_mask_linear_auto_u8 on the stored RGBA8 value
+// (fine/interpreter.hlsli:205-206).
+// Out of line: glyph fills are rare outside text, and the double-precision
+// pow would otherwise weigh on the record loop's registers.
+template <bool IMG>
+__device__ __noinline__ float4 paint_glyph_fill(const FineSmem& S, const Paint P, uint32_t i, uint32_t masked,
+                                                uint32_t gx, uint32_t gy, float4 px) {
+    const uint32_t paint = S.paint[i];
+    const uint32_t color =
+        paint != kGradient ? paint : gradient_at<IMG>(S, P, i, float(gx) + 0.5f, float(gy) + 0.5f);
+    return rgba8_to_unorm(src_over_mask_linear_auto_u8(unorm_to_rgba8(px), color, masked));
+}
+
 // SDF: 0 for scenes without SDF records, 1 with SDF records of the base
 // kinds, 2 with the extended kinds (candlestick, dash line, triangle,
 // checkerboard). Path-only scenes run the instance without the PTCL_SDF
@@ -787,8 +802,8 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                 } else {
                     const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
                     if (masked != 0u) {
-                        if (tag == TK_PTCL_PATH_GLYPH) atomicOr(error, ERR_UNSUPPORTED);
-                        paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
+                        if (tag == TK_PTCL_PATH_GLYPH) px = paint_glyph_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
+                        else paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                     }
                 }
             }
