@@ -158,6 +158,34 @@ typedef struct tk_image_desc {
     uint32_t height;
 } tk_image_desc;
 
+/* Glyph runs drawn from rasterized glyph images (Canvas::push_text_layout,
+ * src/canvas/primitives/text.rs:11-100; the text blob records of
+ * draw_records.hlsli:19-21). A draw whose glyph_run_id is a run index
+ * composites that run's glyphs (coarse/text.hlsli, fine/glyph.hlsli). */
+typedef struct tk_glyph_run {  /* TextRun, 8 bytes */
+    uint32_t first;            /* first glyph */
+    uint32_t count;
+} tk_glyph_run;
+typedef struct tk_glyph {      /* a positioned glyph, 12 bytes */
+    uint32_t image;            /* glyph image, TK_INVALID_INDEX for none */
+    int32_t x, y;              /* pen position in device pixels */
+} tk_glyph;
+typedef struct tk_glyph_image {  /* 24 bytes */
+    int32_t left, top;           /* image placement: x + left, y - top */
+    uint32_t width, height;
+    uint32_t content;            /* TK_GLYPH_* */
+    uint32_t data_offset;        /* first texel in the glyph texels, rows of `width` */
+} tk_glyph_image;
+/* Glyph image contents (fine/constants.hlsli:4-9). Texels are 32-bit words:
+ * masks keep the coverage in the low byte, subpixel masks one coverage per
+ * byte (red in the low byte), colour glyphs premultiplied RGBA8. */
+#define TK_GLYPH_MASK 0u
+#define TK_GLYPH_COLOR 1u
+#define TK_GLYPH_SUBPIXEL_MASK 2u
+#define TK_GLYPH_LINEAR_MASK 3u
+#define TK_GLYPH_LINEAR_COLOR 4u
+#define TK_GLYPH_LINEAR_SUBPIXEL_MASK 5u
+
 /* ------------------------------------------------------------------------ */
 /* Records. Layouts equal the reference's #[repr(C)] Pod types.              */
 /* ------------------------------------------------------------------------ */
@@ -313,6 +341,17 @@ typedef struct tk_scene_desc {
     const tk_image_desc* images;
     uint32_t image_count;
     uint32_t image_reserved;
+    /* The text blob: glyph runs, their glyphs, the glyph images and their
+     * texels (all may be empty). */
+    const tk_glyph_run* glyph_runs;
+    const tk_glyph* glyphs;
+    const tk_glyph_image* glyph_images;
+    const uint32_t* glyph_texels;
+    uint32_t glyph_run_count;
+    uint32_t glyph_count;
+    uint32_t glyph_image_count;
+    uint32_t glyph_reserved;
+    uint64_t glyph_texel_count;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */
@@ -420,6 +459,7 @@ int32_t tk_get_stats(tk_ctx* ctx, tk_stats* out);
 #define TK_STAGE_IMAGE 7u      /* u32[W*H] current target image */
 #define TK_STAGE_PATHS 8u      /* tk_path_record[P] (segment plan applied) */
 #define TK_STAGE_LINES 9u      /* tk_line[L] (device-flattened lines included) */
+#define TK_STAGE_GLYPHS 10u    /* u32[] glyph list of pass `index` (the glyph indices PTCL_GLYPH ranges name) */
 int32_t tk_debug_readback(tk_ctx* ctx, uint32_t stage, uint32_t index,
                           void* dst, size_t bytes, size_t* needed);
 /* Elements [first, first + count) of the same buffers (count clipped to the
@@ -477,8 +517,9 @@ int32_t tk_stage_scan_prefix(tk_ctx* ctx, const uint32_t* counts, uint64_t pool_
                              uint32_t* bumps);
 
 /* Tile prefix (coarse/prefix.hlsl:11-63) on host tile records: the exclusive
- * scan of tiles[i].ptcl_count into ptcl_start / ptcl_end (glyph words
- * cleared) and the total record count. The scan's look-back wait gives up
+ * scan of tiles[i].ptcl_count into ptcl_start / ptcl_end (glyph_start /
+ * glyph_end cleared, glyph_count kept: text scenes scan it after) and the
+ * total record count. The scan's look-back wait gives up
  * after `poll_limit` polls (0: the renderer's limit, 2^22), and the call then
  * returns TK_E_TIMEOUT with the context still usable; this is the library's
  * bounded-wait failure path (the reference latches a failed submission on

@@ -83,6 +83,21 @@ int64_t tk_canvas_push_path(tk_canvas* c, const tk_path* path, const tk_brush_de
                             const double* transform, uint32_t fill_rule, double tolerance);
 int64_t tk_canvas_push_stroke(tk_canvas* c, const tk_path* path, const tk_brush_desc* brush,
                               double width, const double* transform, double tolerance);
+/* A rasterized glyph image (a glyph cache entry of the caller's text stack)
+ * for glyph runs: placement (the image covers x + left .. + width,
+ * y - top .. + height for a glyph at pen position (x, y)), size, content
+ * (TK_GLYPH_*) and width * height texels. The same texels with the same
+ * placement register once. Returns the image index, or -1. */
+int32_t tk_canvas_add_glyph_image(tk_canvas* c, int32_t left, int32_t top, uint32_t width, uint32_t height,
+                                  uint32_t content, const uint32_t* texels);
+/* Canvas::push_text_layout / push_text_layout_clipped
+ * (src/canvas/primitives/text.rs:11-100) after layout: `count` glyphs at pen
+ * positions in device pixels, drawn with `brush` as one glyph run. Its pixel
+ * bounds are the union of its glyph images, intersected with `clip` (x0, y0,
+ * x1, y1 in device pixels, or NULL); glyph runs take no transform. Returns
+ * the draw index, or -1 (no glyphs, an unknown image, or empty bounds). */
+int64_t tk_canvas_push_glyph_run(tk_canvas* c, const tk_glyph* glyphs, uint32_t count, const tk_brush_desc* brush,
+                                 const int32_t* clip);
 /* Canvas::push_text_layout_as_path (src/canvas/primitives/text.rs:107-147)
  * after shaping: `path` holds the glyph outlines of a laid-out text run (the
  * caller's shaping and outline extraction), filled nonzero with `brush` as a

@@ -18,6 +18,7 @@ LIB = HERE / "liboracle.so"
 OR_COUNTS, OR_BACKDROPS, OR_RANGES, OR_SEGMENTS = 0, 1, 2, 3
 OR_BATCH_PTCL, OR_BATCH_TILES, OR_BATCH_KINDS, OR_IMAGE = 4, 5, 6, 7
 OR_PASS_PTCL, OR_PASS_TILES, OR_PASS_KINDS, OR_PATHS, OR_BUMPS = 8, 9, 10, 11, 12
+OR_PASS_GLYPHS = 13
 
 _lib = None
 

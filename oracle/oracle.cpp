@@ -1068,6 +1068,9 @@ struct BatchStream {
     uint32_t batch;  // index into run's batch list
     uint32_t kind;   // kind | skip << 3
     std::vector<tk_ptcl_record> recs;  // reference stream including END
+    // glyph indices of the stream's PTCL_GLYPH records, whose segment
+    // ranges index this list (rebased onto the pass's glyph list on output)
+    std::vector<uint32_t> glyphs;
 };
 
 struct Batch {
@@ -1108,6 +1111,11 @@ struct or_scene {
     std::vector<tk_layer_record> layers;
     std::vector<uint32_t> brush, batch_ids;
     std::vector<uint32_t> sdf, shadow;  // Canvas::sdf_blob, sdf_shadow_blob
+    // the text blob
+    std::vector<tk_glyph_run> glyph_runs;
+    std::vector<tk_glyph> glyphs;
+    std::vector<tk_glyph_image> glyph_images;
+    std::vector<uint32_t> glyph_texels;
     uint32_t tw = 0, th = 0, T = 0;
     uint64_t B = 0, seg_capacity = 0;
     std::vector<int32_t> backdrops;
@@ -1283,12 +1291,55 @@ float sdf_coverage_from_draw(const or_scene& S, const tk_draw_record& d, float x
 struct Particle {
     bool valid = false;
     uint32_t tag = TK_PTCL_FILL, winding = 0, fill_rule = 0, seg0 = 0, seg1 = 0, color = 0;
+    std::vector<uint32_t> glyphs;  // PTCL_GLYPH: the run's glyphs that meet the tile
 };
+// glyph_hits_tile over a run (coarse/text.hlsli:8-35): the glyphs whose
+// image, a pixel wider each way, meets the tile under the draw transform
+// (transformed_rect_hits_tile, shared/draw.hlsli:52-61).
+void run_glyphs_in_tile(const or_scene& S, const tk_draw_record& d, uint32_t tx, uint32_t ty,
+                        std::vector<uint32_t>& out) {
+    const tk_glyph_run& run = S.glyph_runs[d.glyph_run_id];
+    const tk_affine& t = d.transform;
+    const float tlx = float(tx * TK_TILE_SIZE), tly = float(ty * TK_TILE_SIZE);
+    for (uint32_t k = run.first; k < run.first + run.count; ++k) {
+        const tk_glyph& g = S.glyphs[k];
+        if (g.image == TK_INVALID_INDEX) continue;
+        const tk_glyph_image& im = S.glyph_images[g.image];
+        if (im.width == 0u || im.height == 0u) continue;
+        const uint32_t lx = uint32_t(g.x) + uint32_t(im.left), ly = uint32_t(g.y) - uint32_t(im.top);
+        const float x[2] = {float(int32_t(lx - 1u)), float(int32_t(lx + im.width + 1u))};
+        const float y[2] = {float(int32_t(ly - 1u)), float(int32_t(ly + im.height + 1u))};
+        float lox = 0, loy = 0, hix = 0, hiy = 0;
+        // corners in the order rect.xy, rect.zy, rect.xw, rect.zw
+        const int order[4][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}};
+        float px[4], py[4];
+        for (int c = 0; c < 4; ++c) {
+            const float X = x[order[c][0]], Y = y[order[c][1]];
+            px[c] = t.a * X + t.c * Y + t.e;
+            py[c] = t.b * X + t.d * Y + t.f;
+        }
+        lox = fmin_(fmin_(px[0], px[1]), fmin_(px[2], px[3]));
+        loy = fmin_(fmin_(py[0], py[1]), fmin_(py[2], py[3]));
+        hix = fmax_(fmax_(px[0], px[1]), fmax_(px[2], px[3]));
+        hiy = fmax_(fmax_(py[0], py[1]), fmax_(py[2], py[3]));
+        if (lox < tlx + float(TK_TILE_SIZE) && loy < tly + float(TK_TILE_SIZE) && hix > tlx && hiy > tly)
+            out.push_back(k);
+    }
+}
 // coarse/emit_draw.hlsli:10-52 (path draws; coarse/paint.hlsli:14-21)
 Particle draw_particle(const or_scene& S, const Batch& b, uint32_t di, uint32_t tx, uint32_t ty) {
     Particle r;
     if (di >= S.batch_ids.size() || S.batch_ids[di] != b.batch_id) return r;
     const tk_draw_record& d = S.draws[di];
+    if (!S.glyph_runs.empty() && d.glyph_run_id != TK_INVALID_INDEX) {  // coarse/emit_draw.hlsli:15-22
+        if (d.tag == TK_DRAW_BRUSH) {
+            run_glyphs_in_tile(S, d, tx, ty, r.glyphs);
+            r.valid = !r.glyphs.empty();
+            r.tag = TK_PTCL_GLYPH;
+            r.color = di;
+        }
+        return r;
+    }
     if (has_sdf(d)) {  // coarse/emit_draw.hlsli:22-30
         if (d.tag == TK_DRAW_BRUSH && !sdf_stroke_empty(S, d, tx, ty)) {
             r.valid = true;
@@ -1375,6 +1426,7 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
     if (count == 0u) return false;
     count += wrappers * 2u + 1u;
     out.batch = bi;
+    out.glyphs.clear();
     out.recs.assign(count, tk_ptcl_record{});
     uint32_t p = 0;
     uint32_t flags = wrappers != 0u ? CHUNK_CLASS_OTHER : 0u;
@@ -1400,6 +1452,11 @@ bool coarse_tile(const or_scene& S, const Batch& b, uint32_t bi, uint32_t tile, 
             flags |= CHUNK_CLASS_SDF;
         else flags |= CHUNK_CLASS_OTHER;
         if (wrappers == 0u && q.tag == TK_PTCL_COLOR && (q.color >> 24) == 255u && p > 0u) flags |= CHUNK_CLASS_OCCLUDER;
+        if (q.tag == TK_PTCL_GLYPH) {
+            q.seg0 = uint32_t(out.glyphs.size());
+            out.glyphs.insert(out.glyphs.end(), q.glyphs.begin(), q.glyphs.end());
+            q.seg1 = uint32_t(out.glyphs.size());
+        }
         if (p < count) out.recs[p++] = {q.tag, int32_t(q.winding), q.fill_rule, q.seg0, q.seg1, q.color};
     }
     uint32_t q = p;
@@ -1513,11 +1570,129 @@ uint32_t src_over_mask_linear_auto_u8(uint32_t destination, uint32_t source, uin
     return src_over_subpixel_mask_f32(destination, source, corrected, corrected, corrected);
 }
 
+// fine/text/auto.hlsli:6-9
+void text_foreground(uint32_t source, float fg[3]) {
+    float alpha = float(source >> 24);
+    if (!(alpha > 0.0f)) {
+        fg[0] = fg[1] = fg[2] = 0.0f;
+        return;
+    }
+    for (int k = 0; k < 3; ++k) fg[k] = clampf(float((source >> (8 * k)) & 255u) / alpha, 0.0f, 1.0f);
+}
+// basic.hlsli:9-43
+uint32_t src_over_subpixel_mask_u8(uint32_t dst, uint32_t src, uint32_t mask, uint32_t clip) {
+    uint32_t sa = src >> 24;
+    if (sa == 0u || clip == 0u) return dst;
+    uint32_t m[3] = {combine_alpha(mask & 255u, clip), combine_alpha((mask >> 8) & 255u, clip),
+                     combine_alpha((mask >> 16) & 255u, clip)};
+    if ((dst >> 24) != 255u) {
+        uint32_t gray = (m[0] + m[1] + m[2] + 1u) / 3u;
+        m[0] = m[1] = m[2] = gray;
+    }
+    if (m[0] == 0u && m[1] == 0u && m[2] == 0u) return dst;
+    uint32_t cov[3], out[3];
+    for (int k = 0; k < 3; ++k) cov[k] = mul_div255(sa, m[k]);
+    uint32_t ca = std::max(std::max(cov[0], cov[1]), cov[2]);
+    for (int k = 0; k < 3; ++k)
+        out[k] = mul_div255((src >> (8 * k)) & 255u, m[k]) + mul_div255((dst >> (8 * k)) & 255u, 255u - cov[k]);
+    uint32_t a = ca + mul_div255((dst >> 24) & 255u, 255u - ca);
+    return pack(out[0], out[1], out[2], a);
+}
+// fine/glyph.hlsli:17-53: texels, the bilinear sample (lerp as a + t (b - a))
+// and the corrected sample
+uint32_t glyph_texel(const or_scene& S, const tk_glyph_image& im, int32_t x, int32_t y) {
+    if (x < 0 || y < 0 || x >= int32_t(im.width) || y >= int32_t(im.height)) return 0u;
+    return S.glyph_texels[size_t(im.data_offset) + size_t(y) * im.width + size_t(x)];
+}
+inline F4 lerp4(F4 a, F4 b, float t) {
+    return {a.r + t * (b.r - a.r), a.g + t * (b.g - a.g), a.b + t * (b.b - a.b), a.a + t * (b.a - a.a)};
+}
+uint32_t sample_glyph(const or_scene& S, const tk_glyph_image& im, float px, float py) {
+    int32_t bx = f2i(std::floor(px)), by = f2i(std::floor(py));
+    float fx = px - float(bx), fy = py - float(by);
+    uint32_t a = glyph_texel(S, im, bx, by);
+    if (fx == 0.0f && fy == 0.0f) return a;
+    F4 top = lerp4(rgba8_to_unorm(a), rgba8_to_unorm(glyph_texel(S, im, bx + 1, by)), fx);
+    F4 bottom = lerp4(rgba8_to_unorm(glyph_texel(S, im, bx, by + 1)), rgba8_to_unorm(glyph_texel(S, im, bx + 1, by + 1)),
+                      fx);
+    return unorm_to_rgba8(lerp4(top, bottom, fy));
+}
+void corrected_glyph_texel(uint32_t data, const float fg[3], bool lcd, float out[3]) {
+    if (!lcd) {
+        float alpha = text_correcting_coverage(data & 255u, (fg[0] * 0.2126f + fg[1] * 0.7152f) + fg[2] * 0.0722f);
+        out[0] = out[1] = out[2] = alpha;
+        return;
+    }
+    for (int k = 0; k < 3; ++k) out[k] = text_correcting_coverage((data >> (8 * k)) & 255u, fg[k]);
+}
+void sample_corrected_glyph(const or_scene& S, const tk_glyph_image& im, float px, float py, const float fg[3],
+                            bool lcd, float out[3]) {
+    int32_t bx = f2i(std::floor(px)), by = f2i(std::floor(py));
+    float fx = px - float(bx), fy = py - float(by);
+    float a[3], b[3], c[3], d[3];
+    corrected_glyph_texel(glyph_texel(S, im, bx, by), fg, lcd, a);
+    if (fx == 0.0f && fy == 0.0f) {
+        for (int k = 0; k < 3; ++k) out[k] = a[k];
+        return;
+    }
+    corrected_glyph_texel(glyph_texel(S, im, bx + 1, by), fg, lcd, b);
+    corrected_glyph_texel(glyph_texel(S, im, bx, by + 1), fg, lcd, c);
+    corrected_glyph_texel(glyph_texel(S, im, bx + 1, by + 1), fg, lcd, d);
+    for (int k = 0; k < 3; ++k) {
+        float top = a[k] + fx * (b[k] - a[k]);
+        float bottom = c[k] + fx * (d[k] - c[k]);
+        out[k] = top + fy * (bottom - top);
+    }
+}
+
 // --- fine/interpreter.hlsli:21-219 (clip stack and opacity groups) ------------
 struct Group { uint32_t kind; F4 parent; uint32_t parent_clip, layer_alpha, payload; };
 
+// composite_glyphs_at (fine/glyph.hlsli:55-111)
+F4 composite_glyphs_at(const or_scene& S, const Paint& P, F4 pixel, const uint32_t* list, uint32_t g0, uint32_t g1,
+                       const tk_draw_record& d, uint32_t gx, uint32_t gy, uint32_t clip) {
+    const tk_affine& m = d.inverse_transform;
+    const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
+    const float lx = mad(m.a, sx, mad(m.c, sy, m.e)) - 0.5f;
+    const float ly = mad(m.b, sx, mad(m.d, sy, m.f)) - 0.5f;
+    for (uint32_t g = g0; g < g1; ++g) {
+        const tk_glyph& glyph = S.glyphs[list[g]];
+        if (glyph.image == TK_INVALID_INDEX) continue;
+        const tk_glyph_image& im = S.glyph_images[glyph.image];
+        const int32_t x0 = int32_t(uint32_t(glyph.x) + uint32_t(im.left));
+        const int32_t y0 = int32_t(uint32_t(glyph.y) - uint32_t(im.top));
+        const float ux = lx - float(x0), uy = ly - float(y0);
+        if (!(ux > -1.0f && uy > -1.0f && ux < float(int32_t(im.width)) && uy < float(int32_t(im.height)))) continue;
+        const uint32_t content = im.content;
+        if (content == TK_GLYPH_LINEAR_MASK || content == TK_GLYPH_LINEAR_SUBPIXEL_MASK) {
+            const uint32_t color = sample_draw_brush(P, d, sx, sy);
+            float fg[3], cov[3];
+            text_foreground(color, fg);
+            sample_corrected_glyph(S, im, ux, uy, fg, content == TK_GLYPH_LINEAR_SUBPIXEL_MASK, cov);
+            const float k = float(clip) * (1.0f / 255.0f);
+            pixel = rgba8_to_unorm(
+                src_over_subpixel_mask_f32(unorm_to_rgba8(pixel), color, cov[0] * k, cov[1] * k, cov[2] * k));
+        } else {
+            const uint32_t data = sample_glyph(S, im, ux, uy);
+            if (content == TK_GLYPH_MASK) {
+                const uint32_t alpha = combine_alpha(data, clip);
+                if (alpha != 0u)
+                    pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(sample_draw_brush(P, d, sx, sy), alpha));
+            } else if (content == TK_GLYPH_COLOR) {
+                pixel = src_over_premul_unorm(pixel, scale_premul_u8_to_unorm(data, clip));
+            } else if (content == TK_GLYPH_LINEAR_COLOR) {
+                pixel = rgba8_to_unorm(src_over_mask_linear_auto_u8(unorm_to_rgba8(pixel), data, clip));
+            } else if (content == TK_GLYPH_SUBPIXEL_MASK) {
+                pixel = rgba8_to_unorm(
+                    src_over_subpixel_mask_u8(unorm_to_rgba8(pixel), sample_draw_brush(P, d, sx, sy), data, clip));
+            }
+        }
+    }
+    return pixel;
+}
+
 F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_t begin, uint32_t end, F4 pixel,
-             uint32_t lx, uint32_t ly, uint32_t gx, uint32_t gy) {
+             uint32_t lx, uint32_t ly, uint32_t gx, uint32_t gy, const uint32_t* glyph_list = nullptr) {
     Paint P{S.brush.data(), S.brush.size(), S.desc.images, S.desc.image_count};
     uint32_t clip_mask = 255u;
     std::vector<uint32_t> clip_stack;
@@ -1550,6 +1725,13 @@ F4 interpret(const or_scene& S, const std::vector<tk_ptcl_record>& recs, uint32_
                 alpha = coverage_to_u8(sdf_coverage_from_draw(S, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f));
             clip_stack.push_back(parent);
             clip_mask = combine_alpha(parent, alpha);
+        } else if (tag == TK_PTCL_GLYPH) {  // fine/interpreter.hlsli:93-106
+            const tk_draw_record& d = S.draws[r.color];
+            const int32_t x = int32_t(gx), y = int32_t(gy);
+            if (clip_mask != 0u && glyph_list && x >= d.pixel_bounds.x0 && y >= d.pixel_bounds.y0 &&
+                x < d.pixel_bounds.x1 && y < d.pixel_bounds.y1)
+                pixel = composite_glyphs_at(S, P, pixel, glyph_list, r.segment_start, r.segment_end, d, gx, gy,
+                                            clip_mask);
         } else if (tag == TK_PTCL_IMAGE) {  // fine/interpreter.hlsli:65-69
             if (clip_mask != 0u) {
                 uint32_t color = sample_draw_brush(P, S.draws[r.color], float(gx) + 0.5f, float(gy) + 0.5f);
@@ -1843,7 +2025,8 @@ void fine_pass(or_scene& S, uint32_t pass, std::vector<uint32_t>& target, int th
                     uint32_t kind = bs.kind & TK_TILE_KIND_MASK;
                     uint32_t begin = bs.kind >> TK_TILE_PREFIX_SHIFT;
                     uint32_t end = uint32_t(bs.recs.size());
-                    if (kind == TK_TILE_KIND_INTERPRETER) pixel = interpret(S, bs.recs, begin, end, pixel, lx, ly, gx, gy);
+                    if (kind == TK_TILE_KIND_INTERPRETER)
+                        pixel = interpret(S, bs.recs, begin, end, pixel, lx, ly, gx, gy, bs.glyphs.data());
                     else if (kind == TK_TILE_KIND_COLOR) pixel = color_only(bs.recs, begin, end, pixel);
                     else if (kind == TK_TILE_KIND_SDF || kind == TK_TILE_KIND_MIXED)
                         pixel = analytic_solid(S, bs.recs, begin, end, pixel, gx, gy);
@@ -2098,6 +2281,19 @@ extern "C" {
 
 const char* or_error(void) { return g_error.c_str(); }
 
+}  // extern "C"
+
+namespace {
+void copy_text(or_scene& S, const tk_scene_desc* d) {
+    S.glyph_runs.assign(d->glyph_runs, d->glyph_runs + d->glyph_run_count);
+    S.glyphs.assign(d->glyphs, d->glyphs + d->glyph_count);
+    S.glyph_images.assign(d->glyph_images, d->glyph_images + d->glyph_image_count);
+    S.glyph_texels.assign(d->glyph_texels, d->glyph_texels + d->glyph_texel_count);
+}
+}  // namespace
+
+extern "C" {
+
 int32_t or_run(const tk_scene_desc* d, int32_t threads, uint32_t tile_y0, uint32_t tile_y1, or_scene** out) {
     *out = nullptr;
     try {
@@ -2110,6 +2306,7 @@ int32_t or_run(const tk_scene_desc* d, int32_t threads, uint32_t tile_y0, uint32
         S->sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
         S->shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
         S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        copy_text(*S, d);
         S->ty0 = tile_y0;
         S->ty1 = tile_y1;
         scan_scene(*S, threads < 1 ? 1 : threads);
@@ -2134,6 +2331,7 @@ int32_t or_prepare(const tk_scene_desc* d, int32_t threads, or_scene** out) {
         S->sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
         S->shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
         S->batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        copy_text(*S, d);
         scan_scene(*S, threads < 1 ? 1 : threads);
         *out = S;
         return 0;
@@ -2202,7 +2400,8 @@ size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_
         }
         case OR_PASS_PTCL:
         case OR_PASS_TILES:
-        case OR_PASS_KINDS: {
+        case OR_PASS_KINDS:
+        case OR_PASS_GLYPHS: {
             // Merged layout: per tile, for each batch with a stream:
             // BATCH_BEGIN{segment_start=batch_id, segment_end=n-1, color=kind}
             // followed by the batch's records without END; then one END.
@@ -2211,13 +2410,23 @@ size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_
             std::vector<tk_ptcl_record> ptcl;
             std::vector<tk_tile_record> tiles(s->T, tk_tile_record{0, 0, 0, 0, 0, 0});
             std::vector<uint32_t> kinds(s->T, TK_TILE_KIND_EMPTY);
+            std::vector<uint32_t> glyphs;  // the pass's glyph list: tile after tile, stream after stream
             uint32_t next = 0;
             for (uint32_t t = 0; t < s->T; ++t) {
                 uint32_t n = 0;
+                const uint32_t g0 = uint32_t(glyphs.size());
                 for (const auto& bs : streams[t]) {
                     uint32_t m = uint32_t(bs.recs.size());
                     ptcl.push_back({TK_PTCL_BATCH_BEGIN, 0, 0u, s->batches[bs.batch].batch_id, m - 1u, bs.kind});
+                    const size_t first = ptcl.size();
                     ptcl.insert(ptcl.end(), bs.recs.begin(), bs.recs.end() - 1);
+                    const uint32_t base = uint32_t(glyphs.size());
+                    for (size_t k = first; k < ptcl.size(); ++k)
+                        if (ptcl[k].tag == TK_PTCL_GLYPH) {
+                            ptcl[k].segment_start += base;
+                            ptcl[k].segment_end += base;
+                        }
+                    glyphs.insert(glyphs.end(), bs.glyphs.begin(), bs.glyphs.end());
                     n += m;
                 }
                 if (n) {
@@ -2225,9 +2434,11 @@ size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_
                     n += 1;
                     kinds[t] = TK_TILE_KIND_INTERPRETER;
                 }
-                tiles[t] = {n, next, next + n, 0, 0, 0};
+                const uint32_t gn = uint32_t(glyphs.size()) - g0;
+                tiles[t] = {n, next, next + n, gn, s->glyph_runs.empty() ? 0u : g0, s->glyph_runs.empty() ? 0u : g0 + gn};
                 next += n;
             }
+            if (what == OR_PASS_GLYPHS) return copy_out(glyphs.data(), glyphs.size() * 4, dst, bytes);
             if (what == OR_PASS_PTCL) return copy_out(ptcl.data(), ptcl.size() * sizeof(tk_ptcl_record), dst, bytes);
             if (what == OR_PASS_TILES) return copy_out(tiles.data(), tiles.size() * sizeof(tk_tile_record), dst, bytes);
             return copy_out(kinds.data(), kinds.size() * 4, dst, bytes);
@@ -2398,6 +2609,7 @@ int32_t or_interpret_path_draws(const tk_scene_desc* d, int32_t threads, uint32_
         S.sdf.assign(d->sdf_blob, d->sdf_blob + d->sdf_word_count);
         S.shadow.assign(d->sdf_shadow_blob, d->sdf_shadow_blob + d->sdf_shadow_word_count);
         S.batch_ids.assign(d->draw_batch_ids, d->draw_batch_ids + d->draw_count);
+        copy_text(S, d);
         threads = threads < 1 ? 1 : threads;
         scan_scene(S, threads);
         const uint32_t W = d->width, H = d->height;
@@ -2432,8 +2644,16 @@ int32_t or_interpret_path_draws(const tk_scene_desc* d, int32_t threads, uint32_
                     const uint32_t tag = L.tag == TK_LAYER_OPACITY ? TK_PTCL_BEGIN_OPACITY : TK_PTCL_BEGIN_CLIP;
                     recs.push_back({tag, w, dr.fill_rule, s0, s1, L.payload});
                 }
+                std::vector<uint32_t> glyphs;  // every glyph of every run, in every tile
                 for (uint32_t di : draws) {
                     const tk_draw_record& dr = S.draws[di];
+                    if (!S.glyph_runs.empty() && dr.glyph_run_id != TK_INVALID_INDEX) {
+                        const tk_glyph_run& run = S.glyph_runs[dr.glyph_run_id];
+                        const uint32_t g0 = uint32_t(glyphs.size());
+                        for (uint32_t k = run.first; k < run.first + run.count; ++k) glyphs.push_back(k);
+                        recs.push_back({TK_PTCL_GLYPH, 0, 0u, g0, uint32_t(glyphs.size()), di});
+                        continue;
+                    }
                     if (has_sdf(dr)) {
                         recs.push_back({TK_PTCL_SDF, 0, 0u, di, 0u, di});
                         continue;
@@ -2456,7 +2676,7 @@ int32_t or_interpret_path_draws(const tk_scene_desc* d, int32_t threads, uint32_
                         const uint32_t gx = tx * TK_TILE_SIZE + lx;
                         if (gx >= W) break;
                         uint32_t& texel = image[size_t(gy) * W + gx];
-                        texel = texel_store(interpret(S, recs, 0u, n, texel_load(texel), lx, ly, gx, gy));
+                        texel = texel_store(interpret(S, recs, 0u, n, texel_load(texel), lx, ly, gx, gy, glyphs.data()));
                     }
                 }
             });

@@ -75,6 +75,7 @@ int32_t or_raster(or_scene* s, int32_t threads, uint32_t tile_y0, uint32_t tile_
 #define OR_PASS_KINDS 10u  /* u32[T] of target pass `index` */
 #define OR_PATHS 11u       /* tk_path_record[P] as used */
 #define OR_BUMPS 12u       /* u32[P] per-path segment totals */
+#define OR_PASS_GLYPHS 13u /* u32[] glyph list of target pass `index` */
 size_t or_get(const or_scene* s, uint32_t what, uint32_t index, void* dst, size_t bytes);
 /* Elements [first, first + count) of OR_COUNTS, OR_BACKDROPS, OR_RANGES,
  * OR_SEGMENTS, OR_IMAGE or OR_BUMPS (count clipped); returns the array's

@@ -34,14 +34,17 @@ def tiles_with_counts(n, seed):
 @pytest.mark.parametrize("n", [0, 1, 4095, 4096, 4097, 70001])
 def test_gpu_tile_prefix_harness_matches_exclusive_scan(renderer, n):
     """coarse/prefix.hlsl:11-63: ptcl_start is the exclusive prefix of
-    ptcl_count, ptcl_end = start + count, the glyph words are cleared."""
+    ptcl_count, ptcl_end = start + count; this is the PTCL component of the
+    scan, so glyph_count stays as given and the glyph range is cleared (text
+    scenes run the glyph component after it)."""
     t = tiles_with_counts(n, n)
     got, total = renderer.stage_tile_prefix(t)
     excl = np.concatenate([[0], np.cumsum(t["ptcl_count"].astype(np.uint64))[:-1]]) if n else np.zeros(0)
     assert np.array_equal(got["ptcl_count"], t["ptcl_count"])
     assert np.array_equal(got["ptcl_start"], excl.astype(np.uint32))
     assert np.array_equal(got["ptcl_end"], (excl + t["ptcl_count"]).astype(np.uint32))
-    assert not got["glyph_count"].any() and not got["glyph_start"].any() and not got["glyph_end"].any()
+    assert np.array_equal(got["glyph_count"], t["glyph_count"])
+    assert not got["glyph_start"].any() and not got["glyph_end"].any()
     assert total == int(t["ptcl_count"].astype(np.uint64).sum())
 
 

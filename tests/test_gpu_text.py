@@ -1,9 +1,14 @@
-"""Glyph outline fills (DrawTag::PathGlyph -> PTCL_PATH_GLYPH) on the GPU:
-coverage as a fill, composited by src_over_mask_linear_auto_u8
-(fine/interpreter.hlsli:205-206, fine/text/auto.hlsli:28-33), bit-exact
-against the oracle at every stage and against the fine-only oracle, with
-solid and gradient brushes, translucent text, clip layers, text beside SDF
-shapes (the SDF kernel instance) and the C3 glyph workload."""
+"""Text on the GPU, bit-exact against the oracle at every stage and against
+the fine-only oracle:
+
+* glyph outline fills (DrawTag::PathGlyph -> PTCL_PATH_GLYPH): coverage as a
+  fill, composited by src_over_mask_linear_auto_u8 (fine/interpreter.hlsli:
+  205-206, fine/text/auto.hlsli:28-33), with solid and gradient brushes,
+  translucent text, clip layers and text beside SDF shapes (the SDF kernel
+  instance);
+* glyph runs (PTCL_GLYPH): coarse glyph lists per tile (coarse/text.hlsli),
+  fine composite_glyphs_at over glyph images of all six contents
+  (fine/glyph.hlsli), clipped runs, runs under clip layers."""
 from __future__ import annotations
 
 import numpy as np
@@ -14,42 +19,9 @@ import tileink_b200 as tk
 from tileink_b200 import _native as N
 
 from test_gpu_parity import compare_frame
+from text_cases import glyph_run_scene, glyph_scene
 
 pytestmark = pytest.mark.gpu
-
-
-def glyph_scene(seed, width=320, height=200, runs=40, sdf=False, clip=False):
-    rng = np.random.default_rng(seed)
-    c = tk.Canvas(width, height)
-    c.set_clear_color(int(rng.choice([0xFFFFFFFF, 0xFF202020, 0x00000000, 0xFF3366CC])))
-    if clip:
-        c.push_clip_layer(tk.BezPath().move_to(10, 5).line_to(width - 20, 15).line_to(width - 5, height - 10)
-                          .line_to(15, height - 25).close())
-    for k in range(runs):
-        x, y = rng.uniform(0, width - 40), rng.uniform(20, height)
-        em = rng.uniform(6, 48)
-        p = tk.BezPath()
-        for g in range(int(rng.integers(1, 4))):  # a few glyph contours per run
-            gx = x + g * 0.7 * em
-            p.move_to(gx, y)
-            p.quad_to(gx + 0.3 * em, y - 1.1 * em, gx + 0.6 * em, y)
-            p.line_to(gx + 0.45 * em, y)
-            p.quad_to(gx + 0.3 * em, y - 0.6 * em, gx + 0.15 * em, y)
-            p.close()
-        kind = rng.uniform()
-        if kind < 0.5:
-            b = tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.choice([1.0, rng.uniform(0.2, 1.0)])))
-        elif kind < 0.8:
-            b = tk.Brush.linear((x, y - em), (x + 2 * em, y), [(0.0, (1, 0, 0, 1)), (1.0, (0, 0, 1, 0.7))])
-        else:
-            b = tk.Brush.radial((x + em, y - em / 2), 1.0, (x + em, y - em / 2), 1.5 * em,
-                                [(0.0, (1, 1, 1, 1)), (0.6, (0.2, 0.8, 0.3, 1)), (1.0, (0, 0, 0, 0.5))])
-        c.push_glyph_outlines(p, b)
-        if sdf and k % 5 == 0:
-            c.push_rect(x, y - em, x + em, y, tk.Brush.solid(0.9, 0.6, 0.1, 0.6), radius=2.0)
-    if clip:
-        c.pop_layer()
-    return c
 
 
 @pytest.mark.parametrize("seed, sdf, clip", [(1, False, False), (2, False, True), (3, True, False), (4, True, True)])
@@ -73,3 +45,50 @@ def test_gpu_glyph_outlines_differ_from_plain_fills_only_at_edges(renderer):
     fills = renderer.render_to_image(N.ArrayScene(a2)).copy()
     differ = (glyphs != fills).any(axis=2)
     assert differ.any() and differ.mean() < 0.25
+
+
+@pytest.mark.parametrize("seed, clip, outlines", [(1, False, False), (2, True, False), (3, False, True), (4, True, True)])
+def test_gpu_glyph_runs_match_oracle(renderer, seed, clip, outlines):
+    c = glyph_run_scene(seed, clip=clip, outlines=outlines)
+    img, ref = compare_frame(renderer, c)
+    assert np.array_equal(renderer.debug(N.STAGE_GLYPHS, 0), ref.get(oracle.OR_PASS_GLYPHS, np.uint32, 0))
+    tags = renderer.debug(N.STAGE_PTCL, 0)["tag"]
+    assert (tags == N.PTCL_GLYPH).sum() > 20
+    tiles = renderer.debug(N.STAGE_TILES, 0)
+    assert tiles["glyph_count"].sum() == len(renderer.debug(N.STAGE_GLYPHS, 0)) > 0
+    want = oracle.interpret_path_draws(c.scene_desc(), threads=8)
+    assert np.array_equal(img, want), int((img != want).any(axis=2).sum())
+
+
+@pytest.mark.parametrize("content", range(6))
+def test_gpu_glyph_run_contents(renderer, content):
+    c = glyph_run_scene(10 + content, contents=[content], runs=30)
+    img, _ = compare_frame(renderer, c)
+    want = oracle.interpret_path_draws(c.scene_desc(), threads=8)
+    assert np.array_equal(img, want)
+
+
+def test_gpu_glyph_runs_in_incremental_frames(renderer):
+    """Damage-driven frames of a text scene equal full frames (the glyph
+    lists of the redrawn tiles only)."""
+    c = glyph_run_scene(21, runs=30)
+    renderer.upload(c)
+    renderer.render_incremental(None)
+    full = renderer.readback().copy()
+    st = renderer.render_incremental({"full": False, "rects": [[20, 10, 140, 90]]})
+    assert st["full_redraw"] == 0
+    assert np.array_equal(renderer.readback(), full)
+
+
+def test_gpu_rejects_bad_glyph_runs(renderer):
+    c = glyph_run_scene(5, runs=6)
+    a = c.scene_arrays()
+    bad = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in a.items()}
+    bad["glyphs"]["image"][0] = len(a["glyph_images"]) + 3
+    with pytest.raises(tk.TileinkError):
+        renderer.upload(N.ArrayScene(bad))
+    bad = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in a.items()}
+    bad["glyph_images"]["data_offset"][0] = len(a["glyph_texels"])
+    with pytest.raises(tk.TileinkError):
+        renderer.upload(N.ArrayScene(bad))
+    renderer.render_to_image(c)  # the context stays usable

@@ -165,10 +165,65 @@ def test_oracle_glyph_pipeline_equals_fine_only(seed, sdf, clip):
     """Coarse for glyph outline draws, pinned by the fine-only method
     (src/native/runtime/tests/coarse_count/rect_pixels.rs:3-14): every draw
     as a particle in every tile of its bbox gives the pipeline's image."""
-    from test_gpu_text import glyph_scene
+    from text_cases import glyph_scene
     c = glyph_scene(seed, sdf=sdf, clip=clip)
     d = c.scene_desc()
     run = oracle.OracleRun(d, threads=4)
     img = run.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(d.height, d.width, 4)
     assert (run.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0)["tag"] == N.PTCL_PATH_GLYPH).sum() > 50
     assert np.array_equal(img, oracle.interpret_path_draws(d, threads=4))
+
+
+@pytest.mark.parametrize("seed, clip, outlines", [(1, False, False), (2, True, True)])
+def test_oracle_glyph_run_pipeline_equals_fine_only(seed, clip, outlines):
+    """Coarse glyph lists (coarse/text.hlsli: a glyph enters a tile's list when
+    its image, a pixel wider, meets the tile) pinned by the fine-only method:
+    every glyph of every run in every tile gives the same image."""
+    from text_cases import glyph_run_scene
+    c = glyph_run_scene(seed, clip=clip, outlines=outlines)
+    d = c.scene_desc()
+    run = oracle.OracleRun(d, threads=4)
+    img = run.get(oracle.OR_IMAGE, np.uint32).view(np.uint8).reshape(d.height, d.width, 4)
+    ptcl = run.get(oracle.OR_PASS_PTCL, N.PTCL_DTYPE, 0)
+    glyphs = run.get(oracle.OR_PASS_GLYPHS, np.uint32, 0)
+    tiles = run.get(oracle.OR_PASS_TILES, N.TILE_DTYPE, 0)
+    g = ptcl[ptcl["tag"] == N.PTCL_GLYPH]
+    assert len(g) > 20 and (g["segment_end"] > g["segment_start"]).all()
+    assert tiles["glyph_count"].sum() == len(glyphs) and tiles["glyph_end"][-1] == len(glyphs)
+    assert not np.array_equal(img, np.full_like(img, 0))
+    assert np.array_equal(img, oracle.interpret_path_draws(d, threads=4))
+
+
+def test_glyph_run_records():
+    """push_text_layout's draw record (src/canvas/primitives/text.rs:80-96):
+    a brush draw with no path, the run's glyphs and bounds from its images."""
+    c = tk.Canvas(64, 48)
+    im = c.add_glyph_image(1, 10, np.full((12, 6), 255, np.uint32), N.GLYPH_MASK)
+    assert c.add_glyph_image(1, 10, np.full((12, 6), 255, np.uint32), N.GLYPH_MASK) == im + 1  # other texels
+    d = c.push_glyph_run([(im, 10, 30), (None, 20, 30), (im, 30, 32)], tk.Brush.solid(0, 0, 0, 1))
+    a = c.scene_arrays()
+    r = a["draws"][d]
+    assert r["path_id"] == N.INVALID and r["glyph_run_id"] == 0 and r["tag"] == N.DRAW_BRUSH
+    assert tuple(r["pixel_bounds"]) == (11, 20, 37, 34)
+    assert list(a["glyph_runs"][0]) == [0, 3]
+    assert a["glyphs"]["image"][1] == N.INVALID
+    d2 = c.push_glyph_run([(im, 10, 30)], tk.Brush.solid(0, 0, 0, 1), clip=(0, 0, 14, 100))
+    assert tuple(c.scene_arrays()["draws"][d2]["pixel_bounds"]) == (11, 20, 14, 32)
+    with pytest.raises(ValueError):
+        c.push_glyph_run([(im, 10, 30)], tk.Brush.solid(0, 0, 0, 1), clip=(40, 0, 50, 10))
+    with pytest.raises(ValueError):
+        c.push_glyph_run([(im + 5, 10, 30)], tk.Brush.solid(0, 0, 0, 1))
+
+
+def test_retained_replay_moves_glyph_runs_by_whole_pixels():
+    c = tk.Canvas(64, 48)
+    c.keep_commands()
+    im = c.add_glyph_image(0, 8, np.full((8, 5), 200, np.uint32), N.GLYPH_MASK)
+    c.push_glyph_run([(im, 4, 20), (im, 10, 20)], tk.Brush.solid(0, 0, 0, 1))
+    rs = tk.RetainedScene(64, 48)
+    rs.insert(1, c)
+    rs.set_transform(1, (1, 0, 0, 1, 7, 3))
+    m, _ = rs.materialize()
+    a = m.scene_arrays()
+    assert list(a["glyphs"]["x"]) == [11, 17] and list(a["glyphs"]["y"]) == [23, 23]
+    assert len(a["glyph_images"]) == 1 and len(a["glyph_texels"]) == 40

@@ -85,6 +85,15 @@ TILE_DTYPE = np.dtype([(k, "<u4") for k in ("ptcl_count", "ptcl_start", "ptcl_en
                                             "glyph_start", "glyph_end")])
 OP_DTYPE = np.dtype([("kind", "<u4"), ("batch_id", "<u4"), ("layer_start", "<u4"), ("layer_end", "<u4"),
                      ("sigma", "<f4"), ("bounds", "<i4", 4)])
+# the text blob (tk_glyph_run, tk_glyph, tk_glyph_image; draw_records.hlsli:19-21)
+GLYPH_RUN_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4")])
+GLYPH_DTYPE = np.dtype([("image", "<u4"), ("x", "<i4"), ("y", "<i4")])
+GLYPH_IMAGE_DTYPE = np.dtype([("left", "<i4"), ("top", "<i4"), ("width", "<u4"), ("height", "<u4"),
+                              ("content", "<u4"), ("data_offset", "<u4")])
+GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
+GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
+PTCL_GLYPH = 10
+STAGE_GLYPHS = 10
 EL_LINE, EL_QUAD, EL_CUBIC, EL_MOVE = 1, 2, 3, 4
 FLATTEN_EL_DTYPE = np.dtype([("verb", "<u4"), ("path", "<u4"), ("tolerance", "<f8"), ("p", "<f8", (4, 2))])
 POLYLINE_DTYPE = np.dtype([("stroke", "<u4"), ("element0", "<u4"), ("element_count", "<u4"), ("closed", "<u4")])
@@ -94,6 +103,7 @@ assert FLATTEN_EL_DTYPE.itemsize == 80 and POLYLINE_DTYPE.itemsize == 16 and STR
 assert LINE_DTYPE.itemsize == 24 and PATH_DTYPE.itemsize == 76 and DRAW_DTYPE.itemsize == 124
 assert LAYER_DTYPE.itemsize == 12 and PTCL_DTYPE.itemsize == 24 and SEGMENT_DTYPE.itemsize == 20
 assert TILE_DTYPE.itemsize == 24 and OP_DTYPE.itemsize == 36
+assert GLYPH_RUN_DTYPE.itemsize == 8 and GLYPH_DTYPE.itemsize == 12 and GLYPH_IMAGE_DTYPE.itemsize == 24
 
 
 class SceneDesc(C.Structure):
@@ -110,6 +120,9 @@ class SceneDesc(C.Structure):
         ("sdf_blob", C.c_void_p), ("sdf_word_count", C.c_uint64),
         ("sdf_shadow_blob", C.c_void_p), ("sdf_shadow_word_count", C.c_uint64),
         ("images", C.c_void_p), ("image_count", C.c_uint32), ("image_reserved", C.c_uint32),
+        ("glyph_runs", C.c_void_p), ("glyphs", C.c_void_p), ("glyph_images", C.c_void_p),
+        ("glyph_texels", C.c_void_p), ("glyph_run_count", C.c_uint32), ("glyph_count", C.c_uint32),
+        ("glyph_image_count", C.c_uint32), ("glyph_reserved", C.c_uint32), ("glyph_texel_count", C.c_uint64),
     ]
 
 
@@ -278,6 +291,8 @@ def library() -> C.CDLL:
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),
+        "tk_canvas_add_glyph_image": (I32, [P, C.c_int32, C.c_int32, U32, U32, U32, P]),
+        "tk_canvas_push_glyph_run": (I64, [P, P, U32, C.POINTER(BrushDesc), P]),
         "tk_canvas_push_image": (C.c_int64, [P, C.POINTER(C.c_double), U32, U32, U32, U32]),
         "tk_canvas_push_clip_layer": (I32, [P, P, P, U32, F64]),
         "tk_canvas_push_opacity_layer": (I32, [P, P, P, F64, F32]),
@@ -339,6 +354,10 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "sdf_shadow": arr(d.sdf_shadow_blob, d.sdf_shadow_word_count, np.uint32),
         "images": [arr(im.premul_rgba8, im.width * im.height, np.uint32).reshape(im.height, im.width)
                    for im in (C.cast(d.images, C.POINTER(ImageDesc))[k] for k in range(d.image_count))],
+        "glyph_runs": arr(d.glyph_runs, d.glyph_run_count, GLYPH_RUN_DTYPE),
+        "glyphs": arr(d.glyphs, d.glyph_count, GLYPH_DTYPE),
+        "glyph_images": arr(d.glyph_images, d.glyph_image_count, GLYPH_IMAGE_DTYPE),
+        "glyph_texels": arr(d.glyph_texels, d.glyph_texel_count, np.uint32),
     }
 
 
@@ -363,6 +382,12 @@ class ArrayScene:
             d.sdf_blob, d.sdf_word_count = ptr(sdf), len(sdf)
         if shadow is not None and len(shadow):
             d.sdf_shadow_blob, d.sdf_shadow_word_count = ptr(shadow), len(shadow)
+        for key, cnt in (("glyph_runs", "glyph_run_count"), ("glyphs", "glyph_count"),
+                         ("glyph_images", "glyph_image_count"), ("glyph_texels", "glyph_texel_count")):
+            v = a.get(key)
+            if v is not None and len(v):
+                setattr(d, key, ptr(v))
+                setattr(d, cnt, len(v))
         images = [np.ascontiguousarray(im, dtype=np.uint32) for im in a.get("images", [])]
         if images:
             self._images = images

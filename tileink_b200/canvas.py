@@ -261,6 +261,32 @@ class Canvas:
             raise ValueError(f"empty image, or a side above {N.MAX_IMAGE_DIMENSION} texels")
         return r
 
+    def add_glyph_image(self, left: int, top: int, texels, content=N.GLYPH_MASK) -> int:
+        """Registers a rasterized glyph image: (H, W) uint32 texels (masks:
+        coverage in the low byte; subpixel masks: r, g, b coverages; colour
+        glyphs: premultiplied RGBA8), placed at pen + (left, -top)."""
+        im = np.ascontiguousarray(texels, dtype=np.uint32)
+        if im.ndim != 2:
+            raise ValueError("glyph texels must be a (height, width) uint32 array")
+        r = self._lib.tk_canvas_add_glyph_image(self._h, int(left), int(top), im.shape[1], im.shape[0], int(content),
+                                                im.ctypes.data)
+        if r < 0:
+            raise ValueError("bad glyph image")
+        return r
+
+    def push_glyph_run(self, glyphs, brush: Brush, clip=None) -> int:
+        """Canvas::push_text_layout(_clipped) after layout: glyphs as (image,
+        x, y) rows (pen positions in device pixels), one glyph run draw."""
+        g = np.zeros(len(glyphs), dtype=N.GLYPH_DTYPE)
+        for k, (image, x, y) in enumerate(glyphs):
+            g[k] = (N.INVALID if image is None else int(image), int(x), int(y))
+        d, keep = brush._desc()
+        cl = None if clip is None else (C.c_int32 * 4)(*[int(v) for v in clip])
+        r = self._lib.tk_canvas_push_glyph_run(self._h, g.ctypes.data, len(g), C.byref(d), cl)
+        if r < 0:
+            raise ValueError("push_glyph_run rejected the run")
+        return r
+
     def push_image(self, x0, y0, x1, y1, image: int, extend=EXTEND_PAD, sampling=N.PATTERN_NEAREST, opacity=255):
         """Canvas::push_image: registered image `image` scaled into the rect
         (x0, y0)-(x1, y1) with extend EXTEND_* and sampling PATTERN_*."""

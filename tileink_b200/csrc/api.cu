@@ -86,6 +86,8 @@ struct Pass {
     DBuf<tk_ptcl_record> ptcl;
     uint64_t ptcl_needed = 0;  // known after the first frame, 0 = unknown
     uint64_t ptcl_used = 0;
+    DBuf<uint32_t> glyph_list;  // text scenes: the glyph indices PTCL_GLYPH records name
+    uint64_t glyph_needed = 0, glyph_used = 0;
 };
 
 enum StepKind { STEP_PASS, STEP_BLUR_BEGIN, STEP_BLUR_END };
@@ -142,11 +144,19 @@ struct tk_ctx {
     DBuf<uint32_t> brush, sdf, batch_ids, order;
     DBuf<uint32_t> texels;  // the scene's images, concatenated
     DBuf<uint4> image_tab;  // per image: first texel, width, height
+    // the text blob (glyph runs)
+    uint32_t glyph_run_count = 0;
+    DBuf<tk_glyph_run> glyph_runs;
+    DBuf<tk_glyph> glyphs;
+    DBuf<tk_glyph_image> glyph_images;
+    DBuf<uint32_t> glyph_texels;
     DBuf<tk_layer_record> layers;
     DBuf<tk::ScanItem> items;
     DBuf<unsigned long long> item_desc, tile_desc, stats;
     DBuf<int32_t> backdrops;
-    DBuf<uint32_t> counts, cursors, bumps, misc;  // misc: [0] error [1] ticket [2] seg total [3] ptcl total
+    // misc: [0] error [1] ticket [2] seg total [3] ptcl total [4] emit ticket
+    // [5] delta total check [6] glyph list total
+    DBuf<uint32_t> counts, cursors, bumps, misc;
     DBuf<tk_segment_range> ranges;
     DBuf<tk::SegmentRec> segments;
     DBuf<tk::PaintInfo> paints;  // per draw, built at upload
@@ -289,13 +299,38 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         texel_words += uint64_t(im.width) * im.height;
     }
     if (texel_words > 0xFFFFFFFFull) invalid("images exceed u32 indexing");
+    // the text blob: runs inside the glyphs, glyphs naming images, images
+    // inside the texels
+    if ((d.glyph_run_count && !d.glyph_runs) || (d.glyph_count && !d.glyphs) ||
+        (d.glyph_image_count && !d.glyph_images) || (d.glyph_texel_count && !d.glyph_texels))
+        invalid("null text blob array with nonzero count");
+    if (d.glyph_texel_count > 0xFFFFFFFFull) invalid("glyph texels exceed u32 indexing");
+    for (uint32_t k = 0; k < d.glyph_run_count; ++k)
+        if (uint64_t(d.glyph_runs[k].first) + d.glyph_runs[k].count > d.glyph_count)
+            invalid("glyph run " + std::to_string(k) + " outside the glyphs");
+    for (uint32_t k = 0; k < d.glyph_count; ++k)
+        if (d.glyphs[k].image != TK_INVALID_INDEX && d.glyphs[k].image >= d.glyph_image_count)
+            invalid("glyph " + std::to_string(k) + ": image out of range");
+    for (uint32_t k = 0; k < d.glyph_image_count; ++k) {
+        const tk_glyph_image& im = d.glyph_images[k];
+        if (im.content > TK_GLYPH_LINEAR_SUBPIXEL_MASK) invalid("glyph image " + std::to_string(k) + ": bad content");
+        if (im.width > TK_MAX_IMAGE_DIMENSION || im.height > TK_MAX_IMAGE_DIMENSION ||
+            uint64_t(im.data_offset) + uint64_t(im.width) * im.height > d.glyph_texel_count)
+            invalid("glyph image " + std::to_string(k) + " outside the glyph texels");
+    }
     bool sdf_ext = false;
     // Draws: path fills/clips, and brush draws of the SDF kinds this library
     // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
     for (uint32_t i = 0; i < d.draw_count; ++i) {
         const tk_draw_record& r = d.draws[i];
         const std::string at = "draw " + std::to_string(i);
-        if (r.glyph_run_id != TK_INVALID_INDEX) invalid(at + ": text draws are outside this path");
+        if (r.glyph_run_id != TK_INVALID_INDEX) {
+            // a glyph run draw (canvas/primitives/text.rs:80-96)
+            if (r.glyph_run_id >= d.glyph_run_count) invalid(at + ": glyph run out of range");
+            if (r.tag != TK_DRAW_BRUSH || r.path_id != TK_INVALID_INDEX || r.sdf_offset != TK_INVALID_INDEX ||
+                r.sdf_shadow_offset != TK_INVALID_INDEX)
+                invalid(at + ": a glyph run draw is a brush draw without a path or SDF record");
+        }
         const bool plain = r.sdf_offset != TK_INVALID_INDEX, shadow = r.sdf_shadow_offset != TK_INVALID_INDEX;
         if (plain || shadow) {
             if (plain && shadow) invalid(at + ": both an SDF and a shadow record");
@@ -427,6 +462,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     c->sdf_words = d.sdf_word_count + d.sdf_shadow_word_count;
     c->sdf_shadow_base = d.sdf_word_count;
     c->sdf_ext = sdf_ext;
+    c->glyph_run_count = d.glyph_run_count;
     c->pool_len = pool;
     c->host_segment_capacity = seg_cap;
     c->h_paths.assign(d.paths, d.paths + d.path_count);
@@ -459,6 +495,13 @@ tk::SceneView view(tk_ctx* c) {
     s.sdf_shadow_base = c->sdf_shadow_base;
     s.sdf_ext = c->sdf_ext;
     s.texels = c->texels.ptr;
+    if (c->glyph_run_count) {
+        s.glyph_runs = c->glyph_runs.ptr;
+        s.glyphs = c->glyphs.ptr;
+        s.glyph_images = c->glyph_images.ptr;
+        s.glyph_texels = c->glyph_texels.ptr;
+        s.glyph_run_count = c->glyph_run_count;
+    }
     s.layers = c->layers.ptr;
     s.batch_ids = c->batch_ids.ptr;
     s.order = c->order.ptr;
@@ -498,6 +541,9 @@ tk::PassView pass_view(tk_ctx* c, Pass& p) {
     v.tile_desc = c->tile_desc.ptr;
     v.ticket = c->misc.ptr + 1;
     v.ptcl_total = c->misc.ptr + 3;
+    v.glyph_list = p.glyph_list.ptr;
+    v.glyph_capacity = p.glyph_list.ptr ? p.glyph_list.cap : 0;
+    v.glyph_total = c->misc.ptr + 6;
     v.stats = c->stats.ptr;
     if (c->batched) {
         v.scenes = c->d_scenes.ptr;
@@ -605,6 +651,10 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
         TK_CUDA(cudaMemcpyAsync(c->texels.ptr + tab[k].x, d.images[k].premul_rgba8,
                                 uint64_t(tab[k].y) * tab[k].z * 4, cudaMemcpyHostToDevice, st));
     upload(c->image_tab, tab.data(), tab.size(), st);
+    upload(c->glyph_runs, d.glyph_runs, d.glyph_run_count, st);
+    upload(c->glyphs, d.glyphs, d.glyph_count, st);
+    upload(c->glyph_images, d.glyph_images, d.glyph_image_count, st);
+    upload(c->glyph_texels, d.glyph_texels, d.glyph_texel_count, st);
     c->paints.reserve(d.draw_count);
     tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count,
                            uint32_t(c->sdf_shadow_base), c->image_tab.ptr, d.image_count, c->paints.ptr, st);
@@ -635,6 +685,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
         p.bin_counts.reserve(nbins);
         p.tiles.reserve(T);
         p.ptcl_needed = 0;
+        p.glyph_needed = 0;
     }
     size_t blur_depth = 0, cur = 0;
     for (const Step& s : c->steps) {
@@ -709,19 +760,30 @@ void run_pass(tk_ctx* c, Pass& p, uint32_t* target, bool fine = true) {
         tk::launch_coarse(s, v, false, st);
         tk::launch_tile_prefix(s, v, st);
     }
+    const bool text = c->glyph_run_count != 0u;
     if (c->active_mask) {  // incremental frame: size for its tiles, keep the full-frame size unknown
         uint32_t total = read_word(c, c->misc.ptr + 3);
         p.ptcl.reserve(uint64_t(total) + 1);
         p.ptcl_used = total;
+        if (text) {
+            const uint32_t glyphs = read_word(c, c->misc.ptr + 6);
+            p.glyph_list.reserve(uint64_t(glyphs) + 1);
+            p.glyph_used = glyphs;
+        }
         v = pass_view(c, p);
     } else {
-        if (p.ptcl_needed == 0) {  // first frame of this scene: size the PTCL buffer
+        if (p.ptcl_needed == 0) {  // first frame of this scene: size the PTCL buffer (and the glyph lists)
             uint32_t total = read_word(c, c->misc.ptr + 3);
             p.ptcl_needed = uint64_t(total) + 1;
             p.ptcl.reserve(p.ptcl_needed);
+            if (text) {
+                p.glyph_needed = uint64_t(read_word(c, c->misc.ptr + 6)) + 1;
+                p.glyph_list.reserve(p.glyph_needed);
+            }
             v = pass_view(c, p);
         }
         p.ptcl_used = p.ptcl_needed - 1;
+        p.glyph_used = text ? p.glyph_needed - 1 : 0;
     }
     {
         StageMark m(c, 6);
@@ -1123,6 +1185,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
         const tk_scene_desc& d = scenes[s];
         if (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) invalid("batched scenes use host segment planning");
         if (d.image_count) invalid("scene " + std::to_string(s) + ": image patterns are not batched");
+        if (d.glyph_run_count) invalid("scene " + std::to_string(s) + ": glyph runs are not batched");
         validate_and_plan(c, d);
         ext = ext || c->sdf_ext;
         uint32_t npass = 0;
@@ -1665,11 +1728,15 @@ uint64_t debug_read(tk_ctx* c, uint32_t stage, uint32_t index, uint64_t first, u
             break;
         case TK_STAGE_PTCL:
         case TK_STAGE_TILES:
-        case TK_STAGE_KINDS: {
+        case TK_STAGE_KINDS:
+        case TK_STAGE_GLYPHS: {
             if (index >= c->passes.size()) throw Fail{TK_E_INVALID, "pass index out of range"};
             Pass& p = c->passes[index];
             uint32_t T = c->tw * c->th;
-            if (stage == TK_STAGE_PTCL) {
+            if (stage == TK_STAGE_GLYPHS) {
+                src = reinterpret_cast<const unsigned char*>(p.glyph_list.ptr);
+                n = p.glyph_list.ptr ? p.glyph_used : 0;
+            } else if (stage == TK_STAGE_PTCL) {
                 src = reinterpret_cast<const unsigned char*>(p.ptcl.ptr);
                 n = p.ptcl_used;
                 es = sizeof(tk_ptcl_record);

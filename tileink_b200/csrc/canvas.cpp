@@ -367,8 +367,21 @@ struct Cmd {
 
 // One recorded Canvas call with its original geometry, for replay into
 // another canvas under an extra transform (a retained scene node's content).
+// A glyph image with its texels shared, so that replay into another canvas
+// registers the same image there.
+struct GlyphImage {
+    tk_glyph_image desc{};  // data_offset: where the owning canvas put the texels
+    std::shared_ptr<const std::vector<uint32_t>> texels;
+};
+
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS } kind = FILL;
+    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN } kind = FILL;
+    // GLYPH_RUN: the glyphs (image = index into run_images or TK_INVALID_INDEX),
+    // their images and the optional clip rect
+    std::vector<tk_glyph> run_glyphs;
+    std::vector<GlyphImage> run_images;
+    bool has_clip = false;
+    int32_t clip[4] = {0, 0, 0, 0};
     tk_path path;
     tk_sdf_shape shape{};
     // IMAGE: the rect in shape.p0 / p1, the image's texels and brush options;
@@ -417,6 +430,12 @@ struct tk_canvas {
     // registered images (Canvas::scene_images) and their texture table
     std::vector<std::shared_ptr<const std::vector<uint32_t>>> images;
     std::vector<tk_image_desc> image_table;
+    // the text blob: glyph images (with their texels concatenated), runs and glyphs
+    std::vector<GlyphImage> glyph_image_src;
+    std::vector<tk_glyph_image> glyph_images;
+    std::vector<uint32_t> glyph_texels;
+    std::vector<tk_glyph_run> glyph_runs;
+    std::vector<tk_glyph> glyphs;
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -1214,6 +1233,21 @@ namespace {
 // The SDF draw of `shape` with `tag`; -2 when it draws nothing, -1 on error.
 int64_t add_sdf_draw(tk_canvas* c, const tk_sdf_shape* shape, const tk_brush_desc* brush, uint32_t tag,
                      bool emit_command, const uint32_t* brush_words = nullptr);
+int32_t add_glyph_image(tk_canvas* c, const tk_glyph_image& d, std::shared_ptr<const std::vector<uint32_t>> texels) {
+    for (size_t k = 0; k < c->glyph_image_src.size(); ++k) {  // one entry per cached glyph image
+        const tk_glyph_image& e = c->glyph_image_src[k].desc;
+        if (c->glyph_image_src[k].texels == texels && e.left == d.left && e.top == d.top && e.width == d.width &&
+            e.height == d.height && e.content == d.content)
+            return int32_t(k);
+    }
+    if (c->glyph_texels.size() + texels->size() > 0xFFFFFFFFull) return -1;
+    GlyphImage g{d, texels};
+    g.desc.data_offset = uint32_t(c->glyph_texels.size());
+    c->glyph_texels.insert(c->glyph_texels.end(), texels->begin(), texels->end());
+    c->glyph_images.push_back(g.desc);
+    c->glyph_image_src.push_back(std::move(g));
+    return int32_t(c->glyph_images.size() - 1);
+}
 int32_t add_image(tk_canvas* c, std::shared_ptr<const std::vector<uint32_t>> texels, uint32_t w, uint32_t h) {
     for (size_t k = 0; k < c->images.size(); ++k)  // register_scene_image: one entry per image
         if (c->images[k] == texels) return int32_t(k);
@@ -1233,6 +1267,87 @@ int64_t tk_canvas_push_sdf(tk_canvas* c, const tk_sdf_shape* shape, const tk_bru
         c->log.push_back(std::move(r));
     }
     return add_sdf_draw(c, shape, brush, TK_DRAW_BRUSH, true);
+}
+
+int32_t tk_canvas_add_glyph_image(tk_canvas* c, int32_t left, int32_t top, uint32_t width, uint32_t height,
+                                  uint32_t content, const uint32_t* texels) {
+    if (!c || !texels || width == 0u || height == 0u || width > TK_MAX_IMAGE_DIMENSION ||
+        height > TK_MAX_IMAGE_DIMENSION || content > TK_GLYPH_LINEAR_SUBPIXEL_MASK)
+        return -1;
+    tk_glyph_image d{left, top, width, height, content, 0u};
+    const size_t n = size_t(width) * height;
+    return add_glyph_image(c, d, std::make_shared<const std::vector<uint32_t>>(texels, texels + n));
+}
+
+int64_t tk_canvas_push_glyph_run(tk_canvas* c, const tk_glyph* glyphs, uint32_t count, const tk_brush_desc* brush,
+                                 const int32_t* clip) {
+    if (!c || !glyphs || count == 0u) return -1;
+    // the run's bounds: the union of its glyph images (a glyph without an
+    // image draws nothing), then the clip (push_text_layout_clipped)
+    int64_t x0 = INT64_MAX, y0 = INT64_MAX, x1 = INT64_MIN, y1 = INT64_MIN;
+    for (uint32_t k = 0; k < count; ++k) {
+        const tk_glyph& g = glyphs[k];
+        if (g.image == TK_INVALID_INDEX) continue;
+        if (g.image >= c->glyph_images.size()) return -1;
+        const tk_glyph_image& im = c->glyph_images[g.image];
+        const int64_t gx0 = int64_t(g.x) + im.left, gy0 = int64_t(g.y) - im.top;
+        x0 = std::min(x0, gx0);
+        y0 = std::min(y0, gy0);
+        x1 = std::max(x1, gx0 + int64_t(im.width));
+        y1 = std::max(y1, gy0 + int64_t(im.height));
+    }
+    if (clip) {
+        x0 = std::max<int64_t>(x0, clip[0]);
+        y0 = std::max<int64_t>(y0, clip[1]);
+        x1 = std::min<int64_t>(x1, clip[2]);
+        y1 = std::min<int64_t>(y1, clip[3]);
+    }
+    if (x1 <= x0 || y1 <= y0 || x0 < INT32_MIN || y0 < INT32_MIN || x1 > INT32_MAX || y1 > INT32_MAX) return -1;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::GLYPH_RUN, nullptr, brush, nullptr);
+        std::vector<uint32_t> local(c->glyph_images.size(), TK_INVALID_INDEX);
+        for (uint32_t k = 0; k < count; ++k) {
+            tk_glyph g = glyphs[k];
+            if (g.image != TK_INVALID_INDEX) {
+                if (local[g.image] == TK_INVALID_INDEX) {
+                    local[g.image] = uint32_t(r.run_images.size());
+                    r.run_images.push_back(c->glyph_image_src[g.image]);
+                }
+                g.image = local[g.image];
+            }
+            r.run_glyphs.push_back(g);
+        }
+        if (clip) {
+            r.has_clip = true;
+            std::memcpy(r.clip, clip, sizeof(r.clip));
+        }
+        c->log.push_back(std::move(r));
+    }
+    const uint32_t run = uint32_t(c->glyph_runs.size());
+    c->glyph_runs.push_back(tk_glyph_run{uint32_t(c->glyphs.size()), count});
+    c->glyphs.insert(c->glyphs.end(), glyphs, glyphs + count);
+    tk_brush_desc transparent{};
+    transparent.kind = TK_BRUSH_KIND_SOLID;
+    const std::pair<uint32_t, uint32_t> br = push_brush(c->brush, brush ? *brush : transparent);
+    // push_text_layout_inner's draw record (canvas/primitives/text.rs:80-96)
+    tk_draw_record d{};
+    d.path_id = TK_INVALID_INDEX;
+    d.glyph_run_id = run;
+    d.sdf_offset = TK_INVALID_INDEX;
+    d.sdf_shadow_offset = TK_INVALID_INDEX;
+    d.brush_offset = br.first;
+    d.brush_len = br.second;
+    d.tag = TK_DRAW_BRUSH;
+    d.fill_rule = TK_FILL_NONZERO;
+    d.pixel_bounds = tk_pixel_bounds{int32_t(x0), int32_t(y0), int32_t(x1), int32_t(y1)};
+    d.local_pixel_bounds = d.pixel_bounds;
+    d.transform = tk_affine{1, 0, 0, 1, 0, 0};
+    d.inverse_transform = tk_affine{1, 0, 0, 1, 0, 0};
+    const uint32_t draw_ix = uint32_t(c->draws.size());
+    c->draws.push_back(d);
+    c->lists[c->stack.back()].push_back({Cmd::DRAW, draw_ix, 0.0f, 0u});
+    c->dirty = true;
+    return draw_ix;
 }
 
 int32_t tk_canvas_add_image(tk_canvas* c, const uint32_t* premul_rgba8, uint32_t width, uint32_t height) {
@@ -1465,6 +1580,14 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->sdf_shadow_word_count = c->shadow.size();
     out->images = c->image_table.data();
     out->image_count = uint32_t(c->image_table.size());
+    out->glyph_runs = c->glyph_runs.data();
+    out->glyph_run_count = uint32_t(c->glyph_runs.size());
+    out->glyphs = c->glyphs.data();
+    out->glyph_count = uint32_t(c->glyphs.size());
+    out->glyph_images = c->glyph_images.data();
+    out->glyph_image_count = uint32_t(c->glyph_images.size());
+    out->glyph_texels = c->glyph_texels.data();
+    out->glyph_texel_count = c->glyph_texels.size();
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -1919,6 +2042,40 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
     switch (r.kind) {
         case RecCmd::FILL: return tk_canvas_push_path(dst, &r.path, bp, t, r.rule, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::GLYPHS: return tk_canvas_push_glyph_outlines(dst, &r.path, bp, t, r.tolerance) < 0 ? -1 : 0;
+        case RecCmd::GLYPH_RUN: {
+            // glyph runs take whole-pixel translations only (bitmap glyphs
+            // have no transformed path, canvas/primitives/text.rs:7-10)
+            double dx = 0.0, dy = 0.0;
+            if (t) {
+                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+                dx = t[4] * double(dst->scale);
+                dy = t[5] * double(dst->scale);
+                if (dx != std::floor(dx) || dy != std::floor(dy) || std::fabs(dx) > 1.0e9 || std::fabs(dy) > 1.0e9)
+                    return -1;
+            }
+            std::vector<uint32_t> ids(r.run_images.size());
+            for (size_t k = 0; k < r.run_images.size(); ++k) {
+                const int32_t id = add_glyph_image(dst, r.run_images[k].desc, r.run_images[k].texels);
+                if (id < 0) return -1;
+                ids[k] = uint32_t(id);
+            }
+            std::vector<tk_glyph> gl = r.run_glyphs;
+            for (tk_glyph& g : gl) {
+                if (g.image != TK_INVALID_INDEX) g.image = ids[g.image];
+                g.x += int32_t(dx);
+                g.y += int32_t(dy);
+            }
+            int32_t cl[4];
+            if (r.has_clip) {
+                cl[0] = r.clip[0] + int32_t(dx);
+                cl[1] = r.clip[1] + int32_t(dy);
+                cl[2] = r.clip[2] + int32_t(dx);
+                cl[3] = r.clip[3] + int32_t(dy);
+            }
+            return tk_canvas_push_glyph_run(dst, gl.data(), uint32_t(gl.size()), bp, r.has_clip ? cl : nullptr) < 0
+                       ? -1
+                       : 0;
+        }
         case RecCmd::STROKE: return tk_canvas_push_stroke(dst, &r.path, bp, r.width, t, r.tolerance) < 0 ? -1 : 0;
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::OPACITY: return tk_canvas_push_opacity_layer(dst, &r.path, t, r.tolerance, r.sigma);

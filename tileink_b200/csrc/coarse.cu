@@ -31,8 +31,9 @@ constexpr int kQuadSide = 8;
 constexpr int kQuads = (kBinSide / kQuadSide) * (kBinSide / kQuadSide);
 constexpr int kCoarseThreads = kQuadSide * kQuadSide;
 constexpr uint32_t kChunkClassColor = 1u, kChunkClassSdf = 2u, kChunkClassOther = 4u, kChunkClassOccluder = 8u;
-// DrawInfo::meta bits
-constexpr uint32_t kMetaPath = 16u, kMetaSolid = 32u, kMetaSdf = 64u, kMetaSdfSolidClass = 128u;
+// DrawInfo::meta bits (the draw's batch ordinal above them, from bit kMetaBatchShift)
+constexpr uint32_t kMetaPath = 16u, kMetaSolid = 32u, kMetaSdf = 64u, kMetaSdfSolidClass = 128u, kMetaGlyph = 256u;
+constexpr uint32_t kMetaBatchShift = 9u;
 // DrawInfo::py bits of an SDF draw (px holds its first SDF word)
 constexpr uint32_t kSdfPlain = 256u, kSdfIdentity = 512u, kSdfImage = 1024u;
 // Candidates whose tile loads are in flight together, per pass (emission
@@ -110,7 +111,7 @@ struct DrawInfo {
     uint32_t tx, ty;         // draw tile bbox: x0 | x1 << 16, y0 | y1 << 16
     uint32_t px, py;         // path tile bbox packed the same way; SDF draws: first SDF word, kind | flags
     uint32_t data_offset;
-    uint32_t meta;           // tag | fill << 3 | kMeta* bits | batch << 8
+    uint32_t meta;           // tag | fill << 3 | kMeta* bits | batch << kMetaBatchShift
     uint32_t color;
 };
 
@@ -126,7 +127,49 @@ struct Ctx {
     const int32_t* backdrops;
     const tk_segment_range* ranges;
     uint32_t tw, th;
+    // the text blob (glyph_runs null: no text)
+    const tk_glyph_run* glyph_runs;
+    const tk_glyph* glyphs;
+    const tk_glyph_image* glyph_images;
+    uint32_t glyph_run_count;
 };
+
+// count_draw_glyphs / store_draw_glyphs (coarse/text.hlsli:8-35): the glyphs
+// [first, first + count) of a run whose image, widened by a pixel each way
+// (bilinear reach), meets tile (tx, ty) under the draw transform
+// (transformed_rect_hits_tile, shared/draw.hlsli:52-61); with `out`, their
+// indices are stored from `at` on. Out of line: only text draws reach it.
+static __device__ __noinline__ uint32_t draw_glyphs(const Ctx& c, uint32_t di, uint32_t first, uint32_t count,
+                                                   uint32_t tx, uint32_t ty, uint32_t* out, uint64_t at,
+                                                   uint64_t cap, uint32_t* error) {
+    const tk_affine t = c.draws[di].transform;
+    const float tlx = float(tx * TK_TILE_SIZE), tly = float(ty * TK_TILE_SIZE);
+    uint32_t n = 0;
+    for (uint32_t k = first; k < first + count; ++k) {
+        const tk_glyph g = c.glyphs[k];
+        if (g.image == TK_INVALID_INDEX) continue;
+        const tk_glyph_image im = c.glyph_images[g.image];
+        if (im.width == 0u || im.height == 0u) continue;
+        // int2(x + left, y - top) - 1 and + size + 1, in wrapping 32-bit arithmetic
+        const uint32_t lx = uint32_t(g.x) + uint32_t(im.left), ly = uint32_t(g.y) - uint32_t(im.top);
+        const float x0 = float(int32_t(lx - 1u)), y0 = float(int32_t(ly - 1u));
+        const float x1 = float(int32_t(lx + im.width + 1u)), y1 = float(int32_t(ly + im.height + 1u));
+        // draw_point of the four corners: (a x + c y) + e, (b x + d y) + f
+        const float p0x = t.a * x0 + t.c * y0 + t.e, p0y = t.b * x0 + t.d * y0 + t.f;
+        const float p1x = t.a * x1 + t.c * y0 + t.e, p1y = t.b * x1 + t.d * y0 + t.f;
+        const float p2x = t.a * x0 + t.c * y1 + t.e, p2y = t.b * x0 + t.d * y1 + t.f;
+        const float p3x = t.a * x1 + t.c * y1 + t.e, p3y = t.b * x1 + t.d * y1 + t.f;
+        const float lox = fminf(fminf(p0x, p1x), fminf(p2x, p3x)), loy = fminf(fminf(p0y, p1y), fminf(p2y, p3y));
+        const float hix = fmaxf(fmaxf(p0x, p1x), fmaxf(p2x, p3x)), hiy = fmaxf(fmaxf(p0y, p1y), fmaxf(p2y, p3y));
+        if (!(lox < tlx + float(TK_TILE_SIZE) && loy < tly + float(TK_TILE_SIZE) && hix > tlx && hiy > tly)) continue;
+        if (out) {
+            if (at + n < cap) out[at + n] = k;
+            else atomicOr(error, ERR_PTCL_OVERFLOW);
+        }
+        ++n;
+    }
+    return n;
+}
 
 __device__ __forceinline__ uint32_t brush_word(const Ctx& c, uint32_t i) {
     return i < c.brush_words ? __ldg(c.brush + i) : 0u;
@@ -284,7 +327,8 @@ __global__ void __launch_bounds__(kCoarseThreads)
              uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
              uint32_t batch0, tk_tile_record* tiles, tk_ptcl_record* ptcl, uint64_t cap,
              unsigned long long* stats, uint32_t* error, const BatchScene* __restrict__ scenes,
-             const uint32_t* __restrict__ bin_scene, const uint8_t* __restrict__ tile_active) {
+             const uint32_t* __restrict__ bin_scene, const uint8_t* __restrict__ tile_active, uint32_t* glyph_list,
+             uint64_t glyph_cap) {
     __shared__ DrawInfo s_d[kCoarseThreads];
     const uint32_t bin = blockIdx.x / kQuads, quad = blockIdx.x % kQuads;
     uint32_t lbin = bin, tile_base = 0u;
@@ -307,15 +351,21 @@ __global__ void __launch_bounds__(kCoarseThreads)
     // incremental render: tiles that are not redrawn get no particles
     const bool live = in_canvas && (!tile_active || tile_active[tile]);
     if (!__syncthreads_or(live)) {
-        if (!EMIT && in_canvas) tiles[tile].ptcl_count = 0u;
+        if (!EMIT && in_canvas) {
+            tiles[tile].ptcl_count = 0u;
+            tiles[tile].glyph_count = 0u;
+        }
         return;
     }
     const uint32_t* list = bin_lists + list_at;
     const uint32_t n = bin_counts[bin];
 
-    uint64_t at = 0;
-    if (EMIT && live) at = tiles[tile].ptcl_start;
-    uint32_t total = 0;
+    uint64_t at = 0, gat = 0;
+    if (EMIT && live) {
+        at = tiles[tile].ptcl_start;
+        gat = tiles[tile].glyph_start;
+    }
+    uint32_t total = 0, glyph_total = 0;
     uint32_t cur = 0xFFFFFFFFu, wrappers = 0, nb = 0, flags = 0;
     bool rejected = false;
     uint64_t section = 0;
@@ -366,9 +416,21 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 return d.brush_offset != TK_INVALID_INDEX && brush_word(c, d.brush_offset) == TK_BRUSH_SOLID &&
                        brush_word(c, d.brush_offset + TK_BRUSH_COLOR_WORD) != 0u;
             };
-            const bool has_sdf = SDF && (d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX);
+            // a glyph run draw gives a PTCL_GLYPH particle or none
+            // (coarse/emit_draw.hlsli:15-22)
+            const bool glyph = c.glyph_runs && d.glyph_run_id != TK_INVALID_INDEX;
+            const bool has_sdf = !glyph && SDF &&
+                                 (d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX);
             uint32_t sdf_bits = 0u;
-            if (has_sdf) {
+            if (glyph) {
+                valid_path = false;
+                if (d.tag == TK_DRAW_BRUSH && d.glyph_run_id < c.glyph_run_count) {
+                    const tk_glyph_run run = c.glyph_runs[d.glyph_run_id];
+                    info.px = run.first;
+                    info.py = run.count;
+                    sdf_bits |= kMetaGlyph;
+                }
+            } else if (has_sdf) {
                 // draw_has_sdf (shared/draw.hlsli:31): only brush draws give a particle
                 valid_path = false;
                 const bool plain = d.sdf_offset != TK_INVALID_INDEX;
@@ -400,7 +462,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
             uint32_t batch = batch_ids[di] - batch0;
             const uint32_t rule = has_sdf ? 0u : (d.fill_rule & 1u);  // SDF particles carry rule 0
             info.meta = (d.tag & 7u) | (rule << 3) | (valid_path ? kMetaPath : 0u) |
-                        (color_candidate ? kMetaSolid : 0u) | sdf_bits | (batch << 8);
+                        (color_candidate ? kMetaSolid : 0u) | sdf_bits | (batch << kMetaBatchShift);
             s_d[threadIdx.x] = info;
         }
         __syncthreads();
@@ -413,7 +475,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
         for (uint32_t k0 = 0; k0 < m; k0 += kPrefetch) {
             tk_segment_range rr[kPrefetch];
             uint32_t ww[kPrefetch];
-            uint32_t hit = 0u, sdf_hit = 0u;
+            uint32_t hit = 0u, sdf_hit = 0u, glyph_hit = 0u;
 #pragma unroll
             for (uint32_t q = 0; q < kPrefetch; ++q) {
                 rr[q] = tk_segment_range{0u, 0u};
@@ -425,6 +487,10 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 const uint32_t meta = d.meta;
                 if (SDF && (meta & kMetaSdf)) {
                     sdf_hit |= 1u << q;
+                    continue;
+                }
+                if (meta & kMetaGlyph) {
+                    glyph_hit |= 1u << q;
                     continue;
                 }
                 if (!(meta & kMetaPath)) continue;
@@ -439,13 +505,18 @@ __global__ void __launch_bounds__(kCoarseThreads)
             }
 #pragma unroll
             for (uint32_t q = 0; q < kPrefetch; ++q) {
-                if (!((hit | sdf_hit) & (1u << q))) continue;
+                if (!((hit | sdf_hit | glyph_hit) & (1u << q))) continue;
                 const DrawInfo& d = s_d[k0 + q];
                 const uint32_t meta = d.meta, tag = meta & 7u;
                 tk_segment_range r = rr[q];
-                const uint32_t w = ww[q];  // 0 for SDF draws
+                const uint32_t w = ww[q];  // 0 for SDF and glyph draws
                 uint32_t ptag = TK_PTCL_FILL;
-                if (SDF && (sdf_hit & (1u << q))) {
+                uint32_t glyphs_here = 0u;
+                if (glyph_hit & (1u << q)) {
+                    glyphs_here = draw_glyphs(c, d.draw, d.px, d.py, tx, ty, nullptr, 0u, 0u, error);
+                    if (glyphs_here == 0u) continue;
+                    ptag = TK_PTCL_GLYPH;
+                } else if (SDF && (sdf_hit & (1u << q))) {
                     ptag = sdf_particle(c.draws, c.sdf, d.draw, d.px, d.py, meta, tx, ty);
                     if (ptag == 0u) continue;
                     // an SDF particle names its draw in segment_start (coarse/emit_draw.hlsli:28)
@@ -456,7 +527,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     else if (tag == TK_DRAW_PATH_GLYPH) ptag = TK_PTCL_PATH_GLYPH;
                     else if ((meta & kMetaSolid) && r.start == r.end) ptag = TK_PTCL_COLOR;
                 }
-                uint32_t batch = meta >> 8;
+                uint32_t batch = meta >> kMetaBatchShift;
                 if (batch != cur) {
                     close();
                     cur = batch;
@@ -479,18 +550,31 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     flags |= cls;
                     uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
                     if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
-                    store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
-                    if (ptag != TK_PTCL_COLOR && ptag != TK_PTCL_SDF) {
+                    if (ptag == TK_PTCL_GLYPH) {
+                        // the tile's glyph list continues at gat (coarse/emit.hlsl:54-58)
+                        draw_glyphs(c, d.draw, d.px, d.py, tx, ty, glyph_list, gat, glyph_cap, error);
+                        store_ptcl(ptcl, cap, at++, ptag, 0u, 0u, uint32_t(gat), uint32_t(gat + glyphs_here), color,
+                                   error);
+                        gat += glyphs_here;
+                    } else {
+                        store_ptcl(ptcl, cap, at++, ptag, w, (meta >> 3) & 1u, r.start, r.end, color, error);
+                    }
+                    if (ptag != TK_PTCL_COLOR && ptag != TK_PTCL_SDF && ptag != TK_PTCL_GLYPH) {
                         fills += 1;
                         visits += r.end - r.start;
                     }
+                } else {
+                    glyph_total += glyphs_here;
                 }
                 ++nb;
             }
         }
     }
     if (!live) {
-        if (!EMIT && in_canvas) tiles[tile].ptcl_count = 0u;
+        if (!EMIT && in_canvas) {
+            tiles[tile].ptcl_count = 0u;
+            tiles[tile].glyph_count = 0u;
+        }
         return;
     }
     close();
@@ -503,6 +587,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
         }
     } else {
         tiles[tile].ptcl_count = total;
+        tiles[tile].glyph_count = glyph_total;
     }
 }
 
@@ -514,6 +599,9 @@ __global__ void __launch_bounds__(kCoarseThreads)
 constexpr int kTileScanThreads = 256, kTilePer = 16, kTileBlock = kTileScanThreads * kTilePer;
 constexpr unsigned long long kAgg = 1ull << 62, kIncl = 2ull << 62;
 
+// GLYPH: the same scan of glyph_count into glyph_start / glyph_end (the
+// second component of coarse/prefix.hlsl's uint2 scan), for text scenes.
+template <bool GLYPH>
 __global__ void __launch_bounds__(kTileScanThreads)
     k_tile_prefix(tk_tile_record* tiles, uint32_t T, unsigned long long* desc, uint32_t* ticket, uint32_t* total,
                   uint32_t* error, uint32_t poll_limit) {
@@ -529,7 +617,7 @@ __global__ void __launch_bounds__(kTileScanThreads)
 #pragma unroll
     for (int k = 0; k < kTilePer; ++k) {
         uint32_t t = base + tid * kTilePer + k;
-        v[k] = t < T ? tiles[t].ptcl_count : 0u;
+        v[k] = t < T ? (GLYPH ? tiles[t].glyph_count : tiles[t].ptcl_count) : 0u;
         sum += v[k];
     }
     uint32_t incl = sum;
@@ -576,11 +664,15 @@ __global__ void __launch_bounds__(kTileScanThreads)
     for (int k = 0; k < kTilePer; ++k) {
         uint32_t t = base + tid * kTilePer + k;
         if (t < T) {
-            tiles[t].ptcl_start = run;
-            tiles[t].ptcl_end = run + v[k];
-            tiles[t].glyph_count = 0u;
-            tiles[t].glyph_start = 0u;
-            tiles[t].glyph_end = 0u;
+            if (GLYPH) {
+                tiles[t].glyph_start = run;
+                tiles[t].glyph_end = run + v[k];
+            } else {
+                tiles[t].ptcl_start = run;
+                tiles[t].ptcl_end = run + v[k];
+                tiles[t].glyph_start = 0u;
+                tiles[t].glyph_end = 0u;
+            }
         }
         run += v[k];
     }
@@ -601,7 +693,7 @@ void launch_bins(const SceneView& s, const PassView& p, cudaStream_t st) {
 
 void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_t st) {
     Ctx c{s.draws, s.paths, s.path_count, s.layers, s.brush, s.brush_words, s.sdf, s.sdf_shadow_base, s.backdrops,
-          s.ranges, s.tw, s.th};
+          s.ranges, s.tw, s.th, s.glyph_runs, s.glyphs, s.glyph_images, s.glyph_run_count};
     const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
     if (nbins == 0) return;
     const bool sdf = s.sdf_words != 0;
@@ -609,12 +701,21 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
                        : (sdf ? k_coarse<false, true> : k_coarse<false, false>);
     kernel<<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                       p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity, p.stats,
-                                                      s.error, p.scenes, p.bin_scene, p.tile_active);
+                                                      s.error, p.scenes, p.bin_scene, p.tile_active, p.glyph_list,
+                                                      p.glyph_capacity);
 }
 
 void launch_tile_prefix(const SceneView& s, const PassView& p, cudaStream_t st) {
     uint32_t T = p.scenes ? p.total_tiles : s.tw * s.th;
     launch_tile_prefix_on(p.tiles, T, p.tile_desc, p.ticket, p.ptcl_total, s.error, kTilePrefixPollLimit, 0u, st);
+    if (s.glyph_runs) {  // text scenes: the glyph lists' prefix too
+        const uint32_t blocks = tile_prefix_blocks(T);
+        cudaMemsetAsync(p.tile_desc, 0, sizeof(unsigned long long) * blocks, st);
+        cudaMemsetAsync(p.ticket, 0, sizeof(uint32_t), st);
+        if (blocks)
+            k_tile_prefix<true><<<blocks, kTileScanThreads, 0, st>>>(p.tiles, T, p.tile_desc, p.ticket, p.glyph_total,
+                                                                     s.error, kTilePrefixPollLimit);
+    }
 }
 
 uint32_t tile_prefix_blocks(uint32_t T) { return (T + kTileBlock - 1) / kTileBlock; }
@@ -627,7 +728,7 @@ void launch_tile_prefix_on(tk_tile_record* tiles, uint32_t T, unsigned long long
     cudaMemsetAsync(ticket, 0, sizeof(uint32_t), st);
     if (first_ticket) cudaMemcpyAsync(ticket, &first_ticket, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
     if (blocks)
-        k_tile_prefix<<<blocks, kTileScanThreads, 0, st>>>(tiles, T, desc, ticket, total, error, poll_limit);
+        k_tile_prefix<false><<<blocks, kTileScanThreads, 0, st>>>(tiles, T, desc, ticket, total, error, poll_limit);
 }
 
 }  // namespace tk

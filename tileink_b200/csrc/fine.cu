@@ -499,6 +499,64 @@ __device__ __noinline__ float4 paint_glyph_fill(const FineSmem& S, const Paint P
     return rgba8_to_unorm(src_over_mask_linear_auto_u8(unorm_to_rgba8(px), color, masked));
 }
 
+// The text blob as fine raster reads it: the pass's glyph lists, the glyph
+// records, the glyph images and their texels.
+struct GlyphView {
+    const uint32_t* list;
+    const tk_glyph* glyphs;
+    const tk_glyph_image* images;
+    const uint32_t* texels;
+};
+
+// composite_glyphs_at (fine/glyph.hlsli:55-111): the glyphs list[g0, g1) of
+// a glyph run draw over px at pixel (gx, gy), each by its image's content.
+// Out of line like the glyph outline paint.
+template <bool IMG>
+__device__ __noinline__ float4 composite_glyphs(const FineSmem& S, const Paint P, uint32_t i, const GlyphView G,
+                                                const tk_draw_record* dr, uint32_t g0, uint32_t g1, uint32_t gx,
+                                                uint32_t gy, uint32_t clip, float4 px) {
+    const tk_affine& t = dr->inverse_transform;
+    const float a = __ldg(&t.a), b = __ldg(&t.b), c = __ldg(&t.c), d = __ldg(&t.d), e = __ldg(&t.e), f = __ldg(&t.f);
+    const float sx = float(gx) + 0.5f, sy = float(gy) + 0.5f;
+    const float lx = __fmaf_rn(a, sx, __fmaf_rn(c, sy, e)) - 0.5f;
+    const float ly = __fmaf_rn(b, sx, __fmaf_rn(d, sy, f)) - 0.5f;
+    for (uint32_t g = g0; g < g1; ++g) {
+        const tk_glyph glyph = G.glyphs[__ldg(G.list + g)];
+        if (glyph.image == TK_INVALID_INDEX) continue;
+        const tk_glyph_image im = G.images[glyph.image];
+        const int32_t x0 = int32_t(uint32_t(glyph.x) + uint32_t(im.left));
+        const int32_t y0 = int32_t(uint32_t(glyph.y) - uint32_t(im.top));
+        const float ux = lx - float(x0), uy = ly - float(y0);
+        if (!(ux > -1.0f && uy > -1.0f && ux < float(int32_t(im.width)) && uy < float(int32_t(im.height)))) continue;
+        const uint32_t content = im.content;
+        auto brush = [&]() {
+            const uint32_t paint = S.paint[i];
+            return paint != kGradient ? paint : gradient_at<IMG>(S, P, i, sx, sy);
+        };
+        if (content == TK_GLYPH_LINEAR_MASK || content == TK_GLYPH_LINEAR_SUBPIXEL_MASK) {
+            const uint32_t color = brush();
+            float3 cov = sample_corrected_glyph(G.texels, im, ux, uy, text_foreground(color),
+                                                content == TK_GLYPH_LINEAR_SUBPIXEL_MASK);
+            const float k = float(clip) * (1.0f / 255.0f);
+            cov = make_float3(cov.x * k, cov.y * k, cov.z * k);
+            px = rgba8_to_unorm(src_over_subpixel_mask_f32(unorm_to_rgba8(px), color, cov));
+        } else {
+            const uint32_t data = sample_glyph(G.texels, im, ux, uy);
+            if (content == TK_GLYPH_MASK) {
+                const uint32_t alpha = combine_alpha(data, clip);
+                if (alpha != 0u) px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(brush(), alpha));
+            } else if (content == TK_GLYPH_COLOR) {
+                px = src_over_premul_unorm(px, scale_premul_u8_to_unorm(data, clip));
+            } else if (content == TK_GLYPH_LINEAR_COLOR) {
+                px = rgba8_to_unorm(src_over_mask_linear_auto_u8(unorm_to_rgba8(px), data, clip));
+            } else if (content == TK_GLYPH_SUBPIXEL_MASK) {
+                px = rgba8_to_unorm(src_over_subpixel_mask_u8(unorm_to_rgba8(px), brush(), data, clip));
+            }
+        }
+    }
+    return px;
+}
+
 // SDF: 0 for scenes without SDF records, 1 with SDF records of the base
 // kinds, 2 with the extended kinds (candlestick, dash line, triangle,
 // checkerboard). Path-only scenes run the instance without the PTCL_SDF
@@ -512,7 +570,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
            const uint32_t* __restrict__ brush, uint64_t brush_words, const uint32_t* __restrict__ texels,
            const tk_draw_record* __restrict__ draws, const uint32_t* __restrict__ sdf, uint64_t seg_capacity, uint32_t* target,
            uint32_t width, uint32_t height, uint32_t tw, uint32_t* error, const BatchScene* __restrict__ scenes,
-           const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list) {
+           const uint32_t* __restrict__ tile_scene, const uint32_t* __restrict__ tile_list, const GlyphView glyphs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     FineSmem& S = *reinterpret_cast<FineSmem*>(smem_raw);
     const uint32_t tile = tile_list ? tile_list[blockIdx.x] : blockIdx.x;
@@ -572,7 +630,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
             }
             S.nseg[tid] = n;
             if (SDF != 0u && a.x == TK_PTCL_BEGIN_SDF_CLIP) S.umode[tid] = __ldg(&paints[c.y].sdf);
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH ||
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || a.x == TK_PTCL_GLYPH ||
                 (SDF != 0u && (a.x == TK_PTCL_SDF || a.x == TK_PTCL_IMAGE))) {
                 const PaintInfo* pi = paints + c.y;
                 if (SDF != 0u && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
@@ -744,6 +802,14 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                     const uint32_t masked = combine_alpha(alpha, clip);
                     if (masked != 0u) paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                 }
+            } else if (tag == TK_PTCL_GLYPH) {
+                // fine/interpreter.hlsli:93-106: the run's glyphs inside the
+                // draw's exact pixel bounds
+                const tk_draw_record* dr = draws + qb.y;
+                const int32_t x = int32_t(gx), y = int32_t(gy);
+                if (clip != 0u && x >= __ldg(&dr->pixel_bounds.x0) && y >= __ldg(&dr->pixel_bounds.y0) &&
+                    x < __ldg(&dr->pixel_bounds.x1) && y < __ldg(&dr->pixel_bounds.y1))
+                    px = composite_glyphs<SDF != 0u>(S, P, i, glyphs, dr, qa.w, qb.x, gx, gy, clip, px);
             } else if (is_fill_like(tag)) {
                 uint32_t alpha;
                 if (S.nseg[i] == 0u) {
@@ -846,9 +912,10 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     }
     if (s.sdf_ext) k_star_table<<<1, 32, 0, st>>>();
     auto kernel = !s.sdf_words ? k_fine<0u> : (s.sdf_ext ? k_fine<2u> : k_fine<1u>);
+    const GlyphView glyphs{p.glyph_list, s.glyphs, s.glyph_images, s.glyph_texels};
     kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
                                                       s.texels, s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,
-                                                      s.tw, s.error, p.scenes, p.tile_scene, p.tile_list);
+                                                      s.tw, s.error, p.scenes, p.tile_scene, p.tile_list, glyphs);
 }
 
 }  // namespace tk

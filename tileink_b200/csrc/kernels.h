@@ -71,6 +71,12 @@ struct SceneView {
     uint64_t sdf_shadow_base;
     bool sdf_ext;  // some record is of an extended kind (fine's k_fine<2>)
     const uint32_t* texels;  // the scene's images, concatenated (premultiplied RGBA8)
+    // the text blob (null without glyph runs)
+    const tk_glyph_run* glyph_runs;
+    const tk_glyph* glyphs;
+    const tk_glyph_image* glyph_images;
+    const uint32_t* glyph_texels;
+    uint32_t glyph_run_count;
     const tk_layer_record* layers;
     const uint32_t* batch_ids;
     const uint32_t* order;
@@ -150,6 +156,10 @@ struct PassView {
     unsigned long long* tile_desc;    // lookback descriptors for the tile scan
     uint32_t* ticket;
     uint32_t* ptcl_total;
+    // glyph lists: the glyph indices PTCL_GLYPH records name (text scenes)
+    uint32_t* glyph_list;
+    uint64_t glyph_capacity;
+    uint32_t* glyph_total;
     unsigned long long* stats;        // [0] fill records, [1] segment visits
     // batched pass (null for one canvas): per-scene geometry and the scene
     // of every global bin and tile

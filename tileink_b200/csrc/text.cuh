@@ -128,4 +128,97 @@ __device__ __forceinline__ uint32_t src_over_mask_linear_auto_u8(uint32_t destin
     return src_over_gray_mask_f32(destination, source, corrected);
 }
 
+// text_foreground (fine/text/auto.hlsli:6-9)
+__device__ __forceinline__ float3 text_foreground(uint32_t source) {
+    const float alpha = float(source >> 24);
+    if (!(alpha > 0.0f)) return make_float3(0.0f, 0.0f, 0.0f);
+    return make_float3(clampf(float(source & 255u) / alpha, 0.0f, 1.0f),
+                       clampf(float((source >> 8) & 255u) / alpha, 0.0f, 1.0f),
+                       clampf(float((source >> 16) & 255u) / alpha, 0.0f, 1.0f));
+}
+
+// src_over_subpixel_mask_f32 (fine/text/basic.hlsli:95-109), one coverage
+// per channel.
+__device__ __forceinline__ uint32_t src_over_subpixel_mask_f32(uint32_t destination, uint32_t source, float3 cov) {
+    if ((source >> 24) == 0u || (cov.x == 0.0f && cov.y == 0.0f && cov.z == 0.0f)) return destination;
+    if ((destination >> 24) != 255u) {
+        const float gray = (cov.x + cov.y + cov.z) / 3.0f;
+        cov = make_float3(gray, gray, gray);
+    }
+    const float alpha = float(source >> 24) * (1.0f / 255.0f);
+    const float ar = alpha * cov.x, ag = alpha * cov.y, ab = alpha * cov.z;
+    const float r = float(source & 255u) * cov.x + float(destination & 255u) * (1.0f - ar);
+    const float g = float((source >> 8) & 255u) * cov.y + float((destination >> 8) & 255u) * (1.0f - ag);
+    const float b = float((source >> 16) & 255u) * cov.z + float((destination >> 16) & 255u) * (1.0f - ab);
+    const float maximum = fmaxf(fmaxf(ar, ag), ab);
+    const float a = maximum * 255.0f + float(destination >> 24) * (1.0f - maximum);
+    return pack4(f2u(r + 0.5f), f2u(g + 0.5f), f2u(b + 0.5f), f2u(a + 0.5f));
+}
+
+// src_over_subpixel_mask_u8 with text_subpixel_coverage
+// (fine/text/basic.hlsli:9-43): integer subpixel compositing.
+__device__ __forceinline__ uint32_t src_over_subpixel_mask_u8(uint32_t dst, uint32_t src, uint32_t mask, uint32_t clip) {
+    const uint32_t sa = src >> 24;
+    if (sa == 0u || clip == 0u) return dst;
+    uint32_t mr = mul_div255(mask & 255u, clip), mg = mul_div255((mask >> 8) & 255u, clip),
+             mb = mul_div255((mask >> 16) & 255u, clip);
+    if ((dst >> 24) != 255u) mr = mg = mb = (mr + mg + mb + 1u) / 3u;
+    if (mr == 0u && mg == 0u && mb == 0u) return dst;
+    const uint32_t cr = mul_div255(sa, mr), cg = mul_div255(sa, mg), cb = mul_div255(sa, mb);
+    const uint32_t ca = max(max(cr, cg), cb);
+    const uint32_t r = mul_div255(src & 255u, mr) + mul_div255(dst & 255u, 255u - cr);
+    const uint32_t g = mul_div255((src >> 8) & 255u, mg) + mul_div255((dst >> 8) & 255u, 255u - cg);
+    const uint32_t b = mul_div255((src >> 16) & 255u, mb) + mul_div255((dst >> 16) & 255u, 255u - cb);
+    const uint32_t a = ca + mul_div255((dst >> 24) & 255u, 255u - ca);
+    return pack4(r, g, b, a);
+}
+
+// A glyph image's texel, 0 outside it (fine/glyph.hlsli:17-21).
+__device__ __forceinline__ uint32_t glyph_texel(const uint32_t* __restrict__ texels, const tk_glyph_image& im,
+                                                int32_t x, int32_t y) {
+    if (x < 0 || y < 0 || x >= int32_t(im.width) || y >= int32_t(im.height)) return 0u;
+    return __ldg(texels + im.data_offset + uint32_t(y) * im.width + uint32_t(x));
+}
+
+// sample_glyph (fine/glyph.hlsli:22-30): bilinear in unorm, `lerp(a, b, t)`
+// as a + t (b - a).
+__device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
+    return make_float4(a.x + t * (b.x - a.x), a.y + t * (b.y - a.y), a.z + t * (b.z - a.z), a.w + t * (b.w - a.w));
+}
+__device__ __forceinline__ uint32_t sample_glyph(const uint32_t* __restrict__ texels, const tk_glyph_image& im, float px,
+                                                 float py) {
+    const int32_t bx = f2i(floorf(px)), by = f2i(floorf(py));
+    const float fx = px - float(bx), fy = py - float(by);
+    const uint32_t a = glyph_texel(texels, im, bx, by);
+    if (fx == 0.0f && fy == 0.0f) return a;
+    const float4 top = lerp4(rgba8_to_unorm(a), rgba8_to_unorm(glyph_texel(texels, im, bx + 1, by)), fx);
+    const float4 bottom = lerp4(rgba8_to_unorm(glyph_texel(texels, im, bx, by + 1)),
+                                rgba8_to_unorm(glyph_texel(texels, im, bx + 1, by + 1)), fx);
+    return unorm_to_rgba8(lerp4(top, bottom, fy));
+}
+
+// corrected_glyph_texel and sample_corrected_glyph (fine/glyph.hlsli:32-53)
+__device__ __forceinline__ float3 corrected_glyph_texel(uint32_t data, float3 fg, bool lcd) {
+    if (!lcd) {
+        const float alpha = text_correcting_coverage(data & 255u, (fg.x * 0.2126f + fg.y * 0.7152f) + fg.z * 0.0722f);
+        return make_float3(alpha, alpha, alpha);
+    }
+    return make_float3(text_correcting_coverage(data & 255u, fg.x), text_correcting_coverage((data >> 8) & 255u, fg.y),
+                       text_correcting_coverage((data >> 16) & 255u, fg.z));
+}
+__device__ __forceinline__ float3 lerp3(float3 a, float3 b, float t) {
+    return make_float3(a.x + t * (b.x - a.x), a.y + t * (b.y - a.y), a.z + t * (b.z - a.z));
+}
+__device__ __forceinline__ float3 sample_corrected_glyph(const uint32_t* __restrict__ texels, const tk_glyph_image& im,
+                                                         float px, float py, float3 fg, bool lcd) {
+    const int32_t bx = f2i(floorf(px)), by = f2i(floorf(py));
+    const float fx = px - float(bx), fy = py - float(by);
+    const float3 a = corrected_glyph_texel(glyph_texel(texels, im, bx, by), fg, lcd);
+    if (fx == 0.0f && fy == 0.0f) return a;
+    const float3 top = lerp3(a, corrected_glyph_texel(glyph_texel(texels, im, bx + 1, by), fg, lcd), fx);
+    const float3 bottom = lerp3(corrected_glyph_texel(glyph_texel(texels, im, bx, by + 1), fg, lcd),
+                                corrected_glyph_texel(glyph_texel(texels, im, bx + 1, by + 1), fg, lcd), fx);
+    return lerp3(top, bottom, fy);
+}
+
 }  // namespace tkd

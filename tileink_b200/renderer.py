@@ -139,10 +139,7 @@ class NativeRenderer:
     def debug(self, stage: int, index: int = 0) -> np.ndarray:
         need = C.c_size_t(0)
         self._check(self._lib.tk_debug_readback(self._h, stage, index, None, 0, C.byref(need)))
-        dt = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
-              N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
-              N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE,
-              N.STAGE_LINES: N.LINE_DTYPE}[stage]
+        dt = self.DEBUG_DTYPES[stage]
         out = np.zeros(need.value // np.dtype(dt).itemsize, dtype=dt)
         self._check(self._lib.tk_debug_readback(self._h, stage, index, N.ptr(out), need.value, None))
         return out
@@ -180,7 +177,7 @@ class NativeRenderer:
     DEBUG_DTYPES = {N.STAGE_COUNTS: np.uint32, N.STAGE_BACKDROPS: np.int32, N.STAGE_RANGES: N.RANGE_DTYPE,
                     N.STAGE_SEGMENTS: N.SEGMENT_DTYPE, N.STAGE_PTCL: N.PTCL_DTYPE, N.STAGE_TILES: N.TILE_DTYPE,
                     N.STAGE_KINDS: np.uint32, N.STAGE_IMAGE: np.uint32, N.STAGE_PATHS: N.PATH_DTYPE,
-                    N.STAGE_LINES: N.LINE_DTYPE}
+                    N.STAGE_LINES: N.LINE_DTYPE, N.STAGE_GLYPHS: np.uint32}
 
     def debug_size(self, stage: int, index: int = 0) -> int:
         """Element count of a debug stage buffer."""
