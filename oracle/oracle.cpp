@@ -329,36 +329,23 @@ tk_line_segment clipped_segment(const Scan& s, uint32_t sub, float z, int32_t tx
     return {p0x, p0y, p1x, p1y, edge};
 }
 
-// Canonical emit order (or_emit_order): per path, lines in groups of 32
-// consecutive lines; within a group, DDA iteration r (i = imin + r) is the
-// outer loop and the line's lane (0..31) the inner loop. Each emitting step
-// takes the next cursor of its tile. This is one admissible interleaving of
-// the reference's atomic increments (each line's own steps stay in order).
+// Canonical emit order: a path's lines in order, each line's DDA steps
+// (i = imin ..) in order, each emitting step taking the next cursor of its
+// tile. This is the sequential one of the reference's admissible atomic
+// interleavings (scan/emit.hlsl:14-28).
 void emit_path(const tk_line* lines, const tk_path_record* paths, uint32_t np, uint32_t pid, uint32_t* cursors,
                tk_line_segment* segments, uint64_t capacity) {
     const tk_path_record& p = paths[pid];
-    for (uint32_t g = 0; g < p.line_count; g += 32u) {
-        uint32_t n = std::min(32u, p.line_count - g);
-        Scan sc[32];
-        bool ok[32];
-        uint32_t rounds = 0;
-        for (uint32_t l = 0; l < n; ++l) {
-            ok[l] = scan_geometry(lines[p.line_start + g + l], paths, np, sc[l]);
-            if (ok[l]) rounds = std::max(rounds, sc[l].imax - sc[l].imin);
-        }
-        for (uint32_t r = 0; r < rounds; ++r) {
-            for (uint32_t l = 0; l < n; ++l) {
-                if (!ok[l]) continue;
-                const Scan& s = sc[l];
-                if (r >= s.imax - s.imin) continue;
-                uint32_t i = s.imin + r;
-                float z = std::floor(s.a * float(i) + s.b);
-                int32_t tx, ty;
-                scan_tile(s, i, z, tx, ty);
-                if (!scan_tile_inside(s, tx, ty)) continue;
-                uint32_t dst = cursors[scan_tile_offset(s, tx, ty)]++;
-                if (dst < capacity) segments[dst] = clipped_segment(s, i, z, tx, ty);
-            }
+    for (uint32_t l = 0; l < p.line_count; ++l) {
+        Scan s;
+        if (!scan_geometry(lines[p.line_start + l], paths, np, s)) continue;
+        for (uint32_t i = s.imin; i < s.imax; ++i) {
+            float z = std::floor(s.a * float(i) + s.b);
+            int32_t tx, ty;
+            scan_tile(s, i, z, tx, ty);
+            if (!scan_tile_inside(s, tx, ty)) continue;
+            uint32_t dst = cursors[scan_tile_offset(s, tx, ty)]++;
+            if (dst < capacity) segments[dst] = clipped_segment(s, i, z, tx, ty);
         }
     }
 }

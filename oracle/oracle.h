@@ -27,7 +27,8 @@
  * `round` rounds half to even; float->int conversions saturate; RGBA8 target
  * loads are k/255 and stores round to nearest even. The only freedom the
  * reference leaves open, the order of atomic increments, is fixed to the
- * canonical order documented at or_emit_order.
+ * sequential order: a path's lines in order, each line's tile steps in order
+ * (emit_path in oracle.cpp).
  */
 #ifndef TILEINK_ORACLE_H
 #define TILEINK_ORACLE_H

@@ -357,14 +357,26 @@ __global__ void k_path_totals(tk_path_record* paths, uint32_t path_count, const 
     }
 }
 
-__global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths,
-                            uint32_t path_count, uint32_t* cursors, SegmentRec* segments, uint64_t capacity,
-                            uint32_t* error, uint32_t* seg_line, const uint32_t* __restrict__ order,
-                            uint32_t* ticket) {
-    const uint32_t lane = threadIdx.x & 31u;
+// scan_emit (scan/emit.hlsl:14-28) in canonical order: a path's lines in
+// order, each line's DDA steps in order, every emitting step taking the next
+// cursor of its tile. Warps take paths from a queue, longest first (the line
+// counts are heavy-tailed and a path is one warp's sequential work). Per group
+// of 32 lines the warp computes each line's scan geometry, then walks the
+// group's (line, step) pairs 32 at a time, so that lanes do not idle on the
+// group's longest line; pairs that fall in the same tile in one round are
+// ranked by lane, which keeps the canonical order.
+constexpr int kEmitThreads = 256;
+
+__global__ void __launch_bounds__(kEmitThreads, 4)
+    k_scan_emit(const tk_line* __restrict__ lines, const tk_path_record* __restrict__ paths, uint32_t path_count,
+                uint32_t* cursors, SegmentRec* segments, uint64_t capacity, uint32_t* error, uint32_t* seg_line,
+                const uint32_t* __restrict__ order, uint32_t* ticket) {
+    __shared__ Scan s_scan[kEmitThreads / 32][32];
+    __shared__ uint32_t s_first[kEmitThreads / 32][33];  // exclusive prefix of the lines' step counts
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t lt_mask = (1u << lane) - 1u;
-    // Warps take paths from a queue, longest first: the line counts are
-    // heavy-tailed and a path is one warp's sequential work.
+    Scan* sc = s_scan[warp];
+    uint32_t* first = s_first[warp];
     for (;;) {
         uint32_t k = 0;
         if (lane == 0) k = atomicAdd(ticket, 1u);
@@ -373,7 +385,7 @@ __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_rec
         const uint32_t pid = order ? __ldg(order + k) : k;
         const tk_path_record p = load_path(paths, pid);
         for (uint32_t g = 0; g < p.line_count; g += 32u) {
-            uint32_t l = g + lane;
+            const uint32_t l = g + lane;
             Scan s;
             bool ok = false;
             if (l < p.line_count) {
@@ -381,46 +393,67 @@ __global__ void k_scan_emit(const tk_line* __restrict__ lines, const tk_path_rec
                 if (line.path_id != pid) atomicOr(error, ERR_LINE_PATH_MISMATCH);
                 else ok = scan_geometry(line, p, s);
             }
-            uint32_t n = ok ? s.imax - s.imin : 0u;
-            uint32_t rounds = __reduce_max_sync(0xffffffffu, n);
-            for (uint32_t r = 0; r < rounds; ++r) {
+            const uint32_t n = ok ? s.imax - s.imin : 0u;
+            uint32_t incl = n;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= uint32_t(o)) incl += v;
+            }
+            const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();  // the previous group's readers are done with sc / first
+            if (n) sc[lane] = s;
+            first[lane] = incl - n;
+            if (lane == 31) first[32] = total;
+            __syncwarp();
+            for (uint32_t base = 0; base < total; base += 32u) {
+                const uint32_t j = base + lane;
                 bool emitting = false;
-                uint32_t off = 0xFFFFFFFFu, i = 0;
+                uint32_t off = 0xFFFFFFFFu, i = 0, L = 0;
                 float z = 0.0f;
                 int32_t tx = 0, ty = 0;
-                if (r < n) {
-                    i = s.imin + r;
-                    z = floorf(s.a * float(i) + s.b);
-                    scan_tile(s, i, z, tx, ty);
-                    if (scan_tile_inside(s, tx, ty)) {
+                if (j < total) {
+                    // the line whose steps hold pair j: the last lane with first <= j
+                    uint32_t lo = 0, hi = 32;
+                    while (hi - lo > 1u) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (first[mid] <= j) lo = mid;
+                        else hi = mid;
+                    }
+                    L = lo;
+                    const Scan& sl = sc[L];
+                    i = sl.imin + (j - first[L]);
+                    z = floorf(sl.a * float(i) + sl.b);
+                    scan_tile(sl, i, z, tx, ty);
+                    if (scan_tile_inside(sl, tx, ty)) {
                         emitting = true;
-                        off = scan_tile_offset(s, tx, ty);
+                        off = scan_tile_offset(sl, tx, ty);
                     }
                 }
                 // A path's cursors are read and written by its warp alone;
                 // __syncwarp orders the lanes' accesses, so they can be plain
                 // (L1-cached) loads and stores. The cursor load is issued
                 // first and the clipped segment computed while it is in flight.
-                uint32_t group = __match_any_sync(0xffffffffu, off);
-                uint32_t base = 0;
-                if (emitting) base = cursors[off];
+                const uint32_t group = __match_any_sync(0xffffffffu, off);
+                uint32_t cbase = 0;
+                if (emitting) cbase = cursors[off];
                 tk_line_segment seg{};
                 float slope = 0.0f;
                 if (emitting) {
-                    seg = clipped_segment(s, i, z, tx, ty);
+                    seg = clipped_segment(sc[L], i, z, tx, ty);
                     const float delta_y = seg.p1y - seg.p0y;
                     slope = delta_y != 0.0f ? (seg.p1x - seg.p0x) / delta_y : 0.0f;
                 }
                 __syncwarp();
                 if (emitting) {
-                    uint32_t leader = __ffs(group) - 1u;
-                    if (lane == leader) cursors[off] = base + __popc(group);
-                    uint32_t slot = base + __popc(group & lt_mask);
+                    const uint32_t leader = __ffs(group) - 1u;
+                    if (lane == leader) cursors[off] = cbase + __popc(group);
+                    const uint32_t slot = cbase + __popc(group & lt_mask);
                     if (slot < capacity) {
                         float4* dst = reinterpret_cast<float4*>(segments + slot);
                         dst[0] = make_float4(seg.p0x, seg.p0y, seg.p1x, seg.p1y);
                         dst[1] = make_float4(seg.y_edge, slope, 0.0f, 0.0f);
-                        if (seg_line) seg_line[slot] = p.line_start + l;
+                        if (seg_line) seg_line[slot] = p.line_start + g + L;
                     } else {
                         atomicOr(error, ERR_SEGMENT_OVERFLOW);
                     }
@@ -481,7 +514,7 @@ void launch_scan_count_paths(const SceneView& s, const uint32_t* list, uint32_t 
 void launch_scan_emit_paths(const SceneView& s, const uint32_t* list, uint32_t n, cudaStream_t st) {
     if (n == 0) return;
     cudaMemsetAsync(s.emit_ticket, 0, sizeof(uint32_t), st);
-    k_scan_emit<<<grid_for(uint64_t(n) * 32, 256, 148 * 8), 256, 0, st>>>(s.lines, s.paths, n, s.cursors, s.segments,
+    k_scan_emit<<<grid_for(uint64_t(n) * 32, kEmitThreads, 148 * 8), kEmitThreads, 0, st>>>(s.lines, s.paths, n, s.cursors, s.segments,
                                                                         s.segment_capacity, s.error, s.seg_line, list,
                                                                         s.emit_ticket);
 }
@@ -496,7 +529,7 @@ void launch_scan_emit(const SceneView& s, cudaStream_t st) {
     if (s.path_count == 0) return;
     uint64_t threads = uint64_t(s.path_count) * 32;
     cudaMemsetAsync(s.emit_ticket, 0, sizeof(uint32_t), st);
-    k_scan_emit<<<grid_for(threads, 256, 148 * 8), 256, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
+    k_scan_emit<<<grid_for(threads, kEmitThreads, 148 * 8), kEmitThreads, 0, st>>>(s.lines, s.paths, s.path_count, s.cursors,
                                                                 s.segments, s.segment_capacity, s.error, s.seg_line,
                                                                 s.emit_order, s.emit_ticket);
 }
