@@ -285,6 +285,10 @@ typedef struct tk_tile_record {
 #define TK_OP_DRAW_BATCH 0u
 #define TK_OP_BLUR_BEGIN 1u
 #define TK_OP_BLUR_END 2u
+/* A progressive blur group: the group's surface blurred with a spatially
+ * varying standard deviation (Filter::ProgressiveBlur), closed by
+ * TK_OP_BLUR_END. batch_id indexes the scene's progressive blurs. */
+#define TK_OP_PROGRESSIVE_BEGIN 3u
 /* BLUR_BEGIN's batch_id word is the blur's sampling (Filter::Blur's
  * BlurSampling, src/shared/layer/filter.rs:183-227): factor | downsample
  * filter << 8 | upsample filter << 16. Factor 0 or 1 blurs at full
@@ -300,13 +304,28 @@ typedef struct tk_tile_record {
 typedef struct tk_op {
     uint32_t kind;
     uint32_t batch_id;     /* DRAW_BATCH: draw_batch_ids value of its draws;
-                              BLUR_BEGIN: TK_BLUR_SAMPLING word (0: full resolution) */
+                              BLUR_BEGIN: TK_BLUR_SAMPLING word (0: full resolution);
+                              PROGRESSIVE_BEGIN: index of its tk_progressive_blur */
     uint32_t layer_start;  /* DRAW_BATCH: fused layer stack range */
     uint32_t layer_end;
     float sigma;           /* BLUR_BEGIN: physical standard deviation */
     int32_t bounds[4];     /* BLUR_BEGIN: output bounds x0,y0,x1,y1 (children's
-                              paint bounds outset by ceil(3 sigma)) */
+                              paint bounds outset by ceil(3 sigma));
+                              PROGRESSIVE_BEGIN: outset by ceil(20 max_std_dev + 8) */
 } tk_op; /* 36 B */
+
+/* Filter::ProgressiveBlur (src/shared/layer/filter/progressive.rs:14-103) in
+ * device pixels: the blur's projection (projection(): the start point and
+ * (end - start) / |end - start|^2, zero for a uniform blur), its maximum
+ * standard deviation (0..65536) and its quality. */
+typedef struct tk_progressive_blur {
+    float start_x, start_y;
+    float dir_x, dir_y;
+    float max_std_dev;
+    uint32_t quality;  /* TK_PROGRESSIVE_BALANCED or TK_PROGRESSIVE_HIGH */
+} tk_progressive_blur;
+#define TK_PROGRESSIVE_BALANCED 0u
+#define TK_PROGRESSIVE_HIGH 1u
 
 /* Scene flags */
 #define TK_SCENE_SEGMENTS_FROM_DEVICE 1u /* recompute segment_start on device */
@@ -352,6 +371,10 @@ typedef struct tk_scene_desc {
     uint32_t glyph_image_count;
     uint32_t glyph_reserved;
     uint64_t glyph_texel_count;
+    /* the progressive blurs PROGRESSIVE_BEGIN ops index */
+    const tk_progressive_blur* progressive_blurs;
+    uint32_t progressive_count;
+    uint32_t progressive_reserved;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

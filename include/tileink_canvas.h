@@ -182,6 +182,13 @@ int32_t tk_canvas_push_blur_group(tk_canvas* c, float sigma);
  * (src/shared/layer/filter.rs:53-60) over the group's output bounds.
  * Returns -1 for a bad sigma or sampling word. */
 int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sampling);
+/* A group blurred by Filter::ProgressiveBlur (src/shared/layer/filter/
+ * progressive.rs:14-103): unchanged before `start`, max_std_dev after `end`,
+ * smoothstep between along the start-end direction (start == end: a uniform
+ * blur of max_std_dev), in logical coordinates; quality TK_PROGRESSIVE_*.
+ * Returns -1 for a non-finite or out-of-range parameter. */
+int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, double start_y, double end_x,
+                                              double end_y, float max_std_dev, uint32_t quality);
 /* Canvas::push_opacity_layer (src/canvas/layers.rs:122-140): the children
  * until the matching pop are composited at `opacity` (clamped to [0, 1],
  * stored as opacity_f32_to_u8) through the nonzero coverage of `path`. The

@@ -67,6 +67,10 @@ def lib() -> C.CDLL:
         l.or_sincos.argtypes = [F32, P, P]
         l.or_atan2.restype = F32
         l.or_atan2.argtypes = [F32, F32]
+        l.or_progressive_blur.restype = I32
+        l.or_progressive_blur.argtypes = [P, U32, U32, P, P]
+        l.or_progressive_levels.restype = U32
+        l.or_progressive_levels.argtypes = [U32, U32, F32, U32, P, U32]
         l.or_text_pow.restype = F32
         l.or_text_pow.argtypes = [F32, F32]
         l.or_glyph_over.restype = U32

@@ -1940,6 +1940,169 @@ void blur_pass(const uint32_t* src, uint32_t* dst, uint32_t w, uint32_t h, const
 // --- filter/resample.hlsli: reduced-resolution blur (BlurSampling factor > 1) ---
 // filter_downsample_pixel for every low texel of `low_rect`: the cell's centre
 // texel (filter 0) or its byte average rounded half up (filter 1).
+// --- filter/progressive.hlsl and progressive/{mod,pyramid}.rs -------------------
+// The progressive blur: a pyramid of RGBA8 levels (each the previous one
+// convolved with a paired Gaussian kernel along x then y and decimated by its
+// step), then per pixel the smoothstep standard deviation of the gradient,
+// interpolated between the two levels that bracket its variance (a 7-tap
+// kernel for sigma <= 1). Level samples are explicit bilinear lerps
+// (a + t (b - a)) with transparent texels outside a level.
+struct ProgLevel {
+    uint32_t w, h;
+    float scale, variance;
+    uint32_t step;
+    std::vector<float> offset, weight;  // paired kernel
+};
+// levels() and gaussian_kernel() (pyramid.rs:17-90) in f32, the host's
+// expf / powf / sqrtf
+std::vector<ProgLevel> prog_levels(uint32_t w, uint32_t h, float sigma, uint32_t quality) {
+    const float octave_steps = quality == TK_PROGRESSIVE_HIGH ? 3.0f : 2.0f;
+    const float min_sigma = quality == TK_PROGRESSIVE_HIGH ? 2.0f : 1.5f;
+    const float support = quality == TK_PROGRESSIVE_HIGH ? 4.0f : 3.0f;
+    std::vector<ProgLevel> levels{{w, h, 1.0f, 0.0f, 1u, {}, {}}};
+    if (sigma <= 1.0f) return levels;
+    float raw_variance = 0.0f, target_sigma = 1.0f;
+    while (levels.back().variance < sigma * sigma) {
+        if (levels.size() > 64) throw std::runtime_error("progressive blur level count overflow");
+        const ProgLevel prev = levels.back();
+        const uint32_t step = target_sigma >= min_sigma * prev.scale * 2.0f ? 2u : 1u;
+        const float scale = prev.scale * float(step);
+        const float reconstruction = scale == 1.0f ? 0.0f : (2.0f * scale * scale + 1.0f) / 12.0f;
+        const float incremental =
+            std::sqrt((target_sigma * target_sigma - reconstruction - raw_variance) / (prev.scale * prev.scale));
+        const int32_t radius = int32_t(std::ceil(incremental * support));
+        const float center = float(step - 1u) * 0.5f;
+        std::vector<float> xs, ws;
+        for (int32_t x = -radius; x < radius + int32_t(step); ++x) {
+            const float d = (float(x) - center) / incremental;
+            xs.push_back(float(x));
+            ws.push_back(std::exp(-0.5f * (d * d)));
+        }
+        float total = 0.0f;
+        for (float v : ws) total += v;
+        float variance = 0.0f;
+        for (size_t k = 0; k < ws.size(); ++k) {
+            ws[k] /= total;
+            const float d = xs[k] - center;
+            variance += ws[k] * (d * d);
+        }
+        ProgLevel L{(prev.w + step - 1u) / step, (prev.h + step - 1u) / step, scale, 0.0f, step, {}, {}};
+        for (size_t k = 0; k < ws.size(); k += 2) {
+            float weight = ws[k], moment = xs[k] * ws[k];
+            if (k + 1 < ws.size()) {
+                weight += ws[k + 1];
+                moment += xs[k + 1] * ws[k + 1];
+            }
+            L.offset.push_back(moment / weight);
+            L.weight.push_back(weight);
+        }
+        raw_variance += variance * prev.scale * prev.scale;
+        L.variance = raw_variance + reconstruction;
+        levels.push_back(std::move(L));
+        target_sigma *= std::pow(2.0f, 1.0f / octave_steps);
+    }
+    if (levels.size() > 64) throw std::runtime_error("progressive blur level count overflow");
+    return levels;
+}
+inline F4 prog_fetch(const std::vector<uint32_t>& img, uint32_t w, uint32_t h, int32_t x, int32_t y) {
+    if (x < 0 || y < 0 || x >= int32_t(w) || y >= int32_t(h)) return {0, 0, 0, 0};
+    return texel_load(img[size_t(y) * w + size_t(x)]);
+}
+inline F4 lerp_f4(F4 a, F4 b, float t) {
+    return {a.r + t * (b.r - a.r), a.g + t * (b.g - a.g), a.b + t * (b.b - a.b), a.a + t * (b.a - a.a)};
+}
+F4 prog_bilinear(const std::vector<uint32_t>& img, uint32_t w, uint32_t h, float px, float py) {
+    const float bx = std::floor(px), by = std::floor(py);
+    const int32_t ix = f2i(bx), iy = f2i(by);
+    const float fx = px - bx, fy = py - by;
+    return lerp_f4(lerp_f4(prog_fetch(img, w, h, ix, iy), prog_fetch(img, w, h, ix + 1, iy), fx),
+                   lerp_f4(prog_fetch(img, w, h, ix, iy + 1), prog_fetch(img, w, h, ix + 1, iy + 1), fx), fy);
+}
+void progressive_blur(uint32_t* surface, uint32_t width, const int32_t rect[4], const tk_progressive_blur& blur) {
+    const uint32_t w = uint32_t(rect[2] - rect[0]), h = uint32_t(rect[3] - rect[1]);
+    const std::vector<ProgLevel> plan = prog_levels(w, h, blur.max_std_dev, blur.quality);
+    std::vector<std::vector<uint32_t>> img(plan.size());
+    img[0].resize(size_t(w) * h);
+    for (uint32_t y = 0; y < h; ++y)
+        for (uint32_t x = 0; x < w; ++x)
+            img[0][size_t(y) * w + x] = surface[size_t(rect[1] + int32_t(y)) * width + size_t(rect[0]) + x];
+    for (size_t i = 1; i < plan.size(); ++i) {  // progressive_blur_reduce along x, then y
+        const ProgLevel& L = plan[i];
+        const ProgLevel& P = plan[i - 1];
+        auto reduce = [&](const std::vector<uint32_t>& src, uint32_t sw, uint32_t sh, std::vector<uint32_t>& dst,
+                          uint32_t dw, uint32_t dh, uint32_t axis) {
+            dst.assign(size_t(dw) * dh, 0u);
+            for (uint32_t y = 0; y < dh; ++y)
+                for (uint32_t x = 0; x < dw; ++x) {
+                    float cx = float(x), cy = float(y);
+                    if (axis == 0u) cx *= float(L.step);
+                    else cy *= float(L.step);
+                    F4 c{0, 0, 0, 0};
+                    for (size_t k = 0; k < L.offset.size(); ++k) {
+                        float px = cx, py = cy;
+                        if (axis == 0u) px += L.offset[k];
+                        else py += L.offset[k];
+                        const F4 sv = prog_bilinear(src, sw, sh, px, py);
+                        const float wt = L.weight[k];
+                        c = {c.r + wt * sv.r, c.g + wt * sv.g, c.b + wt * sv.b, c.a + wt * sv.a};
+                    }
+                    dst[size_t(y) * dw + x] = texel_store(c);
+                }
+        };
+        std::vector<uint32_t> scratch;
+        reduce(img[i - 1], P.w, P.h, scratch, L.w, P.h, 0u);
+        reduce(scratch, L.w, P.h, img[i], L.w, L.h, 1u);
+    }
+    auto sample_level = [&](size_t i, float px, float py) {
+        const ProgLevel& L = plan[i];
+        return prog_bilinear(img[i], L.w, L.h, px / L.scale - 0.5f, py / L.scale - 0.5f);
+    };
+    for (uint32_t y = uint32_t(rect[1]); y < uint32_t(rect[3]); ++y)  // progressive_blur_resolve
+        for (uint32_t x = uint32_t(rect[0]); x < uint32_t(rect[2]); ++x) {
+            float t = 1.0f;
+            if (!(blur.dir_x == 0.0f && blur.dir_y == 0.0f))
+                t = clampf(((float(x) + 0.5f) - blur.start_x) * blur.dir_x +
+                               ((float(y) + 0.5f) - blur.start_y) * blur.dir_y,
+                           0.0f, 1.0f);
+            const float sigma = blur.max_std_dev * t * t * (3.0f - 2.0f * t);
+            if (sigma < 0.125f) continue;
+            const float px = float(x - uint32_t(rect[0])) + 0.5f, py = float(y - uint32_t(rect[1])) + 0.5f;
+            F4 out;
+            if (sigma <= 1.0f) {  // shallow_blur (progressive.hlsl:68-95)
+                float wts[7], total = 0.0f;
+                for (int k = 0; k < 7; ++k) {
+                    const float d = float(k - 3);
+                    wts[k] = exp_nonpos(-0.5f * d * d / (sigma * sigma));
+                    total += wts[k];
+                }
+                float off[4], comb[4];
+                for (int k = 0; k < 4; ++k) {
+                    const int first = 2 * k;
+                    const float second = first + 1 < 7 ? wts[first + 1] : 0.0f;
+                    comb[k] = wts[first] + second;
+                    off[k] = float(first - 3) + (comb[k] > 0.0f ? second / comb[k] : 0.0f);
+                }
+                F4 c{0, 0, 0, 0};
+                for (int j = 0; j < 4; ++j)
+                    for (int k = 0; k < 4; ++k) {
+                        const float wt = comb[k] * comb[j];
+                        const F4 sv = sample_level(0, px + off[k], py + off[j]);
+                        c = {c.r + wt * sv.r, c.g + wt * sv.g, c.b + wt * sv.b, c.a + wt * sv.a};
+                    }
+                const float tt = total * total;
+                out = {c.r / tt, c.g / tt, c.b / tt, c.a / tt};
+            } else {
+                const float variance = sigma * sigma;
+                size_t upper = 1;
+                while (upper + 1 < plan.size() && plan[upper].variance < variance) ++upper;
+                const float lo = plan[upper - 1].variance, hi = plan[upper].variance;
+                const float weight = clampf((variance - lo) / (hi - lo), 0.0f, 1.0f);
+                out = lerp_f4(sample_level(upper - 1, px, py), sample_level(upper, px, py), weight);
+            }
+            surface[size_t(y) * width + x] = texel_store(out);
+        }
+}
+
 void downsample_region(const uint32_t* src, uint32_t* low, uint32_t width, const int32_t rect[4],
                        const int32_t low_rect[4], uint32_t factor, uint32_t filter) {
     const uint32_t x0 = uint32_t(rect[0]), y0 = uint32_t(rect[1]), x1 = uint32_t(rect[2]), y1 = uint32_t(rect[3]);
@@ -2131,7 +2294,14 @@ void raster_scene(or_scene& S, int threads) {
             for (uint32_t tx = 0; tx < S.tw; ++tx) S.band_tiles.push_back(ty * S.tw + tx);
     // Walk ops: batches, passes, blur layers.
     std::vector<uint32_t> main_target(size_t(D.width) * D.height, D.clear_color);
-    struct Surface { std::vector<uint32_t> img; float sigma; int32_t bounds[4]; uint32_t sampling; };
+    struct Surface {
+        std::vector<uint32_t> img;
+        float sigma;
+        int32_t bounds[4];
+        uint32_t sampling;
+        bool progressive = false;
+        tk_progressive_blur prog{};
+    };
     std::vector<Surface> surfaces;
     auto current = [&]() -> std::vector<uint32_t>& { return surfaces.empty() ? main_target : surfaces.back().img; };
     bool pass_open = false;
@@ -2210,6 +2380,17 @@ void raster_scene(or_scene& S, int threads) {
             std::memcpy(s.bounds, op.bounds, sizeof(s.bounds));
             s.sampling = (op.batch_id & 255u) > 1u ? op.batch_id : 0u;  // BlurSampling word
             surfaces.push_back(std::move(s));
+        } else if (op.kind == TK_OP_PROGRESSIVE_BEGIN) {
+            flush_pass();
+            if (op.batch_id >= D.progressive_count) throw std::runtime_error("progressive blur out of range");
+            Surface s;
+            s.img.assign(size_t(D.width) * D.height, 0u);
+            s.sigma = op.sigma;
+            std::memcpy(s.bounds, op.bounds, sizeof(s.bounds));
+            s.sampling = 0u;
+            s.progressive = true;
+            s.prog = D.progressive_blurs[op.batch_id];
+            surfaces.push_back(std::move(s));
         } else if (op.kind == TK_OP_BLUR_END) {
             flush_pass();
             if (surfaces.empty()) throw std::runtime_error("unbalanced BLUR_END");
@@ -2225,7 +2406,12 @@ void raster_scene(or_scene& S, int threads) {
             int32_t sx0 = std::max(s.bounds[0] - rad, 0), sy0 = std::max(s.bounds[1] - rad, 0);
             int32_t sx1 = std::min(s.bounds[2] + rad, int32_t(D.width));
             int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
-            if (s.sampling != 0u && bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
+            if (s.progressive) {
+                if (bx1 > bx0 && by1 > by0 && s.prog.max_std_dev > 0.0f) {
+                    const int32_t rect[4] = {bx0, by0, bx1, by1};
+                    progressive_blur(s.img.data(), D.width, rect, s.prog);
+                }
+            } else if (s.sampling != 0u && bx1 > bx0 && by1 > by0 && s.sigma > 0.0f) {
                 // BlurSampling factor > 1 (render/filter_program/blur.rs:24-73): reduce
                 // the output bounds, blur at sigma / factor, restore
                 const uint32_t factor = s.sampling & 255u;
@@ -2564,6 +2750,33 @@ float or_exp_nonpos(float x) { return exp_nonpos(x); }
 void or_sincos(float x, float* s, float* c) { lib_sincos(x, *s, *c); }
 float or_atan2(float y, float x) { return lib_atan2(y, x); }
 float or_text_pow(float x, float y) { return text_pow(x, y); }
+int32_t or_progressive_blur(uint32_t* surface, uint32_t width, uint32_t height, const int32_t rect[4],
+                            const tk_progressive_blur* blur) {
+    try {
+        const int32_t r[4] = {std::max(rect[0], 0), std::max(rect[1], 0), std::min(rect[2], int32_t(width)),
+                              std::min(rect[3], int32_t(height))};
+        if (r[2] > r[0] && r[3] > r[1] && blur->max_std_dev > 0.0f) progressive_blur(surface, width, r, *blur);
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return -1;
+    }
+}
+uint32_t or_progressive_levels(uint32_t w, uint32_t h, float sigma, uint32_t quality, float* out, uint32_t cap) {
+    const std::vector<ProgLevel> plan = prog_levels(w, h, sigma, quality);
+    for (uint32_t i = 0; i < plan.size() && i < cap; ++i) {
+        const ProgLevel& L = plan[i];
+        const float center = float(L.step - 1u) * 0.5f;
+        float sum = 0.0f, radius = 0.0f;
+        for (size_t k = 0; k < L.weight.size(); ++k) {
+            sum += L.weight[k];
+            radius = std::max(radius, std::ceil(std::fabs(L.offset[k] - center)) + 1.0f);
+        }
+        const float v[7] = {float(L.w), float(L.h), L.scale, L.variance, float(L.step), sum, radius};
+        std::memcpy(out + 7 * i, v, sizeof(v));
+    }
+    return uint32_t(plan.size());
+}
 uint32_t or_glyph_over(uint32_t destination, uint32_t source, uint32_t coverage) {
     return src_over_mask_linear_auto_u8(destination, source, coverage);
 }

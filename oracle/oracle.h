@@ -126,6 +126,13 @@ float or_atan2(float y, float x);
 /* The library's pow for the text gamma (x > 0), and the glyph outline
  * composite src_over_mask_linear_auto_u8 (fine/text/auto.hlsli:28-33). */
 float or_text_pow(float x, float y);
+/* The progressive blur of `surface` (width x height, RGBA8) inside `rect`,
+ * and its pyramid plan: per level w, h, scale, variance, step, kernel weight
+ * sum and kernel radius (max ceil(|offset - centre|) + 1), 7 floats each;
+ * returns the level count. */
+int32_t or_progressive_blur(uint32_t* surface, uint32_t width, uint32_t height, const int32_t rect[4],
+                            const tk_progressive_blur* blur);
+uint32_t or_progressive_levels(uint32_t w, uint32_t h, float sigma, uint32_t quality, float* out, uint32_t cap);
 uint32_t or_glyph_over(uint32_t destination, uint32_t source, uint32_t coverage);
 /* Fine-only image of a scene of SDF draws: every draw interpreted in every
  * tile as a PTCL_SDF particle, from the clear colour (no coarse stage). */

@@ -92,3 +92,23 @@ def sampled_blur_scene(seed, factor, down, up, w=200, h=150, sigma=5.0):
     c.pop_layer()
     c.push_path(blob(rng, w * 0.5, h * 0.5, 20), tk.Brush.solid(0.1, 0.2, 0.3, 0.5))
     return c
+
+
+def progressive_scene(seed, w=200, h=150, sigma=6.0, quality=0, uniform=False):
+    """Fills inside a progressive blur group (Filter::ProgressiveBlur),
+    sharp at one side and blurred up to `sigma` at the other, over fills
+    outside it."""
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(w, h)
+    c.set_clear_color(0xFFFFFFFF)
+    for _ in range(4):
+        c.push_path(blob(rng, rng.uniform(0, w), rng.uniform(0, h), 30), tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0))
+    start = (rng.uniform(0, w * 0.4), rng.uniform(0, h * 0.4))
+    end = start if uniform else (rng.uniform(w * 0.5, w), rng.uniform(h * 0.5, h))
+    c.push_progressive_blur_group(start, end, sigma, quality)
+    for k in range(10):
+        c.push_path(blob(rng, rng.uniform(10, w - 10), rng.uniform(10, h - 10), rng.uniform(6, 40)),
+                    tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.4, 1))), fill_rule=k % 2)
+    c.pop_layer()
+    c.push_path(blob(rng, w * 0.5, h * 0.5, 20), tk.Brush.solid(0.1, 0.2, 0.3, 0.5))
+    return c

@@ -30,6 +30,7 @@ DTYPE_MIRRORS = {
     "tk_tile_record": N.TILE_DTYPE, "tk_op": N.OP_DTYPE, "tk_flatten_el": N.FLATTEN_EL_DTYPE,
     "tk_stroke_polyline": N.POLYLINE_DTYPE, "tk_stroke_desc": N.STROKE_DTYPE,
     "tk_glyph_run": N.GLYPH_RUN_DTYPE, "tk_glyph": N.GLYPH_DTYPE, "tk_glyph_image": N.GLYPH_IMAGE_DTYPE,
+    "tk_progressive_blur": N.PROGRESSIVE_DTYPE,
 }
 
 

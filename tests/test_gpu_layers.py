@@ -104,3 +104,13 @@ def test_gpu_sampled_blur_matches_oracle(renderer, factor, down, up):
     upsample, composite — bit-exact against the oracle."""
     from layer_cases import sampled_blur_scene
     compare_frame(renderer, sampled_blur_scene(factor * 7 + down, factor, down, up, sigma=6.5))
+
+
+@pytest.mark.parametrize("seed, sigma, quality, uniform", [(1, 6.0, 0, False), (2, 9.5, 1, False), (3, 4.0, 0, True),
+                                                            (4, 0.9, 0, False), (5, 24.0, 1, False)])
+def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uniform):
+    """Progressive blur groups (Filter::ProgressiveBlur; filter/progressive.hlsl):
+    the pyramid reductions, the variance-bracketing resolve and the 7-tap
+    shallow blur, bit-exact against the oracle."""
+    from layer_cases import progressive_scene
+    compare_frame(renderer, progressive_scene(seed, sigma=sigma, quality=quality, uniform=uniform))

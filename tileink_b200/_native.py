@@ -90,6 +90,10 @@ GLYPH_RUN_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4")])
 GLYPH_DTYPE = np.dtype([("image", "<u4"), ("x", "<i4"), ("y", "<i4")])
 GLYPH_IMAGE_DTYPE = np.dtype([("left", "<i4"), ("top", "<i4"), ("width", "<u4"), ("height", "<u4"),
                               ("content", "<u4"), ("data_offset", "<u4")])
+PROGRESSIVE_DTYPE = np.dtype([("start_x", "<f4"), ("start_y", "<f4"), ("dir_x", "<f4"), ("dir_y", "<f4"),
+                              ("max_std_dev", "<f4"), ("quality", "<u4")])
+PROGRESSIVE_BALANCED, PROGRESSIVE_HIGH = 0, 1
+OP_PROGRESSIVE_BEGIN = 3
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
 GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
 PTCL_GLYPH = 10
@@ -123,6 +127,7 @@ class SceneDesc(C.Structure):
         ("glyph_runs", C.c_void_p), ("glyphs", C.c_void_p), ("glyph_images", C.c_void_p),
         ("glyph_texels", C.c_void_p), ("glyph_run_count", C.c_uint32), ("glyph_count", C.c_uint32),
         ("glyph_image_count", C.c_uint32), ("glyph_reserved", C.c_uint32), ("glyph_texel_count", C.c_uint64),
+        ("progressive_blurs", C.c_void_p), ("progressive_count", C.c_uint32), ("progressive_reserved", C.c_uint32),
     ]
 
 
@@ -288,6 +293,7 @@ def library() -> C.CDLL:
         "tk_canvas_push_path": (I64, [P, P, C.POINTER(BrushDesc), P, U32, F64]),
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
         "tk_canvas_push_glyph_outlines": (I64, [P, P, C.POINTER(BrushDesc), P, F64]),
+        "tk_canvas_push_progressive_blur_group": (I32, [P, F64, F64, F64, F64, C.c_float, U32]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),
@@ -358,6 +364,7 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "glyphs": arr(d.glyphs, d.glyph_count, GLYPH_DTYPE),
         "glyph_images": arr(d.glyph_images, d.glyph_image_count, GLYPH_IMAGE_DTYPE),
         "glyph_texels": arr(d.glyph_texels, d.glyph_texel_count, np.uint32),
+        "progressive": arr(d.progressive_blurs, d.progressive_count, PROGRESSIVE_DTYPE),
     }
 
 
@@ -383,10 +390,11 @@ class ArrayScene:
         if shadow is not None and len(shadow):
             d.sdf_shadow_blob, d.sdf_shadow_word_count = ptr(shadow), len(shadow)
         for key, cnt in (("glyph_runs", "glyph_run_count"), ("glyphs", "glyph_count"),
-                         ("glyph_images", "glyph_image_count"), ("glyph_texels", "glyph_texel_count")):
+                         ("glyph_images", "glyph_image_count"), ("glyph_texels", "glyph_texel_count"),
+                         ("progressive", "progressive_count")):
             v = a.get(key)
             if v is not None and len(v):
-                setattr(d, key, ptr(v))
+                setattr(d, "progressive_blurs" if key == "progressive" else key, ptr(v))
                 setattr(d, cnt, len(v))
         images = [np.ascontiguousarray(im, dtype=np.uint32) for im in a.get("images", [])]
         if images:

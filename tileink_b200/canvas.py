@@ -438,6 +438,16 @@ class Canvas:
         if self._lib.tk_canvas_push_opacity_layer(self._h, path._h, t, float(tolerance), float(opacity)) != 0:
             raise ValueError("push_opacity_layer rejected its arguments")
 
+    def push_progressive_blur_group(self, start, end, max_std_dev: float, quality=N.PROGRESSIVE_BALANCED) -> None:
+        """Children until pop_layer() are blurred by Filter::ProgressiveBlur
+        (src/shared/layer/filter/progressive.rs:14-103): unchanged before
+        `start`, max_std_dev after `end`, smoothstep between (start == end: a
+        uniform blur)."""
+        r = self._lib.tk_canvas_push_progressive_blur_group(self._h, float(start[0]), float(start[1]), float(end[0]),
+                                                            float(end[1]), float(max_std_dev), int(quality))
+        if r != 0:
+            raise ValueError("bad progressive blur")
+
     def push_blur_group(self, sigma: float, factor: int = 1, downsample: int = N.BLUR_DOWNSAMPLE_BOX,
                         upsample: int = N.BLUR_UPSAMPLE_BILINEAR):
         """Canvas::push_blur_group; factor > 1 blurs through a copy reduced

@@ -97,6 +97,8 @@ struct Step {
     float sigma;
     int32_t bounds[4];
     uint32_t sampling = 0u;  // BLUR_BEGIN: TK_BLUR_SAMPLING_* word (0: full resolution)
+    bool progressive = false;  // BLUR_BEGIN of a progressive blur group
+    tk_progressive_blur prog{};
 };
 
 // State of the last differentiable forward, kept for its backward.
@@ -162,6 +164,7 @@ struct tk_ctx {
     DBuf<tk::PaintInfo> paints;  // per draw, built at upload
     uint64_t segment_needed = 0;  // device plan: total from the last frame
     DBuf<uint32_t> image, temp, low;  // target, blur temporary, reduced-resolution blur surface
+    tk::ProgressiveScratch prog_scratch;  // progressive blur levels (grown on demand)
     std::vector<DBuf<uint32_t>> surfaces;
     bool rendered = false;
     // paths by decreasing line count: the order scan_emit's warps take them
@@ -434,6 +437,21 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                 invalid("bad blur sampling");
             Step s{STEP_BLUR_BEGIN, 0u, op.sigma, {op.bounds[0], op.bounds[1], op.bounds[2], op.bounds[3]},
                    factor > 1u ? op.batch_id : 0u};
+            c->steps.push_back(s);
+            ++depth;
+        } else if (op.kind == TK_OP_PROGRESSIVE_BEGIN) {
+            open = false;
+            if (op.layer_end > op.layer_start) invalid("blur groups under clip layers are outside this path");
+            if (op.batch_id >= d.progressive_count || !d.progressive_blurs) invalid("progressive blur out of range");
+            const tk_progressive_blur& pb = d.progressive_blurs[op.batch_id];
+            // projection() and the device-space limit (progressive.rs:71-93)
+            if (!std::isfinite(pb.start_x) || !std::isfinite(pb.start_y) || !std::isfinite(pb.dir_x) ||
+                !std::isfinite(pb.dir_y) || !(pb.max_std_dev >= 0.0f && pb.max_std_dev <= 65536.0f) ||
+                pb.quality > TK_PROGRESSIVE_HIGH)
+                invalid("bad progressive blur");
+            Step s{STEP_BLUR_BEGIN, 0u, pb.max_std_dev, {op.bounds[0], op.bounds[1], op.bounds[2], op.bounds[3]}, 0u};
+            s.progressive = true;
+            s.prog = pb;
             c->steps.push_back(s);
             ++depth;
         } else if (op.kind == TK_OP_BLUR_END) {
@@ -936,7 +954,16 @@ void do_render(tk_ctx* c) {
             int32_t sx0 = std::max(b.bounds[0] - rad, 0), sy0 = std::max(b.bounds[1] - rad, 0);
             int32_t sx1 = std::min(b.bounds[2] + rad, W), sy1 = std::min(b.bounds[3] + rad, H);
             StageMark m(c, 8);
-            if (b.sampling != 0u && ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
+            if (b.progressive) {
+                // Filter::ProgressiveBlur over the output bounds
+                // (native/runtime/program/filter/progressive/mod.rs:44-146)
+                if (ob[2] > ob[0] && ob[3] > ob[1] && b.prog.max_std_dev > 0.0f) {
+                    const int32_t rc = tk::launch_progressive_blur(surf, c->width, c->height, ob, b.prog,
+                                                                   c->prog_scratch, st);
+                    if (rc == -1) throw Fail{TK_E_CAPACITY, "progressive blur level count overflow"};
+                    if (rc == -2) throw Fail{TK_E_ALLOC, "progressive blur levels: out of device memory"};
+                }
+            } else if (b.sampling != 0u && ob[2] > ob[0] && ob[3] > ob[1] && b.sigma > 0.0f) {
                 // BlurSampling with factor > 1 (render/filter_program/blur.rs:194-212):
                 // reduce, blur at sigma / factor, restore, over the output bounds
                 tk::launch_blur_downsampled(surf, c->low.ptr, c->temp.ptr, c->width, c->height, ob, b.sigma,
@@ -1434,6 +1461,7 @@ void tk_ctx_destroy(tk_ctx* c) {
     c->item_desc.release(); c->tile_desc.release(); c->stats.release(); c->backdrops.release();
     c->counts.release(); c->cursors.release(); c->bumps.release(); c->misc.release();
     c->ranges.release(); c->segments.release(); c->image.release(); c->temp.release();
+    tk::release_progressive(c->prog_scratch);
     for (auto& s : c->surfaces) s.release();
     for (auto& p : c->passes) {
         p.d_batches.release(); p.bin_lists.release(); p.bin_counts.release(); p.tiles.release(); p.ptcl.release();

@@ -362,7 +362,8 @@ struct Cmd {
     uint32_t draw;
     float sigma;
     uint32_t children;
-    uint32_t payload = 0u;  // OPACITY: opacity_f32_to_u8 of the layer's opacity
+    uint32_t payload = 0u;     // OPACITY: opacity_f32_to_u8 of the layer's opacity; BLUR: sampling
+    int32_t progressive = -1;  // BLUR of a progressive blur: its index in the canvas's progressive blurs
 };
 
 // One recorded Canvas call with its original geometry, for replay into
@@ -375,7 +376,9 @@ struct GlyphImage {
 };
 
 struct RecCmd {
-    enum Kind : uint8_t { FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN } kind = FILL;
+    enum Kind : uint8_t {
+        FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN, PROGRESSIVE
+    } kind = FILL;
     // GLYPH_RUN: the glyphs (image = index into run_images or TK_INVALID_INDEX),
     // their images and the optional clip rect
     std::vector<tk_glyph> run_glyphs;
@@ -436,6 +439,7 @@ struct tk_canvas {
     std::vector<uint32_t> glyph_texels;
     std::vector<tk_glyph_run> glyph_runs;
     std::vector<tk_glyph> glyphs;
+    std::vector<tk_progressive_blur> progressive;  // device-pixel progressive blurs
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -690,6 +694,13 @@ void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record
             bool any = false;
             paint_bounds(c, cmd.children, pb, any);
             int32_t out_r = int32_t(std::ceil(std::max(cmd.sigma, 0.0f) * 3.0f));
+            if (cmd.progressive >= 0) {
+                // sample_outset (shared/layer/filter/progressive.rs:95-103):
+                // the upper pyramid level's support with its reconstruction
+                begin.op.kind = TK_OP_PROGRESSIVE_BEGIN;
+                begin.op.batch_id = uint32_t(cmd.progressive);
+                out_r = cmd.sigma > 0.0f ? int32_t(std::ceil(20.0f * cmd.sigma + 8.0f)) : 0;
+            }
             if (any) {
                 begin.op.bounds[0] = std::max(pb.x0 - out_r, 0);
                 begin.op.bounds[1] = std::max(pb.y0 - out_r, 0);
@@ -1502,6 +1513,45 @@ int32_t tk_canvas_push_clip_layer(tk_canvas* c, const tk_path* path, const doubl
     }
     return 0;
 }
+int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, double start_y, double end_x,
+                                              double end_y, float max_std_dev, uint32_t quality) {
+    if (!c || quality > TK_PROGRESSIVE_HIGH) return -1;
+    // ProgressiveBlur::scaled (the canvas scale), then projection()
+    // (shared/layer/filter/progressive.rs:71-93)
+    const double s = double(c->scale);
+    const double sx = start_x * s, sy = start_y * s, ex = end_x * s, ey = end_y * s;
+    const float sd = max_std_dev * c->scale;
+    const double dx = ex - sx, dy = ey - sy, length2 = dx * dx + dy * dy;
+    if (!std::isfinite(sd) || !(sd >= 0.0f && sd <= 65536.0f) || !std::isfinite(length2)) return -1;
+    tk_progressive_blur pb{float(sx), float(sy), 0.0f, 0.0f, sd, quality};
+    if (length2 != 0.0) {
+        pb.dir_x = float(dx / length2);
+        pb.dir_y = float(dy / length2);
+    }
+    if (!std::isfinite(pb.start_x) || !std::isfinite(pb.start_y) || !std::isfinite(pb.dir_x) ||
+        !std::isfinite(pb.dir_y))
+        return -1;
+    const uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    Cmd cmd{Cmd::BLUR, 0u, sd, child, 0u};
+    cmd.progressive = int32_t(c->progressive.size());
+    c->progressive.push_back(pb);
+    c->lists[c->stack.back()].push_back(cmd);
+    c->stack.push_back(child);
+    c->dirty = true;
+    if (c->keep) {
+        RecCmd r = rec_cmd(RecCmd::PROGRESSIVE, nullptr, nullptr, nullptr);
+        r.shape.p0[0] = start_x;
+        r.shape.p0[1] = start_y;
+        r.shape.p1[0] = end_x;
+        r.shape.p1[1] = end_y;
+        r.sigma = max_std_dev;
+        r.sampling = quality;
+        c->log.push_back(std::move(r));
+    }
+    return 0;
+}
+
 int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sampling) {
     float physical = sigma * c->scale;
     if (!(sigma >= 0.0f) || !std::isfinite(physical)) return -1;
@@ -1588,6 +1638,8 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->glyph_image_count = uint32_t(c->glyph_images.size());
     out->glyph_texels = c->glyph_texels.data();
     out->glyph_texel_count = c->glyph_texels.size();
+    out->progressive_blurs = c->progressive.data();
+    out->progressive_count = uint32_t(c->progressive.size());
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -2080,6 +2132,18 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
         case RecCmd::CLIP: return tk_canvas_push_clip_layer(dst, &r.path, t, r.rule, r.tolerance);
         case RecCmd::OPACITY: return tk_canvas_push_opacity_layer(dst, &r.path, t, r.tolerance, r.sigma);
         case RecCmd::BLUR: return tk_canvas_push_blur_group_sampled(dst, r.sigma, r.sampling);
+        case RecCmd::PROGRESSIVE: {
+            // ProgressiveBlur::translated (canvas/offset.rs:153-154): translations only
+            double dx = 0.0, dy = 0.0;
+            if (t) {
+                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+                dx = t[4];
+                dy = t[5];
+            }
+            return tk_canvas_push_progressive_blur_group(dst, r.shape.p0[0] + dx, r.shape.p0[1] + dy,
+                                                         r.shape.p1[0] + dx, r.shape.p1[1] + dy, r.sigma,
+                                                         r.sampling);
+        }
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
         case RecCmd::SDF:
         case RecCmd::SDF_CLIP: {
@@ -2121,7 +2185,8 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
 
 bool has_layers(const std::vector<RecCmd>& log) {
     for (const RecCmd& r : log)
-        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::SDF_CLIP ||
+        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::PROGRESSIVE ||
+            r.kind == RecCmd::SDF_CLIP ||
             r.kind == RecCmd::OPACITY)
             return true;
     return false;

@@ -3,6 +3,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+#include <vector>
+
 #include "../../include/tileink.h"
 
 namespace tkf {
@@ -213,6 +216,31 @@ struct BlurParams {
 };
 void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaStream_t st);
 void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st);
+
+// Progressive blur (progressive.cu). A pyramid level: its size, scale and
+// cumulative variance, its decimation step and its paired kernel (offset,
+// weight); level 0 is the blurred region itself.
+constexpr uint32_t kProgressiveMaxLevels = 64;  // the reference's level table
+struct ProgressiveLevel {
+    uint32_t w = 0, h = 0;
+    float scale = 1.0f, variance = 0.0f;
+    uint32_t step = 1;
+    std::vector<std::pair<float, float>> kernel;
+};
+std::vector<ProgressiveLevel> progressive_levels(uint32_t w, uint32_t h, float sigma, uint32_t quality);
+// Device memory the context keeps for it (levels concatenated, one scratch).
+struct ProgressiveScratch {
+    uint32_t* levels = nullptr;
+    uint64_t levels_cap = 0;
+    uint32_t* scratch = nullptr;
+    uint64_t scratch_cap = 0;
+};
+// The progressive blur of `surface` inside `rect` (clipped to the surface):
+// 1 when it ran, 0 for an empty rect or no blur, -1 for a pyramid beyond
+// kProgressiveMaxLevels or too many taps, -2 when memory ran out.
+int32_t launch_progressive_blur(uint32_t* surface, uint32_t width, uint32_t height, const int32_t rect[4],
+                                const tk_progressive_blur& blur, ProgressiveScratch& s, cudaStream_t st);
+void release_progressive(ProgressiveScratch& s);
 // The blur of `surface` inside `rect` (x0, y0, x1, y1) through a reduced copy
 // (BlurSampling with factor > 1, filter/resample.hlsli): downsample into
 // `low`, blur there at sigma / factor (`temp` holds the horizontal pass),
