@@ -486,7 +486,7 @@ def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
     return line
 
 
-BANDS = 32  # the CPU arms' step: every BANDS-th tile row of the frame
+BANDS = 64  # the CPU arms' step: every BANDS-th tile row of the frame
 
 
 def oracle_band_step(run, desc, k, threads):

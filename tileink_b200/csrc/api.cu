@@ -133,6 +133,7 @@ struct tk_ctx {
     uint64_t line_count = 0, brush_words = 0, pool_len = 0, host_segment_capacity = 0;
     uint64_t sdf_words = 0, sdf_shadow_base = 0;  // SDF buffer: sdf_blob, then sdf_shadow_blob
     bool sdf_ext = false;                          // a candlestick, dash line, triangle or checkerboard
+    bool text = false;                             // glyph outline fills or glyph runs
     uint32_t path_count = 0, draw_count = 0, layer_count = 0, order_count = 0;
     std::vector<tk_path_record> h_paths;
     std::vector<tk::ScanItem> h_items;
@@ -322,11 +323,13 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             invalid("glyph image " + std::to_string(k) + " outside the glyph texels");
     }
     bool sdf_ext = false;
+    bool text = false;
     // Draws: path fills/clips, and brush draws of the SDF kinds this library
     // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
     for (uint32_t i = 0; i < d.draw_count; ++i) {
         const tk_draw_record& r = d.draws[i];
         const std::string at = "draw " + std::to_string(i);
+        if (r.tag == TK_DRAW_PATH_GLYPH || r.glyph_run_id != TK_INVALID_INDEX) text = true;
         if (r.glyph_run_id != TK_INVALID_INDEX) {
             // a glyph run draw (canvas/primitives/text.rs:80-96)
             if (r.glyph_run_id >= d.glyph_run_count) invalid(at + ": glyph run out of range");
@@ -481,6 +484,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     c->sdf_shadow_base = d.sdf_word_count;
     c->sdf_ext = sdf_ext;
     c->glyph_run_count = d.glyph_run_count;
+    c->text = text;
     c->pool_len = pool;
     c->host_segment_capacity = seg_cap;
     c->h_paths.assign(d.paths, d.paths + d.path_count);
@@ -512,6 +516,7 @@ tk::SceneView view(tk_ctx* c) {
     s.sdf_words = c->sdf_words;
     s.sdf_shadow_base = c->sdf_shadow_base;
     s.sdf_ext = c->sdf_ext;
+    s.text = c->text;
     s.texels = c->texels.ptr;
     if (c->glyph_run_count) {
         s.glyph_runs = c->glyph_runs.ptr;
@@ -1208,6 +1213,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     uint64_t pool = 0, segs = 0, list = 0, pixels = 0;
     uint32_t tiles = 0, bins = 0, batch_base = 0;
     bool ext = false;  // some scene has SDF records of an extended kind
+    bool text = false;  // some scene has glyph outline fills
     for (uint32_t s = 0; s < n; ++s) {
         const tk_scene_desc& d = scenes[s];
         if (d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE) invalid("batched scenes use host segment planning");
@@ -1215,6 +1221,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
         if (d.glyph_run_count) invalid("scene " + std::to_string(s) + ": glyph runs are not batched");
         validate_and_plan(c, d);
         ext = ext || c->sdf_ext;
+        text = text || c->text;
         uint32_t npass = 0;
         for (const Step& st : c->steps) {
             if (st.kind != STEP_PASS) invalid("scene " + std::to_string(s) + ": blur groups are not batched");
@@ -1329,6 +1336,7 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     c->brush_words = brush.size();
     c->sdf_shadow_base = sdf.size();
     c->sdf_ext = ext;
+    c->text = text;
     sdf.insert(sdf.end(), shadow.begin(), shadow.end());
     c->sdf_words = sdf.size();
     c->pool_len = pool;

@@ -563,7 +563,10 @@ __device__ __noinline__ float4 composite_glyphs(const FineSmem& S, const Paint P
 // branch, which costs the record loop about 3% even when never taken; the
 // extended kinds' code costs the base kinds more, so it has its own instance,
 // with the registers of 3 CTAs per SM.
-template <uint32_t SDF>
+// TEXT: the scene has glyph outline fills or glyph runs; their compositing
+// runs out of line, and only this instance holds the calls, so that scenes
+// without text keep the record loop's registers.
+template <uint32_t SDF, bool TEXT>
 __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
     k_fine(const tk_tile_record* __restrict__ tiles, const tk_ptcl_record* __restrict__ ptcl,
            const SegmentRec* __restrict__ segments, const PaintInfo* __restrict__ paints,
@@ -630,7 +633,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
             }
             S.nseg[tid] = n;
             if (SDF != 0u && a.x == TK_PTCL_BEGIN_SDF_CLIP) S.umode[tid] = __ldg(&paints[c.y].sdf);
-            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || a.x == TK_PTCL_GLYPH ||
+            if (a.x == TK_PTCL_FILL || a.x == TK_PTCL_PATH_GLYPH || (TEXT && a.x == TK_PTCL_GLYPH) ||
                 (SDF != 0u && (a.x == TK_PTCL_SDF || a.x == TK_PTCL_IMAGE))) {
                 const PaintInfo* pi = paints + c.y;
                 if (SDF != 0u && a.x == TK_PTCL_SDF) S.umode[tid] = __ldg(&pi->sdf);  // SDF records: the shape's first word
@@ -802,7 +805,7 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                     const uint32_t masked = combine_alpha(alpha, clip);
                     if (masked != 0u) paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
                 }
-            } else if (tag == TK_PTCL_GLYPH) {
+            } else if (TEXT && tag == TK_PTCL_GLYPH) {
                 // fine/interpreter.hlsli:93-106: the run's glyphs inside the
                 // draw's exact pixel bounds
                 const tk_draw_record* dr = draws + qb.y;
@@ -868,8 +871,13 @@ __global__ void __launch_bounds__(kFineThreads, SDF == 2u ? 3 : 4)
                 } else {
                     const uint32_t masked = clip == 255u ? alpha : combine_alpha(alpha, clip);
                     if (masked != 0u) {
-                        if (tag == TK_PTCL_PATH_GLYPH) px = paint_glyph_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
-                        else paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
+                        if (TEXT && tag == TK_PTCL_PATH_GLYPH) {
+                            px = paint_glyph_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
+                        } else {
+                            // text instances take every glyph outline fill
+                            if (!TEXT && tag == TK_PTCL_PATH_GLYPH) atomicOr(error, ERR_UNSUPPORTED);
+                            paint_fill<SDF != 0u>(S, P, i, masked, gx, gy, px);
+                        }
                     }
                 }
             }
@@ -905,13 +913,14 @@ void launch_fine(const SceneView& s, const PassView& p, uint32_t* target, cudaSt
     if (T == 0) return;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(k_fine<0u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
-        cudaFuncSetAttribute(k_fine<1u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
-        cudaFuncSetAttribute(k_fine<2u>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
+        for (auto k : {k_fine<0u, false>, k_fine<1u, false>, k_fine<2u, false>, k_fine<0u, true>, k_fine<1u, true>,
+                       k_fine<2u, true>})
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(FineSmem)));
         configured = true;
     }
     if (s.sdf_ext) k_star_table<<<1, 32, 0, st>>>();
-    auto kernel = !s.sdf_words ? k_fine<0u> : (s.sdf_ext ? k_fine<2u> : k_fine<1u>);
+    auto kernel = s.text ? (!s.sdf_words ? k_fine<0u, true> : (s.sdf_ext ? k_fine<2u, true> : k_fine<1u, true>))
+                         : (!s.sdf_words ? k_fine<0u, false> : (s.sdf_ext ? k_fine<2u, false> : k_fine<1u, false>));
     const GlyphView glyphs{p.glyph_list, s.glyphs, s.glyph_images, s.glyph_texels};
     kernel<<<T, kFineThreads, sizeof(FineSmem), st>>>(p.tiles, p.ptcl, s.segments, s.paints, s.brush, s.brush_words,
                                                       s.texels, s.draws, s.sdf, s.segment_capacity, target, s.width, s.height,

@@ -73,6 +73,7 @@ struct SceneView {
     uint64_t sdf_words;
     uint64_t sdf_shadow_base;
     bool sdf_ext;  // some record is of an extended kind (fine's k_fine<2>)
+    bool text;     // glyph outline fills or glyph runs (fine's text instances)
     const uint32_t* texels;  // the scene's images, concatenated (premultiplied RGBA8)
     // the text blob (null without glyph runs)
     const tk_glyph_run* glyph_runs;
