@@ -320,8 +320,9 @@ static __device__ __noinline__ uint32_t sdf_particle(const tk_draw_record* draws
 }
 
 // SDF: whether the scene has SDF records; path-only scenes run the instance
-// without the SDF candidate handling.
-template <bool EMIT, bool SDF>
+// without the SDF candidate handling. TEXT: whether it has glyph runs; the
+// glyph particle handling (and its calls) lives only in those instances.
+template <bool EMIT, bool SDF, bool TEXT>
 __global__ void __launch_bounds__(kCoarseThreads)
     k_coarse(Ctx c, const uint32_t* __restrict__ bin_lists, const uint32_t* __restrict__ bin_counts, uint32_t draw_n,
              uint32_t nbx, const uint32_t* __restrict__ batch_ids, const PassBatch* __restrict__ batches,
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
     uint64_t at = 0, gat = 0;
     if (EMIT && live) {
         at = tiles[tile].ptcl_start;
-        gat = tiles[tile].glyph_start;
+        if (TEXT) gat = tiles[tile].glyph_start;
     }
     uint32_t total = 0, glyph_total = 0;
     uint32_t cur = 0xFFFFFFFFu, wrappers = 0, nb = 0, flags = 0;
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
             };
             // a glyph run draw gives a PTCL_GLYPH particle or none
             // (coarse/emit_draw.hlsli:15-22)
-            const bool glyph = c.glyph_runs && d.glyph_run_id != TK_INVALID_INDEX;
+            const bool glyph = TEXT && c.glyph_runs && d.glyph_run_id != TK_INVALID_INDEX;
             const bool has_sdf = !glyph && SDF &&
                                  (d.sdf_offset != TK_INVALID_INDEX || d.sdf_shadow_offset != TK_INVALID_INDEX);
             uint32_t sdf_bits = 0u;
@@ -489,7 +490,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     sdf_hit |= 1u << q;
                     continue;
                 }
-                if (meta & kMetaGlyph) {
+                if (TEXT && (meta & kMetaGlyph)) {
                     glyph_hit |= 1u << q;
                     continue;
                 }
@@ -512,7 +513,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                 const uint32_t w = ww[q];  // 0 for SDF and glyph draws
                 uint32_t ptag = TK_PTCL_FILL;
                 uint32_t glyphs_here = 0u;
-                if (glyph_hit & (1u << q)) {
+                if (TEXT && (glyph_hit & (1u << q))) {
                     glyphs_here = draw_glyphs(c, d.draw, d.px, d.py, tx, ty, nullptr, 0u, 0u, error);
                     if (glyphs_here == 0u) continue;
                     ptag = TK_PTCL_GLYPH;
@@ -550,7 +551,7 @@ __global__ void __launch_bounds__(kCoarseThreads)
                     flags |= cls;
                     uint32_t color = ptag == TK_PTCL_COLOR ? d.color : (tag == TK_DRAW_CLIP ? 0u : d.draw);
                     if (wrappers == 0u && ptag == TK_PTCL_COLOR && (color >> 24) == 255u && nb > 0u) flags |= kChunkClassOccluder;
-                    if (ptag == TK_PTCL_GLYPH) {
+                    if (TEXT && ptag == TK_PTCL_GLYPH) {
                         // the tile's glyph list continues at gat (coarse/emit.hlsl:54-58)
                         draw_glyphs(c, d.draw, d.px, d.py, tx, ty, glyph_list, gat, glyph_cap, error);
                         store_ptcl(ptcl, cap, at++, ptag, 0u, 0u, uint32_t(gat), uint32_t(gat + glyphs_here), color,
@@ -696,9 +697,14 @@ void launch_coarse(const SceneView& s, const PassView& p, bool emit, cudaStream_
           s.ranges, s.tw, s.th, s.glyph_runs, s.glyphs, s.glyph_images, s.glyph_run_count};
     const uint32_t nbins = p.scenes ? p.total_bins : p.nbx * p.nby;
     if (nbins == 0) return;
-    const bool sdf = s.sdf_words != 0;
-    auto kernel = emit ? (sdf ? k_coarse<true, true> : k_coarse<true, false>)
-                       : (sdf ? k_coarse<false, true> : k_coarse<false, false>);
+    const bool sdf = s.sdf_words != 0, text = s.glyph_runs != nullptr;
+    using Kernel = decltype(&k_coarse<true, true, true>);
+    const Kernel table[2][2][2] = {
+        {{k_coarse<false, false, false>, k_coarse<false, false, true>},
+         {k_coarse<false, true, false>, k_coarse<false, true, true>}},
+        {{k_coarse<true, false, false>, k_coarse<true, false, true>},
+         {k_coarse<true, true, false>, k_coarse<true, true, true>}}};
+    const Kernel kernel = table[emit][sdf][text];
     kernel<<<nbins * kQuads, kCoarseThreads, 0, st>>>(c, p.bin_lists, p.bin_counts, p.draw_n, p.nbx, s.batch_ids,
                                                       p.batches, p.batch0, p.tiles, p.ptcl, p.ptcl_capacity, p.stats,
                                                       s.error, p.scenes, p.bin_scene, p.tile_active, p.glyph_list,
