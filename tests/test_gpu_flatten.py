@@ -98,6 +98,20 @@ def stroke_scene(device: bool):
                 c.push_stroke(p, tk.Brush.solid((k % 7) / 7, (k % 5) / 5, (k % 3) / 3, 0.6), w, transform=t,
                               tolerance=0.05 + 0.05 * (k % 3))
                 k += 1
+    # long polylines with repeated points inside and across groups of 32
+    # points (the cleanup's sequential rule), open and closed back onto the start
+    for closed in (False, True):
+        pts = [(20.0 + 3.0 * i, 60.0 + (25.0 if i % 2 else 0.0) + 0.5 * i) for i in range(90)]
+        for at in (88, 70, 34, 33, 32, 31, 5, 1):
+            pts.insert(at, pts[at - 1])
+        p = tk.BezPath()
+        p.move_to(*pts[0])
+        for q in pts[1:]:
+            p.line_to(*q)
+        if closed:
+            p.line_to(*pts[0])
+            p.close()
+        c.push_stroke(p, tk.Brush.solid(0.2, 0.4, 0.6, 0.7), 3.0, tolerance=0.1)
     rng = np.random.default_rng(11)
     for _ in range(60):
         p = tk.BezPath()

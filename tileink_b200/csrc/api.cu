@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -31,11 +32,30 @@ struct Fail {
         if (e_ != cudaSuccess) throw Fail{TK_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
     } while (0)
 
-// Device buffer that only grows.
+// Device buffer that only grows; owns its allocation (freed when released,
+// reassigned by a move, or destroyed).
 template <class T>
 struct DBuf {
     T* ptr = nullptr;
     size_t cap = 0;  // elements
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : ptr(o.ptr), cap(o.cap) {
+        o.ptr = nullptr;
+        o.cap = 0;
+    }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            ptr = o.ptr;
+            cap = o.cap;
+            o.ptr = nullptr;
+            o.cap = 0;
+        }
+        return *this;
+    }
+    ~DBuf() { release(); }
     void reserve(size_t n) {
         if (n <= cap && ptr) return;
         if (ptr) cudaFree(ptr);
@@ -61,13 +81,13 @@ struct DBuf {
 // so that a scene re-uploaded every frame does not allocate.
 struct FlattenScratch {
     DBuf<tk_flatten_el> els, sels;
-    DBuf<uint32_t> path_els, offsets, sums, words, soff, ssums, poly_n, line_off;
+    DBuf<uint32_t> path_els, offsets, sums, words, soff, ssums, poly_n, line_off, unit_lines;
     DBuf<tk_stroke_polyline> polys;
     DBuf<tk_stroke_desc> strokes;
     DBuf<unsigned long long> wide;
     DBuf<tkf::Pt> pts;
     void release() {
-        for (auto* b : {&path_els, &offsets, &sums, &words, &soff, &ssums, &poly_n, &line_off}) b->release();
+        for (auto* b : {&path_els, &offsets, &sums, &words, &soff, &ssums, &poly_n, &line_off, &unit_lines}) b->release();
         els.release();
         sels.release();
         polys.release();
@@ -89,6 +109,21 @@ struct Pass {
     DBuf<uint32_t> glyph_list;  // text scenes: the glyph indices PTCL_GLYPH records name
     uint64_t glyph_needed = 0, glyph_used = 0;
 };
+
+// A new upload's passes take over the device buffers of the last upload's
+// passes, position by position (grow-only, so re-uploading a scene allocates
+// nothing); the buffers of passes the new scene does not have are freed.
+void adopt_pass_buffers(std::vector<Pass>& now, std::vector<Pass>& old) {
+    for (size_t i = 0; i < now.size() && i < old.size(); ++i) {
+        now[i].d_batches = std::move(old[i].d_batches);
+        now[i].bin_lists = std::move(old[i].bin_lists);
+        now[i].bin_counts = std::move(old[i].bin_counts);
+        now[i].tiles = std::move(old[i].tiles);
+        now[i].ptcl = std::move(old[i].ptcl);
+        now[i].glyph_list = std::move(old[i].glyph_list);
+    }
+    old.clear();
+}
 
 enum StepKind { STEP_PASS, STEP_BLUR_BEGIN, STEP_BLUR_END };
 struct Step {
@@ -126,6 +161,10 @@ struct DiffState {
 struct tk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // A second stream for the scene records an upload copies while the main
+    // stream flattens on the device, and the events that order the two.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_main = nullptr, ev_copy = nullptr;
     std::string error;
     // scene
     bool have_scene = false;
@@ -328,25 +367,25 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     // renders (one complete record each, src/shared/gpu_sdf.rs:27-46).
     for (uint32_t i = 0; i < d.draw_count; ++i) {
         const tk_draw_record& r = d.draws[i];
-        const std::string at = "draw " + std::to_string(i);
+        const auto at = [i] { return "draw " + std::to_string(i); };  // built only for a message
         if (r.tag == TK_DRAW_PATH_GLYPH || r.glyph_run_id != TK_INVALID_INDEX) text = true;
         if (r.glyph_run_id != TK_INVALID_INDEX) {
             // a glyph run draw (canvas/primitives/text.rs:80-96)
-            if (r.glyph_run_id >= d.glyph_run_count) invalid(at + ": glyph run out of range");
+            if (r.glyph_run_id >= d.glyph_run_count) invalid(at() + ": glyph run out of range");
             if (r.tag != TK_DRAW_BRUSH || r.path_id != TK_INVALID_INDEX || r.sdf_offset != TK_INVALID_INDEX ||
                 r.sdf_shadow_offset != TK_INVALID_INDEX)
-                invalid(at + ": a glyph run draw is a brush draw without a path or SDF record");
+                invalid(at() + ": a glyph run draw is a brush draw without a path or SDF record");
         }
         const bool plain = r.sdf_offset != TK_INVALID_INDEX, shadow = r.sdf_shadow_offset != TK_INVALID_INDEX;
         if (plain || shadow) {
-            if (plain && shadow) invalid(at + ": both an SDF and a shadow record");
+            if (plain && shadow) invalid(at() + ": both an SDF and a shadow record");
             if (r.tag != TK_DRAW_BRUSH && !(r.tag == TK_DRAW_CLIP && plain))
-                invalid(at + ": SDF groups and shadow clips are outside this path");
-            if (r.path_id != TK_INVALID_INDEX) invalid(at + ": an SDF draw with a path");
+                invalid(at() + ": SDF groups and shadow clips are outside this path");
+            if (r.path_id != TK_INVALID_INDEX) invalid(at() + ": an SDF draw with a path");
             const uint64_t off = plain ? r.sdf_offset : r.sdf_shadow_offset;
             const uint64_t len = plain ? r.sdf_len : r.sdf_shadow_len;
             const uint64_t words = plain ? d.sdf_word_count : d.sdf_shadow_word_count;
-            if (len != TK_SDF_RECORD_WORDS || off + len > words) invalid(at + ": SDF record outside its blob");
+            if (len != TK_SDF_RECORD_WORDS || off + len > words) invalid(at() + ": SDF record outside its blob");
             const uint32_t kind = (plain ? d.sdf_blob : d.sdf_shadow_blob)[off];
             const bool ext = plain ? (kind == TK_SDF_CANDLESTICK || kind == TK_SDF_DASH_LINE || kind == TK_SDF_TRIANGLE ||
                                       kind == TK_SDF_CHECKERBOARD || kind == TK_SDF_CALLOUT ||
@@ -357,7 +396,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                                              kind == TK_SDF_CIRCLE_STROKE || kind == TK_SDF_LINE)
                                           : (kind == TK_SDF_RECT_SHADOW || kind == TK_SDF_CIRCLE_SHADOW ||
                                              kind == TK_SDF_LINE_SHADOW));
-            if (!ok) invalid(at + ": SDF kind " + std::to_string(kind) + " is not supported");
+            if (!ok) invalid(at() + ": SDF kind " + std::to_string(kind) + " is not supported");
             sdf_ext = sdf_ext || ext;
         }
         // image pattern brushes (shared/brush/sample.hlsli:32-41): texture-table
@@ -365,16 +404,16 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         const uint64_t bo = r.brush_offset;
         if (bo != TK_INVALID_INDEX && bo < d.brush_word_count && d.brush_blob[bo] == TK_BRUSH_PATTERN_RESOURCE) {
             if (bo + TK_BRUSH_HEADER_WORDS + TK_BRUSH_PARAM_WORDS > d.brush_word_count)
-                invalid(at + ": image brush outside the brush blob");
+                invalid(at() + ": image brush outside the brush blob");
             const uint32_t* w = d.brush_blob + bo;
             const uint32_t ix = w[4] & ~TK_BRUSH_TEXTURE_PLACEMENT_BIT;
-            if (!(w[4] & TK_BRUSH_TEXTURE_PLACEMENT_BIT)) invalid(at + ": atlas image placement is outside this path");
-            if (ix >= d.image_count) invalid(at + ": image index out of range");
+            if (!(w[4] & TK_BRUSH_TEXTURE_PLACEMENT_BIT)) invalid(at() + ": atlas image placement is outside this path");
+            if (ix >= d.image_count) invalid(at() + ": image index out of range");
             if (w[5] != d.images[ix].width || w[6] != d.images[ix].height)
-                invalid(at + ": image brush size differs from its image");
-            if (!plain) invalid(at + ": image patterns fill SDF rects only");
+                invalid(at() + ": image brush size differs from its image");
+            if (!plain) invalid(at() + ": image patterns fill SDF rects only");
             if (w[1] > TK_EXTEND_REFLECT || w[7] > 255u || w[8] > TK_PATTERN_BILINEAR)
-                invalid(at + ": bad image brush extend, opacity or sampling");
+                invalid(at() + ": bad image brush extend, opacity or sampling");
         }
         if (r.tag != TK_DRAW_BRUSH && r.tag != TK_DRAW_CLIP && r.tag != TK_DRAW_OPACITY && r.tag != TK_DRAW_BLEND &&
             r.tag != TK_DRAW_ISOLATE && r.tag != TK_DRAW_PATH_GLYPH)
@@ -404,8 +443,10 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
         if (k && d.draw_batch_ids[d.draw_order[k - 1]] > b) invalid("draw order is not grouped by batch");
         batch_draws[b]++;
     }
-    // Ops -> passes and steps.
-    c->passes.clear();
+    // Ops -> passes and steps. The last scene's passes keep their device
+    // buffers until the new passes take them over (or free them on a throw).
+    std::vector<Pass> old_passes;
+    old_passes.swap(c->passes);
     c->steps.clear();
     uint32_t order_pos = 0, depth = 0;
     int64_t last_batch = -1;
@@ -468,6 +509,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
     }
     if (depth) invalid("unbalanced BLUR_BEGIN");
     if (order_pos != d.draw_order_count) invalid("draw order does not match the batches");
+    adopt_pass_buffers(c->passes, old_passes);
     c->width = d.width;
     c->height = d.height;
     c->tw = tw;
@@ -591,15 +633,41 @@ uint32_t read_word(tk_ctx* c, const uint32_t* dptr) {
 
 // Paths by decreasing line count (stable), for scan_emit's path queue.
 void upload_emit_order(tk_ctx* c) {
-    std::vector<uint32_t> order(c->h_paths.size());
-    for (uint32_t i = 0; i < uint32_t(order.size()); ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        return c->h_paths[a].line_count > c->h_paths[b].line_count;
-    });
+    // Paths longest first, ties in path order: a stable sort by descending
+    // line count, done as an LSD radix sort of the inverted counts (16 bits a
+    // pass; the high pass only when some count reaches 2^16).
+    const uint32_t n = uint32_t(c->h_paths.size());
+    std::vector<uint32_t> key(n), order(n), tmp(n);
+    uint32_t most = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        key[i] = ~c->h_paths[i].line_count;
+        most = std::max(most, c->h_paths[i].line_count);
+        order[i] = i;
+    }
+    std::vector<uint32_t> count(65537);
+    for (uint32_t shift = 0; shift < (most >> 16 ? 32u : 16u); shift += 16) {
+        std::fill(count.begin(), count.end(), 0u);
+        for (uint32_t i = 0; i < n; ++i) ++count[((key[order[i]] >> shift) & 0xFFFFu) + 1u];
+        for (uint32_t k = 1; k < 65537; ++k) count[k] += count[k - 1];
+        for (uint32_t i = 0; i < n; ++i) tmp[count[(key[order[i]] >> shift) & 0xFFFFu]++] = order[i];
+        order.swap(tmp);
+    }
     upload(c->emit_order, order.data(), order.size(), c->stream);
 }
 
-void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl);
+void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl,
+                       const std::function<void()>& side_copies);
+
+// Waits for both streams when an upload leaves, so that no copy still reads
+// the caller's host arrays (on a throw as well; the normal path checks the
+// main stream's status itself).
+struct UploadJoin {
+    tk_ctx* c;
+    ~UploadJoin() {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamSynchronize(c->stream);
+    }
+};
 
 // The scene of one band of tile rows: every path's tile bbox clamped to the
 // band's rows (tile rows are independent after the scan: a backdrop is the
@@ -635,10 +703,42 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     c->graph_exec = nullptr;
     validate_and_plan(c, d);
-    cudaStream_t st = c->stream;
+    cudaStream_t st = c->stream, cs = c->copy_stream;
+    UploadJoin join{c};
+    // The records nothing reads before the paint table go up on the copy
+    // stream, after the main stream's earlier work (the last frame may still
+    // read these buffers); with device flattening they overlap its kernels.
+    std::vector<uint4> tab(d.image_count);  // the texture table: per image its first texel and size
+    auto side_copies = [&] {
+        TK_CUDA(cudaEventRecord(c->ev_main, st));
+        TK_CUDA(cudaStreamWaitEvent(cs, c->ev_main, 0));
+        upload(c->draws, d.draws, d.draw_count, cs);
+        upload(c->brush, d.brush_blob, d.brush_word_count, cs);
+        c->sdf.reserve(c->sdf_words);
+        if (d.sdf_word_count)
+            TK_CUDA(cudaMemcpyAsync(c->sdf.ptr, d.sdf_blob, d.sdf_word_count * 4, cudaMemcpyHostToDevice, cs));
+        if (d.sdf_shadow_word_count)
+            TK_CUDA(cudaMemcpyAsync(c->sdf.ptr + d.sdf_word_count, d.sdf_shadow_blob, d.sdf_shadow_word_count * 4,
+                                    cudaMemcpyHostToDevice, cs));
+        uint64_t texel_words = 0;
+        for (uint32_t k = 0; k < d.image_count; ++k) {
+            tab[k] = make_uint4(uint32_t(texel_words), d.images[k].width, d.images[k].height, 0u);
+            texel_words += uint64_t(d.images[k].width) * d.images[k].height;
+        }
+        c->texels.reserve(texel_words);
+        for (uint32_t k = 0; k < d.image_count; ++k)
+            TK_CUDA(cudaMemcpyAsync(c->texels.ptr + tab[k].x, d.images[k].premul_rgba8,
+                                    uint64_t(tab[k].y) * tab[k].z * 4, cudaMemcpyHostToDevice, cs));
+        upload(c->image_tab, tab.data(), tab.size(), cs);
+        upload(c->glyph_runs, d.glyph_runs, d.glyph_run_count, cs);
+        upload(c->glyphs, d.glyphs, d.glyph_count, cs);
+        upload(c->glyph_images, d.glyph_images, d.glyph_image_count, cs);
+        upload(c->glyph_texels, d.glyph_texels, d.glyph_texel_count, cs);
+        TK_CUDA(cudaEventRecord(c->ev_copy, cs));
+    };
     upload(c->paths, d.paths, d.path_count, st);
     if (fl) {
-        flatten_on_device(c, d, *fl);  // the host lines, then the device lines
+        flatten_on_device(c, d, *fl, side_copies);  // the host lines, then the device lines
     } else if (line_dirty) {  // the changed paths' line ranges, runs coalesced
         c->lines.reserve(d.line_count);
         for (uint32_t p = 0; p < d.path_count;) {
@@ -654,30 +754,8 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     } else {
         upload(c->lines, d.lines, d.line_count, st);
     }
-    upload(c->draws, d.draws, d.draw_count, st);
-    upload(c->brush, d.brush_blob, d.brush_word_count, st);
-    c->sdf.reserve(c->sdf_words);
-    if (d.sdf_word_count)
-        TK_CUDA(cudaMemcpyAsync(c->sdf.ptr, d.sdf_blob, d.sdf_word_count * 4, cudaMemcpyHostToDevice, st));
-    if (d.sdf_shadow_word_count)
-        TK_CUDA(cudaMemcpyAsync(c->sdf.ptr + d.sdf_word_count, d.sdf_shadow_blob, d.sdf_shadow_word_count * 4,
-                                cudaMemcpyHostToDevice, st));
-    // the texture table: texels concatenated, per image its first texel and size
-    std::vector<uint4> tab(d.image_count);
-    uint64_t texel_words = 0;
-    for (uint32_t k = 0; k < d.image_count; ++k) {
-        tab[k] = make_uint4(uint32_t(texel_words), d.images[k].width, d.images[k].height, 0u);
-        texel_words += uint64_t(d.images[k].width) * d.images[k].height;
-    }
-    c->texels.reserve(texel_words);
-    for (uint32_t k = 0; k < d.image_count; ++k)
-        TK_CUDA(cudaMemcpyAsync(c->texels.ptr + tab[k].x, d.images[k].premul_rgba8,
-                                uint64_t(tab[k].y) * tab[k].z * 4, cudaMemcpyHostToDevice, st));
-    upload(c->image_tab, tab.data(), tab.size(), st);
-    upload(c->glyph_runs, d.glyph_runs, d.glyph_run_count, st);
-    upload(c->glyphs, d.glyphs, d.glyph_count, st);
-    upload(c->glyph_images, d.glyph_images, d.glyph_image_count, st);
-    upload(c->glyph_texels, d.glyph_texels, d.glyph_texel_count, st);
+    if (!fl) side_copies();
+    TK_CUDA(cudaStreamWaitEvent(st, c->ev_copy, 0));
     c->paints.reserve(d.draw_count);
     tk::launch_paint_table(c->draws.ptr, d.draw_count, c->brush.ptr, d.brush_word_count,
                            uint32_t(c->sdf_shadow_base), c->image_tab.ptr, d.image_count, c->paints.ptr, st);
@@ -724,6 +802,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     if (c->band && blur_depth) invalid("band rendering takes scenes without blur layers (their reach crosses bands)");
     TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
     TK_CUDA(cudaGetLastError());
+    TK_CUDA(cudaStreamSynchronize(st));  // every copy of the caller's arrays is done
     c->have_scene = true;
     c->rendered = false;
 }
@@ -1076,7 +1155,10 @@ void rebuild_items(tk_ctx* c) {
 
 // Lines of the element paths flattened on the device after the host lines;
 // their path records get their line ranges on the device.
-void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl) {
+// side_copies runs once the element counts are back: the scene records then
+// go up on the copy stream while the stroking and emit kernels run.
+void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc& fl,
+                       const std::function<void()>& side_copies) {
     if (!(d.flags & TK_SCENE_SEGMENTS_FROM_DEVICE)) invalid("device flattening needs device segment planning");
     if ((fl.element_count && !fl.elements) || (d.path_count && !fl.path_elements)) invalid("null flatten arrays");
     // Element ranges are checked here; the elements themselves (verb,
@@ -1097,17 +1179,17 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     if ((ns && !fl.strokes) || (npl && !fl.polylines) || (nse && !fl.stroke_elements)) invalid("null stroke arrays");
     for (uint32_t s = 0; s < ns; ++s) {
         const tk_stroke_desc& S = fl.strokes[s];
-        const std::string at = "stroke " + std::to_string(s) + ": ";
-        if (S.path >= d.path_count) invalid(at + "path out of range");
-        if (taken[S.path] || d.paths[S.path].line_count) invalid(at + "its path already has lines or elements");
+        const auto at = [s] { return "stroke " + std::to_string(s) + ": "; };  // built only for a message
+        if (S.path >= d.path_count) invalid(at() + "path out of range");
+        if (taken[S.path] || d.paths[S.path].line_count) invalid(at() + "its path already has lines or elements");
         taken[S.path] = 1;
-        if (!(S.half_width > 0.0 && S.half_width <= 1e6)) invalid(at + "half width outside (0, 1e6]");
-        if (!(S.tolerance >= 1e-3 && S.tolerance <= 1e6)) invalid(at + "tolerance outside [1e-3, 1e6]");
+        if (!(S.half_width > 0.0 && S.half_width <= 1e6)) invalid(at() + "half width outside (0, 1e6]");
+        if (!(S.tolerance >= 1e-3 && S.tolerance <= 1e6)) invalid(at() + "tolerance outside [1e-3, 1e6]");
         for (double t : S.transform)
-            if (!(std::fabs(t) <= 1e6)) invalid(at + "transform entries must be finite, within 1e6");
-        if (uint64_t(S.polyline0) + S.polyline_count > npl) invalid(at + "polylines out of range");
+            if (!(std::fabs(t) <= 1e6)) invalid(at() + "transform entries must be finite, within 1e6");
+        if (uint64_t(S.polyline0) + S.polyline_count > npl) invalid(at() + "polylines out of range");
         for (uint32_t k = S.polyline0; k < S.polyline0 + S.polyline_count; ++k)
-            if (fl.polylines[k].stroke != s) invalid(at + "polyline " + std::to_string(k) + " belongs elsewhere");
+            if (fl.polylines[k].stroke != s) invalid(at() + "polyline " + std::to_string(k) + " belongs elsewhere");
     }
     for (uint32_t k = 0; k < npl; ++k) {
         const tk_stroke_polyline& P = fl.polylines[k];
@@ -1149,13 +1231,17 @@ void flatten_on_device(tk_ctx* c, const tk_scene_desc& d, const tk_flatten_desc&
     TK_CUDA(cudaMemcpyAsync(w, words.ptr, sizeof(w), cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaMemcpyAsync(wsum, wide.ptr, sizeof(wsum), cudaMemcpyDeviceToHost, st));
     TK_CUDA(cudaStreamSynchronize(st));
+    side_copies();
     if (wsum[0] > 0xFFFFFFFFull) invalid("stroke centerline points exceed u32 indexing");
     tk::StrokeView sv{sels.ptr, nse,        soff.ptr, words.ptr + 2, nullptr,     0,
-                      polys.ptr, npl,       strokes.ptr, ns,         poly_n.ptr, line_off.ptr, words.ptr + 1};
+                      polys.ptr, npl,       strokes.ptr, ns,         poly_n.ptr, line_off.ptr, words.ptr + 1,
+                      nullptr};
     if (npl) {
         pts.reserve(std::max<uint64_t>(w[2], 1));
         sv.pts = pts.ptr;
         sv.pt_cap = w[2];
+        F.unit_lines.reserve(std::max<uint64_t>(2ull * w[2], 1));  // two unit slots per raw point
+        sv.unit_lines = F.unit_lines.ptr;
         tk::launch_stroke_outline_count(sv, ssums.ptr, words.ptr + 3, wide.ptr + 1, st);
         TK_CUDA(cudaMemcpyAsync(w, words.ptr, sizeof(w), cudaMemcpyDeviceToHost, st));
         TK_CUDA(cudaMemcpyAsync(wsum, wide.ptr, sizeof(wsum), cudaMemcpyDeviceToHost, st));
@@ -1346,8 +1432,10 @@ void do_batch_upload(tk_ctx* c, const tk_scene_desc* scenes, uint32_t n) {
     c->tw = tiles;
     c->th = 1;
     c->steps.assign(1, Step{STEP_PASS, 0u, 0.0f, {0, 0, 0, 0}});
-    c->passes.clear();
+    std::vector<Pass> old_passes;
+    old_passes.swap(c->passes);
     c->passes.emplace_back();
+    adopt_pass_buffers(c->passes, old_passes);
     Pass& p = c->passes.back();
     p.order0 = 0;
     p.draw_n = uint32_t(order.size());
@@ -1451,8 +1539,15 @@ int32_t tk_ctx_create(int32_t device, tk_ctx** out) {
     }
     auto* c = new tk_ctx();
     c->device = device;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_copy, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
+        if (c->ev_copy) cudaEventDestroy(c->ev_copy);
+        if (c->ev_main) cudaEventDestroy(c->ev_main);
+        if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return TK_E_CUDA;
     }
@@ -1488,6 +1583,10 @@ void tk_ctx_destroy(tk_ctx* c) {
     D.dpoints.release(); D.taps.release(); D.dtaps.release(); D.ep_w.release(); D.ep_point.release();
     D.sums.release();
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    cudaStreamSynchronize(c->copy_stream);
+    cudaEventDestroy(c->ev_main);
+    cudaEventDestroy(c->ev_copy);
+    cudaStreamDestroy(c->copy_stream);
     cudaStreamDestroy(c->stream);
     delete c;
 }

@@ -1,20 +1,37 @@
 // Device flattening (the Canvas::push_path flattening step,
 // src/shared/path_flatten.rs:20-82, moved onto the GPU): Bezier elements to
-// lines with the count / scan / emit pattern. One thread flattens one element
-// (a line, quadratic or cubic with its start point); the host has already
-// resolved move_to / close into explicit elements, so elements are
-// independent. The arithmetic is flatten_core.h, shared with the host, so the
-// lines are bit-identical to the host Canvas's.
+// lines with the count / scan / emit pattern. One warp emits one element
+// (a line, quadratic or cubic with its start point) 32 points at a time
+// (warp_flatten.cuh); the host has already resolved move_to / close into
+// explicit elements, so elements are independent. The arithmetic is
+// flatten_core.h, shared with the host, so the lines are bit-identical to the
+// host Canvas's. An element's lines are its kept edges (tkf::keep_edge from
+// each point's predecessor), ranked within each round by ballot, so a round
+// stores consecutive lines from consecutive lanes. The count pass, which
+// stores nothing, runs one element per thread.
 #include <cuda_runtime.h>
 
 #include "flatten_core.h"
 #include "kernels.h"
+#include "warp_flatten.cuh"
 
 namespace tk {
 namespace {
 
 using tkf::Pt;
 
+constexpr uint32_t kFlattenThreads = 128;
+
+// The previous point of each lane's point: the lane before it, or for lane 0
+// the last point of the previous round.
+__device__ inline Pt prev_point(const Pt& p, const Pt& last, uint32_t lane) {
+    Pt q{__shfl_up_sync(0xffffffffu, p.x, 1), __shfl_up_sync(0xffffffffu, p.y, 1)};
+    return lane == 0u ? last : q;
+}
+
+// The count pass walks each element on one thread (tkf::element_points):
+// counting needs no stores, and a thread per element keeps more elements in
+// flight than a warp per element.
 struct CountEmit {
     Pt prev;
     uint32_t n;
@@ -24,19 +41,23 @@ struct CountEmit {
     }
 };
 
-struct WriteEmit {
-    Pt prev;
+struct WarpWriteEdges {
+    Pt last;
     tk_line* out;
     uint64_t at, end;
-    uint32_t path;
+    uint32_t path, lane;
     uint32_t* error;
-    __device__ void operator()(Pt p) {
-        if (tkf::keep_edge(prev, p)) {
-            if (at < end) out[at] = tk_line{path, 0.0f, {float(prev.x), float(prev.y)}, {float(p.x), float(p.y)}};
+    __device__ void operator()(bool valid, Pt p, uint32_t k) {
+        const Pt prev = prev_point(p, last, lane);
+        const bool keep = valid && tkf::keep_edge(prev, p);
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const uint64_t q = at + __popc(mask & ((1u << lane) - 1u));
+            if (q < end) out[q] = tk_line{path, 0.0f, {float(prev.x), float(prev.y)}, {float(p.x), float(p.y)}};
             else atomicOr(error, ERR_SEGMENT_OVERFLOW);
-            ++at;
         }
-        prev = p;
+        at += __popc(mask);
+        last = shfl_pt(p, k - 1u);
     }
 };
 
@@ -52,7 +73,8 @@ __device__ bool element_ok(const tk_flatten_el& e) {
     return true;
 }
 
-__global__ void k_flatten_count(const tk_flatten_el* __restrict__ els, uint64_t n, uint32_t* counts, uint32_t* error) {
+__global__ void __launch_bounds__(kFlattenThreads)
+    k_flatten_count(const tk_flatten_el* __restrict__ els, uint64_t n, uint32_t* counts, uint32_t* error) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const tk_flatten_el e = els[i];
         CountEmit c{Pt{e.p[0][0], e.p[0][1]}, 0u};
@@ -153,12 +175,15 @@ __global__ void k_flatten_paths(tk_path_record* paths, uint32_t path_count, cons
     paths[p].line_count = b - a;
 }
 
-__global__ void k_flatten_emit(const tk_flatten_el* __restrict__ els, uint64_t n, const uint32_t* __restrict__ offsets,
-                               tk_line* lines, uint64_t line_base, uint64_t line_end, uint32_t* error) {
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+__global__ void __launch_bounds__(kFlattenThreads)
+    k_flatten_emit(const tk_flatten_el* __restrict__ els, uint64_t n, const uint32_t* __restrict__ offsets,
+                   tk_line* lines, uint64_t line_base, uint64_t line_end, uint32_t* error) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += warps) {
         const tk_flatten_el e = els[i];
-        WriteEmit w{Pt{e.p[0][0], e.p[0][1]}, lines, line_base + offsets[i], line_end, e.path, error};
-        if (element_ok(e)) tkf::element_points(e, w);
+        WarpWriteEdges w{Pt{e.p[0][0], e.p[0][1]}, lines, line_base + offsets[i], line_end, e.path, lane, error};
+        if (element_ok(e)) warp_element_points(e, lane, w);
     }
 }
 
@@ -177,7 +202,7 @@ void launch_exclusive_scan(uint32_t* v, uint64_t n, uint32_t* block_sums, uint32
 
 void launch_flatten_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
                           uint32_t* total, uint32_t* error, cudaStream_t st) {
-    if (n) k_flatten_count<<<148 * 16, 128, 0, st>>>(els, n, counts, error);
+    if (n) k_flatten_count<<<148 * 16, kFlattenThreads, 0, st>>>(els, n, counts, error);
     launch_exclusive_scan(counts, n, block_sums, total, st);
 }
 
@@ -186,7 +211,7 @@ void launch_flatten_emit(const tk_flatten_el* els, uint64_t n, const uint32_t* o
                          uint64_t line_base, uint64_t line_end, uint32_t* error, cudaStream_t st) {
     if (path_count) k_flatten_paths<<<(path_count + 255) / 256, 256, 0, st>>>(paths, path_count, path_els, offsets,
                                                                              total, n, uint32_t(line_base), els, error);
-    if (n) k_flatten_emit<<<148 * 16, 128, 0, st>>>(els, n, offsets, lines, line_base, line_end, error);
+    if (n) k_flatten_emit<<<148 * 16, kFlattenThreads, 0, st>>>(els, n, offsets, lines, line_base, line_end, error);
 }
 
 size_t flatten_block_sums(uint64_t n) { return size_t((n + kScanBlock - 1) / kScanBlock) + 1; }

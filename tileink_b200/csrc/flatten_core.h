@@ -63,37 +63,49 @@ TK_HD inline P quad_eval(P p0, P p1, P p2, double t) {
     double mt = 1.0 - t;
     return p0 * (mt * mt) + p1 * (2.0 * mt * t) + p2 * (t * t);
 }
-template <class P, class Emit>
-TK_HD void flatten_quad(P q0, P q1, P q2, double tol, Emit&& emit) {
-    const Pt &p0 = val(q0), &p1 = val(q1), &p2 = val(q2);
+// One quadratic's flattening plan: n points (n >= 1), the last of them the
+// end point. mode 0: the end point only (degenerate); 1: uniform steps in t
+// (nearly collinear control points); 2: the integral parametrisation.
+struct QuadPlan {
+    int n, mode;
+    double a0, a2, v0, v2;
+};
+TK_HD inline QuadPlan plan_quad(const Pt& p0, const Pt& p1, const Pt& p2, double tol) {
+    QuadPlan q{1, 0, 0.0, 0.0, 0.0, 0.0};
     double ddx = 2.0 * p1.x - p0.x - p2.x, ddy = 2.0 * p1.y - p0.y - p2.y;
     double u0 = (p1.x - p0.x) * ddx + (p1.y - p0.y) * ddy;
     double u2 = (p2.x - p1.x) * ddx + (p2.y - p1.y) * ddy;
     double cross = (p2.x - p0.x) * ddy - (p2.y - p0.y) * ddx;
     double dd = ::sqrt(ddx * ddx + ddy * ddy);
-    if (dd < 1e-12) {
-        emit(q2);
-        return;
-    }
+    if (dd < 1e-12) return q;
     double x0 = u0 / cross, x2 = u2 / cross;
     double scale = ::fabs(cross) / (dd * ::fabs(x2 - x0));
     if (!(isfinite(x0) && isfinite(x2) && isfinite(scale)) || ::fabs(cross) < 1e-12 * dd * dd) {
         // Nearly collinear control points: uniform steps with the chord bound
         // |B''| h^2 / 8 = |dd| h^2 / 4 <= tol.
-        int n = count_of(::sqrt(dd / (4.0 * tol)), kMaxSubdivisions);
-        for (int i = 1; i < n; ++i) emit(quad_eval(q0, q1, q2, double(i) / n));
-        emit(q2);
-        return;
+        q.mode = 1;
+        q.n = count_of(::sqrt(dd / (4.0 * tol)), kMaxSubdivisions);
+        return q;
     }
-    double a0 = approx_integral(x0), a2 = approx_integral(x2);
-    double count = 0.5 * ::fabs(a2 - a0) * ::sqrt(scale / tol);
-    int n = count_of(count, kMaxSubdivisions);
-    double v0 = approx_inv_integral(a0), v2 = approx_inv_integral(a2);
-    for (int i = 1; i < n; ++i) {
-        double v = approx_inv_integral(a0 + (a2 - a0) * double(i) / n);
-        double t = (v - v0) / (v2 - v0);
-        emit(quad_eval(q0, q1, q2, t));
-    }
+    q.mode = 2;
+    q.a0 = approx_integral(x0);
+    q.a2 = approx_integral(x2);
+    double count = 0.5 * ::fabs(q.a2 - q.a0) * ::sqrt(scale / tol);
+    q.n = count_of(count, kMaxSubdivisions);
+    q.v0 = approx_inv_integral(q.a0);
+    q.v2 = approx_inv_integral(q.a2);
+    return q;
+}
+// The curve parameter of point i (1 <= i < n) of a plan of mode 1 or 2.
+TK_HD inline double quad_param(const QuadPlan& q, int i) {
+    if (q.mode == 1) return double(i) / q.n;
+    double v = approx_inv_integral(q.a0 + (q.a2 - q.a0) * double(i) / q.n);
+    return (v - q.v0) / (q.v2 - q.v0);
+}
+template <class P, class Emit>
+TK_HD void flatten_quad(P q0, P q1, P q2, double tol, Emit&& emit) {
+    const QuadPlan q = plan_quad(val(q0), val(q1), val(q2), tol);
+    for (int i = 1; i < q.n; ++i) emit(quad_eval(q0, q1, q2, quad_param(q, i)));
     emit(q2);
 }
 template <class P>
@@ -106,20 +118,35 @@ TK_HD inline P cubic_deriv(const P c[4], double t) {
     double mt = 1.0 - t;
     return (c[1] - c[0]) * (3.0 * mt * mt) + (c[2] - c[1]) * (6.0 * mt * t) + (c[3] - c[2]) * (3.0 * t * t);
 }
-template <class P, class Emit>
-TK_HD void flatten_cubic(const P c[4], double tol, Emit&& emit) {
-    const double quad_share = 0.1;
-    const Pt &c0 = val(c[0]), &c1 = val(c[1]), &c2 = val(c[2]), &c3 = val(c[3]);
+constexpr double kQuadShare = 0.1;  // share of the tolerance spent on the cubic-to-quadratic split
+
+// Number of quadratics a cubic is split into.
+TK_HD inline int cubic_quad_count(const Pt& c0, const Pt& c1, const Pt& c2, const Pt& c3, double tol) {
     Pt third{c3.x - 3.0 * c2.x + 3.0 * c1.x - c0.x, c3.y - 3.0 * c2.y + 3.0 * c1.y - c0.y};
     double err = ::sqrt(3.0) / 36.0 * ::sqrt(third.x * third.x + third.y * third.y);
-    int m = ceil_cbrt(err / (quad_share * tol), kMaxSubdivisions);
+    return ceil_cbrt(err / (kQuadShare * tol), kMaxSubdivisions);
+}
+template <class P>
+struct SubQuad {
+    P q0, ctrl, q3;
+};
+// Quadratic j of the m a cubic is split into (the last one ends exactly at
+// the cubic's end point); flattened with tolerance (1 - kQuadShare) tol.
+template <class P>
+TK_HD inline SubQuad<P> cubic_sub_quad(const P c[4], int j, int m) {
+    double t0 = double(j) / m, t1 = double(j + 1) / m, h = (t1 - t0) / 3.0;
+    P q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
+    P q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
+    P ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
+    if (j == m - 1) q3 = c[3];
+    return SubQuad<P>{q0, ctrl, q3};
+}
+template <class P, class Emit>
+TK_HD void flatten_cubic(const P c[4], double tol, Emit&& emit) {
+    const int m = cubic_quad_count(val(c[0]), val(c[1]), val(c[2]), val(c[3]), tol);
     for (int j = 0; j < m; ++j) {
-        double t0 = double(j) / m, t1 = double(j + 1) / m, h = (t1 - t0) / 3.0;
-        P q0 = cubic_eval(c, t0), q3 = cubic_eval(c, t1);
-        P q1 = q0 + cubic_deriv(c, t0) * h, q2 = q3 - cubic_deriv(c, t1) * h;
-        P ctrl = ((q1 + q2) * 3.0 - q0 - q3) * 0.25;
-        if (j == m - 1) q3 = c[3];
-        flatten_quad(q0, ctrl, q3, (1.0 - quad_share) * tol, emit);
+        const SubQuad<P> s = cubic_sub_quad(c, j, m);
+        flatten_quad(s.q0, s.ctrl, s.q3, (1.0 - kQuadShare) * tol, emit);
     }
 }
 

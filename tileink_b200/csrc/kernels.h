@@ -284,6 +284,7 @@ struct StrokeView {
     uint32_t* poly_n;    // per polyline: points kept
     uint32_t* line_off;  // per polyline: lines, then their exclusive offsets
     uint32_t* error;
+    uint32_t* unit_lines;  // per outline unit: its lines (2 slots per raw point)
 };
 void launch_stroke_count(const tk_flatten_el* els, uint64_t n, uint32_t* counts, uint32_t* block_sums,
                          uint32_t* total, unsigned long long* total64, uint32_t* error, cudaStream_t st);
