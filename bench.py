@@ -268,30 +268,42 @@ def batch_timing(n_scenes, steps):
     """Batched vs serial scenes/s on the uneven-batch workload: n_scenes
     independent scenes, width and height each log-uniform in [64, 1024],
     log-uniform 10..2000 closed cubic paths with solid fills (seeds 1000..).
-    serial: upload + render + readback per scene through tk_render_to_image.
+    The scenes' records sit in pinned host memory and the images are read
+    back into a pinned buffer, as in the end-to-end frame leg.
+    serial: upload + render + readback per scene (tk_scene_upload,
+    tk_render, tk_readback).
     batched: the whole batch in one CUDA graph launch (tk_batch_render) after
     the autotuner picked the pool-scan work item size; `value` with the
     scenes resident on the device, `e2e` with upload and readback."""
+    import torch
     import tileink_b200 as tk
-    scenes = [tk.generate(4, 1000 + i) for i in range(n_scenes)]
+    canvases = [tk.generate(4, 1000 + i) for i in range(n_scenes)]
+    scenes = [pinned_scene(c)[0] for c in canvases]
+    pixels = [c.scene_desc().width * c.scene_desc().height for c in canvases]
+    del canvases
+    out = torch.empty(sum(pixels) * 4, dtype=torch.uint8, pin_memory=True).numpy().view(np.uint32)
     r = tk.NativeRenderer(0)
-    for c in scenes[:8]:
-        r.render_to_image(c)
+    for ps in scenes[:8]:
+        r.upload(ps)
+        r.render()
+        r.readback(out)
     t0 = time.perf_counter()
-    for c in scenes:
-        r.render_to_image(c)
+    for ps in scenes:
+        r.upload(ps)
+        r.render()
+        r.readback(out)
     serial_s = time.perf_counter() - t0
     r.close()
     b = tk.NativeRenderer(0)
     b.batch_upload(scenes)  # warm-up, as the serial path had: first allocations and graph capture
     b.batch_render()
-    imgs = b.batch_readback()
+    imgs = b.batch_readback(out)
     e2e = []
     for _ in range(steps):  # upload (host merge + copies), render, readback, each cycle
         t0 = time.perf_counter()
         b.batch_upload(scenes)
         b.batch_render()
-        imgs = b.batch_readback()
+        imgs = b.batch_readback(out)
         e2e.append(time.perf_counter() - t0)
     e2e_s = statistics.median(e2e)
     tune = b.autotune(3)
@@ -312,7 +324,7 @@ def batch_timing(n_scenes, steps):
             "tune_ms": {str(tune.candidate_elems[i]): tune.candidate_ms[i] for i in range(tune.candidates)},
             "timing": "host wall clock, warmed up; batched = graph replays + one readback, batched e2e = "
                       "median of upload + render + readback cycles, serial = per-scene upload, render and "
-                      "readback"}
+                      "readback; records in pinned host memory, images read into a pinned buffer"}
 
 
 def incremental_timing(r, size, steps):

@@ -1495,11 +1495,14 @@ void do_batch_render(tk_ctx* c) {
     if (!c->have_scene || !c->batched) throw Fail{TK_E_STATE, "no batch uploaded"};
     cudaStream_t st = c->stream;
     if (!c->graph_exec) {
-        // First frame sizes the PTCL (a host read-back), then the same launch
-        // sequence is captured once and replayed from then on.
+        // First frame sizes the PTCL (a host read-back) and is this render's
+        // frame; the same launch sequence is then captured once (capture
+        // runs nothing) and replayed by the renders after it.
+        bool rendered_now = false;
         if (c->passes[0].ptcl_needed == 0) {
             batch_frame(c);
             check_error_word(c);
+            rendered_now = true;
         }
         const bool timing = c->timing;
         c->timing = false;
@@ -1518,6 +1521,10 @@ void do_batch_render(tk_ctx* c) {
         cudaError_t e = cudaGraphInstantiate(&c->graph_exec, g, 0);
         cudaGraphDestroy(g);
         TK_CUDA(e);
+        if (rendered_now) {
+            c->rendered = true;
+            return;
+        }
     }
     TK_CUDA(cudaGraphLaunch(c->graph_exec, st));
     c->rendered = true;

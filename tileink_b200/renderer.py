@@ -226,7 +226,7 @@ class NativeRenderer:
     # --- batched mode -----------------------------------------------------------
     def batch_upload(self, canvases) -> None:
         """Uploads independent one-pass scenes as one batch."""
-        descs = [c.scene_desc() if hasattr(c, "scene_desc") else c for c in canvases]
+        descs = [c.scene_desc() if hasattr(c, "scene_desc") else getattr(c, "desc", c) for c in canvases]
         arr = (N.SceneDesc * len(descs))(*descs)
         self._batch_keep = (canvases, descs, arr)
         self._check(self._lib.tk_batch_upload(self._h, C.cast(arr, C.c_void_p), len(descs)))
@@ -240,11 +240,15 @@ class NativeRenderer:
         self._check(self._lib.tk_batch_info_get(self._h, int(scene), C.byref(out)))
         return out
 
-    def batch_readback(self):
-        """Every scene's premultiplied RGBA8 image, (H, W, 4) uint8 each."""
+    def batch_readback(self, out: np.ndarray | None = None):
+        """Every scene's premultiplied RGBA8 image, (H, W, 4) uint8 each,
+        views into one buffer of all scenes' pixels (`out`: a caller's uint32
+        buffer of exactly that many pixels, e.g. in pinned memory)."""
         infos = self._batch_info
         total = sum(i.width * i.height for i in infos)
-        buf = np.zeros(total, dtype=np.uint32)
+        buf = np.empty(total, dtype=np.uint32) if out is None else out  # every pixel is written
+        if buf.dtype != np.uint32 or buf.size != total or not buf.flags.c_contiguous:
+            raise ValueError(f"batch readback needs a contiguous uint32 buffer of {total} pixels")
         self._check(self._lib.tk_batch_readback(self._h, N.ptr(buf), total))
         return [buf[i.image_offset:i.image_offset + i.width * i.height].view(np.uint8).reshape(i.height, i.width, 4)
                 for i in infos]
