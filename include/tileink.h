@@ -327,6 +327,42 @@ typedef struct tk_progressive_blur {
 #define TK_PROGRESSIVE_BALANCED 0u
 #define TK_PROGRESSIVE_HIGH 1u
 
+/* A filter layer (Canvas::push_filter_layer with Filter::Chain,
+ * src/canvas/layers.rs:222-233, src/shared/layer/filter.rs:28-95): the
+ * group's surface filtered in place by a chain of filters, each over the
+ * layer's processing bounds, then composited src-over onto the enclosing
+ * target (render/filters.rs:71-243, render/filter_program/effects.rs:3-268).
+ * TK_OP_FILTER_BEGIN opens it (batch_id indexes the scene's filter layers;
+ * the output bounds are the layer's surface bounds clipped to the canvas,
+ * derived by the library, and the op's own bounds are not read);
+ * TK_OP_BLUR_END closes it. */
+#define TK_OP_FILTER_BEGIN 4u
+/* Filter kinds: the colour filters of filter/constants.hlsli, then the
+ * colour matrix and the offset. */
+#define TK_FILTER_BRIGHTNESS 1u
+#define TK_FILTER_CONTRAST 2u
+#define TK_FILTER_GRAYSCALE 3u
+#define TK_FILTER_HUE_ROTATE 4u
+#define TK_FILTER_INVERT 5u
+#define TK_FILTER_OPACITY 6u
+#define TK_FILTER_SATURATE 7u
+#define TK_FILTER_SEPIA 8u
+#define TK_FILTER_COLOR_MATRIX 9u /* Filter::ColorMatrix: 4 rows of 5 (r g b a bias), filter/color.hlsli:47-76 */
+#define TK_FILTER_OFFSET 10u      /* Filter::Offset: dx, dy already whole pixels (ceil(d - 0.5)) */
+typedef struct tk_filter {
+    uint32_t kind;
+    float amount;      /* the colour filters' argument (hue rotation in degrees) */
+    int32_t dx, dy;    /* TK_FILTER_OFFSET */
+    float matrix[20];  /* TK_FILTER_COLOR_MATRIX, row-major */
+} tk_filter; /* 96 B */
+/* One filter layer: its chain filters[first, first + count), and the surface
+ * bounds the chain reads (the sample region's pixel bounds grown by the
+ * chain's reach, filter.rs:510-575; may extend past the canvas). */
+typedef struct tk_filter_layer {
+    uint32_t first, count;
+    int32_t surface[4];  /* x0, y0, x1, y1 */
+} tk_filter_layer; /* 24 B */
+
 /* Scene flags */
 #define TK_SCENE_SEGMENTS_FROM_DEVICE 1u /* recompute segment_start on device */
 
@@ -375,6 +411,11 @@ typedef struct tk_scene_desc {
     const tk_progressive_blur* progressive_blurs;
     uint32_t progressive_count;
     uint32_t progressive_reserved;
+    /* the filter layers FILTER_BEGIN ops index, and their chains' filters */
+    const tk_filter_layer* filter_layers;
+    const tk_filter* filters;
+    uint32_t filter_layer_count;
+    uint32_t filter_count;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

@@ -189,6 +189,26 @@ int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sa
  * Returns -1 for a non-finite or out-of-range parameter. */
 int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, double start_y, double end_x,
                                               double end_y, float max_std_dev, uint32_t quality);
+/* One filter of a filter layer's chain, in logical units: a colour filter
+ * (TK_FILTER_BRIGHTNESS .. TK_FILTER_SEPIA with its amount; hue rotation in
+ * degrees), TK_FILTER_COLOR_MATRIX (matrix: 4 rows of r g b a bias) or
+ * TK_FILTER_OFFSET (dx, dy). */
+typedef struct tk_canvas_filter {
+    uint32_t kind;
+    float amount;
+    float dx, dy;
+    float matrix[20];
+} tk_canvas_filter;
+/* Canvas::push_filter_layer with Filter::Chain { filters, fixed_region } and
+ * a Region::Rect sample region without corner radii (src/canvas/layers.rs:
+ * 222-233; physical_filter / physical_region, canvas/surface.rs:197-326):
+ * the children until the matching pop are rendered into a surface, filtered
+ * in place by the chain and composited over the output bounds (the region's
+ * pixel bounds grown by the chain's reach unless fixed_region, clipped to
+ * the canvas; shared/layer/filter.rs:510-597). `rect` = {x0, y0, x1, y1}.
+ * Returns -1 for an unknown kind or a non-finite value. */
+int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double rect[4],
+                                    int32_t fixed_region);
 /* Canvas::push_opacity_layer (src/canvas/layers.rs:122-140): the children
  * until the matching pop are composited at `opacity` (clamped to [0, 1],
  * stored as opacity_f32_to_u8) through the nonzero coverage of `path`. The

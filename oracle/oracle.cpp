@@ -1940,6 +1940,137 @@ void blur_pass(const uint32_t* src, uint32_t* dst, uint32_t w, uint32_t h, const
 // --- filter/resample.hlsli: reduced-resolution blur (BlurSampling factor > 1) ---
 // filter_downsample_pixel for every low texel of `low_rect`: the cell's centre
 // texel (filter 0) or its byte average rounded half up (filter 1).
+// --- filter/color.hlsli:7-76, filter/basic.hlsl:49-56 ------------------------
+// The filter layer chain: colour filters and the colour matrix on the stored
+// RGBA8 word (mad fused, every other product and sum rounded on its own), and
+// the whole-pixel offset, each over the layer's bounds
+// (render/filter_program/effects.rs:3-268).
+inline float svg_luminance(float r, float g, float b) { return (0.2126f * r + 0.7152f * g) + 0.0722f * b; }
+
+uint32_t filter_color_pixel(uint32_t pixel, uint32_t kind, float amount) {
+    if ((kind == TK_FILTER_INVERT || kind == TK_FILTER_SEPIA) && (pixel >> 24) != 0u) {
+        const float cr = float(pixel & 255u), cg = float((pixel >> 8) & 255u), cb = float((pixel >> 16) & 255u);
+        const float alpha = float(pixel >> 24);
+        float mr = alpha - cr, mg = alpha - cg, mb = alpha - cb;
+        if (kind == TK_FILTER_SEPIA) {
+            mr = mad(0.393f, cr, mad(0.769f, cg, 0.189f * cb));
+            mg = mad(0.349f, cr, mad(0.686f, cg, 0.168f * cb));
+            mb = mad(0.272f, cr, mad(0.534f, cg, 0.131f * cb));
+        }
+        const float t = clampf(amount, 0.0f, 1.0f);
+        return pack(f2u(clampf(mad(mr - cr, t, cr), 0.0f, alpha) + 0.5f),
+                    f2u(clampf(mad(mg - cg, t, cg), 0.0f, alpha) + 0.5f),
+                    f2u(clampf(mad(mb - cb, t, cb), 0.0f, alpha) + 0.5f), pixel >> 24);
+    }
+    F4 c = rgba8_to_unorm(pixel);
+    if (kind == TK_FILTER_OPACITY) {
+        const float a = clampf(amount, 0.0f, 1.0f);
+        c = {c.r * a, c.g * a, c.b * a, c.a * a};
+    } else if (c.a > 0.0f) {
+        float r = c.r / c.a, g = c.g / c.a, b = c.b / c.a;
+        if (kind == TK_FILTER_BRIGHTNESS) {
+            r = r * amount;
+            g = g * amount;
+            b = b * amount;
+        } else if (kind == TK_FILTER_CONTRAST) {
+            r = (r - 0.5f) * amount + 0.5f;
+            g = (g - 0.5f) * amount + 0.5f;
+            b = (b - 0.5f) * amount + 0.5f;
+        } else if (kind == TK_FILTER_GRAYSCALE) {
+            const float l = svg_luminance(r, g, b), t = clampf(amount, 0.0f, 1.0f);
+            r = mad(l - r, t, r);
+            g = mad(l - g, t, g);
+            b = mad(l - b, t, b);
+        } else if (kind == TK_FILTER_HUE_ROTATE) {
+            float si, co;
+            lib_sincos(amount * 0.017453292f, si, co);
+            const float nr = ((0.213f + co * 0.787f) - si * 0.213f) * r + ((0.715f - co * 0.715f) - si * 0.715f) * g +
+                             ((0.072f - co * 0.072f) + si * 0.928f) * b;
+            const float ng = ((0.213f - co * 0.213f) + si * 0.143f) * r + ((0.715f + co * 0.285f) + si * 0.140f) * g +
+                             ((0.072f - co * 0.072f) - si * 0.283f) * b;
+            const float nb = ((0.213f - co * 0.213f) - si * 0.787f) * r + ((0.715f - co * 0.715f) + si * 0.715f) * g +
+                             ((0.072f + co * 0.928f) + si * 0.072f) * b;
+            r = nr;
+            g = ng;
+            b = nb;
+        } else if (kind == TK_FILTER_SATURATE) {
+            const float l = svg_luminance(r, g, b);
+            r = l + (r - l) * amount;
+            g = l + (g - l) * amount;
+            b = l + (b - l) * amount;
+        }
+        c = {clampf(r, 0.0f, 1.0f) * c.a, clampf(g, 0.0f, 1.0f) * c.a, clampf(b, 0.0f, 1.0f) * c.a, c.a};
+    }
+    return pack(f2u(clampf(c.r, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c.g, 0.0f, 1.0f) * 255.0f + 0.5f),
+                f2u(clampf(c.b, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c.a, 0.0f, 1.0f) * 255.0f + 0.5f));
+}
+
+inline float filter_dot4(const float* a, float x, float y, float z, float w) {
+    return mad(a[0], x, mad(a[1], y, mad(a[2], z, a[3] * w)));
+}
+
+uint32_t filter_color_matrix_pixel(const float* m, uint32_t pixel) {
+    const float alpha = float(pixel >> 24);
+    const float cr = float(pixel & 255u), cg = float((pixel >> 8) & 255u), cb = float((pixel >> 16) & 255u);
+    float sr = 0.0f, sg = 0.0f, sb = 0.0f;
+    if ((pixel >> 24) == 255u) {
+        sr = cr;
+        sg = cg;
+        sb = cb;
+    } else if (alpha > 0.0f) {
+        const float k = 255.0f / alpha;
+        sr = cr * k;
+        sg = cg * k;
+        sb = cb * k;
+    }
+    const float out_a = std::floor(clampf(filter_dot4(m + 15, sr, sg, sb, alpha) + m[19] * 255.0f, 0.0f, 255.0f) + 0.5f);
+    float rr, rg, rb;
+    if (alpha > 0.0f) {
+        const float sw = alpha * alpha * CHANNEL_SCALE;
+        const float mr = mad(m[4], alpha, filter_dot4(m + 0, cr, cg, cb, sw));
+        const float mg = mad(m[9], alpha, filter_dot4(m + 5, cr, cg, cb, sw));
+        const float mb = mad(m[14], alpha, filter_dot4(m + 10, cr, cg, cb, sw));
+        const float scale = out_a == alpha ? 1.0f : out_a / alpha;
+        rr = mr >= alpha ? out_a : clampf(mr, 0.0f, alpha) * scale;
+        rg = mg >= alpha ? out_a : clampf(mg, 0.0f, alpha) * scale;
+        rb = mb >= alpha ? out_a : clampf(mb, 0.0f, alpha) * scale;
+    } else {
+        rr = clampf(m[4], 0.0f, 1.0f) * out_a;
+        rg = clampf(m[9], 0.0f, 1.0f) * out_a;
+        rb = clampf(m[14], 0.0f, 1.0f) * out_a;
+    }
+    return pack(f2u(clampf(rr, 0.0f, 255.0f) + 0.5f), f2u(clampf(rg, 0.0f, 255.0f) + 0.5f),
+                f2u(clampf(rb, 0.0f, 255.0f) + 0.5f), f2u(clampf(out_a, 0.0f, 255.0f) + 0.5f));
+}
+
+void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const tk_filter* chain, uint32_t count) {
+    if (b[2] <= b[0] || b[3] <= b[1]) return;
+    for (uint32_t k = 0; k < count; ++k) {
+        const tk_filter& f = chain[k];
+        if (f.kind == TK_FILTER_OFFSET) {
+            if (f.dx == 0 && f.dy == 0) continue;
+            std::vector<uint32_t> temp(size_t(b[2] - b[0]) * size_t(b[3] - b[1]));
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) {
+                    const int64_t sx = int64_t(x) - f.dx, sy = int64_t(y) - f.dy;
+                    uint32_t p = 0u;
+                    if (sx >= b[0] && sy >= b[1] && sx < b[2] && sy < b[3]) p = surface[size_t(sy) * width + size_t(sx)];
+                    temp[size_t(y - b[1]) * size_t(b[2] - b[0]) + size_t(x - b[0])] = p;
+                }
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x)
+                    surface[size_t(y) * width + x] = temp[size_t(y - b[1]) * size_t(b[2] - b[0]) + size_t(x - b[0])];
+        } else {
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) {
+                    uint32_t& p = surface[size_t(y) * width + x];
+                    p = f.kind == TK_FILTER_COLOR_MATRIX ? filter_color_matrix_pixel(f.matrix, p)
+                                                         : filter_color_pixel(p, f.kind, f.amount);
+                }
+        }
+    }
+}
+
 // --- filter/progressive.hlsl and progressive/{mod,pyramid}.rs -------------------
 // The progressive blur: a pyramid of RGBA8 levels (each the previous one
 // convolved with a paired Gaussian kernel along x then y and decimated by its
@@ -2301,6 +2432,8 @@ void raster_scene(or_scene& S, int threads) {
         uint32_t sampling;
         bool progressive = false;
         tk_progressive_blur prog{};
+        bool filter = false;  // a filter layer: its chain
+        std::vector<tk_filter> chain;
     };
     std::vector<Surface> surfaces;
     auto current = [&]() -> std::vector<uint32_t>& { return surfaces.empty() ? main_target : surfaces.back().img; };
@@ -2391,6 +2524,23 @@ void raster_scene(or_scene& S, int threads) {
             s.progressive = true;
             s.prog = D.progressive_blurs[op.batch_id];
             surfaces.push_back(std::move(s));
+        } else if (op.kind == TK_OP_FILTER_BEGIN) {
+            flush_pass();
+            if (op.batch_id >= D.filter_layer_count) throw std::runtime_error("filter layer out of range");
+            const tk_filter_layer& L = D.filter_layers[op.batch_id];
+            if (uint64_t(L.first) + L.count > D.filter_count) throw std::runtime_error("filter chain out of range");
+            Surface s;
+            s.img.assign(size_t(D.width) * D.height, 0u);
+            s.sigma = 0.0f;
+            // output bounds: the surface clipped to the canvas (filter.rs:510-527)
+            s.bounds[0] = std::max(L.surface[0], 0);
+            s.bounds[1] = std::max(L.surface[1], 0);
+            s.bounds[2] = std::min(L.surface[2], int32_t(D.width));
+            s.bounds[3] = std::min(L.surface[3], int32_t(D.height));
+            s.sampling = 0u;
+            s.filter = true;
+            s.chain.assign(D.filters + L.first, D.filters + L.first + L.count);
+            surfaces.push_back(std::move(s));
         } else if (op.kind == TK_OP_BLUR_END) {
             flush_pass();
             if (surfaces.empty()) throw std::runtime_error("unbalanced BLUR_END");
@@ -2406,7 +2556,10 @@ void raster_scene(or_scene& S, int threads) {
             int32_t sx0 = std::max(s.bounds[0] - rad, 0), sy0 = std::max(s.bounds[1] - rad, 0);
             int32_t sx1 = std::min(s.bounds[2] + rad, int32_t(D.width));
             int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
-            if (s.progressive) {
+            if (s.filter) {
+                const int32_t rect[4] = {bx0, by0, bx1, by1};
+                filter_chain(s.img.data(), D.width, rect, s.chain.data(), uint32_t(s.chain.size()));
+            } else if (s.progressive) {
                 if (bx1 > bx0 && by1 > by0 && s.prog.max_std_dev > 0.0f) {
                     const int32_t rect[4] = {bx0, by0, bx1, by1};
                     progressive_blur(s.img.data(), D.width, rect, s.prog);
@@ -2750,6 +2903,9 @@ float or_exp_nonpos(float x) { return exp_nonpos(x); }
 void or_sincos(float x, float* s, float* c) { lib_sincos(x, *s, *c); }
 float or_atan2(float y, float x) { return lib_atan2(y, x); }
 float or_text_pow(float x, float y) { return text_pow(x, y); }
+void or_filter_chain(uint32_t* surface, uint32_t width, const int32_t rect[4], const tk_filter* chain, uint32_t count) {
+    filter_chain(surface, width, rect, chain, count);
+}
 int32_t or_progressive_blur(uint32_t* surface, uint32_t width, uint32_t height, const int32_t rect[4],
                             const tk_progressive_blur* blur) {
     try {

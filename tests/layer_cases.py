@@ -112,3 +112,55 @@ def progressive_scene(seed, w=200, h=150, sigma=6.0, quality=0, uniform=False):
     c.pop_layer()
     c.push_path(blob(rng, w * 0.5, h * 0.5, 20), tk.Brush.solid(0.1, 0.2, 0.3, 0.5))
     return c
+
+
+def filter_scene(seed, chain, rect, fixed_region=False, w=200, h=150, children=True):
+    """Fills inside a filter layer (Canvas::push_filter_layer with a chain of
+    filters over a rect sample region), over fills outside it; `chain` as
+    Canvas.push_filter_layer takes it. children=False leaves the layer empty
+    (the same random scene otherwise)."""
+    rng = np.random.default_rng(seed)
+    c = tk.Canvas(w, h)
+    c.set_clear_color(0xFFFFFFFF)
+    for _ in range(4):
+        c.push_path(blob(rng, rng.uniform(0, w), rng.uniform(0, h), 30), tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0))
+    c.push_filter_layer(chain, rect, fixed_region)
+    for k in range(10):
+        if k % 3 == 2:
+            x, y, r = rng.uniform(0, w), rng.uniform(0, h), float(rng.uniform(10, 40))
+            b = tk.Brush.linear((x - r, y), (x + r, y + r), [(0.0, (*rng.uniform(0, 1, 3), 1.0)),
+                                                            (1.0, (*rng.uniform(0, 1, 3), 0.5))])
+        else:
+            b = tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.3, 1)))
+        path = blob(rng, rng.uniform(10, w - 10), rng.uniform(10, h - 10), rng.uniform(6, 40))
+        if children:
+            c.push_path(path, b, fill_rule=k % 2)
+    c.pop_layer()
+    c.push_path(blob(rng, w * 0.5, h * 0.5, 20), tk.Brush.solid(0.1, 0.2, 0.3, 0.5))
+    return c
+
+
+# chains for the filter layer tests: every colour filter, the colour matrix,
+# offsets, and chains mixing them
+SEPIA_MATRIX = [0.393, 0.769, 0.189, 0, 0, 0.349, 0.686, 0.168, 0, 0, 0.272, 0.534, 0.131, 0, 0, 0, 0, 0, 1, 0]
+
+
+def filter_chains():
+    """Named chains for the filter layer tests."""
+    from tileink_b200 import _native as N
+    return {
+        "brightness": [(N.FILTER_BRIGHTNESS, 1.6)],
+        "contrast": [(N.FILTER_CONTRAST, 0.45)],
+        "grayscale": [(N.FILTER_GRAYSCALE, 0.8)],
+        "hue_rotate": [(N.FILTER_HUE_ROTATE, 137.0)],
+        "invert": [(N.FILTER_INVERT, 0.7)],
+        "opacity": [(N.FILTER_OPACITY, 0.55)],
+        "saturate": [(N.FILTER_SATURATE, 2.3)],
+        "sepia": [(N.FILTER_SEPIA, 1.0)],
+        "matrix": [(N.FILTER_COLOR_MATRIX, SEPIA_MATRIX)],
+        "matrix_alpha": [(N.FILTER_COLOR_MATRIX, [1, 0, 0, 0, 0.1, 0, 0.5, 0.5, 0, 0, 0, 0, 1, 0, -0.2,
+                                                  0, 0, 0, 0.6, 0.1])],
+        "offset": [(N.FILTER_OFFSET, (7.5, -4.2))],
+        "chain": [(N.FILTER_GRAYSCALE, 0.5), (N.FILTER_OFFSET, (-3.0, 5.6)), (N.FILTER_HUE_ROTATE, -60.0),
+                  (N.FILTER_CONTRAST, 1.4), (N.FILTER_OPACITY, 0.8)],
+    }

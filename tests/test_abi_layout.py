@@ -31,6 +31,9 @@ DTYPE_MIRRORS = {
     "tk_stroke_polyline": N.POLYLINE_DTYPE, "tk_stroke_desc": N.STROKE_DTYPE,
     "tk_glyph_run": N.GLYPH_RUN_DTYPE, "tk_glyph": N.GLYPH_DTYPE, "tk_glyph_image": N.GLYPH_IMAGE_DTYPE,
     "tk_progressive_blur": N.PROGRESSIVE_DTYPE,
+    "tk_filter": N.FILTER_DTYPE,
+    "tk_filter_layer": N.FILTER_LAYER_DTYPE,
+    "tk_canvas_filter": N.CANVAS_FILTER_DTYPE,
 }
 
 

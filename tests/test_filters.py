@@ -1,0 +1,206 @@
+"""Filter layers on CPU: the oracle's colour filters and colour matrix
+(filter/color.hlsli:7-76) against an independent float32 restatement in
+numpy, their exact identities, the offset (filter/basic.hlsl:49-56), and the
+Canvas's recording of filter layers (layers.rs:222-233, filter.rs:490-597)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import tileink_b200 as tk
+from tileink_b200 import _native as N
+
+from layer_cases import SEPIA_MATRIX, filter_chains, filter_scene
+
+F = np.float32
+
+
+def premul_pixels(n, seed):
+    """n premultiplied RGBA8 words with alpha 0, 255 and in between."""
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, 256, n).astype(np.uint32)
+    a[:8] = [0, 255, 255, 1, 128, 254, 0, 255]
+    rgb = (rng.random((n, 3)) * (a[:, None] + 1)).astype(np.uint32)
+    rgb = np.minimum(rgb, a[:, None])
+    return rgb[:, 0] | (rgb[:, 1] << 8) | (rgb[:, 2] << 16) | (a << 24)
+
+
+def oracle_chain(pixels, chain):
+    """The oracle's filter chain over a one-row surface."""
+    surf = np.ascontiguousarray(pixels, dtype=np.uint32).copy()
+    filters = np.zeros(len(chain), dtype=N.FILTER_DTYPE)
+    for k, (kind, value) in enumerate(chain):
+        filters[k]["kind"] = kind
+        if kind == N.FILTER_COLOR_MATRIX:
+            filters[k]["matrix"] = np.asarray(value, dtype=np.float32)
+        elif kind == N.FILTER_OFFSET:
+            filters[k]["dx"], filters[k]["dy"] = value
+        else:
+            filters[k]["amount"] = value
+    rect = np.array([0, 0, len(surf), 1], dtype=np.int32)
+    oracle.lib().or_filter_chain(N.ptr(surf), len(surf), N.ptr(rect), N.ptr(filters), len(filters))
+    return surf
+
+
+def mad(a, b, c):
+    """A fused multiply-add in float32: the float64 product of two float32
+    values is exact, so one rounding of the sum and one to float32."""
+    return F(np.float64(a) * np.float64(b) + np.float64(c))
+
+
+def np_color_pixel(p, kind, amount):
+    """filter_color_pixel restated with numpy float32 scalars."""
+    amount = F(amount)
+    ch = [F(int(p) >> s & 255) for s in (0, 8, 16)]
+    alpha = int(p) >> 24
+    if kind in (N.FILTER_INVERT, N.FILTER_SEPIA) and alpha:
+        fa = F(alpha)
+        m = [fa - c for c in ch]
+        if kind == N.FILTER_SEPIA:
+            r, g, b = ch
+            m = [mad(F(0.393), r, mad(F(0.769), g, F(0.189) * b)), mad(F(0.349), r, mad(F(0.686), g, F(0.168) * b)),
+                 mad(F(0.272), r, mad(F(0.534), g, F(0.131) * b))]
+        t = F(min(max(amount, F(0)), F(1)))
+        out = [int(F(min(max(mad(mm - c, t, c), F(0)), fa)) + F(0.5)) for mm, c in zip(m, ch)]
+        return out + [alpha]
+    scale = F(1.0) / F(255.0)
+    c = [F(int(p) >> s & 255) * scale for s in (0, 8, 16, 24)]
+    if kind == N.FILTER_OPACITY:
+        a = F(min(max(amount, F(0)), F(1)))
+        c = [x * a for x in c]
+    elif c[3] > 0:
+        st = [x / c[3] for x in c[:3]]
+        lum = lambda v: (F(0.2126) * v[0] + F(0.7152) * v[1]) + F(0.0722) * v[2]  # noqa: E731
+        if kind == N.FILTER_BRIGHTNESS:
+            st = [x * amount for x in st]
+        elif kind == N.FILTER_CONTRAST:
+            st = [(x - F(0.5)) * amount + F(0.5) for x in st]
+        elif kind == N.FILTER_GRAYSCALE:
+            l, t = lum(st), F(min(max(amount, F(0)), F(1)))
+            st = [mad(l - x, t, x) for x in st]
+        elif kind == N.FILTER_HUE_ROTATE:
+            ang = amount * F(0.017453292)
+            co, si = F(math.cos(float(ang))), F(math.sin(float(ang)))
+            r, g, b = st
+            st = [((F(0.213) + co * F(0.787)) - si * F(0.213)) * r + ((F(0.715) - co * F(0.715)) - si * F(0.715)) * g
+                  + ((F(0.072) - co * F(0.072)) + si * F(0.928)) * b,
+                  ((F(0.213) - co * F(0.213)) + si * F(0.143)) * r + ((F(0.715) + co * F(0.285)) + si * F(0.140)) * g
+                  + ((F(0.072) - co * F(0.072)) - si * F(0.283)) * b,
+                  ((F(0.213) - co * F(0.213)) - si * F(0.787)) * r + ((F(0.715) - co * F(0.715)) + si * F(0.715)) * g
+                  + ((F(0.072) + co * F(0.928)) + si * F(0.072)) * b]
+        elif kind == N.FILTER_SATURATE:
+            l = lum(st)
+            st = [l + (x - l) * amount for x in st]
+        c = [F(min(max(x, F(0)), F(1))) * c[3] for x in st] + [c[3]]
+    return [int(F(min(max(x, F(0)), F(1))) * F(255) + F(0.5)) for x in c]
+
+
+COLOR_CASES = [(N.FILTER_BRIGHTNESS, 1.6), (N.FILTER_BRIGHTNESS, 0.3), (N.FILTER_CONTRAST, 0.45),
+               (N.FILTER_CONTRAST, 2.5), (N.FILTER_GRAYSCALE, 0.8), (N.FILTER_GRAYSCALE, 1.0),
+               (N.FILTER_HUE_ROTATE, 137.0), (N.FILTER_HUE_ROTATE, -60.0), (N.FILTER_INVERT, 0.7),
+               (N.FILTER_INVERT, 1.0), (N.FILTER_OPACITY, 0.55), (N.FILTER_SATURATE, 2.3),
+               (N.FILTER_SATURATE, 0.0), (N.FILTER_SEPIA, 1.0), (N.FILTER_SEPIA, 0.4)]
+
+
+@pytest.mark.parametrize("kind, amount", COLOR_CASES)
+def test_color_filters_match_numpy_restatement(kind, amount):
+    px = premul_pixels(3000, kind * 1000 + int(abs(amount) * 10))
+    got = oracle_chain(px, [(kind, amount)])
+    want = np.array([np_color_pixel(p, kind, amount) for p in px], dtype=np.int64)
+    gotc = np.stack([(got >> s) & 255 for s in (0, 8, 16, 24)], axis=1).astype(np.int64)
+    d = np.abs(gotc - want)
+    assert d.max() <= 1, d.max()  # a double-rounded mad or a sin / cos last bit moves one level at most
+    assert (d == 0).mean() >= 0.995
+
+
+def test_color_filter_identities_are_exact():
+    px = premul_pixels(4000, 5)
+    for chain in ([(N.FILTER_INVERT, 0.0)], [(N.FILTER_SEPIA, 0.0)], [(N.FILTER_OPACITY, 1.0)],
+                  [(N.FILTER_COLOR_MATRIX, [1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 1, 0])], []):
+        assert np.array_equal(oracle_chain(px, chain), px), chain
+    # invert of an opaque pixel is 255 - c exactly; opacity 0 clears
+    opaque = (px & 0x00FFFFFF) | 0xFF000000
+    inv = oracle_chain(opaque, [(N.FILTER_INVERT, 1.0)])
+    assert np.array_equal(inv, (0x00FFFFFF - (opaque & 0x00FFFFFF)) | 0xFF000000)
+    assert not oracle_chain(px, [(N.FILTER_OPACITY, 0.0)]).any()
+
+
+def test_color_matrix_keeps_bytes_and_saturates():
+    px = premul_pixels(3000, 9)
+    got = oracle_chain(px, [(N.FILTER_COLOR_MATRIX, SEPIA_MATRIX)])
+    a = px >> 24
+    assert np.array_equal(got >> 24, a)  # alpha row (0 0 0 1 0): alpha unchanged
+    for s in (0, 8, 16):  # premultiplied channels stay within alpha
+        assert np.all(((got >> s) & 255) <= a)
+    # a bias of 1 on every channel saturates to the output alpha
+    sat = oracle_chain(px, [(N.FILTER_COLOR_MATRIX, [0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 1, 0])])
+    assert np.array_equal(sat, a * 0x01010101)
+
+
+def test_offset_moves_pixels_inside_the_bounds():
+    w, h = 23, 17
+    surf = np.arange(1, w * h + 1, dtype=np.uint32)
+    filters = np.zeros(1, dtype=N.FILTER_DTYPE)
+    filters[0]["kind"], filters[0]["dx"], filters[0]["dy"] = N.FILTER_OFFSET, 4, -3
+    rect = np.array([2, 1, 20, 15], dtype=np.int32)
+    out = surf.copy()
+    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(rect), N.ptr(filters), 1)
+    s2, o2 = surf.reshape(h, w), out.reshape(h, w)
+    for y in range(h):
+        for x in range(w):
+            if not (2 <= x < 20 and 1 <= y < 15):
+                assert o2[y, x] == s2[y, x]  # outside the bounds: untouched
+                continue
+            sx, sy = x - 4, y + 3
+            want = s2[sy, sx] if (2 <= sx < 20 and 1 <= sy < 15) else 0
+            assert o2[y, x] == want
+
+
+def test_canvas_records_filter_layers():
+    c = tk.Canvas(128, 96)
+    c.push_filter_layer([(N.FILTER_GRAYSCALE, 0.5), (N.FILTER_OFFSET, (7.5, -4.2)), (N.FILTER_OFFSET, (-2.6, 0.4))],
+                        (10.2, 20.7, 60.1, 50.0))
+    c.push_path(tk.BezPath().move_to(20, 30).line_to(50, 35).line_to(40, 45).close(), tk.Brush.solid(1, 0, 0, 1))
+    c.pop_layer()
+    a = c.scene_arrays()
+    ops = a["ops"]
+    assert list(ops["kind"]) == [N.OP_FILTER_BEGIN, N.OP_DRAW_BATCH, N.OP_BLUR_END]
+    L = a["filter_layers"][ops["batch_id"][0]]
+    fl = a["filters"][L["first"]:L["first"] + L["count"]]
+    assert list(fl["kind"]) == [N.FILTER_GRAYSCALE, N.FILTER_OFFSET, N.FILTER_OFFSET]
+    # filter_offset_to_pixel_delta: ceil(d - 0.5)
+    assert (fl["dx"][1], fl["dy"][1], fl["dx"][2], fl["dy"][2]) == (7, -4, -3, 0)
+    # the region's pixel bounds (floor / ceil) grown by the chain's reach
+    # (max(ceil|dx|, ceil|dy|) per offset: 8 + 3)
+    assert list(L["surface"]) == [10 - 11, 20 - 11, 61 + 11, 50 + 11]
+    assert list(ops["bounds"][0]) == [0, 9, 72, 61]  # clipped to the canvas
+    # fixed_region: no reach; a canvas scale scales the region and the offsets
+    c2 = tk.Canvas(128, 96, scale=2.0)
+    c2.push_filter_layer([(N.FILTER_OFFSET, (1.3, 0.0))], (1.0, 2.0, 10.0, 12.0), fixed_region=True)
+    c2.pop_layer()
+    a2 = c2.scene_arrays()
+    L2 = a2["filter_layers"][0]
+    assert list(L2["surface"]) == [2, 4, 20, 24] and a2["filters"][0]["dx"] == 3  # ceil(2.6 - 0.5)
+    with pytest.raises(ValueError):
+        c.push_filter_layer([(99, 1.0)], (0, 0, 10, 10))
+    with pytest.raises(ValueError):
+        c.push_filter_layer([(N.FILTER_BRIGHTNESS, float("nan"))], (0, 0, 10, 10))
+
+
+def test_filter_layer_that_hides_its_children():
+    # opacity 0 removes the group: the frame equals the one with an empty group
+    rect = (20, 10, 180, 140)
+    ca, cb = filter_scene(3, [(N.FILTER_OPACITY, 0.0)], rect), filter_scene(3, [], rect, children=False)
+    a = oracle.OracleRun(ca.scene_desc(), threads=4)
+    b = oracle.OracleRun(cb.scene_desc(), threads=4)
+    assert np.array_equal(a.get(oracle.OR_IMAGE, np.uint32), b.get(oracle.OR_IMAGE, np.uint32))
+
+
+@pytest.mark.parametrize("name", sorted(filter_chains()))
+def test_filter_scenes_render_in_the_oracle(name):
+    c = filter_scene(7, filter_chains()[name], (15.5, 12.0, 170.2, 131.9))
+    img = oracle.OracleRun(c.scene_desc(), threads=4).get(oracle.OR_IMAGE, np.uint32)
+    assert img.any()

@@ -114,3 +114,50 @@ def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uni
     shallow blur, bit-exact against the oracle."""
     from layer_cases import progressive_scene
     compare_frame(renderer, progressive_scene(seed, sigma=sigma, quality=quality, uniform=uniform))
+
+
+@pytest.mark.parametrize("name", ["brightness", "contrast", "grayscale", "hue_rotate", "invert", "opacity",
+                                  "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain"])
+def test_gpu_filter_layers_match_oracle(renderer, name):
+    """Filter layers (Canvas::push_filter_layer with a chain; filter/color.hlsli,
+    filter/basic.hlsl): every colour filter, the colour matrix, offsets and a
+    mixed chain, bit-exact against the oracle."""
+    from layer_cases import filter_chains, filter_scene
+    compare_frame(renderer, filter_scene(11, filter_chains()[name], (15.5, 12.0, 170.2, 131.9)))
+
+
+def test_gpu_filter_layer_regions(renderer):
+    """Regions partly or wholly off the canvas (colour filters only), a fixed
+    region with an offset, an empty region, and filter layers nested in blur
+    groups and in each other."""
+    from layer_cases import blob, filter_scene
+    compare_frame(renderer, filter_scene(4, [(N.FILTER_SEPIA, 0.9), (N.FILTER_SATURATE, 1.7)], (-40.0, -20.5, 90.0, 80.0)))
+    compare_frame(renderer, filter_scene(5, [(N.FILTER_INVERT, 1.0)], (150.0, 100.0, 400.0, 300.0)))
+    compare_frame(renderer, filter_scene(6, [(N.FILTER_GRAYSCALE, 1.0)], (300.0, 300.0, 400.0, 400.0)))
+    compare_frame(renderer, filter_scene(7, [(N.FILTER_OFFSET, (-9.0, 6.0))], (30.0, 30.0, 120.0, 110.0),
+                                         fixed_region=True))
+    compare_frame(renderer, filter_scene(8, [(N.FILTER_HUE_ROTATE, 90.0)], (50.0, 50.0, 50.0, 90.0)))
+    rng = np.random.default_rng(9)
+    c = tk.Canvas(200, 150)
+    c.set_clear_color(0xFF202020)
+    c.push_blur_group(3.0)
+    c.push_filter_layer([(N.FILTER_CONTRAST, 1.8), (N.FILTER_OFFSET, (4.0, 4.0))], (20.0, 20.0, 150.0, 120.0))
+    for _ in range(6):
+        c.push_path(blob(rng, rng.uniform(40, 130), rng.uniform(40, 100), 25), tk.Brush.solid(*rng.uniform(0, 1, 3), 0.9))
+    c.push_filter_layer([(N.FILTER_INVERT, 0.6)], (60.0, 40.0, 140.0, 110.0))
+    c.push_path(blob(rng, 100, 75, 30), tk.Brush.solid(0.9, 0.4, 0.1, 1.0))
+    c.pop_layer()
+    c.pop_layer()
+    c.pop_layer()
+    compare_frame(renderer, c)
+
+
+def test_gpu_offset_filter_past_the_canvas_is_rejected(renderer):
+    """An offset filter layer whose surface reaches past the canvas would pull
+    pixels this path's canvas-sized surfaces do not hold: refused at upload,
+    and the context stays usable."""
+    from layer_cases import filter_scene
+    c = filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (-10.0, 0.0, 50.0, 50.0))
+    with pytest.raises(tk.TileinkError, match="offset filter layer"):
+        renderer.upload(c)
+    compare_frame(renderer, filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (10.0, 10.0, 50.0, 50.0)))

@@ -94,6 +94,13 @@ PROGRESSIVE_DTYPE = np.dtype([("start_x", "<f4"), ("start_y", "<f4"), ("dir_x", 
                               ("max_std_dev", "<f4"), ("quality", "<u4")])
 PROGRESSIVE_BALANCED, PROGRESSIVE_HIGH = 0, 1
 OP_PROGRESSIVE_BEGIN = 3
+OP_FILTER_BEGIN = 4
+FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<i4"), ("dy", "<i4"), ("matrix", "<f4", (20,))])
+CANVAS_FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<f4"), ("dy", "<f4"),
+                                ("matrix", "<f4", (20,))])
+FILTER_LAYER_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4"), ("surface", "<i4", (4,))])
+(FILTER_BRIGHTNESS, FILTER_CONTRAST, FILTER_GRAYSCALE, FILTER_HUE_ROTATE, FILTER_INVERT, FILTER_OPACITY,
+ FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET) = range(1, 11)
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
 GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
 PTCL_GLYPH = 10
@@ -128,6 +135,8 @@ class SceneDesc(C.Structure):
         ("glyph_texels", C.c_void_p), ("glyph_run_count", C.c_uint32), ("glyph_count", C.c_uint32),
         ("glyph_image_count", C.c_uint32), ("glyph_reserved", C.c_uint32), ("glyph_texel_count", C.c_uint64),
         ("progressive_blurs", C.c_void_p), ("progressive_count", C.c_uint32), ("progressive_reserved", C.c_uint32),
+        ("filter_layers", C.c_void_p), ("filters", C.c_void_p), ("filter_layer_count", C.c_uint32),
+        ("filter_count", C.c_uint32),
     ]
 
 
@@ -294,6 +303,7 @@ def library() -> C.CDLL:
         "tk_canvas_push_stroke": (I64, [P, P, C.POINTER(BrushDesc), F64, P, F64]),
         "tk_canvas_push_glyph_outlines": (I64, [P, P, C.POINTER(BrushDesc), P, F64]),
         "tk_canvas_push_progressive_blur_group": (I32, [P, F64, F64, F64, F64, C.c_float, U32]),
+        "tk_canvas_push_filter_layer": (I32, [P, P, U32, P, C.c_int32]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),
@@ -365,6 +375,8 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "glyph_images": arr(d.glyph_images, d.glyph_image_count, GLYPH_IMAGE_DTYPE),
         "glyph_texels": arr(d.glyph_texels, d.glyph_texel_count, np.uint32),
         "progressive": arr(d.progressive_blurs, d.progressive_count, PROGRESSIVE_DTYPE),
+        "filter_layers": arr(d.filter_layers, d.filter_layer_count, FILTER_LAYER_DTYPE),
+        "filters": arr(d.filters, d.filter_count, FILTER_DTYPE),
     }
 
 
@@ -391,7 +403,8 @@ class ArrayScene:
             d.sdf_shadow_blob, d.sdf_shadow_word_count = ptr(shadow), len(shadow)
         for key, cnt in (("glyph_runs", "glyph_run_count"), ("glyphs", "glyph_count"),
                          ("glyph_images", "glyph_image_count"), ("glyph_texels", "glyph_texel_count"),
-                         ("progressive", "progressive_count")):
+                         ("progressive", "progressive_count"), ("filter_layers", "filter_layer_count"),
+                         ("filters", "filter_count")):
             v = a.get(key)
             if v is not None and len(v):
                 setattr(d, "progressive_blurs" if key == "progressive" else key, ptr(v))

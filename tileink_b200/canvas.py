@@ -448,6 +448,29 @@ class Canvas:
         if r != 0:
             raise ValueError("bad progressive blur")
 
+    def push_filter_layer(self, filters, rect, fixed_region: bool = False) -> None:
+        """Canvas::push_filter_layer with a chain of filters over a Region::Rect
+        sample region (src/canvas/layers.rs:222-233): children until
+        pop_layer() are rendered into a surface, filtered in place by each
+        filter in turn and composited over the region's pixel bounds grown by
+        the chain's reach. `filters`: (kind, value) pairs, kind one of
+        N.FILTER_* — a colour filter's amount (hue rotation in degrees), a
+        20-float matrix for FILTER_COLOR_MATRIX, (dx, dy) for FILTER_OFFSET.
+        `rect` = (x0, y0, x1, y1) in logical units."""
+        chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
+        for k, (kind, value) in enumerate(filters):
+            chain[k]["kind"] = kind
+            if kind == N.FILTER_COLOR_MATRIX:
+                chain[k]["matrix"] = np.asarray(value, dtype=np.float32).reshape(20)
+            elif kind == N.FILTER_OFFSET:
+                chain[k]["dx"], chain[k]["dy"] = value
+            else:
+                chain[k]["amount"] = value
+        r = np.asarray(rect, dtype=np.float64).reshape(4)
+        if self._lib.tk_canvas_push_filter_layer(self._h, N.ptr(chain) if len(chain) else None, len(chain),
+                                                 N.ptr(r), 1 if fixed_region else 0) != 0:
+            raise ValueError("bad filter layer")
+
     def push_blur_group(self, sigma: float, factor: int = 1, downsample: int = N.BLUR_DOWNSAMPLE_BOX,
                         upsample: int = N.BLUR_UPSAMPLE_BILINEAR):
         """Canvas::push_blur_group; factor > 1 blurs through a copy reduced

@@ -134,6 +134,8 @@ struct Step {
     uint32_t sampling = 0u;  // BLUR_BEGIN: TK_BLUR_SAMPLING_* word (0: full resolution)
     bool progressive = false;  // BLUR_BEGIN of a progressive blur group
     tk_progressive_blur prog{};
+    std::vector<tk_filter> chain;  // BLUR_BEGIN of a filter layer: its chain (filter is set)
+    bool filter = false;
 };
 
 // State of the last differentiable forward, kept for its backward.
@@ -497,6 +499,39 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             s.progressive = true;
             s.prog = pb;
             c->steps.push_back(s);
+            ++depth;
+        } else if (op.kind == TK_OP_FILTER_BEGIN) {
+            open = false;
+            if (op.layer_end > op.layer_start) invalid("filter layers under clip layers are outside this path");
+            if (op.batch_id >= d.filter_layer_count || !d.filter_layers) invalid("filter layer out of range");
+            const tk_filter_layer& L = d.filter_layers[op.batch_id];
+            if (uint64_t(L.first) + L.count > d.filter_count || (L.count && !d.filters))
+                invalid("filter layer chain outside the filters");
+            // output bounds: the surface clipped to the canvas (filter.rs:510-527)
+            const int32_t ob[4] = {std::max(L.surface[0], 0), std::max(L.surface[1], 0),
+                                   int32_t(std::min<int64_t>(L.surface[2], d.width)),
+                                   int32_t(std::min<int64_t>(L.surface[3], d.height))};
+            Step s{STEP_BLUR_BEGIN, 0u, 0.0f, {ob[0], ob[1], ob[2], ob[3]}, 0u};
+            s.filter = true;
+            bool offsets = false;
+            for (uint32_t k = L.first; k < L.first + L.count; ++k) {
+                const tk_filter& f = d.filters[k];
+                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_OFFSET || !std::isfinite(f.amount))
+                    invalid("filter " + std::to_string(k) + ": bad kind or amount");
+                if (f.kind == TK_FILTER_COLOR_MATRIX)
+                    for (float v : f.matrix)
+                        if (!std::isfinite(v)) invalid("filter " + std::to_string(k) + ": non-finite matrix");
+                if (f.kind == TK_FILTER_OFFSET) offsets = offsets || f.dx != 0 || f.dy != 0;
+                s.chain.push_back(f);
+            }
+            // The reference renders the group into a surface of the layer's
+            // surface bounds, which may reach past the canvas; an offset can
+            // pull such pixels into view, and this path's surfaces are the
+            // canvas, so those layers are refused.
+            if (offsets && (L.surface[0] < 0 || L.surface[1] < 0 || L.surface[2] > int64_t(d.width) ||
+                            L.surface[3] > int64_t(d.height)))
+                invalid("an offset filter layer whose surface reaches past the canvas is outside this path");
+            c->steps.push_back(std::move(s));
             ++depth;
         } else if (op.kind == TK_OP_BLUR_END) {
             open = false;
@@ -1038,7 +1073,12 @@ void do_render(tk_ctx* c) {
             int32_t sx0 = std::max(b.bounds[0] - rad, 0), sy0 = std::max(b.bounds[1] - rad, 0);
             int32_t sx1 = std::min(b.bounds[2] + rad, W), sy1 = std::min(b.bounds[3] + rad, H);
             StageMark m(c, 8);
-            if (b.progressive) {
+            if (b.filter) {
+                // the chain over the layer's bounds (render/filter_program/effects.rs:3-268)
+                if (ob[2] > ob[0] && ob[3] > ob[1])
+                    tk::launch_filter_chain(surf, c->temp.ptr, c->width, ob, b.chain.data(), uint32_t(b.chain.size()),
+                                            st);
+            } else if (b.progressive) {
                 // Filter::ProgressiveBlur over the output bounds
                 // (native/runtime/program/filter/progressive/mod.rs:44-146)
                 if (ob[2] > ob[0] && ob[3] > ob[1] && b.prog.max_std_dev > 0.0f) {

@@ -364,6 +364,7 @@ struct Cmd {
     uint32_t children;
     uint32_t payload = 0u;     // OPACITY: opacity_f32_to_u8 of the layer's opacity; BLUR: sampling
     int32_t progressive = -1;  // BLUR of a progressive blur: its index in the canvas's progressive blurs
+    int32_t filter = -1;       // BLUR of a filter layer: its index in the canvas's filter layers
 };
 
 // One recorded Canvas call with its original geometry, for replay into
@@ -377,8 +378,11 @@ struct GlyphImage {
 
 struct RecCmd {
     enum Kind : uint8_t {
-        FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN, PROGRESSIVE
+        FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN, PROGRESSIVE, FILTER
     } kind = FILL;
+    // FILTER: the chain as recorded (logical units), the region in shape.p0 / p1
+    std::vector<tk_canvas_filter> chain;
+    bool fixed = false;
     // GLYPH_RUN: the glyphs (image = index into run_images or TK_INVALID_INDEX),
     // their images and the optional clip rect
     std::vector<tk_glyph> run_glyphs;
@@ -440,6 +444,8 @@ struct tk_canvas {
     std::vector<tk_glyph_run> glyph_runs;
     std::vector<tk_glyph> glyphs;
     std::vector<tk_progressive_blur> progressive;  // device-pixel progressive blurs
+    std::vector<tk_filter_layer> filter_layers;    // filter layers and their chains' filters
+    std::vector<tk_filter> filters;
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -700,6 +706,20 @@ void compile_into(const tk_canvas* c, uint32_t list, std::vector<tk_layer_record
                 begin.op.kind = TK_OP_PROGRESSIVE_BEGIN;
                 begin.op.batch_id = uint32_t(cmd.progressive);
                 out_r = cmd.sigma > 0.0f ? int32_t(std::ceil(20.0f * cmd.sigma + 8.0f)) : 0;
+            }
+            if (cmd.filter >= 0) {
+                // output bounds: the surface clipped to the canvas
+                // (filter_surface_bounds, shared/layer/filter.rs:510-527)
+                const int32_t* sf = c->filter_layers[size_t(cmd.filter)].surface;
+                begin.op.kind = TK_OP_FILTER_BEGIN;
+                begin.op.batch_id = uint32_t(cmd.filter);
+                begin.op.bounds[0] = std::max(sf[0], 0);
+                begin.op.bounds[1] = std::max(sf[1], 0);
+                begin.op.bounds[2] = std::min(sf[2], int32_t(c->W));
+                begin.op.bounds[3] = std::min(sf[3], int32_t(c->H));
+                if (begin.op.bounds[2] < begin.op.bounds[0] || begin.op.bounds[3] < begin.op.bounds[1])
+                    begin.op.bounds[0] = begin.op.bounds[1] = begin.op.bounds[2] = begin.op.bounds[3] = 0;
+                any = false;
             }
             if (any) {
                 begin.op.bounds[0] = std::max(pb.x0 - out_r, 0);
@@ -1552,6 +1572,74 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
     return 0;
 }
 
+int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double rect[4],
+                                    int32_t fixed_region) {
+    if (!c || (count && !filters) || !rect) return -1;
+    // physical_region (canvas/surface.rs:197-205,370-386), then region_bounds
+    // (shared/layer/filter.rs:578-597): floor / ceil to whole pixels
+    const double s = double(c->scale);
+    double b[4];
+    for (int k = 0; k < 4; ++k) {
+        const double v = rect[k] * s;
+        if (!std::isfinite(v)) return -1;
+        b[k] = (k < 2) ? std::floor(v) : std::ceil(v);
+        b[k] = std::min(std::max(b[k], -2147483648.0), 2147483647.0);
+    }
+    // physical_filter (canvas/surface.rs:247-326): offsets scale with the
+    // canvas; filter_offset_to_pixel_delta (filter.rs:490-494) rounds them to
+    // whole pixels; filter_outset (filter.rs:533-575) sums the chain's reach
+    std::vector<tk_filter> chain(count);
+    uint64_t reach = 0;
+    for (uint32_t k = 0; k < count; ++k) {
+        const tk_canvas_filter& f = filters[k];
+        tk_filter& g = chain[k];
+        g = tk_filter{};
+        g.kind = f.kind;
+        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_OFFSET || !std::isfinite(f.amount)) return -1;
+        g.amount = f.amount;
+        if (f.kind == TK_FILTER_OFFSET) {
+            const float dx = f.dx * c->scale, dy = f.dy * c->scale;
+            if (!std::isfinite(dx) || !std::isfinite(dy) || std::fabs(dx) > 1.0e6f || std::fabs(dy) > 1.0e6f)
+                return -1;
+            g.dx = int32_t(std::ceil(dx - 0.5f));
+            g.dy = int32_t(std::ceil(dy - 0.5f));
+            reach += uint64_t(std::max(std::ceil(std::fabs(dx)), std::ceil(std::fabs(dy))));
+        }
+        if (f.kind == TK_FILTER_COLOR_MATRIX)
+            for (int m = 0; m < 20; ++m) {
+                if (!std::isfinite(f.matrix[m])) return -1;
+                g.matrix[m] = f.matrix[m];
+            }
+    }
+    if (fixed_region) reach = 0;
+    const double r = double(std::min<uint64_t>(reach, 0xFFFFFFFFull));
+    tk_filter_layer L{uint32_t(c->filters.size()), count, {0, 0, 0, 0}};
+    L.surface[0] = int32_t(std::max(b[0] - r, -2147483648.0));
+    L.surface[1] = int32_t(std::max(b[1] - r, -2147483648.0));
+    L.surface[2] = int32_t(std::min(b[2] + r, 2147483647.0));
+    L.surface[3] = int32_t(std::min(b[3] + r, 2147483647.0));
+    c->filters.insert(c->filters.end(), chain.begin(), chain.end());
+    const uint32_t child = uint32_t(c->lists.size());
+    c->lists.emplace_back();
+    Cmd cmd{Cmd::BLUR, 0u, 0.0f, child, 0u};
+    cmd.filter = int32_t(c->filter_layers.size());
+    c->filter_layers.push_back(L);
+    c->lists[c->stack.back()].push_back(cmd);
+    c->stack.push_back(child);
+    c->dirty = true;
+    if (c->keep) {
+        RecCmd rc = rec_cmd(RecCmd::FILTER, nullptr, nullptr, nullptr);
+        rc.chain.assign(filters, filters + count);
+        rc.fixed = fixed_region != 0;
+        rc.shape.p0[0] = rect[0];
+        rc.shape.p0[1] = rect[1];
+        rc.shape.p1[0] = rect[2];
+        rc.shape.p1[1] = rect[3];
+        c->log.push_back(std::move(rc));
+    }
+    return 0;
+}
+
 int32_t tk_canvas_push_blur_group_sampled(tk_canvas* c, float sigma, uint32_t sampling) {
     float physical = sigma * c->scale;
     if (!(sigma >= 0.0f) || !std::isfinite(physical)) return -1;
@@ -1640,6 +1728,10 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->glyph_texel_count = c->glyph_texels.size();
     out->progressive_blurs = c->progressive.data();
     out->progressive_count = uint32_t(c->progressive.size());
+    out->filter_layers = c->filter_layers.data();
+    out->filter_layer_count = uint32_t(c->filter_layers.size());
+    out->filters = c->filters.data();
+    out->filter_count = uint32_t(c->filters.size());
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -2144,6 +2236,18 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
                                                          r.shape.p1[0] + dx, r.shape.p1[1] + dy, r.sigma,
                                                          r.sampling);
         }
+        case RecCmd::FILTER: {
+            // the region moves with a translation (effect_placement.rs:57-75)
+            double rect[4] = {r.shape.p0[0], r.shape.p0[1], r.shape.p1[0], r.shape.p1[1]};
+            if (t) {
+                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+                rect[0] += t[4];
+                rect[1] += t[5];
+                rect[2] += t[4];
+                rect[3] += t[5];
+            }
+            return tk_canvas_push_filter_layer(dst, r.chain.data(), uint32_t(r.chain.size()), rect, r.fixed ? 1 : 0);
+        }
         case RecCmd::POP: return tk_canvas_pop_layer(dst);
         case RecCmd::SDF:
         case RecCmd::SDF_CLIP: {
@@ -2185,7 +2289,7 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
 
 bool has_layers(const std::vector<RecCmd>& log) {
     for (const RecCmd& r : log)
-        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::PROGRESSIVE ||
+        if (r.kind == RecCmd::CLIP || r.kind == RecCmd::BLUR || r.kind == RecCmd::PROGRESSIVE || r.kind == RecCmd::FILTER ||
             r.kind == RecCmd::SDF_CLIP ||
             r.kind == RecCmd::OPACITY)
             return true;

@@ -1,0 +1,200 @@
+// Filter layers (Canvas::push_filter_layer with Filter::Chain): the group's
+// RGBA8 surface filtered in place, one chain filter after another, over the
+// layer's processing bounds (render/filter_program/effects.rs:3-268).
+//
+// * Colour filters and the colour matrix: one thread per pixel, the
+//   reference's filter_color_pixel / filter_color_matrix_pixel
+//   (filter/color.hlsli:8-76) on the stored RGBA8 word. `mad` is an explicit
+//   fused multiply-add; every other product and sum is rounded on its own.
+//   Hue rotation takes cos / sin from the exactly rounded evaluation shared
+//   with the SDF kinds (sdf.cuh), which the oracle restates.
+// * Offset: out(x, y) = in(x - dx, y - dy) inside the bounds, transparent
+//   where the source falls outside them (filter_offset_region,
+//   filter/basic.hlsl:49-56), into the scratch surface and copied back.
+// All kernels are HBM-bound: 8 bytes per pixel (read and write the word).
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "kernels.h"
+#include "sdf.cuh"
+
+namespace tk {
+namespace {
+
+using namespace tkd;
+
+struct FilterArgs {
+    uint32_t kind;
+    float amount;
+    float m[20];
+};
+
+// svg_luminance (filter/color.hlsli:7)
+__device__ __forceinline__ float svg_luminance(float r, float g, float b) {
+    return (0.2126f * r + 0.7152f * g) + 0.0722f * b;
+}
+
+// filter_color_pixel (filter/color.hlsli:9-45)
+__device__ uint32_t color_filter_pixel(uint32_t pixel, uint32_t kind, float amount) {
+    if ((kind == TK_FILTER_INVERT || kind == TK_FILTER_SEPIA) && (pixel >> 24) != 0u) {
+        // byte channels, no normalize / unpremultiply round trip
+        const float cr = float(pixel & 255u), cg = float((pixel >> 8) & 255u), cb = float((pixel >> 16) & 255u);
+        const float alpha = float(pixel >> 24);
+        float mr = alpha - cr, mg = alpha - cg, mb = alpha - cb;
+        if (kind == TK_FILTER_SEPIA) {
+            mr = mad(0.393f, cr, mad(0.769f, cg, 0.189f * cb));
+            mg = mad(0.349f, cr, mad(0.686f, cg, 0.168f * cb));
+            mb = mad(0.272f, cr, mad(0.534f, cg, 0.131f * cb));
+        }
+        const float t = clampf(amount, 0.0f, 1.0f);
+        const uint32_t r = f2u(clampf(mad(mr - cr, t, cr), 0.0f, alpha) + 0.5f);
+        const uint32_t g = f2u(clampf(mad(mg - cg, t, cg), 0.0f, alpha) + 0.5f);
+        const uint32_t b = f2u(clampf(mad(mb - cb, t, cb), 0.0f, alpha) + 0.5f);
+        return pack4(r, g, b, pixel >> 24);
+    }
+    float4 c = rgba8_to_unorm(pixel);
+    if (kind == TK_FILTER_OPACITY) {
+        const float a = clampf(amount, 0.0f, 1.0f);
+        c = make_float4(c.x * a, c.y * a, c.z * a, c.w * a);
+    } else if (c.w > 0.0f) {
+        float r = c.x / c.w, g = c.y / c.w, b = c.z / c.w;
+        if (kind == TK_FILTER_BRIGHTNESS) {
+            r = r * amount;
+            g = g * amount;
+            b = b * amount;
+        } else if (kind == TK_FILTER_CONTRAST) {
+            r = (r - 0.5f) * amount + 0.5f;
+            g = (g - 0.5f) * amount + 0.5f;
+            b = (b - 0.5f) * amount + 0.5f;
+        } else if (kind == TK_FILTER_GRAYSCALE) {
+            // filter_lerp(straight, luminance, t) = mad(b - a, t, a)
+            const float l = svg_luminance(r, g, b), t = clampf(amount, 0.0f, 1.0f);
+            r = mad(l - r, t, r);
+            g = mad(l - g, t, g);
+            b = mad(l - b, t, b);
+        } else if (kind == TK_FILTER_HUE_ROTATE) {
+            const float angle = amount * 0.017453292f;
+            float si, co;
+            sdf_sincos(angle, si, co);
+            const float nr = ((0.213f + co * 0.787f) - si * 0.213f) * r + ((0.715f - co * 0.715f) - si * 0.715f) * g +
+                             ((0.072f - co * 0.072f) + si * 0.928f) * b;
+            const float ng = ((0.213f - co * 0.213f) + si * 0.143f) * r + ((0.715f + co * 0.285f) + si * 0.140f) * g +
+                             ((0.072f - co * 0.072f) - si * 0.283f) * b;
+            const float nb = ((0.213f - co * 0.213f) - si * 0.787f) * r + ((0.715f - co * 0.715f) + si * 0.715f) * g +
+                             ((0.072f + co * 0.928f) + si * 0.072f) * b;
+            r = nr;
+            g = ng;
+            b = nb;
+        } else if (kind == TK_FILTER_SATURATE) {
+            const float l = svg_luminance(r, g, b);
+            r = l + (r - l) * amount;
+            g = l + (g - l) * amount;
+            b = l + (b - l) * amount;
+        }
+        c = make_float4(clampf(r, 0.0f, 1.0f) * c.w, clampf(g, 0.0f, 1.0f) * c.w, clampf(b, 0.0f, 1.0f) * c.w, c.w);
+    }
+    // pack_premul_rgba8 (shared/pixel.hlsli:51-54)
+    return pack4(f2u(clampf(c.x, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c.y, 0.0f, 1.0f) * 255.0f + 0.5f),
+                 f2u(clampf(c.z, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c.w, 0.0f, 1.0f) * 255.0f + 0.5f));
+}
+
+// filter_dot4 (filter/color.hlsli:47)
+__device__ __forceinline__ float dot4(const float* a, float x, float y, float z, float w) {
+    return mad(a[0], x, mad(a[1], y, mad(a[2], z, a[3] * w)));
+}
+
+// filter_color_matrix_pixel (filter/color.hlsli:49-76); m is the 4 x 5
+// row-major matrix (rows r g b a, columns r g b a bias).
+__device__ uint32_t color_matrix_pixel(const float* m, uint32_t pixel) {
+    const float alpha = float(pixel >> 24);
+    const float cr = float(pixel & 255u), cg = float((pixel >> 8) & 255u), cb = float((pixel >> 16) & 255u);
+    float sr = 0.0f, sg = 0.0f, sb = 0.0f;
+    if ((pixel >> 24) == 255u) {
+        sr = cr;
+        sg = cg;
+        sb = cb;
+    } else if (alpha > 0.0f) {
+        const float k = 255.0f / alpha;
+        sr = cr * k;
+        sg = cg * k;
+        sb = cb * k;
+    }
+    const float out_a = floorf(clampf(dot4(m + 15, sr, sg, sb, alpha) + m[19] * 255.0f, 0.0f, 255.0f) + 0.5f);
+    float rr, rg, rb;
+    if (alpha > 0.0f) {
+        const float sw = alpha * alpha * CHANNEL_SCALE;
+        const float mr = mad(m[4], alpha, dot4(m + 0, cr, cg, cb, sw));
+        const float mg = mad(m[9], alpha, dot4(m + 5, cr, cg, cb, sw));
+        const float mb = mad(m[14], alpha, dot4(m + 10, cr, cg, cb, sw));
+        const float scale = out_a == alpha ? 1.0f : out_a / alpha;
+        rr = mr >= alpha ? out_a : clampf(mr, 0.0f, alpha) * scale;
+        rg = mg >= alpha ? out_a : clampf(mg, 0.0f, alpha) * scale;
+        rb = mb >= alpha ? out_a : clampf(mb, 0.0f, alpha) * scale;
+    } else {
+        rr = clampf(m[4], 0.0f, 1.0f) * out_a;
+        rg = clampf(m[9], 0.0f, 1.0f) * out_a;
+        rb = clampf(m[14], 0.0f, 1.0f) * out_a;
+    }
+    return pack4(f2u(clampf(rr, 0.0f, 255.0f) + 0.5f), f2u(clampf(rg, 0.0f, 255.0f) + 0.5f),
+                 f2u(clampf(rb, 0.0f, 255.0f) + 0.5f), f2u(clampf(out_a, 0.0f, 255.0f) + 0.5f));
+}
+
+__global__ void k_filter_color(uint32_t* surface, uint32_t width, int4 b, FilterArgs f) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t o = uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w);
+        const uint32_t p = surface[o];
+        surface[o] = f.kind == TK_FILTER_COLOR_MATRIX ? color_matrix_pixel(f.m, p) : color_filter_pixel(p, f.kind, f.amount);
+    }
+}
+
+__global__ void k_filter_offset(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t width, int4 b,
+                                int32_t dx, int32_t dy) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const int64_t x = b.x + int64_t(i % w), y = b.y + int64_t(i / w);
+        const int64_t sx = x - dx, sy = y - dy;
+        uint32_t p = 0u;
+        if (sx >= b.x && sy >= b.y && sx < b.z && sy < b.w) p = src[uint64_t(sy) * width + uint64_t(sx)];
+        dst[uint64_t(y) * width + uint64_t(x)] = p;
+    }
+}
+
+__global__ void k_filter_copy(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t width, int4 b) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t o = uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w);
+        dst[o] = src[o];
+    }
+}
+
+unsigned filter_grid(uint64_t n) {
+    const uint64_t g = (n + 255) / 256;
+    return unsigned(g < 148ull * 32 ? (g ? g : 1) : 148ull * 32);
+}
+
+}  // namespace
+
+void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t width, const int32_t bounds[4],
+                         const tk_filter* chain, uint32_t count, cudaStream_t st) {
+    const int4 b = make_int4(bounds[0], bounds[1], bounds[2], bounds[3]);
+    if (b.z <= b.x || b.w <= b.y) return;
+    const uint64_t n = uint64_t(b.z - b.x) * uint64_t(b.w - b.y);
+    for (uint32_t k = 0; k < count; ++k) {
+        const tk_filter& f = chain[k];
+        if (f.kind == TK_FILTER_OFFSET) {
+            if (f.dx == 0 && f.dy == 0) continue;
+            k_filter_offset<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
+            k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+        } else {
+            FilterArgs a{f.kind, f.amount, {}};
+            for (int m = 0; m < 20; ++m) a.m[m] = f.matrix[m];
+            k_filter_color<<<filter_grid(n), 256, 0, st>>>(surface, width, b, a);
+        }
+    }
+}
+
+}  // namespace tk
