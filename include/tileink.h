@@ -349,10 +349,14 @@ typedef struct tk_progressive_blur {
 #define TK_FILTER_SEPIA 8u
 #define TK_FILTER_COLOR_MATRIX 9u /* Filter::ColorMatrix: 4 rows of 5 (r g b a bias), filter/color.hlsli:47-76 */
 #define TK_FILTER_OFFSET 10u      /* Filter::Offset: dx, dy already whole pixels (ceil(d - 0.5)) */
+/* Filter::Morphology (filter/morphology.hlsli): dx, dy are the whole-pixel
+ * radii ceil(max(radius, 0)) along x and y */
+#define TK_FILTER_ERODE 11u
+#define TK_FILTER_DILATE 12u
 typedef struct tk_filter {
     uint32_t kind;
     float amount;      /* the colour filters' argument (hue rotation in degrees) */
-    int32_t dx, dy;    /* TK_FILTER_OFFSET */
+    int32_t dx, dy;    /* TK_FILTER_OFFSET: the offset; TK_FILTER_ERODE / DILATE: the radii */
     float matrix[20];  /* TK_FILTER_COLOR_MATRIX, row-major */
 } tk_filter; /* 96 B */
 /* One filter layer: its chain filters[first, first + count), and the surface

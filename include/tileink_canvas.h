@@ -191,8 +191,9 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
                                               double end_y, float max_std_dev, uint32_t quality);
 /* One filter of a filter layer's chain, in logical units: a colour filter
  * (TK_FILTER_BRIGHTNESS .. TK_FILTER_SEPIA with its amount; hue rotation in
- * degrees), TK_FILTER_COLOR_MATRIX (matrix: 4 rows of r g b a bias) or
- * TK_FILTER_OFFSET (dx, dy). */
+ * degrees), TK_FILTER_COLOR_MATRIX (matrix: 4 rows of r g b a bias),
+ * TK_FILTER_OFFSET (dx, dy) or TK_FILTER_ERODE / TK_FILTER_DILATE (dx, dy:
+ * the radii along x and y). */
 typedef struct tk_canvas_filter {
     uint32_t kind;
     float amount;

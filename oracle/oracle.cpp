@@ -2043,11 +2043,58 @@ uint32_t filter_color_matrix_pixel(const float* m, uint32_t pixel) {
                 f2u(clampf(rb, 0.0f, 255.0f) + 0.5f), f2u(clampf(out_a, 0.0f, 255.0f) + 0.5f));
 }
 
+// filter_morphology_pixel (filter/morphology.hlsli:8-27) over bounds b,
+// whose lines are the surface's, along x (horizontal) or y.
+void morphology_pass(const uint32_t* src, uint32_t* dst, uint32_t width, const int32_t b[4], uint32_t radius,
+                     bool dilate, bool horizontal) {
+    const uint32_t w = uint32_t(b[2] - b[0]), h = uint32_t(b[3] - b[1]), len = horizontal ? w : h;
+    for (uint32_t ly = 0; ly < h; ++ly)
+        for (uint32_t lx = 0; lx < w; ++lx) {
+            const size_t o = size_t(uint32_t(b[1]) + ly) * width + uint32_t(b[0]) + lx;
+            const uint32_t pos = horizontal ? lx : ly;
+            if (!dilate && (pos < radius || pos + radius >= len)) {
+                dst[o] = 0u;
+                continue;
+            }
+            float v[4];
+            for (float& x : v) x = dilate ? 0.0f : 1.0f;
+            const uint32_t start = pos > radius ? pos - radius : 0u, end = std::min(len - 1u, pos + radius);
+            for (uint32_t sp = start; sp <= end; ++sp) {
+                const size_t so = horizontal ? size_t(uint32_t(b[1]) + ly) * width + uint32_t(b[0]) + sp
+                                             : size_t(uint32_t(b[1]) + sp) * width + uint32_t(b[0]) + lx;
+                const uint32_t p = src[so], al = p >> 24;
+                const float s[4] = {al == 0u ? 0.0f : float(p & 255u) / float(al),
+                                    al == 0u ? 0.0f : float((p >> 8) & 255u) / float(al),
+                                    al == 0u ? 0.0f : float((p >> 16) & 255u) / float(al), float(al) / 255.0f};
+                for (int c = 0; c < 4; ++c) v[c] = dilate ? fmax_(v[c], s[c]) : fmin_(v[c], s[c]);
+            }
+            dst[o] = pack(f2u(clampf(v[0] * v[3], 0.0f, 1.0f) * 255.0f + 0.5f),
+                          f2u(clampf(v[1] * v[3], 0.0f, 1.0f) * 255.0f + 0.5f),
+                          f2u(clampf(v[2] * v[3], 0.0f, 1.0f) * 255.0f + 0.5f),
+                          f2u(clampf(v[3], 0.0f, 1.0f) * 255.0f + 0.5f));
+        }
+}
+
 void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const tk_filter* chain, uint32_t count) {
     if (b[2] <= b[0] || b[3] <= b[1]) return;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_filter& f = chain[k];
-        if (f.kind == TK_FILTER_OFFSET) {
+        if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
+            // effects.rs:169-221: nothing for zero radii; an erosion whose
+            // doubled radius reaches the surface size clears it; else x, then y
+            if (f.dx == 0 && f.dy == 0) continue;
+            const uint32_t sw = uint32_t(b[2] - b[0]), sh = uint32_t(b[3] - b[1]);
+            const uint32_t rx = uint32_t(f.dx), ry = uint32_t(f.dy);
+            const bool dilate = f.kind == TK_FILTER_DILATE;
+            if (!dilate && (uint64_t(rx) * 2 >= sw || uint64_t(ry) * 2 >= sh)) {
+                for (int32_t y = b[1]; y < b[3]; ++y)
+                    for (int32_t x = b[0]; x < b[2]; ++x) surface[size_t(y) * width + x] = 0u;
+                continue;
+            }
+            std::vector<uint32_t> temp(size_t(width) * size_t(b[3]), 0u);
+            morphology_pass(surface, temp.data(), width, b, std::min(rx, sw - 1u), dilate, true);
+            morphology_pass(temp.data(), surface, width, b, std::min(ry, sh - 1u), dilate, false);
+        } else if (f.kind == TK_FILTER_OFFSET) {
             if (f.dx == 0 && f.dy == 0) continue;
             std::vector<uint32_t> temp(size_t(b[2] - b[0]) * size_t(b[3] - b[1]));
             for (int32_t y = b[1]; y < b[3]; ++y)

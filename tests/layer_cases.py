@@ -163,4 +163,8 @@ def filter_chains():
         "offset": [(N.FILTER_OFFSET, (7.5, -4.2))],
         "chain": [(N.FILTER_GRAYSCALE, 0.5), (N.FILTER_OFFSET, (-3.0, 5.6)), (N.FILTER_HUE_ROTATE, -60.0),
                   (N.FILTER_CONTRAST, 1.4), (N.FILTER_OPACITY, 0.8)],
+        "erode": [(N.FILTER_ERODE, (2.5, 1.0))],
+        "dilate": [(N.FILTER_DILATE, (3.0, 4.2))],
+        "morphology_chain": [(N.FILTER_DILATE, (2.0, 0.0)), (N.FILTER_SEPIA, 0.6), (N.FILTER_ERODE, (0.0, 1.5)),
+                             (N.FILTER_OFFSET, (2.0, 2.0))],
     }

@@ -184,6 +184,12 @@ def test_canvas_records_filter_layers():
     a2 = c2.scene_arrays()
     L2 = a2["filter_layers"][0]
     assert list(L2["surface"]) == [2, 4, 20, 24] and a2["filters"][0]["dx"] == 3  # ceil(2.6 - 0.5)
+    c3 = tk.Canvas(128, 96)
+    c3.push_filter_layer([(N.FILTER_DILATE, (3.0, 4.2)), (N.FILTER_ERODE, (6.0, 6.0))], (20.0, 20.0, 60.0, 50.0))
+    c3.pop_layer()
+    a3 = c3.scene_arrays()
+    assert list(a3["filter_layers"][0]["surface"]) == [15, 15, 65, 55]  # a dilation reaches ceil(4.2); erosion 0
+    assert [tuple(f) for f in a3["filters"][["dx", "dy"]]] == [(3, 5), (6, 6)]
     with pytest.raises(ValueError):
         c.push_filter_layer([(99, 1.0)], (0, 0, 10, 10))
     with pytest.raises(ValueError):
@@ -204,3 +210,72 @@ def test_filter_scenes_render_in_the_oracle(name):
     c = filter_scene(7, filter_chains()[name], (15.5, 12.0, 170.2, 131.9))
     img = oracle.OracleRun(c.scene_desc(), threads=4).get(oracle.OR_IMAGE, np.uint32)
     assert img.any()
+
+
+def oracle_surface_chain(surf, w, rect, chain):
+    """The oracle's chain over a w-wide surface (a copy), in place over rect."""
+    out = np.ascontiguousarray(surf, dtype=np.uint32).copy()
+    filters = np.zeros(len(chain), dtype=N.FILTER_DTYPE)
+    for k, (kind, value) in enumerate(chain):
+        filters[k]["kind"] = kind
+        filters[k]["dx"], filters[k]["dy"] = value
+    r = np.array(rect, dtype=np.int32)
+    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(r), N.ptr(filters), len(filters))
+    return out
+
+
+def np_morphology(img, rect, rx, ry, dilate):
+    """filter_morphology_pixel along x then y, restated with numpy float32."""
+    x0, y0, x1, y1 = rect
+    sub = img[y0:y1, x0:x1]
+    h, w = sub.shape
+
+    def axis(src, radius, horizontal):
+        out = np.zeros_like(src)
+        n = w if horizontal else h
+        for y in range(h):
+            for x in range(w):
+                pos = x if horizontal else y
+                if not dilate and (pos < radius or pos + radius >= n):
+                    continue
+                acc = np.full(4, F(0.0) if dilate else F(1.0), dtype=np.float32)
+                for sp in range(max(pos - radius, 0), min(n - 1, pos + radius) + 1):
+                    p = int(src[y, sp] if horizontal else src[sp, x])
+                    al = p >> 24
+                    v = np.array([F(0) if al == 0 else F(p >> s & 255) / F(al) for s in (0, 8, 16)] + [F(al) / F(255)],
+                                 dtype=np.float32)
+                    acc = np.maximum(acc, v) if dilate else np.minimum(acc, v)
+                ch = [acc[0] * acc[3], acc[1] * acc[3], acc[2] * acc[3], acc[3]]
+                q = [int(F(min(max(c, F(0)), F(1))) * F(255) + F(0.5)) for c in ch]
+                out[y, x] = q[0] | q[1] << 8 | q[2] << 16 | q[3] << 24
+        return out
+
+    res = img.copy()
+    res[y0:y1, x0:x1] = axis(axis(sub, min(rx, w - 1), True), min(ry, h - 1), False)
+    return res
+
+
+@pytest.mark.parametrize("kind, rx, ry", [(N.FILTER_DILATE, 2, 1), (N.FILTER_ERODE, 1, 2), (N.FILTER_DILATE, 0, 3),
+                                          (N.FILTER_ERODE, 3, 0)])
+def test_morphology_matches_numpy_restatement(kind, rx, ry):
+    w, h = 21, 15
+    img = premul_pixels(w * h, 100 + kind + 10 * rx + ry).reshape(h, w)
+    rect = (3, 2, 19, 14)
+    got = oracle_surface_chain(img.reshape(-1), w, rect, [(kind, (rx, ry))]).reshape(h, w)
+    assert np.array_equal(got, np_morphology(img, rect, rx, ry, kind == N.FILTER_DILATE))
+
+
+def test_morphology_known_answers():
+    w, h = 16, 12
+    img = np.zeros((h, w), dtype=np.uint32)
+    img[5, 7] = 0xFF204080
+    d = oracle_surface_chain(img.reshape(-1), w, (0, 0, w, h), [(N.FILTER_DILATE, (2, 1))]).reshape(h, w)
+    want = np.zeros_like(img)
+    want[4:7, 5:10] = 0xFF204080  # the opaque pixel grows to a 5 x 3 block
+    assert np.array_equal(d, want)
+    e = oracle_surface_chain(want.reshape(-1), w, (0, 0, w, h), [(N.FILTER_ERODE, (2, 1))]).reshape(h, w)
+    assert np.array_equal(e, img)  # and erodes back to the pixel
+    # an erosion whose doubled radius reaches the surface clears it
+    full = np.full((h, w), 0xFF00FF00, dtype=np.uint32)
+    assert not oracle_surface_chain(full.reshape(-1), w, (0, 0, w, h), [(N.FILTER_ERODE, (8, 1))]).any()
+

@@ -117,7 +117,8 @@ def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uni
 
 
 @pytest.mark.parametrize("name", ["brightness", "contrast", "grayscale", "hue_rotate", "invert", "opacity",
-                                  "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain"])
+                                  "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain", "erode",
+                                  "dilate", "morphology_chain"])
 def test_gpu_filter_layers_match_oracle(renderer, name):
     """Filter layers (Canvas::push_filter_layer with a chain; filter/color.hlsli,
     filter/basic.hlsl): every colour filter, the colour matrix, offsets and a
@@ -153,11 +154,14 @@ def test_gpu_filter_layer_regions(renderer):
 
 
 def test_gpu_offset_filter_past_the_canvas_is_rejected(renderer):
-    """An offset filter layer whose surface reaches past the canvas would pull
-    pixels this path's canvas-sized surfaces do not hold: refused at upload,
-    and the context stays usable."""
+    """An offset or morphology filter layer whose surface reaches past the
+    canvas would read pixels this path's canvas-sized surfaces do not hold:
+    refused at upload, and the context stays usable."""
     from layer_cases import filter_scene
     c = filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (-10.0, 0.0, 50.0, 50.0))
-    with pytest.raises(tk.TileinkError, match="offset filter layer"):
+    with pytest.raises(tk.TileinkError, match="offset or morphology filter layer"):
+        renderer.upload(c)
+    c = filter_scene(2, [(N.FILTER_DILATE, (3.0, 3.0))], (10.0, 10.0, 198.0, 100.0))
+    with pytest.raises(tk.TileinkError, match="offset or morphology filter layer"):
         renderer.upload(c)
     compare_frame(renderer, filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (10.0, 10.0, 50.0, 50.0)))

@@ -455,14 +455,15 @@ class Canvas:
         filter in turn and composited over the region's pixel bounds grown by
         the chain's reach. `filters`: (kind, value) pairs, kind one of
         N.FILTER_* — a colour filter's amount (hue rotation in degrees), a
-        20-float matrix for FILTER_COLOR_MATRIX, (dx, dy) for FILTER_OFFSET.
+        20-float matrix for FILTER_COLOR_MATRIX, (dx, dy) for FILTER_OFFSET,
+        (radius_x, radius_y) for FILTER_ERODE / FILTER_DILATE.
         `rect` = (x0, y0, x1, y1) in logical units."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
         for k, (kind, value) in enumerate(filters):
             chain[k]["kind"] = kind
             if kind == N.FILTER_COLOR_MATRIX:
                 chain[k]["matrix"] = np.asarray(value, dtype=np.float32).reshape(20)
-            elif kind == N.FILTER_OFFSET:
+            elif kind in (N.FILTER_OFFSET, N.FILTER_ERODE, N.FILTER_DILATE):
                 chain[k]["dx"], chain[k]["dy"] = value
             else:
                 chain[k]["amount"] = value

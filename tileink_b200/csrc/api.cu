@@ -513,24 +513,28 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                                    int32_t(std::min<int64_t>(L.surface[3], d.height))};
             Step s{STEP_BLUR_BEGIN, 0u, 0.0f, {ob[0], ob[1], ob[2], ob[3]}, 0u};
             s.filter = true;
-            bool offsets = false;
+            bool spatial = false;
             for (uint32_t k = L.first; k < L.first + L.count; ++k) {
                 const tk_filter& f = d.filters[k];
-                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_OFFSET || !std::isfinite(f.amount))
+                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DILATE || !std::isfinite(f.amount))
                     invalid("filter " + std::to_string(k) + ": bad kind or amount");
                 if (f.kind == TK_FILTER_COLOR_MATRIX)
                     for (float v : f.matrix)
                         if (!std::isfinite(v)) invalid("filter " + std::to_string(k) + ": non-finite matrix");
-                if (f.kind == TK_FILTER_OFFSET) offsets = offsets || f.dx != 0 || f.dy != 0;
+                const bool morph = f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE;
+                if (morph && (f.dx < 0 || f.dy < 0 || f.dx > 1000000 || f.dy > 1000000))
+                    invalid("filter " + std::to_string(k) + ": morphology radii outside [0, 1e6]");
+                if ((f.kind == TK_FILTER_OFFSET || morph) && (f.dx != 0 || f.dy != 0)) spatial = true;
                 s.chain.push_back(f);
             }
             // The reference renders the group into a surface of the layer's
-            // surface bounds, which may reach past the canvas; an offset can
-            // pull such pixels into view, and this path's surfaces are the
+            // surface bounds, which may reach past the canvas; an offset or a
+            // morphology reads such pixels, and this path's surfaces are the
             // canvas, so those layers are refused.
-            if (offsets && (L.surface[0] < 0 || L.surface[1] < 0 || L.surface[2] > int64_t(d.width) ||
+            if (spatial && (L.surface[0] < 0 || L.surface[1] < 0 || L.surface[2] > int64_t(d.width) ||
                             L.surface[3] > int64_t(d.height)))
-                invalid("an offset filter layer whose surface reaches past the canvas is outside this path");
+                invalid("an offset or morphology filter layer whose surface reaches past the canvas is outside this "
+                        "path");
             c->steps.push_back(std::move(s));
             ++depth;
         } else if (op.kind == TK_OP_BLUR_END) {

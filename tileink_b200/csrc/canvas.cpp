@@ -1595,7 +1595,7 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
         tk_filter& g = chain[k];
         g = tk_filter{};
         g.kind = f.kind;
-        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_OFFSET || !std::isfinite(f.amount)) return -1;
+        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DILATE || !std::isfinite(f.amount)) return -1;
         g.amount = f.amount;
         if (f.kind == TK_FILTER_OFFSET) {
             const float dx = f.dx * c->scale, dy = f.dy * c->scale;
@@ -1604,6 +1604,15 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
             g.dx = int32_t(std::ceil(dx - 0.5f));
             g.dy = int32_t(std::ceil(dy - 0.5f));
             reach += uint64_t(std::max(std::ceil(std::fabs(dx)), std::ceil(std::fabs(dy))));
+        }
+        if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
+            // the radii scale with the canvas and round up to whole pixels
+            // (effects.rs:169-221); a dilation reaches max(rx, ry) further
+            const float rx = f.dx * c->scale, ry = f.dy * c->scale;
+            if (!std::isfinite(rx) || !std::isfinite(ry) || rx > 1.0e6f || ry > 1.0e6f) return -1;
+            g.dx = int32_t(std::ceil(std::max(rx, 0.0f)));
+            g.dy = int32_t(std::ceil(std::max(ry, 0.0f)));
+            if (f.kind == TK_FILTER_DILATE) reach += uint64_t(std::ceil(std::max(std::max(rx, ry), 0.0f)));
         }
         if (f.kind == TK_FILTER_COLOR_MATRIX)
             for (int m = 0; m < 20; ++m) {

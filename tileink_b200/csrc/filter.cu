@@ -11,7 +11,14 @@
 // * Offset: out(x, y) = in(x - dx, y - dy) inside the bounds, transparent
 //   where the source falls outside them (filter_offset_region,
 //   filter/basic.hlsl:49-56), into the scratch surface and copied back.
-// All kernels are HBM-bound: 8 bytes per pixel (read and write the word).
+// * Erode / dilate: per axis, the componentwise min / max of the
+//   unpremultiplied texels within the radius along the surface line
+//   (filter_morphology_pixel, filter/morphology.hlsli:8-27), x into the
+//   scratch surface, then y back; an erosion clears texels within the radius
+//   of the line's ends, and one whose doubled radius reaches the surface
+//   size clears the bounds (render/filter_program/effects.rs:169-221).
+// The per-pixel kernels are HBM-bound: 8 bytes per pixel (read and write the
+// word); a morphology pass reads 2r + 1 texels per pixel, mostly from L1.
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -171,6 +178,56 @@ __global__ void k_filter_copy(const uint32_t* __restrict__ src, uint32_t* __rest
     }
 }
 
+// One morphology pass along x (horizontal) or y over bounds b, whose lines
+// are the surface's (the bounds are the whole surface here).
+__global__ void k_filter_morphology(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t width,
+                                    int4 b, uint32_t radius, bool dilate, bool horizontal) {
+    const uint32_t w = uint32_t(b.z - b.x), h = uint32_t(b.w - b.y);
+    const uint64_t n = uint64_t(w) * h;
+    const uint32_t len = horizontal ? w : h;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t lx = uint32_t(i % w), ly = uint32_t(i / w);
+        const uint64_t o = uint64_t(uint32_t(b.y) + ly) * width + uint32_t(b.x) + lx;
+        const uint32_t pos = horizontal ? lx : ly;
+        if (!dilate && (pos < radius || pos + radius >= len)) {
+            dst[o] = 0u;
+            continue;
+        }
+        float r = dilate ? 0.0f : 1.0f, g = r, bl = r, a = r;
+        const uint32_t start = pos > radius ? pos - radius : 0u, end = min(len - 1u, pos + radius);
+        for (uint32_t sp = start; sp <= end; ++sp) {
+            const uint64_t so = horizontal ? uint64_t(uint32_t(b.y) + ly) * width + uint32_t(b.x) + sp
+                                           : uint64_t(uint32_t(b.y) + sp) * width + uint32_t(b.x) + lx;
+            const uint32_t p = __ldg(src + so), al = p >> 24;
+            // straight_channel (shared/pixel.hlsli:24) and alpha / 255
+            const float vr = al == 0u ? 0.0f : float(p & 255u) / float(al);
+            const float vg = al == 0u ? 0.0f : float((p >> 8) & 255u) / float(al);
+            const float vb = al == 0u ? 0.0f : float((p >> 16) & 255u) / float(al);
+            const float va = float(al) / 255.0f;
+            if (dilate) {
+                r = fmaxf(r, vr);
+                g = fmaxf(g, vg);
+                bl = fmaxf(bl, vb);
+                a = fmaxf(a, va);
+            } else {
+                r = fminf(r, vr);
+                g = fminf(g, vg);
+                bl = fminf(bl, vb);
+                a = fminf(a, va);
+            }
+        }
+        dst[o] = pack4(f2u(clampf(r * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(g * a, 0.0f, 1.0f) * 255.0f + 0.5f),
+                       f2u(clampf(bl * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
+    }
+}
+
+__global__ void k_filter_clear(uint32_t* dst, uint32_t width, int4 b) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        dst[uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w)] = 0u;
+}
+
 unsigned filter_grid(uint64_t n) {
     const uint64_t g = (n + 255) / 256;
     return unsigned(g < 148ull * 32 ? (g ? g : 1) : 148ull * 32);
@@ -189,6 +246,19 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t width, cons
             if (f.dx == 0 && f.dy == 0) continue;
             k_filter_offset<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
             k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+        } else if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
+            if (f.dx == 0 && f.dy == 0) continue;
+            const uint32_t sw = uint32_t(b.z - b.x), sh = uint32_t(b.w - b.y);
+            const uint32_t rx = uint32_t(f.dx), ry = uint32_t(f.dy);
+            const bool dilate = f.kind == TK_FILTER_DILATE;
+            if (!dilate && (uint64_t(rx) * 2 >= sw || uint64_t(ry) * 2 >= sh)) {
+                k_filter_clear<<<filter_grid(n), 256, 0, st>>>(surface, width, b);
+                continue;
+            }
+            k_filter_morphology<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, min(rx, sw - 1u), dilate,
+                                                                 true);
+            k_filter_morphology<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b, min(ry, sh - 1u), dilate,
+                                                                 false);
         } else {
             FilterArgs a{f.kind, f.amount, {}};
             for (int m = 0; m < 20; ++m) a.m[m] = f.matrix[m];
