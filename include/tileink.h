@@ -353,12 +353,20 @@ typedef struct tk_progressive_blur {
  * radii ceil(max(radius, 0)) along x and y */
 #define TK_FILTER_ERODE 11u
 #define TK_FILTER_DILATE 12u
+/* Filter::Flood and Filter::DropShadow with a solid brush (filter/brush.hlsl,
+ * render/filter_program/shadow.rs): color is the premultiplied RGBA8 colour;
+ * a drop shadow's dx, dy are its offset rounded to whole pixels and std_dev
+ * its Gaussian standard deviation. */
+#define TK_FILTER_FLOOD 13u
+#define TK_FILTER_DROP_SHADOW 14u
 typedef struct tk_filter {
     uint32_t kind;
     float amount;      /* the colour filters' argument (hue rotation in degrees) */
-    int32_t dx, dy;    /* TK_FILTER_OFFSET: the offset; TK_FILTER_ERODE / DILATE: the radii */
+    int32_t dx, dy;    /* OFFSET, DROP_SHADOW: the offset; ERODE / DILATE: the radii */
+    uint32_t color;    /* FLOOD, DROP_SHADOW */
+    float std_dev;     /* DROP_SHADOW */
     float matrix[20];  /* TK_FILTER_COLOR_MATRIX, row-major */
-} tk_filter; /* 96 B */
+} tk_filter; /* 104 B */
 /* One filter layer: its chain filters[first, first + count), and the surface
  * bounds the chain reads (the sample region's pixel bounds grown by the
  * chain's reach, filter.rs:510-575; may extend past the canvas). */

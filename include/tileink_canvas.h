@@ -192,12 +192,15 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
 /* One filter of a filter layer's chain, in logical units: a colour filter
  * (TK_FILTER_BRIGHTNESS .. TK_FILTER_SEPIA with its amount; hue rotation in
  * degrees), TK_FILTER_COLOR_MATRIX (matrix: 4 rows of r g b a bias),
- * TK_FILTER_OFFSET (dx, dy) or TK_FILTER_ERODE / TK_FILTER_DILATE (dx, dy:
- * the radii along x and y). */
+ * TK_FILTER_OFFSET (dx, dy), TK_FILTER_ERODE / TK_FILTER_DILATE (dx, dy:
+ * the radii along x and y), TK_FILTER_FLOOD (rgba: a straight colour) or
+ * TK_FILTER_DROP_SHADOW (dx, dy: the offset, std_dev, rgba). */
 typedef struct tk_canvas_filter {
     uint32_t kind;
     float amount;
     float dx, dy;
+    float rgba[4];
+    float std_dev;
     float matrix[20];
 } tk_canvas_filter;
 /* Canvas::push_filter_layer with Filter::Chain { filters, fixed_region } and

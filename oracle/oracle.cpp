@@ -2079,7 +2079,33 @@ void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const t
     if (b[2] <= b[0] || b[3] <= b[1]) return;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_filter& f = chain[k];
-        if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
+        if (f.kind == TK_FILTER_FLOOD) {  // filter_flood_region (filter/brush.hlsl:19-26)
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) surface[size_t(y) * width + x] = f.color;
+        } else if (f.kind == TK_FILTER_DROP_SHADOW) {
+            // shadow.rs:3-52: the alpha mask at the offset, the blur, the tinted
+            // shadow under the source (filter/basic.hlsl:58-66, filter/brush.hlsl:27-36)
+            std::vector<uint32_t> mask(size_t(width) * size_t(b[3]), 0u), temp(mask.size(), 0u);
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) {
+                    const uint32_t a = surface[size_t(y) * width + x] >> 24;
+                    if (a == 0u) continue;
+                    const int64_t tx = int64_t(x) + f.dx, ty = int64_t(y) + f.dy;
+                    if (tx >= b[0] && ty >= b[1] && tx < b[2] && ty < b[3]) mask[size_t(ty) * width + size_t(tx)] = a * 0x01010101u;
+                }
+            if (f.std_dev > 0.0f) {
+                const uint32_t region[4] = {uint32_t(b[0]), uint32_t(b[1]), uint32_t(b[2] - b[0]), uint32_t(b[3] - b[1])};
+                const uint32_t none[4] = {0, 0, 0, 0};
+                const uint32_t h = uint32_t(b[3]);
+                blur_pass(mask.data(), temp.data(), width, h, region, none, f.std_dev, 0, 1);
+                blur_pass(temp.data(), mask.data(), width, h, region, none, f.std_dev, 1, 1);
+            }
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) {
+                    uint32_t& p = surface[size_t(y) * width + x];
+                    p = src_over_premul_u8(scale_premul_u8(f.color, mask[size_t(y) * width + x] >> 24), p);
+                }
+        } else if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
             // effects.rs:169-221: nothing for zero radii; an erosion whose
             // doubled radius reaches the surface size clears it; else x, then y
             if (f.dx == 0 && f.dy == 0) continue;

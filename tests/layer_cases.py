@@ -167,4 +167,9 @@ def filter_chains():
         "dilate": [(N.FILTER_DILATE, (3.0, 4.2))],
         "morphology_chain": [(N.FILTER_DILATE, (2.0, 0.0)), (N.FILTER_SEPIA, 0.6), (N.FILTER_ERODE, (0.0, 1.5)),
                              (N.FILTER_OFFSET, (2.0, 2.0))],
+        "flood": [(N.FILTER_FLOOD, (0.2, 0.6, 0.9, 0.7))],
+        "drop_shadow": [(N.FILTER_DROP_SHADOW, (4.5, -3.0, 3.0, (0.0, 0.0, 0.2, 0.8)))],
+        "drop_shadow_sharp": [(N.FILTER_DROP_SHADOW, (-6.0, 5.0, 0.0, (0.9, 0.1, 0.1, 1.0))),
+                              (N.FILTER_GRAYSCALE, 0.3)],
+        "drop_shadow_wide": [(N.FILTER_DROP_SHADOW, (2.0, 2.0, 7.5, (0.1, 0.1, 0.1, 0.6)))],
     }

@@ -207,7 +207,7 @@ def test_filter_layer_that_hides_its_children():
 
 @pytest.mark.parametrize("name", sorted(filter_chains()))
 def test_filter_scenes_render_in_the_oracle(name):
-    c = filter_scene(7, filter_chains()[name], (15.5, 12.0, 170.2, 131.9))
+    c = filter_scene(7, filter_chains()[name], (30.5, 28.0, 165.2, 117.9))
     img = oracle.OracleRun(c.scene_desc(), threads=4).get(oracle.OR_IMAGE, np.uint32)
     assert img.any()
 
@@ -278,4 +278,37 @@ def test_morphology_known_answers():
     # an erosion whose doubled radius reaches the surface clears it
     full = np.full((h, w), 0xFF00FF00, dtype=np.uint32)
     assert not oracle_surface_chain(full.reshape(-1), w, (0, 0, w, h), [(N.FILTER_ERODE, (8, 1))]).any()
+
+
+def canvas_chain(chain):
+    """A scene with one filter layer over an opaque 2 x 2 block and the
+    frame's filter arrays."""
+    c = tk.Canvas(64, 48)
+    c.push_filter_layer(chain, (8.0, 8.0, 56.0, 40.0))
+    c.push_path(tk.BezPath().move_to(20, 20).line_to(22, 20).line_to(22, 22).line_to(20, 22).close(),
+                tk.Brush.solid(0.0, 1.0, 0.0, 1.0))
+    c.pop_layer()
+    return c
+
+
+def test_flood_and_drop_shadow_known_answers():
+    flood = canvas_chain([(N.FILTER_FLOOD, (1.0, 0.0, 0.0, 0.5))])
+    img = oracle.OracleRun(flood.scene_desc(), threads=2).get(oracle.OR_IMAGE, np.uint32).reshape(48, 64)
+    # the flood replaces the group over the bounds, composited over the
+    # transparent clear: premultiplied (0.5, 0, 0, 0.5)
+    assert np.all(img[8:40, 8:56] == 0x80000080) and not img[:8].any() and not img[:, :8].any()
+    shadow = canvas_chain([(N.FILTER_DROP_SHADOW, (3.0, 2.0, 0.0, (0.0, 0.0, 1.0, 1.0)))])
+    a = shadow.scene_arrays()
+    L, f = a["filter_layers"][0], a["filters"][0]
+    assert (f["dx"], f["dy"], f["color"]) == (3, 2, 0xFFFF0000)
+    assert list(L["surface"]) == [5, 5, 59, 43]  # reach: ceil(3 * 0) + max(3, 2)
+    img = oracle.OracleRun(shadow.scene_desc(), threads=2).get(oracle.OR_IMAGE, np.uint32).reshape(48, 64)
+    assert np.all(img[20:22, 20:22] == 0xFF00FF00)  # the source over its shadow
+    assert np.all(img[22:24, 23:25] == 0xFFFF0000)  # the shadow where the source is not
+    assert not img[30:, 30:].any()
+    # offsets round half away from zero; the reach adds ceil(3 std_dev)
+    c = canvas_chain([(N.FILTER_DROP_SHADOW, (2.5, -2.5, 1.2, (0, 0, 0, 1)))])
+    a = c.scene_arrays()
+    assert (a["filters"][0]["dx"], a["filters"][0]["dy"]) == (3, -3)
+    assert list(a["filter_layers"][0]["surface"]) == [8 - 7, 8 - 7, 56 + 7, 40 + 7]  # ceil(3.6) + 3
 

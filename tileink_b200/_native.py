@@ -95,12 +95,14 @@ PROGRESSIVE_DTYPE = np.dtype([("start_x", "<f4"), ("start_y", "<f4"), ("dir_x", 
 PROGRESSIVE_BALANCED, PROGRESSIVE_HIGH = 0, 1
 OP_PROGRESSIVE_BEGIN = 3
 OP_FILTER_BEGIN = 4
-FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<i4"), ("dy", "<i4"), ("matrix", "<f4", (20,))])
+FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<i4"), ("dy", "<i4"), ("color", "<u4"),
+                         ("std_dev", "<f4"), ("matrix", "<f4", (20,))])
 CANVAS_FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<f4"), ("dy", "<f4"),
-                                ("matrix", "<f4", (20,))])
+                                ("rgba", "<f4", (4,)), ("std_dev", "<f4"), ("matrix", "<f4", (20,))])
 FILTER_LAYER_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4"), ("surface", "<i4", (4,))])
 (FILTER_BRIGHTNESS, FILTER_CONTRAST, FILTER_GRAYSCALE, FILTER_HUE_ROTATE, FILTER_INVERT, FILTER_OPACITY,
- FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET, FILTER_ERODE, FILTER_DILATE) = range(1, 13)
+ FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET, FILTER_ERODE, FILTER_DILATE, FILTER_FLOOD,
+ FILTER_DROP_SHADOW) = range(1, 15)
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
 GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
 PTCL_GLYPH = 10

@@ -456,7 +456,9 @@ class Canvas:
         the chain's reach. `filters`: (kind, value) pairs, kind one of
         N.FILTER_* — a colour filter's amount (hue rotation in degrees), a
         20-float matrix for FILTER_COLOR_MATRIX, (dx, dy) for FILTER_OFFSET,
-        (radius_x, radius_y) for FILTER_ERODE / FILTER_DILATE.
+        (radius_x, radius_y) for FILTER_ERODE / FILTER_DILATE, a straight
+        (r, g, b, a) for FILTER_FLOOD, (dx, dy, std_dev, (r, g, b, a)) for
+        FILTER_DROP_SHADOW.
         `rect` = (x0, y0, x1, y1) in logical units."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
         for k, (kind, value) in enumerate(filters):
@@ -465,6 +467,11 @@ class Canvas:
                 chain[k]["matrix"] = np.asarray(value, dtype=np.float32).reshape(20)
             elif kind in (N.FILTER_OFFSET, N.FILTER_ERODE, N.FILTER_DILATE):
                 chain[k]["dx"], chain[k]["dy"] = value
+            elif kind == N.FILTER_FLOOD:
+                chain[k]["rgba"] = value
+            elif kind == N.FILTER_DROP_SHADOW:
+                dx, dy, std_dev, rgba = value
+                chain[k]["dx"], chain[k]["dy"], chain[k]["std_dev"], chain[k]["rgba"] = dx, dy, std_dev, rgba
             else:
                 chain[k]["amount"] = value
         r = np.asarray(rect, dtype=np.float64).reshape(4)

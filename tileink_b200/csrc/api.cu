@@ -136,6 +136,7 @@ struct Step {
     tk_progressive_blur prog{};
     std::vector<tk_filter> chain;  // BLUR_BEGIN of a filter layer: its chain (filter is set)
     bool filter = false;
+    bool shadow = false;  // the chain has a drop shadow (a second scratch surface)
 };
 
 // State of the last differentiable forward, kept for its backward.
@@ -513,11 +514,18 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                                    int32_t(std::min<int64_t>(L.surface[3], d.height))};
             Step s{STEP_BLUR_BEGIN, 0u, 0.0f, {ob[0], ob[1], ob[2], ob[3]}, 0u};
             s.filter = true;
-            bool spatial = false;
+            bool spatial = false, shadow = false;
             for (uint32_t k = L.first; k < L.first + L.count; ++k) {
                 const tk_filter& f = d.filters[k];
-                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DILATE || !std::isfinite(f.amount))
+                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DROP_SHADOW || !std::isfinite(f.amount))
                     invalid("filter " + std::to_string(k) + ": bad kind or amount");
+                if (f.kind == TK_FILTER_DROP_SHADOW) {
+                    if (!(f.std_dev >= 0.0f && f.std_dev <= 1.0e4f) || f.dx < -1000000 || f.dx > 1000000 ||
+                        f.dy < -1000000 || f.dy > 1000000)
+                        invalid("filter " + std::to_string(k) + ": drop shadow offset or deviation out of range");
+                    spatial = true;
+                    shadow = true;
+                }
                 if (f.kind == TK_FILTER_COLOR_MATRIX)
                     for (float v : f.matrix)
                         if (!std::isfinite(v)) invalid("filter " + std::to_string(k) + ": non-finite matrix");
@@ -533,8 +541,9 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             // canvas, so those layers are refused.
             if (spatial && (L.surface[0] < 0 || L.surface[1] < 0 || L.surface[2] > int64_t(d.width) ||
                             L.surface[3] > int64_t(d.height)))
-                invalid("an offset or morphology filter layer whose surface reaches past the canvas is outside this "
-                        "path");
+                invalid("an offset, morphology or drop shadow filter layer whose surface reaches past the canvas is "
+                        "outside this path");
+            s.shadow = shadow;
             c->steps.push_back(std::move(s));
             ++depth;
         } else if (op.kind == TK_OP_BLUR_END) {
@@ -836,7 +845,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
     for (size_t i = 0; i < blur_depth; ++i) c->surfaces[i].reserve(uint64_t(c->width) * c->height);
     if (blur_depth) c->temp.reserve(uint64_t(c->width) * c->height);
     bool reduced = false;
-    for (const Step& s : c->steps) reduced = reduced || s.sampling != 0u;
+    for (const Step& s : c->steps) reduced = reduced || s.sampling != 0u || s.shadow;
     if (reduced) c->low.reserve(uint64_t(c->width) * c->height);
     if (c->band && blur_depth) invalid("band rendering takes scenes without blur layers (their reach crosses bands)");
     TK_CUDA(cudaMemsetAsync(c->misc.ptr, 0, 8 * sizeof(uint32_t), st));
@@ -1080,8 +1089,8 @@ void do_render(tk_ctx* c) {
             if (b.filter) {
                 // the chain over the layer's bounds (render/filter_program/effects.rs:3-268)
                 if (ob[2] > ob[0] && ob[3] > ob[1])
-                    tk::launch_filter_chain(surf, c->temp.ptr, c->width, ob, b.chain.data(), uint32_t(b.chain.size()),
-                                            st);
+                    tk::launch_filter_chain(surf, c->temp.ptr, b.shadow ? c->low.ptr : nullptr, c->width, c->height, ob,
+                                            b.chain.data(), uint32_t(b.chain.size()), st);
             } else if (b.progressive) {
                 // Filter::ProgressiveBlur over the output bounds
                 // (native/runtime/program/filter/progressive/mod.rs:44-146)

@@ -1595,7 +1595,26 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
         tk_filter& g = chain[k];
         g = tk_filter{};
         g.kind = f.kind;
-        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DILATE || !std::isfinite(f.amount)) return -1;
+        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_DROP_SHADOW || !std::isfinite(f.amount)) return -1;
+        if (f.kind == TK_FILTER_FLOOD || f.kind == TK_FILTER_DROP_SHADOW) {
+            for (float v : f.rgba)
+                if (!std::isfinite(v)) return -1;
+            g.color = premul_color(f.rgba);  // the solid brush's colour word
+        }
+        if (f.kind == TK_FILTER_DROP_SHADOW) {
+            // physical_filter scales offset and deviation; shadow.rs rounds the
+            // offset (half away from zero); filter_outset adds blur_outset
+            // (ceil(3 std_dev)) and the offset's reach (filter.rs:566-571)
+            const float ox = f.dx * c->scale, oy = f.dy * c->scale, sd = f.std_dev * c->scale;
+            if (!std::isfinite(ox) || !std::isfinite(oy) || !std::isfinite(sd) || std::fabs(ox) > 1.0e6f ||
+                std::fabs(oy) > 1.0e6f || sd > 1.0e4f)
+                return -1;
+            g.dx = int32_t(std::round(ox));
+            g.dy = int32_t(std::round(oy));
+            g.std_dev = sd;
+            reach += uint64_t(std::ceil(std::max(sd, 0.0f) * 3.0f)) +
+                     uint64_t(std::max(std::ceil(std::fabs(ox)), std::ceil(std::fabs(oy))));
+        }
         g.amount = f.amount;
         if (f.kind == TK_FILTER_OFFSET) {
             const float dx = f.dx * c->scale, dy = f.dy * c->scale;

@@ -17,6 +17,14 @@
 //   scratch surface, then y back; an erosion clears texels within the radius
 //   of the line's ends, and one whose doubled radius reaches the surface
 //   size clears the bounds (render/filter_program/effects.rs:169-221).
+// * Flood: the bounds filled with the solid colour (filter_flood_region,
+//   filter/brush.hlsl:19-26).
+// * Drop shadow (render/filter_program/shadow.rs:3-52): the source alpha
+//   copied to all four channels of a cleared scratch surface at the offset
+//   position (filter_drop_shadow_mask_region, filter/basic.hlsl:58-66), the
+//   Gaussian blur of the blur groups over the bounds (x, then y), then the
+//   colour scaled by the shadow's alpha under the source
+//   (filter_composite_drop_shadow_region, filter/brush.hlsl:27-36).
 // The per-pixel kernels are HBM-bound: 8 bytes per pixel (read and write the
 // word); a morphology pass reads 2r + 1 texels per pixel, mostly from L1.
 #include <cuda_runtime.h>
@@ -228,6 +236,38 @@ __global__ void k_filter_clear(uint32_t* dst, uint32_t width, int4 b) {
         dst[uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w)] = 0u;
 }
 
+__global__ void k_filter_fill(uint32_t* dst, uint32_t width, int4 b, uint32_t color) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        dst[uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w)] = color;
+}
+
+// The source alpha in all four channels at the offset position, inside the
+// bounds (the destination cleared beforehand).
+__global__ void k_shadow_mask(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t width, int4 b,
+                              int32_t dx, int32_t dy) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const int64_t x = b.x + int64_t(i % w), y = b.y + int64_t(i / w);
+        const uint32_t a = src[uint64_t(y) * width + uint64_t(x)] >> 24;
+        if (a == 0u) continue;
+        const int64_t tx = x + dx, ty = y + dy;
+        if (tx >= b.x && ty >= b.y && tx < b.z && ty < b.w) dst[uint64_t(ty) * width + uint64_t(tx)] = a * 0x01010101u;
+    }
+}
+
+__global__ void k_shadow_composite(uint32_t* surface, const uint32_t* __restrict__ shadow, uint32_t width, int4 b,
+                                   uint32_t color) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t o = uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w);
+        surface[o] = src_over_premul_u8(scale_premul_u8(color, shadow[o] >> 24), surface[o]);
+    }
+}
+
 unsigned filter_grid(uint64_t n) {
     const uint64_t g = (n + 255) / 256;
     return unsigned(g < 148ull * 32 ? (g ? g : 1) : 148ull * 32);
@@ -235,8 +275,8 @@ unsigned filter_grid(uint64_t n) {
 
 }  // namespace
 
-void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t width, const int32_t bounds[4],
-                         const tk_filter* chain, uint32_t count, cudaStream_t st) {
+void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, uint32_t width, uint32_t height,
+                         const int32_t bounds[4], const tk_filter* chain, uint32_t count, cudaStream_t st) {
     const int4 b = make_int4(bounds[0], bounds[1], bounds[2], bounds[3]);
     if (b.z <= b.x || b.w <= b.y) return;
     const uint64_t n = uint64_t(b.z - b.x) * uint64_t(b.w - b.y);
@@ -246,6 +286,30 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t width, cons
             if (f.dx == 0 && f.dy == 0) continue;
             k_filter_offset<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
             k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+        } else if (f.kind == TK_FILTER_FLOOD) {
+            k_filter_fill<<<filter_grid(n), 256, 0, st>>>(surface, width, b, f.color);
+        } else if (f.kind == TK_FILTER_DROP_SHADOW) {
+            k_filter_fill<<<filter_grid(n), 256, 0, st>>>(temp, width, b, 0u);
+            k_shadow_mask<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
+            if (f.std_dev > 0.0f && temp2) {
+                BlurParams bp{};
+                bp.width = width;
+                bp.height = height;
+                bp.region[0] = uint32_t(b.x);
+                bp.region[1] = uint32_t(b.y);
+                bp.region[2] = uint32_t(b.z - b.x);
+                bp.region[3] = uint32_t(b.w - b.y);
+                bp.bounds[0] = b.x;
+                bp.bounds[1] = b.y;
+                bp.bounds[2] = b.z;
+                bp.bounds[3] = b.w;
+                bp.sigma = f.std_dev;
+                bp.axis = 0;
+                launch_blur(temp, temp2, bp, st);
+                bp.axis = 1;
+                launch_blur(temp2, temp, bp, st);
+            }
+            k_shadow_composite<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.color);
         } else if (f.kind == TK_FILTER_ERODE || f.kind == TK_FILTER_DILATE) {
             if (f.dx == 0 && f.dy == 0) continue;
             const uint32_t sw = uint32_t(b.z - b.x), sh = uint32_t(b.w - b.y);
