@@ -359,11 +359,17 @@ typedef struct tk_progressive_blur {
  * its Gaussian standard deviation. */
 #define TK_FILTER_FLOOD 13u
 #define TK_FILTER_DROP_SHADOW 14u
+/* Filter::ComponentTransfer (filter/transfer.hlsli): color is the index of
+ * a table in the scene's transfer_tables, TK_TRANSFER_TABLE_WORDS words each:
+ * 256 entries (0..255) for red, green, blue and alpha in that order, indexed
+ * by the straight (unpremultiplied) channel byte. */
+#define TK_FILTER_COMPONENT_TRANSFER 15u
+#define TK_TRANSFER_TABLE_WORDS 1024u
 typedef struct tk_filter {
     uint32_t kind;
     float amount;      /* the colour filters' argument (hue rotation in degrees) */
     int32_t dx, dy;    /* OFFSET, DROP_SHADOW: the offset; ERODE / DILATE: the radii */
-    uint32_t color;    /* FLOOD, DROP_SHADOW */
+    uint32_t color;    /* FLOOD, DROP_SHADOW: the colour; COMPONENT_TRANSFER: the table */
     float std_dev;     /* DROP_SHADOW */
     float matrix[20];  /* TK_FILTER_COLOR_MATRIX, row-major */
 } tk_filter; /* 104 B */
@@ -428,6 +434,10 @@ typedef struct tk_scene_desc {
     const tk_filter* filters;
     uint32_t filter_layer_count;
     uint32_t filter_count;
+    /* component transfer tables, TK_TRANSFER_TABLE_WORDS words each */
+    const uint32_t* transfer_tables;
+    uint32_t transfer_table_count;
+    uint32_t transfer_reserved;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

@@ -194,7 +194,9 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
  * degrees), TK_FILTER_COLOR_MATRIX (matrix: 4 rows of r g b a bias),
  * TK_FILTER_OFFSET (dx, dy), TK_FILTER_ERODE / TK_FILTER_DILATE (dx, dy:
  * the radii along x and y), TK_FILTER_FLOOD (rgba: a straight colour) or
- * TK_FILTER_DROP_SHADOW (dx, dy: the offset, std_dev, rgba). */
+ * TK_FILTER_DROP_SHADOW (dx, dy: the offset, std_dev, rgba) or
+ * TK_FILTER_COMPONENT_TRANSFER (table: TK_TRANSFER_TABLE_WORDS words, each
+ * 0..255, copied by the call). */
 typedef struct tk_canvas_filter {
     uint32_t kind;
     float amount;
@@ -202,6 +204,7 @@ typedef struct tk_canvas_filter {
     float rgba[4];
     float std_dev;
     float matrix[20];
+    const uint32_t* table;
 } tk_canvas_filter;
 /* Canvas::push_filter_layer with Filter::Chain { filters, fixed_region } and
  * a Region::Rect sample region without corner radii (src/canvas/layers.rs:

@@ -74,7 +74,7 @@ def lib() -> C.CDLL:
         l.or_text_pow.restype = F32
         l.or_text_pow.argtypes = [F32, F32]
         l.or_filter_chain.restype = None
-        l.or_filter_chain.argtypes = [P, U32, P, P, U32]
+        l.or_filter_chain.argtypes = [P, U32, P, P, U32, P]
         l.or_glyph_over.restype = U32
         l.or_glyph_over.argtypes = [U32, U32, U32]
         l.or_interpret_particles.restype = I32

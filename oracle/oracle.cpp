@@ -2075,7 +2075,22 @@ void morphology_pass(const uint32_t* src, uint32_t* dst, uint32_t width, const i
         }
 }
 
-void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const tk_filter* chain, uint32_t count) {
+// filter_transfer_pixel (filter/transfer.hlsli:5-19)
+inline uint32_t straight_index(uint32_t premul, uint32_t alpha) {
+    return alpha == 0u ? 0u : std::min((premul * 255u + alpha / 2u) / alpha, 255u);
+}
+uint32_t filter_transfer_pixel(const uint32_t* t, uint32_t pixel) {
+    const uint32_t alpha = pixel >> 24;
+    const float r = float(t[straight_index(pixel & 255u, alpha)]) * CHANNEL_SCALE;
+    const float g = float(t[256u + straight_index((pixel >> 8) & 255u, alpha)]) * CHANNEL_SCALE;
+    const float bl = float(t[512u + straight_index((pixel >> 16) & 255u, alpha)]) * CHANNEL_SCALE;
+    const float a = float(t[768u + alpha]) * CHANNEL_SCALE;
+    return pack(f2u(clampf(r * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(g * a, 0.0f, 1.0f) * 255.0f + 0.5f),
+                f2u(clampf(bl * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
+}
+
+void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const tk_filter* chain, uint32_t count,
+                  const uint32_t* tables = nullptr) {
     if (b[2] <= b[0] || b[3] <= b[1]) return;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_filter& f = chain[k];
@@ -2138,7 +2153,9 @@ void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const t
                 for (int32_t x = b[0]; x < b[2]; ++x) {
                     uint32_t& p = surface[size_t(y) * width + x];
                     p = f.kind == TK_FILTER_COLOR_MATRIX ? filter_color_matrix_pixel(f.matrix, p)
-                                                         : filter_color_pixel(p, f.kind, f.amount);
+                        : f.kind == TK_FILTER_COMPONENT_TRANSFER
+                            ? filter_transfer_pixel(tables + size_t(f.color) * TK_TRANSFER_TABLE_WORDS, p)
+                            : filter_color_pixel(p, f.kind, f.amount);
                 }
         }
     }
@@ -2613,6 +2630,9 @@ void raster_scene(or_scene& S, int threads) {
             s.sampling = 0u;
             s.filter = true;
             s.chain.assign(D.filters + L.first, D.filters + L.first + L.count);
+            for (const tk_filter& f : s.chain)
+                if (f.kind == TK_FILTER_COMPONENT_TRANSFER && f.color >= D.transfer_table_count)
+                    throw std::runtime_error("transfer table out of range");
             surfaces.push_back(std::move(s));
         } else if (op.kind == TK_OP_BLUR_END) {
             flush_pass();
@@ -2631,7 +2651,7 @@ void raster_scene(or_scene& S, int threads) {
             int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
             if (s.filter) {
                 const int32_t rect[4] = {bx0, by0, bx1, by1};
-                filter_chain(s.img.data(), D.width, rect, s.chain.data(), uint32_t(s.chain.size()));
+                filter_chain(s.img.data(), D.width, rect, s.chain.data(), uint32_t(s.chain.size()), D.transfer_tables);
             } else if (s.progressive) {
                 if (bx1 > bx0 && by1 > by0 && s.prog.max_std_dev > 0.0f) {
                     const int32_t rect[4] = {bx0, by0, bx1, by1};
@@ -2976,8 +2996,9 @@ float or_exp_nonpos(float x) { return exp_nonpos(x); }
 void or_sincos(float x, float* s, float* c) { lib_sincos(x, *s, *c); }
 float or_atan2(float y, float x) { return lib_atan2(y, x); }
 float or_text_pow(float x, float y) { return text_pow(x, y); }
-void or_filter_chain(uint32_t* surface, uint32_t width, const int32_t rect[4], const tk_filter* chain, uint32_t count) {
-    filter_chain(surface, width, rect, chain, count);
+void or_filter_chain(uint32_t* surface, uint32_t width, const int32_t rect[4], const tk_filter* chain, uint32_t count,
+                     const uint32_t* tables) {
+    filter_chain(surface, width, rect, chain, count, tables);
 }
 int32_t or_progressive_blur(uint32_t* surface, uint32_t width, uint32_t height, const int32_t rect[4],
                             const tk_progressive_blur* blur) {

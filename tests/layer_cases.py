@@ -172,4 +172,8 @@ def filter_chains():
         "drop_shadow_sharp": [(N.FILTER_DROP_SHADOW, (-6.0, 5.0, 0.0, (0.9, 0.1, 0.1, 1.0))),
                               (N.FILTER_GRAYSCALE, 0.3)],
         "drop_shadow_wide": [(N.FILTER_DROP_SHADOW, (2.0, 2.0, 7.5, (0.1, 0.1, 0.1, 0.6)))],
+        "component_transfer": [(N.FILTER_COMPONENT_TRANSFER,
+                                np.concatenate([255 - np.arange(256), (np.arange(256) ** 2) // 255,
+                                                np.minimum(np.arange(256) * 2, 255), np.arange(256)])),
+                               (N.FILTER_SATURATE, 1.5)],
     }

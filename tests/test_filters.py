@@ -41,7 +41,7 @@ def oracle_chain(pixels, chain):
         else:
             filters[k]["amount"] = value
     rect = np.array([0, 0, len(surf), 1], dtype=np.int32)
-    oracle.lib().or_filter_chain(N.ptr(surf), len(surf), N.ptr(rect), N.ptr(filters), len(filters))
+    oracle.lib().or_filter_chain(N.ptr(surf), len(surf), N.ptr(rect), N.ptr(filters), len(filters), None)
     return surf
 
 
@@ -147,7 +147,7 @@ def test_offset_moves_pixels_inside_the_bounds():
     filters[0]["kind"], filters[0]["dx"], filters[0]["dy"] = N.FILTER_OFFSET, 4, -3
     rect = np.array([2, 1, 20, 15], dtype=np.int32)
     out = surf.copy()
-    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(rect), N.ptr(filters), 1)
+    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(rect), N.ptr(filters), 1, None)
     s2, o2 = surf.reshape(h, w), out.reshape(h, w)
     for y in range(h):
         for x in range(w):
@@ -220,7 +220,7 @@ def oracle_surface_chain(surf, w, rect, chain):
         filters[k]["kind"] = kind
         filters[k]["dx"], filters[k]["dy"] = value
     r = np.array(rect, dtype=np.int32)
-    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(r), N.ptr(filters), len(filters))
+    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(r), N.ptr(filters), len(filters), None)
     return out
 
 
@@ -311,4 +311,40 @@ def test_flood_and_drop_shadow_known_answers():
     a = c.scene_arrays()
     assert (a["filters"][0]["dx"], a["filters"][0]["dy"]) == (3, -3)
     assert list(a["filter_layers"][0]["surface"]) == [8 - 7, 8 - 7, 56 + 7, 40 + 7]  # ceil(3.6) + 3
+
+
+def test_component_transfer_matches_numpy_and_identity():
+    rng = np.random.default_rng(21)
+    table = rng.integers(0, 256, N.TRANSFER_TABLE_WORDS).astype(np.uint32)
+    px = premul_pixels(4000, 13)
+    filters = np.zeros(1, dtype=N.FILTER_DTYPE)
+    filters[0]["kind"], filters[0]["color"] = N.FILTER_COMPONENT_TRANSFER, 0
+    got = px.copy()
+    rect = np.array([0, 0, len(px), 1], dtype=np.int32)
+    oracle.lib().or_filter_chain(N.ptr(got), len(px), N.ptr(rect), N.ptr(filters), 1, N.ptr(table))
+    # filter_transfer_pixel restated in numpy float32
+    a = (px >> 24).astype(np.int64)
+    idx = [np.where(a == 0, 0, np.minimum(((px >> s & 255).astype(np.int64) * 255 + a // 2) // np.maximum(a, 1), 255))
+           for s in (0, 8, 16)]
+    sc = F(1.0) / F(255.0)
+    ch = [table[256 * k + idx[k]].astype(np.float32) * sc for k in range(3)]
+    al = table[768 + a].astype(np.float32) * sc
+    q = [(np.clip(c * al, 0, 1) * F(255) + F(0.5)).astype(np.uint32) for c in ch]
+    qa = (np.clip(al, 0, 1) * F(255) + F(0.5)).astype(np.uint32)
+    assert np.array_equal(got, q[0] | q[1] << 8 | q[2] << 16 | qa << 24)
+    # the identity table keeps opaque pixels
+    ident = np.tile(np.arange(256, dtype=np.uint32), 4)
+    opaque = (px & 0x00FFFFFF) | 0xFF000000
+    out = opaque.copy()
+    oracle.lib().or_filter_chain(N.ptr(out), len(px), N.ptr(rect), N.ptr(filters), 1, N.ptr(ident))
+    assert np.array_equal(out, opaque)
+    # the Canvas copies tables and indexes them in order
+    c = tk.Canvas(64, 48)
+    c.push_filter_layer([(N.FILTER_COMPONENT_TRANSFER, table), (N.FILTER_COMPONENT_TRANSFER, ident)], (0, 0, 32, 32))
+    c.pop_layer()
+    arr = c.scene_arrays()
+    assert list(arr["filters"]["color"]) == [0, 1]
+    assert np.array_equal(arr["transfer_tables"], np.concatenate([table, ident]))
+    with pytest.raises(ValueError):
+        c.push_filter_layer([(N.FILTER_COMPONENT_TRANSFER, np.full(1024, 300))], (0, 0, 8, 8))
 

@@ -119,7 +119,7 @@ def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uni
 @pytest.mark.parametrize("name", ["brightness", "contrast", "grayscale", "hue_rotate", "invert", "opacity",
                                   "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain", "erode",
                                   "dilate", "morphology_chain", "flood", "drop_shadow", "drop_shadow_sharp",
-                                  "drop_shadow_wide"])
+                                  "drop_shadow_wide", "component_transfer"])
 def test_gpu_filter_layers_match_oracle(renderer, name):
     """Filter layers (Canvas::push_filter_layer with a chain; filter/color.hlsli,
     filter/basic.hlsl): every colour filter, the colour matrix, offsets and a

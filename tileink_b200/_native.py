@@ -98,11 +98,13 @@ OP_FILTER_BEGIN = 4
 FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<i4"), ("dy", "<i4"), ("color", "<u4"),
                          ("std_dev", "<f4"), ("matrix", "<f4", (20,))])
 CANVAS_FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<f4"), ("dy", "<f4"),
-                                ("rgba", "<f4", (4,)), ("std_dev", "<f4"), ("matrix", "<f4", (20,))])
+                                ("rgba", "<f4", (4,)), ("std_dev", "<f4"), ("matrix", "<f4", (20,)),
+                                ("table", "<u8")], align=True)
 FILTER_LAYER_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4"), ("surface", "<i4", (4,))])
 (FILTER_BRIGHTNESS, FILTER_CONTRAST, FILTER_GRAYSCALE, FILTER_HUE_ROTATE, FILTER_INVERT, FILTER_OPACITY,
  FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET, FILTER_ERODE, FILTER_DILATE, FILTER_FLOOD,
- FILTER_DROP_SHADOW) = range(1, 15)
+ FILTER_DROP_SHADOW, FILTER_COMPONENT_TRANSFER) = range(1, 16)
+TRANSFER_TABLE_WORDS = 1024
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
 GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
 PTCL_GLYPH = 10
@@ -138,7 +140,8 @@ class SceneDesc(C.Structure):
         ("glyph_image_count", C.c_uint32), ("glyph_reserved", C.c_uint32), ("glyph_texel_count", C.c_uint64),
         ("progressive_blurs", C.c_void_p), ("progressive_count", C.c_uint32), ("progressive_reserved", C.c_uint32),
         ("filter_layers", C.c_void_p), ("filters", C.c_void_p), ("filter_layer_count", C.c_uint32),
-        ("filter_count", C.c_uint32),
+        ("filter_count", C.c_uint32), ("transfer_tables", C.c_void_p), ("transfer_table_count", C.c_uint32),
+        ("transfer_reserved", C.c_uint32),
     ]
 
 
@@ -379,6 +382,7 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "progressive": arr(d.progressive_blurs, d.progressive_count, PROGRESSIVE_DTYPE),
         "filter_layers": arr(d.filter_layers, d.filter_layer_count, FILTER_LAYER_DTYPE),
         "filters": arr(d.filters, d.filter_count, FILTER_DTYPE),
+        "transfer_tables": arr(d.transfer_tables, d.transfer_table_count * TRANSFER_TABLE_WORDS, np.uint32),
     }
 
 
@@ -411,6 +415,9 @@ class ArrayScene:
             if v is not None and len(v):
                 setattr(d, "progressive_blurs" if key == "progressive" else key, ptr(v))
                 setattr(d, cnt, len(v))
+        tables = a.get("transfer_tables")
+        if tables is not None and len(tables):
+            d.transfer_tables, d.transfer_table_count = ptr(tables), len(tables) // TRANSFER_TABLE_WORDS
         images = [np.ascontiguousarray(im, dtype=np.uint32) for im in a.get("images", [])]
         if images:
             self._images = images

@@ -458,9 +458,11 @@ class Canvas:
         20-float matrix for FILTER_COLOR_MATRIX, (dx, dy) for FILTER_OFFSET,
         (radius_x, radius_y) for FILTER_ERODE / FILTER_DILATE, a straight
         (r, g, b, a) for FILTER_FLOOD, (dx, dy, std_dev, (r, g, b, a)) for
-        FILTER_DROP_SHADOW.
+        FILTER_DROP_SHADOW, 1024 bytes (R, G, B, A tables of 256) for
+        FILTER_COMPONENT_TRANSFER.
         `rect` = (x0, y0, x1, y1) in logical units."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
+        keep = []  # the transfer tables, alive for the call (the canvas copies them)
         for k, (kind, value) in enumerate(filters):
             chain[k]["kind"] = kind
             if kind == N.FILTER_COLOR_MATRIX:
@@ -472,6 +474,10 @@ class Canvas:
             elif kind == N.FILTER_DROP_SHADOW:
                 dx, dy, std_dev, rgba = value
                 chain[k]["dx"], chain[k]["dy"], chain[k]["std_dev"], chain[k]["rgba"] = dx, dy, std_dev, rgba
+            elif kind == N.FILTER_COMPONENT_TRANSFER:
+                table = np.ascontiguousarray(np.asarray(value, dtype=np.uint32).reshape(N.TRANSFER_TABLE_WORDS))
+                keep.append(table)
+                chain[k]["table"] = table.ctypes.data
             else:
                 chain[k]["amount"] = value
         r = np.asarray(rect, dtype=np.float64).reshape(4)

@@ -17,6 +17,8 @@
 //   scratch surface, then y back; an erosion clears texels within the radius
 //   of the line's ends, and one whose doubled radius reaches the surface
 //   size clears the bounds (render/filter_program/effects.rs:169-221).
+// * Component transfer: each channel's table at its straight byte
+//   (filter_transfer_pixel, filter/transfer.hlsli:5-19).
 // * Flood: the bounds filled with the solid colour (filter_flood_region,
 //   filter/brush.hlsl:19-26).
 // * Drop shadow (render/filter_program/shadow.rs:3-52): the source alpha
@@ -42,7 +44,23 @@ struct FilterArgs {
     uint32_t kind;
     float amount;
     float m[20];
+    const uint32_t* table;  // COMPONENT_TRANSFER: its table
 };
+
+// filter_transfer_pixel (filter/transfer.hlsli:5-19): the straight channel
+// byte (rounded) indexes each channel's table, alpha its own.
+__device__ __forceinline__ uint32_t straight_index(uint32_t premul, uint32_t alpha) {
+    return alpha == 0u ? 0u : min((premul * 255u + alpha / 2u) / alpha, 255u);
+}
+__device__ uint32_t transfer_pixel(const uint32_t* __restrict__ t, uint32_t pixel) {
+    const uint32_t alpha = pixel >> 24;
+    const float r = float(__ldg(t + straight_index(pixel & 255u, alpha))) * CHANNEL_SCALE;
+    const float g = float(__ldg(t + 256u + straight_index((pixel >> 8) & 255u, alpha))) * CHANNEL_SCALE;
+    const float b = float(__ldg(t + 512u + straight_index((pixel >> 16) & 255u, alpha))) * CHANNEL_SCALE;
+    const float a = float(__ldg(t + 768u + alpha)) * CHANNEL_SCALE;
+    return pack4(f2u(clampf(r * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(g * a, 0.0f, 1.0f) * 255.0f + 0.5f),
+                 f2u(clampf(b * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
+}
 
 // svg_luminance (filter/color.hlsli:7)
 __device__ __forceinline__ float svg_luminance(float r, float g, float b) {
@@ -160,7 +178,9 @@ __global__ void k_filter_color(uint32_t* surface, uint32_t width, int4 b, Filter
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const uint64_t o = uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w);
         const uint32_t p = surface[o];
-        surface[o] = f.kind == TK_FILTER_COLOR_MATRIX ? color_matrix_pixel(f.m, p) : color_filter_pixel(p, f.kind, f.amount);
+        surface[o] = f.kind == TK_FILTER_COLOR_MATRIX         ? color_matrix_pixel(f.m, p)
+                     : f.kind == TK_FILTER_COMPONENT_TRANSFER ? transfer_pixel(f.table, p)
+                                                              : color_filter_pixel(p, f.kind, f.amount);
     }
 }
 
@@ -275,8 +295,9 @@ unsigned filter_grid(uint64_t n) {
 
 }  // namespace
 
-void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, uint32_t width, uint32_t height,
-                         const int32_t bounds[4], const tk_filter* chain, uint32_t count, cudaStream_t st) {
+void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, const uint32_t* tables, uint32_t width,
+                         uint32_t height, const int32_t bounds[4], const tk_filter* chain, uint32_t count,
+                         cudaStream_t st) {
     const int4 b = make_int4(bounds[0], bounds[1], bounds[2], bounds[3]);
     if (b.z <= b.x || b.w <= b.y) return;
     const uint64_t n = uint64_t(b.z - b.x) * uint64_t(b.w - b.y);
@@ -324,8 +345,9 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, uin
             k_filter_morphology<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b, min(ry, sh - 1u), dilate,
                                                                  false);
         } else {
-            FilterArgs a{f.kind, f.amount, {}};
+            FilterArgs a{f.kind, f.amount, {}, nullptr};
             for (int m = 0; m < 20; ++m) a.m[m] = f.matrix[m];
+            if (f.kind == TK_FILTER_COMPONENT_TRANSFER) a.table = tables + uint64_t(f.color) * TK_TRANSFER_TABLE_WORDS;
             k_filter_color<<<filter_grid(n), 256, 0, st>>>(surface, width, b, a);
         }
     }

@@ -219,9 +219,11 @@ void launch_blur(const uint32_t* src, uint32_t* dst, const BlurParams& b, cudaSt
 void launch_composite(uint32_t* dst, const uint32_t* src, uint32_t width, const int32_t bounds[4], cudaStream_t st);
 // A filter layer's chain applied in place to `surface` over `bounds`
 // (filter.cu); `temp` is a scratch surface of the same size, `temp2` a second
-// one that drop shadows need (null for chains without one).
-void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, uint32_t width, uint32_t height,
-                         const int32_t bounds[4], const tk_filter* chain, uint32_t count, cudaStream_t st);
+// one that drop shadows need (null for chains without one), `tables` the
+// scene's component transfer tables on the device.
+void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, const uint32_t* tables, uint32_t width,
+                         uint32_t height, const int32_t bounds[4], const tk_filter* chain, uint32_t count,
+                         cudaStream_t st);
 
 // Progressive blur (progressive.cu). A pyramid level: its size, scale and
 // cumulative variance, its decimation step and its paired kernel (offset,
