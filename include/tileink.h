@@ -359,20 +359,31 @@ typedef struct tk_progressive_blur {
  * its Gaussian standard deviation. */
 #define TK_FILTER_FLOOD 13u
 #define TK_FILTER_DROP_SHADOW 14u
-/* Filter::ComponentTransfer (filter/transfer.hlsli): color is the index of
- * a table in the scene's transfer_tables, TK_TRANSFER_TABLE_WORDS words each:
+/* Filter::ComponentTransfer (filter/transfer.hlsli): color is the first word
+ * of its table in the scene's filter_words, TK_TRANSFER_TABLE_WORDS words:
  * 256 entries (0..255) for red, green, blue and alpha in that order, indexed
  * by the straight (unpremultiplied) channel byte. */
 #define TK_FILTER_COMPONENT_TRANSFER 15u
 #define TK_TRANSFER_TABLE_WORDS 1024u
+/* Filter::ConvolveMatrix (filter/convolve.hlsli): color is the first word of
+ * its columns x rows kernel (f32 bits, row-major) in filter_words; target,
+ * divisor, bias, edge mode and preserve_alpha as in the reference. */
+#define TK_FILTER_CONVOLVE 16u
+#define TK_CONVOLVE_EDGE_NONE 0u
+#define TK_CONVOLVE_EDGE_DUPLICATE 1u
+#define TK_CONVOLVE_EDGE_WRAP 2u
+#define TK_CONVOLVE_MAX_TAPS 4096u
 typedef struct tk_filter {
     uint32_t kind;
     float amount;      /* the colour filters' argument (hue rotation in degrees) */
     int32_t dx, dy;    /* OFFSET, DROP_SHADOW: the offset; ERODE / DILATE: the radii */
-    uint32_t color;    /* FLOOD, DROP_SHADOW: the colour; COMPONENT_TRANSFER: the table */
+    uint32_t color;    /* FLOOD, DROP_SHADOW: the colour; COMPONENT_TRANSFER, CONVOLVE: first filter word */
     float std_dev;     /* DROP_SHADOW */
     float matrix[20];  /* TK_FILTER_COLOR_MATRIX, row-major */
-} tk_filter; /* 104 B */
+    /* TK_FILTER_CONVOLVE */
+    uint32_t columns, rows, target_x, target_y, edge_mode, preserve_alpha;
+    float divisor, bias;
+} tk_filter; /* 136 B */
 /* One filter layer: its chain filters[first, first + count), and the surface
  * bounds the chain reads (the sample region's pixel bounds grown by the
  * chain's reach, filter.rs:510-575; may extend past the canvas). */
@@ -434,10 +445,10 @@ typedef struct tk_scene_desc {
     const tk_filter* filters;
     uint32_t filter_layer_count;
     uint32_t filter_count;
-    /* component transfer tables, TK_TRANSFER_TABLE_WORDS words each */
-    const uint32_t* transfer_tables;
-    uint32_t transfer_table_count;
-    uint32_t transfer_reserved;
+    /* words the filters index: component transfer tables, convolution kernels */
+    const uint32_t* filter_words;
+    uint32_t filter_word_count;
+    uint32_t filter_reserved;
 } tk_scene_desc;
 
 /* Per-scene counts measured by the device pipeline. */

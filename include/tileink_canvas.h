@@ -196,7 +196,8 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
  * the radii along x and y), TK_FILTER_FLOOD (rgba: a straight colour) or
  * TK_FILTER_DROP_SHADOW (dx, dy: the offset, std_dev, rgba) or
  * TK_FILTER_COMPONENT_TRANSFER (table: TK_TRANSFER_TABLE_WORDS words, each
- * 0..255, copied by the call). */
+ * 0..255, copied by the call) or TK_FILTER_CONVOLVE (kernel: columns x rows
+ * floats, copied; target, divisor, bias, edge_mode, preserve_alpha). */
 typedef struct tk_canvas_filter {
     uint32_t kind;
     float amount;
@@ -205,6 +206,9 @@ typedef struct tk_canvas_filter {
     float std_dev;
     float matrix[20];
     const uint32_t* table;
+    const float* kernel;
+    uint32_t columns, rows, target_x, target_y, edge_mode, preserve_alpha;
+    float divisor, bias;
 } tk_canvas_filter;
 /* Canvas::push_filter_layer with Filter::Chain { filters, fixed_region } and
  * a Region::Rect sample region without corner radii (src/canvas/layers.rs:

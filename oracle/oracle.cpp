@@ -2089,12 +2089,109 @@ uint32_t filter_transfer_pixel(const uint32_t* t, uint32_t pixel) {
                 f2u(clampf(bl * a, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
 }
 
+// filter_convolve_pixel (filter/convolve.hlsli:9-98) over bounds b
+inline int32_t conv_wrap(int32_t c, int32_t origin, int32_t len) {
+    const int32_t r = (c - origin) % len;
+    return origin + (r < 0 ? r + len : r);
+}
+inline float conv_scale_24(float v) {
+    const uint32_t bits = f_bits(v), mag = bits & 0x7fffffffu, e = mag >> 23;
+    if (e == 0u) {
+        const float s = float(mag) * bits_f(0x01000000u);
+        return (bits & 0x80000000u) ? -s : s;
+    }
+    if (e >= 231u) return bits_f((bits & 0x80000000u) | 0x7f800000u);
+    return bits_f(bits + (24u << 23));
+}
+inline float conv_unscale_24(float v) {
+    const uint32_t bits = f_bits(v), e = (bits & 0x7fffffffu) >> 23;
+    if (e <= 24u) return 0.0f;
+    return bits_f(bits - (24u << 23));
+}
+void convolve_pass(const uint32_t* src, uint32_t* dst, uint32_t width, const int32_t b[4], const tk_filter& k,
+                   const float* kernel) {
+    const uint32_t dmag = f_bits(k.divisor) & 0x7fffffffu;
+    for (int32_t y = b[1]; y < b[3]; ++y)
+        for (int32_t x = b[0]; x < b[2]; ++x) {
+            const size_t o = size_t(y) * width + size_t(x);
+            const uint32_t center = src[o];
+            if (k.columns == 0u || k.rows == 0u || dmag == 0u) {
+                dst[o] = center;
+                continue;
+            }
+            float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            for (uint32_t ky = 0; ky < k.rows; ++ky)
+                for (uint32_t kx = 0; kx < k.columns; ++kx) {
+                    const float wt = kernel[(k.rows - 1u - ky) * k.columns + (k.columns - 1u - kx)];
+                    int32_t px = x + int32_t(kx) - int32_t(k.target_x), py = y + int32_t(ky) - int32_t(k.target_y);
+                    uint32_t p = 0u;
+                    if (k.edge_mode == TK_CONVOLVE_EDGE_DUPLICATE) {
+                        px = std::min(std::max(px, b[0]), b[2] - 1);
+                        py = std::min(std::max(py, b[1]), b[3] - 1);
+                        p = src[size_t(py) * width + size_t(px)];
+                    } else if (k.edge_mode == TK_CONVOLVE_EDGE_WRAP) {
+                        px = conv_wrap(px, b[0], b[2] - b[0]);
+                        py = conv_wrap(py, b[1], b[3] - b[1]);
+                        p = src[size_t(py) * width + size_t(px)];
+                    } else if (px >= b[0] && py >= b[1] && px < b[2] && py < b[3]) {
+                        p = src[size_t(py) * width + size_t(px)];
+                    }
+                    const uint32_t al = p >> 24;
+                    F4 v = rgba8_to_unorm(p);
+                    if (k.preserve_alpha) {
+                        v.r = al == 0u ? 0.0f : v.r / v.a;
+                        v.g = al == 0u ? 0.0f : v.g / v.a;
+                        v.b = al == 0u ? 0.0f : v.b / v.a;
+                    }
+                    v.a = float(al);
+                    s[0] = mad(v.r, wt, s[0]);
+                    s[1] = mad(v.g, wt, s[1]);
+                    s[2] = mad(v.b, wt, s[2]);
+                    s[3] = mad(v.a, wt, s[3]);
+                }
+            float q[3], qa;
+            if (dmag < 0x00800000u) {
+                float sd = float(dmag) * bits_f(0x01000000u);
+                if (f_bits(k.divisor) & 0x80000000u) sd = -sd;
+                for (int c = 0; c < 3; ++c) q[c] = conv_scale_24(s[c]) / sd;
+                qa = conv_scale_24(s[3]) / (sd * 255.0f);
+            } else if (dmag > 0x7e800000u) {
+                const float inv = 1.0f / conv_unscale_24(k.divisor);
+                for (int c = 0; c < 3; ++c) q[c] = conv_unscale_24(s[c]) * inv;
+                qa = conv_unscale_24(s[3]) * inv * CHANNEL_SCALE;
+            } else {
+                const float rc = 1.0f / k.divisor;
+                for (int c = 0; c < 3; ++c) q[c] = s[c] * rc;
+                qa = (s[3] * rc) * CHANNEL_SCALE;
+            }
+            const float ua = k.preserve_alpha ? float(center >> 24) * CHANNEL_SCALE : qa + k.bias;
+            const float a = clampf(ua, 0.0f, 1.0f);
+            const float bb = k.bias * ua;
+            float c3[3];
+            for (int c = 0; c < 3; ++c) {
+                const float v = q[c] + bb;
+                c3[c] = k.preserve_alpha ? clampf(v, 0.0f, 1.0f) * a : clampf(v, 0.0f, a);
+            }
+            dst[o] = pack(f2u(clampf(c3[0], 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c3[1], 0.0f, 1.0f) * 255.0f + 0.5f),
+                          f2u(clampf(c3[2], 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
+        }
+}
+
 void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const tk_filter* chain, uint32_t count,
                   const uint32_t* tables = nullptr) {
     if (b[2] <= b[0] || b[3] <= b[1]) return;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_filter& f = chain[k];
-        if (f.kind == TK_FILTER_FLOOD) {  // filter_flood_region (filter/brush.hlsl:19-26)
+        if (f.kind == TK_FILTER_CONVOLVE) {  // into a scratch copy, then back (effects.rs:115-133)
+            std::vector<uint32_t> temp(size_t(width) * size_t(b[3]), 0u);
+            float* kernel = nullptr;
+            std::vector<float> kv(size_t(f.columns) * f.rows);
+            for (size_t t = 0; t < kv.size(); ++t) kv[t] = bits_f(tables[f.color + t]);
+            kernel = kv.data();
+            convolve_pass(surface, temp.data(), width, b, f, kernel);
+            for (int32_t y = b[1]; y < b[3]; ++y)
+                for (int32_t x = b[0]; x < b[2]; ++x) surface[size_t(y) * width + x] = temp[size_t(y) * width + x];
+        } else if (f.kind == TK_FILTER_FLOOD) {  // filter_flood_region (filter/brush.hlsl:19-26)
             for (int32_t y = b[1]; y < b[3]; ++y)
                 for (int32_t x = b[0]; x < b[2]; ++x) surface[size_t(y) * width + x] = f.color;
         } else if (f.kind == TK_FILTER_DROP_SHADOW) {
@@ -2154,7 +2251,7 @@ void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const t
                     uint32_t& p = surface[size_t(y) * width + x];
                     p = f.kind == TK_FILTER_COLOR_MATRIX ? filter_color_matrix_pixel(f.matrix, p)
                         : f.kind == TK_FILTER_COMPONENT_TRANSFER
-                            ? filter_transfer_pixel(tables + size_t(f.color) * TK_TRANSFER_TABLE_WORDS, p)
+                            ? filter_transfer_pixel(tables + f.color, p)
                             : filter_color_pixel(p, f.kind, f.amount);
                 }
         }
@@ -2631,8 +2728,10 @@ void raster_scene(or_scene& S, int threads) {
             s.filter = true;
             s.chain.assign(D.filters + L.first, D.filters + L.first + L.count);
             for (const tk_filter& f : s.chain)
-                if (f.kind == TK_FILTER_COMPONENT_TRANSFER && f.color >= D.transfer_table_count)
-                    throw std::runtime_error("transfer table out of range");
+                if ((f.kind == TK_FILTER_COMPONENT_TRANSFER &&
+                     uint64_t(f.color) + TK_TRANSFER_TABLE_WORDS > D.filter_word_count) ||
+                    (f.kind == TK_FILTER_CONVOLVE && uint64_t(f.color) + uint64_t(f.columns) * f.rows > D.filter_word_count))
+                    throw std::runtime_error("filter words out of range");
             surfaces.push_back(std::move(s));
         } else if (op.kind == TK_OP_BLUR_END) {
             flush_pass();
@@ -2651,7 +2750,7 @@ void raster_scene(or_scene& S, int threads) {
             int32_t sy1 = std::min(s.bounds[3] + rad, int32_t(D.height));
             if (s.filter) {
                 const int32_t rect[4] = {bx0, by0, bx1, by1};
-                filter_chain(s.img.data(), D.width, rect, s.chain.data(), uint32_t(s.chain.size()), D.transfer_tables);
+                filter_chain(s.img.data(), D.width, rect, s.chain.data(), uint32_t(s.chain.size()), D.filter_words);
             } else if (s.progressive) {
                 if (bx1 > bx0 && by1 > by0 && s.prog.max_std_dev > 0.0f) {
                     const int32_t rect[4] = {bx0, by0, bx1, by1};

@@ -128,7 +128,7 @@ float or_atan2(float y, float x);
 float or_text_pow(float x, float y);
 /* The filter layer chain (filter/color.hlsli, filter/basic.hlsl) applied in
  * place over rect = {x0, y0, x1, y1} of a width-wide RGBA8 surface;
- * `tables` holds the component transfer tables the chain indexes. */
+ * `tables` holds the filter words (transfer tables, kernels) it indexes. */
 void or_filter_chain(uint32_t* surface, uint32_t width, const int32_t rect[4], const tk_filter* chain, uint32_t count,
                      const uint32_t* tables);
 /* The progressive blur of `surface` (width x height, RGBA8) inside `rect`,

@@ -176,4 +176,11 @@ def filter_chains():
                                 np.concatenate([255 - np.arange(256), (np.arange(256) ** 2) // 255,
                                                 np.minimum(np.arange(256) * 2, 255), np.arange(256)])),
                                (N.FILTER_SATURATE, 1.5)],
+        "convolve_box": [(N.FILTER_CONVOLVE, {"kernel": np.ones((3, 3)), "edge_mode": N.CONVOLVE_EDGE_DUPLICATE})],
+        "convolve_edges": [(N.FILTER_CONVOLVE, {"kernel": [[0, -1, 0], [-1, 4, -1], [0, -1, 0]], "divisor": 1.0,
+                                                "bias": 0.3, "edge_mode": N.CONVOLVE_EDGE_WRAP})],
+        "convolve_preserve": [(N.FILTER_CONVOLVE, {"kernel": [[1, 2, 0.5, -1, 3], [0, 1, 0, 2, 1]],
+                                                   "target": (3, 0), "divisor": 6.5, "bias": -0.1,
+                                                   "edge_mode": N.CONVOLVE_EDGE_NONE, "preserve_alpha": True}),
+                              (N.FILTER_OPACITY, 0.9)],
     }

@@ -343,8 +343,106 @@ def test_component_transfer_matches_numpy_and_identity():
     c.push_filter_layer([(N.FILTER_COMPONENT_TRANSFER, table), (N.FILTER_COMPONENT_TRANSFER, ident)], (0, 0, 32, 32))
     c.pop_layer()
     arr = c.scene_arrays()
-    assert list(arr["filters"]["color"]) == [0, 1]
-    assert np.array_equal(arr["transfer_tables"], np.concatenate([table, ident]))
+    assert list(arr["filters"]["color"]) == [0, 1024]
+    assert np.array_equal(arr["filter_words"], np.concatenate([table, ident]))
     with pytest.raises(ValueError):
         c.push_filter_layer([(N.FILTER_COMPONENT_TRANSFER, np.full(1024, 300))], (0, 0, 8, 8))
+
+
+def oracle_convolve(img, rect, kernel, target, divisor, bias, edge, preserve):
+    """The oracle's convolution over rect of a 2-D surface (a copy)."""
+    h, w = img.shape
+    kern = np.ascontiguousarray(kernel, dtype=np.float32)
+    words = kern.view(np.uint32).reshape(-1).copy()
+    f = np.zeros(1, dtype=N.FILTER_DTYPE)
+    f[0]["kind"], f[0]["color"] = N.FILTER_CONVOLVE, 0
+    f[0]["rows"], f[0]["columns"] = kern.shape
+    f[0]["target_x"], f[0]["target_y"] = target
+    f[0]["divisor"], f[0]["bias"], f[0]["edge_mode"], f[0]["preserve_alpha"] = divisor, bias, edge, int(preserve)
+    out = np.ascontiguousarray(img, dtype=np.uint32).reshape(-1).copy()
+    r = np.array(rect, dtype=np.int32)
+    oracle.lib().or_filter_chain(N.ptr(out), w, N.ptr(r), N.ptr(f), 1, N.ptr(words))
+    return out.reshape(h, w)
+
+
+def np_convolve(img, rect, kernel, target, divisor, bias, edge, preserve):
+    """filter_convolve_pixel restated with numpy float32 (normal divisors)."""
+    x0, y0, x1, y1 = rect
+    kern = np.asarray(kernel, dtype=np.float32)
+    rows, cols = kern.shape
+    out = img.copy()
+    sc = F(1.0) / F(255.0)
+    for y in range(y0, y1):
+        for x in range(x0, x1):
+            acc = [F(0)] * 4
+            for ky in range(rows):
+                for kx in range(cols):
+                    wt = kern[rows - 1 - ky, cols - 1 - kx]
+                    px, py = x + kx - target[0], y + ky - target[1]
+                    p = 0
+                    if edge == N.CONVOLVE_EDGE_DUPLICATE:
+                        p = int(img[min(max(py, y0), y1 - 1), min(max(px, x0), x1 - 1)])
+                    elif edge == N.CONVOLVE_EDGE_WRAP:
+                        p = int(img[y0 + (py - y0) % (y1 - y0), x0 + (px - x0) % (x1 - x0)])
+                    elif x0 <= px < x1 and y0 <= py < y1:
+                        p = int(img[py, px])
+                    al = p >> 24
+                    v = [F(p >> s & 255) * sc for s in (0, 8, 16, 24)]
+                    if preserve:
+                        v[:3] = [F(0) if al == 0 else c / v[3] for c in v[:3]]
+                    v[3] = F(al)
+                    acc = [mad(v[c], wt, acc[c]) for c in range(4)]
+            rc = F(1.0) / F(divisor)
+            q = [acc[c] * rc for c in range(3)]
+            qa = (acc[3] * rc) * sc
+            ua = F(int(img[y, x]) >> 24) * sc if preserve else qa + F(bias)
+            a = F(min(max(ua, F(0)), F(1)))
+            bb = F(bias) * ua
+            col = [q[c] + bb for c in range(3)]
+            col = [F(min(max(c, F(0)), F(1))) * a if preserve else F(min(max(c, F(0)), a)) for c in col]
+            b = [int(F(min(max(c, F(0)), F(1))) * F(255) + F(0.5)) for c in col + [a]]
+            out[y, x] = b[0] | b[1] << 8 | b[2] << 16 | b[3] << 24
+    return out
+
+
+CONVOLVE_CASES = [
+    ([[1, 1, 1], [1, 1, 1], [1, 1, 1]], (1, 1), 9.0, 0.0, 1, False),
+    ([[0, -1, 0], [-1, 4, -1], [0, -1, 0]], (1, 1), 1.0, 0.25, 2, False),
+    ([[1, 2, 0.5, -1, 3], [0, 1, 0, 2, 1]], (3, 0), 6.5, -0.1, 0, True),
+    ([[0.2, 0.7], [0.4, -0.3]], (0, 1), 0.8, 0.0, 0, False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CONVOLVE_CASES)))
+def test_convolution_matches_numpy_restatement(case):
+    kernel, target, divisor, bias, edge, preserve = CONVOLVE_CASES[case]
+    w, h = 14, 11
+    img = premul_pixels(w * h, 300 + case).reshape(h, w)
+    rect = (2, 1, 13, 10)
+    got = oracle_convolve(img, rect, kernel, target, divisor, bias, edge, preserve)
+    want = np_convolve(img, rect, kernel, target, divisor, bias, edge, preserve)
+    d = np.abs(np.stack([(got >> s) & 255 for s in (0, 8, 16, 24)]).astype(np.int64)
+               - np.stack([(want >> s) & 255 for s in (0, 8, 16, 24)]).astype(np.int64))
+    assert d.max() <= 1 and (d == 0).mean() >= 0.99, (d.max(), (d == 0).mean())
+
+
+def test_convolution_identity_and_divisor_ranges():
+    w, h = 12, 9
+    img = premul_pixels(w * h, 77).reshape(h, w)
+    ident = [[0, 0, 0], [0, 1, 0], [0, 0, 0]]
+    for edge in (0, 1, 2):
+        assert np.array_equal(oracle_convolve(img, (0, 0, w, h), ident, (1, 1), 1.0, 0.0, edge, False), img)
+    # a zero divisor or an empty kernel keeps the centre
+    assert np.array_equal(oracle_convolve(img, (0, 0, w, h), ident, (1, 1), 0.0, 0.0, 1, False), img)
+    # kernel and divisor scaled together by 2^-140 (a subnormal divisor) or
+    # 2^100 (a huge one) give the same image as unscaled
+    base = oracle_convolve(img, (0, 0, w, h), [[1, 2, 1], [2, 4, 2], [1, 2, 1]], (1, 1), 16.0, 0.0, 1, False)
+    tiny = np.float32(2.0 ** -140)
+    sub = oracle_convolve(img, (0, 0, w, h), np.float32([[1, 2, 1], [2, 4, 2], [1, 2, 1]]) * tiny, (1, 1),
+                          np.float32(16.0) * tiny, 0.0, 1, False)
+    assert np.abs(sub.astype(np.int64) - base.astype(np.int64)).max() <= 0x01010101
+    huge = np.float32(2.0 ** 100)
+    big = oracle_convolve(img, (0, 0, w, h), np.float32([[1, 2, 1], [2, 4, 2], [1, 2, 1]]) * huge, (1, 1),
+                          np.float32(16.0) * huge, 0.0, 1, False)
+    assert np.array_equal(big, base)
 

@@ -119,7 +119,8 @@ def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uni
 @pytest.mark.parametrize("name", ["brightness", "contrast", "grayscale", "hue_rotate", "invert", "opacity",
                                   "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain", "erode",
                                   "dilate", "morphology_chain", "flood", "drop_shadow", "drop_shadow_sharp",
-                                  "drop_shadow_wide", "component_transfer"])
+                                  "drop_shadow_wide", "component_transfer", "convolve_box", "convolve_edges",
+                                  "convolve_preserve"])
 def test_gpu_filter_layers_match_oracle(renderer, name):
     """Filter layers (Canvas::push_filter_layer with a chain; filter/color.hlsli,
     filter/basic.hlsl): every colour filter, the colour matrix, offsets and a
@@ -162,9 +163,9 @@ def test_gpu_offset_filter_past_the_canvas_is_rejected(renderer):
     refused at upload, and the context stays usable."""
     from layer_cases import filter_scene
     c = filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (-10.0, 0.0, 50.0, 50.0))
-    with pytest.raises(tk.TileinkError, match="offset, morphology or drop shadow filter layer"):
+    with pytest.raises(tk.TileinkError, match="whose surface reaches past"):
         renderer.upload(c)
     c = filter_scene(2, [(N.FILTER_DILATE, (3.0, 3.0))], (10.0, 10.0, 198.0, 100.0))
-    with pytest.raises(tk.TileinkError, match="offset, morphology or drop shadow filter layer"):
+    with pytest.raises(tk.TileinkError, match="whose surface reaches past"):
         renderer.upload(c)
     compare_frame(renderer, filter_scene(2, [(N.FILTER_OFFSET, (5.0, 5.0))], (10.0, 10.0, 50.0, 50.0)))

@@ -96,14 +96,19 @@ PROGRESSIVE_BALANCED, PROGRESSIVE_HIGH = 0, 1
 OP_PROGRESSIVE_BEGIN = 3
 OP_FILTER_BEGIN = 4
 FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<i4"), ("dy", "<i4"), ("color", "<u4"),
-                         ("std_dev", "<f4"), ("matrix", "<f4", (20,))])
+                         ("std_dev", "<f4"), ("matrix", "<f4", (20,)), ("columns", "<u4"), ("rows", "<u4"),
+                         ("target_x", "<u4"), ("target_y", "<u4"), ("edge_mode", "<u4"), ("preserve_alpha", "<u4"),
+                         ("divisor", "<f4"), ("bias", "<f4")])
 CANVAS_FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<f4"), ("dy", "<f4"),
                                 ("rgba", "<f4", (4,)), ("std_dev", "<f4"), ("matrix", "<f4", (20,)),
-                                ("table", "<u8")], align=True)
+                                ("table", "<u8"), ("kernel", "<u8"), ("columns", "<u4"), ("rows", "<u4"),
+                                ("target_x", "<u4"), ("target_y", "<u4"), ("edge_mode", "<u4"),
+                                ("preserve_alpha", "<u4"), ("divisor", "<f4"), ("bias", "<f4")], align=True)
 FILTER_LAYER_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4"), ("surface", "<i4", (4,))])
 (FILTER_BRIGHTNESS, FILTER_CONTRAST, FILTER_GRAYSCALE, FILTER_HUE_ROTATE, FILTER_INVERT, FILTER_OPACITY,
  FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET, FILTER_ERODE, FILTER_DILATE, FILTER_FLOOD,
- FILTER_DROP_SHADOW, FILTER_COMPONENT_TRANSFER) = range(1, 16)
+ FILTER_DROP_SHADOW, FILTER_COMPONENT_TRANSFER, FILTER_CONVOLVE) = range(1, 17)
+CONVOLVE_EDGE_NONE, CONVOLVE_EDGE_DUPLICATE, CONVOLVE_EDGE_WRAP = 0, 1, 2
 TRANSFER_TABLE_WORDS = 1024
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2
 GLYPH_LINEAR_MASK, GLYPH_LINEAR_COLOR, GLYPH_LINEAR_SUBPIXEL_MASK = 3, 4, 5
@@ -140,8 +145,8 @@ class SceneDesc(C.Structure):
         ("glyph_image_count", C.c_uint32), ("glyph_reserved", C.c_uint32), ("glyph_texel_count", C.c_uint64),
         ("progressive_blurs", C.c_void_p), ("progressive_count", C.c_uint32), ("progressive_reserved", C.c_uint32),
         ("filter_layers", C.c_void_p), ("filters", C.c_void_p), ("filter_layer_count", C.c_uint32),
-        ("filter_count", C.c_uint32), ("transfer_tables", C.c_void_p), ("transfer_table_count", C.c_uint32),
-        ("transfer_reserved", C.c_uint32),
+        ("filter_count", C.c_uint32), ("filter_words", C.c_void_p), ("filter_word_count", C.c_uint32),
+        ("filter_reserved", C.c_uint32),
     ]
 
 
@@ -382,7 +387,7 @@ def desc_to_arrays(d: SceneDesc) -> dict:
         "progressive": arr(d.progressive_blurs, d.progressive_count, PROGRESSIVE_DTYPE),
         "filter_layers": arr(d.filter_layers, d.filter_layer_count, FILTER_LAYER_DTYPE),
         "filters": arr(d.filters, d.filter_count, FILTER_DTYPE),
-        "transfer_tables": arr(d.transfer_tables, d.transfer_table_count * TRANSFER_TABLE_WORDS, np.uint32),
+        "filter_words": arr(d.filter_words, d.filter_word_count, np.uint32),
     }
 
 
@@ -415,9 +420,9 @@ class ArrayScene:
             if v is not None and len(v):
                 setattr(d, "progressive_blurs" if key == "progressive" else key, ptr(v))
                 setattr(d, cnt, len(v))
-        tables = a.get("transfer_tables")
-        if tables is not None and len(tables):
-            d.transfer_tables, d.transfer_table_count = ptr(tables), len(tables) // TRANSFER_TABLE_WORDS
+        words = a.get("filter_words")
+        if words is not None and len(words):
+            d.filter_words, d.filter_word_count = ptr(words), len(words)
         images = [np.ascontiguousarray(im, dtype=np.uint32) for im in a.get("images", [])]
         if images:
             self._images = images

@@ -459,7 +459,9 @@ class Canvas:
         (radius_x, radius_y) for FILTER_ERODE / FILTER_DILATE, a straight
         (r, g, b, a) for FILTER_FLOOD, (dx, dy, std_dev, (r, g, b, a)) for
         FILTER_DROP_SHADOW, 1024 bytes (R, G, B, A tables of 256) for
-        FILTER_COMPONENT_TRANSFER.
+        FILTER_COMPONENT_TRANSFER, {"kernel": rows x columns floats, "target",
+        "divisor", "bias", "edge_mode", "preserve_alpha"} for FILTER_CONVOLVE
+        (defaults: the centre, the kernel's sum or 1, 0, duplicate, False).
         `rect` = (x0, y0, x1, y1) in logical units."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
         keep = []  # the transfer tables, alive for the call (the canvas copies them)
@@ -478,6 +480,18 @@ class Canvas:
                 table = np.ascontiguousarray(np.asarray(value, dtype=np.uint32).reshape(N.TRANSFER_TABLE_WORDS))
                 keep.append(table)
                 chain[k]["table"] = table.ctypes.data
+            elif kind == N.FILTER_CONVOLVE:
+                kern = np.ascontiguousarray(np.asarray(value["kernel"], dtype=np.float32))
+                keep.append(kern)
+                rows, cols = kern.shape
+                chain[k]["kernel"] = kern.ctypes.data
+                chain[k]["columns"], chain[k]["rows"] = cols, rows
+                chain[k]["target_x"] = value.get("target", (cols // 2, rows // 2))[0]
+                chain[k]["target_y"] = value.get("target", (cols // 2, rows // 2))[1]
+                chain[k]["edge_mode"] = value.get("edge_mode", N.CONVOLVE_EDGE_DUPLICATE)
+                chain[k]["preserve_alpha"] = 1 if value.get("preserve_alpha", False) else 0
+                chain[k]["divisor"] = value.get("divisor", float(kern.sum()) or 1.0)
+                chain[k]["bias"] = value.get("bias", 0.0)
             else:
                 chain[k]["amount"] = value
         r = np.asarray(rect, dtype=np.float64).reshape(4)

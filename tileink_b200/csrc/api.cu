@@ -195,7 +195,7 @@ struct tk_ctx {
     DBuf<tk_glyph> glyphs;
     DBuf<tk_glyph_image> glyph_images;
     DBuf<uint32_t> glyph_texels;
-    DBuf<uint32_t> transfer_tables;  // component transfer tables of filter layers
+    DBuf<uint32_t> filter_words;  // filter layers' transfer tables and convolution kernels
     DBuf<tk_layer_record> layers;
     DBuf<tk::ScanItem> items;
     DBuf<unsigned long long> item_desc, tile_desc, stats;
@@ -518,14 +518,23 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             bool spatial = false, shadow = false;
             for (uint32_t k = L.first; k < L.first + L.count; ++k) {
                 const tk_filter& f = d.filters[k];
-                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_COMPONENT_TRANSFER || !std::isfinite(f.amount))
+                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_CONVOLVE || !std::isfinite(f.amount))
                     invalid("filter " + std::to_string(k) + ": bad kind or amount");
                 if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
-                    if (f.color >= d.transfer_table_count || !d.transfer_tables)
-                        invalid("filter " + std::to_string(k) + ": transfer table out of range");
-                    const uint32_t* t = d.transfer_tables + uint64_t(f.color) * TK_TRANSFER_TABLE_WORDS;
+                    if (uint64_t(f.color) + TK_TRANSFER_TABLE_WORDS > d.filter_word_count || !d.filter_words)
+                        invalid("filter " + std::to_string(k) + ": transfer table outside the filter words");
+                    const uint32_t* t = d.filter_words + f.color;
                     for (uint32_t e = 0; e < TK_TRANSFER_TABLE_WORDS; ++e)
                         if (t[e] > 255u) invalid("filter " + std::to_string(k) + ": transfer table entry above 255");
+                }
+                if (f.kind == TK_FILTER_CONVOLVE) {
+                    const uint64_t taps = uint64_t(f.columns) * f.rows;
+                    if (taps > TK_CONVOLVE_MAX_TAPS || f.edge_mode > TK_CONVOLVE_EDGE_WRAP || f.preserve_alpha > 1u ||
+                        !std::isfinite(f.divisor) || !std::isfinite(f.bias) ||
+                        (taps && (f.target_x >= f.columns || f.target_y >= f.rows)) ||
+                        (taps && (uint64_t(f.color) + taps > d.filter_word_count || !d.filter_words)))
+                        invalid("filter " + std::to_string(k) + ": bad convolution kernel");
+                    if (taps) spatial = true;
                 }
                 if (f.kind == TK_FILTER_DROP_SHADOW) {
                     if (!(f.std_dev >= 0.0f && f.std_dev <= 1.0e4f) || f.dx < -1000000 || f.dx > 1000000 ||
@@ -549,8 +558,8 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             // canvas, so those layers are refused.
             if (spatial && (L.surface[0] < 0 || L.surface[1] < 0 || L.surface[2] > int64_t(d.width) ||
                             L.surface[3] > int64_t(d.height)))
-                invalid("an offset, morphology or drop shadow filter layer whose surface reaches past the canvas is "
-                        "outside this path");
+                invalid("an offset, morphology, drop shadow or convolution filter layer whose surface reaches past "
+                        "the canvas is outside this path");
             s.shadow = shadow;
             c->steps.push_back(std::move(s));
             ++depth;
@@ -790,7 +799,7 @@ void do_upload(tk_ctx* c, const tk_scene_desc& scene, const tk_flatten_desc* fl 
         upload(c->glyphs, d.glyphs, d.glyph_count, cs);
         upload(c->glyph_images, d.glyph_images, d.glyph_image_count, cs);
         upload(c->glyph_texels, d.glyph_texels, d.glyph_texel_count, cs);
-        upload(c->transfer_tables, d.transfer_tables, uint64_t(d.transfer_table_count) * TK_TRANSFER_TABLE_WORDS, cs);
+        upload(c->filter_words, d.filter_words, d.filter_word_count, cs);
         TK_CUDA(cudaEventRecord(c->ev_copy, cs));
     };
     upload(c->paths, d.paths, d.path_count, st);
@@ -1098,7 +1107,7 @@ void do_render(tk_ctx* c) {
             if (b.filter) {
                 // the chain over the layer's bounds (render/filter_program/effects.rs:3-268)
                 if (ob[2] > ob[0] && ob[3] > ob[1])
-                    tk::launch_filter_chain(surf, c->temp.ptr, b.shadow ? c->low.ptr : nullptr, c->transfer_tables.ptr,
+                    tk::launch_filter_chain(surf, c->temp.ptr, b.shadow ? c->low.ptr : nullptr, c->filter_words.ptr,
                                             c->width, c->height, ob, b.chain.data(), uint32_t(b.chain.size()), st);
             } else if (b.progressive) {
                 // Filter::ProgressiveBlur over the output bounds

@@ -381,7 +381,7 @@ struct RecCmd {
         FILL, STROKE, CLIP, BLUR, POP, SDF, SDF_CLIP, IMAGE, OPACITY, GLYPHS, GLYPH_RUN, PROGRESSIVE, FILTER
     } kind = FILL;
     // FILTER: the chain as recorded (logical units), the region in shape.p0 /
-    // p1, and the chain's component transfer tables in chain order
+    // p1, and the chain's transfer tables and kernels (f32 bits) in chain order
     std::vector<tk_canvas_filter> chain;
     std::vector<uint32_t> tables;
     bool fixed = false;
@@ -448,7 +448,7 @@ struct tk_canvas {
     std::vector<tk_progressive_blur> progressive;  // device-pixel progressive blurs
     std::vector<tk_filter_layer> filter_layers;    // filter layers and their chains' filters
     std::vector<tk_filter> filters;
-    std::vector<uint32_t> transfer;                // component transfer tables
+    std::vector<uint32_t> filter_words;            // transfer tables and convolution kernels
     uint32_t backdrop_pool = 0, tile_cnt = 0;
     std::vector<std::vector<Cmd>> lists{std::vector<Cmd>{}};
     std::vector<uint32_t> stack{0};
@@ -1592,21 +1592,43 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
     // canvas; filter_offset_to_pixel_delta (filter.rs:490-494) rounds them to
     // whole pixels; filter_outset (filter.rs:533-575) sums the chain's reach
     std::vector<tk_filter> chain(count);
-    std::vector<uint32_t> tables;  // the chain's component transfer tables
+    std::vector<uint32_t> words;  // the chain's transfer tables and convolution kernels
     uint64_t reach = 0;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_canvas_filter& f = filters[k];
         tk_filter& g = chain[k];
         g = tk_filter{};
         g.kind = f.kind;
-        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_COMPONENT_TRANSFER || !std::isfinite(f.amount))
-            return -1;
+        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_CONVOLVE || !std::isfinite(f.amount)) return -1;
         if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
             if (!f.table) return -1;
             for (uint32_t k2 = 0; k2 < TK_TRANSFER_TABLE_WORDS; ++k2)
                 if (f.table[k2] > 255u) return -1;
-            g.color = uint32_t(tables.size() / TK_TRANSFER_TABLE_WORDS + c->transfer.size() / TK_TRANSFER_TABLE_WORDS);
-            tables.insert(tables.end(), f.table, f.table + TK_TRANSFER_TABLE_WORDS);
+            g.color = uint32_t(c->filter_words.size() + words.size());
+            words.insert(words.end(), f.table, f.table + TK_TRANSFER_TABLE_WORDS);
+        }
+        if (f.kind == TK_FILTER_CONVOLVE) {
+            // ConvolveMatrix (filter.rs:611-628): the kernel copied as f32 bits
+            const uint64_t taps = uint64_t(f.columns) * f.rows;
+            if (taps > TK_CONVOLVE_MAX_TAPS || (taps && !f.kernel) || f.edge_mode > TK_CONVOLVE_EDGE_WRAP ||
+                !std::isfinite(f.divisor) || !std::isfinite(f.bias) || (taps && (f.target_x >= f.columns ||
+                                                                                f.target_y >= f.rows)))
+                return -1;
+            g.color = uint32_t(c->filter_words.size() + words.size());
+            for (uint64_t t = 0; t < taps; ++t) {
+                if (!std::isfinite(f.kernel[t])) return -1;
+                uint32_t w;
+                std::memcpy(&w, &f.kernel[t], 4);
+                words.push_back(w);
+            }
+            g.columns = f.columns;
+            g.rows = f.rows;
+            g.target_x = f.target_x;
+            g.target_y = f.target_y;
+            g.edge_mode = f.edge_mode;
+            g.preserve_alpha = f.preserve_alpha ? 1u : 0u;
+            g.divisor = f.divisor;
+            g.bias = f.bias;
         }
         if (f.kind == TK_FILTER_FLOOD || f.kind == TK_FILTER_DROP_SHADOW) {
             for (float v : f.rgba)
@@ -1659,7 +1681,7 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
     L.surface[2] = int32_t(std::min(b[2] + r, 2147483647.0));
     L.surface[3] = int32_t(std::min(b[3] + r, 2147483647.0));
     c->filters.insert(c->filters.end(), chain.begin(), chain.end());
-    c->transfer.insert(c->transfer.end(), tables.begin(), tables.end());
+    c->filter_words.insert(c->filter_words.end(), words.begin(), words.end());
     const uint32_t child = uint32_t(c->lists.size());
     c->lists.emplace_back();
     Cmd cmd{Cmd::BLUR, 0u, 0.0f, child, 0u};
@@ -1671,11 +1693,18 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
     if (c->keep) {
         RecCmd rc = rec_cmd(RecCmd::FILTER, nullptr, nullptr, nullptr);
         rc.chain.assign(filters, filters + count);
-        // the recorded tables point into this canvas's own copies
+        // the recorded tables and kernels point into this canvas's own copies
         rc.tables.clear();
-        for (uint32_t k = 0; k < count; ++k)
+        for (uint32_t k = 0; k < count; ++k) {
             if (filters[k].kind == TK_FILTER_COMPONENT_TRANSFER)
                 rc.tables.insert(rc.tables.end(), filters[k].table, filters[k].table + TK_TRANSFER_TABLE_WORDS);
+            if (filters[k].kind == TK_FILTER_CONVOLVE)
+                for (uint64_t t = 0; t < uint64_t(filters[k].columns) * filters[k].rows; ++t) {
+                    uint32_t w;
+                    std::memcpy(&w, &filters[k].kernel[t], 4);
+                    rc.tables.push_back(w);
+                }
+        }
         rc.fixed = fixed_region != 0;
         rc.shape.p0[0] = rect[0];
         rc.shape.p0[1] = rect[1];
@@ -1778,8 +1807,8 @@ int32_t tk_canvas_scene(tk_canvas* c, tk_scene_desc* out) {
     out->filter_layer_count = uint32_t(c->filter_layers.size());
     out->filters = c->filters.data();
     out->filter_count = uint32_t(c->filters.size());
-    out->transfer_tables = c->transfer.data();
-    out->transfer_table_count = uint32_t(c->transfer.size() / TK_TRANSFER_TABLE_WORDS);
+    out->filter_words = c->filter_words.data();
+    out->filter_word_count = uint32_t(c->filter_words.size());
     out->layers = c->layers.data();
     out->layer_count = uint32_t(c->layers.size());
     out->draw_order = c->order.data();
@@ -2296,11 +2325,16 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
             }
             std::vector<tk_canvas_filter> chain = r.chain;
             size_t t = 0;
-            for (tk_canvas_filter& f : chain)
+            for (tk_canvas_filter& f : chain) {
                 if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
                     f.table = r.tables.data() + t;
                     t += TK_TRANSFER_TABLE_WORDS;
                 }
+                if (f.kind == TK_FILTER_CONVOLVE) {
+                    f.kernel = reinterpret_cast<const float*>(r.tables.data() + t);
+                    t += size_t(f.columns) * f.rows;
+                }
+            }
             return tk_canvas_push_filter_layer(dst, chain.data(), uint32_t(chain.size()), rect, r.fixed ? 1 : 0);
         }
         case RecCmd::POP: return tk_canvas_pop_layer(dst);

@@ -19,6 +19,10 @@
 //   size clears the bounds (render/filter_program/effects.rs:169-221).
 // * Component transfer: each channel's table at its straight byte
 //   (filter_transfer_pixel, filter/transfer.hlsli:5-19).
+// * Convolution (filter_convolve_pixel, filter/convolve.hlsli:34-98): the
+//   flipped kernel over the bounds with their edge mode, premultiplied taps
+//   (straight with preserve_alpha), alpha in byte units, the divisor's
+//   subnormal and huge ranges rescaled by 2^24, bias on the unbounded alpha.
 // * Flood: the bounds filled with the solid colour (filter_flood_region,
 //   filter/brush.hlsl:19-26).
 // * Drop shadow (render/filter_program/shadow.rs:3-52): the source alpha
@@ -288,6 +292,115 @@ __global__ void k_shadow_composite(uint32_t* surface, const uint32_t* __restrict
     }
 }
 
+// --- filter/convolve.hlsli:9-98 ----------------------------------------------
+__device__ __forceinline__ int32_t conv_wrap(int32_t c, int32_t origin, int32_t len) {
+    const int32_t r = (c - origin) % len;
+    return origin + (r < 0 ? r + len : r);
+}
+// value x 2^24 through the exponent bits (subnormals scaled exactly)
+__device__ __forceinline__ float conv_scale_24(float v) {
+    const uint32_t bits = __float_as_uint(v), mag = bits & 0x7fffffffu, e = mag >> 23;
+    if (e == 0u) {
+        const float s = float(mag) * __uint_as_float(0x01000000u);
+        return (bits & 0x80000000u) ? -s : s;
+    }
+    if (e >= 231u) return __uint_as_float((bits & 0x80000000u) | 0x7f800000u);
+    return __uint_as_float(bits + (24u << 23));
+}
+__device__ __forceinline__ float conv_unscale_24(float v) {
+    const uint32_t bits = __float_as_uint(v), e = (bits & 0x7fffffffu) >> 23;
+    if (e <= 24u) return 0.0f;
+    return __uint_as_float(bits - (24u << 23));
+}
+
+struct ConvArgs {
+    const float* kernel;
+    uint32_t columns, rows, target_x, target_y, edge_mode, preserve_alpha;
+    float divisor, bias;
+};
+
+__global__ void k_filter_convolve(const uint32_t* __restrict__ src, uint32_t* __restrict__ dst, uint32_t width, int4 b,
+                                  ConvArgs k) {
+    const uint32_t w = uint32_t(b.z - b.x);
+    const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
+    const uint32_t dmag = __float_as_uint(k.divisor) & 0x7fffffffu;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const int32_t x = b.x + int32_t(i % w), y = b.y + int32_t(i / w);
+        const uint64_t o = uint64_t(y) * width + uint64_t(x);
+        const uint32_t center = src[o];
+        if (k.columns == 0u || k.rows == 0u || dmag == 0u) {
+            dst[o] = center;
+            continue;
+        }
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+        for (uint32_t ky = 0; ky < k.rows; ++ky)
+            for (uint32_t kx = 0; kx < k.columns; ++kx) {
+                const float wt = __ldg(k.kernel + (k.rows - 1u - ky) * k.columns + (k.columns - 1u - kx));
+                int32_t px = x + int32_t(kx) - int32_t(k.target_x), py = y + int32_t(ky) - int32_t(k.target_y);
+                uint32_t p = 0u;
+                if (k.edge_mode == TK_CONVOLVE_EDGE_DUPLICATE) {
+                    px = min(max(px, b.x), b.z - 1);
+                    py = min(max(py, b.y), b.w - 1);
+                    p = src[uint64_t(py) * width + uint64_t(px)];
+                } else if (k.edge_mode == TK_CONVOLVE_EDGE_WRAP) {
+                    px = conv_wrap(px, b.x, b.z - b.x);
+                    py = conv_wrap(py, b.y, b.w - b.y);
+                    p = src[uint64_t(py) * width + uint64_t(px)];
+                } else if (px >= b.x && py >= b.y && px < b.z && py < b.w) {
+                    p = src[uint64_t(py) * width + uint64_t(px)];
+                }
+                const uint32_t al = p >> 24;
+                float4 v = rgba8_to_unorm(p);
+                if (k.preserve_alpha) {
+                    v.x = al == 0u ? 0.0f : v.x / v.w;
+                    v.y = al == 0u ? 0.0f : v.y / v.w;
+                    v.z = al == 0u ? 0.0f : v.z / v.w;
+                }
+                v.w = float(al);
+                s0 = mad(v.x, wt, s0);
+                s1 = mad(v.y, wt, s1);
+                s2 = mad(v.z, wt, s2);
+                s3 = mad(v.w, wt, s3);
+            }
+        float q0, q1, q2, qa;
+        if (dmag < 0x00800000u) {  // subnormal divisor: both sides scaled by 2^24
+            float sd = float(dmag) * __uint_as_float(0x01000000u);
+            if (__float_as_uint(k.divisor) & 0x80000000u) sd = -sd;
+            q0 = conv_scale_24(s0) / sd;
+            q1 = conv_scale_24(s1) / sd;
+            q2 = conv_scale_24(s2) / sd;
+            qa = conv_scale_24(s3) / (sd * 255.0f);
+        } else if (dmag > 0x7e800000u) {  // huge divisor: both sides reduced by 2^24
+            const float inv = 1.0f / conv_unscale_24(k.divisor);
+            q0 = conv_unscale_24(s0) * inv;
+            q1 = conv_unscale_24(s1) * inv;
+            q2 = conv_unscale_24(s2) * inv;
+            qa = conv_unscale_24(s3) * inv * CHANNEL_SCALE;
+        } else {
+            const float rc = 1.0f / k.divisor;
+            q0 = s0 * rc;
+            q1 = s1 * rc;
+            q2 = s2 * rc;
+            qa = (s3 * rc) * CHANNEL_SCALE;
+        }
+        const float ua = k.preserve_alpha ? float(center >> 24) * CHANNEL_SCALE : qa + k.bias;
+        const float a = clampf(ua, 0.0f, 1.0f);
+        const float bb = k.bias * ua;
+        float c0 = q0 + bb, c1 = q1 + bb, c2 = q2 + bb;
+        if (k.preserve_alpha) {
+            c0 = clampf(c0, 0.0f, 1.0f) * a;
+            c1 = clampf(c1, 0.0f, 1.0f) * a;
+            c2 = clampf(c2, 0.0f, 1.0f) * a;
+        } else {
+            c0 = clampf(c0, 0.0f, a);
+            c1 = clampf(c1, 0.0f, a);
+            c2 = clampf(c2, 0.0f, a);
+        }
+        dst[o] = pack4(f2u(clampf(c0, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(c1, 0.0f, 1.0f) * 255.0f + 0.5f),
+                       f2u(clampf(c2, 0.0f, 1.0f) * 255.0f + 0.5f), f2u(clampf(a, 0.0f, 1.0f) * 255.0f + 0.5f));
+    }
+}
+
 unsigned filter_grid(uint64_t n) {
     const uint64_t g = (n + 255) / 256;
     return unsigned(g < 148ull * 32 ? (g ? g : 1) : 148ull * 32);
@@ -306,6 +419,12 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, con
         if (f.kind == TK_FILTER_OFFSET) {
             if (f.dx == 0 && f.dy == 0) continue;
             k_filter_offset<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
+            k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+        } else if (f.kind == TK_FILTER_CONVOLVE) {
+            // ConvolveMatrixToTarget into the scratch surface, copied back (effects.rs:115-133)
+            const ConvArgs a{reinterpret_cast<const float*>(tables + f.color), f.columns, f.rows, f.target_x,
+                             f.target_y, f.edge_mode, f.preserve_alpha, f.divisor, f.bias};
+            k_filter_convolve<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, a);
             k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
         } else if (f.kind == TK_FILTER_FLOOD) {
             k_filter_fill<<<filter_grid(n), 256, 0, st>>>(surface, width, b, f.color);
@@ -347,7 +466,7 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, con
         } else {
             FilterArgs a{f.kind, f.amount, {}, nullptr};
             for (int m = 0; m < 20; ++m) a.m[m] = f.matrix[m];
-            if (f.kind == TK_FILTER_COMPONENT_TRANSFER) a.table = tables + uint64_t(f.color) * TK_TRANSFER_TABLE_WORDS;
+            if (f.kind == TK_FILTER_COMPONENT_TRANSFER) a.table = tables + f.color;
             k_filter_color<<<filter_grid(n), 256, 0, st>>>(surface, width, b, a);
         }
     }
