@@ -220,6 +220,12 @@ typedef struct tk_canvas_filter {
  * Returns -1 for an unknown kind or a non-finite value. */
 int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double rect[4],
                                     int32_t fixed_region);
+/* The same with a Region::Path sample region: the region's bounds are the
+ * tight box of `path` under `transform` (may be null) and the canvas scale.
+ * Corner radii of a rect region do not change its bounds, so a rounded rect
+ * region is its rect. */
+int32_t tk_canvas_push_filter_layer_path(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count,
+                                         const tk_path* path, const double* transform, int32_t fixed_region);
 /* Canvas::push_opacity_layer (src/canvas/layers.rs:122-140): the children
  * until the matching pop are composited at `opacity` (clamped to [0, 1],
  * stored as opacity_f32_to_u8) through the nonzero coverage of `path`. The

@@ -446,3 +446,30 @@ def test_convolution_identity_and_divisor_ranges():
                           np.float32(16.0) * huge, 0.0, 1, False)
     assert np.array_equal(big, base)
 
+
+def test_path_regions_and_transformed_replay():
+    # a path region's bounds are its tight box under the transform and scale
+    c = tk.Canvas(128, 96, scale=2.0)
+    circle = tk.BezPath().move_to(30, 20)
+    circle.cubic_to(30, 25.5, 25.5, 30, 20, 30).cubic_to(14.5, 30, 10, 25.5, 10, 20)
+    circle.cubic_to(10, 14.5, 14.5, 10, 20, 10).cubic_to(25.5, 10, 30, 14.5, 30, 20).close()
+    c.push_filter_layer([(N.FILTER_INVERT, 1.0)], circle, transform=(1, 0, 0, 1, 3.5, 0))
+    c.pop_layer()
+    L = c.scene_arrays()["filter_layers"][0]
+    # the curve's extrema: x in [13.5, 33.5], y in [10, 30], times the scale 2
+    assert list(L["surface"]) == [27, 20, 67, 60]
+    # a retained node's rect region under a rotation becomes the rotated
+    # rectangle's bounds; under a translation it moves
+    node = tk.Canvas(128, 96)
+    node.keep_commands()
+    node.push_filter_layer([(N.FILTER_GRAYSCALE, 1.0)], (10.0, 10.0, 30.0, 20.0))
+    node.push_path(tk.BezPath().move_to(12, 12).line_to(28, 12).line_to(28, 18).close(), tk.Brush.solid(1, 0, 0, 1))
+    node.pop_layer()
+    rs = tk.RetainedScene(128, 96)
+    rs.insert(1, node, transform=(0.0, 1.0, -1.0, 0.0, 60.0, 0.0))  # x' = 60 - y, y' = x
+    canvas, _ = rs.materialize()
+    assert list(canvas.scene_arrays()["filter_layers"][0]["surface"]) == [40, 10, 50, 30]
+    rs.set_transform(1, (1.0, 0.0, 0.0, 1.0, 5.0, 7.0))
+    canvas, _ = rs.materialize()
+    assert list(canvas.scene_arrays()["filter_layers"][0]["surface"]) == [15, 17, 35, 27]
+

@@ -142,6 +142,8 @@ def test_gpu_filter_layer_regions(renderer):
     compare_frame(renderer, filter_scene(7, [(N.FILTER_OFFSET, (-9.0, 6.0))], (30.0, 30.0, 120.0, 110.0),
                                          fixed_region=True))
     compare_frame(renderer, filter_scene(8, [(N.FILTER_HUE_ROTATE, 90.0)], (50.0, 50.0, 50.0, 90.0)))
+    compare_frame(renderer, filter_scene(12, [(N.FILTER_DILATE, (2.0, 2.0)), (N.FILTER_SEPIA, 1.0)],
+                                         blob(np.random.default_rng(3), 100.0, 75.0, 40.0)))
     rng = np.random.default_rng(9)
     c = tk.Canvas(200, 150)
     c.set_clear_color(0xFF202020)

@@ -314,6 +314,7 @@ def library() -> C.CDLL:
         "tk_canvas_push_glyph_outlines": (I64, [P, P, C.POINTER(BrushDesc), P, F64]),
         "tk_canvas_push_progressive_blur_group": (I32, [P, F64, F64, F64, F64, C.c_float, U32]),
         "tk_canvas_push_filter_layer": (I32, [P, P, U32, P, C.c_int32]),
+        "tk_canvas_push_filter_layer_path": (I32, [P, P, U32, P, P, C.c_int32]),
         "tk_canvas_push_sdf": (I64, [P, C.POINTER(SdfShape), C.POINTER(BrushDesc)]),
         "tk_canvas_push_clip_sdf_layer": (I32, [P, C.POINTER(SdfShape)]),
         "tk_canvas_add_image": (I32, [P, P, U32, U32]),

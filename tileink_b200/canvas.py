@@ -448,7 +448,7 @@ class Canvas:
         if r != 0:
             raise ValueError("bad progressive blur")
 
-    def push_filter_layer(self, filters, rect, fixed_region: bool = False) -> None:
+    def push_filter_layer(self, filters, rect, fixed_region: bool = False, transform=None) -> None:
         """Canvas::push_filter_layer with a chain of filters over a Region::Rect
         sample region (src/canvas/layers.rs:222-233): children until
         pop_layer() are rendered into a surface, filtered in place by each
@@ -462,7 +462,8 @@ class Canvas:
         FILTER_COMPONENT_TRANSFER, {"kernel": rows x columns floats, "target",
         "divisor", "bias", "edge_mode", "preserve_alpha"} for FILTER_CONVOLVE
         (defaults: the centre, the kernel's sum or 1, 0, duplicate, False).
-        `rect` = (x0, y0, x1, y1) in logical units."""
+        `rect` = (x0, y0, x1, y1) in logical units, or a BezPath (a
+        Region::Path, under the optional `transform`)."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
         keep = []  # the transfer tables, alive for the call (the canvas copies them)
         for k, (kind, value) in enumerate(filters):
@@ -494,9 +495,16 @@ class Canvas:
                 chain[k]["bias"] = value.get("bias", 0.0)
             else:
                 chain[k]["amount"] = value
-        r = np.asarray(rect, dtype=np.float64).reshape(4)
-        if self._lib.tk_canvas_push_filter_layer(self._h, N.ptr(chain) if len(chain) else None, len(chain),
-                                                 N.ptr(r), 1 if fixed_region else 0) != 0:
+        if isinstance(rect, BezPath):  # Region::Path (the path's bounds under `transform`)
+            t = None if transform is None else np.asarray(transform, dtype=np.float64).reshape(6)
+            rc = self._lib.tk_canvas_push_filter_layer_path(self._h, N.ptr(chain) if len(chain) else None, len(chain),
+                                                            rect._h, None if t is None else N.ptr(t),
+                                                            1 if fixed_region else 0)
+        else:
+            r = np.asarray(rect, dtype=np.float64).reshape(4)
+            rc = self._lib.tk_canvas_push_filter_layer(self._h, N.ptr(chain) if len(chain) else None, len(chain),
+                                                       N.ptr(r), 1 if fixed_region else 0)
+        if rc != 0:
             raise ValueError("bad filter layer")
 
     def push_blur_group(self, sigma: float, factor: int = 1, downsample: int = N.BLUR_DOWNSAMPLE_BOX,

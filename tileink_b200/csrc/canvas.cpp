@@ -385,6 +385,7 @@ struct RecCmd {
     std::vector<tk_canvas_filter> chain;
     std::vector<uint32_t> tables;
     bool fixed = false;
+    bool region_path = false;  // FILTER: the region is `path` under the transform
     // GLYPH_RUN: the glyphs (image = index into run_images or TK_INVALID_INDEX),
     // their images and the optional clip rect
     std::vector<tk_glyph> run_glyphs;
@@ -1575,19 +1576,23 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
     return 0;
 }
 
-int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double rect[4],
-                                    int32_t fixed_region) {
-    if (!c || (count && !filters) || !rect) return -1;
-    // physical_region (canvas/surface.rs:197-205,370-386), then region_bounds
-    // (shared/layer/filter.rs:578-597): floor / ceil to whole pixels
-    const double s = double(c->scale);
-    double b[4];
+namespace {
+// region_bounds (shared/layer/filter.rs:578-597): a device-space box floored /
+// ceiled to whole pixels (an empty box gives an empty region at the origin)
+bool region_pixel_bounds(double x0, double y0, double x1, double y1, double b[4]) {
+    const double v[4] = {x0, y0, x1, y1};
     for (int k = 0; k < 4; ++k) {
-        const double v = rect[k] * s;
-        if (!std::isfinite(v)) return -1;
-        b[k] = (k < 2) ? std::floor(v) : std::ceil(v);
+        if (!std::isfinite(v[k])) return false;
+        b[k] = (k < 2) ? std::floor(v[k]) : std::ceil(v[k]);
         b[k] = std::min(std::max(b[k], -2147483648.0), 2147483647.0);
     }
+    return true;
+}
+
+// A filter layer over region pixel bounds b: the chain made physical, the
+// surface grown by its reach, the command pushed (recording is the caller's).
+int32_t push_filter_layer_bounds(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double b[4],
+                                 int32_t fixed_region) {
     // physical_filter (canvas/surface.rs:247-326): offsets scale with the
     // canvas; filter_offset_to_pixel_delta (filter.rs:490-494) rounds them to
     // whole pixels; filter_outset (filter.rs:533-575) sums the chain's reach
@@ -1690,6 +1695,18 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
     c->lists[c->stack.back()].push_back(cmd);
     c->stack.push_back(child);
     c->dirty = true;
+    return 0;
+}
+}  // namespace
+
+int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count, const double rect[4],
+                                    int32_t fixed_region) {
+    if (!c || (count && !filters) || !rect) return -1;
+    // physical_region (canvas/surface.rs:197-205,370-386)
+    const double s = double(c->scale);
+    double b[4];
+    if (!region_pixel_bounds(rect[0] * s, rect[1] * s, rect[2] * s, rect[3] * s, b)) return -1;
+    if (push_filter_layer_bounds(c, filters, count, b, fixed_region) != 0) return -1;
     if (c->keep) {
         RecCmd rc = rec_cmd(RecCmd::FILTER, nullptr, nullptr, nullptr);
         rc.chain.assign(filters, filters + count);
@@ -1710,6 +1727,37 @@ int32_t tk_canvas_push_filter_layer(tk_canvas* c, const tk_canvas_filter* filter
         rc.shape.p0[1] = rect[1];
         rc.shape.p1[0] = rect[2];
         rc.shape.p1[1] = rect[3];
+        c->log.push_back(std::move(rc));
+    }
+    return 0;
+}
+
+int32_t tk_canvas_push_filter_layer_path(tk_canvas* c, const tk_canvas_filter* filters, uint32_t count,
+                                         const tk_path* path, const double* transform, int32_t fixed_region) {
+    if (!c || (count && !filters) || !path) return -1;
+    // Region::Path: its bounds are the tight box of the path under the device
+    // transform (physical_region, canvas/surface.rs:376-384; region_bounds)
+    double dev[6];
+    device_transform(c, transform, dev);
+    const Box bb = path_bbox(transform_path(*path, dev));
+    double b[4] = {0.0, 0.0, 0.0, 0.0};
+    if (!bb.empty() && !region_pixel_bounds(bb.x0, bb.y0, bb.x1, bb.y1, b)) return -1;
+    if (push_filter_layer_bounds(c, filters, count, b, fixed_region) != 0) return -1;
+    if (c->keep) {
+        RecCmd rc = rec_cmd(RecCmd::FILTER, path, nullptr, transform);
+        rc.region_path = true;
+        rc.chain.assign(filters, filters + count);
+        rc.fixed = fixed_region != 0;
+        for (uint32_t k = 0; k < count; ++k) {
+            if (filters[k].kind == TK_FILTER_COMPONENT_TRANSFER)
+                rc.tables.insert(rc.tables.end(), filters[k].table, filters[k].table + TK_TRANSFER_TABLE_WORDS);
+            if (filters[k].kind == TK_FILTER_CONVOLVE)
+                for (uint64_t t = 0; t < uint64_t(filters[k].columns) * filters[k].rows; ++t) {
+                    uint32_t w;
+                    std::memcpy(&w, &filters[k].kernel[t], 4);
+                    rc.tables.push_back(w);
+                }
+        }
         c->log.push_back(std::move(rc));
     }
     return 0;
@@ -2314,26 +2362,42 @@ int32_t replay_one(tk_canvas* dst, const RecCmd& r, const double* node_t) {
                                                          r.sampling);
         }
         case RecCmd::FILTER: {
-            // the region moves with a translation (effect_placement.rs:57-75)
+            // a rect region moves with a translation; under any other
+            // transform it becomes the transformed rectangle path, and a path
+            // region composes the transform (effect_placement.rs:57-118)
             double rect[4] = {r.shape.p0[0], r.shape.p0[1], r.shape.p1[0], r.shape.p1[1]};
-            if (t) {
-                if (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0) return -1;
+            const bool moved = t && (t[0] != 1.0 || t[1] != 0.0 || t[2] != 0.0 || t[3] != 1.0);
+            if (t && !moved) {
                 rect[0] += t[4];
                 rect[1] += t[5];
                 rect[2] += t[4];
                 rect[3] += t[5];
             }
             std::vector<tk_canvas_filter> chain = r.chain;
-            size_t t = 0;
+            size_t word = 0;
             for (tk_canvas_filter& f : chain) {
                 if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
-                    f.table = r.tables.data() + t;
-                    t += TK_TRANSFER_TABLE_WORDS;
+                    f.table = r.tables.data() + word;
+                    word += TK_TRANSFER_TABLE_WORDS;
                 }
                 if (f.kind == TK_FILTER_CONVOLVE) {
-                    f.kernel = reinterpret_cast<const float*>(r.tables.data() + t);
-                    t += size_t(f.columns) * f.rows;
+                    f.kernel = reinterpret_cast<const float*>(r.tables.data() + word);
+                    word += size_t(f.columns) * f.rows;
                 }
+            }
+            if (r.region_path || moved) {
+                tk_path region;
+                if (r.region_path) {
+                    region = r.path;
+                } else {
+                    region.els.push_back(El{MOVE, {Pt{rect[0], rect[1]}}});
+                    region.els.push_back(El{LINE, {Pt{rect[2], rect[1]}}});
+                    region.els.push_back(El{LINE, {Pt{rect[2], rect[3]}}});
+                    region.els.push_back(El{LINE, {Pt{rect[0], rect[3]}}});
+                    region.els.push_back(El{CLOSE, {}});
+                }
+                return tk_canvas_push_filter_layer_path(dst, chain.data(), uint32_t(chain.size()), &region, t,
+                                                        r.fixed ? 1 : 0);
             }
             return tk_canvas_push_filter_layer(dst, chain.data(), uint32_t(chain.size()), rect, r.fixed ? 1 : 0);
         }
