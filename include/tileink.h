@@ -373,6 +373,10 @@ typedef struct tk_progressive_blur {
 #define TK_CONVOLVE_EDGE_DUPLICATE 1u
 #define TK_CONVOLVE_EDGE_WRAP 2u
 #define TK_CONVOLVE_MAX_TAPS 4096u
+/* Filter::Blur at full resolution inside a chain (render/filter_program/
+ * blur.rs:194-244): std_dev along x, amount along y, each through the blur
+ * groups' Gaussian over the layer's bounds. */
+#define TK_FILTER_BLUR 17u
 typedef struct tk_filter {
     uint32_t kind;
     float amount;      /* the colour filters' argument (hue rotation in degrees) */

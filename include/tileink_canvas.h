@@ -197,7 +197,8 @@ int32_t tk_canvas_push_progressive_blur_group(tk_canvas* c, double start_x, doub
  * TK_FILTER_DROP_SHADOW (dx, dy: the offset, std_dev, rgba) or
  * TK_FILTER_COMPONENT_TRANSFER (table: TK_TRANSFER_TABLE_WORDS words, each
  * 0..255, copied by the call) or TK_FILTER_CONVOLVE (kernel: columns x rows
- * floats, copied; target, divisor, bias, edge_mode, preserve_alpha). */
+ * floats, copied; target, divisor, bias, edge_mode, preserve_alpha) or
+ * TK_FILTER_BLUR (dx, dy: the standard deviations along x and y). */
 typedef struct tk_canvas_filter {
     uint32_t kind;
     float amount;

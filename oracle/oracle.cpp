@@ -2182,7 +2182,21 @@ void filter_chain(uint32_t* surface, uint32_t width, const int32_t b[4], const t
     if (b[2] <= b[0] || b[3] <= b[1]) return;
     for (uint32_t k = 0; k < count; ++k) {
         const tk_filter& f = chain[k];
-        if (f.kind == TK_FILTER_CONVOLVE) {  // into a scratch copy, then back (effects.rs:115-133)
+        if (f.kind == TK_FILTER_BLUR) {  // apply_blur at full resolution (blur.rs:194-244)
+            const float sx = fmax_(f.std_dev, 0.0f), sy = fmax_(f.amount, 0.0f);
+            if (sx <= 0.0f && sy <= 0.0f) continue;
+            std::vector<uint32_t> temp(size_t(width) * size_t(b[3]), 0u);
+            const uint32_t region[4] = {uint32_t(b[0]), uint32_t(b[1]), uint32_t(b[2] - b[0]), uint32_t(b[3] - b[1])};
+            const uint32_t none[4] = {0, 0, 0, 0};
+            const uint32_t h = uint32_t(b[3]);
+            blur_pass(surface, temp.data(), width, h, region, none, sx > 0.0f ? sx : sy, sx > 0.0f ? 0u : 1u, 1);
+            if (sx > 0.0f && sy > 0.0f) {
+                blur_pass(temp.data(), surface, width, h, region, none, sy, 1, 1);
+            } else {
+                for (int32_t y = b[1]; y < b[3]; ++y)
+                    for (int32_t x = b[0]; x < b[2]; ++x) surface[size_t(y) * width + x] = temp[size_t(y) * width + x];
+            }
+        } else if (f.kind == TK_FILTER_CONVOLVE) {  // into a scratch copy, then back (effects.rs:115-133)
             std::vector<uint32_t> temp(size_t(width) * size_t(b[3]), 0u);
             float* kernel = nullptr;
             std::vector<float> kv(size_t(f.columns) * f.rows);

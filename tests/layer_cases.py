@@ -183,4 +183,6 @@ def filter_chains():
                                                    "target": (3, 0), "divisor": 6.5, "bias": -0.1,
                                                    "edge_mode": N.CONVOLVE_EDGE_NONE, "preserve_alpha": True}),
                               (N.FILTER_OPACITY, 0.9)],
+        "blur_xy": [(N.FILTER_BLUR, (2.5, 6.0)), (N.FILTER_CONTRAST, 1.3)],
+        "blur_x_only": [(N.FILTER_SATURATE, 0.4), (N.FILTER_BLUR, (7.0, 0.0))],
     }

@@ -473,3 +473,37 @@ def test_path_regions_and_transformed_replay():
     canvas, _ = rs.materialize()
     assert list(canvas.scene_arrays()["filter_layers"][0]["surface"]) == [15, 17, 35, 27]
 
+
+def test_chain_blur_equals_a_blur_group_over_the_canvas():
+    """Filter::Blur in a chain over a region covering the canvas blurs what a
+    blur group of the same deviation blurs (both over the whole canvas)."""
+    def scene(as_filter):
+        from layer_cases import blob
+        rng = np.random.default_rng(5)
+        c = tk.Canvas(96, 72)
+        c.set_clear_color(0xFFFFFFFF)
+        if as_filter:
+            c.push_filter_layer([(N.FILTER_BLUR, (3.0, 3.0))], (0.0, 0.0, 96.0, 72.0))
+        else:
+            c.push_blur_group(3.0)
+        c.push_path(tk.BezPath().move_to(-5, -5).line_to(101, -5).line_to(101, 77).line_to(-5, 77).close(),
+                    tk.Brush.solid(0.2, 0.5, 0.7, 0.6))
+        for _ in range(5):
+            c.push_path(blob(rng, rng.uniform(10, 86), rng.uniform(10, 62), 15), tk.Brush.solid(*rng.uniform(0, 1, 3), 1.0))
+        c.pop_layer()
+        return c
+    a, b = scene(True), scene(False)
+    ia = oracle.OracleRun(a.scene_desc(), threads=2).get(oracle.OR_IMAGE, np.uint32)
+    ib = oracle.OracleRun(b.scene_desc(), threads=2).get(oracle.OR_IMAGE, np.uint32)
+    assert np.array_equal(ia, ib)
+    # one axis only blurs along it: a vertical stripe stays within its
+    # columns, whole away from the top and bottom (transparent beyond them)
+    c = tk.Canvas(40, 30)
+    c.push_filter_layer([(N.FILTER_BLUR, (0.0, 2.0))], (0.0, 0.0, 40.0, 30.0))
+    c.push_path(tk.BezPath().move_to(18, -2).line_to(22, -2).line_to(22, 32).line_to(18, 32).close(),
+                tk.Brush.solid(0, 0, 0, 1))
+    c.pop_layer()
+    img = oracle.OracleRun(c.scene_desc(), threads=1).get(oracle.OR_IMAGE, np.uint32).reshape(30, 40)
+    assert np.all(img[7:23, 18:22] == 0xFF000000) and not img[:, :18].any() and not img[:, 22:].any()
+    assert np.all((img[0, 18:22] >> 24) < 255)
+

@@ -120,7 +120,7 @@ def test_gpu_progressive_blur_matches_oracle(renderer, seed, sigma, quality, uni
                                   "saturate", "sepia", "matrix", "matrix_alpha", "offset", "chain", "erode",
                                   "dilate", "morphology_chain", "flood", "drop_shadow", "drop_shadow_sharp",
                                   "drop_shadow_wide", "component_transfer", "convolve_box", "convolve_edges",
-                                  "convolve_preserve"])
+                                  "convolve_preserve", "blur_xy", "blur_x_only"])
 def test_gpu_filter_layers_match_oracle(renderer, name):
     """Filter layers (Canvas::push_filter_layer with a chain; filter/color.hlsli,
     filter/basic.hlsl): every colour filter, the colour matrix, offsets and a

@@ -107,7 +107,7 @@ CANVAS_FILTER_DTYPE = np.dtype([("kind", "<u4"), ("amount", "<f4"), ("dx", "<f4"
 FILTER_LAYER_DTYPE = np.dtype([("first", "<u4"), ("count", "<u4"), ("surface", "<i4", (4,))])
 (FILTER_BRIGHTNESS, FILTER_CONTRAST, FILTER_GRAYSCALE, FILTER_HUE_ROTATE, FILTER_INVERT, FILTER_OPACITY,
  FILTER_SATURATE, FILTER_SEPIA, FILTER_COLOR_MATRIX, FILTER_OFFSET, FILTER_ERODE, FILTER_DILATE, FILTER_FLOOD,
- FILTER_DROP_SHADOW, FILTER_COMPONENT_TRANSFER, FILTER_CONVOLVE) = range(1, 17)
+ FILTER_DROP_SHADOW, FILTER_COMPONENT_TRANSFER, FILTER_CONVOLVE, FILTER_BLUR) = range(1, 18)
 CONVOLVE_EDGE_NONE, CONVOLVE_EDGE_DUPLICATE, CONVOLVE_EDGE_WRAP = 0, 1, 2
 TRANSFER_TABLE_WORDS = 1024
 GLYPH_MASK, GLYPH_COLOR, GLYPH_SUBPIXEL_MASK = 0, 1, 2

@@ -461,7 +461,8 @@ class Canvas:
         FILTER_DROP_SHADOW, 1024 bytes (R, G, B, A tables of 256) for
         FILTER_COMPONENT_TRANSFER, {"kernel": rows x columns floats, "target",
         "divisor", "bias", "edge_mode", "preserve_alpha"} for FILTER_CONVOLVE
-        (defaults: the centre, the kernel's sum or 1, 0, duplicate, False).
+        (defaults: the centre, the kernel's sum or 1, 0, duplicate, False),
+        (std_dev_x, std_dev_y) for FILTER_BLUR.
         `rect` = (x0, y0, x1, y1) in logical units, or a BezPath (a
         Region::Path, under the optional `transform`)."""
         chain = np.zeros(len(filters), dtype=N.CANVAS_FILTER_DTYPE)
@@ -470,7 +471,7 @@ class Canvas:
             chain[k]["kind"] = kind
             if kind == N.FILTER_COLOR_MATRIX:
                 chain[k]["matrix"] = np.asarray(value, dtype=np.float32).reshape(20)
-            elif kind in (N.FILTER_OFFSET, N.FILTER_ERODE, N.FILTER_DILATE):
+            elif kind in (N.FILTER_OFFSET, N.FILTER_ERODE, N.FILTER_DILATE, N.FILTER_BLUR):
                 chain[k]["dx"], chain[k]["dy"] = value
             elif kind == N.FILTER_FLOOD:
                 chain[k]["rgba"] = value

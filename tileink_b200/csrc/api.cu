@@ -518,7 +518,7 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
             bool spatial = false, shadow = false;
             for (uint32_t k = L.first; k < L.first + L.count; ++k) {
                 const tk_filter& f = d.filters[k];
-                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_CONVOLVE || !std::isfinite(f.amount))
+                if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_BLUR || !std::isfinite(f.amount))
                     invalid("filter " + std::to_string(k) + ": bad kind or amount");
                 if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
                     if (uint64_t(f.color) + TK_TRANSFER_TABLE_WORDS > d.filter_word_count || !d.filter_words)
@@ -526,6 +526,11 @@ void validate_and_plan(tk_ctx* c, const tk_scene_desc& d) {
                     const uint32_t* t = d.filter_words + f.color;
                     for (uint32_t e = 0; e < TK_TRANSFER_TABLE_WORDS; ++e)
                         if (t[e] > 255u) invalid("filter " + std::to_string(k) + ": transfer table entry above 255");
+                }
+                if (f.kind == TK_FILTER_BLUR) {
+                    if (!(f.std_dev >= 0.0f && f.std_dev <= 1.0e4f && f.amount >= 0.0f && f.amount <= 1.0e4f))
+                        invalid("filter " + std::to_string(k) + ": blur deviations outside [0, 1e4]");
+                    if (f.std_dev > 0.0f || f.amount > 0.0f) spatial = true;
                 }
                 if (f.kind == TK_FILTER_CONVOLVE) {
                     const uint64_t taps = uint64_t(f.columns) * f.rows;

@@ -1604,7 +1604,15 @@ int32_t push_filter_layer_bounds(tk_canvas* c, const tk_canvas_filter* filters, 
         tk_filter& g = chain[k];
         g = tk_filter{};
         g.kind = f.kind;
-        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_CONVOLVE || !std::isfinite(f.amount)) return -1;
+        if (f.kind < TK_FILTER_BRIGHTNESS || f.kind > TK_FILTER_BLUR || !std::isfinite(f.amount)) return -1;
+        if (f.kind == TK_FILTER_BLUR) {
+            // Filter::Blur scaled by the canvas (surface.rs:284-292); reach
+            // blur_outset(max(sx, sy)) = ceil(3 max)
+            const float sx = std::max(f.dx * c->scale, 0.0f), sy = std::max(f.dy * c->scale, 0.0f);
+            if (!std::isfinite(sx) || !std::isfinite(sy) || sx > 1.0e4f || sy > 1.0e4f) return -1;
+            g.std_dev = sx;
+            reach += uint64_t(std::ceil(std::max(sx, sy) * 3.0f));
+        }
         if (f.kind == TK_FILTER_COMPONENT_TRANSFER) {
             if (!f.table) return -1;
             for (uint32_t k2 = 0; k2 < TK_TRANSFER_TABLE_WORDS; ++k2)
@@ -1654,7 +1662,7 @@ int32_t push_filter_layer_bounds(tk_canvas* c, const tk_canvas_filter* filters, 
             reach += uint64_t(std::ceil(std::max(sd, 0.0f) * 3.0f)) +
                      uint64_t(std::max(std::ceil(std::fabs(ox)), std::ceil(std::fabs(oy))));
         }
-        g.amount = f.amount;
+        g.amount = f.kind == TK_FILTER_BLUR ? std::max(f.dy * c->scale, 0.0f) : f.amount;  // BLUR: y deviation
         if (f.kind == TK_FILTER_OFFSET) {
             const float dx = f.dx * c->scale, dy = f.dy * c->scale;
             if (!std::isfinite(dx) || !std::isfinite(dy) || std::fabs(dx) > 1.0e6f || std::fabs(dy) > 1.0e6f)

@@ -23,6 +23,8 @@
 //   flipped kernel over the bounds with their edge mode, premultiplied taps
 //   (straight with preserve_alpha), alpha in byte units, the divisor's
 //   subnormal and huge ranges rescaled by 2^24, bias on the unbounded alpha.
+// * Blur: the blur groups' Gaussian over the bounds, with its own deviation
+//   along x and y (render/filter_program/blur.rs:194-244).
 // * Flood: the bounds filled with the solid colour (filter_flood_region,
 //   filter/brush.hlsl:19-26).
 // * Drop shadow (render/filter_program/shadow.rs:3-52): the source alpha
@@ -420,6 +422,32 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, con
             if (f.dx == 0 && f.dy == 0) continue;
             k_filter_offset<<<filter_grid(n), 256, 0, st>>>(surface, temp, width, b, f.dx, f.dy);
             k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+        } else if (f.kind == TK_FILTER_BLUR) {
+            // apply_blur at full resolution (blur.rs:194-244): x into the
+            // scratch surface, then y back, or the one axis and a copy back
+            const float sx = fmaxf(f.std_dev, 0.0f), sy = fmaxf(f.amount, 0.0f);
+            if (sx <= 0.0f && sy <= 0.0f) continue;
+            BlurParams bp{};
+            bp.width = width;
+            bp.height = height;
+            bp.region[0] = uint32_t(b.x);
+            bp.region[1] = uint32_t(b.y);
+            bp.region[2] = uint32_t(b.z - b.x);
+            bp.region[3] = uint32_t(b.w - b.y);
+            bp.bounds[0] = b.x;
+            bp.bounds[1] = b.y;
+            bp.bounds[2] = b.z;
+            bp.bounds[3] = b.w;
+            bp.sigma = sx > 0.0f ? sx : sy;
+            bp.axis = sx > 0.0f ? 0 : 1;
+            launch_blur(surface, temp, bp, st);
+            if (sx > 0.0f && sy > 0.0f) {
+                bp.sigma = sy;
+                bp.axis = 1;
+                launch_blur(temp, surface, bp, st);
+            } else {
+                k_filter_copy<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b);
+            }
         } else if (f.kind == TK_FILTER_CONVOLVE) {
             // ConvolveMatrixToTarget into the scratch surface, copied back (effects.rs:115-133)
             const ConvArgs a{reinterpret_cast<const float*>(tables + f.color), f.columns, f.rows, f.target_x,
