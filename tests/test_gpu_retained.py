@@ -105,6 +105,14 @@ def test_gpu_incremental_fallbacks(renderer):
     assert st["full_redraw"] == 1
     st = renderer.render_incremental({"full": False, "rects": [[0, 0, 16, 16]]})
     assert st["full_redraw"] == 1 and st["reason"] == N.FULL_FILTERS
+    # so do filter layers, and the full redraw is the frame
+    from layer_cases import filter_chains, filter_scene
+    fl = filter_scene(4, filter_chains()["chain"], (30.5, 28.0, 165.2, 117.9))
+    want = renderer.render_to_image(fl).copy()
+    renderer.upload(fl)
+    st = renderer.render_incremental({"full": False, "rects": [[0, 0, 16, 16]]})
+    assert st["full_redraw"] == 1 and st["reason"] == N.FULL_FILTERS
+    assert np.array_equal(renderer.readback().view(np.uint8).reshape(want.shape), want)
     # a new size has no history
     c = tk.generate(1, 2, width=200, height=120, paths=20, device_segment_plan=True)
     renderer.upload(c)
