@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--batch-scenes", type=int, default=512, help="scenes of the batched-mode leg (0: skip)")
     p.add_argument("--incremental-steps", type=int, default=10, help="frames of the incremental leg (0: skip)")
     p.add_argument("--sdf-steps", type=int, default=10, help="frames of the SDF-shape leg (0: skip)")
+    p.add_argument("--filter-steps", type=int, default=10, help="frames of the filter-layer leg (0: skip)")
     p.add_argument("--sdf-shapes", type=int, default=50000, help="shapes of the SDF-shape leg")
     p.add_argument("--sdf-kinds", default="base", choices=["base", "all"],
                    help="SDF-only runs: the base kinds, or all nineteen (the extended-kind kernel instance)")
@@ -460,6 +461,57 @@ def sdf_scene(size, n, seed, kinds="base"):
             c.push_line_shadow(x, y, x + w, y + h, float(rng.uniform(1, 6)), b, offset=(2, 2), expand=3.0,
                                intensity=0.5, cap=N.CAP_ROUND)
     return c
+
+
+def filter_timing(r, size, steps):
+    """A filter layer over the whole canvas (Canvas::push_filter_layer with a
+    chain of grayscale, contrast, a colour matrix and a component transfer)
+    over 400 translucent fills: the group's filter-and-composite stage by
+    CUDA events, against the HBM bytes it must move (8 per pixel for the
+    fused per-pixel chain, 12 per pixel for the composite)."""
+    import tileink_b200 as tk
+    from tileink_b200 import _native as N
+    size = size or 4096
+    rng = np.random.default_rng(SEED + 11)
+    c = tk.Canvas(size, size)
+    c.set_clear_color(0xFFFFFFFF)
+    table = np.concatenate([255 - np.arange(256), np.arange(256), (np.arange(256) ** 2) // 255, np.arange(256)])
+    chain = [(N.FILTER_GRAYSCALE, 0.6), (N.FILTER_CONTRAST, 1.3),
+             (N.FILTER_COLOR_MATRIX, [0.393, 0.769, 0.189, 0, 0, 0.349, 0.686, 0.168, 0, 0, 0.272, 0.534, 0.131, 0, 0,
+                                      0, 0, 0, 1, 0]),
+             (N.FILTER_COMPONENT_TRANSFER, table)]
+    c.push_filter_layer(chain, (0.0, 0.0, float(size), float(size)))
+    for _ in range(400):
+        x0, y0 = rng.uniform(-200, size), rng.uniform(-200, size)
+        w, h = rng.uniform(50, 1200, 2)
+        c.push_path(tk.BezPath().move_to(x0, y0).line_to(x0 + w, y0).line_to(x0 + w, y0 + h).line_to(x0, y0 + h)
+                    .close(), tk.Brush.solid(*rng.uniform(0, 1, 3), float(rng.uniform(0.3, 1.0))))
+    c.pop_layer()
+    r.upload(c)
+    r.set_timing(True)
+    for _ in range(3):
+        r.render()
+    r.synchronize()
+    acc = {}
+    for _ in range(steps):
+        r.render()
+        r.synchronize()
+        for k, v in r.stage_times().items():
+            acc[k] = acc.get(k, 0.0) + v / steps
+    r.set_timing(False)
+    filt_ms = acc["blur"]
+    px = size * size
+    algo = px * (8 + 12)  # the chain's per-pixel filters run fused: one read and one write per pixel
+    hbm = measured_peaks().get("hbm_gbs", 6650.0)
+    return {"workload": f"{size}x{size} canvas, 400 translucent rect fills inside one filter layer over the canvas: "
+                        "grayscale, contrast, colour matrix, component transfer",
+            "frame_ms": sum(acc.values()), "filter_stage_ms": filt_ms, "stage_ms": acc, "steps": steps,
+            "roofline": {"bound": "hbm", "achieved": algo / (filt_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": algo / (filt_ms * 1e-3) / 1e9 / hbm, "algorithmic_bytes": algo,
+                         "bytes_rule": "8 B/px for the fused run of per-pixel filters (read and write the "
+                                       "surface once), 12 B/px for the composite (read the surface, read and "
+                                       "write the target)"},
+            "timing": "device, CUDA events per stage (the filter stage: the chain and the composite)"}
 
 
 def sdf_timing(r, size, steps, cpu, n=50000, kinds="base"):
@@ -873,6 +925,9 @@ def main():
     sdf_line = None
     if rank == 0 and world == 1 and args.sdf_steps > 0:
         sdf_line = sdf_timing(r, args.size, args.sdf_steps, not args.no_cpu_baseline, args.sdf_shapes)
+    filter_line = None
+    if rank == 0 and world == 1 and args.filter_steps > 0:
+        filter_line = filter_timing(r, args.size, args.filter_steps)
     del ps_flat, flat_canvas
     bytes_out = out.nbytes  # the whole frame per step (with N GPUs: every rank's band together)
     if world > 1:
@@ -985,6 +1040,7 @@ def main():
             "batched": batch_line,
             "incremental": inc_line,
             "sdf": sdf_line,
+            "filters": filter_line,
             "configs": configs,
             "scene_generation_s": gen_s,
         }

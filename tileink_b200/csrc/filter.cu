@@ -2,7 +2,9 @@
 // RGBA8 surface filtered in place, one chain filter after another, over the
 // layer's processing bounds (render/filter_program/effects.rs:3-268).
 //
-// * Colour filters and the colour matrix: one thread per pixel, the
+// * Colour filters, the colour matrix and component transfers: one thread
+//   per pixel applying a run of up to eight consecutive ones in order (one
+//   read and one write per pixel for the run), each the
 //   reference's filter_color_pixel / filter_color_matrix_pixel
 //   (filter/color.hlsli:8-76) on the stored RGBA8 word. `mad` is an explicit
 //   fused multiply-add; every other product and sum is rounded on its own.
@@ -178,15 +180,27 @@ __device__ uint32_t color_matrix_pixel(const float* m, uint32_t pixel) {
                  f2u(clampf(rb, 0.0f, 255.0f) + 0.5f), f2u(clampf(out_a, 0.0f, 255.0f) + 0.5f));
 }
 
-__global__ void k_filter_color(uint32_t* surface, uint32_t width, int4 b, FilterArgs f) {
+// A run of consecutive per-pixel filters of a chain, applied in order to each
+// pixel in one pass (one read and one write per pixel for the whole run).
+constexpr uint32_t kFilterRun = 8;
+struct FilterRun {
+    uint32_t n;
+    FilterArgs f[kFilterRun];
+};
+
+__global__ void k_filter_color(uint32_t* surface, uint32_t width, int4 b, FilterRun run) {
     const uint32_t w = uint32_t(b.z - b.x);
     const uint64_t n = uint64_t(w) * uint32_t(b.w - b.y);
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
         const uint64_t o = uint64_t(b.y + uint32_t(i / w)) * width + uint32_t(b.x) + uint32_t(i % w);
-        const uint32_t p = surface[o];
-        surface[o] = f.kind == TK_FILTER_COLOR_MATRIX         ? color_matrix_pixel(f.m, p)
-                     : f.kind == TK_FILTER_COMPONENT_TRANSFER ? transfer_pixel(f.table, p)
-                                                              : color_filter_pixel(p, f.kind, f.amount);
+        uint32_t p = surface[o];
+        for (uint32_t k = 0; k < run.n; ++k) {
+            const FilterArgs& f = run.f[k];
+            p = f.kind == TK_FILTER_COLOR_MATRIX         ? color_matrix_pixel(f.m, p)
+                : f.kind == TK_FILTER_COMPONENT_TRANSFER ? transfer_pixel(f.table, p)
+                                                         : color_filter_pixel(p, f.kind, f.amount);
+        }
+        surface[o] = p;
     }
 }
 
@@ -492,10 +506,21 @@ void launch_filter_chain(uint32_t* surface, uint32_t* temp, uint32_t* temp2, con
             k_filter_morphology<<<filter_grid(n), 256, 0, st>>>(temp, surface, width, b, min(ry, sh - 1u), dilate,
                                                                  false);
         } else {
-            FilterArgs a{f.kind, f.amount, {}, nullptr};
-            for (int m = 0; m < 20; ++m) a.m[m] = f.matrix[m];
-            if (f.kind == TK_FILTER_COMPONENT_TRANSFER) a.table = tables + f.color;
-            k_filter_color<<<filter_grid(n), 256, 0, st>>>(surface, width, b, a);
+            // this filter and the per-pixel filters right after it, fused
+            FilterRun run{};
+            for (; k < count && run.n < kFilterRun; ++k) {
+                const tk_filter& g = chain[k];
+                if (g.kind < TK_FILTER_BRIGHTNESS || (g.kind > TK_FILTER_COLOR_MATRIX &&
+                                                      g.kind != TK_FILTER_COMPONENT_TRANSFER))
+                    break;
+                FilterArgs& a = run.f[run.n++];
+                a.kind = g.kind;
+                a.amount = g.amount;
+                for (int m = 0; m < 20; ++m) a.m[m] = g.matrix[m];
+                a.table = g.kind == TK_FILTER_COMPONENT_TRANSFER ? tables + g.color : nullptr;
+            }
+            --k;  // the loop's increment moves past the run's last filter
+            k_filter_color<<<filter_grid(n), 256, 0, st>>>(surface, width, b, run);
         }
     }
 }
